@@ -1,0 +1,316 @@
+/*
+ * rypath_cuda.h -- C ABI of the B200 spectral path-tracing backend.
+ *
+ * This is the boundary that replaces rypath's Metal render adapter.  The reference
+ * binds its renderer through C++ (`build_metal_renderer` / `MetalRenderScene::sample`,
+ * src/metal_render.hpp:14-95) behind the progressive driver's sample-source seam
+ * (`detail::RenderSampleSource`, src/render_driver.hpp:6-14).  Every entry point below is
+ * what a C++ adapter in the reference's tree calls instead of Objective-C++/Metal; the
+ * adapter itself is shown in INTEGRATION.md.
+ *
+ * Conventions (the reference's, src/metal_render.hpp:47-52 and src/render_driver.cpp:280-283):
+ *   - No exceptions cross the boundary: every call returns an rp_status and writes a
+ *     NUL-terminated diagnostic into (diag, diag_capacity) when one is supplied.
+ *   - A scene deep-copies everything it is given and retains no caller storage.
+ *   - Synchronous operations on one scene require external serialisation.
+ *   - Plain pointers and sizes only.  "host" pointers are CPU memory; "device" pointers
+ *     are CUDA global memory on the scene's device.
+ */
+#ifndef RYPATH_CUDA_H
+#define RYPATH_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RP_ABI_VERSION 1u
+#define RP_NONE 0xffffffffu
+#define RP_SPECTRUM_BINS 471u /* 360..830 nm at 1 nm, src/render.hpp:29-36 */
+#define RP_SOBOL_TABLE_BYTES 234208u /* sizeof(sobol::Tables), src/sobol_shared.h:42 */
+#define RP_MAX_DEPTH 64u        /* packet_wire::max_depth, src/packet_wire.h:12 */
+#define RP_MAX_POSITIONAL 64u   /* max_positional_lights, src/render.hpp:173 */
+
+/* Build / call status; mirrors GeometryStatus (src/metal_geometry.hpp:16). */
+typedef enum rp_status {
+    RP_SUCCESS = 0,
+    RP_NOT_BUILT = 1,
+    RP_NO_DEVICE = 2,
+    RP_NO_RAY_TRACING = 3,
+    RP_FAILURE = 4,
+    RP_INVALID_ARGUMENT = 5
+} rp_status;
+
+/* Per-lane sample status; render_wire status codes (src/render_wire.h:20-26). */
+enum {
+    RP_SAMPLE_SUCCESS = 0,
+    RP_SAMPLE_EMERGENCY_DEPTH = 1,
+    RP_SAMPLE_INVALID_ARITHMETIC = 2,
+    RP_SAMPLE_INVALID_HIT = 3,
+    RP_SAMPLE_BOUNDARY_EXHAUSTION = 4
+};
+
+/* Sampler kinds and Sobol randomisations (src/render_wire.h:40, src/sobol_shared.h:26-34). */
+enum { RP_SAMPLER_INDEPENDENT = 0, RP_SAMPLER_SOBOL = 1 };
+enum { RP_RANDOMIZE_NONE = 0, RP_RANDOMIZE_PERMUTEDIGITS = 1, RP_RANDOMIZE_FASTOWEN = 2,
+       RP_RANDOMIZE_OWEN = 3 };
+/* Pixel filters (src/render_wire.h:29). */
+enum { RP_FILTER_BOX = 0, RP_FILTER_TRIANGLE = 1 };
+/* Scattering families (wire::Material::scattering, src/render_wire.h:121). */
+enum { RP_DIFFUSE = 0, RP_CONDUCTOR = 1, RP_DIELECTRIC = 2 };
+/* Reflectance sources (src/render_wire.h:41-48). */
+enum { RP_REFLECTANCE_KNOTS = 0, RP_REFLECTANCE_CONSTANT = 1, RP_REFLECTANCE_BLACKBODY = 4 };
+/* Positional light kinds (src/render_wire.h:200). */
+enum { RP_POINT_LIGHT = 0, RP_SPOT_LIGHT = 1 };
+/* Light selection (LightSamplerKind, src/render.hpp:217; wire word src/render_wire.h:304). */
+enum { RP_LIGHTS_BVH = 0, RP_LIGHTS_POWER = 1, RP_LIGHTS_UNIFORM = 2 };
+/* Spectral transport (SpectralTransport, src/render.hpp:218). */
+enum { RP_TRANSPORT_SCALAR = 0, RP_TRANSPORT_HERO = 2 };
+/* Hero wavelength sampling (HeroWavelengthSampling, src/render.hpp:220). */
+enum { RP_HERO_UNIFORM = 0, RP_HERO_VISIBLE = 1 };
+
+typedef struct rp_knot { float wavelength, value; } rp_knot; /* wire::SpectralKnot */
+
+/* One mesh placement; the subset of wire::Instance (src/render_wire.h:168-188) the hot
+ * path reads.  matrix is row-major 3x4 object-to-world. */
+typedef struct rp_instance {
+    float matrix[12];
+    uint32_t vertex_begin, triangle_begin, triangle_count;
+    uint32_t material;
+    uint32_t reverse_orientation;
+    uint32_t emission;     /* index into emissions or RP_NONE */
+    uint32_t normal_begin; /* index into normals or RP_NONE */
+    uint32_t inside_medium, outside_medium; /* RP_NONE = vacuum */
+} rp_instance;
+
+/* The subset of wire::Material (src/render_wire.h:107-130) used by diffuse, conductor and
+ * dielectric scattering with sampled / constant / blackbody reflectance. */
+typedef struct rp_material {
+    uint32_t scattering;   /* RP_DIFFUSE / RP_CONDUCTOR / RP_DIELECTRIC */
+    uint32_t kind;         /* RP_REFLECTANCE_* */
+    uint32_t knot_begin, knot_count; /* reflectance knots */
+    float scalar_value;    /* constant reflectance or blackbody C2/T factor */
+    uint32_t eta_begin, eta_count, k_begin, k_count;
+    uint32_t optical_extensions; /* bit 0: extend eta endpoints, bit 1: extend k */
+    float u_roughness, v_roughness;
+    uint32_t remap_roughness;
+} rp_material;
+
+typedef struct rp_area_emission { /* wire::AreaEmission subset, src/render_wire.h:219 */
+    float radiance[RP_SPECTRUM_BINS];
+    uint32_t two_sided;
+} rp_area_emission;
+
+typedef struct rp_positional_light { /* PointLight / SpotLight, src/render.hpp:178-191 */
+    float position[3];
+    float intensity[RP_SPECTRUM_BINS];
+    uint32_t kind; /* RP_POINT_LIGHT / RP_SPOT_LIGHT */
+    float light_from_world[9]; /* row-major; spot axis is +z after this map */
+    float cos_falloff_start, cos_falloff_end;
+} rp_positional_light;
+
+typedef struct rp_medium { /* HomogeneousMedium, src/render.hpp:29-36 */
+    float sigma_a[RP_SPECTRUM_BINS];
+    float sigma_s[RP_SPECTRUM_BINS];
+    float emission[RP_SPECTRUM_BINS];
+    float g;
+} rp_medium;
+
+/* PBRT raster camera (RasterCamera, src/render.hpp:152-157): a primary direction is
+ * corner + x*dx + y*dy at normalised raster (x, y). */
+typedef struct rp_camera {
+    float origin[3], corner[3], dx[3], dy[3];
+} rp_camera;
+
+/* Everything build_metal_renderer reads from a RenderScene on the PT/hero path
+ * (src/metal_render.mm:147-290, :505-700).  Arrays are host memory. */
+typedef struct rp_scene_desc {
+    uint32_t abi_version; /* RP_ABI_VERSION */
+    uint32_t vertex_count;   const float *positions;   /* xyz per vertex (object space) */
+    uint32_t normal_count;   const float *normals;     /* xyz per normal, may be 0 */
+    uint32_t triangle_count; const uint32_t *triangles; /* 3 vertex indices per triangle */
+    uint32_t instance_count; const rp_instance *instances;
+    uint32_t material_count; const rp_material *materials;
+    uint32_t knot_count;     const rp_knot *knots;
+    uint32_t emission_count; const rp_area_emission *emissions;
+    uint32_t positional_count; const rp_positional_light *positional;
+    uint32_t medium_count;   const rp_medium *media;
+    uint32_t camera_medium;  /* RP_NONE = vacuum camera */
+    const float *environment; /* RP_SPECTRUM_BINS constant environment radiance, or NULL */
+    rp_camera camera;
+    uint32_t filter_kind; float filter_x_radius, filter_y_radius;
+    uint32_t max_depth;
+    uint32_t light_sampler;    /* RP_LIGHTS_* */
+    uint32_t transport;        /* RP_TRANSPORT_HERO (scalar volpath: RP_TRANSPORT_SCALAR) */
+    uint32_t hero_wavelengths; /* RP_HERO_* */
+    const void *sobol_tables;  /* RP_SOBOL_TABLE_BYTES, sobol::Tables layout */
+} rp_scene_desc;
+
+/* RenderRequest (src/metal_render.hpp:14-32). */
+typedef struct rp_request {
+    uint32_t width, height;
+    uint64_t seed;
+    int32_t material_seed;
+    uint32_t pixel_begin, pixel_count;
+    uint64_t sample_begin;
+    uint32_t sample_count;
+    uint32_t emergency_limit;  /* render_emergency_limit = 1024 */
+    uint32_t sampler_kind;     /* RP_SAMPLER_* */
+    uint32_t randomization;    /* RP_RANDOMIZE_* */
+    uint32_t boundary_limit;   /* medium_boundary_limit = 4096 */
+} rp_request;
+
+/* packet_wire::Result, 80 bytes (src/packet_wire.h:13-18). */
+typedef struct rp_packet_result {
+    uint32_t status, pixel, sample_low, sample_high, splat_count;
+    float wavelengths[4], wavelength_pdfs[4], radiance[4];
+    float filter_weight;
+    uint32_t reserved[2];
+} rp_packet_result;
+
+/* render_wire::Sample-derived scalar output (RenderSample, src/render.hpp:285-294). */
+typedef struct rp_scalar_result {
+    uint32_t status, pixel, sample_low, sample_high;
+    float wavelength, radiance;
+    uint32_t scatterings;
+    uint32_t random_words[4];
+} rp_scalar_result;
+
+/* MetalDeviceInfo analogue. */
+typedef struct rp_device_info {
+    char name[128];
+    int device, sm_count, major, minor;
+    uint64_t total_memory;
+} rp_device_info;
+
+/* Device film: per-pixel FP64 Neumaier sums in canonical (absolute sample, pixel) order,
+ * the reduction PacketFilmBatch::add performs on the host (src/packet_film.cpp:198-265),
+ * plus per-pixel second moments of the XYZ estimate for the 3-sigma statistics. */
+typedef struct rp_film_pixel {
+    double sum[3], correction[3];
+    double weight_sum, weight_correction;
+    double square[3];
+    uint64_t count;
+} rp_film_pixel;
+
+/* Film request: render samples [sample_begin, sample_begin + sample_count) for every pixel,
+ * batch_size absolute samples per launch (RenderSettings, src/render.hpp:240-248). */
+typedef struct rp_film_request {
+    uint32_t width, height;
+    uint64_t seed;
+    uint64_t sample_begin, sample_count, batch_size;
+    uint32_t sampler_kind, randomization;
+    uint32_t emergency_limit;
+} rp_film_request;
+
+/* Kernel-level timing of the last call on a scene (CUDA events on the scene stream). */
+typedef struct rp_timing {
+    double total_ms;          /* whole call, device time */
+    double trace_ms;          /* closest-hit traversal kernels */
+    double shadow_ms;         /* any-hit traversal kernels */
+    double shade_ms;          /* shading kernels */
+    double other_ms;          /* raygen, queue resets, film */
+    uint64_t closest_rays, shadow_rays, kernel_launches, samples;
+    uint64_t nodes_visited, triangles_tested; /* only when counting is enabled */
+} rp_timing;
+
+/* ---- device and lifetime ------------------------------------------------------------ */
+
+/* Device probe; MetalDeviceInfo in build_metal_renderer (src/metal_render.hpp:76-77). */
+rp_status rp_cuda_device_info(int device, rp_device_info *info, char *diag, size_t diag_capacity);
+
+/* build_metal_renderer(const RenderScene&, library, RenderBuildOptions, RenderTimings*)
+ * (src/metal_render.hpp:84-95; stub src/metal_render_stub.cpp:14-50).  Uploads the scene,
+ * builds the LBVH on the device and the light-selection tables on the host.  On failure
+ * *scene is NULL and diag says why. */
+rp_status rp_cuda_scene_create(const rp_scene_desc *desc, int device, struct rp_scene **scene,
+                               char *diag, size_t diag_capacity);
+/* ~MetalRenderScene (src/metal_render.hpp:56). */
+void rp_cuda_scene_destroy(struct rp_scene *scene);
+
+/* ---- sampling (driver-compatible) ----------------------------------------------------- */
+
+/* MetalRenderScene::sample(const RenderRequest&) for the packet/hero transport
+ * (src/metal_render.hpp:56-57; body src/metal_render.mm:1940-2170).  Host output: one
+ * 80-byte packet result per lane, lane order, pixel = pixel_begin + lane % pixel_count,
+ * sample = sample_begin + lane / pixel_count.  capacity is in results.  A nonzero per-lane
+ * status is reported as RP_FAILURE with a diagnostic, as the reference does
+ * (src/metal_render.mm:2058-2064); the results are still written. */
+rp_status rp_cuda_sample(struct rp_scene *scene, const rp_request *request,
+                         rp_packet_result *host_results, size_t capacity, char *diag,
+                         size_t diag_capacity);
+/* Same, device output, asynchronous on `stream` (a cudaStream_t, NULL = the scene stream);
+ * results are complete when the stream is. */
+rp_status rp_cuda_sample_device(struct rp_scene *scene, const rp_request *request,
+                                rp_packet_result *device_results, size_t capacity,
+                                void *stream, char *diag, size_t diag_capacity);
+/* Scalar (one-wavelength) PT / volpath lanes: rypath_render_paths
+ * (shaders/render.metal:2299-2371), RenderSample output (src/metal_render.mm:2136-2166). */
+rp_status rp_cuda_sample_scalar(struct rp_scene *scene, const rp_request *request,
+                                rp_scalar_result *host_results, size_t capacity, char *diag,
+                                size_t diag_capacity);
+
+/* ---- device film ---------------------------------------------------------------------- */
+
+/* Progressive render into a device film: the loop of drive_progressive
+ * (src/render_driver.cpp:166-275) with the packet film reduction of PacketFilmBatch
+ * (src/packet_film.cpp:198-265) done on the device.  film (host, width*height pixels) is
+ * read as the committed state and overwritten with the new one; a failed batch leaves it
+ * unchanged (src/render_driver.cpp:201-214). */
+rp_status rp_cuda_render_film(struct rp_scene *scene, const rp_film_request *request,
+                              rp_film_pixel *host_film, char *diag, size_t diag_capacity);
+/* Same with the film resident on the device (no host copies). */
+rp_status rp_cuda_render_film_device(struct rp_scene *scene, const rp_film_request *request,
+                                     rp_film_pixel *device_film, char *diag,
+                                     size_t diag_capacity);
+
+/* ---- instrumentation ------------------------------------------------------------------ */
+
+/* Timing of the last sample/film call on this scene. */
+rp_status rp_cuda_last_timing(struct rp_scene *scene, rp_timing *timing);
+/* Enable (1) or disable (0) exact node/triangle visit counting in traversal. */
+rp_status rp_cuda_set_counting(struct rp_scene *scene, int enabled);
+
+/* ---- fixed-input probes (the reference's rypath_*_probe kernels) ------------------------ */
+
+/* rypath_sobol_probe (shaders/render.metal:74-93): per query {m, x, y, sample_lo,
+ * sample_hi, dimension, mode, seed} -> {index_lo, index_hi, word, hash, uniform bits,
+ * camera uniform bits}.  8 words in, 6 words out per query; tables from the scene. */
+rp_status rp_cuda_probe_sobol(const void *sobol_tables, const uint32_t *queries, uint32_t count,
+                              uint32_t *results, char *diag, size_t diag_capacity);
+/* Philox4x32-10 (shaders/render.metal:97-109): 6 words in {counter[4], key[2]}, 4 out. */
+rp_status rp_cuda_probe_philox(const uint32_t *queries, uint32_t count, uint32_t *results,
+                               char *diag, size_t diag_capacity);
+/* Hero wavelengths (src/hero_spectrum_shared.h:199-244): u -> lambda[4], pdf[4]. */
+rp_status rp_cuda_probe_wavelengths(const float *u, uint32_t count, uint32_t mode,
+                                    float *results, char *diag, size_t diag_capacity);
+/* Begin-sample words (shaders/render.metal:238-311) for a request: per lane
+ * {pixel, sample_lo, sample_hi, index_lo, index_hi, words[4], lens[2]} (11 words) and the
+ * primary ray {origin[3], direction[3]} (6 floats). */
+rp_status rp_cuda_probe_raygen(struct rp_scene *scene, const rp_request *request,
+                               uint32_t *words, float *rays, size_t capacity, char *diag,
+                               size_t diag_capacity);
+/* BSDF probes (shaders/conductor.h, dielectric.h, transmission.h): per query 16 floats
+ * {kind, p0..p4, wo[3], wi[3], uc, u[2], pad} -> 12 floats {f, pdf, valid, sample wi[3],
+ * weight, sample pdf, flags, eta, pad, pad}. */
+rp_status rp_cuda_probe_bsdf(const float *queries, uint32_t count, float *results, char *diag,
+                             size_t diag_capacity);
+/* Export the scene's binary LBVH: per internal node {left, right, parent} (n-1 nodes,
+ * child index >= n-1 means leaf n-1+i... see DESIGN), leaf order (n triangle ids),
+ * sorted Morton keys (n) and node bounds (2n-1 boxes of 6 floats). */
+rp_status rp_cuda_scene_export_bvh(struct rp_scene *scene, uint32_t *nodes, uint32_t *leaf_order,
+                                   uint64_t *keys, float *bounds, size_t capacity, char *diag,
+                                   size_t diag_capacity);
+/* Closest-hit (any_hit == 0) or occlusion (any_hit == 1) queries for host rays
+ * {origin[3], direction[3], tmax} (7 floats each) -> {t, b1, b2, primitive bits} (4 floats;
+ * primitive RP_NONE bits = miss).  For occlusion only field 0 (1 = occluded) is used. */
+rp_status rp_cuda_trace_rays(struct rp_scene *scene, const float *rays, uint32_t count,
+                             int any_hit, float *hits, char *diag, size_t diag_capacity);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RYPATH_CUDA_H */

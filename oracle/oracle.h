@@ -1,0 +1,61 @@
+/* ORACLE -- test infrastructure only.  C ABI of the CPU restatement of rypath's spectral
+ * path-tracing hot path.  Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline
+ * leg load this library, and only as the checker / CPU baseline. */
+#ifndef RYPATH_ORACLE_H
+#define RYPATH_ORACLE_H
+
+#include "../include/rypath_cuda.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct or_scene or_scene;
+
+/* Deep copy of a scene description; builds the light tables and the CPU LBVH. */
+or_scene *or_scene_create(const rp_scene_desc *desc, char *diag, size_t diag_capacity);
+void or_scene_destroy(or_scene *scene);
+uint32_t or_scene_light_count(const or_scene *scene);
+
+/* Hero packet lanes of a request (rypath_render_packets), threads <= 0: all cores. */
+int or_sample(const or_scene *scene, const rp_request *request, rp_packet_result *results,
+              size_t capacity, int threads);
+
+/* Probes mirroring rp_cuda_probe_* (same layouts). */
+void or_probe_sobol(const void *tables, const uint32_t *queries, uint32_t count, uint32_t *results);
+void or_probe_philox(const uint32_t *queries, uint32_t count, uint32_t *results);
+void or_probe_wavelengths(const float *u, uint32_t count, uint32_t mode, float *results);
+int or_probe_raygen(const or_scene *scene, const rp_request *request, uint32_t *words, float *rays,
+                    size_t capacity);
+void or_probe_bsdf(const float *queries, uint32_t count, float *results);
+
+/* LBVH export in the rp_cuda_scene_export_bvh layout. */
+int or_export_bvh(const or_scene *scene, uint32_t *nodes, uint32_t *leaf_order, uint64_t *keys,
+                  float *bounds, size_t capacity);
+/* Ray queries in the rp_cuda_trace_rays layout; brute != 0 scans every triangle. */
+void or_trace_rays(const or_scene *scene, const float *rays, uint32_t count, int any_hit, int brute,
+                   float *hits);
+
+/* Hero likelihood arithmetic probes (src/hero_spectrum_shared.h): per query 12 floats
+ * {prefix frac[4] as floats, prefix exponent[4] as floats, beta[4]} plus 8 more
+ * {numerator[4], pdf[4]} -> {beta'[4], density frac[4], density exp[4], valid}. */
+void or_probe_advance(const float *queries, uint32_t count, float *results);
+
+/* Light selection tables: lights as LightInput rows of 16 doubles
+ * {power, bounds_power, low[3], high[3], direction[3], cos_outer, cos_emission, two_sided,
+ * infinite, pad} -> alias (4 words each), records (4 words each), nodes (16 words each),
+ * infinite ids.  Returns the node count, or -1. */
+int or_build_light_tables(const double *rows, uint32_t count, uint32_t *alias, uint32_t *records,
+                          uint32_t *nodes, uint32_t *infinite, uint32_t *infinite_count);
+
+/* Light selection probe: queries {px,py,pz,nx,ny,nz,u,id} -> {light bits, pmf, pmf(id)}. */
+void or_probe_light_select(const or_scene *scene, const float *queries, uint32_t count, float *results);
+
+/* Film reduction of packet results in canonical order (PacketFilmBatch::add). */
+int or_film_add(const rp_packet_result *results, size_t count, const double *cie_xyz,
+                uint32_t pixel_count, rp_film_pixel *film);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1009 @@
+// ORACLE -- test infrastructure only (see oracle_math.hpp).  The hero-wavelength path
+// tracer of rypath_render_packets (shaders/render.metal:2424-2469), one lane at a time.
+#include "oracle.h"
+#include "oracle_scene.hpp"
+
+#include <atomic>
+#include <cstdio>
+#include <memory>
+#include <thread>
+
+namespace oracle {
+
+struct Params {
+    u32 width, height, pixel_begin, pixel_count, sample_low, sample_high;
+    u32 seed_low, seed_high, sampler, randomization, m, emergency_limit, max_depth;
+};
+
+struct Sample {
+    u32 status = 0, pixel = 0, sample_low = 0, sample_high = 0;
+    u32 words[4] = {0, 0, 0, 0};
+};
+
+// shaders/render.metal:113-118 (sobol and independent samplers)
+static float sample_uniform(const Params &p, u32 w) {
+    return p.sampler == RP_SAMPLER_INDEPENDENT ? u01(w) : sobol_uniform(w);
+}
+// shaders/render.metal:154-179 (draw_words)
+static U4 draw_words(const Scene &s, const Params &p, const Sample &smp, u64 index, u32 block) {
+    if (p.sampler == RP_SAMPLER_INDEPENDENT)
+        return philox(U4{smp.pixel, smp.sample_low, smp.sample_high, block}, p.seed_low, p.seed_high);
+    const u32 d = 4 * block;
+    const SobolTables &t = *s.sobol;
+    return U4{sobol_word(t, index, d, p.randomization, p.seed_low),
+              sobol_word(t, index, d + 1, p.randomization, p.seed_low),
+              sobol_word(t, index, d + 2, p.randomization, p.seed_low),
+              sobol_word(t, index, d + 3, p.randomization, p.seed_low)};
+}
+// shaders/render.metal:238-311 (begin_sample; pinhole, box/triangle filter)
+static Sample begin_sample(const Scene &s, const Params &p, u32 lane, u64 &index) {
+    Sample r;
+    r.pixel = p.pixel_begin + lane % p.pixel_count;
+    r.sample_low = p.sample_low + lane / p.pixel_count;
+    r.sample_high = p.sample_high + u32(r.sample_low < p.sample_low);
+    const u64 sample = (u64(r.sample_high) << 32) | r.sample_low;
+    if (p.sampler == RP_SAMPLER_SOBOL) {
+        const SobolTables &t = *s.sobol;
+        index = sobol_index(t, p.m, r.pixel % p.width, r.pixel / p.width, sample);
+        r.words[0] = sobol_word(t, index, 0, 0, 0);
+        r.words[1] = sobol_word(t, index, 1, 0, 0);
+        r.words[2] = sobol_word(t, index, 2, p.randomization, p.seed_low);
+        r.words[3] = sobol_word(t, index, 3, p.randomization, p.seed_low);
+    } else {
+        index = 0;
+        const U4 w = philox(U4{r.pixel, r.sample_low, r.sample_high, 0}, p.seed_low, p.seed_high);
+        r.words[0] = w.x;
+        r.words[1] = w.y;
+        r.words[2] = w.z;
+        r.words[3] = w.w;
+    }
+    return r;
+}
+// shaders/render.metal:352-357
+static float triangle_offset(float u, float radius) {
+    const float s = 2.0f * u - 1.0f;
+    return radius * (s / (1.0f + std::sqrt(1.0f - std::fabs(s))));
+}
+// shaders/render.metal:341-350, :400-476 (primary_ray, PBRT model, no lens)
+static void primary_ray(const Scene &s, const Params &p, const Sample &smp, F3 &o, F3 &d) {
+    float ux, uy;
+    if (p.sampler == RP_SAMPLER_SOBOL) {
+        ux = sobol_camera_uniform(smp.words[0], p.m, smp.pixel % p.width);
+        uy = sobol_camera_uniform(smp.words[1], p.m, smp.pixel / p.width);
+    } else {
+        ux = sample_uniform(p, smp.words[0]);
+        uy = sample_uniform(p, smp.words[1]);
+    }
+    o = s.origin;
+    const bool centered = s.filter_kind != RP_FILTER_BOX || s.filter_x != 0.5f || s.filter_y != 0.5f;
+    if (centered) {
+        const float ox = s.filter_kind == RP_FILTER_TRIANGLE ? triangle_offset(ux, s.filter_x)
+                                                             : (2.0f * ux - 1.0f) * s.filter_x;
+        const float oy = s.filter_kind == RP_FILTER_TRIANGLE ? triangle_offset(uy, s.filter_y)
+                                                             : (2.0f * uy - 1.0f) * s.filter_y;
+        const float x = ((float(smp.pixel % p.width) + 0.5f) + ox) / float(p.width);
+        const float y = ((float(smp.pixel / p.width) + 0.5f) + oy) / float(p.height);
+        const F3 dd = fma3(F3{y, y, y}, s.up, fma3(F3{x, x, x}, s.right, s.forward));
+        const float scale = std::max(std::fabs(dd.x), std::max(std::fabs(dd.y), std::fabs(dd.z)));
+        if (!finite3(dd) || !(scale > 0.0f)) {
+            d = F3{NAN, NAN, NAN};
+            return;
+        }
+        const F3 scaled = dd / scale;
+        if (!finite3(scaled) || zero3(scaled)) {
+            d = F3{NAN, NAN, NAN};
+            return;
+        }
+        d = normalize3(scaled);
+        return;
+    }
+    const float x = (float(smp.pixel % p.width) + ux) / float(p.width);
+    const float y = (float(smp.pixel / p.width) + uy) / float(p.height);
+    const F3 dd = s.forward + x * s.right + y * s.up;
+    const float scale = std::max(std::fabs(dd.x), std::max(std::fabs(dd.y), std::fabs(dd.z)));
+    d = normalize3(dd / scale);
+}
+
+// ---------------------------------------------------------------- vertices
+enum : u32 { camera_vertex = 0, surface_vertex = 1, light_vertex = 2, environment_vertex = 3 };
+struct Vertex {
+    u32 type = camera_vertex;
+    SurfacePoint point;
+    Frame frame{};
+    HeroBsdf bsdf{};
+    F4 beta;
+    F3 wo;
+    float u = 0, v = 0;
+    u32 instance = RP_NONE, primitive = 0, light = RP_NONE;
+    bool pair_valid = false, delta = false, connectible = false, delta_light = false;
+    F3 sampled_wo_local, sampled_wi_local;
+};
+inline bool infinite(const Vertex &v) { return v.type == environment_vertex; }
+inline bool on_surface(const Vertex &v) { return any_nonzero3(v.point.geometric_normal); }
+
+// shaders/packet_transport.h:77-83
+static F3 offset(const Vertex &v, F3 direction) {
+    if (!on_surface(v))
+        return v.point.position;
+    const F3 n = dot(direction, v.point.geometric_normal) < 0 ? -v.point.geometric_normal
+                                                              : v.point.geometric_normal;
+    return round_out(v.point.position + dot(fabs3(n), v.point.error) * n, n);
+}
+
+// shaders/packet_walk.h:22-57 (packet_reflectance) for sampled/constant/blackbody
+static bool reflectance(const Scene &s, const Material &m, float w, float &rho) {
+    if (m.scattering != 0) {
+        rho = 1;
+    } else if (m.kind == RP_REFLECTANCE_KNOTS && m.knot_count >= 2 &&
+               m.knot_begin <= s.knots.size() && m.knot_count <= s.knots.size() - m.knot_begin) {
+        rho = pbrt_reflectance(s.knots.data() + m.knot_begin, m.knot_count, w);
+    } else if (m.kind == RP_REFLECTANCE_CONSTANT) {
+        rho = m.scalar_value;
+    } else if (m.kind == RP_REFLECTANCE_BLACKBODY) {
+        rho = blackbody_reflectance(m.scalar_value, w);
+    } else
+        return false;
+    return std::isfinite(rho) && rho >= 0 && rho <= 1;
+}
+// shaders/hero_current_bsdf.h:72-101 with prepare_scattering (shaders/render.metal:2079-2160)
+static bool prepare_bsdf(const Scene &s, const Material &m, const Wavelengths &l, u32 mask,
+                         HeroBsdf &out) {
+    out = HeroBsdf{};
+    out.active_mask = mask;
+    for (int k = 0; k < 4; ++k) {
+        LaneBsdf lane{};
+        lane.kind = m.scattering;
+        if (!(mask & (1u << k))) {
+            out.lane[k] = lane;
+            continue;
+        }
+        float rho;
+        if (!reflectance(s, m, l.lambda[k], rho))
+            return false;
+        if (m.scattering == 0) {
+            lane.reflectance = rho;
+        } else {
+            const u32 total = u32(s.knots.size());
+            const float eta = optical_value(s.knots.data(), m.eta_begin, m.eta_count, total,
+                                            (m.optical_extensions & 1u) != 0, l.lambda[k]);
+            const float kk = optical_value(s.knots.data(), m.k_begin, m.k_count, total,
+                                           (m.optical_extensions & 2u) != 0, l.lambda[k]);
+            if (m.scattering == 1) {
+                if (!conductor_prepare(eta, kk, m.u_roughness, m.v_roughness, m.remap != 0, lane.conductor))
+                    return false;
+            } else if (m.scattering == 2) {
+                if (!dielectric_prepare(eta, m.u_roughness, m.v_roughness, m.remap != 0, lane.dielectric))
+                    return false;
+            } else
+                return false;
+        }
+        out.lane[k] = lane;
+    }
+    // hero_current_structure (shaders/hero_current_bsdf.h:9-14)
+    return (mask & 1u) && !(mask & ~15u) && m.scattering <= 2;
+}
+
+// ---------------------------------------------------------------- emission
+// shaders/render.metal:1811-1830 (area_radiance, plain spectrum)
+static bool emitted(const Scene &s, const Vertex &v, F3 direction, const Wavelengths &l, F4 &rad) {
+    if (infinite(v)) {
+        for (int k = 0; k < 4; ++k)
+            rad[k] = s.environment[dense_index(l.lambda[k])];
+        return finite_nonnegative4(rad);
+    }
+    rad = f4(0);
+    if (v.instance >= s.instances.size())
+        return true;
+    const Instance &in = s.instances[v.instance];
+    if (in.emission == RP_NONE)
+        return true;
+    if (!s.emission_two_sided[in.emission] && dot(v.point.geometric_normal, direction) <= 0)
+        return true;
+    for (int k = 0; k < 4; ++k)
+        rad[k] = v.point.inverse_area_pdf == 0 ? 0.f : s.emission[in.emission][dense_index(l.lambda[k])];
+    return finite_nonnegative4(rad);
+}
+
+// ---------------------------------------------------------------- positional lights
+// shaders/render.metal:654-657, :682-697
+static bool normal_or_zero(float v) {
+    const u32 m = fbits(v) & 0x7fffffffu;
+    return m == 0 || (m >= 0x00800000u && m < 0x7f800000u);
+}
+static bool spot_product(float a, float b, float &r) {
+    if (a != 0 && b != 0 && std::fabs(a) < FLT_MIN / std::fabs(b))
+        return false;
+    r = a * b;
+    return normal_or_zero(r) && (r != 0 || a == 0 || b == 0);
+}
+static bool spot_sum(float a, float b, float &r) {
+    r = a + b;
+    return normal_or_zero(r) && (r != 0 || a == -b);
+}
+static bool spot_divide(float a, float b, float &r) {
+    r = a / b;
+    return normal_or_zero(r) && (r != 0 || a == 0);
+}
+// shaders/render.metal:699-811 (positional_intensity, point and spot)
+static bool positional_intensity(const Positional &L, F3 wi, float &intensity) {
+    if (L.kind == RP_POINT_LIGHT)
+        return true;
+    if (L.kind != RP_SPOT_LIGHT)
+        return false;
+    F3 w;
+    for (int row = 0; row < 3; ++row) {
+        float terms[3];
+        for (int col = 0; col < 3; ++col)
+            if (!spot_product(L.light_from_world[row * 3 + col], -wi[col], terms[col]))
+                return false;
+        float sum, comp;
+        if (!spot_sum(terms[0], terms[1], sum) || !spot_sum(sum, terms[2], comp))
+            return false;
+        w[row] = comp;
+    }
+    const float scale = std::max(std::max(std::fabs(w.x), std::fabs(w.y)), std::fabs(w.z));
+    if (!(scale >= FLT_MIN) || !std::isfinite(scale))
+        return false;
+    for (int i = 0; i < 3; ++i) {
+        float c;
+        if (!spot_divide(w[i], scale, c))
+            return false;
+        w[i] = c;
+    }
+    float cosine;
+    if (!spot_divide(w.z, std::sqrt(dot(w, w)), cosine))
+        return false;
+    const float end = L.cos_falloff_end, start = L.cos_falloff_start;
+    const float t = start == end ? (cosine < end ? 0.0f : 1.0f)
+                                 : std::clamp((cosine - end) / (start - end), 0.0f, 1.0f);
+    const float falloff = start == end ? t : t * t * (3.0f - 2.0f * t);
+    intensity *= falloff;
+    return std::isfinite(intensity) && intensity >= 0;
+}
+
+// ---------------------------------------------------------------- lane state
+struct LaneState {
+    Vertex latest;
+    F3 preceding_position{};
+    u32 preceding_type = 0;
+    Sample sample;
+    Wavelengths lambda{};
+    F4 radiance, beta;
+    F3 ray_o, ray_d;
+    HeroTrack hero;
+    u64 index = 0;
+    u32 count = 1, crossings = 0;
+    bool complete = false;
+};
+
+struct Ctx {
+    const Scene &s;
+    const Bvh &bvh;
+    const Params &p;
+};
+
+// shaders/hero_pt_helpers.h:122-132 (hero_represented_pdf)
+static F4 represented_pdf(const Vertex &v, const Vertex &previous, const Vertex &next) {
+    const F3 before = infinite(previous) ? -previous.point.geometric_normal
+                                         : previous.point.position - v.point.position;
+    const F3 after = infinite(next) ? -next.point.geometric_normal : next.point.position - v.point.position;
+    if (zero3(before) || zero3(after))
+        return f4(0);
+    const HeroEval e = hero_evaluate(v.bsdf, v.frame.local(normalize3(before)), v.frame.local(normalize3(after)));
+    return e.valid ? e.pdf : f4(NAN);
+}
+// shaders/hero_pt_helpers.h:133-148
+static F4 hero_weight(Sample &smp, const Density &prefix, F4 value, F4 sampled, F4 other) {
+    if (!finite_nonnegative4(value) || !finite_nonnegative4(sampled) || !finite_nonnegative4(other)) {
+        smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+        return f4(0);
+    }
+    if (mixture(prefix, other).fraction == 0)
+        return value;
+    const auto r = balance_contribution(prefix, value, sampled, other);
+    if (!r.valid) {
+        smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+        return f4(0);
+    }
+    return r.value;
+}
+// shaders/packet_transport.h:740-758 (direct_pdf / hero_history_light_pdf)
+static float light_pdf(const Ctx &c, const Vertex &from, const Vertex &light) {
+    const float selection = light_pmf(c.s, from.point.position, from.point.shading_normal, light.light);
+    if (infinite(light))
+        return 0.0f * selection; // environment_pdf is 0 for unidirectional PT
+    const F3 delta = light.point.position - from.point.position;
+    if (!(dot(delta, delta) > 0))
+        return 0;
+    if (!on_surface(light))
+        return 0;
+    const u32 emitter = light.light; // area emitters occupy the first light slots
+    return selection * light_geometry_pdf(c.s, emitter, from.point.position, from.point.shading_normal,
+                                          light.point);
+}
+// shaders/hero_pt_helpers.h:157-184
+static F4 hero_endpoint(const Ctx &c, Sample &smp, const Wavelengths &l, const Vertex &pt,
+                        const Vertex &previous, const Vertex &before, u32 t, const Density &prev_density) {
+    F4 rad;
+    bool ok;
+    if (infinite(pt))
+        ok = emitted(c.s, pt, -pt.point.geometric_normal, l, rad);
+    else {
+        const F3 delta = previous.point.position - pt.point.position;
+        if (zero3(delta)) {
+            rad = f4(0);
+            ok = true;
+        } else
+            ok = emitted(c.s, pt, normalize3(delta), l, rad);
+    }
+    if (!ok) {
+        smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+        return f4(0);
+    }
+    const F4 value = pt.beta * rad;
+    if (t <= 2 || previous.delta || !nonzero4(value))
+        return value;
+    const F4 bsdf_pdf = represented_pdf(previous, before, pt);
+    const float lp = light_pdf(c, previous, pt);
+    return hero_weight(smp, prev_density, value, bsdf_pdf, f4(lp));
+}
+// shaders/packet_transport.h:377-446 (visible; opaque surfaces only)
+static bool visible(const Ctx &c, const Vertex &a, const Vertex &b) {
+    const F3 direction = b.point.position - a.point.position;
+    if (zero3(direction))
+        return false;
+    const F3 origin = offset(a, direction);
+    const F3 target = offset(b, -direction);
+    return !trace_any(c.s, c.bvh, origin, target - origin, 0x1.fffffep-1f);
+}
+// shaders/packet_transport.h:470-553 (sample_li): area emitters and positional lights
+static bool sample_li(const Ctx &c, const Vertex &ref, const Wavelengths &l, float u0, float u1, float u2,
+                      Vertex &v, F3 &direction, float &pdf) {
+    const Scene &s = c.s;
+    const auto choice = light_sample(s, ref.point.position, ref.point.shading_normal, u0);
+    const u32 sel = choice.light;
+    v = Vertex{};
+    v.type = light_vertex;
+    v.light = sel;
+    v.connectible = true;
+    if (!(choice.pmf > 0)) {
+        v.beta = f4(0);
+        pdf = 0;
+        return true;
+    }
+    const u32 emitter_count = u32(s.emitters.size());
+    const u32 positional_count = u32(s.positional.size());
+    F4 rad;
+    if (sel < emitter_count) {
+        const auto &e = s.emitters[sel];
+        v.instance = e.instance;
+        v.primitive = e.primitive;
+        if (!light_geometry_sample(s, sel, ref.point.position, ref.point.shading_normal, u1, u2, v.u,
+                                   v.v, v.point, pdf))
+            return false;
+        pdf *= choice.pmf;
+        if (v.point.inverse_area_pdf == 0) {
+            v.beta = f4(0);
+            pdf = 0;
+            return true;
+        }
+        const F3 delta = v.point.position - ref.point.position;
+        const float d2 = dot(delta, delta);
+        if (!(d2 > 0)) {
+            v.beta = f4(0);
+            pdf = 0;
+            return true;
+        }
+        direction = delta * (1.0f / std::sqrt(d2));
+        if (!emitted(s, v, -direction, l, rad))
+            return false;
+    } else if (sel < emitter_count + positional_count) {
+        const Positional &L = s.positional[sel - emitter_count];
+        v.delta_light = true;
+        v.point.position = L.position;
+        const F3 delta = v.point.position - ref.point.position;
+        const float d2 = dot(delta, delta);
+        if (!(d2 > 0)) {
+            v.beta = f4(0);
+            pdf = 0;
+            return true;
+        }
+        direction = delta * (1.0f / std::sqrt(d2));
+        // shaders/packet_transport.h:238-251 (positional_radiance)
+        for (int k = 0; k < 4; ++k) {
+            float intensity = L.intensity[dense_index(l.lambda[k])];
+            if (!positional_intensity(L, direction, intensity))
+                return false;
+            rad[k] = intensity / d2;
+        }
+        pdf = choice.pmf;
+    } else {
+        // constant environment: not sampleable by unidirectional PT (pdf 0)
+        v.type = environment_vertex;
+        direction = F3{0, 0, 1};
+        pdf = 0;
+        rad = f4(0);
+        v.point.position = ref.point.position + 2 * s.scene_radius * direction;
+        v.point.geometric_normal = -direction;
+        v.point.shading_normal = -direction;
+    }
+    v.beta = pdf > 0 ? F4{{rad[0] / pdf, rad[1] / pdf, rad[2] / pdf, rad[3] / pdf}} : f4(0);
+    return finite_nonnegative4(v.beta);
+}
+// shaders/hero_pt_helpers.h:185-221
+static F4 hero_direct(const Ctx &c, Sample &smp, const Wavelengths &l, u64 index, const Vertex &pt,
+                      const Vertex &before, u32 t, F4 beta, const Density &prefix) {
+    if (pt.type != surface_vertex || !pt.connectible)
+        return f4(0);
+    const U4 w = draw_words(c.s, c.p, smp, index, 133 + t - 2);
+    Vertex sampled;
+    F3 direction{};
+    float sampled_pdf = 0;
+    if (!sample_li(c, pt, l, sample_uniform(c.p, w.x), sample_uniform(c.p, w.y),
+                   sample_uniform(c.p, w.z), sampled, direction, sampled_pdf) ||
+        !std::isfinite(sampled_pdf) || sampled_pdf < 0) {
+        smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+        return f4(0);
+    }
+    if (!(sampled_pdf > 0) || !nonzero4(sampled.beta))
+        return f4(0);
+    const HeroEval e = hero_evaluate(pt.bsdf, pt.pair_valid ? pt.sampled_wo_local : pt.frame.local(pt.wo),
+                                     pt.frame.local(direction));
+    if (!e.valid) {
+        smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+        return f4(0);
+    }
+    const F4 value = beta * e.f * sampled.beta * std::fabs(dot(pt.point.shading_normal, direction));
+    if (!nonzero4(value) || !visible(c, pt, sampled))
+        return f4(0);
+    if (sampled.delta_light)
+        return value;
+    sampled_pdf = light_pdf(c, pt, sampled);
+    const F4 bsdf_pdf = represented_pdf(pt, before, sampled);
+    return hero_weight(smp, prefix, value, f4(sampled_pdf), bsdf_pdf);
+}
+
+// shaders/packet_pt_event_body.inc:11-461 (one hero event, vacuum, opaque surfaces)
+static void hero_step(const Ctx &c, LaneState &st) {
+    if (st.complete)
+        return;
+    const Scene &s = c.s;
+    const Params &p = c.p;
+    Sample &smp = st.sample;
+    const Wavelengths &l = st.lambda;
+    F4 &beta = st.beta;
+    u32 &count = st.count;
+    const Density previous_density = st.hero.previous;
+    Density direct_density = st.hero.density;
+    F4 direct_beta = beta;
+    bool direct_allowed = true;
+    const u32 capacity = p.max_depth + 2;
+    F3 ro = st.ray_o, rd = st.ray_d;
+    const u32 old_count = count;
+    bool terminated = true;
+    Vertex current{};
+    do {
+        if (count >= capacity || !nonzero4(beta))
+            break;
+        if (!finite3(ro) || !finite3(rd) || !finite_nonnegative4(beta)) {
+            smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+            break;
+        }
+        const Hit hit = trace_closest(s, c.bvh, ro, rd, INFINITY);
+        if (hit.prim == RP_NONE) {
+            Vertex &v = current;
+            v.type = environment_vertex;
+            v.light = s.environment_light;
+            v.point.position = ro + rd;
+            v.point.geometric_normal = -rd;
+            v.point.shading_normal = -rd;
+            v.wo = -rd;
+            v.beta = beta;
+            v.connectible = true;
+            ++count;
+            break;
+        }
+        if (!std::isfinite(hit.t) || hit.t < 0 || !std::isfinite(hit.b1) || !std::isfinite(hit.b2)) {
+            smp.status = RP_SAMPLE_INVALID_HIT;
+            break;
+        }
+        const u32 inst = s.tri_instance[hit.prim], local = s.tri_local[hit.prim];
+        const Instance &instance = s.instances[inst];
+        if (instance.material >= s.materials.size()) {
+            smp.status = RP_SAMPLE_INVALID_HIT;
+            break;
+        }
+        Vertex &v = current;
+        v.type = surface_vertex;
+        v.instance = inst;
+        v.primitive = local;
+        v.u = hit.b1;
+        v.v = hit.b2;
+        v.light = instance.emission == RP_NONE ? RP_NONE : instance.emitter_begin + local;
+        v.wo = -rd;
+        if (!triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, v.point)) {
+            smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+            break;
+        }
+        const Material &material = s.materials[instance.material];
+        F3 dpdu, dpdv;
+        coordinate_system(v.point.shading_normal, dpdu, dpdv);
+        if (!scattering_frame(v.point.shading_normal, dpdu, v.frame) ||
+            !prepare_bsdf(s, material, l, st.hero.active_mask, v.bsdf)) {
+            smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+            break;
+        }
+        const F3 ray_position = fma3(F3{hit.t, hit.t, hit.t}, rd, ro);
+        const F3 ray_error = gamma_bound(2) * (fabs3(hit.t * rd) + fabs3(ro));
+        v.point.error = v.point.error + (fabs3(v.point.position - ray_position) + ray_error);
+        if (!finite3(v.point.error)) {
+            smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+            break;
+        }
+        v.beta = beta;
+        v.connectible = hero_connectible(v.bsdf);
+        ++count;
+        st.crossings = 0;
+        if (count == capacity)
+            break;
+        if (count - 2 >= p.emergency_limit) {
+            smp.status = RP_SAMPLE_EMERGENCY_DEPTH;
+            break;
+        }
+        const U4 draws = draw_words(s, p, smp, st.index, 4 + count - 2);
+        const F3 wo_local = v.frame.local(v.wo);
+        // hero_prepare_future (shaders/hero_pt_helpers.h:38-50): no single-hero families here
+        current.bsdf.active_mask = st.hero.active_mask;
+        direct_density = st.hero.density;
+        direct_allowed = hero_continue(beta, st.hero, count - 1, sample_uniform(p, draws.w));
+        direct_beta = beta;
+        current.connectible = hero_connectible(current.bsdf);
+        if (!direct_allowed)
+            break;
+        const HeroSample proposed = hero_sample(current.bsdf, wo_local, sample_uniform(p, draws.x),
+                                                sample_uniform(p, draws.y), sample_uniform(p, draws.z));
+        bool cont_valid = proposed.valid;
+        const bool cont_accepted = proposed.accepted;
+        if (proposed.valid && proposed.accepted) {
+            st.hero.previous = direct_density;
+            const Update adv = advance(direct_density, beta, proposed.numerator, proposed.pdf);
+            cont_valid = adv.valid;
+            if (adv.valid) {
+                beta = adv.beta;
+                st.hero.density = adv.density;
+            }
+            hero_account_eta(st.hero, proposed.eta, proposed.transmission);
+            st.hero.active_mask = 1;
+            for (int k = 1; k < 4; ++k)
+                if (st.hero.density.lane[k].fraction > 0 || (fbits(beta[k]) & 0x7fffffffu))
+                    st.hero.active_mask |= 1u << k;
+        }
+        if (!cont_valid) {
+            smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+            break;
+        }
+        if (!cont_accepted)
+            break;
+        current.sampled_wo_local = wo_local;
+        current.sampled_wi_local = proposed.wi;
+        current.pair_valid = true;
+        F3 wi = v.frame.world(proposed.wi);
+        if (!unit_vector(wi, wi)) {
+            smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+            break;
+        }
+        if (!finite_nonnegative4(beta)) {
+            smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+            break;
+        }
+        if (proposed.delta)
+            current.delta = true;
+        const F3 origin = offset(v, wi);
+        if (!finite3(origin)) {
+            smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+            break;
+        }
+        ro = origin;
+        rd = wi;
+        terminated = false;
+    } while (false);
+    st.ray_o = ro;
+    st.ray_d = rd;
+    st.complete = terminated || smp.status != RP_SAMPLE_SUCCESS || count >= capacity || !nonzero4(beta);
+    if (count != old_count && smp.status == RP_SAMPLE_SUCCESS) {
+        Vertex before{};
+        if (count > 2) {
+            before.type = st.preceding_type;
+            before.point.position = st.preceding_position;
+        }
+        st.radiance = st.radiance + hero_endpoint(c, smp, l, current, st.latest, before, count,
+                                                   previous_density);
+        if (smp.status == RP_SAMPLE_SUCCESS && count < capacity && direct_allowed)
+            st.radiance = st.radiance + hero_direct(c, smp, l, st.index, current, st.latest, count,
+                                                     direct_beta, direct_density);
+        if (!finite_nonnegative4(st.radiance))
+            smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+        if (smp.status != RP_SAMPLE_SUCCESS)
+            st.complete = true;
+    }
+    if (count != old_count) {
+        st.preceding_position = st.latest.point.position;
+        st.preceding_type = st.latest.type;
+        st.latest = current;
+    }
+}
+
+static Params make_params(const Scene &s, const rp_request &r) {
+    Params p{};
+    p.width = r.width;
+    p.height = r.height;
+    p.pixel_begin = r.pixel_begin;
+    p.pixel_count = r.pixel_count;
+    p.sample_low = u32(r.sample_begin);
+    p.sample_high = u32(r.sample_begin >> 32);
+    p.seed_low = u32(r.seed);
+    p.seed_high = u32(r.seed >> 32);
+    p.sampler = r.sampler_kind;
+    p.randomization = r.randomization;
+    p.m = r.sampler_kind == RP_SAMPLER_SOBOL ? sobol_scale_exponent(r.width, r.height) : 0;
+    p.emergency_limit = r.emergency_limit ? r.emergency_limit : 1024;
+    p.max_depth = s.max_depth;
+    return p;
+}
+
+// shaders/render.metal:2424-2469 (hero branch) + packet_pt_result (shaders/packet_pt_step.h:225-239)
+static rp_packet_result render_lane(const Ctx &c, u32 lane) {
+    const Scene &s = c.s;
+    LaneState st;
+    u64 index = 0;
+    st.sample = begin_sample(s, c.p, lane, index);
+    st.index = index;
+    const float uw = sample_uniform(c.p, st.sample.words[2]);
+    st.lambda = s.hero_mode == RP_HERO_VISIBLE ? sample_visible(uw) : sample_uniform(uw);
+    F3 o, d;
+    primary_ray(s, c.p, st.sample, o, d);
+    st.ray_o = o;
+    st.ray_d = d;
+    st.beta = f4(1);
+    st.count = 1;
+    Vertex cam{};
+    cam.type = camera_vertex;
+    cam.point.position = o;
+    cam.beta = f4(1);
+    cam.connectible = true;
+    st.latest = cam;
+    if (st.sample.status != RP_SAMPLE_SUCCESS || !finite3(o) || !finite3(d)) {
+        st.sample.status = RP_SAMPLE_INVALID_ARITHMETIC;
+        st.complete = true;
+    }
+    while (!st.complete)
+        hero_step(c, st);
+    rp_packet_result r{};
+    r.status = st.complete ? st.sample.status : u32(RP_SAMPLE_INVALID_ARITHMETIC);
+    r.pixel = st.sample.pixel;
+    r.sample_low = st.sample.sample_low;
+    r.sample_high = st.sample.sample_high;
+    r.filter_weight = 1;
+    for (int k = 0; k < 4; ++k) {
+        r.wavelengths[k] = st.lambda.lambda[k];
+        r.wavelength_pdfs[k] = st.lambda.pdf[k];
+        r.radiance[k] = st.radiance[k];
+    }
+    return r;
+}
+
+} // namespace oracle
+
+using namespace oracle;
+
+struct or_scene {
+    Scene scene;
+    Bvh bvh;
+};
+
+static void put_diag(char *diag, size_t cap, const std::string &msg) {
+    if (diag && cap) {
+        std::snprintf(diag, cap, "%s", msg.c_str());
+    }
+}
+
+extern "C" {
+
+or_scene *or_scene_create(const rp_scene_desc *desc, char *diag, size_t cap) {
+    if (!desc || desc->abi_version != RP_ABI_VERSION || !desc->sobol_tables) {
+        put_diag(diag, cap, "invalid scene description");
+        return nullptr;
+    }
+    auto out = std::make_unique<or_scene>();
+    std::string error;
+    if (!load_scene(*desc, out->scene, error)) {
+        put_diag(diag, cap, error);
+        return nullptr;
+    }
+    build_lbvh(out->scene.world, out->bvh);
+    return out.release();
+}
+
+void or_scene_destroy(or_scene *scene) { delete scene; }
+uint32_t or_scene_light_count(const or_scene *scene) { return scene->scene.light_count; }
+
+int or_sample(const or_scene *scene, const rp_request *request, rp_packet_result *results,
+              size_t capacity, int threads) {
+    const u64 lanes = u64(request->pixel_count) * request->sample_count;
+    if (lanes > capacity || request->pixel_count == 0)
+        return -1;
+    const Params p = make_params(scene->scene, *request);
+    const Ctx c{scene->scene, scene->bvh, p};
+    unsigned n = threads > 0 ? unsigned(threads) : std::max(1u, std::thread::hardware_concurrency());
+    std::atomic<u64> next{0};
+    auto work = [&]() {
+        for (;;) {
+            const u64 begin = next.fetch_add(256);
+            if (begin >= lanes)
+                return;
+            const u64 end = std::min(lanes, begin + 256);
+            for (u64 i = begin; i < end; ++i)
+                results[i] = render_lane(c, u32(i));
+        }
+    };
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < n; ++t)
+        pool.emplace_back(work);
+    work();
+    for (auto &t : pool)
+        t.join();
+    for (u64 i = 0; i < lanes; ++i)
+        if (results[i].status != RP_SAMPLE_SUCCESS)
+            return 1;
+    return 0;
+}
+
+void or_probe_sobol(const void *tables, const uint32_t *q, uint32_t count, uint32_t *r) {
+    const auto &t = *static_cast<const SobolTables *>(tables);
+    for (u32 i = 0; i < count; ++i) {
+        const u32 *a = q + 8 * i;
+        const u64 index = sobol_index(t, a[0], a[1], a[2], (u64(a[4]) << 32) | a[3]);
+        const u32 value = sobol_word(t, index, a[5], a[6], a[7]);
+        const u32 camera = sobol_word(t, index, 0, 0, 0);
+        u32 *o = r + 6 * i;
+        o[0] = u32(index);
+        o[1] = u32(index >> 32);
+        o[2] = value;
+        o[3] = sobol_dimension_hash(a[5], a[7]);
+        o[4] = fbits(sobol_uniform(value));
+        o[5] = fbits(sobol_camera_uniform(camera, a[0], a[1]));
+    }
+}
+
+void or_probe_philox(const uint32_t *q, uint32_t count, uint32_t *r) {
+    for (u32 i = 0; i < count; ++i) {
+        const u32 *a = q + 6 * i;
+        const U4 w = philox(U4{a[0], a[1], a[2], a[3]}, a[4], a[5]);
+        r[4 * i] = w.x;
+        r[4 * i + 1] = w.y;
+        r[4 * i + 2] = w.z;
+        r[4 * i + 3] = w.w;
+    }
+}
+
+void or_probe_wavelengths(const float *u, uint32_t count, uint32_t mode, float *r) {
+    for (u32 i = 0; i < count; ++i) {
+        const Wavelengths w = mode == RP_HERO_VISIBLE ? sample_visible(u[i]) : sample_uniform(u[i]);
+        for (int k = 0; k < 4; ++k) {
+            r[8 * i + k] = w.lambda[k];
+            r[8 * i + 4 + k] = w.pdf[k];
+        }
+    }
+}
+
+int or_probe_raygen(const or_scene *scene, const rp_request *request, uint32_t *words, float *rays,
+                    size_t capacity) {
+    const u64 lanes = u64(request->pixel_count) * request->sample_count;
+    if (lanes > capacity)
+        return -1;
+    const Params p = make_params(scene->scene, *request);
+    for (u64 i = 0; i < lanes; ++i) {
+        u64 index = 0;
+        const Sample smp = begin_sample(scene->scene, p, u32(i), index);
+        u32 *w = words + 11 * i;
+        w[0] = smp.pixel;
+        w[1] = smp.sample_low;
+        w[2] = smp.sample_high;
+        w[3] = u32(index);
+        w[4] = u32(index >> 32);
+        for (int k = 0; k < 4; ++k)
+            w[5 + k] = smp.words[k];
+        w[9] = w[10] = 0;
+        F3 o, d;
+        primary_ray(scene->scene, p, smp, o, d);
+        float *r = rays + 6 * i;
+        for (int a = 0; a < 3; ++a) {
+            r[a] = o[a];
+            r[3 + a] = d[a];
+        }
+    }
+    return 0;
+}
+
+void or_probe_bsdf(const float *q, uint32_t count, float *r) {
+    for (u32 i = 0; i < count; ++i) {
+        const float *a = q + 16 * i;
+        float *o = r + 12 * i;
+        std::fill(o, o + 12, 0.0f);
+        LaneBsdf lane{};
+        lane.kind = u32(a[0]);
+        bool ok = true;
+        if (lane.kind == 0)
+            lane.reflectance = a[1];
+        else if (lane.kind == 1)
+            ok = conductor_prepare(a[1], a[2], a[3], a[4], a[5] != 0, lane.conductor);
+        else
+            ok = dielectric_prepare(a[1], a[3], a[4], a[5] != 0, lane.dielectric);
+        if (!ok) {
+            o[2] = -1;
+            continue;
+        }
+        const F3 wo{a[6], a[7], a[8]}, wi{a[9], a[10], a[11]};
+        const Eval e = scalar_evaluate(lane, wo, wi);
+        o[0] = e.f;
+        o[1] = e.pdf;
+        o[2] = e.valid ? 1.f : 0.f;
+        float eta;
+        const BSample smp = scalar_sample(lane, wo, a[12], a[13], a[14], eta);
+        o[3] = smp.wi.x;
+        o[4] = smp.wi.y;
+        o[5] = smp.wi.z;
+        o[6] = smp.weight;
+        o[7] = smp.pdf;
+        o[8] = float((smp.delta ? 1 : 0) | (smp.accepted ? 2 : 0) | (smp.valid ? 4 : 0));
+        o[9] = eta;
+    }
+}
+
+int or_export_bvh(const or_scene *scene, uint32_t *nodes, uint32_t *leaf_order, uint64_t *keys,
+                  float *bounds, size_t capacity) {
+    const Bvh &b = scene->bvh;
+    if (b.n > capacity)
+        return -1;
+    for (u32 i = 0; i < b.n; ++i) {
+        leaf_order[i] = b.order[i];
+        keys[i] = b.keys[i];
+        for (int a = 0; a < 3; ++a) {
+            bounds[6 * (b.n - 1 + i) + a] = b.leaf_box[i].lo[a];
+            bounds[6 * (b.n - 1 + i) + 3 + a] = b.leaf_box[i].hi[a];
+        }
+    }
+    for (u32 i = 0; i + 1 < b.n; ++i) {
+        nodes[3 * i] = b.left[i];
+        nodes[3 * i + 1] = b.right[i];
+        nodes[3 * i + 2] = b.parent[i];
+        for (int a = 0; a < 3; ++a) {
+            bounds[6 * i + a] = b.node_box[i].lo[a];
+            bounds[6 * i + 3 + a] = b.node_box[i].hi[a];
+        }
+    }
+    return int(b.n);
+}
+
+void or_trace_rays(const or_scene *scene, const float *rays, uint32_t count, int any_hit, int brute,
+                   float *hits) {
+    for (u32 i = 0; i < count; ++i) {
+        const float *r = rays + 7 * i;
+        const F3 o{r[0], r[1], r[2]}, d{r[3], r[4], r[5]};
+        float *h = hits + 4 * i;
+        if (any_hit) {
+            const bool occ = brute ? trace_closest_brute(scene->scene, o, d, r[6]).prim != RP_NONE
+                                   : trace_any(scene->scene, scene->bvh, o, d, r[6]);
+            h[0] = occ ? 1.f : 0.f;
+            h[1] = h[2] = 0;
+            h[3] = ffrom(RP_NONE);
+            continue;
+        }
+        const Hit hit = brute ? trace_closest_brute(scene->scene, o, d, r[6])
+                              : trace_closest(scene->scene, scene->bvh, o, d, r[6]);
+        h[0] = hit.prim == RP_NONE ? INFINITY : hit.t;
+        h[1] = hit.b1;
+        h[2] = hit.b2;
+        h[3] = ffrom(hit.prim);
+    }
+}
+
+void or_probe_advance(const float *q, uint32_t count, float *r) {
+    for (u32 i = 0; i < count; ++i) {
+        const float *a = q + 20 * i;
+        Density prefix;
+        F4 beta, num, pdf;
+        for (int k = 0; k < 4; ++k) {
+            prefix.lane[k].fraction = a[k];
+            prefix.lane[k].exponent = int(a[4 + k]);
+            beta[k] = a[8 + k];
+            num[k] = a[12 + k];
+            pdf[k] = a[16 + k];
+        }
+        const Update u = advance(prefix, beta, num, pdf);
+        float *o = r + 13 * i;
+        for (int k = 0; k < 4; ++k) {
+            o[k] = u.beta[k];
+            o[4 + k] = u.density.lane[k].fraction;
+            o[8 + k] = float(u.density.lane[k].exponent);
+        }
+        o[12] = u.valid ? 1.f : 0.f;
+    }
+}
+
+int or_build_light_tables(const double *rows, uint32_t count, uint32_t *alias, uint32_t *records,
+                          uint32_t *nodes, uint32_t *infinite, uint32_t *infinite_count) {
+    std::vector<LightInput> in(count);
+    for (u32 i = 0; i < count; ++i) {
+        const double *r = rows + 16 * i;
+        in[i].power = r[0];
+        in[i].bounds_power = r[1];
+        for (int a = 0; a < 3; ++a) {
+            in[i].low[a] = float(r[2 + a]);
+            in[i].high[a] = float(r[5 + a]);
+            in[i].direction[a] = float(r[8 + a]);
+        }
+        in[i].cos_outer = float(r[11]);
+        in[i].cos_emission = float(r[12]);
+        in[i].two_sided = r[13] != 0;
+        in[i].infinite = r[14] != 0;
+    }
+    LightTables t;
+    std::string error;
+    if (!build_light_tables(in, t, error))
+        return -1;
+    std::memcpy(alias, t.alias.data(), t.alias.size() * sizeof(LightAlias));
+    std::memcpy(records, t.records.data(), t.records.size() * sizeof(LightRecord));
+    std::memcpy(nodes, t.nodes.data(), t.nodes.size() * sizeof(LightBounds));
+    std::memcpy(infinite, t.infinite.data(), t.infinite.size() * sizeof(u32));
+    *infinite_count = u32(t.infinite.size());
+    return int(t.nodes.size());
+}
+
+void or_probe_light_select(const or_scene *scene, const float *q, uint32_t count, float *r) {
+    for (u32 i = 0; i < count; ++i) {
+        const float *a = q + 8 * i;
+        const F3 pos{a[0], a[1], a[2]}, n{a[3], a[4], a[5]};
+        const Selected sel = light_sample(scene->scene, pos, n, a[6]);
+        r[3 * i] = ffrom(sel.light);
+        r[3 * i + 1] = sel.pmf;
+        r[3 * i + 2] = light_pmf(scene->scene, pos, n, fbits(a[7]));
+    }
+}
+
+// src/packet_film.cpp:10-14 (Neumaier step), :102-114 (packet_sensor_xyz), :198-265 (add)
+static void add_compensated(double value, double &sum, double &correction) {
+    const double next = sum + value;
+    correction += std::abs(sum) >= std::abs(value) ? (sum - next) + value : (value - next) + sum;
+    sum = next;
+}
+int or_film_add(const rp_packet_result *results, size_t count, const double *cie, uint32_t pixel_count,
+                rp_film_pixel *film) {
+    for (size_t i = 0; i < count; ++i) {
+        const auto &s = results[i];
+        if (s.pixel >= pixel_count)
+            return -1;
+        double xyz[3] = {0, 0, 0};
+        for (int k = 0; k < 4; ++k) {
+            if (s.wavelength_pdfs[k] == 0)
+                continue;
+            const double w = s.wavelengths[k];
+            if (!(w >= 360 && w <= 830))
+                continue;
+            const size_t row = size_t(std::round(w) - 360);
+            const double weight = double(s.radiance[k]) / s.wavelength_pdfs[k] / 4;
+            for (int c = 0; c < 3; ++c)
+                xyz[c] += weight * cie[3 * row + c];
+        }
+        auto &px = film[s.pixel];
+        for (int c = 0; c < 3; ++c) {
+            add_compensated(xyz[c] * s.filter_weight, px.sum[c], px.correction[c]);
+            px.square[c] += xyz[c] * xyz[c];
+        }
+        add_compensated(s.filter_weight, px.weight_sum, px.weight_correction);
+        ++px.count;
+    }
+    return 0;
+}
+
+} // extern "C"

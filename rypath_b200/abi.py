@@ -1,0 +1,160 @@
+"""ctypes mirror of include/rypath_cuda.h (the C ABI of the CUDA backend).
+
+The structures below must match the C declarations byte for byte; tests/test_abi.py checks
+their sizes against the values the library itself reports.
+"""
+
+import ctypes as C
+
+RP_ABI_VERSION = 1
+RP_NONE = 0xFFFFFFFF
+RP_SPECTRUM_BINS = 471
+RP_SOBOL_TABLE_BYTES = 234208
+
+RP_SUCCESS, RP_NOT_BUILT, RP_NO_DEVICE, RP_NO_RAY_TRACING, RP_FAILURE, RP_INVALID_ARGUMENT = range(6)
+STATUS_NAMES = {0: "success", 1: "not_built", 2: "no_device", 3: "no_ray_tracing", 4: "failure",
+                5: "invalid_argument"}
+
+SAMPLE_SUCCESS, EMERGENCY_DEPTH, INVALID_ARITHMETIC, INVALID_HIT, BOUNDARY_EXHAUSTION = range(5)
+
+SAMPLER_INDEPENDENT, SAMPLER_SOBOL = 0, 1
+RANDOMIZE_NONE, RANDOMIZE_PERMUTEDIGITS, RANDOMIZE_FASTOWEN, RANDOMIZE_OWEN = range(4)
+FILTER_BOX, FILTER_TRIANGLE = 0, 1
+DIFFUSE, CONDUCTOR, DIELECTRIC = 0, 1, 2
+REFLECTANCE_KNOTS, REFLECTANCE_CONSTANT, REFLECTANCE_BLACKBODY = 0, 1, 4
+POINT_LIGHT, SPOT_LIGHT = 0, 1
+LIGHTS_BVH, LIGHTS_POWER, LIGHTS_UNIFORM = 0, 1, 2
+TRANSPORT_SCALAR, TRANSPORT_HERO = 0, 2
+HERO_UNIFORM, HERO_VISIBLE = 0, 1
+
+u32, u64, i32, f32, f64 = C.c_uint32, C.c_uint64, C.c_int32, C.c_float, C.c_double
+P = C.POINTER
+
+
+class Knot(C.Structure):
+    _fields_ = [("wavelength", f32), ("value", f32)]
+
+
+class Instance(C.Structure):
+    _fields_ = [("matrix", f32 * 12), ("vertex_begin", u32), ("triangle_begin", u32),
+                ("triangle_count", u32), ("material", u32), ("reverse_orientation", u32),
+                ("emission", u32), ("normal_begin", u32), ("inside_medium", u32),
+                ("outside_medium", u32)]
+
+
+class Material(C.Structure):
+    _fields_ = [("scattering", u32), ("kind", u32), ("knot_begin", u32), ("knot_count", u32),
+                ("scalar_value", f32), ("eta_begin", u32), ("eta_count", u32), ("k_begin", u32),
+                ("k_count", u32), ("optical_extensions", u32), ("u_roughness", f32),
+                ("v_roughness", f32), ("remap_roughness", u32)]
+
+
+class AreaEmission(C.Structure):
+    _fields_ = [("radiance", f32 * RP_SPECTRUM_BINS), ("two_sided", u32)]
+
+
+class PositionalLight(C.Structure):
+    _fields_ = [("position", f32 * 3), ("intensity", f32 * RP_SPECTRUM_BINS), ("kind", u32),
+                ("light_from_world", f32 * 9), ("cos_falloff_start", f32),
+                ("cos_falloff_end", f32)]
+
+
+class Medium(C.Structure):
+    _fields_ = [("sigma_a", f32 * RP_SPECTRUM_BINS), ("sigma_s", f32 * RP_SPECTRUM_BINS),
+                ("emission", f32 * RP_SPECTRUM_BINS), ("g", f32)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("origin", f32 * 3), ("corner", f32 * 3), ("dx", f32 * 3), ("dy", f32 * 3)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("abi_version", u32),
+        ("vertex_count", u32), ("positions", P(f32)),
+        ("normal_count", u32), ("normals", P(f32)),
+        ("triangle_count", u32), ("triangles", P(u32)),
+        ("instance_count", u32), ("instances", P(Instance)),
+        ("material_count", u32), ("materials", P(Material)),
+        ("knot_count", u32), ("knots", P(Knot)),
+        ("emission_count", u32), ("emissions", P(AreaEmission)),
+        ("positional_count", u32), ("positional", P(PositionalLight)),
+        ("medium_count", u32), ("media", P(Medium)),
+        ("camera_medium", u32),
+        ("environment", P(f32)),
+        ("camera", Camera),
+        ("filter_kind", u32), ("filter_x_radius", f32), ("filter_y_radius", f32),
+        ("max_depth", u32),
+        ("light_sampler", u32),
+        ("transport", u32),
+        ("hero_wavelengths", u32),
+        ("sobol_tables", C.c_void_p),
+    ]
+
+
+class Request(C.Structure):
+    _fields_ = [("width", u32), ("height", u32), ("seed", u64), ("material_seed", i32),
+                ("pixel_begin", u32), ("pixel_count", u32), ("sample_begin", u64),
+                ("sample_count", u32), ("emergency_limit", u32), ("sampler_kind", u32),
+                ("randomization", u32), ("boundary_limit", u32)]
+
+
+class PacketResult(C.Structure):
+    _fields_ = [("status", u32), ("pixel", u32), ("sample_low", u32), ("sample_high", u32),
+                ("splat_count", u32), ("wavelengths", f32 * 4), ("wavelength_pdfs", f32 * 4),
+                ("radiance", f32 * 4), ("filter_weight", f32), ("reserved", u32 * 2)]
+
+
+class ScalarResult(C.Structure):
+    _fields_ = [("status", u32), ("pixel", u32), ("sample_low", u32), ("sample_high", u32),
+                ("wavelength", f32), ("radiance", f32), ("scatterings", u32),
+                ("random_words", u32 * 4)]
+
+
+class DeviceInfo(C.Structure):
+    _fields_ = [("name", C.c_char * 128), ("device", C.c_int), ("sm_count", C.c_int),
+                ("major", C.c_int), ("minor", C.c_int), ("total_memory", u64)]
+
+
+class FilmPixel(C.Structure):
+    _fields_ = [("sum", f64 * 3), ("correction", f64 * 3), ("weight_sum", f64),
+                ("weight_correction", f64), ("square", f64 * 3), ("count", u64)]
+
+
+class FilmRequest(C.Structure):
+    _fields_ = [("width", u32), ("height", u32), ("seed", u64), ("sample_begin", u64),
+                ("sample_count", u64), ("batch_size", u64), ("sampler_kind", u32),
+                ("randomization", u32), ("emergency_limit", u32)]
+
+
+class Timing(C.Structure):
+    _fields_ = [("total_ms", f64), ("trace_ms", f64), ("shadow_ms", f64), ("shade_ms", f64),
+                ("other_ms", f64), ("closest_rays", u64), ("shadow_rays", u64),
+                ("kernel_launches", u64), ("samples", u64), ("nodes_visited", u64),
+                ("triangles_tested", u64)]
+
+
+# numpy dtypes with the same layouts, for bulk views of result buffers
+def packet_dtype():
+    import numpy as np
+
+    return np.dtype([("status", "<u4"), ("pixel", "<u4"), ("sample_low", "<u4"),
+                     ("sample_high", "<u4"), ("splat_count", "<u4"), ("wavelengths", "<f4", 4),
+                     ("wavelength_pdfs", "<f4", 4), ("radiance", "<f4", 4),
+                     ("filter_weight", "<f4"), ("reserved", "<u4", 2)])
+
+
+def film_dtype():
+    import numpy as np
+
+    return np.dtype([("sum", "<f8", 3), ("correction", "<f8", 3), ("weight_sum", "<f8"),
+                     ("weight_correction", "<f8"), ("square", "<f8", 3), ("count", "<u8")])
+
+
+EXPECTED_SIZES = {
+    "rp_instance": (Instance, 84), "rp_material": (Material, 52), "rp_knot": (Knot, 8),
+    "rp_area_emission": (AreaEmission, 1888), "rp_positional_light": (PositionalLight, 1948),
+    "rp_medium": (Medium, 5656), "rp_camera": (Camera, 48), "rp_request": (Request, 56),
+    "rp_packet_result": (PacketResult, 80), "rp_scalar_result": (ScalarResult, 44),
+    "rp_film_pixel": (FilmPixel, 96), "rp_film_request": (FilmRequest, 56),
+}

@@ -1,0 +1,72 @@
+"""Extract the two fixed data tables the spectral path needs from a rypath checkout.
+
+Both tables are third-party data that must be bit-identical to what rypath compiles in,
+because the integer sample words and the sensor response are pinned to them:
+
+* ``pbrt_sobol_tables.bin`` -- the 234,208-byte ``sobol::Tables`` block (direction
+  matrices, interval and inverse tables) that rypath includes from
+  ``third_party/pbrt/sobol_tables.inc`` (PBRT v4, Apache-2.0; Joe & Kuo 2008 direction
+  numbers as prepared by L. Gruenschloss).  Layout follows ``src/sobol_shared.h:36-52``:
+  ``uint32 directions[1024*52]; uint64 intervals[25*52]; uint64 inverse[26*52]``,
+  little endian.
+* ``cie_xyz_1931.bin`` -- the CIE 1931 2-degree colour matching functions at 1 nm from
+  360 to 830 nm (471 rows of x, y, z as float64), from ``third_party/cie`` (CIE 2019,
+  CC BY-SA 4.0), i.e. the table rypath generates in ``cmake/CieData.cmake``.
+
+Usage: ``python make_tables.py /path/to/rypath`` (writes next to this script).
+"""
+
+import re
+import struct
+import sys
+from pathlib import Path
+
+SOBOL_WORDS = 1024 * 52
+INTERVAL_WORDS = 25 * 52
+INVERSE_WORDS = 26 * 52
+SOBOL_BYTES = 234208
+
+
+def _strip_comments(text: str) -> str:
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    return re.sub(r"//[^\n]*", " ", text)
+
+
+def sobol_tables(reference: Path) -> bytes:
+    text = _strip_comments((reference / "third_party/pbrt/sobol_tables.inc").read_text())
+    literals = re.findall(r"\b(0[xX][0-9a-fA-F]+|\d+)(?:[uU]?[lL]{0,2}|[lL]{1,2}[uU]?)\b", text)
+    values = [int(v, 0) for v in literals]
+    expected = SOBOL_WORDS + INTERVAL_WORDS + INVERSE_WORDS
+    if len(values) != expected:
+        raise SystemExit(f"expected {expected} integers in sobol_tables.inc, found {len(values)}")
+    directions = values[:SOBOL_WORDS]
+    rest = values[SOBOL_WORDS:]
+    blob = struct.pack(f"<{SOBOL_WORDS}I", *directions)
+    blob += struct.pack(f"<{INTERVAL_WORDS + INVERSE_WORDS}Q", *rest)
+    if len(blob) != SOBOL_BYTES:
+        raise SystemExit("unexpected Sobol table size")
+    return blob
+
+
+def cie_table(reference: Path) -> bytes:
+    rows = (reference / "third_party/cie/CIE_xyz_1931_2deg.csv").read_text().split()
+    values = []
+    for expected_nm, row in zip(range(360, 831), rows):
+        fields = row.split(",")
+        if int(fields[0]) != expected_nm:
+            raise SystemExit("CIE table rows are not 360..830 nm at 1 nm")
+        values.extend(float(v) for v in fields[1:4])
+    if len(values) != 471 * 3:
+        raise SystemExit("CIE table must have 471 rows")
+    return struct.pack("<1413d", *values)
+
+
+def main() -> None:
+    reference = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    out = Path(__file__).resolve().parent
+    (out / "pbrt_sobol_tables.bin").write_bytes(sobol_tables(reference))
+    (out / "cie_xyz_1931.bin").write_bytes(cie_table(reference))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,417 @@
+"""Seeded synthetic scenes for the spectral path: the PBRT-profile inputs the benchmarks use.
+
+``cornell_box()`` is the 36-triangle Cornell-style box (256x256, 64 spp, depth 8) and
+``mixed_scene()`` the ~1.44M-triangle mixed-material mesh scene (1920x1080, 16 spp, depth 16).
+Both return a ``Scene`` holding numpy arrays in the layout of ``rp_scene_desc``; ``Scene.desc()``
+produces the C description (the arrays stay owned by the Scene).
+
+Light spectra follow rypath's PBRT blackbody normalisation (src/pbrt_render.cpp:883-935): the
+Planck shape divided by its 830 nm value, scaled by ``scale / sum(shape * ybar)`` over the
+1 nm CIE table.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+from . import abi
+
+DATA = Path(__file__).resolve().parent / "data"
+WAVELENGTHS = np.arange(360, 831, dtype=np.float64)
+
+
+def sobol_tables() -> bytes:
+    blob = (DATA / "pbrt_sobol_tables.bin").read_bytes()
+    assert len(blob) == abi.RP_SOBOL_TABLE_BYTES
+    return blob
+
+
+def cie_xyz() -> np.ndarray:
+    return np.frombuffer((DATA / "cie_xyz_1931.bin").read_bytes(), dtype="<f8").reshape(471, 3)
+
+
+def blackbody_shape(kelvin: float) -> np.ndarray:
+    """Planck radiance over its 830 nm value (src/pbrt_render.cpp:890-905)."""
+    c2 = 6.62606957e-34 * 299792458.0 / 1.3806488e-23 * 1e9
+    ref = 830.0
+    ref_factor = -math.expm1(-(c2 / ref) / kelvin)
+    out = np.empty(471)
+    for i, w in enumerate(WAVELENGTHS):
+        delta = c2 * (ref - w) / (ref * w)
+        out[i] = (ref / w) ** 5 * math.exp(-delta / kelvin) * ref_factor / -math.expm1(-(c2 / w) / kelvin)
+    return out
+
+
+def blackbody_emission(kelvin: float, scale: float) -> np.ndarray:
+    shape = blackbody_shape(kelvin)
+    norm = float(np.sum(shape * cie_xyz()[:, 1]))
+    return (shape * (scale / norm)).astype(np.float32)
+
+
+def knots_from_curve(values, count: int = 32) -> np.ndarray:
+    """A 32-bin spectrum as `count` knots evenly spaced on 360..830 nm."""
+    w = np.linspace(360.0, 830.0, count, dtype=np.float32)
+    v = np.asarray(values, dtype=np.float32)
+    if v.ndim == 0:
+        v = np.full(count, float(v), dtype=np.float32)
+    return np.stack([w, v], axis=1).astype(np.float32)
+
+
+@dataclass
+class Scene:
+    name: str
+    width: int
+    height: int
+    spp: int
+    positions: np.ndarray  # (V, 3) f32
+    triangles: np.ndarray  # (T, 3) u32
+    instances: list = field(default_factory=list)
+    materials: list = field(default_factory=list)
+    knots: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.float32))
+    emissions: list = field(default_factory=list)  # (radiance[471], two_sided)
+    positional: list = field(default_factory=list)  # dicts
+    environment: np.ndarray | None = None
+    camera: tuple = ((0, 0, 0), (0, 0, -1), (1, 0, 0), (0, -1, 0))
+    filter_kind: int = abi.FILTER_BOX
+    filter_radius: tuple = (0.5, 0.5)
+    max_depth: int = 8
+    light_sampler: int = abi.LIGHTS_BVH
+    hero_wavelengths: int = abi.HERO_VISIBLE
+    normals: np.ndarray | None = None
+    _keep: list = field(default_factory=list, repr=False)
+
+    @property
+    def triangle_count(self) -> int:
+        return int(self.triangles.shape[0])
+
+    def desc(self) -> abi.SceneDesc:
+        keep = []
+
+        def arr(a, ctype):
+            a = np.ascontiguousarray(a)
+            keep.append(a)
+            return a.ctypes.data_as(C.POINTER(ctype))
+
+        d = abi.SceneDesc()
+        d.abi_version = abi.RP_ABI_VERSION
+        pos = np.ascontiguousarray(self.positions, dtype=np.float32)
+        tri = np.ascontiguousarray(self.triangles, dtype=np.uint32)
+        d.vertex_count, d.positions = pos.shape[0], arr(pos, C.c_float)
+        d.triangle_count, d.triangles = tri.shape[0], arr(tri, C.c_uint32)
+        if self.normals is not None:
+            nrm = np.ascontiguousarray(self.normals, dtype=np.float32)
+            d.normal_count, d.normals = nrm.shape[0], arr(nrm, C.c_float)
+        inst = (abi.Instance * max(1, len(self.instances)))()
+        for i, x in enumerate(self.instances):
+            inst[i] = x
+        keep.append(inst)
+        d.instance_count, d.instances = len(self.instances), C.cast(inst, C.POINTER(abi.Instance))
+        mats = (abi.Material * max(1, len(self.materials)))()
+        for i, x in enumerate(self.materials):
+            mats[i] = x
+        keep.append(mats)
+        d.material_count, d.materials = len(self.materials), C.cast(mats, C.POINTER(abi.Material))
+        kn = np.ascontiguousarray(self.knots, dtype=np.float32).reshape(-1, 2)
+        keep.append(kn)
+        d.knot_count = kn.shape[0]
+        d.knots = kn.ctypes.data_as(C.POINTER(abi.Knot))
+        em = (abi.AreaEmission * max(1, len(self.emissions)))()
+        for i, (rad, two) in enumerate(self.emissions):
+            em[i].radiance[:] = [float(v) for v in np.asarray(rad, np.float32)]
+            em[i].two_sided = int(two)
+        keep.append(em)
+        d.emission_count, d.emissions = len(self.emissions), C.cast(em, C.POINTER(abi.AreaEmission))
+        pl = (abi.PositionalLight * max(1, len(self.positional)))()
+        for i, L in enumerate(self.positional):
+            pl[i].position[:] = list(L["position"])
+            pl[i].intensity[:] = [float(v) for v in np.asarray(L["intensity"], np.float32)]
+            pl[i].kind = L["kind"]
+            pl[i].light_from_world[:] = list(L.get("light_from_world", (1, 0, 0, 0, 1, 0, 0, 0, 1)))
+            pl[i].cos_falloff_start = L.get("cos_falloff_start", 1.0)
+            pl[i].cos_falloff_end = L.get("cos_falloff_end", 0.0)
+        keep.append(pl)
+        d.positional_count = len(self.positional)
+        d.positional = C.cast(pl, C.POINTER(abi.PositionalLight))
+        d.camera_medium = abi.RP_NONE
+        if self.environment is not None:
+            d.environment = arr(np.asarray(self.environment, np.float32), C.c_float)
+        o, corner, dx, dy = self.camera
+        d.camera.origin[:] = list(o)
+        d.camera.corner[:] = list(corner)
+        d.camera.dx[:] = list(dx)
+        d.camera.dy[:] = list(dy)
+        d.filter_kind = self.filter_kind
+        d.filter_x_radius, d.filter_y_radius = self.filter_radius
+        d.max_depth = self.max_depth
+        d.light_sampler = self.light_sampler
+        d.transport = abi.TRANSPORT_HERO
+        d.hero_wavelengths = self.hero_wavelengths
+        tables = C.create_string_buffer(sobol_tables(), abi.RP_SOBOL_TABLE_BYTES)
+        keep.append(tables)
+        d.sobol_tables = C.cast(tables, C.c_void_p)
+        self._keep = keep
+        return d
+
+
+def identity_instance(vertex_begin, triangle_begin, triangle_count, material, emission=abi.RP_NONE):
+    inst = abi.Instance()
+    inst.matrix[:] = [1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0]
+    inst.vertex_begin, inst.triangle_begin, inst.triangle_count = vertex_begin, triangle_begin, triangle_count
+    inst.material, inst.emission = material, emission
+    inst.reverse_orientation = 0
+    inst.normal_begin = abi.RP_NONE
+    inst.inside_medium = inst.outside_medium = abi.RP_NONE
+    return inst
+
+
+def diffuse_material(knot_begin, knot_count=32):
+    m = abi.Material()
+    m.scattering, m.kind, m.knot_begin, m.knot_count = abi.DIFFUSE, abi.REFLECTANCE_KNOTS, knot_begin, knot_count
+    m.remap_roughness = 1
+    return m
+
+
+def pinhole_camera(origin, target, up, vfov_degrees, width, height):
+    """A PBRT perspective camera as the raster basis of RasterCamera (src/render.hpp:152)."""
+    o = np.asarray(origin, np.float64)
+    f = np.asarray(target, np.float64) - o
+    f /= np.linalg.norm(f)
+    r = np.cross(f, np.asarray(up, np.float64))
+    r /= np.linalg.norm(r)
+    u = np.cross(r, f)
+    aspect = width / height
+    # PBRT's fov spans the shorter image axis.
+    t = math.tan(math.radians(vfov_degrees) / 2)
+    tx, ty = (t * aspect, t) if aspect >= 1 else (t, t / aspect)
+    corner = f - tx * r + ty * u
+    dx = 2 * tx * r
+    dy = -2 * ty * u
+    return tuple(o.astype(np.float32)), tuple(corner.astype(np.float32)), tuple(dx.astype(np.float32)), tuple(
+        dy.astype(np.float32))
+
+
+def _box(lo, hi):
+    """12 outward-wound triangles of an axis-aligned box."""
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    v = np.array([[x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0],
+                  [x0, y0, z1], [x1, y0, z1], [x1, y1, z1], [x0, y1, z1]], np.float32)
+    t = np.array([[0, 2, 1], [0, 3, 2], [4, 5, 6], [4, 6, 7], [0, 1, 5], [0, 5, 4],
+                  [3, 7, 6], [3, 6, 2], [0, 4, 7], [0, 7, 3], [1, 2, 6], [1, 6, 5]], np.uint32)
+    return v, t
+
+
+def _quad(a, b, c, d):
+    return np.array([a, b, c, d], np.float32), np.array([[0, 1, 2], [0, 2, 3]], np.uint32)
+
+
+def cornell_box(width=256, height=256, spp=64, max_depth=8) -> Scene:
+    """Cornell-style box: 5 walls (10 tris), two boxes (24 tris), one quad light (2 tris)."""
+    parts = []  # (verts, tris, material, emission)
+    # walls, wound so their geometric normals face the interior
+    parts.append(_quad((-1, 0, -1), (-1, 0, 1), (1, 0, 1), (1, 0, -1)) + (0, None))    # floor
+    parts.append(_quad((-1, 2, -1), (1, 2, -1), (1, 2, 1), (-1, 2, 1)) + (0, None))    # ceiling
+    parts.append(_quad((-1, 0, -1), (1, 0, -1), (1, 2, -1), (-1, 2, -1)) + (0, None))  # back
+    parts.append(_quad((-1, 0, -1), (-1, 2, -1), (-1, 2, 1), (-1, 0, 1)) + (1, None))  # left (red)
+    parts.append(_quad((1, 0, -1), (1, 0, 1), (1, 2, 1), (1, 2, -1)) + (2, None))      # right (green)
+    # short and tall boxes (axis aligned)
+    parts.append(_box((0.10, 0.0, -0.10), (0.70, 0.60, 0.50)) + (0, None))
+    parts.append(_box((-0.75, 0.0, -0.70), (-0.15, 1.20, -0.10)) + (0, None))
+    # light quad just below the ceiling, facing down
+    parts.append(_quad((-0.25, 1.98, -0.25), (0.25, 1.98, -0.25), (0.25, 1.98, 0.25), (-0.25, 1.98, 0.25))
+                 + (3, 0))
+    positions, triangles, instances = [], [], []
+    vb = tb = 0
+    for verts, tris, mat, emission in parts:
+        positions.append(verts)
+        triangles.append(tris)
+        instances.append(identity_instance(vb, tb, len(tris), mat,
+                                           abi.RP_NONE if emission is None else emission))
+        vb += len(verts)
+        tb += len(tris)
+    positions = np.concatenate(positions)
+    triangles = np.concatenate(triangles)
+    w = np.linspace(360, 830, 32)
+    white = knots_from_curve(0.73)
+    red = knots_from_curve(np.interp(w, [360, 560, 610, 830], [0.05, 0.05, 0.65, 0.70]))
+    green = knots_from_curve(np.interp(w, [360, 470, 530, 580, 830], [0.05, 0.08, 0.55, 0.10, 0.05]))
+    black = knots_from_curve(0.0)
+    knots = np.concatenate([white, red, green, black])
+    materials = [diffuse_material(0), diffuse_material(32), diffuse_material(64), diffuse_material(96)]
+    light = blackbody_emission(6500.0, 17.0)
+    scene = Scene("cornell_box", width, height, spp, positions, triangles, instances, materials, knots,
+                  emissions=[(light, False)], max_depth=max_depth)
+    scene.camera = pinhole_camera((0, 1, 3.94), (0, 1, 0), (0, 1, 0), 40.0, width, height)
+    return scene
+
+
+# ------------------------------------------------------------------ mixed-material scene
+def icosphere(subdivisions: int):
+    t = (1 + 5 ** 0.5) / 2
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t],
+                  [0, 1, -t], [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4],
+                  [11, 10, 2], [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8],
+                  [3, 8, 9], [4, 9, 5], [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], np.int64)
+    for _ in range(subdivisions):
+        edges = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        edges.sort(axis=1)
+        unique, inverse = np.unique(edges, axis=0, return_inverse=True)
+        inverse = inverse.reshape(-1)
+        mid = v[unique[:, 0]] + v[unique[:, 1]]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        base = len(v)
+        v = np.concatenate([v, mid])
+        n = len(f)
+        a = base + inverse[:n]
+        b = base + inverse[n:2 * n]
+        c = base + inverse[2 * n:]
+        f = np.concatenate([np.stack([f[:, 0], a, c], 1), np.stack([f[:, 1], b, a], 1),
+                            np.stack([f[:, 2], c, b], 1), np.stack([a, b, c], 1)])
+    return v, f
+
+
+def uv_sphere(n_phi=32, n_theta=33):
+    """Latitude-longitude sphere with 2*n_phi*(n_theta-1) triangles (2048 by default)."""
+    verts = [[0, 0, 1]]
+    for i in range(1, n_theta):
+        th = math.pi * i / n_theta
+        for j in range(n_phi):
+            ph = 2 * math.pi * j / n_phi
+            verts.append([math.sin(th) * math.cos(ph), math.sin(th) * math.sin(ph), math.cos(th)])
+    verts.append([0, 0, -1])
+    verts = np.array(verts, np.float64)
+    tris = []
+    for j in range(n_phi):
+        tris.append([0, 1 + j, 1 + (j + 1) % n_phi])
+    for i in range(n_theta - 2):
+        r0, r1 = 1 + i * n_phi, 1 + (i + 1) * n_phi
+        for j in range(n_phi):
+            j1 = (j + 1) % n_phi
+            tris.append([r0 + j, r1 + j, r1 + j1])
+            tris.append([r0 + j, r1 + j1, r0 + j1])
+    last = len(verts) - 1
+    r0 = 1 + (n_theta - 2) * n_phi
+    for j in range(n_phi):
+        tris.append([r0 + j, last, r0 + (j + 1) % n_phi])
+    return verts, np.array(tris, np.int64)
+
+
+def _smooth_random_curve(rng, lo, hi, count=32):
+    """A smooth random spectrum: a few random Gaussian bumps, mapped into [lo, hi]."""
+    w = np.linspace(0, 1, count)
+    y = np.zeros(count)
+    for _ in range(3):
+        y += rng.uniform(-1, 1) * np.exp(-((w - rng.uniform(0, 1)) ** 2) / (2 * rng.uniform(0.05, 0.3) ** 2))
+    y = (y - y.min()) / max(1e-6, y.max() - y.min())
+    return lo + (hi - lo) * y
+
+
+def mixed_scene(width=1920, height=1080, spp=16, max_depth=16, seed=1, subdivisions=8,
+                sphere_count=64) -> Scene:
+    rng = np.random.default_rng(seed)
+    positions, triangles, instances, materials = [], [], [], []
+    knots = []
+
+    def add_knots(k):
+        begin = sum(len(x) for x in knots)
+        knots.append(np.asarray(k, np.float32))
+        return begin
+
+    def random_material():
+        r = rng.uniform()
+        if r < 0.4:
+            return diffuse_material(add_knots(knots_from_curve(_smooth_random_curve(rng, 0.05, 0.9))))
+        m = abi.Material()
+        m.remap_roughness = 1
+        if r < 0.8:
+            m.scattering = abi.CONDUCTOR
+            m.kind = abi.REFLECTANCE_CONSTANT
+            m.scalar_value = 1.0
+            m.eta_begin = add_knots(knots_from_curve(_smooth_random_curve(rng, 0.2, 1.8)))
+            m.eta_count = 32
+            m.k_begin = add_knots(knots_from_curve(_smooth_random_curve(rng, 2.0, 4.5)))
+            m.k_count = 32
+            m.optical_extensions = 3
+            rough = rng.uniform(0.05, 0.5)
+            m.u_roughness = m.v_roughness = rough
+        else:
+            m.scattering = abi.DIELECTRIC
+            m.kind = abi.REFLECTANCE_CONSTANT
+            m.scalar_value = 1.0
+            w = np.linspace(360, 830, 32)
+            cauchy = 1.5 + 0.004 / (w / 1000.0) ** 2
+            m.eta_begin = add_knots(knots_from_curve(cauchy))
+            m.eta_count = 32
+            m.optical_extensions = 1
+            m.k_begin = m.k_count = 0
+            m.u_roughness = m.v_roughness = 0.0
+        return m
+
+    vb = tb = 0
+
+    def add_mesh(v, f, material):
+        nonlocal vb, tb
+        positions.append(np.asarray(v, np.float32))
+        triangles.append(np.asarray(f, np.uint32))
+        materials.append(material)
+        instances.append(identity_instance(vb, tb, len(f), len(materials) - 1))
+        vb += len(v)
+        tb += len(f)
+
+    # displaced icosphere at the origin
+    v, f = icosphere(subdivisions)
+    d = np.zeros(len(v))
+    for _ in range(6):
+        k = rng.normal(size=3) * rng.uniform(2, 9)
+        d += np.sin(v @ k + rng.uniform(0, 2 * math.pi))
+    v = v * (1 + 0.02 * d / 6)[:, None]
+    add_mesh(v, f, random_material())
+    # random spheres around it, on a ring above the ground
+    sv, sf = uv_sphere()
+    for i in range(sphere_count):
+        radius = rng.uniform(0.08, 0.3)
+        ang = rng.uniform(0, 2 * math.pi)
+        dist = rng.uniform(1.5, 4.0)
+        center = np.array([dist * math.cos(ang), -1.0 + radius + rng.uniform(0, 1.2), dist * math.sin(ang)])
+        add_mesh(sv * radius + center, sf, random_material())
+    # ground plane
+    g = 12.0
+    add_mesh(np.array([[-g, -1, -g], [-g, -1, g], [g, -1, g], [g, -1, -g]]), np.array([[0, 1, 2], [0, 2, 3]]),
+             diffuse_material(add_knots(knots_from_curve(0.5))))
+    scene = Scene("mixed_material", width, height, spp, np.concatenate(positions), np.concatenate(triangles),
+                  instances, materials, np.concatenate(knots), max_depth=max_depth)
+    # 2 point + 2 spot lights with blackbody intensities
+    def blackbody_intensity(kelvin, scale):
+        return blackbody_emission(kelvin, scale)
+
+    scene.positional = [
+        {"kind": abi.POINT_LIGHT, "position": (3.0, 4.0, 3.0), "intensity": blackbody_intensity(3200, 60.0)},
+        {"kind": abi.POINT_LIGHT, "position": (-4.0, 3.0, 1.0), "intensity": blackbody_intensity(5000, 40.0)},
+        _spot((0.0, 5.0, 0.5), (0.0, 0.0, 0.0), 25.0, 30.0, blackbody_intensity(6500, 120.0)),
+        _spot((-2.0, 3.0, 4.0), (0.0, -0.5, 0.0), 15.0, 20.0, blackbody_intensity(4000, 80.0)),
+    ]
+    scene.environment = (0.08 * blackbody_shape(9000) / blackbody_shape(9000).max()).astype(np.float32)
+    scene.camera = pinhole_camera((0.0, 1.2, 5.5), (0.0, -0.1, 0.0), (0, 1, 0), 38.0, width, height)
+    return scene
+
+
+def _spot(position, target, start_deg, end_deg, intensity):
+    """Spot light whose light_from_world maps the spot axis to +z (src/render.hpp:183-191)."""
+    p = np.asarray(position, np.float64)
+    z = np.asarray(target, np.float64) - p
+    z /= np.linalg.norm(z)
+    helper = np.array([1.0, 0, 0]) if abs(z[0]) < 0.9 else np.array([0, 1.0, 0])
+    x = np.cross(helper, z)
+    x /= np.linalg.norm(x)
+    y = np.cross(z, x)
+    m = np.stack([x, y, z])  # rows: world -> light
+    return {"kind": abi.SPOT_LIGHT, "position": tuple(p), "intensity": intensity,
+            "light_from_world": tuple(m.reshape(-1)), "cos_falloff_start": math.cos(math.radians(start_deg)),
+            "cos_falloff_end": math.cos(math.radians(end_deg))}

@@ -1,0 +1,105 @@
+"""ctypes access to the oracle (the CPU checker) and to the reference-compiled pin library.
+
+Test infrastructure only.  ``oracle()`` builds oracle/_build/liboracle.so with make when it
+is missing; ``reference()`` returns None when oracle/_ref/libref.so was not built (it is built
+from a rypath checkout by oracle/ref.mk).
+"""
+
+import ctypes as C
+import os
+import subprocess
+
+from rypath_b200 import abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
+REF = os.path.join(ROOT, "oracle", "_ref", "libref.so")
+_oracle = None
+_ref = None
+
+
+def oracle():
+    global _oracle
+    if _oracle is None:
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+        lib = C.CDLL(ORACLE)
+        vp, u32, sz = C.c_void_p, C.c_uint32, C.c_size_t
+        lib.or_scene_create.restype = vp
+        lib.or_scene_create.argtypes = [C.POINTER(abi.SceneDesc), C.c_char_p, sz]
+        lib.or_scene_destroy.argtypes = [vp]
+        lib.or_scene_light_count.argtypes = [vp]
+        lib.or_scene_light_count.restype = u32
+        lib.or_sample.argtypes = [vp, C.POINTER(abi.Request), vp, sz, C.c_int]
+        lib.or_probe_sobol.argtypes = [vp, vp, u32, vp]
+        lib.or_probe_philox.argtypes = [vp, u32, vp]
+        lib.or_probe_wavelengths.argtypes = [vp, u32, u32, vp]
+        lib.or_probe_raygen.argtypes = [vp, C.POINTER(abi.Request), vp, vp, sz]
+        lib.or_probe_bsdf.argtypes = [vp, u32, vp]
+        lib.or_export_bvh.argtypes = [vp, vp, vp, vp, vp, sz]
+        lib.or_trace_rays.argtypes = [vp, vp, u32, C.c_int, C.c_int, vp]
+        lib.or_probe_advance.argtypes = [vp, u32, vp]
+        lib.or_build_light_tables.argtypes = [vp, u32, vp, vp, vp, vp, vp]
+        lib.or_probe_light_select.argtypes = [vp, vp, u32, vp]
+        lib.or_film_add.argtypes = [vp, sz, vp, u32, vp]
+        _oracle = lib
+    return _oracle
+
+
+def reference():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF):
+            return None
+        lib = C.CDLL(REF)
+        vp, u32, sz = C.c_void_p, C.c_uint32, C.c_size_t
+        lib.ref_sobol_tables.restype = vp
+        lib.ref_probe_sobol.argtypes = [vp, u32, vp]
+        lib.ref_probe_philox.argtypes = [vp, u32, vp]
+        lib.ref_probe_wavelengths.argtypes = [vp, u32, u32, vp]
+        lib.ref_probe_advance.argtypes = [vp, u32, vp]
+        lib.ref_probe_bsdf.argtypes = [vp, u32, vp]
+        lib.ref_build_light_tables.argtypes = [vp, u32, vp, vp, vp, vp, vp]
+        lib.ref_light_spectrum_power.argtypes = [vp]
+        lib.ref_light_spectrum_power.restype = C.c_double
+        lib.ref_outward.argtypes = [u32, C.c_int, C.POINTER(C.c_int)]
+        lib.ref_outward.restype = u32
+        lib.ref_set_cie.argtypes = [vp]
+        lib.ref_film_add.argtypes = [vp, sz, u32, u32, vp]
+        _ref = lib
+    return _ref
+
+
+class OracleScene:
+    def __init__(self, scene):
+        self.scene = scene
+        self.desc = scene.desc()
+        diag = C.create_string_buffer(512)
+        self.handle = oracle().or_scene_create(C.byref(self.desc), diag, 512)
+        if not self.handle:
+            raise RuntimeError(diag.value.decode())
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            oracle().or_scene_destroy(self.handle)
+            self.handle = None
+
+    def sample(self, request, threads=0):
+        import numpy as np
+
+        lanes = request.pixel_count * request.sample_count
+        out = np.zeros(lanes, abi.packet_dtype())
+        rc = oracle().or_sample(self.handle, C.byref(request), out.ctypes.data, lanes, threads)
+        if rc < 0:
+            raise RuntimeError("oracle sample rejected the request")
+        return out
+
+
+def request(width, height, spp=1, sample_begin=0, pixel_begin=0, pixel_count=None, seed=1,
+            sampler=abi.SAMPLER_SOBOL, randomization=abi.RANDOMIZE_OWEN):
+    r = abi.Request()
+    r.width, r.height, r.seed = width, height, seed
+    r.pixel_begin = pixel_begin
+    r.pixel_count = width * height if pixel_count is None else pixel_count
+    r.sample_begin, r.sample_count = sample_begin, spp
+    r.emergency_limit, r.sampler_kind, r.randomization, r.boundary_limit = 1024, sampler, randomization, 4096
+    return r

@@ -1,0 +1,266 @@
+"""Pin the oracle: rypath's own known-answer vectors, and bit-for-bit agreement with rypath's
+host-compilable sources compiled where they lie (oracle/_ref, built by oracle/ref.mk).
+
+References: Sobol KATs tests/sampling_tests.cpp:26-142; Philox KATs tests/replay_tests.cpp:22-36;
+visible wavelength checks tests/packet_spectrum_tests.cpp:9-56; light tables
+src/light_sampling.cpp:384-572; packet film src/packet_film.cpp:198-265.
+"""
+
+import ctypes as C
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from rypath_b200 import abi, scenes
+from tests.oracle_lib import oracle, reference
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+TABLES = scenes.sobol_tables()
+TABLE_BUF = C.create_string_buffer(TABLES, len(TABLES))
+
+
+def need_ref():
+    lib = reference()
+    if lib is None:
+        pytest.skip("oracle/_ref/libref.so not built (needs a rypath checkout)")
+    return lib
+
+
+def sobol_query(answer, mode=3):
+    seed = answer["seed"] & 0xFFFFFFFF
+    s = answer["sample"]
+    return [answer["m"], answer["x"], answer["y"], s & 0xFFFFFFFF, s >> 32, answer["dimension"], mode, seed]
+
+
+def test_table_identity_with_reference():
+    lib = need_ref()
+    ref = C.string_at(lib.ref_sobol_tables(), abi.RP_SOBOL_TABLE_BYTES)
+    assert ref == TABLES
+
+
+def test_sobol_known_answers():
+    answers = json.load(open(os.path.join(GOLDEN, "sobol_known_answers.json")))
+    assert len(answers) == 8
+    for a in answers:
+        for mode in range(4):
+            q = np.array(sobol_query(a, mode), np.uint32)
+            out = np.zeros(6, np.uint32)
+            oracle().or_probe_sobol(TABLE_BUF, q.ctypes.data, 1, out.ctypes.data)
+            index = int(out[0]) | (int(out[1]) << 32)
+            assert index == a["index"]
+            assert out[3] == a["hash"]
+            assert out[2] == a["words"][mode], (a, mode)
+        # binary32 pixel remap of the unscrambled camera dimensions (sobol::camera_uniform)
+        for dim, pix in ((0, a["x"]), (1, a["y"])):
+            q = np.array(sobol_query(dict(a, dimension=dim), 0), np.uint32)
+            out = np.zeros(6, np.uint32)
+            oracle().or_probe_sobol(TABLE_BUF, q.ctypes.data, 1, out.ctypes.data)
+            assert float(camera_uniform(int(out[2]), a["m"], pix)) == float.fromhex(a["camera"][dim])
+
+
+ONE_MINUS = np.float32(float.fromhex("0x1.fffffep-1"))
+
+
+def sobol_uniform(word):
+    return min(np.float32(np.float32(word) * np.float32(2.0 ** -32)), ONE_MINUS)
+
+
+def camera_uniform(word, m, pixel):
+    local = np.float32(np.float32(sobol_uniform(word) * np.float32(1 << m)) - np.float32(pixel))
+    return np.float32(0) if local < 0 else min(local, ONE_MINUS)
+
+
+def test_sobol_uniform_special_values():
+    # tests/sampling_tests.cpp:136-141
+    assert sobol_uniform(0xFFFFFFFF) == ONE_MINUS
+    assert sobol_uniform(0) == 0
+    assert float(sobol_uniform(0x80000081)) == float.fromhex("0x1.000002p-1")
+    assert camera_uniform(0x7FFFFFFF, 1, 0) == ONE_MINUS
+
+
+def test_philox_known_answers():
+    kats = json.load(open(os.path.join(GOLDEN, "philox_known_answers.json")))
+    assert len(kats) == 3
+    q = np.array([k["counter"] + k["key"] for k in kats], np.uint32)
+    out = np.zeros((len(kats), 4), np.uint32)
+    oracle().or_probe_philox(q.ctypes.data, len(kats), out.ctypes.data)
+    for k, row in zip(kats, out):
+        assert list(map(int, row)) == k["expected"]
+
+
+def test_sobol_matches_reference_random():
+    lib = need_ref()
+    rng = np.random.default_rng(7)
+    n = 4000
+    m = rng.integers(0, 26, n)
+    x = (rng.integers(0, 2**31, n) % np.maximum(1, 1 << m)).astype(np.uint64)
+    y = (rng.integers(0, 2**31, n) % np.maximum(1, 1 << m)).astype(np.uint64)
+    sample = rng.integers(0, 2**40, n).astype(np.uint64) >> (2 * m).astype(np.uint64)
+    q = np.stack([m, x, y, sample & 0xFFFFFFFF, sample >> 32, rng.integers(0, 1024, n),
+                  rng.integers(0, 4, n), rng.integers(0, 2**32, n)], 1).astype(np.uint32)
+    a = np.zeros((n, 6), np.uint32)
+    b = np.zeros((n, 6), np.uint32)
+    oracle().or_probe_sobol(TABLE_BUF, q.ctypes.data, n, a.ctypes.data)
+    lib.ref_probe_sobol(q.ctypes.data, n, b.ctypes.data)
+    np.testing.assert_array_equal(a, b)
+
+
+def test_philox_matches_reference_random():
+    lib = need_ref()
+    q = np.random.default_rng(3).integers(0, 2**32, (5000, 6)).astype(np.uint32)
+    a = np.zeros((5000, 4), np.uint32)
+    b = np.zeros((5000, 4), np.uint32)
+    oracle().or_probe_philox(q.ctypes.data, 5000, a.ctypes.data)
+    lib.ref_probe_philox(q.ctypes.data, 5000, b.ctypes.data)
+    np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("mode", [abi.HERO_UNIFORM, abi.HERO_VISIBLE])
+def test_hero_wavelengths_match_reference(mode):
+    lib = need_ref()
+    u = np.concatenate([(np.arange(4096) + 0.5) / 4096, np.arange(4096) / 4096,
+                        [np.nextafter(np.float32(1), np.float32(0))]]).astype(np.float32)
+    a = np.zeros((u.size, 8), np.float32)
+    b = np.zeros((u.size, 8), np.float32)
+    oracle().or_probe_wavelengths(u.ctypes.data, u.size, mode, a.ctypes.data)
+    lib.ref_probe_wavelengths(u.ctypes.data, u.size, mode, b.ctypes.data)
+    np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_visible_wavelengths_properties():
+    # tests/packet_spectrum_tests.cpp restated for the hero lattice shift
+    u = np.concatenate([(np.arange(4096) + 0.5) / 4096, np.arange(4096) / 4096]).astype(np.float32)
+    out = np.zeros((u.size, 8), np.float32)
+    oracle().or_probe_wavelengths(u.ctypes.data, u.size, abi.HERO_VISIBLE, out.ctypes.data)
+    lam, pdf = out[:, :4].astype(np.float64), out[:, 4:].astype(np.float64)
+    coord = np.floor(u.astype(np.float64) * 16777216.0).astype(np.int64)
+    for k in range(4):
+        shifted = ((coord + k * 4194304) & 0xFFFFFF) * 2.0 ** -24
+        expect = np.clip(538 - 138.888889 * np.arctanh(.85691062 - 1.82750197 * shifted), 360, 830)
+        assert np.all(np.abs(lam[:, k] - expect) <= 1e-3)
+        c = np.cosh(.0072 * (lam[:, k] - 538))
+        assert np.all(np.abs(pdf[:, k] - .0039398042 / (c * c)) <= 1e-8)
+    bad = np.array([-1, -1e-45, 1, 2, np.inf, np.nan], np.float32)
+    out = np.zeros((bad.size, 8), np.float32)
+    oracle().or_probe_wavelengths(bad.ctypes.data, bad.size, abi.HERO_VISIBLE, out.ctypes.data)
+    assert np.all(~np.isfinite(out))
+
+
+def _advance_queries(n, rng):
+    q = np.zeros((n, 20), np.float32)
+    q[:, 0:4] = rng.uniform(0.5, 1.0, (n, 4))
+    q[:, 4:8] = rng.integers(-160, 60, (n, 4))
+    zero = rng.uniform(size=(n, 4)) < 0.1
+    q[:, 0:4][zero] = 0
+    q[:, 4:8][zero] = 0
+    q[:, 8:12] = np.exp(rng.uniform(-80, 40, (n, 4)))
+    q[:, 12:16] = np.exp(rng.uniform(-60, 20, (n, 4))) * (rng.uniform(size=(n, 4)) > 0.1)
+    q[:, 16:20] = np.exp(rng.uniform(-60, 20, (n, 4))) * (rng.uniform(size=(n, 4)) > 0.1)
+    return q
+
+
+def test_hero_advance_matches_reference():
+    lib = need_ref()
+    q = _advance_queries(20000, np.random.default_rng(11))
+    a = np.zeros((q.shape[0], 13), np.float32)
+    b = np.zeros((q.shape[0], 13), np.float32)
+    oracle().or_probe_advance(q.ctypes.data, q.shape[0], a.ctypes.data)
+    lib.ref_probe_advance(q.ctypes.data, q.shape[0], b.ctypes.data)
+    np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert a[:, 12].mean() > 0.3  # the generator exercises valid updates
+
+
+def bsdf_queries(n, rng):
+    q = np.zeros((n, 16), np.float32)
+    kind = rng.integers(1, 3, n)
+    q[:, 0] = kind
+    q[:, 1] = np.where(kind == 1, rng.uniform(0.1, 3, n), rng.uniform(1.0, 2.4, n))
+    q[:, 2] = rng.uniform(0, 5, n)
+    rough = rng.uniform(0, 0.6, n) * (rng.uniform(size=n) > 0.15)
+    q[:, 3] = rough
+    q[:, 4] = rough * rng.uniform(0.5, 1.5, n)
+    q[:, 5] = rng.integers(0, 2, n)
+    for s in (6, 9):
+        v = rng.normal(size=(n, 3))
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        q[:, s:s + 3] = v
+    q[:, 12:15] = rng.uniform(0, 1, (n, 3))
+    return q
+
+
+def test_bsdf_match_reference():
+    lib = need_ref()
+    q = bsdf_queries(20000, np.random.default_rng(5))
+    a = np.zeros((q.shape[0], 12), np.float32)
+    b = np.zeros((q.shape[0], 12), np.float32)
+    oracle().or_probe_bsdf(q.ctypes.data, q.shape[0], a.ctypes.data)
+    lib.ref_probe_bsdf(q.ctypes.data, q.shape[0], b.ctypes.data)
+    np.testing.assert_array_equal(a[:, :10].view(np.uint32), b[:, :10].view(np.uint32))
+
+
+def light_rows(n, rng):
+    rows = np.zeros((n, 16))
+    rows[:, 0] = rng.uniform(0, 10, n) * (rng.uniform(size=n) > 0.05)
+    rows[:, 1] = np.where(rng.uniform(size=n) < 0.5, -1, rng.uniform(0, 20, n))
+    lo = rng.uniform(-5, 5, (n, 3))
+    rows[:, 2:5] = lo
+    rows[:, 5:8] = lo + rng.uniform(0, 1, (n, 3)) * (rng.uniform(size=(n, 1)) > 0.3)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rows[:, 8:11] = d
+    rows[:, 11] = np.where(rng.uniform(size=n) < 0.5, np.nextafter(np.float32(1), np.float32(0)),
+                           rng.uniform(-1, 1, n))
+    rows[:, 12] = rng.uniform(-1, 1, n) * (rng.uniform(size=n) < 0.3)
+    rows[:, 13] = rng.integers(0, 2, n)
+    rows[:, 14] = rng.uniform(size=n) < 0.05
+    # float32-representable values as the C structs hold them
+    rows[:, 2:13] = rows[:, 2:13].astype(np.float32)
+    return rows
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 64, 300])
+def test_light_tables_match_reference(n):
+    lib = need_ref()
+    rows = light_rows(n, np.random.default_rng(n))
+    outs = []
+    for fn in (oracle().or_build_light_tables, lib.ref_build_light_tables):
+        alias = np.zeros((n, 4), np.uint32)
+        rec = np.zeros((n, 4), np.uint32)
+        nodes = np.zeros((2 * n, 16), np.uint32)
+        inf = np.zeros(n, np.uint32)
+        cnt = C.c_uint32(0)
+        k = fn(rows.ctypes.data, n, alias.ctypes.data, rec.ctypes.data, nodes.ctypes.data, inf.ctypes.data,
+               C.byref(cnt))
+        outs.append((k, alias, rec, nodes[:max(k, 0)], inf[:cnt.value]))
+    (ka, *a), (kb, *b) = outs
+    assert ka == kb
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_film_reduction_matches_packet_film_batch():
+    lib = need_ref()
+    cie = scenes.cie_xyz()
+    lib.ref_set_cie(np.ascontiguousarray(cie).ctypes.data)
+    rng = np.random.default_rng(2)
+    w, h, spp = 8, 5, 6
+    res = np.zeros(w * h * spp, abi.packet_dtype())
+    lane = np.arange(res.size)
+    res["pixel"] = lane % (w * h)
+    res["sample_low"] = lane // (w * h)
+    res["wavelengths"] = rng.uniform(360, 830, (res.size, 4))
+    res["wavelength_pdfs"] = rng.uniform(0.001, 0.004, (res.size, 4))
+    res["radiance"] = rng.exponential(1.0, (res.size, 4)) * (rng.uniform(size=(res.size, 4)) > 0.3)
+    res["filter_weight"] = 1.0
+    ref_out = np.zeros((w * h, 9))
+    assert lib.ref_film_add(res.ctypes.data, res.size, w, h, ref_out.ctypes.data) == 0
+    film = np.zeros(w * h, abi.film_dtype())
+    assert oracle().or_film_add(res.ctypes.data, res.size, np.ascontiguousarray(cie).ctypes.data, w * h,
+                                film.ctypes.data) == 0
+    np.testing.assert_array_equal(film["sum"], ref_out[:, 0:3])
+    np.testing.assert_array_equal(film["correction"], ref_out[:, 3:6])
+    np.testing.assert_array_equal(film["weight_sum"], ref_out[:, 6])
+    np.testing.assert_array_equal(film["count"], ref_out[:, 8])
