@@ -266,6 +266,11 @@ rp_status rp_cuda_render_film_device(struct rp_scene *scene, const rp_film_reque
                                      rp_film_pixel *device_film, char *diag,
                                      size_t diag_capacity);
 
+/* CIE 1931 2-degree colour matching functions at 1 nm, 360..830 (471 rows of x, y, z as
+ * doubles): the sensor response of packet_sensor_xyz (src/packet_film.cpp:102-114, table of
+ * src/render.cpp:2147-2152).  Required before the film entry points. */
+rp_status rp_cuda_set_cie(struct rp_scene *scene, const double *cie_xyz);
+
 /* ---- instrumentation ------------------------------------------------------------------ */
 
 /* Timing of the last sample/film call on this scene. */
@@ -297,9 +302,11 @@ rp_status rp_cuda_probe_raygen(struct rp_scene *scene, const rp_request *request
  * weight, sample pdf, flags, eta, pad, pad}. */
 rp_status rp_cuda_probe_bsdf(const float *queries, uint32_t count, float *results, char *diag,
                              size_t diag_capacity);
-/* Export the scene's binary LBVH: per internal node {left, right, parent} (n-1 nodes,
- * child index >= n-1 means leaf n-1+i... see DESIGN), leaf order (n triangle ids),
- * sorted Morton keys (n) and node bounds (2n-1 boxes of 6 floats). */
+/* Export the scene's binary LBVH over its n triangles: per internal node {left, right,
+ * parent} (n-1 nodes; a child with bit 31 set is leaf slot child & 0x7fffffff, the root's
+ * parent is RP_NONE), the leaf order (triangle id of each leaf slot), the sorted 63-bit
+ * Morton keys, and bounds {lo[3], hi[3]}: internal node i at row i, leaf slot j at row n-1+j.
+ * capacity is in triangles. */
 rp_status rp_cuda_scene_export_bvh(struct rp_scene *scene, uint32_t *nodes, uint32_t *leaf_order,
                                    uint64_t *keys, float *bounds, size_t capacity, char *diag,
                                    size_t diag_capacity);
@@ -308,6 +315,19 @@ rp_status rp_cuda_scene_export_bvh(struct rp_scene *scene, uint32_t *nodes, uint
  * primitive RP_NONE bits = miss).  For occlusion only field 0 (1 = occluded) is used. */
 rp_status rp_cuda_trace_rays(struct rp_scene *scene, const float *rays, uint32_t count,
                              int any_hit, float *hits, char *diag, size_t diag_capacity);
+
+/* ---- host helpers ----------------------------------------------------------------------- */
+
+/* sizeof() of an ABI struct by name ("rp_request", ...), 0 if unknown; lets bindings check
+ * their layouts against this library. */
+uint32_t rp_cuda_abi_size(const char *type_name);
+/* The light-selection tables rp_cuda_scene_create builds, for inspection: build_light_sampling
+ * (src/light_sampling.cpp:384-572).  Rows of 16 doubles {power, bounds_power, low[3],
+ * high[3], direction[3], cos_outer, cos_emission, two_sided, infinite, unused}; outputs are
+ * LightAlias (4 words each), LightRecord (4 words each), LightBounds (16 words each) and the
+ * infinite-light ids.  Returns the node count, or -1 on invalid input. */
+int rp_cuda_build_light_tables(const double *rows, uint32_t count, uint32_t *alias, uint32_t *records,
+                               uint32_t *nodes, uint32_t *infinite, uint32_t *infinite_count);
 
 #ifdef __cplusplus
 }

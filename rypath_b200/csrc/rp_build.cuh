@@ -1,0 +1,313 @@
+// GPU LBVH construction: world-space triangles, 63-bit Morton codes of their centroids, a
+// stable LSB radix sort, Karras's binary radix-tree topology and an atomic bottom-up refit.
+// Every step is exact (integer work, min/max), so the tree equals a CPU build of the same
+// algorithm bit for bit.
+#pragma once
+
+#include "rp_scene.cuh"
+
+namespace rp {
+
+RP_DEV int ordered(float f) {
+    const int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+RP_HD float unordered_host(int i) {
+    const int v = i >= 0 ? i : i ^ 0x7fffffff;
+    float f;
+    memcpy(&f, &v, 4);
+    return f;
+}
+
+struct BuildTmp {
+    float4 *box_lo, *box_hi; // per triangle (original order)
+    int *cbounds;            // ordered-int centroid min[3], max[3]
+    u64 *keys[2];
+    u32 *vals[2];
+    u32 *hist;
+    u32 *left, *right, *parent, *leaf_parent;
+    float4 *node_lo, *node_hi; // internal node bounds
+    u32 *flags;
+};
+
+// World-space vertices, boxes and centroid bounds of every triangle.
+__global__ void k_tri_prepare(const __grid_constant__ DeviceScene s, float4 *world, BuildTmp t) {
+    __shared__ int smin[3][32], smax[3][32];
+    int lmin[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, lmax[3] = {int(0x80000000), int(0x80000000), int(0x80000000)};
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < s.prim_count; i += gridDim.x * blockDim.x) {
+        const DInstance &in = s.instances[s.tri_instance[i]];
+        const u32 *tri = s.triangles + 3 * (in.triangle_begin + s.tri_local[i]);
+        V3 v[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            v[k] = world_point(in, load3(s.positions + 3 * (in.vertex_begin + tri[k])));
+            world[3 * i + k] = make_float4(v[k].x, v[k].y, v[k].z, 0);
+        }
+        const V3 lo = v3(fminf(fminf(v[0].x, v[1].x), v[2].x), fminf(fminf(v[0].y, v[1].y), v[2].y),
+                         fminf(fminf(v[0].z, v[1].z), v[2].z));
+        const V3 hi = v3(fmaxf(fmaxf(v[0].x, v[1].x), v[2].x), fmaxf(fmaxf(v[0].y, v[1].y), v[2].y),
+                         fmaxf(fmaxf(v[0].z, v[1].z), v[2].z));
+        t.box_lo[i] = make_float4(lo.x, lo.y, lo.z, 0);
+        t.box_hi[i] = make_float4(hi.x, hi.y, hi.z, 0);
+        const float c[3] = {0.5f * lo.x + 0.5f * hi.x, 0.5f * lo.y + 0.5f * hi.y, 0.5f * lo.z + 0.5f * hi.z};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            lmin[a] = min(lmin[a], ordered(c[a]));
+            lmax[a] = max(lmax[a], ordered(c[a]));
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        for (int o = 16; o > 0; o >>= 1) {
+            lmin[a] = min(lmin[a], __shfl_xor_sync(0xffffffffu, lmin[a], o));
+            lmax[a] = max(lmax[a], __shfl_xor_sync(0xffffffffu, lmax[a], o));
+        }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+        for (int a = 0; a < 3; ++a) {
+            smin[a][warp] = lmin[a];
+            smax[a][warp] = lmax[a];
+        }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        const int a = threadIdx.x;
+        int mn = 0x7fffffff, mx = int(0x80000000);
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) {
+            mn = min(mn, smin[a][w]);
+            mx = max(mx, smax[a][w]);
+        }
+        atomicMin(t.cbounds + a, mn);
+        atomicMax(t.cbounds + 3 + a, mx);
+    }
+}
+
+RP_DEV u64 spread21(u64 x) {
+    x &= 0x1fffff;
+    x = (x | x << 32) & 0x1f00000000ffffull;
+    x = (x | x << 16) & 0x1f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+}
+__global__ void k_morton(u32 n, BuildTmp t, float3 lo, float3 ext) {
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 bl = t.box_lo[i], bh = t.box_hi[i];
+        const float c[3] = {0.5f * bl.x + 0.5f * bh.x, 0.5f * bl.y + 0.5f * bh.y, 0.5f * bl.z + 0.5f * bh.z};
+        const float l[3] = {lo.x, lo.y, lo.z}, e[3] = {ext.x, ext.y, ext.z};
+        u64 q[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float tt = e[a] > 0 ? (c[a] - l[a]) / e[a] : 0.0f;
+            float cell = tt * 2097152.0f;
+            cell = fminf(fmaxf(cell, 0.0f), 2097151.0f);
+            q[a] = u64(cell);
+        }
+        t.keys[0][i] = (spread21(q[0]) << 2) | (spread21(q[1]) << 1) | spread21(q[2]);
+        t.vals[0][i] = i;
+    }
+}
+
+// ---- stable LSB radix sort, 8-bit digits, tiles of 256 threads x 8 items
+constexpr int kSortThreads = 256, kSortItems = 8, kSortTile = kSortThreads * kSortItems;
+
+__global__ void __launch_bounds__(kSortThreads) k_radix_hist(const u64 *keys, u32 n, int shift, u32 *hist, u32 tiles) {
+    __shared__ u32 h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const u32 base = blockIdx.x * kSortTile;
+    for (int c = 0; c < kSortItems; ++c) {
+        const u32 i = base + c * kSortThreads + threadIdx.x;
+        if (i < n)
+            atomicAdd(h + u32((keys[i] >> shift) & 0xff), 1u);
+    }
+    __syncthreads();
+    hist[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
+}
+// exclusive scan of hist (digit-major) in one block
+__global__ void __launch_bounds__(1024) k_radix_scan(u32 *hist, u32 total) {
+    __shared__ u32 warp_sums[32];
+    __shared__ u32 carry;
+    if (threadIdx.x == 0)
+        carry = 0;
+    __syncthreads();
+    for (u32 base = 0; base < total; base += 1024) {
+        const u32 i = base + threadIdx.x;
+        const u32 v = i < total ? hist[i] : 0;
+        u32 x = v;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int o = 1; o < 32; o <<= 1) {
+            const u32 y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o)
+                x += y;
+        }
+        if (lane == 31)
+            warp_sums[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            u32 w = warp_sums[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const u32 y = __shfl_up_sync(0xffffffffu, w, o);
+                if (lane >= o)
+                    w += y;
+            }
+            warp_sums[lane] = w;
+        }
+        __syncthreads();
+        const u32 incl = x + (warp > 0 ? warp_sums[warp - 1] : 0) + carry;
+        if (i < total)
+            hist[i] = incl - v;
+        __syncthreads();
+        if (threadIdx.x == 1023)
+            carry = incl;
+        __syncthreads();
+    }
+}
+__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const u64 *kin, const u32 *vin, u64 *kout, u32 *vout,
+                                                                 u32 n, int shift, const u32 *hist, u32 tiles) {
+    __shared__ u32 digit_base[256];
+    __shared__ u32 warp_counts[kSortThreads / 32][256];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    digit_base[threadIdx.x] = hist[threadIdx.x * tiles + blockIdx.x];
+    for (int w = 0; w < kSortThreads / 32; ++w)
+        warp_counts[w][threadIdx.x] = 0;
+    __syncthreads();
+    const u32 base = blockIdx.x * kSortTile;
+    for (int c = 0; c < kSortItems; ++c) {
+        const u32 i = base + c * kSortThreads + threadIdx.x;
+        const bool valid = i < n;
+        const u64 key = valid ? kin[i] : 0;
+        const u32 val = valid ? vin[i] : 0;
+        const u32 d = valid ? u32((key >> shift) & 0xff) : 0x100u;
+        const u32 peers = __match_any_sync(0xffffffffu, d);
+        const u32 rank = __popc(peers & ((1u << lane) - 1));
+        if (valid && rank == 0)
+            warp_counts[warp][d] = __popc(peers);
+        __syncthreads();
+        if (valid) {
+            u32 offset = digit_base[d] + rank;
+            for (int w = 0; w < warp; ++w)
+                offset += warp_counts[w][d];
+            kout[offset] = key;
+            vout[offset] = val;
+        }
+        __syncthreads();
+        u32 sum = 0;
+        for (int w = 0; w < kSortThreads / 32; ++w) {
+            sum += warp_counts[w][threadIdx.x];
+            warp_counts[w][threadIdx.x] = 0;
+        }
+        digit_base[threadIdx.x] += sum;
+        __syncthreads();
+    }
+}
+
+// Karras 2012, "Maximizing parallelism in the construction of BVHs, octrees and k-d trees".
+RP_DEV int karras_delta(const u64 *keys, u32 n, long i, long j) {
+    if (j < 0 || j >= long(n))
+        return -1;
+    const u64 a = keys[i], c = keys[j];
+    if (a != c)
+        return __clzll(a ^ c);
+    return 64 + __clz(u32(i) ^ u32(j));
+}
+__global__ void k_karras(const u64 *keys, u32 n, BuildTmp t) {
+    for (u32 ii = blockIdx.x * blockDim.x + threadIdx.x; ii + 1 < n; ii += gridDim.x * blockDim.x) {
+        const long i = ii;
+        const int d = (karras_delta(keys, n, i, i + 1) - karras_delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+        const int dmin = karras_delta(keys, n, i, i - d);
+        long lmax = 2;
+        while (karras_delta(keys, n, i, i + lmax * d) > dmin)
+            lmax *= 2;
+        long l = 0;
+        for (long s = lmax / 2; s >= 1; s /= 2)
+            if (karras_delta(keys, n, i, i + (l + s) * d) > dmin)
+                l += s;
+        const long j = i + l * d;
+        const int dnode = karras_delta(keys, n, i, j);
+        long s = 0;
+        for (long div = 2;; div *= 2) {
+            const long step = (l + div - 1) / div;
+            if (karras_delta(keys, n, i, i + (s + step) * d) > dnode)
+                s += step;
+            if (step == 1)
+                break;
+        }
+        const long gamma = i + s * d + (d < 0 ? d : 0);
+        const long first = i < j ? i : j, last = i < j ? j : i;
+        const u32 lc = first == gamma ? (kLeaf | u32(gamma)) : u32(gamma);
+        const u32 rc = last == gamma + 1 ? (kLeaf | u32(gamma + 1)) : u32(gamma + 1);
+        t.left[i] = lc;
+        t.right[i] = rc;
+        if (lc & kLeaf)
+            t.leaf_parent[lc & ~kLeaf] = u32(i);
+        else
+            t.parent[lc] = u32(i);
+        if (rc & kLeaf)
+            t.leaf_parent[rc & ~kLeaf] = u32(i);
+        else
+            t.parent[rc] = u32(i);
+    }
+}
+// Bottom-up refit: the second child to arrive at a node writes its bounds.
+__global__ void k_refit(u32 n, const u32 *order, BuildTmp t) {
+    for (u32 slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
+        u32 node = t.leaf_parent[slot];
+        // a path from a leaf to the root is shorter than 64 + 32 levels for unique-by-index keys
+        for (int level = 0; node != kNone && level < 160; ++level) {
+            __threadfence();
+            if (atomicAdd(t.flags + node, 1u) == 0)
+                break;
+            __threadfence();
+            float4 lo[2], hi[2];
+            const u32 ch[2] = {t.left[node], t.right[node]};
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                if (ch[k] & kLeaf) {
+                    const u32 prim = order[ch[k] & ~kLeaf];
+                    lo[k] = __ldcg(t.box_lo + prim);
+                    hi[k] = __ldcg(t.box_hi + prim);
+                } else {
+                    lo[k] = __ldcg(t.node_lo + ch[k]);
+                    hi[k] = __ldcg(t.node_hi + ch[k]);
+                }
+            }
+            __stcg(t.node_lo + node, make_float4(fminf(lo[0].x, lo[1].x), fminf(lo[0].y, lo[1].y), fminf(lo[0].z, lo[1].z), 0));
+            __stcg(t.node_hi + node, make_float4(fmaxf(hi[0].x, hi[1].x), fmaxf(hi[0].y, hi[1].y), fmaxf(hi[0].z, hi[1].z), 0));
+            node = t.parent[node];
+        }
+    }
+}
+// Traversal layout: child boxes inside each node; leaf triangles in leaf-slot order.
+__global__ void k_pack(u32 n, const u32 *order, const float4 *world, BuildTmp t, BNode *nodes, float4 *leaf_v) {
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const u32 prim = order[i];
+        const float4 a = world[3 * prim];
+        leaf_v[3 * i] = make_float4(a.x, a.y, a.z, __uint_as_float(prim));
+        leaf_v[3 * i + 1] = world[3 * prim + 1];
+        leaf_v[3 * i + 2] = world[3 * prim + 2];
+        if (i + 1 < n) {
+            float4 lo[2], hi[2];
+            const u32 ch[2] = {t.left[i], t.right[i]};
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                if (ch[k] & kLeaf) {
+                    const u32 p = order[ch[k] & ~kLeaf];
+                    lo[k] = t.box_lo[p];
+                    hi[k] = t.box_hi[p];
+                } else {
+                    lo[k] = t.node_lo[ch[k]];
+                    hi[k] = t.node_hi[ch[k]];
+                }
+            }
+            BNode b;
+            b.a = make_float4(lo[0].x, lo[0].y, lo[0].z, hi[0].x);
+            b.b = make_float4(hi[0].y, hi[0].z, lo[1].x, lo[1].y);
+            b.c = make_float4(lo[1].z, hi[1].x, hi[1].y, hi[1].z);
+            b.d = make_uint4(ch[0], ch[1], 0, 0);
+            nodes[i] = b;
+        }
+    }
+}
+
+} // namespace rp

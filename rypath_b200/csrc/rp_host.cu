@@ -1,0 +1,1396 @@
+// C ABI of the B200 spectral path-tracing backend (include/rypath_cuda.h): scene upload,
+// light-selection tables, LBVH build, wave scheduling of the wavefront kernels, device film
+// and probes.  No exception crosses the boundary; every entry point returns an rp_status.
+#include "../../include/rypath_cuda.h"
+#include "rp_build.cuh"
+#include "rp_probes.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cfloat>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <numbers>
+#include <string>
+#include <vector>
+
+using namespace rp;
+
+namespace {
+
+void set_diag(char *diag, size_t cap, const char *fmt, ...) {
+    if (!diag || !cap)
+        return;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(diag, cap, fmt, ap);
+    va_end(ap);
+}
+
+struct CudaError {
+    cudaError_t code;
+    const char *what;
+};
+#define RP_CHECK(call)                                                                                                 \
+    do {                                                                                                               \
+        const cudaError_t rp_e = (call);                                                                               \
+        if (rp_e != cudaSuccess)                                                                                       \
+            throw CudaError{rp_e, #call};                                                                              \
+    } while (0)
+
+struct Invalid {
+    std::string what;
+};
+
+// ---------------------------------------------------------------- host light tables
+// PBRT light-BVH construction as rypath performs it on the host (src/light_sampling.cpp:217-572).
+struct LightInput {
+    double power = 0, bounds_power = -1;
+    float low[3] = {0, 0, 0}, high[3] = {0, 0, 0}, direction[3] = {0, 0, 1};
+    float cos_outer = -1, cos_emission = 0;
+    bool two_sided = true, infinite = false;
+};
+struct LightTables {
+    std::vector<DLightAlias> alias;
+    std::vector<DLightRecord> records;
+    std::vector<DLightBounds> nodes;
+    std::vector<u32> infinite;
+};
+using D3 = std::array<double, 3>;
+double d3dot(D3 a, D3 b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+double d3norm(D3 a) { return std::sqrt(d3dot(a, a)); }
+D3 d3of(const float *a) { return {a[0], a[1], a[2]}; }
+
+// union of two light bounds with a conservative normal cone (src/light_sampling.cpp:226-276)
+LightInput light_union(const LightInput &a, const LightInput &b) {
+    if (a.power == 0)
+        return b;
+    if (b.power == 0)
+        return a;
+    LightInput r = a;
+    r.power = a.power + b.power;
+    r.two_sided = a.two_sided || b.two_sided;
+    r.cos_emission = std::min(a.cos_emission, b.cos_emission);
+    for (int i = 0; i < 3; ++i) {
+        r.low[i] = std::min(a.low[i], b.low[i]);
+        r.high[i] = std::max(a.high[i], b.high[i]);
+    }
+    const double pi = std::numbers::pi;
+    const double ta = std::acos(std::clamp(double(a.cos_outer), -1., 1.));
+    const double tb = std::acos(std::clamp(double(b.cos_outer), -1., 1.));
+    const D3 wa = d3of(a.direction), wb = d3of(b.direction);
+    const double angle = std::acos(std::clamp(d3dot(wa, wb), -1., 1.));
+    if (std::min(angle + tb, pi) <= ta)
+        return r;
+    if (std::min(angle + ta, pi) <= tb) {
+        std::copy(b.direction, b.direction + 3, r.direction);
+        r.cos_outer = b.cos_outer;
+        return r;
+    }
+    const double theta = (ta + tb + angle) / 2 + 1e-6;
+    if (theta >= pi) {
+        r.cos_outer = -1;
+        r.direction[0] = r.direction[1] = 0;
+        r.direction[2] = 1;
+        return r;
+    }
+    D3 tangent;
+    for (int i = 0; i < 3; ++i)
+        tangent[i] = wb[i] - d3dot(wa, wb) * wa[i];
+    double length = d3norm(tangent);
+    if (length < 1e-12) {
+        const int axis = std::abs(wa[0]) < .8 ? 0 : 1;
+        D3 basis{0, 0, 0};
+        basis[axis] = 1;
+        for (int i = 0; i < 3; ++i)
+            tangent[i] = basis[i] - wa[axis] * wa[i];
+        length = d3norm(tangent);
+    }
+    const double rotate = theta - ta;
+    for (int i = 0; i < 3; ++i)
+        r.direction[i] = float(std::cos(rotate) * wa[i] + std::sin(rotate) * tangent[i] / length);
+    const double dl = d3norm(d3of(r.direction));
+    for (int i = 0; i < 3; ++i)
+        r.direction[i] = float(r.direction[i] / dl);
+    r.cos_outer = std::nextafter(float(std::cos(theta)), -INFINITY);
+    return r;
+}
+// PBRT EvaluateCost (src/light_sampling.cpp:277-292)
+double light_cost(const LightInput &b, const LightInput &all, int axis) {
+    if (b.power == 0)
+        return 0;
+    const double pi = std::numbers::pi;
+    const double o = std::acos(std::clamp(double(b.cos_outer), -1., 1.));
+    const double e = std::acos(std::clamp(double(b.cos_emission), -1., 1.));
+    const double w = std::min(o + e, pi);
+    const double omega =
+        2 * pi * (1 - b.cos_outer) + pi / 2 * (2 * w * std::sin(o) - std::cos(o - 2 * w) - 2 * o * std::sin(o) + b.cos_outer);
+    const D3 d{double(b.high[0]) - b.low[0], double(b.high[1]) - b.low[1], double(b.high[2]) - b.low[2]};
+    const D3 ad{double(all.high[0]) - all.low[0], double(all.high[1]) - all.low[1], double(all.high[2]) - all.low[2]};
+    if (ad[axis] <= 0)
+        return INFINITY;
+    return b.power * omega * (std::max({ad[0], ad[1], ad[2]}) / ad[axis]) * 2 * (d[0] * d[1] + d[1] * d[2] + d[2] * d[0]);
+}
+// src/light_sampling.cpp:384-572
+bool build_light_tables(const std::vector<LightInput> &in, LightTables &out, std::string &error) {
+    out = {};
+    out.records.assign(in.size(), {kNone, 0, 0, 0});
+    out.alias.assign(in.size(), {0, 0, 0, 0});
+    if (in.empty())
+        return true;
+    double total = 0, bounds_total = 0;
+    std::vector<double> prob(in.size());
+    std::vector<LightInput> bvh(in.begin(), in.end());
+    std::vector<u32> finite;
+    for (size_t i = 0; i < in.size(); ++i) {
+        const auto &v = in[i];
+        if (!(v.power >= 0 && std::isfinite(v.power))) {
+            error = "Invalid light sampling power";
+            return false;
+        }
+        auto &b = bvh[i];
+        b.power = v.bounds_power < 0 ? v.power : v.bounds_power;
+        if (b.power == 0 && v.power > 0)
+            b.power = v.power;
+        prob[i] = v.power == 0 && b.power > 0 ? b.power : v.power;
+        total += prob[i];
+        if (!v.infinite)
+            bounds_total += b.power;
+        if (v.infinite) {
+            out.infinite.push_back(u32(i));
+            out.records[i].flags = 1;
+        } else if (b.power > 0)
+            finite.push_back(u32(i));
+    }
+    if (!std::isfinite(total) || !std::isfinite(bounds_total)) {
+        error = "Light sampling total power overflow";
+        return false;
+    }
+    // Walker alias table (Vose)
+    std::vector<u32> small, large;
+    for (size_t i = 0; i < in.size(); ++i) {
+        const double p = total > 0 ? prob[i] / total : 1. / double(in.size());
+        out.alias[i].pmf = float(p);
+        prob[i] = p * double(in.size());
+        (prob[i] < 1 ? small : large).push_back(u32(i));
+    }
+    while (!small.empty() && !large.empty()) {
+        const u32 s = small.back();
+        small.pop_back();
+        const u32 l = large.back();
+        large.pop_back();
+        out.alias[s].threshold = float(prob[s]);
+        out.alias[s].alias = l;
+        prob[l] -= 1 - prob[s];
+        (prob[l] < 1 ? small : large).push_back(l);
+    }
+    for (u32 i : small)
+        out.alias[i] = {1, out.alias[i].pmf, i, 0};
+    for (u32 i : large)
+        out.alias[i] = {1, out.alias[i].pmf, i, 0};
+    auto bucket_of = [](const LightInput &v, int axis, const double *clo, const double *chi) {
+        return std::min(11u, unsigned(12 * ((double(v.low[axis]) + v.high[axis]) / 2 - clo[axis]) / (chi[axis] - clo[axis])));
+    };
+    std::function<u32(size_t, size_t, u32, unsigned)> build = [&](size_t begin, size_t end, u32 parent,
+                                                                 unsigned depth) -> u32 {
+        const u32 index = u32(out.nodes.size());
+        out.nodes.emplace_back();
+        LightInput bounds;
+        double clo[3] = {INFINITY, INFINITY, INFINITY}, chi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (size_t k = begin; k < end; ++k) {
+            const auto &v = bvh[finite[k]];
+            bounds = light_union(bounds, v);
+            for (int a = 0; a < 3; ++a) {
+                const double c = (double(v.low[a]) + v.high[a]) / 2;
+                clo[a] = std::min(clo[a], c);
+                chi[a] = std::max(chi[a], c);
+            }
+        }
+        DLightBounds node{};
+        node.parent = parent;
+        node.light = kNone;
+        for (int a = 0; a < 3; ++a) {
+            node.low[a] = bounds.low[a];
+            node.high[a] = bounds.high[a];
+            node.direction[a] = bounds.direction[a];
+        }
+        node.power = float(bounds.power / bounds_total);
+        node.cos_outer = bounds.cos_outer;
+        node.cos_emission = bounds.cos_emission;
+        node.flags = bounds.two_sided ? 1 : 0;
+        if (end - begin == 1) {
+            node.light = finite[begin];
+            out.records[finite[begin]].leaf = index;
+        } else {
+            double best = INFINITY;
+            int split_axis = 0;
+            unsigned split_bucket = 0;
+            bool found = false;
+            if (depth < 48)
+                for (int axis = 0; axis < 3; ++axis) {
+                    if (clo[axis] == chi[axis])
+                        continue;
+                    std::array<LightInput, 12> buckets{};
+                    for (size_t k = begin; k < end; ++k) {
+                        const auto &v = bvh[finite[k]];
+                        const unsigned b = bucket_of(v, axis, clo, chi);
+                        buckets[b] = light_union(buckets[b], v);
+                    }
+                    for (unsigned split = 1; split < 11; ++split) {
+                        LightInput l, r;
+                        for (unsigned k = 0; k <= split; ++k)
+                            l = light_union(l, buckets[k]);
+                        for (unsigned k = split + 1; k < 12; ++k)
+                            r = light_union(r, buckets[k]);
+                        const double c = light_cost(l, bounds, axis) + light_cost(r, bounds, axis);
+                        if (c > 0 && c < best) {
+                            best = c;
+                            split_axis = axis;
+                            split_bucket = split;
+                            found = true;
+                        }
+                    }
+                }
+            size_t mid = begin + (end - begin) / 2;
+            if (found) {
+                auto it = std::stable_partition(finite.begin() + std::ptrdiff_t(begin), finite.begin() + std::ptrdiff_t(end),
+                                                [&](u32 id) { return bucket_of(bvh[id], split_axis, clo, chi) <= split_bucket; });
+                const size_t candidate = size_t(it - finite.begin());
+                if (candidate > begin && candidate < end)
+                    mid = candidate;
+            }
+            build(begin, mid, index, depth + 1);
+            node.child = build(mid, end, index, depth + 1);
+        }
+        out.nodes[index] = node;
+        return index;
+    };
+    if (!finite.empty())
+        build(0, finite.size(), kNone, 0);
+    return true;
+}
+
+// src/packet_spectrum_shared.h:33-59 and src/light_sampling.cpp:17-27
+double light_spectrum_power(const float *spectrum) {
+    double value = 0;
+    for (int i = 0; i < 4; ++i) {
+        float up = .5f + float(i) * .25f;
+        if (up > 1)
+            up -= 1;
+        float w = 538 - 138.888889f * std::atanh(.85691062f - 1.82750197f * up);
+        w = std::clamp(w, 360.f, 830.f);
+        const float c = std::cosh(.0072f * (w - 538));
+        const float pdf = .0039398042f / (c * c);
+        value += double(spectrum[unsigned(std::round(w) - 360)]) / pdf / 4;
+    }
+    if (value == 0)
+        for (int i = 0; i < 471; ++i)
+            value += spectrum[i];
+    return value;
+}
+
+// ---------------------------------------------------------------- device buffers
+template <class T> T *dalloc(std::vector<void *> &owned, size_t count) {
+    void *p = nullptr;
+    RP_CHECK(cudaMalloc(&p, std::max<size_t>(1, count) * sizeof(T)));
+    owned.push_back(p);
+    return static_cast<T *>(p);
+}
+template <class T> T *dupload(std::vector<void *> &owned, const T *src, size_t count, cudaStream_t st) {
+    T *p = dalloc<T>(owned, count);
+    if (count)
+        RP_CHECK(cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyHostToDevice, st));
+    return p;
+}
+
+int grid_for(int sm_count, u32 work, int block, int per_sm) {
+    const u32 needed = (work + block - 1) / block;
+    return int(std::max<u32>(1, std::min<u32>(needed, u32(sm_count * per_sm))));
+}
+
+} // namespace
+
+// ---------------------------------------------------------------- scene
+struct rp_scene {
+    int device = 0, sm_count = 148;
+    cudaStream_t stream = nullptr;
+    std::vector<void *> owned;   // scene lifetime
+    std::vector<void *> pool_owned;
+    DeviceScene ds{};
+    u32 n = 0;
+    // build products kept for export
+    u64 *keys = nullptr;
+    u32 *order = nullptr;
+    BuildTmp tmp{};
+    // wavefront pool
+    PathPool pool{};
+    u32 capacity = 0;
+    unsigned long long *stats = nullptr;
+    double *cie = nullptr;
+    rp_film_pixel *film_stage = nullptr;
+    size_t film_stage_pixels = 0;
+    bool counting = false;
+    rp_timing timing{};
+    std::vector<cudaEvent_t> events;
+    size_t event_cursor = 0;
+    std::vector<int> event_kind;
+    double light_power_total = 0;
+
+    ~rp_scene() {
+        if (device >= 0)
+            cudaSetDevice(device);
+        if (stream)
+            cudaStreamSynchronize(stream);
+        for (void *p : pool_owned)
+            cudaFree(p);
+        for (void *p : owned)
+            cudaFree(p);
+        for (auto e : events)
+            cudaEventDestroy(e);
+        if (stream)
+            cudaStreamDestroy(stream);
+    }
+
+    // timing: pairs of events around launches, grouped by kind (0 trace, 1 shadow, 2 shade, 3 other)
+    void mark(int kind) {
+        if (event_cursor + 2 > events.size()) {
+            for (int k = 0; k < 64; ++k) {
+                cudaEvent_t e;
+                RP_CHECK(cudaEventCreate(&e));
+                events.push_back(e);
+            }
+        }
+        RP_CHECK(cudaEventRecord(events[event_cursor], stream));
+        event_kind.push_back(kind);
+    }
+    void done() {
+        RP_CHECK(cudaEventRecord(events[event_cursor + 1], stream));
+        event_cursor += 2;
+    }
+    void collect() {
+        RP_CHECK(cudaStreamSynchronize(stream));
+        double sums[4] = {0, 0, 0, 0};
+        for (size_t i = 0; i < event_kind.size(); ++i) {
+            float ms = 0;
+            RP_CHECK(cudaEventElapsedTime(&ms, events[2 * i], events[2 * i + 1]));
+            sums[event_kind[i]] += ms;
+        }
+        timing.trace_ms = sums[0];
+        timing.shadow_ms = sums[1];
+        timing.shade_ms = sums[2];
+        timing.other_ms = sums[3];
+        timing.kernel_launches = event_kind.size();
+        event_kind.clear();
+        event_cursor = 0;
+    }
+
+    void ensure_pool(u32 lanes) {
+        if (lanes <= capacity)
+            return;
+        RP_CHECK(cudaStreamSynchronize(stream));
+        for (void *p : pool_owned)
+            cudaFree(p);
+        pool_owned.clear();
+        capacity = 0;
+        const size_t c = lanes;
+        PathPool &q = pool;
+        q.ident = dalloc<uint4>(pool_owned, c);
+        q.cursor = dalloc<uint4>(pool_owned, c);
+        float4 **f4[] = {&q.lambda, &q.lambda_pdf, &q.beta, &q.radiance, &q.dens_f, &q.prev_f, &q.eta_scale, &q.ray_o,
+                         &q.ray_d, &q.latest_p, &q.latest_n, &q.latest_param, &q.latest_k, &q.preceding, &q.hit,
+                         &q.sh_o, &q.sh_d, &q.sh_c};
+        for (auto p : f4)
+            *p = dalloc<float4>(pool_owned, c);
+        q.dens_e = dalloc<int4>(pool_owned, c);
+        q.prev_e = dalloc<int4>(pool_owned, c);
+        q.queue[0] = dalloc<u32>(pool_owned, c);
+        q.queue[1] = dalloc<u32>(pool_owned, c);
+        q.counters = dalloc<u32>(pool_owned, 8);
+        q.stats = stats;
+        capacity = lanes;
+    }
+};
+
+namespace {
+
+WaveParams wave_params(const rp_request &r) {
+    WaveParams p{};
+    p.width = r.width;
+    p.height = r.height;
+    p.pixel_begin = r.pixel_begin;
+    p.pixel_count = r.pixel_count;
+    p.sample_low = u32(r.sample_begin);
+    p.sample_high = u32(r.sample_begin >> 32);
+    p.seed_low = u32(r.seed);
+    p.seed_high = u32(r.seed >> 32);
+    p.sampler = r.sampler_kind;
+    p.randomization = r.randomization;
+    u32 v = std::max(std::max(r.width, r.height), 1u) - 1;
+    p.m = r.sampler_kind == RP_SAMPLER_SOBOL ? (v == 0 ? 0 : 32 - __builtin_clz(v)) : 0;
+    p.emergency_limit = r.emergency_limit ? r.emergency_limit : 1024;
+    p.lanes = r.pixel_count * r.sample_count;
+    return p;
+}
+
+std::string validate_request(const rp_scene *s, const rp_request &r) {
+    if (!r.width || !r.height || !r.pixel_count || !r.sample_count)
+        return "Render request must have nonzero film, pixel and sample counts";
+    if (uint64_t(r.pixel_begin) + r.pixel_count > uint64_t(r.width) * r.height)
+        return "Render request pixels exceed the film";
+    if (uint64_t(r.pixel_count) * r.sample_count > 0xffffffffull)
+        return "Render request lanes exceed 2^32";
+    if (r.sampler_kind != RP_SAMPLER_SOBOL && r.sampler_kind != RP_SAMPLER_INDEPENDENT)
+        return "Unsupported sampler (independent and sobol are built)";
+    if (r.sampler_kind == RP_SAMPLER_SOBOL) {
+        if (r.randomization > 3)
+            return "Invalid Sobol randomization";
+        if (std::max(r.width, r.height) > (1u << 25))
+            return "Sobol film exceeds 2^25 pixels per side";
+    }
+    if (r.sample_begin > UINT64_MAX - (r.sample_count - 1))
+        return "Sampler range must fit the absolute sample indices";
+    (void)s;
+    return {};
+}
+
+// One wave: raygen, then max_depth + 1 events of trace -> shade -> shadow.
+void run_wave(rp_scene *s, const WaveParams &p) {
+    s->ensure_pool(p.lanes);
+    PathPool &pool = s->pool;
+    const int sms = s->sm_count;
+    s->mark(3);
+    RP_CHECK(cudaMemsetAsync(pool.counters, 0, 8 * sizeof(u32), s->stream));
+    k_raygen<<<grid_for(sms, p.lanes, 256, 16), 256, 0, s->stream>>>(s->ds, p, pool);
+    RP_CHECK(cudaMemcpyAsync(pool.counters, &p.lanes, sizeof(u32), cudaMemcpyHostToDevice, s->stream));
+    s->done();
+    int in = 0;
+    const u32 events = s->ds.max_depth + 1;
+    for (u32 e = 0; e < events; ++e) {
+        s->mark(0);
+        if (s->counting)
+            k_trace<true><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, 0, s->stream>>>(s->ds, pool, in);
+        else
+            k_trace<false><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, 0, s->stream>>>(s->ds, pool, in);
+        s->done();
+        s->mark(2);
+        RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), s->stream));
+        RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), s->stream));
+        k_shade<<<grid_for(sms, p.lanes, 128, 16), 128, 0, s->stream>>>(s->ds, p, pool, in);
+        s->done();
+        s->mark(1);
+        if (s->counting)
+            k_shadow<true><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, 0, s->stream>>>(s->ds, pool);
+        else
+            k_shadow<false><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, 0, s->stream>>>(s->ds, pool);
+        s->done();
+        in ^= 1;
+    }
+    RP_CHECK(cudaGetLastError());
+}
+
+template <class F> rp_status guarded(char *diag, size_t cap, F &&f) {
+    try {
+        return f();
+    } catch (const CudaError &e) {
+        set_diag(diag, cap, "CUDA error %s in %s", cudaGetErrorString(e.code), e.what);
+        return RP_FAILURE;
+    } catch (const Invalid &e) {
+        set_diag(diag, cap, "%s", e.what.c_str());
+        return RP_INVALID_ARGUMENT;
+    } catch (const std::bad_alloc &) {
+        set_diag(diag, cap, "host allocation failed");
+        return RP_FAILURE;
+    } catch (...) {
+        set_diag(diag, cap, "unexpected failure");
+        return RP_FAILURE;
+    }
+}
+
+void build_bvh(rp_scene *s) {
+    const u32 n = s->ds.prim_count;
+    s->n = n;
+    auto &own = s->owned;
+    cudaStream_t st = s->stream;
+    BuildTmp &t = s->tmp;
+    t.box_lo = dalloc<float4>(own, n);
+    t.box_hi = dalloc<float4>(own, n);
+    t.cbounds = dalloc<int>(own, 6);
+    t.keys[0] = dalloc<u64>(own, n);
+    t.keys[1] = dalloc<u64>(own, n);
+    t.vals[0] = dalloc<u32>(own, n);
+    t.vals[1] = dalloc<u32>(own, n);
+    const u32 tiles = (n + kSortTile - 1) / kSortTile;
+    t.hist = dalloc<u32>(own, size_t(256) * std::max<u32>(tiles, 1));
+    t.left = dalloc<u32>(own, n);
+    t.right = dalloc<u32>(own, n);
+    t.parent = dalloc<u32>(own, n);
+    t.leaf_parent = dalloc<u32>(own, n);
+    t.node_lo = dalloc<float4>(own, n);
+    t.node_hi = dalloc<float4>(own, n);
+    t.flags = dalloc<u32>(own, n);
+    float4 *world = dalloc<float4>(own, size_t(3) * n);
+    BNode *nodes = dalloc<BNode>(own, n);
+    float4 *leaf_v = dalloc<float4>(own, size_t(3) * n);
+    const int init[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, int(0x80000000), int(0x80000000), int(0x80000000)};
+    RP_CHECK(cudaMemcpyAsync(t.cbounds, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    RP_CHECK(cudaMemsetAsync(t.parent, 0xff, size_t(n) * 4, st));
+    RP_CHECK(cudaMemsetAsync(t.leaf_parent, 0xff, size_t(n) * 4, st));
+    RP_CHECK(cudaMemsetAsync(t.flags, 0, size_t(n) * 4, st));
+    if (n == 0) {
+        s->ds.nodes = nodes;
+        s->ds.leaf_v = leaf_v;
+        return;
+    }
+    k_tri_prepare<<<grid_for(s->sm_count, n, 256, 8), 256, 0, st>>>(s->ds, world, t);
+    int cb[6];
+    RP_CHECK(cudaMemcpyAsync(cb, t.cbounds, sizeof(cb), cudaMemcpyDeviceToHost, st));
+    RP_CHECK(cudaStreamSynchronize(st));
+    const float lo[3] = {unordered_host(cb[0]), unordered_host(cb[1]), unordered_host(cb[2])};
+    const float hi[3] = {unordered_host(cb[3]), unordered_host(cb[4]), unordered_host(cb[5])};
+    const float3 flo = make_float3(lo[0], lo[1], lo[2]);
+    const float3 fext = make_float3(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]);
+    k_morton<<<grid_for(s->sm_count, n, 256, 8), 256, 0, st>>>(n, t, flo, fext);
+    int cur = 0;
+    for (int shift = 0; shift < 64; shift += 8) {
+        k_radix_hist<<<tiles, kSortThreads, 0, st>>>(t.keys[cur], n, shift, t.hist, tiles);
+        k_radix_scan<<<1, 1024, 0, st>>>(t.hist, 256 * tiles);
+        k_radix_scatter<<<tiles, kSortThreads, 0, st>>>(t.keys[cur], t.vals[cur], t.keys[cur ^ 1], t.vals[cur ^ 1], n,
+                                                        shift, t.hist, tiles);
+        cur ^= 1;
+    }
+    s->keys = t.keys[cur];
+    s->order = t.vals[cur];
+    if (n > 1) {
+        k_karras<<<grid_for(s->sm_count, n, 256, 8), 256, 0, st>>>(s->keys, n, t);
+        k_refit<<<grid_for(s->sm_count, n, 256, 8), 256, 0, st>>>(n, s->order, t);
+    }
+    k_pack<<<grid_for(s->sm_count, n, 256, 8), 256, 0, st>>>(n, s->order, world, t, nodes, leaf_v);
+    RP_CHECK(cudaGetLastError());
+    RP_CHECK(cudaStreamSynchronize(st));
+    if (n > 1) {
+        // Structural check before any traversal: every internal node and leaf is reached
+        // exactly once from the root, so traversal loops are finite.
+        std::vector<u32> l(n - 1), r(n - 1);
+        RP_CHECK(cudaMemcpy(l.data(), t.left, size_t(n - 1) * 4, cudaMemcpyDeviceToHost));
+        RP_CHECK(cudaMemcpy(r.data(), t.right, size_t(n - 1) * 4, cudaMemcpyDeviceToHost));
+        std::vector<unsigned char> seen_node(n - 1, 0), seen_leaf(n, 0);
+        std::vector<u32> stack{0};
+        size_t visited = 0;
+        while (!stack.empty()) {
+            const u32 c = stack.back();
+            stack.pop_back();
+            if (c & kLeaf) {
+                const u32 slot = c & ~kLeaf;
+                if (slot >= n || seen_leaf[slot]++)
+                    throw Invalid{"LBVH build produced an invalid leaf reference"};
+                ++visited;
+                continue;
+            }
+            if (c >= n - 1 || seen_node[c]++)
+                throw Invalid{"LBVH build produced an invalid node reference"};
+            ++visited;
+            stack.push_back(r[c]);
+            stack.push_back(l[c]);
+        }
+        if (visited != size_t(2) * n - 1)
+            throw Invalid{"LBVH build did not reach every node"};
+    }
+    s->ds.nodes = nodes;
+    s->ds.leaf_v = leaf_v;
+}
+
+} // namespace
+
+extern "C" {
+
+rp_status rp_cuda_device_info(int device, rp_device_info *info, char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+            set_diag(diag, cap, "no CUDA device");
+            return RP_NO_DEVICE;
+        }
+        if (device < 0 || device >= count)
+            throw Invalid{"device index out of range"};
+        cudaDeviceProp prop;
+        RP_CHECK(cudaGetDeviceProperties(&prop, device));
+        if (info) {
+            memset(info, 0, sizeof(*info));
+            snprintf(info->name, sizeof(info->name), "%s", prop.name);
+            info->device = device;
+            info->sm_count = prop.multiProcessorCount;
+            info->major = prop.major;
+            info->minor = prop.minor;
+            info->total_memory = prop.totalGlobalMem;
+        }
+        return RP_SUCCESS;
+    });
+}
+
+uint32_t rp_cuda_abi_size(const char *name) {
+    const std::string n = name ? name : "";
+    if (n == "rp_instance") return sizeof(rp_instance);
+    if (n == "rp_material") return sizeof(rp_material);
+    if (n == "rp_knot") return sizeof(rp_knot);
+    if (n == "rp_area_emission") return sizeof(rp_area_emission);
+    if (n == "rp_positional_light") return sizeof(rp_positional_light);
+    if (n == "rp_medium") return sizeof(rp_medium);
+    if (n == "rp_camera") return sizeof(rp_camera);
+    if (n == "rp_scene_desc") return sizeof(rp_scene_desc);
+    if (n == "rp_request") return sizeof(rp_request);
+    if (n == "rp_packet_result") return sizeof(rp_packet_result);
+    if (n == "rp_scalar_result") return sizeof(rp_scalar_result);
+    if (n == "rp_film_pixel") return sizeof(rp_film_pixel);
+    if (n == "rp_film_request") return sizeof(rp_film_request);
+    if (n == "rp_timing") return sizeof(rp_timing);
+    if (n == "rp_device_info") return sizeof(rp_device_info);
+    return 0;
+}
+
+int rp_cuda_build_light_tables(const double *rows, uint32_t count, uint32_t *alias, uint32_t *records, uint32_t *nodes,
+                               uint32_t *infinite, uint32_t *infinite_count) {
+    std::vector<LightInput> in(count);
+    for (u32 i = 0; i < count; ++i) {
+        const double *r = rows + 16 * i;
+        in[i].power = r[0];
+        in[i].bounds_power = r[1];
+        for (int a = 0; a < 3; ++a) {
+            in[i].low[a] = float(r[2 + a]);
+            in[i].high[a] = float(r[5 + a]);
+            in[i].direction[a] = float(r[8 + a]);
+        }
+        in[i].cos_outer = float(r[11]);
+        in[i].cos_emission = float(r[12]);
+        in[i].two_sided = r[13] != 0;
+        in[i].infinite = r[14] != 0;
+    }
+    LightTables t;
+    std::string error;
+    if (!build_light_tables(in, t, error))
+        return -1;
+    memcpy(alias, t.alias.data(), t.alias.size() * 16);
+    memcpy(records, t.records.data(), t.records.size() * 16);
+    memcpy(nodes, t.nodes.data(), t.nodes.size() * 64);
+    memcpy(infinite, t.infinite.data(), t.infinite.size() * 4);
+    *infinite_count = u32(t.infinite.size());
+    return int(t.nodes.size());
+}
+
+rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **out, char *diag, size_t cap) {
+    if (out)
+        *out = nullptr;
+    rp_scene *s = nullptr;
+    const rp_status st = guarded(diag, cap, [&]() -> rp_status {
+        if (!d || !out)
+            throw Invalid{"null scene description or output"};
+        if (d->abi_version != RP_ABI_VERSION)
+            throw Invalid{"scene description ABI version mismatch"};
+        if (!d->sobol_tables)
+            throw Invalid{"scene description needs the Sobol tables"};
+        if (d->transport != RP_TRANSPORT_HERO)
+            throw Invalid{"only the hero-wavelength transport is built for this entry point"};
+        if (d->max_depth > RP_MAX_DEPTH + 1)
+            throw Invalid{"hero transport requires max depth <= 65"};
+        if (d->medium_count || d->camera_medium != RP_NONE)
+            throw Invalid{"hero transport requires a vacuum scene (src/render.cpp:1579-1580)"};
+        if (d->filter_kind > RP_FILTER_TRIANGLE)
+            throw Invalid{"unsupported pixel filter"};
+        if (d->light_sampler > RP_LIGHTS_UNIFORM)
+            throw Invalid{"invalid light sampler"};
+        if (d->positional_count > RP_MAX_POSITIONAL)
+            throw Invalid{"too many positional lights"};
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+            set_diag(diag, cap, "no CUDA device");
+            return RP_NO_DEVICE;
+        }
+        RP_CHECK(cudaSetDevice(device));
+        s = new rp_scene();
+        s->device = device;
+        cudaDeviceProp prop;
+        RP_CHECK(cudaGetDeviceProperties(&prop, device));
+        s->sm_count = prop.multiProcessorCount;
+        RP_CHECK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+        cudaStream_t stm = s->stream;
+        auto &own = s->owned;
+        DeviceScene &ds = s->ds;
+        // validation of indices
+        for (u32 i = 0; i < d->instance_count; ++i) {
+            const auto &in = d->instances[i];
+            if (uint64_t(in.triangle_begin) + in.triangle_count > d->triangle_count)
+                throw Invalid{"instance triangles out of range"};
+            if (in.material >= d->material_count)
+                throw Invalid{"instance material out of range"};
+            if (in.emission != RP_NONE && in.emission >= d->emission_count)
+                throw Invalid{"instance emission out of range"};
+            for (u32 t = 0; t < in.triangle_count; ++t)
+                for (int k = 0; k < 3; ++k)
+                    if (uint64_t(in.vertex_begin) + d->triangles[3 * (in.triangle_begin + t) + k] >= d->vertex_count)
+                        throw Invalid{"triangle vertex out of range"};
+        }
+        for (u32 i = 0; i < d->material_count; ++i)
+            if (d->materials[i].scattering > RP_DIELECTRIC)
+                throw Invalid{"unsupported scattering family (diffuse, conductor, dielectric are built)"};
+        // flattened triangles and emitters (src/metal_render.mm:1174-1210)
+        std::vector<u32> tri_instance, tri_local, em_inst, em_local;
+        std::vector<DInstance> instances(d->instance_count);
+        for (u32 i = 0; i < d->instance_count; ++i) {
+            const auto &q = d->instances[i];
+            DInstance &in = instances[i];
+            memcpy(in.m, q.matrix, sizeof(in.m));
+            in.vertex_begin = q.vertex_begin;
+            in.triangle_begin = q.triangle_begin;
+            in.triangle_count = q.triangle_count;
+            in.material = q.material;
+            in.reverse = q.reverse_orientation;
+            in.emission = q.emission;
+            in.normal_begin = q.normal_begin;
+            in.emitter_begin = kNone;
+            if (q.emission != RP_NONE) {
+                in.emitter_begin = u32(em_inst.size());
+                for (u32 t = 0; t < q.triangle_count; ++t) {
+                    em_inst.push_back(i);
+                    em_local.push_back(t);
+                }
+            }
+            for (u32 t = 0; t < q.triangle_count; ++t) {
+                tri_instance.push_back(i);
+                tri_local.push_back(t);
+            }
+        }
+        ds.positions = dupload(own, d->positions, size_t(3) * d->vertex_count, stm);
+        ds.normals = dupload(own, d->normals, size_t(3) * d->normal_count, stm);
+        ds.normal_count = d->normal_count;
+        ds.triangles = dupload(own, d->triangles, size_t(3) * d->triangle_count, stm);
+        ds.instances = dupload(own, instances.data(), instances.size(), stm);
+        ds.instance_count = d->instance_count;
+        ds.tri_instance = dupload(own, tri_instance.data(), tri_instance.size(), stm);
+        ds.tri_local = dupload(own, tri_local.data(), tri_local.size(), stm);
+        ds.prim_count = u32(tri_instance.size());
+        std::vector<DMaterial> mats(d->material_count);
+        for (u32 i = 0; i < d->material_count; ++i) {
+            const auto &m = d->materials[i];
+            mats[i] = {m.scattering, m.kind, m.knot_begin, m.knot_count, m.scalar_value, m.eta_begin, m.eta_count,
+                       m.k_begin, m.k_count, m.optical_extensions, m.u_roughness, m.v_roughness, m.remap_roughness};
+        }
+        ds.materials = dupload(own, mats.data(), mats.size(), stm);
+        ds.material_count = d->material_count;
+        ds.knots = dupload(own, reinterpret_cast<const float2 *>(d->knots), d->knot_count, stm);
+        ds.knot_count = d->knot_count;
+        // spectra: emissions, positional intensities, environment
+        std::vector<float> spectra;
+        std::vector<u32> two_sided(d->emission_count);
+        for (u32 i = 0; i < d->emission_count; ++i) {
+            spectra.insert(spectra.end(), d->emissions[i].radiance, d->emissions[i].radiance + 471);
+            two_sided[i] = d->emissions[i].two_sided;
+        }
+        std::vector<DPositional> pos(d->positional_count);
+        for (u32 i = 0; i < d->positional_count; ++i) {
+            const auto &q = d->positional[i];
+            if (q.kind > RP_SPOT_LIGHT)
+                throw Invalid{"unsupported positional light kind (point and spot are built)"};
+            DPositional &L = pos[i];
+            memcpy(L.position, q.position, sizeof(L.position));
+            L.kind = q.kind;
+            memcpy(L.light_from_world, q.light_from_world, sizeof(L.light_from_world));
+            L.cos_falloff_start = q.cos_falloff_start;
+            L.cos_falloff_end = q.cos_falloff_end;
+            L.spectrum = u32(spectra.size());
+            spectra.insert(spectra.end(), q.intensity, q.intensity + 471);
+        }
+        bool has_environment = false;
+        ds.environment = kNone;
+        if (d->environment) {
+            has_environment = std::any_of(d->environment, d->environment + 471, [](float v) { return v > 0; });
+            ds.environment = u32(spectra.size());
+            spectra.insert(spectra.end(), d->environment, d->environment + 471);
+        }
+        ds.spectra = dupload(own, spectra.data(), spectra.size(), stm);
+        ds.emission_two_sided = dupload(own, two_sided.data(), two_sided.size(), stm);
+        ds.emission_count = d->emission_count;
+        ds.positional = dupload(own, pos.data(), pos.size(), stm);
+        ds.positional_count = d->positional_count;
+        ds.emitter_instance = dupload(own, em_inst.data(), em_inst.size(), stm);
+        ds.emitter_local = dupload(own, em_local.data(), em_local.size(), stm);
+        ds.emitter_count = u32(em_inst.size());
+        // scene sphere (src/metal_render.mm:213-276)
+        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        auto world = [&](const DInstance &in, u32 v, int a) {
+            const float *p = d->positions + 3 * size_t(in.vertex_begin + v);
+            const float x = p[0], y = p[1], z = p[2];
+            return double(in.m[4 * a] * x + in.m[4 * a + 1] * y + in.m[4 * a + 2] * z + in.m[4 * a + 3]);
+        };
+        for (const auto &in : instances)
+            for (u32 t = 0; t < in.triangle_count; ++t)
+                for (int k = 0; k < 3; ++k) {
+                    const u32 v = d->triangles[3 * (in.triangle_begin + t) + k];
+                    for (int a = 0; a < 3; ++a) {
+                        const double w = world(in, v, a);
+                        lo[a] = std::min(lo[a], w);
+                        hi[a] = std::max(hi[a], w);
+                    }
+                }
+        float scene_radius = 1;
+        if (!tri_instance.empty()) {
+            double c[3], e[3];
+            for (int a = 0; a < 3; ++a) {
+                c[a] = float(lo[a] / 2 + hi[a] / 2);
+                e[a] = std::max(std::abs(lo[a] - c[a]), std::abs(hi[a] - c[a]));
+                e[a] += 32 * FLT_EPSILON * std::max(std::abs(lo[a]), std::abs(hi[a]));
+            }
+            scene_radius = std::nextafter(float(std::hypot(e[0], e[1], e[2])), INFINITY);
+        }
+        ds.scene_radius = scene_radius;
+        // light inputs (src/metal_render.mm:525-660, :1565-1660)
+        std::vector<LightInput> input;
+        const double pi = std::numbers::pi;
+        std::vector<double> means(d->emission_count, -1), bounds_mean(d->emission_count, -1);
+        for (u32 ii = 0; ii < d->instance_count; ++ii) {
+            const DInstance &in = instances[ii];
+            if (in.emission == kNone)
+                continue;
+            double &mean = means[in.emission], &bound = bounds_mean[in.emission];
+            const float *rad = d->emissions[in.emission].radiance;
+            if (mean < 0) {
+                mean = light_spectrum_power(rad);
+                bound = *std::max_element(rad, rad + 471);
+            }
+            const bool two = d->emissions[in.emission].two_sided != 0;
+            for (u32 t = 0; t < in.triangle_count; ++t) {
+                D3 p[3];
+                for (int k = 0; k < 3; ++k) {
+                    const float *q = d->positions + 3 * size_t(in.vertex_begin + d->triangles[3 * (in.triangle_begin + t) + k]);
+                    for (int a = 0; a < 3; ++a)
+                        p[k][a] = double(in.m[4 * a]) * q[0] + double(in.m[4 * a + 1]) * q[1] +
+                                  double(in.m[4 * a + 2]) * q[2] + double(in.m[4 * a + 3]);
+                }
+                const D3 e1{p[1][0] - p[0][0], p[1][1] - p[0][1], p[1][2] - p[0][2]};
+                const D3 e2{p[2][0] - p[0][0], p[2][1] - p[0][1], p[2][2] - p[0][2]};
+                D3 nrm{e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+                if (in.reverse)
+                    for (auto &v : nrm)
+                        v = -v;
+                LightInput li;
+                for (int a = 0; a < 3; ++a) {
+                    li.low[a] = INFINITY;
+                    li.high[a] = -INFINITY;
+                }
+                for (int k = 0; k < 3; ++k)
+                    for (int a = 0; a < 3; ++a) {
+                        li.low[a] = std::min(li.low[a], float(p[k][a]));
+                        li.high[a] = std::max(li.high[a], float(p[k][a]));
+                    }
+                const double length = std::hypot(nrm[0], nrm[1], nrm[2]);
+                const double area = .5 * length;
+                li.power = pi * area * mean * 1 * (two ? 2 : 1);
+                li.bounds_power = pi * area * bound * 1;
+                li.two_sided = two;
+                if (length > 0) {
+                    for (int a = 0; a < 3; ++a)
+                        li.direction[a] = float(nrm[a] / length);
+                    li.cos_outer = std::nextafter(1.f, 0.f);
+                }
+                input.push_back(li);
+            }
+        }
+        for (u32 i = 0; i < d->positional_count; ++i) {
+            const auto &q = d->positional[i];
+            LightInput li;
+            for (int a = 0; a < 3; ++a)
+                li.low[a] = li.high[a] = q.position[a];
+            li.two_sided = false;
+            li.bounds_power = 4 * pi * *std::max_element(q.intensity, q.intensity + 471);
+            if (q.kind == RP_POINT_LIGHT) {
+                li.power = 4 * pi * light_spectrum_power(q.intensity);
+            } else {
+                li.power = 2 * pi * ((1 - q.cos_falloff_start) + (q.cos_falloff_start - q.cos_falloff_end) / 2) *
+                           light_spectrum_power(q.intensity);
+                float cos_emission =
+                    float(std::cos(std::acos(double(q.cos_falloff_end)) - std::acos(double(q.cos_falloff_start))));
+                if (cos_emission == 1)
+                    cos_emission = q.cos_falloff_end != q.cos_falloff_start ? .999f : std::nextafter(1.f, 0.f);
+                // src/light_sampling.cpp:314-337 (light_positional_cone)
+                const float *m = q.light_from_world;
+                const D3 a{m[0], m[1], m[2]}, b{m[3], m[4], m[5]}, c{m[6], m[7], m[8]};
+                const double aa = d3dot(a, a), bb = d3dot(b, b), cc = d3dot(c, c), tol = 0x1p-20 * aa;
+                li.cos_outer = -1;
+                li.cos_emission = 0;
+                if ((aa > 0 && std::isfinite(aa)) && !(std::abs(aa - bb) > tol) && !(std::abs(aa - cc) > tol) &&
+                    !(std::abs(d3dot(a, b)) > tol) && !(std::abs(d3dot(a, c)) > tol) && !(std::abs(d3dot(b, c)) > tol)) {
+                    const D3 axis{a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+                    const double det = d3dot(axis, c);
+                    if (std::abs(det) > 0) {
+                        const double length = d3norm(axis);
+                        for (int k = 0; k < 3; ++k)
+                            li.direction[k] = float(axis[k] / std::copysign(length, det));
+                        li.cos_outer = float(std::cos(
+                            std::min(pi, std::acos(std::clamp(double(q.cos_falloff_start), -1., 1.)) + 2e-6)));
+                        li.cos_outer = std::max(-1.f, std::nextafter(li.cos_outer, -INFINITY));
+                        li.cos_emission = cos_emission;
+                    }
+                }
+            }
+            input.push_back(li);
+        }
+        ds.environment_light = kNone;
+        if (has_environment) {
+            LightInput li;
+            li.infinite = true;
+            const double radius = std::max(double(scene_radius), 1e-8);
+            li.power = 4 * pi * pi * radius * radius * light_spectrum_power(d->environment);
+            ds.environment_light = u32(input.size());
+            input.push_back(li);
+        }
+        LightTables lt;
+        std::string error;
+        if (!build_light_tables(input, lt, error))
+            throw Invalid{error};
+        ds.light_nodes = dupload(own, lt.nodes.data(), lt.nodes.size(), stm);
+        ds.light_alias = dupload(own, lt.alias.data(), lt.alias.size(), stm);
+        ds.light_records = dupload(own, lt.records.data(), lt.records.size(), stm);
+        ds.infinite_lights = dupload(own, lt.infinite.data(), lt.infinite.size(), stm);
+        ds.light_node_count = u32(lt.nodes.size());
+        ds.infinite_count = u32(lt.infinite.size());
+        ds.light_count = u32(input.size());
+        ds.light_sampler = d->light_sampler;
+        // Sobol tables (sobol::Tables layout, src/sobol_shared.h:36-52)
+        const unsigned char *tb = static_cast<const unsigned char *>(d->sobol_tables);
+        ds.sobol.directions = dupload(own, reinterpret_cast<const u32 *>(tb), 1024 * 52, stm);
+        ds.sobol.intervals = dupload(own, reinterpret_cast<const u64 *>(tb + 212992), 25 * 52, stm);
+        ds.sobol.inverse = dupload(own, reinterpret_cast<const u64 *>(tb + 223392), 26 * 52, stm);
+        ds.origin = v3(d->camera.origin[0], d->camera.origin[1], d->camera.origin[2]);
+        ds.forward = v3(d->camera.corner[0], d->camera.corner[1], d->camera.corner[2]);
+        ds.right = v3(d->camera.dx[0], d->camera.dx[1], d->camera.dx[2]);
+        ds.up = v3(d->camera.dy[0], d->camera.dy[1], d->camera.dy[2]);
+        ds.filter_kind = d->filter_kind;
+        ds.filter_x = d->filter_x_radius;
+        ds.filter_y = d->filter_y_radius;
+        ds.max_depth = d->max_depth;
+        ds.hero_mode = d->hero_wavelengths;
+        {
+            const float u = 0x1.0p-24f;
+            const float g3 = 3.0f * u / (1.0f - 3.0f * u);
+            ds.slab_scale = 1 + 2 * g3;
+        }
+        s->stats = dalloc<unsigned long long>(own, 4);
+        RP_CHECK(cudaMemsetAsync(s->stats, 0, 4 * sizeof(unsigned long long), stm));
+        build_bvh(s);
+        RP_CHECK(cudaStreamSynchronize(stm));
+        *out = s;
+        return RP_SUCCESS;
+    });
+    if (st != RP_SUCCESS)
+        delete s;
+    return st;
+}
+
+void rp_cuda_scene_destroy(rp_scene *scene) { delete scene; }
+
+rp_status rp_cuda_set_counting(rp_scene *s, int enabled) {
+    if (!s)
+        return RP_INVALID_ARGUMENT;
+    s->counting = enabled != 0;
+    return RP_SUCCESS;
+}
+
+rp_status rp_cuda_last_timing(rp_scene *s, rp_timing *t) {
+    if (!s || !t)
+        return RP_INVALID_ARGUMENT;
+    *t = s->timing;
+    return RP_SUCCESS;
+}
+
+static rp_status sample_impl(rp_scene *s, const rp_request *request, rp_packet_result *out, size_t capacity, bool host,
+                             cudaStream_t user, char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!s || !request || !out)
+            throw Invalid{"null argument"};
+        const std::string err = validate_request(s, *request);
+        if (!err.empty())
+            throw Invalid{err};
+        const WaveParams p = wave_params(*request);
+        if (capacity < p.lanes)
+            throw Invalid{"output capacity is smaller than the request lanes"};
+        RP_CHECK(cudaSetDevice(s->device));
+        cudaEvent_t start, stop;
+        RP_CHECK(cudaEventCreate(&start));
+        RP_CHECK(cudaEventCreate(&stop));
+        if (user) {
+            RP_CHECK(cudaEventRecord(start, user));
+            RP_CHECK(cudaStreamWaitEvent(s->stream, start, 0));
+        }
+        RP_CHECK(cudaEventRecord(start, s->stream));
+        if (s->counting)
+            RP_CHECK(cudaMemsetAsync(s->stats, 0, 4 * sizeof(unsigned long long), s->stream));
+        run_wave(s, p);
+        PacketResult *dst = reinterpret_cast<PacketResult *>(out);
+        PacketResult *staging = nullptr;
+        if (host) {
+            RP_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&staging), size_t(p.lanes) * sizeof(PacketResult), s->stream));
+            dst = staging;
+        }
+        s->mark(3);
+        k_results<<<grid_for(s->sm_count, p.lanes, 256, 16), 256, 0, s->stream>>>(s->pool, p.lanes, dst);
+        s->done();
+        u32 failures = 0;
+        if (host) {
+            RP_CHECK(cudaMemcpyAsync(out, staging, size_t(p.lanes) * sizeof(PacketResult), cudaMemcpyDeviceToHost, s->stream));
+            RP_CHECK(cudaFreeAsync(staging, s->stream));
+        }
+        RP_CHECK(cudaEventRecord(stop, s->stream));
+        if (user)
+            RP_CHECK(cudaStreamWaitEvent(user, stop, 0));
+        s->collect();
+        float total = 0;
+        RP_CHECK(cudaEventElapsedTime(&total, start, stop));
+        cudaEventDestroy(start);
+        cudaEventDestroy(stop);
+        s->timing.total_ms = total;
+        s->timing.samples = p.lanes;
+        if (s->counting) {
+            unsigned long long st[4];
+            RP_CHECK(cudaMemcpy(st, s->stats, sizeof(st), cudaMemcpyDeviceToHost));
+            s->timing.nodes_visited = st[0];
+            s->timing.triangles_tested = st[1];
+            s->timing.closest_rays = st[2];
+            s->timing.shadow_rays = st[3];
+        }
+        if (host) {
+            for (u32 i = 0; i < p.lanes; ++i)
+                if (out[i].status != RP_SAMPLE_SUCCESS) {
+                    if (!failures)
+                        set_diag(diag, cap, "Metal render sample failed with status %u at lane %u", out[i].status, i);
+                    ++failures;
+                }
+        }
+        return failures ? RP_FAILURE : RP_SUCCESS;
+    });
+}
+
+rp_status rp_cuda_sample(rp_scene *s, const rp_request *request, rp_packet_result *results, size_t capacity, char *diag,
+                         size_t cap) {
+    return sample_impl(s, request, results, capacity, true, nullptr, diag, cap);
+}
+
+rp_status rp_cuda_sample_device(rp_scene *s, const rp_request *request, rp_packet_result *results, size_t capacity,
+                                void *stream, char *diag, size_t cap) {
+    return sample_impl(s, request, results, capacity, false, static_cast<cudaStream_t>(stream), diag, cap);
+}
+
+rp_status rp_cuda_sample_scalar(rp_scene *, const rp_request *, rp_scalar_result *, size_t, char *diag, size_t cap) {
+    set_diag(diag, cap, "scalar (single-wavelength) transport is not built in this backend");
+    return RP_NOT_BUILT;
+}
+
+static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel *film, bool host, char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!s || !r || !film)
+            throw Invalid{"null argument"};
+        if (!r->width || !r->height || !r->sample_count || !r->batch_size)
+            throw Invalid{"film request needs nonzero film size, samples and batch size"};
+        const u32 pixels = r->width * r->height;
+        RP_CHECK(cudaSetDevice(s->device));
+        if (!s->cie) {
+            // CIE 1931 2-degree table at 1 nm is supplied by the caller's scene data; it is
+            // uploaded lazily from the package data through rp_cuda_set_cie.
+            throw Invalid{"CIE table not set (rp_cuda_set_cie)"};
+        }
+        // waves of whole sample indices over every pixel (canonical order within a batch)
+        const u64 max_lanes = 1u << 23;
+        const u64 samples_per_wave = std::max<u64>(1, std::min<u64>(r->batch_size, max_lanes / pixels));
+        cudaEvent_t start, stop;
+        RP_CHECK(cudaEventCreate(&start));
+        RP_CHECK(cudaEventCreate(&stop));
+        RP_CHECK(cudaEventRecord(start, s->stream));
+        rp_film_pixel *committed = film;
+        if (host) {
+            if (s->film_stage_pixels < pixels) {
+                if (s->film_stage)
+                    cudaFree(s->film_stage);
+                RP_CHECK(cudaMalloc(&s->film_stage, size_t(pixels) * 2 * sizeof(rp_film_pixel)));
+                s->film_stage_pixels = pixels;
+            }
+            committed = s->film_stage + pixels;
+            RP_CHECK(cudaMemcpyAsync(committed, film, size_t(pixels) * sizeof(rp_film_pixel), cudaMemcpyHostToDevice,
+                                     s->stream));
+        } else if (s->film_stage_pixels < pixels) {
+            if (s->film_stage)
+                cudaFree(s->film_stage);
+            RP_CHECK(cudaMalloc(&s->film_stage, size_t(pixels) * 2 * sizeof(rp_film_pixel)));
+            s->film_stage_pixels = pixels;
+        }
+        rp_film_pixel *staged = s->film_stage;
+        if (s->counting)
+            RP_CHECK(cudaMemsetAsync(s->stats, 0, 4 * sizeof(unsigned long long), s->stream));
+        u64 done = 0;
+        u32 failed_batches = 0;
+        while (done < r->sample_count) {
+            const u64 batch = std::min<u64>(r->batch_size, r->sample_count - done);
+            RP_CHECK(cudaMemcpyAsync(staged, committed, size_t(pixels) * sizeof(rp_film_pixel), cudaMemcpyDeviceToDevice,
+                                     s->stream));
+            u64 in_batch = 0;
+            u32 failures = 0;
+            while (in_batch < batch) {
+                const u64 spw = std::min<u64>(samples_per_wave, batch - in_batch);
+                rp_request q{};
+                q.width = r->width;
+                q.height = r->height;
+                q.seed = r->seed;
+                q.pixel_begin = 0;
+                q.pixel_count = pixels;
+                q.sample_begin = r->sample_begin + done + in_batch;
+                q.sample_count = u32(spw);
+                q.emergency_limit = r->emergency_limit;
+                q.sampler_kind = r->sampler_kind;
+                q.randomization = r->randomization;
+                const std::string err = validate_request(s, q);
+                if (!err.empty())
+                    throw Invalid{err};
+                const WaveParams p = wave_params(q);
+                run_wave(s, p);
+                s->mark(3);
+                k_film<<<grid_for(s->sm_count, pixels, 128, 16), 128, 0, s->stream>>>(
+                    s->pool, pixels, u32(spw), s->cie, reinterpret_cast<FilmPixel *>(staged));
+                s->done();
+                u32 f = 0;
+                RP_CHECK(cudaMemcpyAsync(&f, s->pool.counters + 3, 4, cudaMemcpyDeviceToHost, s->stream));
+                RP_CHECK(cudaStreamSynchronize(s->stream));
+                failures += f;
+                in_batch += spw;
+            }
+            if (failures) {
+                ++failed_batches;
+                break; // keep the previously committed film (src/render_driver.cpp:201-214)
+            }
+            std::swap(staged, committed);
+            done += batch;
+        }
+        if (host)
+            RP_CHECK(cudaMemcpyAsync(film, committed, size_t(pixels) * sizeof(rp_film_pixel), cudaMemcpyDeviceToHost,
+                                     s->stream));
+        else if (committed != film)
+            RP_CHECK(cudaMemcpyAsync(film, committed, size_t(pixels) * sizeof(rp_film_pixel), cudaMemcpyDeviceToDevice,
+                                     s->stream));
+        RP_CHECK(cudaEventRecord(stop, s->stream));
+        s->collect();
+        float total = 0;
+        RP_CHECK(cudaEventElapsedTime(&total, start, stop));
+        cudaEventDestroy(start);
+        cudaEventDestroy(stop);
+        s->timing.total_ms = total;
+        s->timing.samples = done * pixels;
+        if (s->counting) {
+            unsigned long long st[4];
+            RP_CHECK(cudaMemcpy(st, s->stats, sizeof(st), cudaMemcpyDeviceToHost));
+            s->timing.nodes_visited = st[0];
+            s->timing.triangles_tested = st[1];
+            s->timing.closest_rays = st[2];
+            s->timing.shadow_rays = st[3];
+        }
+        if (failed_batches) {
+            set_diag(diag, cap, "a render batch failed; the committed film is unchanged");
+            return RP_FAILURE;
+        }
+        return RP_SUCCESS;
+    });
+}
+
+rp_status rp_cuda_set_cie(rp_scene *s, const double *cie_xyz) {
+    if (!s || !cie_xyz)
+        return RP_INVALID_ARGUMENT;
+    return guarded(nullptr, 0, [&]() -> rp_status {
+        RP_CHECK(cudaSetDevice(s->device));
+        if (!s->cie)
+            s->cie = dalloc<double>(s->owned, 3 * 471);
+        RP_CHECK(cudaMemcpy(s->cie, cie_xyz, 3 * 471 * sizeof(double), cudaMemcpyHostToDevice));
+        return RP_SUCCESS;
+    });
+}
+
+rp_status rp_cuda_render_film(rp_scene *s, const rp_film_request *r, rp_film_pixel *film, char *diag, size_t cap) {
+    return film_impl(s, r, film, true, diag, cap);
+}
+rp_status rp_cuda_render_film_device(rp_scene *s, const rp_film_request *r, rp_film_pixel *film, char *diag, size_t cap) {
+    return film_impl(s, r, film, false, diag, cap);
+}
+
+// ---- probes
+
+rp_status rp_cuda_probe_sobol(const void *tables, const uint32_t *queries, uint32_t count, uint32_t *results, char *diag,
+                              size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        std::vector<void *> own;
+        struct Free {
+            std::vector<void *> &o;
+            ~Free() {
+                for (void *p : o)
+                    cudaFree(p);
+            }
+        } fr{own};
+        const unsigned char *tb = static_cast<const unsigned char *>(tables);
+        SobolTables t;
+        t.directions = dupload(own, reinterpret_cast<const u32 *>(tb), 1024 * 52, nullptr);
+        t.intervals = dupload(own, reinterpret_cast<const u64 *>(tb + 212992), 25 * 52, nullptr);
+        t.inverse = dupload(own, reinterpret_cast<const u64 *>(tb + 223392), 26 * 52, nullptr);
+        const u32 *q = dupload(own, queries, size_t(8) * count, nullptr);
+        u32 *r = dalloc<u32>(own, size_t(6) * count);
+        k_probe_sobol<<<(count + 127) / 128, 128>>>(t, q, count, r);
+        RP_CHECK(cudaGetLastError());
+        RP_CHECK(cudaMemcpy(results, r, size_t(6) * count * 4, cudaMemcpyDeviceToHost));
+        return RP_SUCCESS;
+    });
+}
+
+rp_status rp_cuda_probe_philox(const uint32_t *queries, uint32_t count, uint32_t *results, char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        std::vector<void *> own;
+        struct Free {
+            std::vector<void *> &o;
+            ~Free() {
+                for (void *p : o)
+                    cudaFree(p);
+            }
+        } fr{own};
+        const u32 *q = dupload(own, queries, size_t(6) * count, nullptr);
+        u32 *r = dalloc<u32>(own, size_t(4) * count);
+        k_probe_philox<<<(count + 127) / 128, 128>>>(q, count, r);
+        RP_CHECK(cudaGetLastError());
+        RP_CHECK(cudaMemcpy(results, r, size_t(4) * count * 4, cudaMemcpyDeviceToHost));
+        return RP_SUCCESS;
+    });
+}
+
+rp_status rp_cuda_probe_wavelengths(const float *u, uint32_t count, uint32_t mode, float *results, char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        std::vector<void *> own;
+        struct Free {
+            std::vector<void *> &o;
+            ~Free() {
+                for (void *p : o)
+                    cudaFree(p);
+            }
+        } fr{own};
+        const float *q = dupload(own, u, count, nullptr);
+        float *r = dalloc<float>(own, size_t(8) * count);
+        k_probe_wavelengths<<<(count + 127) / 128, 128>>>(q, count, mode, r);
+        RP_CHECK(cudaGetLastError());
+        RP_CHECK(cudaMemcpy(results, r, size_t(8) * count * 4, cudaMemcpyDeviceToHost));
+        return RP_SUCCESS;
+    });
+}
+
+rp_status rp_cuda_probe_bsdf(const float *queries, uint32_t count, float *results, char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        std::vector<void *> own;
+        struct Free {
+            std::vector<void *> &o;
+            ~Free() {
+                for (void *p : o)
+                    cudaFree(p);
+            }
+        } fr{own};
+        const float *q = dupload(own, queries, size_t(16) * count, nullptr);
+        float *r = dalloc<float>(own, size_t(12) * count);
+        k_probe_bsdf<<<(count + 127) / 128, 128>>>(q, count, r);
+        RP_CHECK(cudaGetLastError());
+        RP_CHECK(cudaMemcpy(results, r, size_t(12) * count * 4, cudaMemcpyDeviceToHost));
+        return RP_SUCCESS;
+    });
+}
+
+rp_status rp_cuda_probe_raygen(rp_scene *s, const rp_request *request, uint32_t *words, float *rays, size_t capacity,
+                               char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!s || !request)
+            throw Invalid{"null argument"};
+        const std::string err = validate_request(s, *request);
+        if (!err.empty())
+            throw Invalid{err};
+        const WaveParams p = wave_params(*request);
+        if (capacity < p.lanes)
+            throw Invalid{"capacity too small"};
+        RP_CHECK(cudaSetDevice(s->device));
+        std::vector<void *> own;
+        struct Free {
+            std::vector<void *> &o;
+            ~Free() {
+                for (void *q : o)
+                    cudaFree(q);
+            }
+        } fr{own};
+        u32 *w = dalloc<u32>(own, size_t(11) * p.lanes);
+        float *r = dalloc<float>(own, size_t(6) * p.lanes);
+        k_probe_raygen<<<(p.lanes + 127) / 128, 128, 0, s->stream>>>(s->ds, p, w, r);
+        RP_CHECK(cudaGetLastError());
+        RP_CHECK(cudaMemcpyAsync(words, w, size_t(11) * p.lanes * 4, cudaMemcpyDeviceToHost, s->stream));
+        RP_CHECK(cudaMemcpyAsync(rays, r, size_t(6) * p.lanes * 4, cudaMemcpyDeviceToHost, s->stream));
+        RP_CHECK(cudaStreamSynchronize(s->stream));
+        return RP_SUCCESS;
+    });
+}
+
+rp_status rp_cuda_scene_export_bvh(rp_scene *s, uint32_t *nodes, uint32_t *leaf_order, uint64_t *keys, float *bounds,
+                                   size_t capacity, char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!s)
+            throw Invalid{"null scene"};
+        const u32 n = s->n;
+        if (capacity < n)
+            throw Invalid{"capacity too small"};
+        RP_CHECK(cudaSetDevice(s->device));
+        if (n == 0)
+            return RP_SUCCESS;
+        RP_CHECK(cudaMemcpy(leaf_order, s->order, size_t(n) * 4, cudaMemcpyDeviceToHost));
+        RP_CHECK(cudaMemcpy(keys, s->keys, size_t(n) * 8, cudaMemcpyDeviceToHost));
+        std::vector<u32> l(n), r(n), p(n);
+        std::vector<float4> lo(n), hi(n), blo(n), bhi(n);
+        RP_CHECK(cudaMemcpy(l.data(), s->tmp.left, size_t(n) * 4, cudaMemcpyDeviceToHost));
+        RP_CHECK(cudaMemcpy(r.data(), s->tmp.right, size_t(n) * 4, cudaMemcpyDeviceToHost));
+        RP_CHECK(cudaMemcpy(p.data(), s->tmp.parent, size_t(n) * 4, cudaMemcpyDeviceToHost));
+        RP_CHECK(cudaMemcpy(lo.data(), s->tmp.node_lo, size_t(n) * 16, cudaMemcpyDeviceToHost));
+        RP_CHECK(cudaMemcpy(hi.data(), s->tmp.node_hi, size_t(n) * 16, cudaMemcpyDeviceToHost));
+        RP_CHECK(cudaMemcpy(blo.data(), s->tmp.box_lo, size_t(n) * 16, cudaMemcpyDeviceToHost));
+        RP_CHECK(cudaMemcpy(bhi.data(), s->tmp.box_hi, size_t(n) * 16, cudaMemcpyDeviceToHost));
+        for (u32 i = 0; i + 1 < n; ++i) {
+            nodes[3 * i] = l[i];
+            nodes[3 * i + 1] = r[i];
+            nodes[3 * i + 2] = p[i];
+            const float b[6] = {lo[i].x, lo[i].y, lo[i].z, hi[i].x, hi[i].y, hi[i].z};
+            memcpy(bounds + 6 * i, b, sizeof(b));
+        }
+        for (u32 j = 0; j < n; ++j) {
+            const u32 prim = leaf_order[j];
+            const float b[6] = {blo[prim].x, blo[prim].y, blo[prim].z, bhi[prim].x, bhi[prim].y, bhi[prim].z};
+            memcpy(bounds + 6 * (size_t(n) - 1 + j), b, sizeof(b));
+        }
+        return RP_SUCCESS;
+    });
+}
+
+rp_status rp_cuda_trace_rays(rp_scene *s, const float *rays, uint32_t count, int any_hit, float *hits, char *diag,
+                             size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!s)
+            throw Invalid{"null scene"};
+        RP_CHECK(cudaSetDevice(s->device));
+        std::vector<void *> own;
+        struct Free {
+            std::vector<void *> &o;
+            ~Free() {
+                for (void *q : o)
+                    cudaFree(q);
+            }
+        } fr{own};
+        const float *q = dupload(own, rays, size_t(7) * count, s->stream);
+        float *h = dalloc<float>(own, size_t(4) * count);
+        k_probe_trace<<<(count + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, s->stream>>>(s->ds, q, count, any_hit, h);
+        RP_CHECK(cudaGetLastError());
+        RP_CHECK(cudaMemcpyAsync(hits, h, size_t(4) * count * 4, cudaMemcpyDeviceToHost, s->stream));
+        RP_CHECK(cudaStreamSynchronize(s->stream));
+        return RP_SUCCESS;
+    });
+}
+
+} // extern "C"

@@ -1,0 +1,613 @@
+// Wavefront kernels of the hero path tracer and the device film reduction.
+#pragma once
+
+#include "rp_transport.cuh"
+
+namespace rp {
+
+constexpr int kTraceBlock = 128;
+
+// Warp-aggregated append to a device queue: one atomicAdd per warp.  Every lane of the warp
+// must call this together (the shade kernel runs a warp-uniform trip count).
+RP_DEV u32 warp_append(u32 *counter, bool want) {
+    const u32 ballot = __ballot_sync(0xffffffffu, want);
+    const int lane = threadIdx.x & 31;
+    u32 base = 0;
+    if (lane == 0 && ballot)
+        base = atomicAdd(counter, __popc(ballot));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    return base + __popc(ballot & ((1u << lane) - 1));
+}
+
+// rypath_render_packets prologue (shaders/render.metal:2424-2460) + packet_pt_initialize
+// (shaders/packet_pt_step.h:84-115)
+__global__ void k_raygen(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p, PathPool pool) {
+    for (u32 lane = blockIdx.x * blockDim.x + threadIdx.x; lane < p.lanes; lane += gridDim.x * blockDim.x) {
+        const BeginSample b = begin_sample(s, p, lane);
+        V4 lambda, pdf;
+        sample_wavelengths(sample_uniform(p, b.words.z), s.hero_mode, lambda, pdf);
+        V3 o, d;
+        primary_ray(s, p, b, o, d);
+        u32 flags = 15u | F_ROULETTE | (kCamera << F_LTYPE_SHIFT);
+        if (!finite3(o) || !finite3(d))
+            flags = set_status(flags, 2) | F_COMPLETE;
+        pool.ident[lane] = make_uint4(b.pixel, b.sample_low, b.sample_high, flags);
+        pool.cursor[lane] = make_uint4(u32(b.index), u32(b.index >> 32), 1, lane);
+        pool.lambda[lane] = to_float4(lambda);
+        pool.lambda_pdf[lane] = to_float4(pdf);
+        pool.beta[lane] = make_float4(1, 1, 1, 1);
+        pool.radiance[lane] = make_float4(0, 0, 0, 0);
+        pool.dens_f[lane] = pool.prev_f[lane] = make_float4(.5f, .5f, .5f, .5f);
+        pool.dens_e[lane] = pool.prev_e[lane] = make_int4(1, 1, 1, 1);
+        pool.eta_scale[lane] = make_float4(1, 1, 1, 1);
+        pool.ray_o[lane] = make_float4(o.x, o.y, o.z, 0);
+        pool.ray_d[lane] = make_float4(d.x, d.y, d.z, 0);
+        pool.latest_p[lane] = make_float4(o.x, o.y, o.z, 0);
+        pool.latest_n[lane] = make_float4(0, 0, 0, 0);
+        pool.queue[0][lane] = lane;
+    }
+}
+
+// Closest-hit queries for the active queue.
+template <bool Count>
+__global__ void __launch_bounds__(kTraceBlock) k_trace(const __grid_constant__ DeviceScene s, PathPool pool, int in) {
+    __shared__ u32 stack[kStackDepth * kTraceBlock];
+    const u32 count = pool.counters[in];
+    const u32 *queue = pool.queue[in];
+    u32 nodes = 0, tris = 0, rays = 0;
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const u32 path = queue[i];
+        if (pool.ident[path].w & F_COMPLETE)
+            continue;
+        const float4 o = pool.ray_o[path], d = pool.ray_d[path];
+        Hit h;
+        const bool ok = trace_closest<Count>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), __int_as_float(0x7f800000), h,
+                                             stack + threadIdx.x, kTraceBlock, nodes, tris);
+        ++rays;
+        pool.hit[path] = make_float4(h.t, h.b1, h.b2, __uint_as_float(ok ? h.prim : 0xfffffffeu));
+    }
+    if (Count) {
+        atomicAdd(pool.stats + 0, (unsigned long long)nodes);
+        atomicAdd(pool.stats + 1, (unsigned long long)tris);
+        atomicAdd(pool.stats + 2, (unsigned long long)rays);
+    }
+}
+
+// One hero event after its closest hit (shaders/packet_pt_event_body.inc:11-461).
+__global__ void __launch_bounds__(128) k_shade(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p,
+                                               PathPool pool, int in) {
+    const u32 count = pool.counters[in];
+    const u32 *queue = pool.queue[in];
+    u32 *out_queue = pool.queue[in ^ 1];
+    u32 *out_count = pool.counters + (in ^ 1);
+    const u32 capacity = s.max_depth + 2;
+    // uniform trip count so warp-level appends see every lane of the warp
+    const u32 stride = gridDim.x * blockDim.x;
+    const u32 trips = (count + stride - 1) / stride;
+    for (u32 trip = 0; trip < trips; ++trip) {
+        const u32 i = trip * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        bool keep = false, shadow = false;
+        float4 sh_o = make_float4(0, 0, 0, 0), sh_d = sh_o, sh_c = sh_o;
+        u32 path = 0;
+        if (i < count) {
+            path = queue[i];
+            uint4 ident = pool.ident[path];
+            u32 flags = ident.w;
+            if (!(flags & F_COMPLETE)) {
+                uint4 cursor = pool.cursor[path];
+                const u64 index = (u64(cursor.y) << 32) | cursor.x;
+                u32 cnt = cursor.z;
+                const V4 lambda = from_float4(pool.lambda[path]);
+                V4 beta = from_float4(pool.beta[path]);
+                V4 radiance = from_float4(pool.radiance[path]);
+                Density density = load_density(pool.dens_f[path], pool.dens_e[path]);
+                const Density previous_density = load_density(pool.prev_f[path], pool.prev_e[path]);
+                Density hero_previous = previous_density;
+                V4 eta_scale = from_float4(pool.eta_scale[path]);
+                bool roulette = (flags & F_ROULETTE) != 0;
+                u32 active_mask = flags & F_MASK;
+                const float4 ro4 = pool.ray_o[path], rd4 = pool.ray_d[path];
+                V3 ro = v3(ro4.x, ro4.y, ro4.z), rd = v3(rd4.x, rd4.y, rd4.z);
+                const float4 hit = pool.hit[path];
+                u32 status = get_status(flags);
+                Density direct_density = density;
+                V4 direct_beta = beta;
+                bool direct_allowed = true;
+                const u32 old_count = cnt;
+                bool terminated = true;
+                // current vertex
+                u32 ctype = kSurface, cinst = kNone, clocal = 0, clight = kNone;
+                SurfacePoint cp;
+                cp.position = cp.error = cp.geometric_normal = cp.shading_normal = v3(0, 0, 0);
+                cp.inverse_area_pdf = 0;
+                Frame cframe;
+                HeroBsdf cbsdf;
+                cbsdf.kind = 0;
+                cbsdf.active_mask = active_mask;
+                cbsdf.g = {0, 0, true};
+                V4 cbeta = beta;
+                V3 cwo = v3(0, 0, 0), swo = v3(0, 0, 0);
+                bool pair_valid = false, cdelta = false, connectible = false;
+                do {
+                    if (cnt >= capacity || !nonzero4(beta))
+                        break;
+                    if (!finite3(ro) || !finite3(rd) || !finite_nonnegative4(beta)) {
+                        status = 2;
+                        break;
+                    }
+                    const u32 prim = __float_as_uint(hit.w);
+                    if (prim == 0xfffffffeu) {
+                        status = 3;
+                        break;
+                    }
+                    if (prim == kNone) {
+                        ctype = kEnvironment;
+                        clight = s.environment_light;
+                        cp.position = ro + rd;
+                        cp.geometric_normal = -rd;
+                        cp.shading_normal = -rd;
+                        cwo = -rd;
+                        cbeta = beta;
+                        connectible = true;
+                        ++cnt;
+                        break;
+                    }
+                    const float t = hit.x, b1 = hit.y, b2 = hit.z;
+                    if (!isfinite(t) || t < 0 || !isfinite(b1) || !isfinite(b2) || prim >= s.prim_count) {
+                        status = 3;
+                        break;
+                    }
+                    cinst = s.tri_instance[prim];
+                    clocal = s.tri_local[prim];
+                    const DInstance &instance = s.instances[cinst];
+                    if (instance.material >= s.material_count) {
+                        status = 3;
+                        break;
+                    }
+                    ctype = kSurface;
+                    clight = instance.emission == kNone ? kNone : instance.emitter_begin + clocal;
+                    cwo = -rd;
+                    if (!triangle_surface_point(s, cinst, clocal, b1, b2, true, cp)) {
+                        status = 2;
+                        break;
+                    }
+                    const DMaterial material = s.materials[instance.material];
+                    if (!shading_frame(cp.shading_normal, cframe) ||
+                        !prepare_bsdf(s, material, lambda, active_mask, cbsdf)) {
+                        status = 2;
+                        break;
+                    }
+                    const V3 ray_position = fma3(v3(t, t, t), rd, ro);
+                    const V3 ray_error = gamma_bound(2) * (vabs(t * rd) + vabs(ro));
+                    cp.error = cp.error + (vabs(cp.position - ray_position) + ray_error);
+                    if (!finite3(cp.error)) {
+                        status = 2;
+                        break;
+                    }
+                    cbeta = beta;
+                    connectible = hero_connectible(cbsdf);
+                    ++cnt;
+                    if (cnt == capacity)
+                        break;
+                    if (cnt - 2 >= p.emergency_limit) {
+                        status = 1;
+                        break;
+                    }
+                    const uint4 draws = draw_words(s, p, ident.x, ident.y, ident.z, index, 4 + cnt - 2);
+                    swo = to_local(cframe, cwo);
+                    cbsdf.active_mask = active_mask;
+                    direct_density = density;
+                    direct_allowed = hero_continue(beta, eta_scale, roulette, cnt - 1, sample_uniform(p, draws.w));
+                    direct_beta = beta;
+                    connectible = hero_connectible(cbsdf);
+                    if (!direct_allowed)
+                        break;
+                    const HeroSample proposed = hero_sample(cbsdf, swo, sample_uniform(p, draws.x),
+                                                            sample_uniform(p, draws.y), sample_uniform(p, draws.z));
+                    bool cont_valid = proposed.valid;
+                    if (proposed.valid && proposed.accepted) {
+                        hero_previous = direct_density;
+                        const Update adv = advance(direct_density, beta, proposed.numerator, proposed.pdf);
+                        cont_valid = adv.valid;
+                        if (adv.valid) {
+                            beta = adv.beta;
+                            density = adv.density;
+                        }
+                        hero_account_eta(eta_scale, roulette, proposed.eta, proposed.transmission);
+                        active_mask = 1;
+#pragma unroll
+                        for (int k = 1; k < 4; ++k)
+                            if (density.lane[k].fraction > 0 || (fbits(beta.v[k]) & 0x7fffffffu))
+                                active_mask |= 1u << k;
+                    }
+                    if (!cont_valid) {
+                        status = 2;
+                        break;
+                    }
+                    if (!proposed.accepted)
+                        break;
+                    pair_valid = true;
+                    V3 wi = to_world(cframe, proposed.wi);
+                    if (!unit_vector(wi, wi)) {
+                        status = 2;
+                        break;
+                    }
+                    if (!finite_nonnegative4(beta)) {
+                        status = 2;
+                        break;
+                    }
+                    if (proposed.delta)
+                        cdelta = true;
+                    const V3 origin = offset_point(cp.position, cp.error, cp.geometric_normal, wi);
+                    if (!finite3(origin)) {
+                        status = 2;
+                        break;
+                    }
+                    ro = origin;
+                    rd = wi;
+                    terminated = false;
+                } while (false);
+                bool complete = terminated || status != 0 || cnt >= capacity || !nonzero4(beta);
+                // latest vertex (the previous event's) for MIS
+                const float4 lp4 = pool.latest_p[path], ln4 = pool.latest_n[path];
+                Latest latest;
+                latest.type = (flags >> F_LTYPE_SHIFT) & 3u;
+                latest.kind = (flags >> F_LKIND_SHIFT) & 3u;
+                latest.mask = (flags >> F_LMASK_SHIFT) & 15u;
+                latest.delta = (flags & F_LDELTA) != 0;
+                latest.smooth = (flags & F_LSMOOTH) != 0;
+                latest.position = v3(lp4.x, lp4.y, lp4.z);
+                latest.shading_normal = v3(ln4.x, ln4.y, ln4.z);
+                latest.alpha_x = lp4.w;
+                latest.alpha_y = ln4.w;
+                if (cnt != old_count && status == 0) {
+                    // hero_endpoint (shaders/hero_pt_helpers.h:157-184)
+                    V4 rad = v4(0);
+                    bool emission_ok = true;
+                    if (ctype == kEnvironment) {
+                        if (s.environment != kNone)
+#pragma unroll
+                            for (int k = 0; k < 4; ++k)
+                                rad.v[k] = spectrum(s, s.environment, lambda.v[k]);
+                        emission_ok = finite_nonnegative4(rad);
+                    } else {
+                        const V3 delta = latest.position - cp.position;
+                        const DInstance &instance = s.instances[cinst];
+                        if (!zero3(delta) && instance.emission != kNone) {
+                            const V3 dir = normalize3(delta);
+                            if (s.emission_two_sided[instance.emission] || dot(cp.geometric_normal, dir) > 0) {
+                                const u32 off = instance.emission * 471u;
+#pragma unroll
+                                for (int k = 0; k < 4; ++k)
+                                    rad.v[k] = cp.inverse_area_pdf == 0 ? 0.f : spectrum(s, off, lambda.v[k]);
+                                emission_ok = finite_nonnegative4(rad);
+                            }
+                        }
+                    }
+                    V4 endpoint = v4(0);
+                    if (!emission_ok) {
+                        status = 2;
+                    } else {
+                        const V4 value = mul4(cbeta, rad);
+                        if (cnt <= 2 || latest.delta || !nonzero4(value)) {
+                            endpoint = value;
+                        } else {
+                            latest.param = from_float4(pool.latest_param[path]);
+                            latest.k = from_float4(pool.latest_k[path]);
+                            const float4 pre = pool.preceding[path];
+                            bool ok;
+                            const V4 bsdf_pdf = represented_pdf(latest_bsdf(latest), latest.shading_normal, latest.position,
+                                                                v3(pre.x, pre.y, pre.z), ctype == kEnvironment,
+                                                                ctype == kEnvironment ? rd : cp.position, ok);
+                            // hero_history_light_pdf / direct_pdf (shaders/packet_transport.h:740-758)
+                            float lpdf = 0;
+                            const float selection = light_pmf(s, latest.position, latest.shading_normal, clight);
+                            if (ctype == kEnvironment) {
+                                lpdf = 0.0f * selection;
+                            } else {
+                                const V3 dl = cp.position - latest.position;
+                                if (dot(dl, dl) > 0 && nonzero3(cp.geometric_normal) && clight < s.emitter_count)
+                                    lpdf = selection * light_geometry_pdf(s, clight, latest.position,
+                                                                          latest.shading_normal, cp);
+                            }
+                            if (!ok || !hero_weight(previous_density, value, ok ? bsdf_pdf : v4(__int_as_float(0x7fffffff)),
+                                                    v4(lpdf), endpoint))
+                                status = 2;
+                        }
+                    }
+                    radiance = add4(radiance, endpoint);
+                    // hero_direct (shaders/hero_pt_helpers.h:185-221): sample, evaluate, weight;
+                    // visibility is resolved by the shadow kernel.
+                    if (status == 0 && cnt < capacity && direct_allowed && ctype == kSurface && connectible) {
+                        const uint4 w = draw_words(s, p, ident.x, ident.y, ident.z, index, 133 + cnt - 2);
+                        const float u0 = sample_uniform(p, w.x), u1 = sample_uniform(p, w.y), u2 = sample_uniform(p, w.z);
+                        // sample_li (shaders/packet_transport.h:470-553)
+                        const Selected choice = light_sample(s, cp.position, cp.shading_normal, u0);
+                        V4 lbeta = v4(0);
+                        float spdf = 0;
+                        bool li_ok = true, delta_light = false;
+                        SurfacePoint lp;
+                        lp.position = lp.error = lp.geometric_normal = lp.shading_normal = v3(0, 0, 0);
+                        lp.inverse_area_pdf = 0;
+                        V3 direction = v3(0, 0, 1);
+                        const u32 sel = choice.light;
+                        if (choice.pmf > 0) {
+                            V4 lrad = v4(0);
+                            if (sel < s.emitter_count) {
+                                if (!light_geometry_sample(s, sel, cp.position, cp.shading_normal, u1, u2, lp, spdf)) {
+                                    li_ok = false;
+                                } else {
+                                    spdf *= choice.pmf;
+                                    const V3 dl = lp.position - cp.position;
+                                    const float d2 = dot(dl, dl);
+                                    if (lp.inverse_area_pdf == 0 || !(d2 > 0)) {
+                                        spdf = 0;
+                                    } else {
+                                        direction = dl * (1.0f / sqrtf(d2));
+                                        const DInstance &li = s.instances[s.emitter_instance[sel]];
+                                        if (s.emission_two_sided[li.emission] || dot(lp.geometric_normal, -direction) > 0) {
+#pragma unroll
+                                            for (int k = 0; k < 4; ++k)
+                                                lrad.v[k] = spectrum(s, li.emission * 471u, lambda.v[k]);
+                                        }
+                                        li_ok = finite_nonnegative4(lrad);
+                                    }
+                                }
+                            } else if (sel < s.emitter_count + s.positional_count) {
+                                const DPositional &L = s.positional[sel - s.emitter_count];
+                                delta_light = true;
+                                lp.position = v3(L.position[0], L.position[1], L.position[2]);
+                                const V3 dl = lp.position - cp.position;
+                                const float d2 = dot(dl, dl);
+                                if (!(d2 > 0)) {
+                                    spdf = 0;
+                                } else {
+                                    direction = dl * (1.0f / sqrtf(d2));
+#pragma unroll
+                                    for (int k = 0; k < 4; ++k) {
+                                        float intensity = spectrum(s, L.spectrum, lambda.v[k]);
+                                        if (!positional_intensity(L, direction, intensity))
+                                            li_ok = false;
+                                        lrad.v[k] = intensity / d2;
+                                    }
+                                    spdf = choice.pmf;
+                                }
+                            } else {
+                                spdf = 0; // constant environment: pdf 0 for unidirectional PT
+                            }
+                            if (li_ok)
+                                lbeta = spdf > 0 ? V4{{lrad.v[0] / spdf, lrad.v[1] / spdf, lrad.v[2] / spdf,
+                                                       lrad.v[3] / spdf}}
+                                                 : v4(0);
+                            li_ok = li_ok && finite_nonnegative4(lbeta);
+                        }
+                        if (!li_ok || !isfinite(spdf) || spdf < 0) {
+                            status = 2;
+                        } else if (spdf > 0 && nonzero4(lbeta)) {
+                            const HeroEval e = hero_evaluate(cbsdf, pair_valid ? swo : to_local(cframe, cwo),
+                                                             to_local(cframe, direction));
+                            if (!e.valid) {
+                                status = 2;
+                            } else {
+                                const V4 value = scale4(mul4(mul4(direct_beta, e.f), lbeta),
+                                                        fabsf(dot(cp.shading_normal, direction)));
+                                if (nonzero4(value)) {
+                                    V4 contribution = value;
+                                    bool weight_ok = true;
+                                    if (!delta_light) {
+                                        const float sel_pmf = light_pmf(s, cp.position, cp.shading_normal, sel);
+                                        const float lpdf =
+                                            nonzero3(lp.geometric_normal)
+                                                ? sel_pmf * light_geometry_pdf(s, sel, cp.position, cp.shading_normal, lp)
+                                                : 0.0f;
+                                        bool ok;
+                                        const V4 bsdf_pdf = represented_pdf(cbsdf, cp.shading_normal, cp.position,
+                                                                            latest.position, false, lp.position, ok);
+                                        weight_ok = ok && hero_weight(direct_density, value, v4(lpdf), bsdf_pdf, contribution);
+                                    }
+                                    // visible(): offset both endpoints (shaders/packet_transport.h:377-446)
+                                    const V3 seg = lp.position - cp.position;
+                                    if (!zero3(seg)) {
+                                        const V3 so = offset_point(cp.position, cp.error, cp.geometric_normal, seg);
+                                        const V3 st = offset_point(lp.position, lp.error, lp.geometric_normal, -seg);
+                                        const V3 sd = st - so;
+                                        shadow = true;
+                                        sh_o = make_float4(so.x, so.y, so.z, kOneMinusEps);
+                                        sh_d = make_float4(sd.x, sd.y, sd.z, __uint_as_float(path));
+                                        sh_c = weight_ok ? to_float4(contribution)
+                                                         : make_float4(__int_as_float(0x7fffffff), 0, 0, 0);
+                                    }
+                                }
+                            }
+                        }
+                    }
+                    if (!finite_nonnegative4(radiance))
+                        status = 2;
+                    if (status != 0) {
+                        complete = true;
+                        shadow = false;
+                    }
+                }
+                if (cnt != old_count) {
+                    // preceding = latest; latest = current (shaders/packet_pt_event_body.inc:453-460)
+                    pool.preceding[path] = make_float4(latest.position.x, latest.position.y, latest.position.z, 0);
+                    flags = (flags & ~(3u << F_PTYPE_SHIFT)) | (latest.type << F_PTYPE_SHIFT);
+                    pool.latest_p[path] = make_float4(cp.position.x, cp.position.y, cp.position.z, cbsdf.g.alpha_x);
+                    pool.latest_n[path] =
+                        make_float4(cp.shading_normal.x, cp.shading_normal.y, cp.shading_normal.z, cbsdf.g.alpha_y);
+                    pool.latest_param[path] = make_float4(cbsdf.param[0], cbsdf.param[1], cbsdf.param[2], cbsdf.param[3]);
+                    pool.latest_k[path] = make_float4(cbsdf.k[0], cbsdf.k[1], cbsdf.k[2], cbsdf.k[3]);
+                    flags &= ~((3u << F_LTYPE_SHIFT) | F_LDELTA | (3u << F_LKIND_SHIFT) | (15u << F_LMASK_SHIFT) | F_LSMOOTH);
+                    flags |= (ctype << F_LTYPE_SHIFT) | (cdelta ? F_LDELTA : 0u) | ((cbsdf.kind & 3u) << F_LKIND_SHIFT) |
+                             ((cbsdf.active_mask & 15u) << F_LMASK_SHIFT) | (cbsdf.g.smooth ? F_LSMOOTH : 0u);
+                }
+                flags = (flags & ~(F_MASK | F_ROULETTE)) | active_mask | (roulette ? F_ROULETTE : 0u);
+                flags = set_status(flags, status) | (complete ? F_COMPLETE : 0u);
+                ident.w = flags;
+                pool.ident[path] = ident;
+                cursor.z = cnt;
+                pool.cursor[path] = cursor;
+                pool.beta[path] = to_float4(beta);
+                pool.radiance[path] = to_float4(radiance);
+                float4 f;
+                int4 e;
+                store_density(density, f, e);
+                pool.dens_f[path] = f;
+                pool.dens_e[path] = e;
+                store_density(hero_previous, f, e);
+                pool.prev_f[path] = f;
+                pool.prev_e[path] = e;
+                pool.eta_scale[path] = to_float4(eta_scale);
+                pool.ray_o[path] = make_float4(ro.x, ro.y, ro.z, 0);
+                pool.ray_d[path] = make_float4(rd.x, rd.y, rd.z, 0);
+                keep = !complete;
+            }
+        }
+        const u32 slot = warp_append(out_count, keep);
+        if (keep)
+            out_queue[slot] = path;
+        const u32 sslot = warp_append(pool.counters + 2, shadow);
+        if (shadow) {
+            pool.sh_o[sslot] = sh_o;
+            pool.sh_d[sslot] = sh_d;
+            pool.sh_c[sslot] = sh_c;
+        }
+    }
+}
+
+// Visibility of the light samples (visible(), shaders/packet_transport.h:377-446, opaque surfaces)
+template <bool Count>
+__global__ void __launch_bounds__(kTraceBlock) k_shadow(const __grid_constant__ DeviceScene s, PathPool pool) {
+    __shared__ u32 stack[kStackDepth * kTraceBlock];
+    const u32 count = pool.counters[2];
+    u32 nodes = 0, tris = 0, rays = 0;
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const float4 o = pool.sh_o[i], d = pool.sh_d[i];
+        const u32 path = __float_as_uint(d.w);
+        bool occluded;
+        const bool ok = trace_any<Count>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), o.w, occluded, stack + threadIdx.x,
+                                         kTraceBlock, nodes, tris);
+        ++rays;
+        uint4 ident = pool.ident[path];
+        if (!ok) {
+            ident.w = set_status(ident.w, 3) | F_COMPLETE;
+            pool.ident[path] = ident;
+            continue;
+        }
+        if (occluded)
+            continue;
+        const float4 c = pool.sh_c[i];
+        if (isnan(c.x)) {
+            ident.w = set_status(ident.w, 2) | F_COMPLETE;
+            pool.ident[path] = ident;
+            continue;
+        }
+        float4 r = pool.radiance[path];
+        r.x += c.x;
+        r.y += c.y;
+        r.z += c.z;
+        r.w += c.w;
+        pool.radiance[path] = r;
+        if (!finite_nonnegative4(from_float4(r))) {
+            ident.w = set_status(ident.w, 2) | F_COMPLETE;
+            pool.ident[path] = ident;
+        }
+    }
+    if (Count) {
+        atomicAdd(pool.stats + 0, (unsigned long long)nodes);
+        atomicAdd(pool.stats + 1, (unsigned long long)tris);
+        atomicAdd(pool.stats + 3, (unsigned long long)rays);
+    }
+}
+
+// packet_pt_result (shaders/packet_pt_step.h:225-239): 80-byte packet result per lane.
+struct PacketResult {
+    u32 status, pixel, sample_low, sample_high, splat_count;
+    float wavelengths[4], wavelength_pdfs[4], radiance[4];
+    float filter_weight;
+    u32 reserved[2];
+};
+__global__ void k_results(PathPool pool, u32 lanes, PacketResult *out) {
+    for (u32 lane = blockIdx.x * blockDim.x + threadIdx.x; lane < lanes; lane += gridDim.x * blockDim.x) {
+        const uint4 id = pool.ident[lane];
+        const float4 l = pool.lambda[lane], pdf = pool.lambda_pdf[lane], r = pool.radiance[lane];
+        PacketResult res;
+        res.status = (id.w & F_COMPLETE) ? get_status(id.w) : 2u;
+        res.pixel = id.x;
+        res.sample_low = id.y;
+        res.sample_high = id.z;
+        res.splat_count = 0;
+        res.wavelengths[0] = l.x;
+        res.wavelengths[1] = l.y;
+        res.wavelengths[2] = l.z;
+        res.wavelengths[3] = l.w;
+        res.wavelength_pdfs[0] = pdf.x;
+        res.wavelength_pdfs[1] = pdf.y;
+        res.wavelength_pdfs[2] = pdf.z;
+        res.wavelength_pdfs[3] = pdf.w;
+        res.radiance[0] = r.x;
+        res.radiance[1] = r.y;
+        res.radiance[2] = r.z;
+        res.radiance[3] = r.w;
+        res.filter_weight = 1;
+        res.reserved[0] = res.reserved[1] = 0;
+        out[lane] = res;
+    }
+}
+
+// Device film pixel: FP64 Neumaier sums (src/packet_film.cpp:10-14, :198-265) plus second moments.
+struct FilmPixel {
+    double sum[3], correction[3];
+    double weight_sum, weight_correction;
+    double square[3];
+    unsigned long long count;
+};
+RP_DEV void add_compensated(double value, double &sum, double &correction) {
+    const double next = __dadd_rn(sum, value);
+    correction = __dadd_rn(correction, fabs(sum) >= fabs(value) ? __dadd_rn(__dsub_rn(sum, next), value)
+                                                                  : __dadd_rn(__dsub_rn(value, next), sum));
+    sum = next;
+}
+// packet_sensor_xyz (src/packet_film.cpp:102-114) for every sample of a wave, reduced per
+// pixel in canonical (absolute sample, pixel) order.  Any failed lane fails the batch.
+__global__ void k_film(PathPool pool, u32 pixel_count, u32 samples, const double *cie, FilmPixel *film) {
+    for (u32 px = blockIdx.x * blockDim.x + threadIdx.x; px < pixel_count; px += gridDim.x * blockDim.x) {
+        FilmPixel f = film[px];
+        for (u32 si = 0; si < samples; ++si) {
+            const u32 lane = si * pixel_count + px;
+            const uint4 id = pool.ident[lane];
+            const u32 status = (id.w & F_COMPLETE) ? get_status(id.w) : 2u;
+            if (status != 0) {
+                atomicAdd(pool.counters + 3, 1u);
+                continue;
+            }
+            const float4 l4 = pool.lambda[lane], p4 = pool.lambda_pdf[lane], r4 = pool.radiance[lane];
+            const float lam[4] = {l4.x, l4.y, l4.z, l4.w}, pdf[4] = {p4.x, p4.y, p4.z, p4.w},
+                        rad[4] = {r4.x, r4.y, r4.z, r4.w};
+            double xyz[3] = {0, 0, 0};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (pdf[k] == 0)
+                    continue;
+                const float w = lam[k];
+                if (!(w >= 360 && w <= 830))
+                    continue;
+                const u32 row = u32(round(double(w)) - 360.0);
+                const double weight = __ddiv_rn(__ddiv_rn(double(rad[k]), double(pdf[k])), 4.0);
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    xyz[c] = __dadd_rn(xyz[c], __dmul_rn(weight, __ldg(cie + 3 * row + c)));
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                add_compensated(xyz[c], f.sum[c], f.correction[c]);
+                f.square[c] = __dadd_rn(f.square[c], __dmul_rn(xyz[c], xyz[c]));
+            }
+            add_compensated(1.0, f.weight_sum, f.weight_correction);
+            ++f.count;
+        }
+        film[px] = f;
+    }
+}
+
+} // namespace rp

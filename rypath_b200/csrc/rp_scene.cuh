@@ -1,0 +1,745 @@
+// Device scene: surface reconstruction, light selection, light geometry sampling and the
+// binary LBVH traversal with watertight triangle tests.
+#pragma once
+
+#include "rp_math.cuh"
+
+namespace rp {
+
+constexpr u32 kNone = 0xffffffffu;
+constexpr u32 kLeaf = 0x80000000u;
+
+// wire::Instance subset (src/render_wire.h:168-188), plus the first emitter slot
+struct DInstance {
+    float m[12];
+    u32 vertex_begin, triangle_begin, triangle_count, material, reverse, emission, normal_begin, emitter_begin;
+};
+// wire::Material subset (src/render_wire.h:107-130)
+struct DMaterial {
+    u32 scattering, kind, knot_begin, knot_count;
+    float scalar_value;
+    u32 eta_begin, eta_count, k_begin, k_count, optical_extensions;
+    float u_roughness, v_roughness;
+    u32 remap;
+};
+struct DPositional {
+    float position[3];
+    u32 kind;
+    float light_from_world[9];
+    float cos_falloff_start, cos_falloff_end;
+    u32 spectrum; // offset of the 471-bin intensity in the spectra buffer
+};
+// wire::LightBounds / LightAlias / LightRecord (src/render_wire.h:227-244)
+struct DLightBounds {
+    float low[3], high[3], direction[3];
+    float power, cos_outer, cos_emission;
+    u32 child, parent, light, flags;
+};
+struct DLightAlias {
+    float threshold, pmf;
+    u32 alias, padding;
+};
+struct DLightRecord {
+    u32 leaf, flags, padding0, padding1;
+};
+// Binary BVH node: both child boxes and both child links (64 bytes).
+struct __align__(16) BNode {
+    float4 a; // left lo.xyz, left hi.x
+    float4 b; // left hi.yz, right lo.xy
+    float4 c; // right lo.z, right hi.xyz
+    uint4 d;  // left, right, unused, unused
+};
+
+struct DeviceScene {
+    const float *positions;
+    const float *normals;
+    u32 normal_count;
+    const u32 *triangles;
+    const DInstance *instances;
+    u32 instance_count;
+    const u32 *tri_instance; // per flattened triangle
+    const u32 *tri_local;
+    u32 prim_count;
+    const BNode *nodes;
+    const float4 *leaf_v; // 3 per leaf slot: world v0 (w = prim id bits), v1, v2
+    const DMaterial *materials;
+    u32 material_count;
+    const float2 *knots;
+    u32 knot_count;
+    const float *spectra; // emissions (471 each), positional intensities, environment
+    const u32 *emission_two_sided;
+    u32 emission_count;
+    const DPositional *positional;
+    u32 positional_count;
+    u32 environment; // offset of the environment spectrum or kNone
+    const u32 *emitter_instance;
+    const u32 *emitter_local;
+    u32 emitter_count;
+    const DLightBounds *light_nodes;
+    const DLightAlias *light_alias;
+    const DLightRecord *light_records;
+    const u32 *infinite_lights;
+    u32 light_node_count, infinite_count, light_count, light_sampler, environment_light;
+    float scene_radius;
+    SobolTables sobol;
+    V3 origin, forward, right, up;
+    u32 filter_kind;
+    float filter_x, filter_y;
+    u32 max_depth, hero_mode;
+    float slab_scale; // 1 + 2 gamma(3), the conservative far-plane factor
+};
+
+RP_DEV V3 load3(const float *p) { return v3(__ldg(p), __ldg(p + 1), __ldg(p + 2)); }
+RP_DEV float spectrum(const DeviceScene &s, u32 offset, float w) { return __ldg(s.spectra + offset + dense_index(w)); }
+
+// shaders/light_geometry_sampling.h:10-15
+RP_DEV V3 world_point(const DInstance &in, V3 p) {
+    return v3(dot(v3(in.m[0], in.m[1], in.m[2]), p), dot(v3(in.m[4], in.m[5], in.m[6]), p),
+              dot(v3(in.m[8], in.m[9], in.m[10]), p)) +
+           v3(in.m[3], in.m[7], in.m[11]);
+}
+
+// SurfacePoint subset (shaders/render.metal:870-881)
+struct SurfacePoint {
+    V3 position, error, geometric_normal, shading_normal;
+    float inverse_area_pdf;
+};
+// shaders/render.metal:865-868
+RP_DEV float triangle_extent(V3 e1, V3 e2) {
+    const V3 a = vabs(e1), b = vabs(e2), c = vabs(e2 - e1);
+    return fmaxf(fmaxf(fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y))), fmaxf(a.z, fmaxf(b.z, c.z)));
+}
+// shaders/render.metal:885-968 (triangle_surface_point)
+RP_DEV bool triangle_surface_point(const DeviceScene &s, u32 instance, u32 local, float u, float v, bool native_hit,
+                                   SurfacePoint &point) {
+    const DInstance &in = s.instances[instance];
+    const u32 *tri = s.triangles + 3 * (in.triangle_begin + local);
+    const u32 i0 = __ldg(tri), i1 = __ldg(tri + 1), i2 = __ldg(tri + 2);
+    const V3 p0 = load3(s.positions + 3 * (in.vertex_begin + i0));
+    const V3 p1 = load3(s.positions + 3 * (in.vertex_begin + i1));
+    const V3 p2 = load3(s.positions + 3 * (in.vertex_begin + i2));
+    const V3 ax = v3(in.m[0], in.m[1], in.m[2]), ay = v3(in.m[4], in.m[5], in.m[6]), az = v3(in.m[8], in.m[9], in.m[10]);
+    const V3 shift = v3(in.m[3], in.m[7], in.m[11]);
+    const V3 e1 = p1 - p0, e2 = p2 - p0;
+    const V3 we1 = v3(dot(ax, e1), dot(ay, e1), dot(az, e1));
+    const V3 we2 = v3(dot(ax, e2), dot(ay, e2), dot(az, e2));
+    const V3 ce = cross(we1, we2);
+    const float n2 = dot(ce, ce);
+    if (n2 == 0.0f && !native_hit) {
+        point.position = point.error = point.geometric_normal = point.shading_normal = v3(0, 0, 0);
+        point.inverse_area_pdf = 0;
+        return true;
+    }
+    if (!(n2 > 0.0f) || !isfinite(n2))
+        return false;
+    const float nl = sqrtf(n2);
+    point.inverse_area_pdf = 0.5f * nl;
+    point.geometric_normal = ce / nl;
+    if (in.reverse)
+        point.geometric_normal = -point.geometric_normal;
+    point.shading_normal = point.geometric_normal;
+    if (in.normal_begin != kNone) {
+        const u32 begin = in.normal_begin, nc = s.normal_count;
+        if (begin >= nc || i0 >= nc - begin || i1 >= nc - begin || i2 >= nc - begin)
+            return false;
+        const V3 n0 = load3(s.normals + 3 * (begin + i0)), n1 = load3(s.normals + 3 * (begin + i1)),
+                 n2v = load3(s.normals + 3 * (begin + i2));
+        const V3 interp = (1.0f - (u + v)) * n0 + u * n1 + v * n2v;
+        if (!finite3(interp))
+            return false;
+        const float scale = max3(vabs(interp));
+        if (scale > 0.0f) {
+            const V3 scaled = interp / scale;
+            point.shading_normal = normalize3(scaled);
+            if (dot(point.geometric_normal, scaled) < 0.0f)
+                point.geometric_normal = -point.geometric_normal;
+        }
+    }
+    const V3 lp = p0 + (u * e1 + v * e2);
+    point.position = v3(dot(ax, lp), dot(ay, lp), dot(az, lp)) + shift;
+    V3 local_error = gamma_bound(7.0f) * (vabs(p0) + vabs(u * e1) + vabs(v * e2));
+    if (native_hit) {
+        const float allowance = 64.0f * 0x1.0p-23f;
+        const float traversal = gamma_bound(7.0f) * triangle_extent(e1, e2);
+        local_error = (local_error + allowance * (vabs(e1) + vabs(e2))) + v3(traversal, traversal, traversal);
+    }
+    const V3 ein = local_error + gamma_bound(4.0f) * vabs(lp);
+    point.error = v3(dot(vabs(ax), ein), dot(vabs(ay), ein), dot(vabs(az), ein)) + gamma_bound(4.0f) * vabs(shift);
+    return finite3(point.position) && finite3(point.error) && finite3(point.geometric_normal) &&
+           finite3(point.shading_normal);
+}
+
+// ------------------------------------------------------------------ light selection (shaders/light_sampling.h)
+// :19-42
+RP_DEV float light_importance(const DLightBounds &b, V3 position, V3 normal) {
+    const V3 lo = v3(b.low[0], b.low[1], b.low[2]), hi = v3(b.high[0], b.high[1], b.high[2]);
+    const V3 center = (lo + hi) * .5f;
+    const V3 delta = position - center;
+    const float r2 = dot(hi - lo, hi - lo) * .25f, d2 = dot(delta, delta);
+    const float radius = sqrtf(r2), distance = sqrtf(d2);
+    const float cb = d2 <= r2 ? -1.f : sqrtf(fmaxf(0.f, 1 - r2 / d2));
+    const float sb = sqrtf(fmaxf(0.f, 1 - cb * cb));
+    const V3 wi = distance > 0 ? delta / distance : v3(0, 0, 1);
+    float cw = fminf(fmaxf(dot(v3(b.direction[0], b.direction[1], b.direction[2]), wi), -1.f), 1.f);
+    if (b.flags & 1)
+        cw = fabsf(cw);
+    const float sw = sqrtf(fmaxf(0.f, 1 - cw * cw)), co = b.cos_outer, so = sqrtf(fmaxf(0.f, 1 - co * co));
+    const float cx = cw > co ? 1.f : cw * co + sw * so, sx = cw > co ? 0.f : sw * co - cw * so;
+    const float cp = cx > cb ? 1.f : cx * cb + sx * sb;
+    if (cp <= b.cos_emission)
+        return 0;
+    float value = b.power * cp / fmaxf(d2, fmaxf(radius, kFltMin));
+    if (nonzero3(normal)) {
+        const float ci = fminf(fmaxf(fabsf(dot(wi, normal)), 0.f), 1.f);
+        const float si = sqrtf(fmaxf(0.f, 1 - ci * ci));
+        value *= ci > cb ? 1.f : ci * cb + si * sb;
+    }
+    return fmaxf(0.f, value);
+}
+struct Selected {
+    u32 light;
+    float pmf;
+};
+// :43-95
+RP_DEV Selected light_sample(const DeviceScene &s, V3 position, V3 normal, float u) {
+    const u32 count = s.light_count;
+    if (!count)
+        return {kNone, 0};
+    u = fminf(fmaxf(u, 0.f), kOneMinusEps);
+    if (s.light_sampler == 2) {
+        const u32 id = min(u32(u * count), count - 1);
+        return {id, 1.f / count};
+    }
+    if (s.light_sampler == 1) {
+        const float v = u * count;
+        const u32 i = min(u32(v), count - 1);
+        const u32 id = v - i < s.light_alias[i].threshold ? i : s.light_alias[i].alias;
+        return {id, s.light_alias[id].pmf};
+    }
+    const u32 ninf = s.infinite_count, nodes = s.light_node_count;
+    const float infinite = float(ninf) / float(ninf + (nodes ? 1 : 0));
+    if (u < infinite) {
+        const u32 i = min(u32((u / infinite) * ninf), ninf - 1);
+        return {s.infinite_lights[i], 1.f / float(ninf + (nodes ? 1 : 0))};
+    }
+    if (!nodes)
+        return {kNone, 0};
+    u = fminf((u - infinite) / (1 - infinite), kOneMinusEps);
+    float pmf = 1 - infinite;
+    u32 i = 0;
+    for (u32 steps = 0; steps < nodes; ++steps) {
+        const DLightBounds &node = s.light_nodes[i];
+        if (node.light != kNone) {
+            if (light_importance(node, position, normal) <= 0)
+                return {kNone, 0};
+            return {node.light, pmf};
+        }
+        const float a = light_importance(s.light_nodes[i + 1], position, normal),
+                    b = light_importance(s.light_nodes[node.child], position, normal), sum = a + b;
+        if (!(sum > 0))
+            return {kNone, 0};
+        const float q = a / sum;
+        if (u < q) {
+            pmf *= q;
+            u = fminf(u / q, kOneMinusEps);
+            i++;
+        } else {
+            pmf *= 1 - q;
+            u = fminf((u - q) / (1 - q), kOneMinusEps);
+            i = node.child;
+        }
+    }
+    return {kNone, 0};
+}
+// :96-126
+RP_DEV float light_pmf(const DeviceScene &s, V3 position, V3 normal, u32 id) {
+    if (id >= s.light_count)
+        return 0;
+    if (s.light_sampler == 2)
+        return 1.f / s.light_count;
+    if (s.light_sampler == 1)
+        return s.light_alias[id].pmf;
+    const u32 ninf = s.infinite_count, nodes = s.light_node_count;
+    if (s.light_records[id].flags & 1)
+        return 1.f / float(ninf + (nodes ? 1 : 0));
+    u32 i = s.light_records[id].leaf;
+    if (i >= nodes)
+        return 0;
+    if (light_importance(s.light_nodes[i], position, normal) <= 0)
+        return 0;
+    float result = 1.f - float(ninf) / float(ninf + (nodes ? 1 : 0));
+    for (u32 steps = 0; steps < nodes; ++steps) {
+        const u32 parent = s.light_nodes[i].parent;
+        if (parent == kNone)
+            return result;
+        const float a = light_importance(s.light_nodes[parent + 1], position, normal),
+                    b = light_importance(s.light_nodes[s.light_nodes[parent].child], position, normal), sum = a + b;
+        if (!(sum > 0))
+            return 0;
+        result *= i == parent + 1 ? a / sum : b / sum;
+        i = parent;
+    }
+    return 0;
+}
+
+// ------------------------------------------------------------------ light geometry (src/light_geometry_sampling_shared.h)
+RP_DEV float clamp01(float v) { return fminf(1.f, fmaxf(0.f, v)); }
+RP_DEV float safe_sqrt(float v) { return sqrtf(fmaxf(0.f, v)); }
+RP_DEV V3 unitv(V3 v) { return v / length3(v); }
+RP_DEV bool nonzero_len(V3 v) { return dot(v, v) > 0; }
+// :74-77
+RP_DEV float sph_angle(V3 a, V3 b) {
+    return dot(a, b) < 0 ? kPi - 2 * asinf(fminf(1.f, length3(a + b) / 2)) : 2 * asinf(fminf(1.f, length3(a - b) / 2));
+}
+// :78-85
+RP_DEV float sph_triangle_area(V3 a, V3 b, V3 c) {
+    return fabsf(2 * atan2f(dot(a, cross(b, c)), 1 + dot(a, b) + dot(a, c) + dot(b, c)));
+}
+RP_DEV float triangle_solid_angle(V3 p0, V3 p1, V3 p2, V3 r) {
+    if (!nonzero_len(p0 - r) || !nonzero_len(p1 - r) || !nonzero_len(p2 - r))
+        return 0;
+    return sph_triangle_area(unitv(p0 - r), unitv(p1 - r), unitv(p2 - r));
+}
+struct W4 {
+    float a, b, c, d;
+};
+// :91-115
+RP_DEV W4 normalized_weights(W4 w) {
+    const float s = fmaxf(fmaxf(w.a, w.b), fmaxf(w.c, w.d));
+    return s > 0 ? W4{w.a / s, w.b / s, w.c / s, w.d / s} : W4{1, 1, 1, 1};
+}
+RP_DEV float linear_sample(float u, float a, float b) {
+    if (u == 0 && a == 0)
+        return 0;
+    return fminf(kOneMinusEps, u * (a + b) / (a + sqrtf((1 - u) * a * a + u * b * b)));
+}
+RP_DEV float bilinear_pdf(float ux, float uy, W4 weights) {
+    if (ux < 0 || ux > 1 || uy < 0 || uy > 1)
+        return 0;
+    const W4 w = normalized_weights(weights);
+    return 4 * ((1 - ux) * (1 - uy) * w.a + ux * (1 - uy) * w.b + (1 - ux) * uy * w.c + ux * uy * w.d) /
+           (w.a + w.b + w.c + w.d);
+}
+// :116-121
+RP_DEV W4 triangle_cosines(V3 a, V3 b, V3 c, V3 r, V3 n) {
+    const float wa = fmaxf(.01f, fabsf(dot(n, unitv(a - r))));
+    const float wb = fmaxf(.01f, fabsf(dot(n, unitv(b - r))));
+    const float wc = fmaxf(.01f, fabsf(dot(n, unitv(c - r))));
+    return {wb, wb, wa, wc};
+}
+// :128-172 (PBRT SampleSphericalTriangle, rationalised)
+RP_DEV bool sph_triangle_sample(V3 p0, V3 p1, V3 p2, V3 r, float ux, float uy, float &b1o, float &b2o) {
+    const V3 a = unitv(p0 - r), b = unitv(p1 - r), c = unitv(p2 - r);
+    const V3 nab = cross(a, b), nca = cross(c, a);
+    if (!nonzero_len(nab) || !nonzero_len(nca))
+        return false;
+    const float alpha = sph_angle(unitv(nab), -unitv(nca));
+    const float area = sph_triangle_area(a, b, c);
+    const float ca = cosf(alpha), sa = sinf(alpha);
+    const float subarea = ux * area;
+    const float sh = sinf(subarea / 2), st = sinf(subarea), ct_area = cosf(subarea);
+    const float one_minus_ct = 2 * sh * sh;
+    const float sp = sa * ct_area - ca * st;
+    const float cp = -ca * ct_area - sa * st;
+    const float k1 = -2 * sinf(alpha - subarea / 2) * sh;
+    const float k2 = sa * (.5f * dot(a - b, a - b) - one_minus_ct) - ca * st;
+    const float divisor = (k2 * sp + k1 * cp) * sa;
+    if (divisor == 0)
+        return false;
+    const float omc = fminf(2.f, fmaxf(0.f, (-k2 * one_minus_ct - k1 * st) / divisor));
+    const float cosbp = 1 - omc;
+    const V3 arc = c - dot(c, a) * a;
+    if (!nonzero_len(arc))
+        return false;
+    const V3 cprime = cosbp * a + safe_sqrt(omc * (2 - omc)) * unitv(arc);
+    const float omct = uy * .5f * dot(cprime - b, cprime - b);
+    const float ct = 1 - omct;
+    const V3 tangent = cprime - dot(cprime, b) * b;
+    if (!nonzero_len(tangent))
+        return false;
+    const V3 direction = ct * b + safe_sqrt(omct * (2 - omct)) * unitv(tangent);
+    const V3 e1 = p1 - p0, e2 = p2 - p0, s1 = cross(direction, e2);
+    const float denom = dot(s1, e1);
+    if (denom == 0)
+        return false;
+    const V3 sv = r - p0;
+    float b1 = clamp01(dot(sv, s1) / denom), b2 = clamp01(dot(direction, cross(sv, e1)) / denom);
+    if (b1 + b2 > 1) {
+        const float sum = b1 + b2;
+        b1 /= sum;
+        b2 /= sum;
+    }
+    b1o = b1;
+    b2o = b2;
+    return isfinite(b1) && isfinite(b2);
+}
+// :174-182
+RP_DEV void sph_triangle_inverse(V3 p0, V3 p1, V3 p2, V3 r, V3 dir, float &u0, float &u1) {
+    const V3 a = unitv(p0 - r), b = unitv(p1 - r), c = unitv(p2 - r);
+    V3 cp = unitv(cross(cross(b, dir), cross(c, a)));
+    if (dot(cp, a + c) < 0)
+        cp = -cp;
+    u0 = clamp01(sph_triangle_area(a, b, cp) / sph_triangle_area(a, b, c));
+    u1 = clamp01(dot(dir - b, dir - b) / dot(cp - b, cp - b));
+}
+// shaders/light_geometry_sampling.h:16-29
+RP_DEV void emitter_corners(const DeviceScene &s, u32 emitter, V3 p[3]) {
+    const DInstance &in = s.instances[s.emitter_instance[emitter]];
+    const u32 *tri = s.triangles + 3 * (in.triangle_begin + s.emitter_local[emitter]);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        p[i] = world_point(in, load3(s.positions + 3 * (in.vertex_begin + __ldg(tri + i))));
+}
+// shaders/light_geometry_sampling.h:58-67
+RP_DEV float area_solid_angle_pdf(float area_density, V3 reference, const SurfacePoint &point) {
+    const V3 delta = point.position - reference;
+    const float d2 = dot(delta, delta);
+    if (!(d2 > 0) || !(area_density > 0))
+        return 0;
+    const float cosine = fabsf(dot(point.geometric_normal, delta * (1.0f / sqrtf(d2))));
+    return cosine > 0 ? area_density * d2 / cosine : 0;
+}
+// shaders/light_geometry_sampling.h:116-153 (triangles)
+RP_DEV float light_geometry_pdf(const DeviceScene &s, u32 emitter, V3 reference, V3 normal, const SurfacePoint &point) {
+    const V3 delta = point.position - reference;
+    if (!(dot(delta, delta) > 0) || !(point.inverse_area_pdf > 0))
+        return 0;
+    V3 p[3];
+    emitter_corners(s, emitter, p);
+    const float area = triangle_solid_angle(p[0], p[1], p[2], reference);
+    if (area >= 3e-4f && area <= 6.22f) {
+        float u0, u1;
+        sph_triangle_inverse(p[0], p[1], p[2], reference, normalize3(delta), u0, u1);
+        return (dot(normal, normal) > 0 ? bilinear_pdf(u0, u1, triangle_cosines(p[0], p[1], p[2], reference, normal))
+                                        : 1.f) /
+               area;
+    }
+    return area_solid_angle_pdf(1 / point.inverse_area_pdf, reference, point);
+}
+// shaders/light_geometry_sampling.h:155-209 (triangles)
+RP_DEV bool light_geometry_sample(const DeviceScene &s, u32 emitter, V3 reference, V3 normal, float ux, float uy,
+                                  SurfacePoint &point, float &pdf) {
+    if (!isfinite(ux) || !isfinite(uy) || ux < 0 || uy < 0 || ux > 1 || uy > 1)
+        return false;
+    ux = fminf(ux, kOneMinusEps);
+    uy = fminf(uy, kOneMinusEps);
+    V3 p[3];
+    emitter_corners(s, emitter, p);
+    float b1, b2;
+    const float area = triangle_solid_angle(p[0], p[1], p[2], reference);
+    if (area >= 3e-4f && area <= 6.22f) {
+        if (dot(normal, normal) > 0) {
+            const W4 w = normalized_weights(triangle_cosines(p[0], p[1], p[2], reference, normal));
+            const float y = linear_sample(uy, w.a + w.b, w.c + w.d);
+            const float x = linear_sample(ux, (1 - y) * w.a + y * w.c, (1 - y) * w.b + y * w.d);
+            ux = x;
+            uy = y;
+        }
+        if (!sph_triangle_sample(p[0], p[1], p[2], reference, ux, uy, b1, b2))
+            return false;
+    } else {
+        const float root = sqrtf(ux);
+        b1 = 1 - root;
+        b2 = uy * root;
+    }
+    if (!isfinite(b1) || !isfinite(b2) ||
+        !triangle_surface_point(s, s.emitter_instance[emitter], s.emitter_local[emitter], b1, b2, false, point))
+        return false;
+    pdf = light_geometry_pdf(s, emitter, reference, normal, point);
+    return isfinite(pdf) && pdf >= 0;
+}
+
+// ------------------------------------------------------------------ positional lights (shaders/render.metal:654-811)
+RP_DEV bool normal_or_zero(float v) {
+    const u32 m = fbits(v) & 0x7fffffffu;
+    return m == 0 || (m >= 0x00800000u && m < 0x7f800000u);
+}
+RP_DEV bool spot_product(float a, float b, float &r) {
+    if (a != 0 && b != 0 && fabsf(a) < kFltMin / fabsf(b))
+        return false;
+    r = a * b;
+    return normal_or_zero(r) && (r != 0 || a == 0 || b == 0);
+}
+RP_DEV bool spot_sum(float a, float b, float &r) {
+    r = a + b;
+    return normal_or_zero(r) && (r != 0 || a == -b);
+}
+RP_DEV bool spot_divide(float a, float b, float &r) {
+    r = a / b;
+    return normal_or_zero(r) && (r != 0 || a == 0);
+}
+RP_DEV bool positional_intensity(const DPositional &L, V3 wi, float &intensity) {
+    if (L.kind == 0)
+        return true;
+    if (L.kind != 1)
+        return false;
+    float w[3];
+    const float nwi[3] = {-wi.x, -wi.y, -wi.z};
+#pragma unroll
+    for (int row = 0; row < 3; ++row) {
+        float terms[3];
+#pragma unroll
+        for (int col = 0; col < 3; ++col)
+            if (!spot_product(L.light_from_world[row * 3 + col], nwi[col], terms[col]))
+                return false;
+        float sum, c;
+        if (!spot_sum(terms[0], terms[1], sum) || !spot_sum(sum, terms[2], c))
+            return false;
+        w[row] = c;
+    }
+    const float scale = fmaxf(fmaxf(fabsf(w[0]), fabsf(w[1])), fabsf(w[2]));
+    if (!(scale >= kFltMin) || !isfinite(scale))
+        return false;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float c;
+        if (!spot_divide(w[i], scale, c))
+            return false;
+        w[i] = c;
+    }
+    float cosine;
+    if (!spot_divide(w[2], sqrtf(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]), cosine))
+        return false;
+    const float end = L.cos_falloff_end, start = L.cos_falloff_start;
+    const float t = start == end ? (cosine < end ? 0.0f : 1.0f) : fminf(fmaxf((cosine - end) / (start - end), 0.0f), 1.0f);
+    const float falloff = start == end ? t : t * t * (3.0f - 2.0f * t);
+    intensity *= falloff;
+    return isfinite(intensity) && intensity >= 0;
+}
+
+// ------------------------------------------------------------------ traversal
+// Watertight ray/triangle intersection (Woop, Benthin and Wald, JCGT 2(1), 2013).
+RP_DEV bool intersect_triangle(V3 o, V3 d, V3 v0, V3 v1, V3 v2, float tmax, float &t, float &b1, float &b2) {
+    const V3 ad = vabs(d);
+    const int kz = ad.x > ad.y ? (ad.x > ad.z ? 0 : 2) : (ad.y > ad.z ? 1 : 2);
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    if (comp(d, kz) < 0) {
+        const int t0 = kx;
+        kx = ky;
+        ky = t0;
+    }
+    const float dz = comp(d, kz);
+    const float sx = comp(d, kx) / dz, sy = comp(d, ky) / dz, sz = 1.0f / dz;
+    const V3 A = v0 - o, B = v1 - o, C = v2 - o;
+    const float ax = fmaf(-sx, comp(A, kz), comp(A, kx)), ay = fmaf(-sy, comp(A, kz), comp(A, ky));
+    const float bx = fmaf(-sx, comp(B, kz), comp(B, kx)), by = fmaf(-sy, comp(B, kz), comp(B, ky));
+    const float cx = fmaf(-sx, comp(C, kz), comp(C, kx)), cy = fmaf(-sy, comp(C, kz), comp(C, ky));
+    float U = fmaf(cx, by, -(cy * bx));
+    float Vv = fmaf(ax, cy, -(ay * cx));
+    float W = fmaf(bx, ay, -(by * ax));
+    if (U == 0 || Vv == 0 || W == 0) {
+        U = float(double(cx) * double(by) - double(cy) * double(bx));
+        Vv = float(double(ax) * double(cy) - double(ay) * double(cx));
+        W = float(double(bx) * double(ay) - double(by) * double(ax));
+    }
+    if ((U < 0 || Vv < 0 || W < 0) && (U > 0 || Vv > 0 || W > 0))
+        return false;
+    const float det = U + Vv + W;
+    if (det == 0)
+        return false;
+    const float az = sz * comp(A, kz), bz = sz * comp(B, kz), cz = sz * comp(C, kz);
+    const float T = fmaf(U, az, fmaf(Vv, bz, W * cz));
+    if (det > 0 ? (T <= 0 || T >= tmax * det) : (T >= 0 || T <= tmax * det))
+        return false;
+    const float rcp = 1.0f / det;
+    t = T * rcp;
+    b1 = Vv * rcp;
+    b2 = W * rcp;
+    return t > 0 && t < tmax;
+}
+
+// Conservative slab test (Ize, JCGT 2(2), 2013), same operation order as the CPU LBVH.
+RP_DEV bool slab(float lx, float ly, float lz, float hx, float hy, float hz, V3 o, V3 inv, float tmax, float scale,
+                 float &tenter) {
+    float t0 = 0, t1 = tmax;
+    {
+        float tn = (lx - o.x) * inv.x, tf = (hx - o.x) * inv.x;
+        if (tn > tf) {
+            const float q = tn;
+            tn = tf;
+            tf = q;
+        }
+        tf *= scale;
+        t0 = tn > t0 ? tn : t0;
+        t1 = tf < t1 ? tf : t1;
+        if (!(t0 <= t1))
+            return false;
+    }
+    {
+        float tn = (ly - o.y) * inv.y, tf = (hy - o.y) * inv.y;
+        if (tn > tf) {
+            const float q = tn;
+            tn = tf;
+            tf = q;
+        }
+        tf *= scale;
+        t0 = tn > t0 ? tn : t0;
+        t1 = tf < t1 ? tf : t1;
+        if (!(t0 <= t1))
+            return false;
+    }
+    {
+        float tn = (lz - o.z) * inv.z, tf = (hz - o.z) * inv.z;
+        if (tn > tf) {
+            const float q = tn;
+            tn = tf;
+            tf = q;
+        }
+        tf *= scale;
+        t0 = tn > t0 ? tn : t0;
+        t1 = tf < t1 ? tf : t1;
+        if (!(t0 <= t1))
+            return false;
+    }
+    tenter = t0;
+    return true;
+}
+
+struct Hit {
+    float t, b1, b2;
+    u32 prim;
+};
+
+// Stack depth for traversal; deeper trees report an invalid hit.
+constexpr int kStackDepth = 64;
+
+// Closest hit: minimises (t, primitive id) so the result is independent of visit order.
+// `stack` is this thread's slice of a shared-memory stack with stride `stride`.
+template <bool Count>
+RP_DEV bool trace_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, u32 *stack, int stride,
+                          u32 &nodes_visited, u32 &tris_tested) {
+    h.t = tmax;
+    h.b1 = h.b2 = 0;
+    h.prim = kNone;
+    if (s.prim_count == 0)
+        return true;
+    const V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    const float scale = s.slab_scale;
+    auto test_leaf = [&](u32 slot) {
+        const float4 a = __ldg(s.leaf_v + 3 * slot), b = __ldg(s.leaf_v + 3 * slot + 1), c = __ldg(s.leaf_v + 3 * slot + 2);
+        const u32 prim = __float_as_uint(a.w);
+        float t, b1, b2;
+        if (Count)
+            ++tris_tested;
+        if (intersect_triangle(o, d, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tmax, t, b1, b2) &&
+            (t < h.t || (t == h.t && prim < h.prim))) {
+            h.t = t;
+            h.b1 = b1;
+            h.b2 = b2;
+            h.prim = prim;
+        }
+    };
+    if (s.prim_count == 1) {
+        test_leaf(0);
+        return true;
+    }
+    int sp = 0;
+    u32 node = 0;
+    // a binary tree over prim_count leaves has prim_count - 1 internal nodes
+    for (u32 guard = 0; guard < s.prim_count; ++guard) {
+        const BNode n = s.nodes[node];
+        if (Count)
+            ++nodes_visited;
+        float tl, tr;
+        bool hl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, o, inv, h.t, scale, tl);
+        bool hr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, o, inv, h.t, scale, tr);
+        const u32 l = n.d.x, r = n.d.y;
+        if (hl && (l & kLeaf)) {
+            test_leaf(l & ~kLeaf);
+            hl = false;
+        }
+        if (hr && (r & kLeaf)) {
+            test_leaf(r & ~kLeaf);
+            hr = false;
+        }
+        u32 next = kNone;
+        if (hl && hr) {
+            const bool right_first = tr < tl;
+            if (sp >= kStackDepth)
+                return false;
+            stack[sp * stride] = right_first ? l : r;
+            ++sp;
+            next = right_first ? r : l;
+        } else if (hl)
+            next = l;
+        else if (hr)
+            next = r;
+        if (next == kNone) {
+            if (sp == 0)
+                return true;
+            --sp;
+            next = stack[sp * stride];
+        }
+        node = next;
+    }
+    return false;
+}
+
+// Any hit in (0, tmax): the shadow-ray occlusion query.
+template <bool Count>
+RP_DEV bool trace_any(const DeviceScene &s, V3 o, V3 d, float tmax, bool &occluded, u32 *stack, int stride,
+                      u32 &nodes_visited, u32 &tris_tested) {
+    occluded = false;
+    if (s.prim_count == 0)
+        return true;
+    const V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    const float scale = s.slab_scale;
+    auto hit_leaf = [&](u32 slot) -> bool {
+        const float4 a = __ldg(s.leaf_v + 3 * slot), b = __ldg(s.leaf_v + 3 * slot + 1), c = __ldg(s.leaf_v + 3 * slot + 2);
+        float t, b1, b2;
+        if (Count)
+            ++tris_tested;
+        return intersect_triangle(o, d, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tmax, t, b1, b2);
+    };
+    if (s.prim_count == 1) {
+        occluded = hit_leaf(0);
+        return true;
+    }
+    int sp = 0;
+    u32 node = 0;
+    for (u32 guard = 0; guard < s.prim_count; ++guard) {
+        const BNode n = s.nodes[node];
+        if (Count)
+            ++nodes_visited;
+        float tl, tr;
+        bool hl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, o, inv, tmax, scale, tl);
+        bool hr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, o, inv, tmax, scale, tr);
+        const u32 l = n.d.x, r = n.d.y;
+        if (hl && (l & kLeaf)) {
+            if (hit_leaf(l & ~kLeaf)) {
+                occluded = true;
+                return true;
+            }
+            hl = false;
+        }
+        if (hr && (r & kLeaf)) {
+            if (hit_leaf(r & ~kLeaf)) {
+                occluded = true;
+                return true;
+            }
+            hr = false;
+        }
+        u32 next = kNone;
+        if (hl && hr) {
+            if (sp >= kStackDepth)
+                return false;
+            stack[sp * stride] = r;
+            ++sp;
+            next = l;
+        } else if (hl)
+            next = l;
+        else if (hr)
+            next = r;
+        if (next == kNone) {
+            if (sp == 0)
+                return true;
+            --sp;
+            next = stack[sp * stride];
+        }
+        node = next;
+    }
+    return false;
+}
+
+} // namespace rp

@@ -1,0 +1,281 @@
+// Wavefront hero-wavelength path tracing: one event of shaders/packet_pt_event_body.inc split
+// at its two traversal points.  The closest-hit query runs in its own kernel, the event body
+// (emission MIS, light sample, BSDF continuation, roulette) in the shade kernel, and the
+// light sample's visibility in the shadow kernel, with SoA path state in HBM in between.
+#pragma once
+
+#include "rp_scene.cuh"
+
+namespace rp {
+
+enum : u32 { kCamera = 0, kSurface = 1, kLight = 2, kEnvironment = 3 };
+
+// Path flags word (ident.w)
+enum : u32 {
+    F_MASK = 0xfu,            // hero active wavelength mask
+    F_ROULETTE = 1u << 4,     // roulette enabled
+    F_COMPLETE = 1u << 5,
+    F_STATUS_SHIFT = 6,       // 3 bits
+    F_LTYPE_SHIFT = 9,        // latest vertex type, 2 bits
+    F_PTYPE_SHIFT = 11,       // preceding vertex type, 2 bits
+    F_LDELTA = 1u << 13,      // latest vertex sampled a Dirac lobe
+    F_LKIND_SHIFT = 14,       // latest BSDF family, 2 bits
+    F_LMASK_SHIFT = 16,       // latest BSDF active mask, 4 bits
+    F_LSMOOTH = 1u << 20,     // latest BSDF roughness is smooth
+};
+RP_DEV u32 get_status(u32 f) { return (f >> F_STATUS_SHIFT) & 7u; }
+RP_DEV u32 set_status(u32 f, u32 s) { return (f & ~(7u << F_STATUS_SHIFT)) | (s << F_STATUS_SHIFT); }
+
+// Structure-of-arrays path pool: one slot per lane of the wave.
+struct PathPool {
+    uint4 *ident;      // pixel, sample_low, sample_high, flags
+    uint4 *cursor;     // sobol index lo, hi, vertex count, lane
+    float4 *lambda, *lambda_pdf, *beta, *radiance;
+    float4 *dens_f, *prev_f; // hero density fractions (arrival / previous)
+    int4 *dens_e, *prev_e;   // and exponents
+    float4 *eta_scale;
+    float4 *ray_o, *ray_d;
+    float4 *latest_p;      // latest vertex position, alpha_x
+    float4 *latest_n;      // latest shading normal, alpha_y
+    float4 *latest_param;  // per-wavelength reflectance or eta
+    float4 *latest_k;      // per-wavelength conductor k
+    float4 *preceding;     // position of the vertex before latest
+    float4 *hit;           // t, b1, b2, primitive bits
+    // queues
+    u32 *queue[2];
+    u32 *counters; // [0] queue0, [1] queue1, [2] shadow, [3] failures
+    float4 *sh_o;  // shadow origin, tmax
+    float4 *sh_d;  // shadow direction, path id bits
+    float4 *sh_c;  // weighted contribution (NaN x: invalid if visible)
+    // statistics (optional)
+    unsigned long long *stats; // [0] nodes visited, [1] triangles tested, [2] closest rays, [3] shadow rays
+};
+
+struct WaveParams {
+    u32 width, height, pixel_begin, pixel_count, sample_low, sample_high;
+    u32 seed_low, seed_high, sampler, randomization, m, emergency_limit;
+    u32 lanes;
+};
+
+RP_DEV float sample_uniform(const WaveParams &p, u32 w) { return p.sampler == 0 ? u01(w) : sobol_uniform(w); }
+
+// shaders/render.metal:154-179 (independent and Sobol samplers)
+RP_DEV uint4 draw_words(const DeviceScene &s, const WaveParams &p, u32 pixel, u32 slo, u32 shi, u64 index, u32 block) {
+    if (p.sampler == 0)
+        return philox(make_uint4(pixel, slo, shi, block), p.seed_low, p.seed_high);
+    const u32 d = 4 * block;
+    return make_uint4(sobol_word(s.sobol, index, d, p.randomization, p.seed_low),
+                      sobol_word(s.sobol, index, d + 1, p.randomization, p.seed_low),
+                      sobol_word(s.sobol, index, d + 2, p.randomization, p.seed_low),
+                      sobol_word(s.sobol, index, d + 3, p.randomization, p.seed_low));
+}
+
+struct BeginSample {
+    u32 pixel, sample_low, sample_high;
+    u64 index;
+    uint4 words;
+};
+// shaders/render.metal:238-311 (begin_sample)
+RP_DEV BeginSample begin_sample(const DeviceScene &s, const WaveParams &p, u32 lane) {
+    BeginSample r;
+    r.pixel = p.pixel_begin + lane % p.pixel_count;
+    r.sample_low = p.sample_low + lane / p.pixel_count;
+    r.sample_high = p.sample_high + u32(r.sample_low < p.sample_low);
+    if (p.sampler == 1) {
+        const u64 sample = (u64(r.sample_high) << 32) | r.sample_low;
+        r.index = sobol_index(s.sobol, p.m, r.pixel % p.width, r.pixel / p.width, sample);
+        r.words = make_uint4(sobol_word(s.sobol, r.index, 0, 0, 0), sobol_word(s.sobol, r.index, 1, 0, 0),
+                             sobol_word(s.sobol, r.index, 2, p.randomization, p.seed_low),
+                             sobol_word(s.sobol, r.index, 3, p.randomization, p.seed_low));
+    } else {
+        r.index = 0;
+        r.words = philox(make_uint4(r.pixel, r.sample_low, r.sample_high, 0), p.seed_low, p.seed_high);
+    }
+    return r;
+}
+// shaders/render.metal:352-357
+RP_DEV float triangle_offset(float u, float radius) {
+    const float sv = 2.0f * u - 1.0f;
+    return radius * (sv / (1.0f + sqrtf(1.0f - fabsf(sv))));
+}
+// shaders/render.metal:341-476 (primary_ray: pinhole, box / triangle filter)
+RP_DEV void primary_ray(const DeviceScene &s, const WaveParams &p, const BeginSample &b, V3 &o, V3 &d) {
+    float ux, uy;
+    if (p.sampler == 1) {
+        ux = sobol_camera_uniform(b.words.x, p.m, b.pixel % p.width);
+        uy = sobol_camera_uniform(b.words.y, p.m, b.pixel / p.width);
+    } else {
+        ux = u01(b.words.x);
+        uy = u01(b.words.y);
+    }
+    o = s.origin;
+    const bool centered = s.filter_kind != 0 || s.filter_x != 0.5f || s.filter_y != 0.5f;
+    if (centered) {
+        const float ox = s.filter_kind == 1 ? triangle_offset(ux, s.filter_x) : (2.0f * ux - 1.0f) * s.filter_x;
+        const float oy = s.filter_kind == 1 ? triangle_offset(uy, s.filter_y) : (2.0f * uy - 1.0f) * s.filter_y;
+        const float x = ((float(b.pixel % p.width) + 0.5f) + ox) / float(p.width);
+        const float y = ((float(b.pixel / p.width) + 0.5f) + oy) / float(p.height);
+        const V3 dd = fma3(v3(y, y, y), s.up, fma3(v3(x, x, x), s.right, s.forward));
+        const float scale = fmaxf(fabsf(dd.x), fmaxf(fabsf(dd.y), fabsf(dd.z)));
+        const float nan = __int_as_float(0x7fffffff);
+        if (!finite3(dd) || !(scale > 0.0f)) {
+            d = v3(nan, nan, nan);
+            return;
+        }
+        const V3 scaled = dd / scale;
+        if (!finite3(scaled) || zero3(scaled)) {
+            d = v3(nan, nan, nan);
+            return;
+        }
+        d = normalize3(scaled);
+        return;
+    }
+    const float x = (float(b.pixel % p.width) + ux) / float(p.width);
+    const float y = (float(b.pixel / p.width) + uy) / float(p.height);
+    const V3 dd = s.forward + x * s.right + y * s.up;
+    const float scale = fmaxf(fabsf(dd.x), fmaxf(fabsf(dd.y), fabsf(dd.z)));
+    d = normalize3(dd / scale);
+}
+
+// shaders/packet_walk.h:22-57 (sampled / constant / blackbody reflectance)
+RP_DEV bool material_reflectance(const DeviceScene &s, const DMaterial &m, float w, float &rho) {
+    if (m.scattering != 0) {
+        rho = 1;
+    } else if (m.kind == 0 && m.knot_count >= 2 && m.knot_begin <= s.knot_count &&
+               m.knot_count <= s.knot_count - m.knot_begin) {
+        rho = pbrt_reflectance(s.knots + m.knot_begin, m.knot_count, w);
+    } else if (m.kind == 1) {
+        rho = m.scalar_value;
+    } else if (m.kind == 4) {
+        rho = blackbody_reflectance(m.scalar_value, w);
+    } else
+        return false;
+    return isfinite(rho) && rho >= 0 && rho <= 1;
+}
+// shaders/hero_current_bsdf.h:72-101 with prepare_scattering (shaders/render.metal:2079-2160)
+RP_DEV bool prepare_bsdf(const DeviceScene &s, const DMaterial &m, V4 lambda, u32 mask, HeroBsdf &out) {
+    out.kind = m.scattering;
+    out.active_mask = mask;
+    out.g = {0, 0, true};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        out.param[k] = 0;
+        out.k[k] = 0;
+    }
+    if (m.scattering > 2)
+        return false;
+    if (m.scattering != 0) {
+        const float u = m.u_roughness, v = m.v_roughness;
+        if (!isfinite(u) || !isfinite(v) || u < 0 || v < 0)
+            return false;
+        prepare_roughness(u, v, m.remap != 0, false, out.g);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (!(mask & (1u << k)))
+            continue;
+        float rho;
+        if (!material_reflectance(s, m, lambda.v[k], rho))
+            return false;
+        if (m.scattering == 0) {
+            out.param[k] = rho;
+            continue;
+        }
+        const float eta = optical_value(s.knots, m.eta_begin, m.eta_count, s.knot_count, (m.optical_extensions & 1u) != 0,
+                                        lambda.v[k]);
+        const float kk = optical_value(s.knots, m.k_begin, m.k_count, s.knot_count, (m.optical_extensions & 2u) != 0,
+                                       lambda.v[k]);
+        if (m.scattering == 1) {
+            // shaders/conductor.h:22-25
+            if (!isfinite(eta) || !isfinite(kk) || eta < 0 || kk < 0 || (eta == 0 && kk == 0))
+                return false;
+            out.param[k] = eta;
+            out.k[k] = kk;
+        } else {
+            // shaders/dielectric.h:15-18
+            if (!isfinite(eta) || eta < 0)
+                return false;
+            out.param[k] = eta == 0 ? 1 : eta;
+        }
+    }
+    return true;
+}
+
+// Compact record of the latest vertex for emission MIS (HeroPrevious, shaders/hero_pt_state.h:6-15).
+struct Latest {
+    u32 type, kind, mask;
+    bool delta, smooth;
+    V3 position, shading_normal;
+    float alpha_x, alpha_y;
+    V4 param, k;
+};
+RP_DEV HeroBsdf latest_bsdf(const Latest &l) {
+    HeroBsdf b;
+    b.kind = l.kind;
+    b.active_mask = l.mask;
+    b.g = {l.alpha_x, l.alpha_y, l.smooth};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        b.param[k] = l.param.v[k];
+        b.k[k] = l.k.v[k];
+    }
+    return b;
+}
+// shaders/hero_pt_helpers.h:122-132 (hero_represented_pdf) for a surface vertex v with
+// finite neighbours (the neighbour after v may be at infinity: pass its direction).
+RP_DEV V4 represented_pdf(const HeroBsdf &b, V3 shading_normal, V3 position, V3 before, bool after_infinite,
+                          V3 after_point, bool &ok) {
+    ok = true;
+    const V3 wb = before - position;
+    const V3 wa = after_infinite ? after_point : after_point - position;
+    if (zero3(wb) || zero3(wa))
+        return v4(0);
+    Frame f;
+    if (!shading_frame(shading_normal, f)) {
+        ok = false;
+        return v4(0);
+    }
+    const HeroEval e = hero_evaluate(b, to_local(f, normalize3(wb)), to_local(f, normalize3(wa)));
+    if (!e.valid) {
+        ok = false;
+        return v4(0);
+    }
+    return e.pdf;
+}
+// shaders/hero_pt_helpers.h:133-148 (hero_weight); returns false for invalid arithmetic
+RP_DEV bool hero_weight(const Density &prefix, V4 value, V4 sampled, V4 other, V4 &out) {
+    if (!finite_nonnegative4(value) || !finite_nonnegative4(sampled) || !finite_nonnegative4(other)) {
+        out = v4(0);
+        return false;
+    }
+    if (mixture(prefix, other).fraction == 0) {
+        out = value;
+        return true;
+    }
+    const Contribution r = balance_contribution(prefix, value, sampled, other);
+    out = r.value;
+    return r.valid;
+}
+
+RP_DEV Density load_density(float4 f, int4 e) {
+    Density d;
+    d.lane[0] = {f.x, e.x};
+    d.lane[1] = {f.y, e.y};
+    d.lane[2] = {f.z, e.z};
+    d.lane[3] = {f.w, e.w};
+    return d;
+}
+RP_DEV void store_density(const Density &d, float4 &f, int4 &e) {
+    f = make_float4(d.lane[0].fraction, d.lane[1].fraction, d.lane[2].fraction, d.lane[3].fraction);
+    e = make_int4(d.lane[0].exponent, d.lane[1].exponent, d.lane[2].exponent, d.lane[3].exponent);
+}
+
+// shaders/packet_transport.h:77-83
+RP_DEV V3 offset_point(V3 position, V3 error, V3 ng, V3 direction) {
+    if (!nonzero3(ng))
+        return position;
+    const V3 n = dot(direction, ng) < 0 ? -ng : ng;
+    return round_out(position + dot(vabs(n), error) * n, n);
+}
+
+} // namespace rp

@@ -1,0 +1,210 @@
+"""Host-side mirror of rypath's renderer interface over the C ABI.
+
+Names and meanings follow the reference (src/metal_render.hpp:14-95, src/render_driver.hpp):
+
+* ``build_renderer(scene)`` ~ ``build_metal_renderer(RenderScene, ...)`` -> ``RenderBuildResult``
+  with ``status``, ``diagnostic`` and ``scene`` (a ``CudaRenderScene``).
+* ``CudaRenderScene.sample(request)`` ~ ``MetalRenderScene::sample(RenderRequest)`` ->
+  ``RenderSamplesResult`` whose ``packet_samples`` are the 80-byte packet results in lane order.
+* ``render_progressive(scene, settings)`` ~ the driver loop of src/render_driver.cpp:166-275 with
+  the packet film reduction performed on the device.
+
+Errors follow the reference: failures are statuses plus diagnostics, never exceptions from
+the native layer (a Python exception is raised only for misuse of this binding).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import abi, native, scenes
+
+
+@dataclass
+class RenderRequest:
+    width: int
+    height: int
+    seed: int = 1
+    material_seed: int = 0
+    pixel_begin: int = 0
+    pixel_count: int = 0
+    sample_begin: int = 0
+    sample_count: int = 1
+    emergency_limit: int = 1024
+    sampler: int = abi.SAMPLER_SOBOL
+    randomization: int = abi.RANDOMIZE_OWEN
+    boundary_limit: int = 4096
+
+    def to_c(self) -> abi.Request:
+        r = abi.Request()
+        r.width, r.height, r.seed, r.material_seed = self.width, self.height, self.seed, self.material_seed
+        r.pixel_begin = self.pixel_begin
+        r.pixel_count = self.pixel_count or self.width * self.height
+        r.sample_begin, r.sample_count = self.sample_begin, self.sample_count
+        r.emergency_limit, r.sampler_kind = self.emergency_limit, self.sampler
+        r.randomization, r.boundary_limit = self.randomization, self.boundary_limit
+        return r
+
+
+@dataclass
+class RenderSamplesResult:
+    status: int = abi.RP_FAILURE
+    diagnostic: str = ""
+    packet_samples: np.ndarray | None = None
+
+
+@dataclass
+class RenderBuildResult:
+    status: int = abi.RP_FAILURE
+    diagnostic: str = ""
+    scene: "CudaRenderScene | None" = None
+    device: abi.DeviceInfo | None = None
+
+
+@dataclass
+class RenderSettings:
+    width: int = 256
+    height: int = 192
+    samples: int = 128
+    batch_size: int = 8
+    seed: int = 1
+    sampler: int = abi.SAMPLER_SOBOL
+    randomization: int = abi.RANDOMIZE_OWEN
+
+
+class CudaRenderScene:
+    """A scene resident on one GPU.  Synchronous calls need external serialisation."""
+
+    def __init__(self, handle):
+        self._handle = C.c_void_p(handle)
+        self._cie_set = False
+
+    def close(self):
+        if self._handle:
+            native.lib().rp_cuda_scene_destroy(self._handle)
+            self._handle = C.c_void_p()
+
+    __del__ = close
+
+    @property
+    def handle(self):
+        return self._handle
+
+    def sample(self, request: RenderRequest) -> RenderSamplesResult:
+        q = request.to_c()
+        lanes = q.pixel_count * q.sample_count
+        out = np.zeros(lanes, abi.packet_dtype())
+        diag = C.create_string_buffer(512)
+        st = native.lib().rp_cuda_sample(self._handle, C.byref(q), out.ctypes.data, lanes, diag, 512)
+        return RenderSamplesResult(st, diag.value.decode(errors="replace"), out)
+
+    def sample_device(self, request: RenderRequest, device_ptr: int, capacity: int, stream: int = 0) -> int:
+        q = request.to_c()
+        diag = C.create_string_buffer(512)
+        st = native.lib().rp_cuda_sample_device(self._handle, C.byref(q), C.c_void_p(device_ptr), capacity,
+                                                C.c_void_p(stream), diag, 512)
+        native.check(st, diag, "rp_cuda_sample_device")
+        return st
+
+    def _ensure_cie(self):
+        if not self._cie_set:
+            cie = np.ascontiguousarray(scenes.cie_xyz())
+            native.check(native.lib().rp_cuda_set_cie(self._handle, cie.ctypes.data), None, "rp_cuda_set_cie")
+            self._cie_set = True
+
+    def render_film(self, settings: RenderSettings, film: np.ndarray | None = None, sample_begin: int = 0):
+        """Progressive render into a host film (structured rp_film_pixel array)."""
+        self._ensure_cie()
+        pixels = settings.width * settings.height
+        if film is None:
+            film = np.zeros(pixels, abi.film_dtype())
+        r = abi.FilmRequest(width=settings.width, height=settings.height, seed=settings.seed,
+                            sample_begin=sample_begin, sample_count=settings.samples, batch_size=settings.batch_size,
+                            sampler_kind=settings.sampler, randomization=settings.randomization, emergency_limit=1024)
+        diag = C.create_string_buffer(512)
+        st = native.lib().rp_cuda_render_film(self._handle, C.byref(r), film.ctypes.data, diag, 512)
+        return st, diag.value.decode(errors="replace"), film
+
+    def render_film_device(self, settings: RenderSettings, device_film_ptr: int, sample_begin: int = 0):
+        self._ensure_cie()
+        r = abi.FilmRequest(width=settings.width, height=settings.height, seed=settings.seed,
+                            sample_begin=sample_begin, sample_count=settings.samples, batch_size=settings.batch_size,
+                            sampler_kind=settings.sampler, randomization=settings.randomization, emergency_limit=1024)
+        diag = C.create_string_buffer(512)
+        st = native.lib().rp_cuda_render_film_device(self._handle, C.byref(r), C.c_void_p(device_film_ptr), diag, 512)
+        native.check(st, diag, "rp_cuda_render_film_device")
+
+    def timing(self) -> abi.Timing:
+        t = abi.Timing()
+        native.lib().rp_cuda_last_timing(self._handle, C.byref(t))
+        return t
+
+    def set_counting(self, enabled: bool):
+        native.lib().rp_cuda_set_counting(self._handle, int(enabled))
+
+    def export_bvh(self, n: int):
+        nodes = np.zeros((max(n - 1, 1), 3), np.uint32)
+        order = np.zeros(n, np.uint32)
+        keys = np.zeros(n, np.uint64)
+        bounds = np.zeros((2 * n - 1 if n else 1, 6), np.float32)
+        diag = C.create_string_buffer(512)
+        st = native.lib().rp_cuda_scene_export_bvh(self._handle, nodes.ctypes.data, order.ctypes.data,
+                                                    keys.ctypes.data, bounds.ctypes.data, n, diag, 512)
+        native.check(st, diag, "rp_cuda_scene_export_bvh")
+        return nodes, order, keys, bounds
+
+    def trace(self, rays: np.ndarray, any_hit: bool = False) -> np.ndarray:
+        rays = np.ascontiguousarray(rays, np.float32)
+        hits = np.zeros((rays.shape[0], 4), np.float32)
+        diag = C.create_string_buffer(512)
+        st = native.lib().rp_cuda_trace_rays(self._handle, rays.ctypes.data, rays.shape[0], int(any_hit),
+                                              hits.ctypes.data, diag, 512)
+        native.check(st, diag, "rp_cuda_trace_rays")
+        return hits
+
+    def raygen(self, request: RenderRequest):
+        q = request.to_c()
+        lanes = q.pixel_count * q.sample_count
+        words = np.zeros((lanes, 11), np.uint32)
+        rays = np.zeros((lanes, 6), np.float32)
+        diag = C.create_string_buffer(512)
+        st = native.lib().rp_cuda_probe_raygen(self._handle, C.byref(q), words.ctypes.data, rays.ctypes.data, lanes,
+                                                diag, 512)
+        native.check(st, diag, "rp_cuda_probe_raygen")
+        return words, rays
+
+
+def build_renderer(scene: scenes.Scene, device: int = 0) -> RenderBuildResult:
+    """build_metal_renderer (src/metal_render.hpp:84-95) for the CUDA backend."""
+    L = native.lib()
+    diag = C.create_string_buffer(1024)
+    info = abi.DeviceInfo()
+    st = L.rp_cuda_device_info(device, C.byref(info), diag, 1024)
+    if st != abi.RP_SUCCESS:
+        return RenderBuildResult(st, diag.value.decode(errors="replace"))
+    desc = scene.desc()
+    handle = C.c_void_p()
+    st = L.rp_cuda_scene_create(C.byref(desc), device, C.byref(handle), diag, 1024)
+    if st != abi.RP_SUCCESS:
+        return RenderBuildResult(st, diag.value.decode(errors="replace"), None, info)
+    return RenderBuildResult(st, "", CudaRenderScene(handle.value), info)
+
+
+def film_mean(film: np.ndarray) -> np.ndarray:
+    """Per-pixel XYZ mean, film_mean (src/packet_film.cpp:116-135) without splats or clamps."""
+    weight = film["weight_sum"] + film["weight_correction"]
+    xyz = film["sum"] + film["correction"]
+    return np.where(weight[:, None] > 0, xyz / np.where(weight > 0, weight, 1)[:, None], 0.0)
+
+
+def render_progressive(scene: scenes.Scene, settings: RenderSettings, device: int = 0):
+    """render_progressive (src/render_driver.cpp:287-316): build, then render every batch."""
+    built = build_renderer(scene, device)
+    if built.status != abi.RP_SUCCESS:
+        return built.status, built.diagnostic, None
+    st, diag, film = built.scene.render_film(settings)
+    built.scene.close()
+    return st, diag, film

@@ -75,6 +75,7 @@ class OracleScene:
         self.desc = scene.desc()
         diag = C.create_string_buffer(512)
         self.handle = oracle().or_scene_create(C.byref(self.desc), diag, 512)
+        self.handle = C.c_void_p(self.handle) if self.handle else None
         if not self.handle:
             raise RuntimeError(diag.value.decode())
 
