@@ -1,0 +1,316 @@
+#!/usr/bin/env python
+"""Benchmark of the spectral path-tracing hot path on B200.
+
+Workload: the mixed-material mesh scene (seeded displaced icosphere, subdivision 8, 64
+spheres of 2048 triangles and a ground plane: 1,441,794 triangles; 40% diffuse / 40% GGX
+conductor / 20% dielectric; 2 point + 2 spot lights and a constant environment) at
+1920x1080, 16 spp, depth 16, four hero wavelengths per sample, Sobol/Owen sampler, seed 1.
+
+One step renders all 16 spp of the 1080p film (33,177,600 samples) into the device FP64
+film.  ``value`` is Msamples/s with the scene resident; ``e2e`` is the same metric through the
+public API (build the scene from host arrays, render into a host film, read it back).
+
+``--impl reference`` times the reference's CPU path (the oracle restatement, all host
+threads) on bounded samples of the same workload.
+
+Multi-GPU (torchrun): every rank renders its own sample range of the same film (independent
+units, no data-path collective); ``value`` is all ranks' samples over the slowest rank's time.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "spectral path Msamples/s"
+UNIT = "Msamples/s"
+WORKLOAD = "mixed_material_1080p_16spp_depth16"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--width", type=int, default=1920)
+    p.add_argument("--height", type=int, default=1080)
+    p.add_argument("--spp", type=int, default=16)
+    p.add_argument("--depth", type=int, default=16)
+    p.add_argument("--subdivisions", type=int, default=8)
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def config(args, n):
+    return {"workload": WORKLOAD, "width": args.width, "height": args.height, "spp": args.spp,
+            "max_depth": args.depth, "triangles": None, "sampler": "sobol-owen", "seed": 1,
+            "hero_wavelengths": 4, "film": "fp64 device film, box filter",
+            "l2": "inputs larger than L2 (path-state pool and BVH exceed 126 MB) and a 256 MB L2 flush between steps",
+            "parallelism": f"replicas{n}" if n > 1 else "single"}
+
+
+class Clocks:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.stop_flag = threading.Event()
+        self.thread = threading.Thread(target=self.run, daemon=True)
+
+    def run(self):
+        while not self.stop_flag.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.rows.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self.stop_flag.wait(0.2)
+
+    def __enter__(self):
+        self.thread.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop_flag.set()
+        self.thread.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        peaks = json.load(open(path))
+        return float(peaks["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_ray():
+    """DRAM bytes per closest-hit ray of k_trace from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "k_trace_mixed.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_ray:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def cpu_baseline(orc, args, seconds, threads=0):
+    """The oracle (the reference's CPU path restated) on a bounded sample of the workload."""
+    from tests.oracle_lib import request
+
+    w, h = args.width, args.height
+    probe = min(w * h, 8192)
+    t0 = time.perf_counter()
+    orc.sample(request(w, h, 1, pixel_begin=(w * h - probe) // 2, pixel_count=probe), threads=threads)
+    rate = probe / max(time.perf_counter() - t0, 1e-6)
+    target = int(max(probe, rate * seconds))
+    if target < w * h:
+        spp, pixels, begin = 1, target, (w * h - target) // 2
+    else:
+        spp, pixels, begin = min(args.spp, max(1, target // (w * h))), w * h, 0
+    t0 = time.perf_counter()
+    out = orc.sample(request(w, h, spp, pixel_begin=begin, pixel_count=pixels), threads=threads)
+    dt = time.perf_counter() - t0
+    ok = int((out["status"] == 0).sum())
+    cores = threads if threads > 0 else (os.cpu_count() or 1)
+    return {"value": out.size / dt / 1e6, "unit": UNIT, "cores": cores, "kind": "port", "seconds": dt,
+            "sample": f"{out.size} lanes (pixels {begin}..{begin + pixels - 1} of the {w}x{h} film, absolute samples "
+                      f"0..{spp - 1}, depth {args.depth}), {dt:.2f} s, {ok} succeeded"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    from rypath_b200 import scenes
+
+    from tests.oracle_lib import OracleScene
+
+    scene = scenes.mixed_scene(args.width, args.height, args.spp, args.depth, subdivisions=args.subdivisions)
+    orc = OracleScene(scene)
+    for _ in range(args.warmup):
+        cpu_baseline(orc, args, 1.0)
+    values = [cpu_baseline(orc, args, args.cpu_seconds / max(args.steps, 1)) for _ in range(args.steps)]
+    value = statistics.median(v["value"] for v in values)
+    cfg = config(args, 1)
+    cfg["triangles"] = scene.triangle_count
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": statistics.median(v["seconds"] * 1e3 for v in values),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": cfg, "cpu_baseline": dict(values[-1], value=value),
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from rypath_b200 import abi, renderer, scenes
+
+    scene = scenes.mixed_scene(args.width, args.height, args.spp, args.depth, subdivisions=args.subdivisions)
+    pixels = args.width * args.height
+    settings = renderer.RenderSettings(args.width, args.height, samples=args.spp, batch_size=args.spp)
+    built = renderer.build_renderer(scene, device=local)
+    if built.status != abi.RP_SUCCESS:
+        raise SystemExit(f"build_renderer failed: {built.diagnostic}")
+    rs = built.scene
+    film = torch.zeros(pixels * 12, dtype=torch.float64, device="cuda")  # rp_film_pixel is 96 bytes
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    sample_base = rank * args.spp * (args.warmup + args.steps + 1)
+
+    # exact traversal counts for the roofline (an untimed counting render of the same workload)
+    rs.set_counting(True)
+    film.zero_()
+    rs.render_film_device(settings, film.data_ptr(), sample_begin=sample_base)
+    counts = rs.timing()
+    rs.set_counting(False)
+
+    for i in range(args.warmup):
+        film.zero_()
+        rs.render_film_device(settings, film.data_ptr(), sample_begin=sample_base + (i + 1) * args.spp)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    steps = []
+    with Clocks(local) as clocks:
+        for i in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            film.zero_()
+            rs.render_film_device(settings, film.data_ptr(),
+                                  sample_begin=sample_base + (args.warmup + 1 + i) * args.spp)
+            steps.append(rs.timing())
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    total_ms = sum(t.total_ms for t in steps)
+    samples = sum(t.samples for t in steps)
+    if dist:
+        v = torch.tensor([total_ms, float(samples)], dtype=torch.float64, device="cuda")
+        mx = v.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(v, op=dist.ReduceOp.SUM)
+        job_ms, job_samples = float(mx[0]), float(v[1])
+    else:
+        job_ms, job_samples = total_ms, float(samples)
+    value = job_samples / (job_ms / 1e3) / 1e6
+
+    # roofline of the dominant kernel: closest-hit traversal
+    trace_ms = sum(t.trace_ms for t in steps)
+    trace_launches = sum(t.trace_launches for t in steps)
+    rays = counts.closest_rays
+    node_bytes, tri_bytes = 64, 48
+    state_bytes = 4 + 16 + 32 + 16  # queue entry, flags, ray read, hit write
+    algo_per_ray = (counts.nodes_visited * node_bytes + counts.triangles_tested * tri_bytes) / max(
+        1, counts.closest_rays) + state_bytes
+    trace_bytes_per_step = algo_per_ray * rays
+    achieved = trace_bytes_per_step * len(steps) / (trace_ms / 1e3) / 1e9 if trace_ms > 0 else None
+    peak, peak_kind = measured_peaks()
+    tpr = traffic_per_ray()
+    shares = {k: sum(getattr(t, k + "_ms") for t in steps) / total_ms for k in ("trace", "shadow", "shade", "other")}
+
+    line = None
+    if rank == 0:
+        cfg = config(args, world)
+        cfg["triangles"] = scene.triangle_count
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": job_ms / len(steps), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+            "config": cfg,
+            "roofline": {"bound": "hbm", "kernel": "k_trace (closest-hit traversal)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None,
+                         "traffic": (tpr * rays / max(1, counts.trace_launches)) if tpr else None,
+                         "algorithmic_bytes_per_launch": trace_bytes_per_step / max(1, counts.trace_launches),
+                         "algorithmic_bytes_per_ray": algo_per_ray, "peak_kind": peak_kind,
+                         "avg_launch_ms": trace_ms / max(1, trace_launches)},
+            "kernel_share": shares,
+            "rays_per_step": {"closest": counts.closest_rays, "shadow": counts.shadow_rays},
+            "mrays_per_s": (counts.closest_rays + counts.shadow_rays) * len(steps) / (total_ms / 1e3) / 1e6,
+            "gpu_launches": int(sum(t.kernel_launches for t in steps)),
+            "clocks": clocks.summary(),
+        }
+    # end to end through the public API: build from host arrays, render into a host film
+    if not args.no_e2e:
+        desc_bytes = (scene.positions.nbytes + scene.triangles.nbytes + scene.knots.nbytes +
+                      len(scene.emissions) * 1888 + len(scene.positional) * 1948 + 234208 + 471 * 4)
+        film_bytes = pixels * 96
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        st, diag, host_film = renderer.render_progressive(scene, settings, device=local)
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if st != abi.RP_SUCCESS:
+            raise SystemExit(f"e2e render failed: {diag}")
+        if dist:
+            v = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+            dist.all_reduce(v, op=dist.ReduceOp.MAX)
+            e2e_s = float(v[0])
+        if line is not None:
+            line["e2e"] = {"value": pixels * args.spp * world / e2e_s / 1e6, "unit": UNIT,
+                           "h2d_bytes_per_step": desc_bytes + film_bytes, "d2h_bytes_per_step": film_bytes,
+                           "seconds": e2e_s, "includes": "scene upload, LBVH build, light tables, render, film readback"}
+    if line is not None and not args.no_cpu_baseline:
+        from tests.oracle_lib import OracleScene
+
+        line["cpu_baseline"] = cpu_baseline(OracleScene(scene), args, args.cpu_seconds)
+    rs.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -213,7 +213,9 @@ typedef struct rp_timing {
     double shade_ms;          /* shading kernels */
     double other_ms;          /* raygen, queue resets, film */
     uint64_t closest_rays, shadow_rays, kernel_launches, samples;
-    uint64_t nodes_visited, triangles_tested; /* only when counting is enabled */
+    uint64_t nodes_visited, triangles_tested; /* closest-hit rays; only when counting */
+    uint64_t trace_launches, shadow_launches, shade_launches, other_launches;
+    uint64_t shadow_nodes_visited, shadow_triangles_tested; /* any-hit rays; only when counting */
 } rp_timing;
 
 /* ---- device and lifetime ------------------------------------------------------------ */

@@ -131,7 +131,9 @@ class Timing(C.Structure):
     _fields_ = [("total_ms", f64), ("trace_ms", f64), ("shadow_ms", f64), ("shade_ms", f64),
                 ("other_ms", f64), ("closest_rays", u64), ("shadow_rays", u64),
                 ("kernel_launches", u64), ("samples", u64), ("nodes_visited", u64),
-                ("triangles_tested", u64)]
+                ("triangles_tested", u64), ("trace_launches", u64), ("shadow_launches", u64),
+                ("shade_launches", u64), ("other_launches", u64), ("shadow_nodes_visited", u64),
+                ("shadow_triangles_tested", u64)]
 
 
 # numpy dtypes with the same layouts, for bulk views of result buffers

@@ -372,11 +372,17 @@ struct rp_scene {
     void collect() {
         RP_CHECK(cudaStreamSynchronize(stream));
         double sums[4] = {0, 0, 0, 0};
+        uint64_t counts[4] = {0, 0, 0, 0};
         for (size_t i = 0; i < event_kind.size(); ++i) {
             float ms = 0;
             RP_CHECK(cudaEventElapsedTime(&ms, events[2 * i], events[2 * i + 1]));
             sums[event_kind[i]] += ms;
+            ++counts[event_kind[i]];
         }
+        timing.trace_launches = counts[0];
+        timing.shadow_launches = counts[1];
+        timing.shade_launches = counts[2];
+        timing.other_launches = counts[3];
         timing.trace_ms = sums[0];
         timing.shadow_ms = sums[1];
         timing.shade_ms = sums[2];
@@ -974,8 +980,8 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             const float g3 = 3.0f * u / (1.0f - 3.0f * u);
             ds.slab_scale = 1 + 2 * g3;
         }
-        s->stats = dalloc<unsigned long long>(own, 4);
-        RP_CHECK(cudaMemsetAsync(s->stats, 0, 4 * sizeof(unsigned long long), stm));
+        s->stats = dalloc<unsigned long long>(own, 8);
+        RP_CHECK(cudaMemsetAsync(s->stats, 0, 8 * sizeof(unsigned long long), stm));
         build_bvh(s);
         RP_CHECK(cudaStreamSynchronize(stm));
         *out = s;
@@ -1023,7 +1029,7 @@ static rp_status sample_impl(rp_scene *s, const rp_request *request, rp_packet_r
         }
         RP_CHECK(cudaEventRecord(start, s->stream));
         if (s->counting)
-            RP_CHECK(cudaMemsetAsync(s->stats, 0, 4 * sizeof(unsigned long long), s->stream));
+            RP_CHECK(cudaMemsetAsync(s->stats, 0, 8 * sizeof(unsigned long long), s->stream));
         run_wave(s, p);
         PacketResult *dst = reinterpret_cast<PacketResult *>(out);
         PacketResult *staging = nullptr;
@@ -1050,12 +1056,14 @@ static rp_status sample_impl(rp_scene *s, const rp_request *request, rp_packet_r
         s->timing.total_ms = total;
         s->timing.samples = p.lanes;
         if (s->counting) {
-            unsigned long long st[4];
+            unsigned long long st[6];
             RP_CHECK(cudaMemcpy(st, s->stats, sizeof(st), cudaMemcpyDeviceToHost));
             s->timing.nodes_visited = st[0];
             s->timing.triangles_tested = st[1];
             s->timing.closest_rays = st[2];
             s->timing.shadow_rays = st[3];
+            s->timing.shadow_nodes_visited = st[4];
+            s->timing.shadow_triangles_tested = st[5];
         }
         if (host) {
             for (u32 i = 0; i < p.lanes; ++i)
@@ -1123,7 +1131,7 @@ static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel 
         }
         rp_film_pixel *staged = s->film_stage;
         if (s->counting)
-            RP_CHECK(cudaMemsetAsync(s->stats, 0, 4 * sizeof(unsigned long long), s->stream));
+            RP_CHECK(cudaMemsetAsync(s->stats, 0, 8 * sizeof(unsigned long long), s->stream));
         u64 done = 0;
         u32 failed_batches = 0;
         while (done < r->sample_count) {
@@ -1182,12 +1190,14 @@ static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel 
         s->timing.total_ms = total;
         s->timing.samples = done * pixels;
         if (s->counting) {
-            unsigned long long st[4];
+            unsigned long long st[6];
             RP_CHECK(cudaMemcpy(st, s->stats, sizeof(st), cudaMemcpyDeviceToHost));
             s->timing.nodes_visited = st[0];
             s->timing.triangles_tested = st[1];
             s->timing.closest_rays = st[2];
             s->timing.shadow_rays = st[3];
+            s->timing.shadow_nodes_visited = st[4];
+            s->timing.shadow_triangles_tested = st[5];
         }
         if (failed_batches) {
             set_diag(diag, cap, "a render batch failed; the committed film is unchanged");

@@ -514,8 +514,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_shadow(const __grid_constant__ 
         }
     }
     if (Count) {
-        atomicAdd(pool.stats + 0, (unsigned long long)nodes);
-        atomicAdd(pool.stats + 1, (unsigned long long)tris);
+        atomicAdd(pool.stats + 4, (unsigned long long)nodes);
+        atomicAdd(pool.stats + 5, (unsigned long long)tris);
         atomicAdd(pool.stats + 3, (unsigned long long)rays);
     }
 }

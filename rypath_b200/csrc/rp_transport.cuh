@@ -48,7 +48,7 @@ struct PathPool {
     float4 *sh_d;  // shadow direction, path id bits
     float4 *sh_c;  // weighted contribution (NaN x: invalid if visible)
     // statistics (optional)
-    unsigned long long *stats; // [0] nodes visited, [1] triangles tested, [2] closest rays, [3] shadow rays
+    unsigned long long *stats; // closest [0] nodes, [1] triangles, [2] rays; shadow [3] rays, [4] nodes, [5] triangles
 };
 
 struct WaveParams {

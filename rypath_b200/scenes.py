@@ -397,7 +397,7 @@ def mixed_scene(width=1920, height=1080, spp=16, max_depth=16, seed=1, subdivisi
         _spot((0.0, 5.0, 0.5), (0.0, 0.0, 0.0), 25.0, 30.0, blackbody_intensity(6500, 120.0)),
         _spot((-2.0, 3.0, 4.0), (0.0, -0.5, 0.0), 15.0, 20.0, blackbody_intensity(4000, 80.0)),
     ]
-    scene.environment = (0.08 * blackbody_shape(9000) / blackbody_shape(9000).max()).astype(np.float32)
+    scene.environment = (0.03 * blackbody_shape(9000) / blackbody_shape(9000).max()).astype(np.float32)
     scene.camera = pinhole_camera((0.0, 1.2, 5.5), (0.0, -0.1, 0.0), (0, 1, 0), 38.0, width, height)
     return scene
 
