@@ -413,7 +413,9 @@ struct rp_scene {
         q.prev_e = dalloc<int4>(pool_owned, c);
         q.queue[0] = dalloc<u32>(pool_owned, c);
         q.queue[1] = dalloc<u32>(pool_owned, c);
-        q.counters = dalloc<u32>(pool_owned, 8);
+        q.counters = dalloc<u32>(pool_owned, 16);
+        q.bins = dalloc<u32>(pool_owned, 4 * c);
+        q.bin_capacity = lanes;
         q.stats = stats;
         capacity = lanes;
     }
@@ -467,7 +469,7 @@ void run_wave(rp_scene *s, const WaveParams &p) {
     PathPool &pool = s->pool;
     const int sms = s->sm_count;
     s->mark(3);
-    RP_CHECK(cudaMemsetAsync(pool.counters, 0, 8 * sizeof(u32), s->stream));
+    RP_CHECK(cudaMemsetAsync(pool.counters, 0, 16 * sizeof(u32), s->stream));
     k_raygen<<<grid_for(sms, p.lanes, 256, 16), 256, 0, s->stream>>>(s->ds, p, pool);
     RP_CHECK(cudaMemcpyAsync(pool.counters, &p.lanes, sizeof(u32), cudaMemcpyHostToDevice, s->stream));
     s->done();
@@ -475,6 +477,7 @@ void run_wave(rp_scene *s, const WaveParams &p) {
     const u32 events = s->ds.max_depth + 1;
     for (u32 e = 0; e < events; ++e) {
         s->mark(0);
+        RP_CHECK(cudaMemsetAsync(pool.counters + 4, 0, 4 * sizeof(u32), s->stream));
         if (s->counting)
             k_trace<true><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, 0, s->stream>>>(s->ds, pool, in);
         else
@@ -483,7 +486,10 @@ void run_wave(rp_scene *s, const WaveParams &p) {
         s->mark(2);
         RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), s->stream));
         RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), s->stream));
-        k_shade<<<grid_for(sms, p.lanes, 128, 16), 128, 0, s->stream>>>(s->ds, p, pool, in);
+        k_shade<0><<<grid_for(sms, p.lanes, 128, 16), 128, 0, s->stream>>>(s->ds, p, pool, in);
+        k_shade<1><<<grid_for(sms, p.lanes, 128, 16), 128, 0, s->stream>>>(s->ds, p, pool, in);
+        k_shade<2><<<grid_for(sms, p.lanes, 128, 16), 128, 0, s->stream>>>(s->ds, p, pool, in);
+        k_shade<3><<<grid_for(sms, p.lanes, 128, 16), 128, 0, s->stream>>>(s->ds, p, pool, in);
         s->done();
         s->mark(1);
         if (s->counting)
@@ -773,6 +779,10 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
         ds.instances = dupload(own, instances.data(), instances.size(), stm);
         ds.instance_count = d->instance_count;
         ds.tri_instance = dupload(own, tri_instance.data(), tri_instance.size(), stm);
+        std::vector<unsigned char> tri_family(tri_instance.size());
+        for (size_t t = 0; t < tri_instance.size(); ++t)
+            tri_family[t] = (unsigned char)d->materials[d->instances[tri_instance[t]].material].scattering;
+        ds.tri_family = dupload(own, tri_family.data(), tri_family.size(), stm);
         ds.tri_local = dupload(own, tri_local.data(), tri_local.size(), stm);
         ds.prim_count = u32(tri_instance.size());
         std::vector<DMaterial> mats(d->material_count);

@@ -48,23 +48,41 @@ __global__ void k_raygen(const __grid_constant__ DeviceScene s, const __grid_con
     }
 }
 
-// Closest-hit queries for the active queue.
+// Closest-hit queries for the active queue; each path is then appended to the bin of the
+// BSDF family it hit (0 diffuse, 1 conductor, 2 dielectric, 3 miss or failed query), so the
+// shade stage runs one specialised kernel per family ("material-sorted shading").
 template <bool Count>
 __global__ void __launch_bounds__(kTraceBlock) k_trace(const __grid_constant__ DeviceScene s, PathPool pool, int in) {
     __shared__ u32 stack[kStackDepth * kTraceBlock];
     const u32 count = pool.counters[in];
     const u32 *queue = pool.queue[in];
     u32 nodes = 0, tris = 0, rays = 0;
-    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        const u32 path = queue[i];
-        if (pool.ident[path].w & F_COMPLETE)
-            continue;
-        const float4 o = pool.ray_o[path], d = pool.ray_d[path];
-        Hit h;
-        const bool ok = trace_closest<Count>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), __int_as_float(0x7f800000), h,
-                                             stack + threadIdx.x, kTraceBlock, nodes, tris);
-        ++rays;
-        pool.hit[path] = make_float4(h.t, h.b1, h.b2, __uint_as_float(ok ? h.prim : 0xfffffffeu));
+    const u32 stride = gridDim.x * blockDim.x;
+    const u32 trips = (count + stride - 1) / stride;
+    const int lane = threadIdx.x & 31;
+    for (u32 trip = 0; trip < trips; ++trip) {
+        const u32 i = trip * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        u32 family = 4, path = 0;
+        if (i < count) {
+            path = queue[i];
+            if (!(pool.ident[path].w & F_COMPLETE)) {
+                const float4 o = pool.ray_o[path], d = pool.ray_d[path];
+                Hit h;
+                const bool ok = trace_closest<Count>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), __int_as_float(0x7f800000),
+                                                     h, stack + threadIdx.x, kTraceBlock, nodes, tris);
+                ++rays;
+                pool.hit[path] = make_float4(h.t, h.b1, h.b2, __uint_as_float(ok ? h.prim : 0xfffffffeu));
+                family = (!ok || h.prim == kNone) ? 3u : u32(__ldg(s.tri_family + h.prim));
+            }
+        }
+        const u32 peers = __match_any_sync(0xffffffffu, family);
+        const int leader = __ffs(peers) - 1;
+        u32 base = 0;
+        if (lane == leader && family < 4)
+            base = atomicAdd(pool.counters + 4 + family, __popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (family < 4)
+            pool.bins[size_t(family) * pool.bin_capacity + base + __popc(peers & ((1u << lane) - 1))] = path;
     }
     if (Count) {
         atomicAdd(pool.stats + 0, (unsigned long long)nodes);
@@ -73,11 +91,13 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(const __grid_constant__ D
     }
 }
 
-// One hero event after its closest hit (shaders/packet_pt_event_body.inc:11-461).
+// One hero event after its closest hit (shaders/packet_pt_event_body.inc:11-461), for the paths
+// whose hit is of BSDF family F (3: no surface -- environment or a failed query).
+template <int F>
 __global__ void __launch_bounds__(128) k_shade(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p,
                                                PathPool pool, int in) {
-    const u32 count = pool.counters[in];
-    const u32 *queue = pool.queue[in];
+    const u32 count = pool.counters[4 + F];
+    const u32 *queue = pool.bins + size_t(F) * pool.bin_capacity;
     u32 *out_queue = pool.queue[in ^ 1];
     u32 *out_count = pool.counters + (in ^ 1);
     const u32 capacity = s.max_depth + 2;
@@ -152,100 +172,105 @@ __global__ void __launch_bounds__(128) k_shade(const __grid_constant__ DeviceSce
                         ++cnt;
                         break;
                     }
-                    const float t = hit.x, b1 = hit.y, b2 = hit.z;
-                    if (!isfinite(t) || t < 0 || !isfinite(b1) || !isfinite(b2) || prim >= s.prim_count) {
-                        status = 3;
+                    if constexpr (F == 3) {
+                        status = 3; // a surface hit never reaches the no-surface bin
                         break;
-                    }
-                    cinst = s.tri_instance[prim];
-                    clocal = s.tri_local[prim];
-                    const DInstance &instance = s.instances[cinst];
-                    if (instance.material >= s.material_count) {
-                        status = 3;
-                        break;
-                    }
-                    ctype = kSurface;
-                    clight = instance.emission == kNone ? kNone : instance.emitter_begin + clocal;
-                    cwo = -rd;
-                    if (!triangle_surface_point(s, cinst, clocal, b1, b2, true, cp)) {
-                        status = 2;
-                        break;
-                    }
-                    const DMaterial material = s.materials[instance.material];
-                    if (!shading_frame(cp.shading_normal, cframe) ||
-                        !prepare_bsdf(s, material, lambda, active_mask, cbsdf)) {
-                        status = 2;
-                        break;
-                    }
-                    const V3 ray_position = fma3(v3(t, t, t), rd, ro);
-                    const V3 ray_error = gamma_bound(2) * (vabs(t * rd) + vabs(ro));
-                    cp.error = cp.error + (vabs(cp.position - ray_position) + ray_error);
-                    if (!finite3(cp.error)) {
-                        status = 2;
-                        break;
-                    }
-                    cbeta = beta;
-                    connectible = hero_connectible(cbsdf);
-                    ++cnt;
-                    if (cnt == capacity)
-                        break;
-                    if (cnt - 2 >= p.emergency_limit) {
-                        status = 1;
-                        break;
-                    }
-                    const uint4 draws = draw_words(s, p, ident.x, ident.y, ident.z, index, 4 + cnt - 2);
-                    swo = to_local(cframe, cwo);
-                    cbsdf.active_mask = active_mask;
-                    direct_density = density;
-                    direct_allowed = hero_continue(beta, eta_scale, roulette, cnt - 1, sample_uniform(p, draws.w));
-                    direct_beta = beta;
-                    connectible = hero_connectible(cbsdf);
-                    if (!direct_allowed)
-                        break;
-                    const HeroSample proposed = hero_sample(cbsdf, swo, sample_uniform(p, draws.x),
-                                                            sample_uniform(p, draws.y), sample_uniform(p, draws.z));
-                    bool cont_valid = proposed.valid;
-                    if (proposed.valid && proposed.accepted) {
-                        hero_previous = direct_density;
-                        const Update adv = advance(direct_density, beta, proposed.numerator, proposed.pdf);
-                        cont_valid = adv.valid;
-                        if (adv.valid) {
-                            beta = adv.beta;
-                            density = adv.density;
+                    } else {
+                        const float t = hit.x, b1 = hit.y, b2 = hit.z;
+                        if (!isfinite(t) || t < 0 || !isfinite(b1) || !isfinite(b2) || prim >= s.prim_count) {
+                            status = 3;
+                            break;
                         }
-                        hero_account_eta(eta_scale, roulette, proposed.eta, proposed.transmission);
-                        active_mask = 1;
-#pragma unroll
-                        for (int k = 1; k < 4; ++k)
-                            if (density.lane[k].fraction > 0 || (fbits(beta.v[k]) & 0x7fffffffu))
-                                active_mask |= 1u << k;
+                        cinst = s.tri_instance[prim];
+                        clocal = s.tri_local[prim];
+                        const DInstance &instance = s.instances[cinst];
+                        if (instance.material >= s.material_count) {
+                            status = 3;
+                            break;
+                        }
+                        ctype = kSurface;
+                        clight = instance.emission == kNone ? kNone : instance.emitter_begin + clocal;
+                        cwo = -rd;
+                        if (!triangle_surface_point(s, cinst, clocal, b1, b2, true, cp)) {
+                            status = 2;
+                            break;
+                        }
+                        const DMaterial material = s.materials[instance.material];
+                        if (!shading_frame(cp.shading_normal, cframe) ||
+                            !prepare_bsdf<F>(s, material, lambda, active_mask, cbsdf)) {
+                            status = 2;
+                            break;
+                        }
+                        const V3 ray_position = fma3(v3(t, t, t), rd, ro);
+                        const V3 ray_error = gamma_bound(2) * (vabs(t * rd) + vabs(ro));
+                        cp.error = cp.error + (vabs(cp.position - ray_position) + ray_error);
+                        if (!finite3(cp.error)) {
+                            status = 2;
+                            break;
+                        }
+                        cbeta = beta;
+                        connectible = hero_connectible(cbsdf);
+                        ++cnt;
+                        if (cnt == capacity)
+                            break;
+                        if (cnt - 2 >= p.emergency_limit) {
+                            status = 1;
+                            break;
+                        }
+                        const uint4 draws = draw_words(s, p, ident.x, ident.y, ident.z, index, 4 + cnt - 2);
+                        swo = to_local(cframe, cwo);
+                        cbsdf.active_mask = active_mask;
+                        direct_density = density;
+                        direct_allowed = hero_continue(beta, eta_scale, roulette, cnt - 1, sample_uniform(p, draws.w));
+                        direct_beta = beta;
+                        connectible = hero_connectible(cbsdf);
+                        if (!direct_allowed)
+                            break;
+                        const HeroSample proposed = hero_sample_k<F>(cbsdf, swo, sample_uniform(p, draws.x),
+                                                                sample_uniform(p, draws.y), sample_uniform(p, draws.z));
+                        bool cont_valid = proposed.valid;
+                        if (proposed.valid && proposed.accepted) {
+                            hero_previous = direct_density;
+                            const Update adv = advance(direct_density, beta, proposed.numerator, proposed.pdf);
+                            cont_valid = adv.valid;
+                            if (adv.valid) {
+                                beta = adv.beta;
+                                density = adv.density;
+                            }
+                            hero_account_eta(eta_scale, roulette, proposed.eta, proposed.transmission);
+                            active_mask = 1;
+    #pragma unroll
+                            for (int k = 1; k < 4; ++k)
+                                if (density.lane[k].fraction > 0 || (fbits(beta.v[k]) & 0x7fffffffu))
+                                    active_mask |= 1u << k;
+                        }
+                        if (!cont_valid) {
+                            status = 2;
+                            break;
+                        }
+                        if (!proposed.accepted)
+                            break;
+                        pair_valid = true;
+                        V3 wi = to_world(cframe, proposed.wi);
+                        if (!unit_vector(wi, wi)) {
+                            status = 2;
+                            break;
+                        }
+                        if (!finite_nonnegative4(beta)) {
+                            status = 2;
+                            break;
+                        }
+                        if (proposed.delta)
+                            cdelta = true;
+                        const V3 origin = offset_point(cp.position, cp.error, cp.geometric_normal, wi);
+                        if (!finite3(origin)) {
+                            status = 2;
+                            break;
+                        }
+                        ro = origin;
+                        rd = wi;
+                        terminated = false;
                     }
-                    if (!cont_valid) {
-                        status = 2;
-                        break;
-                    }
-                    if (!proposed.accepted)
-                        break;
-                    pair_valid = true;
-                    V3 wi = to_world(cframe, proposed.wi);
-                    if (!unit_vector(wi, wi)) {
-                        status = 2;
-                        break;
-                    }
-                    if (!finite_nonnegative4(beta)) {
-                        status = 2;
-                        break;
-                    }
-                    if (proposed.delta)
-                        cdelta = true;
-                    const V3 origin = offset_point(cp.position, cp.error, cp.geometric_normal, wi);
-                    if (!finite3(origin)) {
-                        status = 2;
-                        break;
-                    }
-                    ro = origin;
-                    rd = wi;
-                    terminated = false;
                 } while (false);
                 bool complete = terminated || status != 0 || cnt >= capacity || !nonzero4(beta);
                 // latest vertex (the previous event's) for MIS
@@ -296,7 +321,7 @@ __global__ void __launch_bounds__(128) k_shade(const __grid_constant__ DeviceSce
                             latest.k = from_float4(pool.latest_k[path]);
                             const float4 pre = pool.preceding[path];
                             bool ok;
-                            const V4 bsdf_pdf = represented_pdf(latest_bsdf(latest), latest.shading_normal, latest.position,
+                            const V4 bsdf_pdf = represented_pdf<-1>(latest_bsdf(latest), latest.shading_normal, latest.position,
                                                                 v3(pre.x, pre.y, pre.z), ctype == kEnvironment,
                                                                 ctype == kEnvironment ? rd : cp.position, ok);
                             // hero_history_light_pdf / direct_pdf (shaders/packet_transport.h:740-758)
@@ -318,7 +343,7 @@ __global__ void __launch_bounds__(128) k_shade(const __grid_constant__ DeviceSce
                     radiance = add4(radiance, endpoint);
                     // hero_direct (shaders/hero_pt_helpers.h:185-221): sample, evaluate, weight;
                     // visibility is resolved by the shadow kernel.
-                    if (status == 0 && cnt < capacity && direct_allowed && ctype == kSurface && connectible) {
+                    if (F != 3 && status == 0 && cnt < capacity && direct_allowed && ctype == kSurface && connectible) {
                         const uint4 w = draw_words(s, p, ident.x, ident.y, ident.z, index, 133 + cnt - 2);
                         const float u0 = sample_uniform(p, w.x), u1 = sample_uniform(p, w.y), u2 = sample_uniform(p, w.z);
                         // sample_li (shaders/packet_transport.h:470-553)
@@ -384,8 +409,8 @@ __global__ void __launch_bounds__(128) k_shade(const __grid_constant__ DeviceSce
                         if (!li_ok || !isfinite(spdf) || spdf < 0) {
                             status = 2;
                         } else if (spdf > 0 && nonzero4(lbeta)) {
-                            const HeroEval e = hero_evaluate(cbsdf, pair_valid ? swo : to_local(cframe, cwo),
-                                                             to_local(cframe, direction));
+                            const HeroEval e = hero_evaluate_k<F == 3 ? 0 : F>(
+                                cbsdf, pair_valid ? swo : to_local(cframe, cwo), to_local(cframe, direction));
                             if (!e.valid) {
                                 status = 2;
                             } else {
@@ -401,8 +426,8 @@ __global__ void __launch_bounds__(128) k_shade(const __grid_constant__ DeviceSce
                                                 ? sel_pmf * light_geometry_pdf(s, sel, cp.position, cp.shading_normal, lp)
                                                 : 0.0f;
                                         bool ok;
-                                        const V4 bsdf_pdf = represented_pdf(cbsdf, cp.shading_normal, cp.position,
-                                                                            latest.position, false, lp.position, ok);
+                                        const V4 bsdf_pdf = represented_pdf<F == 3 ? 0 : F>(
+                                            cbsdf, cp.shading_normal, cp.position, latest.position, false, lp.position, ok);
                                         weight_ok = ok && hero_weight(direct_density, value, v4(lpdf), bsdf_pdf, contribution);
                                     }
                                     // visible(): offset both endpoints (shaders/packet_transport.h:377-446)

@@ -880,33 +880,49 @@ RP_DEV bool hero_connectible(const HeroBsdf &p) {
             return true;
     return false;
 }
-RP_DEV Eval lane_evaluate(const HeroBsdf &p, int k, V3 wo, V3 wi) {
-    if (p.kind == 0)
+// One wavelength of a family-K BSDF; a dielectric lane with eta == 1 is smooth, as
+// rypath_dielectric::prepare makes it (shaders/dielectric.h:19).
+template <int K> RP_DEV Eval lane_evaluate_k(const HeroBsdf &p, int k, V3 wo, V3 wi) {
+    if constexpr (K == 0) {
         return diffuse_evaluate(p.param[k], wo, wi);
-    if (p.kind == 1)
+    } else if constexpr (K == 1) {
         return conductor_evaluate(p.param[k], p.k[k], p.g, wo, wi);
-    Ggx g = p.g;
-    if (p.param[k] == 1)
-        g.smooth = true;
-    return dielectric_evaluate(p.param[k], g, wo, wi);
+    } else {
+        Ggx g = p.g;
+        if (p.param[k] == 1)
+            g.smooth = true;
+        return dielectric_evaluate(p.param[k], g, wo, wi);
+    }
+}
+template <int K> RP_DEV BSample lane_sample_k(const HeroBsdf &p, int k, V3 wo, float uc, float ux, float uy, float &eta) {
+    eta = 1;
+    if constexpr (K == 0) {
+        return diffuse_reflection_sample(p.param[k], wo, uc, ux, uy);
+    } else if constexpr (K == 1) {
+        return conductor_sample(p.param[k], p.k[k], p.g, wo, ux, uy);
+    } else {
+        Ggx g = p.g;
+        if (p.param[k] == 1)
+            g.smooth = true;
+        return dielectric_sample(p.param[k], g, wo, uc, ux, uy, eta);
+    }
+}
+RP_DEV Eval lane_evaluate(const HeroBsdf &p, int k, V3 wo, V3 wi) {
+    return p.kind == 0 ? lane_evaluate_k<0>(p, k, wo, wi)
+                       : (p.kind == 1 ? lane_evaluate_k<1>(p, k, wo, wi) : lane_evaluate_k<2>(p, k, wo, wi));
 }
 RP_DEV BSample lane_sample(const HeroBsdf &p, int k, V3 wo, float uc, float ux, float uy, float &eta) {
-    eta = 1;
-    if (p.kind == 0)
-        return diffuse_reflection_sample(p.param[k], wo, uc, ux, uy);
-    if (p.kind == 1)
-        return conductor_sample(p.param[k], p.k[k], p.g, wo, ux, uy);
-    Ggx g = p.g;
-    if (p.param[k] == 1)
-        g.smooth = true;
-    return dielectric_sample(p.param[k], g, wo, uc, ux, uy, eta);
+    return p.kind == 0 ? lane_sample_k<0>(p, k, wo, uc, ux, uy, eta)
+                       : (p.kind == 1 ? lane_sample_k<1>(p, k, wo, uc, ux, uy, eta)
+                                      : lane_sample_k<2>(p, k, wo, uc, ux, uy, eta));
 }
 struct HeroEval {
     V4 f, pdf;
     bool valid;
 };
-// shaders/hero_frozen_bsdf.h:167-250 (radiance mode)
-RP_DEV HeroEval hero_evaluate(const HeroBsdf &p, V3 wo, V3 wi) {
+// shaders/hero_frozen_bsdf.h:167-250 (radiance mode) for family K; out of line so every
+// caller in a kernel shares one copy.
+template <int K> __device__ __noinline__ HeroEval hero_evaluate_k(const HeroBsdf &p, V3 wo, V3 wi) {
     HeroEval out{v4(0), v4(0), false};
     if (!(p.active_mask & 1u) || (p.active_mask & ~15u) || !finite3(wo) || !finite3(wi))
         return out;
@@ -915,7 +931,7 @@ RP_DEV HeroEval hero_evaluate(const HeroBsdf &p, V3 wo, V3 wi) {
     for (int k = 0; k < 4; ++k) {
         if (!(p.active_mask & (1u << k)))
             continue;
-        const Eval e = lane_evaluate(p, k, wo, wi);
+        const Eval e = lane_evaluate_k<K>(p, k, wo, wi);
         out.f.v[k] = e.f;
         out.pdf.v[k] = e.pdf;
         out.valid = out.valid && e.valid;
@@ -923,6 +939,14 @@ RP_DEV HeroEval hero_evaluate(const HeroBsdf &p, V3 wo, V3 wi) {
     if (!finite_nonnegative4(out.f) || !finite_nonnegative4(out.pdf))
         out.valid = false;
     return out;
+}
+// Any family, dispatched at run time (the latest vertex of a path can be of any family).
+__device__ __noinline__ HeroEval hero_evaluate(const HeroBsdf &p, V3 wo, V3 wi) {
+    if (p.kind == 0)
+        return hero_evaluate_k<0>(p, wo, wi);
+    if (p.kind == 1)
+        return hero_evaluate_k<1>(p, wo, wi);
+    return hero_evaluate_k<2>(p, wo, wi);
 }
 // shaders/hero_scattering.h:55-66
 RP_DEV float event_eta(const HeroBsdf &p, int k, V3 wo, V3 wi) {
@@ -975,7 +999,7 @@ struct HeroSample {
     bool delta, transmission, accepted, valid;
 };
 // shaders/hero_current_bsdf.h:121-203 (hero_current_sample)
-RP_DEV HeroSample hero_sample(const HeroBsdf &p, V3 wo, float uc, float ux, float uy) {
+template <int K> RP_DEV HeroSample hero_sample_k(const HeroBsdf &p, V3 wo, float uc, float ux, float uy) {
     HeroSample out;
     out.wi = v3(0, 0, 0);
     out.numerator = v4(0);
@@ -985,7 +1009,7 @@ RP_DEV HeroSample hero_sample(const HeroBsdf &p, V3 wo, float uc, float ux, floa
     if (!(p.active_mask & 1u) || (p.active_mask & ~15u) || p.kind > 2 || !finite3(wo) || !randoms(uc, ux, uy))
         return out;
     float hero_eta;
-    const BSample hero = lane_sample(p, 0, wo, uc, ux, uy, hero_eta);
+    const BSample hero = lane_sample_k<K>(p, 0, wo, uc, ux, uy, hero_eta);
     out.valid = hero.valid;
     out.wi = hero.wi;
     out.delta = hero.delta;
@@ -998,7 +1022,7 @@ RP_DEV HeroSample hero_sample(const HeroBsdf &p, V3 wo, float uc, float ux, floa
     }
     if (hero.pdf == 0 || wo.z == 0 || hero.wi.z == 0)
         return out;
-    if (out.delta) {
+    if (K != 0 && out.delta) {
 #pragma unroll
         for (int k = 0; k < 4; ++k)
             if (p.active_mask & (1u << k)) {
@@ -1009,7 +1033,7 @@ RP_DEV HeroSample hero_sample(const HeroBsdf &p, V3 wo, float uc, float ux, floa
                 out.eta.v[k] = eta;
             }
     } else {
-        const HeroEval e = hero_evaluate(p, wo, hero.wi);
+        const HeroEval e = hero_evaluate_k<K>(p, wo, hero.wi);
         out.numerator = scale4(e.f, fabsf(hero.wi.z));
         out.pdf = e.pdf;
         out.valid = e.valid;

@@ -62,6 +62,7 @@ struct DeviceScene {
     u32 prim_count;
     const BNode *nodes;
     const float4 *leaf_v; // 3 per leaf slot: world v0 (w = prim id bits), v1, v2
+    const unsigned char *tri_family; // BSDF family of each triangle's material
     const DMaterial *materials;
     u32 material_count;
     const float2 *knots;
@@ -110,7 +111,7 @@ RP_DEV float triangle_extent(V3 e1, V3 e2) {
     return fmaxf(fmaxf(fmaxf(a.x, fmaxf(b.x, c.x)), fmaxf(a.y, fmaxf(b.y, c.y))), fmaxf(a.z, fmaxf(b.z, c.z)));
 }
 // shaders/render.metal:885-968 (triangle_surface_point)
-RP_DEV bool triangle_surface_point(const DeviceScene &s, u32 instance, u32 local, float u, float v, bool native_hit,
+__device__ __noinline__ bool triangle_surface_point(const DeviceScene &s, u32 instance, u32 local, float u, float v, bool native_hit,
                                    SurfacePoint &point) {
     const DInstance &in = s.instances[instance];
     const u32 *tri = s.triangles + 3 * (in.triangle_begin + local);
@@ -201,7 +202,7 @@ struct Selected {
     float pmf;
 };
 // :43-95
-RP_DEV Selected light_sample(const DeviceScene &s, V3 position, V3 normal, float u) {
+__device__ __noinline__ Selected light_sample(const DeviceScene &s, V3 position, V3 normal, float u) {
     const u32 count = s.light_count;
     if (!count)
         return {kNone, 0};
@@ -252,7 +253,7 @@ RP_DEV Selected light_sample(const DeviceScene &s, V3 position, V3 normal, float
     return {kNone, 0};
 }
 // :96-126
-RP_DEV float light_pmf(const DeviceScene &s, V3 position, V3 normal, u32 id) {
+__device__ __noinline__ float light_pmf(const DeviceScene &s, V3 position, V3 normal, u32 id) {
     if (id >= s.light_count)
         return 0;
     if (s.light_sampler == 2)
@@ -400,7 +401,7 @@ RP_DEV float area_solid_angle_pdf(float area_density, V3 reference, const Surfac
     return cosine > 0 ? area_density * d2 / cosine : 0;
 }
 // shaders/light_geometry_sampling.h:116-153 (triangles)
-RP_DEV float light_geometry_pdf(const DeviceScene &s, u32 emitter, V3 reference, V3 normal, const SurfacePoint &point) {
+__device__ __noinline__ float light_geometry_pdf(const DeviceScene &s, u32 emitter, V3 reference, V3 normal, const SurfacePoint &point) {
     const V3 delta = point.position - reference;
     if (!(dot(delta, delta) > 0) || !(point.inverse_area_pdf > 0))
         return 0;
@@ -417,7 +418,7 @@ RP_DEV float light_geometry_pdf(const DeviceScene &s, u32 emitter, V3 reference,
     return area_solid_angle_pdf(1 / point.inverse_area_pdf, reference, point);
 }
 // shaders/light_geometry_sampling.h:155-209 (triangles)
-RP_DEV bool light_geometry_sample(const DeviceScene &s, u32 emitter, V3 reference, V3 normal, float ux, float uy,
+__device__ __noinline__ bool light_geometry_sample(const DeviceScene &s, u32 emitter, V3 reference, V3 normal, float ux, float uy,
                                   SurfacePoint &point, float &pdf) {
     if (!isfinite(ux) || !isfinite(uy) || ux < 0 || uy < 0 || ux > 1 || uy > 1)
         return false;

@@ -43,7 +43,9 @@ struct PathPool {
     float4 *hit;           // t, b1, b2, primitive bits
     // queues
     u32 *queue[2];
-    u32 *counters; // [0] queue0, [1] queue1, [2] shadow, [3] failures
+    u32 *counters; // [0] queue0, [1] queue1, [2] shadow, [3] failures, [4..7] family bins
+    u32 *bins;     // 4 family bins of bin_capacity path ids each
+    u32 bin_capacity;
     float4 *sh_o;  // shadow origin, tmax
     float4 *sh_d;  // shadow direction, path id bits
     float4 *sh_c;  // weighted contribution (NaN x: invalid if visible)
@@ -59,15 +61,16 @@ struct WaveParams {
 
 RP_DEV float sample_uniform(const WaveParams &p, u32 w) { return p.sampler == 0 ? u01(w) : sobol_uniform(w); }
 
-// shaders/render.metal:154-179 (independent and Sobol samplers)
-RP_DEV uint4 draw_words(const DeviceScene &s, const WaveParams &p, u32 pixel, u32 slo, u32 shi, u64 index, u32 block) {
+// shaders/render.metal:154-179 (independent and Sobol samplers); out of line, one copy per kernel
+__device__ __noinline__ uint4 draw_words(const DeviceScene &s, const WaveParams &p, u32 pixel, u32 slo, u32 shi,
+                                         u64 index, u32 block) {
     if (p.sampler == 0)
         return philox(make_uint4(pixel, slo, shi, block), p.seed_low, p.seed_high);
-    const u32 d = 4 * block;
-    return make_uint4(sobol_word(s.sobol, index, d, p.randomization, p.seed_low),
-                      sobol_word(s.sobol, index, d + 1, p.randomization, p.seed_low),
-                      sobol_word(s.sobol, index, d + 2, p.randomization, p.seed_low),
-                      sobol_word(s.sobol, index, d + 3, p.randomization, p.seed_low));
+    u32 w[4];
+#pragma unroll 1
+    for (u32 k = 0; k < 4; ++k)
+        w[k] = sobol_word(s.sobol, index, 4 * block + k, p.randomization, p.seed_low);
+    return make_uint4(w[0], w[1], w[2], w[3]);
 }
 
 struct BeginSample {
@@ -153,7 +156,10 @@ RP_DEV bool material_reflectance(const DeviceScene &s, const DMaterial &m, float
     return isfinite(rho) && rho >= 0 && rho <= 1;
 }
 // shaders/hero_current_bsdf.h:72-101 with prepare_scattering (shaders/render.metal:2079-2160)
+template <int K>
 RP_DEV bool prepare_bsdf(const DeviceScene &s, const DMaterial &m, V4 lambda, u32 mask, HeroBsdf &out) {
+    if (m.scattering != u32(K))
+        return false;
     out.kind = m.scattering;
     out.active_mask = mask;
     out.g = {0, 0, true};
@@ -177,7 +183,7 @@ RP_DEV bool prepare_bsdf(const DeviceScene &s, const DMaterial &m, V4 lambda, u3
         float rho;
         if (!material_reflectance(s, m, lambda.v[k], rho))
             return false;
-        if (m.scattering == 0) {
+        if constexpr (K == 0) {
             out.param[k] = rho;
             continue;
         }
@@ -185,7 +191,7 @@ RP_DEV bool prepare_bsdf(const DeviceScene &s, const DMaterial &m, V4 lambda, u3
                                         lambda.v[k]);
         const float kk = optical_value(s.knots, m.k_begin, m.k_count, s.knot_count, (m.optical_extensions & 2u) != 0,
                                        lambda.v[k]);
-        if (m.scattering == 1) {
+        if constexpr (K == 1) {
             // shaders/conductor.h:22-25
             if (!isfinite(eta) || !isfinite(kk) || eta < 0 || kk < 0 || (eta == 0 && kk == 0))
                 return false;
@@ -223,6 +229,8 @@ RP_DEV HeroBsdf latest_bsdf(const Latest &l) {
 }
 // shaders/hero_pt_helpers.h:122-132 (hero_represented_pdf) for a surface vertex v with
 // finite neighbours (the neighbour after v may be at infinity: pass its direction).
+// K selects the BSDF family at compile time; -1 dispatches on the stored family.
+template <int K>
 RP_DEV V4 represented_pdf(const HeroBsdf &b, V3 shading_normal, V3 position, V3 before, bool after_infinite,
                           V3 after_point, bool &ok) {
     ok = true;
@@ -235,7 +243,11 @@ RP_DEV V4 represented_pdf(const HeroBsdf &b, V3 shading_normal, V3 position, V3 
         ok = false;
         return v4(0);
     }
-    const HeroEval e = hero_evaluate(b, to_local(f, normalize3(wb)), to_local(f, normalize3(wa)));
+    HeroEval e;
+    if constexpr (K < 0)
+        e = hero_evaluate(b, to_local(f, normalize3(wb)), to_local(f, normalize3(wa)));
+    else
+        e = hero_evaluate_k<K>(b, to_local(f, normalize3(wb)), to_local(f, normalize3(wa)));
     if (!e.valid) {
         ok = false;
         return v4(0);
