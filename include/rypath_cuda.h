@@ -216,6 +216,7 @@ typedef struct rp_timing {
     uint64_t nodes_visited, triangles_tested; /* closest-hit rays; only when counting */
     uint64_t trace_launches, shadow_launches, shade_launches, other_launches;
     uint64_t shadow_nodes_visited, shadow_triangles_tested; /* any-hit rays; only when counting */
+    double build_ms, build_host_ms, build_bvh_ms; /* scene creation: total, host preparation, LBVH */
 } rp_timing;
 
 /* ---- device and lifetime ------------------------------------------------------------ */

@@ -133,7 +133,8 @@ class Timing(C.Structure):
                 ("kernel_launches", u64), ("samples", u64), ("nodes_visited", u64),
                 ("triangles_tested", u64), ("trace_launches", u64), ("shadow_launches", u64),
                 ("shade_launches", u64), ("other_launches", u64), ("shadow_nodes_visited", u64),
-                ("shadow_triangles_tested", u64)]
+                ("shadow_triangles_tested", u64), ("build_ms", f64), ("build_host_ms", f64),
+                ("build_bvh_ms", f64)]
 
 
 # numpy dtypes with the same layouts, for bulk views of result buffers

@@ -6,6 +6,7 @@
 #include "rp_probes.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cfloat>
 #include <cstdarg>
@@ -292,14 +293,26 @@ double light_spectrum_power(const float *spectrum) {
 }
 
 // ---------------------------------------------------------------- device buffers
-template <class T> T *dalloc(std::vector<void *> &owned, size_t count) {
+// Device memory comes from the device's stream-ordered pool, configured to keep freed memory
+// for reuse by the next scene or pool in this process (no trip to the driver per render job).
+void retain_pool(int device) {
+    static bool configured[64] = {};
+    if (device >= 0 && device < 64 && !configured[device]) {
+        cudaMemPool_t pool;
+        RP_CHECK(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t threshold = UINT64_MAX;
+        RP_CHECK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+        configured[device] = true;
+    }
+}
+template <class T> T *dalloc(std::vector<void *> &owned, size_t count, cudaStream_t st = nullptr) {
     void *p = nullptr;
-    RP_CHECK(cudaMalloc(&p, std::max<size_t>(1, count) * sizeof(T)));
+    RP_CHECK(cudaMallocAsync(&p, std::max<size_t>(1, count) * sizeof(T), st));
     owned.push_back(p);
     return static_cast<T *>(p);
 }
 template <class T> T *dupload(std::vector<void *> &owned, const T *src, size_t count, cudaStream_t st) {
-    T *p = dalloc<T>(owned, count);
+    T *p = dalloc<T>(owned, count, st);
     if (count)
         RP_CHECK(cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyHostToDevice, st));
     return p;
@@ -341,12 +354,14 @@ struct rp_scene {
     ~rp_scene() {
         if (device >= 0)
             cudaSetDevice(device);
+        for (void *p : pool_owned)
+            cudaFreeAsync(p, stream);
+        for (void *p : owned)
+            cudaFreeAsync(p, stream);
+        if (film_stage)
+            cudaFreeAsync(film_stage, stream);
         if (stream)
             cudaStreamSynchronize(stream);
-        for (void *p : pool_owned)
-            cudaFree(p);
-        for (void *p : owned)
-            cudaFree(p);
         for (auto e : events)
             cudaEventDestroy(e);
         if (stream)
@@ -354,7 +369,9 @@ struct rp_scene {
     }
 
     // timing: pairs of events around launches, grouped by kind (0 trace, 1 shadow, 2 shade, 3 other)
-    void mark(int kind) {
+    uint64_t launches = 0;
+    void mark(int kind, int kernels = 1) {
+        launches += kernels;
         if (event_cursor + 2 > events.size()) {
             for (int k = 0; k < 64; ++k) {
                 cudaEvent_t e;
@@ -387,7 +404,8 @@ struct rp_scene {
         timing.shadow_ms = sums[1];
         timing.shade_ms = sums[2];
         timing.other_ms = sums[3];
-        timing.kernel_launches = event_kind.size();
+        timing.kernel_launches = launches;
+        launches = 0;
         event_kind.clear();
         event_cursor = 0;
     }
@@ -395,26 +413,35 @@ struct rp_scene {
     void ensure_pool(u32 lanes) {
         if (lanes <= capacity)
             return;
-        RP_CHECK(cudaStreamSynchronize(stream));
         for (void *p : pool_owned)
-            cudaFree(p);
+            cudaFreeAsync(p, stream);
         pool_owned.clear();
         capacity = 0;
+        // one allocation carved into the SoA arrays (256-byte aligned slices)
         const size_t c = lanes;
+        const size_t v16 = (c * 16 + 255) & ~size_t(255), v4 = (c * 4 + 255) & ~size_t(255);
+        const size_t bytes = 22 * v16 + 6 * v4 + 256;
+        unsigned char *base = dalloc<unsigned char>(pool_owned, bytes, stream);
+        size_t off = 0;
+        auto take = [&](size_t n) {
+            unsigned char *p = base + off;
+            off += n;
+            return p;
+        };
         PathPool &q = pool;
-        q.ident = dalloc<uint4>(pool_owned, c);
-        q.cursor = dalloc<uint4>(pool_owned, c);
+        q.ident = reinterpret_cast<uint4 *>(take(v16));
+        q.cursor = reinterpret_cast<uint4 *>(take(v16));
         float4 **f4[] = {&q.lambda, &q.lambda_pdf, &q.beta, &q.radiance, &q.dens_f, &q.prev_f, &q.eta_scale, &q.ray_o,
                          &q.ray_d, &q.latest_p, &q.latest_n, &q.latest_param, &q.latest_k, &q.preceding, &q.hit,
                          &q.sh_o, &q.sh_d, &q.sh_c};
         for (auto p : f4)
-            *p = dalloc<float4>(pool_owned, c);
-        q.dens_e = dalloc<int4>(pool_owned, c);
-        q.prev_e = dalloc<int4>(pool_owned, c);
-        q.queue[0] = dalloc<u32>(pool_owned, c);
-        q.queue[1] = dalloc<u32>(pool_owned, c);
-        q.counters = dalloc<u32>(pool_owned, 16);
-        q.bins = dalloc<u32>(pool_owned, 4 * c);
+            *p = reinterpret_cast<float4 *>(take(v16));
+        q.dens_e = reinterpret_cast<int4 *>(take(v16));
+        q.prev_e = reinterpret_cast<int4 *>(take(v16));
+        q.queue[0] = reinterpret_cast<u32 *>(take(v4));
+        q.queue[1] = reinterpret_cast<u32 *>(take(v4));
+        q.bins = reinterpret_cast<u32 *>(take(4 * v4));
+        q.counters = reinterpret_cast<u32 *>(take(256));
         q.bin_capacity = lanes;
         q.stats = stats;
         capacity = lanes;
@@ -483,7 +510,7 @@ void run_wave(rp_scene *s, const WaveParams &p) {
         else
             k_trace<false><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, 0, s->stream>>>(s->ds, pool, in);
         s->done();
-        s->mark(2);
+        s->mark(2, 4);
         RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), s->stream));
         RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), s->stream));
         k_shade<0><<<grid_for(sms, p.lanes, 128, 16), 128, 0, s->stream>>>(s->ds, p, pool, in);
@@ -526,25 +553,25 @@ void build_bvh(rp_scene *s) {
     auto &own = s->owned;
     cudaStream_t st = s->stream;
     BuildTmp &t = s->tmp;
-    t.box_lo = dalloc<float4>(own, n);
-    t.box_hi = dalloc<float4>(own, n);
-    t.cbounds = dalloc<int>(own, 6);
-    t.keys[0] = dalloc<u64>(own, n);
-    t.keys[1] = dalloc<u64>(own, n);
-    t.vals[0] = dalloc<u32>(own, n);
-    t.vals[1] = dalloc<u32>(own, n);
+    t.box_lo = dalloc<float4>(own, n, st);
+    t.box_hi = dalloc<float4>(own, n, st);
+    t.cbounds = dalloc<int>(own, 6, st);
+    t.keys[0] = dalloc<u64>(own, n, st);
+    t.keys[1] = dalloc<u64>(own, n, st);
+    t.vals[0] = dalloc<u32>(own, n, st);
+    t.vals[1] = dalloc<u32>(own, n, st);
     const u32 tiles = (n + kSortTile - 1) / kSortTile;
-    t.hist = dalloc<u32>(own, size_t(256) * std::max<u32>(tiles, 1));
-    t.left = dalloc<u32>(own, n);
-    t.right = dalloc<u32>(own, n);
-    t.parent = dalloc<u32>(own, n);
-    t.leaf_parent = dalloc<u32>(own, n);
-    t.node_lo = dalloc<float4>(own, n);
-    t.node_hi = dalloc<float4>(own, n);
-    t.flags = dalloc<u32>(own, n);
-    float4 *world = dalloc<float4>(own, size_t(3) * n);
-    BNode *nodes = dalloc<BNode>(own, n);
-    float4 *leaf_v = dalloc<float4>(own, size_t(3) * n);
+    t.hist = dalloc<u32>(own, size_t(256) * std::max<u32>(tiles, 1), st);
+    t.left = dalloc<u32>(own, n, st);
+    t.right = dalloc<u32>(own, n, st);
+    t.parent = dalloc<u32>(own, n, st);
+    t.leaf_parent = dalloc<u32>(own, n, st);
+    t.node_lo = dalloc<float4>(own, n, st);
+    t.node_hi = dalloc<float4>(own, n, st);
+    t.flags = dalloc<u32>(own, n, st);
+    float4 *world = dalloc<float4>(own, size_t(3) * n, st);
+    BNode *nodes = dalloc<BNode>(own, n, st);
+    float4 *leaf_v = dalloc<float4>(own, size_t(3) * n, st);
     const int init[6] = {0x7fffffff, 0x7fffffff, 0x7fffffff, int(0x80000000), int(0x80000000), int(0x80000000)};
     RP_CHECK(cudaMemcpyAsync(t.cbounds, init, sizeof(init), cudaMemcpyHostToDevice, st));
     RP_CHECK(cudaMemsetAsync(t.parent, 0xff, size_t(n) * 4, st));
@@ -719,6 +746,8 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             return RP_NO_DEVICE;
         }
         RP_CHECK(cudaSetDevice(device));
+        retain_pool(device);
+        const auto t_begin = std::chrono::steady_clock::now();
         s = new rp_scene();
         s->device = device;
         cudaDeviceProp prop;
@@ -990,10 +1019,15 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             const float g3 = 3.0f * u / (1.0f - 3.0f * u);
             ds.slab_scale = 1 + 2 * g3;
         }
-        s->stats = dalloc<unsigned long long>(own, 8);
+        s->stats = dalloc<unsigned long long>(own, 8, stm);
         RP_CHECK(cudaMemsetAsync(s->stats, 0, 8 * sizeof(unsigned long long), stm));
+        const auto t_host = std::chrono::steady_clock::now();
         build_bvh(s);
         RP_CHECK(cudaStreamSynchronize(stm));
+        const auto t_end = std::chrono::steady_clock::now();
+        s->timing.build_ms = std::chrono::duration<double, std::milli>(t_end - t_begin).count();
+        s->timing.build_host_ms = std::chrono::duration<double, std::milli>(t_host - t_begin).count();
+        s->timing.build_bvh_ms = std::chrono::duration<double, std::milli>(t_end - t_host).count();
         *out = s;
         return RP_SUCCESS;
     });
@@ -1012,6 +1046,7 @@ rp_status rp_cuda_set_counting(rp_scene *s, int enabled) {
 }
 
 rp_status rp_cuda_last_timing(rp_scene *s, rp_timing *t) {
+    // build_* fields always describe scene creation
     if (!s || !t)
         return RP_INVALID_ARGUMENT;
     *t = s->timing;
@@ -1126,8 +1161,9 @@ static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel 
         if (host) {
             if (s->film_stage_pixels < pixels) {
                 if (s->film_stage)
-                    cudaFree(s->film_stage);
-                RP_CHECK(cudaMalloc(&s->film_stage, size_t(pixels) * 2 * sizeof(rp_film_pixel)));
+                    cudaFreeAsync(s->film_stage, s->stream);
+                RP_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&s->film_stage),
+                                         size_t(pixels) * 2 * sizeof(rp_film_pixel), s->stream));
                 s->film_stage_pixels = pixels;
             }
             committed = s->film_stage + pixels;
@@ -1135,8 +1171,9 @@ static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel 
                                      s->stream));
         } else if (s->film_stage_pixels < pixels) {
             if (s->film_stage)
-                cudaFree(s->film_stage);
-            RP_CHECK(cudaMalloc(&s->film_stage, size_t(pixels) * 2 * sizeof(rp_film_pixel)));
+                cudaFreeAsync(s->film_stage, s->stream);
+            RP_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&s->film_stage), size_t(pixels) * 2 * sizeof(rp_film_pixel),
+                                     s->stream));
             s->film_stage_pixels = pixels;
         }
         rp_film_pixel *staged = s->film_stage;
@@ -1223,8 +1260,9 @@ rp_status rp_cuda_set_cie(rp_scene *s, const double *cie_xyz) {
     return guarded(nullptr, 0, [&]() -> rp_status {
         RP_CHECK(cudaSetDevice(s->device));
         if (!s->cie)
-            s->cie = dalloc<double>(s->owned, 3 * 471);
-        RP_CHECK(cudaMemcpy(s->cie, cie_xyz, 3 * 471 * sizeof(double), cudaMemcpyHostToDevice));
+            s->cie = dalloc<double>(s->owned, 3 * 471, s->stream);
+        RP_CHECK(cudaMemcpyAsync(s->cie, cie_xyz, 3 * 471 * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+        RP_CHECK(cudaStreamSynchronize(s->stream));
         return RP_SUCCESS;
     });
 }
@@ -1246,7 +1284,8 @@ rp_status rp_cuda_probe_sobol(const void *tables, const uint32_t *queries, uint3
             std::vector<void *> &o;
             ~Free() {
                 for (void *p : o)
-                    cudaFree(p);
+                    cudaFreeAsync(p, nullptr);
+                cudaStreamSynchronize(nullptr);
             }
         } fr{own};
         const unsigned char *tb = static_cast<const unsigned char *>(tables);
@@ -1270,7 +1309,8 @@ rp_status rp_cuda_probe_philox(const uint32_t *queries, uint32_t count, uint32_t
             std::vector<void *> &o;
             ~Free() {
                 for (void *p : o)
-                    cudaFree(p);
+                    cudaFreeAsync(p, nullptr);
+                cudaStreamSynchronize(nullptr);
             }
         } fr{own};
         const u32 *q = dupload(own, queries, size_t(6) * count, nullptr);
@@ -1289,7 +1329,8 @@ rp_status rp_cuda_probe_wavelengths(const float *u, uint32_t count, uint32_t mod
             std::vector<void *> &o;
             ~Free() {
                 for (void *p : o)
-                    cudaFree(p);
+                    cudaFreeAsync(p, nullptr);
+                cudaStreamSynchronize(nullptr);
             }
         } fr{own};
         const float *q = dupload(own, u, count, nullptr);
@@ -1308,7 +1349,8 @@ rp_status rp_cuda_probe_bsdf(const float *queries, uint32_t count, float *result
             std::vector<void *> &o;
             ~Free() {
                 for (void *p : o)
-                    cudaFree(p);
+                    cudaFreeAsync(p, nullptr);
+                cudaStreamSynchronize(nullptr);
             }
         } fr{own};
         const float *q = dupload(own, queries, size_t(16) * count, nullptr);
@@ -1337,7 +1379,8 @@ rp_status rp_cuda_probe_raygen(rp_scene *s, const rp_request *request, uint32_t 
             std::vector<void *> &o;
             ~Free() {
                 for (void *q : o)
-                    cudaFree(q);
+                    cudaFreeAsync(q, nullptr);
+                cudaStreamSynchronize(nullptr);
             }
         } fr{own};
         u32 *w = dalloc<u32>(own, size_t(11) * p.lanes);
@@ -1400,7 +1443,8 @@ rp_status rp_cuda_trace_rays(rp_scene *s, const float *rays, uint32_t count, int
             std::vector<void *> &o;
             ~Free() {
                 for (void *q : o)
-                    cudaFree(q);
+                    cudaFreeAsync(q, nullptr);
+                cudaStreamSynchronize(nullptr);
             }
         } fr{own};
         const float *q = dupload(own, rays, size_t(7) * count, s->stream);

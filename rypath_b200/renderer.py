@@ -200,11 +200,13 @@ def film_mean(film: np.ndarray) -> np.ndarray:
     return np.where(weight[:, None] > 0, xyz / np.where(weight > 0, weight, 1)[:, None], 0.0)
 
 
-def render_progressive(scene: scenes.Scene, settings: RenderSettings, device: int = 0):
-    """render_progressive (src/render_driver.cpp:287-316): build, then render every batch."""
+def render_progressive(scene: scenes.Scene, settings: RenderSettings, device: int = 0,
+                       film: np.ndarray | None = None):
+    """render_progressive (src/render_driver.cpp:287-316): build, then render every batch into
+    ``film`` (a host rp_film_pixel array holding the committed state; zeros for a new render)."""
     built = build_renderer(scene, device)
     if built.status != abi.RP_SUCCESS:
         return built.status, built.diagnostic, None
-    st, diag, film = built.scene.render_film(settings)
+    st, diag, film = built.scene.render_film(settings, film)
     built.scene.close()
     return st, diag, film
