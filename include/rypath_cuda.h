@@ -319,6 +319,33 @@ rp_status rp_cuda_scene_export_bvh(struct rp_scene *scene, uint32_t *nodes, uint
 rp_status rp_cuda_trace_rays(struct rp_scene *scene, const float *rays, uint32_t count,
                              int any_hit, float *hits, char *diag, size_t diag_capacity);
 
+/* ---- allocation-free sampling -------------------------------------------------------------- */
+
+/* Size of the library's file-scope device scratch array used by rp_cuda_sample_device_static.
+ * Every GPU that loads this library holds this much device memory until the process exits. */
+#define RP_STATIC_SCRATCH_BYTES (64u << 20)
+/* Largest request, in lanes (pixel_count * sample_count), that fits that scratch. */
+#define RP_STATIC_MAX_LANES 178464u
+
+/* No counterpart in rypath.  Same work and results as rp_cuda_sample_device, for callers that
+ * must not allocate device memory during a render call -- for example a host that hands the
+ * GPU to us between its own allocation-free phases, or code running where the allocator is
+ * unavailable or forbidden (inside a memory budget owned by someone else).  The wavefront's
+ * per-lane scratch (path state, queues, family bins, counters) lives in one file-scope
+ * __device__ array of RP_STATIC_SCRATCH_BYTES instead of memory from the scene's pool; the
+ * caller still passes the scene (created earlier) and a device output buffer.  Nothing is
+ * allocated: no cudaMalloc / cudaMallocAsync / cudaFree and no allocating library call.
+ *   - Limit: request lanes (pixel_count * sample_count) <= RP_STATIC_MAX_LANES;
+ *     larger requests return RP_INVALID_ARGUMENT with a diagnostic naming the maximum.
+ *   - The first call on a device looks up the array's device address once, with that device
+ *     current; make that first call before any stream capture.
+ *   - Work runs on `stream` (a cudaStream_t; NULL = the scene's stream) and is complete when
+ *     the stream is.  Every call shares the one array: calls whose GPU work overlaps (two
+ *     streams, two scenes, two threads) race and corrupt each other; serialise them. */
+rp_status rp_cuda_sample_device_static(struct rp_scene *scene, const rp_request *request,
+                                       rp_packet_result *device_results, size_t capacity,
+                                       void *stream, char *diag, size_t diag_capacity);
+
 /* ---- host helpers ----------------------------------------------------------------------- */
 
 /* sizeof() of an ABI struct by name ("rp_request", ...), 0 if unknown; lets bindings check

@@ -1458,3 +1458,125 @@ rp_status rp_cuda_trace_rays(rp_scene *s, const float *rays, uint32_t count, int
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------- allocation-free sampling
+// The scratch of rp_cuda_sample_device_static: one file-scope device array, shared by every
+// call on a device (see include/rypath_cuda.h).  Host code must not use its name as an
+// address: the device address is looked up with cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_static_scratch[RP_STATIC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr size_t kStaticArrays16 = 22, kStaticArrays4 = 6; // same SoA carve as the pool
+
+constexpr size_t static_bytes_for(u32 lanes) {
+    return kStaticArrays16 * ((size_t(lanes) * 16 + 255) & ~size_t(255)) +
+           kStaticArrays4 * ((size_t(lanes) * 4 + 255) & ~size_t(255)) + 256;
+}
+static_assert(static_bytes_for(RP_STATIC_MAX_LANES) <= RP_STATIC_SCRATCH_BYTES &&
+                  static_bytes_for(RP_STATIC_MAX_LANES + 1) > RP_STATIC_SCRATCH_BYTES,
+              "RP_STATIC_MAX_LANES is the largest request that fits the static scratch");
+
+// Device address of the scratch array, looked up once per device with that device current.
+unsigned char *static_scratch(int device, cudaError_t &err) {
+    static unsigned char *address[64] = {};
+    err = cudaSuccess;
+    if (device < 0 || device >= 64)
+        return nullptr;
+    if (!address[device]) {
+        void *ptr = nullptr;
+        err = cudaGetSymbolAddress(&ptr, g_static_scratch);
+        if (err != cudaSuccess)
+            return nullptr;
+        address[device] = static_cast<unsigned char *>(ptr);
+    }
+    return address[device];
+}
+
+PathPool static_pool(unsigned char *base, u32 lanes, unsigned long long *stats) {
+    const size_t v16 = (size_t(lanes) * 16 + 255) & ~size_t(255), v4 = (size_t(lanes) * 4 + 255) & ~size_t(255);
+    size_t off = 0;
+    auto take = [&](size_t n) {
+        unsigned char *p = base + off;
+        off += n;
+        return p;
+    };
+    PathPool q{};
+    q.ident = reinterpret_cast<uint4 *>(take(v16));
+    q.cursor = reinterpret_cast<uint4 *>(take(v16));
+    float4 **f4[] = {&q.lambda, &q.lambda_pdf, &q.beta, &q.radiance, &q.dens_f, &q.prev_f, &q.eta_scale, &q.ray_o,
+                     &q.ray_d, &q.latest_p, &q.latest_n, &q.latest_param, &q.latest_k, &q.preceding, &q.hit,
+                     &q.sh_o, &q.sh_d, &q.sh_c};
+    for (auto p : f4)
+        *p = reinterpret_cast<float4 *>(take(v16));
+    q.dens_e = reinterpret_cast<int4 *>(take(v16));
+    q.prev_e = reinterpret_cast<int4 *>(take(v16));
+    q.queue[0] = reinterpret_cast<u32 *>(take(v4));
+    q.queue[1] = reinterpret_cast<u32 *>(take(v4));
+    q.bins = reinterpret_cast<u32 *>(take(4 * v4));
+    q.counters = reinterpret_cast<u32 *>(take(256));
+    q.bin_capacity = lanes;
+    q.stats = stats;
+    return q;
+}
+
+__global__ void k_static_set_lanes(u32 *counter, u32 lanes) { *counter = lanes; }
+
+} // namespace
+
+extern "C" {
+
+rp_status rp_cuda_sample_device_static(rp_scene *s, const rp_request *request, rp_packet_result *device_results,
+                                       size_t capacity, void *stream, char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!s || !request || !device_results)
+            throw Invalid{"null argument"};
+        const std::string err = validate_request(s, *request);
+        if (!err.empty())
+            throw Invalid{err};
+        const WaveParams p = wave_params(*request);
+        if (capacity < p.lanes)
+            throw Invalid{"output capacity is smaller than the request lanes"};
+        const u32 max_lanes = RP_STATIC_MAX_LANES;
+        if (p.lanes > max_lanes) {
+            set_diag(diag, cap,
+                     "request has %u lanes; the allocation-free entry point accepts at most %u lanes "
+                     "(%u bytes of static scratch)",
+                     p.lanes, max_lanes, RP_STATIC_SCRATCH_BYTES);
+            return RP_INVALID_ARGUMENT;
+        }
+        RP_CHECK(cudaSetDevice(s->device));
+        cudaError_t e;
+        unsigned char *base = static_scratch(s->device, e);
+        if (!base) {
+            set_diag(diag, cap, "cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
+            return RP_FAILURE;
+        }
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+        PathPool pool = static_pool(base, p.lanes, s->stats);
+        const int sms = s->sm_count;
+        // counters start at zero on every call; every other array is written before it is read
+        RP_CHECK(cudaMemsetAsync(pool.counters, 0, 256, st));
+        k_raygen<<<grid_for(sms, p.lanes, 256, 16), 256, 0, st>>>(s->ds, p, pool);
+        k_static_set_lanes<<<1, 1, 0, st>>>(pool.counters, p.lanes);
+        int in = 0;
+        for (u32 ev = 0; ev < s->ds.max_depth + 1; ++ev) {
+            RP_CHECK(cudaMemsetAsync(pool.counters + 4, 0, 4 * sizeof(u32), st));
+            k_trace<false><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, 0, st>>>(s->ds, pool, in);
+            RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), st));
+            RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), st));
+            k_shade<0><<<grid_for(sms, p.lanes, 128, 16), 128, 0, st>>>(s->ds, p, pool, in);
+            k_shade<1><<<grid_for(sms, p.lanes, 128, 16), 128, 0, st>>>(s->ds, p, pool, in);
+            k_shade<2><<<grid_for(sms, p.lanes, 128, 16), 128, 0, st>>>(s->ds, p, pool, in);
+            k_shade<3><<<grid_for(sms, p.lanes, 128, 16), 128, 0, st>>>(s->ds, p, pool, in);
+            k_shadow<false><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, 0, st>>>(s->ds, pool);
+            in ^= 1;
+        }
+        k_results<<<grid_for(sms, p.lanes, 256, 16), 256, 0, st>>>(pool, p.lanes,
+                                                                   reinterpret_cast<PacketResult *>(device_results));
+        RP_CHECK(cudaGetLastError());
+        return RP_SUCCESS;
+    });
+}
+
+} // extern "C"

@@ -55,6 +55,7 @@ def lib():
         "rp_cuda_scene_export_bvh": (st, [vp, vp, vp, vp, vp, sz, cp, sz]),
         "rp_cuda_trace_rays": (st, [vp, vp, u32, C.c_int, vp, cp, sz]),
         "rp_cuda_abi_size": (u32, [cp]),
+        "rp_cuda_sample_device_static": (st, [vp, C.POINTER(abi.Request), vp, sz, vp, cp, sz]),
         "rp_cuda_build_light_tables": (C.c_int, [vp, u32, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
