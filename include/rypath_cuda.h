@@ -60,6 +60,10 @@ enum { RP_RANDOMIZE_NONE = 0, RP_RANDOMIZE_PERMUTEDIGITS = 1, RP_RANDOMIZE_FASTO
 enum { RP_FILTER_BOX = 0, RP_FILTER_TRIANGLE = 1 };
 /* Scattering families (wire::Material::scattering, src/render_wire.h:121). */
 enum { RP_DIFFUSE = 0, RP_CONDUCTOR = 1, RP_DIELECTRIC = 2 };
+/* Null medium interface (ScatteringKind::null_interface, wire scattering 10,
+ * shaders/scalar_transport.h:450-472): changes the medium, scatters nothing.  Scalar
+ * transport only. */
+enum { RP_INTERFACE = 10 };
 /* Reflectance sources (src/render_wire.h:41-48). */
 enum { RP_REFLECTANCE_KNOTS = 0, RP_REFLECTANCE_CONSTANT = 1, RP_REFLECTANCE_BLACKBODY = 4 };
 /* Positional light kinds (src/render_wire.h:200). */

@@ -55,6 +55,19 @@ void or_probe_light_select(const or_scene *scene, const float *queries, uint32_t
 int or_film_add(const rp_packet_result *results, size_t count, const double *cie_xyz,
                 uint32_t pixel_count, rp_film_pixel *film);
 
+/* Scalar (one-wavelength) PT / volpath lanes of a request (rypath_render_paths); the scene
+ * must be built with RP_TRANSPORT_SCALAR.  threads <= 0: all cores.  0, 1 on a failed
+ * lane, -1 on a bad request. */
+int or_sample_scalar(const or_scene *scene, const rp_request *request, rp_scalar_result *results,
+                     size_t capacity, int threads);
+/* Homogeneous-medium equations (shaders/medium.h): per query 15 floats {sigma_a, sigma_s,
+ * Le, distance, sigma_t, u, wo[3], wi[3], g, ux, uy} -> 8 floats {transmission, emission,
+ * valid, flight, phase, sampled direction[3]}. */
+void or_probe_medium(const float *queries, uint32_t count, float *results);
+/* Film reduction of scalar samples in the given order (FilmBatch::add). */
+int or_scalar_film_add(const rp_scalar_result *results, size_t count, const double *cie_xyz,
+                       uint32_t pixel_count, rp_film_pixel *film);
+
 #ifdef __cplusplus
 }
 #endif

@@ -335,6 +335,8 @@ bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error) {
         in.emission = q.emission;
         in.normal_begin = q.normal_begin;
         in.emitter_begin = RP_NONE;
+        in.inside_medium = q.inside_medium;
+        in.outside_medium = q.outside_medium;
         if (q.emission != RP_NONE) {
             in.emitter_begin = u32(s.emitters.size());
             for (u32 t = 0; t < q.triangle_count; ++t)
@@ -362,6 +364,20 @@ bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error) {
     s.max_depth = d.max_depth;
     s.light_sampler = d.light_sampler;
     s.hero_mode = d.hero_wavelengths;
+    s.transport = d.transport;
+    s.camera_medium = d.camera_medium;
+    bool interfaces = false;
+    for (const auto &m : s.materials)
+        interfaces = interfaces || m.scattering == RP_INTERFACE;
+    for (u32 i = 0; i < d.medium_count; ++i) {
+        Medium m;
+        std::copy(d.media[i].sigma_a, d.media[i].sigma_a + 471, m.sigma_a.begin());
+        std::copy(d.media[i].sigma_s, d.media[i].sigma_s + 471, m.sigma_s.begin());
+        std::copy(d.media[i].emission, d.media[i].emission + 471, m.emission.begin());
+        m.g = d.media[i].g;
+        s.media.push_back(m);
+    }
+    s.media_enabled = d.medium_count > 0 || interfaces || d.camera_medium != RP_NONE;
     s.sobol_storage.assign((const unsigned char *)d.sobol_tables,
                            (const unsigned char *)d.sobol_tables + sizeof(SobolTables));
     s.sobol = reinterpret_cast<const SobolTables *>(s.sobol_storage.data());
@@ -842,6 +858,7 @@ bool triangle_surface_point(const Scene &s, u32 instance, u32 local, float u, fl
         return false;
     const float nl = std::sqrt(n2);
     point.inverse_area_pdf = 0.5f * nl;
+    point.world_extent = triangle_extent(we1, we2);
     point.geometric_normal = ce / nl;
     if (in.reverse)
         point.geometric_normal = -point.geometric_normal;

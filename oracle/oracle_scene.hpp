@@ -51,6 +51,12 @@ struct Instance {
     float m[12];
     u32 vertex_begin, triangle_begin, triangle_count, material, reverse, emission, normal_begin;
     u32 emitter_begin;
+    u32 inside_medium = RP_NONE, outside_medium = RP_NONE;
+};
+// HomogeneousMedium (src/render.hpp:29-36)
+struct Medium {
+    std::array<float, 471> sigma_a, sigma_s, emission;
+    float g;
 };
 struct Material {
     u32 scattering, kind, knot_begin, knot_count;
@@ -81,6 +87,10 @@ struct Scene {
     std::vector<Emitter> emitters;
     std::array<float, 471> environment{};
     bool has_environment = false;
+    // media (scalar transport)
+    std::vector<Medium> media;
+    u32 camera_medium = RP_NONE, transport = RP_TRANSPORT_HERO;
+    bool media_enabled = false;
     // camera (wire::Parameters slots for the PBRT model, src/metal_render.mm:158-191)
     F3 origin, forward, right, up, camera_normal;
     u32 filter_kind = 0;
@@ -130,6 +140,7 @@ Hit trace_closest_brute(const Scene &s, F3 o, F3 d, float tmax);
 struct SurfacePoint {
     F3 position, error, geometric_normal, shading_normal;
     float inverse_area_pdf = 0;
+    float world_extent = 0;
 };
 bool triangle_surface_point(const Scene &s, u32 instance, u32 local, float u, float v,
                             bool native_hit, SurfacePoint &p);
@@ -147,3 +158,9 @@ float light_geometry_pdf(const Scene &s, u32 emitter, F3 reference, F3 normal,
                          const SurfacePoint &point);
 
 } // namespace oracle
+
+// The opaque scene handle of the oracle's C ABI (oracle.h).
+struct or_scene {
+    oracle::Scene scene;
+    oracle::Bvh bvh;
+};

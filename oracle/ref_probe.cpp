@@ -14,6 +14,7 @@
 #include "conductor.h"
 #include "dielectric.h"
 #include "transmission.h"
+#include "medium.h"
 
 #include <cstring>
 #include <vector>
@@ -184,6 +185,24 @@ uint32_t ref_outward(uint32_t bits, int toward_negative, int *valid) {
 // Packet film reduction through the reference's own PacketFilmBatch
 // (src/packet_film.cpp); pbrt_cie_xyz is supplied below from the same CIE table.
 static std::vector<double> g_cie;
+// shaders/medium.h, in the or_probe_medium layout (oracle.h)
+void ref_probe_medium(const float *q, uint32_t count, float *r) {
+    for (uint32_t i = 0; i < count; ++i) {
+        const float *a = q + 15 * i;
+        float *o = r + 8 * i;
+        const auto seg = rypath_medium::segment(a[0], a[1], a[2], a[3]);
+        o[0] = seg.transmission;
+        o[1] = seg.emission;
+        o[2] = seg.valid ? 1.0f : 0.0f;
+        o[3] = rypath_medium::flight(a[4], a[5]);
+        o[4] = rypath_medium::phase(float3(a[6], a[7], a[8]), float3(a[9], a[10], a[11]), a[12]);
+        const float3 w = rypath_medium::phase_sample(float3(a[6], a[7], a[8]), a[12], float2(a[13], a[14]));
+        o[5] = w.x;
+        o[6] = w.y;
+        o[7] = w.z;
+    }
+}
+
 void ref_set_cie(const double *cie) { g_cie.assign(cie, cie + 3 * 471); }
 int ref_film_add(const uint32_t *words, size_t count, uint32_t width, uint32_t height,
                  double *out_sum_weight_count) {

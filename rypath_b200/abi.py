@@ -21,6 +21,7 @@ SAMPLER_INDEPENDENT, SAMPLER_SOBOL = 0, 1
 RANDOMIZE_NONE, RANDOMIZE_PERMUTEDIGITS, RANDOMIZE_FASTOWEN, RANDOMIZE_OWEN = range(4)
 FILTER_BOX, FILTER_TRIANGLE = 0, 1
 DIFFUSE, CONDUCTOR, DIELECTRIC = 0, 1, 2
+INTERFACE = 10  # null medium interface (scalar transport)
 REFLECTANCE_KNOTS, REFLECTANCE_CONSTANT, REFLECTANCE_BLACKBODY = 0, 1, 4
 POINT_LIGHT, SPOT_LIGHT = 0, 1
 LIGHTS_BVH, LIGHTS_POWER, LIGHTS_UNIFORM = 0, 1, 2
@@ -145,6 +146,14 @@ def packet_dtype():
                      ("sample_high", "<u4"), ("splat_count", "<u4"), ("wavelengths", "<f4", 4),
                      ("wavelength_pdfs", "<f4", 4), ("radiance", "<f4", 4),
                      ("filter_weight", "<f4"), ("reserved", "<u4", 2)])
+
+
+def scalar_dtype():
+    import numpy as np
+
+    return np.dtype([("status", "<u4"), ("pixel", "<u4"), ("sample_low", "<u4"),
+                     ("sample_high", "<u4"), ("wavelength", "<f4"), ("radiance", "<f4"),
+                     ("scatterings", "<u4"), ("random_words", "<u4", 4)])
 
 
 def film_dtype():

@@ -4,6 +4,7 @@
 #include "../../include/rypath_cuda.h"
 #include "rp_build.cuh"
 #include "rp_probes.cuh"
+#include "rp_volpath.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -42,6 +43,10 @@ struct CudaError {
     } while (0)
 
 struct Invalid {
+    std::string what;
+};
+// A valid request for a part of the reference this backend does not build.
+struct NotBuilt {
     std::string what;
 };
 
@@ -350,6 +355,12 @@ struct rp_scene {
     size_t event_cursor = 0;
     std::vector<int> event_kind;
     double light_power_total = 0;
+    u32 transport = RP_TRANSPORT_HERO;
+    // scalar transport: one 16-byte record per lane, regeneration and failure counters
+    uint4 *scalar_records = nullptr;
+    u32 *scalar_counters = nullptr;
+    u32 scalar_capacity = 0;
+    int volpath_blocks = 0; // resident persistent blocks per SM
 
     ~rp_scene() {
         if (device >= 0)
@@ -358,6 +369,8 @@ struct rp_scene {
             cudaFreeAsync(p, stream);
         for (void *p : owned)
             cudaFreeAsync(p, stream);
+        if (scalar_records)
+            cudaFreeAsync(scalar_records, stream);
         if (film_stage)
             cudaFreeAsync(film_stage, stream);
         if (stream)
@@ -408,6 +421,20 @@ struct rp_scene {
         launches = 0;
         event_kind.clear();
         event_cursor = 0;
+    }
+
+    void ensure_scalar(u32 lanes) {
+        if (lanes <= scalar_capacity)
+            return;
+        if (scalar_records)
+            cudaFreeAsync(scalar_records, stream);
+        scalar_records = nullptr;
+        scalar_capacity = 0;
+        const size_t bytes = size_t(lanes) * sizeof(uint4) + 256;
+        RP_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&scalar_records), bytes, stream));
+        scalar_counters = reinterpret_cast<u32 *>(reinterpret_cast<unsigned char *>(scalar_records) +
+                                                  size_t(lanes) * sizeof(uint4));
+        scalar_capacity = lanes;
     }
 
     void ensure_pool(u32 lanes) {
@@ -529,6 +556,34 @@ void run_wave(rp_scene *s, const WaveParams &p) {
     RP_CHECK(cudaGetLastError());
 }
 
+// One wave of the scalar transport: the persistent regeneration kernel over p.lanes lanes,
+// one record per lane in s->scalar_records.
+void run_scalar_wave(rp_scene *s, const WaveParams &p, u32 boundary_limit) {
+    s->ensure_scalar(p.lanes);
+    if (!s->volpath_blocks) {
+        int per_sm = 0;
+        RP_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_volpath<false>, kTraceBlock, 0));
+        s->volpath_blocks = std::max(1, per_sm);
+    }
+    s->mark(3);
+    RP_CHECK(cudaMemsetAsync(s->scalar_counters, 0, 64, s->stream));
+    s->done();
+    ScalarParams q;
+    q.boundary_limit = boundary_limit;
+    q.out = s->scalar_records;
+    q.next_lane = s->scalar_counters;
+    q.stats = s->stats;
+    const u32 blocks_needed = (p.lanes + kTraceBlock - 1) / kTraceBlock;
+    const int grid = int(std::max<u32>(1, std::min<u32>(blocks_needed, u32(s->sm_count * s->volpath_blocks))));
+    s->mark(2);
+    if (s->counting)
+        k_volpath<true><<<grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q);
+    else
+        k_volpath<false><<<grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q);
+    s->done();
+    RP_CHECK(cudaGetLastError());
+}
+
 template <class F> rp_status guarded(char *diag, size_t cap, F &&f) {
     try {
         return f();
@@ -538,6 +593,9 @@ template <class F> rp_status guarded(char *diag, size_t cap, F &&f) {
     } catch (const Invalid &e) {
         set_diag(diag, cap, "%s", e.what.c_str());
         return RP_INVALID_ARGUMENT;
+    } catch (const NotBuilt &e) {
+        set_diag(diag, cap, "%s", e.what.c_str());
+        return RP_NOT_BUILT;
     } catch (const std::bad_alloc &) {
         set_diag(diag, cap, "host allocation failed");
         return RP_FAILURE;
@@ -728,12 +786,24 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             throw Invalid{"scene description ABI version mismatch"};
         if (!d->sobol_tables)
             throw Invalid{"scene description needs the Sobol tables"};
-        if (d->transport != RP_TRANSPORT_HERO)
-            throw Invalid{"only the hero-wavelength transport is built for this entry point"};
-        if (d->max_depth > RP_MAX_DEPTH + 1)
-            throw Invalid{"hero transport requires max depth <= 65"};
-        if (d->medium_count || d->camera_medium != RP_NONE)
-            throw Invalid{"hero transport requires a vacuum scene (src/render.cpp:1579-1580)"};
+        if (d->transport != RP_TRANSPORT_HERO && d->transport != RP_TRANSPORT_SCALAR)
+            throw NotBuilt{"only the hero-wavelength and scalar transports are built"};
+        const bool scalar = d->transport == RP_TRANSPORT_SCALAR;
+        bool interfaces = false;
+        for (u32 i = 0; i < d->material_count; ++i)
+            interfaces = interfaces || d->materials[i].scattering == RP_INTERFACE;
+        if (!scalar) {
+            if (d->max_depth > RP_MAX_DEPTH + 1)
+                throw Invalid{"hero transport requires max depth <= 65"};
+            bool instance_media = false;
+            for (u32 i = 0; i < d->instance_count; ++i)
+                instance_media = instance_media || d->instances[i].inside_medium != RP_NONE ||
+                                 d->instances[i].outside_medium != RP_NONE;
+            if (d->medium_count || d->camera_medium != RP_NONE || interfaces || instance_media)
+                throw Invalid{"Packet/hero spectral transport requires a PBRT scene with vacuum media"};
+        }
+        if (d->camera_medium != RP_NONE && d->camera_medium >= d->medium_count)
+            throw Invalid{"camera medium out of range"};
         if (d->filter_kind > RP_FILTER_TRIANGLE)
             throw Invalid{"unsupported pixel filter"};
         if (d->light_sampler > RP_LIGHTS_UNIFORM)
@@ -771,9 +841,30 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
                     if (uint64_t(in.vertex_begin) + d->triangles[3 * (in.triangle_begin + t) + k] >= d->vertex_count)
                         throw Invalid{"triangle vertex out of range"};
         }
-        for (u32 i = 0; i < d->material_count; ++i)
-            if (d->materials[i].scattering > RP_DIELECTRIC)
-                throw Invalid{"unsupported scattering family (diffuse, conductor, dielectric are built)"};
+        for (u32 i = 0; i < d->material_count; ++i) {
+            const u32 f = d->materials[i].scattering;
+            if (f > RP_DIELECTRIC && !(scalar && f == RP_INTERFACE))
+                throw NotBuilt{"unsupported scattering family (diffuse, conductor, dielectric; null interfaces with "
+                               "the scalar transport)"};
+            if (scalar && (f == RP_CONDUCTOR || f == RP_DIELECTRIC))
+                throw NotBuilt{"the scalar transport builds diffuse surfaces and null interfaces; conductor and "
+                               "dielectric surfaces render with the hero transport"};
+        }
+        for (u32 i = 0; i < d->instance_count; ++i) {
+            const auto &in = d->instances[i];
+            if ((in.inside_medium != RP_NONE && in.inside_medium >= d->medium_count) ||
+                (in.outside_medium != RP_NONE && in.outside_medium >= d->medium_count))
+                throw Invalid{"instance medium out of range"};
+        }
+        for (u32 i = 0; i < d->medium_count; ++i) {
+            const auto &m = d->media[i];
+            for (int k = 0; k < RP_SPECTRUM_BINS; ++k)
+                if (!(m.sigma_a[k] >= 0 && std::isfinite(m.sigma_a[k]) && m.sigma_s[k] >= 0 &&
+                      std::isfinite(m.sigma_s[k]) && m.emission[k] >= 0 && std::isfinite(m.emission[k])))
+                    throw Invalid{"medium coefficients must be finite and nonnegative"};
+            if (!std::isfinite(m.g))
+                throw Invalid{"medium asymmetry must be finite"};
+        }
         // flattened triangles and emitters (src/metal_render.mm:1174-1210)
         std::vector<u32> tri_instance, tri_local, em_inst, em_local;
         std::vector<DInstance> instances(d->instance_count);
@@ -789,6 +880,8 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             in.emission = q.emission;
             in.normal_begin = q.normal_begin;
             in.emitter_begin = kNone;
+            in.inside_medium = q.inside_medium;
+            in.outside_medium = q.outside_medium;
             if (q.emission != RP_NONE) {
                 in.emitter_begin = u32(em_inst.size());
                 for (u32 t = 0; t < q.triangle_count; ++t) {
@@ -1014,6 +1107,21 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
         ds.filter_y = d->filter_y_radius;
         ds.max_depth = d->max_depth;
         ds.hero_mode = d->hero_wavelengths;
+        s->transport = d->transport;
+        {
+            std::vector<float> media(size_t(d->medium_count) * kMediumStride, 0.0f);
+            for (u32 i = 0; i < d->medium_count; ++i) {
+                float *m = media.data() + size_t(i) * kMediumStride;
+                std::copy(d->media[i].sigma_a, d->media[i].sigma_a + 471, m);
+                std::copy(d->media[i].sigma_s, d->media[i].sigma_s + 471, m + 471);
+                std::copy(d->media[i].emission, d->media[i].emission + 471, m + 942);
+                m[1413] = d->media[i].g;
+            }
+            ds.media = dupload(own, media.data(), media.size(), stm);
+            ds.medium_count = d->medium_count;
+            ds.camera_medium = d->camera_medium;
+            ds.media_enabled = d->medium_count > 0 || interfaces || d->camera_medium != RP_NONE;
+        }
         {
             const float u = 0x1.0p-24f;
             const float g3 = 3.0f * u / (1.0f - 3.0f * u);
@@ -1061,6 +1169,8 @@ static rp_status sample_impl(rp_scene *s, const rp_request *request, rp_packet_r
         const std::string err = validate_request(s, *request);
         if (!err.empty())
             throw Invalid{err};
+        if (s->transport != RP_TRANSPORT_HERO)
+            throw Invalid{"the scene was built for the scalar transport; sample it with rp_cuda_sample_scalar"};
         const WaveParams p = wave_params(*request);
         if (capacity < p.lanes)
             throw Invalid{"output capacity is smaller than the request lanes"};
@@ -1132,9 +1242,65 @@ rp_status rp_cuda_sample_device(rp_scene *s, const rp_request *request, rp_packe
     return sample_impl(s, request, results, capacity, false, static_cast<cudaStream_t>(stream), diag, cap);
 }
 
-rp_status rp_cuda_sample_scalar(rp_scene *, const rp_request *, rp_scalar_result *, size_t, char *diag, size_t cap) {
-    set_diag(diag, cap, "scalar (single-wavelength) transport is not built in this backend");
-    return RP_NOT_BUILT;
+static_assert(sizeof(ScalarResult) == sizeof(rp_scalar_result), "scalar result layout");
+
+rp_status rp_cuda_sample_scalar(rp_scene *s, const rp_request *request, rp_scalar_result *out, size_t capacity,
+                                char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!s || !request || !out)
+            throw Invalid{"null argument"};
+        const std::string err = validate_request(s, *request);
+        if (!err.empty())
+            throw Invalid{err};
+        if (s->transport != RP_TRANSPORT_SCALAR)
+            throw Invalid{"the scene was built for the hero transport; sample it with rp_cuda_sample"};
+        const WaveParams p = wave_params(*request);
+        if (capacity < p.lanes)
+            throw Invalid{"output capacity is smaller than the request lanes"};
+        RP_CHECK(cudaSetDevice(s->device));
+        cudaEvent_t start, stop;
+        RP_CHECK(cudaEventCreate(&start));
+        RP_CHECK(cudaEventCreate(&stop));
+        RP_CHECK(cudaEventRecord(start, s->stream));
+        if (s->counting)
+            RP_CHECK(cudaMemsetAsync(s->stats, 0, 8 * sizeof(unsigned long long), s->stream));
+        run_scalar_wave(s, p, request->boundary_limit ? request->boundary_limit : 4096u);
+        ScalarResult *staging = nullptr;
+        RP_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&staging), size_t(p.lanes) * sizeof(ScalarResult), s->stream));
+        s->mark(3);
+        k_scalar_results<<<grid_for(s->sm_count, p.lanes, 256, 16), 256, 0, s->stream>>>(s->ds, p, s->scalar_records,
+                                                                                          staging);
+        s->done();
+        RP_CHECK(cudaMemcpyAsync(out, staging, size_t(p.lanes) * sizeof(ScalarResult), cudaMemcpyDeviceToHost,
+                                 s->stream));
+        RP_CHECK(cudaFreeAsync(staging, s->stream));
+        RP_CHECK(cudaEventRecord(stop, s->stream));
+        s->collect();
+        float total = 0;
+        RP_CHECK(cudaEventElapsedTime(&total, start, stop));
+        cudaEventDestroy(start);
+        cudaEventDestroy(stop);
+        s->timing.total_ms = total;
+        s->timing.samples = p.lanes;
+        if (s->counting) {
+            unsigned long long st[6];
+            RP_CHECK(cudaMemcpy(st, s->stats, sizeof(st), cudaMemcpyDeviceToHost));
+            s->timing.nodes_visited = st[0];
+            s->timing.triangles_tested = st[1];
+            s->timing.closest_rays = st[2];
+            s->timing.shadow_rays = st[3];
+            s->timing.shadow_nodes_visited = st[4];
+            s->timing.shadow_triangles_tested = st[5];
+        }
+        u32 failures = 0;
+        for (u32 i = 0; i < p.lanes; ++i)
+            if (out[i].status != RP_SAMPLE_SUCCESS) {
+                if (!failures)
+                    set_diag(diag, cap, "Metal render sample failed with status %u at lane %u", out[i].status, i);
+                ++failures;
+            }
+        return failures ? RP_FAILURE : RP_SUCCESS;
+    });
 }
 
 static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel *film, bool host, char *diag, size_t cap) {
@@ -1204,13 +1370,23 @@ static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel 
                 if (!err.empty())
                     throw Invalid{err};
                 const WaveParams p = wave_params(q);
-                run_wave(s, p);
-                s->mark(3);
-                k_film<<<grid_for(s->sm_count, pixels, 128, 16), 128, 0, s->stream>>>(
-                    s->pool, pixels, u32(spw), s->cie, reinterpret_cast<FilmPixel *>(staged));
-                s->done();
                 u32 f = 0;
-                RP_CHECK(cudaMemcpyAsync(&f, s->pool.counters + 3, 4, cudaMemcpyDeviceToHost, s->stream));
+                if (s->transport == RP_TRANSPORT_SCALAR) {
+                    run_scalar_wave(s, p, 4096u);
+                    s->mark(3);
+                    k_scalar_film<<<grid_for(s->sm_count, pixels, 128, 16), 128, 0, s->stream>>>(
+                        s->scalar_records, pixels, u32(spw), s->cie, reinterpret_cast<FilmPixel *>(staged),
+                        s->scalar_counters + 1);
+                    s->done();
+                    RP_CHECK(cudaMemcpyAsync(&f, s->scalar_counters + 1, 4, cudaMemcpyDeviceToHost, s->stream));
+                } else {
+                    run_wave(s, p);
+                    s->mark(3);
+                    k_film<<<grid_for(s->sm_count, pixels, 128, 16), 128, 0, s->stream>>>(
+                        s->pool, pixels, u32(spw), s->cie, reinterpret_cast<FilmPixel *>(staged));
+                    s->done();
+                    RP_CHECK(cudaMemcpyAsync(&f, s->pool.counters + 3, 4, cudaMemcpyDeviceToHost, s->stream));
+                }
                 RP_CHECK(cudaStreamSynchronize(s->stream));
                 failures += f;
                 in_batch += spw;
@@ -1534,6 +1710,8 @@ rp_status rp_cuda_sample_device_static(rp_scene *s, const rp_request *request, r
         const std::string err = validate_request(s, *request);
         if (!err.empty())
             throw Invalid{err};
+        if (s->transport != RP_TRANSPORT_HERO)
+            throw Invalid{"the allocation-free entry point samples hero-transport scenes"};
         const WaveParams p = wave_params(*request);
         if (capacity < p.lanes)
             throw Invalid{"output capacity is smaller than the request lanes"};

@@ -13,6 +13,7 @@ constexpr u32 kLeaf = 0x80000000u;
 struct DInstance {
     float m[12];
     u32 vertex_begin, triangle_begin, triangle_count, material, reverse, emission, normal_begin, emitter_begin;
+    u32 inside_medium, outside_medium; // kNone = vacuum
 };
 // wire::Material subset (src/render_wire.h:107-130)
 struct DMaterial {
@@ -88,6 +89,11 @@ struct DeviceScene {
     float filter_x, filter_y;
     u32 max_depth, hero_mode;
     float slab_scale; // 1 + 2 gamma(3), the conservative far-plane factor
+    // homogeneous media (scalar transport): kMediumStride floats each -- sigma_a[471],
+    // sigma_s[471], emission[471], g
+    const float *media;
+    u32 medium_count, camera_medium;
+    u32 media_enabled; // any medium or null interface: shadow connections track media
 };
 
 RP_DEV V3 load3(const float *p) { return v3(__ldg(p), __ldg(p + 1), __ldg(p + 2)); }
@@ -104,6 +110,7 @@ RP_DEV V3 world_point(const DInstance &in, V3 p) {
 struct SurfacePoint {
     V3 position, error, geometric_normal, shading_normal;
     float inverse_area_pdf;
+    float world_extent;
 };
 // shaders/render.metal:865-868
 RP_DEV float triangle_extent(V3 e1, V3 e2) {
@@ -129,12 +136,14 @@ __device__ __noinline__ bool triangle_surface_point(const DeviceScene &s, u32 in
     if (n2 == 0.0f && !native_hit) {
         point.position = point.error = point.geometric_normal = point.shading_normal = v3(0, 0, 0);
         point.inverse_area_pdf = 0;
+        point.world_extent = 0;
         return true;
     }
     if (!(n2 > 0.0f) || !isfinite(n2))
         return false;
     const float nl = sqrtf(n2);
     point.inverse_area_pdf = 0.5f * nl;
+    point.world_extent = triangle_extent(we1, we2);
     point.geometric_normal = ce / nl;
     if (in.reverse)
         point.geometric_normal = -point.geometric_normal;

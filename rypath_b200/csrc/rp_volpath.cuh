@@ -1,0 +1,956 @@
+// Scalar (one-wavelength) path tracing with homogeneous media: the estimator of
+// rypath_render_paths (shaders/render.metal:2299-2371), which runs scalar_init / scalar_trace /
+// scalar_shade (shaders/scalar_transport.h) until each lane finishes.  The reference renders
+// participating media with this transport only (hero transport requires vacuum,
+// src/render.cpp:1579-1580).
+//
+// B200 form: one persistent kernel whose threads regenerate paths.  Every thread owns one
+// path in registers and runs one event (closest hit, then medium or surface interaction
+// with its light connection) per loop trip; a thread whose path finished takes the next
+// lane from a global counter (one atomic per warp), so warps stay full until the wave's
+// lanes run out instead of idling behind their longest path.  Results leave as one 16-byte
+// record per lane; the film reduction reads them in canonical order.
+//
+// Surfaces: diffuse reflectance and null interfaces (material scattering 10).  Lights: area
+// triangles, point and spot lights, constant environment.  Media: homogeneous, 471-bin
+// sigma_a / sigma_s / emission with a Henyey-Greenstein phase function.
+#pragma once
+
+#include "rp_kernels.cuh"
+
+namespace rp {
+
+constexpr u32 kMediumStride = 1416; // sigma_a[471], sigma_s[471], emission[471], g, 2 pad
+constexpr u32 kInterfaceScattering = 10;
+constexpr u32 kMediumBlockLimit = 0x20000000u;   // src/sampling_contract.h:45
+constexpr u32 kMediumStream = 0x6d656431u;       // medium_stream_v1
+enum : u32 {
+    S_SUCCESS = 0,
+    S_EMERGENCY = 1,
+    S_ARITHMETIC = 2,
+    S_HIT = 3,
+    S_BOUNDARY = 4,
+};
+
+RP_DEV float fnan() { return __int_as_float(0x7fffffff); }
+RP_DEV float finf() { return __int_as_float(0x7f800000); }
+RP_DEV V3 nan3() { return v3(fnan(), fnan(), fnan()); }
+
+// ------------------------------------------------------------------ shaders/medium.h
+// :11-17 three positive factors over a fourth without an intermediate range loss
+RP_DEV float product_ratio(float a, float b, float c, float d) {
+    if (a == 0 || b == 0 || c == 0)
+        return 0;
+    int ea, eb, ec, ed;
+    const float ma = frexpf(a, &ea), mb = frexpf(b, &eb), mc = frexpf(c, &ec), md = frexpf(d, &ed);
+    return ldexpf(((ma * mb) * mc) / md, ea + eb + ec - ed);
+}
+// :19-31 (1 - exp(-x)) / x, series near zero
+RP_DEV float attenuation_integral_ratio(float x) {
+    if (x <= 0.125f) {
+        float v = 1.0f / 40320.0f;
+        v = fmaf(v, -x, 1.0f / 5040.0f);
+        v = fmaf(v, -x, 1.0f / 720.0f);
+        v = fmaf(v, -x, 1.0f / 120.0f);
+        v = fmaf(v, -x, 1.0f / 24.0f);
+        v = fmaf(v, -x, 1.0f / 6.0f);
+        v = fmaf(v, -x, 0.5f);
+        return fmaf(v, -x, 1.0f);
+    }
+    return (1.0f - expf(-x)) / x;
+}
+struct Segment {
+    float transmission, emission;
+    bool valid;
+};
+// :32-57 Beer transmission and the absorbed-emission integral of one segment
+RP_DEV Segment medium_segment(float sa, float ss, float le, float distance) {
+    if (!isfinite(sa) || !isfinite(ss) || !isfinite(le) || sa < 0 || ss < 0 || le < 0 || isnan(distance) ||
+        distance < 0)
+        return {0, 0, false};
+    const float st = sa + ss;
+    if (!isfinite(st))
+        return {0, 0, false};
+    if (distance == 0 || st == 0)
+        return {1, 0, true};
+    const float depth = st * distance;
+    const float transmission = expf(-depth);
+    float emission = 0;
+    if (le > 0 && sa > 0) {
+        if (depth <= 0.125f) {
+            emission = product_ratio(le, sa, distance, 1.0f / attenuation_integral_ratio(depth));
+        } else {
+            const float loss = isinf(depth) ? 1.0f : 1.0f - transmission;
+            emission = product_ratio(le, sa, loss, st);
+        }
+    }
+    return {transmission, emission, isfinite(emission) && emission >= 0};
+}
+// :58-76 free-flight distance for extinction sigma_t
+RP_DEV float medium_flight(float st, float u) {
+    if (!isfinite(st) || st < 0 || !isfinite(u) || u < 0 || u > 1)
+        return fnan();
+    if (st == 0 || u == 1)
+        return finf();
+    if (u == 0)
+        return 0;
+    float depth;
+    if (u <= 0.125f) {
+        float v = 1.0f / 10.0f;
+#pragma unroll
+        for (int n = 9; n >= 2; --n)
+            v = fmaf(v, u, 1.0f / float(n));
+        depth = u * fmaf(v, u, 1.0f);
+    } else {
+        depth = -logf(1.0f - u);
+    }
+    return depth / st;
+}
+// :77-87 Henyey-Greenstein, both directions pointing away from the scattering point
+RP_DEV float hg_phase(V3 wo, V3 wi, float g) {
+    if (!finite3(wo) || !finite3(wi) || !isfinite(g) || fabsf(dot(wo, wo) - 1.0f) > 2e-5f ||
+        fabsf(dot(wi, wi) - 1.0f) > 2e-5f)
+        return fnan();
+    g = fminf(fmaxf(g, -0.99f), 0.99f);
+    const float cosine = fminf(fmaxf(dot(wo, wi), -1.0f), 1.0f);
+    const float base = 1.0f - fabsf(g);
+    const float denominator = fmaf(2.0f * fabsf(g), 1.0f + (g >= 0 ? cosine : -cosine), base * base);
+    return (1.0f / (4.0f * kPi)) * ((1.0f - g) * (1.0f + g)) / (denominator * sqrtf(denominator));
+}
+// :88-112 exact inverse CDF of HG about wo
+RP_DEV V3 hg_sample(V3 wo, float g, float ux, float uy) {
+    if (!finite3(wo) || !isfinite(g) || !isfinite(ux) || !isfinite(uy) || ux < 0 || uy < 0 || ux > 1 || uy > 1 ||
+        fabsf(dot(wo, wo) - 1.0f) > 2e-5f)
+        return nan3();
+    g = fminf(fmaxf(g, -0.99f), 0.99f);
+    const float h = fabsf(g), v = g < 0 ? 1.0f - ux : ux;
+    const float d = fmaf(h, 1.0f - 2.0f * v, 1.0f);
+    const float ratio = (1.0f - h) / d;
+    const float c = fminf(fmaxf(fmaf(2.0f * v * ratio * ratio, fmaf(h, 1.0f - v, 1.0f), -1.0f), -1.0f), 1.0f);
+    const float cosine = g < 0 ? -c : c;
+    const float sine = sqrtf(fmaxf(0.0f, (1.0f - cosine) * (1.0f + cosine)));
+    V3 x;
+    if (!unit(cross(fabsf(wo.z) < 0.9f ? v3(0, 0, 1) : v3(0, 1, 0), wo), x))
+        return nan3();
+    const V3 y = cross(wo, x);
+    const float phi = 2.0f * kPi * uy;
+    V3 r;
+    if (!unit(cosine * wo + sine * (cosf(phi) * x + sinf(phi) * y), r))
+        return nan3();
+    return r;
+}
+
+// ------------------------------------------------------------------ scalar helpers (shaders/render.metal)
+// :1901-1909 power heuristic with exponent two, scale-invariant
+RP_DEV float power_weight(float a, float b) {
+    const float scale = fmaxf(a, b);
+    if (!(scale > 0) || !isfinite(scale))
+        return fnan();
+    a /= scale;
+    b /= scale;
+    return a * a / (a * a + b * b);
+}
+// :843-847
+RP_DEV float bsdf_weight(float cosine) {
+    const float relative = 4.0f * cosine;
+    const float square = relative * relative;
+    return square / (1.0f + square);
+}
+// :828-835 cosine-weighted direction about n
+RP_DEV V3 cosine_hemisphere(V3 n, float u, float v) {
+    const float r = sqrtf(u);
+    const float phi = 2.0f * kPi * v;
+    const V3 axis = fabsf(n.z) < 0.999f ? v3(0, 0, 1) : v3(0, 1, 0);
+    const V3 t = normalize3(cross(axis, n));
+    const V3 b = cross(n, t);
+    return normalize3((r * cosf(phi)) * t + (r * sinf(phi)) * b + sqrtf(1.0f - u) * n);
+}
+// :1912-1929 (triangles): conservative offset of a hit along n, rounded outward
+RP_DEV V3 spawn_origin(V3 o, V3 d, float t, const SurfacePoint &pt, V3 n) {
+    const V3 ray_position = fma3(v3(t, t, t), d, o);
+    const V3 ray_error = gamma_bound(2.0f) * (vabs(t * d) + vabs(o));
+    const V3 error = (pt.error + vabs(pt.position - ray_position)) + ray_error;
+    return round_out(pt.position + dot(vabs(n), error) * n, n);
+}
+// :1931-1934
+RP_DEV V3 spawn_toward(V3 o, V3 d, float t, const SurfacePoint &pt, V3 direction) {
+    const V3 ng = pt.geometric_normal;
+    return spawn_origin(o, d, t, pt, dot(ng, direction) < 0.0f ? -ng : ng);
+}
+// :1939-1977 null-interface crossing anchored at the ray hit, with certified separation
+RP_DEV bool spawn_boundary(V3 o, V3 d, float t, const SurfacePoint &pt, V3 direction, V3 &origin) {
+    if (!(t >= 0) || !isfinite(t))
+        return false;
+    const V3 ng = pt.geometric_normal;
+    const V3 n = dot(ng, direction) < 0 ? -ng : ng;
+    const float facing = dot(n, direction);
+    if (!(facing > gamma_bound(5) * dot(vabs(n), vabs(direction))))
+        return false;
+    const V3 position = fma3(v3(t, t, t), d, o);
+    const V3 ray_error = gamma_bound(2) * (vabs(t * d) + vabs(o));
+    const V3 error = (pt.error + vabs(pt.position - position)) + ray_error;
+    const float norm_lower = dot(n, n) * (1 - gamma_bound(4));
+    const float height = dot(vabs(n), error) * (1 + gamma_bound(8)) / norm_lower;
+    origin = round_out(fma3(v3(height, height, height), n, position), n);
+    if (!(norm_lower > 0) || !isfinite(height) || !finite3(origin) || eq3(origin, o))
+        return false;
+    const V3 departure = origin - pt.position;
+    const float separation = dot(n, departure);
+    const float rounding = gamma_bound(5) * dot(vabs(n), vabs(departure));
+    const float uncertainty = dot(vabs(n), pt.error) * (1 + gamma_bound(4));
+    return isfinite(separation) && isfinite(rounding) && isfinite(uncertainty) && separation - rounding > uncertainty;
+}
+// :2221-2232 connection to a sampled area point, ending on its near side
+RP_DEV V3 shadow_segment_direction(V3 origin, V3 delta, const SurfacePoint &target, float signed_cosine) {
+    const V3 n = signed_cosine > 0.0f ? target.geometric_normal : -target.geometric_normal;
+    const float g7 = gamma_bound(7.0f) * target.world_extent;
+    const V3 error = (target.error + gamma_bound(2.0f) * (vabs(origin) + vabs(delta))) + v3(g7, g7, g7);
+    const V3 endpoint = round_out(target.position + dot(vabs(n), error) * n, n);
+    return endpoint - origin;
+}
+// :659-677
+RP_DEV bool point_direction(V3 from, V3 to, V3 &direction, float &distance_squared, bool spot) {
+    if (spot) {
+        if (!normal_or_zero(from.x) || !normal_or_zero(from.y) || !normal_or_zero(from.z) || !normal_or_zero(to.x) ||
+            !normal_or_zero(to.y) || !normal_or_zero(to.z))
+            return false;
+    }
+    const V3 delta = to - from;
+    distance_squared = dot(delta, delta);
+    if (!(distance_squared >= kFltMin) || !isfinite(distance_squared))
+        return false;
+    direction = delta / sqrtf(distance_squared);
+    if (spot) {
+        const float f[3] = {from.x, from.y, from.z}, tt[3] = {to.x, to.y, to.z}, dl[3] = {delta.x, delta.y, delta.z},
+                    dr[3] = {direction.x, direction.y, direction.z};
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            if ((f[i] != tt[i] && dl[i] == 0) || (dl[i] != 0 && dr[i] == 0) || !normal_or_zero(dr[i]))
+                return false;
+    }
+    return finite3(direction);
+}
+// :145-150
+RP_DEV u32 outgoing_medium(const DInstance &in, u32 current, V3 normal, V3 direction) {
+    return in.inside_medium == in.outside_medium ? current
+           : dot(normal, direction) > 0          ? in.outside_medium
+                                                 : in.inside_medium;
+}
+// :128-136 Philox stream of medium draws
+RP_DEV uint4 medium_words(const WaveParams &p, u32 pixel, u32 slo, u32 shi, u32 &draw) {
+    return philox(make_uint4(pixel, slo, shi, kMediumBlockLimit | draw++), p.seed_low, p.seed_high ^ kMediumStream);
+}
+RP_DEV const float *medium_record(const DeviceScene &s, u32 id) { return s.media + size_t(id) * kMediumStride; }
+
+// ------------------------------------------------------------------ scalar lights (shaders/scalar_lighting.h)
+enum : u32 { kIncidentArea = 0, kIncidentPositional = 1, kIncidentDistant = 2, kIncidentEnvironment = 3 };
+struct Incident {
+    V3 direction, endpoint;
+    SurfacePoint target;
+    float radiance, pdf;
+    u32 kind;
+    bool valid;
+};
+// :23-121 (area, point and spot lights; a constant environment offers no light sample)
+__device__ __noinline__ Incident scalar_light_sample(const DeviceScene &s, float wavelength, V3 position, V3 normal,
+                                                     float selection, float ux, float uy) {
+    Incident r;
+    r.direction = r.endpoint = v3(0, 0, 0);
+    r.target.position = r.target.error = r.target.geometric_normal = r.target.shading_normal = v3(0, 0, 0);
+    r.target.inverse_area_pdf = r.target.world_extent = 0;
+    r.radiance = r.pdf = 0;
+    r.kind = kIncidentEnvironment;
+    r.valid = true;
+    const Selected chosen = light_sample(s, position, normal, selection);
+    if (!(chosen.pmf > 0))
+        return r;
+    const u32 id = chosen.light;
+    if (id < s.emitter_count) {
+        r.kind = kIncidentArea;
+        float conditional = 0;
+        if (!light_geometry_sample(s, id, position, normal, ux, uy, r.target, conditional)) {
+            r.valid = false;
+            return r;
+        }
+        if (!(conditional > 0))
+            return r;
+        const V3 d = r.target.position - position;
+        const float d2 = dot(d, d);
+        if (!(d2 > 0))
+            return r;
+        r.direction = d / sqrtf(d2);
+        r.endpoint = r.target.position;
+        r.pdf = chosen.pmf * conditional;
+        const DInstance &in = s.instances[s.emitter_instance[id]];
+        const float cosine = dot(r.target.geometric_normal, -r.direction);
+        if (cosine == 0 || (!s.emission_two_sided[in.emission] && cosine < 0))
+            return r;
+        // area_radiance (shaders/render.metal:1811-1819)
+        r.radiance = r.target.inverse_area_pdf == 0 ? 0.0f : spectrum(s, in.emission * 471u, wavelength);
+    } else if (id < s.emitter_count + s.positional_count) {
+        r.kind = kIncidentPositional;
+        const DPositional &L = s.positional[id - s.emitter_count];
+        float intensity = spectrum(s, L.spectrum, wavelength);
+        if (intensity == 0)
+            return r;
+        r.endpoint = v3(L.position[0], L.position[1], L.position[2]);
+        float d2 = 0;
+        r.valid = point_direction(position, r.endpoint, r.direction, d2, L.kind != 0);
+        if (!r.valid)
+            return r;
+        r.valid = positional_intensity(L, r.direction, intensity);
+        r.radiance = intensity / d2;
+        r.pdf = chosen.pmf;
+    } else if (id == s.environment_light) {
+        return r;
+    } else {
+        r.valid = false;
+    }
+    r.valid = r.valid && isfinite(r.radiance) && r.radiance >= 0 && isfinite(r.pdf) && r.pdf >= 0;
+    return r;
+}
+RP_DEV bool incident_delta(const Incident &l) { return l.kind == kIncidentPositional || l.kind == kIncidentDistant; }
+
+struct Transmission {
+    float value;
+    u32 status;
+};
+// medium_connection (shaders/render.metal:1588-1677): transmittance of a light connection
+// through media and null interfaces, by ordered closest hits; any other surface blocks it.
+template <bool Count>
+__device__ __noinline__ Transmission medium_connection(const DeviceScene &s, float wavelength, V3 o, V3 d, float tmax,
+                                                       u32 medium, u32 boundary_limit, u32 *stack, u32 &rays,
+                                                       u32 &nodes, u32 &tris) {
+    const float length = length3(d);
+    if (!(length > 0) || !isfinite(length))
+        return {0, S_ARITHMETIC};
+    V3 direction = d / length;
+    float remaining = tmax * length;
+    const bool finite_connection = isfinite(tmax);
+    const V3 endpoint = finite_connection ? fma3(v3(tmax, tmax, tmax), d, o) : v3(0, 0, 0);
+    if (!(remaining > 0) || (finite_connection && (!isfinite(remaining) || !finite3(endpoint) || eq3(endpoint, o))))
+        return {0, S_ARITHMETIC};
+    float transmission = 1;
+    const u32 wi = dense_index(wavelength);
+    for (u32 crossings = 0;;) {
+        Hit h;
+        ++rays;
+        if (!trace_closest<Count>(s, o, direction, remaining, h, stack, kTraceBlock, nodes, tris))
+            return {0, S_HIT};
+        const bool miss = h.prim == kNone;
+        const float distance = miss ? remaining : h.t;
+        if (medium != kNone) {
+            const float *m = medium_record(s, medium);
+            const Segment seg = medium_segment(__ldg(m + wi), __ldg(m + 471 + wi), 0, distance);
+            if (!seg.valid)
+                return {0, S_ARITHMETIC};
+            transmission *= seg.transmission;
+        }
+        if (miss || transmission == 0)
+            return {transmission, S_SUCCESS};
+        if (!isfinite(h.t) || h.prim >= s.prim_count)
+            return {0, S_HIT};
+        const u32 inst = s.tri_instance[h.prim];
+        const DInstance &in = s.instances[inst];
+        if (in.material >= s.material_count)
+            return {0, S_HIT};
+        if (s.materials[in.material].scattering != kInterfaceScattering)
+            return {0, S_SUCCESS};
+        if (crossings++ >= boundary_limit)
+            return {0, S_BOUNDARY};
+        SurfacePoint pt;
+        if (!triangle_surface_point(s, inst, s.tri_local[h.prim], h.b1, h.b2, true, pt))
+            return {0, S_ARITHMETIC};
+        V3 next;
+        if (!spawn_boundary(o, direction, h.t, pt, direction, next))
+            return {0, S_ARITHMETIC};
+        const V3 outgoing_normal = dot(pt.geometric_normal, direction) < 0 ? -pt.geometric_normal : pt.geometric_normal;
+        if (finite_connection) {
+            const V3 delta = endpoint - next;
+            remaining = length3(delta);
+            if (!(remaining > 0) || !isfinite(remaining))
+                return {0, S_ARITHMETIC};
+            direction = delta / remaining;
+            const float facing = dot(outgoing_normal, direction);
+            const float facing_error = gamma_bound(5) * dot(vabs(outgoing_normal), vabs(direction));
+            if (!(facing > facing_error))
+                return {0, S_ARITHMETIC};
+        }
+        medium = outgoing_medium(in, medium, pt.geometric_normal, direction);
+        o = next;
+    }
+}
+
+// ------------------------------------------------------------------ path state
+// ScalarState (shaders/scalar_transport.h:38-52) held in registers for the life of a path.
+struct ScalarPath {
+    u32 lane, pixel, slo, shi, status, scatterings;
+    u64 index;
+    float wavelength, radiance;
+    V3 o, d;
+    float throughput, escape_weight, previous_bsdf_pdf;
+    bool previous_delta;
+    V3 prev_p, prev_n; // previous light-sampling context
+    float E;
+    u32 current_medium, medium_draw, boundary_crossings;
+};
+
+struct ScalarParams {
+    u32 boundary_limit;
+    uint4 *out;        // per lane: status, wavelength bits, radiance bits, scatterings
+    u32 *next_lane;    // regeneration counter
+    unsigned long long *stats; // closest [0] nodes, [1] triangles, [2] rays; connection [3] rays, [4] nodes, [5] triangles
+};
+
+// scalar_init (shaders/scalar_transport.h:64-77)
+RP_DEV void scalar_init(const DeviceScene &s, const WaveParams &p, u32 lane, ScalarPath &path) {
+    const BeginSample b = begin_sample(s, p, lane);
+    path.lane = lane;
+    path.pixel = b.pixel;
+    path.slo = b.sample_low;
+    path.shi = b.sample_high;
+    path.index = b.index;
+    path.status = S_SUCCESS;
+    path.scatterings = 0;
+    path.wavelength = 360.0f + 470.0f * sample_uniform(p, b.words.z);
+    path.radiance = 0;
+    primary_ray(s, p, b, path.o, path.d);
+    path.throughput = 1;
+    path.escape_weight = 1;
+    path.previous_bsdf_pdf = 0;
+    path.previous_delta = false;
+    path.prev_p = path.o;
+    path.prev_n = v3(0, 0, 0);
+    path.E = s.environment == kNone ? 0.0f : spectrum(s, s.environment, path.wavelength);
+    path.current_medium = s.camera_medium;
+    path.medium_draw = 0;
+    path.boundary_crossings = 0;
+}
+
+// scalar_sky_step (shaders/scalar_transport.h:88-210): scenes without geometry.  Light
+// selection shares the flight draw and phase sampling takes the next medium block.
+// Returns true when the path finished.
+RP_DEV bool scalar_sky_step(const DeviceScene &s, const WaveParams &p, ScalarPath &path) {
+    if (!finite3(path.o) || !finite3(path.d)) {
+        path.status = S_ARITHMETIC;
+        return true;
+    }
+    if (s.camera_medium != kNone) {
+        const float *m = medium_record(s, s.camera_medium);
+        const u32 wi = dense_index(path.wavelength);
+        const float a = __ldg(m + wi), sc = __ldg(m + 471 + wi), total = a + sc;
+        if (total > 0) {
+            const Segment seg = medium_segment(a, sc, __ldg(m + 942 + wi), finf());
+            if (!seg.valid) {
+                path.status = S_ARITHMETIC;
+                return true;
+            }
+            if (path.scatterings < s.max_depth)
+                path.radiance += path.throughput * seg.emission;
+            if (path.scatterings >= s.max_depth || sc == 0)
+                return true;
+            if (path.scatterings >= p.emergency_limit) {
+                path.status = S_EMERGENCY;
+                return true;
+            }
+            const uint4 flight_words = medium_words(p, path.pixel, path.slo, path.shi, path.medium_draw);
+            const float distance = medium_flight(total, u01(flight_words.x));
+            const V3 point = fma3(v3(distance, distance, distance), path.d, path.o);
+            if (!isfinite(distance) || !finite3(point)) {
+                path.status = S_ARITHMETIC;
+                return true;
+            }
+            path.throughput *= sc / total;
+            const float g = __ldg(m + 1413);
+            const Selected chosen = light_sample(s, point, v3(0, 0, 0), u01(flight_words.y));
+            if (chosen.pmf > 0) {
+                V3 direction = v3(0, 0, 0);
+                float radiance = 0, distance_to_light = 0;
+                if (chosen.light >= s.emitter_count && chosen.light < s.emitter_count + s.positional_count) {
+                    const DPositional &L = s.positional[chosen.light - s.emitter_count];
+                    float d2 = 0, intensity = spectrum(s, L.spectrum, path.wavelength);
+                    if (intensity != 0) {
+                        if (!point_direction(point, v3(L.position[0], L.position[1], L.position[2]), direction, d2,
+                                             L.kind != 0) ||
+                            !positional_intensity(L, direction, intensity)) {
+                            path.status = S_ARITHMETIC;
+                            return true;
+                        }
+                        radiance = intensity / d2;
+                        distance_to_light = sqrtf(d2);
+                    }
+                }
+                if (radiance > 0) {
+                    const float tr = expf(-total * distance_to_light);
+                    path.radiance += path.throughput * hg_phase(-path.d, direction, g) * (radiance / chosen.pmf) * tr;
+                }
+                if (!isfinite(path.radiance) || path.radiance < 0) {
+                    path.status = S_ARITHMETIC;
+                    return true;
+                }
+            }
+            const uint4 phase_words = medium_words(p, path.pixel, path.slo, path.shi, path.medium_draw);
+            const V3 wi = hg_sample(-path.d, g, u01(phase_words.x), u01(phase_words.y));
+            ++path.scatterings;
+            if (path.scatterings >= 3) {
+                if (phase_words.z >= 0xc0000000u)
+                    return true;
+                path.throughput /= .75f;
+            }
+            if (!finite3(wi) || !isfinite(path.throughput)) {
+                path.status = S_ARITHMETIC;
+                return true;
+            }
+            path.o = point;
+            path.d = wi;
+            return false;
+        }
+    }
+    path.radiance = path.E;
+    return true;
+}
+
+// One event: scalar_trace + scalar_shade (shaders/scalar_transport.h:213-900) for diffuse and
+// null-interface surfaces.  Returns true when the path finished.
+template <bool Count>
+__device__ __noinline__ bool scalar_event(const DeviceScene &s, const WaveParams &p, const ScalarParams &q,
+                                          ScalarPath &path, u32 *stack, u32 *counts) {
+    if (s.instance_count == 0)
+        return scalar_sky_step(s, p, path);
+    // scalar_trace
+    if (!finite3(path.o) || !finite3(path.d) || !isfinite(path.throughput) || !isfinite(path.radiance)) {
+        path.status = S_ARITHMETIC;
+        return true;
+    }
+    Hit hit;
+    ++counts[2];
+    if (!trace_closest<Count>(s, path.o, path.d, finf(), hit, stack, kTraceBlock, counts[0], counts[1])) {
+        path.status = S_HIT;
+        return true;
+    }
+    const bool miss = hit.prim == kNone;
+    // medium interaction (:354-420)
+    if (path.current_medium != kNone) {
+        if (path.current_medium >= s.medium_count) {
+            path.status = S_HIT;
+            return true;
+        }
+        if (path.medium_draw >= kMediumBlockLimit - 3) {
+            path.status = S_BOUNDARY;
+            return true;
+        }
+        const float *m = medium_record(s, path.current_medium);
+        const u32 wi = dense_index(path.wavelength);
+        const float a = __ldg(m + wi), sc = __ldg(m + 471 + wi), total = a + sc;
+        const float ray_length = length3(path.d);
+        const float distance = miss ? finf() : hit.t * ray_length;
+        const Segment seg =
+            medium_segment(a, sc, path.scatterings < s.max_depth ? __ldg(m + 942 + wi) : 0.0f, distance);
+        if (!seg.valid || !(ray_length > 0) || !isfinite(ray_length)) {
+            path.status = S_ARITHMETIC;
+            return true;
+        }
+        path.radiance += path.throughput * seg.emission;
+        if (total > 0) {
+            const uint4 flight_words = medium_words(p, path.pixel, path.slo, path.shi, path.medium_draw);
+            const float flight = medium_flight(total, u01(flight_words.x));
+            if (flight < distance || isinf(distance)) {
+                if (!isfinite(flight)) {
+                    path.status = S_ARITHMETIC;
+                    return true;
+                }
+                if (path.scatterings >= s.max_depth || sc == 0)
+                    return true;
+                if (path.scatterings >= p.emergency_limit) {
+                    path.status = S_EMERGENCY;
+                    return true;
+                }
+                const V3 direction = path.d / ray_length;
+                const V3 position = fma3(v3(flight, flight, flight), direction, path.o);
+                if (!finite3(position)) {
+                    path.status = S_ARITHMETIC;
+                    return true;
+                }
+                path.throughput *= sc / total;
+                const uint4 light_words = medium_words(p, path.pixel, path.slo, path.shi, path.medium_draw);
+                const uint4 phase_words = medium_words(p, path.pixel, path.slo, path.shi, path.medium_draw);
+                const float g = __ldg(m + 1413);
+                // medium_direct (shaders/render.metal:2237-2260)
+                {
+                    const Incident light = scalar_light_sample(s, path.wavelength, position, v3(0, 0, 0),
+                                                               u01(light_words.x), u01(light_words.y),
+                                                               u01(light_words.z));
+                    if (!light.valid) {
+                        path.status = S_ARITHMETIC;
+                        return true;
+                    }
+                    if (light.pdf > 0 && light.radiance != 0) {
+                        V3 cd;
+                        if (light.kind == kIncidentArea) {
+                            const V3 delta = light.target.position - position;
+                            cd = shadow_segment_direction(position, delta, light.target,
+                                                          dot(light.target.geometric_normal, -delta));
+                        } else {
+                            cd = light.endpoint - position;
+                        }
+                        const Transmission tr = medium_connection<Count>(s, path.wavelength, position, cd, kOneMinusEps,
+                                                                         path.current_medium, q.boundary_limit, stack,
+                                                                         counts[3], counts[4], counts[5]);
+                        if (tr.status != S_SUCCESS) {
+                            path.status = tr.status;
+                            return true;
+                        }
+                        const float phase = hg_phase(-direction, light.direction, g);
+                        const float weight = incident_delta(light) ? 1.f : power_weight(light.pdf, phase);
+                        const float value = (phase / light.pdf) * weight * light.radiance * tr.value;
+                        if (!isfinite(value) || !(value >= 0)) {
+                            path.status = S_ARITHMETIC;
+                            return true;
+                        }
+                        path.radiance += path.throughput * value;
+                    }
+                }
+                const V3 wi_dir = hg_sample(-direction, g, u01(phase_words.x), u01(phase_words.y));
+                path.previous_bsdf_pdf = hg_phase(-direction, wi_dir, g);
+                if (!finite3(wi_dir) || !(path.previous_bsdf_pdf > 0) || !isfinite(path.previous_bsdf_pdf)) {
+                    path.status = S_ARITHMETIC;
+                    return true;
+                }
+                ++path.scatterings;
+                if (path.scatterings >= 3) {
+                    if (phase_words.z >= 0xc0000000u)
+                        return true;
+                    path.throughput /= .75f;
+                }
+                path.previous_delta = false;
+                path.prev_p = position;
+                path.prev_n = v3(0, 0, 0);
+                path.escape_weight = 1;
+                path.o = position;
+                path.d = wi_dir;
+                path.boundary_crossings = 0;
+                return false;
+            }
+        }
+    }
+    if (miss) {
+        // escape (:421-433): a constant environment has no light-sampling density
+        if (path.scatterings != 0u && !path.previous_delta)
+            path.escape_weight = power_weight(path.previous_bsdf_pdf, 0.0f);
+        path.radiance += path.throughput * path.escape_weight * path.E;
+        return true;
+    }
+    const u32 bounce = path.scatterings;
+    if (!isfinite(hit.t) || hit.prim >= s.prim_count) {
+        path.status = S_HIT;
+        return true;
+    }
+    const u32 inst = s.tri_instance[hit.prim], local = s.tri_local[hit.prim];
+    const DInstance &instance = s.instances[inst];
+    if (instance.material >= s.material_count || !isfinite(hit.b1) || !isfinite(hit.b2)) {
+        path.status = S_HIT;
+        return true;
+    }
+    const DMaterial material = s.materials[instance.material];
+    SurfacePoint point;
+    if (material.scattering == kInterfaceScattering) {
+        // null interface (:450-472): change media, no scattering event
+        if (path.boundary_crossings++ >= q.boundary_limit) {
+            path.status = S_BOUNDARY;
+            return true;
+        }
+        if (!triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point)) {
+            path.status = S_ARITHMETIC;
+            return true;
+        }
+        path.current_medium = outgoing_medium(instance, path.current_medium, point.geometric_normal, path.d);
+        V3 origin;
+        if (!spawn_boundary(path.o, path.d, hit.t, point, path.d, origin)) {
+            path.status = S_ARITHMETIC;
+            return true;
+        }
+        path.o = origin;
+        return false;
+    }
+    const bool emissive = instance.emission != kNone;
+    if (emissive) {
+        // area emission with MIS against the light sampler (:473-520)
+        if (!triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point)) {
+            path.status = S_ARITHMETIC;
+            return true;
+        }
+        const float Le = point.inverse_area_pdf == 0 ? 0.0f : spectrum(s, instance.emission * 471u, path.wavelength);
+        if (Le > 0.0f && (s.emission_two_sided[instance.emission] || dot(point.geometric_normal, -path.d) >= 0.0f)) {
+            float weight = 1.0f;
+            if (bounce != 0u && !path.previous_delta) {
+                const u32 light_id = instance.emitter_begin + local;
+                if (light_id >= s.emitter_count) {
+                    path.status = S_HIT;
+                    return true;
+                }
+                const float pdf = light_pmf(s, path.prev_p, path.prev_n, light_id) *
+                                  light_geometry_pdf(s, light_id, path.prev_p, path.prev_n, point);
+                weight = power_weight(path.previous_bsdf_pdf, pdf);
+            }
+            if (!isfinite(weight)) {
+                path.status = S_ARITHMETIC;
+                return true;
+            }
+            path.radiance += path.throughput * (weight * Le);
+        }
+    }
+    if (bounce >= s.max_depth)
+        return true;
+    float rho = 0;
+    if (material.scattering != 0) {
+        path.status = S_HIT; // microfacet surfaces are not built for the scalar transport
+        return true;
+    }
+    if (material.kind == 0 && material.knot_count >= 2 && material.knot_begin <= s.knot_count &&
+        material.knot_count <= s.knot_count - material.knot_begin) {
+        rho = pbrt_reflectance(s.knots + material.knot_begin, material.knot_count, path.wavelength);
+    } else if (material.kind == 1) {
+        rho = material.scalar_value;
+    } else if (material.kind == 4) {
+        rho = blackbody_reflectance(material.scalar_value, path.wavelength);
+    } else {
+        path.status = S_HIT;
+        return true;
+    }
+    if (!isfinite(rho) || !(rho >= 0.0f && rho <= 1.0f)) {
+        path.status = S_ARITHMETIC;
+        return true;
+    }
+    if (rho == 0.0f)
+        return true;
+    const bool authored_normals = instance.normal_begin != kNone;
+    if (!authored_normals && bounce >= p.emergency_limit) {
+        path.status = S_EMERGENCY;
+        return true;
+    }
+    if (!emissive && !triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point)) {
+        path.status = S_ARITHMETIC;
+        return true;
+    }
+    const float incident_cosine = dot(point.shading_normal, path.d);
+    if (authored_normals && incident_cosine == 0.0f)
+        return true;
+    if (bounce >= p.emergency_limit) {
+        path.status = S_EMERGENCY;
+        return true;
+    }
+    const V3 n = incident_cosine > 0.0f ? -point.shading_normal : point.shading_normal;
+    const bool directional_offset = authored_normals;
+    const V3 area_reference = directional_offset ? point.position : spawn_origin(path.o, path.d, hit.t, point, n);
+    if (!finite3(area_reference)) {
+        path.status = S_ARITHMETIC;
+        return true;
+    }
+    const uint4 light_words = draw_words(s, p, path.pixel, path.slo, path.shi, path.index, 2 + 2 * bounce);
+    const uint4 bsdf_words = draw_words(s, p, path.pixel, path.slo, path.shi, path.index, 1 + 2 * bounce);
+    // light sample with power-heuristic MIS (:705-835)
+    {
+        const Incident light = scalar_light_sample(s, path.wavelength, point.position, point.shading_normal,
+                                                   sample_uniform(p, light_words.x), sample_uniform(p, light_words.y),
+                                                   sample_uniform(p, light_words.z));
+        if (!light.valid) {
+            path.status = S_ARITHMETIC;
+            return true;
+        }
+        if (light.pdf > 0 && light.radiance > 0) {
+            const float cosine = dot(n, light.direction);
+            if (cosine > 0) {
+                const float f_cos = rho * cosine / kPi;
+                const float bsdf_pdf = cosine / kPi;
+                // scattering_direct (shaders/render.metal:2212-2219)
+                float factor;
+                if (!(f_cos >= 0) || !(bsdf_pdf >= 0) || !(light.pdf > 0) || !isfinite(f_cos) || !isfinite(bsdf_pdf) ||
+                    !isfinite(light.pdf))
+                    factor = fnan();
+                else if (f_cos == 0)
+                    factor = 0;
+                else
+                    factor = (f_cos / light.pdf) * (incident_delta(light) ? 1.0f : power_weight(light.pdf, bsdf_pdf));
+                const V3 origin = directional_offset ? spawn_toward(path.o, path.d, hit.t, point, light.direction)
+                                                     : area_reference;
+                V3 cd;
+                if (light.kind == kIncidentArea) {
+                    const V3 delta = light.target.position - origin;
+                    cd = shadow_segment_direction(origin, delta, light.target, dot(light.target.geometric_normal, -delta));
+                } else {
+                    cd = light.endpoint - origin;
+                }
+                if (!isfinite(factor) || !finite3(cd) || !(dot(cd, light.direction) > 0)) {
+                    path.status = S_ARITHMETIC;
+                    return true;
+                }
+                Transmission vis;
+                const u32 medium = outgoing_medium(instance, path.current_medium, point.geometric_normal, light.direction);
+                if (s.media_enabled) {
+                    vis = medium_connection<Count>(s, path.wavelength, origin, cd, kOneMinusEps, medium, q.boundary_limit,
+                                                   stack, counts[3], counts[4], counts[5]);
+                } else {
+                    bool occluded = false;
+                    ++counts[3];
+                    const bool ok = trace_any<Count>(s, origin, cd, kOneMinusEps, occluded, stack, kTraceBlock, counts[4],
+                                                     counts[5]);
+                    vis = {occluded ? 0.0f : 1.0f, ok ? S_SUCCESS : S_ARITHMETIC};
+                }
+                if (vis.status != S_SUCCESS) {
+                    path.status = vis.status;
+                    return true;
+                }
+                path.radiance += path.throughput * factor * light.radiance * vis.value;
+            }
+        }
+    }
+    // continuation (:837-900)
+    const V3 wi = cosine_hemisphere(n, sample_uniform(p, bsdf_words.x), sample_uniform(p, bsdf_words.y));
+    path.throughput *= rho;
+    if (!isfinite(path.throughput) || path.throughput < 0.0f) {
+        path.status = S_ARITHMETIC;
+        return true;
+    }
+    ++path.scatterings;
+    if (path.scatterings >= 3) {
+        if (bsdf_words.z >= 0xc0000000u)
+            return true;
+        path.throughput /= 0.75f;
+        if (!isfinite(path.throughput)) {
+            path.status = S_ARITHMETIC;
+            return true;
+        }
+    }
+    const float cosine = dot(n, wi);
+    if (!(cosine > 0.0f)) {
+        path.status = S_ARITHMETIC;
+        return true;
+    }
+    path.previous_bsdf_pdf = cosine / kPi;
+    path.previous_delta = false;
+    path.prev_p = point.position;
+    path.prev_n = point.shading_normal;
+    path.escape_weight = bsdf_weight(cosine);
+    const V3 origin = directional_offset ? spawn_toward(path.o, path.d, hit.t, point, wi) : area_reference;
+    if (!finite3(origin)) {
+        path.status = S_ARITHMETIC;
+        return true;
+    }
+    path.o = origin;
+    path.d = wi;
+    path.current_medium = outgoing_medium(instance, path.current_medium, point.geometric_normal, wi);
+    path.boundary_crossings = 0;
+    return false;
+}
+
+// scalar_finish (shaders/scalar_transport.h:79-84)
+RP_DEV uint4 scalar_record(const ScalarPath &path) {
+    u32 status = path.status;
+    if (status == S_SUCCESS && (!isfinite(path.radiance) || path.radiance < 0.0f))
+        status = S_ARITHMETIC;
+    return make_uint4(status, __float_as_uint(path.wavelength), __float_as_uint(path.radiance), path.scatterings);
+}
+
+// Persistent path-regeneration kernel over the lanes of one wave.
+template <bool Count>
+__global__ void __launch_bounds__(kTraceBlock) k_volpath(const __grid_constant__ DeviceScene s,
+                                                         const __grid_constant__ WaveParams p, ScalarParams q) {
+    __shared__ u32 stack[kStackDepth * kTraceBlock];
+    u32 *my_stack = stack + threadIdx.x;
+    const int lane_in_warp = threadIdx.x & 31;
+    u32 counts[6] = {0, 0, 0, 0, 0, 0};
+    ScalarPath path;
+    bool active = false;
+    bool exhausted = false; // the wave's lanes are all taken
+    // Each trip runs at most one event per thread; a thread whose path finished first takes
+    // a new lane.  Every lane is taken exactly once, so the loop ends when all are done.
+    while (true) {
+        if (!exhausted) {
+            const u32 want = __ballot_sync(0xffffffffu, !active);
+            u32 base = 0;
+            if (lane_in_warp == 0 && want)
+                base = atomicAdd(q.next_lane, __popc(want));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (!active) {
+                const u32 lane = base + __popc(want & ((1u << lane_in_warp) - 1));
+                if (lane < p.lanes) {
+                    scalar_init(s, p, lane, path);
+                    active = true;
+                }
+            }
+            exhausted = base + __popc(want) >= p.lanes;
+        }
+        if (!__any_sync(0xffffffffu, active))
+            break;
+        if (active && scalar_event<Count>(s, p, q, path, my_stack, counts)) {
+            q.out[path.lane] = scalar_record(path);
+            active = false;
+        }
+    }
+    if (Count) {
+        atomicAdd(q.stats + 0, (unsigned long long)counts[0]);
+        atomicAdd(q.stats + 1, (unsigned long long)counts[1]);
+        atomicAdd(q.stats + 2, (unsigned long long)counts[2]);
+        atomicAdd(q.stats + 3, (unsigned long long)counts[3]);
+        atomicAdd(q.stats + 4, (unsigned long long)counts[4]);
+        atomicAdd(q.stats + 5, (unsigned long long)counts[5]);
+    }
+}
+
+// RenderSample rows for the driver-compatible scalar entry point (src/metal_render.mm:2136-2166).
+struct ScalarResult {
+    u32 status, pixel, sample_low, sample_high;
+    float wavelength, radiance;
+    u32 scatterings;
+    u32 random_words[4];
+};
+__global__ void k_scalar_results(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p,
+                                 const uint4 *records, ScalarResult *out) {
+    for (u32 lane = blockIdx.x * blockDim.x + threadIdx.x; lane < p.lanes; lane += gridDim.x * blockDim.x) {
+        const BeginSample b = begin_sample(s, p, lane);
+        const uint4 r = records[lane];
+        ScalarResult o;
+        o.status = r.x;
+        o.pixel = b.pixel;
+        o.sample_low = b.sample_low;
+        o.sample_high = b.sample_high;
+        o.wavelength = __uint_as_float(r.y);
+        o.radiance = __uint_as_float(r.z);
+        o.scatterings = r.w;
+        o.random_words[0] = b.words.x;
+        o.random_words[1] = b.words.y;
+        o.random_words[2] = b.words.z;
+        o.random_words[3] = b.words.w;
+        out[lane] = o;
+    }
+}
+
+// FilmBatch::add for scalar samples (src/render.cpp:2355-2385): XYZ = CIE(round(lambda)) *
+// 470 * L, FP64 Neumaier sums per pixel in canonical (absolute sample, pixel) order.
+__global__ void k_scalar_film(const uint4 *records, u32 pixel_count, u32 samples, const double *cie, FilmPixel *film,
+                              u32 *failures) {
+    for (u32 px = blockIdx.x * blockDim.x + threadIdx.x; px < pixel_count; px += gridDim.x * blockDim.x) {
+        FilmPixel f = film[px];
+        for (u32 si = 0; si < samples; ++si) {
+            const uint4 r = records[size_t(si) * pixel_count + px];
+            const float w = __uint_as_float(r.y), L = __uint_as_float(r.z);
+            if (r.x != 0 || !(w >= 360 && w <= 830) || !isfinite(L) || L < 0) {
+                atomicAdd(failures, 1u);
+                continue;
+            }
+            const u32 row = u32(round(double(w)) - 360.0);
+            const double weighted = __dmul_rn(470.0, double(L));
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const double v = __dmul_rn(__ldg(cie + 3 * row + c), weighted);
+                add_compensated(v, f.sum[c], f.correction[c]);
+                f.square[c] = __dadd_rn(f.square[c], __dmul_rn(v, v));
+            }
+            add_compensated(1.0, f.weight_sum, f.weight_correction);
+            ++f.count;
+        }
+        film[px] = f;
+    }
+}
+
+} // namespace rp

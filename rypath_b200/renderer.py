@@ -5,7 +5,9 @@ Names and meanings follow the reference (src/metal_render.hpp:14-95, src/render_
 * ``build_renderer(scene)`` ~ ``build_metal_renderer(RenderScene, ...)`` -> ``RenderBuildResult``
   with ``status``, ``diagnostic`` and ``scene`` (a ``CudaRenderScene``).
 * ``CudaRenderScene.sample(request)`` ~ ``MetalRenderScene::sample(RenderRequest)`` ->
-  ``RenderSamplesResult`` whose ``packet_samples`` are the 80-byte packet results in lane order.
+  ``RenderSamplesResult`` whose ``packet_samples`` are the 80-byte packet results in lane order;
+  ``sample_scalar(request)`` the same for scalar-transport (media) scenes, whose ``samples``
+  are RenderSample rows (src/metal_render.mm:2136-2166).
 * ``render_progressive(scene, settings)`` ~ the driver loop of src/render_driver.cpp:166-275 with
   the packet film reduction performed on the device.
 
@@ -54,6 +56,7 @@ class RenderSamplesResult:
     status: int = abi.RP_FAILURE
     diagnostic: str = ""
     packet_samples: np.ndarray | None = None
+    samples: np.ndarray | None = None  # scalar transport: RenderSample rows (abi.scalar_dtype)
 
 
 @dataclass
@@ -100,6 +103,15 @@ class CudaRenderScene:
         diag = C.create_string_buffer(512)
         st = native.lib().rp_cuda_sample(self._handle, C.byref(q), out.ctypes.data, lanes, diag, 512)
         return RenderSamplesResult(st, diag.value.decode(errors="replace"), out)
+
+    def sample_scalar(self, request: RenderRequest) -> RenderSamplesResult:
+        """Scalar-transport lanes (``samples``): scenes built with ``transport=TRANSPORT_SCALAR``."""
+        q = request.to_c()
+        lanes = q.pixel_count * q.sample_count
+        out = np.zeros(lanes, abi.scalar_dtype())
+        diag = C.create_string_buffer(512)
+        st = native.lib().rp_cuda_sample_scalar(self._handle, C.byref(q), out.ctypes.data, lanes, diag, 512)
+        return RenderSamplesResult(st, diag.value.decode(errors="replace"), None, out)
 
     def sample_device(self, request: RenderRequest, device_ptr: int, capacity: int, stream: int = 0) -> int:
         q = request.to_c()

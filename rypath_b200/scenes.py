@@ -83,6 +83,10 @@ class Scene:
     light_sampler: int = abi.LIGHTS_BVH
     hero_wavelengths: int = abi.HERO_VISIBLE
     normals: np.ndarray | None = None
+    # homogeneous media (scalar transport): dicts of sigma_a, sigma_s, emission (471 each), g
+    media: list = field(default_factory=list)
+    camera_medium: int = abi.RP_NONE
+    transport: int = abi.TRANSPORT_HERO
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -137,7 +141,15 @@ class Scene:
         keep.append(pl)
         d.positional_count = len(self.positional)
         d.positional = C.cast(pl, C.POINTER(abi.PositionalLight))
-        d.camera_medium = abi.RP_NONE
+        md = (abi.Medium * max(1, len(self.media)))()
+        for i, m in enumerate(self.media):
+            for name in ("sigma_a", "sigma_s", "emission"):
+                getattr(md[i], name)[:] = [float(v) for v in np.broadcast_to(np.asarray(m.get(name, 0.0), np.float32),
+                                                                             (471,))]
+            md[i].g = float(m.get("g", 0.0))
+        keep.append(md)
+        d.medium_count, d.media = len(self.media), C.cast(md, C.POINTER(abi.Medium))
+        d.camera_medium = self.camera_medium
         if self.environment is not None:
             d.environment = arr(np.asarray(self.environment, np.float32), C.c_float)
         o, corner, dx, dy = self.camera
@@ -149,7 +161,7 @@ class Scene:
         d.filter_x_radius, d.filter_y_radius = self.filter_radius
         d.max_depth = self.max_depth
         d.light_sampler = self.light_sampler
-        d.transport = abi.TRANSPORT_HERO
+        d.transport = self.transport
         d.hero_wavelengths = self.hero_wavelengths
         tables = C.create_string_buffer(sobol_tables(), abi.RP_SOBOL_TABLE_BYTES)
         keep.append(tables)
@@ -247,6 +259,71 @@ def cornell_box(width=256, height=256, spp=64, max_depth=8) -> Scene:
     scene = Scene("cornell_box", width, height, spp, positions, triangles, instances, materials, knots,
                   emissions=[(light, False)], max_depth=max_depth)
     scene.camera = pinhole_camera((0, 1, 3.94), (0, 1, 0), (0, 1, 0), 40.0, width, height)
+    return scene
+
+
+def cornell_fog(width=1024, height=1024, spp=64, max_depth=32, sigma_s_mean=0.5, albedo=0.9, g=0.7) -> Scene:
+    """The Cornell-style box filled with a homogeneous medium, rendered by the scalar transport.
+
+    The box interior is closed at the open front by a null interface quad (inside: the medium,
+    outside: vacuum), so camera rays enter the medium there.  sigma_s ramps linearly over the
+    spectrum around its mean (+-20%), sigma_a = sigma_s (1 - albedo) / albedo, HG asymmetry g.
+    """
+    scene = cornell_box(width, height, spp, max_depth)
+    scene.name = "cornell_fog"
+    sigma_s = sigma_s_mean * (1.0 + 0.2 * np.linspace(-1.0, 1.0, 471))
+    sigma_a = sigma_s * (1.0 - albedo) / albedo
+    scene.media = [dict(sigma_a=sigma_a.astype(np.float32), sigma_s=sigma_s.astype(np.float32), emission=0.0, g=g)]
+    # front interface: the plane z = 1 over the box opening, normal +z (towards the camera)
+    verts, tris = _quad((-1, 0, 1), (1, 0, 1), (1, 2, 1), (-1, 2, 1))
+    interface = abi.Material()
+    interface.scattering, interface.kind = abi.INTERFACE, abi.REFLECTANCE_CONSTANT
+    scene.materials.append(interface)
+    inst = identity_instance(scene.positions.shape[0], scene.triangles.shape[0], 2, len(scene.materials) - 1)
+    inst.inside_medium, inst.outside_medium = 0, abi.RP_NONE
+    scene.instances.append(inst)
+    # every other surface keeps the medium on both sides: inside == outside (no change)
+    scene.positions = np.concatenate([scene.positions, verts])
+    scene.triangles = np.concatenate([scene.triangles, tris])
+    scene.transport = abi.TRANSPORT_SCALAR
+    return scene
+
+
+def slab_scene(media, planes, camera_medium=abi.RP_NONE, environment=1.0, max_depth=1, materials=None,
+               positional=None) -> Scene:
+    """Analytic medium scenes in the style of rypath's medium tests (tests/medium_render_tests.cpp:24-85).
+
+    A 1x1 film looks along +z from the origin through a nearly collimated camera; each plane is
+    a 32x32 quad at z with its normal along +z (positive) or -z, bounding media through
+    (inside, outside) medium ids, with material 0 the null interface unless given.
+    """
+    positions, triangles, instances = [], [], []
+    mats = [abi.Material()]
+    mats[0].scattering, mats[0].kind = abi.INTERFACE, abi.REFLECTANCE_CONSTANT
+    for m in materials or []:
+        mats.append(m)
+    for plane in planes:
+        z, positive = plane["z"], plane["positive"]
+        inside, outside = plane.get("media", (abi.RP_NONE, abi.RP_NONE))
+        v = np.array([[-16, -16, z], [16, -16, z], [16, 16, z], [-16, 16, z]], np.float32)
+        t = np.array([[0, 1, 2], [0, 2, 3]] if positive else [[0, 2, 1], [0, 3, 2]], np.uint32)
+        inst = identity_instance(sum(len(p) for p in positions), sum(len(x) for x in triangles), 2,
+                                 plane.get("material", 0), plane.get("emission", abi.RP_NONE))
+        inst.inside_medium, inst.outside_medium = inside, outside
+        inst.reverse_orientation = int(plane.get("reverse", False))
+        if "matrix" in plane:
+            inst.matrix[:] = list(plane["matrix"])
+        positions.append(v)
+        triangles.append(t)
+        instances.append(inst)
+    scene = Scene("slab", 1, 1, 1, np.concatenate(positions) if positions else np.zeros((0, 3), np.float32),
+                  np.concatenate(triangles) if triangles else np.zeros((0, 3), np.uint32), instances, mats,
+                  environment=np.full(471, environment, np.float32), max_depth=max_depth)
+    scene.camera = ((0.0, 0.0, 0.0), (-1e-7, -1e-7, 1.0), (2e-7, 0.0, 0.0), (0.0, 2e-7, 0.0))
+    scene.media = media
+    scene.camera_medium = camera_medium
+    scene.positional = positional or []
+    scene.transport = abi.TRANSPORT_SCALAR
     return scene
 
 

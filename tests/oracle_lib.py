@@ -41,6 +41,9 @@ def oracle():
         lib.or_build_light_tables.argtypes = [vp, u32, vp, vp, vp, vp, vp]
         lib.or_probe_light_select.argtypes = [vp, vp, u32, vp]
         lib.or_film_add.argtypes = [vp, sz, vp, u32, vp]
+        lib.or_sample_scalar.argtypes = [vp, C.POINTER(abi.Request), vp, sz, C.c_int]
+        lib.or_probe_medium.argtypes = [vp, u32, vp]
+        lib.or_scalar_film_add.argtypes = [vp, sz, vp, u32, vp]
         _oracle = lib
     return _oracle
 
@@ -65,6 +68,7 @@ def reference():
         lib.ref_outward.restype = u32
         lib.ref_set_cie.argtypes = [vp]
         lib.ref_film_add.argtypes = [vp, sz, u32, u32, vp]
+        lib.ref_probe_medium.argtypes = [vp, u32, vp]
         _ref = lib
     return _ref
 
@@ -92,6 +96,16 @@ class OracleScene:
         rc = oracle().or_sample(self.handle, C.byref(request), out.ctypes.data, lanes, threads)
         if rc < 0:
             raise RuntimeError("oracle sample rejected the request")
+        return out
+
+    def sample_scalar(self, request, threads=0):
+        import numpy as np
+
+        lanes = request.pixel_count * request.sample_count
+        out = np.zeros(lanes, abi.scalar_dtype())
+        rc = oracle().or_sample_scalar(self.handle, C.byref(request), out.ctypes.data, lanes, threads)
+        if rc < 0:
+            raise RuntimeError("oracle scalar sample rejected the request")
         return out
 
 
