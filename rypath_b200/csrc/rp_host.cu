@@ -358,6 +358,8 @@ struct rp_scene {
     u32 transport = RP_TRANSPORT_HERO;
     // scalar transport: one 16-byte record per lane, regeneration and failure counters
     uint4 *scalar_records = nullptr;
+    float4 *scalar_fresh_ray = nullptr;
+    uint2 *scalar_fresh_index = nullptr;
     u32 *scalar_counters = nullptr;
     u32 scalar_capacity = 0;
     int volpath_blocks = 0; // resident persistent blocks per SM
@@ -430,10 +432,14 @@ struct rp_scene {
             cudaFreeAsync(scalar_records, stream);
         scalar_records = nullptr;
         scalar_capacity = 0;
-        const size_t bytes = size_t(lanes) * sizeof(uint4) + 256;
+        // records (16 B), raygen directions and wavelengths (16 B), Sobol indices (8 B), counters
+        const size_t n = size_t(lanes);
+        const size_t bytes = n * 16 + n * 16 + ((n * 8 + 255) & ~size_t(255)) + 256;
         RP_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&scalar_records), bytes, stream));
-        scalar_counters = reinterpret_cast<u32 *>(reinterpret_cast<unsigned char *>(scalar_records) +
-                                                  size_t(lanes) * sizeof(uint4));
+        unsigned char *base = reinterpret_cast<unsigned char *>(scalar_records);
+        scalar_fresh_ray = reinterpret_cast<float4 *>(base + n * 16);
+        scalar_fresh_index = reinterpret_cast<uint2 *>(base + n * 32);
+        scalar_counters = reinterpret_cast<u32 *>(base + n * 32 + ((n * 8 + 255) & ~size_t(255)));
         scalar_capacity = lanes;
     }
 
@@ -567,10 +573,14 @@ void run_scalar_wave(rp_scene *s, const WaveParams &p, u32 boundary_limit) {
     }
     s->mark(3);
     RP_CHECK(cudaMemsetAsync(s->scalar_counters, 0, 64, s->stream));
+    k_scalar_raygen<<<grid_for(s->sm_count, p.lanes, 256, 16), 256, 0, s->stream>>>(s->ds, p, s->scalar_fresh_ray,
+                                                                                     s->scalar_fresh_index);
     s->done();
     ScalarParams q;
     q.boundary_limit = boundary_limit;
     q.out = s->scalar_records;
+    q.fresh_ray = s->scalar_fresh_ray;
+    q.fresh_index = s->scalar_fresh_index;
     q.next_lane = s->scalar_counters;
     q.stats = s->stats;
     const u32 blocks_needed = (p.lanes + kTraceBlock - 1) / kTraceBlock;

@@ -311,75 +311,6 @@ __device__ __noinline__ Incident scalar_light_sample(const DeviceScene &s, float
 }
 RP_DEV bool incident_delta(const Incident &l) { return l.kind == kIncidentPositional || l.kind == kIncidentDistant; }
 
-struct Transmission {
-    float value;
-    u32 status;
-};
-// medium_connection (shaders/render.metal:1588-1677): transmittance of a light connection
-// through media and null interfaces, by ordered closest hits; any other surface blocks it.
-template <bool Count>
-__device__ __noinline__ Transmission medium_connection(const DeviceScene &s, float wavelength, V3 o, V3 d, float tmax,
-                                                       u32 medium, u32 boundary_limit, u32 *stack, u32 &rays,
-                                                       u32 &nodes, u32 &tris) {
-    const float length = length3(d);
-    if (!(length > 0) || !isfinite(length))
-        return {0, S_ARITHMETIC};
-    V3 direction = d / length;
-    float remaining = tmax * length;
-    const bool finite_connection = isfinite(tmax);
-    const V3 endpoint = finite_connection ? fma3(v3(tmax, tmax, tmax), d, o) : v3(0, 0, 0);
-    if (!(remaining > 0) || (finite_connection && (!isfinite(remaining) || !finite3(endpoint) || eq3(endpoint, o))))
-        return {0, S_ARITHMETIC};
-    float transmission = 1;
-    const u32 wi = dense_index(wavelength);
-    for (u32 crossings = 0;;) {
-        Hit h;
-        ++rays;
-        if (!trace_closest<Count>(s, o, direction, remaining, h, stack, kTraceBlock, nodes, tris))
-            return {0, S_HIT};
-        const bool miss = h.prim == kNone;
-        const float distance = miss ? remaining : h.t;
-        if (medium != kNone) {
-            const float *m = medium_record(s, medium);
-            const Segment seg = medium_segment(__ldg(m + wi), __ldg(m + 471 + wi), 0, distance);
-            if (!seg.valid)
-                return {0, S_ARITHMETIC};
-            transmission *= seg.transmission;
-        }
-        if (miss || transmission == 0)
-            return {transmission, S_SUCCESS};
-        if (!isfinite(h.t) || h.prim >= s.prim_count)
-            return {0, S_HIT};
-        const u32 inst = s.tri_instance[h.prim];
-        const DInstance &in = s.instances[inst];
-        if (in.material >= s.material_count)
-            return {0, S_HIT};
-        if (s.materials[in.material].scattering != kInterfaceScattering)
-            return {0, S_SUCCESS};
-        if (crossings++ >= boundary_limit)
-            return {0, S_BOUNDARY};
-        SurfacePoint pt;
-        if (!triangle_surface_point(s, inst, s.tri_local[h.prim], h.b1, h.b2, true, pt))
-            return {0, S_ARITHMETIC};
-        V3 next;
-        if (!spawn_boundary(o, direction, h.t, pt, direction, next))
-            return {0, S_ARITHMETIC};
-        const V3 outgoing_normal = dot(pt.geometric_normal, direction) < 0 ? -pt.geometric_normal : pt.geometric_normal;
-        if (finite_connection) {
-            const V3 delta = endpoint - next;
-            remaining = length3(delta);
-            if (!(remaining > 0) || !isfinite(remaining))
-                return {0, S_ARITHMETIC};
-            direction = delta / remaining;
-            const float facing = dot(outgoing_normal, direction);
-            const float facing_error = gamma_bound(5) * dot(vabs(outgoing_normal), vabs(direction));
-            if (!(facing > facing_error))
-                return {0, S_ARITHMETIC};
-        }
-        medium = outgoing_medium(in, medium, pt.geometric_normal, direction);
-        o = next;
-    }
-}
 
 // ------------------------------------------------------------------ path state
 // ScalarState (shaders/scalar_transport.h:38-52) held in registers for the life of a path.
@@ -391,46 +322,81 @@ struct ScalarPath {
     float throughput, escape_weight, previous_bsdf_pdf;
     bool previous_delta;
     V3 prev_p, prev_n; // previous light-sampling context
-    float E;
     u32 current_medium, medium_draw, boundary_crossings;
+};
+
+// What a path does once its pending light connection resolves.
+enum : u32 { kAfterContinue = 0, kAfterFinish = 1, kAfterFail = 2 /* + status << 8 */ };
+
+// A light connection in flight: medium_connection (shaders/render.metal:1588-1677) one leg per
+// trace, or visible_shadow (:1570-1576) in scenes without media.  It carries the contribution
+// it adds when it resolves with transmittance T: a surface sample adds a * T, a medium sample
+// checks value = a * T and adds b * value (shaders/render.metal:2237-2260).
+struct Connection {
+    V3 o, d;         // current leg; d is a unit vector except for the vacuum query
+    float remaining; // leg length (world), or the parametric limit of the vacuum query
+    V3 end;
+    float T;
+    u32 medium, crossings, after;
+    bool finite_end, vacuum, medium_sample;
+    float a, b;
 };
 
 struct ScalarParams {
     u32 boundary_limit;
-    uint4 *out;        // per lane: status, wavelength bits, radiance bits, scatterings
-    u32 *next_lane;    // regeneration counter
+    uint4 *out;               // per lane: status, wavelength bits, radiance bits, scatterings
+    const float4 *fresh_ray;  // per lane: primary direction, wavelength
+    const uint2 *fresh_index; // per lane: Sobol index
+    u32 *next_lane;           // regeneration counter
     unsigned long long *stats; // closest [0] nodes, [1] triangles, [2] rays; connection [3] rays, [4] nodes, [5] triangles
 };
 
-// scalar_init (shaders/scalar_transport.h:64-77)
-RP_DEV void scalar_init(const DeviceScene &s, const WaveParams &p, u32 lane, ScalarPath &path) {
-    const BeginSample b = begin_sample(s, p, lane);
+// begin_sample + primary_ray + the wavelength of scalar_init (shaders/scalar_transport.h:64-77)
+// for every lane of a wave, written once so the persistent kernel starts paths with loads.
+__global__ void k_scalar_raygen(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p,
+                                float4 *ray, uint2 *index) {
+    for (u32 lane = blockIdx.x * blockDim.x + threadIdx.x; lane < p.lanes; lane += gridDim.x * blockDim.x) {
+        const BeginSample b = begin_sample(s, p, lane);
+        V3 o, d;
+        primary_ray(s, p, b, o, d);
+        ray[lane] = make_float4(d.x, d.y, d.z, 360.0f + 470.0f * sample_uniform(p, b.words.z));
+        index[lane] = make_uint2(u32(b.index), u32(b.index >> 32));
+    }
+}
+
+// scalar_init (shaders/scalar_transport.h:64-77) from the raygen records
+RP_DEV void scalar_start(const DeviceScene &s, const WaveParams &p, const ScalarParams &q, u32 lane, ScalarPath &path) {
     path.lane = lane;
-    path.pixel = b.pixel;
-    path.slo = b.sample_low;
-    path.shi = b.sample_high;
-    path.index = b.index;
+    path.pixel = p.pixel_begin + lane % p.pixel_count;
+    path.slo = p.sample_low + lane / p.pixel_count;
+    path.shi = p.sample_high + u32(path.slo < p.sample_low);
+    const float4 r = q.fresh_ray[lane];
+    const uint2 ix = q.fresh_index[lane];
+    path.index = (u64(ix.y) << 32) | ix.x;
     path.status = S_SUCCESS;
     path.scatterings = 0;
-    path.wavelength = 360.0f + 470.0f * sample_uniform(p, b.words.z);
+    path.wavelength = r.w;
     path.radiance = 0;
-    primary_ray(s, p, b, path.o, path.d);
+    path.o = s.origin;
+    path.d = v3(r.x, r.y, r.z);
     path.throughput = 1;
     path.escape_weight = 1;
     path.previous_bsdf_pdf = 0;
     path.previous_delta = false;
     path.prev_p = path.o;
     path.prev_n = v3(0, 0, 0);
-    path.E = s.environment == kNone ? 0.0f : spectrum(s, s.environment, path.wavelength);
     path.current_medium = s.camera_medium;
     path.medium_draw = 0;
     path.boundary_crossings = 0;
+}
+RP_DEV float environment_radiance(const DeviceScene &s, float wavelength) {
+    return s.environment == kNone ? 0.0f : spectrum(s, s.environment, wavelength);
 }
 
 // scalar_sky_step (shaders/scalar_transport.h:88-210): scenes without geometry.  Light
 // selection shares the flight draw and phase sampling takes the next medium block.
 // Returns true when the path finished.
-RP_DEV bool scalar_sky_step(const DeviceScene &s, const WaveParams &p, ScalarPath &path) {
+__device__ __noinline__ bool scalar_sky_step(const DeviceScene &s, const WaveParams &p, ScalarPath &path) {
     if (!finite3(path.o) || !finite3(path.d)) {
         path.status = S_ARITHMETIC;
         return true;
@@ -506,38 +472,153 @@ RP_DEV bool scalar_sky_step(const DeviceScene &s, const WaveParams &p, ScalarPat
             return false;
         }
     }
-    path.radiance = path.E;
+    path.radiance = environment_radiance(s, path.wavelength);
     return true;
 }
 
-// One event: scalar_trace + scalar_shade (shaders/scalar_transport.h:213-900) for diffuse and
-// null-interface surfaces.  Returns true when the path finished.
-template <bool Count>
-__device__ __noinline__ bool scalar_event(const DeviceScene &s, const WaveParams &p, const ScalarParams &q,
-                                          ScalarPath &path, u32 *stack, u32 *counts) {
-    if (s.instance_count == 0)
-        return scalar_sky_step(s, p, path);
-    // scalar_trace
-    if (!finite3(path.o) || !finite3(path.d) || !isfinite(path.throughput) || !isfinite(path.radiance)) {
-        path.status = S_ARITHMETIC;
-        return true;
+// The prologue of medium_connection (shaders/render.metal:1593-1606): false on an invalid
+// connection, which fails the sample with invalid arithmetic.
+RP_DEV bool connection_begin(V3 o, V3 d, float tmax, u32 medium, Connection &c) {
+    const float length = length3(d);
+    if (!(length > 0) || !isfinite(length))
+        return false;
+    c.d = d / length;
+    c.remaining = tmax * length;
+    c.finite_end = isfinite(tmax);
+    c.end = c.finite_end ? fma3(v3(tmax, tmax, tmax), d, o) : v3(0, 0, 0);
+    if (!(c.remaining > 0) || (c.finite_end && (!isfinite(c.remaining) || !finite3(c.end) || eq3(c.end, o))))
+        return false;
+    c.o = o;
+    c.T = 1;
+    c.medium = medium;
+    c.crossings = 0;
+    c.vacuum = false;
+    return true;
+}
+
+enum : int { kEventPath = 0, kEventFinished = 1, kEventConnect = 2 };
+
+// Apply what the path does after its connection (or directly, when it made none).
+RP_DEV int apply_after(ScalarPath &path, u32 after) {
+    if (after == kAfterContinue)
+        return kEventPath;
+    if (after != kAfterFinish)
+        path.status = after >> 8;
+    return kEventFinished;
+}
+
+// One connection leg after its closest hit.  Returns kEventConnect while legs remain.
+RP_DEV int connection_step(const DeviceScene &s, const ScalarParams &q, ScalarPath &path, Connection &c, bool ok,
+                           const Hit &h) {
+    float T;
+    if (c.vacuum) {
+        // visible_shadow: any hit occludes; a failed query is invalid arithmetic
+        if (!ok) {
+            path.status = S_ARITHMETIC;
+            return kEventFinished;
+        }
+        T = h.prim == kNone ? 1.0f : 0.0f;
+    } else {
+        if (!ok) {
+            path.status = S_HIT;
+            return kEventFinished;
+        }
+        const bool miss = h.prim == kNone;
+        const float distance = miss ? c.remaining : h.t;
+        if (c.medium != kNone) {
+            const float *m = medium_record(s, c.medium);
+            const u32 wi = dense_index(path.wavelength);
+            const Segment seg = medium_segment(__ldg(m + wi), __ldg(m + 471 + wi), 0, distance);
+            if (!seg.valid) {
+                path.status = S_ARITHMETIC;
+                return kEventFinished;
+            }
+            c.T *= seg.transmission;
+        }
+        T = c.T;
+        if (!(miss || T == 0)) {
+            if (!isfinite(h.t) || h.prim >= s.prim_count) {
+                path.status = S_HIT;
+                return kEventFinished;
+            }
+            const u32 inst = s.tri_instance[h.prim];
+            const DInstance &in = s.instances[inst];
+            if (in.material >= s.material_count) {
+                path.status = S_HIT;
+                return kEventFinished;
+            }
+            if (s.materials[in.material].scattering != kInterfaceScattering) {
+                T = 0;
+            } else {
+                // cross the null interface and continue towards the endpoint
+                if (c.crossings++ >= q.boundary_limit) {
+                    path.status = S_BOUNDARY;
+                    return kEventFinished;
+                }
+                SurfacePoint pt;
+                V3 next;
+                if (!triangle_surface_point(s, inst, s.tri_local[h.prim], h.b1, h.b2, true, pt) ||
+                    !spawn_boundary(c.o, c.d, h.t, pt, c.d, next)) {
+                    path.status = S_ARITHMETIC;
+                    return kEventFinished;
+                }
+                const V3 outgoing_normal =
+                    dot(pt.geometric_normal, c.d) < 0 ? -pt.geometric_normal : pt.geometric_normal;
+                if (c.finite_end) {
+                    const V3 delta = c.end - next;
+                    c.remaining = length3(delta);
+                    if (!(c.remaining > 0) || !isfinite(c.remaining)) {
+                        path.status = S_ARITHMETIC;
+                        return kEventFinished;
+                    }
+                    c.d = delta / c.remaining;
+                    const float facing = dot(outgoing_normal, c.d);
+                    const float facing_error = gamma_bound(5) * dot(vabs(outgoing_normal), vabs(c.d));
+                    if (!(facing > facing_error)) {
+                        path.status = S_ARITHMETIC;
+                        return kEventFinished;
+                    }
+                }
+                c.medium = outgoing_medium(in, c.medium, pt.geometric_normal, c.d);
+                c.o = next;
+                return kEventConnect;
+            }
+        }
     }
-    Hit hit;
-    ++counts[2];
-    if (!trace_closest<Count>(s, path.o, path.d, finf(), hit, stack, kTraceBlock, counts[0], counts[1])) {
+    // resolved with transmittance T
+    if (c.medium_sample) {
+        const float value = c.a * T;
+        if (!isfinite(value) || !(value >= 0)) {
+            path.status = S_ARITHMETIC;
+            return kEventFinished;
+        }
+        path.radiance += c.b * value;
+    } else {
+        path.radiance += c.a * T;
+    }
+    return apply_after(path, c.after);
+}
+
+// One event after the path ray's closest hit: scalar_shade (shaders/scalar_transport.h:286-900)
+// for diffuse surfaces and null interfaces.  A light sample that needs a connection leaves it in
+// `c` (returning kEventConnect) after the continuation has been sampled: the two use disjoint
+// draws, and the connection's contribution and status are applied before the continuation's.
+RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarParams &q, ScalarPath &path, bool ok,
+                       const Hit &hit, Connection &c) {
+    if (!ok) {
         path.status = S_HIT;
-        return true;
+        return kEventFinished;
     }
     const bool miss = hit.prim == kNone;
     // medium interaction (:354-420)
     if (path.current_medium != kNone) {
         if (path.current_medium >= s.medium_count) {
             path.status = S_HIT;
-            return true;
+            return kEventFinished;
         }
         if (path.medium_draw >= kMediumBlockLimit - 3) {
             path.status = S_BOUNDARY;
-            return true;
+            return kEventFinished;
         }
         const float *m = medium_record(s, path.current_medium);
         const u32 wi = dense_index(path.wavelength);
@@ -548,7 +629,7 @@ __device__ __noinline__ bool scalar_event(const DeviceScene &s, const WaveParams
             medium_segment(a, sc, path.scatterings < s.max_depth ? __ldg(m + 942 + wi) : 0.0f, distance);
         if (!seg.valid || !(ray_length > 0) || !isfinite(ray_length)) {
             path.status = S_ARITHMETIC;
-            return true;
+            return kEventFinished;
         }
         path.radiance += path.throughput * seg.emission;
         if (total > 0) {
@@ -557,79 +638,80 @@ __device__ __noinline__ bool scalar_event(const DeviceScene &s, const WaveParams
             if (flight < distance || isinf(distance)) {
                 if (!isfinite(flight)) {
                     path.status = S_ARITHMETIC;
-                    return true;
+                    return kEventFinished;
                 }
                 if (path.scatterings >= s.max_depth || sc == 0)
-                    return true;
+                    return kEventFinished;
                 if (path.scatterings >= p.emergency_limit) {
                     path.status = S_EMERGENCY;
-                    return true;
+                    return kEventFinished;
                 }
                 const V3 direction = path.d / ray_length;
                 const V3 position = fma3(v3(flight, flight, flight), direction, path.o);
                 if (!finite3(position)) {
                     path.status = S_ARITHMETIC;
-                    return true;
+                    return kEventFinished;
                 }
                 path.throughput *= sc / total;
                 const uint4 light_words = medium_words(p, path.pixel, path.slo, path.shi, path.medium_draw);
                 const uint4 phase_words = medium_words(p, path.pixel, path.slo, path.shi, path.medium_draw);
                 const float g = __ldg(m + 1413);
                 // medium_direct (shaders/render.metal:2237-2260)
-                {
-                    const Incident light = scalar_light_sample(s, path.wavelength, position, v3(0, 0, 0),
-                                                               u01(light_words.x), u01(light_words.y),
-                                                               u01(light_words.z));
-                    if (!light.valid) {
-                        path.status = S_ARITHMETIC;
-                        return true;
-                    }
-                    if (light.pdf > 0 && light.radiance != 0) {
-                        V3 cd;
-                        if (light.kind == kIncidentArea) {
-                            const V3 delta = light.target.position - position;
-                            cd = shadow_segment_direction(position, delta, light.target,
-                                                          dot(light.target.geometric_normal, -delta));
-                        } else {
-                            cd = light.endpoint - position;
-                        }
-                        const Transmission tr = medium_connection<Count>(s, path.wavelength, position, cd, kOneMinusEps,
-                                                                         path.current_medium, q.boundary_limit, stack,
-                                                                         counts[3], counts[4], counts[5]);
-                        if (tr.status != S_SUCCESS) {
-                            path.status = tr.status;
-                            return true;
-                        }
-                        const float phase = hg_phase(-direction, light.direction, g);
-                        const float weight = incident_delta(light) ? 1.f : power_weight(light.pdf, phase);
-                        const float value = (phase / light.pdf) * weight * light.radiance * tr.value;
-                        if (!isfinite(value) || !(value >= 0)) {
-                            path.status = S_ARITHMETIC;
-                            return true;
-                        }
-                        path.radiance += path.throughput * value;
-                    }
-                }
-                const V3 wi_dir = hg_sample(-direction, g, u01(phase_words.x), u01(phase_words.y));
-                path.previous_bsdf_pdf = hg_phase(-direction, wi_dir, g);
-                if (!finite3(wi_dir) || !(path.previous_bsdf_pdf > 0) || !isfinite(path.previous_bsdf_pdf)) {
+                const Incident light = scalar_light_sample(s, path.wavelength, position, v3(0, 0, 0),
+                                                           u01(light_words.x), u01(light_words.y), u01(light_words.z));
+                if (!light.valid) {
                     path.status = S_ARITHMETIC;
-                    return true;
+                    return kEventFinished;
                 }
-                ++path.scatterings;
-                if (path.scatterings >= 3) {
-                    if (phase_words.z >= 0xc0000000u)
-                        return true;
-                    path.throughput /= .75f;
+                bool connect = false;
+                if (light.pdf > 0 && light.radiance != 0) {
+                    V3 cd;
+                    if (light.kind == kIncidentArea) {
+                        const V3 delta = light.target.position - position;
+                        cd = shadow_segment_direction(position, delta, light.target,
+                                                      dot(light.target.geometric_normal, -delta));
+                    } else {
+                        cd = light.endpoint - position;
+                    }
+                    if (!connection_begin(position, cd, kOneMinusEps, path.current_medium, c)) {
+                        path.status = S_ARITHMETIC;
+                        return kEventFinished;
+                    }
+                    const float phase = hg_phase(-direction, light.direction, g);
+                    const float weight = incident_delta(light) ? 1.f : power_weight(light.pdf, phase);
+                    c.medium_sample = true;
+                    c.a = ((phase / light.pdf) * weight) * light.radiance;
+                    c.b = path.throughput;
+                    connect = true;
                 }
-                path.previous_delta = false;
-                path.prev_p = position;
-                path.prev_n = v3(0, 0, 0);
-                path.escape_weight = 1;
-                path.o = position;
-                path.d = wi_dir;
-                path.boundary_crossings = 0;
-                return false;
+                // phase continuation and roulette
+                u32 after = kAfterContinue;
+                const V3 wi_dir = hg_sample(-direction, g, u01(phase_words.x), u01(phase_words.y));
+                const float pdf = hg_phase(-direction, wi_dir, g);
+                if (!finite3(wi_dir) || !(pdf > 0) || !isfinite(pdf)) {
+                    after = kAfterFail | (S_ARITHMETIC << 8);
+                } else {
+                    path.previous_bsdf_pdf = pdf;
+                    ++path.scatterings;
+                    if (path.scatterings >= 3 && phase_words.z >= 0xc0000000u) {
+                        after = kAfterFinish;
+                    } else {
+                        if (path.scatterings >= 3)
+                            path.throughput /= .75f;
+                        path.previous_delta = false;
+                        path.prev_p = position;
+                        path.prev_n = v3(0, 0, 0);
+                        path.escape_weight = 1;
+                        path.o = position;
+                        path.d = wi_dir;
+                        path.boundary_crossings = 0;
+                    }
+                }
+                if (connect) {
+                    c.after = after;
+                    return kEventConnect;
+                }
+                return apply_after(path, after);
             }
         }
     }
@@ -637,19 +719,19 @@ __device__ __noinline__ bool scalar_event(const DeviceScene &s, const WaveParams
         // escape (:421-433): a constant environment has no light-sampling density
         if (path.scatterings != 0u && !path.previous_delta)
             path.escape_weight = power_weight(path.previous_bsdf_pdf, 0.0f);
-        path.radiance += path.throughput * path.escape_weight * path.E;
-        return true;
+        path.radiance += path.throughput * path.escape_weight * environment_radiance(s, path.wavelength);
+        return kEventFinished;
     }
     const u32 bounce = path.scatterings;
     if (!isfinite(hit.t) || hit.prim >= s.prim_count) {
         path.status = S_HIT;
-        return true;
+        return kEventFinished;
     }
     const u32 inst = s.tri_instance[hit.prim], local = s.tri_local[hit.prim];
     const DInstance &instance = s.instances[inst];
     if (instance.material >= s.material_count || !isfinite(hit.b1) || !isfinite(hit.b2)) {
         path.status = S_HIT;
-        return true;
+        return kEventFinished;
     }
     const DMaterial material = s.materials[instance.material];
     SurfacePoint point;
@@ -657,27 +739,27 @@ __device__ __noinline__ bool scalar_event(const DeviceScene &s, const WaveParams
         // null interface (:450-472): change media, no scattering event
         if (path.boundary_crossings++ >= q.boundary_limit) {
             path.status = S_BOUNDARY;
-            return true;
+            return kEventFinished;
         }
         if (!triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point)) {
             path.status = S_ARITHMETIC;
-            return true;
+            return kEventFinished;
         }
         path.current_medium = outgoing_medium(instance, path.current_medium, point.geometric_normal, path.d);
         V3 origin;
         if (!spawn_boundary(path.o, path.d, hit.t, point, path.d, origin)) {
             path.status = S_ARITHMETIC;
-            return true;
+            return kEventFinished;
         }
         path.o = origin;
-        return false;
+        return kEventPath;
     }
     const bool emissive = instance.emission != kNone;
     if (emissive) {
         // area emission with MIS against the light sampler (:473-520)
         if (!triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point)) {
             path.status = S_ARITHMETIC;
-            return true;
+            return kEventFinished;
         }
         const float Le = point.inverse_area_pdf == 0 ? 0.0f : spectrum(s, instance.emission * 471u, path.wavelength);
         if (Le > 0.0f && (s.emission_two_sided[instance.emission] || dot(point.geometric_normal, -path.d) >= 0.0f)) {
@@ -686,7 +768,7 @@ __device__ __noinline__ bool scalar_event(const DeviceScene &s, const WaveParams
                 const u32 light_id = instance.emitter_begin + local;
                 if (light_id >= s.emitter_count) {
                     path.status = S_HIT;
-                    return true;
+                    return kEventFinished;
                 }
                 const float pdf = light_pmf(s, path.prev_p, path.prev_n, light_id) *
                                   light_geometry_pdf(s, light_id, path.prev_p, path.prev_n, point);
@@ -694,17 +776,17 @@ __device__ __noinline__ bool scalar_event(const DeviceScene &s, const WaveParams
             }
             if (!isfinite(weight)) {
                 path.status = S_ARITHMETIC;
-                return true;
+                return kEventFinished;
             }
             path.radiance += path.throughput * (weight * Le);
         }
     }
     if (bounce >= s.max_depth)
-        return true;
+        return kEventFinished;
     float rho = 0;
     if (material.scattering != 0) {
         path.status = S_HIT; // microfacet surfaces are not built for the scalar transport
-        return true;
+        return kEventFinished;
     }
     if (material.kind == 0 && material.knot_count >= 2 && material.knot_begin <= s.knot_count &&
         material.knot_count <= s.knot_count - material.knot_begin) {
@@ -715,47 +797,48 @@ __device__ __noinline__ bool scalar_event(const DeviceScene &s, const WaveParams
         rho = blackbody_reflectance(material.scalar_value, path.wavelength);
     } else {
         path.status = S_HIT;
-        return true;
+        return kEventFinished;
     }
     if (!isfinite(rho) || !(rho >= 0.0f && rho <= 1.0f)) {
         path.status = S_ARITHMETIC;
-        return true;
+        return kEventFinished;
     }
     if (rho == 0.0f)
-        return true;
+        return kEventFinished;
     const bool authored_normals = instance.normal_begin != kNone;
     if (!authored_normals && bounce >= p.emergency_limit) {
         path.status = S_EMERGENCY;
-        return true;
+        return kEventFinished;
     }
     if (!emissive && !triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point)) {
         path.status = S_ARITHMETIC;
-        return true;
+        return kEventFinished;
     }
     const float incident_cosine = dot(point.shading_normal, path.d);
     if (authored_normals && incident_cosine == 0.0f)
-        return true;
+        return kEventFinished;
     if (bounce >= p.emergency_limit) {
         path.status = S_EMERGENCY;
-        return true;
+        return kEventFinished;
     }
     const V3 n = incident_cosine > 0.0f ? -point.shading_normal : point.shading_normal;
     const bool directional_offset = authored_normals;
     const V3 area_reference = directional_offset ? point.position : spawn_origin(path.o, path.d, hit.t, point, n);
     if (!finite3(area_reference)) {
         path.status = S_ARITHMETIC;
-        return true;
+        return kEventFinished;
     }
     const uint4 light_words = draw_words(s, p, path.pixel, path.slo, path.shi, path.index, 2 + 2 * bounce);
     const uint4 bsdf_words = draw_words(s, p, path.pixel, path.slo, path.shi, path.index, 1 + 2 * bounce);
-    // light sample with power-heuristic MIS (:705-835)
+    // light sample with power-heuristic MIS (:783-835)
+    bool connect = false;
     {
         const Incident light = scalar_light_sample(s, path.wavelength, point.position, point.shading_normal,
                                                    sample_uniform(p, light_words.x), sample_uniform(p, light_words.y),
                                                    sample_uniform(p, light_words.z));
         if (!light.valid) {
             path.status = S_ARITHMETIC;
-            return true;
+            return kEventFinished;
         }
         if (light.pdf > 0 && light.radiance > 0) {
             const float cosine = dot(n, light.direction);
@@ -782,65 +865,65 @@ __device__ __noinline__ bool scalar_event(const DeviceScene &s, const WaveParams
                 }
                 if (!isfinite(factor) || !finite3(cd) || !(dot(cd, light.direction) > 0)) {
                     path.status = S_ARITHMETIC;
-                    return true;
+                    return kEventFinished;
                 }
-                Transmission vis;
                 const u32 medium = outgoing_medium(instance, path.current_medium, point.geometric_normal, light.direction);
                 if (s.media_enabled) {
-                    vis = medium_connection<Count>(s, path.wavelength, origin, cd, kOneMinusEps, medium, q.boundary_limit,
-                                                   stack, counts[3], counts[4], counts[5]);
+                    if (!connection_begin(origin, cd, kOneMinusEps, medium, c)) {
+                        path.status = S_ARITHMETIC;
+                        return kEventFinished;
+                    }
                 } else {
-                    bool occluded = false;
-                    ++counts[3];
-                    const bool ok = trace_any<Count>(s, origin, cd, kOneMinusEps, occluded, stack, kTraceBlock, counts[4],
-                                                     counts[5]);
-                    vis = {occluded ? 0.0f : 1.0f, ok ? S_SUCCESS : S_ARITHMETIC};
+                    c.o = origin;
+                    c.d = cd;
+                    c.remaining = kOneMinusEps;
+                    c.vacuum = true;
                 }
-                if (vis.status != S_SUCCESS) {
-                    path.status = vis.status;
-                    return true;
-                }
-                path.radiance += path.throughput * factor * light.radiance * vis.value;
+                c.medium_sample = false;
+                c.a = (path.throughput * factor) * light.radiance;
+                connect = true;
             }
         }
     }
     // continuation (:837-900)
+    u32 after = kAfterContinue;
     const V3 wi = cosine_hemisphere(n, sample_uniform(p, bsdf_words.x), sample_uniform(p, bsdf_words.y));
     path.throughput *= rho;
     if (!isfinite(path.throughput) || path.throughput < 0.0f) {
-        path.status = S_ARITHMETIC;
-        return true;
-    }
-    ++path.scatterings;
-    if (path.scatterings >= 3) {
-        if (bsdf_words.z >= 0xc0000000u)
-            return true;
-        path.throughput /= 0.75f;
-        if (!isfinite(path.throughput)) {
-            path.status = S_ARITHMETIC;
-            return true;
+        after = kAfterFail | (S_ARITHMETIC << 8);
+    } else {
+        ++path.scatterings;
+        if (path.scatterings >= 3 && bsdf_words.z >= 0xc0000000u) {
+            after = kAfterFinish;
+        } else {
+            if (path.scatterings >= 3)
+                path.throughput /= 0.75f;
+            const float cosine = dot(n, wi);
+            if (!isfinite(path.throughput) || !(cosine > 0.0f)) {
+                after = kAfterFail | (S_ARITHMETIC << 8);
+            } else {
+                path.previous_bsdf_pdf = cosine / kPi;
+                path.previous_delta = false;
+                path.prev_p = point.position;
+                path.prev_n = point.shading_normal;
+                path.escape_weight = bsdf_weight(cosine);
+                const V3 origin = directional_offset ? spawn_toward(path.o, path.d, hit.t, point, wi) : area_reference;
+                if (!finite3(origin)) {
+                    after = kAfterFail | (S_ARITHMETIC << 8);
+                } else {
+                    path.o = origin;
+                    path.d = wi;
+                    path.current_medium = outgoing_medium(instance, path.current_medium, point.geometric_normal, wi);
+                    path.boundary_crossings = 0;
+                }
+            }
         }
     }
-    const float cosine = dot(n, wi);
-    if (!(cosine > 0.0f)) {
-        path.status = S_ARITHMETIC;
-        return true;
+    if (connect) {
+        c.after = after;
+        return kEventConnect;
     }
-    path.previous_bsdf_pdf = cosine / kPi;
-    path.previous_delta = false;
-    path.prev_p = point.position;
-    path.prev_n = point.shading_normal;
-    path.escape_weight = bsdf_weight(cosine);
-    const V3 origin = directional_offset ? spawn_toward(path.o, path.d, hit.t, point, wi) : area_reference;
-    if (!finite3(origin)) {
-        path.status = S_ARITHMETIC;
-        return true;
-    }
-    path.o = origin;
-    path.d = wi;
-    path.current_medium = outgoing_medium(instance, path.current_medium, point.geometric_normal, wi);
-    path.boundary_crossings = 0;
-    return false;
+    return apply_after(path, after);
 }
 
 // scalar_finish (shaders/scalar_transport.h:79-84)
@@ -851,7 +934,11 @@ RP_DEV uint4 scalar_record(const ScalarPath &path) {
     return make_uint4(status, __float_as_uint(path.wavelength), __float_as_uint(path.radiance), path.scatterings);
 }
 
-// Persistent path-regeneration kernel over the lanes of one wave.
+// Persistent path-regeneration kernel over the lanes of one wave.  Each trip of the loop
+// runs one closest-hit query per thread -- the path's ray or the current leg of its light
+// connection -- at a single call site, then the path event or the connection step.  A thread
+// whose path finished takes the next lane (one atomic per warp), so warps stay full until
+// the wave's lanes run out.
 template <bool Count>
 __global__ void __launch_bounds__(kTraceBlock) k_volpath(const __grid_constant__ DeviceScene s,
                                                          const __grid_constant__ WaveParams p, ScalarParams q) {
@@ -860,32 +947,71 @@ __global__ void __launch_bounds__(kTraceBlock) k_volpath(const __grid_constant__
     const int lane_in_warp = threadIdx.x & 31;
     u32 counts[6] = {0, 0, 0, 0, 0, 0};
     ScalarPath path;
-    bool active = false;
+    Connection c;
+    int mode = kEventFinished;
     bool exhausted = false; // the wave's lanes are all taken
-    // Each trip runs at most one event per thread; a thread whose path finished first takes
-    // a new lane.  Every lane is taken exactly once, so the loop ends when all are done.
     while (true) {
         if (!exhausted) {
-            const u32 want = __ballot_sync(0xffffffffu, !active);
+            const u32 want = __ballot_sync(0xffffffffu, mode == kEventFinished);
             u32 base = 0;
             if (lane_in_warp == 0 && want)
                 base = atomicAdd(q.next_lane, __popc(want));
             base = __shfl_sync(0xffffffffu, base, 0);
-            if (!active) {
+            if (mode == kEventFinished) {
                 const u32 lane = base + __popc(want & ((1u << lane_in_warp) - 1));
                 if (lane < p.lanes) {
-                    scalar_init(s, p, lane, path);
-                    active = true;
+                    scalar_start(s, p, q, lane, path);
+                    mode = kEventPath;
                 }
             }
             exhausted = base + __popc(want) >= p.lanes;
         }
-        if (!__any_sync(0xffffffffu, active))
+        if (!__any_sync(0xffffffffu, mode != kEventFinished))
             break;
-        if (active && scalar_event<Count>(s, p, q, path, my_stack, counts)) {
-            q.out[path.lane] = scalar_record(path);
-            active = false;
+        if (mode == kEventFinished)
+            continue;
+        if (s.instance_count == 0) {
+            if (scalar_sky_step(s, p, path)) {
+                q.out[path.lane] = scalar_record(path);
+                mode = kEventFinished;
+            }
+            continue;
         }
+        // scalar_trace (shaders/scalar_transport.h:268-283): validate, then the one query
+        V3 ro, rd;
+        float tmax;
+        if (mode == kEventPath) {
+            if (!finite3(path.o) || !finite3(path.d) || !isfinite(path.throughput) || !isfinite(path.radiance)) {
+                path.status = S_ARITHMETIC;
+                q.out[path.lane] = scalar_record(path);
+                mode = kEventFinished;
+                continue;
+            }
+            ro = path.o;
+            rd = path.d;
+            tmax = finf();
+        } else {
+            ro = c.o;
+            rd = c.d;
+            tmax = c.remaining;
+        }
+        Hit hit;
+        u32 nodes = 0, tris = 0;
+        const bool ok = trace_closest<Count>(s, ro, rd, tmax, hit, my_stack, kTraceBlock, nodes, tris);
+        if (Count) {
+            if (mode == kEventPath) {
+                counts[0] += nodes;
+                counts[1] += tris;
+                counts[2] += 1;
+            } else {
+                counts[3] += 1;
+                counts[4] += nodes;
+                counts[5] += tris;
+            }
+        }
+        mode = mode == kEventPath ? shade_event(s, p, q, path, ok, hit, c) : connection_step(s, q, path, c, ok, hit);
+        if (mode == kEventFinished)
+            q.out[path.lane] = scalar_record(path);
     }
     if (Count) {
         atomicAdd(q.stats + 0, (unsigned long long)counts[0]);
