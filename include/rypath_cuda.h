@@ -278,6 +278,51 @@ rp_status rp_cuda_render_film_device(struct rp_scene *scene, const rp_film_reque
  * src/render.cpp:2147-2152).  Required before the film entry points. */
 rp_status rp_cuda_set_cie(struct rp_scene *scene, const double *cie_xyz);
 
+/* ---- batched views ------------------------------------------------------------------- */
+
+/* One camera view of a batch: a PBRT raster camera, its film size, its absolute sample range
+ * and where its pixels start in the batch film.  Views share the scene (and its filter,
+ * depth, lights and materials). */
+typedef struct rp_view {
+    rp_camera camera;
+    uint32_t width, height;
+    uint64_t sample_begin, sample_count;
+    uint64_t film_offset; /* first rp_film_pixel of this view in the batch film */
+} rp_view;
+
+/* Batch execution: lanes per wave, block shapes and grid size of the wavefront kernels, and
+ * whether each wave replays a CUDA graph.  A zero field is picked by the autotuner. */
+typedef struct rp_batch_config {
+    uint32_t wave_lanes;    /* up to 2^23 */
+    uint32_t trace_block;   /* 64 or 128 threads (closest-hit and any-hit kernels) */
+    uint32_t shade_block;   /* 128 or 256 threads (shading kernels) */
+    uint32_t blocks_per_sm; /* resident blocks per SM the grids are sized for */
+    uint32_t use_graph;     /* 1: one CUDA graph replayed per wave; 2: direct launches */
+    float probe_ms_per_mlane; /* tuning: measured cost of the chosen configuration */
+} rp_batch_config;
+
+typedef struct rp_batch_request {
+    uint64_t seed;
+    uint32_t sampler_kind, randomization, emergency_limit;
+    rp_batch_config config;
+} rp_batch_request;
+
+/* Renders every view's samples into one device film (the views' pixels, in rp_film_pixel
+ * rows, accumulating onto what it holds), all views' lanes sharing one wavefront: the
+ * batched form of rp_cuda_render_film_device.  Each view's film equals a plain render of
+ * that view (same camera, size and samples) bit for bit.  `used` (optional) receives the
+ * configuration that ran.  A failed lane fails the call (the film is then partial).  No
+ * counterpart in rypath, which renders one view per job (src/render_driver.cpp:166-275). */
+rp_status rp_cuda_render_views_device(struct rp_scene *scene, const rp_view *views, uint32_t view_count,
+                                      const rp_batch_request *request, rp_film_pixel *device_film,
+                                      rp_batch_config *used, char *diag, size_t diag_capacity);
+/* The autotuner alone: times one probe wave of the batch per candidate configuration (wave
+ * size, then trace block, shade block and grid size, each with the others fixed) and
+ * returns the fastest.  Nonzero fields of request->config are kept as given. */
+rp_status rp_cuda_tune_views(struct rp_scene *scene, const rp_view *views, uint32_t view_count,
+                             const rp_batch_request *request, rp_batch_config *chosen, char *diag,
+                             size_t diag_capacity);
+
 /* ---- instrumentation ------------------------------------------------------------------ */
 
 /* Timing of the last sample/film call on this scene. */

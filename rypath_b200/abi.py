@@ -128,6 +128,21 @@ class FilmRequest(C.Structure):
                 ("randomization", u32), ("emergency_limit", u32)]
 
 
+class View(C.Structure):
+    _fields_ = [("camera", Camera), ("width", u32), ("height", u32), ("sample_begin", u64),
+                ("sample_count", u64), ("film_offset", u64)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("wave_lanes", u32), ("trace_block", u32), ("shade_block", u32), ("blocks_per_sm", u32),
+                ("use_graph", u32), ("probe_ms_per_mlane", f32)]
+
+
+class BatchRequest(C.Structure):
+    _fields_ = [("seed", u64), ("sampler_kind", u32), ("randomization", u32), ("emergency_limit", u32),
+                ("config", BatchConfig)]
+
+
 class Timing(C.Structure):
     _fields_ = [("total_ms", f64), ("trace_ms", f64), ("shadow_ms", f64), ("shade_ms", f64),
                 ("other_ms", f64), ("closest_rays", u64), ("shadow_rays", u64),
@@ -169,4 +184,5 @@ EXPECTED_SIZES = {
     "rp_medium": (Medium, 5656), "rp_camera": (Camera, 48), "rp_request": (Request, 56),
     "rp_packet_result": (PacketResult, 80), "rp_scalar_result": (ScalarResult, 44),
     "rp_film_pixel": (FilmPixel, 96), "rp_film_request": (FilmRequest, 56),
+    "rp_view": (View, 80), "rp_batch_config": (BatchConfig, 24), "rp_batch_request": (BatchRequest, 48),
 }

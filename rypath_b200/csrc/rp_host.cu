@@ -5,6 +5,7 @@
 #include "rp_build.cuh"
 #include "rp_probes.cuh"
 #include "rp_volpath.cuh"
+#include "rp_batch.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -753,6 +754,9 @@ uint32_t rp_cuda_abi_size(const char *name) {
     if (n == "rp_film_request") return sizeof(rp_film_request);
     if (n == "rp_timing") return sizeof(rp_timing);
     if (n == "rp_device_info") return sizeof(rp_device_info);
+    if (n == "rp_view") return sizeof(rp_view);
+    if (n == "rp_batch_config") return sizeof(rp_batch_config);
+    if (n == "rp_batch_request") return sizeof(rp_batch_request);
     return 0;
 }
 
@@ -1458,6 +1462,328 @@ rp_status rp_cuda_render_film(rp_scene *s, const rp_film_request *r, rp_film_pix
 }
 rp_status rp_cuda_render_film_device(rp_scene *s, const rp_film_request *r, rp_film_pixel *film, char *diag, size_t cap) {
     return film_impl(s, r, film, false, diag, cap);
+}
+
+// ---- batched views
+
+} // extern "C"
+
+namespace {
+
+struct BatchPlan {
+    std::vector<DView> views;
+    std::vector<WaveDesc> waves;
+    unsigned long long lanes = 0, film_pixels = 0;
+};
+
+u32 sobol_scale_exponent(u32 width, u32 height) {
+    const u32 v = std::max(std::max(width, height), 1u) - 1;
+    return v == 0 ? 0 : 32 - __builtin_clz(v);
+}
+
+BatchPlan plan_batch(const rp_view *views, u32 count, const rp_batch_request &r, u32 wave_lanes) {
+    if (!views || !count)
+        throw Invalid{"a batch needs at least one view"};
+    if (r.sampler_kind != RP_SAMPLER_SOBOL && r.sampler_kind != RP_SAMPLER_INDEPENDENT)
+        throw Invalid{"Unsupported sampler (independent and sobol are built)"};
+    if (r.sampler_kind == RP_SAMPLER_SOBOL && r.randomization > 3)
+        throw Invalid{"Invalid Sobol randomization"};
+    BatchPlan plan;
+    unsigned long long film_end = 0;
+    for (u32 i = 0; i < count; ++i) {
+        const rp_view &v = views[i];
+        if (!v.width || !v.height || !v.sample_count)
+            throw Invalid{"every view needs a nonzero film and sample count"};
+        if (uint64_t(v.width) * v.height > 0xffffffffull || v.sample_count > 0xffffffffull)
+            throw Invalid{"view film or sample count too large"};
+        if (r.sampler_kind == RP_SAMPLER_SOBOL && std::max(v.width, v.height) > (1u << 25))
+            throw Invalid{"Sobol film exceeds 2^25 pixels per side"};
+        if (v.sample_begin > UINT64_MAX - (v.sample_count - 1))
+            throw Invalid{"Sampler range must fit the absolute sample indices"};
+        if (v.film_offset < film_end)
+            throw Invalid{"view films must be in view order and must not overlap"};
+        DView d{};
+        d.cam = RasterCam{v3(v.camera.origin[0], v.camera.origin[1], v.camera.origin[2]),
+                          v3(v.camera.corner[0], v.camera.corner[1], v.camera.corner[2]),
+                          v3(v.camera.dx[0], v.camera.dx[1], v.camera.dx[2]),
+                          v3(v.camera.dy[0], v.camera.dy[1], v.camera.dy[2])};
+        d.width = v.width;
+        d.height = v.height;
+        d.m = r.sampler_kind == RP_SAMPLER_SOBOL ? sobol_scale_exponent(v.width, v.height) : 0;
+        d.pixels = v.width * v.height;
+        d.sample_low = u32(v.sample_begin);
+        d.sample_high = u32(v.sample_begin >> 32);
+        d.spp = u32(v.sample_count);
+        d.lane_begin = plan.lanes;
+        d.film_begin = v.film_offset;
+        plan.lanes += uint64_t(d.pixels) * d.spp;
+        film_end = v.film_offset + d.pixels;
+        plan.views.push_back(d);
+    }
+    plan.film_pixels = film_end;
+    wave_lanes = std::max<u32>(1, std::min<u32>(wave_lanes, 1u << 23));
+    for (unsigned long long l = 0; l < plan.lanes; l += wave_lanes)
+        plan.waves.push_back(WaveDesc{l, u32(std::min<unsigned long long>(wave_lanes, plan.lanes - l)), 0});
+    return plan;
+}
+
+WaveParams batch_params(const rp_batch_request &r) {
+    WaveParams p{};
+    p.seed_low = u32(r.seed);
+    p.seed_high = u32(r.seed >> 32);
+    p.sampler = r.sampler_kind;
+    p.randomization = r.randomization;
+    p.emergency_limit = r.emergency_limit ? r.emergency_limit : 1024;
+    return p;
+}
+
+template <int TB, int SB>
+void batch_wave_kernels(rp_scene *s, const WaveParams &p, const Batch &b, u32 wave_lanes, u32 blocks_per_sm,
+                        FilmPixel *film) {
+    PathPool &pool = s->pool;
+    const int sms = s->sm_count;
+    cudaStream_t st = s->stream;
+    RP_CHECK(cudaMemsetAsync(pool.counters, 0, 16 * sizeof(u32), st));
+    k_raygen_views<<<grid_for(sms, wave_lanes, 256, 16), 256, 0, st>>>(s->ds, p, b, pool);
+    const int trace_grid = grid_for(sms, wave_lanes, TB, int(blocks_per_sm * 128 / TB));
+    const int shade_grid = grid_for(sms, wave_lanes, SB, int(blocks_per_sm * 128 / SB));
+    int in = 0;
+    for (u32 e = 0; e <= s->ds.max_depth; ++e) {
+        RP_CHECK(cudaMemsetAsync(pool.counters + 4, 0, 4 * sizeof(u32), st));
+        k_trace<false, TB><<<trace_grid, TB, 0, st>>>(s->ds, pool, in);
+        RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), st));
+        RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), st));
+        k_shade<0, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
+        k_shade<1, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
+        k_shade<2, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
+        k_shade<3, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
+        k_shadow<false, TB><<<trace_grid, TB, 0, st>>>(s->ds, pool);
+        in ^= 1;
+    }
+    k_film_views<<<grid_for(sms, wave_lanes, 128, 16), 128, 0, st>>>(pool, b, s->cie, film);
+    k_next_wave<<<1, 32, 0, st>>>(b);
+    RP_CHECK(cudaGetLastError());
+}
+
+void batch_wave(rp_scene *s, const WaveParams &p, const Batch &b, const rp_batch_config &c, FilmPixel *film) {
+    const u32 w = c.wave_lanes, bpm = c.blocks_per_sm;
+    if (c.trace_block == 64 && c.shade_block == 128)
+        batch_wave_kernels<64, 128>(s, p, b, w, bpm, film);
+    else if (c.trace_block == 64 && c.shade_block == 256)
+        batch_wave_kernels<64, 256>(s, p, b, w, bpm, film);
+    else if (c.trace_block == 128 && c.shade_block == 256)
+        batch_wave_kernels<128, 256>(s, p, b, w, bpm, film);
+    else
+        batch_wave_kernels<128, 128>(s, p, b, w, bpm, film);
+}
+
+void check_config(const rp_batch_config &c) {
+    if (c.trace_block != 64 && c.trace_block != 128)
+        throw Invalid{"trace block must be 64 or 128 threads"};
+    if (c.shade_block != 128 && c.shade_block != 256)
+        throw Invalid{"shade block must be 128 or 256 threads"};
+    if (c.blocks_per_sm < 1 || c.blocks_per_sm > 32)
+        throw Invalid{"blocks per SM must be 1..32"};
+    if (!c.wave_lanes || c.wave_lanes > (1u << 23))
+        throw Invalid{"wave lanes must be 1..2^23"};
+}
+
+// Device copies of a plan; freed on the scene stream when the holder goes out of scope.
+struct BatchBuffers {
+    rp_scene *s;
+    DView *views = nullptr;
+    WaveDesc *waves = nullptr;
+    u32 *cursor = nullptr;
+    BatchBuffers(rp_scene *scene, const BatchPlan &plan) : s(scene) {
+        RP_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&views), plan.views.size() * sizeof(DView), s->stream));
+        RP_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&waves), plan.waves.size() * sizeof(WaveDesc), s->stream));
+        RP_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&cursor), 64, s->stream));
+        RP_CHECK(cudaMemcpyAsync(views, plan.views.data(), plan.views.size() * sizeof(DView), cudaMemcpyHostToDevice,
+                                 s->stream));
+        RP_CHECK(cudaMemcpyAsync(waves, plan.waves.data(), plan.waves.size() * sizeof(WaveDesc),
+                                 cudaMemcpyHostToDevice, s->stream));
+        RP_CHECK(cudaMemsetAsync(cursor, 0, 64, s->stream));
+    }
+    ~BatchBuffers() {
+        cudaFreeAsync(views, s->stream);
+        cudaFreeAsync(waves, s->stream);
+        cudaFreeAsync(cursor, s->stream);
+        cudaStreamSynchronize(s->stream);
+    }
+    Batch batch(const BatchPlan &plan) const {
+        return Batch{views, u32(plan.views.size()), waves, cursor, plan.film_pixels};
+    }
+};
+
+// Runs `waves` waves of the plan from wave 0, as graph replays or direct launches; returns the
+// device time in ms.
+float run_batch(rp_scene *s, const BatchPlan &plan, const BatchBuffers &buf, const rp_batch_request &r,
+                const rp_batch_config &c, FilmPixel *film, size_t waves) {
+    s->ensure_pool(c.wave_lanes);
+    const WaveParams p = batch_params(r);
+    const Batch b = buf.batch(plan);
+    RP_CHECK(cudaMemsetAsync(buf.cursor, 0, 8, s->stream));
+    cudaEvent_t start, stop;
+    RP_CHECK(cudaEventCreate(&start));
+    RP_CHECK(cudaEventCreate(&stop));
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    if (c.use_graph != 2) {
+        RP_CHECK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            batch_wave(s, p, b, c, film);
+        } catch (...) {
+            cudaStreamEndCapture(s->stream, &graph);
+            if (graph)
+                cudaGraphDestroy(graph);
+            throw;
+        }
+        RP_CHECK(cudaStreamEndCapture(s->stream, &graph));
+        RP_CHECK(cudaGraphInstantiate(&exec, graph, 0));
+    }
+    RP_CHECK(cudaEventRecord(start, s->stream));
+    for (size_t w = 0; w < waves; ++w) {
+        if (exec)
+            RP_CHECK(cudaGraphLaunch(exec, s->stream));
+        else
+            batch_wave(s, p, b, c, film);
+    }
+    RP_CHECK(cudaEventRecord(stop, s->stream));
+    RP_CHECK(cudaStreamSynchronize(s->stream));
+    float ms = 0;
+    RP_CHECK(cudaEventElapsedTime(&ms, start, stop));
+    cudaEventDestroy(start);
+    cudaEventDestroy(stop);
+    if (exec)
+        cudaGraphExecDestroy(exec);
+    if (graph)
+        cudaGraphDestroy(graph);
+    return ms;
+}
+
+// Coordinate search over the configuration, one probe wave per candidate (a warm-up replay,
+// then a timed one), keeping the fields the request fixes.
+rp_batch_config tune_batch(rp_scene *s, const rp_view *views, u32 count, const rp_batch_request &r) {
+    rp_batch_config best = r.config;
+    const bool fixed_wave = best.wave_lanes != 0, fixed_tb = best.trace_block != 0, fixed_sb = best.shade_block != 0,
+               fixed_bpm = best.blocks_per_sm != 0;
+    if (!best.use_graph)
+        best.use_graph = 1;
+    if (!fixed_tb)
+        best.trace_block = 128;
+    if (!fixed_sb)
+        best.shade_block = 128;
+    if (!fixed_bpm)
+        best.blocks_per_sm = 12;
+    const BatchPlan whole = plan_batch(views, count, r, 1u << 23);
+    float best_cost = INFINITY;
+    auto probe = [&](rp_batch_config c) {
+        const BatchPlan plan = plan_batch(views, count, r, c.wave_lanes);
+        const BatchBuffers buf(s, plan);
+        run_batch(s, plan, buf, r, c, nullptr, 1); // warm-up (module load, pool growth)
+        const float ms = run_batch(s, plan, buf, r, c, nullptr, 1);
+        const float cost = ms / (float(plan.waves[0].lanes) * 1e-6f);
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = c;
+        }
+    };
+    std::vector<u32> sizes;
+    if (fixed_wave) {
+        sizes.push_back(best.wave_lanes);
+    } else {
+        for (u32 w = 1u << 20; w <= (1u << 23); w <<= 1)
+            if (w <= whole.lanes || sizes.empty())
+                sizes.push_back(u32(std::min<unsigned long long>(w, whole.lanes)));
+    }
+    rp_batch_config c = best;
+    for (u32 w : sizes) {
+        c.wave_lanes = w;
+        probe(c);
+    }
+    c = best;
+    if (!fixed_tb)
+        for (u32 tb : {64u, 128u})
+            if (tb != best.trace_block) {
+                c = best;
+                c.trace_block = tb;
+                probe(c);
+            }
+    if (!fixed_sb)
+        for (u32 sb : {128u, 256u})
+            if (sb != best.shade_block) {
+                c = best;
+                c.shade_block = sb;
+                probe(c);
+            }
+    if (!fixed_bpm)
+        for (u32 bpm : {8u, 16u})
+            if (bpm != best.blocks_per_sm) {
+                c = best;
+                c.blocks_per_sm = bpm;
+                probe(c);
+            }
+    best.probe_ms_per_mlane = best_cost;
+    return best;
+}
+
+} // namespace
+
+extern "C" {
+
+rp_status rp_cuda_tune_views(rp_scene *s, const rp_view *views, uint32_t count, const rp_batch_request *request,
+                             rp_batch_config *chosen, char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!s || !request || !chosen)
+            throw Invalid{"null argument"};
+        if (s->transport != RP_TRANSPORT_HERO)
+            throw Invalid{"batched views render hero-transport scenes"};
+        RP_CHECK(cudaSetDevice(s->device));
+        if (!s->cie)
+            throw Invalid{"CIE table not set (rp_cuda_set_cie)"};
+        *chosen = tune_batch(s, views, count, *request);
+        return RP_SUCCESS;
+    });
+}
+
+rp_status rp_cuda_render_views_device(rp_scene *s, const rp_view *views, uint32_t count, const rp_batch_request *request,
+                                      rp_film_pixel *device_film, rp_batch_config *used, char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!s || !request || !device_film)
+            throw Invalid{"null argument"};
+        if (s->transport != RP_TRANSPORT_HERO)
+            throw Invalid{"batched views render hero-transport scenes"};
+        RP_CHECK(cudaSetDevice(s->device));
+        if (!s->cie)
+            throw Invalid{"CIE table not set (rp_cuda_set_cie)"};
+        rp_batch_config c = request->config;
+        if (!c.wave_lanes || !c.trace_block || !c.shade_block || !c.blocks_per_sm)
+            c = tune_batch(s, views, count, *request);
+        if (!c.use_graph)
+            c.use_graph = 1;
+        check_config(c);
+        const BatchPlan plan = plan_batch(views, count, *request, c.wave_lanes);
+        const BatchBuffers buf(s, plan);
+        const float ms = run_batch(s, plan, buf, *request, c, reinterpret_cast<FilmPixel *>(device_film),
+                                   plan.waves.size());
+        u32 failures = 0;
+        RP_CHECK(cudaMemcpy(&failures, buf.cursor + 1, 4, cudaMemcpyDeviceToHost));
+        const rp_timing build = s->timing;
+        s->timing = rp_timing{};
+        s->timing.build_ms = build.build_ms;
+        s->timing.build_host_ms = build.build_host_ms;
+        s->timing.build_bvh_ms = build.build_bvh_ms;
+        s->timing.total_ms = ms;
+        s->timing.samples = plan.lanes;
+        s->timing.kernel_launches = uint64_t(plan.waves.size()) * (3 + 6 * (s->ds.max_depth + 1));
+        if (used)
+            *used = c;
+        if (failures) {
+            set_diag(diag, cap, "%u lanes of the batch failed", failures);
+            return RP_FAILURE;
+        }
+        return RP_SUCCESS;
+    });
 }
 
 // ---- probes

@@ -20,40 +20,46 @@ RP_DEV u32 warp_append(u32 *counter, bool want) {
 }
 
 // rypath_render_packets prologue (shaders/render.metal:2424-2460) + packet_pt_initialize
-// (shaders/packet_pt_step.h:84-115)
-__global__ void k_raygen(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p, PathPool pool) {
-    for (u32 lane = blockIdx.x * blockDim.x + threadIdx.x; lane < p.lanes; lane += gridDim.x * blockDim.x) {
+// (shaders/packet_pt_step.h:84-115) for request lane `lane`, stored in pool slot `slot`.
+RP_DEV void raygen_lane(const DeviceScene &s, const RasterCam &cam, const WaveParams &p, u32 lane, u32 slot,
+                        PathPool &pool) {
+    {
         const BeginSample b = begin_sample(s, p, lane);
         V4 lambda, pdf;
         sample_wavelengths(sample_uniform(p, b.words.z), s.hero_mode, lambda, pdf);
         V3 o, d;
-        primary_ray(s, p, b, o, d);
+        primary_ray_from(s, cam, p, b, o, d);
         u32 flags = 15u | F_ROULETTE | (kCamera << F_LTYPE_SHIFT);
         if (!finite3(o) || !finite3(d))
             flags = set_status(flags, 2) | F_COMPLETE;
-        pool.ident[lane] = make_uint4(b.pixel, b.sample_low, b.sample_high, flags);
-        pool.cursor[lane] = make_uint4(u32(b.index), u32(b.index >> 32), 1, lane);
-        pool.lambda[lane] = to_float4(lambda);
-        pool.lambda_pdf[lane] = to_float4(pdf);
-        pool.beta[lane] = make_float4(1, 1, 1, 1);
-        pool.radiance[lane] = make_float4(0, 0, 0, 0);
-        pool.dens_f[lane] = pool.prev_f[lane] = make_float4(.5f, .5f, .5f, .5f);
-        pool.dens_e[lane] = pool.prev_e[lane] = make_int4(1, 1, 1, 1);
-        pool.eta_scale[lane] = make_float4(1, 1, 1, 1);
-        pool.ray_o[lane] = make_float4(o.x, o.y, o.z, 0);
-        pool.ray_d[lane] = make_float4(d.x, d.y, d.z, 0);
-        pool.latest_p[lane] = make_float4(o.x, o.y, o.z, 0);
-        pool.latest_n[lane] = make_float4(0, 0, 0, 0);
-        pool.queue[0][lane] = lane;
+        pool.ident[slot] = make_uint4(b.pixel, b.sample_low, b.sample_high, flags);
+        pool.cursor[slot] = make_uint4(u32(b.index), u32(b.index >> 32), 1, slot);
+        pool.lambda[slot] = to_float4(lambda);
+        pool.lambda_pdf[slot] = to_float4(pdf);
+        pool.beta[slot] = make_float4(1, 1, 1, 1);
+        pool.radiance[slot] = make_float4(0, 0, 0, 0);
+        pool.dens_f[slot] = pool.prev_f[slot] = make_float4(.5f, .5f, .5f, .5f);
+        pool.dens_e[slot] = pool.prev_e[slot] = make_int4(1, 1, 1, 1);
+        pool.eta_scale[slot] = make_float4(1, 1, 1, 1);
+        pool.ray_o[slot] = make_float4(o.x, o.y, o.z, 0);
+        pool.ray_d[slot] = make_float4(d.x, d.y, d.z, 0);
+        pool.latest_p[slot] = make_float4(o.x, o.y, o.z, 0);
+        pool.latest_n[slot] = make_float4(0, 0, 0, 0);
+        pool.queue[0][slot] = slot;
     }
+}
+__global__ void k_raygen(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p, PathPool pool) {
+    const RasterCam cam{s.origin, s.forward, s.right, s.up};
+    for (u32 lane = blockIdx.x * blockDim.x + threadIdx.x; lane < p.lanes; lane += gridDim.x * blockDim.x)
+        raygen_lane(s, cam, p, lane, lane, pool);
 }
 
 // Closest-hit queries for the active queue; each path is then appended to the bin of the
 // BSDF family it hit (0 diffuse, 1 conductor, 2 dielectric, 3 miss or failed query), so the
 // shade stage runs one specialised kernel per family ("material-sorted shading").
-template <bool Count>
-__global__ void __launch_bounds__(kTraceBlock) k_trace(const __grid_constant__ DeviceScene s, PathPool pool, int in) {
-    __shared__ u32 stack[kStackDepth * kTraceBlock];
+template <bool Count, int Block = kTraceBlock>
+__global__ void __launch_bounds__(Block) k_trace(const __grid_constant__ DeviceScene s, PathPool pool, int in) {
+    __shared__ u32 stack[kStackDepth * Block];
     const u32 count = pool.counters[in];
     const u32 *queue = pool.queue[in];
     u32 nodes = 0, tris = 0, rays = 0;
@@ -69,7 +75,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(const __grid_constant__ D
                 const float4 o = pool.ray_o[path], d = pool.ray_d[path];
                 Hit h;
                 const bool ok = trace_closest<Count>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), __int_as_float(0x7f800000),
-                                                     h, stack + threadIdx.x, kTraceBlock, nodes, tris);
+                                                     h, stack + threadIdx.x, Block, nodes, tris);
                 ++rays;
                 pool.hit[path] = make_float4(h.t, h.b1, h.b2, __uint_as_float(ok ? h.prim : 0xfffffffeu));
                 family = (!ok || h.prim == kNone) ? 3u : u32(__ldg(s.tri_family + h.prim));
@@ -93,8 +99,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(const __grid_constant__ D
 
 // One hero event after its closest hit (shaders/packet_pt_event_body.inc:11-461), for the paths
 // whose hit is of BSDF family F (3: no surface -- environment or a failed query).
-template <int F>
-__global__ void __launch_bounds__(128) k_shade(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p,
+template <int F, int Block = 128>
+__global__ void __launch_bounds__(Block) k_shade(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p,
                                                PathPool pool, int in) {
     const u32 count = pool.counters[4 + F];
     const u32 *queue = pool.bins + size_t(F) * pool.bin_capacity;
@@ -501,9 +507,9 @@ __global__ void __launch_bounds__(128) k_shade(const __grid_constant__ DeviceSce
 }
 
 // Visibility of the light samples (visible(), shaders/packet_transport.h:377-446, opaque surfaces)
-template <bool Count>
-__global__ void __launch_bounds__(kTraceBlock) k_shadow(const __grid_constant__ DeviceScene s, PathPool pool) {
-    __shared__ u32 stack[kStackDepth * kTraceBlock];
+template <bool Count, int Block = kTraceBlock>
+__global__ void __launch_bounds__(Block) k_shadow(const __grid_constant__ DeviceScene s, PathPool pool) {
+    __shared__ u32 stack[kStackDepth * Block];
     const u32 count = pool.counters[2];
     u32 nodes = 0, tris = 0, rays = 0;
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
@@ -511,7 +517,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_shadow(const __grid_constant__ 
         const u32 path = __float_as_uint(d.w);
         bool occluded;
         const bool ok = trace_any<Count>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), o.w, occluded, stack + threadIdx.x,
-                                         kTraceBlock, nodes, tris);
+                                         Block, nodes, tris);
         ++rays;
         uint4 ident = pool.ident[path];
         if (!ok) {
@@ -593,44 +599,45 @@ RP_DEV void add_compensated(double value, double &sum, double &correction) {
                                                                   : __dadd_rn(__dsub_rn(value, next), sum));
     sum = next;
 }
-// packet_sensor_xyz (src/packet_film.cpp:102-114) for every sample of a wave, reduced per
-// pixel in canonical (absolute sample, pixel) order.  Any failed lane fails the batch.
+// packet_sensor_xyz (src/packet_film.cpp:102-114) of one lane added to its pixel; false when
+// the lane failed (a failed lane fails its batch).
+RP_DEV bool film_add_lane(const PathPool &pool, u32 lane, const double *cie, FilmPixel &f) {
+    const uint4 id = pool.ident[lane];
+    const u32 status = (id.w & F_COMPLETE) ? get_status(id.w) : 2u;
+    if (status != 0)
+        return false;
+    const float4 l4 = pool.lambda[lane], p4 = pool.lambda_pdf[lane], r4 = pool.radiance[lane];
+    const float lam[4] = {l4.x, l4.y, l4.z, l4.w}, pdf[4] = {p4.x, p4.y, p4.z, p4.w}, rad[4] = {r4.x, r4.y, r4.z, r4.w};
+    double xyz[3] = {0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (pdf[k] == 0)
+            continue;
+        const float w = lam[k];
+        if (!(w >= 360 && w <= 830))
+            continue;
+        const u32 row = u32(round(double(w)) - 360.0);
+        const double weight = __ddiv_rn(__ddiv_rn(double(rad[k]), double(pdf[k])), 4.0);
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            xyz[c] = __dadd_rn(xyz[c], __dmul_rn(weight, __ldg(cie + 3 * row + c)));
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        add_compensated(xyz[c], f.sum[c], f.correction[c]);
+        f.square[c] = __dadd_rn(f.square[c], __dmul_rn(xyz[c], xyz[c]));
+    }
+    add_compensated(1.0, f.weight_sum, f.weight_correction);
+    ++f.count;
+    return true;
+}
+// Every sample of a wave reduced per pixel in canonical (absolute sample, pixel) order.
 __global__ void k_film(PathPool pool, u32 pixel_count, u32 samples, const double *cie, FilmPixel *film) {
     for (u32 px = blockIdx.x * blockDim.x + threadIdx.x; px < pixel_count; px += gridDim.x * blockDim.x) {
         FilmPixel f = film[px];
-        for (u32 si = 0; si < samples; ++si) {
-            const u32 lane = si * pixel_count + px;
-            const uint4 id = pool.ident[lane];
-            const u32 status = (id.w & F_COMPLETE) ? get_status(id.w) : 2u;
-            if (status != 0) {
+        for (u32 si = 0; si < samples; ++si)
+            if (!film_add_lane(pool, si * pixel_count + px, cie, f))
                 atomicAdd(pool.counters + 3, 1u);
-                continue;
-            }
-            const float4 l4 = pool.lambda[lane], p4 = pool.lambda_pdf[lane], r4 = pool.radiance[lane];
-            const float lam[4] = {l4.x, l4.y, l4.z, l4.w}, pdf[4] = {p4.x, p4.y, p4.z, p4.w},
-                        rad[4] = {r4.x, r4.y, r4.z, r4.w};
-            double xyz[3] = {0, 0, 0};
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                if (pdf[k] == 0)
-                    continue;
-                const float w = lam[k];
-                if (!(w >= 360 && w <= 830))
-                    continue;
-                const u32 row = u32(round(double(w)) - 360.0);
-                const double weight = __ddiv_rn(__ddiv_rn(double(rad[k]), double(pdf[k])), 4.0);
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-                    xyz[c] = __dadd_rn(xyz[c], __dmul_rn(weight, __ldg(cie + 3 * row + c)));
-            }
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                add_compensated(xyz[c], f.sum[c], f.correction[c]);
-                f.square[c] = __dadd_rn(f.square[c], __dmul_rn(xyz[c], xyz[c]));
-            }
-            add_compensated(1.0, f.weight_sum, f.weight_correction);
-            ++f.count;
-        }
         film[px] = f;
     }
 }

@@ -101,8 +101,13 @@ RP_DEV float triangle_offset(float u, float radius) {
     const float sv = 2.0f * u - 1.0f;
     return radius * (sv / (1.0f + sqrtf(1.0f - fabsf(sv))));
 }
-// shaders/render.metal:341-476 (primary_ray: pinhole, box / triangle filter)
-RP_DEV void primary_ray(const DeviceScene &s, const WaveParams &p, const BeginSample &b, V3 &o, V3 &d) {
+// A PBRT raster camera (RasterCamera, src/render.hpp:152-157)
+struct RasterCam {
+    V3 origin, forward, right, up;
+};
+// shaders/render.metal:341-476 (primary_ray: pinhole, box / triangle filter) for camera `cam`
+RP_DEV void primary_ray_from(const DeviceScene &s, const RasterCam &cam, const WaveParams &p, const BeginSample &b,
+                             V3 &o, V3 &d) {
     float ux, uy;
     if (p.sampler == 1) {
         ux = sobol_camera_uniform(b.words.x, p.m, b.pixel % p.width);
@@ -111,14 +116,14 @@ RP_DEV void primary_ray(const DeviceScene &s, const WaveParams &p, const BeginSa
         ux = u01(b.words.x);
         uy = u01(b.words.y);
     }
-    o = s.origin;
+    o = cam.origin;
     const bool centered = s.filter_kind != 0 || s.filter_x != 0.5f || s.filter_y != 0.5f;
     if (centered) {
         const float ox = s.filter_kind == 1 ? triangle_offset(ux, s.filter_x) : (2.0f * ux - 1.0f) * s.filter_x;
         const float oy = s.filter_kind == 1 ? triangle_offset(uy, s.filter_y) : (2.0f * uy - 1.0f) * s.filter_y;
         const float x = ((float(b.pixel % p.width) + 0.5f) + ox) / float(p.width);
         const float y = ((float(b.pixel / p.width) + 0.5f) + oy) / float(p.height);
-        const V3 dd = fma3(v3(y, y, y), s.up, fma3(v3(x, x, x), s.right, s.forward));
+        const V3 dd = fma3(v3(y, y, y), cam.up, fma3(v3(x, x, x), cam.right, cam.forward));
         const float scale = fmaxf(fabsf(dd.x), fmaxf(fabsf(dd.y), fabsf(dd.z)));
         const float nan = __int_as_float(0x7fffffff);
         if (!finite3(dd) || !(scale > 0.0f)) {
@@ -135,9 +140,13 @@ RP_DEV void primary_ray(const DeviceScene &s, const WaveParams &p, const BeginSa
     }
     const float x = (float(b.pixel % p.width) + ux) / float(p.width);
     const float y = (float(b.pixel / p.width) + uy) / float(p.height);
-    const V3 dd = s.forward + x * s.right + y * s.up;
+    const V3 dd = cam.forward + x * cam.right + y * cam.up;
     const float scale = fmaxf(fabsf(dd.x), fmaxf(fabsf(dd.y), fabsf(dd.z)));
     d = normalize3(dd / scale);
+}
+
+RP_DEV void primary_ray(const DeviceScene &s, const WaveParams &p, const BeginSample &b, V3 &o, V3 &d) {
+    primary_ray_from(s, RasterCam{s.origin, s.forward, s.right, s.up}, p, b, o, d);
 }
 
 // shaders/packet_walk.h:22-57 (sampled / constant / blackbody reflectance)

@@ -57,6 +57,10 @@ def lib():
         "rp_cuda_abi_size": (u32, [cp]),
         "rp_cuda_sample_device_static": (st, [vp, C.POINTER(abi.Request), vp, sz, vp, cp, sz]),
         "rp_cuda_build_light_tables": (C.c_int, [vp, u32, vp, vp, vp, vp, vp]),
+        "rp_cuda_render_views_device": (st, [vp, C.POINTER(abi.View), u32, C.POINTER(abi.BatchRequest), vp,
+                                             C.POINTER(abi.BatchConfig), cp, sz]),
+        "rp_cuda_tune_views": (st, [vp, C.POINTER(abi.View), u32, C.POINTER(abi.BatchRequest),
+                                    C.POINTER(abi.BatchConfig), cp, sz]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -78,6 +78,60 @@ class RenderSettings:
     randomization: int = abi.RANDOMIZE_OWEN
 
 
+@dataclass
+class View:
+    """One camera view of a batch (rp_view): camera as (origin, corner, dx, dy), film size,
+    absolute sample range and the first film pixel of the view in the batch film."""
+    camera: tuple
+    width: int
+    height: int
+    sample_begin: int = 0
+    sample_count: int = 1
+    film_offset: int = 0
+
+    def to_c(self) -> abi.View:
+        v = abi.View()
+        o, corner, dx, dy = self.camera
+        v.camera.origin[:] = list(o)
+        v.camera.corner[:] = list(corner)
+        v.camera.dx[:] = list(dx)
+        v.camera.dy[:] = list(dy)
+        v.width, v.height = self.width, self.height
+        v.sample_begin, v.sample_count, v.film_offset = self.sample_begin, self.sample_count, self.film_offset
+        return v
+
+
+@dataclass
+class BatchRequest:
+    seed: int = 1
+    sampler: int = abi.SAMPLER_SOBOL
+    randomization: int = abi.RANDOMIZE_OWEN
+    emergency_limit: int = 1024
+    wave_lanes: int = 0     # 0: tuned
+    trace_block: int = 0    # 0: tuned
+    shade_block: int = 0    # 0: tuned
+    blocks_per_sm: int = 0  # 0: tuned
+    use_graph: int = 1      # 1: CUDA graph replay per wave, 2: direct launches
+
+    def to_c(self) -> abi.BatchRequest:
+        r = abi.BatchRequest()
+        r.seed, r.sampler_kind, r.randomization, r.emergency_limit = (self.seed, self.sampler, self.randomization,
+                                                                      self.emergency_limit)
+        c = r.config
+        c.wave_lanes, c.trace_block, c.shade_block = self.wave_lanes, self.trace_block, self.shade_block
+        c.blocks_per_sm, c.use_graph = self.blocks_per_sm, self.use_graph
+        return r
+
+
+def pack_views(views):
+    """Assign consecutive film offsets; returns the total film pixels."""
+    offset = 0
+    for v in views:
+        v.film_offset = offset
+        offset += v.width * v.height
+    return offset
+
+
 class CudaRenderScene:
     """A scene resident on one GPU.  Synchronous calls need external serialisation."""
 
@@ -148,6 +202,29 @@ class CudaRenderScene:
         diag = C.create_string_buffer(512)
         st = native.lib().rp_cuda_render_film_device(self._handle, C.byref(r), C.c_void_p(device_film_ptr), diag, 512)
         native.check(st, diag, "rp_cuda_render_film_device")
+
+    def render_views_device(self, views, request: "BatchRequest", device_film_ptr: int) -> abi.BatchConfig:
+        """All ``views`` (a list of ``View``) into one device film, sharing one wavefront.
+
+        Returns the batch configuration that ran (the autotuner fills fields left at zero)."""
+        self._ensure_cie()
+        arr = (abi.View * len(views))(*[v.to_c() for v in views])
+        used = abi.BatchConfig()
+        diag = C.create_string_buffer(512)
+        st = native.lib().rp_cuda_render_views_device(self._handle, arr, len(views), C.byref(request.to_c()),
+                                                       C.c_void_p(device_film_ptr), C.byref(used), diag, 512)
+        native.check(st, diag, "rp_cuda_render_views_device")
+        return used
+
+    def tune_views(self, views, request: "BatchRequest") -> abi.BatchConfig:
+        self._ensure_cie()
+        arr = (abi.View * len(views))(*[v.to_c() for v in views])
+        chosen = abi.BatchConfig()
+        diag = C.create_string_buffer(512)
+        st = native.lib().rp_cuda_tune_views(self._handle, arr, len(views), C.byref(request.to_c()), C.byref(chosen),
+                                              diag, 512)
+        native.check(st, diag, "rp_cuda_tune_views")
+        return chosen
 
     def timing(self) -> abi.Timing:
         t = abi.Timing()

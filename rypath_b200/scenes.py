@@ -289,6 +289,30 @@ def cornell_fog(width=1024, height=1024, spp=64, max_depth=32, sigma_s_mean=0.5,
     return scene
 
 
+def view_batch(scene: Scene, count=64, seed=1, min_size=(256, 256), max_size=(1280, 720), spp=(4, 8, 16, 32, 64),
+               target=(0.0, 0.35, 0.0), distance=(2.2, 4.0), vfov=40.0):
+    """Seeded camera views of one scene for batched rendering: uniform resolutions between
+    min_size and max_size, sample counts drawn from ``spp``, and poses on a sphere around
+    ``target`` (distance range, elevation 5..45 degrees, any azimuth).  Returns a list of
+    ``renderer.View`` with consecutive film offsets."""
+    from . import renderer
+
+    rng = np.random.default_rng(seed)
+    views = []
+    for _ in range(count):
+        w = int(rng.integers(min_size[0], max_size[0] + 1))
+        h = int(rng.integers(min_size[1], max_size[1] + 1))
+        n = int(rng.choice(spp))
+        r = float(rng.uniform(*distance))
+        az = float(rng.uniform(0, 2 * math.pi))
+        el = math.radians(float(rng.uniform(5, 45)))
+        eye = (target[0] + r * math.cos(el) * math.sin(az), target[1] + r * math.sin(el),
+               target[2] + r * math.cos(el) * math.cos(az))
+        views.append(renderer.View(pinhole_camera(eye, target, (0, 1, 0), vfov, w, h), w, h, 0, n))
+    renderer.pack_views(views)
+    return views
+
+
 def slab_scene(media, planes, camera_medium=abi.RP_NONE, environment=1.0, max_depth=1, materials=None,
                positional=None) -> Scene:
     """Analytic medium scenes in the style of rypath's medium tests (tests/medium_render_tests.cpp:24-85).
