@@ -323,6 +323,31 @@ rp_status rp_cuda_tune_views(struct rp_scene *scene, const rp_view *views, uint3
                              const rp_batch_request *request, rp_batch_config *chosen, char *diag,
                              size_t diag_capacity);
 
+/* ---- differentiation ------------------------------------------------------------------- */
+
+/* Overwrites knot values [first, first + count) of the scene's spectral knots (the
+ * reflectance spectra of materials with RP_REFLECTANCE_KNOTS); wavelengths are kept.  The
+ * forward render of new parameters is then an ordinary rp_cuda_render_film(_device).  No
+ * counterpart in rypath. */
+rp_status rp_cuda_set_knot_values(struct rp_scene *scene, uint32_t first, uint32_t count, const float *values,
+                                  char *diag, size_t diag_capacity);
+
+/* The backward pass of a film render: the film request's lanes (samples [sample_begin,
+ * sample_begin + sample_count) of every pixel) are traced again with the same random numbers
+ * and, given d loss / d XYZ of every pixel's film mean (device, 3 doubles per pixel), the
+ * gradient of the loss with respect to the knot values of the listed materials (diffuse,
+ * RP_REFLECTANCE_KNOTS) is accumulated into device_gradient (zeroed first; the listed
+ * materials' knot_count entries each, in list order).  Depth at most 15; at most 2048
+ * gradient entries.  No counterpart in rypath. */
+typedef struct rp_adjoint_request {
+    rp_film_request film;
+    uint32_t material_count;
+    const uint32_t *materials; /* host array of scene material indices */
+} rp_adjoint_request;
+rp_status rp_cuda_adjoint_device(struct rp_scene *scene, const rp_adjoint_request *request,
+                                 const double *device_d_loss_d_xyz, float *device_gradient, char *diag,
+                                 size_t diag_capacity);
+
 /* ---- instrumentation ------------------------------------------------------------------ */
 
 /* Timing of the last sample/film call on this scene. */

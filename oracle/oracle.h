@@ -55,6 +55,12 @@ void or_probe_light_select(const or_scene *scene, const float *queries, uint32_t
 int or_film_add(const rp_packet_result *results, size_t count, const double *cie_xyz,
                 uint32_t pixel_count, rp_film_pixel *film);
 
+/* FP64 path-replay adjoint of a film render (the rp_cuda_adjoint_device contract): gradient of
+ * the loss with respect to the knot values of `materials`, given d loss / d film-mean XYZ per
+ * pixel and the CIE table.  0, 1 when a lane failed, -1 on a bad material list. */
+int or_adjoint(const or_scene *scene, const rp_film_request *film, const uint32_t *materials, uint32_t count,
+               const double *d_loss_d_xyz, const double *cie_xyz, double *gradient, int threads);
+
 /* Scalar (one-wavelength) PT / volpath lanes of a request (rypath_render_paths); the scene
  * must be built with RP_TRANSPORT_SCALAR.  threads <= 0: all cores.  0, 1 on a failed
  * lane, -1 on a bad request. */

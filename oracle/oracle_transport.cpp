@@ -112,7 +112,18 @@ static bool emitted(const Scene &s, const Vertex &v, F3 direction, const Wavelen
 }
 
 // ---------------------------------------------------------------- lane state
+// Path-replay adjoint state of one lane (FP64): d loss / d radiance per wavelength lane, the
+// parameter materials of the diffuse vertices so far, and the gradient being accumulated.
+struct AdjointLane {
+    const std::vector<u32> *slot = nullptr; // per scene material: first gradient entry or RP_NONE
+    double w[4] = {0, 0, 0, 0};
+    u32 history[16];
+    u32 history_count = 0;
+    double *grad = nullptr;
+};
+
 struct LaneState {
+    AdjointLane *adj = nullptr;
     Vertex latest;
     F3 preceding_position{};
     u32 preceding_type = 0;
@@ -313,6 +324,40 @@ static F4 hero_direct(const Ctx &c, Sample &smp, const Wavelengths &l, u64 index
     return hero_weight(smp, prefix, value, f4(sampled_pdf), bsdf_pdf);
 }
 
+// d loss / d knots of one contribution: contribution * w / rho over the history's vertices,
+// rho piecewise linear in the knots (pbrt_reflectance), all in FP64.
+static void adjoint_accumulate(const Scene &s, AdjointLane &a, const Wavelengths &l, F4 contribution) {
+    for (u32 j = 0; j < a.history_count; ++j) {
+        const u32 m = a.history[j];
+        const Material &M = s.materials[m];
+        const Knot *kn = s.knots.data() + M.knot_begin;
+        const u32 slot = (*a.slot)[m];
+        for (int k = 0; k < 4; ++k) {
+            const double g0 = a.w[k] * double(contribution[k]);
+            const float x = l.lambda[k];
+            if (g0 == 0 || !(x >= kn[0].wavelength && x <= kn[M.knot_count - 1].wavelength))
+                continue;
+            u32 lo = 0, hi = M.knot_count - 1;
+            while (hi - lo > 1) {
+                const u32 mid = lo + (hi - lo) / 2;
+                if (x < kn[mid].wavelength)
+                    hi = mid;
+                else
+                    lo = mid;
+            }
+            const double t = lo == hi ? 0.0
+                                      : (double(x) - kn[lo].wavelength) / (double(kn[hi].wavelength) - kn[lo].wavelength);
+            const double rho = kn[lo].value + (double(kn[hi].value) - kn[lo].value) * t;
+            if (!(rho > 0))
+                continue;
+            const double g = g0 / rho;
+            a.grad[slot + lo] += g * (1.0 - t);
+            if (hi != lo)
+                a.grad[slot + hi] += g * t;
+        }
+    }
+}
+
 // shaders/packet_pt_event_body.inc:11-461 (one hero event, vacuum, opaque surfaces)
 static void hero_step(const Ctx &c, LaneState &st) {
     if (st.complete)
@@ -466,11 +511,24 @@ static void hero_step(const Ctx &c, LaneState &st) {
             before.type = st.preceding_type;
             before.point.position = st.preceding_position;
         }
-        st.radiance = st.radiance + hero_endpoint(c, smp, l, current, st.latest, before, count,
-                                                   previous_density);
-        if (smp.status == RP_SAMPLE_SUCCESS && count < capacity && direct_allowed)
-            st.radiance = st.radiance + hero_direct(c, smp, l, st.index, current, st.latest, count,
-                                                     direct_beta, direct_density);
+        const F4 endpoint = hero_endpoint(c, smp, l, current, st.latest, before, count, previous_density);
+        st.radiance = st.radiance + endpoint;
+        if (st.adj) {
+            if (smp.status == RP_SAMPLE_SUCCESS && nonzero4(endpoint))
+                adjoint_accumulate(s, *st.adj, l, endpoint);
+            if (current.type == surface_vertex && smp.status == RP_SAMPLE_SUCCESS) {
+                const u32 m = s.instances[current.instance].material;
+                if (s.materials[m].scattering == RP_DIFFUSE && (*st.adj->slot)[m] != RP_NONE &&
+                    st.adj->history_count < 16)
+                    st.adj->history[st.adj->history_count++] = m;
+            }
+        }
+        if (smp.status == RP_SAMPLE_SUCCESS && count < capacity && direct_allowed) {
+            const F4 direct = hero_direct(c, smp, l, st.index, current, st.latest, count, direct_beta, direct_density);
+            st.radiance = st.radiance + direct;
+            if (st.adj && smp.status == RP_SAMPLE_SUCCESS && nonzero4(direct))
+                adjoint_accumulate(s, *st.adj, l, direct);
+        }
         if (!finite_nonnegative4(st.radiance))
             smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
         if (smp.status != RP_SAMPLE_SUCCESS)
@@ -484,9 +542,10 @@ static void hero_step(const Ctx &c, LaneState &st) {
 }
 
 // shaders/render.metal:2424-2469 (hero branch) + packet_pt_result (shaders/packet_pt_step.h:225-239)
-static rp_packet_result render_lane(const Ctx &c, u32 lane) {
+static rp_packet_result render_lane(const Ctx &c, u32 lane, AdjointLane *adj = nullptr) {
     const Scene &s = c.s;
     LaneState st;
+    st.adj = adj;
     u64 index = 0;
     st.sample = begin_sample(s, c.p, lane, index);
     st.index = index;
@@ -584,6 +643,80 @@ int or_sample(const or_scene *scene, const rp_request *request, rp_packet_result
         if (results[i].status != RP_SAMPLE_SUCCESS)
             return 1;
     return 0;
+}
+
+// The FP64 path-replay adjoint of a film render: d loss / d knots of the listed materials
+// given d loss / d film-mean XYZ per pixel (the rp_cuda_adjoint_device contract, in double).
+int or_adjoint(const or_scene *scene, const rp_film_request *f, const uint32_t *materials, uint32_t count,
+               const double *d_loss_d_xyz, const double *cie, double *grad, int threads) {
+    const Scene &s = scene->scene;
+    std::vector<u32> slot(s.materials.size(), RP_NONE);
+    u32 params = 0;
+    for (u32 i = 0; i < count; ++i) {
+        const u32 m = materials[i];
+        if (m >= s.materials.size() || slot[m] != RP_NONE || s.materials[m].scattering != RP_DIFFUSE ||
+            s.materials[m].kind != RP_REFLECTANCE_KNOTS)
+            return -1;
+        slot[m] = params;
+        params += s.materials[m].knot_count;
+    }
+    rp_request q{};
+    q.width = f->width;
+    q.height = f->height;
+    q.seed = f->seed;
+    q.pixel_count = f->width * f->height;
+    q.sample_begin = f->sample_begin;
+    q.sample_count = u32(f->sample_count);
+    q.emergency_limit = f->emergency_limit;
+    q.sampler_kind = f->sampler_kind;
+    q.randomization = f->randomization;
+    const Params p = make_params(s, q);
+    const Ctx c{s, scene->bvh, p};
+    const u64 lanes = u64(q.pixel_count) * q.sample_count;
+    const unsigned n = threads > 0 ? unsigned(threads) : std::max(1u, std::thread::hardware_concurrency());
+    std::vector<std::vector<double>> local(n, std::vector<double>(params, 0.0));
+    std::atomic<u64> next{0};
+    std::atomic<u32> failures{0};
+    auto work = [&](unsigned t) {
+        for (;;) {
+            const u64 begin = next.fetch_add(256);
+            if (begin >= lanes)
+                return;
+            for (u64 i = begin; i < std::min(lanes, begin + 256); ++i) {
+                u64 index = 0;
+                const Sample smp = begin_sample(s, p, u32(i), index);
+                const float uw = sample_uniform(p, smp.words[2]);
+                const Wavelengths l = s.hero_mode == RP_HERO_VISIBLE ? sample_visible(uw) : sample_uniform(uw);
+                AdjointLane a;
+                a.slot = &slot;
+                a.grad = local[t].data();
+                for (int k = 0; k < 4; ++k) {
+                    if (l.pdf[k] == 0 || !(l.lambda[k] >= 360 && l.lambda[k] <= 830))
+                        continue;
+                    const size_t row = size_t(std::round(double(l.lambda[k])) - 360.0);
+                    double g = 0;
+                    for (int ch = 0; ch < 3; ++ch)
+                        g += d_loss_d_xyz[3 * size_t(smp.pixel) + ch] * cie[3 * row + ch];
+                    a.w[k] = g / (double(l.pdf[k]) * 4.0) / double(q.sample_count);
+                }
+                if (render_lane(c, u32(i), &a).status != RP_SAMPLE_SUCCESS)
+                    ++failures;
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < n; ++t)
+        pool.emplace_back(work, t);
+    work(0);
+    for (auto &t : pool)
+        t.join();
+    for (u32 j = 0; j < params; ++j) {
+        double sum = 0;
+        for (unsigned t = 0; t < n; ++t)
+            sum += local[t][j];
+        grad[j] = sum;
+    }
+    return failures ? 1 : 0;
 }
 
 void or_probe_sobol(const void *tables, const uint32_t *q, uint32_t count, uint32_t *r) {

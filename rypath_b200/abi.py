@@ -143,6 +143,10 @@ class BatchRequest(C.Structure):
                 ("config", BatchConfig)]
 
 
+class AdjointRequest(C.Structure):
+    _fields_ = [("film", FilmRequest), ("material_count", u32), ("materials", P(u32))]
+
+
 class Timing(C.Structure):
     _fields_ = [("total_ms", f64), ("trace_ms", f64), ("shadow_ms", f64), ("shade_ms", f64),
                 ("other_ms", f64), ("closest_rays", u64), ("shadow_rays", u64),
@@ -185,4 +189,5 @@ EXPECTED_SIZES = {
     "rp_packet_result": (PacketResult, 80), "rp_scalar_result": (ScalarResult, 44),
     "rp_film_pixel": (FilmPixel, 96), "rp_film_request": (FilmRequest, 56),
     "rp_view": (View, 80), "rp_batch_config": (BatchConfig, 24), "rp_batch_request": (BatchRequest, 48),
+    "rp_adjoint_request": (AdjointRequest, 72),
 }

@@ -364,6 +364,9 @@ struct rp_scene {
     u32 *scalar_counters = nullptr;
     u32 scalar_capacity = 0;
     int volpath_blocks = 0; // resident persistent blocks per SM
+    // adjoint: per-lane history and lane weights
+    void *adjoint_storage = nullptr;
+    u32 adjoint_capacity = 0;
 
     ~rp_scene() {
         if (device >= 0)
@@ -374,6 +377,8 @@ struct rp_scene {
             cudaFreeAsync(p, stream);
         if (scalar_records)
             cudaFreeAsync(scalar_records, stream);
+        if (adjoint_storage)
+            cudaFreeAsync(adjoint_storage, stream);
         if (film_stage)
             cudaFreeAsync(film_stage, stream);
         if (stream)
@@ -525,7 +530,7 @@ std::string validate_request(const rp_scene *s, const rp_request &r) {
 }
 
 // One wave: raygen, then max_depth + 1 events of trace -> shade -> shadow.
-void run_wave(rp_scene *s, const WaveParams &p) {
+void run_wave(rp_scene *s, const WaveParams &p, size_t adjoint_smem = 0) {
     s->ensure_pool(p.lanes);
     PathPool &pool = s->pool;
     const int sms = s->sm_count;
@@ -547,16 +552,17 @@ void run_wave(rp_scene *s, const WaveParams &p) {
         s->mark(2, 4);
         RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), s->stream));
         RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), s->stream));
-        k_shade<0><<<grid_for(sms, p.lanes, 128, 16), 128, 0, s->stream>>>(s->ds, p, pool, in);
-        k_shade<1><<<grid_for(sms, p.lanes, 128, 16), 128, 0, s->stream>>>(s->ds, p, pool, in);
-        k_shade<2><<<grid_for(sms, p.lanes, 128, 16), 128, 0, s->stream>>>(s->ds, p, pool, in);
-        k_shade<3><<<grid_for(sms, p.lanes, 128, 16), 128, 0, s->stream>>>(s->ds, p, pool, in);
+        const size_t smem = adjoint_smem;
+        k_shade<0><<<grid_for(sms, p.lanes, 128, 16), 128, smem, s->stream>>>(s->ds, p, pool, in);
+        k_shade<1><<<grid_for(sms, p.lanes, 128, 16), 128, smem, s->stream>>>(s->ds, p, pool, in);
+        k_shade<2><<<grid_for(sms, p.lanes, 128, 16), 128, smem, s->stream>>>(s->ds, p, pool, in);
+        k_shade<3><<<grid_for(sms, p.lanes, 128, 16), 128, smem, s->stream>>>(s->ds, p, pool, in);
         s->done();
         s->mark(1);
         if (s->counting)
-            k_shadow<true><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, 0, s->stream>>>(s->ds, pool);
+            k_shadow<true><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, smem, s->stream>>>(s->ds, pool);
         else
-            k_shadow<false><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, 0, s->stream>>>(s->ds, pool);
+            k_shadow<false><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, smem, s->stream>>>(s->ds, pool);
         s->done();
         in ^= 1;
     }
@@ -757,6 +763,7 @@ uint32_t rp_cuda_abi_size(const char *name) {
     if (n == "rp_view") return sizeof(rp_view);
     if (n == "rp_batch_config") return sizeof(rp_batch_config);
     if (n == "rp_batch_request") return sizeof(rp_batch_request);
+    if (n == "rp_adjoint_request") return sizeof(rp_adjoint_request);
     return 0;
 }
 
@@ -1462,6 +1469,151 @@ rp_status rp_cuda_render_film(rp_scene *s, const rp_film_request *r, rp_film_pix
 }
 rp_status rp_cuda_render_film_device(rp_scene *s, const rp_film_request *r, rp_film_pixel *film, char *diag, size_t cap) {
     return film_impl(s, r, film, false, diag, cap);
+}
+
+// ---- differentiation
+
+rp_status rp_cuda_set_knot_values(rp_scene *s, uint32_t first, uint32_t count, const float *values, char *diag,
+                                  size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!s || (!values && count))
+            throw Invalid{"null argument"};
+        if (uint64_t(first) + count > s->ds.knot_count)
+            throw Invalid{"knot range out of range"};
+        for (u32 i = 0; i < count; ++i)
+            if (!std::isfinite(values[i]))
+                throw Invalid{"knot values must be finite"};
+        RP_CHECK(cudaSetDevice(s->device));
+        if (count) {
+            float2 *dst = const_cast<float2 *>(s->ds.knots) + first;
+            RP_CHECK(cudaMemcpy2DAsync(reinterpret_cast<float *>(dst) + 1, sizeof(float2), values, sizeof(float),
+                                       sizeof(float), count, cudaMemcpyHostToDevice, s->stream));
+            RP_CHECK(cudaStreamSynchronize(s->stream));
+        }
+        return RP_SUCCESS;
+    });
+}
+
+rp_status rp_cuda_adjoint_device(rp_scene *s, const rp_adjoint_request *r, const double *d_loss_d_xyz, float *gradient,
+                                 char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!s || !r || !d_loss_d_xyz || !gradient || (r->material_count && !r->materials))
+            throw Invalid{"null argument"};
+        if (s->transport != RP_TRANSPORT_HERO)
+            throw Invalid{"the adjoint differentiates hero-transport renders"};
+        const rp_film_request &f = r->film;
+        if (!f.width || !f.height || !f.sample_count || !f.batch_size)
+            throw Invalid{"film request needs nonzero film size, samples and batch size"};
+        if (s->ds.max_depth > 15)
+            throw Invalid{"the adjoint records at most 16 vertices: max depth must be at most 15"};
+        if (s->ds.material_count > 255)
+            throw Invalid{"the adjoint addresses at most 255 materials"};
+        // gradient slots of the parameter materials
+        std::vector<u32> slot(std::max<u32>(1, s->ds.material_count), kNone);
+        std::vector<DMaterial> mats(s->ds.material_count);
+        RP_CHECK(cudaSetDevice(s->device));
+        RP_CHECK(cudaMemcpy(mats.data(), s->ds.materials, mats.size() * sizeof(DMaterial), cudaMemcpyDeviceToHost));
+        u32 params = 0;
+        for (u32 i = 0; i < r->material_count; ++i) {
+            const u32 m = r->materials[i];
+            if (m >= s->ds.material_count)
+                throw Invalid{"adjoint material out of range"};
+            if (slot[m] != kNone)
+                throw Invalid{"adjoint material listed twice"};
+            if (mats[m].scattering != RP_DIFFUSE || mats[m].kind != RP_REFLECTANCE_KNOTS || mats[m].knot_count < 2)
+                throw Invalid{"adjoint materials must be diffuse with knot reflectance"};
+            slot[m] = params;
+            params += mats[m].knot_count;
+        }
+        if (params > 2048)
+            throw Invalid{"the adjoint accumulates at most 2048 gradient entries"};
+        if (!s->cie)
+            throw Invalid{"CIE table not set (rp_cuda_set_cie)"};
+        const u32 pixels = f.width * f.height;
+        const u64 max_lanes = 1u << 23;
+        const u64 samples_per_wave = std::max<u64>(1, std::min<u64>(f.batch_size, max_lanes / pixels));
+        const u32 lanes_cap = u32(std::min<u64>(max_lanes, samples_per_wave * pixels));
+        s->ensure_pool(lanes_cap);
+        if (s->adjoint_capacity < s->capacity) {
+            if (s->adjoint_storage)
+                cudaFreeAsync(s->adjoint_storage, s->stream);
+            s->adjoint_storage = nullptr;
+            s->adjoint_capacity = 0;
+            RP_CHECK(cudaMallocAsync(&s->adjoint_storage, size_t(s->capacity) * 32, s->stream));
+            s->adjoint_capacity = s->capacity;
+        }
+        u32 *slot_dev = nullptr;
+        RP_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&slot_dev), slot.size() * 4, s->stream));
+        RP_CHECK(cudaMemcpyAsync(slot_dev, slot.data(), slot.size() * 4, cudaMemcpyHostToDevice, s->stream));
+        RP_CHECK(cudaMemsetAsync(gradient, 0, size_t(std::max<u32>(params, 1)) * sizeof(float), s->stream));
+        PathPool &pool = s->pool;
+        const PathPool saved = pool;
+        pool.hist = reinterpret_cast<uint4 *>(s->adjoint_storage);
+        pool.adj_w = reinterpret_cast<float4 *>(static_cast<unsigned char *>(s->adjoint_storage) +
+                                                size_t(s->adjoint_capacity) * 16);
+        pool.adj_slot = slot_dev;
+        pool.adj_grad = gradient;
+        pool.adj_g = d_loss_d_xyz;
+        pool.adj_cie = s->cie;
+        pool.adj_inv_weight = 1.0 / double(f.sample_count);
+        pool.adj_params = params;
+        cudaEvent_t start, stop;
+        RP_CHECK(cudaEventCreate(&start));
+        RP_CHECK(cudaEventCreate(&stop));
+        RP_CHECK(cudaEventRecord(start, s->stream));
+        u32 failures = 0;
+        try {
+            u64 done = 0;
+            while (done < f.sample_count) {
+                const u64 spw = std::min<u64>(samples_per_wave, f.sample_count - done);
+                rp_request q{};
+                q.width = f.width;
+                q.height = f.height;
+                q.seed = f.seed;
+                q.pixel_count = pixels;
+                q.sample_begin = f.sample_begin + done;
+                q.sample_count = u32(spw);
+                q.emergency_limit = f.emergency_limit;
+                q.sampler_kind = f.sampler_kind;
+                q.randomization = f.randomization;
+                const std::string err = validate_request(s, q);
+                if (!err.empty())
+                    throw Invalid{err};
+                const WaveParams p = wave_params(q);
+                run_wave(s, p, size_t(params) * sizeof(float));
+                // a failed lane (as in the forward film) fails the gradient
+                s->mark(3);
+                k_count_failures<<<grid_for(s->sm_count, p.lanes, 256, 8), 256, 0, s->stream>>>(pool, p.lanes);
+                s->done();
+                u32 wave_failures = 0;
+                RP_CHECK(cudaMemcpyAsync(&wave_failures, pool.counters + 3, 4, cudaMemcpyDeviceToHost, s->stream));
+                RP_CHECK(cudaStreamSynchronize(s->stream));
+                failures += wave_failures;
+                done += spw;
+            }
+            RP_CHECK(cudaEventRecord(stop, s->stream));
+            s->collect();
+        } catch (...) {
+            pool = saved;
+            cudaFreeAsync(slot_dev, s->stream);
+            cudaEventDestroy(start);
+            cudaEventDestroy(stop);
+            throw;
+        }
+        pool = saved;
+        cudaFreeAsync(slot_dev, s->stream);
+        float total = 0;
+        RP_CHECK(cudaEventElapsedTime(&total, start, stop));
+        cudaEventDestroy(start);
+        cudaEventDestroy(stop);
+        s->timing.total_ms = total;
+        s->timing.samples = f.sample_count * pixels;
+        if (failures) {
+            set_diag(diag, cap, "%u lanes failed; the gradient is not valid", failures);
+            return RP_FAILURE;
+        }
+        return RP_SUCCESS;
+    });
 }
 
 // ---- batched views

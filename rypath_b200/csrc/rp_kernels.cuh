@@ -46,6 +46,10 @@ RP_DEV void raygen_lane(const DeviceScene &s, const RasterCam &cam, const WavePa
         pool.latest_p[slot] = make_float4(o.x, o.y, o.z, 0);
         pool.latest_n[slot] = make_float4(0, 0, 0, 0);
         pool.queue[0][slot] = slot;
+        if (pool.hist) {
+            pool.hist[slot] = empty_history();
+            pool.adj_w[slot] = adjoint_lane_weight(pool, b.pixel, lambda, pdf);
+        }
     }
 }
 __global__ void k_raygen(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p, PathPool pool) {
@@ -102,6 +106,8 @@ __global__ void __launch_bounds__(Block) k_trace(const __grid_constant__ DeviceS
 template <int F, int Block = 128>
 __global__ void __launch_bounds__(Block) k_shade(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p,
                                                PathPool pool, int in) {
+    extern __shared__ float sgrad[]; // adjoint only
+    adjoint_begin(pool, sgrad);
     const u32 count = pool.counters[4 + F];
     const u32 *queue = pool.bins + size_t(F) * pool.bin_capacity;
     u32 *out_queue = pool.queue[in ^ 1];
@@ -347,6 +353,20 @@ __global__ void __launch_bounds__(Block) k_shade(const __grid_constant__ DeviceS
                         }
                     }
                     radiance = add4(radiance, endpoint);
+                    if (pool.hist) {
+                        // replay: the emission's gradient over the vertices before this one,
+                        // then this diffuse vertex joins the history of what follows it
+                        uint4 h = pool.hist[path];
+                        if (status == 0 && nonzero4(endpoint))
+                            adjoint_accumulate(s, pool, sgrad, h, lambda, endpoint, pool.adj_w[path]);
+                        if (F == 0 && ctype == kSurface && status == 0) {
+                            const u32 m = s.instances[cinst].material;
+                            if (__ldg(pool.adj_slot + m) != kNone) {
+                                h = history_push(h, m);
+                                pool.hist[path] = h;
+                            }
+                        }
+                    }
                     // hero_direct (shaders/hero_pt_helpers.h:185-221): sample, evaluate, weight;
                     // visibility is resolved by the shadow kernel.
                     if (F != 3 && status == 0 && cnt < capacity && direct_allowed && ctype == kSurface && connectible) {
@@ -504,12 +524,15 @@ __global__ void __launch_bounds__(Block) k_shade(const __grid_constant__ DeviceS
             pool.sh_c[sslot] = sh_c;
         }
     }
+    adjoint_end(pool, sgrad);
 }
 
 // Visibility of the light samples (visible(), shaders/packet_transport.h:377-446, opaque surfaces)
 template <bool Count, int Block = kTraceBlock>
 __global__ void __launch_bounds__(Block) k_shadow(const __grid_constant__ DeviceScene s, PathPool pool) {
     __shared__ u32 stack[kStackDepth * Block];
+    extern __shared__ float sgrad[]; // adjoint only
+    adjoint_begin(pool, sgrad);
     const u32 count = pool.counters[2];
     u32 nodes = 0, tris = 0, rays = 0;
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
@@ -542,8 +565,13 @@ __global__ void __launch_bounds__(Block) k_shadow(const __grid_constant__ Device
         if (!finite_nonnegative4(from_float4(r))) {
             ident.w = set_status(ident.w, 2) | F_COMPLETE;
             pool.ident[path] = ident;
+        } else if (pool.hist) {
+            // replay: the light sample's gradient, over the history including its vertex
+            adjoint_accumulate(s, pool, sgrad, pool.hist[path], from_float4(pool.lambda[path]), from_float4(c),
+                               pool.adj_w[path]);
         }
     }
+    adjoint_end(pool, sgrad);
     if (Count) {
         atomicAdd(pool.stats + 4, (unsigned long long)nodes);
         atomicAdd(pool.stats + 5, (unsigned long long)tris);
@@ -630,6 +658,15 @@ RP_DEV bool film_add_lane(const PathPool &pool, u32 lane, const double *cie, Fil
     add_compensated(1.0, f.weight_sum, f.weight_correction);
     ++f.count;
     return true;
+}
+// Failed lanes of a wave (counters[3]), for passes that produce no film.  counters[3] is
+// cleared with the wave's counters, so callers accumulate it per wave.
+__global__ void k_count_failures(PathPool pool, u32 lanes) {
+    for (u32 lane = blockIdx.x * blockDim.x + threadIdx.x; lane < lanes; lane += gridDim.x * blockDim.x) {
+        const u32 w = pool.ident[lane].w;
+        if (!(w & F_COMPLETE) || get_status(w) != 0)
+            atomicAdd(pool.counters + 3, 1u);
+    }
 }
 // Every sample of a wave reduced per pixel in canonical (absolute sample, pixel) order.
 __global__ void k_film(PathPool pool, u32 pixel_count, u32 samples, const double *cie, FilmPixel *film) {

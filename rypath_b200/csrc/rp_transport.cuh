@@ -51,6 +51,15 @@ struct PathPool {
     float4 *sh_c;  // weighted contribution (NaN x: invalid if visible)
     // statistics (optional)
     unsigned long long *stats; // closest [0] nodes, [1] triangles, [2] rays; shadow [3] rays, [4] nodes, [5] triangles
+    // path-replay adjoint (hist == nullptr: off)
+    uint4 *hist;            // parameter materials of the diffuse vertices so far, a byte each, 0xff = none
+    float4 *adj_w;          // d loss / d radiance of each wavelength lane
+    const u32 *adj_slot;    // per scene material: its first gradient entry, kNone if not a parameter
+    float *adj_grad;        // gradient of the loss, one entry per parameter knot
+    const double *adj_g;    // d loss / d film-mean XYZ, 3 per pixel
+    const double *adj_cie;  // CIE 1931 table, 3 per nm from 360 nm
+    double adj_inv_weight;  // 1 / film weight of a pixel (its sample count)
+    u32 adj_params;         // gradient entries
 };
 
 struct WaveParams {
@@ -297,6 +306,106 @@ RP_DEV V3 offset_point(V3 position, V3 error, V3 ng, V3 direction) {
         return position;
     const V3 n = dot(direction, ng) < 0 ? -ng : ng;
     return round_out(position + dot(vabs(n), error) * n, n);
+}
+
+// ------------------------------------------------------------------ path-replay adjoint
+// A lane's radiance is a sum of contributions, each a product in which every diffuse vertex
+// before it (and, for a light sample, the vertex it leaves from) enters once through its
+// reflectance rho(lambda); the selection probabilities, wavelength and light MIS weights
+// depend on densities only.  So d contribution / d rho_m(lambda) = contribution * n_m / rho_m,
+// and rho is piecewise linear in the knot values (pbrt_reflectance).  Russian roulette is held
+// fixed (its survival test only picks which paths are traced).
+
+// d loss / d radiance of each lane: the packet film weight (packet_sensor_xyz,
+// src/packet_film.cpp:102-114) against d loss / d XYZ of the lane's pixel.
+RP_DEV float4 adjoint_lane_weight(const PathPool &pool, u32 pixel, V4 lambda, V4 pdf) {
+    float w[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        w[k] = 0;
+        if (pdf.v[k] == 0 || !(lambda.v[k] >= 360 && lambda.v[k] <= 830))
+            continue;
+        const u32 row = u32(round(double(lambda.v[k])) - 360.0);
+        const double scale = pool.adj_inv_weight / (double(pdf.v[k]) * 4.0);
+        double g = 0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            g += pool.adj_g[3 * size_t(pixel) + c] * pool.adj_cie[3 * row + c];
+        w[k] = float(g * scale);
+    }
+    return make_float4(w[0], w[1], w[2], w[3]);
+}
+RP_DEV uint4 empty_history() { return make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu); }
+RP_DEV u32 history_byte(uint4 h, u32 j) {
+    const u32 word = j < 4 ? h.x : j < 8 ? h.y : j < 12 ? h.z : h.w;
+    return (word >> (8 * (j & 3))) & 0xffu;
+}
+// appends material m; a full history (16 vertices) is refused by the adjoint's depth limit
+RP_DEV uint4 history_push(uint4 h, u32 m) {
+    for (u32 j = 0; j < 16; ++j)
+        if (history_byte(h, j) == 0xffu) {
+            const u32 shift = 8 * (j & 3), mask = ~(0xffu << shift), v = (m & 0xffu) << shift;
+            if (j < 4)
+                h.x = (h.x & mask) | v;
+            else if (j < 8)
+                h.y = (h.y & mask) | v;
+            else if (j < 12)
+                h.z = (h.z & mask) | v;
+            else
+                h.w = (h.w & mask) | v;
+            break;
+        }
+    return h;
+}
+// d loss / d knots of one contribution, accumulated into the block's shared gradient
+__device__ __noinline__ void adjoint_accumulate(const DeviceScene &s, const PathPool &pool, float *sgrad, uint4 hist,
+                                                V4 lambda, V4 contribution, float4 w4) {
+    const float w[4] = {w4.x, w4.y, w4.z, w4.w};
+    for (u32 j = 0; j < 16; ++j) {
+        const u32 m = history_byte(hist, j);
+        if (m == 0xffu)
+            break;
+        const u32 slot = __ldg(pool.adj_slot + m);
+        const DMaterial M = s.materials[m];
+        const float2 *kn = s.knots + M.knot_begin;
+        for (int k = 0; k < 4; ++k) {
+            const float g0 = w[k] * contribution.v[k];
+            const float x = lambda.v[k];
+            if (g0 == 0 || !(x >= kn[0].x && x <= kn[M.knot_count - 1].x))
+                continue;
+            u32 lo = 0, hi = M.knot_count - 1;
+            while (hi - lo > 1) {
+                const u32 mid = lo + (hi - lo) / 2;
+                if (x < kn[mid].x)
+                    hi = mid;
+                else
+                    lo = mid;
+            }
+            const float t = lo == hi ? 0.0f : (x - kn[lo].x) / (kn[hi].x - kn[lo].x);
+            const float rho = kn[lo].y + (kn[hi].y - kn[lo].y) * t;
+            if (!(rho > 0))
+                continue;
+            const float g = g0 / rho;
+            atomicAdd(sgrad + slot + lo, g * (1.0f - t));
+            if (hi != lo)
+                atomicAdd(sgrad + slot + hi, g * t);
+        }
+    }
+}
+RP_DEV void adjoint_begin(const PathPool &pool, float *sgrad) {
+    if (!pool.hist)
+        return;
+    for (u32 i = threadIdx.x; i < pool.adj_params; i += blockDim.x)
+        sgrad[i] = 0;
+    __syncthreads();
+}
+RP_DEV void adjoint_end(const PathPool &pool, const float *sgrad) {
+    if (!pool.hist)
+        return;
+    __syncthreads();
+    for (u32 i = threadIdx.x; i < pool.adj_params; i += blockDim.x)
+        if (sgrad[i] != 0)
+            atomicAdd(pool.adj_grad + i, sgrad[i]);
 }
 
 } // namespace rp

@@ -59,6 +59,8 @@ def lib():
         "rp_cuda_build_light_tables": (C.c_int, [vp, u32, vp, vp, vp, vp, vp]),
         "rp_cuda_render_views_device": (st, [vp, C.POINTER(abi.View), u32, C.POINTER(abi.BatchRequest), vp,
                                              C.POINTER(abi.BatchConfig), cp, sz]),
+        "rp_cuda_set_knot_values": (st, [vp, u32, u32, vp, cp, sz]),
+        "rp_cuda_adjoint_device": (st, [vp, C.POINTER(abi.AdjointRequest), vp, vp, cp, sz]),
         "rp_cuda_tune_views": (st, [vp, C.POINTER(abi.View), u32, C.POINTER(abi.BatchRequest),
                                     C.POINTER(abi.BatchConfig), cp, sz]),
     }

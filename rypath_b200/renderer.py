@@ -140,7 +140,7 @@ class CudaRenderScene:
         self._cie_set = False
 
     def close(self):
-        if self._handle:
+        if self._handle and native is not None:
             native.lib().rp_cuda_scene_destroy(self._handle)
             self._handle = C.c_void_p()
 
@@ -225,6 +225,31 @@ class CudaRenderScene:
                                               diag, 512)
         native.check(st, diag, "rp_cuda_tune_views")
         return chosen
+
+    def set_knot_values(self, first: int, values):
+        """Overwrite knot values [first, first + len(values)) of the scene's spectral knots."""
+        v = np.ascontiguousarray(values, np.float32)
+        diag = C.create_string_buffer(512)
+        st = native.lib().rp_cuda_set_knot_values(self._handle, first, v.size, v.ctypes.data, diag, 512)
+        native.check(st, diag, "rp_cuda_set_knot_values")
+
+    def adjoint_device(self, settings: RenderSettings, materials, d_loss_d_xyz_ptr: int, gradient_ptr: int,
+                       sample_begin: int = 0):
+        """Backward pass of ``render_film`` with these settings: d loss / d knot values of
+        ``materials`` (device float gradient) from d loss / d film-mean XYZ (device doubles)."""
+        self._ensure_cie()
+        mats = np.ascontiguousarray(materials, np.uint32)
+        r = abi.AdjointRequest()
+        r.film = abi.FilmRequest(width=settings.width, height=settings.height, seed=settings.seed,
+                                 sample_begin=sample_begin, sample_count=settings.samples,
+                                 batch_size=settings.batch_size, sampler_kind=settings.sampler,
+                                 randomization=settings.randomization, emergency_limit=1024)
+        r.material_count = mats.size
+        r.materials = mats.ctypes.data_as(C.POINTER(C.c_uint32))
+        diag = C.create_string_buffer(512)
+        st = native.lib().rp_cuda_adjoint_device(self._handle, C.byref(r), C.c_void_p(d_loss_d_xyz_ptr),
+                                                  C.c_void_p(gradient_ptr), diag, 512)
+        native.check(st, diag, "rp_cuda_adjoint_device")
 
     def timing(self) -> abi.Timing:
         t = abi.Timing()

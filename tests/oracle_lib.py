@@ -44,6 +44,7 @@ def oracle():
         lib.or_sample_scalar.argtypes = [vp, C.POINTER(abi.Request), vp, sz, C.c_int]
         lib.or_probe_medium.argtypes = [vp, u32, vp]
         lib.or_scalar_film_add.argtypes = [vp, sz, vp, u32, vp]
+        lib.or_adjoint.argtypes = [vp, C.POINTER(abi.FilmRequest), vp, u32, vp, vp, vp, C.c_int]
         _oracle = lib
     return _oracle
 
@@ -118,3 +119,41 @@ def request(width, height, spp=1, sample_begin=0, pixel_begin=0, pixel_count=Non
     r.sample_begin, r.sample_count = sample_begin, spp
     r.emergency_limit, r.sampler_kind, r.randomization, r.boundary_limit = 1024, sampler, randomization, 4096
     return r
+
+
+def film_request(width, height, spp, seed=1, sample_begin=0, sampler=abi.SAMPLER_SOBOL,
+                 randomization=abi.RANDOMIZE_OWEN, batch_size=None):
+    return abi.FilmRequest(width=width, height=height, seed=seed, sample_begin=sample_begin, sample_count=spp,
+                           batch_size=batch_size or spp, sampler_kind=sampler, randomization=randomization,
+                           emergency_limit=1024)
+
+
+def oracle_film_mean(scene, width, height, spp, seed=1, sampler=abi.SAMPLER_SOBOL, threads=0):
+    """Film-mean XYZ (pixels x 3) of the oracle's hero render."""
+    import numpy as np
+
+    from rypath_b200 import renderer, scenes
+
+    lanes = OracleScene(scene).sample(request(width, height, spp, seed=seed, sampler=sampler), threads)
+    film = np.zeros(width * height, abi.film_dtype())
+    cie = np.ascontiguousarray(scenes.cie_xyz())
+    assert oracle().or_film_add(lanes.ctypes.data, lanes.size, cie.ctypes.data, width * height, film.ctypes.data) == 0
+    return renderer.film_mean(film)
+
+
+def oracle_adjoint(scene, width, height, spp, materials, d_loss_d_xyz, seed=1, sampler=abi.SAMPLER_SOBOL, threads=0):
+    import numpy as np
+
+    from rypath_b200 import scenes
+
+    o = OracleScene(scene)
+    mats = np.ascontiguousarray(materials, np.uint32)
+    params = sum(int(scene.materials[m].knot_count) for m in materials)
+    grad = np.zeros(params, np.float64)
+    g = np.ascontiguousarray(d_loss_d_xyz, np.float64)
+    cie = np.ascontiguousarray(scenes.cie_xyz())
+    fr = film_request(width, height, spp, seed=seed, sampler=sampler)
+    rc = oracle().or_adjoint(o.handle, C.byref(fr), mats.ctypes.data, len(materials), g.ctypes.data, cie.ctypes.data,
+                             grad.ctypes.data, threads)
+    assert rc == 0, rc
+    return grad
