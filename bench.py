@@ -50,6 +50,9 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-secondary", action="store_true",
+                   help="skip the fog, batched-views and adjoint workloads (run at N=1 only)")
+    p.add_argument("--adam-steps", type=int, default=200)
     return p.parse_args()
 
 
@@ -169,6 +172,173 @@ def run_reference(args, rank):
             "config": cfg, "cpu_baseline": dict(values[-1], value=value),
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def bench_fog(torch, cpu_seconds):
+    """Scalar volpath: the Cornell-style box filled with a homogeneous medium (sigma_s mean 0.5,
+    albedo 0.9, HG g = 0.7), 1024x1024, 64 spp, depth 32, one wavelength per sample."""
+    from rypath_b200 import renderer, scenes
+
+    from tests.oracle_lib import OracleScene, request
+
+    w, spp = 1024, 64
+    scene = scenes.cornell_fog(w, w, spp, 32)
+    rs = renderer.build_renderer(scene).scene
+    film = torch.zeros(w * w * 12, dtype=torch.float64, device="cuda")
+    probe = renderer.RenderSettings(w, w, samples=8, batch_size=8, seed=1)
+    rs.render_film_device(probe, film.data_ptr())
+    rs.set_counting(True)
+    film.zero_()
+    rs.render_film_device(probe, film.data_ptr())
+    counts = rs.timing()
+    rs.set_counting(False)
+    film.zero_()
+    rs.render_film_device(renderer.RenderSettings(w, w, samples=spp, batch_size=spp, seed=1), film.data_ptr(),
+                          sample_begin=8)
+    t = rs.timing()
+    rays_per_sample = (counts.closest_rays + counts.shadow_rays) / counts.samples
+    value = t.samples / t.total_ms / 1e3
+    rs.close()
+    orc = OracleScene(scene)
+    n = 16384
+    t0 = time.perf_counter()
+    orc.sample_scalar(request(w, w, 1, pixel_begin=(w * w - n) // 2, pixel_count=n))
+    rate = n / (time.perf_counter() - t0)
+    n = int(min(w * w, max(n, rate * cpu_seconds)))
+    t0 = time.perf_counter()
+    out = orc.sample_scalar(request(w, w, 1, pixel_begin=(w * w - n) // 2, pixel_count=n))
+    dt = time.perf_counter() - t0
+    return {"workload": "cornell_fog_1024x1024_64spp_depth32 (scalar volpath, homogeneous medium)",
+            "metric": "scalar path Msamples/s", "value": value, "unit": UNIT, "ms_per_step": t.total_ms,
+            "kernel": "k_volpath (persistent path regeneration, one closest-hit query per loop trip)",
+            "rays_per_sample": rays_per_sample, "mrays_per_s": value * rays_per_sample,
+            "cpu_baseline": {"value": out.size / dt / 1e6, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                             "sample": f"{out.size} lanes (1 spp of pixels around the film centre), {dt:.2f} s"}}
+
+
+def bench_views(torch):
+    """Batched form: 64 seeded views of the mixed scene (resolutions U[256x256, 1280x720],
+    spp from {4, 8, 16, 32, 64}) in one wavefront with graph replay and tuned shapes, against
+    one plain wavefront per view; both films are compared bit for bit."""
+    from rypath_b200 import renderer, scenes
+
+    scene = scenes.mixed_scene(64, 64, 1, 16)
+    views = scenes.view_batch(scene, count=64, seed=1)
+    total = renderer.pack_views(views)
+    lanes = sum(v.width * v.height * v.sample_count for v in views)
+    rs = renderer.build_renderer(scene).scene
+    film = torch.zeros(total * 96, dtype=torch.uint8, device="cuda")
+    t0 = time.perf_counter()
+    chosen = rs.tune_views(views, renderer.BatchRequest())
+    tune_s = time.perf_counter() - t0
+    req = renderer.BatchRequest(wave_lanes=chosen.wave_lanes, trace_block=chosen.trace_block,
+                                shade_block=chosen.shade_block, blocks_per_sm=chosen.blocks_per_sm, use_graph=1)
+    batched_ms = []
+    for _ in range(2):
+        film.zero_()
+        rs.render_views_device(views, req, film.data_ptr())
+        batched_ms.append(rs.timing().total_ms)
+    batched = film.clone()
+    plain_req = renderer.BatchRequest(wave_lanes=1 << 23, trace_block=128, shade_block=128, blocks_per_sm=12,
+                                      use_graph=2)
+    film.zero_()
+    plain_ms = 0.0
+    for v in views:
+        one = renderer.View(v.camera, v.width, v.height, v.sample_begin, v.sample_count, 0)
+        sub = film[v.film_offset * 96:(v.film_offset + v.width * v.height) * 96]
+        rs.render_views_device([one], plain_req, sub.data_ptr())
+        plain_ms += rs.timing().total_ms
+    identical = bool(torch.equal(batched, film))
+    rs.close()
+    ms = min(batched_ms)
+    return {"workload": "64 views of the mixed scene, resolutions U[256x256, 1280x720], spp {4..64}",
+            "metric": "batched Msamples/s (all views)", "value": lanes / ms / 1e3, "unit": UNIT,
+            "plain_per_view_value": lanes / plain_ms / 1e3, "speedup_vs_plain": plain_ms / ms,
+            "films_identical_to_plain": identical, "lanes": lanes, "batched_ms": ms, "plain_ms": plain_ms,
+            "tuned": {"wave_lanes": chosen.wave_lanes, "trace_block": chosen.trace_block,
+                      "shade_block": chosen.shade_block, "blocks_per_sm": chosen.blocks_per_sm,
+                      "probe_ms_per_mlane": chosen.probe_ms_per_mlane, "tuning_s": tune_s},
+            "equal_rmse": "identical films: the batched form renders exactly the plain lanes"}
+
+
+def bench_adjoint(torch, adam_steps):
+    """Differentiation: 16 reflectance groups x 32 knots of the Cornell geometry, 512x512,
+    32 spp, depth 8, L2 loss on film-mean XYZ against a 128-spp render of seeded true
+    spectra.  The path-replay adjoint gradient against central differences (h = 1e-3, common
+    random numbers) of the same renders; errors against an 8x-spp adjoint gradient."""
+    from rypath_b200 import renderer, scenes
+
+    w, spp, params = 512, 32, 512
+    scene, truth = scenes.cornell_groups(w, w, spp, 8)
+    mats = list(range(16))
+    rs = renderer.build_renderer(scene).scene
+    rt = renderer.build_renderer(truth).scene
+
+    def mean(r, n, seed):
+        film = torch.zeros(w * w * 12, dtype=torch.float64, device="cuda")
+        r.render_film_device(renderer.RenderSettings(w, w, samples=n, batch_size=n, seed=seed), film.data_ptr())
+        torch.cuda.synchronize()
+        f = film.reshape(w * w, 12)
+        return (f[:, 0:3] + f[:, 3:6]) / (f[:, 6:7] + f[:, 7:8]), r.timing().total_ms
+
+    def adjoint(r, n, seed, g):
+        grad = torch.zeros(params, dtype=torch.float32, device="cuda")
+        r.adjoint_device(renderer.RenderSettings(w, w, samples=n, batch_size=n, seed=seed), mats,
+                         g.contiguous().data_ptr(), grad.data_ptr())
+        torch.cuda.synchronize()
+        return grad.cpu().numpy().astype(np.float64), r.timing().total_ms
+
+    target, _ = mean(rt, 128, 11)
+    rt.close()
+    theta0 = np.concatenate([scene.knots[32 * g:32 * g + 32, 1] for g in range(16)]).astype(np.float32)
+    for _ in range(2):
+        m, f_ms = mean(rs, spp, 1)
+        grad, b_ms = adjoint(rs, spp, 1, 2 * (m - target))
+    mref, _ = mean(rs, 8 * spp, 7)
+    gref, _ = adjoint(rs, 8 * spp, 7, 2 * (mref - target))
+    sub = list(range(3, params, 32))
+    fd, fd_ms = [], 0.0
+    h = 1e-3
+    for j in sub:
+        th = theta0.copy()
+        th[j] += h
+        rs.set_knot_values(0, th)
+        mp, a = mean(rs, spp, 1)
+        th[j] -= 2 * h
+        rs.set_knot_values(0, th)
+        mm, b = mean(rs, spp, 1)
+        fd_ms += a + b
+        fd.append((float(((mp - target) ** 2).sum()) - float(((mm - target) ** 2).sum())) / (2 * h))
+    rs.set_knot_values(0, theta0)
+    fd = np.array(fd)
+    rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
+    th, mom, vel, losses, dev_ms = theta0.copy(), np.zeros(params), np.zeros(params), [], 0.0
+    t0 = time.perf_counter()
+    for k in range(1, adam_steps + 1):
+        rs.set_knot_values(0, th)
+        m, a = mean(rs, spp, k)
+        gr, b = adjoint(rs, spp, k, 2 * (m - target))
+        dev_ms += a + b
+        losses.append(float(((m - target) ** 2).sum()))
+        mom = 0.9 * mom + 0.1 * gr
+        vel = 0.999 * vel + 0.001 * gr * gr
+        step = 0.02 * (mom / (1 - 0.9 ** k)) / (np.sqrt(vel / (1 - 0.999 ** k)) + 1e-8)
+        th = np.clip(th - step, 0.01, 1.0).astype(np.float32)
+    adam_s = time.perf_counter() - t0
+    rs.close()
+    adjoint_ms = f_ms + b_ms
+    fd_full_ms = fd_ms / len(sub) * params
+    return {"workload": "cornell_groups 512x512, 32 spp, depth 8, 16 groups x 32 knots, L2 on XYZ",
+            "metric": "gradient ms (forward + backward)", "value": adjoint_ms, "unit": "ms", "higher_is_better": False,
+            "forward_ms": f_ms, "backward_ms": b_ms,
+            "finite_difference_ms": fd_full_ms, "speedup_vs_finite_difference": fd_full_ms / adjoint_ms,
+            "finite_difference": f"central, h = {h}, common random numbers, {len(sub)} of {params} parameters "
+                                 f"timed ({fd_ms:.0f} ms), whole-gradient time scaled by parameter count",
+            "relative_error_vs_8x_adjoint": {"adjoint_all": rel(grad, gref), "adjoint_subset": rel(grad[sub], gref[sub]),
+                                             "finite_difference_subset": rel(fd, gref[sub])},
+            "adam": {"steps": adam_steps, "lr": 0.02, "loss_first": losses[0] if losses else None,
+                     "loss_last": losses[-1] if losses else None, "device_ms_per_step": dev_ms / max(1, adam_steps),
+                     "wall_s": adam_s}}
 
 
 def main():
@@ -330,6 +500,9 @@ def main():
         from tests.oracle_lib import OracleScene
 
         line["cpu_baseline"] = cpu_baseline(OracleScene(scene), args, args.cpu_seconds)
+    if line is not None and world == 1 and not args.no_secondary:
+        line["secondary"] = {"volpath": bench_fog(torch, 4.0), "batched_views": bench_views(torch),
+                             "adjoint": bench_adjoint(torch, args.adam_steps)}
     if dist:
         dist.barrier()
         dist.destroy_process_group()

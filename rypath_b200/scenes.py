@@ -289,6 +289,58 @@ def cornell_fog(width=1024, height=1024, spp=64, max_depth=32, sigma_s_mean=0.5,
     return scene
 
 
+def cornell_groups(width=512, height=512, spp=32, max_depth=8, seed=1, start=0.5):
+    """The Cornell-style box with 16 reflectance groups of 32 knots each, for differentiation.
+
+    Groups: the 5 walls, the 6 faces of the short box, and the tall box's faces with its top
+    and bottom sharing a group (5), 16 in all; the light keeps its black material.  Returns
+    (scene, truth): ``scene`` starts every group at the constant ``start`` reflectance and
+    ``truth`` (same geometry) holds seeded smooth ground-truth spectra in [0.1, 0.9].
+    Materials 0..15 are the groups.
+    """
+    base = cornell_box(width, height, spp, max_depth)
+    positions, triangles, instances = [], [], []
+    group_of_triangle = [0, 0, 1, 1, 2, 2, 3, 3, 4, 4]  # walls (floor, ceiling, back, left, right)
+    group_of_triangle += [5 + f // 2 for f in range(12)]  # short box: 6 faces
+    tall = [11, 11, 12, 12, 13, 13, 14, 14, 15, 15, 16, 16]  # faces z0, z1, y0, y1, x0, x1
+    tall = [t if t != 16 else 11 for t in tall]  # x1 face joins the z0 face's group
+    group_of_triangle += [t for t in tall]
+    # one instance per triangle of the groups, then the light
+    rng = np.random.default_rng(seed)
+    # world-space corners of every triangle (triangle indices are local to their instance)
+    corners = []
+    for inst in base.instances:
+        for t in range(inst.triangle_count):
+            corners.append(base.positions[inst.vertex_begin + base.triangles[inst.triangle_begin + t]])
+    light_inst = base.instances[-1]
+    for t in range(34):
+        positions.append(corners[t])
+        triangles.append(np.array([[0, 1, 2]], np.uint32))
+        instances.append(identity_instance(3 * t, t, 1, group_of_triangle[t]))
+    lv = np.concatenate(corners[34:36])
+    positions.append(lv)
+    triangles.append(np.array([[0, 1, 2], [3, 4, 5]], np.uint32))
+    instances.append(identity_instance(3 * 34, 34, 2, 16, light_inst.emission))
+    positions = np.concatenate(positions).astype(np.float32)
+    triangles = np.concatenate(triangles)
+    # rebase triangle vertex indices to instance-local ones
+    w = np.linspace(360.0, 830.0, 32)
+
+    def make(values_per_group):
+        knots = np.concatenate([knots_from_curve(v) for v in values_per_group] + [knots_from_curve(0.0)])
+        materials = [diffuse_material(32 * g) for g in range(17)]
+        sc = Scene("cornell_groups", width, height, spp, positions.copy(), triangles.copy(), list(instances),
+                   materials, knots, emissions=list(base.emissions), max_depth=max_depth)
+        sc.camera = base.camera
+        return sc
+
+    truth_values = []
+    for _ in range(16):
+        anchors = rng.uniform(0.1, 0.9, 6)
+        truth_values.append(np.interp(w, np.linspace(360, 830, 6), anchors))
+    return make([np.full(32, start)] * 16), make(truth_values)
+
+
 def view_batch(scene: Scene, count=64, seed=1, min_size=(256, 256), max_size=(1280, 720), spp=(4, 8, 16, 32, 64),
                target=(0.0, 0.35, 0.0), distance=(2.2, 4.0), vfov=40.0):
     """Seeded camera views of one scene for batched rendering: uniform resolutions between
