@@ -57,7 +57,7 @@ enum { RP_SAMPLER_INDEPENDENT = 0, RP_SAMPLER_SOBOL = 1 };
 enum { RP_RANDOMIZE_NONE = 0, RP_RANDOMIZE_PERMUTEDIGITS = 1, RP_RANDOMIZE_FASTOWEN = 2,
        RP_RANDOMIZE_OWEN = 3 };
 /* Pixel filters (src/render_wire.h:29). */
-enum { RP_FILTER_BOX = 0, RP_FILTER_TRIANGLE = 1 };
+enum { RP_FILTER_BOX = 0, RP_FILTER_TRIANGLE = 1, RP_FILTER_GAUSSIAN = 2 };
 /* Scattering families (wire::Material::scattering, src/render_wire.h:121). */
 enum { RP_DIFFUSE = 0, RP_CONDUCTOR = 1, RP_DIELECTRIC = 2 };
 /* Null medium interface (ScatteringKind::null_interface, wire scattering 10,
@@ -150,6 +150,12 @@ typedef struct rp_scene_desc {
     uint32_t transport;        /* RP_TRANSPORT_HERO (scalar volpath: RP_TRANSPORT_SCALAR) */
     uint32_t hero_wavelengths; /* RP_HERO_* */
     const void *sobol_tables;  /* RP_SOBOL_TABLE_BYTES, sobol::Tables layout */
+    /* PerspectiveLens (src/render.hpp:159-164): aperture radius (0 = pinhole), focal
+     * distance, and the camera's x / y axes in world space.  Batched views are pinhole. */
+    float lens_radius, focal_distance;
+    float lens_x[3], lens_y[3];
+    /* RP_FILTER_GAUSSIAN: PBRT sigma; the radii are filter_x_radius / filter_y_radius. */
+    float filter_sigma;
 } rp_scene_desc;
 
 /* RenderRequest (src/metal_render.hpp:14-32). */

@@ -55,6 +55,12 @@ void or_probe_light_select(const or_scene *scene, const float *queries, uint32_t
 int or_film_add(const rp_packet_result *results, size_t count, const double *cie_xyz,
                 uint32_t pixel_count, rp_film_pixel *film);
 
+/* Gaussian pixel filter: the table of compile_gaussian_filter (src/gaussian_filter.cpp) and the
+ * device inverse of shaders/render.metal:200-236 on count (u, v) pairs.  Returns the table
+ * size in floats (conditional rows then marginal), or -1. */
+int or_gaussian_filter(float x_radius, float y_radius, float sigma, float *cdf, size_t capacity, uint32_t *size,
+                       float *integral, const float *uv, uint32_t count, float *samples);
+
 /* FP64 path-replay adjoint of a film render (the rp_cuda_adjoint_device contract): gradient of
  * the loss with respect to the knot values of `materials`, given d loss / d film-mean XYZ per
  * pixel and the CIE table.  0, 1 when a lane failed, -1 on a bad material list. */

@@ -16,7 +16,37 @@ struct Params {
 struct Sample {
     u32 status = 0, pixel = 0, sample_low = 0, sample_high = 0;
     u32 words[4] = {0, 0, 0, 0};
+    u32 lens_words[2] = {0, 0};
+    float filter_offsets[2] = {0, 0};
 };
+// shaders/render.metal:200-236 (gaussian_filter_offsets)
+inline void gaussian_filter_offsets(const Scene &s, float ux, float uy, float &x, float &y) {
+    const float *cdf = s.gauss_cdf.data();
+    const float *marginal = cdf + size_t(s.gauss_h) * (s.gauss_w + 1);
+    u32 low = 0, high = s.gauss_h;
+    while (low + 1 < high) {
+        const u32 mid = (low + high) / 2;
+        if (marginal[mid] <= uy)
+            low = mid;
+        else
+            high = mid;
+    }
+    const u32 row = low;
+    const float ty = (float(row) + (uy - marginal[row]) / (marginal[row + 1] - marginal[row])) / float(s.gauss_h);
+    const float *conditional = cdf + size_t(row) * (s.gauss_w + 1);
+    low = 0;
+    high = s.gauss_w;
+    while (low + 1 < high) {
+        const u32 mid = (low + high) / 2;
+        if (conditional[mid] <= ux)
+            low = mid;
+        else
+            high = mid;
+    }
+    const float tx = (float(low) + (ux - conditional[low]) / (conditional[low + 1] - conditional[low])) / float(s.gauss_w);
+    x = (1 - tx) * (-s.filter_x) + tx * s.filter_x;
+    y = (1 - ty) * (-s.filter_y) + ty * s.filter_y;
+}
 
 // shaders/render.metal:113-118 (sobol and independent samplers)
 inline float sample_uniform(const Params &p, u32 w) {
@@ -55,6 +85,24 @@ inline Sample begin_sample(const Scene &s, const Params &p, u32 lane, u64 &index
         r.words[2] = w.z;
         r.words[3] = w.w;
     }
+    if (s.lens_radius > 0) {
+        if (p.sampler == RP_SAMPLER_SOBOL) {
+            const SobolTables &t = *s.sobol;
+            r.lens_words[0] = sobol_word(t, index, 1022, p.randomization, p.seed_low); // lens_x_dimension
+            r.lens_words[1] = sobol_word(t, index, 1023, p.randomization, p.seed_low);
+        } else {
+            const U4 w = philox(U4{r.pixel, r.sample_low, r.sample_high, 0xc0000000u}, p.seed_low, p.seed_high);
+            r.lens_words[0] = w.x;
+            r.lens_words[1] = w.y;
+        }
+    }
+    if (s.filter_kind == RP_FILTER_GAUSSIAN) {
+        const float ux = p.sampler == RP_SAMPLER_SOBOL ? sobol_camera_uniform(r.words[0], p.m, r.pixel % p.width)
+                                                       : u01(r.words[0]);
+        const float uy = p.sampler == RP_SAMPLER_SOBOL ? sobol_camera_uniform(r.words[1], p.m, r.pixel / p.width)
+                                                       : u01(r.words[1]);
+        gaussian_filter_offsets(s, ux, uy, r.filter_offsets[0], r.filter_offsets[1]);
+    }
     return r;
 }
 // shaders/render.metal:352-357
@@ -62,7 +110,7 @@ inline float triangle_offset(float u, float radius) {
     const float s = 2.0f * u - 1.0f;
     return radius * (s / (1.0f + std::sqrt(1.0f - std::fabs(s))));
 }
-// shaders/render.metal:341-350, :400-476 (primary_ray, PBRT model, no lens)
+// shaders/render.metal:341-476 (primary_ray: pinhole or thin lens; box, triangle or Gaussian filter)
 inline void primary_ray(const Scene &s, const Params &p, const Sample &smp, F3 &o, F3 &d) {
     float ux, uy;
     if (p.sampler == RP_SAMPLER_SOBOL) {
@@ -74,15 +122,50 @@ inline void primary_ray(const Scene &s, const Params &p, const Sample &smp, F3 &
     }
     o = s.origin;
     const bool centered = s.filter_kind != RP_FILTER_BOX || s.filter_x != 0.5f || s.filter_y != 0.5f;
+    F3 dd;
     if (centered) {
-        const float ox = s.filter_kind == RP_FILTER_TRIANGLE ? triangle_offset(ux, s.filter_x)
-                                                             : (2.0f * ux - 1.0f) * s.filter_x;
-        const float oy = s.filter_kind == RP_FILTER_TRIANGLE ? triangle_offset(uy, s.filter_y)
-                                                             : (2.0f * uy - 1.0f) * s.filter_y;
+        const float ox = s.filter_kind == RP_FILTER_GAUSSIAN   ? smp.filter_offsets[0]
+                         : s.filter_kind == RP_FILTER_TRIANGLE ? triangle_offset(ux, s.filter_x)
+                                                               : (2.0f * ux - 1.0f) * s.filter_x;
+        const float oy = s.filter_kind == RP_FILTER_GAUSSIAN   ? smp.filter_offsets[1]
+                         : s.filter_kind == RP_FILTER_TRIANGLE ? triangle_offset(uy, s.filter_y)
+                                                               : (2.0f * uy - 1.0f) * s.filter_y;
         const float x = ((float(smp.pixel % p.width) + 0.5f) + ox) / float(p.width);
         const float y = ((float(smp.pixel / p.width) + 0.5f) + oy) / float(p.height);
-        const F3 dd = fma3(F3{y, y, y}, s.up, fma3(F3{x, x, x}, s.right, s.forward));
+        dd = fma3(F3{y, y, y}, s.up, fma3(F3{x, x, x}, s.right, s.forward));
+    } else {
+        const float x = (float(smp.pixel % p.width) + ux) / float(p.width);
+        const float y = (float(smp.pixel / p.width) + uy) / float(p.height);
+        dd = s.forward + x * s.right + y * s.up;
+    }
+    if (s.lens_radius > 0) {
+        // lens_point (shaders/render.metal:366-387): concentric disk, PBRT perspective lens
+        const float lx = 2.0f * sample_uniform(p, smp.lens_words[0]) - 1.0f;
+        const float ly = 2.0f * sample_uniform(p, smp.lens_words[1]) - 1.0f;
+        F3 offset{0, 0, 0};
+        if (!(lx == 0 && ly == 0)) {
+            const float pi = 3.14159265358979323846f;
+            float radius, theta;
+            if (std::fabs(lx) > std::fabs(ly)) {
+                radius = lx;
+                theta = (pi / 4.0f) * (ly / lx);
+            } else {
+                radius = ly;
+                theta = pi / 2.0f - (pi / 4.0f) * (lx / ly);
+            }
+            const float r = s.lens_radius * radius;
+            const F3 ideal = (r * std::cos(theta)) * s.lens_x + (r * std::sin(theta)) * s.lens_y;
+            o = s.origin + ideal;
+            offset = o - s.origin;
+        }
+        // lens_primary_ray (:413-432) and rypath_texture_direction (shaders/texture_footprint.h:14-20)
+        dd = dd - offset / s.focal_distance;
         const float scale = std::max(std::fabs(dd.x), std::max(std::fabs(dd.y), std::fabs(dd.z)));
+        d = (!(scale > 0.0f) || !finite3(dd)) ? F3{NAN, NAN, NAN} : normalize3(dd / scale);
+        return;
+    }
+    const float scale = std::max(std::fabs(dd.x), std::max(std::fabs(dd.y), std::fabs(dd.z)));
+    if (centered) {
         if (!finite3(dd) || !(scale > 0.0f)) {
             d = F3{NAN, NAN, NAN};
             return;
@@ -95,10 +178,6 @@ inline void primary_ray(const Scene &s, const Params &p, const Sample &smp, F3 &
         d = normalize3(scaled);
         return;
     }
-    const float x = (float(smp.pixel % p.width) + ux) / float(p.width);
-    const float y = (float(smp.pixel / p.width) + uy) / float(p.height);
-    const F3 dd = s.forward + x * s.right + y * s.up;
-    const float scale = std::max(std::fabs(dd.x), std::max(std::fabs(dd.y), std::fabs(dd.z)));
     d = normalize3(dd / scale);
 }
 

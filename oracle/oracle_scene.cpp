@@ -361,6 +361,18 @@ bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error) {
     s.filter_kind = d.filter_kind;
     s.filter_x = d.filter_x_radius;
     s.filter_y = d.filter_y_radius;
+    if (d.filter_kind == RP_FILTER_GAUSSIAN) {
+        float integral = 0;
+        error = gaussian_filter_table(d.filter_x_radius, d.filter_y_radius, d.filter_sigma, s.gauss_cdf, s.gauss_w,
+                                      s.gauss_h, integral);
+        if (!error.empty())
+            return false;
+        s.filter_weight = d.transport == RP_TRANSPORT_HERO ? integral : 1.0f;
+    }
+    s.lens_radius = d.lens_radius;
+    s.focal_distance = d.lens_radius > 0 ? d.focal_distance : 1e6f;
+    s.lens_x = F3{d.lens_x[0], d.lens_x[1], d.lens_x[2]};
+    s.lens_y = F3{d.lens_y[0], d.lens_y[1], d.lens_y[2]};
     s.max_depth = d.max_depth;
     s.light_sampler = d.light_sampler;
     s.hero_mode = d.hero_wavelengths;
@@ -825,6 +837,81 @@ Hit trace_closest_brute(const Scene &s, F3 o, F3 d, float tmax) {
             h = Hit{t, b1, b2, p};
     }
     return h.prim == RP_NONE ? Hit{} : h;
+}
+
+// ================================================================= Gaussian pixel filter
+// PBRT FastExp (as in src/gaussian_filter.cpp:19-35)
+static float fast_exp(float x) {
+    if (x < -100.f)
+        return 0;
+    const float xp = x * 1.442695041f;
+    const float fxp = std::floor(xp);
+    const float f = xp - fxp;
+    const int i = int(fxp);
+    const float polynomial = std::fma(f, std::fma(f, std::fma(f, 0.0781455737f, 0.226173572f), 0.695556856f), 1.f);
+    u32 bits = fbits(polynomial);
+    const int exponent = int((bits >> 23) & 255) - 127 + i;
+    if (exponent < -126)
+        return 0;
+    bits = (bits & 0x807fffffu) | (u32(exponent + 127) << 23);
+    return ffrom(bits);
+}
+// src/gaussian_filter.cpp:39-68 (normalised piecewise-constant CDF of n values over 2 radius)
+static bool table_cdf(const float *values, size_t n, float radius, float *cdf, float &integral) {
+    cdf[0] = 0;
+    for (size_t i = 0; i < n; ++i) {
+        cdf[i + 1] = cdf[i] + values[i] * (2 * radius) / float(n);
+        if (!std::isfinite(cdf[i + 1]))
+            return false;
+    }
+    integral = cdf[n];
+    if (integral > 0 && !std::isnormal(integral))
+        return false;
+    for (size_t i = 1; i <= n; ++i)
+        cdf[i] = integral == 0 ? float(i) / float(n) : cdf[i] / integral;
+    for (size_t i = 1; i <= n; ++i) {
+        const float gap = cdf[i] - cdf[i - 1];
+        if (!std::isfinite(cdf[i]) || (cdf[i] > 0 && !std::isnormal(cdf[i])) || (gap > 0 && !std::isnormal(gap)))
+            return false;
+    }
+    return true;
+}
+std::string gaussian_filter_table(float xr, float yr, float sigma, std::vector<float> &cdf, u32 &width, u32 &height,
+                                  float &integral) {
+    if (!std::isnormal(xr) || xr <= 0 || !std::isnormal(yr) || yr <= 0 || !std::isnormal(sigma) || sigma <= 0)
+        return "Gaussian radii and sigma must be positive normal binary32 values";
+    const float nx = 32 * xr, ny = 32 * yr;
+    if (!(nx >= 1 && nx < 4097.f && ny >= 1 && ny < 4097.f))
+        return "Gaussian table axis must contain 1 to 4096 cells";
+    width = u32(nx);
+    height = u32(ny);
+    if (u64(width) * height > 1048576)
+        return "Gaussian table exceeds the 1048576-cell limit";
+    const float denominator = 2 * 3.14159265358979323846f * sigma * sigma;
+    const float tss = 2 * sigma * sigma;
+    const float scale = 1 / std::sqrt(denominator);
+    if (!(denominator > 0 && std::isfinite(denominator) && tss > 0 && std::isfinite(tss) && std::isfinite(scale)))
+        return "Gaussian sigma arithmetic overflows or collapses in binary32";
+    const auto gaussian = [&](float x) { return scale * fast_exp(-(x * x) / tss); };
+    const auto lerp = [](float t, float a, float b) { return (1 - t) * a + t * b; };
+    const float ex = gaussian(xr), ey = gaussian(yr);
+    cdf.assign(size_t(height) * (width + 1) + height + 1, 0.f);
+    std::vector<float> values(width), rows(height);
+    for (u32 y = 0; y < height; ++y) {
+        const float py = lerp((float(y) + 0.5f) / float(height), -yr, yr);
+        const float fy = std::max(0.f, gaussian(py) - ey);
+        for (u32 x = 0; x < width; ++x) {
+            const float px = lerp((float(x) + 0.5f) / float(width), -xr, xr);
+            values[x] = std::max(0.f, gaussian(px) - ex) * fy;
+            if (!std::isfinite(values[x]))
+                return "Gaussian table contains nonfinite binary32 values";
+        }
+        if (!table_cdf(values.data(), width, xr, cdf.data() + size_t(y) * (width + 1), rows[y]))
+            return "Gaussian conditional distribution overflows or collapses in binary32";
+    }
+    if (!table_cdf(rows.data(), height, yr, cdf.data() + size_t(height) * (width + 1), integral) || !(integral > 0))
+        return "Gaussian table has a zero or nonfinite binary32 integral";
+    return {};
 }
 
 // ================================================================= surface points

@@ -95,6 +95,13 @@ struct Scene {
     F3 origin, forward, right, up, camera_normal;
     u32 filter_kind = 0;
     float filter_x = .5f, filter_y = .5f;
+    // Gaussian filter table (conditional rows of gauss_w + 1, then the marginal) and the
+    // packet film weight; thin lens
+    std::vector<float> gauss_cdf;
+    u32 gauss_w = 0, gauss_h = 0;
+    float filter_weight = 1;
+    float lens_radius = 0, focal_distance = 1e6f;
+    F3 lens_x{1, 0, 0}, lens_y{0, 1, 0};
     u32 max_depth = 5, light_sampler = 0, hero_mode = 1;
     float scene_radius = 1;
     F3 scene_center{};
@@ -108,6 +115,9 @@ struct Scene {
     std::vector<u32> tri_instance, tri_local;
 };
 bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error);
+// compile_gaussian_filter (src/gaussian_filter.cpp:84-137); empty string on success
+std::string gaussian_filter_table(float x_radius, float y_radius, float sigma, std::vector<float> &cdf, u32 &width,
+                                  u32 &height, float &integral);
 
 // ---------------------------------------------------------------- binary LBVH
 struct Box {

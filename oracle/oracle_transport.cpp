@@ -574,7 +574,7 @@ static rp_packet_result render_lane(const Ctx &c, u32 lane, AdjointLane *adj = n
     r.pixel = st.sample.pixel;
     r.sample_low = st.sample.sample_low;
     r.sample_high = st.sample.sample_high;
-    r.filter_weight = 1;
+    r.filter_weight = s.filter_weight;
     for (int k = 0; k < 4; ++k) {
         r.wavelengths[k] = st.lambda.lambda[k];
         r.wavelength_pdfs[k] = st.lambda.pdf[k];
@@ -719,6 +719,26 @@ int or_adjoint(const or_scene *scene, const rp_film_request *f, const uint32_t *
     return failures ? 1 : 0;
 }
 
+// The Gaussian filter table (compile_gaussian_filter) and its inverse as the device samples it
+// (gaussian_filter_offsets): cdf receives the conditional rows then the marginal; samples
+// receive (x, y) for each of count (u, v) pairs.  Returns the table size in floats, or -1.
+int or_gaussian_filter(float x_radius, float y_radius, float sigma, float *cdf, size_t capacity, uint32_t *size,
+                       float *integral, const float *uv, uint32_t count, float *samples) {
+    Scene s;
+    s.filter_kind = RP_FILTER_GAUSSIAN;
+    s.filter_x = x_radius;
+    s.filter_y = y_radius;
+    if (!gaussian_filter_table(x_radius, y_radius, sigma, s.gauss_cdf, s.gauss_w, s.gauss_h, *integral).empty() ||
+        s.gauss_cdf.size() > capacity)
+        return -1;
+    std::copy(s.gauss_cdf.begin(), s.gauss_cdf.end(), cdf);
+    size[0] = s.gauss_w;
+    size[1] = s.gauss_h;
+    for (uint32_t i = 0; i < count; ++i)
+        gaussian_filter_offsets(s, uv[2 * i], uv[2 * i + 1], samples[2 * i], samples[2 * i + 1]);
+    return int(s.gauss_cdf.size());
+}
+
 void or_probe_sobol(const void *tables, const uint32_t *q, uint32_t count, uint32_t *r) {
     const auto &t = *static_cast<const SobolTables *>(tables);
     for (u32 i = 0; i < count; ++i) {
@@ -774,7 +794,8 @@ int or_probe_raygen(const or_scene *scene, const rp_request *request, uint32_t *
         w[4] = u32(index >> 32);
         for (int k = 0; k < 4; ++k)
             w[5 + k] = smp.words[k];
-        w[9] = w[10] = 0;
+        w[9] = smp.lens_words[0];
+        w[10] = smp.lens_words[1];
         F3 o, d;
         primary_ray(scene->scene, p, smp, o, d);
         float *r = rays + 6 * i;
@@ -958,8 +979,9 @@ int or_film_add(const rp_packet_result *results, size_t count, const double *cie
         }
         auto &px = film[s.pixel];
         for (int c = 0; c < 3; ++c) {
-            add_compensated(xyz[c] * s.filter_weight, px.sum[c], px.correction[c]);
-            px.square[c] += xyz[c] * xyz[c];
+            const double v = xyz[c] * s.filter_weight;
+            add_compensated(v, px.sum[c], px.correction[c]);
+            px.square[c] += v * v;
         }
         add_compensated(s.filter_weight, px.weight_sum, px.weight_correction);
         ++px.count;

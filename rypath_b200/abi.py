@@ -19,7 +19,7 @@ SAMPLE_SUCCESS, EMERGENCY_DEPTH, INVALID_ARITHMETIC, INVALID_HIT, BOUNDARY_EXHAU
 
 SAMPLER_INDEPENDENT, SAMPLER_SOBOL = 0, 1
 RANDOMIZE_NONE, RANDOMIZE_PERMUTEDIGITS, RANDOMIZE_FASTOWEN, RANDOMIZE_OWEN = range(4)
-FILTER_BOX, FILTER_TRIANGLE = 0, 1
+FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = 0, 1, 2
 DIFFUSE, CONDUCTOR, DIELECTRIC = 0, 1, 2
 INTERFACE = 10  # null medium interface (scalar transport)
 REFLECTANCE_KNOTS, REFLECTANCE_CONSTANT, REFLECTANCE_BLACKBODY = 0, 1, 4
@@ -90,6 +90,8 @@ class SceneDesc(C.Structure):
         ("transport", u32),
         ("hero_wavelengths", u32),
         ("sobol_tables", C.c_void_p),
+        ("lens_radius", f32), ("focal_distance", f32), ("lens_x", f32 * 3), ("lens_y", f32 * 3),
+        ("filter_sigma", f32),
     ]
 
 

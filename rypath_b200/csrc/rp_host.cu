@@ -298,6 +298,99 @@ double light_spectrum_power(const float *spectrum) {
     return value;
 }
 
+// ---------------------------------------------------------------- Gaussian pixel filter
+// compile_gaussian_filter (src/gaussian_filter.cpp:84-137): PBRT's Gaussian filter minus its
+// value at the radius, tabulated at 32 cells per unit radius at cell midpoints, with PBRT's
+// FastExp, normalised as a 2-D piecewise-constant distribution (conditional rows of width + 1
+// entries, then the marginal of height + 1).
+struct GaussianTable {
+    u32 width = 0, height = 0;
+    std::vector<float> conditional, marginal;
+    float integral = 0;
+};
+float pbrt_fast_exp(float x) {
+    if (x < -100.f)
+        return 0;
+    const float xp = x * 1.442695041f;
+    const float fxp = std::floor(xp);
+    const float f = xp - fxp;
+    const int i = int(fxp);
+    const float poly = std::fma(f, std::fma(f, std::fma(f, 0.0781455737f, 0.226173572f), 0.695556856f), 1.f);
+    uint32_t bits;
+    memcpy(&bits, &poly, 4);
+    const int exponent = int((bits >> 23) & 255) - 127 + i;
+    if (exponent < -126)
+        return 0;
+    bits = (bits & 0x807fffffu) | (uint32_t(exponent + 127) << 23);
+    float out;
+    memcpy(&out, &bits, 4);
+    return out;
+}
+float lerp_pbrt(float t, float a, float b) { return (1 - t) * a + t * b; }
+bool cdf_of(const float *values, size_t n, float radius, float *cdf, float &integral) {
+    cdf[0] = 0;
+    for (size_t i = 0; i < n; ++i) {
+        cdf[i + 1] = cdf[i] + values[i] * (2 * radius) / float(n);
+        if (!std::isfinite(cdf[i + 1]))
+            return false;
+    }
+    integral = cdf[n];
+    if (integral > 0 && !std::isnormal(integral))
+        return false;
+    if (integral == 0) {
+        for (size_t i = 1; i <= n; ++i)
+            cdf[i] = float(i) / float(n);
+    } else {
+        for (size_t i = 1; i <= n; ++i)
+            cdf[i] /= integral;
+    }
+    for (size_t i = 1; i <= n; ++i) {
+        const float gap = cdf[i] - cdf[i - 1];
+        if (!std::isfinite(cdf[i]) || (cdf[i] > 0 && !std::isnormal(cdf[i])) || (gap > 0 && !std::isnormal(gap)))
+            return false;
+    }
+    return true;
+}
+std::string gaussian_table(float xr, float yr, float sigma, GaussianTable &g) {
+    if (!std::isnormal(xr) || xr <= 0 || !std::isnormal(yr) || yr <= 0 || !std::isnormal(sigma) || sigma <= 0)
+        return "Gaussian radii and sigma must be positive normal binary32 values";
+    const float nx = 32 * xr, ny = 32 * yr;
+    if (!(nx >= 1 && nx < 4096 + 1.f && ny >= 1 && ny < 4096 + 1.f))
+        return "Gaussian table axis must contain 1 to 4096 cells";
+    g.width = u32(nx);
+    g.height = u32(ny);
+    if (uint64_t(g.width) * g.height > 1048576)
+        return "Gaussian table exceeds the 1048576-cell limit";
+    const float denominator = 2 * std::numbers::pi_v<float> * sigma * sigma;
+    const float two_sigma_squared = 2 * sigma * sigma;
+    const float scale = 1 / std::sqrt(denominator);
+    if (!(denominator > 0 && std::isfinite(denominator) && two_sigma_squared > 0 && std::isfinite(two_sigma_squared) &&
+          std::isfinite(scale)))
+        return "Gaussian sigma arithmetic overflows or collapses in binary32";
+    auto gaussian = [&](float x) { return scale * pbrt_fast_exp(-(x * x) / two_sigma_squared); };
+    const float exp_x = gaussian(xr), exp_y = gaussian(yr);
+    g.conditional.assign(size_t(g.height) * (g.width + 1), 0.f);
+    g.marginal.assign(g.height + 1, 0.f);
+    std::vector<float> values(g.width), rows(g.height);
+    for (u32 y = 0; y < g.height; ++y) {
+        const float py = lerp_pbrt((float(y) + 0.5f) / float(g.height), -yr, yr);
+        const float fy = std::max(0.f, gaussian(py) - exp_y);
+        for (u32 x = 0; x < g.width; ++x) {
+            const float px = lerp_pbrt((float(x) + 0.5f) / float(g.width), -xr, xr);
+            values[x] = std::max(0.f, gaussian(px) - exp_x) * fy;
+            if (!std::isfinite(values[x]))
+                return "Gaussian table contains nonfinite binary32 values";
+        }
+        if (!cdf_of(values.data(), g.width, xr, g.conditional.data() + size_t(y) * (g.width + 1), rows[y]))
+            return "Gaussian conditional distribution overflows or collapses in binary32";
+    }
+    float integral = 0;
+    if (!cdf_of(rows.data(), g.height, yr, g.marginal.data(), integral) || !(integral > 0))
+        return "Gaussian table has a zero or nonfinite binary32 integral";
+    g.integral = integral;
+    return {};
+}
+
 // ---------------------------------------------------------------- device buffers
 // Device memory comes from the device's stream-ordered pool, configured to keep freed memory
 // for reuse by the next scene or pool in this process (no trip to the driver per render job).
@@ -825,8 +918,11 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
         }
         if (d->camera_medium != RP_NONE && d->camera_medium >= d->medium_count)
             throw Invalid{"camera medium out of range"};
-        if (d->filter_kind > RP_FILTER_TRIANGLE)
+        if (d->filter_kind > RP_FILTER_GAUSSIAN)
             throw Invalid{"unsupported pixel filter"};
+        if (!(d->lens_radius >= 0) || !std::isfinite(d->lens_radius) ||
+            (d->lens_radius > 0 && (!(d->focal_distance > 0) || !std::isfinite(d->focal_distance))))
+            throw Invalid{"lens radius must be finite and nonnegative, with a positive finite focal distance"};
         if (d->light_sampler > RP_LIGHTS_UNIFORM)
             throw Invalid{"invalid light sampler"};
         if (d->positional_count > RP_MAX_POSITIONAL)
@@ -1126,6 +1222,26 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
         ds.filter_kind = d->filter_kind;
         ds.filter_x = d->filter_x_radius;
         ds.filter_y = d->filter_y_radius;
+        ds.filter_weight = 1;
+        ds.gauss_cdf = nullptr;
+        ds.gauss_w = ds.gauss_h = 0;
+        if (d->filter_kind == RP_FILTER_GAUSSIAN) {
+            GaussianTable g;
+            const std::string err = gaussian_table(d->filter_x_radius, d->filter_y_radius, d->filter_sigma, g);
+            if (!err.empty())
+                throw Invalid{err};
+            std::vector<float> cdf(g.conditional);
+            cdf.insert(cdf.end(), g.marginal.begin(), g.marginal.end());
+            ds.gauss_cdf = dupload(own, cdf.data(), cdf.size(), stm);
+            ds.gauss_w = g.width;
+            ds.gauss_h = g.height;
+            // the packet film weight of the hero transport (src/metal_render.mm:4851-4861)
+            ds.filter_weight = d->transport == RP_TRANSPORT_HERO ? g.integral : 1.0f;
+        }
+        ds.lens_radius = d->lens_radius;
+        ds.focal_distance = d->lens_radius > 0 ? d->focal_distance : 1e6f;
+        ds.lens_x = v3(d->lens_x[0], d->lens_x[1], d->lens_x[2]);
+        ds.lens_y = v3(d->lens_y[0], d->lens_y[1], d->lens_y[2]);
         ds.max_depth = d->max_depth;
         ds.hero_mode = d->hero_wavelengths;
         s->transport = d->transport;
@@ -1214,7 +1330,7 @@ static rp_status sample_impl(rp_scene *s, const rp_request *request, rp_packet_r
             dst = staging;
         }
         s->mark(3);
-        k_results<<<grid_for(s->sm_count, p.lanes, 256, 16), 256, 0, s->stream>>>(s->pool, p.lanes, dst);
+        k_results<<<grid_for(s->sm_count, p.lanes, 256, 16), 256, 0, s->stream>>>(s->pool, p.lanes, s->ds.filter_weight, dst);
         s->done();
         u32 failures = 0;
         if (host) {
@@ -1404,7 +1520,7 @@ static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel 
                     run_wave(s, p);
                     s->mark(3);
                     k_film<<<grid_for(s->sm_count, pixels, 128, 16), 128, 0, s->stream>>>(
-                        s->pool, pixels, u32(spw), s->cie, reinterpret_cast<FilmPixel *>(staged));
+                        s->pool, pixels, u32(spw), s->cie, double(s->ds.filter_weight), reinterpret_cast<FilmPixel *>(staged));
                     s->done();
                     RP_CHECK(cudaMemcpyAsync(&f, s->pool.counters + 3, 4, cudaMemcpyDeviceToHost, s->stream));
                 }
@@ -1712,7 +1828,7 @@ void batch_wave_kernels(rp_scene *s, const WaveParams &p, const Batch &b, u32 wa
         k_shadow<false, TB><<<trace_grid, TB, 0, st>>>(s->ds, pool);
         in ^= 1;
     }
-    k_film_views<<<grid_for(sms, wave_lanes, 128, 16), 128, 0, st>>>(pool, b, s->cie, film);
+    k_film_views<<<grid_for(sms, wave_lanes, 128, 16), 128, 0, st>>>(pool, b, s->cie, double(s->ds.filter_weight), film);
     k_next_wave<<<1, 32, 0, st>>>(b);
     RP_CHECK(cudaGetLastError());
 }
@@ -1890,6 +2006,8 @@ rp_status rp_cuda_tune_views(rp_scene *s, const rp_view *views, uint32_t count, 
             throw Invalid{"null argument"};
         if (s->transport != RP_TRANSPORT_HERO)
             throw Invalid{"batched views render hero-transport scenes"};
+        if (s->ds.lens_radius > 0)
+            throw Invalid{"batched views render pinhole cameras"};
         RP_CHECK(cudaSetDevice(s->device));
         if (!s->cie)
             throw Invalid{"CIE table not set (rp_cuda_set_cie)"};
@@ -1905,6 +2023,8 @@ rp_status rp_cuda_render_views_device(rp_scene *s, const rp_view *views, uint32_
             throw Invalid{"null argument"};
         if (s->transport != RP_TRANSPORT_HERO)
             throw Invalid{"batched views render hero-transport scenes"};
+        if (s->ds.lens_radius > 0)
+            throw Invalid{"batched views render pinhole cameras"};
         RP_CHECK(cudaSetDevice(s->device));
         if (!s->cie)
             throw Invalid{"CIE table not set (rp_cuda_set_cie)"};
@@ -2238,7 +2358,7 @@ rp_status rp_cuda_sample_device_static(rp_scene *s, const rp_request *request, r
             k_shadow<false><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, 0, st>>>(s->ds, pool);
             in ^= 1;
         }
-        k_results<<<grid_for(sms, p.lanes, 256, 16), 256, 0, st>>>(pool, p.lanes,
+        k_results<<<grid_for(sms, p.lanes, 256, 16), 256, 0, st>>>(pool, p.lanes, s->ds.filter_weight,
                                                                    reinterpret_cast<PacketResult *>(device_results));
         RP_CHECK(cudaGetLastError());
         return RP_SUCCESS;

@@ -586,7 +586,7 @@ struct PacketResult {
     float filter_weight;
     u32 reserved[2];
 };
-__global__ void k_results(PathPool pool, u32 lanes, PacketResult *out) {
+__global__ void k_results(PathPool pool, u32 lanes, float filter_weight, PacketResult *out) {
     for (u32 lane = blockIdx.x * blockDim.x + threadIdx.x; lane < lanes; lane += gridDim.x * blockDim.x) {
         const uint4 id = pool.ident[lane];
         const float4 l = pool.lambda[lane], pdf = pool.lambda_pdf[lane], r = pool.radiance[lane];
@@ -608,7 +608,7 @@ __global__ void k_results(PathPool pool, u32 lanes, PacketResult *out) {
         res.radiance[1] = r.y;
         res.radiance[2] = r.z;
         res.radiance[3] = r.w;
-        res.filter_weight = 1;
+        res.filter_weight = filter_weight;
         res.reserved[0] = res.reserved[1] = 0;
         out[lane] = res;
     }
@@ -629,7 +629,7 @@ RP_DEV void add_compensated(double value, double &sum, double &correction) {
 }
 // packet_sensor_xyz (src/packet_film.cpp:102-114) of one lane added to its pixel; false when
 // the lane failed (a failed lane fails its batch).
-RP_DEV bool film_add_lane(const PathPool &pool, u32 lane, const double *cie, FilmPixel &f) {
+RP_DEV bool film_add_lane(const PathPool &pool, u32 lane, const double *cie, double weight, FilmPixel &f) {
     const uint4 id = pool.ident[lane];
     const u32 status = (id.w & F_COMPLETE) ? get_status(id.w) : 2u;
     if (status != 0)
@@ -652,10 +652,11 @@ RP_DEV bool film_add_lane(const PathPool &pool, u32 lane, const double *cie, Fil
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        add_compensated(xyz[c], f.sum[c], f.correction[c]);
-        f.square[c] = __dadd_rn(f.square[c], __dmul_rn(xyz[c], xyz[c]));
+        const double v = __dmul_rn(xyz[c], weight); // add_xyz (src/packet_film.cpp:46-56)
+        add_compensated(v, f.sum[c], f.correction[c]);
+        f.square[c] = __dadd_rn(f.square[c], __dmul_rn(v, v));
     }
-    add_compensated(1.0, f.weight_sum, f.weight_correction);
+    add_compensated(weight, f.weight_sum, f.weight_correction);
     ++f.count;
     return true;
 }
@@ -669,11 +670,11 @@ __global__ void k_count_failures(PathPool pool, u32 lanes) {
     }
 }
 // Every sample of a wave reduced per pixel in canonical (absolute sample, pixel) order.
-__global__ void k_film(PathPool pool, u32 pixel_count, u32 samples, const double *cie, FilmPixel *film) {
+__global__ void k_film(PathPool pool, u32 pixel_count, u32 samples, const double *cie, double weight, FilmPixel *film) {
     for (u32 px = blockIdx.x * blockDim.x + threadIdx.x; px < pixel_count; px += gridDim.x * blockDim.x) {
         FilmPixel f = film[px];
         for (u32 si = 0; si < samples; ++si)
-            if (!film_add_lane(pool, si * pixel_count + px, cie, f))
+            if (!film_add_lane(pool, si * pixel_count + px, cie, weight, f))
                 atomicAdd(pool.counters + 3, 1u);
         film[px] = f;
     }

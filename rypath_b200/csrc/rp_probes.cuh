@@ -112,7 +112,8 @@ __global__ void k_probe_raygen(const __grid_constant__ DeviceScene s, const __gr
     w[6] = b.words.y;
     w[7] = b.words.z;
     w[8] = b.words.w;
-    w[9] = w[10] = 0;
+    w[9] = b.lens_words.x;
+    w[10] = b.lens_words.y;
     V3 o, d;
     primary_ray(s, p, b, o, d);
     float *r = rays + 6 * lane;

@@ -94,6 +94,14 @@ struct DeviceScene {
     const float *media;
     u32 medium_count, camera_medium;
     u32 media_enabled; // any medium or null interface: shadow connections track media
+    // thin lens (lens_radius 0: pinhole)
+    float lens_radius, focal_distance;
+    V3 lens_x, lens_y;
+    // Gaussian filter: tabulated CDFs (gauss_h rows of gauss_w + 1, then the marginal of
+    // gauss_h + 1) and the packet film weight (the table's integral; 1 for other filters)
+    const float *gauss_cdf;
+    u32 gauss_w, gauss_h;
+    float filter_weight;
 };
 
 RP_DEV V3 load3(const float *p) { return v3(__ldg(p), __ldg(p + 1), __ldg(p + 2)); }

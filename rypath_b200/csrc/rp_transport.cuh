@@ -86,7 +86,42 @@ struct BeginSample {
     u32 pixel, sample_low, sample_high;
     u64 index;
     uint4 words;
+    uint2 lens_words;
+    float filter_x, filter_y; // Gaussian filter offsets
 };
+constexpr u32 kLensBlock = 0xc0000000u;   // src/sampling_contract.h:24
+constexpr u32 kLensDimensionX = 1022u;
+// shaders/render.metal:200-236 (gaussian_filter_offsets): inverse of the tabulated marginal,
+// then of the selected row's conditional
+RP_DEV void gaussian_filter_offsets(const DeviceScene &s, float ux, float uy, float &x, float &y) {
+    const float *cdf = s.gauss_cdf;
+    const float *marginal = cdf + size_t(s.gauss_h) * (s.gauss_w + 1);
+    u32 low = 0, high = s.gauss_h;
+    while (low + 1 < high) {
+        const u32 mid = (low + high) / 2;
+        if (__ldg(marginal + mid) <= uy)
+            low = mid;
+        else
+            high = mid;
+    }
+    const u32 row = low;
+    const float m0 = __ldg(marginal + row), m1 = __ldg(marginal + row + 1);
+    const float ty = (float(row) + (uy - m0) / (m1 - m0)) / float(s.gauss_h);
+    const float *conditional = cdf + size_t(row) * (s.gauss_w + 1);
+    low = 0;
+    high = s.gauss_w;
+    while (low + 1 < high) {
+        const u32 mid = (low + high) / 2;
+        if (__ldg(conditional + mid) <= ux)
+            low = mid;
+        else
+            high = mid;
+    }
+    const float c0 = __ldg(conditional + low), c1 = __ldg(conditional + low + 1);
+    const float tx = (float(low) + (ux - c0) / (c1 - c0)) / float(s.gauss_w);
+    x = (1 - tx) * (-s.filter_x) + tx * s.filter_x;
+    y = (1 - ty) * (-s.filter_y) + ty * s.filter_y;
+}
 // shaders/render.metal:238-311 (begin_sample)
 RP_DEV BeginSample begin_sample(const DeviceScene &s, const WaveParams &p, u32 lane) {
     BeginSample r;
@@ -102,6 +137,22 @@ RP_DEV BeginSample begin_sample(const DeviceScene &s, const WaveParams &p, u32 l
     } else {
         r.index = 0;
         r.words = philox(make_uint4(r.pixel, r.sample_low, r.sample_high, 0), p.seed_low, p.seed_high);
+    }
+    r.lens_words = make_uint2(0, 0);
+    if (s.lens_radius > 0) {
+        if (p.sampler == 1) {
+            r.lens_words = make_uint2(sobol_word(s.sobol, r.index, kLensDimensionX, p.randomization, p.seed_low),
+                                      sobol_word(s.sobol, r.index, kLensDimensionX + 1, p.randomization, p.seed_low));
+        } else {
+            const uint4 w = philox(make_uint4(r.pixel, r.sample_low, r.sample_high, kLensBlock), p.seed_low, p.seed_high);
+            r.lens_words = make_uint2(w.x, w.y);
+        }
+    }
+    r.filter_x = r.filter_y = 0;
+    if (s.filter_kind == 2) {
+        const float ux = p.sampler == 1 ? sobol_camera_uniform(r.words.x, p.m, r.pixel % p.width) : u01(r.words.x);
+        const float uy = p.sampler == 1 ? sobol_camera_uniform(r.words.y, p.m, r.pixel / p.width) : u01(r.words.y);
+        gaussian_filter_offsets(s, ux, uy, r.filter_x, r.filter_y);
     }
     return r;
 }
@@ -126,15 +177,54 @@ RP_DEV void primary_ray_from(const DeviceScene &s, const RasterCam &cam, const W
         uy = u01(b.words.y);
     }
     o = cam.origin;
+    const float nan = __int_as_float(0x7fffffff);
+    // centered_filter / filter_offset (shaders/render.metal:395-411)
     const bool centered = s.filter_kind != 0 || s.filter_x != 0.5f || s.filter_y != 0.5f;
+    V3 dd;
     if (centered) {
-        const float ox = s.filter_kind == 1 ? triangle_offset(ux, s.filter_x) : (2.0f * ux - 1.0f) * s.filter_x;
-        const float oy = s.filter_kind == 1 ? triangle_offset(uy, s.filter_y) : (2.0f * uy - 1.0f) * s.filter_y;
+        const float ox = s.filter_kind == 2   ? b.filter_x
+                         : s.filter_kind == 1 ? triangle_offset(ux, s.filter_x)
+                                              : (2.0f * ux - 1.0f) * s.filter_x;
+        const float oy = s.filter_kind == 2   ? b.filter_y
+                         : s.filter_kind == 1 ? triangle_offset(uy, s.filter_y)
+                                              : (2.0f * uy - 1.0f) * s.filter_y;
         const float x = ((float(b.pixel % p.width) + 0.5f) + ox) / float(p.width);
         const float y = ((float(b.pixel / p.width) + 0.5f) + oy) / float(p.height);
-        const V3 dd = fma3(v3(y, y, y), cam.up, fma3(v3(x, x, x), cam.right, cam.forward));
+        dd = fma3(v3(y, y, y), cam.up, fma3(v3(x, x, x), cam.right, cam.forward));
+    } else {
+        const float x = (float(b.pixel % p.width) + ux) / float(p.width);
+        const float y = (float(b.pixel / p.width) + uy) / float(p.height);
+        dd = cam.forward + x * cam.right + y * cam.up;
+    }
+    if (s.lens_radius > 0) {
+        // lens_primary_ray / lens_point (shaders/render.metal:366-432): concentric disk sample
+        // on the aperture, direction through the focus plane
+        const float lx = 2.0f * sample_uniform(p, b.lens_words.x) - 1.0f;
+        const float ly = 2.0f * sample_uniform(p, b.lens_words.y) - 1.0f;
+        V3 offset = v3(0, 0, 0);
+        if (!(lx == 0 && ly == 0)) {
+            float radius, theta;
+            if (fabsf(lx) > fabsf(ly)) {
+                radius = lx;
+                theta = (kPi / 4.0f) * (ly / lx);
+            } else {
+                radius = ly;
+                theta = kPi / 2.0f - (kPi / 4.0f) * (lx / ly);
+            }
+            const float r = s.lens_radius * radius;
+            const float disk_x = r * cosf(theta), disk_y = r * sinf(theta);
+            const V3 ideal = disk_x * s.lens_x + disk_y * s.lens_y;
+            o = cam.origin + ideal;
+            offset = o - cam.origin;
+        }
+        dd = dd - offset / s.focal_distance;
+        // rypath_texture_direction (shaders/texture_footprint.h:14-20)
         const float scale = fmaxf(fabsf(dd.x), fmaxf(fabsf(dd.y), fabsf(dd.z)));
-        const float nan = __int_as_float(0x7fffffff);
+        d = (!(scale > 0.0f) || !finite3(dd)) ? v3(nan, nan, nan) : normalize3(dd / scale);
+        return;
+    }
+    if (centered) {
+        const float scale = fmaxf(fabsf(dd.x), fmaxf(fabsf(dd.y), fabsf(dd.z)));
         if (!finite3(dd) || !(scale > 0.0f)) {
             d = v3(nan, nan, nan);
             return;
@@ -147,13 +237,9 @@ RP_DEV void primary_ray_from(const DeviceScene &s, const RasterCam &cam, const W
         d = normalize3(scaled);
         return;
     }
-    const float x = (float(b.pixel % p.width) + ux) / float(p.width);
-    const float y = (float(b.pixel / p.width) + uy) / float(p.height);
-    const V3 dd = cam.forward + x * cam.right + y * cam.up;
     const float scale = fmaxf(fabsf(dd.x), fmaxf(fabsf(dd.y), fabsf(dd.z)));
     d = normalize3(dd / scale);
 }
-
 RP_DEV void primary_ray(const DeviceScene &s, const WaveParams &p, const BeginSample &b, V3 &o, V3 &d) {
     primary_ray_from(s, RasterCam{s.origin, s.forward, s.right, s.up}, p, b, o, d);
 }

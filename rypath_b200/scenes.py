@@ -87,6 +87,9 @@ class Scene:
     media: list = field(default_factory=list)
     camera_medium: int = abi.RP_NONE
     transport: int = abi.TRANSPORT_HERO
+    # thin lens (radius 0: pinhole): radius, focal distance, camera x / y axes
+    lens: tuple = (0.0, 1e6, (1.0, 0.0, 0.0), (0.0, 1.0, 0.0))
+    filter_sigma: float = 0.5
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -159,6 +162,10 @@ class Scene:
         d.camera.dy[:] = list(dy)
         d.filter_kind = self.filter_kind
         d.filter_x_radius, d.filter_y_radius = self.filter_radius
+        d.filter_sigma = self.filter_sigma
+        d.lens_radius, d.focal_distance = self.lens[0], self.lens[1]
+        d.lens_x[:] = list(self.lens[2])
+        d.lens_y[:] = list(self.lens[3])
         d.max_depth = self.max_depth
         d.light_sampler = self.light_sampler
         d.transport = self.transport
@@ -186,6 +193,19 @@ def diffuse_material(knot_begin, knot_count=32):
     m.scattering, m.kind, m.knot_begin, m.knot_count = abi.DIFFUSE, abi.REFLECTANCE_KNOTS, knot_begin, knot_count
     m.remap_roughness = 1
     return m
+
+
+def thin_lens(origin, target, up, radius, focal_distance=None):
+    """PerspectiveLens (src/render.hpp:159-164) of a pinhole_camera pose: aperture radius, focal
+    distance (default: the distance to target) and the camera's x / y axes in world space."""
+    o = np.asarray(origin, np.float64)
+    f = np.asarray(target, np.float64) - o
+    dist = float(np.linalg.norm(f))
+    f /= dist
+    r = np.cross(f, np.asarray(up, np.float64))
+    r /= np.linalg.norm(r)
+    u = np.cross(r, f)
+    return (float(radius), float(focal_distance or dist), tuple(r.astype(np.float32)), tuple(u.astype(np.float32)))
 
 
 def pinhole_camera(origin, target, up, vfov_degrees, width, height):

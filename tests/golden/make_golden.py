@@ -6,6 +6,9 @@ Reads the reference's test sources as text (nothing is executed):
   dimension hash, words for the four randomisations, binary32 pixel remap), generated by
   the reference from PBRT v4 b0bdf461.
 * ``tests/replay_tests.cpp`` -- Random123 v1.14.0 Philox4x32-10 known-answer vectors.
+* ``tests/gaussian_filter_tests.cpp`` -- FNV-1a digests of the Gaussian filter tables (every
+  CDF entry) and of 33x33 filter samples for three (x radius, y radius, sigma)
+  configurations, obtained by the reference from PBRT v4 b0bdf461.
 
 Usage: ``python tests/golden/make_golden.py /path/to/rypath`` (writes next to this file).
 """
@@ -67,15 +70,27 @@ def philox_answers(text: str):
     return out
 
 
+def gaussian_answers(text: str):
+    configs = re.findall(r"Configuration\{([^}]*)\}", text)
+    configs = [[_float(t) for t in c.split(",")] for c in configs]
+    block = re.search(r"expected\{(.*?)\};", text, flags=re.S).group(1)
+    pairs = re.findall(r"\{(0x[0-9a-fA-F]+ULL),\s*(0x[0-9a-fA-F]+ULL)\}", block)
+    return [{"x_radius": c[0], "y_radius": c[1], "sigma": c[2], "cdf_hash": _int(a), "sample_hash": _int(b)}
+            for c, (a, b) in zip(configs, pairs)]
+
+
 def main() -> None:
     reference = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
     here = Path(__file__).resolve().parent
     sobol = sobol_answers((reference / "tests/sampling_tests.cpp").read_text())
     philox = philox_answers((reference / "tests/replay_tests.cpp").read_text())
-    if len(sobol) != 8 or len(philox) != 3:
-        raise SystemExit(f"unexpected vector counts: sobol {len(sobol)}, philox {len(philox)}")
+    gaussian = gaussian_answers((reference / "tests/gaussian_filter_tests.cpp").read_text())
+    if len(sobol) != 8 or len(philox) != 3 or len(gaussian) != 3:
+        raise SystemExit(f"unexpected vector counts: sobol {len(sobol)}, philox {len(philox)}, "
+                         f"gaussian {len(gaussian)}")
     (here / "sobol_known_answers.json").write_text(json.dumps(sobol, indent=1) + "\n")
     (here / "philox_known_answers.json").write_text(json.dumps(philox, indent=1) + "\n")
+    (here / "gaussian_filter_known_answers.json").write_text(json.dumps(gaussian, indent=1) + "\n")
 
 
 if __name__ == "__main__":

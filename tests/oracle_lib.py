@@ -45,6 +45,7 @@ def oracle():
         lib.or_probe_medium.argtypes = [vp, u32, vp]
         lib.or_scalar_film_add.argtypes = [vp, sz, vp, u32, vp]
         lib.or_adjoint.argtypes = [vp, C.POINTER(abi.FilmRequest), vp, u32, vp, vp, vp, C.c_int]
+        lib.or_gaussian_filter.argtypes = [C.c_float, C.c_float, C.c_float, vp, sz, vp, vp, vp, u32, vp]
         _oracle = lib
     return _oracle
 

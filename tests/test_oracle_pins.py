@@ -3,7 +3,8 @@ host-compilable sources compiled where they lie (oracle/_ref, built by oracle/re
 
 References: Sobol KATs tests/sampling_tests.cpp:26-142; Philox KATs tests/replay_tests.cpp:22-36;
 visible wavelength checks tests/packet_spectrum_tests.cpp:9-56; light tables
-src/light_sampling.cpp:384-572; packet film src/packet_film.cpp:198-265.
+src/light_sampling.cpp:384-572; packet film src/packet_film.cpp:198-265; Gaussian filter
+digests tests/gaussian_filter_tests.cpp:89-127.
 """
 
 import ctypes as C
@@ -264,3 +265,33 @@ def test_film_reduction_matches_packet_film_batch():
     np.testing.assert_array_equal(film["correction"], ref_out[:, 3:6])
     np.testing.assert_array_equal(film["weight_sum"], ref_out[:, 6])
     np.testing.assert_array_equal(film["count"], ref_out[:, 8])
+
+
+def _fnv_floats(values, h=14695981039346656037):
+    for b in np.asarray(values, np.float32).tobytes():
+        h ^= b
+        h = (h * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+def test_gaussian_filter_table_and_samples_match_rypath_known_answers():
+    """tests/gaussian_filter_tests.cpp:89-127: FNV-1a digests of every CDF entry and of 33x33
+    samples (u, v = k / 32 clamped below 1) for three configurations, pinned by rypath against
+    PBRT v4 b0bdf461."""
+    import ctypes as C
+
+    known = json.load(open(os.path.join(GOLDEN, "gaussian_filter_known_answers.json")))
+    grid = np.array([[min(x / 32, float.fromhex("0x1.fffffep-1")), min(y / 32, float.fromhex("0x1.fffffep-1"))]
+                     for y in range(33) for x in range(33)], np.float32)
+    for k in known:
+        cdf = np.zeros(1 << 20, np.float32)
+        size = np.zeros(2, np.uint32)
+        integral = C.c_float()
+        out = np.zeros((grid.shape[0], 2), np.float32)
+        n = oracle().or_gaussian_filter(k["x_radius"], k["y_radius"], k["sigma"], cdf.ctypes.data, cdf.size,
+                                        size.ctypes.data, C.byref(integral), grid.ctypes.data, grid.shape[0],
+                                        out.ctypes.data)
+        assert n > 0
+        assert _fnv_floats(cdf[:n]) == k["cdf_hash"]
+        assert _fnv_floats(out.reshape(-1)) == k["sample_hash"]
+        assert integral.value > 0
