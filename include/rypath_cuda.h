@@ -53,7 +53,7 @@ enum {
 };
 
 /* Sampler kinds and Sobol randomisations (src/render_wire.h:40, src/sobol_shared.h:26-34). */
-enum { RP_SAMPLER_INDEPENDENT = 0, RP_SAMPLER_SOBOL = 1 };
+enum { RP_SAMPLER_INDEPENDENT = 0, RP_SAMPLER_SOBOL = 1, RP_SAMPLER_HALTON = 2, RP_SAMPLER_ZSOBOL = 3 };
 enum { RP_RANDOMIZE_NONE = 0, RP_RANDOMIZE_PERMUTEDIGITS = 1, RP_RANDOMIZE_FASTOWEN = 2,
        RP_RANDOMIZE_OWEN = 3 };
 /* Pixel filters (src/render_wire.h:29). */
@@ -170,6 +170,7 @@ typedef struct rp_request {
     uint32_t sampler_kind;     /* RP_SAMPLER_* */
     uint32_t randomization;    /* RP_RANDOMIZE_* */
     uint32_t boundary_limit;   /* medium_boundary_limit = 4096 */
+    uint64_t total_samples;    /* the render's sample budget (RenderRequest::total_samples); ZSobol needs it */
 } rp_request;
 
 /* packet_wire::Result, 80 bytes (src/packet_wire.h:13-18). */
@@ -213,6 +214,7 @@ typedef struct rp_film_request {
     uint64_t sample_begin, sample_count, batch_size;
     uint32_t sampler_kind, randomization;
     uint32_t emergency_limit;
+    uint64_t total_samples; /* the render's sample budget; 0 = sample_begin + sample_count */
 } rp_film_request;
 
 /* Kernel-level timing of the last call on a scene (CUDA events on the scene stream). */

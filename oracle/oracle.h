@@ -61,6 +61,9 @@ int or_film_add(const rp_packet_result *results, size_t count, const double *cie
 int or_gaussian_filter(float x_radius, float y_radius, float sigma, float *cdf, size_t capacity, uint32_t *size,
                        float *integral, const float *uv, uint32_t count, float *samples);
 
+/* Halton / ZSobol probe (rypath's QMC known-answer layout): 10 int64 per query -> 6 uint64. */
+void or_probe_qmc(const void *sobol_tables, const int64_t *queries, uint32_t count, uint64_t *results);
+
 /* FP64 path-replay adjoint of a film render (the rp_cuda_adjoint_device contract): gradient of
  * the loss with respect to the knot values of `materials`, given d loss / d film-mean XYZ per
  * pixel and the CIE table.  0, 1 when a lane failed, -1 on a bad material list. */

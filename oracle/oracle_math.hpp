@@ -11,6 +11,7 @@
 #include <bit>
 #include <cfloat>
 #include <cmath>
+#include <vector>
 #include <cstdint>
 #include <cstring>
 
@@ -130,14 +131,11 @@ inline u64 mix_bits(u64 v) {
     return v ^ (v >> 33);
 }
 // src/sobol_shared.h:108-141
-inline u32 sobol_word(const SobolTables &t, u64 index, u32 dimension, u32 mode, u32 seed) {
-    u32 value = 0;
-    for (u32 c = dimension * sobol_matrix; index != 0; ++c, index >>= 1)
-        if (index & 1)
-            value ^= t.directions[c];
+// the randomisations of a 32-bit word with a 32-bit hash (src/sobol_shared.h:115-141,
+// src/qmc_shared.h:190-212)
+inline u32 scramble_word(u32 value, u32 mode, u32 hash) {
     if (mode == 0)
         return value;
-    const u32 hash = sobol_dimension_hash(dimension, seed);
     if (mode == 1)
         return value ^ hash;
     if (mode == 2) {
@@ -156,6 +154,198 @@ inline u32 sobol_word(const SobolTables &t, u64 index, u32 dimension, u32 mode, 
             value ^= u32(1) << (31 - bit);
     }
     return value;
+}
+inline u32 sobol_raw(const SobolTables &t, u64 index, u32 dimension) {
+    u32 value = 0;
+    for (u32 c = dimension * sobol_matrix; index != 0; ++c, index >>= 1)
+        if (index & 1)
+            value ^= t.directions[c];
+    return value;
+}
+inline u32 sobol_word(const SobolTables &t, u64 index, u32 dimension, u32 mode, u32 seed) {
+    const u32 value = sobol_raw(t, index, dimension);
+    return mode == 0 ? value : scramble_word(value, mode, sobol_dimension_hash(dimension, seed));
+}
+
+// ---------------------------------------------------------------- Halton / ZSobol
+// src/qmc_shared.h (PBRT v4 HaltonSampler / ZSobolSampler arithmetic)
+// the first 1000 primes, the Halton bases (:14-18)
+inline const u32 *qmc_primes() {
+    static const std::vector<u32> primes = [] {
+        std::vector<u32> out;
+        for (u32 n = 2; out.size() < 1000; ++n) {
+            bool prime = true;
+            for (u32 q : out) {
+                if (q * q > n)
+                    break;
+                if (n % q == 0) {
+                    prime = false;
+                    break;
+                }
+            }
+            if (prime)
+                out.push_back(n);
+        }
+        return out;
+    }();
+    return primes.data();
+}
+// :20-40
+inline u64 qmc_hash2(u32 a, u32 b) {
+    const u64 m = 0xc6a4a7935bd1e995ull;
+    u64 k = ((u64(b) << 32) | a) * m;
+    k ^= k >> 47;
+    k *= m;
+    u64 h = (8 * m ^ k) * m;
+    h ^= h >> 47;
+    h *= m;
+    return h ^ (h >> 47);
+}
+inline u64 qmc_hash3(u32 a, u32 b, u32 c) {
+    const u64 m = 0xc6a4a7935bd1e995ull;
+    u64 k = ((u64(b) << 32) | a) * m;
+    k ^= k >> 47;
+    k *= m;
+    u64 h = (12 * m ^ k) * m;
+    h ^= c;
+    h *= m;
+    h ^= h >> 47;
+    h *= m;
+    return h ^ (h >> 47);
+}
+// :41-66 (Kensler's hashed permutation by cycle walking)
+inline u32 qmc_permutation(u32 i, u32 l, u32 p) {
+    u32 w = l - 1;
+    w |= w >> 1;
+    w |= w >> 2;
+    w |= w >> 4;
+    w |= w >> 8;
+    w |= w >> 16;
+    do {
+        i ^= p;
+        i *= 0xe170893du;
+        i ^= p >> 16;
+        i ^= (i & w) >> 4;
+        i ^= p >> 8;
+        i *= 0x0929eb3fu;
+        i ^= p >> 23;
+        i ^= (i & w) >> 1;
+        i *= 1 | p >> 27;
+        i *= 0x6935fa69u;
+        i ^= (i & w) >> 11;
+        i *= 0x74dcb303u;
+        i ^= (i & w) >> 2;
+        i *= 0x9e501cc3u;
+        i ^= (i & w) >> 2;
+        i *= 0xc860a3dfu;
+        i &= w;
+        i ^= i >> 5;
+    } while (i >= l);
+    return (i + p) % l;
+}
+// :84-106
+inline float qmc_radical(u32 dimension, u64 a, u32 mode = 0, u32 seed = 0) {
+    const u32 base = qmc_primes()[dimension];
+    const u64 limit = ~u64(0) / base - base;
+    const float inv = 1.f / float(base);
+    float inv_m = 1;
+    u64 reversed = 0;
+    u32 digit_index = 0;
+    const u32 owen_hash = u32(mix_bits(1 + (dimension << 4)));
+    while ((mode == 0 ? a != 0 : (mode == 1 ? 1.f - float(base - 1) * inv_m < 1.f : 1.f - inv_m < 1.f)) &&
+           reversed < limit) {
+        const u64 next = a / base;
+        u32 digit = u32(a - next * base);
+        if (mode == 1)
+            digit = qmc_permutation(digit, base, u32(qmc_hash3(base, digit_index, seed)));
+        else if (mode == 3)
+            digit = qmc_permutation(digit, base, u32(mix_bits(owen_hash ^ reversed)));
+        reversed = reversed * base + digit;
+        inv_m *= inv;
+        ++digit_index;
+        a = next;
+    }
+    const float value = float(reversed) * inv_m;
+    return value < 0x1.fffffep-1f ? value : 0x1.fffffep-1f;
+}
+// :107-148
+inline u32 qmc_base_scale(u32 resolution, u32 base) {
+    u32 scale = 1;
+    while (scale < std::min(resolution, 128u))
+        scale *= base;
+    return scale;
+}
+inline u64 halton_index(u32 width, u32 height, u32 x, u32 y, u64 sample) {
+    const u32 sx = qmc_base_scale(width, 2), sy = qmc_base_scale(height, 3), stride = sx * sy;
+    const auto exponent = [](u32 scale, u32 base) {
+        u32 e = 0;
+        for (; scale > 1; scale /= base)
+            ++e;
+        return e;
+    };
+    const auto inverse_radical = [](u32 a, u32 base, u32 count) {
+        u64 r = 0;
+        for (u32 i = 0; i < count; ++i, a /= base)
+            r = r * base + a % base;
+        return r;
+    };
+    const auto inverse_mod = [](u32 a, u32 modulus) -> u32 {
+        if (modulus == 1)
+            return 0;
+        for (u32 i = 1; i < modulus; ++i)
+            if ((a * i) % modulus == 1)
+                return i;
+        return 0;
+    };
+    u64 offset = 0;
+    if (stride > 1) {
+        offset = inverse_radical(x % 128, 2, exponent(sx, 2)) * sy * inverse_mod(sy, sx);
+        offset += inverse_radical(y % 128, 3, exponent(sy, 3)) * sx * inverse_mod(sx, sy);
+        offset %= stride;
+    }
+    return offset + sample * stride;
+}
+// :176-179
+inline float halton_camera(u32 axis, u32 resolution, u64 index) {
+    return qmc_radical(axis, index / qmc_base_scale(resolution, axis == 0 ? 2 : 3));
+}
+// :213-220
+inline u64 zsobol_morton(u32 x, u32 y, u32 log_spp, u64 sample) {
+    u64 result = 0;
+    for (u32 b = 0; b < 26; ++b) {
+        result |= u64((x >> b) & 1) << (2 * b);
+        result |= u64((y >> b) & 1) << (2 * b + 1);
+    }
+    return (result << log_spp) | sample;
+}
+// :221-238
+inline u64 zsobol_index(u64 morton, u32 dimension, u32 exponent, u32 log_spp) {
+    static const u32 permutations[24][4] = {
+        {0, 1, 2, 3}, {0, 1, 3, 2}, {0, 2, 1, 3}, {0, 2, 3, 1}, {0, 3, 2, 1}, {0, 3, 1, 2},
+        {1, 0, 2, 3}, {1, 0, 3, 2}, {1, 2, 0, 3}, {1, 2, 3, 0}, {1, 3, 2, 0}, {1, 3, 0, 2},
+        {2, 1, 0, 3}, {2, 1, 3, 0}, {2, 0, 1, 3}, {2, 0, 3, 1}, {2, 3, 0, 1}, {2, 3, 1, 0},
+        {3, 1, 2, 0}, {3, 1, 0, 2}, {3, 2, 1, 0}, {3, 2, 0, 1}, {3, 0, 2, 1}, {3, 0, 1, 2}};
+    const u32 odd = log_spp & 1;
+    const u32 digits = exponent + (log_spp + 1) / 2;
+    u64 result = 0;
+    for (int i = int(digits) - 1; i >= int(odd); --i) {
+        const u32 shift = 2 * u32(i) - odd;
+        const u32 digit = u32((morton >> shift) & 3);
+        const u64 higher = morton >> (shift + 2);
+        const u32 p = u32((mix_bits(higher ^ u32(0x55555555u * dimension)) >> 24) % 24);
+        result |= u64(permutations[p][digit]) << shift;
+    }
+    if (odd)
+        result |= (morton & 1) ^ (mix_bits((morton >> 1) ^ u32(0x55555555u * dimension)) & 1);
+    return result;
+}
+// :244-249
+inline u32 zsobol_word(const SobolTables &t, u64 morton, u32 dimension, u32 axis, bool pair, u32 exponent,
+                       u32 log_spp, u32 mode, u32 seed) {
+    const u64 index = zsobol_index(morton, dimension, exponent, log_spp);
+    const u64 hash = qmc_hash2(dimension + (pair ? 2 : 1), seed);
+    const u32 random = pair && axis == 1 ? u32(hash >> 32) : u32(hash);
+    return scramble_word(sobol_raw(t, index, axis), mode, random);
 }
 // src/sobol_shared.h:143-146
 inline float sobol_uniform(u32 v) {

@@ -11,6 +11,7 @@ namespace oracle {
 struct Params {
     u32 width, height, pixel_begin, pixel_count, sample_low, sample_high;
     u32 seed_low, seed_high, sampler, randomization, m, emergency_limit, max_depth;
+    u32 log_spp; // ZSobol: floor(log2(total samples))
 };
 
 struct Sample {
@@ -48,15 +49,34 @@ inline void gaussian_filter_offsets(const Scene &s, float ux, float uy, float &x
     y = (1 - ty) * (-s.filter_y) + ty * s.filter_y;
 }
 
-// shaders/render.metal:113-118 (sobol and independent samplers)
+// shaders/render.metal:113-122
 inline float sample_uniform(const Params &p, u32 w) {
+    if (p.sampler == RP_SAMPLER_HALTON)
+        return ffrom(w);
     return p.sampler == RP_SAMPLER_INDEPENDENT ? u01(w) : sobol_uniform(w);
+}
+inline u32 decision_word(const Params &p, u32 w) {
+    return p.sampler == RP_SAMPLER_HALTON ? u32(ffrom(w) * 0x1p32f) : w;
+}
+// shaders/render.metal:123-127
+inline u32 zdraw(const Scene &s, const Params &p, u64 index, u32 dimension, u32 axis = 0, bool pair = false) {
+    return zsobol_word(*s.sobol, index, dimension, axis, pair, p.m, p.log_spp, p.randomization, p.seed_low);
 }
 // shaders/render.metal:154-179 (draw_words)
 inline U4 draw_words(const Scene &s, const Params &p, const Sample &smp, u64 index, u32 block) {
     if (p.sampler == RP_SAMPLER_INDEPENDENT)
         return philox(U4{smp.pixel, smp.sample_low, smp.sample_high, block}, p.seed_low, p.seed_high);
     const u32 d = 4 * block;
+    if (p.sampler == RP_SAMPLER_HALTON)
+        return U4{fbits(qmc_radical(d, index, p.randomization, p.seed_low)),
+                  fbits(qmc_radical(d + 1, index, p.randomization, p.seed_low)),
+                  fbits(qmc_radical(d + 2, index, p.randomization, p.seed_low)),
+                  fbits(qmc_radical(d + 3, index, p.randomization, p.seed_low))};
+    if (p.sampler == RP_SAMPLER_ZSOBOL) {
+        const bool even = (block & 1) == 0;
+        return U4{zdraw(s, p, index, d, 0, true), zdraw(s, p, index, d, 1, true), zdraw(s, p, index, d + 2, 0, even),
+                  zdraw(s, p, index, even ? d + 2 : d + 3, even ? 1 : 0, even)};
+    }
     const SobolTables &t = *s.sobol;
     return U4{sobol_word(t, index, d, p.randomization, p.seed_low),
               sobol_word(t, index, d + 1, p.randomization, p.seed_low),
@@ -77,6 +97,18 @@ inline Sample begin_sample(const Scene &s, const Params &p, u32 lane, u64 &index
         r.words[1] = sobol_word(t, index, 1, 0, 0);
         r.words[2] = sobol_word(t, index, 2, p.randomization, p.seed_low);
         r.words[3] = sobol_word(t, index, 3, p.randomization, p.seed_low);
+    } else if (p.sampler == RP_SAMPLER_HALTON) {
+        index = halton_index(p.width, p.height, r.pixel % p.width, r.pixel / p.width, sample);
+        r.words[0] = fbits(halton_camera(0, p.width, index));
+        r.words[1] = fbits(halton_camera(1, p.height, index));
+        r.words[2] = fbits(qmc_radical(2, index, p.randomization, p.seed_low));
+        r.words[3] = fbits(qmc_radical(3, index, p.randomization, p.seed_low));
+    } else if (p.sampler == RP_SAMPLER_ZSOBOL) {
+        index = zsobol_morton(r.pixel % p.width, r.pixel / p.width, p.log_spp, sample);
+        r.words[0] = zdraw(s, p, index, 1, 0, true);
+        r.words[1] = zdraw(s, p, index, 1, 1, true);
+        r.words[2] = zdraw(s, p, index, 0);
+        r.words[3] = zdraw(s, p, index, 3);
     } else {
         index = 0;
         const U4 w = philox(U4{r.pixel, r.sample_low, r.sample_high, 0}, p.seed_low, p.seed_high);
@@ -90,6 +122,12 @@ inline Sample begin_sample(const Scene &s, const Params &p, u32 lane, u64 &index
             const SobolTables &t = *s.sobol;
             r.lens_words[0] = sobol_word(t, index, 1022, p.randomization, p.seed_low); // lens_x_dimension
             r.lens_words[1] = sobol_word(t, index, 1023, p.randomization, p.seed_low);
+        } else if (p.sampler == RP_SAMPLER_HALTON) {
+            r.lens_words[0] = fbits(qmc_radical(998, index, p.randomization, p.seed_low));
+            r.lens_words[1] = fbits(qmc_radical(999, index, p.randomization, p.seed_low));
+        } else if (p.sampler == RP_SAMPLER_ZSOBOL) {
+            r.lens_words[0] = zdraw(s, p, index, 1022, 0, true);
+            r.lens_words[1] = zdraw(s, p, index, 1022, 1, true);
         } else {
             const U4 w = philox(U4{r.pixel, r.sample_low, r.sample_high, 0xc0000000u}, p.seed_low, p.seed_high);
             r.lens_words[0] = w.x;
@@ -98,9 +136,9 @@ inline Sample begin_sample(const Scene &s, const Params &p, u32 lane, u64 &index
     }
     if (s.filter_kind == RP_FILTER_GAUSSIAN) {
         const float ux = p.sampler == RP_SAMPLER_SOBOL ? sobol_camera_uniform(r.words[0], p.m, r.pixel % p.width)
-                                                       : u01(r.words[0]);
+                                                       : sample_uniform(p, r.words[0]);
         const float uy = p.sampler == RP_SAMPLER_SOBOL ? sobol_camera_uniform(r.words[1], p.m, r.pixel / p.width)
-                                                       : u01(r.words[1]);
+                                                       : sample_uniform(p, r.words[1]);
         gaussian_filter_offsets(s, ux, uy, r.filter_offsets[0], r.filter_offsets[1]);
     }
     return r;
@@ -250,7 +288,10 @@ inline Params make_params(const Scene &s, const rp_request &r) {
     p.seed_high = u32(r.seed >> 32);
     p.sampler = r.sampler_kind;
     p.randomization = r.randomization;
-    p.m = r.sampler_kind == RP_SAMPLER_SOBOL ? sobol_scale_exponent(r.width, r.height) : 0;
+    p.m = r.sampler_kind == RP_SAMPLER_SOBOL || r.sampler_kind == RP_SAMPLER_ZSOBOL
+              ? sobol_scale_exponent(r.width, r.height)
+              : 0;
+    p.log_spp = r.sampler_kind == RP_SAMPLER_ZSOBOL && r.total_samples ? 63 - __builtin_clzll(r.total_samples) : 0;
     p.emergency_limit = r.emergency_limit ? r.emergency_limit : 1024;
     p.max_depth = s.max_depth;
     return p;

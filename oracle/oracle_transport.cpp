@@ -739,6 +739,39 @@ int or_gaussian_filter(float x_radius, float y_radius, float sigma, float *cdf, 
     return int(s.gauss_cdf.size());
 }
 
+// Halton / ZSobol probe in the layout of rypath's QMC known answers
+// (tests/qmc_sampling_tests.cpp:184-219): query (kind, width, height, x, y, sample, dimension,
+// mode, seed, spp) as 10 int64, result 6 uint64 (index, camera x/y and three draws, as float
+// bits except the ZSobol index).
+void or_probe_qmc(const void *sobol_tables, const int64_t *queries, uint32_t count, uint64_t *results) {
+    const SobolTables &t = *static_cast<const SobolTables *>(sobol_tables);
+    for (uint32_t i = 0; i < count; ++i) {
+        const int64_t *q = queries + 10 * i;
+        const u32 w = u32(q[1]), h = u32(q[2]), x = u32(q[3]), y = u32(q[4]), d = u32(q[6]), mode = u32(q[7]),
+                  seed = u32(q[8]), spp = u32(q[9]);
+        const u64 sample = u64(q[5]);
+        uint64_t *a = results + 6 * i;
+        if (q[0] == RP_SAMPLER_HALTON) {
+            const u64 index = halton_index(w, h, x, y, sample);
+            a[0] = 0;
+            a[1] = fbits(halton_camera(0, w, index));
+            a[2] = fbits(halton_camera(1, h, index));
+            a[3] = a[4] = fbits(qmc_radical(d, index, mode, seed));
+            a[5] = fbits(qmc_radical(d + 1, index, mode, seed));
+        } else {
+            const u32 m = sobol_scale_exponent(w, h);
+            const u32 log = 31 - __builtin_clz(spp);
+            const u64 morton = zsobol_morton(x, y, log, sample);
+            a[0] = zsobol_index(morton, d, m, log);
+            a[1] = fbits(sobol_uniform(zsobol_word(t, morton, 1, 0, true, m, log, mode, seed)));
+            a[2] = fbits(sobol_uniform(zsobol_word(t, morton, 1, 1, true, m, log, mode, seed)));
+            a[3] = fbits(sobol_uniform(zsobol_word(t, morton, d, 0, false, m, log, mode, seed)));
+            a[4] = fbits(sobol_uniform(zsobol_word(t, morton, d, 0, true, m, log, mode, seed)));
+            a[5] = fbits(sobol_uniform(zsobol_word(t, morton, d, 1, true, m, log, mode, seed)));
+        }
+    }
+}
+
 void or_probe_sobol(const void *tables, const uint32_t *q, uint32_t count, uint32_t *r) {
     const auto &t = *static_cast<const SobolTables *>(tables);
     for (u32 i = 0; i < count; ++i) {

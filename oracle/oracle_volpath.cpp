@@ -689,7 +689,7 @@ bool scalar_event(const Ctx &c, Lane &l) {
         return fail(RP_SAMPLE_INVALID_ARITHMETIC);
     ++l.scatterings;
     if (l.scatterings >= 3) {
-        if (bsdf_words.z >= 0xc0000000u)
+        if (decision_word(p, bsdf_words.z) >= 0xc0000000u)
             return true;
         l.throughput /= 0.75f;
         if (!std::isfinite(l.throughput))

@@ -2,6 +2,7 @@
 // where they lie (oracle/ref.mk), used to pin the oracle's restatement.  Nothing here is
 // shipped; the built library lives in oracle/_ref/.
 #include "sobol_shared.h"
+#include "qmc_shared.h"
 #include "hero_spectrum_shared.h"
 #include "packet_roulette_shared.h"
 #include "offset_rounding_shared.h"
@@ -200,6 +201,38 @@ void ref_probe_medium(const float *q, uint32_t count, float *r) {
         o[5] = w.x;
         o[6] = w.y;
         o[7] = w.z;
+    }
+}
+
+// src/qmc_shared.h in the or_probe_qmc layout
+void ref_probe_qmc(const int64_t *queries, uint32_t count, uint64_t *results) {
+    namespace q = rypath::qmc;
+    namespace s = rypath::sobol;
+    for (uint32_t i = 0; i < count; ++i) {
+        const int64_t *a = queries + 10 * i;
+        const unsigned w = unsigned(a[1]), h = unsigned(a[2]), x = unsigned(a[3]), y = unsigned(a[4]),
+                       d = unsigned(a[6]), mode = unsigned(a[7]), seed = unsigned(a[8]), spp = unsigned(a[9]);
+        const uint64_t sample = uint64_t(a[5]);
+        uint64_t *o = results + 6 * i;
+        if (a[0] == 2) {
+            const auto index = q::halton_index(w, h, x, y, sample);
+            o[0] = 0;
+            o[1] = q::float_bits(q::halton_camera(0, w, index));
+            o[2] = q::float_bits(q::halton_camera(1, h, index));
+            o[3] = o[4] = q::float_bits(q::radical(d, index, mode, seed));
+            o[5] = q::float_bits(q::radical(d + 1, index, mode, seed));
+        } else {
+            const unsigned v = std::max({w, h, 1u}) - 1;
+            const unsigned m = v == 0 ? 0 : 32 - __builtin_clz(v);
+            const unsigned log = 31 - __builtin_clz(spp);
+            const auto morton = q::morton(x, y, log, sample);
+            o[0] = q::zindex(morton, d, m, log);
+            o[1] = q::float_bits(s::uniform(q::zword(ref_tables, morton, 1, 0, true, m, log, mode, seed)));
+            o[2] = q::float_bits(s::uniform(q::zword(ref_tables, morton, 1, 1, true, m, log, mode, seed)));
+            o[3] = q::float_bits(s::uniform(q::zword(ref_tables, morton, d, 0, false, m, log, mode, seed)));
+            o[4] = q::float_bits(s::uniform(q::zword(ref_tables, morton, d, 0, true, m, log, mode, seed)));
+            o[5] = q::float_bits(s::uniform(q::zword(ref_tables, morton, d, 1, true, m, log, mode, seed)));
+        }
     }
 }
 

@@ -17,7 +17,7 @@ STATUS_NAMES = {0: "success", 1: "not_built", 2: "no_device", 3: "no_ray_tracing
 
 SAMPLE_SUCCESS, EMERGENCY_DEPTH, INVALID_ARITHMETIC, INVALID_HIT, BOUNDARY_EXHAUSTION = range(5)
 
-SAMPLER_INDEPENDENT, SAMPLER_SOBOL = 0, 1
+SAMPLER_INDEPENDENT, SAMPLER_SOBOL, SAMPLER_HALTON, SAMPLER_ZSOBOL = 0, 1, 2, 3
 RANDOMIZE_NONE, RANDOMIZE_PERMUTEDIGITS, RANDOMIZE_FASTOWEN, RANDOMIZE_OWEN = range(4)
 FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = 0, 1, 2
 DIFFUSE, CONDUCTOR, DIELECTRIC = 0, 1, 2
@@ -99,7 +99,7 @@ class Request(C.Structure):
     _fields_ = [("width", u32), ("height", u32), ("seed", u64), ("material_seed", i32),
                 ("pixel_begin", u32), ("pixel_count", u32), ("sample_begin", u64),
                 ("sample_count", u32), ("emergency_limit", u32), ("sampler_kind", u32),
-                ("randomization", u32), ("boundary_limit", u32)]
+                ("randomization", u32), ("boundary_limit", u32), ("total_samples", u64)]
 
 
 class PacketResult(C.Structure):
@@ -127,7 +127,7 @@ class FilmPixel(C.Structure):
 class FilmRequest(C.Structure):
     _fields_ = [("width", u32), ("height", u32), ("seed", u64), ("sample_begin", u64),
                 ("sample_count", u64), ("batch_size", u64), ("sampler_kind", u32),
-                ("randomization", u32), ("emergency_limit", u32)]
+                ("randomization", u32), ("emergency_limit", u32), ("total_samples", u64)]
 
 
 class View(C.Structure):
@@ -187,9 +187,9 @@ def film_dtype():
 EXPECTED_SIZES = {
     "rp_instance": (Instance, 84), "rp_material": (Material, 52), "rp_knot": (Knot, 8),
     "rp_area_emission": (AreaEmission, 1888), "rp_positional_light": (PositionalLight, 1948),
-    "rp_medium": (Medium, 5656), "rp_camera": (Camera, 48), "rp_request": (Request, 56),
+    "rp_medium": (Medium, 5656), "rp_camera": (Camera, 48), "rp_request": (Request, 64),
     "rp_packet_result": (PacketResult, 80), "rp_scalar_result": (ScalarResult, 44),
-    "rp_film_pixel": (FilmPixel, 96), "rp_film_request": (FilmRequest, 56),
+    "rp_film_pixel": (FilmPixel, 96), "rp_film_request": (FilmRequest, 64),
     "rp_view": (View, 80), "rp_batch_config": (BatchConfig, 24), "rp_batch_request": (BatchRequest, 48),
-    "rp_adjoint_request": (AdjointRequest, 72),
+    "rp_adjoint_request": (AdjointRequest, 80),
 }

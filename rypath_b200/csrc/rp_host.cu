@@ -595,10 +595,19 @@ WaveParams wave_params(const rp_request &r) {
     p.sampler = r.sampler_kind;
     p.randomization = r.randomization;
     u32 v = std::max(std::max(r.width, r.height), 1u) - 1;
-    p.m = r.sampler_kind == RP_SAMPLER_SOBOL ? (v == 0 ? 0 : 32 - __builtin_clz(v)) : 0;
+    const bool sobol_scale = r.sampler_kind == RP_SAMPLER_SOBOL || r.sampler_kind == RP_SAMPLER_ZSOBOL;
+    p.m = sobol_scale ? (v == 0 ? 0 : 32 - __builtin_clz(v)) : 0;
     p.emergency_limit = r.emergency_limit ? r.emergency_limit : 1024;
     p.lanes = r.pixel_count * r.sample_count;
+    // src/metal_render.mm:1979-1981: floor(log2(total samples)) for ZSobol
+    p.log_spp = r.sampler_kind == RP_SAMPLER_ZSOBOL && r.total_samples ? 63 - __builtin_clzll(r.total_samples) : 0;
     return p;
+}
+u32 halton_scale(u32 resolution, u32 base) {
+    u32 scale = 1;
+    while (scale < std::min(resolution, 128u))
+        scale *= base;
+    return scale;
 }
 
 std::string validate_request(const rp_scene *s, const rp_request &r) {
@@ -608,17 +617,46 @@ std::string validate_request(const rp_scene *s, const rp_request &r) {
         return "Render request pixels exceed the film";
     if (uint64_t(r.pixel_count) * r.sample_count > 0xffffffffull)
         return "Render request lanes exceed 2^32";
-    if (r.sampler_kind != RP_SAMPLER_SOBOL && r.sampler_kind != RP_SAMPLER_INDEPENDENT)
-        return "Unsupported sampler (independent and sobol are built)";
-    if (r.sampler_kind == RP_SAMPLER_SOBOL) {
-        if (r.randomization > 3)
-            return "Invalid Sobol randomization";
-        if (std::max(r.width, r.height) > (1u << 25))
-            return "Sobol film exceeds 2^25 pixels per side";
-    }
+    // validate_sampler_range (src/sampling.cpp:51-113)
     if (r.sample_begin > UINT64_MAX - (r.sample_count - 1))
-        return "Sampler range must fit the absolute sample indices";
-    (void)s;
+        return "Sampler range must be nonempty and fit the absolute sample indices";
+    if (r.sampler_kind == RP_SAMPLER_INDEPENDENT)
+        return {};
+    if (r.sampler_kind > RP_SAMPLER_ZSOBOL)
+        return "Invalid render sampler kind";
+    if (r.randomization > 3)
+        return "Invalid QMC randomization mode";
+    if (r.seed != uint64_t(int64_t(int32_t(uint32_t(r.seed)))))
+        return "QMC seed must have a canonical signed 32-bit encoding";
+    const uint64_t last = r.sample_begin + (r.sample_count - 1);
+    if (r.sampler_kind == RP_SAMPLER_HALTON) {
+        if (r.randomization == RP_RANDOMIZE_FASTOWEN)
+            return "Halton does not support fastowen randomization";
+        const uint64_t stride = uint64_t(halton_scale(r.width, 2)) * halton_scale(r.height, 3);
+        if (last > (uint64_t(INT64_MAX) - (stride - 1)) / stride)
+            return "Halton absolute sample range exceeds the signed 64-bit index capacity";
+        const u32 depth_limit = s && s->transport == RP_TRANSPORT_SCALAR ? 124u : 1024u;
+        if (s && s->ds.max_depth > depth_limit)
+            return "Halton supports at most depth 124 for this transport";
+        return {};
+    }
+    const u32 v = std::max(std::max(r.width, r.height), 1u) - 1;
+    const u32 m = v == 0 ? 0 : 32 - __builtin_clz(v);
+    if (m > (r.sampler_kind == RP_SAMPLER_ZSOBOL ? 26u : 25u))
+        return r.sampler_kind == RP_SAMPLER_ZSOBOL ? "ZSobol film dimensions must be positive and at most 2^26"
+                                                   : "Sobol film dimensions must be positive and at most 2^25";
+    if (r.sampler_kind == RP_SAMPLER_ZSOBOL) {
+        if (r.total_samples == 0 || (r.total_samples & (r.total_samples - 1)) != 0)
+            return "ZSobol requires a fixed power-of-two total sample budget";
+        const u32 log_spp = 63 - __builtin_clzll(r.total_samples);
+        if (2 * m + log_spp > 52)
+            return "ZSobol resolution and total sample budget exceed the 52-bit index capacity";
+        if (r.sample_begin >= r.total_samples || r.sample_count > r.total_samples - r.sample_begin)
+            return "ZSobol absolute sample range exceeds its fixed total sample budget";
+        return {};
+    }
+    if (last >= (uint64_t(1) << (52 - 2 * m)))
+        return "Sobol absolute sample range exceeds the 52-bit interval index capacity";
     return {};
 }
 
@@ -1238,6 +1276,24 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             // the packet film weight of the hero transport (src/metal_render.mm:4851-4861)
             ds.filter_weight = d->transport == RP_TRANSPORT_HERO ? g.integral : 1.0f;
         }
+        {
+            // the first 1000 primes, the Halton bases (src/qmc_shared.h:14-18)
+            std::vector<u32> primes;
+            for (u32 n = 2; primes.size() < 1000; ++n) {
+                bool prime = true;
+                for (u32 q : primes) {
+                    if (q * q > n)
+                        break;
+                    if (n % q == 0) {
+                        prime = false;
+                        break;
+                    }
+                }
+                if (prime)
+                    primes.push_back(n);
+            }
+            ds.primes = dupload(own, primes.data(), primes.size(), stm);
+        }
         ds.lens_radius = d->lens_radius;
         ds.focal_distance = d->lens_radius > 0 ? d->focal_distance : 1e6f;
         ds.lens_x = v3(d->lens_x[0], d->lens_x[1], d->lens_x[2]);
@@ -1503,6 +1559,7 @@ static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel 
                 q.emergency_limit = r->emergency_limit;
                 q.sampler_kind = r->sampler_kind;
                 q.randomization = r->randomization;
+                q.total_samples = r->total_samples ? r->total_samples : r->sample_begin + r->sample_count;
                 const std::string err = validate_request(s, q);
                 if (!err.empty())
                     throw Invalid{err};
@@ -1692,6 +1749,7 @@ rp_status rp_cuda_adjoint_device(rp_scene *s, const rp_adjoint_request *r, const
                 q.emergency_limit = f.emergency_limit;
                 q.sampler_kind = f.sampler_kind;
                 q.randomization = f.randomization;
+                q.total_samples = f.total_samples ? f.total_samples : f.sample_begin + f.sample_count;
                 const std::string err = validate_request(s, q);
                 if (!err.empty())
                     throw Invalid{err};
@@ -1753,7 +1811,7 @@ BatchPlan plan_batch(const rp_view *views, u32 count, const rp_batch_request &r,
     if (!views || !count)
         throw Invalid{"a batch needs at least one view"};
     if (r.sampler_kind != RP_SAMPLER_SOBOL && r.sampler_kind != RP_SAMPLER_INDEPENDENT)
-        throw Invalid{"Unsupported sampler (independent and sobol are built)"};
+        throw Invalid{"batched views use the independent or Sobol sampler"};
     if (r.sampler_kind == RP_SAMPLER_SOBOL && r.randomization > 3)
         throw Invalid{"Invalid Sobol randomization"};
     BatchPlan plan;

@@ -127,12 +127,11 @@ RP_DEV u32 sobol_raw(const SobolTables &t, u64 index, u32 dimension) {
     }
     return value;
 }
-// src/sobol_shared.h:108-141
-RP_DEV u32 sobol_word(const SobolTables &t, u64 index, u32 dimension, u32 mode, u32 seed) {
-    u32 value = sobol_raw(t, index, dimension);
+// The randomisations of a 32-bit sample word with a 32-bit hash: none, permute digits (xor),
+// fast Owen (Laine-Karras style hash), Owen (src/sobol_shared.h:115-141, src/qmc_shared.h:190-212)
+RP_DEV u32 scramble_word(u32 value, u32 mode, u32 hash) {
     if (mode == 0)
         return value;
-    const u32 hash = sobol_dimension_hash(dimension, seed);
     if (mode == 1)
         return value ^ hash;
     if (mode == 2) {
@@ -153,6 +152,13 @@ RP_DEV u32 sobol_word(const SobolTables &t, u64 index, u32 dimension, u32 mode, 
     }
     return value;
 }
+// src/sobol_shared.h:108-141
+RP_DEV u32 sobol_word(const SobolTables &t, u64 index, u32 dimension, u32 mode, u32 seed) {
+    const u32 value = sobol_raw(t, index, dimension);
+    if (mode == 0)
+        return value;
+    return scramble_word(value, mode, sobol_dimension_hash(dimension, seed));
+}
 // src/sobol_shared.h:143-154
 RP_DEV float sobol_uniform(u32 v) {
     const float unit = float(v) * 0x1p-32f;
@@ -163,6 +169,177 @@ RP_DEV float sobol_camera_uniform(u32 global, u32 m, u32 pixel) {
     if (local < 0.0f)
         return 0.0f;
     return local < kOneMinusEps ? local : kOneMinusEps;
+}
+
+// ------------------------------------------------------------------ Halton and ZSobol (src/qmc_shared.h, PBRT v4)
+RP_DEV float bits_float(u32 x) { return __uint_as_float(x); }
+RP_DEV u32 float_bits(float x) { return __float_as_uint(x); }
+// :20-40 (MurmurHash64A of two or three words)
+RP_DEV u64 qmc_hash2(u32 a, u32 b) {
+    const u64 m = 0xc6a4a7935bd1e995ull;
+    u64 k = ((u64(b) << 32) | a) * m;
+    k ^= k >> 47;
+    k *= m;
+    u64 h = (8 * m ^ k) * m;
+    h ^= h >> 47;
+    h *= m;
+    return h ^ (h >> 47);
+}
+RP_DEV u64 qmc_hash3(u32 a, u32 b, u32 c) {
+    const u64 m = 0xc6a4a7935bd1e995ull;
+    u64 k = ((u64(b) << 32) | a) * m;
+    k ^= k >> 47;
+    k *= m;
+    u64 h = (12 * m ^ k) * m;
+    h ^= c;
+    h *= m;
+    h ^= h >> 47;
+    h *= m;
+    return h ^ (h >> 47);
+}
+// :41-66 element i of a hashed permutation of [0, l): cycle-walks a bijection on [0, w],
+// w + 1 the next power of two, so it ends within w + 1 steps
+RP_DEV u32 qmc_permutation(u32 i, u32 l, u32 p) {
+    u32 w = l - 1;
+    w |= w >> 1;
+    w |= w >> 2;
+    w |= w >> 4;
+    w |= w >> 8;
+    w |= w >> 16;
+    for (u32 guard = 0; guard <= w; ++guard) {
+        i ^= p;
+        i *= 0xe170893du;
+        i ^= p >> 16;
+        i ^= (i & w) >> 4;
+        i ^= p >> 8;
+        i *= 0x0929eb3fu;
+        i ^= p >> 23;
+        i ^= (i & w) >> 1;
+        i *= 1 | p >> 27;
+        i *= 0x6935fa69u;
+        i ^= (i & w) >> 11;
+        i *= 0x74dcb303u;
+        i ^= (i & w) >> 2;
+        i *= 0x9e501cc3u;
+        i ^= (i & w) >> 2;
+        i *= 0xc860a3dfu;
+        i &= w;
+        i ^= i >> 5;
+        if (i < l)
+            break;
+    }
+    return (i + p) % l;
+}
+// :84-106 scrambled radical inverse of `a` in the base of `dimension`
+RP_DEV float qmc_radical(const u32 *primes, u32 dimension, u64 a, u32 mode, u32 seed) {
+    const u32 base = __ldg(primes + dimension);
+    const u64 limit = ~u64(0) / base - base;
+    const float inv = 1.f / float(base);
+    float inv_m = 1;
+    u64 reversed = 0;
+    u32 digit_index = 0;
+    const u32 owen_hash = u32(mix_bits(1 + (dimension << 4)));
+    while ((mode == 0 ? a != 0 : (mode == 1 ? 1.f - float(base - 1) * inv_m < 1.f : 1.f - inv_m < 1.f)) &&
+           reversed < limit) {
+        const u64 next = a / base;
+        u32 digit = u32(a - next * base);
+        if (mode == 1)
+            digit = qmc_permutation(digit, base, u32(qmc_hash3(base, digit_index, seed)));
+        else if (mode == 3)
+            digit = qmc_permutation(digit, base, u32(mix_bits(owen_hash ^ reversed)));
+        reversed = reversed * base + digit;
+        inv_m *= inv;
+        ++digit_index;
+        a = next;
+    }
+    const float value = float(reversed) * inv_m;
+    return value < kOneMinusEps ? value : kOneMinusEps;
+}
+// :107-114
+RP_DEV u64 qmc_inverse_radical(u32 a, u32 base, u32 count) {
+    u64 result = 0;
+    for (u32 i = 0; i < count; ++i) {
+        result = result * base + a % base;
+        a /= base;
+    }
+    return result;
+}
+// :115-129
+RP_DEV u32 qmc_base_scale(u32 resolution, u32 base) {
+    u32 scale = 1;
+    const u32 bound = resolution < 128 ? resolution : 128;
+    while (scale < bound)
+        scale *= base;
+    return scale;
+}
+RP_DEV u32 qmc_base_exponent(u32 scale, u32 base) {
+    u32 e = 0;
+    while (scale > 1) {
+        scale /= base;
+        ++e;
+    }
+    return e;
+}
+// :130-138 (scales are at most 243)
+RP_DEV u32 qmc_inverse_mod(u32 a, u32 modulus) {
+    if (modulus == 1)
+        return 0;
+    for (u32 i = 1; i < modulus; ++i)
+        if ((a * i) % modulus == 1)
+            return i;
+    return 0;
+}
+// :139-148 Halton index of sample `sample` of pixel (x, y)
+RP_DEV u64 halton_index(u32 width, u32 height, u32 x, u32 y, u64 sample) {
+    const u32 sx = qmc_base_scale(width, 2), sy = qmc_base_scale(height, 3), stride = sx * sy;
+    u64 offset = 0;
+    if (stride > 1) {
+        offset = qmc_inverse_radical(x % 128, 2, qmc_base_exponent(sx, 2)) * sy * qmc_inverse_mod(sy, sx);
+        offset += qmc_inverse_radical(y % 128, 3, qmc_base_exponent(sy, 3)) * sx * qmc_inverse_mod(sx, sy);
+        offset %= stride;
+    }
+    return offset + sample * stride;
+}
+// :176-179
+RP_DEV float halton_camera(const u32 *primes, u32 axis, u32 resolution, u64 index) {
+    const u32 scale = qmc_base_scale(resolution, axis == 0 ? 2 : 3);
+    return qmc_radical(primes, axis, index / scale, 0, 0);
+}
+// :213-220
+RP_DEV u64 zsobol_morton(u32 x, u32 y, u32 log_spp, u64 sample) {
+    u64 result = 0;
+    for (u32 b = 0; b < 26; ++b) {
+        result |= u64((x >> b) & 1) << (2 * b);
+        result |= u64((y >> b) & 1) << (2 * b + 1);
+    }
+    return (result << log_spp) | sample;
+}
+// :221-238 ZSobol index: base-4 digits of the Morton index permuted by a hash of their prefix
+RP_DEV u64 zsobol_index(u64 morton_index, u32 dimension, u32 exponent, u32 log_spp) {
+    // the 24 permutations of 4 elements, 2 bits each (digit d at bits 2d..2d+1)
+    constexpr unsigned char perm[24] = {0xe4, 0xb4, 0xd8, 0x78, 0x6c, 0x9c, 0xe1, 0xb1, 0xc9, 0x39, 0x2d, 0x8d,
+                                        0xc6, 0x36, 0xd2, 0x72, 0x4e, 0x1e, 0x27, 0x87, 0x1b, 0x4b, 0x63, 0x93};
+    const u32 odd = log_spp & 1;
+    const u32 digits = exponent + (log_spp + 1) / 2;
+    u64 result = 0;
+    for (int i = int(digits) - 1; i >= int(odd); --i) {
+        const u32 shift = 2 * u32(i) - odd;
+        const u32 digit = u32((morton_index >> shift) & 3);
+        const u64 higher = morton_index >> (shift + 2);
+        const u32 p = u32((mix_bits(higher ^ u32(0x55555555u * dimension)) >> 24) % 24);
+        result |= u64((perm[p] >> (2 * digit)) & 3) << shift;
+    }
+    if (odd)
+        result |= (morton_index & 1) ^ (mix_bits((morton_index >> 1) ^ u32(0x55555555u * dimension)) & 1);
+    return result;
+}
+// :244-249
+RP_DEV u32 zsobol_word(const SobolTables &t, u64 morton_index, u32 dimension, u32 axis, bool pair, u32 exponent,
+                       u32 log_spp, u32 mode, u32 seed) {
+    const u64 index = zsobol_index(morton_index, dimension, exponent, log_spp);
+    const u64 hash = qmc_hash2(dimension + (pair ? 2 : 1), seed);
+    const u32 random = pair && axis == 1 ? u32(hash >> 32) : u32(hash);
+    return scramble_word(sobol_raw(t, index, axis), mode, random);
 }
 
 // ------------------------------------------------------------------ Philox (shaders/render.metal:97-111)

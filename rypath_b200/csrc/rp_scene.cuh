@@ -102,6 +102,7 @@ struct DeviceScene {
     const float *gauss_cdf;
     u32 gauss_w, gauss_h;
     float filter_weight;
+    const u32 *primes; // the first 1000 primes (Halton bases)
 };
 
 RP_DEV V3 load3(const float *p) { return v3(__ldg(p), __ldg(p + 1), __ldg(p + 2)); }

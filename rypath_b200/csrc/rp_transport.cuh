@@ -62,19 +62,43 @@ struct PathPool {
     u32 adj_params;         // gradient entries
 };
 
+// sampler: 0 independent, 1 Sobol, 2 Halton, 3 ZSobol (src/render_wire.h:41)
 struct WaveParams {
     u32 width, height, pixel_begin, pixel_count, sample_low, sample_high;
     u32 seed_low, seed_high, sampler, randomization, m, emergency_limit;
     u32 lanes;
+    u32 log_spp; // ZSobol: log2 of the total sample budget
 };
 
-RP_DEV float sample_uniform(const WaveParams &p, u32 w) { return p.sampler == 0 ? u01(w) : sobol_uniform(w); }
+// shaders/render.metal:113-122
+RP_DEV float sample_uniform(const WaveParams &p, u32 w) {
+    if (p.sampler == 2)
+        return bits_float(w);
+    return p.sampler == 0 ? u01(w) : sobol_uniform(w);
+}
+// Integer decisions quantise the Halton uniform, not its binary32 representation.
+RP_DEV u32 decision_word(const WaveParams &p, u32 w) { return p.sampler == 2 ? u32(bits_float(w) * 0x1p32f) : w; }
+// shaders/render.metal:123-127
+RP_DEV u32 zdraw(const DeviceScene &s, const WaveParams &p, u64 index, u32 dimension, u32 axis = 0, bool pair = false) {
+    return zsobol_word(s.sobol, index, dimension, axis, pair, p.m, p.log_spp, p.randomization, p.seed_low);
+}
 
 // shaders/render.metal:154-179 (independent and Sobol samplers); out of line, one copy per kernel
 __device__ __noinline__ uint4 draw_words(const DeviceScene &s, const WaveParams &p, u32 pixel, u32 slo, u32 shi,
                                          u64 index, u32 block) {
     if (p.sampler == 0)
         return philox(make_uint4(pixel, slo, shi, block), p.seed_low, p.seed_high);
+    const u32 d = 4 * block;
+    if (p.sampler == 2)
+        return make_uint4(float_bits(qmc_radical(s.primes, d, index, p.randomization, p.seed_low)),
+                          float_bits(qmc_radical(s.primes, d + 1, index, p.randomization, p.seed_low)),
+                          float_bits(qmc_radical(s.primes, d + 2, index, p.randomization, p.seed_low)),
+                          float_bits(qmc_radical(s.primes, d + 3, index, p.randomization, p.seed_low)));
+    if (p.sampler == 3) {
+        const bool even = (block & 1) == 0;
+        return make_uint4(zdraw(s, p, index, d, 0, true), zdraw(s, p, index, d, 1, true),
+                          zdraw(s, p, index, d + 2, 0, even), zdraw(s, p, index, even ? d + 2 : d + 3, even ? 1 : 0, even));
+    }
     u32 w[4];
 #pragma unroll 1
     for (u32 k = 0; k < 4; ++k)
@@ -134,6 +158,18 @@ RP_DEV BeginSample begin_sample(const DeviceScene &s, const WaveParams &p, u32 l
         r.words = make_uint4(sobol_word(s.sobol, r.index, 0, 0, 0), sobol_word(s.sobol, r.index, 1, 0, 0),
                              sobol_word(s.sobol, r.index, 2, p.randomization, p.seed_low),
                              sobol_word(s.sobol, r.index, 3, p.randomization, p.seed_low));
+    } else if (p.sampler == 2) {
+        const u64 sample = (u64(r.sample_high) << 32) | r.sample_low;
+        r.index = halton_index(p.width, p.height, r.pixel % p.width, r.pixel / p.width, sample);
+        r.words = make_uint4(float_bits(halton_camera(s.primes, 0, p.width, r.index)),
+                             float_bits(halton_camera(s.primes, 1, p.height, r.index)),
+                             float_bits(qmc_radical(s.primes, 2, r.index, p.randomization, p.seed_low)),
+                             float_bits(qmc_radical(s.primes, 3, r.index, p.randomization, p.seed_low)));
+    } else if (p.sampler == 3) {
+        const u64 sample = (u64(r.sample_high) << 32) | r.sample_low;
+        r.index = zsobol_morton(r.pixel % p.width, r.pixel / p.width, p.log_spp, sample);
+        r.words = make_uint4(zdraw(s, p, r.index, 1, 0, true), zdraw(s, p, r.index, 1, 1, true),
+                             zdraw(s, p, r.index, 0), zdraw(s, p, r.index, 3));
     } else {
         r.index = 0;
         r.words = philox(make_uint4(r.pixel, r.sample_low, r.sample_high, 0), p.seed_low, p.seed_high);
@@ -143,6 +179,12 @@ RP_DEV BeginSample begin_sample(const DeviceScene &s, const WaveParams &p, u32 l
         if (p.sampler == 1) {
             r.lens_words = make_uint2(sobol_word(s.sobol, r.index, kLensDimensionX, p.randomization, p.seed_low),
                                       sobol_word(s.sobol, r.index, kLensDimensionX + 1, p.randomization, p.seed_low));
+        } else if (p.sampler == 2) {
+            r.lens_words = make_uint2(float_bits(qmc_radical(s.primes, 998, r.index, p.randomization, p.seed_low)),
+                                      float_bits(qmc_radical(s.primes, 999, r.index, p.randomization, p.seed_low)));
+        } else if (p.sampler == 3) {
+            r.lens_words = make_uint2(zdraw(s, p, r.index, kLensDimensionX, 0, true),
+                                      zdraw(s, p, r.index, kLensDimensionX, 1, true));
         } else {
             const uint4 w = philox(make_uint4(r.pixel, r.sample_low, r.sample_high, kLensBlock), p.seed_low, p.seed_high);
             r.lens_words = make_uint2(w.x, w.y);
@@ -150,8 +192,10 @@ RP_DEV BeginSample begin_sample(const DeviceScene &s, const WaveParams &p, u32 l
     }
     r.filter_x = r.filter_y = 0;
     if (s.filter_kind == 2) {
-        const float ux = p.sampler == 1 ? sobol_camera_uniform(r.words.x, p.m, r.pixel % p.width) : u01(r.words.x);
-        const float uy = p.sampler == 1 ? sobol_camera_uniform(r.words.y, p.m, r.pixel / p.width) : u01(r.words.y);
+        const float ux =
+            p.sampler == 1 ? sobol_camera_uniform(r.words.x, p.m, r.pixel % p.width) : sample_uniform(p, r.words.x);
+        const float uy =
+            p.sampler == 1 ? sobol_camera_uniform(r.words.y, p.m, r.pixel / p.width) : sample_uniform(p, r.words.y);
         gaussian_filter_offsets(s, ux, uy, r.filter_x, r.filter_y);
     }
     return r;
@@ -169,12 +213,13 @@ struct RasterCam {
 RP_DEV void primary_ray_from(const DeviceScene &s, const RasterCam &cam, const WaveParams &p, const BeginSample &b,
                              V3 &o, V3 &d) {
     float ux, uy;
+    // camera_uniforms (shaders/render.metal:341-350)
     if (p.sampler == 1) {
         ux = sobol_camera_uniform(b.words.x, p.m, b.pixel % p.width);
         uy = sobol_camera_uniform(b.words.y, p.m, b.pixel / p.width);
     } else {
-        ux = u01(b.words.x);
-        uy = u01(b.words.y);
+        ux = sample_uniform(p, b.words.x);
+        uy = sample_uniform(p, b.words.y);
     }
     o = cam.origin;
     const float nan = __int_as_float(0x7fffffff);

@@ -893,7 +893,7 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
         after = kAfterFail | (S_ARITHMETIC << 8);
     } else {
         ++path.scatterings;
-        if (path.scatterings >= 3 && bsdf_words.z >= 0xc0000000u) {
+        if (path.scatterings >= 3 && decision_word(p, bsdf_words.z) >= 0xc0000000u) {
             after = kAfterFinish;
         } else {
             if (path.scatterings >= 3)

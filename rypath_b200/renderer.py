@@ -39,6 +39,7 @@ class RenderRequest:
     sampler: int = abi.SAMPLER_SOBOL
     randomization: int = abi.RANDOMIZE_OWEN
     boundary_limit: int = 4096
+    total_samples: int = 0  # the render's sample budget (ZSobol); 0: sample_begin + sample_count
 
     def to_c(self) -> abi.Request:
         r = abi.Request()
@@ -48,6 +49,7 @@ class RenderRequest:
         r.sample_begin, r.sample_count = self.sample_begin, self.sample_count
         r.emergency_limit, r.sampler_kind = self.emergency_limit, self.sampler
         r.randomization, r.boundary_limit = self.randomization, self.boundary_limit
+        r.total_samples = self.total_samples or (self.sample_begin + self.sample_count)
         return r
 
 

@@ -6,6 +6,9 @@ Reads the reference's test sources as text (nothing is executed):
   dimension hash, words for the four randomisations, binary32 pixel remap), generated by
   the reference from PBRT v4 b0bdf461.
 * ``tests/replay_tests.cpp`` -- Random123 v1.14.0 Philox4x32-10 known-answer vectors.
+* ``tests/qmc_sampling_tests.cpp`` -- PBRT v4 Halton and ZSobol known answers (index, camera
+  samples and scrambled radical inverse / ZSobol words for four randomisations), generated
+  by the reference from PBRT v4 b0bdf461.
 * ``tests/gaussian_filter_tests.cpp`` -- FNV-1a digests of the Gaussian filter tables (every
   CDF entry) and of 33x33 filter samples for three (x radius, y radius, sigma)
   configurations, obtained by the reference from PBRT v4 b0bdf461.
@@ -70,6 +73,13 @@ def philox_answers(text: str):
     return out
 
 
+def qmc_answers(text: str):
+    out = []
+    for q, a in re.findall(r"\{\{([-0-9, ]+)\},\s*\{([0-9ul, ]+)\}\}", text):
+        out.append({"q": [int(t) for t in q.split(",")], "a": [_int(t) for t in a.split(",")]})
+    return out
+
+
 def gaussian_answers(text: str):
     configs = re.findall(r"Configuration\{([^}]*)\}", text)
     configs = [[_float(t) for t in c.split(",")] for c in configs]
@@ -85,12 +95,14 @@ def main() -> None:
     sobol = sobol_answers((reference / "tests/sampling_tests.cpp").read_text())
     philox = philox_answers((reference / "tests/replay_tests.cpp").read_text())
     gaussian = gaussian_answers((reference / "tests/gaussian_filter_tests.cpp").read_text())
-    if len(sobol) != 8 or len(philox) != 3 or len(gaussian) != 3:
+    qmc = qmc_answers((reference / "tests/qmc_sampling_tests.cpp").read_text())
+    if len(sobol) != 8 or len(philox) != 3 or len(gaussian) != 3 or len(qmc) != 28:
         raise SystemExit(f"unexpected vector counts: sobol {len(sobol)}, philox {len(philox)}, "
-                         f"gaussian {len(gaussian)}")
+                         f"gaussian {len(gaussian)}, qmc {len(qmc)}")
     (here / "sobol_known_answers.json").write_text(json.dumps(sobol, indent=1) + "\n")
     (here / "philox_known_answers.json").write_text(json.dumps(philox, indent=1) + "\n")
     (here / "gaussian_filter_known_answers.json").write_text(json.dumps(gaussian, indent=1) + "\n")
+    (here / "qmc_known_answers.json").write_text(json.dumps(qmc, indent=1) + "\n")
 
 
 if __name__ == "__main__":

@@ -45,6 +45,7 @@ def oracle():
         lib.or_probe_medium.argtypes = [vp, u32, vp]
         lib.or_scalar_film_add.argtypes = [vp, sz, vp, u32, vp]
         lib.or_adjoint.argtypes = [vp, C.POINTER(abi.FilmRequest), vp, u32, vp, vp, vp, C.c_int]
+        lib.or_probe_qmc.argtypes = [vp, vp, u32, vp]
         lib.or_gaussian_filter.argtypes = [C.c_float, C.c_float, C.c_float, vp, sz, vp, vp, vp, u32, vp]
         _oracle = lib
     return _oracle
@@ -71,6 +72,7 @@ def reference():
         lib.ref_set_cie.argtypes = [vp]
         lib.ref_film_add.argtypes = [vp, sz, u32, u32, vp]
         lib.ref_probe_medium.argtypes = [vp, u32, vp]
+        lib.ref_probe_qmc.argtypes = [vp, u32, vp]
         _ref = lib
     return _ref
 
@@ -119,6 +121,7 @@ def request(width, height, spp=1, sample_begin=0, pixel_begin=0, pixel_count=Non
     r.pixel_count = width * height if pixel_count is None else pixel_count
     r.sample_begin, r.sample_count = sample_begin, spp
     r.emergency_limit, r.sampler_kind, r.randomization, r.boundary_limit = 1024, sampler, randomization, 4096
+    r.total_samples = sample_begin + spp
     return r
 
 

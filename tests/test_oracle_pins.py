@@ -295,3 +295,36 @@ def test_gaussian_filter_table_and_samples_match_rypath_known_answers():
         assert _fnv_floats(cdf[:n]) == k["cdf_hash"]
         assert _fnv_floats(out.reshape(-1)) == k["sample_hash"]
         assert integral.value > 0
+
+
+def _qmc_queries(rng, n):
+    q = []
+    for _ in range(n):
+        kind = int(rng.choice([2, 3]))
+        w, h = int(rng.integers(1, 400)), int(rng.integers(1, 300))
+        spp = int(2 ** rng.integers(0, 11))
+        sample = int(rng.integers(0, spp if kind == 3 else 1 << 20))
+        mode = int(rng.choice([0, 1, 3] if kind == 2 else [0, 1, 2, 3]))
+        d = int(rng.integers(2, 997)) if kind == 2 else int(rng.integers(0, 1023))
+        seed = int(rng.integers(-(2 ** 31), 2 ** 31))
+        q.append([kind, w, h, int(rng.integers(0, w)), int(rng.integers(0, h)), sample, d, mode, seed, spp])
+    return np.ascontiguousarray(q, np.int64)
+
+
+def test_qmc_halton_and_zsobol_match_rypath_known_answers():
+    """tests/qmc_sampling_tests.cpp:21-77: 28 PBRT v4 known answers (12 Halton, 16 ZSobol)."""
+    known = json.load(open(os.path.join(GOLDEN, "qmc_known_answers.json")))
+    q = np.ascontiguousarray([k["q"] for k in known], np.int64)
+    out = np.zeros((len(known), 6), np.uint64)
+    oracle().or_probe_qmc(C.cast(TABLE_BUF, C.c_void_p), q.ctypes.data, len(known), out.ctypes.data)
+    np.testing.assert_array_equal(out, np.array([k["a"] for k in known], np.uint64))
+
+
+def test_qmc_matches_reference_header():
+    ref = need_ref()
+    q = _qmc_queries(np.random.default_rng(11), 3000)
+    a = np.zeros((q.shape[0], 6), np.uint64)
+    b = np.zeros_like(a)
+    oracle().or_probe_qmc(C.cast(TABLE_BUF, C.c_void_p), q.ctypes.data, q.shape[0], a.ctypes.data)
+    ref.ref_probe_qmc(q.ctypes.data, q.shape[0], b.ctypes.data)
+    np.testing.assert_array_equal(a, b)
