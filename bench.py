@@ -468,7 +468,7 @@ def main():
         film_bytes = pixels * 96
 
         def e2e_step(i):
-            film_host[...] = np.zeros(1, abi.film_dtype())
+            film_host.view(np.uint8).fill(0)  # a fresh film each step (a memset, not a structured broadcast)
             st, diag, _ = renderer.render_progressive(
                 scene, renderer.RenderSettings(args.width, args.height, samples=args.spp, batch_size=args.spp,
                                                seed=1), device=local, film=film_host)

@@ -21,27 +21,98 @@ RP_HD float unordered_host(int i) {
 
 struct BuildTmp {
     float4 *box_lo, *box_hi; // per triangle (original order)
-    int *cbounds;            // ordered-int centroid min[3], max[3]
+    int *cbounds;            // ordered ints: centroid min[3], max[3], then vertex min[3], max[3]
     u64 *keys[2];
     u32 *vals[2];
     u32 *hist;
     u32 *left, *right, *parent, *leaf_parent;
     float4 *node_lo, *node_hi; // internal node bounds
     u32 *flags;
+    u32 *error;                // kBuildVertexRange | kBuildTree bits
+    u32 *refs;                 // references to internal nodes [0, n-1) and leaves [n-1, 2n-1)
+    u32 vertex_count;
 };
+constexpr u32 kBuildVertexRange = 1, kBuildTree = 2;
+// a path from a leaf to the root is shorter than 64 + 32 levels for unique-by-index keys
+constexpr int kMaxTreeLevels = 160;
 
-// World-space vertices, boxes and centroid bounds of every triangle.
+// Flattened triangle i -> (instance, triangle within the instance, BSDF family of its
+// material).  prim_begin: the first flattened triangle of each instance (an exclusive prefix
+// of the instances' triangle counts), so the instance of i is the last one beginning at or
+// before i.
+__global__ void k_flatten(const DInstance *instances, const u32 *prim_begin, u32 instance_count,
+                          const DMaterial *materials, u32 n, u32 *tri_instance, u32 *tri_local,
+                          unsigned char *tri_family) {
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        u32 lo = 0, hi = instance_count;
+        while (hi - lo > 1) {
+            const u32 mid = (lo + hi) / 2;
+            if (prim_begin[mid] <= i)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        tri_instance[i] = lo;
+        tri_local[i] = i - prim_begin[lo];
+        tri_family[i] = (unsigned char)materials[instances[lo].material].scattering;
+    }
+}
+
+// Block reduction of six (min, max) pairs; pair a < 3 goes to gmin[a], gmax[a], pair a >= 3
+// to gmin[a + 3], gmax[a + 3].
+RP_DEV void block_min_max(int (&lmin)[6], int (&lmax)[6], int *gmin, int *gmax) {
+    __shared__ int smin[6][32], smax[6][32];
+#pragma unroll
+    for (int a = 0; a < 6; ++a)
+        for (int o = 16; o > 0; o >>= 1) {
+            lmin[a] = min(lmin[a], __shfl_xor_sync(0xffffffffu, lmin[a], o));
+            lmax[a] = max(lmax[a], __shfl_xor_sync(0xffffffffu, lmax[a], o));
+        }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+        for (int a = 0; a < 6; ++a) {
+            smin[a][warp] = lmin[a];
+            smax[a][warp] = lmax[a];
+        }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int a = threadIdx.x;
+        int mn = 0x7fffffff, mx = int(0x80000000);
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) {
+            mn = min(mn, smin[a][w]);
+            mx = max(mx, smax[a][w]);
+        }
+        atomicMin(gmin + (a < 3 ? a : a + 3), mn);
+        atomicMax(gmax + (a < 3 ? a : a + 3), mx);
+    }
+}
+
+// World-space vertices, boxes, centroid bounds and vertex bounds of every triangle.  A vertex
+// index outside the vertex array sets kBuildVertexRange and is not read.
 __global__ void k_tri_prepare(const __grid_constant__ DeviceScene s, float4 *world, BuildTmp t) {
-    __shared__ int smin[3][32], smax[3][32];
-    int lmin[3] = {0x7fffffff, 0x7fffffff, 0x7fffffff}, lmax[3] = {int(0x80000000), int(0x80000000), int(0x80000000)};
+    // [0, 3): centroid axes (into cbounds), [3, 6): vertex axes (into vbounds)
+    int lmin[6], lmax[6];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+        lmin[a] = 0x7fffffff;
+        lmax[a] = int(0x80000000);
+    }
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < s.prim_count; i += gridDim.x * blockDim.x) {
         const DInstance &in = s.instances[s.tri_instance[i]];
-        const u32 *tri = s.triangles + 3 * (in.triangle_begin + s.tri_local[i]);
+        const u32 *tri = s.triangles + 3 * size_t(in.triangle_begin + s.tri_local[i]);
+        bool valid = true;
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            valid = valid && (unsigned long long)in.vertex_begin + tri[k] < t.vertex_count;
+        if (!valid) {
+            atomicOr(t.error, kBuildVertexRange);
+            continue;
+        }
         V3 v[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            v[k] = world_point(in, load3(s.positions + 3 * (in.vertex_begin + tri[k])));
-            world[3 * i + k] = make_float4(v[k].x, v[k].y, v[k].z, 0);
+            v[k] = world_point(in, load3(s.positions + 3 * size_t(in.vertex_begin + tri[k])));
+            world[3 * size_t(i) + k] = make_float4(v[k].x, v[k].y, v[k].z, 0);
         }
         const V3 lo = v3(fminf(fminf(v[0].x, v[1].x), v[2].x), fminf(fminf(v[0].y, v[1].y), v[2].y),
                          fminf(fminf(v[0].z, v[1].z), v[2].z));
@@ -50,35 +121,16 @@ __global__ void k_tri_prepare(const __grid_constant__ DeviceScene s, float4 *wor
         t.box_lo[i] = make_float4(lo.x, lo.y, lo.z, 0);
         t.box_hi[i] = make_float4(hi.x, hi.y, hi.z, 0);
         const float c[3] = {0.5f * lo.x + 0.5f * hi.x, 0.5f * lo.y + 0.5f * hi.y, 0.5f * lo.z + 0.5f * hi.z};
+        const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             lmin[a] = min(lmin[a], ordered(c[a]));
             lmax[a] = max(lmax[a], ordered(c[a]));
+            lmin[3 + a] = min(lmin[3 + a], ordered(l[a]));
+            lmax[3 + a] = max(lmax[3 + a], ordered(h[a]));
         }
     }
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-        for (int o = 16; o > 0; o >>= 1) {
-            lmin[a] = min(lmin[a], __shfl_xor_sync(0xffffffffu, lmin[a], o));
-            lmax[a] = max(lmax[a], __shfl_xor_sync(0xffffffffu, lmax[a], o));
-        }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0)
-        for (int a = 0; a < 3; ++a) {
-            smin[a][warp] = lmin[a];
-            smax[a][warp] = lmax[a];
-        }
-    __syncthreads();
-    if (threadIdx.x < 3) {
-        const int a = threadIdx.x;
-        int mn = 0x7fffffff, mx = int(0x80000000);
-        for (int w = 0; w < int(blockDim.x >> 5); ++w) {
-            mn = min(mn, smin[a][w]);
-            mx = max(mx, smax[a][w]);
-        }
-        atomicMin(t.cbounds + a, mn);
-        atomicMax(t.cbounds + 3 + a, mx);
-    }
+    block_min_max(lmin, lmax, t.cbounds, t.cbounds + 3);
 }
 
 RP_DEV u64 spread21(u64 x) {
@@ -253,8 +305,7 @@ __global__ void k_karras(const u64 *keys, u32 n, BuildTmp t) {
 __global__ void k_refit(u32 n, const u32 *order, BuildTmp t) {
     for (u32 slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
         u32 node = t.leaf_parent[slot];
-        // a path from a leaf to the root is shorter than 64 + 32 levels for unique-by-index keys
-        for (int level = 0; node != kNone && level < 160; ++level) {
+        for (int level = 0; node != kNone && level < kMaxTreeLevels; ++level) {
             __threadfence();
             if (atomicAdd(t.flags + node, 1u) == 0)
                 break;
@@ -307,6 +358,47 @@ __global__ void k_pack(u32 n, const u32 *order, const float4 *world, BuildTmp t,
             b.d = make_uint4(ch[0], ch[1], 0, 0);
             nodes[i] = b;
         }
+    }
+}
+
+// Structural check of the topology before any traversal.  k_tree_refs counts the references
+// to every internal node and leaf (a child index out of range sets kBuildTree); k_tree_verify
+// requires exactly one reference to each node but the root (none) and each leaf, and a walk
+// from every leaf up its parents that reaches the root within kMaxTreeLevels.  Together they
+// make the topology a tree of all 2n - 1 nodes: a part unreachable from the root would give
+// one of its leaves a parent chain that never reaches the root.  Traversal loops are then
+// finite, and k_refit (bounded by the same level count) has refit every node.
+__global__ void k_tree_refs(u32 n, BuildTmp t) {
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i + 1 < n; i += gridDim.x * blockDim.x) {
+        const u32 ch[2] = {t.left[i], t.right[i]};
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const u32 c = ch[k] & ~kLeaf;
+            const bool leaf = (ch[k] & kLeaf) != 0;
+            if (leaf ? c >= n : c >= n - 1) {
+                atomicOr(t.error, kBuildTree);
+                continue;
+            }
+            atomicAdd(t.refs + (leaf ? n - 1 + c : c), 1u);
+        }
+    }
+}
+__global__ void k_tree_verify(u32 n, BuildTmp t) {
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < 2 * n - 1; i += gridDim.x * blockDim.x) {
+        if (t.refs[i] != (i == 0 ? 0u : 1u)) {
+            atomicOr(t.error, kBuildTree);
+            continue;
+        }
+        if (i < n - 1)
+            continue;
+        u32 node = t.leaf_parent[i - (n - 1)];
+        int level = 0;
+        while (node != 0 && node < n - 1 && level + 1 < kMaxTreeLevels) {
+            node = t.parent[node];
+            ++level;
+        }
+        if (node != 0)
+            atomicOr(t.error, kBuildTree);
     }
 }
 

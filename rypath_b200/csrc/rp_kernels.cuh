@@ -103,11 +103,15 @@ __global__ void __launch_bounds__(Block) k_trace(const __grid_constant__ DeviceS
 
 // One hero event after its closest hit (shaders/packet_pt_event_body.inc:11-461), for the paths
 // whose hit is of BSDF family F (3: no surface -- environment or a failed query).
-template <int F, int Block = 128>
-__global__ void __launch_bounds__(Block) k_shade(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p,
-                                               PathPool pool, int in) {
+// Adjoint: the path-replay adjoint hooks are compiled in (the plain forward kernel carries none
+// of their registers).  The minimum of 384 resident threads per SM caps registers at 168, so
+// three 128-thread blocks fit an SM.
+template <int F, int Block = 128, bool Adjoint = false>
+__global__ void __launch_bounds__(Block, 384 / Block) k_shade(const __grid_constant__ DeviceScene s,
+                                                              const __grid_constant__ WaveParams p, PathPool pool, int in) {
     extern __shared__ float sgrad[]; // adjoint only
-    adjoint_begin(pool, sgrad);
+    if (Adjoint)
+        adjoint_begin(pool, sgrad);
     const u32 count = pool.counters[4 + F];
     const u32 *queue = pool.bins + size_t(F) * pool.bin_capacity;
     u32 *out_queue = pool.queue[in ^ 1];
@@ -353,7 +357,7 @@ __global__ void __launch_bounds__(Block) k_shade(const __grid_constant__ DeviceS
                         }
                     }
                     radiance = add4(radiance, endpoint);
-                    if (pool.hist) {
+                    if (Adjoint) {
                         // replay: the emission's gradient over the vertices before this one,
                         // then this diffuse vertex joins the history of what follows it
                         uint4 h = pool.hist[path];
@@ -524,15 +528,17 @@ __global__ void __launch_bounds__(Block) k_shade(const __grid_constant__ DeviceS
             pool.sh_c[sslot] = sh_c;
         }
     }
-    adjoint_end(pool, sgrad);
+    if (Adjoint)
+        adjoint_end(pool, sgrad);
 }
 
 // Visibility of the light samples (visible(), shaders/packet_transport.h:377-446, opaque surfaces)
-template <bool Count, int Block = kTraceBlock>
+template <bool Count, int Block = kTraceBlock, bool Adjoint = false>
 __global__ void __launch_bounds__(Block) k_shadow(const __grid_constant__ DeviceScene s, PathPool pool) {
     __shared__ u32 stack[kStackDepth * Block];
     extern __shared__ float sgrad[]; // adjoint only
-    adjoint_begin(pool, sgrad);
+    if (Adjoint)
+        adjoint_begin(pool, sgrad);
     const u32 count = pool.counters[2];
     u32 nodes = 0, tris = 0, rays = 0;
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
@@ -565,13 +571,14 @@ __global__ void __launch_bounds__(Block) k_shadow(const __grid_constant__ Device
         if (!finite_nonnegative4(from_float4(r))) {
             ident.w = set_status(ident.w, 2) | F_COMPLETE;
             pool.ident[path] = ident;
-        } else if (pool.hist) {
+        } else if (Adjoint) {
             // replay: the light sample's gradient, over the history including its vertex
             adjoint_accumulate(s, pool, sgrad, pool.hist[path], from_float4(pool.lambda[path]), from_float4(c),
                                pool.adj_w[path]);
         }
     }
-    adjoint_end(pool, sgrad);
+    if (Adjoint)
+        adjoint_end(pool, sgrad);
     if (Count) {
         atomicAdd(pool.stats + 4, (unsigned long long)nodes);
         atomicAdd(pool.stats + 5, (unsigned long long)tris);
