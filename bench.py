@@ -360,7 +360,7 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    from rypath_b200 import abi, renderer, scenes
+    from rypath_b200 import abi, renderer, scenes, shard
 
     scene = scenes.mixed_scene(args.width, args.height, args.spp, args.depth, subdivisions=args.subdivisions)
     pixels = args.width * args.height
@@ -371,7 +371,9 @@ def main():
     rs = built.scene
     film = torch.zeros(pixels * 12, dtype=torch.float64, device="cuda")  # rp_film_pixel is 96 bytes
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
-    sample_base = rank * args.spp * (args.warmup + args.steps + 1)
+    # each rank's disjoint block of absolute samples: the counting render, warm-up and timed steps
+    per_rank = args.spp * (args.warmup + args.steps + 1)
+    sample_base, _ = shard.sample_range(per_rank * world, rank, world)
 
     # exact traversal counts for the roofline (an untimed counting render of the same workload)
     rs.set_counting(True)
