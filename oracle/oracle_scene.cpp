@@ -577,9 +577,15 @@ void build_lbvh(const std::vector<std::array<F3, 3>> &tris, Bvh &b) {
         }
     }
     const F3 ext = hi - lo;
+    // bit 63: a box side longer than 1/16 of the largest centroid extent (the device builder's
+    // large-triangle split at the root, rypath_b200/csrc/rp_build.cuh k_morton)
+    const float large = std::max(std::max(ext[0], ext[1]), ext[2]) * 0.0625f;
     std::vector<std::pair<u64, u32>> items(n);
-    for (u32 i = 0; i < n; ++i)
-        items[i] = {morton63(centroid[i], lo, ext), i};
+    for (u32 i = 0; i < n; ++i) {
+        const bool is_large = box[i].hi[0] - box[i].lo[0] > large || box[i].hi[1] - box[i].lo[1] > large ||
+                              box[i].hi[2] - box[i].lo[2] > large;
+        items[i] = {(is_large ? 1ull << 63 : 0ull) | morton63(centroid[i], lo, ext), i};
+    }
     std::stable_sort(items.begin(), items.end(),
                      [](const auto &x, const auto &y) { return x.first < y.first; });
     b.keys.resize(n);

@@ -142,9 +142,16 @@ RP_DEV u64 spread21(u64 x) {
     x = (x | x << 2) & 0x1249249249249249ull;
     return x;
 }
+// Sort key of a triangle: the 63-bit Morton code of its centroid, with bit 63 set for a large
+// triangle (a box side longer than 1/16 of the largest centroid extent).  Large triangles then
+// sort after all others and Karras's topology splits them off at the root, so their boxes do
+// not inflate the nodes above the small triangles near their centroids (a ground plane of two
+// triangles would otherwise widen every node on its two root-to-leaf paths).
 __global__ void k_morton(u32 n, BuildTmp t, float3 lo, float3 ext) {
+    const float large = fmaxf(fmaxf(ext.x, ext.y), ext.z) * 0.0625f;
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 bl = t.box_lo[i], bh = t.box_hi[i];
+        const bool is_large = bh.x - bl.x > large || bh.y - bl.y > large || bh.z - bl.z > large;
         const float c[3] = {0.5f * bl.x + 0.5f * bh.x, 0.5f * bl.y + 0.5f * bh.y, 0.5f * bl.z + 0.5f * bh.z};
         const float l[3] = {lo.x, lo.y, lo.z}, e[3] = {ext.x, ext.y, ext.z};
         u64 q[3];
@@ -155,7 +162,7 @@ __global__ void k_morton(u32 n, BuildTmp t, float3 lo, float3 ext) {
             cell = fminf(fmaxf(cell, 0.0f), 2097151.0f);
             q[a] = u64(cell);
         }
-        t.keys[0][i] = (spread21(q[0]) << 2) | (spread21(q[1]) << 1) | spread21(q[2]);
+        t.keys[0][i] = (is_large ? 1ull << 63 : 0ull) | (spread21(q[0]) << 2) | (spread21(q[1]) << 1) | spread21(q[2]);
         t.vals[0][i] = i;
     }
 }

@@ -623,8 +623,80 @@ struct Hit {
 // Stack depth for traversal; deeper trees report an invalid hit.
 constexpr int kStackDepth = 64;
 
+// Outcome of one node visit of a walk.
+enum WalkStep : int { kWalkMore = 0, kWalkDone = 1, kWalkFailed = 2 };
+
+// Ray of a walk: origin, direction and the slab reciprocals.
+struct WalkRay {
+    V3 o, d, inv;
+};
+RP_DEV WalkRay walk_ray(V3 o, V3 d) { return {o, d, v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z)}; }
+
+// Closest-hit triangle test of leaf slot `slot`: keeps the minimum (t, primitive id).
+template <bool Count>
+RP_DEV void closest_leaf(const DeviceScene &s, const WalkRay &r, float tmax, Hit &h, u32 slot, u32 &tris_tested) {
+    const float4 a = __ldg(s.leaf_v + 3 * slot), b = __ldg(s.leaf_v + 3 * slot + 1), c = __ldg(s.leaf_v + 3 * slot + 2);
+    const u32 prim = __float_as_uint(a.w);
+    float t, b1, b2;
+    if (Count)
+        ++tris_tested;
+    if (intersect_triangle(r.o, r.d, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tmax, t, b1, b2) &&
+        (t < h.t || (t == h.t && prim < h.prim))) {
+        h.t = t;
+        h.b1 = b1;
+        h.b2 = b2;
+        h.prim = prim;
+    }
+}
+
+// One node visit of the closest-hit walk (prim_count >= 2): tests both children, the leaf
+// ones at once, and moves `node` to the nearer hit child, or pops the stack.  The walk starts
+// at node 0 with an empty stack; the visit order depends on the ray alone.
+template <bool Count>
+RP_DEV int closest_visit(const DeviceScene &s, const WalkRay &r, float tmax, Hit &h, u32 &node, int &sp, u32 *stack,
+                         int stride, u32 &nodes_visited, u32 &tris_tested) {
+    const BNode n = s.nodes[node];
+    if (Count)
+        ++nodes_visited;
+    const float scale = s.slab_scale;
+    float tl, tr;
+    bool hl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, r.o, r.inv, h.t, scale, tl);
+    bool hr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, r.o, r.inv, h.t, scale, tr);
+    const u32 l = n.d.x, rc = n.d.y;
+    if (hl && (l & kLeaf)) {
+        closest_leaf<Count>(s, r, tmax, h, l & ~kLeaf, tris_tested);
+        hl = false;
+    }
+    if (hr && (rc & kLeaf)) {
+        closest_leaf<Count>(s, r, tmax, h, rc & ~kLeaf, tris_tested);
+        hr = false;
+    }
+    u32 next = kNone;
+    if (hl && hr) {
+        const bool right_first = tr < tl;
+        if (sp >= kStackDepth)
+            return kWalkFailed;
+        stack[sp * stride] = right_first ? l : rc;
+        ++sp;
+        next = right_first ? rc : l;
+    } else if (hl)
+        next = l;
+    else if (hr)
+        next = rc;
+    if (next == kNone) {
+        if (sp == 0)
+            return kWalkDone;
+        --sp;
+        next = stack[sp * stride];
+    }
+    node = next;
+    return kWalkMore;
+}
+
 // Closest hit: minimises (t, primitive id) so the result is independent of visit order.
-// `stack` is this thread's slice of a shared-memory stack with stride `stride`.
+// `stack` is this thread's slice of a shared-memory stack with stride `stride`.  A walk makes
+// at most prim_count visits (a binary tree over prim_count leaves has prim_count - 1 internal
+// nodes); a deeper stack than kStackDepth or more visits report a failed query.
 template <bool Count>
 RP_DEV bool trace_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, u32 *stack, int stride,
                           u32 &nodes_visited, u32 &tris_tested) {
@@ -633,66 +705,77 @@ RP_DEV bool trace_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, 
     h.prim = kNone;
     if (s.prim_count == 0)
         return true;
-    const V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-    const float scale = s.slab_scale;
-    auto test_leaf = [&](u32 slot) {
-        const float4 a = __ldg(s.leaf_v + 3 * slot), b = __ldg(s.leaf_v + 3 * slot + 1), c = __ldg(s.leaf_v + 3 * slot + 2);
-        const u32 prim = __float_as_uint(a.w);
-        float t, b1, b2;
-        if (Count)
-            ++tris_tested;
-        if (intersect_triangle(o, d, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tmax, t, b1, b2) &&
-            (t < h.t || (t == h.t && prim < h.prim))) {
-            h.t = t;
-            h.b1 = b1;
-            h.b2 = b2;
-            h.prim = prim;
-        }
-    };
+    const WalkRay r = walk_ray(o, d);
     if (s.prim_count == 1) {
-        test_leaf(0);
+        closest_leaf<Count>(s, r, tmax, h, 0, tris_tested);
         return true;
     }
     int sp = 0;
     u32 node = 0;
-    // a binary tree over prim_count leaves has prim_count - 1 internal nodes
     for (u32 guard = 0; guard < s.prim_count; ++guard) {
-        const BNode n = s.nodes[node];
-        if (Count)
-            ++nodes_visited;
-        float tl, tr;
-        bool hl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, o, inv, h.t, scale, tl);
-        bool hr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, o, inv, h.t, scale, tr);
-        const u32 l = n.d.x, r = n.d.y;
-        if (hl && (l & kLeaf)) {
-            test_leaf(l & ~kLeaf);
-            hl = false;
-        }
-        if (hr && (r & kLeaf)) {
-            test_leaf(r & ~kLeaf);
-            hr = false;
-        }
-        u32 next = kNone;
-        if (hl && hr) {
-            const bool right_first = tr < tl;
-            if (sp >= kStackDepth)
-                return false;
-            stack[sp * stride] = right_first ? l : r;
-            ++sp;
-            next = right_first ? r : l;
-        } else if (hl)
-            next = l;
-        else if (hr)
-            next = r;
-        if (next == kNone) {
-            if (sp == 0)
-                return true;
-            --sp;
-            next = stack[sp * stride];
-        }
-        node = next;
+        const int step = closest_visit<Count>(s, r, tmax, h, node, sp, stack, stride, nodes_visited, tris_tested);
+        if (step != kWalkMore)
+            return step == kWalkDone;
     }
     return false;
+}
+
+// Any-hit triangle test of leaf slot `slot` in (0, tmax).
+template <bool Count>
+RP_DEV bool any_leaf(const DeviceScene &s, const WalkRay &r, float tmax, u32 slot, u32 &tris_tested) {
+    const float4 a = __ldg(s.leaf_v + 3 * slot), b = __ldg(s.leaf_v + 3 * slot + 1), c = __ldg(s.leaf_v + 3 * slot + 2);
+    float t, b1, b2;
+    if (Count)
+        ++tris_tested;
+    return intersect_triangle(r.o, r.d, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tmax, t, b1, b2);
+}
+
+// One node visit of the any-hit walk (prim_count >= 2); kWalkDone with `occluded` set on the
+// first hit, or with it clear once the stack is empty.
+template <bool Count>
+RP_DEV int any_visit(const DeviceScene &s, const WalkRay &r, float tmax, bool &occluded, u32 &node, int &sp,
+                     u32 *stack, int stride, u32 &nodes_visited, u32 &tris_tested) {
+    const BNode n = s.nodes[node];
+    if (Count)
+        ++nodes_visited;
+    const float scale = s.slab_scale;
+    float tl, tr;
+    bool hl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, r.o, r.inv, tmax, scale, tl);
+    bool hr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, r.o, r.inv, tmax, scale, tr);
+    const u32 l = n.d.x, rc = n.d.y;
+    if (hl && (l & kLeaf)) {
+        if (any_leaf<Count>(s, r, tmax, l & ~kLeaf, tris_tested)) {
+            occluded = true;
+            return kWalkDone;
+        }
+        hl = false;
+    }
+    if (hr && (rc & kLeaf)) {
+        if (any_leaf<Count>(s, r, tmax, rc & ~kLeaf, tris_tested)) {
+            occluded = true;
+            return kWalkDone;
+        }
+        hr = false;
+    }
+    u32 next = kNone;
+    if (hl && hr) {
+        if (sp >= kStackDepth)
+            return kWalkFailed;
+        stack[sp * stride] = rc;
+        ++sp;
+        next = l;
+    } else if (hl)
+        next = l;
+    else if (hr)
+        next = rc;
+    if (next == kNone) {
+        if (sp == 0)
+            return kWalkDone;
+        --sp;
+        next = stack[sp * stride];
+    }
+    node = next;
+    return kWalkMore;
 }
 
 // Any hit in (0, tmax): the shadow-ray occlusion query.
@@ -702,61 +785,17 @@ RP_DEV bool trace_any(const DeviceScene &s, V3 o, V3 d, float tmax, bool &occlud
     occluded = false;
     if (s.prim_count == 0)
         return true;
-    const V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-    const float scale = s.slab_scale;
-    auto hit_leaf = [&](u32 slot) -> bool {
-        const float4 a = __ldg(s.leaf_v + 3 * slot), b = __ldg(s.leaf_v + 3 * slot + 1), c = __ldg(s.leaf_v + 3 * slot + 2);
-        float t, b1, b2;
-        if (Count)
-            ++tris_tested;
-        return intersect_triangle(o, d, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tmax, t, b1, b2);
-    };
+    const WalkRay r = walk_ray(o, d);
     if (s.prim_count == 1) {
-        occluded = hit_leaf(0);
+        occluded = any_leaf<Count>(s, r, tmax, 0, tris_tested);
         return true;
     }
     int sp = 0;
     u32 node = 0;
     for (u32 guard = 0; guard < s.prim_count; ++guard) {
-        const BNode n = s.nodes[node];
-        if (Count)
-            ++nodes_visited;
-        float tl, tr;
-        bool hl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, o, inv, tmax, scale, tl);
-        bool hr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, o, inv, tmax, scale, tr);
-        const u32 l = n.d.x, r = n.d.y;
-        if (hl && (l & kLeaf)) {
-            if (hit_leaf(l & ~kLeaf)) {
-                occluded = true;
-                return true;
-            }
-            hl = false;
-        }
-        if (hr && (r & kLeaf)) {
-            if (hit_leaf(r & ~kLeaf)) {
-                occluded = true;
-                return true;
-            }
-            hr = false;
-        }
-        u32 next = kNone;
-        if (hl && hr) {
-            if (sp >= kStackDepth)
-                return false;
-            stack[sp * stride] = r;
-            ++sp;
-            next = l;
-        } else if (hl)
-            next = l;
-        else if (hr)
-            next = r;
-        if (next == kNone) {
-            if (sp == 0)
-                return true;
-            --sp;
-            next = stack[sp * stride];
-        }
-        node = next;
+        const int step = any_visit<Count>(s, r, tmax, occluded, node, sp, stack, stride, nodes_visited, tris_tested);
+        if (step != kWalkMore)
+            return step == kWalkDone;
     }
     return false;
 }
