@@ -568,51 +568,25 @@ RP_DEV bool intersect_triangle(V3 o, V3 d, V3 v0, V3 v1, V3 v2, float tmax, floa
     return t > 0 && t < tmax;
 }
 
-// Conservative slab test (Ize, JCGT 2(2), 2013), same operation order as the CPU LBVH.
+// Conservative slab test (Ize, JCGT 2(2), 2013), same operation order as the CPU LBVH.  The
+// three axes run without early exits and one comparison decides: t0 only grows and t1 only
+// shrinks, and neither takes a NaN (a NaN bound loses every comparison), so the answer and
+// the entry distance equal those of the per-axis early-exit form.
+RP_DEV void slab_axis(float l, float h, float o, float inv, float scale, float &t0, float &t1) {
+    const float tn = (l - o) * inv, tf = (h - o) * inv;
+    const bool swap = tn > tf;
+    const float near = swap ? tf : tn, far = (swap ? tn : tf) * scale;
+    t0 = near > t0 ? near : t0;
+    t1 = far < t1 ? far : t1;
+}
 RP_DEV bool slab(float lx, float ly, float lz, float hx, float hy, float hz, V3 o, V3 inv, float tmax, float scale,
                  float &tenter) {
     float t0 = 0, t1 = tmax;
-    {
-        float tn = (lx - o.x) * inv.x, tf = (hx - o.x) * inv.x;
-        if (tn > tf) {
-            const float q = tn;
-            tn = tf;
-            tf = q;
-        }
-        tf *= scale;
-        t0 = tn > t0 ? tn : t0;
-        t1 = tf < t1 ? tf : t1;
-        if (!(t0 <= t1))
-            return false;
-    }
-    {
-        float tn = (ly - o.y) * inv.y, tf = (hy - o.y) * inv.y;
-        if (tn > tf) {
-            const float q = tn;
-            tn = tf;
-            tf = q;
-        }
-        tf *= scale;
-        t0 = tn > t0 ? tn : t0;
-        t1 = tf < t1 ? tf : t1;
-        if (!(t0 <= t1))
-            return false;
-    }
-    {
-        float tn = (lz - o.z) * inv.z, tf = (hz - o.z) * inv.z;
-        if (tn > tf) {
-            const float q = tn;
-            tn = tf;
-            tf = q;
-        }
-        tf *= scale;
-        t0 = tn > t0 ? tn : t0;
-        t1 = tf < t1 ? tf : t1;
-        if (!(t0 <= t1))
-            return false;
-    }
+    slab_axis(lx, hx, o.x, inv.x, scale, t0, t1);
+    slab_axis(ly, hy, o.y, inv.y, scale, t0, t1);
+    slab_axis(lz, hz, o.z, inv.z, scale, t0, t1);
     tenter = t0;
-    return true;
+    return t0 <= t1;
 }
 
 struct Hit {
