@@ -527,20 +527,40 @@ RP_DEV bool positional_intensity(const DPositional &L, V3 wi, float &intensity) 
 }
 
 // ------------------------------------------------------------------ traversal
-// Watertight ray/triangle intersection (Woop, Benthin and Wald, JCGT 2(1), 2013).
-RP_DEV bool intersect_triangle(V3 o, V3 d, V3 v0, V3 v1, V3 v2, float tmax, float &t, float &b1, float &b2) {
+// Ray of a traversal walk: origin, direction, the slab reciprocals, and the per-ray part of
+// the watertight triangle test (the dominant axis kz, the other two axes kx, ky, swapped when
+// the direction along kz is negative to keep the winding, and the shear constants).
+struct WalkRay {
+    V3 o, d, inv;
+    int kx, ky, kz;
+    float sx, sy, sz;
+};
+RP_DEV WalkRay walk_ray(V3 o, V3 d) {
+    WalkRay r;
+    r.o = o;
+    r.d = d;
+    r.inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
     const V3 ad = vabs(d);
-    const int kz = ad.x > ad.y ? (ad.x > ad.z ? 0 : 2) : (ad.y > ad.z ? 1 : 2);
-    int kx = kz == 2 ? 0 : kz + 1;
-    int ky = kx == 2 ? 0 : kx + 1;
-    if (comp(d, kz) < 0) {
-        const int t0 = kx;
-        kx = ky;
-        ky = t0;
+    r.kz = ad.x > ad.y ? (ad.x > ad.z ? 0 : 2) : (ad.y > ad.z ? 1 : 2);
+    r.kx = r.kz == 2 ? 0 : r.kz + 1;
+    r.ky = r.kx == 2 ? 0 : r.kx + 1;
+    if (comp(d, r.kz) < 0) {
+        const int t0 = r.kx;
+        r.kx = r.ky;
+        r.ky = t0;
     }
-    const float dz = comp(d, kz);
-    const float sx = comp(d, kx) / dz, sy = comp(d, ky) / dz, sz = 1.0f / dz;
-    const V3 A = v0 - o, B = v1 - o, C = v2 - o;
+    const float dz = comp(d, r.kz);
+    r.sx = comp(d, r.kx) / dz;
+    r.sy = comp(d, r.ky) / dz;
+    r.sz = 1.0f / dz;
+    return r;
+}
+
+// Watertight ray/triangle intersection (Woop, Benthin and Wald, JCGT 2(1), 2013).
+RP_DEV bool intersect_triangle(const WalkRay &r, V3 v0, V3 v1, V3 v2, float tmax, float &t, float &b1, float &b2) {
+    const int kx = r.kx, ky = r.ky, kz = r.kz;
+    const float sx = r.sx, sy = r.sy, sz = r.sz;
+    const V3 A = v0 - r.o, B = v1 - r.o, C = v2 - r.o;
     const float ax = fmaf(-sx, comp(A, kz), comp(A, kx)), ay = fmaf(-sy, comp(A, kz), comp(A, ky));
     const float bx = fmaf(-sx, comp(B, kz), comp(B, kx)), by = fmaf(-sy, comp(B, kz), comp(B, ky));
     const float cx = fmaf(-sx, comp(C, kz), comp(C, kx)), cy = fmaf(-sy, comp(C, kz), comp(C, ky));
@@ -600,12 +620,6 @@ constexpr int kStackDepth = 64;
 // Outcome of one node visit of a walk.
 enum WalkStep : int { kWalkMore = 0, kWalkDone = 1, kWalkFailed = 2 };
 
-// Ray of a walk: origin, direction and the slab reciprocals.
-struct WalkRay {
-    V3 o, d, inv;
-};
-RP_DEV WalkRay walk_ray(V3 o, V3 d) { return {o, d, v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z)}; }
-
 // Closest-hit triangle test of leaf slot `slot`: keeps the minimum (t, primitive id).
 template <bool Count>
 RP_DEV void closest_leaf(const DeviceScene &s, const WalkRay &r, float tmax, Hit &h, u32 slot, u32 &tris_tested) {
@@ -614,7 +628,7 @@ RP_DEV void closest_leaf(const DeviceScene &s, const WalkRay &r, float tmax, Hit
     float t, b1, b2;
     if (Count)
         ++tris_tested;
-    if (intersect_triangle(r.o, r.d, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tmax, t, b1, b2) &&
+    if (intersect_triangle(r, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tmax, t, b1, b2) &&
         (t < h.t || (t == h.t && prim < h.prim))) {
         h.t = t;
         h.b1 = b1;
@@ -701,7 +715,7 @@ RP_DEV bool any_leaf(const DeviceScene &s, const WalkRay &r, float tmax, u32 slo
     float t, b1, b2;
     if (Count)
         ++tris_tested;
-    return intersect_triangle(r.o, r.d, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tmax, t, b1, b2);
+    return intersect_triangle(r, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tmax, t, b1, b2);
 }
 
 // One node visit of the any-hit walk (prim_count >= 2); kWalkDone with `occluded` set on the
