@@ -29,6 +29,7 @@ struct BuildTmp {
     float4 *node_lo, *node_hi; // internal node bounds
     u32 *flags;
     u32 *error;                // kBuildVertexRange | kBuildTree bits
+    u32 *levels;               // most internal nodes on a root-to-leaf path
     u32 *refs;                 // references to internal nodes [0, n-1) and leaves [n-1, 2n-1)
     u32 vertex_count;
 };
@@ -406,6 +407,8 @@ __global__ void k_tree_verify(u32 n, BuildTmp t) {
         }
         if (node != 0)
             atomicOr(t.error, kBuildTree);
+        else
+            atomicMax(t.levels, u32(level + 1));
     }
 }
 

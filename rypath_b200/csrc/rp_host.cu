@@ -436,6 +436,7 @@ struct rp_scene {
     u64 *keys = nullptr;
     u32 *order = nullptr;
     BuildTmp tmp{};
+    u32 tree_levels = 0;     // most internal nodes on a root-to-leaf path of the LBVH
     float4 *world = nullptr; // world-space triangle vertices in original order
     BNode *nodes = nullptr;  // traversal layout (ds.nodes, ds.leaf_v)
     float4 *leaf_v = nullptr;
@@ -663,6 +664,22 @@ std::string validate_request(const rp_scene *s, const rp_request &r) {
     return {};
 }
 
+// The closest-hit and shadow kernels with the traversal stack the built tree needs.
+template <bool Count, int Block>
+void launch_trace(const rp_scene *s, const PathPool &pool, int in, unsigned grid, cudaStream_t st) {
+    if (s->tree_levels <= u32(kShortStack))
+        k_trace<Count, Block, kShortStack><<<grid, Block, 0, st>>>(s->ds, pool, in);
+    else
+        k_trace<Count, Block, kStackDepth><<<grid, Block, 0, st>>>(s->ds, pool, in);
+}
+template <bool Count, int Block, bool Adjoint>
+void launch_shadow(const rp_scene *s, const PathPool &pool, unsigned grid, size_t smem, cudaStream_t st) {
+    if (s->tree_levels <= u32(kShortStack))
+        k_shadow<Count, Block, Adjoint, kShortStack><<<grid, Block, smem, st>>>(s->ds, pool);
+    else
+        k_shadow<Count, Block, Adjoint, kStackDepth><<<grid, Block, smem, st>>>(s->ds, pool);
+}
+
 // One wave: raygen, then max_depth + 1 events of trace -> shade -> shadow.
 void run_wave(rp_scene *s, const WaveParams &p, size_t adjoint_smem = 0) {
     s->ensure_pool(p.lanes);
@@ -678,16 +695,17 @@ void run_wave(rp_scene *s, const WaveParams &p, size_t adjoint_smem = 0) {
     for (u32 e = 0; e < events; ++e) {
         s->mark(0);
         RP_CHECK(cudaMemsetAsync(pool.counters + 4, 0, 4 * sizeof(u32), s->stream));
+        const unsigned trace_grid = grid_for(sms, p.lanes, kTraceBlock, 12);
         if (s->counting)
-            k_trace<true><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, 0, s->stream>>>(s->ds, pool, in);
+            launch_trace<true, kTraceBlock>(s, pool, in, trace_grid, s->stream);
         else
-            k_trace<false><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, 0, s->stream>>>(s->ds, pool, in);
+            launch_trace<false, kTraceBlock>(s, pool, in, trace_grid, s->stream);
         s->done();
         s->mark(2, 4);
         RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), s->stream));
         RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), s->stream));
         const size_t smem = adjoint_smem;
-        const unsigned shade_grid = grid_for(sms, p.lanes, 128, 16), trace_grid = grid_for(sms, p.lanes, kTraceBlock, 12);
+        const unsigned shade_grid = grid_for(sms, p.lanes, 128, 16);
         if (pool.hist) {
             k_shade<0, 128, true><<<shade_grid, 128, smem, s->stream>>>(s->ds, p, pool, in);
             k_shade<1, 128, true><<<shade_grid, 128, smem, s->stream>>>(s->ds, p, pool, in);
@@ -702,11 +720,11 @@ void run_wave(rp_scene *s, const WaveParams &p, size_t adjoint_smem = 0) {
         s->done();
         s->mark(1);
         if (pool.hist)
-            k_shadow<false, kTraceBlock, true><<<trace_grid, kTraceBlock, smem, s->stream>>>(s->ds, pool);
+            launch_shadow<false, kTraceBlock, true>(s, pool, trace_grid, smem, s->stream);
         else if (s->counting)
-            k_shadow<true><<<trace_grid, kTraceBlock, 0, s->stream>>>(s->ds, pool);
+            launch_shadow<true, kTraceBlock, false>(s, pool, trace_grid, 0, s->stream);
         else
-            k_shadow<false><<<trace_grid, kTraceBlock, 0, s->stream>>>(s->ds, pool);
+            launch_shadow<false, kTraceBlock, false>(s, pool, trace_grid, 0, s->stream);
         s->done();
         in ^= 1;
     }
@@ -779,6 +797,7 @@ void build_prepare(rp_scene *s, u32 vertex_count) {
     t.box_hi = dalloc<float4>(own, n, st);
     t.cbounds = dalloc<int>(own, 16, st);
     t.error = reinterpret_cast<u32 *>(t.cbounds + 12);
+    t.levels = t.error + 1;
     t.keys[0] = dalloc<u64>(own, n, st);
     t.keys[1] = dalloc<u64>(own, n, st);
     t.vals[0] = dalloc<u32>(own, n, st);
@@ -856,11 +875,12 @@ void build_finish(rp_scene *s, const int (&cb)[12]) {
     }
     k_pack<<<grid_for(s->sm_count, n, 256, 8), 256, 0, st>>>(n, s->order, s->world, t, s->nodes, s->leaf_v);
     RP_CHECK(cudaGetLastError());
-    u32 error = 0;
-    RP_CHECK(cudaMemcpyAsync(&error, t.error, sizeof(error), cudaMemcpyDeviceToHost, st));
+    u32 result[2] = {0, 0}; // error bits, tree levels
+    RP_CHECK(cudaMemcpyAsync(result, t.error, sizeof(result), cudaMemcpyDeviceToHost, st));
     RP_CHECK(cudaStreamSynchronize(st));
-    if (error & kBuildTree)
+    if (result[0] & kBuildTree)
         throw Invalid{"LBVH build produced an invalid tree"};
+    s->tree_levels = result[1];
 }
 
 } // namespace
@@ -1903,14 +1923,14 @@ void batch_wave_kernels(rp_scene *s, const WaveParams &p, const Batch &b, u32 wa
     int in = 0;
     for (u32 e = 0; e <= s->ds.max_depth; ++e) {
         RP_CHECK(cudaMemsetAsync(pool.counters + 4, 0, 4 * sizeof(u32), st));
-        k_trace<false, TB><<<trace_grid, TB, 0, st>>>(s->ds, pool, in);
+        launch_trace<false, TB>(s, pool, in, trace_grid, st);
         RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), st));
         RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), st));
         k_shade<0, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
         k_shade<1, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
         k_shade<2, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
         k_shade<3, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
-        k_shadow<false, TB><<<trace_grid, TB, 0, st>>>(s->ds, pool);
+        launch_shadow<false, TB, false>(s, pool, trace_grid, 0, st);
         in ^= 1;
     }
     k_film_views<<<grid_for(sms, wave_lanes, 128, 16), 128, 0, st>>>(pool, b, s->cie, double(s->ds.filter_weight), film);
@@ -2433,14 +2453,14 @@ rp_status rp_cuda_sample_device_static(rp_scene *s, const rp_request *request, r
         int in = 0;
         for (u32 ev = 0; ev < s->ds.max_depth + 1; ++ev) {
             RP_CHECK(cudaMemsetAsync(pool.counters + 4, 0, 4 * sizeof(u32), st));
-            k_trace<false><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, 0, st>>>(s->ds, pool, in);
+            launch_trace<false, kTraceBlock>(s, pool, in, grid_for(sms, p.lanes, kTraceBlock, 12), st);
             RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), st));
             RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), st));
             k_shade<0><<<grid_for(sms, p.lanes, 128, 16), 128, 0, st>>>(s->ds, p, pool, in);
             k_shade<1><<<grid_for(sms, p.lanes, 128, 16), 128, 0, st>>>(s->ds, p, pool, in);
             k_shade<2><<<grid_for(sms, p.lanes, 128, 16), 128, 0, st>>>(s->ds, p, pool, in);
             k_shade<3><<<grid_for(sms, p.lanes, 128, 16), 128, 0, st>>>(s->ds, p, pool, in);
-            k_shadow<false><<<grid_for(sms, p.lanes, kTraceBlock, 12), kTraceBlock, 0, st>>>(s->ds, pool);
+            launch_shadow<false, kTraceBlock, false>(s, pool, grid_for(sms, p.lanes, kTraceBlock, 12), 0, st);
             in ^= 1;
         }
         k_results<<<grid_for(sms, p.lanes, 256, 16), 256, 0, st>>>(pool, p.lanes, s->ds.filter_weight,

@@ -61,9 +61,12 @@ __global__ void k_raygen(const __grid_constant__ DeviceScene s, const __grid_con
 // Closest-hit queries for the active queue; each path is then appended to the bin of the
 // BSDF family it hit (0 diffuse, 1 conductor, 2 dielectric, 3 miss or failed query), so the
 // shade stage runs one specialised kernel per family ("material-sorted shading").
-template <bool Count, int Block = kTraceBlock>
-__global__ void __launch_bounds__(Block) k_trace(const __grid_constant__ DeviceScene s, PathPool pool, int in) {
-    __shared__ u32 stack[kStackDepth * Block];
+// Stack: traversal stack entries per thread (kShortStack for shallow trees, whose walks then
+// fit eight 128-thread blocks per SM).
+template <bool Count, int Block = kTraceBlock, int Stack = kStackDepth>
+__global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1)
+    k_trace(const __grid_constant__ DeviceScene s, PathPool pool, int in) {
+    __shared__ u32 stack[Stack * Block];
     const u32 count = pool.counters[in];
     const u32 *queue = pool.queue[in];
     u32 nodes = 0, tris = 0, rays = 0;
@@ -78,8 +81,9 @@ __global__ void __launch_bounds__(Block) k_trace(const __grid_constant__ DeviceS
             if (!(pool.ident[path].w & F_COMPLETE)) {
                 const float4 o = pool.ray_o[path], d = pool.ray_d[path];
                 Hit h;
-                const bool ok = trace_closest<Count>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), __int_as_float(0x7f800000),
-                                                     h, stack + threadIdx.x, Block, nodes, tris);
+                const bool ok = walk_closest<Count, Stack>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z),
+                                                           __int_as_float(0x7f800000), h, stack + threadIdx.x, Block,
+                                                           nodes, tris);
                 ++rays;
                 pool.hit[path] = make_float4(h.t, h.b1, h.b2, __uint_as_float(ok ? h.prim : 0xfffffffeu));
                 family = (!ok || h.prim == kNone) ? 3u : u32(__ldg(s.tri_family + h.prim));
@@ -533,9 +537,10 @@ __global__ void __launch_bounds__(Block, 384 / Block) k_shade(const __grid_const
 }
 
 // Visibility of the light samples (visible(), shaders/packet_transport.h:377-446, opaque surfaces)
-template <bool Count, int Block = kTraceBlock, bool Adjoint = false>
-__global__ void __launch_bounds__(Block) k_shadow(const __grid_constant__ DeviceScene s, PathPool pool) {
-    __shared__ u32 stack[kStackDepth * Block];
+template <bool Count, int Block = kTraceBlock, bool Adjoint = false, int Stack = kStackDepth>
+__global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1)
+    k_shadow(const __grid_constant__ DeviceScene s, PathPool pool) {
+    __shared__ u32 stack[Stack * Block];
     extern __shared__ float sgrad[]; // adjoint only
     if (Adjoint)
         adjoint_begin(pool, sgrad);
@@ -545,8 +550,8 @@ __global__ void __launch_bounds__(Block) k_shadow(const __grid_constant__ Device
         const float4 o = pool.sh_o[i], d = pool.sh_d[i];
         const u32 path = __float_as_uint(d.w);
         bool occluded;
-        const bool ok = trace_any<Count>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), o.w, occluded, stack + threadIdx.x,
-                                         Block, nodes, tris);
+        const bool ok = walk_any<Count, Stack>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), o.w, occluded,
+                                               stack + threadIdx.x, Block, nodes, tris);
         ++rays;
         uint4 ident = pool.ident[path];
         if (!ok) {

@@ -614,8 +614,11 @@ struct Hit {
     u32 prim;
 };
 
-// Stack depth for traversal; deeper trees report an invalid hit.
-constexpr int kStackDepth = 64;
+// Stack depth for traversal; deeper trees report an invalid hit.  The wavefront walks use
+// kShortStack entries when every root-to-leaf path of the built tree has at most that many
+// internal nodes (a walk never holds more entries than that), freeing shared memory for more
+// resident warps.
+constexpr int kStackDepth = 64, kShortStack = 40;
 
 // Outcome of one node visit of a walk.
 enum WalkStep : int { kWalkMore = 0, kWalkDone = 1, kWalkFailed = 2 };
@@ -640,7 +643,7 @@ RP_DEV void closest_leaf(const DeviceScene &s, const WalkRay &r, float tmax, Hit
 // One node visit of the closest-hit walk (prim_count >= 2): tests both children, the leaf
 // ones at once, and moves `node` to the nearer hit child, or pops the stack.  The walk starts
 // at node 0 with an empty stack; the visit order depends on the ray alone.
-template <bool Count>
+template <bool Count, int Stack = kStackDepth>
 RP_DEV int closest_visit(const DeviceScene &s, const WalkRay &r, float tmax, Hit &h, u32 &node, int &sp, u32 *stack,
                          int stride, u32 &nodes_visited, u32 &tris_tested) {
     const BNode n = s.nodes[node];
@@ -662,7 +665,7 @@ RP_DEV int closest_visit(const DeviceScene &s, const WalkRay &r, float tmax, Hit
     u32 next = kNone;
     if (hl && hr) {
         const bool right_first = tr < tl;
-        if (sp >= kStackDepth)
+        if (sp >= Stack)
             return kWalkFailed;
         stack[sp * stride] = right_first ? l : rc;
         ++sp;
@@ -685,9 +688,9 @@ RP_DEV int closest_visit(const DeviceScene &s, const WalkRay &r, float tmax, Hit
 // `stack` is this thread's slice of a shared-memory stack with stride `stride`.  A walk makes
 // at most prim_count visits (a binary tree over prim_count leaves has prim_count - 1 internal
 // nodes); a deeper stack than kStackDepth or more visits report a failed query.
-template <bool Count>
-RP_DEV bool trace_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, u32 *stack, int stride,
-                          u32 &nodes_visited, u32 &tris_tested) {
+template <bool Count, int Stack = kStackDepth>
+RP_DEV bool walk_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, u32 *stack, int stride,
+                         u32 &nodes_visited, u32 &tris_tested) {
     h.t = tmax;
     h.b1 = h.b2 = 0;
     h.prim = kNone;
@@ -701,11 +704,17 @@ RP_DEV bool trace_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, 
     int sp = 0;
     u32 node = 0;
     for (u32 guard = 0; guard < s.prim_count; ++guard) {
-        const int step = closest_visit<Count>(s, r, tmax, h, node, sp, stack, stride, nodes_visited, tris_tested);
+        const int step =
+            closest_visit<Count, Stack>(s, r, tmax, h, node, sp, stack, stride, nodes_visited, tris_tested);
         if (step != kWalkMore)
             return step == kWalkDone;
     }
     return false;
+}
+template <bool Count>
+RP_DEV bool trace_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, u32 *stack, int stride,
+                          u32 &nodes_visited, u32 &tris_tested) {
+    return walk_closest<Count>(s, o, d, tmax, h, stack, stride, nodes_visited, tris_tested);
 }
 
 // Any-hit triangle test of leaf slot `slot` in (0, tmax).
@@ -720,7 +729,7 @@ RP_DEV bool any_leaf(const DeviceScene &s, const WalkRay &r, float tmax, u32 slo
 
 // One node visit of the any-hit walk (prim_count >= 2); kWalkDone with `occluded` set on the
 // first hit, or with it clear once the stack is empty.
-template <bool Count>
+template <bool Count, int Stack = kStackDepth>
 RP_DEV int any_visit(const DeviceScene &s, const WalkRay &r, float tmax, bool &occluded, u32 &node, int &sp,
                      u32 *stack, int stride, u32 &nodes_visited, u32 &tris_tested) {
     const BNode n = s.nodes[node];
@@ -747,7 +756,7 @@ RP_DEV int any_visit(const DeviceScene &s, const WalkRay &r, float tmax, bool &o
     }
     u32 next = kNone;
     if (hl && hr) {
-        if (sp >= kStackDepth)
+        if (sp >= Stack)
             return kWalkFailed;
         stack[sp * stride] = rc;
         ++sp;
@@ -767,9 +776,9 @@ RP_DEV int any_visit(const DeviceScene &s, const WalkRay &r, float tmax, bool &o
 }
 
 // Any hit in (0, tmax): the shadow-ray occlusion query.
-template <bool Count>
-RP_DEV bool trace_any(const DeviceScene &s, V3 o, V3 d, float tmax, bool &occluded, u32 *stack, int stride,
-                      u32 &nodes_visited, u32 &tris_tested) {
+template <bool Count, int Stack = kStackDepth>
+RP_DEV bool walk_any(const DeviceScene &s, V3 o, V3 d, float tmax, bool &occluded, u32 *stack, int stride,
+                     u32 &nodes_visited, u32 &tris_tested) {
     occluded = false;
     if (s.prim_count == 0)
         return true;
@@ -781,11 +790,17 @@ RP_DEV bool trace_any(const DeviceScene &s, V3 o, V3 d, float tmax, bool &occlud
     int sp = 0;
     u32 node = 0;
     for (u32 guard = 0; guard < s.prim_count; ++guard) {
-        const int step = any_visit<Count>(s, r, tmax, occluded, node, sp, stack, stride, nodes_visited, tris_tested);
+        const int step =
+            any_visit<Count, Stack>(s, r, tmax, occluded, node, sp, stack, stride, nodes_visited, tris_tested);
         if (step != kWalkMore)
             return step == kWalkDone;
     }
     return false;
+}
+template <bool Count>
+RP_DEV bool trace_any(const DeviceScene &s, V3 o, V3 d, float tmax, bool &occluded, u32 *stack, int stride,
+                      u32 &nodes_visited, u32 &tris_tested) {
+    return walk_any<Count>(s, o, d, tmax, occluded, stack, stride, nodes_visited, tris_tested);
 }
 
 } // namespace rp
