@@ -159,6 +159,55 @@ RP_DEV u32 sobol_word(const SobolTables &t, u64 index, u32 dimension, u32 mode, 
         return value;
     return scramble_word(value, mode, sobol_dimension_hash(dimension, seed));
 }
+// Four consecutive dimensions [dimension, dimension + 4) of one Sobol index, each equal to
+// sobol_word of its dimension.  The four generator products share the walk over the index
+// bits, and the four Owen bit loops run in lockstep: each loop is a chain of dependent 64-bit
+// hashes, so four independent chains keep the pipelines busy where one would stall on each
+// hash.
+RP_DEV uint4 sobol_words4(const SobolTables &t, u64 index, u32 dimension, u32 mode, u32 seed) {
+    const u32 *col = t.directions + dimension * kSobolMatrix;
+    u32 v[4] = {0, 0, 0, 0};
+    u32 lo = u32(index), hi = u32(index >> 32);
+    while (lo) {
+        const int b = __ffs(lo) - 1;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            v[k] ^= __ldg(col + k * kSobolMatrix + b);
+        lo &= lo - 1;
+    }
+    while (hi) {
+        const int b = __ffs(hi) - 1;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            v[k] ^= __ldg(col + k * kSobolMatrix + 32 + b);
+        hi &= hi - 1;
+    }
+    if (mode == 0)
+        return make_uint4(v[0], v[1], v[2], v[3]);
+    u32 h[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        h[k] = sobol_dimension_hash(dimension + k, seed);
+    if (mode != 3) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            v[k] = scramble_word(v[k], mode, h[k]);
+        return make_uint4(v[0], v[1], v[2], v[3]);
+    }
+    // Owen (the mode-3 loop of scramble_word), four words at once
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        v[k] ^= (h[k] & 1) << 31;
+#pragma unroll 1
+    for (u32 bit = 1; bit < 32; ++bit) {
+        const u32 mask = ~u32(0) << (32 - bit), flip = u32(1) << (31 - bit);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (u32(mix_bits((v[k] & mask) ^ h[k])) & (u32(1) << bit))
+                v[k] ^= flip;
+    }
+    return make_uint4(v[0], v[1], v[2], v[3]);
+}
 // src/sobol_shared.h:143-154
 RP_DEV float sobol_uniform(u32 v) {
     const float unit = float(v) * 0x1p-32f;

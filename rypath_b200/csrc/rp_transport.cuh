@@ -99,11 +99,7 @@ __device__ __noinline__ uint4 draw_words(const DeviceScene &s, const WaveParams 
         return make_uint4(zdraw(s, p, index, d, 0, true), zdraw(s, p, index, d, 1, true),
                           zdraw(s, p, index, d + 2, 0, even), zdraw(s, p, index, even ? d + 2 : d + 3, even ? 1 : 0, even));
     }
-    u32 w[4];
-#pragma unroll 1
-    for (u32 k = 0; k < 4; ++k)
-        w[k] = sobol_word(s.sobol, index, 4 * block + k, p.randomization, p.seed_low);
-    return make_uint4(w[0], w[1], w[2], w[3]);
+    return sobol_words4(s.sobol, index, 4 * block, p.randomization, p.seed_low);
 }
 
 struct BeginSample {
