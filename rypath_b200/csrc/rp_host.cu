@@ -59,6 +59,20 @@ struct LightInput {
     float cos_outer = -1, cos_emission = 0;
     bool two_sided = true, infinite = false;
 };
+
+// The per-node terms of light_importance in the device's float operations (host compiled
+// without contraction): center, squared half-diagonal, its square root, sine of the cone.
+void light_node_terms(DLightBounds &node) {
+    float d[3];
+    for (int a = 0; a < 3; ++a) {
+        node.center[a] = (node.low[a] + node.high[a]) * .5f;
+        d[a] = node.high[a] - node.low[a];
+    }
+    node.r2 = (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) * .25f;
+    node.radius = std::sqrt(node.r2);
+    node.sin_outer = std::sqrt(std::max(0.f, 1 - node.cos_outer * node.cos_outer));
+}
+
 struct LightTables {
     std::vector<DLightAlias> alias;
     std::vector<DLightRecord> records;
@@ -227,6 +241,7 @@ bool build_light_tables(const std::vector<LightInput> &in, LightTables &out, std
         node.cos_outer = bounds.cos_outer;
         node.cos_emission = bounds.cos_emission;
         node.flags = bounds.two_sided ? 1 : 0;
+        light_node_terms(node);
         if (end - begin == 1) {
             node.light = finite[begin];
             out.records[finite[begin]].leaf = index;
@@ -958,7 +973,8 @@ int rp_cuda_build_light_tables(const double *rows, uint32_t count, uint32_t *ali
         return -1;
     memcpy(alias, t.alias.data(), t.alias.size() * 16);
     memcpy(records, t.records.data(), t.records.size() * 16);
-    memcpy(nodes, t.nodes.data(), t.nodes.size() * 64);
+    for (size_t i = 0; i < t.nodes.size(); ++i) // the 16-word LightBounds head of each node
+        memcpy(nodes + 16 * i, &t.nodes[i], 64);
     memcpy(infinite, t.infinite.data(), t.infinite.size() * 4);
     *infinite_count = u32(t.infinite.size());
     return int(t.nodes.size());

@@ -35,7 +35,13 @@ struct DLightBounds {
     float low[3], high[3], direction[3];
     float power, cos_outer, cos_emission;
     u32 child, parent, light, flags;
+    // per-node terms of light_importance, computed on the host with the same float operations
+    float center[3]; // (low + high) * 0.5
+    float r2;        // |high - low|^2 / 4
+    float radius;    // sqrt(r2)
+    float sin_outer; // sqrt(max(0, 1 - cos_outer^2))
 };
+static_assert(offsetof(DLightBounds, center) == 64, "the first 16 words are LightBounds");
 struct DLightAlias {
     float threshold, pmf;
     u32 alias, padding;
@@ -190,19 +196,26 @@ __device__ __noinline__ bool triangle_surface_point(const DeviceScene &s, u32 in
 
 // ------------------------------------------------------------------ light selection (shaders/light_sampling.h)
 // :19-42
+// Point-light nodes (r2 == 0) take the bound angle's closed form: cos = 1 (or -1 at the light,
+// 0 for a NaN distance, as 1 - 0 / d2 gives), sin = 0 (1 when cos is 0).
 RP_DEV float light_importance(const DLightBounds &b, V3 position, V3 normal) {
-    const V3 lo = v3(b.low[0], b.low[1], b.low[2]), hi = v3(b.high[0], b.high[1], b.high[2]);
-    const V3 center = (lo + hi) * .5f;
+    const V3 center = v3(b.center[0], b.center[1], b.center[2]);
     const V3 delta = position - center;
-    const float r2 = dot(hi - lo, hi - lo) * .25f, d2 = dot(delta, delta);
-    const float radius = sqrtf(r2), distance = sqrtf(d2);
-    const float cb = d2 <= r2 ? -1.f : sqrtf(fmaxf(0.f, 1 - r2 / d2));
-    const float sb = sqrtf(fmaxf(0.f, 1 - cb * cb));
+    const float r2 = b.r2, d2 = dot(delta, delta);
+    const float radius = b.radius, distance = sqrtf(d2);
+    float cb, sb;
+    if (r2 == 0) {
+        cb = d2 <= 0 ? -1.f : (d2 == d2 ? 1.f : 0.f);
+        sb = cb == 0 ? 1.f : 0.f;
+    } else {
+        cb = d2 <= r2 ? -1.f : sqrtf(fmaxf(0.f, 1 - r2 / d2));
+        sb = sqrtf(fmaxf(0.f, 1 - cb * cb));
+    }
     const V3 wi = distance > 0 ? delta / distance : v3(0, 0, 1);
     float cw = fminf(fmaxf(dot(v3(b.direction[0], b.direction[1], b.direction[2]), wi), -1.f), 1.f);
     if (b.flags & 1)
         cw = fabsf(cw);
-    const float sw = sqrtf(fmaxf(0.f, 1 - cw * cw)), co = b.cos_outer, so = sqrtf(fmaxf(0.f, 1 - co * co));
+    const float sw = sqrtf(fmaxf(0.f, 1 - cw * cw)), co = b.cos_outer, so = b.sin_outer;
     const float cx = cw > co ? 1.f : cw * co + sw * so, sx = cw > co ? 0.f : sw * co - cw * so;
     const float cp = cx > cb ? 1.f : cx * cb + sx * sb;
     if (cp <= b.cos_emission)
@@ -246,10 +259,11 @@ __device__ __noinline__ Selected light_sample(const DeviceScene &s, V3 position,
     u = fminf((u - infinite) / (1 - infinite), kOneMinusEps);
     float pmf = 1 - infinite;
     u32 i = 0;
+    float reached = 0; // importance of node i, once a parent has computed it
     for (u32 steps = 0; steps < nodes; ++steps) {
         const DLightBounds &node = s.light_nodes[i];
         if (node.light != kNone) {
-            if (light_importance(node, position, normal) <= 0)
+            if ((steps == 0 ? light_importance(node, position, normal) : reached) <= 0)
                 return {kNone, 0};
             return {node.light, pmf};
         }
@@ -262,10 +276,12 @@ __device__ __noinline__ Selected light_sample(const DeviceScene &s, V3 position,
             pmf *= q;
             u = fminf(u / q, kOneMinusEps);
             i++;
+            reached = a;
         } else {
             pmf *= 1 - q;
             u = fminf((u - q) / (1 - q), kOneMinusEps);
             i = node.child;
+            reached = b;
         }
     }
     return {kNone, 0};
