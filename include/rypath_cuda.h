@@ -60,10 +60,18 @@ enum { RP_RANDOMIZE_NONE = 0, RP_RANDOMIZE_PERMUTEDIGITS = 1, RP_RANDOMIZE_FASTO
 enum { RP_FILTER_BOX = 0, RP_FILTER_TRIANGLE = 1, RP_FILTER_GAUSSIAN = 2 };
 /* Scattering families (wire::Material::scattering, src/render_wire.h:121). */
 enum { RP_DIFFUSE = 0, RP_CONDUCTOR = 1, RP_DIELECTRIC = 2 };
-/* Null medium interface (ScatteringKind::null_interface, wire scattering 10,
- * shaders/scalar_transport.h:450-472): changes the medium, scatters nothing.  Scalar
- * transport only. */
+/* Null medium interface (ScatteringKind::null_interface, wire scattering 10): scatters
+ * nothing.  The scalar transport changes the ray's medium there
+ * (shaders/scalar_transport.h:450-472); the hero transport, in vacuum, passes through it
+ * (shaders/packet_pt_event_body.inc:130-145, 193-205), and so do shadow rays
+ * (shaders/packet_transport.h:377-446). */
 enum { RP_INTERFACE = 10 };
+/* Mix of two materials (ScatteringKind::mix, wire scattering 9): each hit resolves to
+ * second_material where the PBRT alpha hash of (point, -direction, material index) is below
+ * mix_amount, else first_material (shaders/packet_pt_event_body.inc:165-190,
+ * shaders/scalar_transport.h:566-587); nesting is acyclic, at most 64 levels, and reaches no
+ * null interface (src/render.cpp:1955-1995). */
+enum { RP_MIX = 9 };
 /* Reflectance sources (src/render_wire.h:41-48). */
 enum { RP_REFLECTANCE_KNOTS = 0, RP_REFLECTANCE_CONSTANT = 1, RP_REFLECTANCE_BLACKBODY = 4 };
 /* Positional light kinds (src/render_wire.h:200). */
@@ -87,6 +95,7 @@ typedef struct rp_instance {
     uint32_t emission;     /* index into emissions or RP_NONE */
     uint32_t normal_begin; /* index into normals or RP_NONE */
     uint32_t inside_medium, outside_medium; /* RP_NONE = vacuum */
+    uint32_t invisible_emitter; /* nonzero: rays pass through it (RenderScene::instance_invisible_emitters) */
 } rp_instance;
 
 /* The subset of wire::Material (src/render_wire.h:107-130) used by diffuse, conductor and
@@ -100,6 +109,8 @@ typedef struct rp_material {
     uint32_t optical_extensions; /* bit 0: extend eta endpoints, bit 1: extend k */
     float u_roughness, v_roughness;
     uint32_t remap_roughness;
+    uint32_t first_material, second_material; /* RP_MIX children (MaterialAuxiliary, src/render_wire.h:159) */
+    float mix_amount;                         /* RP_MIX constant amount (src/render_wire.h:160) */
 } rp_material;
 
 typedef struct rp_area_emission { /* wire::AreaEmission subset, src/render_wire.h:219 */

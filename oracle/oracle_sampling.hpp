@@ -11,7 +11,8 @@ namespace oracle {
 struct Params {
     u32 width, height, pixel_begin, pixel_count, sample_low, sample_high;
     u32 seed_low, seed_high, sampler, randomization, m, emergency_limit, max_depth;
-    u32 log_spp; // ZSobol: floor(log2(total samples))
+    u32 log_spp;        // ZSobol: floor(log2(total samples))
+    u32 boundary_limit; // pass-through crossings allowed between two vertices
 };
 
 struct Sample {
@@ -294,6 +295,7 @@ inline Params make_params(const Scene &s, const rp_request &r) {
     p.log_spp = r.sampler_kind == RP_SAMPLER_ZSOBOL && r.total_samples ? 63 - __builtin_clzll(r.total_samples) : 0;
     p.emergency_limit = r.emergency_limit ? r.emergency_limit : 1024;
     p.max_depth = s.max_depth;
+    p.boundary_limit = r.boundary_limit ? r.boundary_limit : 4096; // medium_boundary_limit, src/render.hpp:26
     return p;
 }
 

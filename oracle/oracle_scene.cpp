@@ -296,7 +296,8 @@ bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error) {
         const auto &m = d.materials[i];
         s.materials.push_back({m.scattering, m.kind, m.knot_begin, m.knot_count, m.scalar_value,
                                m.eta_begin, m.eta_count, m.k_begin, m.k_count, m.optical_extensions,
-                               m.u_roughness, m.v_roughness, m.remap_roughness});
+                               m.u_roughness, m.v_roughness, m.remap_roughness, m.first_material,
+                               m.second_material, m.mix_amount});
     }
     for (u32 i = 0; i < d.knot_count; ++i)
         s.knots.push_back({d.knots[i].wavelength, d.knots[i].value});
@@ -337,6 +338,7 @@ bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error) {
         in.emitter_begin = RP_NONE;
         in.inside_medium = q.inside_medium;
         in.outside_medium = q.outside_medium;
+        in.invisible = q.invisible_emitter;
         if (q.emission != RP_NONE) {
             in.emitter_begin = u32(s.emitters.size());
             for (u32 t = 0; t < q.triangle_count; ++t)
@@ -986,6 +988,76 @@ bool triangle_surface_point(const Scene &s, u32 instance, u32 local, float u, fl
                   gamma_bound(4.0f) * fabs3(shift);
     return finite3(point.position) && finite3(point.error) && finite3(point.geometric_normal) &&
            finite3(point.shading_normal);
+}
+
+// shaders/render.metal:1939-1977
+bool spawn_boundary(F3 o, F3 d, float t, const SurfacePoint &pt, F3 direction, F3 &origin) {
+    if (!(t >= 0) || !std::isfinite(t))
+        return false;
+    const F3 ng = pt.geometric_normal;
+    const F3 n = dot(ng, direction) < 0 ? -ng : ng;
+    const float facing = dot(n, direction);
+    if (!(facing > gamma_bound(5) * dot(fabs3(n), fabs3(direction))))
+        return false;
+    const F3 position = fma3(F3{t, t, t}, d, o);
+    const F3 ray_error = gamma_bound(2) * (fabs3(t * d) + fabs3(o));
+    const F3 error = (pt.error + fabs3(pt.position - position)) + ray_error;
+    const float norm_lower = dot(n, n) * (1 - gamma_bound(4));
+    const float height = dot(fabs3(n), error) * (1 + gamma_bound(8)) / norm_lower;
+    origin = round_out(fma3(F3{height, height, height}, n, position), n);
+    if (!(norm_lower > 0) || !std::isfinite(height) || !finite3(origin) ||
+        (origin.x == o.x && origin.y == o.y && origin.z == o.z))
+        return false;
+    const F3 departure = origin - pt.position;
+    const float separation = dot(n, departure);
+    const float rounding = gamma_bound(5) * dot(fabs3(n), fabs3(departure));
+    const float uncertainty = dot(fabs3(n), pt.error) * (1 + gamma_bound(4));
+    return std::isfinite(separation) && std::isfinite(rounding) && std::isfinite(uncertainty) &&
+           separation - rounding > uncertainty;
+}
+
+// shaders/alpha_hash.h:10-36 (PBRT MurmurHash64A over the binary32 words)
+float alpha_uniform(F3 origin, F3 direction, u32 t_bits) {
+    constexpr u64 m = 0xc6a4a7935bd1e995ull;
+    const u32 words[7] = {fbits(origin.x), fbits(origin.y), fbits(origin.z), fbits(direction.x), fbits(direction.y),
+                          fbits(direction.z), t_bits};
+    u64 h = 28ull * m;
+    for (u32 i = 0; i < 6; i += 2) {
+        u64 k = u64(words[i]) | (u64(words[i + 1]) << 32);
+        k *= m;
+        k ^= k >> 47;
+        k *= m;
+        h ^= k;
+        h *= m;
+    }
+    h ^= u64(words[6]);
+    h *= m;
+    h ^= h >> 47;
+    h *= m;
+    h ^= h >> 47;
+    return float(u32(h)) * 0x1p-32f;
+}
+// shaders/packet_pt_event_body.inc:165-190 and shaders/scalar_transport.h:566-587 (constant amounts)
+u32 resolve_mix(const Scene &s, F3 position, F3 toward_origin, u32 &material) {
+    for (u32 depth = 0; depth <= 64; ++depth) {
+        const Material &node = s.materials[material];
+        if (node.scattering != 9)
+            return RP_SAMPLE_SUCCESS;
+        const float amount = node.mix_amount;
+        if (depth == 64 || !std::isfinite(amount))
+            return RP_SAMPLE_INVALID_ARITHMETIC;
+        const float selector = alpha_uniform(position, toward_origin, material);
+        material = amount <= 0         ? node.first
+                   : amount >= 1       ? node.second
+                   : selector < amount ? node.second
+                                       : node.first;
+        if (material >= s.materials.size())
+            return RP_SAMPLE_INVALID_HIT;
+    }
+    return RP_SAMPLE_SUCCESS;
+}
+bool pass_through(const Scene &s, const Instance &in) {
+    return in.invisible != 0 || s.materials[in.material].scattering == RP_INTERFACE;
 }
 
 // ================================================================= light selection

@@ -52,6 +52,7 @@ struct Instance {
     u32 vertex_begin, triangle_begin, triangle_count, material, reverse, emission, normal_begin;
     u32 emitter_begin;
     u32 inside_medium = RP_NONE, outside_medium = RP_NONE;
+    u32 invisible = 0; // RenderScene::instance_invisible_emitters
 };
 // HomogeneousMedium (src/render.hpp:29-36)
 struct Medium {
@@ -64,6 +65,8 @@ struct Material {
     u32 eta_begin, eta_count, k_begin, k_count, optical_extensions;
     float u_roughness, v_roughness;
     u32 remap;
+    u32 first = RP_NONE, second = RP_NONE; // mix children (MaterialAuxiliary, src/render_wire.h:159-161)
+    float mix_amount = 0;
 };
 struct Positional {
     F3 position;
@@ -154,6 +157,19 @@ struct SurfacePoint {
 };
 bool triangle_surface_point(const Scene &s, u32 instance, u32 local, float u, float v,
                             bool native_hit, SurfacePoint &p);
+
+// ---------------------------------------------------------------- pass-through and mix surfaces
+// PBRT's alpha hash as a uniform (shaders/alpha_hash.h:10-36); t is the bit pattern of the
+// material index the event passes as a float.
+float alpha_uniform(F3 origin, F3 direction, u32 t_bits);
+// The material a hit on mix root `material` resolves to (shaders/packet_pt_event_body.inc:
+// 165-190); returns the sample status (0, RP_SAMPLE_INVALID_ARITHMETIC or _INVALID_HIT).
+u32 resolve_mix(const Scene &s, F3 position, F3 toward_origin, u32 &material);
+// A hero pass-through instance: an invisible emitter or a null-interface root material
+// (shaders/packet_pt_event_body.inc:130-145).
+bool pass_through(const Scene &s, const Instance &in);
+// shaders/render.metal:1939-1977: the origin past a pass-through surface hit at t
+bool spawn_boundary(F3 o, F3 d, float t, const SurfacePoint &pt, F3 direction, F3 &origin);
 
 // ---------------------------------------------------------------- light selection / geometry
 struct Selected {

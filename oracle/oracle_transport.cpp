@@ -22,6 +22,7 @@ struct Vertex {
     F3 wo;
     float u = 0, v = 0;
     u32 instance = RP_NONE, primitive = 0, light = RP_NONE;
+    u32 material = RP_NONE; // the resolved material of a surface vertex
     bool pair_valid = false, delta = false, connectible = false, delta_light = false;
     F3 sampled_wo_local, sampled_wi_local;
 };
@@ -208,14 +209,42 @@ static F4 hero_endpoint(const Ctx &c, Sample &smp, const Wavelengths &l, const V
     const float lp = light_pdf(c, previous, pt);
     return hero_weight(smp, prev_density, value, bsdf_pdf, f4(lp));
 }
-// shaders/packet_transport.h:377-446 (visible; opaque surfaces only)
-static bool visible(const Ctx &c, const Vertex &a, const Vertex &b) {
+// shaders/packet_transport.h:377-446 (visible): any surface occludes in an opaque scene; with
+// pass-through instances, nearest hits along the segment, restarting past each pass-through one
+static bool visible(const Ctx &c, Sample &smp, const Vertex &a, const Vertex &b) {
     const F3 direction = b.point.position - a.point.position;
     if (zero3(direction))
         return false;
     const F3 origin = offset(a, direction);
     const F3 target = offset(b, -direction);
-    return !trace_any(c.s, c.bvh, origin, target - origin, 0x1.fffffep-1f);
+    const Scene &s = c.s;
+    if (!std::any_of(s.instances.begin(), s.instances.end(), [&](const Instance &in) { return pass_through(s, in); }))
+        return !trace_any(s, c.bvh, origin, target - origin, 0x1.fffffep-1f);
+    F3 o = origin, d = target - origin;
+    for (u32 crossings = 0; crossings <= c.p.boundary_limit; ++crossings) {
+        const Hit h = trace_closest(s, c.bvh, o, d, 0x1.fffffep-1f);
+        if (h.prim == RP_NONE)
+            return true;
+        const u32 inst = s.tri_instance[h.prim];
+        const Instance &in = s.instances[inst];
+        if (in.material >= s.materials.size()) {
+            smp.status = RP_SAMPLE_INVALID_HIT;
+            return false;
+        }
+        if (!pass_through(s, in))
+            return false;
+        SurfacePoint pt;
+        F3 next;
+        if (!triangle_surface_point(s, inst, s.tri_local[h.prim], h.b1, h.b2, true, pt) ||
+            !spawn_boundary(o, d, h.t, pt, normalize3(d), next)) {
+            smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+            return false;
+        }
+        o = next;
+        d = target - next;
+    }
+    smp.status = RP_SAMPLE_BOUNDARY_EXHAUSTION;
+    return false;
 }
 // shaders/packet_transport.h:470-553 (sample_li): area emitters and positional lights
 static bool sample_li(const Ctx &c, const Vertex &ref, const Wavelengths &l, float u0, float u1, float u2,
@@ -315,7 +344,7 @@ static F4 hero_direct(const Ctx &c, Sample &smp, const Wavelengths &l, u64 index
         return f4(0);
     }
     const F4 value = beta * e.f * sampled.beta * std::fabs(dot(pt.point.shading_normal, direction));
-    if (!nonzero4(value) || !visible(c, pt, sampled))
+    if (!nonzero4(value) || !visible(c, smp, pt, sampled))
         return f4(0);
     if (sampled.delta_light)
         return value;
@@ -420,7 +449,30 @@ static void hero_step(const Ctx &c, LaneState &st) {
             smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
             break;
         }
-        const Material &material = s.materials[instance.material];
+        // shaders/packet_pt_event_body.inc:130-145: a pass-through surface makes no vertex; the
+        // next event continues the ray from past it
+        if (pass_through(s, instance)) {
+            if (st.crossings++ >= p.boundary_limit) {
+                smp.status = RP_SAMPLE_BOUNDARY_EXHAUSTION;
+                break;
+            }
+            F3 origin;
+            if (!spawn_boundary(ro, rd, hit.t, v.point, rd, origin)) {
+                smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+                break;
+            }
+            ro = origin;
+            terminated = false;
+            break;
+        }
+        // :165-190: mix materials resolve at the hit
+        u32 material_index = instance.material;
+        if (const u32 mix_status = resolve_mix(s, v.point.position, -rd, material_index)) {
+            smp.status = mix_status;
+            break;
+        }
+        v.material = material_index;
+        const Material &material = s.materials[material_index];
         F3 dpdu, dpdv;
         coordinate_system(v.point.shading_normal, dpdu, dpdv);
         if (!scattering_frame(v.point.shading_normal, dpdu, v.frame) ||
@@ -517,7 +569,7 @@ static void hero_step(const Ctx &c, LaneState &st) {
             if (smp.status == RP_SAMPLE_SUCCESS && nonzero4(endpoint))
                 adjoint_accumulate(s, *st.adj, l, endpoint);
             if (current.type == surface_vertex && smp.status == RP_SAMPLE_SUCCESS) {
-                const u32 m = s.instances[current.instance].material;
+                const u32 m = current.material;
                 if (s.materials[m].scattering == RP_DIFFUSE && (*st.adj->slot)[m] != RP_NONE &&
                     st.adj->history_count < 16)
                     st.adj->history[st.adj->history_count++] = m;

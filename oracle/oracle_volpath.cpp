@@ -161,31 +161,6 @@ F3 spawn_toward(F3 o, F3 d, float t, const SurfacePoint &pt, F3 direction) {
     const F3 ng = pt.geometric_normal;
     return spawn_origin(o, d, t, pt, dot(ng, direction) < 0.0f ? -ng : ng);
 }
-// :1939-1977
-bool spawn_boundary(F3 o, F3 d, float t, const SurfacePoint &pt, F3 direction, F3 &origin) {
-    if (!(t >= 0) || !std::isfinite(t))
-        return false;
-    const F3 ng = pt.geometric_normal;
-    const F3 n = dot(ng, direction) < 0 ? -ng : ng;
-    const float facing = dot(n, direction);
-    if (!(facing > gamma_bound(5) * dot(fabs3(n), fabs3(direction))))
-        return false;
-    const F3 position = fma3(F3{t, t, t}, d, o);
-    const F3 ray_error = gamma_bound(2) * (fabs3(t * d) + fabs3(o));
-    const F3 error = (pt.error + fabs3(pt.position - position)) + ray_error;
-    const float norm_lower = dot(n, n) * (1 - gamma_bound(4));
-    const float height = dot(fabs3(n), error) * (1 + gamma_bound(8)) / norm_lower;
-    origin = round_out(fma3(F3{height, height, height}, n, position), n);
-    if (!(norm_lower > 0) || !std::isfinite(height) || !finite3(origin) ||
-        (origin.x == o.x && origin.y == o.y && origin.z == o.z))
-        return false;
-    const F3 departure = origin - pt.position;
-    const float separation = dot(n, departure);
-    const float rounding = gamma_bound(5) * dot(fabs3(n), fabs3(departure));
-    const float uncertainty = dot(fabs3(n), pt.error) * (1 + gamma_bound(4));
-    return std::isfinite(separation) && std::isfinite(rounding) && std::isfinite(uncertainty) &&
-           separation - rounding > uncertainty;
-}
 // :2221-2232
 F3 shadow_segment_direction(F3 origin, F3 delta, const SurfacePoint &target, float signed_cosine) {
     const F3 n = signed_cosine > 0.0f ? target.geometric_normal : -target.geometric_normal;
@@ -612,17 +587,28 @@ bool scalar_event(const Ctx &c, Lane &l) {
     }
     if (bounce >= s.max_depth)
         return true;
+    // mix materials resolve at the hit's point (shaders/scalar_transport.h:541-587)
+    bool point_ready = emissive;
+    u32 material_index = instance.material;
+    if (material.scattering == 9) {
+        if (!emissive && !triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point))
+            return fail(RP_SAMPLE_INVALID_ARITHMETIC);
+        point_ready = true;
+        if (const u32 mix_status = resolve_mix(s, point.position, -l.d, material_index))
+            return fail(mix_status);
+    }
+    const Material &surface = s.materials[material_index];
     // reflectance, shaders/scalar_transport.h:580-625
     float rho = 0;
-    if (material.scattering != RP_DIFFUSE)
+    if (surface.scattering != RP_DIFFUSE)
         return fail(RP_SAMPLE_INVALID_HIT);
-    if (material.kind == RP_REFLECTANCE_KNOTS && material.knot_count >= 2 && material.knot_begin <= s.knots.size() &&
-        material.knot_count <= s.knots.size() - material.knot_begin) {
-        rho = pbrt_reflectance(s.knots.data() + material.knot_begin, material.knot_count, l.wavelength);
-    } else if (material.kind == RP_REFLECTANCE_CONSTANT) {
-        rho = material.scalar_value;
-    } else if (material.kind == RP_REFLECTANCE_BLACKBODY) {
-        rho = blackbody_reflectance(material.scalar_value, l.wavelength);
+    if (surface.kind == RP_REFLECTANCE_KNOTS && surface.knot_count >= 2 && surface.knot_begin <= s.knots.size() &&
+        surface.knot_count <= s.knots.size() - surface.knot_begin) {
+        rho = pbrt_reflectance(s.knots.data() + surface.knot_begin, surface.knot_count, l.wavelength);
+    } else if (surface.kind == RP_REFLECTANCE_CONSTANT) {
+        rho = surface.scalar_value;
+    } else if (surface.kind == RP_REFLECTANCE_BLACKBODY) {
+        rho = blackbody_reflectance(surface.scalar_value, l.wavelength);
     } else {
         return fail(RP_SAMPLE_INVALID_HIT);
     }
@@ -633,7 +619,7 @@ bool scalar_event(const Ctx &c, Lane &l) {
     const bool authored_normals = instance.normal_begin != RP_NONE;
     if (!authored_normals && bounce >= p.emergency_limit)
         return fail(RP_SAMPLE_EMERGENCY_DEPTH);
-    if (!emissive && !triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point))
+    if (!point_ready && !triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point))
         return fail(RP_SAMPLE_INVALID_ARITHMETIC);
     const float incident_cosine = dot(point.shading_normal, l.d);
     if (authored_normals && incident_cosine == 0.0f)

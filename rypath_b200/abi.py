@@ -21,7 +21,8 @@ SAMPLER_INDEPENDENT, SAMPLER_SOBOL, SAMPLER_HALTON, SAMPLER_ZSOBOL = 0, 1, 2, 3
 RANDOMIZE_NONE, RANDOMIZE_PERMUTEDIGITS, RANDOMIZE_FASTOWEN, RANDOMIZE_OWEN = range(4)
 FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = 0, 1, 2
 DIFFUSE, CONDUCTOR, DIELECTRIC = 0, 1, 2
-INTERFACE = 10  # null medium interface (scalar transport)
+INTERFACE = 10  # null interface: medium change (scalar transport), pass-through (hero transport)
+MIX = 9  # stochastic mix of two materials
 REFLECTANCE_KNOTS, REFLECTANCE_CONSTANT, REFLECTANCE_BLACKBODY = 0, 1, 4
 POINT_LIGHT, SPOT_LIGHT = 0, 1
 LIGHTS_BVH, LIGHTS_POWER, LIGHTS_UNIFORM = 0, 1, 2
@@ -40,14 +41,15 @@ class Instance(C.Structure):
     _fields_ = [("matrix", f32 * 12), ("vertex_begin", u32), ("triangle_begin", u32),
                 ("triangle_count", u32), ("material", u32), ("reverse_orientation", u32),
                 ("emission", u32), ("normal_begin", u32), ("inside_medium", u32),
-                ("outside_medium", u32)]
+                ("outside_medium", u32), ("invisible_emitter", u32)]
 
 
 class Material(C.Structure):
     _fields_ = [("scattering", u32), ("kind", u32), ("knot_begin", u32), ("knot_count", u32),
                 ("scalar_value", f32), ("eta_begin", u32), ("eta_count", u32), ("k_begin", u32),
                 ("k_count", u32), ("optical_extensions", u32), ("u_roughness", f32),
-                ("v_roughness", f32), ("remap_roughness", u32)]
+                ("v_roughness", f32), ("remap_roughness", u32), ("first_material", u32),
+                ("second_material", u32), ("mix_amount", f32)]
 
 
 class AreaEmission(C.Structure):
@@ -185,7 +187,7 @@ def film_dtype():
 
 
 EXPECTED_SIZES = {
-    "rp_instance": (Instance, 84), "rp_material": (Material, 52), "rp_knot": (Knot, 8),
+    "rp_instance": (Instance, 88), "rp_material": (Material, 64), "rp_knot": (Knot, 8),
     "rp_area_emission": (AreaEmission, 1888), "rp_positional_light": (PositionalLight, 1948),
     "rp_medium": (Medium, 5656), "rp_camera": (Camera, 48), "rp_request": (Request, 64),
     "rp_packet_result": (PacketResult, 80), "rp_scalar_result": (ScalarResult, 44),

@@ -38,7 +38,7 @@ constexpr u32 kBuildVertexRange = 1, kBuildTree = 2;
 constexpr int kMaxTreeLevels = 160;
 
 // Flattened triangle i -> (instance, triangle within the instance, BSDF family of its
-// material).  prim_begin: the first flattened triangle of each instance (an exclusive prefix
+// material, or kResolveFamily for pass-through and mix-root instances).  prim_begin: the first flattened triangle of each instance (an exclusive prefix
 // of the instances' triangle counts), so the instance of i is the last one beginning at or
 // before i.
 __global__ void k_flatten(const DInstance *instances, const u32 *prim_begin, u32 instance_count,
@@ -55,7 +55,8 @@ __global__ void k_flatten(const DInstance *instances, const u32 *prim_begin, u32
         }
         tri_instance[i] = lo;
         tri_local[i] = i - prim_begin[lo];
-        tri_family[i] = (unsigned char)materials[instances[lo].material].scattering;
+        const DInstance &in = instances[lo];
+        tri_family[i] = (unsigned char)(in.resolve ? kResolveFamily : materials[in.material].scattering);
     }
 }
 

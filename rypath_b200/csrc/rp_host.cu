@@ -60,6 +60,53 @@ struct LightInput {
     bool two_sided = true, infinite = false;
 };
 
+// Mix materials (src/render.cpp:302-315, :1955-1995): finite amounts, children in range, no
+// cycle, at most 64 nested levels, and no null interface as a child.  Empty when valid.
+std::string validate_mix(const rp_scene_desc *d) {
+    const u32 n = d->material_count;
+    std::vector<unsigned char> state(n, 0); // 0 unvisited, 1 on the walk, 2 done
+    std::vector<u32> depth(n, 0);
+    std::vector<std::pair<u32, bool>> stack;
+    for (u32 root = 0; root < n; ++root) {
+        if (state[root] == 2)
+            continue;
+        stack.emplace_back(root, false);
+        while (!stack.empty()) {
+            const auto [index, leaving] = stack.back();
+            stack.pop_back();
+            if (index >= n)
+                return "Mix material references an invalid child";
+            const rp_material &m = d->materials[index];
+            if (leaving) {
+                if (m.scattering == RP_MIX) {
+                    depth[index] = 1 + std::max(depth[m.first_material], depth[m.second_material]);
+                    if (depth[index] > 64)
+                        return "Mix material nesting exceeds 64 levels";
+                }
+                state[index] = 2;
+                continue;
+            }
+            if (state[index] == 2)
+                continue;
+            if (state[index] == 1)
+                return "Cyclic mix materials are unsupported";
+            state[index] = 1;
+            stack.emplace_back(index, true);
+            if (m.scattering == RP_MIX) {
+                if (!std::isfinite(m.mix_amount))
+                    return "Mix material requires a finite amount and child-owned surface detail";
+                if (m.first_material < n && m.second_material < n &&
+                    (d->materials[m.first_material].scattering == RP_INTERFACE ||
+                     d->materials[m.second_material].scattering == RP_INTERFACE))
+                    return "Mix materials cannot contain null boundaries";
+                stack.emplace_back(m.second_material, false);
+                stack.emplace_back(m.first_material, false);
+            }
+        }
+    }
+    return {};
+}
+
 // The per-node terms of light_importance in the device's float operations (host compiled
 // without contraction): center, squared half-diagonal, its square root, sine of the cone.
 void light_node_terms(DLightBounds &node) {
@@ -452,6 +499,7 @@ struct rp_scene {
     u32 *order = nullptr;
     BuildTmp tmp{};
     u32 tree_levels = 0;     // most internal nodes on a root-to-leaf path of the LBVH
+    bool resolve = false;    // hero scene with pass-through or mix-root instances
     float4 *world = nullptr; // world-space triangle vertices in original order
     BNode *nodes = nullptr;  // traversal layout (ds.nodes, ds.leaf_v)
     float4 *leaf_v = nullptr;
@@ -571,7 +619,7 @@ struct rp_scene {
         // one allocation carved into the SoA arrays (256-byte aligned slices)
         const size_t c = lanes;
         const size_t v16 = (c * 16 + 255) & ~size_t(255), v4 = (c * 4 + 255) & ~size_t(255);
-        const size_t bytes = 22 * v16 + 6 * v4 + 256;
+        const size_t bytes = 23 * v16 + 7 * v4 + 256;
         unsigned char *base = dalloc<unsigned char>(pool_owned, bytes, stream);
         size_t off = 0;
         auto take = [&](size_t n) {
@@ -593,6 +641,8 @@ struct rp_scene {
         q.queue[1] = reinterpret_cast<u32 *>(take(v4));
         q.bins = reinterpret_cast<u32 *>(take(4 * v4));
         q.counters = reinterpret_cast<u32 *>(take(256));
+        q.sh_t = reinterpret_cast<float4 *>(take(v16));
+        q.material = reinterpret_cast<u32 *>(take(v4));
         q.bin_capacity = lanes;
         q.stats = stats;
         capacity = lanes;
@@ -620,6 +670,7 @@ WaveParams wave_params(const rp_request &r) {
     p.lanes = r.pixel_count * r.sample_count;
     // src/metal_render.mm:1979-1981: floor(log2(total samples)) for ZSobol
     p.log_spp = r.sampler_kind == RP_SAMPLER_ZSOBOL && r.total_samples ? 63 - __builtin_clzll(r.total_samples) : 0;
+    p.boundary_limit = r.boundary_limit ? r.boundary_limit : 4096; // medium_boundary_limit, src/render.hpp:26
     return p;
 }
 u32 halton_scale(u32 resolution, u32 base) {
@@ -679,20 +730,36 @@ std::string validate_request(const rp_scene *s, const rp_request &r) {
     return {};
 }
 
-// The closest-hit and shadow kernels with the traversal stack the built tree needs.
-template <bool Count, int Block>
-void launch_trace(const rp_scene *s, const PathPool &pool, int in, unsigned grid, cudaStream_t st) {
-    if (s->tree_levels <= u32(kShortStack))
-        k_trace<Count, Block, kShortStack><<<grid, Block, 0, st>>>(s->ds, pool, in);
+// The closest-hit and shadow kernels with the traversal stack the built tree needs, resolving
+// pass-through and mix-root hits when the scene has them.
+template <bool Count, int Block, int Stack>
+void launch_trace_stack(const rp_scene *s, const PathPool &pool, int in, unsigned grid, cudaStream_t st, u32 limit) {
+    if (s->resolve)
+        k_trace<Count, Block, Stack, true><<<grid, Block, 0, st>>>(s->ds, pool, in, limit);
     else
-        k_trace<Count, Block, kStackDepth><<<grid, Block, 0, st>>>(s->ds, pool, in);
+        k_trace<Count, Block, Stack, false><<<grid, Block, 0, st>>>(s->ds, pool, in, limit);
+}
+template <bool Count, int Block>
+void launch_trace(const rp_scene *s, const PathPool &pool, int in, unsigned grid, cudaStream_t st, u32 limit) {
+    if (s->tree_levels <= u32(kShortStack))
+        launch_trace_stack<Count, Block, kShortStack>(s, pool, in, grid, st, limit);
+    else
+        launch_trace_stack<Count, Block, kStackDepth>(s, pool, in, grid, st, limit);
+}
+template <bool Count, int Block, bool Adjoint, int Stack>
+void launch_shadow_stack(const rp_scene *s, const PathPool &pool, unsigned grid, size_t smem, cudaStream_t st,
+                         u32 limit) {
+    if (s->resolve)
+        k_shadow<Count, Block, Adjoint, Stack, true><<<grid, Block, smem, st>>>(s->ds, pool, limit);
+    else
+        k_shadow<Count, Block, Adjoint, Stack, false><<<grid, Block, smem, st>>>(s->ds, pool, limit);
 }
 template <bool Count, int Block, bool Adjoint>
-void launch_shadow(const rp_scene *s, const PathPool &pool, unsigned grid, size_t smem, cudaStream_t st) {
+void launch_shadow(const rp_scene *s, const PathPool &pool, unsigned grid, size_t smem, cudaStream_t st, u32 limit) {
     if (s->tree_levels <= u32(kShortStack))
-        k_shadow<Count, Block, Adjoint, kShortStack><<<grid, Block, smem, st>>>(s->ds, pool);
+        launch_shadow_stack<Count, Block, Adjoint, kShortStack>(s, pool, grid, smem, st, limit);
     else
-        k_shadow<Count, Block, Adjoint, kStackDepth><<<grid, Block, smem, st>>>(s->ds, pool);
+        launch_shadow_stack<Count, Block, Adjoint, kStackDepth>(s, pool, grid, smem, st, limit);
 }
 
 // One wave: raygen, then max_depth + 1 events of trace -> shade -> shadow.
@@ -712,9 +779,9 @@ void run_wave(rp_scene *s, const WaveParams &p, size_t adjoint_smem = 0) {
         RP_CHECK(cudaMemsetAsync(pool.counters + 4, 0, 4 * sizeof(u32), s->stream));
         const unsigned trace_grid = grid_for(sms, p.lanes, kTraceBlock, 12);
         if (s->counting)
-            launch_trace<true, kTraceBlock>(s, pool, in, trace_grid, s->stream);
+            launch_trace<true, kTraceBlock>(s, pool, in, trace_grid, s->stream, p.boundary_limit);
         else
-            launch_trace<false, kTraceBlock>(s, pool, in, trace_grid, s->stream);
+            launch_trace<false, kTraceBlock>(s, pool, in, trace_grid, s->stream, p.boundary_limit);
         s->done();
         s->mark(2, 4);
         RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), s->stream));
@@ -735,11 +802,11 @@ void run_wave(rp_scene *s, const WaveParams &p, size_t adjoint_smem = 0) {
         s->done();
         s->mark(1);
         if (pool.hist)
-            launch_shadow<false, kTraceBlock, true>(s, pool, trace_grid, smem, s->stream);
+            launch_shadow<false, kTraceBlock, true>(s, pool, trace_grid, smem, s->stream, p.boundary_limit);
         else if (s->counting)
-            launch_shadow<true, kTraceBlock, false>(s, pool, trace_grid, 0, s->stream);
+            launch_shadow<true, kTraceBlock, false>(s, pool, trace_grid, 0, s->stream, p.boundary_limit);
         else
-            launch_shadow<false, kTraceBlock, false>(s, pool, trace_grid, 0, s->stream);
+            launch_shadow<false, kTraceBlock, false>(s, pool, trace_grid, 0, s->stream, p.boundary_limit);
         s->done();
         in ^= 1;
     }
@@ -997,18 +1064,22 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
         bool interfaces = false;
         for (u32 i = 0; i < d->material_count; ++i)
             interfaces = interfaces || d->materials[i].scattering == RP_INTERFACE;
-        if (!scalar) {
-            if (d->max_depth > RP_MAX_DEPTH + 1)
-                throw Invalid{"hero transport requires max depth <= 65"};
-            bool instance_media = false;
-            for (u32 i = 0; i < d->instance_count; ++i)
-                instance_media = instance_media || d->instances[i].inside_medium != RP_NONE ||
-                                 d->instances[i].outside_medium != RP_NONE;
-            if (d->medium_count || d->camera_medium != RP_NONE || interfaces || instance_media)
-                throw Invalid{"Packet/hero spectral transport requires a PBRT scene with vacuum media"};
-        }
         if (d->camera_medium != RP_NONE && d->camera_medium >= d->medium_count)
             throw Invalid{"camera medium out of range"};
+        if (!scalar) {
+            // src/render.cpp:1537-1590: hero transport needs every declared medium inactive
+            // (all coefficients zero); the camera and instance media are then vacuum
+            if (d->max_depth > RP_MAX_DEPTH + 1)
+                throw Invalid{"hero transport requires max depth <= 65"};
+            for (u32 i = 0; i < d->medium_count; ++i) {
+                const auto &m = d->media[i];
+                const auto nonzero = [](const float *v) { return std::any_of(v, v + 471, [](float x) { return x != 0; }); };
+                if (nonzero(m.sigma_a) || nonzero(m.sigma_s) || nonzero(m.emission))
+                    throw Invalid{"Packet/hero spectral transport requires a PBRT scene with vacuum media"};
+            }
+        }
+        if (const std::string mix = validate_mix(d); !mix.empty())
+            throw Invalid{mix};
         if (d->filter_kind > RP_FILTER_GAUSSIAN)
             throw Invalid{"unsupported pixel filter"};
         if (!(d->lens_radius >= 0) || !std::isfinite(d->lens_radius) ||
@@ -1059,9 +1130,9 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             throw Invalid{"a scene holds fewer than 2^30 triangle instances"};
         for (u32 i = 0; i < d->material_count; ++i) {
             const u32 f = d->materials[i].scattering;
-            if (f > RP_DIELECTRIC && !(scalar && f == RP_INTERFACE))
-                throw NotBuilt{"unsupported scattering family (diffuse, conductor, dielectric; null interfaces with "
-                               "the scalar transport)"};
+            if (f > RP_DIELECTRIC && f != RP_INTERFACE && f != RP_MIX)
+                throw NotBuilt{"unsupported scattering family (diffuse, conductor, dielectric, mix and null "
+                               "interfaces are built)"};
             if (scalar && (f == RP_CONDUCTOR || f == RP_DIELECTRIC))
                 throw NotBuilt{"the scalar transport builds diffuse surfaces and null interfaces; conductor and "
                                "dielectric surfaces render with the hero transport"};
@@ -1097,8 +1168,14 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             in.emission = q.emission;
             in.normal_begin = q.normal_begin;
             in.emitter_begin = kNone;
-            in.inside_medium = q.inside_medium;
-            in.outside_medium = q.outside_medium;
+            // the hero transport is vacuum: its camera and instance media are cleared
+            // (src/render.cpp:1587-1590)
+            in.inside_medium = scalar ? q.inside_medium : RP_NONE;
+            in.outside_medium = scalar ? q.outside_medium : RP_NONE;
+            const u32 root = d->materials[q.material].scattering;
+            in.resolve = (!scalar && (q.invisible_emitter != 0 || root == RP_INTERFACE) ? kPassThrough : 0u) |
+                         (root == RP_MIX ? kMixRoot : 0u);
+            s->resolve = s->resolve || (!scalar && in.resolve != 0);
             if (q.emission != RP_NONE) {
                 in.emitter_begin = u32(em_inst.size());
                 for (u32 t = 0; t < q.triangle_count; ++t) {
@@ -1118,8 +1195,10 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
         std::vector<DMaterial> mats(d->material_count);
         for (u32 i = 0; i < d->material_count; ++i) {
             const auto &m = d->materials[i];
-            mats[i] = {m.scattering, m.kind, m.knot_begin, m.knot_count, m.scalar_value, m.eta_begin, m.eta_count,
-                       m.k_begin, m.k_count, m.optical_extensions, m.u_roughness, m.v_roughness, m.remap_roughness};
+            mats[i] = {m.scattering, m.kind,        m.knot_begin,        m.knot_count,      m.scalar_value,
+                       m.eta_begin,  m.eta_count,   m.k_begin,           m.k_count,         m.optical_extensions,
+                       m.u_roughness, m.v_roughness, m.remap_roughness,    m.first_material,  m.second_material,
+                       m.mix_amount};
         }
         ds.materials = dupload(own, mats.data(), mats.size(), stm);
         ds.material_count = d->material_count;
@@ -1373,8 +1452,8 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             }
             ds.media = dupload(own, media.data(), media.size(), stm);
             ds.medium_count = d->medium_count;
-            ds.camera_medium = d->camera_medium;
-            ds.media_enabled = d->medium_count > 0 || interfaces || d->camera_medium != RP_NONE;
+            ds.camera_medium = scalar ? d->camera_medium : RP_NONE;
+            ds.media_enabled = scalar && (d->medium_count > 0 || interfaces || d->camera_medium != RP_NONE);
         }
         {
             const float u = 0x1.0p-24f;
@@ -1923,6 +2002,7 @@ WaveParams batch_params(const rp_batch_request &r) {
     p.sampler = r.sampler_kind;
     p.randomization = r.randomization;
     p.emergency_limit = r.emergency_limit ? r.emergency_limit : 1024;
+    p.boundary_limit = 4096;
     return p;
 }
 
@@ -1939,14 +2019,14 @@ void batch_wave_kernels(rp_scene *s, const WaveParams &p, const Batch &b, u32 wa
     int in = 0;
     for (u32 e = 0; e <= s->ds.max_depth; ++e) {
         RP_CHECK(cudaMemsetAsync(pool.counters + 4, 0, 4 * sizeof(u32), st));
-        launch_trace<false, TB>(s, pool, in, trace_grid, st);
+        launch_trace<false, TB>(s, pool, in, trace_grid, st, p.boundary_limit);
         RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), st));
         RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), st));
         k_shade<0, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
         k_shade<1, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
         k_shade<2, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
         k_shade<3, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
-        launch_shadow<false, TB, false>(s, pool, trace_grid, 0, st);
+        launch_shadow<false, TB, false>(s, pool, trace_grid, 0, st, p.boundary_limit);
         in ^= 1;
     }
     k_film_views<<<grid_for(sms, wave_lanes, 128, 16), 128, 0, st>>>(pool, b, s->cie, double(s->ds.filter_weight), film);
@@ -2444,6 +2524,8 @@ rp_status rp_cuda_sample_device_static(rp_scene *s, const rp_request *request, r
         const WaveParams p = wave_params(*request);
         if (capacity < p.lanes)
             throw Invalid{"output capacity is smaller than the request lanes"};
+        if (s->resolve)
+            throw Invalid{"the allocation-free entry point renders scenes without pass-through or mix surfaces"};
         const u32 max_lanes = RP_STATIC_MAX_LANES;
         if (p.lanes > max_lanes) {
             set_diag(diag, cap,
@@ -2469,14 +2551,14 @@ rp_status rp_cuda_sample_device_static(rp_scene *s, const rp_request *request, r
         int in = 0;
         for (u32 ev = 0; ev < s->ds.max_depth + 1; ++ev) {
             RP_CHECK(cudaMemsetAsync(pool.counters + 4, 0, 4 * sizeof(u32), st));
-            launch_trace<false, kTraceBlock>(s, pool, in, grid_for(sms, p.lanes, kTraceBlock, 12), st);
+            launch_trace<false, kTraceBlock>(s, pool, in, grid_for(sms, p.lanes, kTraceBlock, 12), st, p.boundary_limit);
             RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), st));
             RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), st));
             k_shade<0><<<grid_for(sms, p.lanes, 128, 16), 128, 0, st>>>(s->ds, p, pool, in);
             k_shade<1><<<grid_for(sms, p.lanes, 128, 16), 128, 0, st>>>(s->ds, p, pool, in);
             k_shade<2><<<grid_for(sms, p.lanes, 128, 16), 128, 0, st>>>(s->ds, p, pool, in);
             k_shade<3><<<grid_for(sms, p.lanes, 128, 16), 128, 0, st>>>(s->ds, p, pool, in);
-            launch_shadow<false, kTraceBlock, false>(s, pool, grid_for(sms, p.lanes, kTraceBlock, 12), 0, st);
+            launch_shadow<false, kTraceBlock, false>(s, pool, grid_for(sms, p.lanes, kTraceBlock, 12), 0, st, p.boundary_limit);
             in ^= 1;
         }
         k_results<<<grid_for(sms, p.lanes, 256, 16), 256, 0, st>>>(pool, p.lanes, s->ds.filter_weight,

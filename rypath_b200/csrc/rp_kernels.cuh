@@ -58,14 +58,88 @@ __global__ void k_raygen(const __grid_constant__ DeviceScene s, const __grid_con
         raygen_lane(s, cam, p, lane, lane, pool);
 }
 
+// Hit records the shade kernels read as a failed event (rp_sample_status 3, 4, 2).
+constexpr u32 kHitInvalid = 0xfffffffeu, kHitExhausted = 0xfffffffdu, kHitArithmetic = 0xfffffffcu;
+
+// A hit on a pass-through or mix-root instance, resolved before shading
+// (shaders/packet_pt_event_body.inc:100-205): the same validity checks and surface point as
+// the event, then either a crossing (at most boundary_limit in a row, each a new walk from
+// the spawned origin, which is written to ray_o) or the mix resolution (the resolved material
+// written to pool.material).  Returns the family to bin (3 for a failure or a miss) and sets
+// `prim` to the primitive or failure code to record.
+template <bool Count, int Stack>
+__device__ __noinline__ u32 resolve_hit(const DeviceScene &s, const PathPool &pool, u32 path, V3 ro, V3 rd, Hit &h,
+                                        u32 &prim, u32 *stack, int stride, u32 boundary_limit, u32 &nodes, u32 &tris,
+                                        u32 &rays) {
+    u32 crossings = 0;
+    bool moved = false;
+    u32 family = 3;
+    for (;;) {
+        if (!isfinite(h.t) || h.t < 0 || !isfinite(h.b1) || !isfinite(h.b2)) {
+            prim = kHitInvalid;
+            break;
+        }
+        const u32 inst = s.tri_instance[h.prim];
+        const DInstance &in = s.instances[inst];
+        if (in.material >= s.material_count) {
+            prim = kHitInvalid;
+            break;
+        }
+        SurfacePoint pt;
+        if (!triangle_surface_point(s, inst, s.tri_local[h.prim], h.b1, h.b2, true, pt)) {
+            prim = kHitArithmetic;
+            break;
+        }
+        if (in.resolve & kPassThrough) {
+            V3 origin;
+            if (crossings++ >= boundary_limit) {
+                prim = kHitExhausted;
+                break;
+            }
+            if (!spawn_boundary(ro, rd, h.t, pt, rd, origin)) {
+                prim = kHitArithmetic;
+                break;
+            }
+            ro = origin;
+            moved = true;
+            ++rays;
+            if (!walk_closest<Count, Stack>(s, ro, rd, __int_as_float(0x7f800000), h, stack, stride, nodes, tris)) {
+                prim = kHitInvalid;
+                break;
+            }
+            prim = h.prim;
+            if (prim == kNone)
+                break;
+            family = __ldg(s.tri_family + prim);
+            if (family != kResolveFamily)
+                break;
+            continue;
+        }
+        u32 material = in.material;
+        const u32 status = resolve_mix(s, pt.position, -rd, material);
+        if (status != 0) {
+            prim = status == 2 ? kHitArithmetic : kHitInvalid;
+            break;
+        }
+        pool.material[path] = material;
+        prim = h.prim;
+        family = s.materials[material].scattering;
+        break;
+    }
+    if (moved)
+        pool.ray_o[path] = make_float4(ro.x, ro.y, ro.z, 0);
+    return prim >= kHitArithmetic || prim == kNone ? 3u : family;
+}
+
 // Closest-hit queries for the active queue; each path is then appended to the bin of the
 // BSDF family it hit (0 diffuse, 1 conductor, 2 dielectric, 3 miss or failed query), so the
 // shade stage runs one specialised kernel per family ("material-sorted shading").
 // Stack: traversal stack entries per thread (kShortStack for shallow trees, whose walks then
 // fit eight 128-thread blocks per SM).
-template <bool Count, int Block = kTraceBlock, int Stack = kStackDepth>
+// Resolve: the scene has pass-through or mix-root instances (resolve_hit).
+template <bool Count, int Block = kTraceBlock, int Stack = kStackDepth, bool Resolve = false>
 __global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1)
-    k_trace(const __grid_constant__ DeviceScene s, PathPool pool, int in) {
+    k_trace(const __grid_constant__ DeviceScene s, PathPool pool, int in, u32 boundary_limit) {
     __shared__ u32 stack[Stack * Block];
     const u32 count = pool.counters[in];
     const u32 *queue = pool.queue[in];
@@ -85,8 +159,12 @@ __global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1
                                                            __int_as_float(0x7f800000), h, stack + threadIdx.x, Block,
                                                            nodes, tris);
                 ++rays;
-                pool.hit[path] = make_float4(h.t, h.b1, h.b2, __uint_as_float(ok ? h.prim : 0xfffffffeu));
+                u32 prim = ok ? h.prim : kHitInvalid;
                 family = (!ok || h.prim == kNone) ? 3u : u32(__ldg(s.tri_family + h.prim));
+                if (Resolve && family == kResolveFamily)
+                    family = resolve_hit<Count, Stack>(s, pool, path, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), h, prim,
+                                                       stack + threadIdx.x, Block, boundary_limit, nodes, tris, rays);
+                pool.hit[path] = make_float4(h.t, h.b1, h.b2, __uint_as_float(prim));
             }
         }
         const u32 peers = __match_any_sync(0xffffffffu, family);
@@ -127,7 +205,7 @@ __global__ void __launch_bounds__(Block, 384 / Block) k_shade(const __grid_const
     for (u32 trip = 0; trip < trips; ++trip) {
         const u32 i = trip * stride + blockIdx.x * blockDim.x + threadIdx.x;
         bool keep = false, shadow = false;
-        float4 sh_o = make_float4(0, 0, 0, 0), sh_d = sh_o, sh_c = sh_o;
+        float4 sh_o = make_float4(0, 0, 0, 0), sh_d = sh_o, sh_c = sh_o, sh_t = sh_o;
         u32 path = 0;
         if (i < count) {
             path = queue[i];
@@ -156,7 +234,7 @@ __global__ void __launch_bounds__(Block, 384 / Block) k_shade(const __grid_const
                 const u32 old_count = cnt;
                 bool terminated = true;
                 // current vertex
-                u32 ctype = kSurface, cinst = kNone, clocal = 0, clight = kNone;
+                u32 ctype = kSurface, cinst = kNone, clocal = 0, clight = kNone, cmat = kNone;
                 SurfacePoint cp;
                 cp.position = cp.error = cp.geometric_normal = cp.shading_normal = v3(0, 0, 0);
                 cp.inverse_area_pdf = 0;
@@ -176,8 +254,8 @@ __global__ void __launch_bounds__(Block, 384 / Block) k_shade(const __grid_const
                         break;
                     }
                     const u32 prim = __float_as_uint(hit.w);
-                    if (prim == 0xfffffffeu) {
-                        status = 3;
+                    if (prim >= kHitArithmetic && prim != kNone) {
+                        status = prim == kHitInvalid ? 3u : prim == kHitExhausted ? 4u : 2u;
                         break;
                     }
                     if (prim == kNone) {
@@ -208,6 +286,8 @@ __global__ void __launch_bounds__(Block, 384 / Block) k_shade(const __grid_const
                             status = 3;
                             break;
                         }
+                        // a mix root's hit was resolved by the closest-hit kernel
+                        cmat = (instance.resolve & kMixRoot) ? pool.material[path] : instance.material;
                         ctype = kSurface;
                         clight = instance.emission == kNone ? kNone : instance.emitter_begin + clocal;
                         cwo = -rd;
@@ -215,7 +295,7 @@ __global__ void __launch_bounds__(Block, 384 / Block) k_shade(const __grid_const
                             status = 2;
                             break;
                         }
-                        const DMaterial material = s.materials[instance.material];
+                        const DMaterial material = s.materials[cmat];
                         if (!shading_frame(cp.shading_normal, cframe) ||
                             !prepare_bsdf<F>(s, material, lambda, active_mask, cbsdf)) {
                             status = 2;
@@ -368,7 +448,7 @@ __global__ void __launch_bounds__(Block, 384 / Block) k_shade(const __grid_const
                         if (status == 0 && nonzero4(endpoint))
                             adjoint_accumulate(s, pool, sgrad, h, lambda, endpoint, pool.adj_w[path]);
                         if (F == 0 && ctype == kSurface && status == 0) {
-                            const u32 m = s.instances[cinst].material;
+                            const u32 m = cmat;
                             if (__ldg(pool.adj_slot + m) != kNone) {
                                 h = history_push(h, m);
                                 pool.hist[path] = h;
@@ -473,6 +553,7 @@ __global__ void __launch_bounds__(Block, 384 / Block) k_shade(const __grid_const
                                         shadow = true;
                                         sh_o = make_float4(so.x, so.y, so.z, kOneMinusEps);
                                         sh_d = make_float4(sd.x, sd.y, sd.z, __uint_as_float(path));
+                                        sh_t = make_float4(st.x, st.y, st.z, 0);
                                         sh_c = weight_ok ? to_float4(contribution)
                                                          : make_float4(__int_as_float(0x7fffffff), 0, 0, 0);
                                     }
@@ -530,16 +611,56 @@ __global__ void __launch_bounds__(Block, 384 / Block) k_shade(const __grid_const
             pool.sh_o[sslot] = sh_o;
             pool.sh_d[sslot] = sh_d;
             pool.sh_c[sslot] = sh_c;
+            if (pool.sh_t)
+                pool.sh_t[sslot] = sh_t;
         }
     }
     if (Adjoint)
         adjoint_end(pool, sgrad);
 }
 
+// visible() through pass-through surfaces (shaders/packet_transport.h:393-445): nearest hits
+// along the segment; an opaque one occludes, a pass-through one restarts the segment past it
+// toward the target (at most boundary_limit + 1 walks).  Returns 0 with `occluded` set, or
+// the failed sample's status (3 invalid hit, 2 invalid arithmetic, 4 boundary exhaustion).
+template <bool Count, int Stack>
+__device__ __noinline__ u32 pass_through_visible(const DeviceScene &s, V3 o, V3 d, float tmax, float4 target4,
+                                                 bool &occluded, u32 *stack, int stride, u32 boundary_limit,
+                                                 u32 &nodes, u32 &tris, u32 &rays) {
+    const V3 target = v3(target4.x, target4.y, target4.z);
+    occluded = true;
+    for (u32 crossings = 0; crossings <= boundary_limit; ++crossings) {
+        Hit h;
+        ++rays;
+        if (!walk_closest<Count, Stack>(s, o, d, tmax, h, stack, stride, nodes, tris))
+            return 3;
+        if (h.prim == kNone) {
+            occluded = false;
+            return 0;
+        }
+        const u32 inst = s.tri_instance[h.prim];
+        const DInstance &in = s.instances[inst];
+        if (in.material >= s.material_count)
+            return 3;
+        if (!(in.resolve & kPassThrough))
+            return 0;
+        SurfacePoint pt;
+        if (!triangle_surface_point(s, inst, s.tri_local[h.prim], h.b1, h.b2, true, pt))
+            return 2;
+        V3 next;
+        if (!spawn_boundary(o, d, h.t, pt, normalize3(d), next))
+            return 2;
+        o = next;
+        d = target - next;
+    }
+    return 4;
+}
+
 // Visibility of the light samples (visible(), shaders/packet_transport.h:377-446, opaque surfaces)
-template <bool Count, int Block = kTraceBlock, bool Adjoint = false, int Stack = kStackDepth>
+// Resolve: the scene has pass-through instances, which shadow rays cross (pass_through_visible).
+template <bool Count, int Block = kTraceBlock, bool Adjoint = false, int Stack = kStackDepth, bool Resolve = false>
 __global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1)
-    k_shadow(const __grid_constant__ DeviceScene s, PathPool pool) {
+    k_shadow(const __grid_constant__ DeviceScene s, PathPool pool, u32 boundary_limit) {
     __shared__ u32 stack[Stack * Block];
     extern __shared__ float sgrad[]; // adjoint only
     if (Adjoint)
@@ -550,12 +671,20 @@ __global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1
         const float4 o = pool.sh_o[i], d = pool.sh_d[i];
         const u32 path = __float_as_uint(d.w);
         bool occluded;
-        const bool ok = walk_any<Count, Stack>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), o.w, occluded,
-                                               stack + threadIdx.x, Block, nodes, tris);
-        ++rays;
+        u32 failure = 0;
+        if (Resolve) {
+            failure = pass_through_visible<Count, Stack>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), o.w, pool.sh_t[i],
+                                                         occluded, stack + threadIdx.x, Block, boundary_limit, nodes,
+                                                         tris, rays);
+        } else {
+            if (!walk_any<Count, Stack>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), o.w, occluded, stack + threadIdx.x,
+                                        Block, nodes, tris))
+                failure = 3;
+            ++rays;
+        }
         uint4 ident = pool.ident[path];
-        if (!ok) {
-            ident.w = set_status(ident.w, 3) | F_COMPLETE;
+        if (failure) {
+            ident.w = set_status(ident.w, failure) | F_COMPLETE;
             pool.ident[path] = ident;
             continue;
         }

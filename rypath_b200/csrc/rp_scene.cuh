@@ -14,7 +14,14 @@ struct DInstance {
     float m[12];
     u32 vertex_begin, triangle_begin, triangle_count, material, reverse, emission, normal_begin, emitter_begin;
     u32 inside_medium, outside_medium; // kNone = vacuum
+    u32 resolve;                       // kPassThrough | kMixRoot: hits resolve before shading
 };
+constexpr u32 kMixScattering = 9, kInterfaceScattering = 10;
+// DInstance::resolve bits: the hero transport passes through the instance (an invisible
+// emitter or a null-interface root material), or its root material is a mix.
+constexpr u32 kPassThrough = 1, kMixRoot = 2;
+// tri_family of triangles whose hits resolve in the closest-hit kernel before binning
+constexpr u32 kResolveFamily = 4;
 // wire::Material subset (src/render_wire.h:107-130)
 struct DMaterial {
     u32 scattering, kind, knot_begin, knot_count;
@@ -22,6 +29,8 @@ struct DMaterial {
     u32 eta_begin, eta_count, k_begin, k_count, optical_extensions;
     float u_roughness, v_roughness;
     u32 remap;
+    u32 first, second; // mix children
+    float mix_amount;
 };
 struct DPositional {
     float position[3];
@@ -192,6 +201,49 @@ __device__ __noinline__ bool triangle_surface_point(const DeviceScene &s, u32 in
     point.error = v3(dot(vabs(ax), ein), dot(vabs(ay), ein), dot(vabs(az), ein)) + gamma_bound(4.0f) * vabs(shift);
     return finite3(point.position) && finite3(point.error) && finite3(point.geometric_normal) &&
            finite3(point.shading_normal);
+}
+
+// PBRT's alpha hash (MurmurHash64A over the binary32 words of origin, direction and t;
+// shaders/alpha_hash.h:10-36) as a uniform in [0, 1).  t arrives as its bit pattern.
+RP_DEV float alpha_uniform(V3 o, V3 d, u32 t_bits) {
+    const u64 m = 0xc6a4a7935bd1e995ull;
+    const u32 w[6] = {__float_as_uint(o.x), __float_as_uint(o.y), __float_as_uint(o.z),
+                      __float_as_uint(d.x), __float_as_uint(d.y), __float_as_uint(d.z)};
+    u64 h = 28ull * m;
+#pragma unroll
+    for (int i = 0; i < 6; i += 2) {
+        u64 k = u64(w[i]) | (u64(w[i + 1]) << 32);
+        k *= m;
+        k ^= k >> 47;
+        k *= m;
+        h ^= k;
+        h *= m;
+    }
+    h ^= u64(t_bits);
+    h *= m;
+    h ^= h >> 47;
+    h *= m;
+    h ^= h >> 47;
+    return float(u32(h)) * 0x1p-32f;
+}
+// The material a hit on mix root `material` resolves to (shaders/packet_pt_event_body.inc:
+// 165-190): at each mix node, second where the alpha hash of (position, -direction, node
+// index) is below the amount, else first.  Returns the sample status: 0, 2 (a 65th level
+// or a non-finite amount) or 3 (a child out of range).
+RP_DEV u32 resolve_mix(const DeviceScene &s, V3 position, V3 toward_origin, u32 &material) {
+    for (u32 depth = 0; depth <= 64; ++depth) {
+        const DMaterial &node = s.materials[material];
+        if (node.scattering != kMixScattering)
+            return 0;
+        const float amount = node.mix_amount;
+        if (depth == 64 || !isfinite(amount))
+            return 2;
+        const float selector = alpha_uniform(position, toward_origin, material);
+        material = amount <= 0 ? node.first : amount >= 1 ? node.second : selector < amount ? node.second : node.first;
+        if (material >= s.material_count)
+            return 3;
+    }
+    return 0;
 }
 
 // ------------------------------------------------------------------ light selection (shaders/light_sampling.h)

@@ -49,6 +49,8 @@ struct PathPool {
     float4 *sh_o;  // shadow origin, tmax
     float4 *sh_d;  // shadow direction, path id bits
     float4 *sh_c;  // weighted contribution (NaN x: invalid if visible)
+    float4 *sh_t;  // shadow target (pass-through walks restart toward it), or nullptr
+    u32 *material; // material a mix-root hit resolved to (written by the closest-hit kernel)
     // statistics (optional)
     unsigned long long *stats; // closest [0] nodes, [1] triangles, [2] rays; shadow [3] rays, [4] nodes, [5] triangles
     // path-replay adjoint (hist == nullptr: off)
@@ -67,7 +69,8 @@ struct WaveParams {
     u32 width, height, pixel_begin, pixel_count, sample_low, sample_high;
     u32 seed_low, seed_high, sampler, randomization, m, emergency_limit;
     u32 lanes;
-    u32 log_spp; // ZSobol: log2 of the total sample budget
+    u32 log_spp;        // ZSobol: log2 of the total sample budget
+    u32 boundary_limit; // pass-through crossings allowed between two vertices
 };
 
 // shaders/render.metal:113-122
@@ -433,6 +436,30 @@ RP_DEV V3 offset_point(V3 position, V3 error, V3 ng, V3 direction) {
         return position;
     const V3 n = dot(direction, ng) < 0 ? -ng : ng;
     return round_out(position + dot(vabs(n), error) * n, n);
+}
+// shaders/render.metal:1939-1977: null-interface crossing anchored at the ray hit, with
+// certified separation
+RP_DEV bool spawn_boundary(V3 o, V3 d, float t, const SurfacePoint &pt, V3 direction, V3 &origin) {
+    if (!(t >= 0) || !isfinite(t))
+        return false;
+    const V3 ng = pt.geometric_normal;
+    const V3 n = dot(ng, direction) < 0 ? -ng : ng;
+    const float facing = dot(n, direction);
+    if (!(facing > gamma_bound(5) * dot(vabs(n), vabs(direction))))
+        return false;
+    const V3 position = fma3(v3(t, t, t), d, o);
+    const V3 ray_error = gamma_bound(2) * (vabs(t * d) + vabs(o));
+    const V3 error = (pt.error + vabs(pt.position - position)) + ray_error;
+    const float norm_lower = dot(n, n) * (1 - gamma_bound(4));
+    const float height = dot(vabs(n), error) * (1 + gamma_bound(8)) / norm_lower;
+    origin = round_out(fma3(v3(height, height, height), n, position), n);
+    if (!(norm_lower > 0) || !isfinite(height) || !finite3(origin) || eq3(origin, o))
+        return false;
+    const V3 departure = origin - pt.position;
+    const float separation = dot(n, departure);
+    const float rounding = gamma_bound(5) * dot(vabs(n), vabs(departure));
+    const float uncertainty = dot(vabs(n), pt.error) * (1 + gamma_bound(4));
+    return isfinite(separation) && isfinite(rounding) && isfinite(uncertainty) && separation - rounding > uncertainty;
 }
 
 // ------------------------------------------------------------------ path-replay adjoint

@@ -21,7 +21,6 @@
 namespace rp {
 
 constexpr u32 kMediumStride = 1416; // sigma_a[471], sigma_s[471], emission[471], g, 2 pad
-constexpr u32 kInterfaceScattering = 10;
 constexpr u32 kMediumBlockLimit = 0x20000000u;   // src/sampling_contract.h:45
 constexpr u32 kMediumStream = 0x6d656431u;       // medium_stream_v1
 enum : u32 {
@@ -176,29 +175,6 @@ RP_DEV V3 spawn_origin(V3 o, V3 d, float t, const SurfacePoint &pt, V3 n) {
 RP_DEV V3 spawn_toward(V3 o, V3 d, float t, const SurfacePoint &pt, V3 direction) {
     const V3 ng = pt.geometric_normal;
     return spawn_origin(o, d, t, pt, dot(ng, direction) < 0.0f ? -ng : ng);
-}
-// :1939-1977 null-interface crossing anchored at the ray hit, with certified separation
-RP_DEV bool spawn_boundary(V3 o, V3 d, float t, const SurfacePoint &pt, V3 direction, V3 &origin) {
-    if (!(t >= 0) || !isfinite(t))
-        return false;
-    const V3 ng = pt.geometric_normal;
-    const V3 n = dot(ng, direction) < 0 ? -ng : ng;
-    const float facing = dot(n, direction);
-    if (!(facing > gamma_bound(5) * dot(vabs(n), vabs(direction))))
-        return false;
-    const V3 position = fma3(v3(t, t, t), d, o);
-    const V3 ray_error = gamma_bound(2) * (vabs(t * d) + vabs(o));
-    const V3 error = (pt.error + vabs(pt.position - position)) + ray_error;
-    const float norm_lower = dot(n, n) * (1 - gamma_bound(4));
-    const float height = dot(vabs(n), error) * (1 + gamma_bound(8)) / norm_lower;
-    origin = round_out(fma3(v3(height, height, height), n, position), n);
-    if (!(norm_lower > 0) || !isfinite(height) || !finite3(origin) || eq3(origin, o))
-        return false;
-    const V3 departure = origin - pt.position;
-    const float separation = dot(n, departure);
-    const float rounding = gamma_bound(5) * dot(vabs(n), vabs(departure));
-    const float uncertainty = dot(vabs(n), pt.error) * (1 + gamma_bound(4));
-    return isfinite(separation) && isfinite(rounding) && isfinite(uncertainty) && separation - rounding > uncertainty;
 }
 // :2221-2232 connection to a sampled area point, ending on its near side
 RP_DEV V3 shadow_segment_direction(V3 origin, V3 delta, const SurfacePoint &target, float signed_cosine) {
@@ -783,18 +759,34 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
     }
     if (bounce >= s.max_depth)
         return kEventFinished;
+    // mix materials resolve at the hit's point (:541-587)
+    bool point_ready = emissive;
+    u32 material_index = instance.material;
+    if (material.scattering == kMixScattering) {
+        if (!emissive && !triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point)) {
+            path.status = S_ARITHMETIC;
+            return kEventFinished;
+        }
+        point_ready = true;
+        const u32 mix_status = resolve_mix(s, point.position, -path.d, material_index);
+        if (mix_status != 0) {
+            path.status = mix_status == 2 ? S_ARITHMETIC : S_HIT;
+            return kEventFinished;
+        }
+    }
+    const DMaterial surface = s.materials[material_index];
     float rho = 0;
-    if (material.scattering != 0) {
+    if (surface.scattering != 0) {
         path.status = S_HIT; // microfacet surfaces are not built for the scalar transport
         return kEventFinished;
     }
-    if (material.kind == 0 && material.knot_count >= 2 && material.knot_begin <= s.knot_count &&
-        material.knot_count <= s.knot_count - material.knot_begin) {
-        rho = pbrt_reflectance(s.knots + material.knot_begin, material.knot_count, path.wavelength);
-    } else if (material.kind == 1) {
-        rho = material.scalar_value;
-    } else if (material.kind == 4) {
-        rho = blackbody_reflectance(material.scalar_value, path.wavelength);
+    if (surface.kind == 0 && surface.knot_count >= 2 && surface.knot_begin <= s.knot_count &&
+        surface.knot_count <= s.knot_count - surface.knot_begin) {
+        rho = pbrt_reflectance(s.knots + surface.knot_begin, surface.knot_count, path.wavelength);
+    } else if (surface.kind == 1) {
+        rho = surface.scalar_value;
+    } else if (surface.kind == 4) {
+        rho = blackbody_reflectance(surface.scalar_value, path.wavelength);
     } else {
         path.status = S_HIT;
         return kEventFinished;
@@ -810,7 +802,7 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
         path.status = S_EMERGENCY;
         return kEventFinished;
     }
-    if (!emissive && !triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point)) {
+    if (!point_ready && !triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point)) {
         path.status = S_ARITHMETIC;
         return kEventFinished;
     }

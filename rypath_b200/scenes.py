@@ -282,6 +282,62 @@ def cornell_box(width=256, height=256, spp=64, max_depth=8) -> Scene:
     return scene
 
 
+def mix_material(first, second, amount):
+    """A mix of materials `first` and `second` (indices): second where the alpha hash is below amount."""
+    m = abi.Material()
+    m.scattering, m.kind = abi.MIX, abi.REFLECTANCE_CONSTANT
+    m.first_material, m.second_material, m.mix_amount = first, second, amount
+    return m
+
+
+def _append_knots(scene, values):
+    begin = scene.knots.shape[0]
+    scene.knots = np.concatenate([scene.knots, knots_from_curve(values)])
+    return begin
+
+
+def cornell_pass_through(width=256, height=256, spp=64, max_depth=8, pane=True, invisible_light=True,
+                         mixes=True) -> Scene:
+    """The Cornell-style box with the hero transport's pass-through and mix surfaces.
+
+    pane: a null-interface quad across the box opening (camera and shadow rays cross it);
+    invisible_light: the area light is an invisible emitter (rays pass through it, light
+    sampling still reaches it); mixes: the short box is mix(white, rough conductor, 0.35), the
+    tall box mix(mix(white, glass, 0.5), red, 0.7).
+    """
+    scene = cornell_box(width, height, spp, max_depth)
+    scene.name = "cornell_pass_through"
+    if invisible_light:
+        scene.instances[-1].invisible_emitter = 1
+    if mixes:
+        conductor = abi.Material()
+        conductor.scattering, conductor.kind, conductor.scalar_value = abi.CONDUCTOR, abi.REFLECTANCE_CONSTANT, 1.0
+        conductor.eta_begin, conductor.eta_count = _append_knots(scene, 0.25), 32
+        conductor.k_begin, conductor.k_count = _append_knots(scene, 3.2), 32
+        conductor.optical_extensions, conductor.u_roughness, conductor.v_roughness = 3, 0.3, 0.3
+        conductor.remap_roughness = 1
+        glass = abi.Material()
+        glass.scattering, glass.kind, glass.scalar_value = abi.DIELECTRIC, abi.REFLECTANCE_CONSTANT, 1.0
+        glass.eta_begin, glass.eta_count, glass.optical_extensions = _append_knots(scene, 1.5), 32, 1
+        base = len(scene.materials)
+        scene.materials += [conductor, glass]
+        scene.materials.append(mix_material(0, base, 0.35))          # base + 2: short box
+        scene.materials.append(mix_material(0, base + 1, 0.5))       # base + 3: inner mix
+        scene.materials.append(mix_material(base + 3, 1, 0.7))       # base + 4: tall box
+        scene.instances[5].material = base + 2
+        scene.instances[6].material = base + 4
+    if pane:
+        verts, tris = _quad((-1, 0.3, 0.8), (1, 0.3, 0.8), (1, 1.7, 0.8), (-1, 1.7, 0.8))
+        interface = abi.Material()
+        interface.scattering, interface.kind = abi.INTERFACE, abi.REFLECTANCE_CONSTANT
+        scene.materials.append(interface)
+        scene.instances.append(identity_instance(scene.positions.shape[0], scene.triangles.shape[0], 2,
+                                                 len(scene.materials) - 1))
+        scene.positions = np.concatenate([scene.positions, verts])
+        scene.triangles = np.concatenate([scene.triangles, tris])
+    return scene
+
+
 def cornell_fog(width=1024, height=1024, spp=64, max_depth=32, sigma_s_mean=0.5, albedo=0.9, g=0.7) -> Scene:
     """The Cornell-style box filled with a homogeneous medium, rendered by the scalar transport.
 
