@@ -244,3 +244,35 @@ def test_image_statistics_match_oracle():
     # 3-sigma per pixel; allow the expected tail (about 0.3% per channel, plus heavy-tail slack)
     assert (z > 3).mean() < 0.02, (z > 3).mean()
     assert abs(gm[:, 1].mean() - cm[:, 1].mean()) < 3 * np.sqrt(gv[:, 1].sum() + cv[:, 1].sum()) / (w * h)
+
+
+def test_relative_rmse_against_a_4096_spp_fp64_render():
+    """Convergence gate: against a 4096-spp oracle render accumulated in FP64, the device's 64-spp
+    film (Sobol, Owen scrambling) has relative RMSE (root-mean-square error over pixels and XYZ
+    channels, divided by the root-mean-square of the reference) below 0.06, and within 30% of the
+    relative RMSE of an oracle render with the same sampler on another seed: the device converges
+    to the same image at the same rate (observed in the oracle alone: 0.034 at 64 spp, against
+    0.06-0.08 for the independent sampler)."""
+    w = h = 16
+    s = scenes.cornell_box(w, h, 64)
+    cie = np.ascontiguousarray(scenes.cie_xyz())
+
+    def oracle_mean(spp, seed, sampler=abi.SAMPLER_INDEPENDENT):
+        lanes = OracleScene(s).sample(request(w, h, spp, seed=seed, sampler=sampler), threads=0)
+        f = np.zeros(w * h, abi.film_dtype())
+        assert oracle().or_film_add(lanes.ctypes.data, lanes.size, cie.ctypes.data, w * h, f.ctypes.data) == 0
+        return renderer.film_mean(f)
+
+    reference = oracle_mean(4096, 101)
+    built = renderer.build_renderer(s)
+    st, diag, film = built.scene.render_film(renderer.RenderSettings(w, h, samples=64, batch_size=64, seed=1))
+    built.scene.close()
+    assert st == abi.RP_SUCCESS, diag
+
+    def relative_rmse(x):
+        return np.sqrt(np.mean((x - reference) ** 2)) / np.sqrt(np.mean(reference ** 2))
+
+    device = relative_rmse(renderer.film_mean(film))
+    other_seed = relative_rmse(oracle_mean(64, 2, abi.SAMPLER_SOBOL))
+    assert device < 0.06, device
+    assert device < 1.3 * other_seed, (device, other_seed)
