@@ -418,7 +418,7 @@ def main():
     trace_ms = sum(t.trace_ms for t in steps)
     trace_launches = sum(t.trace_launches for t in steps)
     rays = counts.closest_rays
-    node_bytes, tri_bytes = 64, 48
+    node_bytes, tri_bytes = 80, 48  # compressed 8-wide node, one triangle (3 float4)
     state_bytes = 4 + 16 + 32 + 16  # queue entry, flags, ray read, hit write
     algo_per_ray = (counts.nodes_visited * node_bytes + counts.triangles_tested * tri_bytes) / max(
         1, counts.closest_rays) + state_bytes

@@ -370,6 +370,230 @@ __global__ void k_pack(u32 n, const u32 *order, const float4 *world, BuildTmp t,
     }
 }
 
+// ---- compressed 8-wide tree, collapsed top-down from the binary one
+struct WideBuild {
+    const u32 *left, *right;          // binary topology
+    const float4 *node_lo, *node_hi;  // binary internal boxes
+    const float4 *box_lo, *box_hi;    // triangle boxes (original order)
+    const u32 *order;                 // leaf slot -> triangle
+    const float4 *leaf_v;             // triangles by leaf slot
+    WNode *wnodes;
+    float4 *wtri;
+    u32 *counters;                    // [0] wide nodes, [1] wide leaves, [2] [3] level queue lengths, [4] error, [5] levels
+    uint2 *queue[2];                  // (binary internal node, wide node index) per level
+    u32 capacity;                     // wide nodes available (binary internal nodes)
+    u32 n;                            // triangles
+};
+
+RP_DEV float box_area(float4 lo, float4 hi) {
+    const float x = hi.x - lo.x, y = hi.y - lo.y, z = hi.z - lo.z;
+    return x * y + y * z + z * x;
+}
+
+// Biased exponent of the power-of-two step that spans [lo, hi] in 255 steps, and the 8-bit
+// bounds of every child along this axis: each plane lo + q step (in real arithmetic, checked
+// with directed rounding) is at or below the child's low bound (or at or above its high
+// bound).  A larger step is taken when 255 steps fall short.
+RP_DEV u32 quantize_axis(float lo, float hi, const float *clo, const float *chi, int count, unsigned char *qlo,
+                         unsigned char *qhi) {
+    const float extent = hi - lo;
+    int e = -126;
+    if (extent > 0 && isfinite(extent)) {
+        frexpf(extent / 255.0f, &e); // extent / 255 < 2^e
+        e = max(e, -126);
+    }
+    for (; e <= 127; ++e) {
+        const float step = __uint_as_float(u32(e + 127) << 23);
+        bool ok = true;
+        for (int k = 0; k < count && ok; ++k) {
+            // clamped in float first: a NaN bound clamps to 0 (and a NaN decode never passes)
+            int a = int(fminf(fmaxf(floorf((clo[k] - lo) / step), 0.0f), 255.0f));
+            int b = int(fminf(fmaxf(ceilf((chi[k] - lo) / step), 0.0f), 255.0f));
+            // the real planes lo + q step: at or below clo, at or above chi
+            while (a > 0 && !(__fmaf_ru(float(a), step, lo) <= clo[k]))
+                --a;
+            while (b < 255 && !(__fmaf_rd(float(b), step, lo) >= chi[k]))
+                ++b;
+            ok = __fmaf_rd(float(b), step, lo) >= chi[k] || !(chi[k] == chi[k]);
+            qlo[k] = (unsigned char)a;
+            qhi[k] = (unsigned char)b;
+        }
+        if (ok)
+            break;
+    }
+    return u32(min(e, 127) + 127);
+}
+
+// One level of the collapse: each queued binary node becomes a wide node of up to 8 children,
+// expanding the internal child of largest surface area until 8 are reached or none is left.
+// Internal children are queued for the next level with the wide indices allocated for them.
+__global__ void k_wide_level(WideBuild w, int parity, u32 level) {
+    const u32 count = min(w.counters[2 + parity], w.capacity); // an overflowing level has set the error bit
+    const uint2 *in = w.queue[parity];
+    uint2 *out = w.queue[parity ^ 1];
+    u32 *out_count = w.counters + 2 + (parity ^ 1);
+    if (count && blockIdx.x == 0 && threadIdx.x == 0)
+        atomicMax(w.counters + 5, level + 1);
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const uint2 item = in[i];
+        u32 ch[8];
+        int nc = 2;
+        ch[0] = w.left[item.x];
+        ch[1] = w.right[item.x];
+        while (nc < 8) {
+            int best = -1;
+            float best_area = -1;
+            for (int k = 0; k < nc; ++k)
+                if (!(ch[k] & kLeaf)) {
+                    const float a = box_area(w.node_lo[ch[k]], w.node_hi[ch[k]]);
+                    if (a > best_area) {
+                        best_area = a;
+                        best = k;
+                    }
+                }
+            if (best < 0)
+                break;
+            const u32 c = ch[best];
+            ch[best] = w.left[c];
+            ch[nc++] = w.right[c];
+        }
+        // child boxes and the node box
+        float4 lo[8], hi[8];
+        float4 nlo = make_float4(INFINITY, INFINITY, INFINITY, 0), nhi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0);
+        for (int k = 0; k < nc; ++k) {
+            if (ch[k] & kLeaf) {
+                const u32 prim = w.order[ch[k] & ~kLeaf];
+                lo[k] = w.box_lo[prim];
+                hi[k] = w.box_hi[prim];
+            } else {
+                lo[k] = w.node_lo[ch[k]];
+                hi[k] = w.node_hi[ch[k]];
+            }
+            nlo = make_float4(fminf(nlo.x, lo[k].x), fminf(nlo.y, lo[k].y), fminf(nlo.z, lo[k].z), 0);
+            nhi = make_float4(fmaxf(nhi.x, hi[k].x), fmaxf(nhi.y, hi[k].y), fmaxf(nhi.z, hi[k].z), 0);
+        }
+        // slots: each child to the free slot whose octant direction best matches its offset
+        // from the node centre (children with the largest offsets choose first)
+        const float cx = 0.5f * nlo.x + 0.5f * nhi.x, cy = 0.5f * nlo.y + 0.5f * nhi.y, cz = 0.5f * nlo.z + 0.5f * nhi.z;
+        float ox[8], oy[8], oz[8];
+        int slot_of[8];
+        bool placed[8];
+        for (int k = 0; k < nc; ++k) {
+            ox[k] = (0.5f * lo[k].x + 0.5f * hi[k].x) - cx;
+            oy[k] = (0.5f * lo[k].y + 0.5f * hi[k].y) - cy;
+            oz[k] = (0.5f * lo[k].z + 0.5f * hi[k].z) - cz;
+            placed[k] = false;
+        }
+        u32 used = 0;
+        for (int round = 0; round < nc; ++round) {
+            int pick = -1;
+            float reach = -1;
+            for (int k = 0; k < nc; ++k)
+                if (!placed[k]) {
+                    const float m = fabsf(ox[k]) + fabsf(oy[k]) + fabsf(oz[k]);
+                    if (m > reach) {
+                        reach = m;
+                        pick = k;
+                    }
+                }
+            int best_slot = -1;
+            float best_score = -INFINITY;
+            for (int sl = 0; sl < 8; ++sl)
+                if (!((used >> sl) & 1u)) {
+                    const float score = ((sl & 1) ? ox[pick] : -ox[pick]) + ((sl & 2) ? oy[pick] : -oy[pick]) +
+                                        ((sl & 4) ? oz[pick] : -oz[pick]);
+                    if (score > best_score) {
+                        best_score = score;
+                        best_slot = sl;
+                    }
+                }
+            placed[pick] = true;
+            slot_of[pick] = best_slot;
+            used |= 1u << best_slot;
+        }
+        int child_at[8];
+        for (int sl = 0; sl < 8; ++sl)
+            child_at[sl] = -1;
+        for (int k = 0; k < nc; ++k)
+            child_at[slot_of[k]] = k;
+        u32 imask = 0, lmask = 0, internal = 0, leaves = 0;
+        for (int sl = 0; sl < 8; ++sl)
+            if (child_at[sl] >= 0) {
+                if (ch[child_at[sl]] & kLeaf) {
+                    lmask |= 1u << sl;
+                    ++leaves;
+                } else {
+                    imask |= 1u << sl;
+                    ++internal;
+                }
+            }
+        const u32 base = internal ? atomicAdd(w.counters + 0, internal) : 0;
+        const u32 tri_base = leaves ? atomicAdd(w.counters + 1, leaves) : 0;
+        if (base + internal > w.capacity || tri_base + leaves > w.n) {
+            atomicOr(w.counters + 4, 1u);
+            continue;
+        }
+        // quantized bounds, slot order
+        float clo[8], chi[8];
+        unsigned char q[6][8];
+        for (int sl = 0; sl < 8; ++sl)
+            for (int a = 0; a < 6; ++a)
+                q[a][sl] = 0;
+        u32 ebytes = 0;
+        const float nl[3] = {nlo.x, nlo.y, nlo.z}, nh[3] = {nhi.x, nhi.y, nhi.z};
+        for (int a = 0; a < 3; ++a) {
+            int m = 0;
+            int slots[8];
+            for (int sl = 0; sl < 8; ++sl)
+                if (child_at[sl] >= 0) {
+                    const int k = child_at[sl];
+                    clo[m] = a == 0 ? lo[k].x : a == 1 ? lo[k].y : lo[k].z;
+                    chi[m] = a == 0 ? hi[k].x : a == 1 ? hi[k].y : hi[k].z;
+                    slots[m++] = sl;
+                }
+            unsigned char ql[8], qh[8];
+            const u32 eb = quantize_axis(nl[a], nh[a], clo, chi, m, ql, qh);
+            ebytes |= eb << (8 * a);
+            for (int j = 0; j < m; ++j) {
+                q[a][slots[j]] = ql[j];
+                q[3 + a][slots[j]] = qh[j];
+            }
+        }
+        auto pack = [&](int row, int half) {
+            u32 v = 0;
+            for (int b = 0; b < 4; ++b)
+                v |= u32(q[row][4 * half + b]) << (8 * b);
+            return v;
+        };
+        WNode node;
+        node.origin = make_float4(nlo.x, nlo.y, nlo.z, __uint_as_float(ebytes | (imask << 24)));
+        node.links = make_uint4(base, tri_base, lmask, 0);
+        node.q0 = make_uint4(pack(0, 0), pack(0, 1), pack(1, 0), pack(1, 1));
+        node.q1 = make_uint4(pack(2, 0), pack(2, 1), pack(3, 0), pack(3, 1));
+        node.q2 = make_uint4(pack(4, 0), pack(4, 1), pack(5, 0), pack(5, 1));
+        w.wnodes[item.y] = node;
+        u32 ji = 0, jl = 0;
+        for (int sl = 0; sl < 8; ++sl) {
+            const int k = child_at[sl];
+            if (k < 0)
+                continue;
+            if (ch[k] & kLeaf) {
+                const u32 slot = ch[k] & ~kLeaf, dst = tri_base + jl++;
+                w.wtri[3 * size_t(dst)] = w.leaf_v[3 * size_t(slot)];
+                w.wtri[3 * size_t(dst) + 1] = w.leaf_v[3 * size_t(slot) + 1];
+                w.wtri[3 * size_t(dst) + 2] = w.leaf_v[3 * size_t(slot) + 2];
+            } else {
+                const u32 at = atomicAdd(out_count, 1u);
+                if (at < w.capacity)
+                    out[at] = make_uint2(ch[k], base + ji);
+                else
+                    atomicOr(w.counters + 4, 1u);
+                ++ji;
+            }
+        }
+    }
+}
+
 // Structural check of the topology before any traversal.  k_tree_refs counts the references
 // to every internal node and leaf (a child index out of range sets kBuildTree); k_tree_verify
 // requires exactly one reference to each node but the root (none) and each leaf, and a walk

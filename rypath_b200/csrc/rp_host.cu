@@ -499,6 +499,7 @@ struct rp_scene {
     u32 *order = nullptr;
     BuildTmp tmp{};
     u32 tree_levels = 0;     // most internal nodes on a root-to-leaf path of the LBVH
+    u32 wide_levels = 0;     // levels of the compressed 8-wide traversal tree
     bool resolve = false;    // hero scene with pass-through or mix-root instances
     float4 *world = nullptr; // world-space triangle vertices in original order
     BNode *nodes = nullptr;  // traversal layout (ds.nodes, ds.leaf_v)
@@ -741,7 +742,7 @@ void launch_trace_stack(const rp_scene *s, const PathPool &pool, int in, unsigne
 }
 template <bool Count, int Block>
 void launch_trace(const rp_scene *s, const PathPool &pool, int in, unsigned grid, cudaStream_t st, u32 limit) {
-    if (s->tree_levels <= u32(kShortStack))
+    if (s->wide_levels <= u32(kShortStack))
         launch_trace_stack<Count, Block, kShortStack>(s, pool, in, grid, st, limit);
     else
         launch_trace_stack<Count, Block, kStackDepth>(s, pool, in, grid, st, limit);
@@ -756,7 +757,7 @@ void launch_shadow_stack(const rp_scene *s, const PathPool &pool, unsigned grid,
 }
 template <bool Count, int Block, bool Adjoint>
 void launch_shadow(const rp_scene *s, const PathPool &pool, unsigned grid, size_t smem, cudaStream_t st, u32 limit) {
-    if (s->tree_levels <= u32(kShortStack))
+    if (s->wide_levels <= u32(kShortStack))
         launch_shadow_stack<Count, Block, Adjoint, kShortStack>(s, pool, grid, smem, st, limit);
     else
         launch_shadow_stack<Count, Block, Adjoint, kStackDepth>(s, pool, grid, smem, st, limit);
@@ -819,7 +820,7 @@ void run_scalar_wave(rp_scene *s, const WaveParams &p, u32 boundary_limit) {
     s->ensure_scalar(p.lanes);
     if (!s->volpath_blocks) {
         int per_sm = 0;
-        RP_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_volpath<false>, kTraceBlock, 0));
+        RP_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_volpath<false, kShortStack>, kTraceBlock, 0));
         s->volpath_blocks = std::max(1, per_sm);
     }
     s->mark(3);
@@ -837,10 +838,15 @@ void run_scalar_wave(rp_scene *s, const WaveParams &p, u32 boundary_limit) {
     const u32 blocks_needed = (p.lanes + kTraceBlock - 1) / kTraceBlock;
     const int grid = int(std::max<u32>(1, std::min<u32>(blocks_needed, u32(s->sm_count * s->volpath_blocks))));
     s->mark(2);
-    if (s->counting)
-        k_volpath<true><<<grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q);
+    const bool short_stack = s->wide_levels <= u32(kShortStack);
+    if (s->counting && short_stack)
+        k_volpath<true, kShortStack><<<grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q);
+    else if (s->counting)
+        k_volpath<true, kStackDepth><<<grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q);
+    else if (short_stack)
+        k_volpath<false, kShortStack><<<grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q);
     else
-        k_volpath<false><<<grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q);
+        k_volpath<false, kStackDepth><<<grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q);
     s->done();
     RP_CHECK(cudaGetLastError());
 }
@@ -925,6 +931,63 @@ void build_bounds(rp_scene *s, int (&cb)[12]) {
     std::copy(out, out + 12, cb);
 }
 
+// The compressed 8-wide traversal tree, collapsed level by level from the checked binary tree
+// (one launch per binary level at most: each wide level consumes at least one), then checked:
+// every triangle placed once, no allocation beyond the binary tree's size.
+void build_wide(rp_scene *s) {
+    const u32 n = s->n;
+    auto &own = s->owned;
+    cudaStream_t st = s->stream;
+    BuildTmp &t = s->tmp;
+    const u32 capacity = std::max<u32>(n, 2) - 1;
+    WNode *wnodes = dalloc<WNode>(own, capacity, st);
+    float4 *wtri = dalloc<float4>(own, size_t(3) * std::max<u32>(n, 1), st);
+    s->ds.wnodes = wnodes;
+    s->ds.wtri = wtri;
+    s->ds.wnode_count = 0;
+    s->wide_levels = 0;
+    if (n == 0)
+        return;
+    if (n == 1) {
+        RP_CHECK(cudaMemcpyAsync(wtri, s->leaf_v, 3 * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+        RP_CHECK(cudaStreamSynchronize(st));
+        return;
+    }
+    WideBuild w{};
+    w.left = t.left;
+    w.right = t.right;
+    w.node_lo = t.node_lo;
+    w.node_hi = t.node_hi;
+    w.box_lo = t.box_lo;
+    w.box_hi = t.box_hi;
+    w.order = s->order;
+    w.leaf_v = s->leaf_v;
+    w.wnodes = wnodes;
+    w.wtri = wtri;
+    w.counters = dalloc<u32>(own, 8, st);
+    w.queue[0] = dalloc<uint2>(own, capacity, st);
+    w.queue[1] = dalloc<uint2>(own, capacity, st);
+    w.capacity = capacity;
+    w.n = n;
+    const u32 init[8] = {1, 0, 1, 0, 0, 0, 0, 0}; // the root is wide node 0, queued at level 0
+    const uint2 root = make_uint2(0, 0);
+    RP_CHECK(cudaMemcpyAsync(w.counters, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    RP_CHECK(cudaMemcpyAsync(w.queue[0], &root, sizeof(root), cudaMemcpyHostToDevice, st));
+    for (u32 level = 0; level < s->tree_levels; ++level) {
+        const int parity = int(level & 1);
+        RP_CHECK(cudaMemsetAsync(w.counters + 2 + (parity ^ 1), 0, sizeof(u32), st));
+        k_wide_level<<<grid_for(s->sm_count, n, 128, 8), 128, 0, st>>>(w, parity, level);
+    }
+    RP_CHECK(cudaGetLastError());
+    u32 result[8];
+    RP_CHECK(cudaMemcpyAsync(result, w.counters, sizeof(result), cudaMemcpyDeviceToHost, st));
+    RP_CHECK(cudaStreamSynchronize(st));
+    if (result[4] || result[1] != n || result[0] > capacity)
+        throw Invalid{"wide BVH collapse did not place every triangle once"};
+    s->ds.wnode_count = result[0];
+    s->wide_levels = result[5];
+}
+
 // Second half: Morton codes, radix sort, Karras topology, refit, the traversal layout and the
 // structural check (k_tree_refs / k_tree_verify), then one wait for the whole build.
 void build_finish(rp_scene *s, const int (&cb)[12]) {
@@ -963,6 +1026,7 @@ void build_finish(rp_scene *s, const int (&cb)[12]) {
     if (result[0] & kBuildTree)
         throw Invalid{"LBVH build produced an invalid tree"};
     s->tree_levels = result[1];
+    build_wide(s);
 }
 
 } // namespace

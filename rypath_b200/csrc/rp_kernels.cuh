@@ -69,7 +69,7 @@ constexpr u32 kHitInvalid = 0xfffffffeu, kHitExhausted = 0xfffffffdu, kHitArithm
 // `prim` to the primitive or failure code to record.
 template <bool Count, int Stack>
 __device__ __noinline__ u32 resolve_hit(const DeviceScene &s, const PathPool &pool, u32 path, V3 ro, V3 rd, Hit &h,
-                                        u32 &prim, u32 *stack, int stride, u32 boundary_limit, u32 &nodes, u32 &tris,
+                                        u32 &prim, uint2 *stack, int stride, u32 boundary_limit, u32 &nodes, u32 &tris,
                                         u32 &rays) {
     u32 crossings = 0;
     bool moved = false;
@@ -140,7 +140,7 @@ __device__ __noinline__ u32 resolve_hit(const DeviceScene &s, const PathPool &po
 template <bool Count, int Block = kTraceBlock, int Stack = kStackDepth, bool Resolve = false>
 __global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1)
     k_trace(const __grid_constant__ DeviceScene s, PathPool pool, int in, u32 boundary_limit) {
-    __shared__ u32 stack[Stack * Block];
+    __shared__ uint2 stack[Stack * Block];
     const u32 count = pool.counters[in];
     const u32 *queue = pool.queue[in];
     u32 nodes = 0, tris = 0, rays = 0;
@@ -625,7 +625,7 @@ __global__ void __launch_bounds__(Block, 384 / Block) k_shade(const __grid_const
 // the failed sample's status (3 invalid hit, 2 invalid arithmetic, 4 boundary exhaustion).
 template <bool Count, int Stack>
 __device__ __noinline__ u32 pass_through_visible(const DeviceScene &s, V3 o, V3 d, float tmax, float4 target4,
-                                                 bool &occluded, u32 *stack, int stride, u32 boundary_limit,
+                                                 bool &occluded, uint2 *stack, int stride, u32 boundary_limit,
                                                  u32 &nodes, u32 &tris, u32 &rays) {
     const V3 target = v3(target4.x, target4.y, target4.z);
     occluded = true;
@@ -661,7 +661,7 @@ __device__ __noinline__ u32 pass_through_visible(const DeviceScene &s, V3 o, V3 
 template <bool Count, int Block = kTraceBlock, bool Adjoint = false, int Stack = kStackDepth, bool Resolve = false>
 __global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1)
     k_shadow(const __grid_constant__ DeviceScene s, PathPool pool, u32 boundary_limit) {
-    __shared__ u32 stack[Stack * Block];
+    __shared__ uint2 stack[Stack * Block];
     extern __shared__ float sgrad[]; // adjoint only
     if (Adjoint)
         adjoint_begin(pool, sgrad);

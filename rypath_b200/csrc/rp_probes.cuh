@@ -126,7 +126,7 @@ __global__ void k_probe_raygen(const __grid_constant__ DeviceScene s, const __gr
 }
 __global__ void __launch_bounds__(kTraceBlock) k_probe_trace(const __grid_constant__ DeviceScene s, const float *rays,
                                                              u32 count, int any_hit, float *hits) {
-    __shared__ u32 stack[kStackDepth * kTraceBlock];
+    __shared__ uint2 stack[kStackDepth * kTraceBlock];
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count)
         return;

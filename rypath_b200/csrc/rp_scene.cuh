@@ -66,6 +66,21 @@ struct __align__(16) BNode {
     uint4 d;  // left, right, unused, unused
 };
 
+// Compressed 8-wide BVH node (80 bytes).  Child k's box is bounded per axis by the planes
+// p + q 2^e of its 8-bit lo and hi bytes q (the builder widens q until the planes, in real
+// arithmetic, enclose the child's box).  Internal children are stored
+// contiguously from child_base and leaf triangles from tri_base, each in slot order; slot bit a
+// is set when the child's centre lies on the positive side of the node's centre along axis a,
+// so a ray visits hit children in the order slot ^ (its direction's negative-axis bits): near
+// side first.
+struct __align__(16) WNode {
+    float4 origin;  // p.x, p.y, p.z; w bits: biased exponents e.x, e.y, e.z (bytes 0-2), internal mask (byte 3)
+    uint4 links;    // child_base, tri_base, leaf mask, unused
+    uint4 q0;       // lo.x[0..7], lo.y[0..7]
+    uint4 q1;       // lo.z[0..7], hi.x[0..7]
+    uint4 q2;       // hi.y[0..7], hi.z[0..7]
+};
+
 struct DeviceScene {
     const float *positions;
     const float *normals;
@@ -78,6 +93,9 @@ struct DeviceScene {
     u32 prim_count;
     const BNode *nodes;
     const float4 *leaf_v; // 3 per leaf slot: world v0 (w = prim id bits), v1, v2
+    const WNode *wnodes;  // traversal tree (root 0)
+    const float4 *wtri;   // 3 per wide leaf, in the wide nodes' tri_base order
+    u32 wnode_count;
     const unsigned char *tri_family; // BSDF family of each triangle's material
     const DMaterial *materials;
     u32 material_count;
@@ -682,19 +700,15 @@ struct Hit {
     u32 prim;
 };
 
-// Stack depth for traversal; deeper trees report an invalid hit.  The wavefront walks use
-// kShortStack entries when every root-to-leaf path of the built tree has at most that many
-// internal nodes (a walk never holds more entries than that), freeing shared memory for more
-// resident warps.
-constexpr int kStackDepth = 64, kShortStack = 40;
+// Traversal stack entries (node groups) per thread.  A walk holds at most one entry per level
+// of the wide tree, so the wavefront walks take kShortStack entries when the built tree has at
+// most that many levels, and kStackDepth otherwise (deeper trees report an invalid hit).
+constexpr int kStackDepth = 40, kShortStack = 16;
 
-// Outcome of one node visit of a walk.
-enum WalkStep : int { kWalkMore = 0, kWalkDone = 1, kWalkFailed = 2 };
-
-// Closest-hit triangle test of leaf slot `slot`: keeps the minimum (t, primitive id).
+// Closest-hit triangle test of wide leaf `index`: keeps the minimum (t, primitive id).
 template <bool Count>
-RP_DEV void closest_leaf(const DeviceScene &s, const WalkRay &r, float tmax, Hit &h, u32 slot, u32 &tris_tested) {
-    const float4 a = __ldg(s.leaf_v + 3 * slot), b = __ldg(s.leaf_v + 3 * slot + 1), c = __ldg(s.leaf_v + 3 * slot + 2);
+RP_DEV void closest_leaf(const DeviceScene &s, const WalkRay &r, float tmax, Hit &h, u32 index, u32 &tris_tested) {
+    const float4 a = __ldg(s.wtri + 3 * index), b = __ldg(s.wtri + 3 * index + 1), c = __ldg(s.wtri + 3 * index + 2);
     const u32 prim = __float_as_uint(a.w);
     float t, b1, b2;
     if (Count)
@@ -707,57 +721,115 @@ RP_DEV void closest_leaf(const DeviceScene &s, const WalkRay &r, float tmax, Hit
         h.prim = prim;
     }
 }
-
-// One node visit of the closest-hit walk (prim_count >= 2): tests both children, the leaf
-// ones at once, and moves `node` to the nearer hit child, or pops the stack.  The walk starts
-// at node 0 with an empty stack; the visit order depends on the ray alone.
-template <bool Count, int Stack = kStackDepth>
-RP_DEV int closest_visit(const DeviceScene &s, const WalkRay &r, float tmax, Hit &h, u32 &node, int &sp, u32 *stack,
-                         int stride, u32 &nodes_visited, u32 &tris_tested) {
-    const BNode n = s.nodes[node];
+// Any-hit triangle test of wide leaf `index` in (0, tmax).
+template <bool Count>
+RP_DEV bool any_leaf(const DeviceScene &s, const WalkRay &r, float tmax, u32 index, u32 &tris_tested) {
+    const float4 a = __ldg(s.wtri + 3 * index), b = __ldg(s.wtri + 3 * index + 1), c = __ldg(s.wtri + 3 * index + 2);
+    float t, b1, b2;
     if (Count)
-        ++nodes_visited;
-    const float scale = s.slab_scale;
-    float tl, tr;
-    bool hl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, r.o, r.inv, h.t, scale, tl);
-    bool hr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, r.o, r.inv, h.t, scale, tr);
-    const u32 l = n.d.x, rc = n.d.y;
-    if (hl && (l & kLeaf)) {
-        closest_leaf<Count>(s, r, tmax, h, l & ~kLeaf, tris_tested);
-        hl = false;
-    }
-    if (hr && (rc & kLeaf)) {
-        closest_leaf<Count>(s, r, tmax, h, rc & ~kLeaf, tris_tested);
-        hr = false;
-    }
-    u32 next = kNone;
-    if (hl && hr) {
-        const bool right_first = tr < tl;
-        if (sp >= Stack)
-            return kWalkFailed;
-        stack[sp * stride] = right_first ? l : rc;
-        ++sp;
-        next = right_first ? rc : l;
-    } else if (hl)
-        next = l;
-    else if (hr)
-        next = rc;
-    if (next == kNone) {
-        if (sp == 0)
-            return kWalkDone;
-        --sp;
-        next = stack[sp * stride];
-    }
-    node = next;
-    return kWalkMore;
+        ++tris_tested;
+    return intersect_triangle(r, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tmax, t, b1, b2);
 }
 
-// Closest hit: minimises (t, primitive id) so the result is independent of visit order.
-// `stack` is this thread's slice of a shared-memory stack with stride `stride`.  A walk makes
-// at most prim_count visits (a binary tree over prim_count leaves has prim_count - 1 internal
-// nodes); a deeper stack than kStackDepth or more visits report a failed query.
+// The quantized planes of a wide node against a ray, in interval arithmetic.  Along an axis
+// the plane of byte q lies at p + q s (real arithmetic; the builder guarantees lo planes at
+// or below and hi planes at or above the child's box), and the ray reaches it at
+// t = (p - o) / d + q s / d.  With [a_lo, a_hi] containing (p - o) / d - 2^23 s / d and
+// [b_lo, b_hi] containing s / d, a lower bound of t is fmaf_rd(2^23 + q, b_lo, a_lo) and an upper
+// bound fmaf_ru(2^23 + q, b_hi, a_hi), where 2^23 + q is the float whose bits are 0x4b0000qq
+// (one byte permute).  A direction component of zero (or one whose reciprocal overflows) makes
+// that axis's bounds NaN or infinite in the direction that leaves the axis unconstrained; the
+// NaN-ignoring min and max then skip it, which is conservative.
+struct WideRay {
+    float a_lo[3], a_hi[3], b_lo[3], b_hi[3]; // per axis, for the node being visited
+    float rcp_lo[3], rcp_hi[3];                // directed-rounding bounds of 1 / d
+    u32 negative;                              // axis bits: d < 0 (the near plane is the hi one)
+};
+RP_DEV WideRay wide_ray(V3 d) {
+    WideRay w;
+    const float dd[3] = {d.x, d.y, d.z};
+    w.negative = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        w.rcp_lo[a] = __frcp_rd(dd[a]);
+        w.rcp_hi[a] = __frcp_ru(dd[a]);
+        w.negative |= (__float_as_uint(dd[a]) >> 31) << a;
+    }
+    return w;
+}
+// [lo, hi] bounds of x * y for x in [x_lo, x_hi] and y in [y_lo, y_hi] with y of one sign.
+RP_DEV void interval_mul(float x_lo, float x_hi, float y_lo, float y_hi, bool y_negative, float &lo, float &hi) {
+    if (!y_negative) {
+        lo = __fmul_rd(x_lo, x_lo >= 0 ? y_lo : y_hi);
+        hi = __fmul_ru(x_hi, x_hi >= 0 ? y_hi : y_lo);
+    } else {
+        lo = __fmul_rd(x_hi, x_hi >= 0 ? y_lo : y_hi);
+        hi = __fmul_ru(x_lo, x_lo >= 0 ? y_hi : y_lo);
+    }
+}
+RP_DEV float qfloat(u32 word, int byte) { return __uint_as_float(__byte_perm(word, 0x4b000000u, 0x7540u | u32(byte))); }
+
+// The children of a wide node whose boxes the ray's segment [0, tmax] may enter: internal ones
+// as bits at slot ^ order (near side first), leaves as bits at their slot.  Conservative: the
+// computed entry is at or below the true one and the exit at or above, so no child that holds
+// a hit in [0, tmax] is missed; all eight slots are tested without branches and masked.
+RP_DEV void wide_children(const WNode &n, V3 o, WideRay &w, float tmax, u32 order, u32 &inner, u32 &leaves) {
+    const u32 meta = __float_as_uint(n.origin.w);
+    const u32 imask = meta >> 24, lmask = n.links.z;
+    const float p[3] = {n.origin.x, n.origin.y, n.origin.z}, oo[3] = {o.x, o.y, o.z};
+    // byte words of each bound row: lo.x, lo.y, lo.z, hi.x, hi.y, hi.z (slots 0-3, 4-7)
+    const u32 rows[6][2] = {{n.q0.x, n.q0.y}, {n.q0.z, n.q0.w}, {n.q1.x, n.q1.y},
+                            {n.q1.z, n.q1.w}, {n.q2.x, n.q2.y}, {n.q2.z, n.q2.w}};
+    u32 near_w[3][2], far_w[3][2];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float s = __uint_as_float(((meta >> (8 * a)) & 0xffu) << 23);
+        const bool neg = (w.negative >> a) & 1u;
+        float d_lo, d_hi, c_lo, c_hi;
+        // (p - o) / d, then minus 2^23 s / d
+        interval_mul(__fsub_rd(p[a], oo[a]), __fsub_ru(p[a], oo[a]), w.rcp_lo[a], w.rcp_hi[a], neg, d_lo, d_hi);
+        w.b_lo[a] = __fmul_rd(s, w.rcp_lo[a]);
+        w.b_hi[a] = __fmul_ru(s, w.rcp_hi[a]);
+        c_lo = __fmaf_rd(-8388608.0f, w.b_hi[a], d_lo);
+        c_hi = __fmaf_ru(-8388608.0f, w.b_lo[a], d_hi);
+        w.a_lo[a] = c_lo;
+        w.a_hi[a] = c_hi;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            near_w[a][h] = neg ? rows[3 + a][h] : rows[a][h];
+            far_w[a][h] = neg ? rows[a][h] : rows[3 + a][h];
+        }
+    }
+    u32 hits = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int h = k >> 2, byte = k & 3;
+        float t0 = 0.0f, t1 = tmax;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            t0 = fmaxf(t0, __fmaf_rd(qfloat(near_w[a][h], byte), w.b_lo[a], w.a_lo[a]));
+            t1 = fminf(t1, __fmaf_ru(qfloat(far_w[a][h], byte), w.b_hi[a], w.a_hi[a]));
+        }
+        hits |= (t0 <= t1 ? 1u : 0u) << k;
+    }
+    leaves = hits & lmask;
+    u32 m = hits & imask; // to traversal order: bit k moves to k ^ order
+    if (order & 1u)
+        m = ((m & 0x55u) << 1) | ((m >> 1) & 0x55u);
+    if (order & 2u)
+        m = ((m & 0x33u) << 2) | ((m >> 2) & 0x33u);
+    if (order & 4u)
+        m = ((m & 0x0fu) << 4) | ((m >> 4) & 0x0fu);
+    inner = m;
+}
+
+// Closest hit: minimises (t, primitive id), so the result is independent of visit order.
+// `stack` is this thread's slice of a shared-memory stack with stride `stride`; an entry is a
+// node group: the parent's child_base and internal mask, and the hit children not yet
+// visited.  A walk visits each wide node at most once; a stack deeper than Stack reports a
+// failed query.
 template <bool Count, int Stack = kStackDepth>
-RP_DEV bool walk_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, u32 *stack, int stride,
+RP_DEV bool walk_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, uint2 *stack, int stride,
                          u32 &nodes_visited, u32 &tris_tested) {
     h.t = tmax;
     h.b1 = h.b2 = 0;
@@ -769,83 +841,61 @@ RP_DEV bool walk_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, u
         closest_leaf<Count>(s, r, tmax, h, 0, tris_tested);
         return true;
     }
+    const u32 order = (d.x < 0 ? 1u : 0u) | (d.y < 0 ? 2u : 0u) | (d.z < 0 ? 4u : 0u);
+    WideRay wr = wide_ray(d);
     int sp = 0;
     u32 node = 0;
-    for (u32 guard = 0; guard < s.prim_count; ++guard) {
-        const int step =
-            closest_visit<Count, Stack>(s, r, tmax, h, node, sp, stack, stride, nodes_visited, tris_tested);
-        if (step != kWalkMore)
-            return step == kWalkDone;
+    for (u32 guard = 0; guard <= s.wnode_count; ++guard) {
+        const WNode *np = s.wnodes + node;
+        WNode n;
+        n.origin = __ldg(&np->origin);
+        n.links = __ldg(&np->links);
+        n.q0 = __ldg(&np->q0);
+        n.q1 = __ldg(&np->q1);
+        n.q2 = __ldg(&np->q2);
+        if (Count)
+            ++nodes_visited;
+        u32 inner, leaves;
+        wide_children(n, o, wr, h.t, order, inner, leaves);
+        const u32 lmask = n.links.z;
+        while (leaves) {
+            const u32 k = __ffs(leaves) - 1;
+            leaves &= leaves - 1;
+            closest_leaf<Count>(s, r, tmax, h, n.links.y + __popc(lmask & ((1u << k) - 1)), tris_tested);
+        }
+        const u32 imask = __float_as_uint(n.origin.w) >> 24;
+        u32 base = n.links.x, group_mask = imask;
+        if (!inner) {
+            if (sp == 0)
+                return true;
+            const uint2 e = stack[(sp - 1) * stride];
+            base = e.x;
+            group_mask = e.y >> 8;
+            inner = e.y & 0xffu;
+            --sp;
+        }
+        const u32 b = __ffs(inner) - 1;
+        inner &= inner - 1;
+        const u32 slot = b ^ order;
+        node = base + __popc(group_mask & ((1u << slot) - 1));
+        if (inner) {
+            if (sp >= Stack)
+                return false;
+            stack[sp * stride] = make_uint2(base, (group_mask << 8) | inner);
+            ++sp;
+        }
     }
     return false;
 }
 template <bool Count>
-RP_DEV bool trace_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, u32 *stack, int stride,
+RP_DEV bool trace_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, uint2 *stack, int stride,
                           u32 &nodes_visited, u32 &tris_tested) {
     return walk_closest<Count>(s, o, d, tmax, h, stack, stride, nodes_visited, tris_tested);
 }
 
-// Any-hit triangle test of leaf slot `slot` in (0, tmax).
-template <bool Count>
-RP_DEV bool any_leaf(const DeviceScene &s, const WalkRay &r, float tmax, u32 slot, u32 &tris_tested) {
-    const float4 a = __ldg(s.leaf_v + 3 * slot), b = __ldg(s.leaf_v + 3 * slot + 1), c = __ldg(s.leaf_v + 3 * slot + 2);
-    float t, b1, b2;
-    if (Count)
-        ++tris_tested;
-    return intersect_triangle(r, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tmax, t, b1, b2);
-}
-
-// One node visit of the any-hit walk (prim_count >= 2); kWalkDone with `occluded` set on the
-// first hit, or with it clear once the stack is empty.
+// Any hit in (0, tmax): the shadow-ray occlusion query, the same walk stopped at the first hit.
 template <bool Count, int Stack = kStackDepth>
-RP_DEV int any_visit(const DeviceScene &s, const WalkRay &r, float tmax, bool &occluded, u32 &node, int &sp,
-                     u32 *stack, int stride, u32 &nodes_visited, u32 &tris_tested) {
-    const BNode n = s.nodes[node];
-    if (Count)
-        ++nodes_visited;
-    const float scale = s.slab_scale;
-    float tl, tr;
-    bool hl = slab(n.a.x, n.a.y, n.a.z, n.a.w, n.b.x, n.b.y, r.o, r.inv, tmax, scale, tl);
-    bool hr = slab(n.b.z, n.b.w, n.c.x, n.c.y, n.c.z, n.c.w, r.o, r.inv, tmax, scale, tr);
-    const u32 l = n.d.x, rc = n.d.y;
-    if (hl && (l & kLeaf)) {
-        if (any_leaf<Count>(s, r, tmax, l & ~kLeaf, tris_tested)) {
-            occluded = true;
-            return kWalkDone;
-        }
-        hl = false;
-    }
-    if (hr && (rc & kLeaf)) {
-        if (any_leaf<Count>(s, r, tmax, rc & ~kLeaf, tris_tested)) {
-            occluded = true;
-            return kWalkDone;
-        }
-        hr = false;
-    }
-    u32 next = kNone;
-    if (hl && hr) {
-        if (sp >= Stack)
-            return kWalkFailed;
-        stack[sp * stride] = rc;
-        ++sp;
-        next = l;
-    } else if (hl)
-        next = l;
-    else if (hr)
-        next = rc;
-    if (next == kNone) {
-        if (sp == 0)
-            return kWalkDone;
-        --sp;
-        next = stack[sp * stride];
-    }
-    node = next;
-    return kWalkMore;
-}
-
-// Any hit in (0, tmax): the shadow-ray occlusion query.
-template <bool Count, int Stack = kStackDepth>
-RP_DEV bool walk_any(const DeviceScene &s, V3 o, V3 d, float tmax, bool &occluded, u32 *stack, int stride,
+RP_DEV bool walk_any(const DeviceScene &s, V3 o, V3 d, float tmax, bool &occluded, uint2 *stack, int stride,
                      u32 &nodes_visited, u32 &tris_tested) {
     occluded = false;
     if (s.prim_count == 0)
@@ -855,18 +905,57 @@ RP_DEV bool walk_any(const DeviceScene &s, V3 o, V3 d, float tmax, bool &occlude
         occluded = any_leaf<Count>(s, r, tmax, 0, tris_tested);
         return true;
     }
+    const u32 order = (d.x < 0 ? 1u : 0u) | (d.y < 0 ? 2u : 0u) | (d.z < 0 ? 4u : 0u);
+    WideRay wr = wide_ray(d);
     int sp = 0;
     u32 node = 0;
-    for (u32 guard = 0; guard < s.prim_count; ++guard) {
-        const int step =
-            any_visit<Count, Stack>(s, r, tmax, occluded, node, sp, stack, stride, nodes_visited, tris_tested);
-        if (step != kWalkMore)
-            return step == kWalkDone;
+    for (u32 guard = 0; guard <= s.wnode_count; ++guard) {
+        const WNode *np = s.wnodes + node;
+        WNode n;
+        n.origin = __ldg(&np->origin);
+        n.links = __ldg(&np->links);
+        n.q0 = __ldg(&np->q0);
+        n.q1 = __ldg(&np->q1);
+        n.q2 = __ldg(&np->q2);
+        if (Count)
+            ++nodes_visited;
+        u32 inner, leaves;
+        wide_children(n, o, wr, tmax, order, inner, leaves);
+        const u32 lmask = n.links.z;
+        while (leaves) {
+            const u32 k = __ffs(leaves) - 1;
+            leaves &= leaves - 1;
+            if (any_leaf<Count>(s, r, tmax, n.links.y + __popc(lmask & ((1u << k) - 1)), tris_tested)) {
+                occluded = true;
+                return true;
+            }
+        }
+        const u32 imask = __float_as_uint(n.origin.w) >> 24;
+        u32 base = n.links.x, group_mask = imask;
+        if (!inner) {
+            if (sp == 0)
+                return true;
+            const uint2 e = stack[(sp - 1) * stride];
+            base = e.x;
+            group_mask = e.y >> 8;
+            inner = e.y & 0xffu;
+            --sp;
+        }
+        const u32 b = __ffs(inner) - 1;
+        inner &= inner - 1;
+        const u32 slot = b ^ order;
+        node = base + __popc(group_mask & ((1u << slot) - 1));
+        if (inner) {
+            if (sp >= Stack)
+                return false;
+            stack[sp * stride] = make_uint2(base, (group_mask << 8) | inner);
+            ++sp;
+        }
     }
     return false;
 }
 template <bool Count>
-RP_DEV bool trace_any(const DeviceScene &s, V3 o, V3 d, float tmax, bool &occluded, u32 *stack, int stride,
+RP_DEV bool trace_any(const DeviceScene &s, V3 o, V3 d, float tmax, bool &occluded, uint2 *stack, int stride,
                       u32 &nodes_visited, u32 &tris_tested) {
     return walk_any<Count>(s, o, d, tmax, occluded, stack, stride, nodes_visited, tris_tested);
 }

@@ -931,11 +931,11 @@ RP_DEV uint4 scalar_record(const ScalarPath &path) {
 // connection -- at a single call site, then the path event or the connection step.  A thread
 // whose path finished takes the next lane (one atomic per warp), so warps stay full until
 // the wave's lanes run out.
-template <bool Count>
+template <bool Count, int Stack = kStackDepth>
 __global__ void __launch_bounds__(kTraceBlock) k_volpath(const __grid_constant__ DeviceScene s,
                                                          const __grid_constant__ WaveParams p, ScalarParams q) {
-    __shared__ u32 stack[kStackDepth * kTraceBlock];
-    u32 *my_stack = stack + threadIdx.x;
+    __shared__ uint2 stack[Stack * kTraceBlock];
+    uint2 *my_stack = stack + threadIdx.x;
     const int lane_in_warp = threadIdx.x & 31;
     u32 counts[6] = {0, 0, 0, 0, 0, 0};
     ScalarPath path;
@@ -989,7 +989,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_volpath(const __grid_constant__
         }
         Hit hit;
         u32 nodes = 0, tris = 0;
-        const bool ok = trace_closest<Count>(s, ro, rd, tmax, hit, my_stack, kTraceBlock, nodes, tris);
+        const bool ok = walk_closest<Count, Stack>(s, ro, rd, tmax, hit, my_stack, kTraceBlock, nodes, tris);
         if (Count) {
             if (mode == kEventPath) {
                 counts[0] += nodes;
