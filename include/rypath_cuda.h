@@ -406,6 +406,18 @@ rp_status rp_cuda_probe_bsdf(const float *queries, uint32_t count, float *result
 rp_status rp_cuda_scene_export_bvh(struct rp_scene *scene, uint32_t *nodes, uint32_t *leaf_order,
                                    uint64_t *keys, float *bounds, size_t capacity, char *diag,
                                    size_t diag_capacity);
+/* Export the compressed 8-wide traversal tree the walks use: *node_count 80-byte nodes into
+ * `nodes` (when node_capacity suffices) and the n wide leaves (3 x 4 floats each: v0 with the
+ * triangle id's bits in w, v1, v2) into `triangles`.  Node layout (little endian): p[3] floats,
+ * then bytes e.x, e.y, e.z (biased exponents of the plane steps) and the internal-child mask;
+ * child_base, tri_base, leaf mask, unused (u32 each); then the 8 child slots' bytes of lo.x,
+ * lo.y, lo.z, hi.x, hi.y, hi.z.  Child k's box lies within the planes p + q 2^(e - 127) of
+ * its bytes; internal children are nodes child_base + (internal children before slot k),
+ * leaves are tri_base + (leaves before slot k).  No counterpart in rypath (Metal's
+ * acceleration structure is opaque). */
+rp_status rp_cuda_scene_export_wide(struct rp_scene *scene, void *nodes, size_t node_capacity, float *triangles,
+                                    size_t triangle_capacity, uint32_t *node_count, char *diag,
+                                    size_t diag_capacity);
 /* Closest-hit (any_hit == 0) or occlusion (any_hit == 1) queries for host rays
  * {origin[3], direction[3], tmax} (7 floats each) -> {t, b1, b2, primitive bits} (4 floats;
  * primitive RP_NONE bits = miss).  For occlusion only field 0 (1 = occluded) is used. */

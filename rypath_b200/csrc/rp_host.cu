@@ -2443,6 +2443,23 @@ rp_status rp_cuda_probe_raygen(rp_scene *s, const rp_request *request, uint32_t 
     });
 }
 
+rp_status rp_cuda_scene_export_wide(rp_scene *s, void *nodes, size_t node_capacity, float *triangles,
+                                    size_t triangle_capacity, uint32_t *node_count, char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!s || !node_count)
+            throw Invalid{"null argument"};
+        *node_count = s->ds.wnode_count;
+        if (node_capacity < s->ds.wnode_count || triangle_capacity < s->n)
+            throw Invalid{"capacity too small"};
+        RP_CHECK(cudaSetDevice(s->device));
+        if (s->ds.wnode_count)
+            RP_CHECK(cudaMemcpy(nodes, s->ds.wnodes, size_t(s->ds.wnode_count) * sizeof(WNode), cudaMemcpyDeviceToHost));
+        if (s->n)
+            RP_CHECK(cudaMemcpy(triangles, s->ds.wtri, size_t(s->n) * 3 * sizeof(float4), cudaMemcpyDeviceToHost));
+        return RP_SUCCESS;
+    });
+}
+
 rp_status rp_cuda_scene_export_bvh(rp_scene *s, uint32_t *nodes, uint32_t *leaf_order, uint64_t *keys, float *bounds,
                                    size_t capacity, char *diag, size_t cap) {
     return guarded(diag, cap, [&]() -> rp_status {

@@ -272,6 +272,20 @@ class CudaRenderScene:
         native.check(st, diag, "rp_cuda_scene_export_bvh")
         return nodes, order, keys, bounds
 
+    def export_wide(self, n: int):
+        """The compressed 8-wide traversal tree: (80-byte node records as a uint8 array of shape
+        (nodes, 80), wide leaves as float32 (n, 3, 4))."""
+        count = C.c_uint32()
+        diag = C.create_string_buffer(512)
+        tris = np.zeros((max(n, 1), 3, 4), np.float32)
+        st = native.lib().rp_cuda_scene_export_wide(self._handle, None, 0, tris.ctypes.data, n, C.byref(count), diag,
+                                                     512)
+        nodes = np.zeros((max(count.value, 1), 80), np.uint8)
+        st = native.lib().rp_cuda_scene_export_wide(self._handle, nodes.ctypes.data, count.value, tris.ctypes.data, n,
+                                                     C.byref(count), diag, 512)
+        native.check(st, diag, "rp_cuda_scene_export_wide")
+        return nodes[:count.value], tris[:n]
+
     def trace(self, rays: np.ndarray, any_hit: bool = False) -> np.ndarray:
         rays = np.ascontiguousarray(rays, np.float32)
         hits = np.zeros((rays.shape[0], 4), np.float32)
