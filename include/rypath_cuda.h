@@ -226,7 +226,9 @@ typedef struct rp_film_request {
     uint32_t sampler_kind, randomization;
     uint32_t emergency_limit;
     uint64_t total_samples; /* the render's sample budget; 0 = sample_begin + sample_count */
+    uint32_t flags;         /* RP_FILM_FRESH: the film starts from zero, its contents are not read */
 } rp_film_request;
+enum { RP_FILM_FRESH = 1 };
 
 /* Kernel-level timing of the last call on a scene (CUDA events on the scene stream). */
 typedef struct rp_timing {

@@ -129,7 +129,10 @@ class FilmPixel(C.Structure):
 class FilmRequest(C.Structure):
     _fields_ = [("width", u32), ("height", u32), ("seed", u64), ("sample_begin", u64),
                 ("sample_count", u64), ("batch_size", u64), ("sampler_kind", u32),
-                ("randomization", u32), ("emergency_limit", u32), ("total_samples", u64)]
+                ("randomization", u32), ("emergency_limit", u32), ("total_samples", u64), ("flags", u32)]
+
+
+FILM_FRESH = 1
 
 
 class View(C.Structure):
@@ -191,7 +194,7 @@ EXPECTED_SIZES = {
     "rp_area_emission": (AreaEmission, 1888), "rp_positional_light": (PositionalLight, 1948),
     "rp_medium": (Medium, 5656), "rp_camera": (Camera, 48), "rp_request": (Request, 64),
     "rp_packet_result": (PacketResult, 80), "rp_scalar_result": (ScalarResult, 44),
-    "rp_film_pixel": (FilmPixel, 96), "rp_film_request": (FilmRequest, 64),
+    "rp_film_pixel": (FilmPixel, 96), "rp_film_request": (FilmRequest, 72),
     "rp_view": (View, 80), "rp_batch_config": (BatchConfig, 24), "rp_batch_request": (BatchRequest, 48),
-    "rp_adjoint_request": (AdjointRequest, 80),
+    "rp_adjoint_request": (AdjointRequest, 88),
 }

@@ -15,6 +15,8 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <map>
+#include <mutex>
 #include <numbers>
 #include <string>
 #include <vector>
@@ -456,6 +458,20 @@ std::string gaussian_table(float xr, float yr, float sigma, GaussianTable &g) {
 // ---------------------------------------------------------------- device buffers
 // Device memory comes from the device's stream-ordered pool, configured to keep freed memory
 // for reuse by the next scene or pool in this process (no trip to the driver per render job).
+// cudaGetDeviceProperties queries every property (milliseconds); scene creation asks once per
+// device and process.
+const cudaDeviceProp &device_properties(int device) {
+    static std::mutex mutex;
+    static std::map<int, cudaDeviceProp> cache;
+    std::lock_guard<std::mutex> lock(mutex);
+    auto it = cache.find(device);
+    if (it == cache.end()) {
+        cudaDeviceProp prop;
+        RP_CHECK(cudaGetDeviceProperties(&prop, device));
+        it = cache.emplace(device, prop).first;
+    }
+    return it->second;
+}
 void retain_pool(int device) {
     static bool configured[64] = {};
     if (device >= 0 && device < 64 && !configured[device]) {
@@ -1042,8 +1058,7 @@ rp_status rp_cuda_device_info(int device, rp_device_info *info, char *diag, size
         }
         if (device < 0 || device >= count)
             throw Invalid{"device index out of range"};
-        cudaDeviceProp prop;
-        RP_CHECK(cudaGetDeviceProperties(&prop, device));
+        const cudaDeviceProp &prop = device_properties(device);
         if (info) {
             memset(info, 0, sizeof(*info));
             snprintf(info->name, sizeof(info->name), "%s", prop.name);
@@ -1163,9 +1178,7 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
         const auto t_begin = std::chrono::steady_clock::now();
         s = new rp_scene();
         s->device = device;
-        cudaDeviceProp prop;
-        RP_CHECK(cudaGetDeviceProperties(&prop, device));
-        s->sm_count = prop.multiProcessorCount;
+        s->sm_count = device_properties(device).multiProcessorCount;
         RP_CHECK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
         cudaStream_t stm = s->stream;
         auto &own = s->owned;
@@ -1732,8 +1745,11 @@ static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel 
                 s->film_stage_pixels = pixels;
             }
             committed = s->film_stage + pixels;
-            RP_CHECK(cudaMemcpyAsync(committed, film, size_t(pixels) * sizeof(rp_film_pixel), cudaMemcpyHostToDevice,
-                                     s->stream));
+            if (r->flags & RP_FILM_FRESH)
+                RP_CHECK(cudaMemsetAsync(committed, 0, size_t(pixels) * sizeof(rp_film_pixel), s->stream));
+            else
+                RP_CHECK(cudaMemcpyAsync(committed, film, size_t(pixels) * sizeof(rp_film_pixel),
+                                         cudaMemcpyHostToDevice, s->stream));
         } else if (s->film_stage_pixels < pixels) {
             if (s->film_stage)
                 cudaFreeAsync(s->film_stage, s->stream);
@@ -1742,6 +1758,8 @@ static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel 
             s->film_stage_pixels = pixels;
         }
         rp_film_pixel *staged = s->film_stage;
+        if (!host && (r->flags & RP_FILM_FRESH))
+            RP_CHECK(cudaMemsetAsync(committed, 0, size_t(pixels) * sizeof(rp_film_pixel), s->stream));
         if (s->counting)
             RP_CHECK(cudaMemsetAsync(s->stats, 0, 8 * sizeof(unsigned long long), s->stream));
         u64 done = 0;

@@ -183,15 +183,21 @@ class CudaRenderScene:
             native.check(native.lib().rp_cuda_set_cie(self._handle, cie.ctypes.data), None, "rp_cuda_set_cie")
             self._cie_set = True
 
-    def render_film(self, settings: RenderSettings, film: np.ndarray | None = None, sample_begin: int = 0):
-        """Progressive render into a host film (structured rp_film_pixel array)."""
+    def render_film(self, settings: RenderSettings, film: np.ndarray | None = None, sample_begin: int = 0,
+                    fresh: bool = False):
+        """Progressive render into a host film (structured rp_film_pixel array).
+
+        The render accumulates onto ``film``'s committed state; with ``fresh`` (or no film given)
+        it starts from an empty film without reading or uploading ``film``."""
         self._ensure_cie()
         pixels = settings.width * settings.height
         if film is None:
-            film = np.zeros(pixels, abi.film_dtype())
+            film = np.empty(pixels, abi.film_dtype())
+            fresh = True
         r = abi.FilmRequest(width=settings.width, height=settings.height, seed=settings.seed,
                             sample_begin=sample_begin, sample_count=settings.samples, batch_size=settings.batch_size,
-                            sampler_kind=settings.sampler, randomization=settings.randomization, emergency_limit=1024)
+                            sampler_kind=settings.sampler, randomization=settings.randomization, emergency_limit=1024,
+                            flags=abi.FILM_FRESH if fresh else 0)
         diag = C.create_string_buffer(512)
         st = native.lib().rp_cuda_render_film(self._handle, C.byref(r), film.ctypes.data, diag, 512)
         return st, diag.value.decode(errors="replace"), film
@@ -331,12 +337,13 @@ def film_mean(film: np.ndarray) -> np.ndarray:
 
 
 def render_progressive(scene: scenes.Scene, settings: RenderSettings, device: int = 0,
-                       film: np.ndarray | None = None):
+                       film: np.ndarray | None = None, fresh: bool = False):
     """render_progressive (src/render_driver.cpp:287-316): build, then render every batch into
-    ``film`` (a host rp_film_pixel array holding the committed state; zeros for a new render)."""
+    ``film`` (a host rp_film_pixel array holding the committed state; ``fresh`` starts a new
+    render without reading it)."""
     built = build_renderer(scene, device)
     if built.status != abi.RP_SUCCESS:
         return built.status, built.diagnostic, None
-    st, diag, film = built.scene.render_film(settings, film)
+    st, diag, film = built.scene.render_film(settings, film, fresh=fresh)
     built.scene.close()
     return st, diag, film
