@@ -115,15 +115,23 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def trace_profile():
+    """Figures of k_trace from the committed ncu summary (DRAM and L2 bytes per closest-hit ray,
+    issue activity, SIMD efficiency, L2 throughput), keyed as in the summary; {} if absent."""
+    path = os.path.join(ROOT, "profiles", "k_trace_mixed.md")
+    figures = {}
+    if os.path.exists(path):
+        for line in open(path):
+            key, sep, value = line.partition(":")
+            if sep and key in ("dram_bytes_per_ray", "l2_bytes_per_ray", "issue_active_pct", "simd_efficiency",
+                               "l2_throughput_pct"):
+                figures[key] = float(value)
+    return figures
+
+
 def traffic_per_ray():
     """DRAM bytes per closest-hit ray of k_trace from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "k_trace_mixed.md")
-    if not os.path.exists(path):
-        return None
-    for line in open(path):
-        if line.startswith("dram_bytes_per_ray:"):
-            return float(line.split(":")[1])
-    return None
+    return trace_profile().get("dram_bytes_per_ray")
 
 
 def cpu_baseline(orc, args, seconds, threads=0):
@@ -443,7 +451,9 @@ def main():
                          "traffic": (tpr * rays / max(1, counts.trace_launches)) if tpr else None,
                          "algorithmic_bytes_per_launch": trace_bytes_per_step / max(1, counts.trace_launches),
                          "algorithmic_bytes_per_ray": algo_per_ray, "peak_kind": peak_kind,
-                         "avg_launch_ms": trace_ms / max(1, trace_launches)},
+                         "avg_launch_ms": trace_ms / max(1, trace_launches),
+                         # the same kernel's ncu figures (profiles/k_trace_mixed.md): it is issue-bound
+                         "ncu": dict(trace_profile(), source="profiles/k_trace_mixed.md")},
             "kernel_share": shares,
             "rays_per_step": {"closest": counts.closest_rays, "shadow": counts.shadow_rays},
             "mrays_per_s": (counts.closest_rays + counts.shadow_rays) * len(steps) / (total_ms / 1e3) / 1e6,
