@@ -185,7 +185,7 @@ def run_reference(args, rank):
 def bench_fog(torch, cpu_seconds):
     """Scalar volpath: the Cornell-style box filled with a homogeneous medium (sigma_s mean 0.5,
     albedo 0.9, HG g = 0.7), 1024x1024, 64 spp, depth 32, one wavelength per sample."""
-    from rypath_b200 import renderer, scenes
+    from rypath_b200 import abi, renderer, scenes
 
     from tests.oracle_lib import OracleScene, request
 
@@ -228,14 +228,14 @@ def bench_views(torch):
     """Batched form: 64 seeded views of the mixed scene (resolutions U[256x256, 1280x720],
     spp from {4, 8, 16, 32, 64}) in one wavefront with graph replay and tuned shapes, against
     one plain wavefront per view; both films are compared bit for bit."""
-    from rypath_b200 import renderer, scenes
+    from rypath_b200 import abi, renderer, scenes
 
     scene = scenes.mixed_scene(64, 64, 1, 16)
     views = scenes.view_batch(scene, count=64, seed=1)
     total = renderer.pack_views(views)
     lanes = sum(v.width * v.height * v.sample_count for v in views)
     rs = renderer.build_renderer(scene).scene
-    film = torch.zeros(total * 96, dtype=torch.uint8, device="cuda")
+    film = torch.zeros(total * abi.FILM_PIXEL_BYTES, dtype=torch.uint8, device="cuda")
     t0 = time.perf_counter()
     chosen = rs.tune_views(views, renderer.BatchRequest())
     tune_s = time.perf_counter() - t0
@@ -253,7 +253,7 @@ def bench_views(torch):
     plain_ms = 0.0
     for v in views:
         one = renderer.View(v.camera, v.width, v.height, v.sample_begin, v.sample_count, 0)
-        sub = film[v.film_offset * 96:(v.film_offset + v.width * v.height) * 96]
+        sub = film[v.film_offset * abi.FILM_PIXEL_BYTES:(v.film_offset + v.width * v.height) * abi.FILM_PIXEL_BYTES]
         rs.render_views_device([one], plain_req, sub.data_ptr())
         plain_ms += rs.timing().total_ms
     identical = bool(torch.equal(batched, film))
@@ -274,7 +274,7 @@ def bench_adjoint(torch, adam_steps):
     32 spp, depth 8, L2 loss on film-mean XYZ against a 128-spp render of seeded true
     spectra.  The path-replay adjoint gradient against central differences (h = 1e-3, common
     random numbers) of the same renders; errors against an 8x-spp adjoint gradient."""
-    from rypath_b200 import renderer, scenes
+    from rypath_b200 import abi, renderer, scenes
 
     w, spp, params = 512, 32, 512
     scene, truth = scenes.cornell_groups(w, w, spp, 8)
@@ -283,10 +283,11 @@ def bench_adjoint(torch, adam_steps):
     rt = renderer.build_renderer(truth).scene
 
     def mean(r, n, seed):
-        film = torch.zeros(w * w * 12, dtype=torch.float64, device="cuda")
+        doubles = abi.FILM_PIXEL_BYTES // 8
+        film = torch.zeros(w * w * doubles, dtype=torch.float64, device="cuda")
         r.render_film_device(renderer.RenderSettings(w, w, samples=n, batch_size=n, seed=seed), film.data_ptr())
         torch.cuda.synchronize()
-        f = film.reshape(w * w, 12)
+        f = film.reshape(w * w, doubles)
         return (f[:, 0:3] + f[:, 3:6]) / (f[:, 6:7] + f[:, 7:8]), r.timing().total_ms
 
     def adjoint(r, n, seed, g):
@@ -377,7 +378,7 @@ def main():
     if built.status != abi.RP_SUCCESS:
         raise SystemExit(f"build_renderer failed: {built.diagnostic}")
     rs = built.scene
-    film = torch.zeros(pixels * 12, dtype=torch.float64, device="cuda")  # rp_film_pixel is 96 bytes
+    film = torch.zeros(pixels * abi.FILM_PIXEL_BYTES // 8, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     # each rank's disjoint block of absolute samples: the counting render, warm-up and timed steps
     per_rank = args.spp * (args.warmup + args.steps + 1)
@@ -477,7 +478,7 @@ def main():
         film_host, keep_f = pinned(np.zeros(pixels, abi.film_dtype()))
         desc_bytes = (scene.positions.nbytes + scene.triangles.nbytes + scene.knots.nbytes +
                       len(scene.emissions) * 1888 + len(scene.positional) * 1948 + 234208 + 471 * 4)
-        film_bytes = pixels * 96
+        film_bytes = pixels * abi.FILM_PIXEL_BYTES
 
         def e2e_step(i):
             # a new render each step: the film starts empty on the device and is read back

@@ -209,12 +209,16 @@ typedef struct rp_device_info {
 
 /* Device film: per-pixel FP64 Neumaier sums in canonical (absolute sample, pixel) order,
  * the reduction PacketFilmBatch::add performs on the host (src/packet_film.cpp:198-265),
- * plus per-pixel second moments of the XYZ estimate for the 3-sigma statistics. */
+ * plus per-pixel second moments of the XYZ estimate for the 3-sigma statistics and, under a
+ * finite film clamp, the compatibility planes: the sums of the exposed XYZ scaled down to
+ * the maximum component (clamp_sensor, src/packet_film.cpp:39-47; FilmPixel,
+ * src/render.hpp:317-326). */
 typedef struct rp_film_pixel {
     double sum[3], correction[3];
     double weight_sum, weight_correction;
     double square[3];
     uint64_t count;
+    double compatibility_sum[3], compatibility_correction[3];
 } rp_film_pixel;
 
 /* Film request: render samples [sample_begin, sample_begin + sample_count) for every pixel,
@@ -227,6 +231,8 @@ typedef struct rp_film_request {
     uint32_t emergency_limit;
     uint64_t total_samples; /* the render's sample budget; 0 = sample_begin + sample_count */
     uint32_t flags;         /* RP_FILM_FRESH: the film starts from zero, its contents are not read */
+    double exposure;        /* Film::exposure, applied to the compatibility planes only */
+    double max_component_value; /* Film::max_component_value; 0 or infinity: no clamp, no compatibility planes */
 } rp_film_request;
 enum { RP_FILM_FRESH = 1 };
 
@@ -326,6 +332,7 @@ typedef struct rp_batch_request {
     uint64_t seed;
     uint32_t sampler_kind, randomization, emergency_limit;
     rp_batch_config config;
+    double exposure, max_component_value; /* the film clamp, as in rp_film_request */
 } rp_batch_request;
 
 /* Renders every view's samples into one device film (the views' pixels, in rp_film_pixel

@@ -54,6 +54,10 @@ void or_probe_light_select(const or_scene *scene, const float *queries, uint32_t
 /* Film reduction of packet results in canonical order (PacketFilmBatch::add). */
 int or_film_add(const rp_packet_result *results, size_t count, const double *cie_xyz,
                 uint32_t pixel_count, rp_film_pixel *film);
+/* The same with a finite film clamp: the compatibility planes of clamp_sensor
+ * (src/packet_film.cpp:39-47); max_component_value 0 or infinity: none. */
+int or_film_add_clamped(const rp_packet_result *results, size_t count, const double *cie_xyz,
+                        uint32_t pixel_count, double exposure, double max_component_value, rp_film_pixel *film);
 
 /* Gaussian pixel filter: the table of compile_gaussian_filter (src/gaussian_filter.cpp) and the
  * device inverse of shaders/render.metal:200-236 on count (u, v) pairs.  Returns the table

@@ -1044,8 +1044,17 @@ static void add_compensated(double value, double &sum, double &correction) {
     correction += std::abs(sum) >= std::abs(value) ? (sum - next) + value : (value - next) + sum;
     sum = next;
 }
+int or_film_add_clamped(const rp_packet_result *results, size_t count, const double *cie, uint32_t pixel_count,
+                        double exposure, double max_component_value, rp_film_pixel *film);
 int or_film_add(const rp_packet_result *results, size_t count, const double *cie, uint32_t pixel_count,
                 rp_film_pixel *film) {
+    return or_film_add_clamped(results, count, cie, pixel_count, 1.0, INFINITY, film);
+}
+// PacketFilmBatch::add (src/packet_film.cpp:198-265) without splats, with the compatibility
+// planes of a finite clamp (clamp_sensor, :39-47)
+int or_film_add_clamped(const rp_packet_result *results, size_t count, const double *cie, uint32_t pixel_count,
+                        double exposure, double max_component_value, rp_film_pixel *film) {
+    const bool clamp = std::isfinite(max_component_value) && max_component_value > 0;
     for (size_t i = 0; i < count; ++i) {
         const auto &s = results[i];
         if (s.pixel >= pixel_count)
@@ -1067,6 +1076,15 @@ int or_film_add(const rp_packet_result *results, size_t count, const double *cie
             const double v = xyz[c] * s.filter_weight;
             add_compensated(v, px.sum[c], px.correction[c]);
             px.square[c] += v * v;
+        }
+        if (clamp) {
+            double e[3] = {xyz[0] * exposure, xyz[1] * exposure, xyz[2] * exposure};
+            const double maximum = std::max(std::max(e[0], e[1]), e[2]);
+            if (maximum > max_component_value)
+                for (double &v : e)
+                    v *= max_component_value / maximum;
+            for (int c = 0; c < 3; ++c)
+                add_compensated(e[c] * s.filter_weight, px.compatibility_sum[c], px.compatibility_correction[c]);
         }
         add_compensated(s.filter_weight, px.weight_sum, px.weight_correction);
         ++px.count;

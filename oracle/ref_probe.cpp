@@ -237,10 +237,24 @@ void ref_probe_qmc(const int64_t *queries, uint32_t count, uint64_t *results) {
 }
 
 void ref_set_cie(const double *cie) { g_cie.assign(cie, cie + 3 * 471); }
+// PacketFilmBatch with a film clamp: per pixel sum[3], correction[3], weight sum, weight
+// correction, count, compatibility sum[3], compatibility correction[3] (15 doubles).
+int ref_film_add_clamped(const uint32_t *words, size_t count, uint32_t width, uint32_t height, double exposure,
+                         double max_component_value, double *out);
 int ref_film_add(const uint32_t *words, size_t count, uint32_t width, uint32_t height,
                  double *out_sum_weight_count) {
+    std::vector<double> full(size_t(width) * height * 15);
+    const int rc = ref_film_add_clamped(words, count, width, height, 1.0, INFINITY, full.data());
+    for (size_t p = 0; rc == 0 && p < size_t(width) * height; ++p)
+        std::memcpy(out_sum_weight_count + 9 * p, full.data() + 15 * p, 9 * sizeof(double));
+    return rc;
+}
+int ref_film_add_clamped(const uint32_t *words, size_t count, uint32_t width, uint32_t height, double exposure,
+                         double max_component_value, double *out) {
     rypath::RenderScene scene{};
     scene.model = rypath::RenderModel::pbrt;
+    scene.exposure = exposure;
+    scene.max_component_value = max_component_value;
     rypath::RenderSettings settings{};
     settings.width = width;
     settings.height = height;
@@ -266,10 +280,12 @@ int ref_film_add(const uint32_t *words, size_t count, uint32_t width, uint32_t h
         return -3;
     for (size_t p = 0; p < pixels; ++p) {
         const auto &px = film.pixels[p];
-        double *o = out_sum_weight_count + 9 * p;
+        double *o = out + 15 * p;
         for (int c = 0; c < 3; ++c) {
             o[c] = px.sum[c];
             o[3 + c] = px.correction[c];
+            o[9 + c] = px.compatibility_sum[c];
+            o[12 + c] = px.compatibility_correction[c];
         }
         o[6] = px.weight_sum;
         o[7] = px.weight_correction;

@@ -123,13 +123,15 @@ class DeviceInfo(C.Structure):
 
 class FilmPixel(C.Structure):
     _fields_ = [("sum", f64 * 3), ("correction", f64 * 3), ("weight_sum", f64),
-                ("weight_correction", f64), ("square", f64 * 3), ("count", u64)]
+                ("weight_correction", f64), ("square", f64 * 3), ("count", u64),
+                ("compatibility_sum", f64 * 3), ("compatibility_correction", f64 * 3)]
 
 
 class FilmRequest(C.Structure):
     _fields_ = [("width", u32), ("height", u32), ("seed", u64), ("sample_begin", u64),
                 ("sample_count", u64), ("batch_size", u64), ("sampler_kind", u32),
-                ("randomization", u32), ("emergency_limit", u32), ("total_samples", u64), ("flags", u32)]
+                ("randomization", u32), ("emergency_limit", u32), ("total_samples", u64), ("flags", u32),
+                ("exposure", C.c_double), ("max_component_value", C.c_double)]
 
 
 FILM_FRESH = 1
@@ -147,7 +149,7 @@ class BatchConfig(C.Structure):
 
 class BatchRequest(C.Structure):
     _fields_ = [("seed", u64), ("sampler_kind", u32), ("randomization", u32), ("emergency_limit", u32),
-                ("config", BatchConfig)]
+                ("config", BatchConfig), ("exposure", C.c_double), ("max_component_value", C.c_double)]
 
 
 class AdjointRequest(C.Structure):
@@ -186,7 +188,11 @@ def film_dtype():
     import numpy as np
 
     return np.dtype([("sum", "<f8", 3), ("correction", "<f8", 3), ("weight_sum", "<f8"),
-                     ("weight_correction", "<f8"), ("square", "<f8", 3), ("count", "<u8")])
+                     ("weight_correction", "<f8"), ("square", "<f8", 3), ("count", "<u8"),
+                     ("compatibility_sum", "<f8", 3), ("compatibility_correction", "<f8", 3)])
+
+
+FILM_PIXEL_BYTES = 144  # sizeof(rp_film_pixel)
 
 
 EXPECTED_SIZES = {
@@ -194,7 +200,7 @@ EXPECTED_SIZES = {
     "rp_area_emission": (AreaEmission, 1888), "rp_positional_light": (PositionalLight, 1948),
     "rp_medium": (Medium, 5656), "rp_camera": (Camera, 48), "rp_request": (Request, 64),
     "rp_packet_result": (PacketResult, 80), "rp_scalar_result": (ScalarResult, 44),
-    "rp_film_pixel": (FilmPixel, 96), "rp_film_request": (FilmRequest, 72),
-    "rp_view": (View, 80), "rp_batch_config": (BatchConfig, 24), "rp_batch_request": (BatchRequest, 48),
-    "rp_adjoint_request": (AdjointRequest, 88),
+    "rp_film_pixel": (FilmPixel, 144), "rp_film_request": (FilmRequest, 88),
+    "rp_view": (View, 80), "rp_batch_config": (BatchConfig, 24), "rp_batch_request": (BatchRequest, 64),
+    "rp_adjoint_request": (AdjointRequest, 104),
 }

@@ -84,7 +84,8 @@ __global__ void k_raygen_views(const __grid_constant__ DeviceScene s, const __gr
 
 // The current wave's samples reduced into the batch film, per view pixel in canonical order
 // (k_film), then the wave cursor advances.  film == nullptr: count failures only (tuning).
-__global__ void k_film_views(PathPool pool, Batch b, const double *cie, double weight, FilmPixel *film) {
+__global__ void k_film_views(PathPool pool, Batch b, const double *cie, double weight, FilmClamp clamp,
+                             FilmPixel *film) {
     const WaveDesc w = b.waves[*b.cursor];
     const unsigned long long first = w.lane_begin, last = w.lane_begin + w.lanes; // [first, last)
     // the views the wave overlaps are contiguous, and so are their film pixels
@@ -113,7 +114,7 @@ __global__ void k_film_views(PathPool pool, Batch b, const double *cie, double w
         for (unsigned long long si = s0; si < s1; ++si) {
             const u32 lane = u32(base + si * v.pixels - first);
             FilmPixel scratch{};
-            if (!film_add_lane(pool, lane, cie, weight, film ? f : scratch))
+            if (!film_add_lane(pool, lane, cie, weight, clamp, film ? f : scratch))
                 atomicAdd(b.cursor + 1, 1u);
         }
         if (film)

@@ -668,6 +668,17 @@ struct rp_scene {
 
 namespace {
 
+// The film clamp of a request: on for a finite positive maximum component (0 or infinity:
+// off); its exposure must then be finite and nonnegative (src/packet_film.cpp:151-160).
+FilmClamp film_clamp(double exposure, double max_component_value) {
+    FilmClamp c{exposure, max_component_value, max_component_value > 0 && std::isfinite(max_component_value)};
+    if (!(max_component_value >= 0) && !std::isinf(max_component_value))
+        throw Invalid{"film clamp must be positive (or 0 / infinity for none)"};
+    if (c.on && !(exposure >= 0 && std::isfinite(exposure)))
+        throw Invalid{"film exposure must be finite and nonnegative"};
+    return c;
+}
+
 WaveParams wave_params(const rp_request &r) {
     WaveParams p{};
     p.width = r.width;
@@ -1721,6 +1732,9 @@ static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel 
             throw Invalid{"null argument"};
         if (!r->width || !r->height || !r->sample_count || !r->batch_size)
             throw Invalid{"film request needs nonzero film size, samples and batch size"};
+        const FilmClamp clamp = film_clamp(r->exposure, r->max_component_value);
+        if (clamp.on && s && s->transport == RP_TRANSPORT_SCALAR)
+            throw Invalid{"BDPT and finite film clamping require packet or hero spectral transport"};
         const u32 pixels = r->width * r->height;
         RP_CHECK(cudaSetDevice(s->device));
         if (!s->cie) {
@@ -1801,7 +1815,8 @@ static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel 
                     run_wave(s, p);
                     s->mark(3);
                     k_film<<<grid_for(s->sm_count, pixels, 128, 16), 128, 0, s->stream>>>(
-                        s->pool, pixels, u32(spw), s->cie, double(s->ds.filter_weight), reinterpret_cast<FilmPixel *>(staged));
+                        s->pool, pixels, u32(spw), s->cie, double(s->ds.filter_weight), clamp,
+                        reinterpret_cast<FilmPixel *>(staged));
                     s->done();
                     RP_CHECK(cudaMemcpyAsync(&f, s->pool.counters + 3, 4, cudaMemcpyDeviceToHost, s->stream));
                 }
@@ -2090,7 +2105,7 @@ WaveParams batch_params(const rp_batch_request &r) {
 
 template <int TB, int SB>
 void batch_wave_kernels(rp_scene *s, const WaveParams &p, const Batch &b, u32 wave_lanes, u32 blocks_per_sm,
-                        FilmPixel *film) {
+                        const FilmClamp &clamp, FilmPixel *film) {
     PathPool &pool = s->pool;
     const int sms = s->sm_count;
     cudaStream_t st = s->stream;
@@ -2111,21 +2126,23 @@ void batch_wave_kernels(rp_scene *s, const WaveParams &p, const Batch &b, u32 wa
         launch_shadow<false, TB, false>(s, pool, trace_grid, 0, st, p.boundary_limit);
         in ^= 1;
     }
-    k_film_views<<<grid_for(sms, wave_lanes, 128, 16), 128, 0, st>>>(pool, b, s->cie, double(s->ds.filter_weight), film);
+    k_film_views<<<grid_for(sms, wave_lanes, 128, 16), 128, 0, st>>>(pool, b, s->cie, double(s->ds.filter_weight), clamp,
+                                                                       film);
     k_next_wave<<<1, 32, 0, st>>>(b);
     RP_CHECK(cudaGetLastError());
 }
 
-void batch_wave(rp_scene *s, const WaveParams &p, const Batch &b, const rp_batch_config &c, FilmPixel *film) {
+void batch_wave(rp_scene *s, const WaveParams &p, const Batch &b, const rp_batch_config &c, const FilmClamp &clamp,
+                FilmPixel *film) {
     const u32 w = c.wave_lanes, bpm = c.blocks_per_sm;
     if (c.trace_block == 64 && c.shade_block == 128)
-        batch_wave_kernels<64, 128>(s, p, b, w, bpm, film);
+        batch_wave_kernels<64, 128>(s, p, b, w, bpm, clamp, film);
     else if (c.trace_block == 64 && c.shade_block == 256)
-        batch_wave_kernels<64, 256>(s, p, b, w, bpm, film);
+        batch_wave_kernels<64, 256>(s, p, b, w, bpm, clamp, film);
     else if (c.trace_block == 128 && c.shade_block == 256)
-        batch_wave_kernels<128, 256>(s, p, b, w, bpm, film);
+        batch_wave_kernels<128, 256>(s, p, b, w, bpm, clamp, film);
     else
-        batch_wave_kernels<128, 128>(s, p, b, w, bpm, film);
+        batch_wave_kernels<128, 128>(s, p, b, w, bpm, clamp, film);
 }
 
 void check_config(const rp_batch_config &c) {
@@ -2172,6 +2189,7 @@ float run_batch(rp_scene *s, const BatchPlan &plan, const BatchBuffers &buf, con
                 const rp_batch_config &c, FilmPixel *film, size_t waves) {
     s->ensure_pool(c.wave_lanes);
     const WaveParams p = batch_params(r);
+    const FilmClamp clamp = film_clamp(r.exposure, r.max_component_value);
     const Batch b = buf.batch(plan);
     RP_CHECK(cudaMemsetAsync(buf.cursor, 0, 8, s->stream));
     cudaEvent_t start, stop;
@@ -2182,7 +2200,7 @@ float run_batch(rp_scene *s, const BatchPlan &plan, const BatchBuffers &buf, con
     if (c.use_graph != 2) {
         RP_CHECK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
         try {
-            batch_wave(s, p, b, c, film);
+            batch_wave(s, p, b, c, clamp, film);
         } catch (...) {
             cudaStreamEndCapture(s->stream, &graph);
             if (graph)
@@ -2197,7 +2215,7 @@ float run_batch(rp_scene *s, const BatchPlan &plan, const BatchBuffers &buf, con
         if (exec)
             RP_CHECK(cudaGraphLaunch(exec, s->stream));
         else
-            batch_wave(s, p, b, c, film);
+            batch_wave(s, p, b, c, clamp, film);
     }
     RP_CHECK(cudaEventRecord(stop, s->stream));
     RP_CHECK(cudaStreamSynchronize(s->stream));

@@ -761,6 +761,12 @@ struct FilmPixel {
     double weight_sum, weight_correction;
     double square[3];
     unsigned long long count;
+    double compatibility_sum[3], compatibility_correction[3];
+};
+// A finite film clamp (on: max_component_value finite and positive).
+struct FilmClamp {
+    double exposure, max_component_value;
+    bool on;
 };
 RP_DEV void add_compensated(double value, double &sum, double &correction) {
     const double next = __dadd_rn(sum, value);
@@ -770,7 +776,29 @@ RP_DEV void add_compensated(double value, double &sum, double &correction) {
 }
 // packet_sensor_xyz (src/packet_film.cpp:102-114) of one lane added to its pixel; false when
 // the lane failed (a failed lane fails its batch).
-RP_DEV bool film_add_lane(const PathPool &pool, u32 lane, const double *cie, double weight, FilmPixel &f) {
+// clamp_sensor + add_xyz into the compatibility planes (src/packet_film.cpp:39-56, :217-220)
+RP_DEV void film_add_compatibility(const double (&xyz)[3], double weight, const FilmClamp &c, FilmPixel &f) {
+    double v[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        v[k] = __dmul_rn(xyz[k], c.exposure);
+    double maximum = v[0];
+    if (v[1] > maximum)
+        maximum = v[1];
+    if (v[2] > maximum)
+        maximum = v[2];
+    if (maximum > c.max_component_value) {
+        const double scale = __ddiv_rn(c.max_component_value, maximum);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            v[k] = __dmul_rn(v[k], scale);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        add_compensated(__dmul_rn(v[k], weight), f.compatibility_sum[k], f.compatibility_correction[k]);
+}
+RP_DEV bool film_add_lane(const PathPool &pool, u32 lane, const double *cie, double weight, const FilmClamp &clamp,
+                          FilmPixel &f) {
     const uint4 id = pool.ident[lane];
     const u32 status = (id.w & F_COMPLETE) ? get_status(id.w) : 2u;
     if (status != 0)
@@ -797,6 +825,8 @@ RP_DEV bool film_add_lane(const PathPool &pool, u32 lane, const double *cie, dou
         add_compensated(v, f.sum[c], f.correction[c]);
         f.square[c] = __dadd_rn(f.square[c], __dmul_rn(v, v));
     }
+    if (clamp.on)
+        film_add_compatibility(xyz, weight, clamp, f);
     add_compensated(weight, f.weight_sum, f.weight_correction);
     ++f.count;
     return true;
@@ -811,11 +841,12 @@ __global__ void k_count_failures(PathPool pool, u32 lanes) {
     }
 }
 // Every sample of a wave reduced per pixel in canonical (absolute sample, pixel) order.
-__global__ void k_film(PathPool pool, u32 pixel_count, u32 samples, const double *cie, double weight, FilmPixel *film) {
+__global__ void k_film(PathPool pool, u32 pixel_count, u32 samples, const double *cie, double weight, FilmClamp clamp,
+                       FilmPixel *film) {
     for (u32 px = blockIdx.x * blockDim.x + threadIdx.x; px < pixel_count; px += gridDim.x * blockDim.x) {
         FilmPixel f = film[px];
         for (u32 si = 0; si < samples; ++si)
-            if (!film_add_lane(pool, si * pixel_count + px, cie, weight, f))
+            if (!film_add_lane(pool, si * pixel_count + px, cie, weight, clamp, f))
                 atomicAdd(pool.counters + 3, 1u);
         film[px] = f;
     }

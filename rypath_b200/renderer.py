@@ -78,6 +78,8 @@ class RenderSettings:
     seed: int = 1
     sampler: int = abi.SAMPLER_SOBOL
     randomization: int = abi.RANDOMIZE_OWEN
+    exposure: float = 1.0             # Film::exposure (compatibility planes only)
+    max_component_value: float = 0.0  # Film::max_component_value; 0 or inf: no clamp
 
 
 @dataclass
@@ -114,6 +116,8 @@ class BatchRequest:
     shade_block: int = 0    # 0: tuned
     blocks_per_sm: int = 0  # 0: tuned
     use_graph: int = 1      # 1: CUDA graph replay per wave, 2: direct launches
+    exposure: float = 1.0
+    max_component_value: float = 0.0  # 0 or inf: no film clamp
 
     def to_c(self) -> abi.BatchRequest:
         r = abi.BatchRequest()
@@ -122,6 +126,7 @@ class BatchRequest:
         c = r.config
         c.wave_lanes, c.trace_block, c.shade_block = self.wave_lanes, self.trace_block, self.shade_block
         c.blocks_per_sm, c.use_graph = self.blocks_per_sm, self.use_graph
+        r.exposure, r.max_component_value = self.exposure, self.max_component_value
         return r
 
 
@@ -197,7 +202,8 @@ class CudaRenderScene:
         r = abi.FilmRequest(width=settings.width, height=settings.height, seed=settings.seed,
                             sample_begin=sample_begin, sample_count=settings.samples, batch_size=settings.batch_size,
                             sampler_kind=settings.sampler, randomization=settings.randomization, emergency_limit=1024,
-                            flags=abi.FILM_FRESH if fresh else 0)
+                            flags=abi.FILM_FRESH if fresh else 0, exposure=settings.exposure,
+                            max_component_value=settings.max_component_value)
         diag = C.create_string_buffer(512)
         st = native.lib().rp_cuda_render_film(self._handle, C.byref(r), film.ctypes.data, diag, 512)
         return st, diag.value.decode(errors="replace"), film
@@ -329,10 +335,14 @@ def build_renderer(scene: scenes.Scene, device: int = 0) -> RenderBuildResult:
     return RenderBuildResult(st, "", CudaRenderScene(handle.value), info)
 
 
-def film_mean(film: np.ndarray) -> np.ndarray:
-    """Per-pixel XYZ mean, film_mean (src/packet_film.cpp:116-135) without splats or clamps."""
+def film_mean(film: np.ndarray, compatibility: bool = False) -> np.ndarray:
+    """Per-pixel XYZ mean, film_mean (src/packet_film.cpp:116-135) without splats; with
+    ``compatibility``, of the clamped compatibility planes."""
     weight = film["weight_sum"] + film["weight_correction"]
-    xyz = film["sum"] + film["correction"]
+    if compatibility:
+        xyz = film["compatibility_sum"] + film["compatibility_correction"]
+    else:
+        xyz = film["sum"] + film["correction"]
     return np.where(weight[:, None] > 0, xyz / np.where(weight > 0, weight, 1)[:, None], 0.0)
 
 

@@ -41,6 +41,7 @@ def oracle():
         lib.or_build_light_tables.argtypes = [vp, u32, vp, vp, vp, vp, vp]
         lib.or_probe_light_select.argtypes = [vp, vp, u32, vp]
         lib.or_film_add.argtypes = [vp, sz, vp, u32, vp]
+        lib.or_film_add_clamped.argtypes = [vp, sz, vp, u32, C.c_double, C.c_double, vp]
         lib.or_sample_scalar.argtypes = [vp, C.POINTER(abi.Request), vp, sz, C.c_int]
         lib.or_probe_medium.argtypes = [vp, u32, vp]
         lib.or_scalar_film_add.argtypes = [vp, sz, vp, u32, vp]
@@ -71,6 +72,7 @@ def reference():
         lib.ref_outward.restype = u32
         lib.ref_set_cie.argtypes = [vp]
         lib.ref_film_add.argtypes = [vp, sz, u32, u32, vp]
+        lib.ref_film_add_clamped.argtypes = [vp, sz, u32, u32, C.c_double, C.c_double, vp]
         lib.ref_probe_medium.argtypes = [vp, u32, vp]
         lib.ref_probe_qmc.argtypes = [vp, u32, vp]
         _ref = lib

@@ -28,7 +28,7 @@ def device_mean(rs, settings, torch):
     from torch_adjoint import film_mean_device
 
     pixels = settings.width * settings.height
-    film = torch.zeros(pixels * 96, dtype=torch.uint8, device="cuda")
+    film = torch.zeros(pixels * abi.FILM_PIXEL_BYTES, dtype=torch.uint8, device="cuda")
     rs.render_film_device(settings, film.data_ptr())
     torch.cuda.synchronize()
     return film_mean_device(film, pixels)

@@ -20,7 +20,7 @@ def build(scene):
 
 def batch_film(rs, views, request, torch):
     total = renderer.pack_views(views)
-    film = torch.zeros(total * 96, dtype=torch.uint8, device="cuda")
+    film = torch.zeros(total * abi.FILM_PIXEL_BYTES, dtype=torch.uint8, device="cuda")
     used = rs.render_views_device(views, request, film.data_ptr())
     torch.cuda.synchronize()
     return film.cpu().numpy().view(abi.film_dtype()), used
@@ -103,7 +103,7 @@ def test_batch_validation():
     scene, views = cornell_views()
     rs = build(scene)
     total = renderer.pack_views(views)
-    film = torch.zeros(total * 96, dtype=torch.uint8, device="cuda")  # a valid film: rejection precedes launches
+    film = torch.zeros(total * abi.FILM_PIXEL_BYTES, dtype=torch.uint8, device="cuda")  # a valid film: rejection precedes launches
     views[2].film_offset = 0  # overlaps view 0
     with pytest.raises(RuntimeError, match="overlap"):
         rs.render_views_device(views, renderer.BatchRequest(wave_lanes=1000, trace_block=64, shade_block=128,

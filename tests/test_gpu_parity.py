@@ -216,6 +216,26 @@ def test_film_reduction_bit_exact_with_oracle(cornell):
         np.testing.assert_array_equal(film[f], ref[f])
 
 
+@pytest.mark.parametrize("exposure, clamp", [(1.0, 0.02), (3.0, 0.1)])
+def test_clamped_film_bit_exact_with_oracle(cornell, exposure, clamp):
+    """The device film's compatibility planes under a finite clamp equal the oracle's
+    PacketFilmBatch arithmetic on the same lanes, bit for bit (the canonical planes too)."""
+    scene, gpu_scene, orc = cornell
+    settings = renderer.RenderSettings(32, 32, samples=4, batch_size=2, exposure=exposure, max_component_value=clamp)
+    st, diag, film = gpu_scene.render_film(settings)
+    assert st == abi.RP_SUCCESS, diag
+    lanes = np.concatenate([gpu_scene.sample(renderer.RenderRequest(32, 32, sample_begin=b, sample_count=1))
+                            .packet_samples for b in range(4)])
+    ref = np.zeros(32 * 32, abi.film_dtype())
+    cie = np.ascontiguousarray(scenes.cie_xyz())
+    assert oracle().or_film_add_clamped(lanes.ctypes.data, lanes.size, cie.ctypes.data, 32 * 32, exposure, clamp,
+                                        ref.ctypes.data) == 0
+    for f in ("sum", "correction", "weight_sum", "count", "compatibility_sum", "compatibility_correction"):
+        np.testing.assert_array_equal(film[f], ref[f])
+    clamped = renderer.film_mean(film, compatibility=True)
+    assert clamped.max() <= clamp * (1 + 1e-9) and (clamped < renderer.film_mean(film) * exposure - 1e-12).any()
+
+
 def test_image_statistics_match_oracle():
     """Per-pixel XYZ of GPU and oracle renders agree within 3 combined standard errors."""
     w = h = 24

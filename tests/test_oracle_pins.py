@@ -267,6 +267,35 @@ def test_film_reduction_matches_packet_film_batch():
     np.testing.assert_array_equal(film["count"], ref_out[:, 8])
 
 
+@pytest.mark.parametrize("exposure, clamp", [(1.0, 0.35), (2.5, 1.2), (0.7, 0.05)])
+def test_clamped_film_matches_packet_film_batch(exposure, clamp):
+    """The compatibility planes of a finite film clamp (clamp_sensor, src/packet_film.cpp:39-47)
+    bit for bit against rypath's own PacketFilmBatch with the same exposure and clamp."""
+    lib = need_ref()
+    cie = scenes.cie_xyz()
+    lib.ref_set_cie(np.ascontiguousarray(cie).ctypes.data)
+    rng = np.random.default_rng(3)
+    w, h, spp = 7, 6, 5
+    res = np.zeros(w * h * spp, abi.packet_dtype())
+    lane = np.arange(res.size)
+    res["pixel"] = lane % (w * h)
+    res["sample_low"] = lane // (w * h)
+    res["wavelengths"] = rng.uniform(360, 830, (res.size, 4))
+    res["wavelength_pdfs"] = rng.uniform(0.001, 0.004, (res.size, 4))
+    res["radiance"] = rng.exponential(1.0, (res.size, 4)) * (rng.uniform(size=(res.size, 4)) > 0.3)
+    res["filter_weight"] = rng.uniform(0.5, 1.0, res.size).astype(np.float32)
+    ref_out = np.zeros((w * h, 15))
+    assert lib.ref_film_add_clamped(res.ctypes.data, res.size, w, h, exposure, clamp, ref_out.ctypes.data) == 0
+    film = np.zeros(w * h, abi.film_dtype())
+    assert oracle().or_film_add_clamped(res.ctypes.data, res.size, np.ascontiguousarray(cie).ctypes.data, w * h,
+                                        exposure, clamp, film.ctypes.data) == 0
+    np.testing.assert_array_equal(film["sum"], ref_out[:, 0:3])
+    np.testing.assert_array_equal(film["weight_sum"], ref_out[:, 6])
+    np.testing.assert_array_equal(film["compatibility_sum"], ref_out[:, 9:12])
+    np.testing.assert_array_equal(film["compatibility_correction"], ref_out[:, 12:15])
+    assert (film["compatibility_sum"] < film["sum"] * exposure - 1e-12).any()  # the clamp bites
+
+
 def _fnv_floats(values, h=14695981039346656037):
     for b in np.asarray(values, np.float32).tobytes():
         h ^= b

@@ -7,10 +7,12 @@ losses and optimisers.
 import numpy as np
 import torch
 
+from rypath_b200 import abi
+
 
 def film_mean_device(film_bytes, pixels):
     """Film-mean XYZ (pixels x 3, float64) of a device rp_film_pixel buffer."""
-    f = film_bytes.view(torch.float64).reshape(pixels, 12)
+    f = film_bytes.view(torch.float64).reshape(pixels, abi.FILM_PIXEL_BYTES // 8)
     return (f[:, 0:3] + f[:, 3:6]) / (f[:, 6:7] + f[:, 7:8])
 
 
@@ -26,7 +28,7 @@ class SpectralFilm(torch.autograd.Function):
             rs.set_knot_values(int(mat.knot_begin), values[offset:offset + mat.knot_count])
             offset += mat.knot_count
         pixels = settings.width * settings.height
-        film = torch.zeros(pixels * 96, dtype=torch.uint8, device="cuda")
+        film = torch.zeros(pixels * abi.FILM_PIXEL_BYTES, dtype=torch.uint8, device="cuda")
         rs.render_film_device(settings, film.data_ptr())
         ctx.rs, ctx.settings, ctx.materials, ctx.params = rs, settings, list(materials), offset
         ctx.theta_device, ctx.theta_dtype = theta.device, theta.dtype
