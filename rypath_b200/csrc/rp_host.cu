@@ -506,6 +506,10 @@ int grid_for(int sm_count, u32 work, int block, int per_sm) {
 struct rp_scene {
     int device = 0, sm_count = 148;
     cudaStream_t stream = nullptr;
+    // the shadow walks of one event run on `side` while the next event's closest-hit walk runs
+    // on `stream`; `forked` and `joined` order the two (timing disabled)
+    cudaStream_t side = nullptr;
+    cudaEvent_t forked = nullptr, joined = nullptr;
     std::vector<void *> owned;   // scene lifetime
     std::vector<void *> pool_owned;
     DeviceScene ds{};
@@ -562,13 +566,19 @@ struct rp_scene {
             cudaStreamSynchronize(stream);
         for (auto e : events)
             cudaEventDestroy(e);
+        if (forked)
+            cudaEventDestroy(forked);
+        if (joined)
+            cudaEventDestroy(joined);
+        if (side)
+            cudaStreamDestroy(side);
         if (stream)
             cudaStreamDestroy(stream);
     }
 
     // timing: pairs of events around launches, grouped by kind (0 trace, 1 shadow, 2 shade, 3 other)
     uint64_t launches = 0;
-    void mark(int kind, int kernels = 1) {
+    void mark(int kind, int kernels = 1, cudaStream_t on = nullptr) {
         launches += kernels;
         if (event_cursor + 2 > events.size()) {
             for (int k = 0; k < 64; ++k) {
@@ -577,11 +587,11 @@ struct rp_scene {
                 events.push_back(e);
             }
         }
-        RP_CHECK(cudaEventRecord(events[event_cursor], stream));
+        RP_CHECK(cudaEventRecord(events[event_cursor], on ? on : stream));
         event_kind.push_back(kind);
     }
-    void done() {
-        RP_CHECK(cudaEventRecord(events[event_cursor + 1], stream));
+    void done(cudaStream_t on = nullptr) {
+        RP_CHECK(cudaEventRecord(events[event_cursor + 1], on ? on : stream));
         event_cursor += 2;
     }
     void collect() {
@@ -791,6 +801,14 @@ void launch_shadow(const rp_scene *s, const PathPool &pool, unsigned grid, size_
 }
 
 // One wave: raygen, then max_depth + 1 events of trace -> shade -> shadow.
+// The shadow walks of event e run on the side stream, overlapping the closest-hit walk of
+// event e + 1 on the scene stream; the shade kernels of e + 1 wait for them.  The two walks
+// share no written data: the shadow walk reads its own queue (written by shade e) and writes
+// the radiance and, on a failure, the status of a path; the closest-hit walk reads the rays of
+// queued paths and writes their hits and the family bins.  A closest-hit walk that reads a
+// path's flags before a concurrent shadow failure marks it complete only computes a hit the
+// shade kernel then ignores (it skips complete paths), so every result equals the serial
+// order's.
 void run_wave(rp_scene *s, const WaveParams &p, size_t adjoint_smem = 0) {
     s->ensure_pool(p.lanes);
     PathPool &pool = s->pool;
@@ -802,6 +820,7 @@ void run_wave(rp_scene *s, const WaveParams &p, size_t adjoint_smem = 0) {
     s->done();
     int in = 0;
     const u32 events = s->ds.max_depth + 1;
+    bool shadow_pending = false;
     for (u32 e = 0; e < events; ++e) {
         s->mark(0);
         RP_CHECK(cudaMemsetAsync(pool.counters + 4, 0, 4 * sizeof(u32), s->stream));
@@ -811,6 +830,10 @@ void run_wave(rp_scene *s, const WaveParams &p, size_t adjoint_smem = 0) {
         else
             launch_trace<false, kTraceBlock>(s, pool, in, trace_grid, s->stream, p.boundary_limit);
         s->done();
+        if (shadow_pending) {
+            RP_CHECK(cudaStreamWaitEvent(s->stream, s->joined, 0));
+            shadow_pending = false;
+        }
         s->mark(2, 4);
         RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), s->stream));
         RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), s->stream));
@@ -828,16 +851,22 @@ void run_wave(rp_scene *s, const WaveParams &p, size_t adjoint_smem = 0) {
             k_shade<3><<<shade_grid, 128, 0, s->stream>>>(s->ds, p, pool, in);
         }
         s->done();
-        s->mark(1);
+        RP_CHECK(cudaEventRecord(s->forked, s->stream));
+        RP_CHECK(cudaStreamWaitEvent(s->side, s->forked, 0));
+        s->mark(1, 1, s->side);
         if (pool.hist)
-            launch_shadow<false, kTraceBlock, true>(s, pool, trace_grid, smem, s->stream, p.boundary_limit);
+            launch_shadow<false, kTraceBlock, true>(s, pool, trace_grid, smem, s->side, p.boundary_limit);
         else if (s->counting)
-            launch_shadow<true, kTraceBlock, false>(s, pool, trace_grid, 0, s->stream, p.boundary_limit);
+            launch_shadow<true, kTraceBlock, false>(s, pool, trace_grid, 0, s->side, p.boundary_limit);
         else
-            launch_shadow<false, kTraceBlock, false>(s, pool, trace_grid, 0, s->stream, p.boundary_limit);
-        s->done();
+            launch_shadow<false, kTraceBlock, false>(s, pool, trace_grid, 0, s->side, p.boundary_limit);
+        s->done(s->side);
+        RP_CHECK(cudaEventRecord(s->joined, s->side));
+        shadow_pending = true;
         in ^= 1;
     }
+    if (shadow_pending)
+        RP_CHECK(cudaStreamWaitEvent(s->stream, s->joined, 0));
     RP_CHECK(cudaGetLastError());
 }
 
@@ -1191,6 +1220,9 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
         s->device = device;
         s->sm_count = device_properties(device).multiProcessorCount;
         RP_CHECK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+        RP_CHECK(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking));
+        RP_CHECK(cudaEventCreateWithFlags(&s->forked, cudaEventDisableTiming));
+        RP_CHECK(cudaEventCreateWithFlags(&s->joined, cudaEventDisableTiming));
         cudaStream_t stm = s->stream;
         auto &own = s->owned;
         DeviceScene &ds = s->ds;
