@@ -510,6 +510,9 @@ struct rp_scene {
     // on `stream`; `forked` and `joined` order the two (timing disabled)
     cudaStream_t side = nullptr;
     cudaEvent_t forked = nullptr, joined = nullptr;
+    // the shade kernels of BSDF families 1-3 run on their own streams beside family 0's
+    cudaStream_t family[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t family_done[3] = {nullptr, nullptr, nullptr};
     std::vector<void *> owned;   // scene lifetime
     std::vector<void *> pool_owned;
     DeviceScene ds{};
@@ -566,6 +569,12 @@ struct rp_scene {
             cudaStreamSynchronize(stream);
         for (auto e : events)
             cudaEventDestroy(e);
+        for (int k = 0; k < 3; ++k) {
+            if (family_done[k])
+                cudaEventDestroy(family_done[k]);
+            if (family[k])
+                cudaStreamDestroy(family[k]);
+        }
         if (forked)
             cudaEventDestroy(forked);
         if (joined)
@@ -800,6 +809,26 @@ void launch_shadow(const rp_scene *s, const PathPool &pool, unsigned grid, size_
         launch_shadow_stack<Count, Block, Adjoint, kStackDepth>(s, pool, grid, smem, st, limit);
 }
 
+// The four shade kernels of one event (one per BSDF family), run side by side: family 0 on
+// the scene stream, families 1-3 on their own streams, joined back before the shadow walks.
+// Each reads only its own bin and appends to the path and shadow queues with atomics, so the
+// queue order may differ from a serial launch but no path's result does (every later kernel
+// reads a path by its id, and the film reduces by lane).
+template <bool Adjoint>
+void launch_shade(rp_scene *s, const WaveParams &p, const PathPool &pool, int in, unsigned grid, size_t smem) {
+    RP_CHECK(cudaEventRecord(s->forked, s->stream));
+    for (int k = 0; k < 3; ++k)
+        RP_CHECK(cudaStreamWaitEvent(s->family[k], s->forked, 0));
+    k_shade<0, 128, Adjoint><<<grid, 128, smem, s->stream>>>(s->ds, p, pool, in);
+    k_shade<1, 128, Adjoint><<<grid, 128, smem, s->family[0]>>>(s->ds, p, pool, in);
+    k_shade<2, 128, Adjoint><<<grid, 128, smem, s->family[1]>>>(s->ds, p, pool, in);
+    k_shade<3, 128, Adjoint><<<grid, 128, smem, s->family[2]>>>(s->ds, p, pool, in);
+    for (int k = 0; k < 3; ++k) {
+        RP_CHECK(cudaEventRecord(s->family_done[k], s->family[k]));
+        RP_CHECK(cudaStreamWaitEvent(s->stream, s->family_done[k], 0));
+    }
+}
+
 // One wave: raygen, then max_depth + 1 events of trace -> shade -> shadow.
 // The shadow walks of event e run on the side stream, overlapping the closest-hit walk of
 // event e + 1 on the scene stream; the shade kernels of e + 1 wait for them.  The two walks
@@ -839,17 +868,10 @@ void run_wave(rp_scene *s, const WaveParams &p, size_t adjoint_smem = 0) {
         RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), s->stream));
         const size_t smem = adjoint_smem;
         const unsigned shade_grid = grid_for(sms, p.lanes, 128, 16);
-        if (pool.hist) {
-            k_shade<0, 128, true><<<shade_grid, 128, smem, s->stream>>>(s->ds, p, pool, in);
-            k_shade<1, 128, true><<<shade_grid, 128, smem, s->stream>>>(s->ds, p, pool, in);
-            k_shade<2, 128, true><<<shade_grid, 128, smem, s->stream>>>(s->ds, p, pool, in);
-            k_shade<3, 128, true><<<shade_grid, 128, smem, s->stream>>>(s->ds, p, pool, in);
-        } else {
-            k_shade<0><<<shade_grid, 128, 0, s->stream>>>(s->ds, p, pool, in);
-            k_shade<1><<<shade_grid, 128, 0, s->stream>>>(s->ds, p, pool, in);
-            k_shade<2><<<shade_grid, 128, 0, s->stream>>>(s->ds, p, pool, in);
-            k_shade<3><<<shade_grid, 128, 0, s->stream>>>(s->ds, p, pool, in);
-        }
+        if (pool.hist)
+            launch_shade<true>(s, p, pool, in, shade_grid, smem);
+        else
+            launch_shade<false>(s, p, pool, in, shade_grid, 0);
         s->done();
         RP_CHECK(cudaEventRecord(s->forked, s->stream));
         RP_CHECK(cudaStreamWaitEvent(s->side, s->forked, 0));
@@ -1223,6 +1245,10 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
         RP_CHECK(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking));
         RP_CHECK(cudaEventCreateWithFlags(&s->forked, cudaEventDisableTiming));
         RP_CHECK(cudaEventCreateWithFlags(&s->joined, cudaEventDisableTiming));
+        for (int k = 0; k < 3; ++k) {
+            RP_CHECK(cudaStreamCreateWithFlags(&s->family[k], cudaStreamNonBlocking));
+            RP_CHECK(cudaEventCreateWithFlags(&s->family_done[k], cudaEventDisableTiming));
+        }
         cudaStream_t stm = s->stream;
         auto &own = s->owned;
         DeviceScene &ds = s->ds;
