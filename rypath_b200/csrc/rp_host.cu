@@ -2171,19 +2171,40 @@ void batch_wave_kernels(rp_scene *s, const WaveParams &p, const Batch &b, u32 wa
     k_raygen_views<<<grid_for(sms, wave_lanes, 256, 16), 256, 0, st>>>(s->ds, p, b, pool);
     const int trace_grid = grid_for(sms, wave_lanes, TB, int(blocks_per_sm * 128 / TB));
     const int shade_grid = grid_for(sms, wave_lanes, SB, int(blocks_per_sm * 128 / SB));
+    // the same stream layout as run_wave: family shade kernels side by side, each event's
+    // shadow walks beside the next event's closest-hit walk (in a captured graph these forks
+    // and joins become parallel branches)
     int in = 0;
+    bool shadow_pending = false;
     for (u32 e = 0; e <= s->ds.max_depth; ++e) {
         RP_CHECK(cudaMemsetAsync(pool.counters + 4, 0, 4 * sizeof(u32), st));
         launch_trace<false, TB>(s, pool, in, trace_grid, st, p.boundary_limit);
+        if (shadow_pending) {
+            RP_CHECK(cudaStreamWaitEvent(st, s->joined, 0));
+            shadow_pending = false;
+        }
         RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), st));
         RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), st));
+        RP_CHECK(cudaEventRecord(s->forked, st));
+        for (int k = 0; k < 3; ++k)
+            RP_CHECK(cudaStreamWaitEvent(s->family[k], s->forked, 0));
         k_shade<0, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
-        k_shade<1, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
-        k_shade<2, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
-        k_shade<3, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
-        launch_shadow<false, TB, false>(s, pool, trace_grid, 0, st, p.boundary_limit);
+        k_shade<1, SB><<<shade_grid, SB, 0, s->family[0]>>>(s->ds, p, pool, in);
+        k_shade<2, SB><<<shade_grid, SB, 0, s->family[1]>>>(s->ds, p, pool, in);
+        k_shade<3, SB><<<shade_grid, SB, 0, s->family[2]>>>(s->ds, p, pool, in);
+        for (int k = 0; k < 3; ++k) {
+            RP_CHECK(cudaEventRecord(s->family_done[k], s->family[k]));
+            RP_CHECK(cudaStreamWaitEvent(st, s->family_done[k], 0));
+        }
+        RP_CHECK(cudaEventRecord(s->forked, st));
+        RP_CHECK(cudaStreamWaitEvent(s->side, s->forked, 0));
+        launch_shadow<false, TB, false>(s, pool, trace_grid, 0, s->side, p.boundary_limit);
+        RP_CHECK(cudaEventRecord(s->joined, s->side));
+        shadow_pending = true;
         in ^= 1;
     }
+    if (shadow_pending)
+        RP_CHECK(cudaStreamWaitEvent(st, s->joined, 0));
     k_film_views<<<grid_for(sms, wave_lanes, 128, 16), 128, 0, st>>>(pool, b, s->cie, double(s->ds.filter_weight), clamp,
                                                                        film);
     k_next_wave<<<1, 32, 0, st>>>(b);
