@@ -510,6 +510,10 @@ struct rp_scene {
     // on `stream`; `forked` and `joined` order the two (timing disabled)
     cudaStream_t side = nullptr;
     cudaEvent_t forked = nullptr, joined = nullptr;
+    // Owen prefix table of the draw blocks (attach_owen_prefix), built for one seed
+    unsigned short *owen_prefix = nullptr;
+    u32 owen_capacity = 0, owen_blocks = 0, owen_seed = 0;
+    bool owen_built = false;
     // the shade kernels of BSDF families 1-3 run on their own streams beside family 0's
     cudaStream_t family[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t family_done[3] = {nullptr, nullptr, nullptr};
@@ -561,6 +565,8 @@ struct rp_scene {
             cudaFreeAsync(p, stream);
         if (scalar_records)
             cudaFreeAsync(scalar_records, stream);
+        if (owen_prefix)
+            cudaFreeAsync(owen_prefix, stream);
         if (adjoint_storage)
             cudaFreeAsync(adjoint_storage, stream);
         if (film_stage)
@@ -829,6 +835,39 @@ void launch_shade(rp_scene *s, const WaveParams &p, const PathPool &pool, int in
     }
 }
 
+// Sobol sampler with Owen randomisation: attaches the table of the first kOwenPrefixBits
+// scrambling rounds of the continuation and light-sample draw blocks (one block per vertex up to
+// the maximum depth), building it on the scene stream when the seed or depth changed.  Every
+// word drawn through it equals the fully computed word.
+void attach_owen_prefix(rp_scene *s, WaveParams &p) {
+    p.owen_prefix = nullptr;
+    p.owen_blocks = 0;
+    if (p.sampler != RP_SAMPLER_SOBOL || p.randomization != RP_RANDOMIZE_OWEN)
+        return;
+    const u32 blocks = std::min<u32>(std::max<u32>(s->ds.max_depth, 1), 129);
+    if (s->owen_capacity < blocks) {
+        if (s->owen_prefix)
+            cudaFreeAsync(s->owen_prefix, s->stream);
+        s->owen_prefix = nullptr;
+        s->owen_capacity = 0;
+        s->owen_built = false;
+        RP_CHECK(cudaMallocAsync(reinterpret_cast<void **>(&s->owen_prefix),
+                                 size_t(2) * blocks * 4 * kOwenPrefixEntries * sizeof(unsigned short), s->stream));
+        s->owen_capacity = blocks;
+    }
+    if (!s->owen_built || s->owen_seed != p.seed_low || s->owen_blocks != blocks) {
+        const u32 total = 2 * blocks * 4 * kOwenPrefixEntries;
+        k_owen_prefix<<<grid_for(s->sm_count, total, 256, 8), 256, 0, s->stream>>>(s->owen_prefix, blocks, p.seed_low);
+        RP_CHECK(cudaGetLastError());
+        ++s->launches;
+        s->owen_seed = p.seed_low;
+        s->owen_blocks = blocks;
+        s->owen_built = true;
+    }
+    p.owen_prefix = s->owen_prefix;
+    p.owen_blocks = blocks;
+}
+
 // One wave: raygen, then max_depth + 1 events of trace -> shade -> shadow.
 // The shadow walks of event e run on the side stream, overlapping the closest-hit walk of
 // event e + 1 on the scene stream; the shade kernels of e + 1 wait for them.  The two walks
@@ -838,7 +877,9 @@ void launch_shade(rp_scene *s, const WaveParams &p, const PathPool &pool, int in
 // path's flags before a concurrent shadow failure marks it complete only computes a hit the
 // shade kernel then ignores (it skips complete paths), so every result equals the serial
 // order's.
-void run_wave(rp_scene *s, const WaveParams &p, size_t adjoint_smem = 0) {
+void run_wave(rp_scene *s, const WaveParams &request_params, size_t adjoint_smem = 0) {
+    WaveParams p = request_params;
+    attach_owen_prefix(s, p);
     s->ensure_pool(p.lanes);
     PathPool &pool = s->pool;
     const int sms = s->sm_count;
@@ -2267,7 +2308,8 @@ struct BatchBuffers {
 float run_batch(rp_scene *s, const BatchPlan &plan, const BatchBuffers &buf, const rp_batch_request &r,
                 const rp_batch_config &c, FilmPixel *film, size_t waves) {
     s->ensure_pool(c.wave_lanes);
-    const WaveParams p = batch_params(r);
+    WaveParams p = batch_params(r);
+    attach_owen_prefix(s, p);
     const FilmClamp clamp = film_clamp(r.exposure, r.max_component_value);
     const Batch b = buf.batch(plan);
     RP_CHECK(cudaMemsetAsync(buf.cursor, 0, 8, s->stream));

@@ -841,6 +841,17 @@ __global__ void k_count_failures(PathPool pool, u32 lanes) {
     }
 }
 // Every sample of a wave reduced per pixel in canonical (absolute sample, pixel) order.
+// Owen prefix table (owen_prefix_rounds of every prefix) of the draw blocks [4, 4 + blocks)
+// and [133, 133 + blocks), four dimensions each.
+__global__ void k_owen_prefix(unsigned short *table, u32 blocks, u32 seed) {
+    const u32 total = 2 * blocks * 4 * kOwenPrefixEntries;
+    for (u32 e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        const u32 slot = e / (4 * kOwenPrefixEntries), k = (e / kOwenPrefixEntries) & 3u, prefix = e % kOwenPrefixEntries;
+        const u32 block = slot < blocks ? 4 + slot : 133 + (slot - blocks);
+        table[e] = (unsigned short)owen_prefix_rounds(prefix, sobol_dimension_hash(4 * block + k, seed));
+    }
+}
+
 __global__ void k_film(PathPool pool, u32 pixel_count, u32 samples, const double *cie, double weight, FilmClamp clamp,
                        FilmPixel *film) {
     for (u32 px = blockIdx.x * blockDim.x + threadIdx.x; px < pixel_count; px += gridDim.x * blockDim.x) {

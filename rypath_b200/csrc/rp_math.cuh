@@ -159,12 +159,25 @@ RP_DEV u32 sobol_word(const SobolTables &t, u64 index, u32 dimension, u32 mode, 
         return value;
     return scramble_word(value, mode, sobol_dimension_hash(dimension, seed));
 }
+// Owen scrambling rounds 0 .. kOwenPrefixBits - 1 decide the top kOwenPrefixBits bits of a
+// word from those bits alone (round b flips bit 31 - b from the b bits above it), so a table
+// of every prefix per dimension replaces them.
+constexpr u32 kOwenPrefixBits = 12, kOwenPrefixEntries = 1u << kOwenPrefixBits;
+RP_DEV u32 owen_prefix_rounds(u32 prefix, u32 hash) {
+    u32 value = (prefix << (32 - kOwenPrefixBits)) ^ ((hash & 1) << 31);
+    for (u32 bit = 1; bit < kOwenPrefixBits; ++bit)
+        if (u32(mix_bits((value & (~u32(0) << (32 - bit))) ^ hash)) & (u32(1) << bit))
+            value ^= u32(1) << (31 - bit);
+    return value >> (32 - kOwenPrefixBits);
+}
 // Four consecutive dimensions [dimension, dimension + 4) of one Sobol index, each equal to
-// sobol_word of its dimension.  The four generator products share the walk over the index
+// sobol_word of its dimension.  `prefix` (optional, Owen only): the four dimensions' tables of
+// owen_prefix_rounds, kOwenPrefixEntries entries each.  The four generator products share the walk over the index
 // bits, and the four Owen bit loops run in lockstep: each loop is a chain of dependent 64-bit
 // hashes, so four independent chains keep the pipelines busy where one would stall on each
 // hash.
-RP_DEV uint4 sobol_words4(const SobolTables &t, u64 index, u32 dimension, u32 mode, u32 seed) {
+RP_DEV uint4 sobol_words4(const SobolTables &t, u64 index, u32 dimension, u32 mode, u32 seed,
+                          const unsigned short *prefix = nullptr) {
     const u32 *col = t.directions + dimension * kSobolMatrix;
     u32 v[4] = {0, 0, 0, 0};
     u32 lo = u32(index), hi = u32(index >> 32);
@@ -195,11 +208,20 @@ RP_DEV uint4 sobol_words4(const SobolTables &t, u64 index, u32 dimension, u32 mo
         return make_uint4(v[0], v[1], v[2], v[3]);
     }
     // Owen (the mode-3 loop of scramble_word), four words at once
+    u32 first = 1;
+    if (prefix) {
+        constexpr u32 low = 32 - kOwenPrefixBits;
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-        v[k] ^= (h[k] & 1) << 31;
+        for (int k = 0; k < 4; ++k)
+            v[k] = (v[k] & ((u32(1) << low) - 1)) | (u32(__ldg(prefix + k * kOwenPrefixEntries + (v[k] >> low))) << low);
+        first = kOwenPrefixBits;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            v[k] ^= (h[k] & 1) << 31;
+    }
 #pragma unroll 1
-    for (u32 bit = 1; bit < 32; ++bit) {
+    for (u32 bit = first; bit < 32; ++bit) {
         const u32 mask = ~u32(0) << (32 - bit), flip = u32(1) << (31 - bit);
 #pragma unroll
         for (int k = 0; k < 4; ++k)

@@ -71,7 +71,21 @@ struct WaveParams {
     u32 lanes;
     u32 log_spp;        // ZSobol: log2 of the total sample budget
     u32 boundary_limit; // pass-through crossings allowed between two vertices
+    // Sobol sampler with Owen randomisation: the first kOwenPrefixBits scrambling rounds of the
+    // draw blocks [4, 4 + owen_blocks) and [133, 133 + owen_blocks), tabulated (null: none)
+    const unsigned short *owen_prefix;
+    u32 owen_blocks;
 };
+// Table of one draw block's four dimensions in the Owen prefix table (null if not tabulated).
+RP_DEV const unsigned short *owen_prefix_table(const WaveParams &p, u32 block) {
+    if (!p.owen_prefix || p.randomization != 3)
+        return nullptr;
+    if (block - 4u < p.owen_blocks)
+        return p.owen_prefix + size_t(block - 4u) * 4 * kOwenPrefixEntries;
+    if (block - 133u < p.owen_blocks)
+        return p.owen_prefix + size_t(p.owen_blocks + block - 133u) * 4 * kOwenPrefixEntries;
+    return nullptr;
+}
 
 // shaders/render.metal:113-122
 RP_DEV float sample_uniform(const WaveParams &p, u32 w) {
@@ -102,7 +116,7 @@ __device__ __noinline__ uint4 draw_words(const DeviceScene &s, const WaveParams 
         return make_uint4(zdraw(s, p, index, d, 0, true), zdraw(s, p, index, d, 1, true),
                           zdraw(s, p, index, d + 2, 0, even), zdraw(s, p, index, even ? d + 2 : d + 3, even ? 1 : 0, even));
     }
-    return sobol_words4(s.sobol, index, 4 * block, p.randomization, p.seed_low);
+    return sobol_words4(s.sobol, index, 4 * block, p.randomization, p.seed_low, owen_prefix_table(p, block));
 }
 
 struct BeginSample {
