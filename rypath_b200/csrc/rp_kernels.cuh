@@ -187,9 +187,10 @@ __global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1
 // whose hit is of BSDF family F (3: no surface -- environment or a failed query).
 // Adjoint: the path-replay adjoint hooks are compiled in (the plain forward kernel carries none
 // of their registers).  The minimum of 384 resident threads per SM caps registers at 168, so
-// three 128-thread blocks fit an SM.
+// three 128-thread blocks fit an SM; the escape kernel (F = 3, no BSDF sampling or light
+// sample) fits 128 registers without spilling, so four.
 template <int F, int Block = 128, bool Adjoint = false>
-__global__ void __launch_bounds__(Block, 384 / Block) k_shade(const __grid_constant__ DeviceScene s,
+__global__ void __launch_bounds__(Block, (F == 3 ? 512 : 384) / Block) k_shade(const __grid_constant__ DeviceScene s,
                                                               const __grid_constant__ WaveParams p, PathPool pool, int in) {
     extern __shared__ float sgrad[]; // adjoint only
     if (Adjoint)
@@ -568,15 +569,22 @@ __global__ void __launch_bounds__(Block, 384 / Block) k_shade(const __grid_const
                         shadow = false;
                     }
                 }
+                // A complete path is read again only for its identity, status and radiance (the
+                // shadow walk, the film and the packet results), so the rest of its state is not
+                // written back.
                 if (cnt != old_count) {
                     // preceding = latest; latest = current (shaders/packet_pt_event_body.inc:453-460)
-                    pool.preceding[path] = make_float4(latest.position.x, latest.position.y, latest.position.z, 0);
                     flags = (flags & ~(3u << F_PTYPE_SHIFT)) | (latest.type << F_PTYPE_SHIFT);
-                    pool.latest_p[path] = make_float4(cp.position.x, cp.position.y, cp.position.z, cbsdf.g.alpha_x);
-                    pool.latest_n[path] =
-                        make_float4(cp.shading_normal.x, cp.shading_normal.y, cp.shading_normal.z, cbsdf.g.alpha_y);
-                    pool.latest_param[path] = make_float4(cbsdf.param[0], cbsdf.param[1], cbsdf.param[2], cbsdf.param[3]);
-                    pool.latest_k[path] = make_float4(cbsdf.k[0], cbsdf.k[1], cbsdf.k[2], cbsdf.k[3]);
+                    if (!complete) {
+                        pool.preceding[path] = make_float4(latest.position.x, latest.position.y, latest.position.z, 0);
+                        pool.latest_p[path] =
+                            make_float4(cp.position.x, cp.position.y, cp.position.z, cbsdf.g.alpha_x);
+                        pool.latest_n[path] =
+                            make_float4(cp.shading_normal.x, cp.shading_normal.y, cp.shading_normal.z, cbsdf.g.alpha_y);
+                        pool.latest_param[path] =
+                            make_float4(cbsdf.param[0], cbsdf.param[1], cbsdf.param[2], cbsdf.param[3]);
+                        pool.latest_k[path] = make_float4(cbsdf.k[0], cbsdf.k[1], cbsdf.k[2], cbsdf.k[3]);
+                    }
                     flags &= ~((3u << F_LTYPE_SHIFT) | F_LDELTA | (3u << F_LKIND_SHIFT) | (15u << F_LMASK_SHIFT) | F_LSMOOTH);
                     flags |= (ctype << F_LTYPE_SHIFT) | (cdelta ? F_LDELTA : 0u) | ((cbsdf.kind & 3u) << F_LKIND_SHIFT) |
                              ((cbsdf.active_mask & 15u) << F_LMASK_SHIFT) | (cbsdf.g.smooth ? F_LSMOOTH : 0u);
@@ -585,21 +593,23 @@ __global__ void __launch_bounds__(Block, 384 / Block) k_shade(const __grid_const
                 flags = set_status(flags, status) | (complete ? F_COMPLETE : 0u);
                 ident.w = flags;
                 pool.ident[path] = ident;
-                cursor.z = cnt;
-                pool.cursor[path] = cursor;
-                pool.beta[path] = to_float4(beta);
                 pool.radiance[path] = to_float4(radiance);
-                float4 f;
-                int4 e;
-                store_density(density, f, e);
-                pool.dens_f[path] = f;
-                pool.dens_e[path] = e;
-                store_density(hero_previous, f, e);
-                pool.prev_f[path] = f;
-                pool.prev_e[path] = e;
-                pool.eta_scale[path] = to_float4(eta_scale);
-                pool.ray_o[path] = make_float4(ro.x, ro.y, ro.z, 0);
-                pool.ray_d[path] = make_float4(rd.x, rd.y, rd.z, 0);
+                if (!complete) {
+                    cursor.z = cnt;
+                    pool.cursor[path] = cursor;
+                    pool.beta[path] = to_float4(beta);
+                    float4 f;
+                    int4 e;
+                    store_density(density, f, e);
+                    pool.dens_f[path] = f;
+                    pool.dens_e[path] = e;
+                    store_density(hero_previous, f, e);
+                    pool.prev_f[path] = f;
+                    pool.prev_e[path] = e;
+                    pool.eta_scale[path] = to_float4(eta_scale);
+                    pool.ray_o[path] = make_float4(ro.x, ro.y, ro.z, 0);
+                    pool.ray_d[path] = make_float4(rd.x, rd.y, rd.z, 0);
+                }
                 keep = !complete;
             }
         }
