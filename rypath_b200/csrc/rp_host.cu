@@ -551,7 +551,10 @@ struct rp_scene {
     uint2 *scalar_fresh_index = nullptr;
     u32 *scalar_counters = nullptr;
     u32 scalar_capacity = 0;
-    int volpath_blocks = 0; // resident persistent blocks per SM
+    // scalar transport slots of the wavefront form (paths, connections, modes, hits)
+    void *slot_storage = nullptr;
+    u32 slot_capacity = 0;
+    int step_blocks = 0; // resident k_scalar_step blocks per SM
     // adjoint: per-lane history and lane weights
     void *adjoint_storage = nullptr;
     u32 adjoint_capacity = 0;
@@ -565,6 +568,8 @@ struct rp_scene {
             cudaFreeAsync(p, stream);
         if (scalar_records)
             cudaFreeAsync(scalar_records, stream);
+        if (slot_storage)
+            cudaFreeAsync(slot_storage, stream);
         if (owen_prefix)
             cudaFreeAsync(owen_prefix, stream);
         if (adjoint_storage)
@@ -935,12 +940,44 @@ void run_wave(rp_scene *s, const WaveParams &request_params, size_t adjoint_smem
 
 // One wave of the scalar transport: the persistent regeneration kernel over p.lanes lanes,
 // one record per lane in s->scalar_records.
+// Slots of the scalar wavefront: per slot one ScalarPath, one Connection, a mode word and a hit.
+ScalarSlots scalar_slots(rp_scene *s, u32 count) {
+    const size_t a = (size_t(count) * sizeof(ScalarPath) + 255) & ~size_t(255);
+    const size_t b = (size_t(count) * sizeof(Connection) + 255) & ~size_t(255);
+    const size_t c = (size_t(count) * sizeof(u32) + 255) & ~size_t(255);
+    const size_t d = (size_t(count) * sizeof(Hit) + 255) & ~size_t(255);
+    if (s->slot_capacity < count) {
+        if (s->slot_storage)
+            cudaFreeAsync(s->slot_storage, s->stream);
+        s->slot_storage = nullptr;
+        s->slot_capacity = 0;
+        RP_CHECK(cudaMallocAsync(&s->slot_storage, a + b + c + d, s->stream));
+        s->slot_capacity = count;
+    }
+    unsigned char *base = static_cast<unsigned char *>(s->slot_storage);
+    ScalarSlots w;
+    w.path = reinterpret_cast<ScalarPath *>(base);
+    w.conn = reinterpret_cast<Connection *>(base + a);
+    w.mode = reinterpret_cast<u32 *>(base + a + b);
+    w.hit = reinterpret_cast<Hit *>(base + a + b + c);
+    w.count = count;
+    w.remaining = s->scalar_counters + 2;
+    return w;
+}
+
+// Slots of the scalar wavefront (at most this many paths in flight per wave), and the
+// walk/step trips between two host reads of the wave's remaining lanes.
+constexpr u32 kScalarSlots = 1u << 20;
+constexpr int kScalarTripsPerCheck = 8;
+
+// One wave of the scalar transport, one record per lane in s->scalar_records: camera rays,
+// then walk / step trips over the slots until every lane's record is written.
 void run_scalar_wave(rp_scene *s, const WaveParams &p, u32 boundary_limit) {
     s->ensure_scalar(p.lanes);
-    if (!s->volpath_blocks) {
+    if (!s->step_blocks) {
         int per_sm = 0;
-        RP_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_volpath<false, kShortStack>, kTraceBlock, 0));
-        s->volpath_blocks = std::max(1, per_sm);
+        RP_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scalar_step, kTraceBlock, 0));
+        s->step_blocks = std::max(1, per_sm);
     }
     s->mark(3);
     RP_CHECK(cudaMemsetAsync(s->scalar_counters, 0, 64, s->stream));
@@ -954,20 +991,40 @@ void run_scalar_wave(rp_scene *s, const WaveParams &p, u32 boundary_limit) {
     q.fresh_index = s->scalar_fresh_index;
     q.next_lane = s->scalar_counters;
     q.stats = s->stats;
-    const u32 blocks_needed = (p.lanes + kTraceBlock - 1) / kTraceBlock;
-    const int grid = int(std::max<u32>(1, std::min<u32>(blocks_needed, u32(s->sm_count * s->volpath_blocks))));
-    s->mark(2);
+    const u32 slots = std::min<u32>(std::max<u32>(p.lanes, 1), kScalarSlots);
+    const ScalarSlots w = scalar_slots(s, slots);
+    const u32 lanes = p.lanes;
+    RP_CHECK(cudaMemcpyAsync(w.remaining, &lanes, sizeof(u32), cudaMemcpyHostToDevice, s->stream));
+    const int walk_grid = grid_for(s->sm_count, slots, kTraceBlock, 8);
+    const int step_grid = grid_for(s->sm_count, slots, kTraceBlock, s->step_blocks);
     const bool short_stack = s->wide_levels <= u32(kShortStack);
-    if (s->counting && short_stack)
-        k_volpath<true, kShortStack><<<grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q);
-    else if (s->counting)
-        k_volpath<true, kStackDepth><<<grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q);
-    else if (short_stack)
-        k_volpath<false, kShortStack><<<grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q);
-    else
-        k_volpath<false, kStackDepth><<<grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q);
-    s->done();
+    s->mark(2, 2);
+    k_scalar_slots_init<<<grid_for(s->sm_count, slots, 256, 8), 256, 0, s->stream>>>(w.mode, slots);
+    k_scalar_step<<<step_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q, w);
     RP_CHECK(cudaGetLastError());
+    // every trip advances each unfinished path by one walk and one step, so a wave ends after
+    // at most (its lanes' steps) trips; the bound only guards the host loop
+    u32 remaining = lanes;
+    for (u64 trip = 0; remaining; trip += kScalarTripsPerCheck) {
+        if (trip > (u64(1) << 22))
+            throw Invalid{"scalar wave did not finish"};
+        for (int k = 0; k < kScalarTripsPerCheck; ++k) {
+            if (s->counting && short_stack)
+                k_scalar_walk<true, kShortStack><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, w, s->stats);
+            else if (s->counting)
+                k_scalar_walk<true, kStackDepth><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, w, s->stats);
+            else if (short_stack)
+                k_scalar_walk<false, kShortStack><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, w, s->stats);
+            else
+                k_scalar_walk<false, kStackDepth><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, w, s->stats);
+            k_scalar_step<<<step_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q, w);
+            s->launches += 2;
+        }
+        RP_CHECK(cudaGetLastError());
+        RP_CHECK(cudaMemcpyAsync(&remaining, w.remaining, sizeof(u32), cudaMemcpyDeviceToHost, s->stream));
+        RP_CHECK(cudaStreamSynchronize(s->stream));
+    }
+    s->done();
 }
 
 template <class F> rp_status guarded(char *diag, size_t cap, F &&f) {

@@ -1015,6 +1015,145 @@ __global__ void __launch_bounds__(kTraceBlock) k_volpath(const __grid_constant__
     }
 }
 
+// Wavefront form of the scalar transport: the loop body of k_volpath split at its one
+// closest-hit query, with each path and its light connection in flight held in a slot in
+// global memory between the two kernels.  k_scalar_walk runs the query of every slot (the
+// path's ray or the current leg of its connection) at the walk's own occupancy;
+// k_scalar_step runs the event or connection step that consumes it and hands finished slots
+// the wave's next lanes.  Each lane's path depends only on its own indices, so every record
+// equals the persistent kernel's.
+struct ScalarSlots {
+    ScalarPath *path;
+    Connection *conn;
+    u32 *mode;      // kEvent* in the low byte; bit 8: the walk of this trip succeeded
+    Hit *hit;       // the walk's hit
+    u32 count;      // slots
+    u32 *remaining; // lanes of the wave whose record is not written yet
+};
+constexpr u32 kWalkOk = 1u << 8;
+
+RP_DEV bool scalar_ray_valid(const ScalarPath &path) {
+    return finite3(path.o) && finite3(path.d) && isfinite(path.throughput) && isfinite(path.radiance);
+}
+
+template <bool Count, int Stack = kStackDepth>
+__global__ void __launch_bounds__(kTraceBlock, Stack <= kShortStack ? 1024 / kTraceBlock : 1)
+    k_scalar_walk(const __grid_constant__ DeviceScene s, ScalarSlots w, unsigned long long *stats) {
+    __shared__ uint2 stack[Stack * kTraceBlock];
+    u32 counts[6] = {0, 0, 0, 0, 0, 0};
+    if (s.instance_count == 0)
+        return; // geometry-free scenes take the sky step, which needs no walk
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < w.count; i += gridDim.x * blockDim.x) {
+        const u32 mode = w.mode[i] & 0xffu;
+        if (mode == kEventFinished)
+            continue;
+        V3 ro, rd;
+        float tmax;
+        if (mode == kEventPath) {
+            const ScalarPath &path = w.path[i];
+            ro = path.o;
+            rd = path.d;
+            if (!scalar_ray_valid(path))
+                continue; // the step kernel records the failure
+            tmax = finf();
+        } else {
+            const Connection &c = w.conn[i];
+            ro = c.o;
+            rd = c.d;
+            tmax = c.remaining;
+        }
+        Hit hit;
+        u32 nodes = 0, tris = 0;
+        const bool ok = walk_closest<Count, Stack>(s, ro, rd, tmax, hit, stack + threadIdx.x, kTraceBlock, nodes, tris);
+        w.hit[i] = hit;
+        w.mode[i] = mode | (ok ? kWalkOk : 0u);
+        if (Count && mode == kEventPath) {
+            counts[0] += nodes;
+            counts[1] += tris;
+            counts[2] += 1;
+        } else if (Count) {
+            counts[3] += 1;
+            counts[4] += nodes;
+            counts[5] += tris;
+        }
+    }
+    if (Count) {
+        atomicAdd(stats + 0, (unsigned long long)counts[0]);
+        atomicAdd(stats + 1, (unsigned long long)counts[1]);
+        atomicAdd(stats + 2, (unsigned long long)counts[2]);
+        atomicAdd(stats + 3, (unsigned long long)counts[3]);
+        atomicAdd(stats + 4, (unsigned long long)counts[4]);
+        atomicAdd(stats + 5, (unsigned long long)counts[5]);
+    }
+}
+
+__global__ void k_scalar_slots_init(u32 *mode, u32 count) {
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+        mode[i] = kEventFinished;
+}
+
+// The event (or connection step, or geometry-free sky step) of every active slot, then new
+// lanes for the finished ones (one atomic per warp).
+__global__ void __launch_bounds__(kTraceBlock) k_scalar_step(const __grid_constant__ DeviceScene s,
+                                                             const __grid_constant__ WaveParams p, ScalarParams q,
+                                                             ScalarSlots w) {
+    const int lane_in_warp = threadIdx.x & 31;
+    const u32 stride = gridDim.x * blockDim.x;
+    const u32 trips = (w.count + stride - 1) / stride;
+    for (u32 trip = 0; trip < trips; ++trip) {
+        const u32 i = trip * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        u32 mode = kEventFinished;
+        bool finished_now = false;
+        if (i < w.count) {
+            const u32 m = w.mode[i];
+            mode = m & 0xffu;
+            if (mode != kEventFinished) {
+                ScalarPath path = w.path[i];
+                Connection c = w.conn[i];
+                if (s.instance_count == 0) {
+                    if (scalar_sky_step(s, p, path))
+                        mode = kEventFinished;
+                } else if (mode == kEventPath && !scalar_ray_valid(path)) {
+                    path.status = S_ARITHMETIC;
+                    mode = kEventFinished;
+                } else {
+                    const Hit hit = w.hit[i];
+                    const bool ok = (m & kWalkOk) != 0;
+                    mode = mode == kEventPath ? shade_event(s, p, q, path, ok, hit, c)
+                                              : connection_step(s, q, path, c, ok, hit);
+                }
+                if (mode == kEventFinished) {
+                    q.out[path.lane] = scalar_record(path);
+                    finished_now = true;
+                } else {
+                    w.path[i] = path;
+                    w.conn[i] = c;
+                }
+                w.mode[i] = mode;
+            }
+        }
+        // records written this trip
+        const u32 done = __ballot_sync(0xffffffffu, finished_now);
+        if (lane_in_warp == 0 && done)
+            atomicSub(w.remaining, __popc(done));
+        // refill (the counter stops growing once the wave's lanes are all taken)
+        const u32 want = __ballot_sync(0xffffffffu, i < w.count && mode == kEventFinished);
+        u32 base = p.lanes;
+        if (lane_in_warp == 0 && want && *reinterpret_cast<volatile u32 *>(q.next_lane) < p.lanes)
+            base = atomicAdd(q.next_lane, __popc(want));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (i < w.count && mode == kEventFinished) {
+            const u32 lane = base + __popc(want & ((1u << lane_in_warp) - 1));
+            if (lane < p.lanes) {
+                ScalarPath path;
+                scalar_start(s, p, q, lane, path);
+                w.path[i] = path;
+                w.mode[i] = kEventPath;
+            }
+        }
+    }
+}
+
 // RenderSample rows for the driver-compatible scalar entry point (src/metal_render.mm:2136-2166).
 struct ScalarResult {
     u32 status, pixel, sample_low, sample_high;
