@@ -938,8 +938,6 @@ void run_wave(rp_scene *s, const WaveParams &request_params, size_t adjoint_smem
     RP_CHECK(cudaGetLastError());
 }
 
-// One wave of the scalar transport: the persistent regeneration kernel over p.lanes lanes,
-// one record per lane in s->scalar_records.
 // Slots of the scalar wavefront: per slot one ScalarPath, one Connection, a mode word and a hit.
 ScalarSlots scalar_slots(rp_scene *s, u32 count) {
     const size_t a = (size_t(count) * sizeof(ScalarPath) + 255) & ~size_t(255);
@@ -966,8 +964,11 @@ ScalarSlots scalar_slots(rp_scene *s, u32 count) {
 }
 
 // Slots of the scalar wavefront (at most this many paths in flight per wave), and the
-// walk/step trips between two host reads of the wave's remaining lanes.
-constexpr u32 kScalarSlots = 1u << 20;
+// walk/step trips between two host reads of the wave's remaining lanes.  131,072 slots of
+// about 212 bytes keep the whole path state (28 MB) in L2 and still give the step kernel
+// more than two paths per resident thread; measured on the fog box (1024x1024, 16 spp):
+// 2^16 slots 440 ms, 2^17 415 ms, 2^18 431-448 ms, 2^19 529 ms, 2^20 634 ms.
+constexpr u32 kScalarSlots = 1u << 17;
 constexpr int kScalarTripsPerCheck = 8;
 
 // One wave of the scalar transport, one record per lane in s->scalar_records: camera rays,

@@ -4,12 +4,13 @@
 // participating media with this transport only (hero transport requires vacuum,
 // src/render.cpp:1579-1580).
 //
-// B200 form: one persistent kernel whose threads regenerate paths.  Every thread owns one
-// path in registers and runs one event (closest hit, then medium or surface interaction
-// with its light connection) per loop trip; a thread whose path finished takes the next
-// lane from a global counter (one atomic per warp), so warps stay full until the wave's
-// lanes run out instead of idling behind their longest path.  Results leave as one 16-byte
-// record per lane; the film reduction reads them in canonical order.
+// B200 form: a wavefront over 131,072 resident path slots.  A trip of every slot is one
+// closest-hit query (k_scalar_walk: the path's ray or the current leg of its light
+// connection, at the walk's own occupancy) and the medium / surface event or connection step
+// that consumes it (k_scalar_step); a slot whose path finished takes the next lane from a
+// global counter (one atomic per warp), so the slots stay full until the wave's lanes run
+// out.  Results leave as one 16-byte record per lane; the film reduction reads them in
+// canonical order.
 //
 // Surfaces: diffuse reflectance and null interfaces (material scattering 10).  Lights: area
 // triangles, point and spot lights, constant environment.  Media: homogeneous, 471-bin
@@ -289,7 +290,7 @@ RP_DEV bool incident_delta(const Incident &l) { return l.kind == kIncidentPositi
 
 
 // ------------------------------------------------------------------ path state
-// ScalarState (shaders/scalar_transport.h:38-52) held in registers for the life of a path.
+// ScalarState (shaders/scalar_transport.h:38-52), kept in a wavefront slot between trips.
 struct ScalarPath {
     u32 lane, pixel, slo, shi, status, scatterings;
     u64 index;
@@ -328,7 +329,7 @@ struct ScalarParams {
 };
 
 // begin_sample + primary_ray + the wavelength of scalar_init (shaders/scalar_transport.h:64-77)
-// for every lane of a wave, written once so the persistent kernel starts paths with loads.
+// for every lane of a wave, written once so the step kernel starts paths with loads.
 __global__ void k_scalar_raygen(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p,
                                 float4 *ray, uint2 *index) {
     for (u32 lane = blockIdx.x * blockDim.x + threadIdx.x; lane < p.lanes; lane += gridDim.x * blockDim.x) {
@@ -926,102 +927,14 @@ RP_DEV uint4 scalar_record(const ScalarPath &path) {
     return make_uint4(status, __float_as_uint(path.wavelength), __float_as_uint(path.radiance), path.scatterings);
 }
 
-// Persistent path-regeneration kernel over the lanes of one wave.  Each trip of the loop
-// runs one closest-hit query per thread -- the path's ray or the current leg of its light
-// connection -- at a single call site, then the path event or the connection step.  A thread
-// whose path finished takes the next lane (one atomic per warp), so warps stay full until
-// the wave's lanes run out.
-template <bool Count, int Stack = kStackDepth>
-__global__ void __launch_bounds__(kTraceBlock) k_volpath(const __grid_constant__ DeviceScene s,
-                                                         const __grid_constant__ WaveParams p, ScalarParams q) {
-    __shared__ uint2 stack[Stack * kTraceBlock];
-    uint2 *my_stack = stack + threadIdx.x;
-    const int lane_in_warp = threadIdx.x & 31;
-    u32 counts[6] = {0, 0, 0, 0, 0, 0};
-    ScalarPath path;
-    Connection c;
-    int mode = kEventFinished;
-    bool exhausted = false; // the wave's lanes are all taken
-    while (true) {
-        if (!exhausted) {
-            const u32 want = __ballot_sync(0xffffffffu, mode == kEventFinished);
-            u32 base = 0;
-            if (lane_in_warp == 0 && want)
-                base = atomicAdd(q.next_lane, __popc(want));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (mode == kEventFinished) {
-                const u32 lane = base + __popc(want & ((1u << lane_in_warp) - 1));
-                if (lane < p.lanes) {
-                    scalar_start(s, p, q, lane, path);
-                    mode = kEventPath;
-                }
-            }
-            exhausted = base + __popc(want) >= p.lanes;
-        }
-        if (!__any_sync(0xffffffffu, mode != kEventFinished))
-            break;
-        if (mode == kEventFinished)
-            continue;
-        if (s.instance_count == 0) {
-            if (scalar_sky_step(s, p, path)) {
-                q.out[path.lane] = scalar_record(path);
-                mode = kEventFinished;
-            }
-            continue;
-        }
-        // scalar_trace (shaders/scalar_transport.h:268-283): validate, then the one query
-        V3 ro, rd;
-        float tmax;
-        if (mode == kEventPath) {
-            if (!finite3(path.o) || !finite3(path.d) || !isfinite(path.throughput) || !isfinite(path.radiance)) {
-                path.status = S_ARITHMETIC;
-                q.out[path.lane] = scalar_record(path);
-                mode = kEventFinished;
-                continue;
-            }
-            ro = path.o;
-            rd = path.d;
-            tmax = finf();
-        } else {
-            ro = c.o;
-            rd = c.d;
-            tmax = c.remaining;
-        }
-        Hit hit;
-        u32 nodes = 0, tris = 0;
-        const bool ok = walk_closest<Count, Stack>(s, ro, rd, tmax, hit, my_stack, kTraceBlock, nodes, tris);
-        if (Count) {
-            if (mode == kEventPath) {
-                counts[0] += nodes;
-                counts[1] += tris;
-                counts[2] += 1;
-            } else {
-                counts[3] += 1;
-                counts[4] += nodes;
-                counts[5] += tris;
-            }
-        }
-        mode = mode == kEventPath ? shade_event(s, p, q, path, ok, hit, c) : connection_step(s, q, path, c, ok, hit);
-        if (mode == kEventFinished)
-            q.out[path.lane] = scalar_record(path);
-    }
-    if (Count) {
-        atomicAdd(q.stats + 0, (unsigned long long)counts[0]);
-        atomicAdd(q.stats + 1, (unsigned long long)counts[1]);
-        atomicAdd(q.stats + 2, (unsigned long long)counts[2]);
-        atomicAdd(q.stats + 3, (unsigned long long)counts[3]);
-        atomicAdd(q.stats + 4, (unsigned long long)counts[4]);
-        atomicAdd(q.stats + 5, (unsigned long long)counts[5]);
-    }
-}
-
-// Wavefront form of the scalar transport: the loop body of k_volpath split at its one
-// closest-hit query, with each path and its light connection in flight held in a slot in
-// global memory between the two kernels.  k_scalar_walk runs the query of every slot (the
-// path's ray or the current leg of its connection) at the walk's own occupancy;
-// k_scalar_step runs the event or connection step that consumes it and hands finished slots
-// the wave's next lanes.  Each lane's path depends only on its own indices, so every record
-// equals the persistent kernel's.
+// Wavefront form of the scalar transport (rypath_render_paths, shaders/scalar_transport.h):
+// each trip of a path is one closest-hit query -- the path's ray or the current leg of its
+// light connection -- and the event or connection step that consumes it.  Each path and its
+// connection in flight stay in a slot in global memory between the two kernels:
+// k_scalar_walk runs the query of every slot at the walk's own occupancy, k_scalar_step the
+// event or connection step and hands finished slots the wave's next lanes.  Each lane's path
+// depends only on its own indices, so its record does not depend on the slot or trip that
+// ran it.
 struct ScalarSlots {
     ScalarPath *path;
     Connection *conn;
