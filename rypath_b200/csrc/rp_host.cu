@@ -938,18 +938,20 @@ void run_wave(rp_scene *s, const WaveParams &request_params, size_t adjoint_smem
     RP_CHECK(cudaGetLastError());
 }
 
-// Slots of the scalar wavefront: per slot one ScalarPath, one Connection, a mode word and a hit.
+// Slots of the scalar wavefront: per slot one ScalarPath, one Connection, a mode word and a
+// hit, and per trip parity the two step queues.
 ScalarSlots scalar_slots(rp_scene *s, u32 count) {
     const size_t a = (size_t(count) * sizeof(ScalarPath) + 255) & ~size_t(255);
     const size_t b = (size_t(count) * sizeof(Connection) + 255) & ~size_t(255);
     const size_t c = (size_t(count) * sizeof(u32) + 255) & ~size_t(255);
     const size_t d = (size_t(count) * sizeof(Hit) + 255) & ~size_t(255);
+    const size_t e = (size_t(count) * sizeof(u32) + 255) & ~size_t(255);
     if (s->slot_capacity < count) {
         if (s->slot_storage)
             cudaFreeAsync(s->slot_storage, s->stream);
         s->slot_storage = nullptr;
         s->slot_capacity = 0;
-        RP_CHECK(cudaMallocAsync(&s->slot_storage, a + b + c + d, s->stream));
+        RP_CHECK(cudaMallocAsync(&s->slot_storage, a + b + c + d + 4 * e, s->stream));
         s->slot_capacity = count;
     }
     unsigned char *base = static_cast<unsigned char *>(s->slot_storage);
@@ -958,8 +960,13 @@ ScalarSlots scalar_slots(rp_scene *s, u32 count) {
     w.conn = reinterpret_cast<Connection *>(base + a);
     w.mode = reinterpret_cast<u32 *>(base + a + b);
     w.hit = reinterpret_cast<Hit *>(base + a + b + c);
+    for (int k = 0; k < 2; ++k) {
+        w.queue_connect[k] = reinterpret_cast<u32 *>(base + a + b + c + d + (2 * k) * e);
+        w.queue_path[k] = reinterpret_cast<u32 *>(base + a + b + c + d + (2 * k + 1) * e);
+    }
     w.count = count;
     w.remaining = s->scalar_counters + 2;
+    w.qcount = s->scalar_counters + 4; // zeroed with the wave's counters
     return w;
 }
 
@@ -1001,7 +1008,9 @@ void run_scalar_wave(rp_scene *s, const WaveParams &p, u32 boundary_limit) {
     const bool short_stack = s->wide_levels <= u32(kShortStack);
     s->mark(2, 2);
     k_scalar_slots_init<<<grid_for(s->sm_count, slots, 256, 8), 256, 0, s->stream>>>(w.mode, slots);
-    k_scalar_step<<<step_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q, w);
+    k_scalar_step<<<step_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q, w, -1);
+    const bool walks = s->ds.instance_count != 0; // geometry-free scenes take the sky step
+    int parity = 0;
     RP_CHECK(cudaGetLastError());
     // every trip advances each unfinished path by one walk and one step, so a wave ends after
     // at most (its lanes' steps) trips; the bound only guards the host loop
@@ -1010,16 +1019,22 @@ void run_scalar_wave(rp_scene *s, const WaveParams &p, u32 boundary_limit) {
         if (trip > (u64(1) << 22))
             throw Invalid{"scalar wave did not finish"};
         for (int k = 0; k < kScalarTripsPerCheck; ++k) {
+            if (!walks) {
+                k_scalar_step<<<step_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q, w, -1);
+                s->launches += 1;
+                continue;
+            }
             if (s->counting && short_stack)
-                k_scalar_walk<true, kShortStack><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, w, s->stats);
+                k_scalar_walk<true, kShortStack><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, w, parity, s->stats);
             else if (s->counting)
-                k_scalar_walk<true, kStackDepth><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, w, s->stats);
+                k_scalar_walk<true, kStackDepth><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, w, parity, s->stats);
             else if (short_stack)
-                k_scalar_walk<false, kShortStack><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, w, s->stats);
+                k_scalar_walk<false, kShortStack><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, w, parity, s->stats);
             else
-                k_scalar_walk<false, kStackDepth><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, w, s->stats);
-            k_scalar_step<<<step_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q, w);
+                k_scalar_walk<false, kStackDepth><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, w, parity, s->stats);
+            k_scalar_step<<<step_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q, w, parity);
             s->launches += 2;
+            parity ^= 1;
         }
         RP_CHECK(cudaGetLastError());
         RP_CHECK(cudaMemcpyAsync(&remaining, w.remaining, sizeof(u32), cudaMemcpyDeviceToHost, s->stream));

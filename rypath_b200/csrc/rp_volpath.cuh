@@ -942,6 +942,10 @@ struct ScalarSlots {
     Hit *hit;       // the walk's hit
     u32 count;      // slots
     u32 *remaining; // lanes of the wave whose record is not written yet
+    // the active slots of a trip sorted by what their step runs, so that a step warp runs one
+    // kind: [parity] connection steps and path events, counted in qcount[2 parity + 0 / 1]
+    u32 *queue_connect[2], *queue_path[2];
+    u32 *qcount;
 };
 constexpr u32 kWalkOk = 1u << 8;
 
@@ -949,46 +953,67 @@ RP_DEV bool scalar_ray_valid(const ScalarPath &path) {
     return finite3(path.o) && finite3(path.d) && isfinite(path.throughput) && isfinite(path.radiance);
 }
 
+// Warp-aggregated append of `slot` to `queue` (counter `count`) for the lanes with `want`.
+RP_DEV void slot_append(u32 *queue, u32 *count, bool want, u32 slot) {
+    const u32 ballot = __ballot_sync(0xffffffffu, want);
+    const int lane = threadIdx.x & 31;
+    u32 base = 0;
+    if (lane == 0 && ballot)
+        base = atomicAdd(count, __popc(ballot));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (want)
+        queue[base + __popc(ballot & ((1u << lane) - 1))] = slot;
+}
+
 template <bool Count, int Stack = kStackDepth>
 __global__ void __launch_bounds__(kTraceBlock, Stack <= kShortStack ? 1024 / kTraceBlock : 1)
-    k_scalar_walk(const __grid_constant__ DeviceScene s, ScalarSlots w, unsigned long long *stats) {
+    k_scalar_walk(const __grid_constant__ DeviceScene s, ScalarSlots w, int parity, unsigned long long *stats) {
     __shared__ uint2 stack[Stack * kTraceBlock];
     u32 counts[6] = {0, 0, 0, 0, 0, 0};
-    if (s.instance_count == 0)
-        return; // geometry-free scenes take the sky step, which needs no walk
-    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < w.count; i += gridDim.x * blockDim.x) {
-        const u32 mode = w.mode[i] & 0xffu;
-        if (mode == kEventFinished)
-            continue;
-        V3 ro, rd;
-        float tmax;
-        if (mode == kEventPath) {
-            const ScalarPath &path = w.path[i];
-            ro = path.o;
-            rd = path.d;
-            if (!scalar_ray_valid(path))
-                continue; // the step kernel records the failure
-            tmax = finf();
-        } else {
-            const Connection &c = w.conn[i];
-            ro = c.o;
-            rd = c.d;
-            tmax = c.remaining;
+    const u32 stride = gridDim.x * blockDim.x;
+    const u32 trips = (w.count + stride - 1) / stride;
+    for (u32 trip = 0; trip < trips; ++trip) {
+        const u32 i = trip * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        u32 mode = kEventFinished;
+        if (i < w.count) {
+            mode = w.mode[i] & 0xffu;
+            if (mode != kEventFinished) {
+                V3 ro, rd;
+                float tmax;
+                bool walk = true;
+                if (mode == kEventPath) {
+                    const ScalarPath &path = w.path[i];
+                    ro = path.o;
+                    rd = path.d;
+                    walk = scalar_ray_valid(path); // else the step kernel records the failure
+                    tmax = finf();
+                } else {
+                    const Connection &c = w.conn[i];
+                    ro = c.o;
+                    rd = c.d;
+                    tmax = c.remaining;
+                }
+                if (walk) {
+                    Hit hit;
+                    u32 nodes = 0, tris = 0;
+                    const bool ok =
+                        walk_closest<Count, Stack>(s, ro, rd, tmax, hit, stack + threadIdx.x, kTraceBlock, nodes, tris);
+                    w.hit[i] = hit;
+                    w.mode[i] = mode | (ok ? kWalkOk : 0u);
+                    if (Count && mode == kEventPath) {
+                        counts[0] += nodes;
+                        counts[1] += tris;
+                        counts[2] += 1;
+                    } else if (Count) {
+                        counts[3] += 1;
+                        counts[4] += nodes;
+                        counts[5] += tris;
+                    }
+                }
+            }
         }
-        Hit hit;
-        u32 nodes = 0, tris = 0;
-        const bool ok = walk_closest<Count, Stack>(s, ro, rd, tmax, hit, stack + threadIdx.x, kTraceBlock, nodes, tris);
-        w.hit[i] = hit;
-        w.mode[i] = mode | (ok ? kWalkOk : 0u);
-        if (Count && mode == kEventPath) {
-            counts[0] += nodes;
-            counts[1] += tris;
-            counts[2] += 1;
-        } else if (Count) {
-            counts[3] += 1;
-            counts[4] += nodes;
-            counts[5] += tris;
-        }
+        slot_append(w.queue_connect[parity], w.qcount + 2 * parity, mode == kEventConnect, i);
+        slot_append(w.queue_path[parity], w.qcount + 2 * parity + 1, mode == kEventPath, i);
     }
     if (Count) {
         atomicAdd(stats + 0, (unsigned long long)counts[0]);
@@ -1005,19 +1030,31 @@ __global__ void k_scalar_slots_init(u32 *mode, u32 count) {
         mode[i] = kEventFinished;
 }
 
-// The event (or connection step, or geometry-free sky step) of every active slot, then new
-// lanes for the finished ones (one atomic per warp).
+// The event (or connection step, or geometry-free sky step) of the active slots, then new
+// lanes for the finished ones (one atomic per warp).  parity >= 0: the slots the walk of this
+// trip queued, connection steps first, then path events; parity < 0: every slot (the wave's
+// first fill, and geometry-free scenes, which take no walk).
 __global__ void __launch_bounds__(kTraceBlock) k_scalar_step(const __grid_constant__ DeviceScene s,
                                                              const __grid_constant__ WaveParams p, ScalarParams q,
-                                                             ScalarSlots w) {
+                                                             ScalarSlots w, int parity) {
     const int lane_in_warp = threadIdx.x & 31;
+    u32 n_connect = 0, total = w.count;
+    if (parity >= 0) {
+        n_connect = w.qcount[2 * parity];
+        total = n_connect + w.qcount[2 * parity + 1];
+        if (blockIdx.x == 0 && threadIdx.x < 2)
+            w.qcount[2 * (parity ^ 1) + threadIdx.x] = 0; // the next trip's walk appends there
+    }
     const u32 stride = gridDim.x * blockDim.x;
-    const u32 trips = (w.count + stride - 1) / stride;
+    const u32 trips = (total + stride - 1) / stride;
     for (u32 trip = 0; trip < trips; ++trip) {
-        const u32 i = trip * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        const u32 k = trip * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        u32 i = k;
+        if (parity >= 0 && k < total)
+            i = k < n_connect ? w.queue_connect[parity][k] : w.queue_path[parity][k - n_connect];
         u32 mode = kEventFinished;
         bool finished_now = false;
-        if (i < w.count) {
+        if (k < total) {
             const u32 m = w.mode[i];
             mode = m & 0xffu;
             if (mode != kEventFinished) {
@@ -1050,12 +1087,12 @@ __global__ void __launch_bounds__(kTraceBlock) k_scalar_step(const __grid_consta
         if (lane_in_warp == 0 && done)
             atomicSub(w.remaining, __popc(done));
         // refill (the counter stops growing once the wave's lanes are all taken)
-        const u32 want = __ballot_sync(0xffffffffu, i < w.count && mode == kEventFinished);
+        const u32 want = __ballot_sync(0xffffffffu, k < total && mode == kEventFinished);
         u32 base = p.lanes;
         if (lane_in_warp == 0 && want && *reinterpret_cast<volatile u32 *>(q.next_lane) < p.lanes)
             base = atomicAdd(q.next_lane, __popc(want));
         base = __shfl_sync(0xffffffffu, base, 0);
-        if (i < w.count && mode == kEventFinished) {
+        if (k < total && mode == kEventFinished) {
             const u32 lane = base + __popc(want & ((1u << lane_in_warp) - 1));
             if (lane < p.lanes) {
                 ScalarPath path;
