@@ -218,7 +218,7 @@ def bench_fog(torch, cpu_seconds):
     dt = time.perf_counter() - t0
     return {"workload": "cornell_fog_1024x1024_64spp_depth32 (scalar volpath, homogeneous medium)",
             "metric": "scalar path Msamples/s", "value": value, "unit": UNIT, "ms_per_step": t.total_ms,
-            "kernel": "k_scalar_walk + k_scalar_step (wavefront over 131,072 resident path slots)",
+            "kernel": "k_scalar_walk + k_scalar_step (wavefront over 262,144 resident path slots)",
             "rays_per_sample": rays_per_sample, "mrays_per_s": value * rays_per_sample,
             "cpu_baseline": {"value": out.size / dt / 1e6, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                              "sample": f"{out.size} lanes (1 spp of pixels around the film centre), {dt:.2f} s"}}

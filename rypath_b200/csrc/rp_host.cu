@@ -971,11 +971,12 @@ ScalarSlots scalar_slots(rp_scene *s, u32 count) {
 }
 
 // Slots of the scalar wavefront (at most this many paths in flight per wave), and the
-// walk/step trips between two host reads of the wave's remaining lanes.  131,072 slots of
-// about 212 bytes keep the whole path state (28 MB) in L2 and still give the step kernel
-// more than two paths per resident thread; measured on the fog box (1024x1024, 16 spp):
-// 2^16 slots 440 ms, 2^17 415 ms, 2^18 431-448 ms, 2^19 529 ms, 2^20 634 ms.
-constexpr u32 kScalarSlots = 1u << 17;
+// walk/step trips between two host reads of the wave's remaining lanes.  262,144 slots of
+// about 230 bytes (path, connection, mode, hit, queue entries) keep the path state (60 MB)
+// in L2 and give the step kernel several paths per resident thread; measured on the fog box
+// (1024x1024, 16 spp) with the step queues: 2^16 slots 314 ms, 2^17 317 ms, 2^18 300 ms;
+// without them 2^17 415 ms, 2^19 529 ms, 2^20 634 ms.
+constexpr u32 kScalarSlots = 1u << 18;
 constexpr int kScalarTripsPerCheck = 8;
 
 // One wave of the scalar transport, one record per lane in s->scalar_records: camera rays,

@@ -4,7 +4,7 @@
 // participating media with this transport only (hero transport requires vacuum,
 // src/render.cpp:1579-1580).
 //
-// B200 form: a wavefront over 131,072 resident path slots.  A trip of every slot is one
+// B200 form: a wavefront over 262,144 resident path slots.  A trip of every slot is one
 // closest-hit query (k_scalar_walk: the path's ray or the current leg of its light
 // connection, at the walk's own occupancy) and the medium / surface event or connection step
 // that consumes it (k_scalar_step); a slot whose path finished takes the next lane from a
