@@ -951,7 +951,7 @@ ScalarSlots scalar_slots(rp_scene *s, u32 count) {
             cudaFreeAsync(s->slot_storage, s->stream);
         s->slot_storage = nullptr;
         s->slot_capacity = 0;
-        RP_CHECK(cudaMallocAsync(&s->slot_storage, a + b + c + d + 4 * e, s->stream));
+        RP_CHECK(cudaMallocAsync(&s->slot_storage, a + b + c + d + 6 * e, s->stream));
         s->slot_capacity = count;
     }
     unsigned char *base = static_cast<unsigned char *>(s->slot_storage);
@@ -961,8 +961,9 @@ ScalarSlots scalar_slots(rp_scene *s, u32 count) {
     w.mode = reinterpret_cast<u32 *>(base + a + b);
     w.hit = reinterpret_cast<Hit *>(base + a + b + c);
     for (int k = 0; k < 2; ++k) {
-        w.queue_connect[k] = reinterpret_cast<u32 *>(base + a + b + c + d + (2 * k) * e);
-        w.queue_path[k] = reinterpret_cast<u32 *>(base + a + b + c + d + (2 * k + 1) * e);
+        w.queue_connect[k] = reinterpret_cast<u32 *>(base + a + b + c + d + (3 * k) * e);
+        w.queue_medium[k] = reinterpret_cast<u32 *>(base + a + b + c + d + (3 * k + 1) * e);
+        w.queue_path[k] = reinterpret_cast<u32 *>(base + a + b + c + d + (3 * k + 2) * e);
     }
     w.count = count;
     w.remaining = s->scalar_counters + 2;
@@ -1026,13 +1027,13 @@ void run_scalar_wave(rp_scene *s, const WaveParams &p, u32 boundary_limit) {
                 continue;
             }
             if (s->counting && short_stack)
-                k_scalar_walk<true, kShortStack><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, w, parity, s->stats);
+                k_scalar_walk<true, kShortStack><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, w, parity, s->stats);
             else if (s->counting)
-                k_scalar_walk<true, kStackDepth><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, w, parity, s->stats);
+                k_scalar_walk<true, kStackDepth><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, w, parity, s->stats);
             else if (short_stack)
-                k_scalar_walk<false, kShortStack><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, w, parity, s->stats);
+                k_scalar_walk<false, kShortStack><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, w, parity, s->stats);
             else
-                k_scalar_walk<false, kStackDepth><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, w, parity, s->stats);
+                k_scalar_walk<false, kStackDepth><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, w, parity, s->stats);
             k_scalar_step<<<step_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q, w, parity);
             s->launches += 2;
             parity ^= 1;

@@ -943,8 +943,9 @@ struct ScalarSlots {
     u32 count;      // slots
     u32 *remaining; // lanes of the wave whose record is not written yet
     // the active slots of a trip sorted by what their step runs, so that a step warp runs one
-    // kind: [parity] connection steps and path events, counted in qcount[2 parity + 0 / 1]
-    u32 *queue_connect[2], *queue_path[2];
+    // kind: [parity] connection steps, path events that scatter in their medium, other path
+    // events, counted in qcount[3 parity + 0 / 1 / 2]
+    u32 *queue_connect[2], *queue_medium[2], *queue_path[2];
     u32 *qcount;
 };
 constexpr u32 kWalkOk = 1u << 8;
@@ -965,9 +966,28 @@ RP_DEV void slot_append(u32 *queue, u32 *count, bool want, u32 slot) {
         queue[base + __popc(ballot & ((1u << lane) - 1))] = slot;
 }
 
+// Whether shade_event will take its medium-scattering branch for this hit: the same medium
+// lookup and free-flight draw, without consuming the draw.  Only groups the step warps; the
+// step itself decides.
+RP_DEV bool predicts_medium_scatter(const DeviceScene &s, const WaveParams &p, const ScalarPath &path, const Hit &hit) {
+    if (path.current_medium == kNone || path.current_medium >= s.medium_count ||
+        path.medium_draw >= kMediumBlockLimit - 3)
+        return false;
+    const float *m = medium_record(s, path.current_medium);
+    const u32 wi = dense_index(path.wavelength);
+    const float total = __ldg(m + wi) + __ldg(m + 471 + wi);
+    if (!(total > 0))
+        return false;
+    const float distance = hit.prim == kNone ? finf() : hit.t * length3(path.d);
+    u32 draw = path.medium_draw;
+    const float flight = medium_flight(total, u01(medium_words(p, path.pixel, path.slo, path.shi, draw).x));
+    return flight < distance || isinf(distance);
+}
+
 template <bool Count, int Stack = kStackDepth>
 __global__ void __launch_bounds__(kTraceBlock, Stack <= kShortStack ? 1024 / kTraceBlock : 1)
-    k_scalar_walk(const __grid_constant__ DeviceScene s, ScalarSlots w, int parity, unsigned long long *stats) {
+    k_scalar_walk(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p, ScalarSlots w,
+                  int parity, unsigned long long *stats) {
     __shared__ uint2 stack[Stack * kTraceBlock];
     u32 counts[6] = {0, 0, 0, 0, 0, 0};
     const u32 stride = gridDim.x * blockDim.x;
@@ -975,14 +995,15 @@ __global__ void __launch_bounds__(kTraceBlock, Stack <= kShortStack ? 1024 / kTr
     for (u32 trip = 0; trip < trips; ++trip) {
         const u32 i = trip * stride + blockIdx.x * blockDim.x + threadIdx.x;
         u32 mode = kEventFinished;
+        bool scatter = false;
         if (i < w.count) {
             mode = w.mode[i] & 0xffu;
             if (mode != kEventFinished) {
                 V3 ro, rd;
                 float tmax;
                 bool walk = true;
+                const ScalarPath &path = w.path[i];
                 if (mode == kEventPath) {
-                    const ScalarPath &path = w.path[i];
                     ro = path.o;
                     rd = path.d;
                     walk = scalar_ray_valid(path); // else the step kernel records the failure
@@ -1000,6 +1021,7 @@ __global__ void __launch_bounds__(kTraceBlock, Stack <= kShortStack ? 1024 / kTr
                         walk_closest<Count, Stack>(s, ro, rd, tmax, hit, stack + threadIdx.x, kTraceBlock, nodes, tris);
                     w.hit[i] = hit;
                     w.mode[i] = mode | (ok ? kWalkOk : 0u);
+                    scatter = ok && mode == kEventPath && predicts_medium_scatter(s, p, path, hit);
                     if (Count && mode == kEventPath) {
                         counts[0] += nodes;
                         counts[1] += tris;
@@ -1012,8 +1034,9 @@ __global__ void __launch_bounds__(kTraceBlock, Stack <= kShortStack ? 1024 / kTr
                 }
             }
         }
-        slot_append(w.queue_connect[parity], w.qcount + 2 * parity, mode == kEventConnect, i);
-        slot_append(w.queue_path[parity], w.qcount + 2 * parity + 1, mode == kEventPath, i);
+        slot_append(w.queue_connect[parity], w.qcount + 3 * parity, mode == kEventConnect, i);
+        slot_append(w.queue_medium[parity], w.qcount + 3 * parity + 1, mode == kEventPath && scatter, i);
+        slot_append(w.queue_path[parity], w.qcount + 3 * parity + 2, mode == kEventPath && !scatter, i);
     }
     if (Count) {
         atomicAdd(stats + 0, (unsigned long long)counts[0]);
@@ -1032,18 +1055,20 @@ __global__ void k_scalar_slots_init(u32 *mode, u32 count) {
 
 // The event (or connection step, or geometry-free sky step) of the active slots, then new
 // lanes for the finished ones (one atomic per warp).  parity >= 0: the slots the walk of this
-// trip queued, connection steps first, then path events; parity < 0: every slot (the wave's
-// first fill, and geometry-free scenes, which take no walk).
+// trip queued, connection steps first, then medium-scattering path events, then the other
+// path events; parity < 0: every slot (the wave's first fill, and geometry-free scenes, which
+// take no walk).
 __global__ void __launch_bounds__(kTraceBlock) k_scalar_step(const __grid_constant__ DeviceScene s,
                                                              const __grid_constant__ WaveParams p, ScalarParams q,
                                                              ScalarSlots w, int parity) {
     const int lane_in_warp = threadIdx.x & 31;
-    u32 n_connect = 0, total = w.count;
+    u32 n_connect = 0, n_medium = 0, total = w.count;
     if (parity >= 0) {
-        n_connect = w.qcount[2 * parity];
-        total = n_connect + w.qcount[2 * parity + 1];
-        if (blockIdx.x == 0 && threadIdx.x < 2)
-            w.qcount[2 * (parity ^ 1) + threadIdx.x] = 0; // the next trip's walk appends there
+        n_connect = w.qcount[3 * parity];
+        n_medium = n_connect + w.qcount[3 * parity + 1];
+        total = n_medium + w.qcount[3 * parity + 2];
+        if (blockIdx.x == 0 && threadIdx.x < 3)
+            w.qcount[3 * (parity ^ 1) + threadIdx.x] = 0; // the next trip's walk appends there
     }
     const u32 stride = gridDim.x * blockDim.x;
     const u32 trips = (total + stride - 1) / stride;
@@ -1051,7 +1076,9 @@ __global__ void __launch_bounds__(kTraceBlock) k_scalar_step(const __grid_consta
         const u32 k = trip * stride + blockIdx.x * blockDim.x + threadIdx.x;
         u32 i = k;
         if (parity >= 0 && k < total)
-            i = k < n_connect ? w.queue_connect[parity][k] : w.queue_path[parity][k - n_connect];
+            i = k < n_connect  ? w.queue_connect[parity][k]
+                : k < n_medium ? w.queue_medium[parity][k - n_connect]
+                               : w.queue_path[parity][k - n_medium];
         u32 mode = kEventFinished;
         bool finished_now = false;
         if (k < total) {
