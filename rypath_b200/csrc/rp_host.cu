@@ -951,7 +951,7 @@ ScalarSlots scalar_slots(rp_scene *s, u32 count) {
             cudaFreeAsync(s->slot_storage, s->stream);
         s->slot_storage = nullptr;
         s->slot_capacity = 0;
-        RP_CHECK(cudaMallocAsync(&s->slot_storage, a + b + c + d + 6 * e, s->stream));
+        RP_CHECK(cudaMallocAsync(&s->slot_storage, a + b + c + d + 8 * e, s->stream));
         s->slot_capacity = count;
     }
     unsigned char *base = static_cast<unsigned char *>(s->slot_storage);
@@ -961,9 +961,10 @@ ScalarSlots scalar_slots(rp_scene *s, u32 count) {
     w.mode = reinterpret_cast<u32 *>(base + a + b);
     w.hit = reinterpret_cast<Hit *>(base + a + b + c);
     for (int k = 0; k < 2; ++k) {
-        w.queue_connect[k] = reinterpret_cast<u32 *>(base + a + b + c + d + (3 * k) * e);
-        w.queue_medium[k] = reinterpret_cast<u32 *>(base + a + b + c + d + (3 * k + 1) * e);
-        w.queue_path[k] = reinterpret_cast<u32 *>(base + a + b + c + d + (3 * k + 2) * e);
+        w.queue_connect[k] = reinterpret_cast<u32 *>(base + a + b + c + d + (4 * k) * e);
+        w.queue_medium[k] = reinterpret_cast<u32 *>(base + a + b + c + d + (4 * k + 1) * e);
+        w.queue_interface[k] = reinterpret_cast<u32 *>(base + a + b + c + d + (4 * k + 2) * e);
+        w.queue_path[k] = reinterpret_cast<u32 *>(base + a + b + c + d + (4 * k + 3) * e);
     }
     w.count = count;
     w.remaining = s->scalar_counters + 2;

@@ -943,9 +943,9 @@ struct ScalarSlots {
     u32 count;      // slots
     u32 *remaining; // lanes of the wave whose record is not written yet
     // the active slots of a trip sorted by what their step runs, so that a step warp runs one
-    // kind: [parity] connection steps, path events that scatter in their medium, other path
-    // events, counted in qcount[3 parity + 0 / 1 / 2]
-    u32 *queue_connect[2], *queue_medium[2], *queue_path[2];
+    // kind: [parity] connection steps, path events that scatter in their medium, path events
+    // at a null interface, other path events, counted in qcount[4 parity + 0 / 1 / 2 / 3]
+    u32 *queue_connect[2], *queue_medium[2], *queue_interface[2], *queue_path[2];
     u32 *qcount;
 };
 constexpr u32 kWalkOk = 1u << 8;
@@ -983,6 +983,13 @@ RP_DEV bool predicts_medium_scatter(const DeviceScene &s, const WaveParams &p, c
     const float flight = medium_flight(total, u01(medium_words(p, path.pixel, path.slo, path.shi, draw).x));
     return flight < distance || isinf(distance);
 }
+// Whether the hit of a path event that does not scatter in its medium is a null interface.
+RP_DEV bool hits_interface(const DeviceScene &s, const Hit &hit) {
+    if (hit.prim == kNone || hit.prim >= s.prim_count)
+        return false;
+    const u32 material = s.instances[s.tri_instance[hit.prim]].material;
+    return material < s.material_count && s.materials[material].scattering == kInterfaceScattering;
+}
 
 template <bool Count, int Stack = kStackDepth>
 __global__ void __launch_bounds__(kTraceBlock, Stack <= kShortStack ? 1024 / kTraceBlock : 1)
@@ -995,7 +1002,7 @@ __global__ void __launch_bounds__(kTraceBlock, Stack <= kShortStack ? 1024 / kTr
     for (u32 trip = 0; trip < trips; ++trip) {
         const u32 i = trip * stride + blockIdx.x * blockDim.x + threadIdx.x;
         u32 mode = kEventFinished;
-        bool scatter = false;
+        bool scatter = false, interface = false;
         if (i < w.count) {
             mode = w.mode[i] & 0xffu;
             if (mode != kEventFinished) {
@@ -1022,6 +1029,7 @@ __global__ void __launch_bounds__(kTraceBlock, Stack <= kShortStack ? 1024 / kTr
                     w.hit[i] = hit;
                     w.mode[i] = mode | (ok ? kWalkOk : 0u);
                     scatter = ok && mode == kEventPath && predicts_medium_scatter(s, p, path, hit);
+                    interface = ok && mode == kEventPath && !scatter && hits_interface(s, hit);
                     if (Count && mode == kEventPath) {
                         counts[0] += nodes;
                         counts[1] += tris;
@@ -1034,9 +1042,10 @@ __global__ void __launch_bounds__(kTraceBlock, Stack <= kShortStack ? 1024 / kTr
                 }
             }
         }
-        slot_append(w.queue_connect[parity], w.qcount + 3 * parity, mode == kEventConnect, i);
-        slot_append(w.queue_medium[parity], w.qcount + 3 * parity + 1, mode == kEventPath && scatter, i);
-        slot_append(w.queue_path[parity], w.qcount + 3 * parity + 2, mode == kEventPath && !scatter, i);
+        slot_append(w.queue_connect[parity], w.qcount + 4 * parity, mode == kEventConnect, i);
+        slot_append(w.queue_medium[parity], w.qcount + 4 * parity + 1, mode == kEventPath && scatter, i);
+        slot_append(w.queue_interface[parity], w.qcount + 4 * parity + 2, mode == kEventPath && interface, i);
+        slot_append(w.queue_path[parity], w.qcount + 4 * parity + 3, mode == kEventPath && !scatter && !interface, i);
     }
     if (Count) {
         atomicAdd(stats + 0, (unsigned long long)counts[0]);
@@ -1055,20 +1064,21 @@ __global__ void k_scalar_slots_init(u32 *mode, u32 count) {
 
 // The event (or connection step, or geometry-free sky step) of the active slots, then new
 // lanes for the finished ones (one atomic per warp).  parity >= 0: the slots the walk of this
-// trip queued, connection steps first, then medium-scattering path events, then the other
-// path events; parity < 0: every slot (the wave's first fill, and geometry-free scenes, which
+// trip queued, connection steps first, then medium-scattering path events, null-interface
+// events and the other path events; parity < 0: every slot (the wave's first fill, and geometry-free scenes, which
 // take no walk).
 __global__ void __launch_bounds__(kTraceBlock) k_scalar_step(const __grid_constant__ DeviceScene s,
                                                              const __grid_constant__ WaveParams p, ScalarParams q,
                                                              ScalarSlots w, int parity) {
     const int lane_in_warp = threadIdx.x & 31;
-    u32 n_connect = 0, n_medium = 0, total = w.count;
+    u32 n_connect = 0, n_medium = 0, n_interface = 0, total = w.count;
     if (parity >= 0) {
-        n_connect = w.qcount[3 * parity];
-        n_medium = n_connect + w.qcount[3 * parity + 1];
-        total = n_medium + w.qcount[3 * parity + 2];
-        if (blockIdx.x == 0 && threadIdx.x < 3)
-            w.qcount[3 * (parity ^ 1) + threadIdx.x] = 0; // the next trip's walk appends there
+        n_connect = w.qcount[4 * parity];
+        n_medium = n_connect + w.qcount[4 * parity + 1];
+        n_interface = n_medium + w.qcount[4 * parity + 2];
+        total = n_interface + w.qcount[4 * parity + 3];
+        if (blockIdx.x == 0 && threadIdx.x < 4)
+            w.qcount[4 * (parity ^ 1) + threadIdx.x] = 0; // the next trip's walk appends there
     }
     const u32 stride = gridDim.x * blockDim.x;
     const u32 trips = (total + stride - 1) / stride;
@@ -1076,9 +1086,10 @@ __global__ void __launch_bounds__(kTraceBlock) k_scalar_step(const __grid_consta
         const u32 k = trip * stride + blockIdx.x * blockDim.x + threadIdx.x;
         u32 i = k;
         if (parity >= 0 && k < total)
-            i = k < n_connect  ? w.queue_connect[parity][k]
-                : k < n_medium ? w.queue_medium[parity][k - n_connect]
-                               : w.queue_path[parity][k - n_medium];
+            i = k < n_connect     ? w.queue_connect[parity][k]
+                : k < n_medium    ? w.queue_medium[parity][k - n_connect]
+                : k < n_interface ? w.queue_interface[parity][k - n_medium]
+                                  : w.queue_path[parity][k - n_interface];
         u32 mode = kEventFinished;
         bool finished_now = false;
         if (k < total) {
