@@ -1097,7 +1097,11 @@ __global__ void __launch_bounds__(kTraceBlock) k_scalar_step(const __grid_consta
             mode = m & 0xffu;
             if (mode != kEventFinished) {
                 ScalarPath path = w.path[i];
-                Connection c = w.conn[i];
+                // a connection in flight is read only by its steps, and a path event that
+                // begins one sets it up whole (connection_begin and the event's weights)
+                Connection c;
+                if (mode == kEventConnect)
+                    c = w.conn[i];
                 if (s.instance_count == 0) {
                     if (scalar_sky_step(s, p, path))
                         mode = kEventFinished;
@@ -1115,7 +1119,8 @@ __global__ void __launch_bounds__(kTraceBlock) k_scalar_step(const __grid_consta
                     finished_now = true;
                 } else {
                     w.path[i] = path;
-                    w.conn[i] = c;
+                    if (mode == kEventConnect)
+                        w.conn[i] = c;
                 }
                 w.mode[i] = mode;
             }
