@@ -1066,8 +1066,9 @@ __global__ void k_scalar_slots_init(u32 *mode, u32 count) {
 // lanes for the finished ones (one atomic per warp).  parity >= 0: the slots the walk of this
 // trip queued, connection steps first, then medium-scattering path events, null-interface
 // events and the other path events; parity < 0: every slot (the wave's first fill, and geometry-free scenes, which
-// take no walk).
-__global__ void __launch_bounds__(kTraceBlock) k_scalar_step(const __grid_constant__ DeviceScene s,
+// take no walk).  Four blocks of 128 per SM (128 registers, a few spilled) hide more of the
+// slot loads' latency than three at 154 registers: 133 against 143 ms on the fog box.
+__global__ void __launch_bounds__(kTraceBlock, 4) k_scalar_step(const __grid_constant__ DeviceScene s,
                                                              const __grid_constant__ WaveParams p, ScalarParams q,
                                                              ScalarSlots w, int parity) {
     const int lane_in_warp = threadIdx.x & 31;
