@@ -186,11 +186,12 @@ __global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1
 // One hero event after its closest hit (shaders/packet_pt_event_body.inc:11-461), for the paths
 // whose hit is of BSDF family F (3: no surface -- environment or a failed query).
 // Adjoint: the path-replay adjoint hooks are compiled in (the plain forward kernel carries none
-// of their registers).  The minimum of 384 resident threads per SM caps registers at 168, so
-// three 128-thread blocks fit an SM; the escape kernel (F = 3, no BSDF sampling or light
-// sample) fits 128 registers without spilling, so four.
+// of their registers).  The minimum of 512 resident threads per SM caps registers at 128, so
+// four 128-thread blocks fit an SM; the escape kernel (F = 3) fits without spilling, the
+// other families spill about 500 bytes to L1 and still run a little faster than three blocks
+// at 168 registers (113.5 against 115.0 ms per 1080p 16-spp frame of the mixed scene).
 template <int F, int Block = 128, bool Adjoint = false>
-__global__ void __launch_bounds__(Block, (F == 3 ? 512 : 384) / Block) k_shade(const __grid_constant__ DeviceScene s,
+__global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_constant__ DeviceScene s,
                                                               const __grid_constant__ WaveParams p, PathPool pool, int in) {
     extern __shared__ float sgrad[]; // adjoint only
     if (Adjoint)
