@@ -5,8 +5,7 @@
  * binds its renderer through C++ (`build_metal_renderer` / `MetalRenderScene::sample`,
  * src/metal_render.hpp:14-95) behind the progressive driver's sample-source seam
  * (`detail::RenderSampleSource`, src/render_driver.hpp:6-14).  Every entry point below is
- * what a C++ adapter in the reference's tree calls instead of Objective-C++/Metal; the
- * adapter itself is shown in INTEGRATION.md.
+ * what a C++ adapter in the reference's tree calls instead of Objective-C++/Metal.
  *
  * Conventions (the reference's, src/metal_render.hpp:47-52 and src/render_driver.cpp:280-283):
  *   - No exceptions cross the boundary: every call returns an rp_status and writes a
@@ -451,8 +450,9 @@ rp_status rp_cuda_trace_rays(struct rp_scene *scene, const float *rays, uint32_t
  * allocated: no cudaMalloc / cudaMallocAsync / cudaFree and no allocating library call.
  *   - Limit: request lanes (pixel_count * sample_count) <= RP_STATIC_MAX_LANES;
  *     larger requests return RP_INVALID_ARGUMENT with a diagnostic naming the maximum.
- *   - The first call on a device looks up the array's device address once, with that device
- *     current; make that first call before any stream capture.
+ *   - The first call on a scene looks up the array's device address once, with the scene's
+ *     device current, and keeps it with the scene; make that first call before any stream
+ *     capture.
  *   - Work runs on `stream` (a cudaStream_t; NULL = the scene's stream) and is complete when
  *     the stream is.  Every call shares the one array: calls whose GPU work overlaps (two
  *     streams, two scenes, two threads) race and corrupt each other; serialise them. */

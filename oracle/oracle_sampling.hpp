@@ -20,6 +20,7 @@ struct Sample {
     u32 words[4] = {0, 0, 0, 0};
     u32 lens_words[2] = {0, 0};
     float filter_offsets[2] = {0, 0};
+    u32 closest_walks = 0, shadow_walks = 0; // traversal queries of the lane (closest hit / occlusion)
 };
 // shaders/render.metal:200-236 (gaussian_filter_offsets)
 inline void gaussian_filter_offsets(const Scene &s, float ux, float uy, float &x, float &y) {

@@ -218,10 +218,13 @@ static bool visible(const Ctx &c, Sample &smp, const Vertex &a, const Vertex &b)
     const F3 origin = offset(a, direction);
     const F3 target = offset(b, -direction);
     const Scene &s = c.s;
-    if (!std::any_of(s.instances.begin(), s.instances.end(), [&](const Instance &in) { return pass_through(s, in); }))
+    if (!std::any_of(s.instances.begin(), s.instances.end(), [&](const Instance &in) { return pass_through(s, in); })) {
+        ++smp.shadow_walks;
         return !trace_any(s, c.bvh, origin, target - origin, 0x1.fffffep-1f);
+    }
     F3 o = origin, d = target - origin;
     for (u32 crossings = 0; crossings <= c.p.boundary_limit; ++crossings) {
+        ++smp.shadow_walks;
         const Hit h = trace_closest(s, c.bvh, o, d, 0x1.fffffep-1f);
         if (h.prim == RP_NONE)
             return true;
@@ -413,6 +416,7 @@ static void hero_step(const Ctx &c, LaneState &st) {
             smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
             break;
         }
+        ++smp.closest_walks;
         const Hit hit = trace_closest(s, c.bvh, ro, rd, INFINITY);
         if (hit.prim == RP_NONE) {
             Vertex &v = current;
@@ -632,6 +636,9 @@ static rp_packet_result render_lane(const Ctx &c, u32 lane, AdjointLane *adj = n
         r.wavelength_pdfs[k] = st.lambda.pdf[k];
         r.radiance[k] = st.radiance[k];
     }
+    // the reserved words, unread by rypath, carry the lane's traversal counts
+    r.reserved[0] = st.sample.closest_walks;
+    r.reserved[1] = st.sample.shadow_walks;
     return r;
 }
 
@@ -995,6 +1002,113 @@ void or_probe_advance(const float *q, uint32_t count, float *r) {
             o[8 + k] = float(u.density.lane[k].exponent);
         }
         o[12] = u.valid ? 1.f : 0.f;
+    }
+}
+
+// Hero BSDF probe: per query 32 floats {kind, active mask, remap, unused, 4 lanes x {eta or
+// reflectance, k, roughness u, roughness v}, wo[3], wi[3], uc, ux, uy, unused[3]} -> 32 floats
+// {sample: wi[3], numerator[4], pdf[4], eta[4], flags (delta 1, transmission 2, accepted 4,
+// valid 8); evaluation at wi: f[4], pdf[4], valid; Dirac lane 0 at wi: mass, pdf, eta, ok;
+// connectible; prepared 1 / failed 0; unused}.  kind 0 diffuse, 1 conductor, 2 dielectric.
+void or_probe_hero(const float *q, uint32_t count, float *r) {
+    for (u32 i = 0; i < count; ++i) {
+        const float *a = q + 32 * i;
+        float *o = r + 32 * i;
+        std::fill(o, o + 32, 0.0f);
+        HeroBsdf p;
+        p.active_mask = u32(a[1]);
+        const bool remap = a[2] != 0;
+        bool ok = true;
+        for (int k = 0; k < 4; ++k) {
+            const float *l = a + 4 + 4 * k;
+            LaneBsdf &lane = p.lane[k];
+            lane.kind = u32(a[0]);
+            if (lane.kind == 0)
+                lane.reflectance = l[0];
+            else if (lane.kind == 1)
+                ok = conductor_prepare(l[0], l[1], l[2], l[3], remap, lane.conductor) && ok;
+            else
+                ok = dielectric_prepare(l[0], l[2], l[3], remap, lane.dielectric) && ok;
+        }
+        o[30] = ok ? 1.f : 0.f;
+        if (!ok)
+            continue;
+        const F3 wo{a[20], a[21], a[22]}, wi{a[23], a[24], a[25]};
+        const HeroSample smp = hero_sample(p, wo, a[26], a[27], a[28]);
+        o[0] = smp.wi.x;
+        o[1] = smp.wi.y;
+        o[2] = smp.wi.z;
+        for (int k = 0; k < 4; ++k) {
+            o[3 + k] = smp.numerator[k];
+            o[7 + k] = smp.pdf[k];
+            o[11 + k] = smp.eta[k];
+        }
+        o[15] = float((smp.delta ? 1 : 0) | (smp.transmission ? 2 : 0) | (smp.accepted ? 4 : 0) | (smp.valid ? 8 : 0));
+        const HeroEval e = hero_evaluate(p, wo, wi);
+        for (int k = 0; k < 4; ++k) {
+            o[16 + k] = e.f[k];
+            o[20 + k] = e.pdf[k];
+        }
+        o[24] = e.valid ? 1.f : 0.f;
+        float mass, density, eta;
+        const bool dirac = dirac_lane(p.lane[0], wo, wi, a[27], a[28], mass, density, eta);
+        o[25] = mass;
+        o[26] = density;
+        o[27] = eta;
+        o[28] = dirac ? 1.f : 0.f;
+        o[29] = hero_connectible(p) ? 1.f : 0.f;
+    }
+}
+
+// Roulette probe: per query 16 floats {beta[4], eta scale[4], roulette enabled, depth, u,
+// transmission, eta[4]} -> 12 floats {continues, beta after[4], eta scale after accounting
+// eta[4], roulette enabled after, unused[2]}: hero_continue, then hero_account_eta on the
+// query's track (shaders/hero_pt_helpers.h:56-98).
+void or_probe_roulette(const float *q, uint32_t count, float *r) {
+    for (u32 i = 0; i < count; ++i) {
+        const float *a = q + 16 * i;
+        float *o = r + 12 * i;
+        std::fill(o, o + 12, 0.0f);
+        HeroTrack track;
+        F4 beta, eta;
+        for (int k = 0; k < 4; ++k) {
+            beta[k] = a[k];
+            track.eta_scale[k] = a[4 + k];
+            eta[k] = a[12 + k];
+        }
+        track.roulette_enabled = a[8] != 0;
+        const bool alive = hero_continue(beta, track, u32(a[9]), a[10]);
+        hero_account_eta(track, eta, a[11] != 0);
+        o[0] = alive ? 1.f : 0.f;
+        for (int k = 0; k < 4; ++k) {
+            o[1 + k] = beta[k];
+            o[5 + k] = track.eta_scale[k];
+        }
+        o[9] = track.roulette_enabled ? 1.f : 0.f;
+    }
+}
+
+// MIS weight probe: per query 20 floats {prefix fractions[4], prefix exponents[4], value[4],
+// sampled[4], other[4]} -> 5 floats {weighted contribution[4], failed}
+// (hero_weight, shaders/hero_pt_helpers.h:122-138).
+void or_probe_hero_weight(const float *q, uint32_t count, float *r) {
+    for (u32 i = 0; i < count; ++i) {
+        const float *a = q + 20 * i;
+        float *o = r + 5 * i;
+        Density prefix;
+        F4 value, sampled, other;
+        for (int k = 0; k < 4; ++k) {
+            prefix.lane[k].fraction = a[k];
+            prefix.lane[k].exponent = int(a[4 + k]);
+            value[k] = a[8 + k];
+            sampled[k] = a[12 + k];
+            other[k] = a[16 + k];
+        }
+        Sample smp;
+        const F4 w = hero_weight(smp, prefix, value, sampled, other);
+        for (int k = 0; k < 4; ++k)
+            o[k] = w[k];
+        o[4] = smp.status != RP_SAMPLE_SUCCESS ? 1.f : 0.f;
     }
 }
 

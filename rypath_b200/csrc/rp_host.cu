@@ -500,6 +500,57 @@ int grid_for(int sm_count, u32 work, int block, int per_sm) {
     return int(std::max<u32>(1, std::min<u32>(needed, u32(sm_count * per_sm))));
 }
 
+// The structure-of-arrays carve of a path pool of `lanes` slots over `base` (nullptr: only
+// the size is computed): the 16-byte arrays, the queues and family bins, the counters, and,
+// when `full`, the arrays only some runs read (shadow targets and resolved materials of
+// scenes with pass-through or mix surfaces, per-lane walk counts of counting runs).  Every
+// slice starts on a 256-byte boundary.  The scene pool and the allocation-free scratch both
+// carve through here, so a new PathPool array is added in one place; a pool without `full`
+// leaves those pointers null, and only scenes without pass-through or mix surfaces, without
+// counting and without the adjoint may run on it.
+constexpr size_t pool_bytes(u32 lanes, bool full) {
+    const size_t v16 = (size_t(lanes) * 16 + 255) & ~size_t(255), v4 = (size_t(lanes) * 4 + 255) & ~size_t(255);
+    return 22 * v16 + 6 * v4 + 256 + (full ? v16 + 3 * v4 : 0);
+}
+size_t carve_pool(unsigned char *base, u32 lanes, bool full, PathPool *out) {
+    const size_t v16 = (size_t(lanes) * 16 + 255) & ~size_t(255), v4 = (size_t(lanes) * 4 + 255) & ~size_t(255);
+    size_t off = 0;
+    auto take = [&](size_t n) {
+        unsigned char *p = base ? base + off : nullptr;
+        off += n;
+        return p;
+    };
+    PathPool q{};
+    q.ident = reinterpret_cast<uint4 *>(take(v16));
+    q.cursor = reinterpret_cast<uint4 *>(take(v16));
+    float4 **f4[] = {&q.lambda, &q.lambda_pdf, &q.beta, &q.radiance, &q.dens_f, &q.prev_f, &q.eta_scale, &q.ray_o,
+                     &q.ray_d, &q.latest_p, &q.latest_n, &q.latest_param, &q.latest_k, &q.preceding, &q.hit,
+                     &q.sh_o, &q.sh_d, &q.sh_c};
+    for (auto p : f4)
+        *p = reinterpret_cast<float4 *>(take(v16));
+    q.dens_e = reinterpret_cast<int4 *>(take(v16));
+    q.prev_e = reinterpret_cast<int4 *>(take(v16));
+    q.queue[0] = reinterpret_cast<u32 *>(take(v4));
+    q.queue[1] = reinterpret_cast<u32 *>(take(v4));
+    q.bins = reinterpret_cast<u32 *>(take(4 * v4));
+    q.counters = reinterpret_cast<u32 *>(take(256));
+    if (full) {
+        q.sh_t = reinterpret_cast<float4 *>(take(v16));
+        q.material = reinterpret_cast<u32 *>(take(v4));
+        q.lane_closest = reinterpret_cast<u32 *>(take(v4));
+        q.lane_shadow = reinterpret_cast<u32 *>(take(v4));
+    }
+    q.bin_capacity = lanes;
+    if (off != pool_bytes(lanes, full))
+        throw std::logic_error("carve_pool and pool_bytes disagree");
+    if (out)
+        *out = q;
+    return off;
+}
+// Every PathPool member is a pointer carved above, set elsewhere (stats, the adjoint's), or
+// a count: a new member changes this size and so comes past this check.
+static_assert(sizeof(PathPool) == 38 * sizeof(void *) + 16, "PathPool changed: review carve_pool");
+
 } // namespace
 
 // ---------------------------------------------------------------- scene
@@ -534,6 +585,8 @@ struct rp_scene {
     // wavefront pool
     PathPool pool{};
     u32 capacity = 0;
+    u32 *lane_closest = nullptr, *lane_shadow = nullptr; // per-lane walk counts (pool.lane_* while counting)
+    unsigned char *static_base = nullptr; // device address of the allocation-free scratch, once looked up
     unsigned long long *stats = nullptr;
     double *cie = nullptr;
     rp_film_pixel *film_stage = nullptr;
@@ -663,35 +716,25 @@ struct rp_scene {
             cudaFreeAsync(p, stream);
         pool_owned.clear();
         capacity = 0;
-        // one allocation carved into the SoA arrays (256-byte aligned slices)
-        const size_t c = lanes;
-        const size_t v16 = (c * 16 + 255) & ~size_t(255), v4 = (c * 4 + 255) & ~size_t(255);
-        const size_t bytes = 23 * v16 + 7 * v4 + 256;
+        // one allocation carved into the SoA arrays
+        const size_t bytes = carve_pool(nullptr, lanes, true, nullptr);
         unsigned char *base = dalloc<unsigned char>(pool_owned, bytes, stream);
-        size_t off = 0;
-        auto take = [&](size_t n) {
-            unsigned char *p = base + off;
-            off += n;
-            return p;
-        };
-        PathPool &q = pool;
-        q.ident = reinterpret_cast<uint4 *>(take(v16));
-        q.cursor = reinterpret_cast<uint4 *>(take(v16));
-        float4 **f4[] = {&q.lambda, &q.lambda_pdf, &q.beta, &q.radiance, &q.dens_f, &q.prev_f, &q.eta_scale, &q.ray_o,
-                         &q.ray_d, &q.latest_p, &q.latest_n, &q.latest_param, &q.latest_k, &q.preceding, &q.hit,
-                         &q.sh_o, &q.sh_d, &q.sh_c};
-        for (auto p : f4)
-            *p = reinterpret_cast<float4 *>(take(v16));
-        q.dens_e = reinterpret_cast<int4 *>(take(v16));
-        q.prev_e = reinterpret_cast<int4 *>(take(v16));
-        q.queue[0] = reinterpret_cast<u32 *>(take(v4));
-        q.queue[1] = reinterpret_cast<u32 *>(take(v4));
-        q.bins = reinterpret_cast<u32 *>(take(4 * v4));
-        q.counters = reinterpret_cast<u32 *>(take(256));
-        q.sh_t = reinterpret_cast<float4 *>(take(v16));
-        q.material = reinterpret_cast<u32 *>(take(v4));
-        q.bin_capacity = lanes;
+        PathPool q;
+        carve_pool(base, lanes, true, &q);
+        lane_closest = q.lane_closest;
+        lane_shadow = q.lane_shadow;
+        q.lane_closest = q.lane_shadow = nullptr; // set by counting waves
         q.stats = stats;
+        // the adjoint's members are set per run
+        q.hist = pool.hist;
+        q.adj_w = pool.adj_w;
+        q.adj_slot = pool.adj_slot;
+        q.adj_grad = pool.adj_grad;
+        q.adj_g = pool.adj_g;
+        q.adj_cie = pool.adj_cie;
+        q.adj_inv_weight = pool.adj_inv_weight;
+        q.adj_params = pool.adj_params;
+        pool = q;
         capacity = lanes;
     }
 };
@@ -887,6 +930,8 @@ void run_wave(rp_scene *s, const WaveParams &request_params, size_t adjoint_smem
     attach_owen_prefix(s, p);
     s->ensure_pool(p.lanes);
     PathPool &pool = s->pool;
+    pool.lane_closest = s->counting ? s->lane_closest : nullptr;
+    pool.lane_shadow = s->counting ? s->lane_shadow : nullptr;
     const int sms = s->sm_count;
     s->mark(3);
     RP_CHECK(cudaMemsetAsync(pool.counters, 0, 16 * sizeof(u32), s->stream));
@@ -2766,55 +2811,24 @@ static __device__ __align__(256) unsigned char g_static_scratch[RP_STATIC_SCRATC
 
 namespace {
 
-constexpr size_t kStaticArrays16 = 22, kStaticArrays4 = 6; // same SoA carve as the pool
-
-constexpr size_t static_bytes_for(u32 lanes) {
-    return kStaticArrays16 * ((size_t(lanes) * 16 + 255) & ~size_t(255)) +
-           kStaticArrays4 * ((size_t(lanes) * 4 + 255) & ~size_t(255)) + 256;
-}
-static_assert(static_bytes_for(RP_STATIC_MAX_LANES) <= RP_STATIC_SCRATCH_BYTES &&
-                  static_bytes_for(RP_STATIC_MAX_LANES + 1) > RP_STATIC_SCRATCH_BYTES,
+static_assert(pool_bytes(RP_STATIC_MAX_LANES, false) <= RP_STATIC_SCRATCH_BYTES &&
+                  pool_bytes(RP_STATIC_MAX_LANES + 1, false) > RP_STATIC_SCRATCH_BYTES,
               "RP_STATIC_MAX_LANES is the largest request that fits the static scratch");
 
-// Device address of the scratch array, looked up once per device with that device current.
-unsigned char *static_scratch(int device, cudaError_t &err) {
-    static unsigned char *address[64] = {};
-    err = cudaSuccess;
-    if (device < 0 || device >= 64)
-        return nullptr;
-    if (!address[device]) {
-        void *ptr = nullptr;
-        err = cudaGetSymbolAddress(&ptr, g_static_scratch);
-        if (err != cudaSuccess)
-            return nullptr;
-        address[device] = static_cast<unsigned char *>(ptr);
-    }
-    return address[device];
+// Device address of the scratch array in the current device's context.  The caller keeps it
+// with the scene, whose own device memory lives in the same context: a scene cannot outlive
+// a reset of its device, so neither can the cached address.
+unsigned char *static_scratch(cudaError_t &err) {
+    void *ptr = nullptr;
+    err = cudaGetSymbolAddress(&ptr, g_static_scratch);
+    return err == cudaSuccess ? static_cast<unsigned char *>(ptr) : nullptr;
 }
 
+// The pool of the allocation-free entry point: the scene pool's carve without the optional
+// arrays (the entry point refuses scenes with pass-through or mix surfaces and never counts).
 PathPool static_pool(unsigned char *base, u32 lanes, unsigned long long *stats) {
-    const size_t v16 = (size_t(lanes) * 16 + 255) & ~size_t(255), v4 = (size_t(lanes) * 4 + 255) & ~size_t(255);
-    size_t off = 0;
-    auto take = [&](size_t n) {
-        unsigned char *p = base + off;
-        off += n;
-        return p;
-    };
-    PathPool q{};
-    q.ident = reinterpret_cast<uint4 *>(take(v16));
-    q.cursor = reinterpret_cast<uint4 *>(take(v16));
-    float4 **f4[] = {&q.lambda, &q.lambda_pdf, &q.beta, &q.radiance, &q.dens_f, &q.prev_f, &q.eta_scale, &q.ray_o,
-                     &q.ray_d, &q.latest_p, &q.latest_n, &q.latest_param, &q.latest_k, &q.preceding, &q.hit,
-                     &q.sh_o, &q.sh_d, &q.sh_c};
-    for (auto p : f4)
-        *p = reinterpret_cast<float4 *>(take(v16));
-    q.dens_e = reinterpret_cast<int4 *>(take(v16));
-    q.prev_e = reinterpret_cast<int4 *>(take(v16));
-    q.queue[0] = reinterpret_cast<u32 *>(take(v4));
-    q.queue[1] = reinterpret_cast<u32 *>(take(v4));
-    q.bins = reinterpret_cast<u32 *>(take(4 * v4));
-    q.counters = reinterpret_cast<u32 *>(take(256));
-    q.bin_capacity = lanes;
+    PathPool q;
+    carve_pool(base, lanes, false, &q);
     q.stats = stats;
     return q;
 }
@@ -2849,12 +2863,16 @@ rp_status rp_cuda_sample_device_static(rp_scene *s, const rp_request *request, r
             return RP_INVALID_ARGUMENT;
         }
         RP_CHECK(cudaSetDevice(s->device));
-        cudaError_t e;
-        unsigned char *base = static_scratch(s->device, e);
-        if (!base) {
-            set_diag(diag, cap, "cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
-            return RP_FAILURE;
+        if (!s->static_base) {
+            // the scene's first call: look the array up once, with the scene's device current
+            cudaError_t e;
+            s->static_base = static_scratch(e);
+            if (!s->static_base) {
+                set_diag(diag, cap, "cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
+                return RP_FAILURE;
+            }
         }
+        unsigned char *base = s->static_base;
         cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : s->stream;
         PathPool pool = static_pool(base, p.lanes, s->stats);
         const int sms = s->sm_count;

@@ -46,6 +46,10 @@ RP_DEV void raygen_lane(const DeviceScene &s, const RasterCam &cam, const WavePa
         pool.latest_p[slot] = make_float4(o.x, o.y, o.z, 0);
         pool.latest_n[slot] = make_float4(0, 0, 0, 0);
         pool.queue[0][slot] = slot;
+        if (pool.lane_closest) {
+            pool.lane_closest[slot] = 0;
+            pool.lane_shadow[slot] = 0;
+        }
         if (pool.hist) {
             pool.hist[slot] = empty_history();
             pool.adj_w[slot] = adjoint_lane_weight(pool, b.pixel, lambda, pdf);
@@ -154,6 +158,7 @@ __global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1
             path = queue[i];
             if (!(pool.ident[path].w & F_COMPLETE)) {
                 const float4 o = pool.ray_o[path], d = pool.ray_d[path];
+                const u32 walks_before = rays;
                 Hit h;
                 const bool ok = walk_closest<Count, Stack>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z),
                                                            __int_as_float(0x7f800000), h, stack + threadIdx.x, Block,
@@ -165,6 +170,8 @@ __global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1
                     family = resolve_hit<Count, Stack>(s, pool, path, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), h, prim,
                                                        stack + threadIdx.x, Block, boundary_limit, nodes, tris, rays);
                 pool.hit[path] = make_float4(h.t, h.b1, h.b2, __uint_as_float(prim));
+                if (Count && pool.lane_closest)
+                    pool.lane_closest[path] += rays - walks_before;
             }
         }
         const u32 peers = __match_any_sync(0xffffffffu, family);
@@ -681,6 +688,7 @@ __global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
         const float4 o = pool.sh_o[i], d = pool.sh_d[i];
         const u32 path = __float_as_uint(d.w);
+        const u32 walks_before = rays;
         bool occluded;
         u32 failure = 0;
         if (Resolve) {
@@ -693,6 +701,8 @@ __global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1
                 failure = 3;
             ++rays;
         }
+        if (Count && pool.lane_shadow)
+            pool.lane_shadow[path] += rays - walks_before;
         uint4 ident = pool.ident[path];
         if (failure) {
             ident.w = set_status(ident.w, failure) | F_COMPLETE;
@@ -731,7 +741,9 @@ __global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1
     }
 }
 
-// packet_pt_result (shaders/packet_pt_step.h:225-239): 80-byte packet result per lane.
+// packet_pt_result (shaders/packet_pt_step.h:225-239): 80-byte packet result per lane.  The
+// reserved words, which rypath leaves unread, carry the lane's closest-hit and any-hit walk
+// counts in counting runs (zero otherwise).
 struct PacketResult {
     u32 status, pixel, sample_low, sample_high, splat_count;
     float wavelengths[4], wavelength_pdfs[4], radiance[4];
@@ -761,7 +773,8 @@ __global__ void k_results(PathPool pool, u32 lanes, float filter_weight, PacketR
         res.radiance[2] = r.z;
         res.radiance[3] = r.w;
         res.filter_weight = filter_weight;
-        res.reserved[0] = res.reserved[1] = 0;
+        res.reserved[0] = pool.lane_closest ? pool.lane_closest[lane] : 0u;
+        res.reserved[1] = pool.lane_shadow ? pool.lane_shadow[lane] : 0u;
         out[lane] = res;
     }
 }

@@ -53,6 +53,10 @@ struct PathPool {
     u32 *material; // material a mix-root hit resolved to (written by the closest-hit kernel)
     // statistics (optional)
     unsigned long long *stats; // closest [0] nodes, [1] triangles, [2] rays; shadow [3] rays, [4] nodes, [5] triangles
+    // per-lane walk counts of counting runs (pool slot = request lane), or nullptr: closest-hit
+    // walks (written by the closest-hit kernel) and any-hit walks (by the shadow kernel, which
+    // runs beside the next closest-hit walk, hence two arrays)
+    u32 *lane_closest, *lane_shadow;
     // path-replay adjoint (hist == nullptr: off)
     uint4 *hist;            // parameter materials of the diffuse vertices so far, a byte each, 0xff = none
     float4 *adj_w;          // d loss / d radiance of each wavelength lane

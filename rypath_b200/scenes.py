@@ -338,6 +338,80 @@ def cornell_pass_through(width=256, height=256, spp=64, max_depth=8, pane=True, 
     return scene
 
 
+CORNELL_FEATURES = ("point", "spot", "environment", "cauchy")
+
+
+def cauchy_dielectric(scene, a=1.5, b_um2=0.004):
+    """A smooth dielectric whose eta follows Cauchy's n = a + b / lambda^2 (lambda in um), as
+    32 sampled knots (rypath has no Cauchy model; a sampled eta spectrum stands in)."""
+    w = np.linspace(360, 830, 32)
+    m = abi.Material()
+    m.scattering, m.kind, m.scalar_value = abi.DIELECTRIC, abi.REFLECTANCE_CONSTANT, 1.0
+    m.eta_begin, m.eta_count, m.optical_extensions = _append_knots(scene, a + b_um2 / (w / 1000.0) ** 2), 32, 1
+    m.k_begin = m.k_count = 0
+    m.u_roughness = m.v_roughness = 0.0
+    m.remap_roughness = 1
+    return m
+
+
+def cornell_features(feature, width=32, height=32, spp=4, max_depth=8) -> Scene:
+    """The Cornell-style box with one light or material feature of the mixed-material scene, so
+    that each can be checked on its own:
+
+    point: the area light replaced by a blackbody point light below the ceiling;
+    spot: the area light replaced by a spot light pointing down at the short box;
+    environment: the area light replaced by a constant environment seen through the open front;
+    cauchy: the tall box made of a smooth dispersive (Cauchy) dielectric, the short box of a
+    rough conductor, under the area light.
+    """
+    if feature not in CORNELL_FEATURES:
+        raise ValueError(f"unknown feature {feature!r}")
+    scene = cornell_box(width, height, spp, max_depth)
+    scene.name = f"cornell_{feature}"
+    if feature in ("point", "spot", "environment"):
+        scene.instances[-1].emission = abi.RP_NONE  # the quad stays, as a black diffuse panel
+        scene.emissions = []
+    if feature == "point":
+        scene.positional = [{"kind": abi.POINT_LIGHT, "position": (0.2, 1.7, 0.3),
+                             "intensity": blackbody_emission(3200, 3.0)}]
+    elif feature == "spot":
+        scene.positional = [_spot((-0.1, 1.9, 0.4), (0.4, 0.6, 0.2), 20.0, 30.0, blackbody_emission(5000, 8.0))]
+    elif feature == "environment":
+        scene.environment = (1.5 * blackbody_shape(9000) / blackbody_shape(9000).max()).astype(np.float32)
+    else:
+        conductor = abi.Material()
+        conductor.scattering, conductor.kind, conductor.scalar_value = abi.CONDUCTOR, abi.REFLECTANCE_CONSTANT, 1.0
+        conductor.eta_begin, conductor.eta_count = _append_knots(scene, 0.4), 32
+        conductor.k_begin, conductor.k_count = _append_knots(scene, 3.0), 32
+        conductor.optical_extensions, conductor.u_roughness, conductor.v_roughness = 3, 0.2, 0.2
+        conductor.remap_roughness = 1
+        base = len(scene.materials)
+        scene.materials += [conductor, cauchy_dielectric(scene)]
+        scene.instances[5].material = base
+        scene.instances[6].material = base + 1
+    return scene
+
+
+def crop(scene: Scene, x0: int, y0: int, width: int, height: int) -> Scene:
+    """The window [x0, x0 + width) x [y0, y0 + height) of a scene's film as a scene of its own:
+    the same geometry, lights and materials, its raster camera narrowed to the window."""
+    if not (0 <= x0 and 0 <= y0 and width > 0 and height > 0 and x0 + width <= scene.width
+            and y0 + height <= scene.height):
+        raise ValueError("crop window outside the film")
+    import copy
+
+    out = copy.copy(scene)
+    o, corner, dx, dy = (np.asarray(v, np.float64) for v in scene.camera)
+    corner = corner + (x0 / scene.width) * dx + (y0 / scene.height) * dy
+    dx = dx * (width / scene.width)
+    dy = dy * (height / scene.height)
+    out.camera = tuple(tuple(v.astype(np.float32)) for v in (o, corner, dx, dy))
+    out.width, out.height = width, height
+    out.name = f"{scene.name}_crop"
+    out._keep = []
+    return out
+
+
 def cornell_fog(width=1024, height=1024, spp=64, max_depth=32, sigma_s_mean=0.5, albedo=0.9, g=0.7) -> Scene:
     """The Cornell-style box filled with a homogeneous medium, rendered by the scalar transport.
 

@@ -14,6 +14,7 @@ from rypath_b200 import abi
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
 REF = os.path.join(ROOT, "oracle", "_ref", "libref.so")
+ROULETTE_KNOWN_ANSWERS = os.path.join(ROOT, "oracle", "_ref", "roulette_known_answers")
 _oracle = None
 _ref = None
 
@@ -48,6 +49,9 @@ def oracle():
         lib.or_adjoint.argtypes = [vp, C.POINTER(abi.FilmRequest), vp, u32, vp, vp, vp, C.c_int]
         lib.or_probe_qmc.argtypes = [vp, vp, u32, vp]
         lib.or_gaussian_filter.argtypes = [C.c_float, C.c_float, C.c_float, vp, sz, vp, vp, vp, u32, vp]
+        lib.or_probe_hero.argtypes = [vp, u32, vp]
+        lib.or_probe_roulette.argtypes = [vp, u32, vp]
+        lib.or_probe_hero_weight.argtypes = [vp, u32, vp]
         _oracle = lib
     return _oracle
 
@@ -75,6 +79,9 @@ def reference():
         lib.ref_film_add_clamped.argtypes = [vp, sz, u32, u32, C.c_double, C.c_double, vp]
         lib.ref_probe_medium.argtypes = [vp, u32, vp]
         lib.ref_probe_qmc.argtypes = [vp, u32, vp]
+        lib.ref_probe_hero.argtypes = [vp, u32, vp]
+        lib.ref_probe_roulette.argtypes = [vp, u32, vp]
+        lib.ref_probe_hero_weight.argtypes = [vp, u32, vp]
         _ref = lib
     return _ref
 
@@ -163,3 +170,40 @@ def oracle_adjoint(scene, width, height, spp, materials, d_loss_d_xyz, seed=1, s
                              grad.ctypes.data, threads)
     assert rc == 0, rc
     return grad
+
+
+def oracle_film(scene, width, height, spp, seed=1, sampler=abi.SAMPLER_SOBOL, scalar=False, chunk=256, threads=0):
+    """The oracle's FP64 film (rp_film_pixel rows) of samples [0, spp) of every pixel, rendered
+    and reduced in chunks of `chunk` samples (canonical order: absolute sample, then pixel)."""
+    import numpy as np
+
+    from rypath_b200 import scenes
+
+    o = OracleScene(scene)
+    film = np.zeros(width * height, abi.film_dtype())
+    cie = np.ascontiguousarray(scenes.cie_xyz())
+    for begin in range(0, spp, chunk):
+        count = min(chunk, spp - begin)
+        r = request(width, height, count, sample_begin=begin, seed=seed, sampler=sampler)
+        r.total_samples = spp
+        if scalar:
+            lanes = o.sample_scalar(r, threads)
+            rc = oracle().or_scalar_film_add(lanes.ctypes.data, lanes.size, cie.ctypes.data, width * height,
+                                             film.ctypes.data)
+        else:
+            lanes = o.sample(r, threads)
+            rc = oracle().or_film_add(lanes.ctypes.data, lanes.size, cie.ctypes.data, width * height,
+                                      film.ctypes.data)
+        if rc != 0:
+            raise RuntimeError("oracle film reduction rejected a lane")
+    return film
+
+
+def film_mean_variance(film):
+    """Per-pixel mean XYZ and the variance of that mean (second moments over the count)."""
+    import numpy as np
+
+    n = film["count"].astype(np.float64)[:, None]
+    m = (film["sum"] + film["correction"]) / n
+    var = np.maximum(film["square"] / n - m * m, 0) / n
+    return m, var

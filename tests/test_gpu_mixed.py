@@ -1,0 +1,149 @@
+"""GPU parity on the mixed-material benchmark scene and on one-feature Cornell variants.
+
+The mixed scene (1920x1080, depth 16: displaced icosphere, 64 spheres, ground; diffuse, rough
+conductor and dispersive Cauchy dielectric materials; two point lights, two spot lights and a
+constant environment) is rendered through the C ABI in windows spread over its film and
+compared with the oracle lane by lane:
+
+* identity (pixel, sample) and status bit-exact for every lane;
+* wavelengths within 4 ulp (CUDA's atanhf / coshf against the host libm);
+* radiance within RTOL for at least MATCH_FRACTION of lanes (a lane that takes another
+  discrete branch after a last-bit difference in a transcendental is another sample);
+* the lane's closest-hit and any-hit walk counts (reported by counting runs in the packet
+  result's reserved words, by the device and by the oracle) equal on every lane whose
+  radiance matches, and their totals within 1%.
+
+Each of the scene's light and material features also runs on its own in a Cornell variant
+(point light, spot light, constant environment, dispersive dielectric), so that a mistake in
+one fails its own test.  The statistical gates (3 combined standard errors per pixel; relative
+RMSE against a 4096-spp FP64 oracle render) run on crops of the mixed scene and of the fog box.
+"""
+
+import numpy as np
+import pytest
+
+from rypath_b200 import abi, renderer, scenes
+from tests.oracle_lib import OracleScene, film_mean_variance, oracle_film, request
+from tests.test_gpu_parity import MATCH_FRACTION, RTOL, ulp_diff
+
+pytestmark = pytest.mark.gpu
+
+WINDOWS = 8          # windows of the 1080p film
+WINDOW_PIXELS = 4096
+SPP = 2
+SAMPLERS = {"sobol_owen": abi.SAMPLER_SOBOL, "independent": abi.SAMPLER_INDEPENDENT}
+
+
+@pytest.fixture(scope="module")
+def mixed():
+    scene = scenes.mixed_scene()
+    built = renderer.build_renderer(scene)
+    assert built.status == abi.RP_SUCCESS, built.diagnostic
+    built.scene.set_counting(True)
+    yield scene, built.scene, OracleScene(scene)
+    built.scene.close()
+
+
+def compare_lanes(g, c, min_shadow_fraction=0.0):
+    """The lane gates above; returns the matching-lane mask."""
+    np.testing.assert_array_equal(g["status"], c["status"])
+    np.testing.assert_array_equal(g["status"], 0)
+    for f in ("pixel", "sample_low", "sample_high"):
+        np.testing.assert_array_equal(g[f], c[f])
+    assert ulp_diff(g["wavelengths"], c["wavelengths"]).max() <= 4
+    np.testing.assert_allclose(g["wavelength_pdfs"], c["wavelength_pdfs"], rtol=4e-6, atol=0)
+    gr, cr = g["radiance"].astype(np.float64), c["radiance"].astype(np.float64)
+    close = np.all(np.abs(gr - cr) <= RTOL * np.maximum(np.abs(cr), 1e-6) + 1e-7, axis=1)
+    assert close.mean() >= MATCH_FRACTION, close.mean()
+    gw, cw = g["reserved"].astype(np.int64), c["reserved"].astype(np.int64)
+    same_walks = np.all(gw == cw, axis=1)
+    # a lane with the same radiance took the same branches: the same walks
+    assert same_walks[close].mean() >= 0.999, same_walks[close].mean()
+    for k in range(2):
+        assert abs(gw[:, k].sum() - cw[:, k].sum()) <= 0.01 * max(cw[:, k].sum(), 1), (k, gw[:, k].sum(), cw[:, k].sum())
+    assert (cw[:, 1] > 0).mean() >= min_shadow_fraction, (cw[:, 1] > 0).mean()
+    return close
+
+
+@pytest.mark.parametrize("sampler", list(SAMPLERS))
+def test_mixed_scene_lanes_match_oracle(mixed, sampler):
+    scene, gpu, orc = mixed
+    total = scene.width * scene.height
+    gpu_lanes, cpu_lanes = [], []
+    for begin in np.linspace(0, total - WINDOW_PIXELS, WINDOWS).astype(int):
+        req = renderer.RenderRequest(scene.width, scene.height, pixel_begin=int(begin), pixel_count=WINDOW_PIXELS,
+                                     sample_count=SPP, sampler=SAMPLERS[sampler])
+        res = gpu.sample(req)
+        assert res.status == abi.RP_SUCCESS, res.diagnostic
+        t = gpu.timing()
+        g = res.packet_samples
+        # the per-lane walk counts add up to the call's ray counters
+        assert g["reserved"][:, 0].sum() == t.closest_rays and g["reserved"][:, 1].sum() == t.shadow_rays
+        gpu_lanes.append(g)
+        cpu_lanes.append(orc.sample(request(scene.width, scene.height, SPP, pixel_begin=int(begin),
+                                            pixel_count=WINDOW_PIXELS, sampler=SAMPLERS[sampler])))
+    g, c = np.concatenate(gpu_lanes), np.concatenate(cpu_lanes)
+    compare_lanes(g, c, min_shadow_fraction=0.2)
+    # the scene's features are exercised: environment escapes (one walk, light), long paths
+    # through glass and metal, and many light samples
+    assert ((c["reserved"][:, 0] == 1) & (c["radiance"].sum(1) > 0)).mean() > 0.05
+    assert (c["reserved"][:, 0] >= 5).mean() > 0.02
+
+
+@pytest.mark.parametrize("sampler", list(SAMPLERS))
+@pytest.mark.parametrize("feature", scenes.CORNELL_FEATURES)
+def test_cornell_feature_lanes_match_oracle(feature, sampler):
+    scene = scenes.cornell_features(feature, 32, 32, 4)
+    built = renderer.build_renderer(scene)
+    assert built.status == abi.RP_SUCCESS, built.diagnostic
+    built.scene.set_counting(True)
+    res = built.scene.sample(renderer.RenderRequest(32, 32, sample_count=4, sampler=SAMPLERS[sampler]))
+    built.scene.close()
+    assert res.status == abi.RP_SUCCESS, res.diagnostic
+    c = OracleScene(scene).sample(request(32, 32, 4, sampler=SAMPLERS[sampler]))
+    compare_lanes(res.packet_samples, c, min_shadow_fraction=0.0 if feature == "environment" else 0.2)
+    assert (c["radiance"].sum(1) > 0).mean() > 0.1
+
+
+def statistics_gates(scene, spp, bound, scalar=False):
+    """Device film (spp, Sobol / Owen, seed 1) against oracle renders: within 3 combined standard
+    errors per pixel of an independent oracle render (independent sampler, seed 7), and
+    relative RMSE against a 4096-spp FP64 oracle render below `bound` and within 30% of an
+    oracle render with the device's sampler on another seed."""
+    w, h = scene.width, scene.height
+    built = renderer.build_renderer(scene)
+    assert built.status == abi.RP_SUCCESS, built.diagnostic
+    st, diag, film = built.scene.render_film(renderer.RenderSettings(w, h, samples=spp, batch_size=spp, seed=1))
+    built.scene.close()
+    assert st == abi.RP_SUCCESS, diag
+    independent = oracle_film(scene, w, h, spp, seed=7, sampler=abi.SAMPLER_INDEPENDENT, scalar=scalar)
+    gm, gv = film_mean_variance(film)
+    cm, cv = film_mean_variance(independent)
+    z = np.abs(gm - cm) / np.sqrt(gv + cv + 1e-12)
+    assert (z > 3).mean() < 0.02, (z > 3).mean()
+    assert abs(gm[:, 1].mean() - cm[:, 1].mean()) < 3 * np.sqrt(gv[:, 1].sum() + cv[:, 1].sum()) / (w * h)
+    reference = renderer.film_mean(oracle_film(scene, w, h, 4096, seed=101, sampler=abi.SAMPLER_INDEPENDENT,
+                                               scalar=scalar))
+
+    def relative_rmse(x):
+        return np.sqrt(np.mean((x - reference) ** 2)) / np.sqrt(np.mean(reference ** 2))
+
+    device = relative_rmse(renderer.film_mean(film))
+    other_seed = relative_rmse(renderer.film_mean(oracle_film(scene, w, h, spp, seed=2, scalar=scalar)))
+    assert device < bound, device
+    assert device < 1.3 * other_seed, (device, other_seed)
+    return device, other_seed
+
+
+def test_mixed_crop_statistics():
+    """64x36 window at the film centre of the 1080p mixed scene, 64 spp (relative RMSE bound 0.10;
+    the oracle alone gives 0.07 with Sobol / Owen and 0.13 with the independent sampler)."""
+    statistics_gates(scenes.crop(scenes.mixed_scene(), 928, 522, 64, 36), 64, 0.10)
+
+
+def test_fog_crop_statistics():
+    """64x64 window at the centre of the 1024x1024 fog box (scalar volpath, depth 32), 64 spp.  The
+    scalar transport carries one wavelength per sample, so a pixel's XYZ at 64 spp is noisy: the
+    oracle alone gives a relative RMSE of 0.67 (Sobol / Owen) and 0.68 (independent), hence the
+    bound of 0.75."""
+    statistics_gates(scenes.crop(scenes.cornell_fog(), 480, 480, 64, 64), 64, 0.75, scalar=True)

@@ -4,7 +4,9 @@ host-compilable sources compiled where they lie (oracle/_ref, built by oracle/re
 References: Sobol KATs tests/sampling_tests.cpp:26-142; Philox KATs tests/replay_tests.cpp:22-36;
 visible wavelength checks tests/packet_spectrum_tests.cpp:9-56; light tables
 src/light_sampling.cpp:384-572; packet film src/packet_film.cpp:198-265; Gaussian filter
-digests tests/gaussian_filter_tests.cpp:89-127.
+digests tests/gaussian_filter_tests.cpp:89-127; roulette known answers
+tests/packet_roulette_tests.cpp:18-139; hero BSDF proposals shaders/hero_scattering.h:67-231;
+hero roulette and MIS weight shaders/hero_pt_helpers.h:56-138.
 """
 
 import ctypes as C
@@ -16,7 +18,7 @@ import numpy as np
 import pytest
 
 from rypath_b200 import abi, scenes
-from tests.oracle_lib import oracle, reference
+from tests.oracle_lib import ROULETTE_KNOWN_ANSWERS, oracle, reference
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 TABLES = scenes.sobol_tables()
@@ -357,3 +359,120 @@ def test_qmc_matches_reference_header():
     oracle().or_probe_qmc(C.cast(TABLE_BUF, C.c_void_p), q.ctypes.data, q.shape[0], a.ctypes.data)
     ref.ref_probe_qmc(q.ctypes.data, q.shape[0], b.ctypes.data)
     np.testing.assert_array_equal(a, b)
+
+
+def test_roulette_known_answers_of_rypath_against_the_oracle():
+    """rypath's own roulette test program (tests/packet_roulette_tests.cpp: dyadic Bernoulli
+    means, eta accounting and its unsafe-value fallbacks, tiny-probability fallbacks, lane
+    permutation symmetry), compiled by oracle/ref.mk with the roulette header replaced by the
+    oracle's restatement, passes."""
+    import subprocess
+
+    if not os.path.exists(ROULETTE_KNOWN_ANSWERS):
+        pytest.skip("oracle/_ref/roulette_known_answers not built (needs a rypath checkout)")
+    run = subprocess.run([ROULETTE_KNOWN_ANSWERS], capture_output=True, text=True, timeout=60)
+    assert run.returncode == 0, run.stderr
+
+
+def _unit(rng, n):
+    v = rng.normal(size=(n, 3))
+    return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+
+def hero_queries(n, rng):
+    """Hero BSDF queries (layout of or_probe_hero): diffuse, conductor and dielectric packets
+    with per-lane parameters (dispersive eta, smooth and rough lanes, matched indices), random
+    masks; evaluation directions random, mirrored or refracted (so Dirac lanes see their own
+    direction)."""
+    q = np.zeros((n, 32), np.float32)
+    kind = rng.integers(0, 3, n)
+    q[:, 0] = kind
+    mask = rng.integers(0, 16, n) | 1
+    q[:, 1] = np.where(rng.uniform(size=n) < 0.5, 15, mask)
+    q[:, 2] = rng.integers(0, 2, n)
+    base_eta = np.where(kind == 1, rng.uniform(0.1, 3, n), rng.uniform(1.0, 2.4, n))
+    base_eta = np.where((kind == 2) & (rng.uniform(size=n) < 0.05), 1.0, base_eta)
+    dispersion = rng.uniform(0, 0.05, n) * (rng.uniform(size=n) < 0.6)
+    rough = rng.uniform(0, 0.6, n) * (rng.uniform(size=n) > 0.35)
+    for k in range(4):
+        lane = 4 + 4 * k
+        q[:, lane] = np.where(kind == 0, rng.uniform(0, 1, n), base_eta * (1 + dispersion * (k - 1.5)))
+        q[:, lane + 1] = rng.uniform(0, 5, n)
+        q[:, lane + 2] = rough
+        q[:, lane + 3] = rough * rng.uniform(0.5, 1.5, n)
+    wo = _unit(rng, n)
+    q[:, 20:23] = wo
+    wi = _unit(rng, n)
+    mirror = wo * np.array([-1, -1, 1])
+    eta = np.where(wo[:, 2] > 0, q[:, 4], 1 / q[:, 4]).astype(np.float64)
+    cos_t2 = 1 - (1 - wo[:, 2] ** 2) / eta ** 2
+    refract = np.concatenate([-wo[:, :2] / eta[:, None],
+                              (-np.sign(wo[:, 2]) * np.sqrt(np.maximum(cos_t2, 0)))[:, None]], 1)
+    choice = rng.integers(0, 3, n)
+    q[:, 23:26] = np.where(choice[:, None] == 0, wi, np.where(choice[:, None] == 1, mirror, refract))
+    q[:, 26:29] = rng.uniform(0, 1, (n, 3))
+    return q
+
+
+def test_hero_bsdf_matches_reference():
+    """The oracle's hero proposals (companion densities on the hero direction, Dirac masses,
+    dispersive companion support, event eta) equal rypath_hero_scattering's, compiled from
+    shaders/hero_scattering.h, bit for bit."""
+    lib = need_ref()
+    q = hero_queries(30000, np.random.default_rng(21))
+    a = np.zeros((q.shape[0], 32), np.float32)
+    b = np.zeros((q.shape[0], 32), np.float32)
+    oracle().or_probe_hero(q.ctypes.data, q.shape[0], a.ctypes.data)
+    lib.ref_probe_hero(q.ctypes.data, q.shape[0], b.ctypes.data)
+    np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+    flags = a[:, 15].astype(np.int64)
+    # the generator reaches every branch: accepted continuous and Dirac samples, transmissions,
+    # dispersive Dirac companions with zero support, valid evaluations and Dirac lane masses
+    assert ((flags & 5) == 5).mean() > 0.05 and ((flags & 5) == 4).mean() > 0.2
+    assert ((flags & 2) != 0).mean() > 0.05
+    dirac = (flags & 1) == 1
+    assert ((a[:, 7:11] == 0) & (q[:, 1:2].astype(np.int64) == 15))[dirac].any()
+    assert (a[:, 24] == 1).mean() > 0.5 and (a[:, 25] > 0).mean() > 0.02
+
+
+def test_hero_roulette_matches_reference():
+    """hero_continue and hero_account_eta (shaders/hero_pt_helpers.h:56-98), compiled from
+    rypath's header, against the oracle's restatement on random tracks and edge values."""
+    lib = need_ref()
+    rng = np.random.default_rng(22)
+    n = 30000
+    q = np.zeros((n, 16), np.float32)
+    q[:, 0:4] = np.exp(rng.uniform(-12, 1, (n, 4))) * (rng.uniform(size=(n, 4)) > 0.2)
+    special = rng.uniform(size=(n, 4))
+    q[:, 0:4] = np.where(special < 0.01, np.float32(1e-40), q[:, 0:4])
+    q[:, 0:4] = np.where((special > 0.01) & (special < 0.015), np.inf, q[:, 0:4])
+    q[:, 4:8] = np.exp(rng.uniform(-3, 3, (n, 4)))
+    q[:, 4:8] = np.where(rng.uniform(size=(n, 4)) < 0.01, np.float32(2.0 ** 120), q[:, 4:8])
+    q[:, 8] = rng.uniform(size=n) > 0.1
+    q[:, 9] = rng.integers(0, 5, n)
+    q[:, 10] = rng.uniform(0, 1, n)
+    q[:, 11] = rng.integers(0, 2, n)
+    q[:, 12:16] = rng.uniform(0.3, 2.5, (n, 4))
+    q[:, 12:16] = np.where(rng.uniform(size=(n, 4)) < 0.01, 0.0, q[:, 12:16])
+    a = np.zeros((n, 12), np.float32)
+    b = np.zeros((n, 12), np.float32)
+    oracle().or_probe_roulette(q.ctypes.data, n, a.ctypes.data)
+    lib.ref_probe_roulette(q.ctypes.data, n, b.ctypes.data)
+    np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert 0.05 < (a[:, 0] == 0).mean() < 0.8  # paths are terminated and survive
+    assert ((a[:, 1:5] != q[:, 0:4]).any(1) & (a[:, 0] == 1)).mean() > 0.05  # survivors are rescaled
+    assert (a[:, 9] == 0).mean() > (q[:, 8] == 0).mean()  # unsafe eta disables roulette
+
+
+def test_hero_weight_matches_reference():
+    """The MIS weight of hero contributions (hero_weight, shaders/hero_pt_helpers.h:122-138)."""
+    lib = need_ref()
+    q = _advance_queries(30000, np.random.default_rng(23))
+    rng = np.random.default_rng(24)
+    q[:, 16:20] = np.where(rng.uniform(size=(q.shape[0], 1)) < 0.1, 0, q[:, 16:20])
+    a = np.zeros((q.shape[0], 5), np.float32)
+    b = np.zeros((q.shape[0], 5), np.float32)
+    oracle().or_probe_hero_weight(q.ctypes.data, q.shape[0], a.ctypes.data)
+    lib.ref_probe_hero_weight(q.ctypes.data, q.shape[0], b.ctypes.data)
+    np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert (a[:, 4] == 0).mean() > 0.3
