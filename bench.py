@@ -116,46 +116,63 @@ def measured_peaks():
 
 
 def trace_profile():
-    """Figures of k_trace from the committed ncu summary (DRAM and L2 bytes per closest-hit ray,
-    issue activity, SIMD efficiency, L2 throughput), keyed as in the summary; {} if absent."""
-    path = os.path.join(ROOT, "profiles", "k_trace_mixed.md")
-    figures = {}
-    if os.path.exists(path):
-        for line in open(path):
-            key, sep, value = line.partition(":")
-            if sep and key in ("dram_bytes_per_ray", "l2_bytes_per_ray", "issue_active_pct", "simd_efficiency",
-                               "l2_throughput_pct"):
-                figures[key] = float(value)
-    return figures
+    """The closest-hit kernel's ncu figures, per ray, from the small-case capture recorded in
+    rypath_b200/data/k_trace_ncu.json (DRAM and L2 bytes per ray, issue activity, SIMD
+    efficiency); {} if the file is absent."""
+    path = os.path.join(ROOT, "rypath_b200", "data", "k_trace_ncu.json")
+    return json.load(open(path)) if os.path.exists(path) else {}
 
 
-def traffic_per_ray():
-    """DRAM bytes per closest-hit ray of k_trace from the committed ncu summary, if present."""
-    return trace_profile().get("dram_bytes_per_ray")
+def l2_copy_gbs(torch):
+    """This GPU's L2 bandwidth, measured here: a device-to-device copy between two 24 MB buffers
+    (both resident in the 126 MB L2) repeated 200 times; bytes read plus written per second."""
+    src = torch.empty(24 << 20, dtype=torch.uint8, device="cuda")
+    dst = torch.empty_like(src)
+    for _ in range(20):
+        dst.copy_(src)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(200):
+        dst.copy_(src)
+    stop.record()
+    torch.cuda.synchronize()
+    return 2 * src.numel() * 200 / (start.elapsed_time(stop) / 1e3) / 1e9
+
+
+def strided_rows(w, h, lanes, max_spp):
+    """A bounded sample of the whole film, independent of how it is timed: every stride-th row
+    (rows stride // 2, stride // 2 + stride, ...), the stride the smallest that keeps the rows'
+    pixels within `lanes`, at as many absolute samples (0, 1, ...) as then fit, at most max_spp."""
+    stride = max(1, -(-w * h // max(1, lanes)))
+    rows = list(range(stride // 2, h, stride))
+    spp = max(1, min(max_spp, lanes // max(1, len(rows) * w)))
+    return rows, spp
 
 
 def cpu_baseline(orc, args, seconds, threads=0):
-    """The oracle (the reference's CPU path restated) on a bounded sample of the workload."""
+    """The oracle (the reference's CPU path restated) on a bounded sample of the workload: whole
+    rows spread over the film (strided_rows), sized from a short probe to about `seconds`."""
     from tests.oracle_lib import request
 
     w, h = args.width, args.height
-    probe = min(w * h, 8192)
-    t0 = time.perf_counter()
-    orc.sample(request(w, h, 1, pixel_begin=(w * h - probe) // 2, pixel_count=probe), threads=threads)
-    rate = probe / max(time.perf_counter() - t0, 1e-6)
-    target = int(max(probe, rate * seconds))
-    if target < w * h:
-        spp, pixels, begin = 1, target, (w * h - target) // 2
-    else:
-        spp, pixels, begin = min(args.spp, max(1, target // (w * h))), w * h, 0
-    t0 = time.perf_counter()
-    out = orc.sample(request(w, h, spp, pixel_begin=begin, pixel_count=pixels), threads=threads)
-    dt = time.perf_counter() - t0
+
+    def render(rows, spp):
+        t0 = time.perf_counter()
+        outs = [orc.sample(request(w, h, spp, pixel_begin=r * w, pixel_count=w), threads=threads) for r in rows]
+        return np.concatenate(outs), time.perf_counter() - t0
+
+    probe_rows, _ = strided_rows(w, h, 8 * w, 1)
+    out, dt = render(probe_rows, 1)
+    rate = out.size / max(dt, 1e-6)
+    rows, spp = strided_rows(w, h, int(max(8 * w, rate * seconds)), args.spp)
+    out, dt = render(rows, spp)
     ok = int((out["status"] == 0).sum())
     cores = threads if threads > 0 else (os.cpu_count() or 1)
+    stride = rows[1] - rows[0] if len(rows) > 1 else h
     return {"value": out.size / dt / 1e6, "unit": UNIT, "cores": cores, "kind": "port", "seconds": dt,
-            "sample": f"{out.size} lanes (pixels {begin}..{begin + pixels - 1} of the {w}x{h} film, absolute samples "
-                      f"0..{spp - 1}, depth {args.depth}), {dt:.2f} s, {ok} succeeded"}
+            "sample": f"{out.size} lanes: {len(rows)} whole rows of the {w}x{h} film (every {stride}th row from row "
+                      f"{rows[0]}), absolute samples 0..{spp - 1}, depth {args.depth}; {dt:.2f} s, {ok} succeeded"}
 
 
 def run_reference(args, rank):
@@ -247,22 +264,30 @@ def bench_views(torch):
         rs.render_views_device(views, req, film.data_ptr())
         batched_ms.append(rs.timing().total_ms)
     batched = film.clone()
-    plain_req = renderer.BatchRequest(wave_lanes=1 << 23, trace_block=128, shade_block=128, blocks_per_sm=12,
-                                      use_graph=2)
+    rs.close()
+    # the plain form: one scene per view (the reference renders one camera per job), each view
+    # rendered through rp_cuda_render_film_device into its part of the film
+    import copy
+
     film.zero_()
     plain_ms = 0.0
     for v in views:
-        one = renderer.View(v.camera, v.width, v.height, v.sample_begin, v.sample_count, 0)
+        one = copy.copy(scene)
+        one.camera, one.width, one.height, one._keep = v.camera, v.width, v.height, []
+        plain = renderer.build_renderer(one).scene
         sub = film[v.film_offset * abi.FILM_PIXEL_BYTES:(v.film_offset + v.width * v.height) * abi.FILM_PIXEL_BYTES]
-        rs.render_views_device([one], plain_req, sub.data_ptr())
-        plain_ms += rs.timing().total_ms
+        plain.render_film_device(renderer.RenderSettings(v.width, v.height, samples=v.sample_count,
+                                                         batch_size=v.sample_count, seed=1),
+                                 sub.data_ptr(), sample_begin=v.sample_begin)
+        plain_ms += plain.timing().total_ms
+        plain.close()
     identical = bool(torch.equal(batched, film))
-    rs.close()
     ms = min(batched_ms)
     return {"workload": "64 views of the mixed scene, resolutions U[256x256, 1280x720], spp {4..64}",
             "metric": "batched Msamples/s (all views)", "value": lanes / ms / 1e3, "unit": UNIT,
             "plain_per_view_value": lanes / plain_ms / 1e3, "speedup_vs_plain": plain_ms / ms,
             "films_identical_to_plain": identical, "lanes": lanes, "batched_ms": ms, "plain_ms": plain_ms,
+            "plain_form": "one scene per view, rp_cuda_render_film_device per view (render time only)",
             "tuned": {"wave_lanes": chosen.wave_lanes, "trace_block": chosen.trace_block,
                       "shade_block": chosen.shade_block, "blocks_per_sm": chosen.blocks_per_sm,
                       "probe_ms_per_mlane": chosen.probe_ms_per_mlane, "tuning_s": tune_s},
@@ -273,7 +298,8 @@ def bench_adjoint(torch, adam_steps):
     """Differentiation: 16 reflectance groups x 32 knots of the Cornell geometry, 512x512,
     32 spp, depth 8, L2 loss on film-mean XYZ against a 128-spp render of seeded true
     spectra.  The path-replay adjoint gradient against central differences (h = 1e-3, common
-    random numbers) of the same renders; errors against an 8x-spp adjoint gradient."""
+    random numbers) of the same renders; errors against a 32x-spp adjoint gradient on another
+    seed, and the adjoint's sample count at which its error matches the differences'."""
     from rypath_b200 import abi, renderer, scenes
 
     w, spp, params = 512, 32, 512
@@ -303,8 +329,9 @@ def bench_adjoint(torch, adam_steps):
     for _ in range(2):
         m, f_ms = mean(rs, spp, 1)
         grad, b_ms = adjoint(rs, spp, 1, 2 * (m - target))
-    mref, _ = mean(rs, 8 * spp, 7)
-    gref, _ = adjoint(rs, 8 * spp, 7, 2 * (mref - target))
+    # the reference gradient: the adjoint at 32x the samples, on another seed
+    mref, _ = mean(rs, 32 * spp, 7)
+    gref, _ = adjoint(rs, 32 * spp, 7, 2 * (mref - target))
     sub = list(range(3, params, 32))
     fd, fd_ms = [], 0.0
     h = 1e-3
@@ -321,6 +348,21 @@ def bench_adjoint(torch, adam_steps):
     rs.set_knot_values(0, theta0)
     fd = np.array(fd)
     rel = lambda x, y: float(np.linalg.norm(x - y) / np.linalg.norm(y))
+    fd_error = rel(fd, gref[sub])
+    fd_full_ms = fd_ms / len(sub) * params
+    # equal gradient error: the adjoint at growing sample counts until its error on the same
+    # parameters is at most the finite differences' error; that adjoint's time against theirs
+    ladder = []
+    matched = None
+    for n in (spp, 2 * spp, 4 * spp, 8 * spp, 16 * spp):
+        for _ in range(2):
+            m, a = mean(rs, n, 1)
+            g, b = adjoint(rs, n, 1, 2 * (m - target))
+        err = rel(g[sub], gref[sub])
+        ladder.append({"spp": n, "ms": a + b, "relative_error_subset": err, "relative_error_all": rel(g, gref)})
+        if err <= fd_error:
+            matched = ladder[-1]
+            break
     th, mom, vel, losses, dev_ms = theta0.copy(), np.zeros(params), np.zeros(params), [], 0.0
     t0 = time.perf_counter()
     for k in range(1, adam_steps + 1):
@@ -336,15 +378,19 @@ def bench_adjoint(torch, adam_steps):
     adam_s = time.perf_counter() - t0
     rs.close()
     adjoint_ms = f_ms + b_ms
-    fd_full_ms = fd_ms / len(sub) * params
     return {"workload": "cornell_groups 512x512, 32 spp, depth 8, 16 groups x 32 knots, L2 on XYZ",
             "metric": "gradient ms (forward + backward)", "value": adjoint_ms, "unit": "ms", "higher_is_better": False,
             "forward_ms": f_ms, "backward_ms": b_ms,
             "finite_difference_ms": fd_full_ms, "speedup_vs_finite_difference": fd_full_ms / adjoint_ms,
             "finite_difference": f"central, h = {h}, common random numbers, {len(sub)} of {params} parameters "
                                  f"timed ({fd_ms:.0f} ms), whole-gradient time scaled by parameter count",
-            "relative_error_vs_8x_adjoint": {"adjoint_all": rel(grad, gref), "adjoint_subset": rel(grad[sub], gref[sub]),
-                                             "finite_difference_subset": rel(fd, gref[sub])},
+            "relative_error_vs_32x_adjoint": {"adjoint_all": rel(grad, gref), "adjoint_subset": rel(grad[sub], gref[sub]),
+                                              "finite_difference_subset": fd_error},
+            "equal_error": {"adjoint_ladder": ladder, "matched": matched,
+                            "speedup_vs_finite_difference": (fd_full_ms / matched["ms"]) if matched else None,
+                            "rule": "smallest adjoint spp (32 x 2^k) whose error on the finite-difference parameters "
+                                    "is at most the finite differences' error at 32 spp; both against the "
+                                    "1024-spp adjoint on another seed"},
             "adam": {"steps": adam_steps, "lr": 0.02, "loss_first": losses[0] if losses else None,
                      "loss_last": losses[-1] if losses else None, "device_ms_per_step": dev_ms / max(1, adam_steps),
                      "wall_s": adam_s}}
@@ -434,7 +480,11 @@ def main():
     trace_bytes_per_step = algo_per_ray * rays
     achieved = trace_bytes_per_step * len(steps) / (trace_ms / 1e3) / 1e9 if trace_ms > 0 else None
     peak, peak_kind = measured_peaks()
-    tpr = traffic_per_ray()
+    ncu = trace_profile()
+    tpr = ncu.get("dram_bytes_per_ray")
+    l2_peak = l2_copy_gbs(torch)
+    avg_launch_s = trace_ms / max(1, trace_launches) / 1e3
+    rays_per_launch = rays / max(1, counts.trace_launches)
     # launch time per kernel group over the summed launch time of all groups (the shadow walks of
     # one event overlap the next event's closest-hit walk on a second stream, so the groups'
     # launch times add up to more than the step time)
@@ -453,12 +503,31 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "k_trace (closest-hit traversal)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
-                         "traffic": (tpr * rays / max(1, counts.trace_launches)) if tpr else None,
+                         "traffic": (tpr * rays_per_launch) if tpr else None,
                          "algorithmic_bytes_per_launch": trace_bytes_per_step / max(1, counts.trace_launches),
                          "algorithmic_bytes_per_ray": algo_per_ray, "peak_kind": peak_kind,
                          "avg_launch_ms": trace_ms / max(1, trace_launches),
-                         # the same kernel's ncu figures (profiles/k_trace_mixed.md): it is issue-bound
-                         "ncu": dict(trace_profile(), source="profiles/k_trace_mixed.md")},
+                         # what limits the walk: most of its bytes come from L2, and it is
+                         # issue-bound at low SIMD efficiency (ncu, rypath_b200/data/k_trace_ncu.json)
+                         "limiter": "issue (SIMD efficiency of uneven ray lengths), not HBM",
+                         "l2": {"peak_gbs": l2_peak, "peak_kind": "measured here (L2-resident device copy)",
+                                "achieved_gbs": (ncu["l2_bytes_per_ray"] * rays_per_launch / avg_launch_s / 1e9)
+                                if ncu.get("l2_bytes_per_ray") and trace_ms > 0 else None,
+                                "algorithmic_frac": (achieved / l2_peak) if achieved else None,
+                                "bytes_per_ray": ncu.get("l2_bytes_per_ray")},
+                         "issue": {"issue_active": ncu.get("issue_active"), "simd_efficiency": ncu.get("simd_efficiency"),
+                                   "useful_lane_fraction": (ncu["issue_active"] * ncu["simd_efficiency"])
+                                   if ncu.get("issue_active") else None},
+                         "ncu_source": ncu.get("capture")},
+            "traversal_per_ray": {
+                "closest": {"nodes": counts.nodes_visited / max(1, counts.closest_rays),
+                            "triangles": counts.triangles_tested / max(1, counts.closest_rays),
+                            "ns_per_ray": trace_ms / len(steps) * 1e6 / max(1, counts.closest_rays)},
+                "shadow": {"nodes": counts.shadow_nodes_visited / max(1, counts.shadow_rays),
+                           "triangles": counts.shadow_triangles_tested / max(1, counts.shadow_rays),
+                           "ns_per_ray": group_ms["shadow"] / len(steps) * 1e6 / max(1, counts.shadow_rays)}},
+            "shade_family_ms_per_step": dict(zip(("diffuse", "conductor", "dielectric", "escape"),
+                                                 list(counts.shade_family_ms))),
             "kernel_share": shares,
             "kernel_group_ms_per_step": {k: v / len(steps) for k, v in group_ms.items()},
             "rays_per_step": {"closest": counts.closest_rays, "shadow": counts.shadow_rays},

@@ -163,7 +163,7 @@ class Timing(C.Structure):
                 ("triangles_tested", u64), ("trace_launches", u64), ("shadow_launches", u64),
                 ("shade_launches", u64), ("other_launches", u64), ("shadow_nodes_visited", u64),
                 ("shadow_triangles_tested", u64), ("build_ms", f64), ("build_host_ms", f64),
-                ("build_bvh_ms", f64)]
+                ("build_bvh_ms", f64), ("shade_family_ms", f64 * 4)]
 
 
 # numpy dtypes with the same layouts, for bulk views of result buffers

@@ -633,6 +633,8 @@ struct rp_scene {
             cudaStreamSynchronize(stream);
         for (auto e : events)
             cudaEventDestroy(e);
+        for (auto e : family_events)
+            cudaEventDestroy(e);
         for (int k = 0; k < 3; ++k) {
             if (family_done[k])
                 cudaEventDestroy(family_done[k]);
@@ -667,6 +669,22 @@ struct rp_scene {
         RP_CHECK(cudaEventRecord(events[event_cursor + 1], on ? on : stream));
         event_cursor += 2;
     }
+    // per-family shade timing of counting runs: a pair of events around each family kernel, on
+    // that kernel's stream, apart from the group pairs above
+    std::vector<cudaEvent_t> family_events;
+    std::vector<int> family_kind;
+    void mark_family(int family_index, cudaStream_t on) {
+        if (2 * family_kind.size() + 2 > family_events.size()) {
+            for (int k = 0; k < 64; ++k) {
+                cudaEvent_t e;
+                RP_CHECK(cudaEventCreate(&e));
+                family_events.push_back(e);
+            }
+        }
+        RP_CHECK(cudaEventRecord(family_events[2 * family_kind.size()], on));
+        family_kind.push_back(family_index);
+    }
+    void done_family(cudaStream_t on) { RP_CHECK(cudaEventRecord(family_events[2 * family_kind.size() - 1], on)); }
     void collect() {
         RP_CHECK(cudaStreamSynchronize(stream));
         double sums[4] = {0, 0, 0, 0};
@@ -677,6 +695,14 @@ struct rp_scene {
             sums[event_kind[i]] += ms;
             ++counts[event_kind[i]];
         }
+        for (int k = 0; k < 4; ++k)
+            timing.shade_family_ms[k] = 0;
+        for (size_t i = 0; i < family_kind.size(); ++i) {
+            float ms = 0;
+            RP_CHECK(cudaEventElapsedTime(&ms, family_events[2 * i], family_events[2 * i + 1]));
+            timing.shade_family_ms[family_kind[i]] += ms;
+        }
+        family_kind.clear();
         timing.trace_launches = counts[0];
         timing.shadow_launches = counts[1];
         timing.shade_launches = counts[2];
@@ -873,10 +899,28 @@ void launch_shade(rp_scene *s, const WaveParams &p, const PathPool &pool, int in
     RP_CHECK(cudaEventRecord(s->forked, s->stream));
     for (int k = 0; k < 3; ++k)
         RP_CHECK(cudaStreamWaitEvent(s->family[k], s->forked, 0));
-    k_shade<0, 128, Adjoint><<<grid, 128, smem, s->stream>>>(s->ds, p, pool, in);
-    k_shade<1, 128, Adjoint><<<grid, 128, smem, s->family[0]>>>(s->ds, p, pool, in);
-    k_shade<2, 128, Adjoint><<<grid, 128, smem, s->family[1]>>>(s->ds, p, pool, in);
-    k_shade<3, 128, Adjoint><<<grid, 128, smem, s->family[2]>>>(s->ds, p, pool, in);
+    const bool timed = s->counting;
+    cudaStream_t on[4] = {s->stream, s->family[0], s->family[1], s->family[2]};
+    if (timed)
+        s->mark_family(0, on[0]);
+    k_shade<0, 128, Adjoint><<<grid, 128, smem, on[0]>>>(s->ds, p, pool, in);
+    if (timed) {
+        s->done_family(on[0]);
+        s->mark_family(1, on[1]);
+    }
+    k_shade<1, 128, Adjoint><<<grid, 128, smem, on[1]>>>(s->ds, p, pool, in);
+    if (timed) {
+        s->done_family(on[1]);
+        s->mark_family(2, on[2]);
+    }
+    k_shade<2, 128, Adjoint><<<grid, 128, smem, on[2]>>>(s->ds, p, pool, in);
+    if (timed) {
+        s->done_family(on[2]);
+        s->mark_family(3, on[3]);
+    }
+    k_shade<3, 128, Adjoint><<<grid, 128, smem, on[3]>>>(s->ds, p, pool, in);
+    if (timed)
+        s->done_family(on[3]);
     for (int k = 0; k < 3; ++k) {
         RP_CHECK(cudaEventRecord(s->family_done[k], s->family[k]));
         RP_CHECK(cudaStreamWaitEvent(s->stream, s->family_done[k], 0));

@@ -16,6 +16,7 @@ because the integer sample words and the sensor response are pinned to them:
 Usage: ``python make_tables.py /path/to/rypath`` (writes next to this script).
 """
 
+import os
 import re
 import struct
 import sys
@@ -62,7 +63,11 @@ def cie_table(reference: Path) -> bytes:
 
 
 def main() -> None:
-    reference = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # the rypath checkout: the first argument, else the RYPATH_REFERENCE environment variable
+    source = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RYPATH_REFERENCE")
+    if not source:
+        raise SystemExit("usage: name a rypath checkout as the argument or in RYPATH_REFERENCE")
+    reference = Path(source)
     out = Path(__file__).resolve().parent
     (out / "pbrt_sobol_tables.bin").write_bytes(sobol_tables(reference))
     (out / "cie_xyz_1931.bin").write_bytes(cie_table(reference))

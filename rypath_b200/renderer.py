@@ -80,6 +80,7 @@ class RenderSettings:
     randomization: int = abi.RANDOMIZE_OWEN
     exposure: float = 1.0             # Film::exposure (compatibility planes only)
     max_component_value: float = 0.0  # Film::max_component_value; 0 or inf: no clamp
+    emergency_limit: int = 1024       # render_emergency_limit (src/render.hpp:22-26)
 
 
 @dataclass
@@ -201,21 +202,30 @@ class CudaRenderScene:
             fresh = True
         r = abi.FilmRequest(width=settings.width, height=settings.height, seed=settings.seed,
                             sample_begin=sample_begin, sample_count=settings.samples, batch_size=settings.batch_size,
-                            sampler_kind=settings.sampler, randomization=settings.randomization, emergency_limit=1024,
+                            sampler_kind=settings.sampler, randomization=settings.randomization,
+                            emergency_limit=settings.emergency_limit,
                             flags=abi.FILM_FRESH if fresh else 0, exposure=settings.exposure,
                             max_component_value=settings.max_component_value)
         diag = C.create_string_buffer(512)
         st = native.lib().rp_cuda_render_film(self._handle, C.byref(r), film.ctypes.data, diag, 512)
         return st, diag.value.decode(errors="replace"), film
 
-    def render_film_device(self, settings: RenderSettings, device_film_ptr: int, sample_begin: int = 0):
+    def render_film_device(self, settings: RenderSettings, device_film_ptr: int, sample_begin: int = 0,
+                           fresh: bool = False, check: bool = True):
+        """Progressive render into a device film (rp_film_pixel rows at ``device_film_ptr``), onto
+        its committed state (``fresh``: from an empty film).  Returns (status, diagnostic); with
+        ``check`` a failed call raises instead."""
         self._ensure_cie()
         r = abi.FilmRequest(width=settings.width, height=settings.height, seed=settings.seed,
                             sample_begin=sample_begin, sample_count=settings.samples, batch_size=settings.batch_size,
-                            sampler_kind=settings.sampler, randomization=settings.randomization, emergency_limit=1024)
+                            sampler_kind=settings.sampler, randomization=settings.randomization,
+                            emergency_limit=settings.emergency_limit, flags=abi.FILM_FRESH if fresh else 0,
+                            exposure=settings.exposure, max_component_value=settings.max_component_value)
         diag = C.create_string_buffer(512)
         st = native.lib().rp_cuda_render_film_device(self._handle, C.byref(r), C.c_void_p(device_film_ptr), diag, 512)
-        native.check(st, diag, "rp_cuda_render_film_device")
+        if check:
+            native.check(st, diag, "rp_cuda_render_film_device")
+        return st, diag.value.decode(errors="replace")
 
     def render_views_device(self, views, request: "BatchRequest", device_film_ptr: int) -> abi.BatchConfig:
         """All ``views`` (a list of ``View``) into one device film, sharing one wavefront.

@@ -17,6 +17,7 @@ Usage: ``python tests/golden/make_golden.py /path/to/rypath`` (writes next to th
 """
 
 import json
+import os
 import re
 import sys
 from pathlib import Path
@@ -90,7 +91,11 @@ def gaussian_answers(text: str):
 
 
 def main() -> None:
-    reference = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # the rypath checkout: the first argument, else the RYPATH_REFERENCE environment variable
+    source = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RYPATH_REFERENCE")
+    if not source:
+        raise SystemExit("usage: name a rypath checkout as the argument or in RYPATH_REFERENCE")
+    reference = Path(source)
     here = Path(__file__).resolve().parent
     sobol = sobol_answers((reference / "tests/sampling_tests.cpp").read_text())
     philox = philox_answers((reference / "tests/replay_tests.cpp").read_text())

@@ -9,6 +9,12 @@ These tests check, through the C ABI, that it returns what the allocating entry 
 scratch keeps the previous call's contents, which must not leak into the next), and that a
 request larger than the scratch is refused with a clear message.
 
+The allocation-free entry point runs the same kernels in the same order as the allocating
+one, so their packets are compared byte for byte: a value left over in the shared scratch from
+an earlier call would show as a difference.  The checks also run on the scene's own stream
+(stream NULL), and the device's free memory is the same before and after a call on a scene
+that has never sampled (so it owns no wavefront pool yet).
+
 This file is named so pytest collects it last.
 """
 
@@ -21,45 +27,66 @@ from rypath_b200 import abi, native, renderer, scenes
 
 pytestmark = pytest.mark.gpu
 
-RTOL = 1e-3  # the per-lane tolerance of tests/test_gpu_parity.py
 RP_STATIC_MAX_LANES = 178464  # include/rypath_cuda.h
+REQUESTS = [renderer.RenderRequest(32, 32, sample_begin=0, sample_count=4),
+            renderer.RenderRequest(32, 32, pixel_begin=100, pixel_count=600, sample_begin=9, sample_count=3,
+                                   sampler=abi.SAMPLER_INDEPENDENT)]
 
 
-def _static_sample(scene_handle, request, torch):
+def _static_sample(scene_handle, request, torch, own_stream=True):
+    """One call of the allocation-free entry point into a buffer poisoned with 0xff; on a
+    stream of the caller's (own_stream) or on the scene's own stream (NULL)."""
     q = request.to_c()
     lanes = q.pixel_count * q.sample_count
-    stream = torch.cuda.Stream()  # an explicit stream: a NULL stream means the scene's own stream
-    with torch.cuda.stream(stream):
-        out = torch.full((lanes * 80,), 0xFF, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream() if own_stream else None
+    out = torch.full((lanes * 80,), 0xFF, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
     diag = C.create_string_buffer(512)
     st = native.lib().rp_cuda_sample_device_static(scene_handle, C.byref(q), C.c_void_p(out.data_ptr()), lanes,
-                                                    C.c_void_p(stream.cuda_stream), diag, 512)
-    stream.synchronize()
+                                                    C.c_void_p(stream.cuda_stream if stream else None), diag, 512)
     torch.cuda.synchronize()
     return st, diag.value.decode(), out.cpu().numpy().view(abi.packet_dtype())
 
 
-def _same(static, reference):
-    for f in ("status", "pixel", "sample_low", "sample_high", "splat_count"):
-        np.testing.assert_array_equal(static[f], reference[f])
-    for f in ("wavelengths", "wavelength_pdfs", "radiance", "filter_weight"):
-        np.testing.assert_allclose(static[f], reference[f], rtol=RTOL, atol=1e-7)
-
-
-def test_static_entry_point_matches_allocating_one_twice():
+@pytest.mark.parametrize("own_stream", [True, False])
+def test_static_entry_point_matches_allocating_one_twice(own_stream):
     torch = pytest.importorskip("torch")
-    scene = scenes.cornell_box(32, 32, 4)
-    built = renderer.build_renderer(scene)
+    built = renderer.build_renderer(scenes.cornell_box(32, 32, 4))
     assert built.status == abi.RP_SUCCESS, built.diagnostic
-    requests = [renderer.RenderRequest(32, 32, sample_begin=0, sample_count=4),
-                renderer.RenderRequest(32, 32, pixel_begin=100, pixel_count=600, sample_begin=9, sample_count=3,
-                                       sampler=abi.SAMPLER_INDEPENDENT)]
-    for req in requests:
-        st, diag, static = _static_sample(built.scene.handle, req, torch)
+    for req in REQUESTS:
+        st, diag, static = _static_sample(built.scene.handle, req, torch, own_stream)
         assert st == abi.RP_SUCCESS, diag
         ref = built.scene.sample(req)
         assert ref.status == abi.RP_SUCCESS, ref.diagnostic
-        _same(static, ref.packet_samples)
+        assert static.tobytes() == ref.packet_samples.tobytes()
+    built.scene.close()
+
+
+def test_static_entry_point_allocates_no_device_memory():
+    torch = pytest.importorskip("torch")
+    # load the kernels first (lazy module loading places their code in device memory)
+    warm = renderer.build_renderer(scenes.cornell_box(32, 32, 4))
+    assert warm.status == abi.RP_SUCCESS, warm.diagnostic
+    st, diag, _ = _static_sample(warm.scene.handle, REQUESTS[0], torch)
+    assert st == abi.RP_SUCCESS, diag
+    warm.scene.close()
+    built = renderer.build_renderer(scenes.cornell_box(32, 32, 4))
+    assert built.status == abi.RP_SUCCESS, built.diagnostic
+    q = REQUESTS[0].to_c()
+    lanes = q.pixel_count * q.sample_count
+    out = torch.empty(lanes * 80, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    diag = C.create_string_buffer(512)
+    for _ in range(2):
+        st = native.lib().rp_cuda_sample_device_static(built.scene.handle, C.byref(q), C.c_void_p(out.data_ptr()),
+                                                        lanes, None, diag, 512)
+        assert st == abi.RP_SUCCESS, diag.value.decode()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free_before
+    static = out.cpu().numpy().view(abi.packet_dtype())
+    ref = built.scene.sample(REQUESTS[0])
+    assert static.tobytes() == ref.packet_samples.tobytes()
     built.scene.close()
 
 
