@@ -379,6 +379,59 @@ rp_status rp_cuda_adjoint_device(struct rp_scene *scene, const rp_adjoint_reques
                                  const double *device_d_loss_d_xyz, float *device_gradient, char *diag,
                                  size_t diag_capacity);
 
+/* ---- frame sessions ------------------------------------------------------------------- */
+
+/* An interactive frame session (FrameSession, src/frame_session.hpp:182-212, with the
+ * independent estimator and the path tracer): each frame renders one fresh absolute sample of
+ * every pixel into raw XYZ that stays on the device until it is captured, asynchronously on
+ * the session's stream.  A session has two frame slots; a submitted frame holds its slot until
+ * it is released, also after completion.  The session renders its scene on that scene's
+ * device; the scene must outlive the session.  Calls on one session need external
+ * serialisation, and a session shares its scene's stream and wavefront with the scene's other
+ * calls (serialise them too). */
+typedef struct rp_frame_config { /* FrameConfig subset, src/frame_session.hpp:58-100 */
+    uint32_t width, height;
+    uint64_t seed;
+    uint32_t sampler_kind, randomization;
+    uint64_t footprint_samples; /* the fixed sample budget ZSobol needs (FrameConfig::footprint_samples) */
+} rp_frame_config;
+typedef struct rp_frame_request { /* FrameRequest, src/frame_session.hpp:113-116 */
+    uint64_t sample_index, epoch;
+    const rp_camera *camera; /* NULL: the scene's camera; else this raster camera from now on */
+} rp_frame_request;
+enum { RP_FRAME_PENDING = 0, RP_FRAME_COMPLETE = 1, RP_FRAME_FAILED = 2 }; /* FrameStatus */
+typedef struct rp_frame_info { /* FrameInfo subset, src/frame_session.hpp:118-150 */
+    uint32_t status;           /* RP_FRAME_* */
+    uint32_t width, height;
+    uint64_t sample_index, epoch;
+    double gpu_ms;             /* device time of the frame's work, when complete */
+    uint64_t completed_samples;
+    uint32_t failed_pixels;    /* pixels whose sample failed (a failed frame has at least one) */
+} rp_frame_info;
+
+rp_status rp_cuda_frame_session_create(struct rp_scene *scene, const rp_frame_config *config,
+                                       struct rp_frame_session **session, char *diag, size_t diag_capacity);
+/* Waits for the session's frames and frees them. */
+void rp_cuda_frame_session_destroy(struct rp_frame_session *session);
+/* FrameSession::submit.  On success *frame is the frame's slot (0 or 1).  When both slots are
+ * held the call returns RP_FAILURE with *busy set (FrameSubmitResult::busy). */
+rp_status rp_cuda_frame_submit(struct rp_frame_session *session, const rp_frame_request *request, uint32_t *frame,
+                               int *busy, char *diag, size_t diag_capacity);
+/* Frame::poll (no wait) and Frame::wait. */
+rp_status rp_cuda_frame_poll(struct rp_frame_session *session, uint32_t frame, rp_frame_info *info);
+rp_status rp_cuda_frame_wait(struct rp_frame_session *session, uint32_t frame, rp_frame_info *info);
+/* Frame::capture: waits, then copies the frame's raw XYZ (3 floats per pixel, row major) into
+ * host memory of capacity_pixels pixels.  The sensor value of a pixel is packet_sensor_xyz of
+ * its sample without the filter weight, which cancels (shaders/frame_sensor.h:33-52); the
+ * scalar transport's is its wavelength's matching-function value times 470 times radiance
+ * (:22-31). */
+rp_status rp_cuda_frame_capture(struct rp_frame_session *session, uint32_t frame, float *host_xyz,
+                                size_t capacity_pixels, char *diag, size_t diag_capacity);
+/* The frame's device raw XYZ (valid until the frame is released). */
+rp_status rp_cuda_frame_device_xyz(struct rp_frame_session *session, uint32_t frame, const float **device_xyz);
+/* Releases the frame's slot (the Frame's destructor); waits for its work first. */
+rp_status rp_cuda_frame_release(struct rp_frame_session *session, uint32_t frame);
+
 /* ---- instrumentation ------------------------------------------------------------------ */
 
 /* Timing of the last sample/film call on this scene. */

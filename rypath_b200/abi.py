@@ -195,6 +195,22 @@ def film_dtype():
 FILM_PIXEL_BYTES = 144  # sizeof(rp_film_pixel)
 
 
+class FrameConfig(C.Structure):
+    _fields_ = [("width", u32), ("height", u32), ("seed", u64), ("sampler_kind", u32), ("randomization", u32),
+                ("footprint_samples", u64)]
+
+
+class FrameRequest(C.Structure):
+    _fields_ = [("sample_index", u64), ("epoch", u64), ("camera", C.POINTER(Camera))]
+
+
+class FrameInfo(C.Structure):
+    _fields_ = [("status", u32), ("width", u32), ("height", u32), ("sample_index", u64), ("epoch", u64),
+                ("gpu_ms", f64), ("completed_samples", u64), ("failed_pixels", u32)]
+
+
+FRAME_PENDING, FRAME_COMPLETE, FRAME_FAILED = 0, 1, 2
+
 EXPECTED_SIZES = {
     "rp_instance": (Instance, 88), "rp_material": (Material, 64), "rp_knot": (Knot, 8),
     "rp_area_emission": (AreaEmission, 1888), "rp_positional_light": (PositionalLight, 1948),
@@ -203,4 +219,5 @@ EXPECTED_SIZES = {
     "rp_film_pixel": (FilmPixel, 144), "rp_film_request": (FilmRequest, 88),
     "rp_view": (View, 80), "rp_batch_config": (BatchConfig, 24), "rp_batch_request": (BatchRequest, 64),
     "rp_adjoint_request": (AdjointRequest, 104),
+    "rp_frame_config": (FrameConfig, 32), "rp_frame_request": (FrameRequest, 24), "rp_frame_info": (FrameInfo, 56),
 }

@@ -3,7 +3,8 @@
 // (include/rypath_cuda.h).  This translation unit takes the place of src/metal_render_stub.cpp
 // in rypath_metal_backend (CMakeLists.txt:190-236): the progressive driver, job, checkpoint,
 // CLI and output code are unchanged and reach the B200 kernels through build_metal_renderer
-// and MetalRenderScene::sample, exactly as they reach Metal on Apple hardware.
+// and MetalRenderScene::sample, exactly as they reach Metal on Apple hardware; interactive
+// callers reach them through build_frame_session / FrameSession (src/frame_session.hpp).
 //
 // Beyond that boundary, cuda_backend::FilmRenderer (cuda_render.hpp) renders whole batches into
 // rypath's Film on the device (the PacketFilmBatch reduction done there, film_fold.hpp).
@@ -412,34 +413,150 @@ ShadingNormalProbeResult probe_shading_normal(const std::vector<shading_normal_p
             .guard_count = 0};
 }
 
-// The interactive frame session (src/frame_session.hpp) is not part of this backend: it
-// reports not_built, as the stub does on platforms without Metal.
-struct Frame::Impl {};
-struct FrameSession::Impl {};
+// ---- frame sessions (src/frame_session.hpp) over rp_cuda_frame_*: the independent estimator
+// and the path tracer, rypath's FrameSession sampler (the independent sampler,
+// src/metal_render.mm:4035).  A session and the frames it returns share one handle, so a Frame
+// stays valid after its FrameSession is destroyed (src/frame_session.hpp:176-181).
+namespace cuda_backend {
+struct FrameHandle {
+    rp_scene *scene = nullptr;
+    rp_frame_session *session = nullptr;
+    std::uint32_t width = 0, height = 0;
+    ~FrameHandle() {
+        rp_cuda_frame_session_destroy(session);
+        rp_cuda_scene_destroy(scene);
+    }
+};
+} // namespace cuda_backend
+
+struct Frame::Impl {
+    std::shared_ptr<cuda_backend::FrameHandle> handle;
+    std::uint32_t slot = 0;
+    ~Impl() { rp_cuda_frame_release(handle->session, slot); }
+};
+struct FrameSession::Impl {
+    std::shared_ptr<cuda_backend::FrameHandle> handle;
+};
+
+namespace {
+FrameInfo frame_info(const rp_frame_info &f) {
+    FrameInfo info;
+    info.width = f.width;
+    info.height = f.height;
+    info.sample_index = f.sample_index;
+    info.epoch = f.epoch;
+    info.status = f.status == RP_FRAME_PENDING    ? FrameStatus::pending
+                  : f.status == RP_FRAME_COMPLETE ? FrameStatus::complete
+                                                  : FrameStatus::failed;
+    info.gpu_seconds = f.gpu_ms / 1e3;
+    info.gpu_time_valid = f.status != RP_FRAME_PENDING;
+    info.completed_samples = f.completed_samples;
+    info.command_count = 1;
+    if (f.status == RP_FRAME_FAILED)
+        info.diagnostic = std::to_string(f.failed_pixels) + " pixel samples failed";
+    return info;
+}
+} // namespace
+
 Frame::Frame(std::shared_ptr<Impl> impl) : impl_(std::move(impl)) {}
 Frame::~Frame() = default;
 Frame::Frame(Frame &&) noexcept = default;
 Frame &Frame::operator=(Frame &&) noexcept = default;
-FrameInfo Frame::poll() const { return {.status = FrameStatus::failed, .diagnostic = "CUDA frame sessions not built"}; }
-FrameInfo Frame::wait() const { return poll(); }
+FrameInfo Frame::poll() const {
+    rp_frame_info f{};
+    if (rp_cuda_frame_poll(impl_->handle->session, impl_->slot, &f) != RP_SUCCESS)
+        return {.status = FrameStatus::failed, .diagnostic = "CUDA frame poll failed"};
+    return frame_info(f);
+}
+FrameInfo Frame::wait() const {
+    rp_frame_info f{};
+    if (rp_cuda_frame_wait(impl_->handle->session, impl_->slot, &f) != RP_SUCCESS)
+        return {.status = FrameStatus::failed, .diagnostic = "CUDA frame wait failed"};
+    return frame_info(f);
+}
 FrameCapture Frame::capture() const {
-    return {.status = GeometryStatus::not_built, .diagnostic = "CUDA frame sessions not built", .raw_xyz = {}};
+    FrameCapture out;
+    const auto &h = *impl_->handle;
+    out.width = h.width;
+    out.height = h.height;
+    out.raw_xyz.resize(std::size_t(h.width) * h.height);
+    char diag[1024] = {};
+    const rp_status st = rp_cuda_frame_capture(h.session, impl_->slot, out.raw_xyz.front().data(), out.raw_xyz.size(),
+                                               diag, sizeof diag);
+    out.status = cuda_backend::status_of(st);
+    out.diagnostic = diag;
+    return out;
 }
 FrameSession::FrameSession(std::unique_ptr<Impl> impl) : impl_(std::move(impl)) {}
 FrameSession::~FrameSession() = default;
 FrameSession::FrameSession(FrameSession &&) noexcept = default;
 FrameSession &FrameSession::operator=(FrameSession &&) noexcept = default;
-FrameSubmitResult FrameSession::submit(const FrameRequest &) {
-    return {.status = GeometryStatus::not_built, .diagnostic = "CUDA frame sessions not built", .frame = {}};
+FrameSubmitResult FrameSession::submit(const FrameRequest &request) {
+    FrameSubmitResult out;
+    rp_camera camera{};
+    rp_frame_request q{request.sample_index, request.epoch, nullptr};
+    if (request.camera) {
+        if (!request.camera->raster_camera) {
+            out.status = GeometryStatus::not_built;
+            out.diagnostic = "CUDA frame sessions take PBRT raster cameras";
+            return out;
+        }
+        const RasterCamera &c = *request.camera->raster_camera;
+        const GeometryPoint *points[4] = {&c.origin, &c.corner, &c.dx, &c.dy};
+        float *dst[4] = {camera.origin, camera.corner, camera.dx, camera.dy};
+        for (int k = 0; k < 4; ++k) {
+            dst[k][0] = points[k]->x;
+            dst[k][1] = points[k]->y;
+            dst[k][2] = points[k]->z;
+        }
+        q.camera = &camera;
+    }
+    std::uint32_t slot = 0;
+    int busy = 0;
+    char diag[1024] = {};
+    const rp_status st = rp_cuda_frame_submit(impl_->handle->session, &q, &slot, &busy, diag, sizeof diag);
+    out.status = cuda_backend::status_of(st);
+    out.busy = busy != 0;
+    out.diagnostic = diag;
+    if (st == RP_SUCCESS) {
+        auto frame = std::make_shared<Frame::Impl>();
+        frame->handle = impl_->handle;
+        frame->slot = slot;
+        out.frame.reset(new Frame(std::move(frame)));
+    }
+    return out;
 }
-FrameSessionBuildResult build_frame_session(const RenderScene &, const FrameConfig &config,
+FrameSessionBuildResult build_frame_session(const RenderScene &scene, const FrameConfig &config,
                                             const std::filesystem::path &) {
     FrameSessionBuildResult result;
-    result.status = GeometryStatus::not_built;
-    result.diagnostic = "CUDA frame sessions not built";
     result.shadow_traversal.requested = config.shadow_traversal;
     result.acceleration_build.requested = config.acceleration_build_policy;
+    auto handle = std::make_shared<cuda_backend::FrameHandle>();
+    handle->width = config.width;
+    handle->height = config.height;
+    rp_status st = cuda_backend::create(scene, &handle->scene, result.diagnostic);
+    if (st == RP_SUCCESS) {
+        const std::vector<double> cie = cuda_backend::cie_rows();
+        st = rp_cuda_set_cie(handle->scene, cie.data());
+    }
+    if (st == RP_SUCCESS) {
+        rp_frame_config c{};
+        c.width = config.width;
+        c.height = config.height;
+        c.seed = config.seed;
+        c.sampler_kind = RP_SAMPLER_INDEPENDENT;
+        c.footprint_samples = config.footprint_samples;
+        char diag[1024] = {};
+        st = rp_cuda_frame_session_create(handle->scene, &c, &handle->session, diag, sizeof diag);
+        result.diagnostic = diag;
+    }
+    result.status = cuda_backend::status_of(st);
     result.acceleration_build.diagnostic = result.diagnostic;
+    if (st == RP_SUCCESS) {
+        auto impl = std::make_unique<FrameSession::Impl>();
+        impl->handle = std::move(handle);
+        result.session.reset(new FrameSession(std::move(impl)));
+    }
     return result;
 }
 

@@ -669,6 +669,13 @@ struct rp_scene {
         RP_CHECK(cudaEventRecord(events[event_cursor + 1], on ? on : stream));
         event_cursor += 2;
     }
+    // forget the recorded pairs without reading them (asynchronous calls)
+    void discard_marks() {
+        launches = 0;
+        event_kind.clear();
+        event_cursor = 0;
+        family_kind.clear();
+    }
     // per-family shade timing of counting runs: a pair of events around each family kernel, on
     // that kernel's stream, apart from the group pairs above
     std::vector<cudaEvent_t> family_events;
@@ -1361,6 +1368,9 @@ uint32_t rp_cuda_abi_size(const char *name) {
     if (n == "rp_batch_config") return sizeof(rp_batch_config);
     if (n == "rp_batch_request") return sizeof(rp_batch_request);
     if (n == "rp_adjoint_request") return sizeof(rp_adjoint_request);
+    if (n == "rp_frame_config") return sizeof(rp_frame_config);
+    if (n == "rp_frame_request") return sizeof(rp_frame_request);
+    if (n == "rp_frame_info") return sizeof(rp_frame_info);
     return 0;
 }
 
@@ -2843,6 +2853,251 @@ rp_status rp_cuda_trace_rays(rp_scene *s, const float *rays, uint32_t count, int
         RP_CHECK(cudaStreamSynchronize(s->stream));
         return RP_SUCCESS;
     });
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------- frame sessions
+// FrameSession (src/frame_session.hpp:182-212), independent estimator: one absolute sample of
+// every pixel per frame, raw XYZ on the device, two frame slots, asynchronous on the scene's
+// stream.  A frame is one wave of the scene's wavefront (hero or scalar transport) followed by
+// the frame-sensor kernel; its camera, when the request names one, is the scene camera for
+// that wave.
+struct rp_frame_session {
+    rp_scene *scene = nullptr;
+    rp_frame_config config{};
+    bool camera_set = false;
+    rp_camera camera{};
+    struct Slot {
+        float *xyz = nullptr;   // 3 floats per pixel (device)
+        u32 *failures = nullptr; // device counter
+        u32 *host_failures = nullptr; // pinned copy, valid once `done` has completed
+        cudaEvent_t start = nullptr, done = nullptr;
+        bool held = false;
+        uint64_t sample_index = 0, epoch = 0;
+    } slot[2];
+    ~rp_frame_session() {
+        if (scene && scene->device >= 0)
+            cudaSetDevice(scene->device);
+        for (Slot &f : slot) {
+            if (f.done)
+                cudaEventSynchronize(f.done);
+            if (f.xyz)
+                cudaFree(f.xyz);
+            if (f.failures)
+                cudaFree(f.failures);
+            if (f.host_failures)
+                cudaFreeHost(f.host_failures);
+            if (f.start)
+                cudaEventDestroy(f.start);
+            if (f.done)
+                cudaEventDestroy(f.done);
+        }
+    }
+};
+
+namespace {
+
+// The scene camera fields a frame's raygen reads (PBRT raster basis), swapped in for one wave.
+void set_camera(DeviceScene &ds, const rp_camera &c) {
+    ds.origin = v3(c.origin[0], c.origin[1], c.origin[2]);
+    ds.forward = v3(c.corner[0], c.corner[1], c.corner[2]);
+    ds.right = v3(c.dx[0], c.dx[1], c.dx[2]);
+    ds.up = v3(c.dy[0], c.dy[1], c.dy[2]);
+}
+
+rp_frame_info frame_info(const rp_frame_session *fs, u32 k, bool complete) {
+    const rp_frame_session::Slot &f = fs->slot[k];
+    rp_frame_info info{};
+    info.width = fs->config.width;
+    info.height = fs->config.height;
+    info.sample_index = f.sample_index;
+    info.epoch = f.epoch;
+    info.status = RP_FRAME_PENDING;
+    if (complete) {
+        info.failed_pixels = *f.host_failures;
+        info.status = info.failed_pixels ? RP_FRAME_FAILED : RP_FRAME_COMPLETE;
+        info.completed_samples = uint64_t(info.width) * info.height - info.failed_pixels;
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, f.start, f.done) == cudaSuccess)
+            info.gpu_ms = ms;
+    }
+    return info;
+}
+
+} // namespace
+
+extern "C" {
+
+rp_status rp_cuda_frame_session_create(rp_scene *s, const rp_frame_config *config, rp_frame_session **out, char *diag,
+                                       size_t cap) {
+    if (out)
+        *out = nullptr;
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!s || !config || !out)
+            throw Invalid{"null argument"};
+        rp_request q{};
+        q.width = config->width;
+        q.height = config->height;
+        q.seed = config->seed;
+        q.pixel_count = config->width * config->height;
+        q.sample_count = 1;
+        q.sampler_kind = config->sampler_kind;
+        q.randomization = config->randomization;
+        q.total_samples = config->footprint_samples ? config->footprint_samples : 1;
+        const std::string err = validate_request(s, q);
+        if (!err.empty())
+            throw Invalid{err};
+        if (q.pixel_count > (1u << 23))
+            throw Invalid{"frame sessions render at most 2^23 pixels"};
+        if (!s->cie)
+            throw Invalid{"CIE table not set (rp_cuda_set_cie)"};
+        RP_CHECK(cudaSetDevice(s->device));
+        auto fs = std::make_unique<rp_frame_session>();
+        fs->scene = s;
+        fs->config = *config;
+        for (auto &f : fs->slot) {
+            RP_CHECK(cudaMalloc(reinterpret_cast<void **>(&f.xyz), size_t(q.pixel_count) * 3 * sizeof(float)));
+            RP_CHECK(cudaMalloc(reinterpret_cast<void **>(&f.failures), sizeof(u32)));
+            RP_CHECK(cudaMallocHost(reinterpret_cast<void **>(&f.host_failures), sizeof(u32)));
+            RP_CHECK(cudaEventCreate(&f.start));
+            RP_CHECK(cudaEventCreate(&f.done));
+        }
+        *out = fs.release();
+        return RP_SUCCESS;
+    });
+}
+
+void rp_cuda_frame_session_destroy(rp_frame_session *fs) { delete fs; }
+
+rp_status rp_cuda_frame_submit(rp_frame_session *fs, const rp_frame_request *request, uint32_t *frame, int *busy,
+                               char *diag, size_t cap) {
+    if (busy)
+        *busy = 0;
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!fs || !request || !frame)
+            throw Invalid{"null argument"};
+        u32 k = 0;
+        while (k < 2 && fs->slot[k].held)
+            ++k;
+        if (k == 2) {
+            if (busy)
+                *busy = 1;
+            set_diag(diag, cap, "both frame slots are held; release a frame first");
+            return RP_FAILURE;
+        }
+        rp_scene *s = fs->scene;
+        const rp_frame_config &c = fs->config;
+        rp_request q{};
+        q.width = c.width;
+        q.height = c.height;
+        q.seed = c.seed;
+        q.pixel_count = c.width * c.height;
+        q.sample_begin = request->sample_index;
+        q.sample_count = 1;
+        q.emergency_limit = 1024;
+        q.sampler_kind = c.sampler_kind;
+        q.randomization = c.randomization;
+        q.boundary_limit = 4096;
+        q.total_samples = c.footprint_samples ? c.footprint_samples : request->sample_index + 1;
+        const std::string err = validate_request(s, q);
+        if (!err.empty())
+            throw Invalid{err};
+        if (request->camera) {
+            fs->camera = *request->camera;
+            fs->camera_set = true;
+        }
+        RP_CHECK(cudaSetDevice(s->device));
+        rp_frame_session::Slot &f = fs->slot[k];
+        f.held = true;
+        f.sample_index = request->sample_index;
+        f.epoch = request->epoch;
+        const DeviceScene scene_camera = s->ds;
+        try {
+            if (fs->camera_set)
+                set_camera(s->ds, fs->camera);
+            const WaveParams p = wave_params(q);
+            RP_CHECK(cudaEventRecord(f.start, s->stream));
+            RP_CHECK(cudaMemsetAsync(f.failures, 0, sizeof(u32), s->stream));
+            const unsigned grid = grid_for(s->sm_count, p.lanes, 128, 16);
+            if (s->transport == RP_TRANSPORT_SCALAR) {
+                run_scalar_wave(s, p, q.boundary_limit);
+                k_frame_scalar<<<grid, 128, 0, s->stream>>>(s->scalar_records, p.lanes, s->cie, f.xyz, f.failures);
+            } else {
+                run_wave(s, p);
+                k_frame_packet<<<grid, 128, 0, s->stream>>>(s->pool, p.lanes, 0, p.sample_low, p.sample_high, s->cie,
+                                                             f.xyz, f.failures);
+            }
+            RP_CHECK(cudaGetLastError());
+            RP_CHECK(cudaMemcpyAsync(f.host_failures, f.failures, sizeof(u32), cudaMemcpyDeviceToHost, s->stream));
+            RP_CHECK(cudaEventRecord(f.done, s->stream));
+        } catch (...) {
+            s->ds = scene_camera;
+            f.held = false;
+            s->discard_marks();
+            throw;
+        }
+        s->ds = scene_camera;
+        // a frame is asynchronous: its per-kernel timing events are not read back
+        s->discard_marks();
+        *frame = k;
+        return RP_SUCCESS;
+    });
+}
+
+rp_status rp_cuda_frame_poll(rp_frame_session *fs, uint32_t frame, rp_frame_info *info) {
+    if (!fs || !info || frame > 1 || !fs->slot[frame].held)
+        return RP_INVALID_ARGUMENT;
+    const cudaError_t q = cudaEventQuery(fs->slot[frame].done);
+    if (q != cudaSuccess && q != cudaErrorNotReady)
+        return RP_FAILURE;
+    *info = frame_info(fs, frame, q == cudaSuccess);
+    return RP_SUCCESS;
+}
+
+rp_status rp_cuda_frame_wait(rp_frame_session *fs, uint32_t frame, rp_frame_info *info) {
+    if (!fs || !info || frame > 1 || !fs->slot[frame].held)
+        return RP_INVALID_ARGUMENT;
+    if (cudaEventSynchronize(fs->slot[frame].done) != cudaSuccess)
+        return RP_FAILURE;
+    *info = frame_info(fs, frame, true);
+    return RP_SUCCESS;
+}
+
+rp_status rp_cuda_frame_capture(rp_frame_session *fs, uint32_t frame, float *host_xyz, size_t capacity, char *diag,
+                                size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!fs || !host_xyz || frame > 1 || !fs->slot[frame].held)
+            throw Invalid{"no such frame"};
+        const size_t pixels = size_t(fs->config.width) * fs->config.height;
+        if (capacity < pixels)
+            throw Invalid{"capture capacity is smaller than the frame"};
+        RP_CHECK(cudaSetDevice(fs->scene->device));
+        RP_CHECK(cudaEventSynchronize(fs->slot[frame].done));
+        RP_CHECK(cudaMemcpy(host_xyz, fs->slot[frame].xyz, pixels * 3 * sizeof(float), cudaMemcpyDeviceToHost));
+        const u32 failed = *fs->slot[frame].host_failures;
+        if (failed) {
+            set_diag(diag, cap, "frame failed: %u pixel samples failed", failed);
+            return RP_FAILURE;
+        }
+        return RP_SUCCESS;
+    });
+}
+
+rp_status rp_cuda_frame_device_xyz(rp_frame_session *fs, uint32_t frame, const float **device_xyz) {
+    if (!fs || !device_xyz || frame > 1 || !fs->slot[frame].held)
+        return RP_INVALID_ARGUMENT;
+    *device_xyz = fs->slot[frame].xyz;
+    return RP_SUCCESS;
+}
+
+rp_status rp_cuda_frame_release(rp_frame_session *fs, uint32_t frame) {
+    if (!fs || frame > 1 || !fs->slot[frame].held)
+        return RP_INVALID_ARGUMENT;
+    cudaSetDevice(fs->scene->device);
+    const cudaError_t e = cudaEventSynchronize(fs->slot[frame].done);
+    fs->slot[frame].held = false;
+    return e == cudaSuccess ? RP_SUCCESS : RP_FAILURE;
 }
 
 } // extern "C"

@@ -887,4 +887,47 @@ __global__ void k_film(PathPool pool, u32 pixel_count, u32 samples, const double
     }
 }
 
+// The frame sensor of a packet lane (shaders/frame_sensor.h:33-52): raw XYZ of one camera
+// sample, sum over the valid wavelength lanes of the matching functions at the nearest
+// nanometre times radiance / pdf / 4, in binary32 (the filter weight cancels against its own
+// normalisation).  A failed or inconsistent lane (status, identity, a companion terminated
+// beside a surviving one, a non-finite value) writes zero and counts a failure.
+__global__ void k_frame_packet(PathPool pool, u32 pixel_count, u32 pixel_begin, u32 sample_low, u32 sample_high,
+                               const double *cie, float *xyz, u32 *failures) {
+    for (u32 px = blockIdx.x * blockDim.x + threadIdx.x; px < pixel_count; px += gridDim.x * blockDim.x) {
+        const uint4 id = pool.ident[px];
+        bool valid = (id.w & F_COMPLETE) && get_status(id.w) == 0 && id.x == pixel_begin + px && id.y == sample_low &&
+                     id.z == sample_high;
+        const float4 l4 = pool.lambda[px], p4 = pool.lambda_pdf[px], r4 = pool.radiance[px];
+        const float lam[4] = {l4.x, l4.y, l4.z, l4.w}, pdf[4] = {p4.x, p4.y, p4.z, p4.w}, rad[4] = {r4.x, r4.y, r4.z, r4.w};
+        bool secondary = false, terminated = false;
+        float v[3] = {0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const bool good = lam[k] >= 360 && lam[k] <= 830 && isfinite(pdf[k]) && pdf[k] >= 0 && (k != 0 || pdf[k] > 0) &&
+                              isfinite(rad[k]) && rad[k] >= 0;
+            valid = valid && good;
+            if (k > 0) {
+                secondary = secondary || pdf[k] > 0;
+                terminated = terminated || pdf[k] == 0;
+            }
+            if (good && pdf[k] > 0) {
+                const u32 row = u32(floorf(lam[k] + .5f) - 360.f);
+                const float w = rad[k] / pdf[k] / 4.f;
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    v[c] = v[c] + float(__ldg(cie + 3 * row + c)) * w;
+            }
+        }
+        valid = valid && !(secondary && terminated) && isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]);
+        if (!valid) {
+            v[0] = v[1] = v[2] = 0;
+            atomicAdd(failures, 1u);
+        }
+        xyz[3 * size_t(px)] = v[0];
+        xyz[3 * size_t(px) + 1] = v[1];
+        xyz[3 * size_t(px) + 2] = v[2];
+    }
+}
+
 } // namespace rp

@@ -1204,4 +1204,30 @@ __global__ void k_scalar_film(const uint4 *records, u32 pixel_count, u32 samples
     }
 }
 
+// The frame sensor of a scalar lane (shaders/frame_sensor.h:22-31, PBRT model): the matching
+// functions at the nearest nanometre times 470 times radiance, in binary32; a failed lane
+// writes zero and counts a failure.
+__global__ void k_frame_scalar(const uint4 *records, u32 pixel_count, const double *cie, float *xyz, u32 *failures) {
+    for (u32 px = blockIdx.x * blockDim.x + threadIdx.x; px < pixel_count; px += gridDim.x * blockDim.x) {
+        const uint4 r = records[px];
+        const float w = __uint_as_float(r.y), L = __uint_as_float(r.z);
+        bool valid = r.x == 0 && w >= 360 && w <= 830 && isfinite(L) && L >= 0;
+        float v[3] = {0, 0, 0};
+        if (valid) {
+            const u32 row = u32(floorf(w + .5f) - 360.f);
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                v[c] = float(__ldg(cie + 3 * row + c)) * L * 470.f;
+            valid = isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]);
+        }
+        if (!valid) {
+            v[0] = v[1] = v[2] = 0;
+            atomicAdd(failures, 1u);
+        }
+        xyz[3 * size_t(px)] = v[0];
+        xyz[3 * size_t(px) + 1] = v[1];
+        xyz[3 * size_t(px) + 2] = v[2];
+    }
+}
+
 } // namespace rp

@@ -64,6 +64,14 @@ def lib():
         "rp_cuda_adjoint_device": (st, [vp, C.POINTER(abi.AdjointRequest), vp, vp, cp, sz]),
         "rp_cuda_tune_views": (st, [vp, C.POINTER(abi.View), u32, C.POINTER(abi.BatchRequest),
                                     C.POINTER(abi.BatchConfig), cp, sz]),
+        "rp_cuda_frame_session_create": (st, [vp, C.POINTER(abi.FrameConfig), C.POINTER(vp), cp, sz]),
+        "rp_cuda_frame_session_destroy": (None, [vp]),
+        "rp_cuda_frame_submit": (st, [vp, C.POINTER(abi.FrameRequest), C.POINTER(u32), C.POINTER(C.c_int), cp, sz]),
+        "rp_cuda_frame_poll": (st, [vp, u32, C.POINTER(abi.FrameInfo)]),
+        "rp_cuda_frame_wait": (st, [vp, u32, C.POINTER(abi.FrameInfo)]),
+        "rp_cuda_frame_capture": (st, [vp, u32, vp, sz, cp, sz]),
+        "rp_cuda_frame_device_xyz": (st, [vp, u32, C.POINTER(vp)]),
+        "rp_cuda_frame_release": (st, [vp, u32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

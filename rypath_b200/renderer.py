@@ -329,6 +329,85 @@ class CudaRenderScene:
         return words, rays
 
 
+@dataclass
+class FrameConfig:
+    """FrameConfig (src/frame_session.hpp:58-100): film size, sampler and its seed."""
+    width: int
+    height: int
+    seed: int = 1
+    sampler: int = abi.SAMPLER_SOBOL
+    randomization: int = abi.RANDOMIZE_OWEN
+    footprint_samples: int = 0  # the fixed budget ZSobol needs; 0: none
+
+    def to_c(self) -> abi.FrameConfig:
+        return abi.FrameConfig(self.width, self.height, self.seed, self.sampler, self.randomization,
+                               self.footprint_samples)
+
+
+class FrameSession:
+    """FrameSession (src/frame_session.hpp:182-212) over the C ABI: each submitted frame renders
+    one absolute sample of every pixel into raw XYZ on the device, asynchronously; two frame
+    slots, each held by its frame until ``release``."""
+
+    def __init__(self, scene: "CudaRenderScene", config: FrameConfig):
+        scene._ensure_cie()
+        self.scene = scene  # the scene outlives the session
+        self.config = config
+        handle = C.c_void_p()
+        diag = C.create_string_buffer(512)
+        st = native.lib().rp_cuda_frame_session_create(scene.handle, C.byref(config.to_c()), C.byref(handle), diag, 512)
+        native.check(st, diag, "rp_cuda_frame_session_create")
+        self._handle = handle
+
+    def close(self):
+        if getattr(self, "_handle", None) and self._handle.value and native is not None:
+            native.lib().rp_cuda_frame_session_destroy(self._handle)
+            self._handle = C.c_void_p()
+
+    __del__ = close
+
+    def submit(self, sample_index: int, epoch: int = 0, camera=None):
+        """Returns (status, frame slot or None, busy, diagnostic); ``camera`` (origin, corner, dx, dy)
+        replaces the session's camera from this frame on."""
+        cam = None
+        if camera is not None:
+            cam = abi.Camera()
+            o, corner, dx, dy = camera
+            cam.origin[:], cam.corner[:], cam.dx[:], cam.dy[:] = list(o), list(corner), list(dx), list(dy)
+        req = abi.FrameRequest(sample_index, epoch, C.pointer(cam) if cam is not None else None)
+        frame, busy = C.c_uint32(), C.c_int()
+        diag = C.create_string_buffer(512)
+        st = native.lib().rp_cuda_frame_submit(self._handle, C.byref(req), C.byref(frame), C.byref(busy), diag, 512)
+        return st, (frame.value if st == abi.RP_SUCCESS else None), bool(busy.value), diag.value.decode()
+
+    def poll(self, frame: int) -> abi.FrameInfo:
+        info = abi.FrameInfo()
+        native.check(native.lib().rp_cuda_frame_poll(self._handle, frame, C.byref(info)), None, "rp_cuda_frame_poll")
+        return info
+
+    def wait(self, frame: int) -> abi.FrameInfo:
+        info = abi.FrameInfo()
+        native.check(native.lib().rp_cuda_frame_wait(self._handle, frame, C.byref(info)), None, "rp_cuda_frame_wait")
+        return info
+
+    def capture(self, frame: int):
+        """(status, diagnostic, raw XYZ as float32 (height, width, 3))."""
+        xyz = np.zeros((self.config.height, self.config.width, 3), np.float32)
+        diag = C.create_string_buffer(512)
+        st = native.lib().rp_cuda_frame_capture(self._handle, frame, xyz.ctypes.data, xyz.shape[0] * xyz.shape[1],
+                                                diag, 512)
+        return st, diag.value.decode(), xyz
+
+    def device_xyz(self, frame: int) -> int:
+        ptr = C.c_void_p()
+        native.check(native.lib().rp_cuda_frame_device_xyz(self._handle, frame, C.byref(ptr)), None,
+                     "rp_cuda_frame_device_xyz")
+        return ptr.value
+
+    def release(self, frame: int):
+        native.check(native.lib().rp_cuda_frame_release(self._handle, frame), None, "rp_cuda_frame_release")
+
+
 def build_renderer(scene: scenes.Scene, device: int = 0) -> RenderBuildResult:
     """build_metal_renderer (src/metal_render.hpp:84-95) for the CUDA backend."""
     L = native.lib()

@@ -39,6 +39,9 @@ REFERENCE_SYMBOLS = [
     "rypath::build_frame_session(rypath::RenderScene const&, rypath::FrameConfig const&, "
     "std::filesystem::__cxx11::path const&)",
     "rypath::FrameSession::submit(rypath::FrameRequest const&)",
+    "rypath::Frame::poll() const",
+    "rypath::Frame::wait() const",
+    "rypath::Frame::capture() const",
     "rypath::cuda_backend::FilmRenderer::build(rypath::RenderScene const&, std::__cxx11::basic_string<char, "
     "std::char_traits<char>, std::allocator<char> >&)",
 ]
@@ -80,7 +83,8 @@ def test_adapter_calls_only_exported_entry_points():
     assert "[librypath_cuda.so]" in needed
     calls = {s for s in symbols(lib, "--undefined-only") if s.startswith("rp_cuda_")}
     exported = {s for s in symbols(LIB, "--defined-only") if s.startswith("rp_cuda_")}
-    assert {"rp_cuda_scene_create", "rp_cuda_sample", "rp_cuda_sample_scalar", "rp_cuda_render_film"} <= calls
+    assert {"rp_cuda_scene_create", "rp_cuda_sample", "rp_cuda_sample_scalar", "rp_cuda_render_film",
+            "rp_cuda_frame_session_create", "rp_cuda_frame_submit", "rp_cuda_frame_capture"} <= calls
     assert calls <= exported, calls - exported
 
 
