@@ -140,39 +140,50 @@ def l2_copy_gbs(torch):
     return 2 * src.numel() * 200 / (start.elapsed_time(stop) / 1e3) / 1e9
 
 
+BAND = 8  # rows per contiguous block of the CPU sample
+
+
 def strided_rows(w, h, lanes, max_spp):
-    """A bounded sample of the whole film, independent of how it is timed: every stride-th row
-    (rows stride // 2, stride // 2 + stride, ...), the stride the smallest that keeps the rows'
-    pixels within `lanes`, at as many absolute samples (0, 1, ...) as then fit, at most max_spp."""
-    stride = max(1, -(-w * h // max(1, lanes)))
-    rows = list(range(stride // 2, h, stride))
-    spp = max(1, min(max_spp, lanes // max(1, len(rows) * w)))
-    return rows, spp
+    """A bounded sample of the whole film, independent of how it is timed: blocks of BAND
+    consecutive rows spread evenly over the film (one block every `stride` rows, the smallest
+    multiple of BAND that keeps the blocks' pixels within `lanes`), at as many absolute samples
+    (0, 1, ...) as then fit, at most max_spp.  Returns the blocks' first rows and row counts,
+    and the samples."""
+    fit = max(1, lanes // (BAND * w))   # blocks within the budget
+    total = -(-h // BAND)                # blocks of the whole film
+    stride = BAND * -(-total // fit)
+    blocks = [(r, min(BAND, h - r)) for r in range(((stride - BAND) // 2) // BAND * BAND, h, stride)]
+    pixels = sum(n for _, n in blocks) * w
+    spp = max(1, min(max_spp, lanes // max(1, pixels)))
+    return blocks, spp
 
 
 def cpu_baseline(orc, args, seconds, threads=0):
-    """The oracle (the reference's CPU path restated) on a bounded sample of the workload: whole
-    rows spread over the film (strided_rows), sized from a short probe to about `seconds`."""
+    """The oracle (the reference's CPU path restated) on a bounded sample of the workload: blocks
+    of whole rows spread over the film (strided_rows), sized from a short probe to about
+    `seconds`; one oracle call per block, so every host thread has work."""
     from tests.oracle_lib import request
 
     w, h = args.width, args.height
 
-    def render(rows, spp):
+    def render(blocks, spp):
         t0 = time.perf_counter()
-        outs = [orc.sample(request(w, h, spp, pixel_begin=r * w, pixel_count=w), threads=threads) for r in rows]
+        outs = [orc.sample(request(w, h, spp, pixel_begin=r * w, pixel_count=n * w), threads=threads)
+                for r, n in blocks]
         return np.concatenate(outs), time.perf_counter() - t0
 
-    probe_rows, _ = strided_rows(w, h, 8 * w, 1)
-    out, dt = render(probe_rows, 1)
+    probe, _ = strided_rows(w, h, 4 * BAND * w, 1)
+    out, dt = render(probe, 1)
     rate = out.size / max(dt, 1e-6)
-    rows, spp = strided_rows(w, h, int(max(8 * w, rate * seconds)), args.spp)
-    out, dt = render(rows, spp)
+    blocks, spp = strided_rows(w, h, int(max(BAND * w, rate * seconds)), args.spp)
+    out, dt = render(blocks, spp)
     ok = int((out["status"] == 0).sum())
     cores = threads if threads > 0 else (os.cpu_count() or 1)
-    stride = rows[1] - rows[0] if len(rows) > 1 else h
+    stride = blocks[1][0] - blocks[0][0] if len(blocks) > 1 else h
     return {"value": out.size / dt / 1e6, "unit": UNIT, "cores": cores, "kind": "port", "seconds": dt,
-            "sample": f"{out.size} lanes: {len(rows)} whole rows of the {w}x{h} film (every {stride}th row from row "
-                      f"{rows[0]}), absolute samples 0..{spp - 1}, depth {args.depth}; {dt:.2f} s, {ok} succeeded"}
+            "sample": f"{out.size} lanes: {len(blocks)} blocks of {BAND} whole rows of the {w}x{h} film, one every "
+                      f"{stride} rows from row {blocks[0][0]}, absolute samples 0..{spp - 1}, depth {args.depth}; "
+                      f"{dt:.2f} s, {ok} succeeded"}
 
 
 def run_reference(args, rank):

@@ -248,8 +248,8 @@ typedef struct rp_timing {
     uint64_t shadow_nodes_visited, shadow_triangles_tested; /* any-hit rays; only when counting */
     double build_ms, build_host_ms, build_bvh_ms; /* scene creation: total, host preparation, LBVH */
     /* hero shade kernels by BSDF family (0 diffuse, 1 conductor, 2 dielectric, 3 escape), each
-     * kernel's own launch time summed over the call; only when counting (the families run side
-     * by side, so these add up to more than shade_ms) */
+     * kernel's own launch time summed over the call; only when counting, whose family kernels
+     * run one after another (otherwise they run side by side) */
     double shade_family_ms[4];
 } rp_timing;
 

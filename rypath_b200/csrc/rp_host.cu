@@ -587,6 +587,8 @@ struct rp_scene {
     u32 capacity = 0;
     u32 *lane_closest = nullptr, *lane_shadow = nullptr; // per-lane walk counts (pool.lane_* while counting)
     unsigned char *static_base = nullptr; // device address of the allocation-free scratch, once looked up
+    cudaStream_t copy = nullptr;          // film readback beside the render (host films)
+    cudaEvent_t copied = nullptr;
     unsigned long long *stats = nullptr;
     double *cie = nullptr;
     rp_film_pixel *film_stage = nullptr;
@@ -641,6 +643,10 @@ struct rp_scene {
             if (family[k])
                 cudaStreamDestroy(family[k]);
         }
+        if (copied)
+            cudaEventDestroy(copied);
+        if (copy)
+            cudaStreamDestroy(copy);
         if (forked)
             cudaEventDestroy(forked);
         if (joined)
@@ -906,8 +912,12 @@ void launch_shade(rp_scene *s, const WaveParams &p, const PathPool &pool, int in
     RP_CHECK(cudaEventRecord(s->forked, s->stream));
     for (int k = 0; k < 3; ++k)
         RP_CHECK(cudaStreamWaitEvent(s->family[k], s->forked, 0));
+    // counting runs time each family kernel alone: the four run one after another on the scene
+    // stream, so each one's events bracket its own work (side by side they share the SMs)
     const bool timed = s->counting;
     cudaStream_t on[4] = {s->stream, s->family[0], s->family[1], s->family[2]};
+    if (timed)
+        on[1] = on[2] = on[3] = s->stream;
     if (timed)
         s->mark_family(0, on[0]);
     k_shade<0, 128, Adjoint><<<grid, 128, smem, on[0]>>>(s->ds, p, pool, in);
@@ -2052,60 +2062,88 @@ static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel 
             RP_CHECK(cudaMemsetAsync(s->stats, 0, 8 * sizeof(unsigned long long), s->stream));
         u64 done = 0;
         u32 failed_batches = 0;
+        bool read_back = false; // the host film already holds every committed row
         while (done < r->sample_count) {
             const u64 batch = std::min<u64>(r->batch_size, r->sample_count - done);
             RP_CHECK(cudaMemcpyAsync(staged, committed, size_t(pixels) * sizeof(rp_film_pixel), cudaMemcpyDeviceToDevice,
                                      s->stream));
-            u64 in_batch = 0;
+            // A batch whose samples of every pixel exceed one wave runs as waves over pixel ranges
+            // that hold all of the batch's samples: each pixel is still reduced once per batch in
+            // absolute-sample order, and a range's rows are final for the batch when its wave
+            // ends, so the last batch of a host render copies them back (on the copy stream)
+            // while the next range renders.  Larger batches split over samples instead.
+            const bool by_pixels = batch * pixels > max_lanes && batch <= max_lanes;
+            const bool overlap = host && by_pixels && done + batch == r->sample_count;
+            if (overlap && !s->copy) {
+                RP_CHECK(cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking));
+                RP_CHECK(cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming));
+            }
+            const u32 range = by_pixels ? u32(max_lanes / batch) : pixels;
             u32 failures = 0;
-            while (in_batch < batch) {
-                const u64 spw = std::min<u64>(samples_per_wave, batch - in_batch);
-                rp_request q{};
-                q.width = r->width;
-                q.height = r->height;
-                q.seed = r->seed;
-                q.pixel_begin = 0;
-                q.pixel_count = pixels;
-                q.sample_begin = r->sample_begin + done + in_batch;
-                q.sample_count = u32(spw);
-                q.emergency_limit = r->emergency_limit;
-                q.sampler_kind = r->sampler_kind;
-                q.randomization = r->randomization;
-                q.total_samples = r->total_samples ? r->total_samples : r->sample_begin + r->sample_count;
-                const std::string err = validate_request(s, q);
-                if (!err.empty())
-                    throw Invalid{err};
-                const WaveParams p = wave_params(q);
-                u32 f = 0;
-                if (s->transport == RP_TRANSPORT_SCALAR) {
-                    run_scalar_wave(s, p, 4096u);
-                    s->mark(3);
-                    k_scalar_film<<<grid_for(s->sm_count, pixels, 128, 16), 128, 0, s->stream>>>(
-                        s->scalar_records, pixels, u32(spw), s->cie, reinterpret_cast<FilmPixel *>(staged),
-                        s->scalar_counters + 1);
-                    s->done();
-                    RP_CHECK(cudaMemcpyAsync(&f, s->scalar_counters + 1, 4, cudaMemcpyDeviceToHost, s->stream));
-                } else {
-                    run_wave(s, p);
-                    s->mark(3);
-                    k_film<<<grid_for(s->sm_count, pixels, 128, 16), 128, 0, s->stream>>>(
-                        s->pool, pixels, u32(spw), s->cie, double(s->ds.filter_weight), clamp,
-                        reinterpret_cast<FilmPixel *>(staged));
-                    s->done();
-                    RP_CHECK(cudaMemcpyAsync(&f, s->pool.counters + 3, 4, cudaMemcpyDeviceToHost, s->stream));
+            for (u32 pixel_begin = 0; pixel_begin < pixels && !failures; pixel_begin += range) {
+                const u32 pixel_count = std::min(range, pixels - pixel_begin);
+                u64 in_batch = 0;
+                while (in_batch < batch) {
+                    const u64 spw = by_pixels ? batch : std::min<u64>(samples_per_wave, batch - in_batch);
+                    rp_request q{};
+                    q.width = r->width;
+                    q.height = r->height;
+                    q.seed = r->seed;
+                    q.pixel_begin = pixel_begin;
+                    q.pixel_count = pixel_count;
+                    q.sample_begin = r->sample_begin + done + in_batch;
+                    q.sample_count = u32(spw);
+                    q.emergency_limit = r->emergency_limit;
+                    q.sampler_kind = r->sampler_kind;
+                    q.randomization = r->randomization;
+                    q.total_samples = r->total_samples ? r->total_samples : r->sample_begin + r->sample_count;
+                    const std::string err = validate_request(s, q);
+                    if (!err.empty())
+                        throw Invalid{err};
+                    const WaveParams p = wave_params(q);
+                    FilmPixel *rows = reinterpret_cast<FilmPixel *>(staged + pixel_begin);
+                    u32 f = 0;
+                    if (s->transport == RP_TRANSPORT_SCALAR) {
+                        run_scalar_wave(s, p, 4096u);
+                        s->mark(3);
+                        k_scalar_film<<<grid_for(s->sm_count, pixel_count, 128, 16), 128, 0, s->stream>>>(
+                            s->scalar_records, pixel_count, u32(spw), s->cie, rows, s->scalar_counters + 1);
+                        s->done();
+                        RP_CHECK(cudaMemcpyAsync(&f, s->scalar_counters + 1, 4, cudaMemcpyDeviceToHost, s->stream));
+                    } else {
+                        run_wave(s, p);
+                        s->mark(3);
+                        k_film<<<grid_for(s->sm_count, pixel_count, 128, 16), 128, 0, s->stream>>>(
+                            s->pool, pixel_count, u32(spw), s->cie, double(s->ds.filter_weight), clamp, rows);
+                        s->done();
+                        RP_CHECK(cudaMemcpyAsync(&f, s->pool.counters + 3, 4, cudaMemcpyDeviceToHost, s->stream));
+                    }
+                    if (overlap) {
+                        RP_CHECK(cudaEventRecord(s->copied, s->stream));
+                        RP_CHECK(cudaStreamWaitEvent(s->copy, s->copied, 0));
+                        RP_CHECK(cudaMemcpyAsync(film + pixel_begin, staged + pixel_begin,
+                                                 size_t(pixel_count) * sizeof(rp_film_pixel), cudaMemcpyDeviceToHost,
+                                                 s->copy));
+                    }
+                    RP_CHECK(cudaStreamSynchronize(s->stream));
+                    failures += f;
+                    in_batch += spw;
                 }
-                RP_CHECK(cudaStreamSynchronize(s->stream));
-                failures += f;
-                in_batch += spw;
+            }
+            if (overlap) {
+                // the scene stream continues after the copies (also before a restoring copy)
+                RP_CHECK(cudaEventRecord(s->copied, s->copy));
+                RP_CHECK(cudaStreamWaitEvent(s->stream, s->copied, 0));
             }
             if (failures) {
                 ++failed_batches;
                 break; // keep the previously committed film (src/render_driver.cpp:201-214)
             }
+            read_back = overlap;
             std::swap(staged, committed);
             done += batch;
         }
-        if (host)
+        if (host && !read_back)
             RP_CHECK(cudaMemcpyAsync(film, committed, size_t(pixels) * sizeof(rp_film_pixel), cudaMemcpyDeviceToHost,
                                      s->stream));
         else if (committed != film)

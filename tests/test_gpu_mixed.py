@@ -10,8 +10,9 @@ compared with the oracle lane by lane:
 * radiance within RTOL for at least MATCH_FRACTION of lanes (a lane that takes another
   discrete branch after a last-bit difference in a transcendental is another sample);
 * the lane's closest-hit and any-hit walk counts (reported by counting runs in the packet
-  result's reserved words, by the device and by the oracle) equal on every lane whose
-  radiance matches, and their totals within 1%.
+  result's reserved words, by the device and by the oracle) equal for at least MATCH_FRACTION
+  of all lanes and for at least 99.5% of the lanes whose radiance matches, and their totals
+  within 1%.
 
 Each of the scene's light and material features also runs on its own in a Cornell variant
 (point light, spot light, constant environment, dispersive dielectric), so that a mistake in
@@ -57,8 +58,12 @@ def compare_lanes(g, c, min_shadow_fraction=0.0):
     assert close.mean() >= MATCH_FRACTION, close.mean()
     gw, cw = g["reserved"].astype(np.int64), c["reserved"].astype(np.int64)
     same_walks = np.all(gw == cw, axis=1)
-    # a lane with the same radiance took the same branches: the same walks
-    assert same_walks[close].mean() >= 0.999, same_walks[close].mean()
+    assert same_walks.mean() >= MATCH_FRACTION, same_walks.mean()
+    # a lane with the same radiance took the same branches, but for the rare lane whose later
+    # bounces contribute nothing, which can take another branch (a roulette draw, a
+    # dispersive companion's refraction) after a last-bit difference without changing its
+    # radiance (observed: 0.2% of the matching lanes of the Cauchy-glass box, none elsewhere)
+    assert same_walks[close].mean() >= 0.995, same_walks[close].mean()
     for k in range(2):
         assert abs(gw[:, k].sum() - cw[:, k].sum()) <= 0.01 * max(cw[:, k].sum(), 1), (k, gw[:, k].sum(), cw[:, k].sum())
     assert (cw[:, 1] > 0).mean() >= min_shadow_fraction, (cw[:, 1] > 0).mean()
