@@ -495,7 +495,7 @@ rp_status rp_cuda_trace_rays(struct rp_scene *scene, const float *rays, uint32_t
  * Every GPU that loads this library holds this much device memory until the process exits. */
 #define RP_STATIC_SCRATCH_BYTES (64u << 20)
 /* Largest request, in lanes (pixel_count * sample_count), that fits that scratch. */
-#define RP_STATIC_MAX_LANES 178464u
+#define RP_STATIC_MAX_LANES 118976u
 
 /* No counterpart in rypath.  Same work and results as rp_cuda_sample_device, for callers that
  * must not allocate device memory during a render call -- for example a host that hands the

@@ -510,7 +510,7 @@ int grid_for(int sm_count, u32 work, int block, int per_sm) {
 // counting and without the adjoint may run on it.
 constexpr size_t pool_bytes(u32 lanes, bool full) {
     const size_t v16 = (size_t(lanes) * 16 + 255) & ~size_t(255), v4 = (size_t(lanes) * 4 + 255) & ~size_t(255);
-    return 22 * v16 + 6 * v4 + 256 + (full ? v16 + 3 * v4 : 0);
+    return 33 * v16 + 9 * v4 + 256 + (full ? v16 + 3 * v4 : 0);
 }
 size_t carve_pool(unsigned char *base, u32 lanes, bool full, PathPool *out) {
     const size_t v16 = (size_t(lanes) * 16 + 255) & ~size_t(255), v4 = (size_t(lanes) * 4 + 255) & ~size_t(255);
@@ -530,9 +530,15 @@ size_t carve_pool(unsigned char *base, u32 lanes, bool full, PathPool *out) {
         *p = reinterpret_cast<float4 *>(take(v16));
     q.dens_e = reinterpret_cast<int4 *>(take(v16));
     q.prev_e = reinterpret_cast<int4 *>(take(v16));
+    float4 **nee[] = {&q.nee_p, &q.nee_n, &q.nee_g, &q.nee_e, &q.nee_wo, &q.nee_prev, &q.nee_beta, &q.nee_df,
+                      &q.nee_param, &q.nee_k};
+    for (auto p : nee)
+        *p = reinterpret_cast<float4 *>(take(v16));
+    q.nee_de = reinterpret_cast<int4 *>(take(v16));
     q.queue[0] = reinterpret_cast<u32 *>(take(v4));
     q.queue[1] = reinterpret_cast<u32 *>(take(v4));
     q.bins = reinterpret_cast<u32 *>(take(4 * v4));
+    q.nee_queue = reinterpret_cast<u32 *>(take(3 * v4));
     q.counters = reinterpret_cast<u32 *>(take(256));
     if (full) {
         q.sh_t = reinterpret_cast<float4 *>(take(v16));
@@ -549,7 +555,7 @@ size_t carve_pool(unsigned char *base, u32 lanes, bool full, PathPool *out) {
 }
 // Every PathPool member is a pointer carved above, set elsewhere (stats, the adjoint's), or
 // a count: a new member changes this size and so comes past this check.
-static_assert(sizeof(PathPool) == 38 * sizeof(void *) + 16, "PathPool changed: review carve_pool");
+static_assert(sizeof(PathPool) == 50 * sizeof(void *) + 16, "PathPool changed: review carve_pool");
 
 } // namespace
 
@@ -587,8 +593,6 @@ struct rp_scene {
     u32 capacity = 0;
     u32 *lane_closest = nullptr, *lane_shadow = nullptr; // per-lane walk counts (pool.lane_* while counting)
     unsigned char *static_base = nullptr; // device address of the allocation-free scratch, once looked up
-    cudaStream_t copy = nullptr;          // film readback beside the render (host films)
-    cudaEvent_t copied = nullptr;
     unsigned long long *stats = nullptr;
     double *cie = nullptr;
     rp_film_pixel *film_stage = nullptr;
@@ -643,10 +647,6 @@ struct rp_scene {
             if (family[k])
                 cudaStreamDestroy(family[k]);
         }
-        if (copied)
-            cudaEventDestroy(copied);
-        if (copy)
-            cudaStreamDestroy(copy);
         if (forked)
             cudaEventDestroy(forked);
         if (joined)
@@ -921,16 +921,19 @@ void launch_shade(rp_scene *s, const WaveParams &p, const PathPool &pool, int in
     if (timed)
         s->mark_family(0, on[0]);
     k_shade<0, 128, Adjoint><<<grid, 128, smem, on[0]>>>(s->ds, p, pool, in);
+    k_nee<0><<<grid, 128, 0, on[0]>>>(s->ds, p, pool);
     if (timed) {
         s->done_family(on[0]);
         s->mark_family(1, on[1]);
     }
     k_shade<1, 128, Adjoint><<<grid, 128, smem, on[1]>>>(s->ds, p, pool, in);
+    k_nee<1><<<grid, 128, 0, on[1]>>>(s->ds, p, pool);
     if (timed) {
         s->done_family(on[1]);
         s->mark_family(2, on[2]);
     }
     k_shade<2, 128, Adjoint><<<grid, 128, smem, on[2]>>>(s->ds, p, pool, in);
+    k_nee<2><<<grid, 128, 0, on[2]>>>(s->ds, p, pool);
     if (timed) {
         s->done_family(on[2]);
         s->mark_family(3, on[3]);
@@ -1015,9 +1018,10 @@ void run_wave(rp_scene *s, const WaveParams &request_params, size_t adjoint_smem
             RP_CHECK(cudaStreamWaitEvent(s->stream, s->joined, 0));
             shadow_pending = false;
         }
-        s->mark(2, 4);
+        s->mark(2, 7);
         RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), s->stream));
         RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), s->stream));
+        RP_CHECK(cudaMemsetAsync(pool.counters + 8, 0, 3 * sizeof(u32), s->stream));
         const size_t smem = adjoint_smem;
         const unsigned shade_grid = grid_for(sms, p.lanes, 128, 16);
         if (pool.hist)
@@ -2062,88 +2066,64 @@ static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel 
             RP_CHECK(cudaMemsetAsync(s->stats, 0, 8 * sizeof(unsigned long long), s->stream));
         u64 done = 0;
         u32 failed_batches = 0;
-        bool read_back = false; // the host film already holds every committed row
         while (done < r->sample_count) {
             const u64 batch = std::min<u64>(r->batch_size, r->sample_count - done);
             RP_CHECK(cudaMemcpyAsync(staged, committed, size_t(pixels) * sizeof(rp_film_pixel), cudaMemcpyDeviceToDevice,
                                      s->stream));
-            // A batch whose samples of every pixel exceed one wave runs as waves over pixel ranges
-            // that hold all of the batch's samples: each pixel is still reduced once per batch in
-            // absolute-sample order, and a range's rows are final for the batch when its wave
-            // ends, so the last batch of a host render copies them back (on the copy stream)
-            // while the next range renders.  Larger batches split over samples instead.
-            const bool by_pixels = batch * pixels > max_lanes && batch <= max_lanes;
-            const bool overlap = host && by_pixels && done + batch == r->sample_count;
-            if (overlap && !s->copy) {
-                RP_CHECK(cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking));
-                RP_CHECK(cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming));
-            }
-            const u32 range = by_pixels ? u32(max_lanes / batch) : pixels;
+            // waves of whole sample indices over every pixel: each wave holds every BSDF family
+            // of the image, so the family shade kernels, which run side by side, stay balanced
+            // (waves over pixel bands, whose rows would be final early enough to read back beside
+            // the render, measured slower: the bands' family mixes are uneven)
             u32 failures = 0;
-            for (u32 pixel_begin = 0; pixel_begin < pixels && !failures; pixel_begin += range) {
-                const u32 pixel_count = std::min(range, pixels - pixel_begin);
-                u64 in_batch = 0;
-                while (in_batch < batch) {
-                    const u64 spw = by_pixels ? batch : std::min<u64>(samples_per_wave, batch - in_batch);
-                    rp_request q{};
-                    q.width = r->width;
-                    q.height = r->height;
-                    q.seed = r->seed;
-                    q.pixel_begin = pixel_begin;
-                    q.pixel_count = pixel_count;
-                    q.sample_begin = r->sample_begin + done + in_batch;
-                    q.sample_count = u32(spw);
-                    q.emergency_limit = r->emergency_limit;
-                    q.sampler_kind = r->sampler_kind;
-                    q.randomization = r->randomization;
-                    q.total_samples = r->total_samples ? r->total_samples : r->sample_begin + r->sample_count;
-                    const std::string err = validate_request(s, q);
-                    if (!err.empty())
-                        throw Invalid{err};
-                    const WaveParams p = wave_params(q);
-                    FilmPixel *rows = reinterpret_cast<FilmPixel *>(staged + pixel_begin);
-                    u32 f = 0;
-                    if (s->transport == RP_TRANSPORT_SCALAR) {
-                        run_scalar_wave(s, p, 4096u);
-                        s->mark(3);
-                        k_scalar_film<<<grid_for(s->sm_count, pixel_count, 128, 16), 128, 0, s->stream>>>(
-                            s->scalar_records, pixel_count, u32(spw), s->cie, rows, s->scalar_counters + 1);
-                        s->done();
-                        RP_CHECK(cudaMemcpyAsync(&f, s->scalar_counters + 1, 4, cudaMemcpyDeviceToHost, s->stream));
-                    } else {
-                        run_wave(s, p);
-                        s->mark(3);
-                        k_film<<<grid_for(s->sm_count, pixel_count, 128, 16), 128, 0, s->stream>>>(
-                            s->pool, pixel_count, u32(spw), s->cie, double(s->ds.filter_weight), clamp, rows);
-                        s->done();
-                        RP_CHECK(cudaMemcpyAsync(&f, s->pool.counters + 3, 4, cudaMemcpyDeviceToHost, s->stream));
-                    }
-                    if (overlap) {
-                        RP_CHECK(cudaEventRecord(s->copied, s->stream));
-                        RP_CHECK(cudaStreamWaitEvent(s->copy, s->copied, 0));
-                        RP_CHECK(cudaMemcpyAsync(film + pixel_begin, staged + pixel_begin,
-                                                 size_t(pixel_count) * sizeof(rp_film_pixel), cudaMemcpyDeviceToHost,
-                                                 s->copy));
-                    }
-                    RP_CHECK(cudaStreamSynchronize(s->stream));
-                    failures += f;
-                    in_batch += spw;
+            u64 in_batch = 0;
+            while (in_batch < batch) {
+                const u64 spw = std::min<u64>(samples_per_wave, batch - in_batch);
+                rp_request q{};
+                q.width = r->width;
+                q.height = r->height;
+                q.seed = r->seed;
+                q.pixel_begin = 0;
+                q.pixel_count = pixels;
+                q.sample_begin = r->sample_begin + done + in_batch;
+                q.sample_count = u32(spw);
+                q.emergency_limit = r->emergency_limit;
+                q.sampler_kind = r->sampler_kind;
+                q.randomization = r->randomization;
+                q.total_samples = r->total_samples ? r->total_samples : r->sample_begin + r->sample_count;
+                const std::string err = validate_request(s, q);
+                if (!err.empty())
+                    throw Invalid{err};
+                const WaveParams p = wave_params(q);
+                u32 f = 0;
+                if (s->transport == RP_TRANSPORT_SCALAR) {
+                    run_scalar_wave(s, p, 4096u);
+                    s->mark(3);
+                    k_scalar_film<<<grid_for(s->sm_count, pixels, 128, 16), 128, 0, s->stream>>>(
+                        s->scalar_records, pixels, u32(spw), s->cie, reinterpret_cast<FilmPixel *>(staged),
+                        s->scalar_counters + 1);
+                    s->done();
+                    RP_CHECK(cudaMemcpyAsync(&f, s->scalar_counters + 1, 4, cudaMemcpyDeviceToHost, s->stream));
+                } else {
+                    run_wave(s, p);
+                    s->mark(3);
+                    k_film<<<grid_for(s->sm_count, pixels, 128, 16), 128, 0, s->stream>>>(
+                        s->pool, pixels, u32(spw), s->cie, double(s->ds.filter_weight), clamp,
+                        reinterpret_cast<FilmPixel *>(staged));
+                    s->done();
+                    RP_CHECK(cudaMemcpyAsync(&f, s->pool.counters + 3, 4, cudaMemcpyDeviceToHost, s->stream));
                 }
-            }
-            if (overlap) {
-                // the scene stream continues after the copies (also before a restoring copy)
-                RP_CHECK(cudaEventRecord(s->copied, s->copy));
-                RP_CHECK(cudaStreamWaitEvent(s->stream, s->copied, 0));
+                RP_CHECK(cudaStreamSynchronize(s->stream));
+                failures += f;
+                in_batch += spw;
             }
             if (failures) {
                 ++failed_batches;
                 break; // keep the previously committed film (src/render_driver.cpp:201-214)
             }
-            read_back = overlap;
             std::swap(staged, committed);
             done += batch;
         }
-        if (host && !read_back)
+        if (host)
             RP_CHECK(cudaMemcpyAsync(film, committed, size_t(pixels) * sizeof(rp_film_pixel), cudaMemcpyDeviceToHost,
                                      s->stream));
         else if (committed != film)
@@ -2439,12 +2419,16 @@ void batch_wave_kernels(rp_scene *s, const WaveParams &p, const Batch &b, u32 wa
         }
         RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), st));
         RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), st));
+        RP_CHECK(cudaMemsetAsync(pool.counters + 8, 0, 3 * sizeof(u32), st));
         RP_CHECK(cudaEventRecord(s->forked, st));
         for (int k = 0; k < 3; ++k)
             RP_CHECK(cudaStreamWaitEvent(s->family[k], s->forked, 0));
         k_shade<0, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool, in);
+        k_nee<0, SB><<<shade_grid, SB, 0, st>>>(s->ds, p, pool);
         k_shade<1, SB><<<shade_grid, SB, 0, s->family[0]>>>(s->ds, p, pool, in);
+        k_nee<1, SB><<<shade_grid, SB, 0, s->family[0]>>>(s->ds, p, pool);
         k_shade<2, SB><<<shade_grid, SB, 0, s->family[1]>>>(s->ds, p, pool, in);
+        k_nee<2, SB><<<shade_grid, SB, 0, s->family[1]>>>(s->ds, p, pool);
         k_shade<3, SB><<<shade_grid, SB, 0, s->family[2]>>>(s->ds, p, pool, in);
         for (int k = 0; k < 3; ++k) {
             RP_CHECK(cudaEventRecord(s->family_done[k], s->family[k]));
@@ -3223,10 +3207,15 @@ rp_status rp_cuda_sample_device_static(rp_scene *s, const rp_request *request, r
             launch_trace<false, kTraceBlock>(s, pool, in, grid_for(sms, p.lanes, kTraceBlock, 12), st, p.boundary_limit);
             RP_CHECK(cudaMemsetAsync(pool.counters + (in ^ 1), 0, sizeof(u32), st));
             RP_CHECK(cudaMemsetAsync(pool.counters + 2, 0, sizeof(u32), st));
-            k_shade<0><<<grid_for(sms, p.lanes, 128, 16), 128, 0, st>>>(s->ds, p, pool, in);
-            k_shade<1><<<grid_for(sms, p.lanes, 128, 16), 128, 0, st>>>(s->ds, p, pool, in);
-            k_shade<2><<<grid_for(sms, p.lanes, 128, 16), 128, 0, st>>>(s->ds, p, pool, in);
-            k_shade<3><<<grid_for(sms, p.lanes, 128, 16), 128, 0, st>>>(s->ds, p, pool, in);
+            RP_CHECK(cudaMemsetAsync(pool.counters + 8, 0, 3 * sizeof(u32), st));
+            const unsigned shade_grid = grid_for(sms, p.lanes, 128, 16);
+            k_shade<0><<<shade_grid, 128, 0, st>>>(s->ds, p, pool, in);
+            k_nee<0><<<shade_grid, 128, 0, st>>>(s->ds, p, pool);
+            k_shade<1><<<shade_grid, 128, 0, st>>>(s->ds, p, pool, in);
+            k_nee<1><<<shade_grid, 128, 0, st>>>(s->ds, p, pool);
+            k_shade<2><<<shade_grid, 128, 0, st>>>(s->ds, p, pool, in);
+            k_nee<2><<<shade_grid, 128, 0, st>>>(s->ds, p, pool);
+            k_shade<3><<<shade_grid, 128, 0, st>>>(s->ds, p, pool, in);
             launch_shadow<false, kTraceBlock, false>(s, pool, grid_for(sms, p.lanes, kTraceBlock, 12), 0, st, p.boundary_limit);
             in ^= 1;
         }

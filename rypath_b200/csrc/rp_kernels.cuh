@@ -213,8 +213,7 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_const
     const u32 trips = (count + stride - 1) / stride;
     for (u32 trip = 0; trip < trips; ++trip) {
         const u32 i = trip * stride + blockIdx.x * blockDim.x + threadIdx.x;
-        bool keep = false, shadow = false;
-        float4 sh_o = make_float4(0, 0, 0, 0), sh_d = sh_o, sh_c = sh_o, sh_t = sh_o;
+        bool keep = false, nee = false;
         u32 path = 0;
         if (i < count) {
             path = queue[i];
@@ -464,9 +463,116 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_const
                             }
                         }
                     }
-                    // hero_direct (shaders/hero_pt_helpers.h:185-221): sample, evaluate, weight;
-                    // visibility is resolved by the shadow kernel.
-                    if (F != 3 && status == 0 && cnt < capacity && direct_allowed && ctype == kSurface && connectible) {
+                    // hero_direct (shaders/hero_pt_helpers.h:185-221) runs in the light-sample kernel
+                    // (k_nee), from the request this event leaves (write_nee_request); its failures fail the
+                    // path there.
+                    nee = F != 3 && status == 0 && cnt < capacity && direct_allowed && ctype == kSurface && connectible;
+                    if (!finite_nonnegative4(radiance))
+                        status = 2;
+                    if (status != 0) {
+                        complete = true;
+                        nee = false;
+                    }
+                    if (nee) {
+                        Density dd = direct_density;
+                        write_nee_request(pool, path, cnt, cp, cbsdf, cwo, latest.position, direct_beta, dd);
+                    }
+                }
+                // A complete path is read again only for its identity, status and radiance (the
+                // shadow walk, the film and the packet results), so the rest of its state is not
+                // written back.
+                if (cnt != old_count) {
+                    // preceding = latest; latest = current (shaders/packet_pt_event_body.inc:453-460)
+                    flags = (flags & ~(3u << F_PTYPE_SHIFT)) | (latest.type << F_PTYPE_SHIFT);
+                    if (!complete) {
+                        pool.preceding[path] = make_float4(latest.position.x, latest.position.y, latest.position.z, 0);
+                        pool.latest_p[path] =
+                            make_float4(cp.position.x, cp.position.y, cp.position.z, cbsdf.g.alpha_x);
+                        pool.latest_n[path] =
+                            make_float4(cp.shading_normal.x, cp.shading_normal.y, cp.shading_normal.z, cbsdf.g.alpha_y);
+                        pool.latest_param[path] =
+                            make_float4(cbsdf.param[0], cbsdf.param[1], cbsdf.param[2], cbsdf.param[3]);
+                        pool.latest_k[path] = make_float4(cbsdf.k[0], cbsdf.k[1], cbsdf.k[2], cbsdf.k[3]);
+                    }
+                    flags &= ~((3u << F_LTYPE_SHIFT) | F_LDELTA | (3u << F_LKIND_SHIFT) | (15u << F_LMASK_SHIFT) | F_LSMOOTH);
+                    flags |= (ctype << F_LTYPE_SHIFT) | (cdelta ? F_LDELTA : 0u) | ((cbsdf.kind & 3u) << F_LKIND_SHIFT) |
+                             ((cbsdf.active_mask & 15u) << F_LMASK_SHIFT) | (cbsdf.g.smooth ? F_LSMOOTH : 0u);
+                }
+                flags = (flags & ~(F_MASK | F_ROULETTE)) | active_mask | (roulette ? F_ROULETTE : 0u);
+                flags = set_status(flags, status) | (complete ? F_COMPLETE : 0u);
+                ident.w = flags;
+                pool.ident[path] = ident;
+                pool.radiance[path] = to_float4(radiance);
+                if (!complete) {
+                    cursor.z = cnt;
+                    pool.cursor[path] = cursor;
+                    pool.beta[path] = to_float4(beta);
+                    float4 f;
+                    int4 e;
+                    store_density(density, f, e);
+                    pool.dens_f[path] = f;
+                    pool.dens_e[path] = e;
+                    store_density(hero_previous, f, e);
+                    pool.prev_f[path] = f;
+                    pool.prev_e[path] = e;
+                    pool.eta_scale[path] = to_float4(eta_scale);
+                    pool.ray_o[path] = make_float4(ro.x, ro.y, ro.z, 0);
+                    pool.ray_d[path] = make_float4(rd.x, rd.y, rd.z, 0);
+                }
+                keep = !complete;
+            }
+        }
+        const u32 slot = warp_append(out_count, keep);
+        if (keep)
+            out_queue[slot] = path;
+        if (F != 3) {
+            const u32 nslot = warp_append(pool.counters + 8 + F, nee);
+            if (nee)
+                pool.nee_queue[size_t(F) * pool.bin_capacity + nslot] = path;
+        }
+    }
+    if (Adjoint)
+        adjoint_end(pool, sgrad);
+}
+
+// The light sample of one hero event (hero_direct, shaders/hero_pt_helpers.h:185-221) for the
+// paths of BSDF family F whose event asked for one: light selection, the light's point and
+// radiance, the BSDF on the light direction, the balance weight, and the visibility segment
+// queued for the shadow kernel.  Its own failures (invalid arithmetic) fail the path.  Split
+// from the shade kernel, which leaves the request (write_nee_request), so that each kernel
+// holds half the live state.
+template <int F, int Block = 128>
+__global__ void __launch_bounds__(Block, 512 / Block) k_nee(const __grid_constant__ DeviceScene s,
+                                                            const __grid_constant__ WaveParams p, PathPool pool) {
+    const u32 count = pool.counters[8 + F];
+    const u32 *queue = pool.nee_queue + size_t(F) * pool.bin_capacity;
+    const u32 stride = gridDim.x * blockDim.x;
+    const u32 trips = (count + stride - 1) / stride;
+    for (u32 trip = 0; trip < trips; ++trip) {
+        const u32 i = trip * stride + blockIdx.x * blockDim.x + threadIdx.x;
+        bool shadow = false;
+        float4 sh_o = make_float4(0, 0, 0, 0), sh_d = sh_o, sh_c = sh_o, sh_t = sh_o;
+        if (i < count) {
+            const u32 path = queue[i];
+            uint4 ident = pool.ident[path];
+            const uint4 cursor = pool.cursor[path];
+            const u64 index = (u64(cursor.y) << 32) | cursor.x;
+            const V4 lambda = from_float4(pool.lambda[path]);
+            u32 cnt;
+            SurfacePoint cp;
+            HeroBsdf cbsdf;
+            V3 cwo, previous;
+            V4 direct_beta;
+            Density direct_density;
+            read_nee_request(pool, path, cnt, cp, cbsdf, cwo, previous, direct_beta, direct_density);
+            Latest latest;
+            latest.position = previous;
+            Frame cframe;
+            shading_frame(cp.shading_normal, cframe); // succeeded in the shade kernel
+            const bool pair_valid = false;
+            const V3 swo = v3(0, 0, 0);
+            u32 status = 0;
+            {
                         const uint4 w = draw_words(s, p, ident.x, ident.y, ident.z, index, 133 + cnt - 2);
                         const float u0 = sample_uniform(p, w.x), u1 = sample_uniform(p, w.y), u2 = sample_uniform(p, w.z);
                         // sample_li (shaders/packet_transport.h:470-553)
@@ -569,61 +675,13 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_const
                                 }
                             }
                         }
-                    }
-                    if (!finite_nonnegative4(radiance))
-                        status = 2;
-                    if (status != 0) {
-                        complete = true;
-                        shadow = false;
-                    }
-                }
-                // A complete path is read again only for its identity, status and radiance (the
-                // shadow walk, the film and the packet results), so the rest of its state is not
-                // written back.
-                if (cnt != old_count) {
-                    // preceding = latest; latest = current (shaders/packet_pt_event_body.inc:453-460)
-                    flags = (flags & ~(3u << F_PTYPE_SHIFT)) | (latest.type << F_PTYPE_SHIFT);
-                    if (!complete) {
-                        pool.preceding[path] = make_float4(latest.position.x, latest.position.y, latest.position.z, 0);
-                        pool.latest_p[path] =
-                            make_float4(cp.position.x, cp.position.y, cp.position.z, cbsdf.g.alpha_x);
-                        pool.latest_n[path] =
-                            make_float4(cp.shading_normal.x, cp.shading_normal.y, cp.shading_normal.z, cbsdf.g.alpha_y);
-                        pool.latest_param[path] =
-                            make_float4(cbsdf.param[0], cbsdf.param[1], cbsdf.param[2], cbsdf.param[3]);
-                        pool.latest_k[path] = make_float4(cbsdf.k[0], cbsdf.k[1], cbsdf.k[2], cbsdf.k[3]);
-                    }
-                    flags &= ~((3u << F_LTYPE_SHIFT) | F_LDELTA | (3u << F_LKIND_SHIFT) | (15u << F_LMASK_SHIFT) | F_LSMOOTH);
-                    flags |= (ctype << F_LTYPE_SHIFT) | (cdelta ? F_LDELTA : 0u) | ((cbsdf.kind & 3u) << F_LKIND_SHIFT) |
-                             ((cbsdf.active_mask & 15u) << F_LMASK_SHIFT) | (cbsdf.g.smooth ? F_LSMOOTH : 0u);
-                }
-                flags = (flags & ~(F_MASK | F_ROULETTE)) | active_mask | (roulette ? F_ROULETTE : 0u);
-                flags = set_status(flags, status) | (complete ? F_COMPLETE : 0u);
-                ident.w = flags;
+            }
+            if (status != 0) {
+                ident.w = set_status(ident.w, status) | F_COMPLETE;
                 pool.ident[path] = ident;
-                pool.radiance[path] = to_float4(radiance);
-                if (!complete) {
-                    cursor.z = cnt;
-                    pool.cursor[path] = cursor;
-                    pool.beta[path] = to_float4(beta);
-                    float4 f;
-                    int4 e;
-                    store_density(density, f, e);
-                    pool.dens_f[path] = f;
-                    pool.dens_e[path] = e;
-                    store_density(hero_previous, f, e);
-                    pool.prev_f[path] = f;
-                    pool.prev_e[path] = e;
-                    pool.eta_scale[path] = to_float4(eta_scale);
-                    pool.ray_o[path] = make_float4(ro.x, ro.y, ro.z, 0);
-                    pool.ray_d[path] = make_float4(rd.x, rd.y, rd.z, 0);
-                }
-                keep = !complete;
+                shadow = false;
             }
         }
-        const u32 slot = warp_append(out_count, keep);
-        if (keep)
-            out_queue[slot] = path;
         const u32 sslot = warp_append(pool.counters + 2, shadow);
         if (shadow) {
             pool.sh_o[sslot] = sh_o;
@@ -633,8 +691,6 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_const
                 pool.sh_t[sslot] = sh_t;
         }
     }
-    if (Adjoint)
-        adjoint_end(pool, sgrad);
 }
 
 // visible() through pass-through surfaces (shaders/packet_transport.h:393-445): nearest hits

@@ -53,6 +53,13 @@ struct PathPool {
     u32 *material; // material a mix-root hit resolved to (written by the closest-hit kernel)
     // statistics (optional)
     unsigned long long *stats; // closest [0] nodes, [1] triangles, [2] rays; shadow [3] rays, [4] nodes, [5] triangles
+    // light-sample requests, one per path (written by the shade kernel, read by k_nee): the
+    // vertex (position + vertex count, shading normal + BSDF bits, geometric normal + alpha_x,
+    // error + alpha_y), the outgoing direction, the previous vertex, the throughput and hero
+    // density before this event's continuation, and the BSDF's per-wavelength parameters
+    float4 *nee_p, *nee_n, *nee_g, *nee_e, *nee_wo, *nee_prev, *nee_beta, *nee_df, *nee_param, *nee_k;
+    int4 *nee_de;
+    u32 *nee_queue; // three family queues of bin_capacity path ids; counts in counters[8..10]
     // per-lane walk counts of counting runs (pool slot = request lane), or nullptr: closest-hit
     // walks (written by the closest-hit kernel) and any-hit walks (by the shadow kernel, which
     // runs beside the next closest-hit walk, hence two arrays)
@@ -446,6 +453,54 @@ RP_DEV Density load_density(float4 f, int4 e) {
 RP_DEV void store_density(const Density &d, float4 &f, int4 &e) {
     f = make_float4(d.lane[0].fraction, d.lane[1].fraction, d.lane[2].fraction, d.lane[3].fraction);
     e = make_int4(d.lane[0].exponent, d.lane[1].exponent, d.lane[2].exponent, d.lane[3].exponent);
+}
+
+// The light-sample request of a path's event (PathPool::nee_*).
+RP_DEV void write_nee_request(const PathPool &pool, u32 path, u32 cnt, const SurfacePoint &cp, const HeroBsdf &b,
+                              V3 wo, V3 previous, V4 beta, const Density &density) {
+    const u32 bits = (b.kind & 3u) | ((b.active_mask & 15u) << 2) | (b.g.smooth ? 64u : 0u);
+    pool.nee_p[path] = make_float4(cp.position.x, cp.position.y, cp.position.z, __uint_as_float(cnt));
+    pool.nee_n[path] = make_float4(cp.shading_normal.x, cp.shading_normal.y, cp.shading_normal.z, __uint_as_float(bits));
+    pool.nee_g[path] = make_float4(cp.geometric_normal.x, cp.geometric_normal.y, cp.geometric_normal.z, b.g.alpha_x);
+    pool.nee_e[path] = make_float4(cp.error.x, cp.error.y, cp.error.z, b.g.alpha_y);
+    pool.nee_wo[path] = make_float4(wo.x, wo.y, wo.z, 0);
+    pool.nee_prev[path] = make_float4(previous.x, previous.y, previous.z, 0);
+    pool.nee_beta[path] = to_float4(beta);
+    float4 f;
+    int4 e;
+    store_density(density, f, e);
+    pool.nee_df[path] = f;
+    pool.nee_de[path] = e;
+    pool.nee_param[path] = make_float4(b.param[0], b.param[1], b.param[2], b.param[3]);
+    pool.nee_k[path] = make_float4(b.k[0], b.k[1], b.k[2], b.k[3]);
+}
+RP_DEV void read_nee_request(const PathPool &pool, u32 path, u32 &cnt, SurfacePoint &cp, HeroBsdf &b, V3 &wo,
+                             V3 &previous, V4 &beta, Density &density) {
+    const float4 pp = pool.nee_p[path], n = pool.nee_n[path], g = pool.nee_g[path], e = pool.nee_e[path];
+    const float4 w = pool.nee_wo[path], v = pool.nee_prev[path], pa = pool.nee_param[path], k = pool.nee_k[path];
+    cnt = __float_as_uint(pp.w);
+    const u32 bits = __float_as_uint(n.w);
+    cp.position = v3(pp.x, pp.y, pp.z);
+    cp.shading_normal = v3(n.x, n.y, n.z);
+    cp.geometric_normal = v3(g.x, g.y, g.z);
+    cp.error = v3(e.x, e.y, e.z);
+    cp.inverse_area_pdf = 0;
+    cp.world_extent = 0;
+    b.kind = bits & 3u;
+    b.active_mask = (bits >> 2) & 15u;
+    b.g = {g.w, e.w, (bits & 64u) != 0};
+    b.param[0] = pa.x;
+    b.param[1] = pa.y;
+    b.param[2] = pa.z;
+    b.param[3] = pa.w;
+    b.k[0] = k.x;
+    b.k[1] = k.y;
+    b.k[2] = k.z;
+    b.k[3] = k.w;
+    wo = v3(w.x, w.y, w.z);
+    previous = v3(v.x, v.y, v.z);
+    beta = from_float4(pool.nee_beta[path]);
+    density = load_density(pool.nee_df[path], pool.nee_de[path]);
 }
 
 // shaders/packet_transport.h:77-83

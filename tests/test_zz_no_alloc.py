@@ -27,7 +27,7 @@ from rypath_b200 import abi, native, renderer, scenes
 
 pytestmark = pytest.mark.gpu
 
-RP_STATIC_MAX_LANES = 178464  # include/rypath_cuda.h
+RP_STATIC_MAX_LANES = 118976  # include/rypath_cuda.h
 REQUESTS = [renderer.RenderRequest(32, 32, sample_begin=0, sample_count=4),
             renderer.RenderRequest(32, 32, pixel_begin=100, pixel_count=600, sample_begin=9, sample_count=3,
                                    sampler=abi.SAMPLER_INDEPENDENT)]
