@@ -573,10 +573,19 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_nee(const __grid_constan
             const V3 swo = v3(0, 0, 0);
             u32 status = 0;
             {
-                        const uint4 w = draw_words(s, p, ident.x, ident.y, ident.z, index, 133 + cnt - 2);
-                        const float u0 = sample_uniform(p, w.x), u1 = sample_uniform(p, w.y), u2 = sample_uniform(p, w.z);
+                        // the light-sample draw: its first word selects the light; the next two, a
+                        // point on an area light, are drawn only when an area light was selected
+                        // (the same words either way)
+                        const u32 block = 133 + cnt - 2;
+                        const float u0 = sample_uniform(p, draw_word0(s, p, ident.x, ident.y, ident.z, index, block));
                         // sample_li (shaders/packet_transport.h:470-553)
                         const Selected choice = light_sample(s, cp.position, cp.shading_normal, u0);
+                        float u1 = 0, u2 = 0;
+                        if (choice.pmf > 0 && choice.light < s.emitter_count) {
+                            const uint4 w = draw_words(s, p, ident.x, ident.y, ident.z, index, block);
+                            u1 = sample_uniform(p, w.y);
+                            u2 = sample_uniform(p, w.z);
+                        }
                         V4 lbeta = v4(0);
                         float spdf = 0;
                         bool li_ok = true, delta_light = false;

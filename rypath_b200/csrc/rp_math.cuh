@@ -230,6 +230,22 @@ RP_DEV uint4 sobol_words4(const SobolTables &t, u64 index, u32 dimension, u32 mo
     }
     return make_uint4(v[0], v[1], v[2], v[3]);
 }
+// sobol_word of one dimension; with Owen randomisation and that dimension's table of
+// owen_prefix_rounds (`prefix`, optional), the table replaces the first kOwenPrefixBits rounds.
+RP_DEV u32 sobol_word_prefixed(const SobolTables &t, u64 index, u32 dimension, u32 mode, u32 seed,
+                               const unsigned short *prefix) {
+    if (mode != 3 || !prefix)
+        return sobol_word(t, index, dimension, mode, seed);
+    constexpr u32 low = 32 - kOwenPrefixBits;
+    u32 v = sobol_raw(t, index, dimension);
+    const u32 h = sobol_dimension_hash(dimension, seed);
+    v = (v & ((u32(1) << low) - 1)) | (u32(__ldg(prefix + (v >> low))) << low);
+#pragma unroll 1
+    for (u32 bit = kOwenPrefixBits; bit < 32; ++bit)
+        if (u32(mix_bits((v & (~u32(0) << (32 - bit))) ^ h)) & (u32(1) << bit))
+            v ^= u32(1) << (31 - bit);
+    return v;
+}
 // src/sobol_shared.h:143-154
 RP_DEV float sobol_uniform(u32 v) {
     const float unit = float(v) * 0x1p-32f;

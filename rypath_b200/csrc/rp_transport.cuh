@@ -130,6 +130,14 @@ __device__ __noinline__ uint4 draw_words(const DeviceScene &s, const WaveParams 
     return sobol_words4(s.sobol, index, 4 * block, p.randomization, p.seed_low, owen_prefix_table(p, block));
 }
 
+// The first word of draw_words (the block's first dimension) alone.
+__device__ __noinline__ u32 draw_word0(const DeviceScene &s, const WaveParams &p, u32 pixel, u32 slo, u32 shi,
+                                       u64 index, u32 block) {
+    if (p.sampler == 1)
+        return sobol_word_prefixed(s.sobol, index, 4 * block, p.randomization, p.seed_low, owen_prefix_table(p, block));
+    return draw_words(s, p, pixel, slo, shi, index, block).x;
+}
+
 struct BeginSample {
     u32 pixel, sample_low, sample_high;
     u64 index;
