@@ -2510,41 +2510,47 @@ float run_batch(rp_scene *s, const BatchPlan &plan, const BatchBuffers &buf, con
     const FilmClamp clamp = film_clamp(r.exposure, r.max_component_value);
     const Batch b = buf.batch(plan);
     RP_CHECK(cudaMemsetAsync(buf.cursor, 0, 8, s->stream));
-    cudaEvent_t start, stop;
-    RP_CHECK(cudaEventCreate(&start));
-    RP_CHECK(cudaEventCreate(&stop));
-    cudaGraphExec_t exec = nullptr;
-    cudaGraph_t graph = nullptr;
+    // the events, the captured graph and its executable are released on every exit, error
+    // paths included (a failed launch or timing call throws)
+    struct Owned {
+        cudaEvent_t start = nullptr, stop = nullptr;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        ~Owned() {
+            if (exec)
+                cudaGraphExecDestroy(exec);
+            if (graph)
+                cudaGraphDestroy(graph);
+            if (start)
+                cudaEventDestroy(start);
+            if (stop)
+                cudaEventDestroy(stop);
+        }
+    } o;
+    RP_CHECK(cudaEventCreate(&o.start));
+    RP_CHECK(cudaEventCreate(&o.stop));
     if (c.use_graph != 2) {
         RP_CHECK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
         try {
             batch_wave(s, p, b, c, clamp, film);
         } catch (...) {
-            cudaStreamEndCapture(s->stream, &graph);
-            if (graph)
-                cudaGraphDestroy(graph);
+            cudaStreamEndCapture(s->stream, &o.graph);
             throw;
         }
-        RP_CHECK(cudaStreamEndCapture(s->stream, &graph));
-        RP_CHECK(cudaGraphInstantiate(&exec, graph, 0));
+        RP_CHECK(cudaStreamEndCapture(s->stream, &o.graph));
+        RP_CHECK(cudaGraphInstantiate(&o.exec, o.graph, 0));
     }
-    RP_CHECK(cudaEventRecord(start, s->stream));
+    RP_CHECK(cudaEventRecord(o.start, s->stream));
     for (size_t w = 0; w < waves; ++w) {
-        if (exec)
-            RP_CHECK(cudaGraphLaunch(exec, s->stream));
+        if (o.exec)
+            RP_CHECK(cudaGraphLaunch(o.exec, s->stream));
         else
             batch_wave(s, p, b, c, clamp, film);
     }
-    RP_CHECK(cudaEventRecord(stop, s->stream));
+    RP_CHECK(cudaEventRecord(o.stop, s->stream));
     RP_CHECK(cudaStreamSynchronize(s->stream));
     float ms = 0;
-    RP_CHECK(cudaEventElapsedTime(&ms, start, stop));
-    cudaEventDestroy(start);
-    cudaEventDestroy(stop);
-    if (exec)
-        cudaGraphExecDestroy(exec);
-    if (graph)
-        cudaGraphDestroy(graph);
+    RP_CHECK(cudaEventElapsedTime(&ms, o.start, o.stop));
     return ms;
 }
 
