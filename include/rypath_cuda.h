@@ -463,6 +463,15 @@ rp_status rp_cuda_probe_raygen(struct rp_scene *scene, const rp_request *request
  * weight, sample pdf, flags, eta, pad, pad}. */
 rp_status rp_cuda_probe_bsdf(const float *queries, uint32_t count, float *results, char *diag,
                              size_t diag_capacity);
+/* Hero BSDF probe (shaders/hero_current_bsdf.h:121-203, hero_frozen_bsdf.h:167-250,
+ * hero_scattering.h:100-138): per query 32 floats {kind, active mask, remap, unused, per
+ * wavelength {eta or reflectance, k, roughness u, roughness v}, wo[3], wi[3], uc, ux, uy,
+ * unused[3]} -> 32 floats {sampled wi[3], numerator[4], pdf[4], eta[4], flags (delta 1 |
+ * transmission 2 | accepted 4 | valid 8), evaluated f[4], pdf[4], valid, wavelength 0's Dirac
+ * mass, pdf, eta, Dirac ok, connectible, prepared, unused}.  The wavelengths share wavelength
+ * 0's roughness. */
+rp_status rp_cuda_probe_hero(const float *queries, uint32_t count, float *results, char *diag,
+                             size_t diag_capacity);
 /* Export the scene's binary LBVH over its n triangles: per internal node {left, right,
  * parent} (n-1 nodes; a child with bit 31 set is leaf slot child & 0x7fffffff, the root's
  * parent is RP_NONE), the leaf order (triangle id of each leaf slot), the sorted 63-bit

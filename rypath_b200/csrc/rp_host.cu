@@ -2771,6 +2771,26 @@ rp_status rp_cuda_probe_bsdf(const float *queries, uint32_t count, float *result
     });
 }
 
+rp_status rp_cuda_probe_hero(const float *queries, uint32_t count, float *results, char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        std::vector<void *> own;
+        struct Free {
+            std::vector<void *> &o;
+            ~Free() {
+                for (void *p : o)
+                    cudaFreeAsync(p, nullptr);
+                cudaStreamSynchronize(nullptr);
+            }
+        } fr{own};
+        const float *q = dupload(own, queries, size_t(32) * count, nullptr);
+        float *r = dalloc<float>(own, size_t(32) * count);
+        k_probe_hero<<<(count + 127) / 128, 128>>>(q, count, r);
+        RP_CHECK(cudaGetLastError());
+        RP_CHECK(cudaMemcpy(results, r, size_t(32) * count * 4, cudaMemcpyDeviceToHost));
+        return RP_SUCCESS;
+    });
+}
+
 rp_status rp_cuda_probe_raygen(rp_scene *s, const rp_request *request, uint32_t *words, float *rays, size_t capacity,
                                char *diag, size_t cap) {
     return guarded(diag, cap, [&]() -> rp_status {

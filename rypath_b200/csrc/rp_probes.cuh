@@ -96,6 +96,72 @@ __global__ void k_probe_bsdf(const float *q, u32 count, float *r) {
     o[8] = float((sm.delta ? 1 : 0) | (sm.accepted ? 2 : 0) | (sm.valid ? 4 : 0));
     o[9] = eta;
 }
+// Hero BSDF probe (shaders/hero_current_bsdf.h:121-203, hero_frozen_bsdf.h:167-250,
+// hero_scattering.h:100-138): per query 32 floats {kind, active mask, remap, unused, per
+// wavelength {eta or reflectance, k, roughness u, roughness v}, wo[3], wi[3], uc, ux, uy,
+// unused[3]} -> 32 floats {sampled wi[3], numerator[4], pdf[4], eta[4], flags (delta 1 |
+// transmission 2 | accepted 4 | valid 8), evaluated f[4], evaluated pdf[4], evaluation valid,
+// wavelength 0's Dirac mass, pdf and eta, Dirac ok, connectible, prepared, unused}.  A hero
+// BSDF shares one roughness over its wavelengths, so wavelength 0's roughness is the one used;
+// every wavelength's parameters are checked as the family's prepare checks them.
+__global__ void k_probe_hero(const float *queries, u32 count, float *results) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count)
+        return;
+    const float *a = queries + 32 * i;
+    float *o = results + 32 * i;
+    for (int j = 0; j < 32; ++j)
+        o[j] = 0;
+    HeroBsdf p;
+    p.kind = u32(a[0]);
+    p.active_mask = u32(a[1]);
+    p.g = {0, 0, true};
+    bool ok = p.kind <= 2;
+    for (int k = 0; k < 4; ++k) {
+        const float *l = a + 4 + 4 * k;
+        p.param[k] = p.kind == 2 && l[0] == 0 ? 1.f : l[0];
+        p.k[k] = p.kind == 1 ? l[1] : 0.f;
+        if (p.kind == 0)
+            continue;
+        const bool rough_ok = isfinite(l[2]) && isfinite(l[3]) && l[2] >= 0 && l[3] >= 0;
+        if (p.kind == 1)
+            ok = ok && rough_ok && isfinite(l[0]) && isfinite(l[1]) && l[0] >= 0 && l[1] >= 0 &&
+                 !(l[0] == 0 && l[1] == 0);
+        else
+            ok = ok && rough_ok && isfinite(l[0]) && l[0] >= 0;
+    }
+    if (ok && p.kind != 0)
+        prepare_roughness(a[6], a[7], a[2] != 0, false, p.g);
+    o[30] = ok ? 1.f : 0.f;
+    if (!ok)
+        return;
+    const V3 wo = v3(a[20], a[21], a[22]), wi = v3(a[23], a[24], a[25]);
+    const HeroSample sm = p.kind == 0   ? hero_sample_k<0>(p, wo, a[26], a[27], a[28])
+                          : p.kind == 1 ? hero_sample_k<1>(p, wo, a[26], a[27], a[28])
+                                        : hero_sample_k<2>(p, wo, a[26], a[27], a[28]);
+    o[0] = sm.wi.x;
+    o[1] = sm.wi.y;
+    o[2] = sm.wi.z;
+    for (int k = 0; k < 4; ++k) {
+        o[3 + k] = sm.numerator.v[k];
+        o[7 + k] = sm.pdf.v[k];
+        o[11 + k] = sm.eta.v[k];
+    }
+    o[15] = float((sm.delta ? 1 : 0) | (sm.transmission ? 2 : 0) | (sm.accepted ? 4 : 0) | (sm.valid ? 8 : 0));
+    const HeroEval e = hero_evaluate(p, wo, wi);
+    for (int k = 0; k < 4; ++k) {
+        o[16 + k] = e.f.v[k];
+        o[20 + k] = e.pdf.v[k];
+    }
+    o[24] = e.valid ? 1.f : 0.f;
+    float mass, density, eta;
+    const bool dirac = dirac_lane(p, 0, wo, wi, a[27], a[28], mass, density, eta);
+    o[25] = mass;
+    o[26] = density;
+    o[27] = eta;
+    o[28] = dirac ? 1.f : 0.f;
+    o[29] = hero_connectible(p) ? 1.f : 0.f;
+}
 __global__ void k_probe_raygen(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p, u32 *words,
                                float *rays) {
     const u32 lane = blockIdx.x * blockDim.x + threadIdx.x;

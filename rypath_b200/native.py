@@ -52,6 +52,7 @@ def lib():
         "rp_cuda_probe_wavelengths": (st, [vp, u32, u32, vp, cp, sz]),
         "rp_cuda_probe_raygen": (st, [vp, C.POINTER(abi.Request), vp, vp, sz, cp, sz]),
         "rp_cuda_probe_bsdf": (st, [vp, u32, vp, cp, sz]),
+        "rp_cuda_probe_hero": (st, [vp, u32, vp, cp, sz]),
         "rp_cuda_scene_export_bvh": (st, [vp, vp, vp, vp, vp, sz, cp, sz]),
         "rp_cuda_scene_export_wide": (st, [vp, vp, sz, vp, sz, C.POINTER(u32), cp, sz]),
         "rp_cuda_trace_rays": (st, [vp, vp, u32, C.c_int, vp, cp, sz]),

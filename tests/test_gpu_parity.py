@@ -100,6 +100,38 @@ def test_bsdf_probe_matches_oracle():
     assert close.mean() >= 0.999
 
 
+def test_hero_probe_matches_oracle():
+    """The device hero BSDF (hero_sample_k, hero_evaluate, dirac_lane, hero_connectible) against
+    the oracle's restatement, which is pinned to shaders/hero_scattering.h compiled for the host,
+    on diffuse, conductor and dielectric packets with dispersive, smooth and rough wavelengths."""
+    from tests.test_oracle_pins import hero_queries
+
+    q = hero_queries(30000, np.random.default_rng(23))
+    # a hero BSDF shares one roughness over its wavelengths
+    for k in range(1, 4):
+        q[:, 6 + 4 * k:8 + 4 * k] = q[:, 6:8]
+    gpu = np.zeros((q.shape[0], 32), np.float32)
+    cpu = np.zeros((q.shape[0], 32), np.float32)
+    native.check(native.lib().rp_cuda_probe_hero(q.ctypes.data, q.shape[0], gpu.ctypes.data, None, 0))
+    oracle().or_probe_hero(q.ctypes.data, q.shape[0], cpu.ctypes.data)
+    g32, c32 = gpu.view(np.uint32), cpu.view(np.uint32)
+    # preparation and connectibility, evaluation and the Dirac masses on the given direction use
+    # only IEEE arithmetic: bit exact
+    np.testing.assert_array_equal(g32[:, 29:31], c32[:, 29:31])
+    np.testing.assert_array_equal(g32[:, 16:25], c32[:, 16:25])
+    np.testing.assert_array_equal(g32[:, 25:29], c32[:, 25:29])
+    # sampling uses sin/cos: identical flags for >= 99.9% of queries, and with equal flags the
+    # direction, numerators, densities and etas within 1e-4 relative for >= 99.9%
+    same_flags = gpu[:, 15] == cpu[:, 15]
+    assert same_flags.mean() >= 0.999, same_flags.mean()
+    close = np.all(np.isclose(gpu[:, 0:15], cpu[:, 0:15], rtol=1e-4, atol=1e-6), axis=1) & same_flags
+    assert close.mean() >= 0.999, close.mean()
+    # Dirac samples (no trigonometry on their path) agree bit for bit
+    dirac = same_flags & ((cpu[:, 15].astype(np.int64) & 1) == 1)
+    assert dirac.mean() > 0.05
+    assert (g32[dirac, 3:15] == c32[dirac, 3:15]).all(axis=1).mean() >= 0.999
+
+
 def test_raygen_words_bit_exact(cornell):
     scene, gpu_scene, orc = cornell
     for sampler in (abi.SAMPLER_SOBOL, abi.SAMPLER_INDEPENDENT):
