@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define RP_ABI_VERSION 1u
+#define RP_ABI_VERSION 2u
 #define RP_NONE 0xffffffffu
 #define RP_SPECTRUM_BINS 471u /* 360..830 nm at 1 nm, src/render.hpp:29-36 */
 #define RP_SOBOL_TABLE_BYTES 234208u /* sizeof(sobol::Tables), src/sobol_shared.h:42 */
@@ -71,8 +71,23 @@ enum { RP_INTERFACE = 10 };
  * shaders/scalar_transport.h:566-587); nesting is acyclic, at most 64 levels, and reaches no
  * null interface (src/render.cpp:1955-1995). */
 enum { RP_MIX = 9 };
-/* Reflectance sources (src/render_wire.h:41-48). */
-enum { RP_REFLECTANCE_KNOTS = 0, RP_REFLECTANCE_CONSTANT = 1, RP_REFLECTANCE_BLACKBODY = 4 };
+/* Reflectance sources (src/render_wire.h:41-48).  RP_REFLECTANCE_IMAGE (wire::image_material)
+ * reads images->textures[image_texture] at the hit's texture coordinates and reconstructs a
+ * bounded spectrum from the filtered linear RGB (shaders/packet_walk.h:22-57). */
+enum {
+    RP_REFLECTANCE_KNOTS = 0,
+    RP_REFLECTANCE_CONSTANT = 1,
+    RP_REFLECTANCE_IMAGE = 3,
+    RP_REFLECTANCE_BLACKBODY = 4
+};
+/* Image wrap, filter and texel storage (ImageWrap / ImageFilter, src/image_texture.hpp:14-15;
+ * texel formats src/render_wire.h:35-40). */
+enum { RP_WRAP_REPEAT = 0, RP_WRAP_CLAMP = 1, RP_WRAP_BLACK = 2 };
+enum { RP_TEXTURE_BILINEAR = 0, RP_TEXTURE_TRILINEAR = 1, RP_TEXTURE_POINT = 2, RP_TEXTURE_EWA = 3 };
+enum { RP_TEXELS_SRGB8 = 0, RP_TEXELS_LINEAR8 = 1, RP_TEXELS_HALF = 2, RP_TEXELS_FLOAT = 3 };
+/* Floats of rypath's sRGB reconstruction table (srgb_reconstruction_table,
+ * src/rgb_spectrum.hpp:31): 64 z nodes, then 3 x 64^3 cells of 3 quadratic coefficients. */
+#define RP_RGB_TABLE_FLOATS (64u + 3u * 64u * 64u * 64u * 3u)
 /* Positional light kinds (src/render_wire.h:200). */
 enum { RP_POINT_LIGHT = 0, RP_SPOT_LIGHT = 1 };
 /* Light selection (LightSamplerKind, src/render.hpp:217; wire word src/render_wire.h:304). */
@@ -110,7 +125,58 @@ typedef struct rp_material {
     uint32_t remap_roughness;
     uint32_t first_material, second_material; /* RP_MIX children (MaterialAuxiliary, src/render_wire.h:159) */
     float mix_amount;                         /* RP_MIX constant amount (src/render_wire.h:160) */
+    uint32_t image_texture; /* RP_REFLECTANCE_IMAGE: index into images->textures */
 } rp_material;
+
+/* wire::ImageTexture (src/render_wire.h:68-87), field for field.  level_begin/level_count
+ * select a mip chain in images->levels (level 0 the finest); the glTF fields are carried
+ * for layout only (glTF images are refused). */
+typedef struct rp_image_texture {
+    uint32_t level_begin, level_count;
+    uint32_t wrap;          /* RP_WRAP_* */
+    uint32_t texel_format;  /* RP_TEXELS_* */
+    float uscale, vscale, udelta, vdelta;
+    float scale;            /* RGB multiplier after the lookup */
+    uint32_t invert;        /* nonzero: 1 - rgb after scaling */
+    uint32_t filter;        /* RP_TEXTURE_* */
+    float max_anisotropy;   /* EWA cap, 1..16 */
+    uint32_t transfer_offset; /* 8-bit formats: first of 256 floats in images->transfer */
+    uint32_t channels;      /* 1, 3 or 4 */
+    uint32_t gltf, wrap_t, min_filter, mag_filter;
+} rp_image_texture;
+
+/* wire::TextureLevel (src/render_wire.h:63-67): a level of width x height texels starting
+ * at texel word `offset` (4 words a texel for float storage, 2 for half, 1 for 8-bit). */
+typedef struct rp_texture_level {
+    uint32_t width, height, offset;
+} rp_texture_level;
+
+/* The image inputs of a RenderScene (image_textures, texture_camera, instance_texture_frames,
+ * environment_image, src/render.hpp:251-261) in rypath's wire layout.  rgb_table and
+ * illuminant are rypath's srgb_reconstruction_table() and pbrt_d65() (src/rgb_spectrum.hpp).
+ * An environment image (RP_NONE: none) is a square equal-area octahedral map with one level;
+ * it replaces the constant environment, and its importance tables are built from its
+ * texels when the scene is created (src/environment_sampling.cpp).  Image reflectance needs
+ * texture coordinates: per instance the first of its vertices' uvs (instance_uv_begin[i],
+ * RP_NONE: the triangle's default (0,0), (1,0), (1,1)), per textured triangle its tangents
+ * dpdu, dpdv (6 floats, TextureTriangleFrame, from instance_frame_begin[i] on), and the
+ * texture camera (TextureCamera, src/texture_footprint.hpp:9-12; row-major). */
+typedef struct rp_images {
+    uint32_t texture_count;    const rp_image_texture *textures;
+    uint32_t level_count;      const rp_texture_level *levels;
+    uint32_t texel_word_count; const uint32_t *texels;
+    uint32_t transfer_count;   const float *transfer;
+    const float *rgb_table;    /* RP_RGB_TABLE_FLOATS */
+    const float *illuminant;   /* RP_SPECTRUM_BINS */
+    uint32_t environment_image;
+    float environment_scale;
+    float environment_from_world[9]; /* environment_texture_from_world, linear part */
+    uint32_t uv_count;         const float *uvs; /* 2 floats per uv */
+    const uint32_t *instance_uv_begin;    /* instance_count entries */
+    uint32_t frame_count;      const float *frames;
+    const uint32_t *instance_frame_begin; /* instance_count entries (RP_NONE: untextured) */
+    float world_from_camera[9], camera_from_world[9];
+} rp_images;
 
 typedef struct rp_area_emission { /* wire::AreaEmission subset, src/render_wire.h:219 */
     float radiance[RP_SPECTRUM_BINS];
@@ -166,6 +232,7 @@ typedef struct rp_scene_desc {
     float lens_x[3], lens_y[3];
     /* RP_FILTER_GAUSSIAN: PBRT sigma; the radii are filter_x_radius / filter_y_radius. */
     float filter_sigma;
+    const rp_images *images; /* NULL: no image textures and no environment image */
 } rp_scene_desc;
 
 /* RenderRequest (src/metal_render.hpp:14-32). */
@@ -463,6 +530,29 @@ rp_status rp_cuda_probe_raygen(struct rp_scene *scene, const rp_request *request
  * weight, sample pdf, flags, eta, pad, pad}. */
 rp_status rp_cuda_probe_bsdf(const float *queries, uint32_t count, float *results, char *diag,
                              size_t diag_capacity);
+/* Image probes over a description's images (uploaded as scene creation uploads them, the
+ * environment tables included): texture lookups of texture `index` through the point /
+ * bilinear / trilinear filters (shaders/image_texture.h:403-456; 6 floats {u, v, dudx, dvdx,
+ * dudy, dvdy} -> 4 {rgb[3], scalar}); the sRGB reconstruction (shaders/image_texture.h:458-507;
+ * 4 {r, g, b, wavelength} -> 2 {bounded, unbounded}); environment queries
+ * (shaders/image_lighting.h:170-325; 8 {direction[3], wavelength, u[2], unused[2]} -> 12
+ * {radiance, compensated pdf, full pdf, sample ok, direction[3], pdf, full-table sample ok,
+ * direction[3]}). */
+rp_status rp_cuda_probe_image_lookup(const rp_images *images, uint32_t index, const float *queries,
+                                     uint32_t count, float *results, char *diag,
+                                     size_t diag_capacity);
+rp_status rp_cuda_probe_rgb_spectrum(const rp_images *images, const float *queries, uint32_t count,
+                                     float *results, char *diag, size_t diag_capacity);
+rp_status rp_cuda_probe_environment(const rp_images *images, const float *queries, uint32_t count,
+                                    float *results, char *diag, size_t diag_capacity);
+/* The environment image's importance tables as scene creation builds them, on the host (no
+ * device is used): the full then the compensated table (each a marginal CDF and one
+ * conditional CDF per row, width + 1 floats apiece; build_environment_sampling,
+ * src/environment_sampling.cpp:20-115) into cdf (2 (width + 1)^2 floats), and the image's mean
+ * RGB illuminant power (light_image_power, src/light_sampling.cpp:78-95). */
+rp_status rp_cuda_environment_tables(const rp_images *images, float *cdf, size_t capacity,
+                                     uint32_t *width, uint32_t *compensated_offset,
+                                     double *mean_power, char *diag, size_t diag_capacity);
 /* Hero BSDF probe (shaders/hero_current_bsdf.h:121-203, hero_frozen_bsdf.h:167-250,
  * hero_scattering.h:100-138): per query 32 floats {kind, active mask, remap, unused, per
  * wavelength {eta or reflectance, k, roughness u, roughness v}, wo[3], wi[3], uc, ux, uy,

@@ -323,6 +323,10 @@ bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error) {
         s.has_environment = std::any_of(s.environment.begin(), s.environment.end(),
                                         [](float v) { return v > 0; });
     }
+    if (const std::string images = load_images(d.images, s.images); !images.empty()) {
+        error = images;
+        return false;
+    }
     // emitters in instance order (src/metal_render.mm:1174-1210)
     for (u32 i = 0; i < d.instance_count; ++i) {
         const auto &q = d.instances[i];
@@ -513,11 +517,14 @@ bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error) {
         input.push_back(li);
     }
     s.environment_light = RP_NONE;
-    if (s.has_environment) {
+    const bool env_image = s.images.env_image != RP_NONE;
+    if (s.has_environment || env_image) {
+        // src/metal_render.mm:617-630: an environment image replaces the constant environment
         LightInput li;
         li.infinite = true;
         const double radius = std::max(double(s.scene_radius), 1e-8);
-        li.power = 4 * pi * pi * radius * radius * light_spectrum_power(s.environment.data());
+        li.power = 4 * pi * pi * radius * radius *
+                   (env_image ? s.images.env_power * s.images.env_scale : light_spectrum_power(s.environment.data()));
         s.environment_light = u32(input.size());
         input.push_back(li);
     }

@@ -4,6 +4,7 @@
 #pragma once
 
 #include "oracle_math.hpp"
+#include "oracle_image.hpp"
 #include "../include/rypath_cuda.h"
 
 #include <functional>
@@ -90,6 +91,7 @@ struct Scene {
     std::vector<Emitter> emitters;
     std::array<float, 471> environment{};
     bool has_environment = false;
+    Images images; // image textures and the environment image (env_image RP_NONE: none)
     // media (scalar transport)
     std::vector<Medium> media;
     u32 camera_medium = RP_NONE, transport = RP_TRANSPORT_HERO;

@@ -95,8 +95,10 @@ static bool prepare_bsdf(const Scene &s, const Material &m, const Wavelengths &l
 // shaders/render.metal:1811-1830 (area_radiance, plain spectrum)
 static bool emitted(const Scene &s, const Vertex &v, F3 direction, const Wavelengths &l, F4 &rad) {
     if (infinite(v)) {
+        // shaders/packet_transport.h:92-101: the environment image when there is one
         for (int k = 0; k < 4; ++k)
-            rad[k] = s.environment[dense_index(l.lambda[k])];
+            rad[k] = s.images.env_image != RP_NONE ? env_image_radiance(s.images, direction, l.lambda[k])
+                                                   : s.environment[dense_index(l.lambda[k])];
         return finite_nonnegative4(rad);
     }
     rad = f4(0);
@@ -172,8 +174,13 @@ static F4 hero_weight(Sample &smp, const Density &prefix, F4 value, F4 sampled, 
 // shaders/packet_transport.h:740-758 (direct_pdf / hero_history_light_pdf)
 static float light_pdf(const Ctx &c, const Vertex &from, const Vertex &light) {
     const float selection = light_pmf(c.s, from.point.position, from.point.shading_normal, light.light);
-    if (infinite(light))
-        return 0.0f * selection; // environment_pdf is 0 for unidirectional PT
+    if (infinite(light)) {
+        // shaders/packet_transport.h:102-108: unidirectional PT samples the image's compensated
+        // table; a constant environment has no proposal
+        if (c.s.images.env_image != RP_NONE)
+            return env_image_pdf(c.s.images, -light.point.geometric_normal, true) * selection;
+        return 0.0f * selection;
+    }
     const F3 delta = light.point.position - from.point.position;
     if (!(dot(delta, delta) > 0))
         return 0;
@@ -310,6 +317,17 @@ static bool sample_li(const Ctx &c, const Vertex &ref, const Wavelengths &l, flo
             rad[k] = intensity / d2;
         }
         pdf = choice.pmf;
+    } else if (s.images.env_image != RP_NONE) {
+        // shaders/packet_transport.h:536-552 with sample_environment (:109-123)
+        v.type = environment_vertex;
+        if (!env_image_sample(s.images, u1, u2, true, direction, pdf))
+            return false;
+        for (int k = 0; k < 4; ++k)
+            rad[k] = env_image_radiance(s.images, direction, l.lambda[k]);
+        pdf *= choice.pmf;
+        v.point.position = ref.point.position + 2 * s.scene_radius * direction;
+        v.point.geometric_normal = -direction;
+        v.point.shading_normal = -direction;
     } else {
         // constant environment: not sampleable by unidirectional PT (pdf 0)
         v.type = environment_vertex;

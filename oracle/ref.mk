@@ -1,5 +1,7 @@
 # Compiles rypath's own host-compilable sources, where they lie in a rypath checkout, into
-# oracle/_ref/: libref.so, the pin for the oracle's restatement, and roulette_known_answers,
+# oracle/_ref/: libref.so, the pin for the oracle's restatement; libref_image.so, rypath's
+# image shader headers and host image sources (with the PNG / JPEG decoders they link); and
+# roulette_known_answers,
 # rypath's own roulette test program built against the oracle's restatement of the roulette
 # header (oracle/roulette_as_ref).  Test infrastructure only; not rypath's build system.
 # Usage: make -f oracle/ref.mk REF=/path/to/rypath
@@ -13,11 +15,29 @@ BASE := -O2 -std=c++20 -fPIC -ffp-contract=off -fno-fast-math -w
 FLAGS := $(BASE) -shared -I$(REF)/src -I$(REF)/shaders -I$(HERE)ref_shim
 SRC := $(HERE)ref_probe.cpp $(HERE)ref_hero_probe.cpp $(REF)/src/light_sampling.cpp $(REF)/src/packet_film.cpp
 
-all: $(OUT)/libref.so $(OUT)/roulette_known_answers
+IMAGE_SRC := $(HERE)ref_image_probe.cpp $(HERE)ref_image_host.cpp $(REF)/src/image_texture.cpp \
+	$(REF)/src/environment_sampling.cpp $(REF)/src/rgb_spectrum.cpp $(REF)/src/pbrt_spectra.cpp \
+	$(REF)/src/light_sampling.cpp $(REF)/src/png_allocator.cpp $(REF)/third_party/lodepng/lodepng.cpp \
+	$(REF)/third_party/stb/jpeg.cpp
+IMAGE_FLAGS := $(FLAGS) -I$(REF)/third_party/stb -I$(REF)/third_party/lodepng -I$(REF)/third_party/pbrt \
+	-DRYPATH_SRGB_BIN='"$(REF)/third_party/pbrt/srgb.bin"'
+
+all: $(OUT)/libref.so $(OUT)/libref_image.so $(OUT)/roulette_known_answers
 
 $(OUT)/libref.so: $(SRC) $(HERE)ref_shim/metal_stdlib
 	mkdir -p $(OUT)
 	$(CXX) $(FLAGS) -o $@ $(SRC)
+
+# Metal's constant address space is read-only, which C++ spells const: the image probe maps
+# `constant` to `const`, and this rule writes a copy of shaders/image_lighting.h into the
+# build folder with the one spelling that mapping would double (`const constant` -> `const`).
+$(OUT)/gen/image_lighting.h: $(REF)/shaders/image_lighting.h
+	mkdir -p $(OUT)/gen
+	sed 's/const constant /const /g' $< > $@
+
+$(OUT)/libref_image.so: $(IMAGE_SRC) $(HERE)ref_shim/metal_stdlib $(OUT)/gen/image_lighting.h
+	mkdir -p $(OUT)
+	$(CXX) -I$(OUT)/gen $(IMAGE_FLAGS) -Wl,--no-undefined -o $@ $(IMAGE_SRC)
 
 $(OUT)/roulette_known_answers: $(REF)/tests/packet_roulette_tests.cpp $(HERE)roulette_as_ref/packet_roulette_shared.h $(HERE)oracle_math.hpp
 	mkdir -p $(OUT)

@@ -6,7 +6,7 @@ their sizes against the values the library itself reports.
 
 import ctypes as C
 
-RP_ABI_VERSION = 1
+RP_ABI_VERSION = 2
 RP_NONE = 0xFFFFFFFF
 RP_SPECTRUM_BINS = 471
 RP_SOBOL_TABLE_BYTES = 234208
@@ -23,7 +23,10 @@ FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = 0, 1, 2
 DIFFUSE, CONDUCTOR, DIELECTRIC = 0, 1, 2
 INTERFACE = 10  # null interface: medium change (scalar transport), pass-through (hero transport)
 MIX = 9  # stochastic mix of two materials
-REFLECTANCE_KNOTS, REFLECTANCE_CONSTANT, REFLECTANCE_BLACKBODY = 0, 1, 4
+REFLECTANCE_KNOTS, REFLECTANCE_CONSTANT, REFLECTANCE_IMAGE, REFLECTANCE_BLACKBODY = 0, 1, 3, 4
+WRAP_REPEAT, WRAP_CLAMP, WRAP_BLACK = 0, 1, 2
+TEXTURE_BILINEAR, TEXTURE_TRILINEAR, TEXTURE_POINT, TEXTURE_EWA = 0, 1, 2, 3
+TEXELS_SRGB8, TEXELS_LINEAR8, TEXELS_HALF, TEXELS_FLOAT = 0, 1, 2, 3
 POINT_LIGHT, SPOT_LIGHT = 0, 1
 LIGHTS_BVH, LIGHTS_POWER, LIGHTS_UNIFORM = 0, 1, 2
 TRANSPORT_SCALAR, TRANSPORT_HERO = 0, 2
@@ -49,7 +52,34 @@ class Material(C.Structure):
                 ("scalar_value", f32), ("eta_begin", u32), ("eta_count", u32), ("k_begin", u32),
                 ("k_count", u32), ("optical_extensions", u32), ("u_roughness", f32),
                 ("v_roughness", f32), ("remap_roughness", u32), ("first_material", u32),
-                ("second_material", u32), ("mix_amount", f32)]
+                ("second_material", u32), ("mix_amount", f32), ("image_texture", u32)]
+
+
+class ImageTexture(C.Structure):
+    _fields_ = [("level_begin", u32), ("level_count", u32), ("wrap", u32), ("texel_format", u32),
+                ("uscale", f32), ("vscale", f32), ("udelta", f32), ("vdelta", f32), ("scale", f32),
+                ("invert", u32), ("filter", u32), ("max_anisotropy", f32), ("transfer_offset", u32),
+                ("channels", u32), ("gltf", u32), ("wrap_t", u32), ("min_filter", u32),
+                ("mag_filter", u32)]
+
+
+class TextureLevel(C.Structure):
+    _fields_ = [("width", u32), ("height", u32), ("offset", u32)]
+
+
+class Images(C.Structure):
+    _fields_ = [
+        ("texture_count", u32), ("textures", P(ImageTexture)),
+        ("level_count", u32), ("levels", P(TextureLevel)),
+        ("texel_word_count", u32), ("texels", P(u32)),
+        ("transfer_count", u32), ("transfer", P(f32)),
+        ("rgb_table", P(f32)), ("illuminant", P(f32)),
+        ("environment_image", u32), ("environment_scale", f32),
+        ("environment_from_world", f32 * 9),
+        ("uv_count", u32), ("uvs", P(f32)), ("instance_uv_begin", P(u32)),
+        ("frame_count", u32), ("frames", P(f32)), ("instance_frame_begin", P(u32)),
+        ("world_from_camera", f32 * 9), ("camera_from_world", f32 * 9),
+    ]
 
 
 class AreaEmission(C.Structure):
@@ -94,6 +124,7 @@ class SceneDesc(C.Structure):
         ("sobol_tables", C.c_void_p),
         ("lens_radius", f32), ("focal_distance", f32), ("lens_x", f32 * 3), ("lens_y", f32 * 3),
         ("filter_sigma", f32),
+        ("images", P(Images)),
     ]
 
 
@@ -212,12 +243,14 @@ class FrameInfo(C.Structure):
 FRAME_PENDING, FRAME_COMPLETE, FRAME_FAILED = 0, 1, 2
 
 EXPECTED_SIZES = {
-    "rp_instance": (Instance, 88), "rp_material": (Material, 64), "rp_knot": (Knot, 8),
+    "rp_instance": (Instance, 88), "rp_material": (Material, 68), "rp_knot": (Knot, 8),
     "rp_area_emission": (AreaEmission, 1888), "rp_positional_light": (PositionalLight, 1948),
     "rp_medium": (Medium, 5656), "rp_camera": (Camera, 48), "rp_request": (Request, 64),
     "rp_packet_result": (PacketResult, 80), "rp_scalar_result": (ScalarResult, 44),
     "rp_film_pixel": (FilmPixel, 144), "rp_film_request": (FilmRequest, 88),
     "rp_view": (View, 80), "rp_batch_config": (BatchConfig, 24), "rp_batch_request": (BatchRequest, 64),
     "rp_adjoint_request": (AdjointRequest, 104),
+    "rp_image_texture": (ImageTexture, 72), "rp_texture_level": (TextureLevel, 12),
+    "rp_images": (Images, 240),
     "rp_frame_config": (FrameConfig, 32), "rp_frame_request": (FrameRequest, 24), "rp_frame_info": (FrameInfo, 56),
 }

@@ -13,8 +13,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librypath_cuda.so")
 SOURCES = ["rp_host.cu"]
-HEADERS = ["rp_math.cuh", "rp_scene.cuh", "rp_transport.cuh", "rp_kernels.cuh", "rp_build.cuh", "rp_probes.cuh",
-           "rp_volpath.cuh", "rp_batch.cuh"]
+HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith(".cuh"))
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 
 

@@ -362,6 +362,225 @@ double light_spectrum_power(const float *spectrum) {
     return value;
 }
 
+// ---------------------------------------------------------------- images on the host
+// The scene-build side of the image inputs: texel decoding for the environment tables and
+// light power, rypath's host sRGB reconstruction (src/rgb_spectrum.cpp:62-127), the
+// environment importance tables (src/environment_sampling.cpp:20-115) and the environment
+// light's power (src/light_sampling.cpp:28-95).
+float half_to_float_host(u32 bits) {
+    const u32 sign = (bits & 0x8000u) << 16, e = (bits >> 10) & 31u, m = bits & 1023u;
+    u32 out;
+    if (e == 0) {
+        if (m == 0)
+            out = sign;
+        else {
+            const u32 top = 31u - u32(__builtin_clz(m));
+            out = sign | ((103u + top) << 23) | ((m << (23u - top)) & 0x7fffffu);
+        }
+    } else {
+        out = sign | ((e == 31u ? 255u : e + 112u) << 23) | (m << 13);
+    }
+    float f;
+    memcpy(&f, &out, 4);
+    return f;
+}
+u32 texel_words(u32 format) { return format == RP_TEXELS_FLOAT ? 4u : format == RP_TEXELS_HALF ? 2u : 1u; }
+// Linear RGB of texel (x, y) of a level; false when a channel is not finite
+// (image_base_texel_linear_rgb, src/image_texture.cpp:1324-1332).
+bool host_texel(const rp_images &im, const rp_image_texture &t, const rp_texture_level &l, u32 x, u32 y,
+                float rgb[3]) {
+    const size_t index = size_t(y) * l.width + x;
+    if (t.texel_format == RP_TEXELS_FLOAT) {
+        memcpy(rgb, im.texels + l.offset + 4 * index, 12);
+    } else if (t.texel_format == RP_TEXELS_HALF) {
+        const u32 rg = im.texels[l.offset + 2 * index], b = im.texels[l.offset + 2 * index + 1];
+        rgb[0] = half_to_float_host(rg & 0xffffu);
+        rgb[1] = half_to_float_host(rg >> 16);
+        rgb[2] = half_to_float_host(b & 0xffffu);
+    } else {
+        const u32 v = im.texels[l.offset + index];
+        const float *lut = im.transfer + t.transfer_offset;
+        rgb[0] = lut[v & 255u];
+        rgb[1] = lut[(v >> 8) & 255u];
+        rgb[2] = lut[(v >> 16) & 255u];
+    }
+    return std::isfinite(rgb[0]) && std::isfinite(rgb[1]) && std::isfinite(rgb[2]);
+}
+// reconstruct_srgb + evaluate_srgb at one wavelength; rgb in [0, 1]
+bool host_srgb_spectrum(const float *table, const float rgb[3], float wavelength, float &value) {
+    for (int c = 0; c < 3; ++c)
+        if (!std::isfinite(rgb[c]) || rgb[c] < 0 || rgb[c] > 1)
+            return false;
+    if (rgb[0] == rgb[1] && rgb[1] == rgb[2]) {
+        value = rgb[0];
+        return true;
+    }
+    int top = 0; // the last of tied maxima
+    for (int c = 1; c < 3; ++c)
+        if (rgb[c] >= rgb[top])
+            top = c;
+    const float z = rgb[top];
+    const float x = rgb[(top + 1) % 3] * 63 / z, y = rgb[(top + 2) % 3] * 63 / z;
+    const int xi = std::min(int(x), 62), yi = std::min(int(y), 62);
+    const float *nodes = table;
+    const int zi = int(std::lower_bound(nodes + 1, nodes + 63, z) - nodes) - 1;
+    const float dx = x - float(xi), dy = y - float(yi), dz = (z - nodes[zi]) / (nodes[zi + 1] - nodes[zi]);
+    const auto lerp = [](float t, float a, float b) { return (1.0f - t) * a + t * b; };
+    float co[3];
+    for (int i = 0; i < 3; ++i) {
+        const auto at = [&](int ox, int oy, int oz) {
+            return table[64 + 3 * (((top * 64 + zi + oz) * 64 + yi + oy) * 64 + xi + ox) + i];
+        };
+        co[i] = lerp(dz, lerp(dy, lerp(dx, at(0, 0, 0), at(1, 0, 0)), lerp(dx, at(0, 1, 0), at(1, 1, 0))),
+                     lerp(dy, lerp(dx, at(0, 0, 1), at(1, 0, 1)), lerp(dx, at(0, 1, 1), at(1, 1, 1))));
+    }
+    const float poly = std::fma(wavelength, std::fma(wavelength, co[0], co[1]), co[2]);
+    if (!std::isfinite(poly)) {
+        value = NAN;
+        return true;
+    }
+    if (std::abs(poly) <= 1.0f) {
+        value = 0.5f + 0.5f * (poly / std::sqrt(1.0f + poly * poly));
+    } else {
+        const float r = 1.0f / poly;
+        value = 0.5f + 0.5f * std::copysign(1.0f / std::sqrt(1.0f + r * r), poly);
+    }
+    return true;
+}
+// light_rgb_power (src/light_sampling.cpp:28-44): the RGB illuminant's spectrum at the four
+// visible hero wavelengths of u = 0.5, over their densities.
+bool light_rgb_power(const rp_images &im, const float rgb[3], double &value) {
+    const float amplitude = 2 * std::max({rgb[0], rgb[1], rgb[2]});
+    value = 0;
+    if (amplitude == 0)
+        return true;
+    if (!std::isfinite(amplitude))
+        return false;
+    const float normalized[3] = {rgb[0] / amplitude, rgb[1] / amplitude, rgb[2] / amplitude};
+    for (int i = 0; i < 3; ++i)
+        if (!(normalized[i] >= 0 && normalized[i] <= 1))
+            return false;
+    for (int i = 0; i < 4; ++i) {
+        float up = .5f + float(i) * .25f;
+        if (up > 1)
+            up -= 1;
+        float w = 538 - 138.888889f * std::atanh(.85691062f - 1.82750197f * up);
+        w = std::clamp(w, 360.f, 830.f);
+        const float c = std::cosh(.0072f * (w - 538));
+        const float pdf = .0039398042f / (c * c);
+        const unsigned bin = unsigned(std::round(w) - 360);
+        float spectral;
+        host_srgb_spectrum(im.rgb_table, normalized, float(bin + 360), spectral);
+        value += double(amplitude) * spectral * im.illuminant[bin] / pdf / 4;
+    }
+    return true;
+}
+// The environment image's full and compensated importance tables (a marginal CDF then one
+// conditional CDF per row, each width + 1 floats; the compensated table keeps only the mass
+// above the mean) and its mean RGB power (light_image_power).
+std::string environment_tables(const rp_images &im, std::vector<float> &cdf, u32 &width, u32 &compensated_offset,
+                               double &mean_power) {
+    const rp_image_texture &t = im.textures[im.environment_image];
+    const rp_texture_level &l = im.levels[t.level_begin];
+    if (t.level_count != 1 || l.width != l.height)
+        return "Environment sampling requires a square native image base";
+    width = l.width;
+    const size_t side = size_t(width) + 1;
+    compensated_offset = u32(side * side);
+    cdf.assign(2 * side * side, 0.f);
+    std::vector<double> mass(size_t(width) * width), full_rows(width), comp_rows(width), full_prefix(side),
+        comp_prefix(side);
+    double total = 0, power = 0;
+    for (u32 y = 0; y < width; ++y) {
+        double row = 0;
+        for (u32 x = 0; x < width; ++x) {
+            float rgb[3];
+            if (!host_texel(im, t, l, x, y, rgb))
+                return "Environment sampling texel is invalid";
+            const double v =
+                (double(std::max(rgb[0], 0.f)) + double(std::max(rgb[1], 0.f)) + double(std::max(rgb[2], 0.f))) / 3;
+            mass[size_t(y) * width + x] = v;
+            row += v;
+            double p;
+            if (!light_rgb_power(im, rgb, p))
+                return "Invalid environment light sampling image";
+            power += p;
+        }
+        full_rows[y] = row;
+        total += row;
+    }
+    mean_power = power / (double(width) * width);
+    const double average = total / (double(width) * width);
+    const auto write_prefix = [&](size_t offset, const std::vector<double> &prefix, double sum) {
+        for (u32 x = 1; x <= width; ++x)
+            cdf[offset + x] = sum > 0 ? float(prefix[x] / sum) : float(x) / float(width);
+        cdf[offset + width] = 1.f;
+    };
+    double comp_total = 0;
+    for (u32 y = 0; y < width; ++y) {
+        full_prefix[0] = comp_prefix[0] = 0;
+        for (u32 x = 0; x < width; ++x) {
+            const double v = mass[size_t(y) * width + x];
+            full_prefix[x + 1] = full_prefix[x] + v;
+            comp_prefix[x + 1] = comp_prefix[x] + std::max(v - average, 0.);
+        }
+        comp_rows[y] = comp_prefix[width];
+        comp_total += comp_rows[y];
+        write_prefix(side * (y + 1), full_prefix, full_rows[y]);
+        write_prefix(compensated_offset + side * (y + 1), comp_prefix, comp_rows[y]);
+    }
+    double full_sum = 0, comp_sum = 0;
+    for (u32 y = 0; y < width; ++y) {
+        full_sum += full_rows[y];
+        comp_sum += comp_rows[y];
+        cdf[y + 1] = total > 0 ? float(full_sum / total) : float(y + 1) / float(width);
+        cdf[compensated_offset + y + 1] = comp_total > 0 ? float(comp_sum / comp_total) : float(y + 1) / float(width);
+    }
+    cdf[width] = cdf[compensated_offset + width] = 1.f;
+    return {};
+}
+// Structural checks of the image inputs (valid ranges and sizes; texel values are checked
+// where they are read).
+std::string validate_images(const rp_scene_desc *d) {
+    const rp_images *im = d->images;
+    if (!im)
+        return {};
+    if ((im->texture_count && !im->textures) || (im->level_count && !im->levels) ||
+        (im->texel_word_count && !im->texels) || (im->transfer_count && !im->transfer))
+        return "image arrays must be given with their counts";
+    if (im->texture_count && (!im->rgb_table || !im->illuminant))
+        return "images need the sRGB reconstruction table and the D65 illuminant";
+    for (u32 i = 0; i < im->texture_count; ++i) {
+        const rp_image_texture &t = im->textures[i];
+        if (t.gltf)
+            return "glTF image textures are not built";
+        if (t.level_count == 0 || t.level_count > 14 || t.level_begin > im->level_count ||
+            t.level_count > im->level_count - t.level_begin || t.texel_format > RP_TEXELS_FLOAT || t.wrap > 2 ||
+            t.filter > RP_TEXTURE_EWA || (t.channels != 1 && t.channels != 3 && t.channels != 4))
+            return "invalid image texture descriptor";
+        if (t.texel_format < RP_TEXELS_HALF && (t.transfer_offset > im->transfer_count ||
+                                                im->transfer_count - t.transfer_offset < 256))
+            return "8-bit image texture needs 256 transfer values";
+        for (u32 k = 0; k < t.level_count; ++k) {
+            const rp_texture_level &l = im->levels[t.level_begin + k];
+            const uint64_t words = uint64_t(l.width) * l.height * texel_words(t.texel_format);
+            if (l.width == 0 || l.height == 0 || l.width > 8192 || l.height > 8192 || l.offset > im->texel_word_count ||
+                words > im->texel_word_count - l.offset)
+                return "image level outside the texel words";
+        }
+    }
+    if (im->environment_image != RP_NONE) {
+        if (im->environment_image >= im->texture_count)
+            return "environment image out of range";
+        if (!std::isfinite(im->environment_scale) || im->environment_scale < 0)
+            return "environment image scale must be finite and nonnegative";
+        for (float v : im->environment_from_world)
+            if (!std::isfinite(v))
+                return "environment transform must be finite";
+    }
+    return {};
+}
+
 // ---------------------------------------------------------------- Gaussian pixel filter
 // compile_gaussian_filter (src/gaussian_filter.cpp:84-137): PBRT's Gaussian filter minus its
 // value at the radius, tabulated at 32 cells per unit radius at cell midpoints, with PBRT's
@@ -493,6 +712,83 @@ template <class T> T *dupload(std::vector<void *> &owned, const T *src, size_t c
     if (count)
         RP_CHECK(cudaMemcpyAsync(p, src, count * sizeof(T), cudaMemcpyHostToDevice, st));
     return p;
+}
+
+// Upload a description's images in their wire layout; an environment image also gets its
+// importance tables and its light power (mean RGB illuminant power times its scale; -1 when
+// there is no environment image).
+void upload_images(const rp_images *im, DImages &g, std::vector<void *> &own, cudaStream_t stm, double &env_power) {
+    static_assert(sizeof(DImageTexture) == sizeof(rp_image_texture) && sizeof(DLevel) == sizeof(rp_texture_level));
+    g = DImages{};
+    g.env_image = kNone;
+    env_power = -1;
+    if (!im)
+        return;
+    g.textures = dupload(own, reinterpret_cast<const DImageTexture *>(im->textures), im->texture_count, stm);
+    g.levels = dupload(own, reinterpret_cast<const DLevel *>(im->levels), im->level_count, stm);
+    g.texels = dupload(own, im->texels, im->texel_word_count, stm);
+    g.transfer = dupload(own, im->transfer, im->transfer_count, stm);
+    g.texture_count = im->texture_count;
+    g.level_count = im->level_count;
+    g.texel_word_count = im->texel_word_count;
+    g.transfer_count = im->transfer_count;
+    if (im->texture_count) {
+        g.rgb_table = dupload(own, im->rgb_table, RP_RGB_TABLE_FLOATS, stm);
+        g.illuminant = dupload(own, im->illuminant, 471, stm);
+    }
+    if (im->environment_image != RP_NONE) {
+        std::vector<float> cdf;
+        u32 width = 0, offset = 0;
+        double mean = 0;
+        const std::string err = environment_tables(*im, cdf, width, offset, mean);
+        if (!err.empty())
+            throw Invalid{err};
+        g.env_cdf = dupload(own, cdf.data(), cdf.size(), stm);
+        g.env_width = width;
+        g.env_comp_offset = offset;
+        g.env_cdf_count = u32(cdf.size());
+        g.env_image = im->environment_image;
+        g.env_scale = im->environment_scale;
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) {
+                g.env_from_world[3 * r + c] = im->environment_from_world[3 * r + c];
+                g.world_from_env[3 * c + r] = im->environment_from_world[3 * r + c];
+            }
+        env_power = mean * im->environment_scale;
+    }
+}
+
+// One image probe: upload the images (and environment tables) and the queries, run `launch`,
+// read back `out_per` floats per query.
+template <class Launch>
+rp_status image_probe(const rp_images *images, const float *queries, u32 count, u32 in_per, u32 out_per,
+                      float *results, char *diag, size_t cap, Launch launch) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!images || !queries || !results)
+            throw Invalid{"null argument"};
+        rp_scene_desc d{};
+        d.images = images;
+        if (const std::string err = validate_images(&d); !err.empty())
+            throw Invalid{err};
+        std::vector<void *> own;
+        struct Free {
+            std::vector<void *> &o;
+            ~Free() {
+                for (void *p : o)
+                    cudaFreeAsync(p, nullptr);
+                cudaStreamSynchronize(nullptr);
+            }
+        } fr{own};
+        DImages g;
+        double power;
+        upload_images(images, g, own, nullptr, power);
+        const float *q = dupload(own, queries, size_t(in_per) * count, nullptr);
+        float *r = dalloc<float>(own, size_t(out_per) * count);
+        launch(g, q, r);
+        RP_CHECK(cudaGetLastError());
+        RP_CHECK(cudaMemcpy(results, r, size_t(out_per) * count * 4, cudaMemcpyDeviceToHost));
+        return RP_SUCCESS;
+    });
 }
 
 int grid_for(int sm_count, u32 work, int block, int per_sm) {
@@ -1371,6 +1667,9 @@ uint32_t rp_cuda_abi_size(const char *name) {
     if (n == "rp_medium") return sizeof(rp_medium);
     if (n == "rp_camera") return sizeof(rp_camera);
     if (n == "rp_scene_desc") return sizeof(rp_scene_desc);
+    if (n == "rp_image_texture") return sizeof(rp_image_texture);
+    if (n == "rp_texture_level") return sizeof(rp_texture_level);
+    if (n == "rp_images") return sizeof(rp_images);
     if (n == "rp_request") return sizeof(rp_request);
     if (n == "rp_packet_result") return sizeof(rp_packet_result);
     if (n == "rp_scalar_result") return sizeof(rp_scalar_result);
@@ -1451,6 +1750,13 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
         }
         if (const std::string mix = validate_mix(d); !mix.empty())
             throw Invalid{mix};
+        if (const std::string images = validate_images(d); !images.empty())
+            throw Invalid{images};
+        if (d->images && scalar && (d->images->environment_image != RP_NONE || d->images->texture_count))
+            throw NotBuilt{"the scalar transport does not read images"};
+        for (u32 i = 0; i < d->material_count; ++i)
+            if (d->materials[i].kind == RP_REFLECTANCE_IMAGE)
+                throw NotBuilt{"image reflectance is not built yet"};
         if (d->filter_kind > RP_FILTER_GAUSSIAN)
             throw Invalid{"unsupported pixel filter"};
         if (!(d->lens_radius >= 0) || !std::isfinite(d->lens_radius) ||
@@ -1631,6 +1937,10 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
         ds.emitter_instance = dupload(own, em_inst.data(), em_inst.size(), stm);
         ds.emitter_local = dupload(own, em_local.data(), em_local.size(), stm);
         ds.emitter_count = u32(em_inst.size());
+        // images (RenderScene::image_textures ... environment_image, src/render.hpp:251-261),
+        // uploaded in rypath's wire layout
+        double env_power = -1;
+        upload_images(d->images, ds.img, own, stm, env_power);
         // scene sphere (src/metal_render.mm:213-276) over the world vertices of k_tri_prepare
         int bounds[12];
         const auto t_wait = std::chrono::steady_clock::now();
@@ -1744,11 +2054,12 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             input.push_back(li);
         }
         ds.environment_light = kNone;
-        if (has_environment) {
+        if (has_environment || env_power >= 0) {
+            // an environment image replaces the constant environment (src/metal_render.mm:617-630)
             LightInput li;
             li.infinite = true;
             const double radius = std::max(double(scene_radius), 1e-8);
-            li.power = 4 * pi * pi * radius * radius * light_spectrum_power(d->environment);
+            li.power = 4 * pi * pi * radius * radius * (env_power >= 0 ? env_power : light_spectrum_power(d->environment));
             ds.environment_light = u32(input.size());
             input.push_back(li);
         }
@@ -2767,6 +3078,55 @@ rp_status rp_cuda_probe_bsdf(const float *queries, uint32_t count, float *result
         k_probe_bsdf<<<(count + 127) / 128, 128>>>(q, count, r);
         RP_CHECK(cudaGetLastError());
         RP_CHECK(cudaMemcpy(results, r, size_t(12) * count * 4, cudaMemcpyDeviceToHost));
+        return RP_SUCCESS;
+    });
+}
+
+rp_status rp_cuda_probe_image_lookup(const rp_images *images, uint32_t index, const float *queries, uint32_t count,
+                                     float *results, char *diag, size_t cap) {
+    if (images && index >= images->texture_count)
+        return guarded(diag, cap, []() -> rp_status { throw Invalid{"texture index out of range"}; });
+    return image_probe(images, queries, count, 6, 4, results, diag, cap, [&](const DImages &g, const float *q, float *r) {
+        k_probe_image_lookup<<<(count + 127) / 128, 128>>>(g, index, q, count, r);
+    });
+}
+
+rp_status rp_cuda_probe_rgb_spectrum(const rp_images *images, const float *queries, uint32_t count, float *results,
+                                     char *diag, size_t cap) {
+    if (images && !images->rgb_table)
+        return guarded(diag, cap, []() -> rp_status { throw Invalid{"no sRGB reconstruction table"}; });
+    return image_probe(images, queries, count, 4, 2, results, diag, cap, [&](const DImages &g, const float *q, float *r) {
+        k_probe_rgb_spectrum<<<(count + 127) / 128, 128>>>(g.rgb_table, q, count, r);
+    });
+}
+
+rp_status rp_cuda_probe_environment(const rp_images *images, const float *queries, uint32_t count, float *results,
+                                    char *diag, size_t cap) {
+    if (images && images->environment_image == RP_NONE)
+        return guarded(diag, cap, []() -> rp_status { throw Invalid{"no environment image"}; });
+    return image_probe(images, queries, count, 8, 12, results, diag, cap, [&](const DImages &g, const float *q, float *r) {
+        k_probe_environment<<<(count + 127) / 128, 128>>>(g, q, count, r);
+    });
+}
+
+rp_status rp_cuda_environment_tables(const rp_images *images, float *cdf, size_t capacity, uint32_t *width,
+                                     uint32_t *compensated_offset, double *mean_power, char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!images || !cdf || !width || !compensated_offset || !mean_power)
+            throw Invalid{"null argument"};
+        rp_scene_desc d{};
+        d.images = images;
+        if (const std::string err = validate_images(&d); !err.empty())
+            throw Invalid{err};
+        if (images->environment_image == RP_NONE)
+            throw Invalid{"no environment image"};
+        std::vector<float> tables;
+        const std::string err = environment_tables(*images, tables, *width, *compensated_offset, *mean_power);
+        if (!err.empty())
+            throw Invalid{err};
+        if (tables.size() > capacity)
+            throw Invalid{"capacity too small"};
+        std::copy(tables.begin(), tables.end(), cdf);
         return RP_SUCCESS;
     });
 }

@@ -398,10 +398,15 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_const
                     V4 rad = v4(0);
                     bool emission_ok = true;
                     if (ctype == kEnvironment) {
-                        if (s.environment != kNone)
+                        if (s.img.env_image != kNone) {
+#pragma unroll
+                            for (int k = 0; k < 4; ++k)
+                                rad.v[k] = environment_image_radiance(s.img, rd, lambda.v[k]);
+                        } else if (s.environment != kNone) {
 #pragma unroll
                             for (int k = 0; k < 4; ++k)
                                 rad.v[k] = spectrum(s, s.environment, lambda.v[k]);
+                        }
                         emission_ok = finite_nonnegative4(rad);
                     } else {
                         const V3 delta = latest.position - cp.position;
@@ -436,7 +441,10 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_const
                             float lpdf = 0;
                             const float selection = light_pmf(s, latest.position, latest.shading_normal, clight);
                             if (ctype == kEnvironment) {
-                                lpdf = 0.0f * selection;
+                                // the constant environment has no unidirectional proposal;
+                                // the image's is its compensated table
+                                lpdf = s.img.env_image != kNone ? environment_image_pdf(s.img, rd, true) * selection
+                                                                : 0.0f * selection;
                             } else {
                                 const V3 dl = cp.position - latest.position;
                                 if (dot(dl, dl) > 0 && nonzero3(cp.geometric_normal) && clight < s.emitter_count)
@@ -581,7 +589,8 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_nee(const __grid_constan
                         // sample_li (shaders/packet_transport.h:470-553)
                         const Selected choice = light_sample(s, cp.position, cp.shading_normal, u0);
                         float u1 = 0, u2 = 0;
-                        if (choice.pmf > 0 && choice.light < s.emitter_count) {
+                        const bool env_image = s.img.env_image != kNone && choice.light == s.environment_light;
+                        if (choice.pmf > 0 && (choice.light < s.emitter_count || env_image)) {
                             const uint4 w = draw_words(s, p, ident.x, ident.y, ident.z, index, block);
                             u1 = sample_uniform(p, w.y);
                             u2 = sample_uniform(p, w.z);
@@ -635,6 +644,20 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_nee(const __grid_constan
                                     }
                                     spdf = choice.pmf;
                                 }
+                            } else if (env_image) {
+                                // the environment image's compensated table
+                                // (shaders/packet_transport.h:536-552)
+                                float epdf = 0;
+                                if (!sample_environment_image(s.img, u1, u2, true, direction, epdf)) {
+                                    li_ok = false;
+                                } else {
+#pragma unroll
+                                    for (int k = 0; k < 4; ++k)
+                                        lrad.v[k] = environment_image_radiance(s.img, direction, lambda.v[k]);
+                                    spdf = epdf * choice.pmf;
+                                    lp.position = cp.position + (2 * s.scene_radius) * direction;
+                                    lp.geometric_normal = lp.shading_normal = -direction;
+                                }
                             } else {
                                 spdf = 0; // constant environment: pdf 0 for unidirectional PT
                             }
@@ -660,12 +683,14 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_nee(const __grid_constan
                                     if (!delta_light) {
                                         const float sel_pmf = light_pmf(s, cp.position, cp.shading_normal, sel);
                                         const float lpdf =
-                                            nonzero3(lp.geometric_normal)
+                                            env_image ? environment_image_pdf(s.img, direction, true) * sel_pmf
+                                            : nonzero3(lp.geometric_normal)
                                                 ? sel_pmf * light_geometry_pdf(s, sel, cp.position, cp.shading_normal, lp)
                                                 : 0.0f;
                                         bool ok;
                                         const V4 bsdf_pdf = represented_pdf<F == 3 ? 0 : F>(
-                                            cbsdf, cp.shading_normal, cp.position, latest.position, false, lp.position, ok);
+                                            cbsdf, cp.shading_normal, cp.position, latest.position, env_image,
+                                            env_image ? direction : lp.position, ok);
                                         weight_ok = ok && hero_weight(direct_density, value, v4(lpdf), bsdf_pdf, contribution);
                                     }
                                     // visible(): offset both endpoints (shaders/packet_transport.h:377-446)

@@ -162,6 +162,58 @@ __global__ void k_probe_hero(const float *queries, u32 count, float *results) {
     o[28] = dirac ? 1.f : 0.f;
     o[29] = hero_connectible(p) ? 1.f : 0.f;
 }
+// Image probes, in the oracle's layouts: texture lookups of texture `index` (6 floats {u, v,
+// dudx, dvdx, dudy, dvdy} -> 4 {rgb[3], scalar}); RGB reconstruction (4 {r, g, b, wavelength}
+// -> 2 {bounded, unbounded}); environment queries (8 {direction[3], wavelength, u[2], unused[2]}
+// -> 12 {radiance, compensated pdf, full pdf, sample ok, direction[3], pdf, full-table sample
+// ok, direction[3]}).
+__global__ void k_probe_image_lookup(const DImages im, u32 index, const float *q, u32 count, float *out) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count)
+        return;
+    const float *a = q + 6 * i;
+    float *o = out + 4 * i;
+    const DImageTexture t = im.textures[index];
+    const F2 uv = f2(a[0], a[1]), dx = f2(a[2], a[3]), dy = f2(a[4], a[5]);
+    const RGB c = lookup_standard(im, t, uv, dx, dy, false, false);
+    o[0] = c.r;
+    o[1] = c.g;
+    o[2] = c.b;
+    o[3] = lookup_standard(im, t, uv, dx, dy, true, false).r;
+}
+__global__ void k_probe_rgb_spectrum(const float *table, const float *q, u32 count, float *out) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count)
+        return;
+    const float *a = q + 4 * i;
+    const RGB c = rgb3(a[0], a[1], a[2]);
+    out[2 * i] = rgb_spectrum(table, c, a[3]);
+    out[2 * i + 1] = rgb_spectrum_unbounded(table, c, a[3]);
+}
+__global__ void k_probe_environment(const DImages im, const float *q, u32 count, float *out) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count)
+        return;
+    const float *a = q + 8 * i;
+    float *o = out + 12 * i;
+    const V3 d = v3(a[0], a[1], a[2]);
+    o[0] = environment_image_radiance(im, d, a[3]);
+    o[1] = environment_image_pdf(im, d, true);
+    o[2] = environment_image_pdf(im, d, false);
+    V3 w = v3(0, 0, 0);
+    float pdf = 0;
+    o[3] = sample_environment_image(im, a[4], a[5], true, w, pdf) ? 1.f : 0.f;
+    o[4] = w.x;
+    o[5] = w.y;
+    o[6] = w.z;
+    o[7] = pdf;
+    V3 w2 = v3(0, 0, 0);
+    float pdf2 = 0;
+    o[8] = sample_environment_image(im, a[4], a[5], false, w2, pdf2) ? 1.f : 0.f;
+    o[9] = w2.x;
+    o[10] = w2.y;
+    o[11] = w2.z;
+}
 __global__ void k_probe_raygen(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p, u32 *words,
                                float *rays) {
     const u32 lane = blockIdx.x * blockDim.x + threadIdx.x;

@@ -2,7 +2,7 @@
 // binary LBVH traversal with watertight triangle tests.
 #pragma once
 
-#include "rp_math.cuh"
+#include "rp_image.cuh"
 
 namespace rp {
 
@@ -136,6 +136,7 @@ struct DeviceScene {
     u32 gauss_w, gauss_h;
     float filter_weight;
     const u32 *primes; // the first 1000 primes (Halton bases)
+    DImages img;       // image textures and the environment image (env_image kNone: none)
 };
 
 RP_DEV V3 load3(const float *p) { return v3(__ldg(p), __ldg(p + 1), __ldg(p + 2)); }

@@ -53,6 +53,10 @@ def lib():
         "rp_cuda_probe_raygen": (st, [vp, C.POINTER(abi.Request), vp, vp, sz, cp, sz]),
         "rp_cuda_probe_bsdf": (st, [vp, u32, vp, cp, sz]),
         "rp_cuda_probe_hero": (st, [vp, u32, vp, cp, sz]),
+        "rp_cuda_probe_image_lookup": (st, [vp, u32, vp, u32, vp, cp, sz]),
+        "rp_cuda_probe_rgb_spectrum": (st, [vp, vp, u32, vp, cp, sz]),
+        "rp_cuda_probe_environment": (st, [vp, vp, u32, vp, cp, sz]),
+        "rp_cuda_environment_tables": (st, [vp, vp, sz, C.POINTER(u32), C.POINTER(u32), C.POINTER(C.c_double), cp, sz]),
         "rp_cuda_scene_export_bvh": (st, [vp, vp, vp, vp, vp, sz, cp, sz]),
         "rp_cuda_scene_export_wide": (st, [vp, vp, sz, vp, sz, C.POINTER(u32), cp, sz]),
         "rp_cuda_trace_rays": (st, [vp, vp, u32, C.c_int, vp, cp, sz]),

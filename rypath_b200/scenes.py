@@ -90,6 +90,7 @@ class Scene:
     # thin lens (radius 0: pinhole): radius, focal distance, camera x / y axes
     lens: tuple = (0.0, 1e6, (1.0, 0.0, 0.0), (0.0, 1.0, 0.0))
     filter_sigma: float = 0.5
+    images: object = None  # images.ImageSet: image textures and the environment image
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -173,6 +174,10 @@ class Scene:
         tables = C.create_string_buffer(sobol_tables(), abi.RP_SOBOL_TABLE_BYTES)
         keep.append(tables)
         d.sobol_tables = C.cast(tables, C.c_void_p)
+        if self.images is not None:
+            im = self.images.to_c(keep)
+            keep.append(im)
+            d.images = C.pointer(im)
         self._keep = keep
         return d
 
@@ -338,7 +343,7 @@ def cornell_pass_through(width=256, height=256, spp=64, max_depth=8, pane=True, 
     return scene
 
 
-CORNELL_FEATURES = ("point", "spot", "environment", "cauchy")
+CORNELL_FEATURES = ("point", "spot", "environment", "cauchy", "env_image")
 
 
 def cauchy_dielectric(scene, a=1.5, b_um2=0.004):
@@ -362,13 +367,15 @@ def cornell_features(feature, width=32, height=32, spp=4, max_depth=8) -> Scene:
     spot: the area light replaced by a spot light pointing down at the short box;
     environment: the area light replaced by a constant environment seen through the open front;
     cauchy: the tall box made of a smooth dispersive (Cauchy) dielectric, the short box of a
-    rough conductor, under the area light.
+    rough conductor, under the area light;
+    env_image: the area light replaced by an equal-area octahedral sky image (float texels,
+    a bright sun shining in through the open front), sampled by its importance tables.
     """
     if feature not in CORNELL_FEATURES:
         raise ValueError(f"unknown feature {feature!r}")
     scene = cornell_box(width, height, spp, max_depth)
     scene.name = f"cornell_{feature}"
-    if feature in ("point", "spot", "environment"):
+    if feature in ("point", "spot", "environment", "env_image"):
         scene.instances[-1].emission = abi.RP_NONE  # the quad stays, as a black diffuse panel
         scene.emissions = []
     if feature == "point":
@@ -378,6 +385,12 @@ def cornell_features(feature, width=32, height=32, spp=4, max_depth=8) -> Scene:
         scene.positional = [_spot((-0.1, 1.9, 0.4), (0.4, 0.6, 0.2), 20.0, 30.0, blackbody_emission(5000, 8.0))]
     elif feature == "environment":
         scene.environment = (1.5 * blackbody_shape(9000) / blackbody_shape(9000).max()).astype(np.float32)
+    elif feature == "env_image":
+        from . import images
+
+        scene.images = images.ImageSet()
+        scene.images.environment_image = scene.images.add_image(images.sky_image(32, seed=3), wrap=abi.WRAP_CLAMP)
+        scene.images.environment_scale = 1.5
     else:
         conductor = abi.Material()
         conductor.scattering, conductor.kind, conductor.scalar_value = abi.CONDUCTOR, abi.REFLECTANCE_CONSTANT, 1.0

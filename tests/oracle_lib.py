@@ -14,9 +14,19 @@ from rypath_b200 import abi
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
 REF = os.path.join(ROOT, "oracle", "_ref", "libref.so")
+REF_IMAGE = os.path.join(ROOT, "oracle", "_ref", "libref_image.so")
 ROULETTE_KNOWN_ANSWERS = os.path.join(ROOT, "oracle", "_ref", "roulette_known_answers")
 _oracle = None
 _ref = None
+_ref_image = None
+
+
+def _image_args(lib, prefix):
+    vp, u32, sz, fp = C.c_void_p, C.c_uint32, C.c_size_t, C.c_float
+    getattr(lib, prefix + "image_lookup").argtypes = [vp, u32, u32, vp, u32, vp, u32, vp, u32, vp, u32, vp]
+    getattr(lib, prefix + "rgb_spectrum").argtypes = [vp, vp, u32, vp]
+    getattr(lib, prefix + "environment_queries").argtypes = [vp, u32, u32, vp, u32, vp, u32, vp, u32, vp, vp, vp,
+                                                               u32, u32, u32, fp, vp, vp, u32, vp]
 
 
 def oracle():
@@ -28,6 +38,9 @@ def oracle():
         lib.or_scene_create.restype = vp
         lib.or_scene_create.argtypes = [C.POINTER(abi.SceneDesc), C.c_char_p, sz]
         lib.or_scene_destroy.argtypes = [vp]
+        _image_args(lib, "or_")
+        lib.or_environment_tables.argtypes = [vp, u32, vp, vp, u32, vp, vp, vp, vp, sz, C.POINTER(u32),
+                                              C.POINTER(u32), C.POINTER(C.c_double)]
         lib.or_scene_light_count.argtypes = [vp]
         lib.or_scene_light_count.restype = u32
         lib.or_sample.argtypes = [vp, C.POINTER(abi.Request), vp, sz, C.c_int]
@@ -84,6 +97,24 @@ def reference():
         lib.ref_probe_hero_weight.argtypes = [vp, u32, vp]
         _ref = lib
     return _ref
+
+
+def reference_image():
+    """rypath's image shader headers and host image sources (oracle/_ref/libref_image.so), or
+    None when oracle/ref.mk has not built them."""
+    global _ref_image
+    if _ref_image is None:
+        if not os.path.exists(REF_IMAGE):
+            return None
+        lib = C.CDLL(REF_IMAGE)
+        vp, u32, sz = C.c_void_p, C.c_uint32, C.c_size_t
+        _image_args(lib, "ref_")
+        lib.ref_host_image_lookup.argtypes = [vp, u32, vp, vp, u32, vp, vp, u32, vp]
+        lib.ref_host_rgb_spectrum.argtypes = [vp, u32, vp]
+        lib.ref_environment_tables.argtypes = [vp, u32, vp, vp, u32, vp, vp, sz, C.POINTER(u32), C.POINTER(u32),
+                                               C.POINTER(C.c_double)]
+        _ref_image = lib
+    return _ref_image
 
 
 class OracleScene:
