@@ -545,6 +545,21 @@ rp_status rp_cuda_probe_rgb_spectrum(const rp_images *images, const float *queri
                                      float *results, char *diag, size_t diag_capacity);
 rp_status rp_cuda_probe_environment(const rp_images *images, const float *queries, uint32_t count,
                                     float *results, char *diag, size_t diag_capacity);
+/* Texture footprint probe (shaders/texture_footprint.h): per query 48 floats {camera-relative
+ * point[3], geometric normal[3], ray direction[3], one-pixel x and y camera rays[3 + 3], spp
+ * scale, world_from_camera[9], camera_from_world[9] (row-major), minimum dx[3], dy[3], dpdu[3],
+ * dpdv[3], unused[2]} -> 24 floats {primary ok, primary dpdx[3], dpdy[3], approximate dpdx[3],
+ * dpdy[3], derivatives ok, dstdx[2], dstdy[2] (of the primary footprint where it exists),
+ * texture direction of the x ray[3], unused[3]}. */
+rp_status rp_cuda_probe_texture_footprint(const float *queries, uint32_t count, float *results,
+                                          char *diag, size_t diag_capacity);
+/* The minimum one-pixel camera-ray differentials a film of width x height gives the texture
+ * footprints of a scene with image reflectance (prepare_texture_camera_differentials,
+ * src/texture_footprint.cpp:199-232), on the host. */
+rp_status rp_cuda_texture_camera_differentials(const rp_camera *camera, uint32_t width,
+                                               uint32_t height, float *minimum_dx,
+                                               float *minimum_dy, char *diag,
+                                               size_t diag_capacity);
 /* The environment image's importance tables as scene creation builds them, on the host (no
  * device is used): the full then the compensated table (each a marginal CDF and one
  * conditional CDF per row, width + 1 floats apiece; build_environment_sampling,

@@ -109,6 +109,13 @@ void or_environment_queries(const void *textures, uint32_t texture_count, uint32
                             float scale, const float *env_from_world, const float *queries, uint32_t count,
                             float *results);
 
+/* Texture footprints (shaders/texture_footprint.h) in the layout of oracle/_ref's
+ * ref_texture_footprint (48 floats -> 24), and the texture camera's minimum differentials
+ * (src/texture_footprint.cpp:199-232; 0, or -1 when refused). */
+void or_texture_footprint(const float *queries, uint32_t count, float *results);
+int or_texture_camera_differentials(const float *corner, const float *dx, const float *dy, uint32_t width,
+                                    uint32_t height, float *out);
+
 #ifdef __cplusplus
 }
 #endif

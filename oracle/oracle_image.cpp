@@ -150,10 +150,81 @@ std::string build_environment_tables(Images &im) {
     return {};
 }
 
-std::string load_images(const rp_images *in, Images &out) {
+std::string texture_camera_differentials(F3 corner, F3 dx, F3 dy, u32 width, u32 height, F3 &min_dx, F3 &min_dy) {
+    if (width == 0 || height == 0)
+        return "Texture camera raster extent must be positive";
+    using V = std::array<double, 3>;
+    const V c{corner.x, corner.y, corner.z}, u{dx.x, dx.y, dx.z}, v{dy.x, dy.y, dy.z};
+    const auto dotd = [](const V &a, const V &b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+    const auto unit = [](V a, V &out) {
+        const double len = std::hypot(a[0], a[1], a[2]);
+        if (!(len > 0 && std::isfinite(len)))
+            return false;
+        for (auto &x : a)
+            x /= len;
+        out = a;
+        return true;
+    };
+    const auto direction = [&](double x, double y, V &out) {
+        V d;
+        for (int i = 0; i < 3; ++i) {
+            d[i] = std::fma(y, v[i], std::fma(x, u[i], c[i]));
+            if (!(std::abs(d[i]) <= double(FLT_MAX)))
+                return false;
+        }
+        return unit(d, out);
+    };
+    const double px = 1. / width, py = 1. / height;
+    V best_x{}, best_y{};
+    double len_x = INFINITY, len_y = INFINITY;
+    for (unsigned i = 0; i < 512; ++i) {
+        const double t = double(i) / 511;
+        V d, xr, yr;
+        if (!direction(t, t, d) || !direction(t + px, t, xr) || !direction(t, t + py, yr))
+            return "Texture camera differential ray is unrepresentable or zero";
+        // PBRT's CoordinateSystem of the ray direction (Duff et al. 2017)
+        const double sign = std::copysign(1., d[2]);
+        const double a = -1 / (sign + d[2]);
+        const double b = d[0] * d[1] * a;
+        const V b0{1 + sign * d[0] * d[0] * a, sign * b, -sign * d[0]}, b1{b, sign + d[1] * d[1] * a, -d[1]};
+        const auto local = [&](const V &r) { return V{dotd(b0, r), dotd(b1, r), dotd(d, r)}; };
+        const V base = local(d);
+        V lx, ly;
+        if (!unit(local(xr), lx) || !unit(local(yr), ly))
+            return "Texture camera differential ray collapses in its local frame";
+        const V ex{lx[0] - base[0], lx[1] - base[1], lx[2] - base[2]}, ey{ly[0] - base[0], ly[1] - base[1], ly[2] - base[2]};
+        if (dotd(ex, ex) < len_x) {
+            len_x = dotd(ex, ex);
+            best_x = ex;
+        }
+        if (dotd(ey, ey) < len_y) {
+            len_y = dotd(ey, ey);
+            best_y = ey;
+        }
+    }
+    min_dx = {float(best_x[0]), float(best_x[1]), float(best_x[2])};
+    min_dy = {float(best_y[0]), float(best_y[1]), float(best_y[2])};
+    return {};
+}
+
+std::string load_images(const rp_images *in, u32 instance_count, Images &out) {
     out = Images{};
     if (!in)
         return {};
+    for (u32 i = 0; i < in->uv_count; ++i)
+        out.uvs.push_back({in->uvs[2 * i], in->uvs[2 * i + 1]});
+    for (u32 i = 0; i < in->frame_count; ++i) {
+        const float *f = in->frames + 6 * i;
+        out.frames.push_back({F3{f[0], f[1], f[2]}, F3{f[3], f[4], f[5]}});
+    }
+    out.inst_uv_begin.assign(instance_count, RP_NONE);
+    out.inst_frame_begin.assign(instance_count, RP_NONE);
+    if (in->instance_uv_begin)
+        out.inst_uv_begin.assign(in->instance_uv_begin, in->instance_uv_begin + instance_count);
+    if (in->instance_frame_begin)
+        out.inst_frame_begin.assign(in->instance_frame_begin, in->instance_frame_begin + instance_count);
+    std::copy(in->world_from_camera, in->world_from_camera + 9, out.world_from_camera);
+    std::copy(in->camera_from_world, in->camera_from_world + 9, out.camera_from_world);
     out.textures.assign(in->textures, in->textures + in->texture_count);
     out.levels.assign(in->levels, in->levels + in->level_count);
     out.texels.assign(in->texels, in->texels + in->texel_word_count);
@@ -285,6 +356,39 @@ void or_environment_queries(const void *textures, uint32_t texture_count, uint32
         o[10] = w2.y;
         o[11] = w2.z;
     }
+}
+
+void or_texture_footprint(const float *q, uint32_t count, float *out) {
+    using oracle::F3;
+    for (uint32_t i = 0; i < count; ++i) {
+        const float *a = q + 48 * i;
+        float *o = out + 24 * i;
+        const F3 rp{a[0], a[1], a[2]}, n{a[3], a[4], a[5]}, d{a[6], a[7], a[8]}, rx{a[9], a[10], a[11]},
+            ry{a[12], a[13], a[14]};
+        F3 pdx, pdy, adx, ady;
+        const bool primary = oracle::texture_primary_dp(rp, n, d, rx, ry, a[15], pdx, pdy);
+        oracle::texture_approximate_dp(rp, n, a + 16, a + 25, F3{a[34], a[35], a[36]}, F3{a[37], a[38], a[39]}, a[15],
+                                       adx, ady);
+        oracle::F2 sx, sy;
+        const bool ok = oracle::texture_uv_derivatives(F3{a[40], a[41], a[42]}, F3{a[43], a[44], a[45]},
+                                                       primary ? pdx : adx, primary ? pdy : ady, sx, sy);
+        const F3 td = oracle::texture_direction(rx);
+        const float v[24] = {primary ? 1.f : 0.f, pdx.x, pdx.y, pdx.z, pdy.x, pdy.y, pdy.z, adx.x, adx.y, adx.z,
+                             ady.x, ady.y, ady.z, ok ? 1.f : 0.f, sx.x, sx.y, sy.x, sy.y, td.x, td.y, td.z, 0, 0, 0};
+        std::copy(v, v + 24, o);
+    }
+}
+
+int or_texture_camera_differentials(const float *corner, const float *dx, const float *dy, uint32_t width,
+                                    uint32_t height, float *out) {
+    oracle::F3 mx, my;
+    if (!oracle::texture_camera_differentials({corner[0], corner[1], corner[2]}, {dx[0], dx[1], dx[2]},
+                                              {dy[0], dy[1], dy[2]}, width, height, mx, my)
+             .empty())
+        return -1;
+    const float v[6] = {mx.x, mx.y, mx.z, my.x, my.y, my.z};
+    std::copy(v, v + 6, out);
+    return 0;
 }
 
 } // extern "C"

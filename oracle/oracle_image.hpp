@@ -34,6 +34,12 @@ struct Images {
     std::vector<float> env_cdf;
     u32 env_width = 0, env_comp_offset = 0;
     double env_power = 0; // mean RGB illuminant power of the environment texels
+    // texture coordinates: per-vertex uvs, per-triangle tangents (dpdu, dpdv), per-instance
+    // first uv and first frame (RP_NONE: default uvs / no frames), the texture camera
+    std::vector<F2> uvs;
+    std::vector<std::array<F3, 2>> frames;
+    std::vector<u32> inst_uv_begin, inst_frame_begin;
+    float world_from_camera[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, camera_from_world[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
 };
 
 // shaders/image_texture.h:14-27
@@ -431,10 +437,106 @@ inline bool env_image_sample(const Images &im, float ux, float uy, bool compensa
     return std::isfinite(pdf) && pdf > 0;
 }
 
+// ---------------------------------------------------------------- texture footprints
+// src/metal_render.mm:1962-1963 (spp_scale; shaders/texture_footprint.h:10-12 in binary32)
+inline float texture_differential_scale(uint64_t total_spp) {
+    return float(std::max(0.125, 1.0 / std::sqrt(double(total_spp))));
+}
+// shaders/texture_footprint.h:14-20
+inline F3 texture_direction(F3 d) {
+    const float scale = std::max(std::fabs(d.x), std::max(std::fabs(d.y), std::fabs(d.z)));
+    if (!(scale > 0.0f) || !finite3(d))
+        return {NAN, NAN, NAN};
+    return env_unit(F3{d.x / scale, d.y / scale, d.z / scale});
+}
+// shaders/texture_footprint.h:22-38
+inline bool texture_primary_dp(F3 rel, F3 n, F3 dir, F3 xr, F3 yr, float spp_scale, F3 &dpdx, F3 &dpdy) {
+    const F3 rx = dir + spp_scale * (texture_direction(xr) - dir);
+    const F3 ry = dir + spp_scale * (texture_direction(yr) - dir);
+    const float nx = dot(n, rx), ny = dot(n, ry);
+    if (nx == 0.0f || ny == 0.0f || !std::isfinite(nx) || !std::isfinite(ny))
+        return false;
+    const float plane = dot(n, rel);
+    dpdx = (plane / nx) * rx - rel;
+    dpdy = (plane / ny) * ry - rel;
+    return true;
+}
+// shaders/texture_footprint.h:40-43
+inline F3 texture_reflect(F3 x, F3 normal) { return x - ((2.0f * dot(normal, x)) / dot(normal, normal)) * normal; }
+// row-major matrix times vector, summing columns in order (Metal's float3x3 product)
+inline F3 texture_apply(const float *m, F3 v) {
+    const F3 c0{m[0], m[3], m[6]}, c1{m[1], m[4], m[7]}, c2{m[2], m[5], m[8]};
+    return (c0 * v.x + c1 * v.y) + c2 * v.z;
+}
+inline F3 texture_apply_transposed(const float *m, F3 v) {
+    const F3 c0{m[0], m[1], m[2]}, c1{m[3], m[4], m[5]}, c2{m[6], m[7], m[8]};
+    return (c0 * v.x + c1 * v.y) + c2 * v.z;
+}
+// shaders/texture_footprint.h:45-58
+inline F3 texture_approximate_axis(F3 p_down_z, F3 n_down_z, F3 delta, F3 u, F3 v, const float *world_from_camera,
+                                   float spp_scale) {
+    const F3 ray = F3{0, 0, 1} + delta;
+    const float denom = dot(n_down_z, ray);
+    if (denom == 0.0f)
+        return {};
+    const F3 offset = ((n_down_z.z * p_down_z.z) / denom) * ray - p_down_z;
+    const F3 dp = spp_scale * texture_apply(world_from_camera, texture_reflect(texture_reflect(offset, v), u));
+    return finite3(dp) ? dp : F3{};
+}
+// shaders/texture_footprint.h:60-86 (PBRT's Camera::Approximate_dp_dxy)
+inline void texture_approximate_dp(F3 rel, F3 n, const float *world_from_camera, const float *camera_from_world,
+                                   F3 min_dx, F3 min_dy, float spp_scale, F3 &dpdx, F3 &dpdy) {
+    const F3 p_camera = texture_apply(camera_from_world, rel);
+    const F3 direction = texture_direction(p_camera);
+    if (!finite3(direction)) {
+        dpdx = dpdy = F3{};
+        return;
+    }
+    const F3 z{0, 0, 1};
+    const F3 ref = std::fabs(direction.x) < 0.72f ? F3{1, 0, 0} : F3{0, 1, 0};
+    const F3 u = ref - direction, v = ref - z;
+    const F3 p_down_z = texture_reflect(texture_reflect(p_camera, u), v);
+    const F3 n_camera = texture_apply_transposed(world_from_camera, n);
+    const F3 n_down_z = texture_reflect(texture_reflect(n_camera, u), v);
+    dpdx = texture_approximate_axis(p_down_z, n_down_z, min_dx, u, v, world_from_camera, spp_scale);
+    dpdy = texture_approximate_axis(p_down_z, n_down_z, min_dy, u, v, world_from_camera, spp_scale);
+}
+// shaders/texture_footprint.h:139-142
+inline float texture_difference_of_products(float a, float b, float c, float d) {
+    const float cd = c * d;
+    return std::fma(a, b, -cd) + std::fma(-c, d, cd);
+}
+// shaders/texture_footprint.h:144-159
+inline float texture_sanitize(float d) { return std::isfinite(d) ? std::clamp(d, -1e8f, 1e8f) : 0.0f; }
+inline F2 texture_solve_axis(F3 dpdu, F3 dpdv, F3 dp, float aa, float ab, float bb, float inv_det) {
+    const float u = dot(dpdu, dp), v = dot(dpdv, dp);
+    return {texture_sanitize(inv_det * texture_difference_of_products(bb, u, ab, v)),
+            texture_sanitize(inv_det * texture_difference_of_products(aa, v, ab, u))};
+}
+// shaders/texture_footprint.h:161-185
+inline bool texture_uv_derivatives(F3 dpdu, F3 dpdv, F3 dpdx, F3 dpdy, F2 &dstdx, F2 &dstdy) {
+    if (!finite3(dpdu) || !finite3(dpdv))
+        return false;
+    const float aa = dot(dpdu, dpdu), ab = dot(dpdu, dpdv), bb = dot(dpdv, dpdv);
+    const float det = texture_difference_of_products(aa, bb, ab, ab);
+    const float inv_det = 1.0f / det;
+    if (!std::isfinite(inv_det)) {
+        dstdx = dstdy = F2{};
+        return true;
+    }
+    dstdx = texture_solve_axis(dpdu, dpdv, dpdx, aa, ab, bb, inv_det);
+    dstdy = texture_solve_axis(dpdu, dpdv, dpdy, aa, ab, bb, inv_det);
+    return true;
+}
+// The smallest one-pixel change of a camera ray's direction, over 512 rays along the film's
+// diagonal, in each ray's local frame (src/texture_footprint.cpp:199-232, PBRT's
+// Camera::FindMinimumDifferentials); empty on success.
+std::string texture_camera_differentials(F3 corner, F3 dx, F3 dy, u32 width, u32 height, F3 &min_dx, F3 &min_dy);
+
 // The environment importance tables and the image's mean illuminant power
 // (src/environment_sampling.cpp:20-115, src/light_sampling.cpp:28-95); empty on success.
 std::string build_environment_tables(Images &im);
 // Copy and check a scene description's images; empty on success.
-std::string load_images(const rp_images *in, Images &out);
+std::string load_images(const rp_images *in, u32 instance_count, Images &out);
 
 } // namespace oracle

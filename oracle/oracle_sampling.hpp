@@ -13,6 +13,10 @@ struct Params {
     u32 seed_low, seed_high, sampler, randomization, m, emergency_limit, max_depth;
     u32 log_spp;        // ZSobol: floor(log2(total samples))
     u32 boundary_limit; // pass-through crossings allowed between two vertices
+    // texture footprints (scenes with image reflectance): the request's differential scale and
+    // the camera's minimum one-pixel differentials (src/metal_render.mm:1940-1963)
+    float tex_spp_scale = 1;
+    F3 tex_min_dx{}, tex_min_dy{};
 };
 
 struct Sample {
@@ -221,6 +225,118 @@ inline void primary_ray(const Scene &s, const Params &p, const Sample &smp, F3 &
     d = normalize3(dd / scale);
 }
 
+// shaders/render.metal:479-501 (texture_camera_rays): the camera directions one pixel right and
+// one pixel down of the sample's film position, through the lens sample's focus shift; and the
+// lens sample's aperture offset (lens_offset, :390-392)
+inline void texture_camera_rays(const Scene &s, const Params &p, const Sample &smp, F3 &rx, F3 &ry, F3 &lens) {
+    float ux, uy;
+    if (p.sampler == RP_SAMPLER_SOBOL) {
+        ux = sobol_camera_uniform(smp.words[0], p.m, smp.pixel % p.width);
+        uy = sobol_camera_uniform(smp.words[1], p.m, smp.pixel / p.width);
+    } else {
+        ux = sample_uniform(p, smp.words[0]);
+        uy = sample_uniform(p, smp.words[1]);
+    }
+    const bool centered = s.filter_kind != RP_FILTER_BOX || s.filter_x != 0.5f || s.filter_y != 0.5f;
+    F3 dd;
+    if (centered) {
+        const float ox = s.filter_kind == RP_FILTER_GAUSSIAN   ? smp.filter_offsets[0]
+                         : s.filter_kind == RP_FILTER_TRIANGLE ? triangle_offset(ux, s.filter_x)
+                                                               : (2.0f * ux - 1.0f) * s.filter_x;
+        const float oy = s.filter_kind == RP_FILTER_GAUSSIAN   ? smp.filter_offsets[1]
+                         : s.filter_kind == RP_FILTER_TRIANGLE ? triangle_offset(uy, s.filter_y)
+                                                               : (2.0f * uy - 1.0f) * s.filter_y;
+        const float x = ((float(smp.pixel % p.width) + 0.5f) + ox) / float(p.width);
+        const float y = ((float(smp.pixel / p.width) + 0.5f) + oy) / float(p.height);
+        dd = fma3(F3{y, y, y}, s.up, fma3(F3{x, x, x}, s.right, s.forward));
+    } else {
+        const float x = (float(smp.pixel % p.width) + ux) / float(p.width);
+        const float y = (float(smp.pixel / p.width) + uy) / float(p.height);
+        dd = s.forward + x * s.right + y * s.up;
+    }
+    rx = dd + s.right / float(p.width);
+    ry = dd + s.up / float(p.height);
+    lens = F3{0, 0, 0};
+    if (s.lens_radius > 0) {
+        const float lx = 2.0f * sample_uniform(p, smp.lens_words[0]) - 1.0f;
+        const float ly = 2.0f * sample_uniform(p, smp.lens_words[1]) - 1.0f;
+        if (!(lx == 0 && ly == 0)) {
+            const float pi = 3.14159265358979323846f;
+            float radius, theta;
+            if (std::fabs(lx) > std::fabs(ly)) {
+                radius = lx;
+                theta = (pi / 4.0f) * (ly / lx);
+            } else {
+                radius = ly;
+                theta = pi / 2.0f - (pi / 4.0f) * (lx / ly);
+            }
+            const float r = s.lens_radius * radius;
+            const F3 ideal = (r * std::cos(theta)) * s.lens_x + (r * std::sin(theta)) * s.lens_y;
+            lens = (s.origin + ideal) - s.origin;
+        }
+        const F3 shift = lens / s.focal_distance;
+        rx = rx - shift;
+        ry = ry - shift;
+    }
+}
+
+// shaders/render.metal:1312-1408 (surface_texture_context) for a triangle hit (b1, b2) of
+// instance `inst`, local triangle `local`: the texture coordinates and their screen-space
+// derivatives.  scatterings: the path's scattering events so far (0 at the primary hit, which
+// uses the camera's ray differentials).  False when the inputs are invalid.
+inline bool texture_context(const Scene &s, const Params &p, const Sample &smp, u32 inst, u32 local, float b1,
+                            float b2, F3 geometric_normal, F3 primary_direction, u32 scatterings, F2 &st, F2 &dstdx,
+                            F2 &dstdy) {
+    const Instance &in = s.instances[inst];
+    const Images &im = s.images;
+    const auto &tri = s.triangles[in.triangle_begin + local];
+    const F3 p0 = s.positions[in.vertex_begin + tri[0]], p1 = s.positions[in.vertex_begin + tri[1]],
+             p2 = s.positions[in.vertex_begin + tri[2]];
+    const F3 local_p = fma3(F3{b2, b2, b2}, p2 - p0, fma3(F3{b1, b1, b1}, p1 - p0, p0));
+    F2 uv[3] = {{0, 0}, {1, 0}, {1, 1}};
+    const u32 uv_begin = im.inst_uv_begin.empty() ? RP_NONE : im.inst_uv_begin[inst];
+    if (uv_begin != RP_NONE) {
+        const u32 count = u32(im.uvs.size());
+        for (int k = 0; k < 3; ++k) {
+            if (uv_begin >= count || tri[k] >= count - uv_begin)
+                return false;
+            uv[k] = im.uvs[uv_begin + tri[k]];
+            if (!std::isfinite(uv[k].x) || !std::isfinite(uv[k].y))
+                return false;
+        }
+    }
+    const float w0 = 1.0f - (b1 + b2);
+    st = {(w0 * uv[0].x + b1 * uv[1].x) + b2 * uv[2].x, (w0 * uv[0].y + b1 * uv[1].y) + b2 * uv[2].y};
+    const u32 frame_begin = im.inst_frame_begin.empty() ? RP_NONE : im.inst_frame_begin[inst];
+    const u32 frame_count = u32(im.frames.size());
+    if (!std::isfinite(st.x) || !std::isfinite(st.y) || frame_begin >= frame_count || local >= frame_count - frame_begin)
+        return false;
+    const F3 dpdu = im.frames[frame_begin + local][0], dpdv = im.frames[frame_begin + local][1];
+    // texture_world_vector (:1139-1143) of the local point, plus the translation less the camera
+    const auto world_vector = [&](F3 v) {
+        return F3{dot(F3{in.m[0], in.m[1], in.m[2]}, v), dot(F3{in.m[4], in.m[5], in.m[6]}, v),
+                  dot(F3{in.m[8], in.m[9], in.m[10]}, v)};
+    };
+    const F3 relative_p = world_vector(local_p) + (F3{in.m[3], in.m[7], in.m[11]} - s.origin);
+    if (!finite3(relative_p))
+        return false;
+    F3 dpdx{}, dpdy{};
+    bool primary = false;
+    if (scatterings == 0) {
+        F3 rx, ry, lens;
+        texture_camera_rays(s, p, smp, rx, ry, lens);
+        if (!finite3(rx) || !finite3(ry))
+            return false;
+        const F3 lens_relative = s.lens_radius > 0 ? relative_p - lens : relative_p;
+        primary = texture_primary_dp(lens_relative, geometric_normal, primary_direction, rx, ry, p.tex_spp_scale,
+                                     dpdx, dpdy);
+    }
+    if (!primary)
+        texture_approximate_dp(relative_p, geometric_normal, im.world_from_camera, im.camera_from_world, p.tex_min_dx,
+                               p.tex_min_dy, p.tex_spp_scale, dpdx, dpdy);
+    return texture_uv_derivatives(dpdu, dpdv, dpdx, dpdy, dstdx, dstdy);
+}
+
 // ---------------------------------------------------------------- positional lights
 // shaders/render.metal:654-657, :682-697
 inline bool normal_or_zero(float v) {
@@ -297,6 +413,10 @@ inline Params make_params(const Scene &s, const rp_request &r) {
     p.emergency_limit = r.emergency_limit ? r.emergency_limit : 1024;
     p.max_depth = s.max_depth;
     p.boundary_limit = r.boundary_limit ? r.boundary_limit : 4096; // medium_boundary_limit, src/render.hpp:26
+    if (s.textured) {
+        p.tex_spp_scale = texture_differential_scale(r.total_samples);
+        texture_camera_differentials(s.forward, s.right, s.up, r.width, r.height, p.tex_min_dx, p.tex_min_dy);
+    }
     return p;
 }
 

@@ -297,7 +297,9 @@ bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error) {
         s.materials.push_back({m.scattering, m.kind, m.knot_begin, m.knot_count, m.scalar_value,
                                m.eta_begin, m.eta_count, m.k_begin, m.k_count, m.optical_extensions,
                                m.u_roughness, m.v_roughness, m.remap_roughness, m.first_material,
-                               m.second_material, m.mix_amount});
+                               m.second_material, m.mix_amount, m.image_texture});
+        if (m.scattering == RP_DIFFUSE && m.kind == RP_REFLECTANCE_IMAGE)
+            s.textured = true;
     }
     for (u32 i = 0; i < d.knot_count; ++i)
         s.knots.push_back({d.knots[i].wavelength, d.knots[i].value});
@@ -323,7 +325,7 @@ bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error) {
         s.has_environment = std::any_of(s.environment.begin(), s.environment.end(),
                                         [](float v) { return v > 0; });
     }
-    if (const std::string images = load_images(d.images, s.images); !images.empty()) {
+    if (const std::string images = load_images(d.images, d.instance_count, s.images); !images.empty()) {
         error = images;
         return false;
     }

@@ -68,6 +68,7 @@ struct Material {
     u32 remap;
     u32 first = RP_NONE, second = RP_NONE; // mix children (MaterialAuxiliary, src/render_wire.h:159-161)
     float mix_amount = 0;
+    u32 image_texture = RP_NONE; // RP_REFLECTANCE_IMAGE
 };
 struct Positional {
     F3 position;
@@ -92,6 +93,7 @@ struct Scene {
     std::array<float, 471> environment{};
     bool has_environment = false;
     Images images; // image textures and the environment image (env_image RP_NONE: none)
+    bool textured = false; // a diffuse material reads an image
     // media (scalar transport)
     std::vector<Medium> media;
     u32 camera_medium = RP_NONE, transport = RP_TRANSPORT_HERO;

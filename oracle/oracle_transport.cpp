@@ -38,10 +38,13 @@ static F3 offset(const Vertex &v, F3 direction) {
     return round_out(v.point.position + dot(fabs3(n), v.point.error) * n, n);
 }
 
-// shaders/packet_walk.h:22-57 (packet_reflectance) for sampled/constant/blackbody
-static bool reflectance(const Scene &s, const Material &m, float w, float &rho) {
+// shaders/packet_walk.h:22-57 (packet_reflectance) for sampled/constant/blackbody/image; image:
+// the hit's filtered, scaled linear RGB
+static bool reflectance(const Scene &s, const Material &m, float w, const Rgb *image, float &rho) {
     if (m.scattering != 0) {
         rho = 1;
+    } else if (m.kind == RP_REFLECTANCE_IMAGE && image && m.image_texture < s.images.textures.size()) {
+        rho = srgb_spectrum(s.images.rgb_table.data(), *image, w);
     } else if (m.kind == RP_REFLECTANCE_KNOTS && m.knot_count >= 2 &&
                m.knot_begin <= s.knots.size() && m.knot_count <= s.knots.size() - m.knot_begin) {
         rho = pbrt_reflectance(s.knots.data() + m.knot_begin, m.knot_count, w);
@@ -55,7 +58,7 @@ static bool reflectance(const Scene &s, const Material &m, float w, float &rho) 
 }
 // shaders/hero_current_bsdf.h:72-101 with prepare_scattering (shaders/render.metal:2079-2160)
 static bool prepare_bsdf(const Scene &s, const Material &m, const Wavelengths &l, u32 mask,
-                         HeroBsdf &out) {
+                         HeroBsdf &out, const Rgb *image = nullptr) {
     out = HeroBsdf{};
     out.active_mask = mask;
     for (int k = 0; k < 4; ++k) {
@@ -66,7 +69,7 @@ static bool prepare_bsdf(const Scene &s, const Material &m, const Wavelengths &l
             continue;
         }
         float rho;
-        if (!reflectance(s, m, l.lambda[k], rho))
+        if (!reflectance(s, m, l.lambda[k], image, rho))
             return false;
         if (m.scattering == 0) {
             lane.reflectance = rho;
@@ -495,10 +498,29 @@ static void hero_step(const Ctx &c, LaneState &st) {
         }
         v.material = material_index;
         const Material &material = s.materials[material_index];
+        // :147-163 and shaders/packet_walk.h:39-49: an image reflectance reads the texture at the
+        // hit's footprint (the context of its root material; here, of the image material)
+        Rgb image_rgb;
+        const Rgb *image = nullptr;
+        if (material.scattering == RP_DIFFUSE && material.kind == RP_REFLECTANCE_IMAGE &&
+            material.image_texture < s.images.textures.size()) {
+            F2 uvst, dstdx, dstdy;
+            if (!texture_context(s, p, smp, inst, local, hit.b1, hit.b2, v.point.geometric_normal, rd, count - 1,
+                                 uvst, dstdx, dstdy)) {
+                smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
+                break;
+            }
+            const rp_image_texture &t = s.images.textures[material.image_texture];
+            image_rgb = image_lookup_standard(s.images, t, uvst, dstdx, dstdy, false, false);
+            image_rgb = {image_rgb.r * t.scale, image_rgb.g * t.scale, image_rgb.b * t.scale};
+            if (t.invert)
+                image_rgb = {1 - image_rgb.r, 1 - image_rgb.g, 1 - image_rgb.b};
+            image = &image_rgb;
+        }
         F3 dpdu, dpdv;
         coordinate_system(v.point.shading_normal, dpdu, dpdv);
         if (!scattering_frame(v.point.shading_normal, dpdu, v.frame) ||
-            !prepare_bsdf(s, material, l, st.hero.active_mask, v.bsdf)) {
+            !prepare_bsdf(s, material, l, st.hero.active_mask, v.bsdf, image)) {
             smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
             break;
         }

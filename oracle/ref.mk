@@ -18,6 +18,7 @@ SRC := $(HERE)ref_probe.cpp $(HERE)ref_hero_probe.cpp $(REF)/src/light_sampling.
 IMAGE_SRC := $(HERE)ref_image_probe.cpp $(HERE)ref_image_host.cpp $(REF)/src/image_texture.cpp \
 	$(REF)/src/environment_sampling.cpp $(REF)/src/rgb_spectrum.cpp $(REF)/src/pbrt_spectra.cpp \
 	$(REF)/src/light_sampling.cpp $(REF)/src/png_allocator.cpp $(REF)/third_party/lodepng/lodepng.cpp \
+	$(REF)/src/texture_footprint.cpp $(REF)/src/geometry.cpp $(REF)/src/bilinear.cpp \
 	$(REF)/third_party/stb/jpeg.cpp
 IMAGE_FLAGS := $(FLAGS) -I$(REF)/third_party/stb -I$(REF)/third_party/lodepng -I$(REF)/third_party/pbrt \
 	-DRYPATH_SRGB_BIN='"$(REF)/third_party/pbrt/srgb.bin"'

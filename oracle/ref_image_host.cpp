@@ -9,6 +9,7 @@
 #include "light_sampling.hpp"
 #include "render_wire.h"
 #include "rgb_spectrum.hpp"
+#include "texture_footprint.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -130,6 +131,21 @@ int ref_environment_tables(const void *textures, uint32_t index, const void *lev
     *compensated_offset = tables->compensated_offset;
     const auto p = rypath::light_image_power(*image);
     *power = p ? *p : -1;
+    return 0;
+}
+
+// prepare_texture_camera_differentials (src/texture_footprint.cpp:199-232): the raster corner
+// and full-extent steps of a PBRT camera and the film size -> minimum dx[3], dy[3]; 0, or -1
+// with rypath's diagnostic refused.
+int ref_texture_camera_differentials(const float *corner, const float *dx, const float *dy, uint32_t width,
+                                     uint32_t height, float *out) {
+    rypath::TextureCameraDifferentials d;
+    const std::string err = rypath::prepare_texture_camera_differentials(
+        {corner[0], corner[1], corner[2]}, {dx[0], dx[1], dx[2]}, {dy[0], dy[1], dy[2]}, width, height, d);
+    if (!err.empty())
+        return -1;
+    const float v[6] = {d.minimum_dx.x, d.minimum_dx.y, d.minimum_dx.z, d.minimum_dy.x, d.minimum_dy.y, d.minimum_dy.z};
+    std::memcpy(out, v, sizeof(v));
     return 0;
 }
 

@@ -1,5 +1,5 @@
 // Test infrastructure only: rypath's image shader headers (shaders/image_texture.h,
-// shaders/image_lighting.h) compiled from the checkout (oracle/ref.mk), behind the host
+// shaders/image_lighting.h, shaders/texture_footprint.h) compiled from the checkout (oracle/ref.mk), behind the host
 // stand-in for <metal_stdlib>, as a C ABI that pins the oracle's restatement.  The code of this file is
 // only the marshalling: wire records in, results out.  rypath's host image sources are bound in
 // ref_image_host.cpp (a separate unit: the stand-in's address-space macros would rewrite
@@ -11,6 +11,7 @@
 #define constant const
 #include "render_wire.h"
 #include "image_lighting.h"
+#include "texture_footprint.h"
 
 #include <cstdint>
 
@@ -111,6 +112,36 @@ void ref_environment_queries(const void *textures, uint32_t texture_count, uint3
         o[9] = w2.x;
         o[10] = w2.y;
         o[11] = w2.z;
+    }
+}
+
+// Texture footprints through shaders/texture_footprint.h: per query 48 floats {relative p[3],
+// n[3], ray direction[3], x ray[3], y ray[3], spp scale, world_from_camera[9] (row-major),
+// camera_from_world[9], minimum dx[3], minimum dy[3], dpdu[3], dpdv[3], unused[2]} -> 24
+// floats {primary ok, primary dpdx[3], dpdy[3], approximate dpdx[3], dpdy[3], derivatives ok,
+// dstdx[2], dstdy[2] (of the primary footprint when it exists, else the approximate one),
+// texture direction of the x ray[3], unused[3]}.
+void ref_texture_footprint(const float *q, uint32_t count, float *out) {
+    const auto matrix = [](const float *m) {
+        return float3x3(float3(m[0], m[3], m[6]), float3(m[1], m[4], m[7]), float3(m[2], m[5], m[8]));
+    };
+    for (uint32_t i = 0; i < count; ++i) {
+        const float *a = q + 48 * i;
+        float *o = out + 24 * i;
+        const float3 rp(a[0], a[1], a[2]), n(a[3], a[4], a[5]), d(a[6], a[7], a[8]);
+        const float3 rx(a[9], a[10], a[11]), ry(a[12], a[13], a[14]);
+        float3 pdx(0), pdy(0), adx(0), ady(0);
+        const bool primary = rypath_texture_primary_dp(rp, n, d, rx, ry, a[15], pdx, pdy);
+        rypath_texture_approximate_dp(rp, n, matrix(a + 16), matrix(a + 25), float3(a[34], a[35], a[36]),
+                                      float3(a[37], a[38], a[39]), a[15], adx, ady);
+        float2 sx(0), sy(0);
+        const bool ok = rypath_texture_uv_derivatives(float3(a[40], a[41], a[42]), float3(a[43], a[44], a[45]),
+                                                      primary ? pdx : adx, primary ? pdy : ady, sx, sy);
+        const float3 td = rypath_texture_direction(rx);
+        const float v[24] = {primary ? 1.f : 0.f, pdx.x, pdx.y, pdx.z, pdy.x, pdy.y, pdy.z, adx.x, adx.y, adx.z,
+                             ady.x, ady.y, ady.z, ok ? 1.f : 0.f, sx.x, sx.y, sy.x, sy.y, td.x, td.y, td.z, 0, 0, 0};
+        for (int k = 0; k < 24; ++k)
+            o[k] = v[k];
     }
 }
 

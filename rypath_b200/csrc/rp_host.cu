@@ -717,7 +717,8 @@ template <class T> T *dupload(std::vector<void *> &owned, const T *src, size_t c
 // Upload a description's images in their wire layout; an environment image also gets its
 // importance tables and its light power (mean RGB illuminant power times its scale; -1 when
 // there is no environment image).
-void upload_images(const rp_images *im, DImages &g, std::vector<void *> &own, cudaStream_t stm, double &env_power) {
+void upload_images(const rp_images *im, u32 instances, DImages &g, std::vector<void *> &own, cudaStream_t stm,
+                   double &env_power) {
     static_assert(sizeof(DImageTexture) == sizeof(rp_image_texture) && sizeof(DLevel) == sizeof(rp_texture_level));
     g = DImages{};
     g.env_image = kNone;
@@ -732,6 +733,16 @@ void upload_images(const rp_images *im, DImages &g, std::vector<void *> &own, cu
     g.level_count = im->level_count;
     g.texel_word_count = im->texel_word_count;
     g.transfer_count = im->transfer_count;
+    g.uvs = dupload(own, reinterpret_cast<const float2 *>(im->uvs), im->uv_count, stm);
+    g.uv_count = im->uv_count;
+    g.frames = dupload(own, im->frames, size_t(6) * im->frame_count, stm);
+    g.frame_count = im->frame_count;
+    if (im->instance_uv_begin)
+        g.inst_uv_begin = dupload(own, im->instance_uv_begin, instances, stm);
+    if (im->instance_frame_begin)
+        g.inst_frame_begin = dupload(own, im->instance_frame_begin, instances, stm);
+    memcpy(g.world_from_camera, im->world_from_camera, sizeof(g.world_from_camera));
+    memcpy(g.camera_from_world, im->camera_from_world, sizeof(g.camera_from_world));
     if (im->texture_count) {
         g.rgb_table = dupload(own, im->rgb_table, RP_RGB_TABLE_FLOATS, stm);
         g.illuminant = dupload(own, im->illuminant, 471, stm);
@@ -781,7 +792,7 @@ rp_status image_probe(const rp_images *images, const float *queries, u32 count, 
         } fr{own};
         DImages g;
         double power;
-        upload_images(images, g, own, nullptr, power);
+        upload_images(images, 0, g, own, nullptr, power);
         const float *q = dupload(own, queries, size_t(in_per) * count, nullptr);
         float *r = dalloc<float>(own, size_t(out_per) * count);
         launch(g, q, r);
@@ -881,6 +892,7 @@ struct rp_scene {
     u32 tree_levels = 0;     // most internal nodes on a root-to-leaf path of the LBVH
     u32 wide_levels = 0;     // levels of the compressed 8-wide traversal tree
     bool resolve = false;    // hero scene with pass-through or mix-root instances
+    u32 tex_width = 0, tex_height = 0; // film size the texture camera differentials were found for
     float4 *world = nullptr; // world-space triangle vertices in original order
     BNode *nodes = nullptr;  // traversal layout (ds.nodes, ds.leaf_v)
     float4 *leaf_v = nullptr;
@@ -1085,6 +1097,89 @@ FilmClamp film_clamp(double exposure, double max_component_value) {
     if (c.on && !(exposure >= 0 && std::isfinite(exposure)))
         throw Invalid{"film exposure must be finite and nonnegative"};
     return c;
+}
+
+// prepare_texture_camera_differentials (src/texture_footprint.cpp:199-232, PBRT's
+// Camera::FindMinimumDifferentials): over 512 camera rays along the film's diagonal, the
+// smallest change of a ray's direction, in the ray's own frame, for one pixel right (dx) and
+// one pixel down (dy).  Empty on success.
+std::string texture_camera_differentials(V3 corner, V3 dx, V3 dy, u32 width, u32 height, float *min_dx,
+                                         float *min_dy) {
+    if (width == 0 || height == 0)
+        return "Texture camera raster extent must be positive";
+    using Vd = std::array<double, 3>;
+    const Vd c{corner.x, corner.y, corner.z}, u{dx.x, dx.y, dx.z}, v{dy.x, dy.y, dy.z};
+    const auto dotd = [](const Vd &a, const Vd &b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+    const auto unit = [](Vd a, Vd &out) {
+        const double len = std::hypot(a[0], a[1], a[2]);
+        if (!(len > 0 && std::isfinite(len)))
+            return false;
+        for (auto &x : a)
+            x /= len;
+        out = a;
+        return true;
+    };
+    const auto ray = [&](double x, double y, Vd &out) {
+        Vd d;
+        for (int i = 0; i < 3; ++i) {
+            d[i] = std::fma(y, v[i], std::fma(x, u[i], c[i]));
+            if (!(std::abs(d[i]) <= double(FLT_MAX)))
+                return false;
+        }
+        return unit(d, out);
+    };
+    const double px = 1. / width, py = 1. / height;
+    Vd bx{}, by{};
+    double lx = INFINITY, ly = INFINITY;
+    for (unsigned i = 0; i < 512; ++i) {
+        const double t = double(i) / 511;
+        Vd d, xr, yr;
+        if (!ray(t, t, d) || !ray(t + px, t, xr) || !ray(t, t + py, yr))
+            return "Texture camera differential ray is unrepresentable or zero";
+        // CoordinateSystem of the ray (Duff et al. 2017)
+        const double sign = std::copysign(1., d[2]), a = -1 / (sign + d[2]), b = d[0] * d[1] * a;
+        const Vd e0{1 + sign * d[0] * d[0] * a, sign * b, -sign * d[0]}, e1{b, sign + d[1] * d[1] * a, -d[1]};
+        const auto local = [&](const Vd &r) { return Vd{dotd(e0, r), dotd(e1, r), dotd(d, r)}; };
+        const Vd base = local(d);
+        Vd x, y;
+        if (!unit(local(xr), x) || !unit(local(yr), y))
+            return "Texture camera differential ray collapses in its local frame";
+        const Vd ex{x[0] - base[0], x[1] - base[1], x[2] - base[2]}, ey{y[0] - base[0], y[1] - base[1], y[2] - base[2]};
+        if (dotd(ex, ex) < lx) {
+            lx = dotd(ex, ex);
+            bx = ex;
+        }
+        if (dotd(ey, ey) < ly) {
+            ly = dotd(ey, ey);
+            by = ey;
+        }
+    }
+    for (int k = 0; k < 3; ++k) {
+        min_dx[k] = float(bx[k]);
+        min_dy[k] = float(by[k]);
+    }
+    return {};
+}
+
+// The footprint inputs of a request on a scene with image reflectance (src/metal_render.mm:
+// 1940-1963): a fixed sample budget containing the request's samples, the differential scale
+// max(1/8, 1/sqrt(budget)) and the camera's minimum differentials for the film size (found once
+// per size).  They go into the scene's device parameters for the launches that follow.
+void apply_texture_request(rp_scene *s, const rp_request &r) {
+    DImages &im = s->ds.img;
+    if (!im.textured)
+        return;
+    if (r.total_samples == 0 || r.sample_begin >= r.total_samples || r.sample_count > r.total_samples - r.sample_begin)
+        throw Invalid{"Image texture request requires a fixed total sample budget containing the sample range"};
+    if (s->tex_width != r.width || s->tex_height != r.height) {
+        const std::string err =
+            texture_camera_differentials(s->ds.forward, s->ds.right, s->ds.up, r.width, r.height, im.tex_min_dx, im.tex_min_dy);
+        if (!err.empty())
+            throw Invalid{err};
+        s->tex_width = r.width;
+        s->tex_height = r.height;
+    }
+    im.tex_spp_scale = float(std::max(0.125, 1.0 / std::sqrt(double(r.total_samples))));
 }
 
 WaveParams wave_params(const rp_request &r) {
@@ -1754,9 +1849,17 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             throw Invalid{images};
         if (d->images && scalar && (d->images->environment_image != RP_NONE || d->images->texture_count))
             throw NotBuilt{"the scalar transport does not read images"};
-        for (u32 i = 0; i < d->material_count; ++i)
-            if (d->materials[i].kind == RP_REFLECTANCE_IMAGE)
-                throw NotBuilt{"image reflectance is not built yet"};
+        for (u32 i = 0; i < d->material_count; ++i) {
+            const rp_material &m = d->materials[i];
+            if (m.kind != RP_REFLECTANCE_IMAGE || m.scattering != RP_DIFFUSE)
+                continue;
+            if (!d->images || m.image_texture >= d->images->texture_count)
+                throw Invalid{"image reflectance names no image texture"};
+            if (d->images->textures[m.image_texture].filter == RP_TEXTURE_EWA)
+                throw NotBuilt{"EWA-filtered image reflectance is not built (point, bilinear and trilinear are)"};
+            if (!d->images->instance_frame_begin || (d->images->uv_count && !d->images->instance_uv_begin))
+                throw Invalid{"image reflectance needs per-instance texture frames"};
+        }
         if (d->filter_kind > RP_FILTER_GAUSSIAN)
             throw Invalid{"unsupported pixel filter"};
         if (!(d->lens_radius >= 0) || !std::isfinite(d->lens_radius) ||
@@ -1880,7 +1983,7 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             mats[i] = {m.scattering, m.kind,        m.knot_begin,        m.knot_count,      m.scalar_value,
                        m.eta_begin,  m.eta_count,   m.k_begin,           m.k_count,         m.optical_extensions,
                        m.u_roughness, m.v_roughness, m.remap_roughness,    m.first_material,  m.second_material,
-                       m.mix_amount};
+                       m.mix_amount,  m.image_texture};
         }
         ds.materials = dupload(own, mats.data(), mats.size(), stm);
         ds.material_count = d->material_count;
@@ -1940,7 +2043,10 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
         // images (RenderScene::image_textures ... environment_image, src/render.hpp:251-261),
         // uploaded in rypath's wire layout
         double env_power = -1;
-        upload_images(d->images, ds.img, own, stm, env_power);
+        upload_images(d->images, d->instance_count, ds.img, own, stm, env_power);
+        for (u32 i = 0; i < d->material_count; ++i)
+            if (d->materials[i].kind == RP_REFLECTANCE_IMAGE && d->materials[i].scattering == RP_DIFFUSE)
+                ds.img.textured = 1;
         // scene sphere (src/metal_render.mm:213-276) over the world vertices of k_tri_prepare
         int bounds[12];
         const auto t_wait = std::chrono::steady_clock::now();
@@ -2193,6 +2299,7 @@ static rp_status sample_impl(rp_scene *s, const rp_request *request, rp_packet_r
             throw Invalid{err};
         if (s->transport != RP_TRANSPORT_HERO)
             throw Invalid{"the scene was built for the scalar transport; sample it with rp_cuda_sample_scalar"};
+        apply_texture_request(s, *request);
         const WaveParams p = wave_params(*request);
         if (capacity < p.lanes)
             throw Invalid{"output capacity is smaller than the request lanes"};
@@ -2404,6 +2511,7 @@ static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel 
                 const std::string err = validate_request(s, q);
                 if (!err.empty())
                     throw Invalid{err};
+                apply_texture_request(s, q);
                 const WaveParams p = wave_params(q);
                 u32 f = 0;
                 if (s->transport == RP_TRANSPORT_SCALAR) {
@@ -2595,6 +2703,7 @@ rp_status rp_cuda_adjoint_device(rp_scene *s, const rp_adjoint_request *r, const
                 const std::string err = validate_request(s, q);
                 if (!err.empty())
                     throw Invalid{err};
+                apply_texture_request(s, q);
                 const WaveParams p = wave_params(q);
                 run_wave(s, p, size_t(params) * sizeof(float));
                 // a failed lane (as in the forward film) fails the gradient
@@ -2944,6 +3053,8 @@ rp_status rp_cuda_tune_views(rp_scene *s, const rp_view *views, uint32_t count, 
             throw Invalid{"batched views render hero-transport scenes"};
         if (s->ds.lens_radius > 0)
             throw Invalid{"batched views render pinhole cameras"};
+        if (s->ds.img.textured)
+            throw NotBuilt{"batched views of scenes with image reflectance are not built (their texture cameras differ per view)"};
         RP_CHECK(cudaSetDevice(s->device));
         if (!s->cie)
             throw Invalid{"CIE table not set (rp_cuda_set_cie)"};
@@ -2961,6 +3072,8 @@ rp_status rp_cuda_render_views_device(rp_scene *s, const rp_view *views, uint32_
             throw Invalid{"batched views render hero-transport scenes"};
         if (s->ds.lens_radius > 0)
             throw Invalid{"batched views render pinhole cameras"};
+        if (s->ds.img.textured)
+            throw NotBuilt{"batched views of scenes with image reflectance are not built (their texture cameras differ per view)"};
         RP_CHECK(cudaSetDevice(s->device));
         if (!s->cie)
             throw Invalid{"CIE table not set (rp_cuda_set_cie)"};
@@ -3106,6 +3219,41 @@ rp_status rp_cuda_probe_environment(const rp_images *images, const float *querie
         return guarded(diag, cap, []() -> rp_status { throw Invalid{"no environment image"}; });
     return image_probe(images, queries, count, 8, 12, results, diag, cap, [&](const DImages &g, const float *q, float *r) {
         k_probe_environment<<<(count + 127) / 128, 128>>>(g, q, count, r);
+    });
+}
+
+rp_status rp_cuda_probe_texture_footprint(const float *queries, uint32_t count, float *results, char *diag,
+                                          size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        std::vector<void *> own;
+        struct Free {
+            std::vector<void *> &o;
+            ~Free() {
+                for (void *p : o)
+                    cudaFreeAsync(p, nullptr);
+                cudaStreamSynchronize(nullptr);
+            }
+        } fr{own};
+        const float *q = dupload(own, queries, size_t(48) * count, nullptr);
+        float *r = dalloc<float>(own, size_t(24) * count);
+        k_probe_texture_footprint<<<(count + 127) / 128, 128>>>(q, count, r);
+        RP_CHECK(cudaGetLastError());
+        RP_CHECK(cudaMemcpy(results, r, size_t(24) * count * 4, cudaMemcpyDeviceToHost));
+        return RP_SUCCESS;
+    });
+}
+
+rp_status rp_cuda_texture_camera_differentials(const rp_camera *camera, uint32_t width, uint32_t height,
+                                               float *minimum_dx, float *minimum_dy, char *diag, size_t cap) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        if (!camera || !minimum_dx || !minimum_dy)
+            throw Invalid{"null argument"};
+        const std::string err = texture_camera_differentials(
+            v3(camera->corner[0], camera->corner[1], camera->corner[2]), v3(camera->dx[0], camera->dx[1], camera->dx[2]),
+            v3(camera->dy[0], camera->dy[1], camera->dy[2]), width, height, minimum_dx, minimum_dy);
+        if (!err.empty())
+            throw Invalid{err};
+        return RP_SUCCESS;
     });
 }
 
@@ -3344,6 +3492,8 @@ rp_status rp_cuda_frame_session_create(rp_scene *s, const rp_frame_config *confi
     return guarded(diag, cap, [&]() -> rp_status {
         if (!s || !config || !out)
             throw Invalid{"null argument"};
+        if (s->ds.img.textured)
+            throw NotBuilt{"frame sessions of scenes with image reflectance are not built (the texture camera follows the scene camera)"};
         rp_request q{};
         q.width = config->width;
         q.height = config->height;
@@ -3556,6 +3706,7 @@ rp_status rp_cuda_sample_device_static(rp_scene *s, const rp_request *request, r
             throw Invalid{err};
         if (s->transport != RP_TRANSPORT_HERO)
             throw Invalid{"the allocation-free entry point samples hero-transport scenes"};
+        apply_texture_request(s, *request);
         const WaveParams p = wave_params(*request);
         if (capacity < p.lanes)
             throw Invalid{"output capacity is smaller than the request lanes"};

@@ -48,6 +48,11 @@ struct DImages {
     const u32 *inst_frame_begin; // per instance
     u32 uv_count, frame_count;
     float world_from_camera[9], camera_from_world[9];
+    // the request's footprint scale and the camera's minimum one-pixel differentials, set by
+    // the host before each render of a scene with image reflectance (textured != 0)
+    u32 textured;
+    float tex_spp_scale;
+    float tex_min_dx[3], tex_min_dy[3];
 };
 
 // The quiet NaN of C's NAN, so that failed lookups read like the host's
@@ -495,6 +500,96 @@ RP_DEV bool sample_environment_image(const DImages &im, float ux, float uy, bool
     }
     pdf = environment_cell_density(im, cx, cy, compensated);
     return isfinite(pdf) && pdf > 0;
+}
+
+// ------------------------------------------------------------------ texture footprints
+// PBRT ray differentials as rypath's shaders/texture_footprint.h computes them: at the primary
+// hit from the camera rays one pixel over, elsewhere from the camera's minimum differentials
+// (PBRT's Camera::Approximate_dp_dxy); then the texture-coordinate derivatives by least
+// squares against the triangle's tangents.
+// shaders/texture_footprint.h:14-20
+RP_DEV V3 texture_direction(V3 d) {
+    const float scale = fmaxf(fabsf(d.x), fmaxf(fabsf(d.y), fabsf(d.z)));
+    if (!(scale > 0.0f) || !finite3(d))
+        return v3(image_nan(), image_nan(), image_nan());
+    return unit_scaled(v3(d.x / scale, d.y / scale, d.z / scale));
+}
+// shaders/texture_footprint.h:22-38
+RP_DEV bool texture_primary_dp(V3 rel, V3 n, V3 dir, V3 xr, V3 yr, float spp_scale, V3 &dpdx, V3 &dpdy) {
+    const V3 rx = dir + spp_scale * (texture_direction(xr) - dir);
+    const V3 ry = dir + spp_scale * (texture_direction(yr) - dir);
+    const float nx = dot(n, rx), ny = dot(n, ry);
+    if (nx == 0.0f || ny == 0.0f || !isfinite(nx) || !isfinite(ny))
+        return false;
+    const float plane = dot(n, rel);
+    dpdx = (plane / nx) * rx - rel;
+    dpdy = (plane / ny) * ry - rel;
+    return true;
+}
+// shaders/texture_footprint.h:40-43
+RP_DEV V3 texture_reflect(V3 x, V3 normal) { return x - ((2.0f * dot(normal, x)) / dot(normal, normal)) * normal; }
+// a row-major 3x3 matrix times a vector, summing the columns in order
+RP_DEV V3 texture_apply(const float *m, V3 v) {
+    return (v3(m[0], m[3], m[6]) * v.x + v3(m[1], m[4], m[7]) * v.y) + v3(m[2], m[5], m[8]) * v.z;
+}
+RP_DEV V3 texture_apply_transposed(const float *m, V3 v) {
+    return (v3(m[0], m[1], m[2]) * v.x + v3(m[3], m[4], m[5]) * v.y) + v3(m[6], m[7], m[8]) * v.z;
+}
+// shaders/texture_footprint.h:45-58
+RP_DEV V3 texture_approximate_axis(V3 pz, V3 nz, V3 delta, V3 u, V3 v, const float *world_from_camera,
+                                   float spp_scale) {
+    const V3 ray = v3(0, 0, 1) + delta;
+    const float denom = dot(nz, ray);
+    if (denom == 0.0f)
+        return v3(0, 0, 0);
+    const V3 offset = ((nz.z * pz.z) / denom) * ray - pz;
+    const V3 dp = spp_scale * texture_apply(world_from_camera, texture_reflect(texture_reflect(offset, v), u));
+    return finite3(dp) ? dp : v3(0, 0, 0);
+}
+// shaders/texture_footprint.h:60-86
+RP_DEV void texture_approximate_dp(const DImages &im, V3 rel, V3 n, V3 &dpdx, V3 &dpdy) {
+    const V3 pc = texture_apply(im.camera_from_world, rel);
+    const V3 direction = texture_direction(pc);
+    if (!finite3(direction)) {
+        dpdx = dpdy = v3(0, 0, 0);
+        return;
+    }
+    // RotateFromTo(direction, +z) as two reflections
+    const V3 ref = fabsf(direction.x) < 0.72f ? v3(1, 0, 0) : v3(0, 1, 0);
+    const V3 u = ref - direction, v = ref - v3(0, 0, 1);
+    const V3 pz = texture_reflect(texture_reflect(pc, u), v);
+    const V3 nz = texture_reflect(texture_reflect(texture_apply_transposed(im.world_from_camera, n), u), v);
+    const V3 mdx = v3(im.tex_min_dx[0], im.tex_min_dx[1], im.tex_min_dx[2]);
+    const V3 mdy = v3(im.tex_min_dy[0], im.tex_min_dy[1], im.tex_min_dy[2]);
+    dpdx = texture_approximate_axis(pz, nz, mdx, u, v, im.world_from_camera, im.tex_spp_scale);
+    dpdy = texture_approximate_axis(pz, nz, mdy, u, v, im.world_from_camera, im.tex_spp_scale);
+}
+// Kahan's difference of products (shaders/texture_footprint.h:139-142)
+RP_DEV float texture_difference_of_products(float a, float b, float c, float d) {
+    const float cd = c * d;
+    return fmaf(a, b, -cd) + fmaf(-c, d, cd);
+}
+// shaders/texture_footprint.h:144-159
+RP_DEV float texture_sanitize(float d) { return isfinite(d) ? fminf(fmaxf(d, -1e8f), 1e8f) : 0.0f; }
+RP_DEV F2 texture_solve_axis(V3 dpdu, V3 dpdv, V3 dp, float aa, float ab, float bb, float inv_det) {
+    const float u = dot(dpdu, dp), v = dot(dpdv, dp);
+    return f2(texture_sanitize(inv_det * texture_difference_of_products(bb, u, ab, v)),
+              texture_sanitize(inv_det * texture_difference_of_products(aa, v, ab, u)));
+}
+// shaders/texture_footprint.h:161-185
+RP_DEV bool texture_uv_derivatives(V3 dpdu, V3 dpdv, V3 dpdx, V3 dpdy, F2 &dstdx, F2 &dstdy) {
+    if (!finite3(dpdu) || !finite3(dpdv))
+        return false;
+    const float aa = dot(dpdu, dpdu), ab = dot(dpdu, dpdv), bb = dot(dpdv, dpdv);
+    const float det = texture_difference_of_products(aa, bb, ab, ab);
+    const float inv_det = 1.0f / det;
+    if (!isfinite(inv_det)) {
+        dstdx = dstdy = f2(0, 0);
+        return true;
+    }
+    dstdx = texture_solve_axis(dpdu, dpdv, dpdx, aa, ab, bb, inv_det);
+    dstdy = texture_solve_axis(dpdu, dpdv, dpdy, aa, ab, bb, inv_det);
+    return true;
 }
 
 } // namespace rp

@@ -304,8 +304,24 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_const
                             break;
                         }
                         const DMaterial material = s.materials[cmat];
+                        // an image reflectance reads its texture at the hit's footprint
+                        // (shaders/packet_pt_event_body.inc:147-163, packet_walk.h:39-49)
+                        RGB image_rgb;
+                        bool image = false;
+                        if constexpr (F == 0) {
+                            if (s.img.textured && material.kind == 3 && material.image_texture < s.img.texture_count) {
+                                F2 st, dstdx, dstdy;
+                                if (!texture_context(s, p, ident.x, ident.y, ident.z, cinst, clocal, b1, b2,
+                                                     cp.geometric_normal, rd, cnt - 1, st, dstdx, dstdy)) {
+                                    status = 2;
+                                    break;
+                                }
+                                image_rgb = image_reflectance_rgb(s.img, material.image_texture, st, dstdx, dstdy);
+                                image = true;
+                            }
+                        }
                         if (!shading_frame(cp.shading_normal, cframe) ||
-                            !prepare_bsdf<F>(s, material, lambda, active_mask, cbsdf)) {
+                            !prepare_bsdf<F>(s, material, lambda, active_mask, cbsdf, image ? &image_rgb : nullptr)) {
                             status = 2;
                             break;
                         }

@@ -214,6 +214,41 @@ __global__ void k_probe_environment(const DImages im, const float *q, u32 count,
     o[10] = w2.y;
     o[11] = w2.z;
 }
+// Texture footprint probe, in the oracle's layout (48 floats {relative p[3], n[3], ray
+// direction[3], x ray[3], y ray[3], spp scale, world_from_camera[9], camera_from_world[9],
+// minimum dx[3], minimum dy[3], dpdu[3], dpdv[3], unused[2]} -> 24 {primary ok, primary
+// dpdx[3], dpdy[3], approximate dpdx[3], dpdy[3], derivatives ok, dstdx[2], dstdy[2],
+// texture direction of the x ray[3], unused[3]}).
+__global__ void k_probe_texture_footprint(const float *q, u32 count, float *out) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count)
+        return;
+    const float *a = q + 48 * i;
+    float *o = out + 24 * i;
+    DImages im{};
+    for (int k = 0; k < 9; ++k) {
+        im.world_from_camera[k] = a[16 + k];
+        im.camera_from_world[k] = a[25 + k];
+    }
+    for (int k = 0; k < 3; ++k) {
+        im.tex_min_dx[k] = a[34 + k];
+        im.tex_min_dy[k] = a[37 + k];
+    }
+    im.tex_spp_scale = a[15];
+    const V3 rp = v3(a[0], a[1], a[2]), n = v3(a[3], a[4], a[5]), d = v3(a[6], a[7], a[8]);
+    const V3 rx = v3(a[9], a[10], a[11]), ry = v3(a[12], a[13], a[14]);
+    V3 pdx = v3(0, 0, 0), pdy = v3(0, 0, 0), adx, ady;
+    const bool primary = texture_primary_dp(rp, n, d, rx, ry, a[15], pdx, pdy);
+    texture_approximate_dp(im, rp, n, adx, ady);
+    F2 sx = f2(0, 0), sy = f2(0, 0);
+    const bool ok = texture_uv_derivatives(v3(a[40], a[41], a[42]), v3(a[43], a[44], a[45]), primary ? pdx : adx,
+                                           primary ? pdy : ady, sx, sy);
+    const V3 td = texture_direction(rx);
+    const float v[24] = {primary ? 1.f : 0.f, pdx.x, pdx.y, pdx.z, pdy.x, pdy.y, pdy.z, adx.x, adx.y, adx.z,
+                         ady.x, ady.y, ady.z, ok ? 1.f : 0.f, sx.x, sx.y, sy.x, sy.y, td.x, td.y, td.z, 0, 0, 0};
+    for (int k = 0; k < 24; ++k)
+        o[k] = v[k];
+}
 __global__ void k_probe_raygen(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p, u32 *words,
                                float *rays) {
     const u32 lane = blockIdx.x * blockDim.x + threadIdx.x;

@@ -31,6 +31,7 @@ struct DMaterial {
     u32 remap;
     u32 first, second; // mix children
     float mix_amount;
+    u32 image_texture; // image reflectance (kind 3)
 };
 struct DPositional {
     float position[3];

@@ -179,11 +179,14 @@ RP_DEV void gaussian_filter_offsets(const DeviceScene &s, float ux, float uy, fl
     y = (1 - ty) * (-s.filter_y) + ty * s.filter_y;
 }
 // shaders/render.metal:238-311 (begin_sample)
-RP_DEV BeginSample begin_sample(const DeviceScene &s, const WaveParams &p, u32 lane) {
+// The sample of (pixel, absolute sample index): its index, camera and lens words and filter
+// offsets (the part of begin_sample that does not depend on the lane).
+RP_DEV BeginSample begin_sample_at(const DeviceScene &s, const WaveParams &p, u32 pixel, u32 sample_low,
+                                   u32 sample_high) {
     BeginSample r;
-    r.pixel = p.pixel_begin + lane % p.pixel_count;
-    r.sample_low = p.sample_low + lane / p.pixel_count;
-    r.sample_high = p.sample_high + u32(r.sample_low < p.sample_low);
+    r.pixel = pixel;
+    r.sample_low = sample_low;
+    r.sample_high = sample_high;
     if (p.sampler == 1) {
         const u64 sample = (u64(r.sample_high) << 32) | r.sample_low;
         r.index = sobol_index(s.sobol, p.m, r.pixel % p.width, r.pixel / p.width, sample);
@@ -231,6 +234,11 @@ RP_DEV BeginSample begin_sample(const DeviceScene &s, const WaveParams &p, u32 l
         gaussian_filter_offsets(s, ux, uy, r.filter_x, r.filter_y);
     }
     return r;
+}
+RP_DEV BeginSample begin_sample(const DeviceScene &s, const WaveParams &p, u32 lane) {
+    const u32 sample_low = p.sample_low + lane / p.pixel_count;
+    return begin_sample_at(s, p, p.pixel_begin + lane % p.pixel_count, sample_low,
+                           p.sample_high + u32(sample_low < p.sample_low));
 }
 // shaders/render.metal:352-357
 RP_DEV float triangle_offset(float u, float radius) {
@@ -321,10 +329,134 @@ RP_DEV void primary_ray(const DeviceScene &s, const WaveParams &p, const BeginSa
     primary_ray_from(s, RasterCam{s.origin, s.forward, s.right, s.up}, p, b, o, d);
 }
 
-// shaders/packet_walk.h:22-57 (sampled / constant / blackbody reflectance)
-RP_DEV bool material_reflectance(const DeviceScene &s, const DMaterial &m, float w, float &rho) {
+// shaders/render.metal:479-501 (texture_camera_rays): the camera directions one pixel right and
+// one pixel down of the sample's film position, shifted by the lens sample; and the lens
+// sample's aperture offset (lens_offset, :390-392)
+RP_DEV void texture_camera_rays(const DeviceScene &s, const WaveParams &p, const BeginSample &b, V3 &rx, V3 &ry,
+                                V3 &lens) {
+    float ux, uy;
+    if (p.sampler == 1) {
+        ux = sobol_camera_uniform(b.words.x, p.m, b.pixel % p.width);
+        uy = sobol_camera_uniform(b.words.y, p.m, b.pixel / p.width);
+    } else {
+        ux = sample_uniform(p, b.words.x);
+        uy = sample_uniform(p, b.words.y);
+    }
+    const bool centered = s.filter_kind != 0 || s.filter_x != 0.5f || s.filter_y != 0.5f;
+    V3 dd;
+    if (centered) {
+        const float ox = s.filter_kind == 2   ? b.filter_x
+                         : s.filter_kind == 1 ? triangle_offset(ux, s.filter_x)
+                                              : (2.0f * ux - 1.0f) * s.filter_x;
+        const float oy = s.filter_kind == 2   ? b.filter_y
+                         : s.filter_kind == 1 ? triangle_offset(uy, s.filter_y)
+                                              : (2.0f * uy - 1.0f) * s.filter_y;
+        const float x = ((float(b.pixel % p.width) + 0.5f) + ox) / float(p.width);
+        const float y = ((float(b.pixel / p.width) + 0.5f) + oy) / float(p.height);
+        dd = fma3(v3(y, y, y), s.up, fma3(v3(x, x, x), s.right, s.forward));
+    } else {
+        const float x = (float(b.pixel % p.width) + ux) / float(p.width);
+        const float y = (float(b.pixel / p.width) + uy) / float(p.height);
+        dd = s.forward + x * s.right + y * s.up;
+    }
+    rx = dd + s.right / float(p.width);
+    ry = dd + s.up / float(p.height);
+    lens = v3(0, 0, 0);
+    if (s.lens_radius > 0) {
+        const float lx = 2.0f * sample_uniform(p, b.lens_words.x) - 1.0f;
+        const float ly = 2.0f * sample_uniform(p, b.lens_words.y) - 1.0f;
+        if (!(lx == 0 && ly == 0)) {
+            float radius, theta;
+            if (fabsf(lx) > fabsf(ly)) {
+                radius = lx;
+                theta = (kPi / 4.0f) * (ly / lx);
+            } else {
+                radius = ly;
+                theta = kPi / 2.0f - (kPi / 4.0f) * (lx / ly);
+            }
+            const float r = s.lens_radius * radius;
+            const V3 ideal = (r * cosf(theta)) * s.lens_x + (r * sinf(theta)) * s.lens_y;
+            lens = (s.origin + ideal) - s.origin;
+        }
+        const V3 shift = v3(lens.x / s.focal_distance, lens.y / s.focal_distance, lens.z / s.focal_distance);
+        rx = rx - shift;
+        ry = ry - shift;
+    }
+}
+
+// shaders/render.metal:1312-1408 (surface_texture_context) at a triangle hit (b1, b2) of
+// instance `instance`, local triangle `local`: the texture coordinates and their screen-space
+// derivatives.  scatterings: the path's scattering events so far (0 at the primary hit, whose
+// footprint comes from the camera rays of the sample (pixel, sample_low, sample_high)).
+RP_DEV bool texture_context(const DeviceScene &s, const WaveParams &p, u32 pixel, u32 sample_low, u32 sample_high,
+                            u32 instance, u32 local, float b1, float b2, V3 geometric_normal, V3 primary_direction,
+                            u32 scatterings, F2 &st, F2 &dstdx, F2 &dstdy) {
+    const DInstance &in = s.instances[instance];
+    const DImages &im = s.img;
+    const u32 *tri = s.triangles + 3 * (in.triangle_begin + local);
+    const u32 i0 = __ldg(tri), i1 = __ldg(tri + 1), i2 = __ldg(tri + 2);
+    const V3 p0 = load3(s.positions + 3 * (in.vertex_begin + i0));
+    const V3 p1 = load3(s.positions + 3 * (in.vertex_begin + i1));
+    const V3 p2 = load3(s.positions + 3 * (in.vertex_begin + i2));
+    const V3 local_p = fma3(v3(b2, b2, b2), p2 - p0, fma3(v3(b1, b1, b1), p1 - p0, p0));
+    F2 uv0 = f2(0, 0), uv1 = f2(1, 0), uv2 = f2(1, 1);
+    const u32 uv_begin = im.inst_uv_begin ? __ldg(im.inst_uv_begin + instance) : kNone;
+    if (uv_begin != kNone) {
+        if (uv_begin >= im.uv_count || i0 >= im.uv_count - uv_begin || i1 >= im.uv_count - uv_begin ||
+            i2 >= im.uv_count - uv_begin)
+            return false;
+        const float2 a = im.uvs[uv_begin + i0], b = im.uvs[uv_begin + i1], c = im.uvs[uv_begin + i2];
+        uv0 = f2(a.x, a.y);
+        uv1 = f2(b.x, b.y);
+        uv2 = f2(c.x, c.y);
+        if (!isfinite(uv0.x) || !isfinite(uv0.y) || !isfinite(uv1.x) || !isfinite(uv1.y) || !isfinite(uv2.x) ||
+            !isfinite(uv2.y))
+            return false;
+    }
+    const float w0 = 1.0f - (b1 + b2);
+    st = f2((w0 * uv0.x + b1 * uv1.x) + b2 * uv2.x, (w0 * uv0.y + b1 * uv1.y) + b2 * uv2.y);
+    const u32 frame_begin = im.inst_frame_begin ? __ldg(im.inst_frame_begin + instance) : kNone;
+    if (!isfinite(st.x) || !isfinite(st.y) || frame_begin >= im.frame_count || local >= im.frame_count - frame_begin)
+        return false;
+    const float *fr = im.frames + 6 * size_t(frame_begin + local);
+    const V3 dpdu = load3(fr), dpdv = load3(fr + 3);
+    const V3 world = v3(dot(v3(in.m[0], in.m[1], in.m[2]), local_p), dot(v3(in.m[4], in.m[5], in.m[6]), local_p),
+                        dot(v3(in.m[8], in.m[9], in.m[10]), local_p));
+    const V3 rel = world + (v3(in.m[3], in.m[7], in.m[11]) - s.origin);
+    if (!finite3(rel))
+        return false;
+    V3 dpdx = v3(0, 0, 0), dpdy = v3(0, 0, 0);
+    bool primary = false;
+    if (scatterings == 0) {
+        V3 rx, ry, lens;
+        texture_camera_rays(s, p, begin_sample_at(s, p, pixel, sample_low, sample_high), rx, ry, lens);
+        if (!finite3(rx) || !finite3(ry))
+            return false;
+        primary = texture_primary_dp(s.lens_radius > 0 ? rel - lens : rel, geometric_normal, primary_direction, rx,
+                                     ry, im.tex_spp_scale, dpdx, dpdy);
+    }
+    if (!primary)
+        texture_approximate_dp(im, rel, geometric_normal, dpdx, dpdy);
+    return texture_uv_derivatives(dpdu, dpdv, dpdx, dpdy, dstdx, dstdy);
+}
+// The filtered, scaled (and inverted) linear RGB of an image reflectance at a footprint
+// (shaders/packet_walk.h:39-49)
+RP_DEV RGB image_reflectance_rgb(const DImages &im, u32 texture, F2 st, F2 dstdx, F2 dstdy) {
+    const DImageTexture t = im.textures[texture];
+    RGB c = lookup_standard(im, t, st, dstdx, dstdy, false, false);
+    c = rgb3(c.r * t.scale, c.g * t.scale, c.b * t.scale);
+    if (t.invert)
+        c = rgb3(1 - c.r, 1 - c.g, 1 - c.b);
+    return c;
+}
+
+// shaders/packet_walk.h:22-57 (sampled / constant / blackbody / image reflectance; image: the
+// hit's filtered RGB)
+RP_DEV bool material_reflectance(const DeviceScene &s, const DMaterial &m, float w, const RGB *image, float &rho) {
     if (m.scattering != 0) {
         rho = 1;
+    } else if (m.kind == 3 && image && m.image_texture < s.img.texture_count) {
+        rho = rgb_spectrum(s.img.rgb_table, *image, w);
     } else if (m.kind == 0 && m.knot_count >= 2 && m.knot_begin <= s.knot_count &&
                m.knot_count <= s.knot_count - m.knot_begin) {
         rho = pbrt_reflectance(s.knots + m.knot_begin, m.knot_count, w);
@@ -338,7 +470,8 @@ RP_DEV bool material_reflectance(const DeviceScene &s, const DMaterial &m, float
 }
 // shaders/hero_current_bsdf.h:72-101 with prepare_scattering (shaders/render.metal:2079-2160)
 template <int K>
-RP_DEV bool prepare_bsdf(const DeviceScene &s, const DMaterial &m, V4 lambda, u32 mask, HeroBsdf &out) {
+RP_DEV bool prepare_bsdf(const DeviceScene &s, const DMaterial &m, V4 lambda, u32 mask, HeroBsdf &out,
+                         const RGB *image = nullptr) {
     if (m.scattering != u32(K))
         return false;
     out.kind = m.scattering;
@@ -362,7 +495,7 @@ RP_DEV bool prepare_bsdf(const DeviceScene &s, const DMaterial &m, V4 lambda, u3
         if (!(mask & (1u << k)))
             continue;
         float rho;
-        if (!material_reflectance(s, m, lambda.v[k], rho))
+        if (!material_reflectance(s, m, lambda.v[k], image, rho))
             return false;
         if constexpr (K == 0) {
             out.param[k] = rho;

@@ -343,7 +343,7 @@ def cornell_pass_through(width=256, height=256, spp=64, max_depth=8, pane=True, 
     return scene
 
 
-CORNELL_FEATURES = ("point", "spot", "environment", "cauchy", "env_image")
+CORNELL_FEATURES = ("point", "spot", "environment", "cauchy", "env_image", "texture")
 
 
 def cauchy_dielectric(scene, a=1.5, b_um2=0.004):
@@ -369,7 +369,9 @@ def cornell_features(feature, width=32, height=32, spp=4, max_depth=8) -> Scene:
     cauchy: the tall box made of a smooth dispersive (Cauchy) dielectric, the short box of a
     rough conductor, under the area light;
     env_image: the area light replaced by an equal-area octahedral sky image (float texels,
-    a bright sun shining in through the open front), sampled by its importance tables.
+    a bright sun shining in through the open front), sampled by its importance tables;
+    texture: image reflectance on the back wall (sRGB 8-bit, trilinear, tiled), the floor (float,
+    bilinear) and the tall box (half, point, clamped), under the area light.
     """
     if feature not in CORNELL_FEATURES:
         raise ValueError(f"unknown feature {feature!r}")
@@ -385,6 +387,8 @@ def cornell_features(feature, width=32, height=32, spp=4, max_depth=8) -> Scene:
         scene.positional = [_spot((-0.1, 1.9, 0.4), (0.4, 0.6, 0.2), 20.0, 30.0, blackbody_emission(5000, 8.0))]
     elif feature == "environment":
         scene.environment = (1.5 * blackbody_shape(9000) / blackbody_shape(9000).max()).astype(np.float32)
+    elif feature == "texture":
+        textured_cornell(scene)
     elif feature == "env_image":
         from . import images
 
@@ -403,6 +407,90 @@ def cornell_features(feature, width=32, height=32, spp=4, max_depth=8) -> Scene:
         scene.instances[5].material = base
         scene.instances[6].material = base + 1
     return scene
+
+
+def triangle_frames(positions, triangles, uvs):
+    """PBRT's triangle texture partials (dp/du, dp/dv from the vertices' uvs; for a degenerate
+    uv parameterisation a frame around the geometric normal), per triangle, as (T, 6) float32."""
+    p = np.asarray(positions, np.float64)[np.asarray(triangles)]
+    t = np.asarray(uvs, np.float64)[np.asarray(triangles)]
+    duv02, duv12 = t[:, 0] - t[:, 2], t[:, 1] - t[:, 2]
+    dp02, dp12 = p[:, 0] - p[:, 2], p[:, 1] - p[:, 2]
+    det = duv02[:, 0] * duv12[:, 1] - duv02[:, 1] * duv12[:, 0]
+    safe = np.where(np.abs(det) < 1e-9, 1.0, det)
+    dpdu = (duv12[:, 1:2] * dp02 - duv02[:, 1:2] * dp12) / safe[:, None]
+    dpdv = (duv02[:, 0:1] * dp12 - duv12[:, 0:1] * dp02) / safe[:, None]
+    n = np.cross(p[:, 2] - p[:, 0], p[:, 1] - p[:, 0])
+    n /= np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-30)
+    sign = np.copysign(1.0, n[:, 2])
+    a = -1 / (sign + n[:, 2])
+    b = n[:, 0] * n[:, 1] * a
+    fu = np.stack([1 + sign * n[:, 0] ** 2 * a, sign * b, -sign * n[:, 0]], 1)
+    fv = np.stack([b, sign + n[:, 1] ** 2 * a, -n[:, 1]], 1)
+    bad = (np.abs(det) < 1e-9)[:, None] | (np.linalg.norm(np.cross(dpdu, dpdv), axis=1) == 0)[:, None]
+    dpdu, dpdv = np.where(bad, fu, dpdu), np.where(bad, fv, dpdv)
+    return np.concatenate([dpdu, dpdv], axis=1).astype(np.float32)
+
+
+def texture_camera(origin, target, up):
+    """TextureCamera (src/texture_footprint.hpp:9-12) of a look-at pose: world_from_camera's
+    columns are the camera's right, up and forward axes (row-major), camera_from_world its
+    transpose."""
+    o, t = np.asarray(origin, np.float64), np.asarray(target, np.float64)
+    f = (t - o) / np.linalg.norm(t - o)
+    r = np.cross(np.asarray(up, np.float64), f)
+    r /= np.linalg.norm(r)
+    u = np.cross(f, r)
+    m = np.stack([r, u, f], axis=1)
+    return tuple(m.reshape(-1).astype(np.float32)), tuple(m.T.reshape(-1).astype(np.float32))
+
+
+def textured_cornell(scene: Scene) -> None:
+    """Give the Cornell box's back wall, floor and tall box image reflectance (see
+    cornell_features("texture")): per-vertex uvs by planar projection, PBRT triangle frames, the
+    texture camera of the box's pose, and three seeded images."""
+    from . import images
+
+    rng = np.random.default_rng(11)
+    pos = scene.positions.astype(np.float64)
+    # planar projections: floor / ceiling / boxes' tops on (x, z), walls on (x, y) or (z, y)
+    uv = np.stack([0.5 * pos[:, 0] + 0.5, 0.5 * pos[:, 1]], 1)
+    for inst in (scene.instances[0], scene.instances[1]):
+        vs = slice(inst.vertex_begin, inst.vertex_begin + 4)
+        uv[vs] = np.stack([0.5 * pos[vs, 0] + 0.5, 0.5 * pos[vs, 2] + 0.5], 1)
+    for k in (3, 4):
+        inst = scene.instances[k]
+        vs = slice(inst.vertex_begin, inst.vertex_begin + 4)
+        uv[vs] = np.stack([0.5 * pos[vs, 2] + 0.5, 0.5 * pos[vs, 1]], 1)
+    tall = scene.instances[6]
+    vs = slice(tall.vertex_begin, tall.vertex_begin + 8)
+    uv[vs] = np.stack([(pos[vs, 0] + pos[vs, 2]) * 0.8 + 0.5, pos[vs, 1] / 1.2], 1)
+    s = images.ImageSet()
+    yy, xx = np.mgrid[0:64, 0:64]
+    check = ((xx // 8 + yy // 8) % 2).astype(np.float64)
+    base = np.stack([0.15 + 0.7 * check, 0.2 + 0.5 * (1 - check), 0.3 + 0.2 * rng.uniform(size=(64, 64))], 2)
+    codes = [np.round(np.clip(c, 0, 1) * 255).astype(np.uint8) for c in images.box_pyramid(base)]
+    back = s.add_image(codes, abi.TEXELS_SRGB8, abi.WRAP_REPEAT, abi.TEXTURE_TRILINEAR, uvscale=(3.0, 2.0))
+    stripes = np.stack([0.3 + 0.6 * ((xx % 16) < 8), np.full((64, 64), 0.5), 0.2 + 0.7 * (yy / 63.0)], 2)
+    floor = s.add_image([c.astype(np.float32) for c in images.box_pyramid(stripes[:32, :32])], abi.TEXELS_FLOAT,
+                        abi.WRAP_REPEAT, abi.TEXTURE_BILINEAR, uvscale=(2.0, 2.0), uvdelta=(0.25, 0.0))
+    noise = rng.uniform(0.05, 0.95, (16, 16, 3)).astype(np.float32)
+    box = s.add_image(noise, abi.TEXELS_HALF, abi.WRAP_CLAMP, abi.TEXTURE_POINT)
+    first = len(scene.materials)
+    for index in (back, floor, box):
+        m = abi.Material()
+        m.scattering, m.kind, m.image_texture = abi.DIFFUSE, abi.REFLECTANCE_IMAGE, index
+        m.remap_roughness = 1
+        scene.materials.append(m)
+    scene.instances[2].material = first
+    scene.instances[0].material = first + 1
+    scene.instances[6].material = first + 2
+    s.uvs = uv.astype(np.float32)
+    s.instance_uv_begin = [inst.vertex_begin for inst in scene.instances]
+    s.frames = triangle_frames(scene.positions, scene.triangles, s.uvs)
+    s.instance_frame_begin = [inst.triangle_begin for inst in scene.instances]
+    s.world_from_camera, s.camera_from_world = texture_camera((0, 1, 3.94), (0, 1, 0), (0, 1, 0))
+    scene.images = s
 
 
 def crop(scene: Scene, x0: int, y0: int, width: int, height: int) -> Scene:

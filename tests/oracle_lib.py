@@ -27,6 +27,8 @@ def _image_args(lib, prefix):
     getattr(lib, prefix + "rgb_spectrum").argtypes = [vp, vp, u32, vp]
     getattr(lib, prefix + "environment_queries").argtypes = [vp, u32, u32, vp, u32, vp, u32, vp, u32, vp, vp, vp,
                                                                u32, u32, u32, fp, vp, vp, u32, vp]
+    getattr(lib, prefix + "texture_footprint").argtypes = [vp, u32, vp]
+    getattr(lib, prefix + "texture_camera_differentials").argtypes = [vp, vp, vp, u32, u32, vp]
 
 
 def oracle():

@@ -242,3 +242,92 @@ def test_environment_queries_match_reference(width, seed, fmt):
     np.testing.assert_array_equal(out["or_"].view(np.uint32), out["ref_"].view(np.uint32))
     o = out["or_"]
     assert (o[:, 3] == 1).mean() > 0.99 and (o[:, 0] > 0).mean() > 0.5
+
+
+def footprint_queries(rng, n):
+    """Texture footprint inputs: camera-relative points on random planes seen along random
+    rays, one-pixel ray offsets, texture tangents and camera frames (some degenerate)."""
+    q = np.zeros((n, 48), np.float32)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    t = np.exp(rng.uniform(-2, 4, (n, 1)))
+    q[:, 0:3] = d * t
+    nrm = rng.normal(size=(n, 3))
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    q[:, 3:6] = nrm
+    q[:, 6:9] = d
+    eps = np.exp(rng.uniform(np.log(1e-4), np.log(1e-2), (n, 1)))
+    q[:, 9:12] = d + eps * rng.normal(size=(n, 3))
+    q[:, 12:15] = d + eps * rng.normal(size=(n, 3))
+    q[:, 15] = rng.choice([0.125, 0.25, 1.0], n)
+    for k in range(n):
+        a = rng.normal(size=(3, 3))
+        qm, _ = np.linalg.qr(a)
+        q[k, 16:25] = qm.reshape(-1)
+        q[k, 25:34] = qm.T.reshape(-1)
+    q[:, 34:37] = rng.normal(0, 1e-3, (n, 3))
+    q[:, 37:40] = rng.normal(0, 1e-3, (n, 3))
+    q[:, 40:43] = rng.normal(size=(n, 3))
+    q[:, 43:46] = rng.normal(size=(n, 3))
+    q[: n // 20, 43:46] = q[: n // 20, 40:43] * 2   # parallel tangents: a singular system
+    q[n // 20: n // 10, 3:6] = 0                   # a zero normal: no primary footprint
+    return q
+
+
+def test_texture_footprint_matches_reference():
+    """rypath_texture_primary_dp / approximate_dp / uv_derivatives / direction
+    (shaders/texture_footprint.h) against the oracle, bit for bit."""
+    lib = need_ref()
+    rng = np.random.default_rng(44)
+    q = footprint_queries(rng, 5000)
+    a = np.zeros((q.shape[0], 24), np.float32)
+    b = np.zeros_like(a)
+    oracle().or_texture_footprint(q.ctypes.data, q.shape[0], a.ctypes.data)
+    lib.ref_texture_footprint(q.ctypes.data, q.shape[0], b.ctypes.data)
+    np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert (a[:, 0] == 1).mean() > 0.8 and (a[:, 13] == 1).mean() > 0.99
+
+
+@pytest.mark.parametrize("size", [(32, 32), (1920, 1080), (7, 3)])
+def test_texture_camera_differentials_match_reference(size):
+    """prepare_texture_camera_differentials (src/texture_footprint.cpp:199-232) of pinhole
+    cameras of several poses and films against the oracle's restatement, bit for bit."""
+    from rypath_b200 import scenes
+
+    lib = need_ref()
+    rng = np.random.default_rng(45)
+    for k in range(6):
+        origin = rng.normal(size=3) * 3
+        target = origin + rng.normal(size=3)
+        up = rng.normal(size=3)
+        _, corner, dx, dy = scenes.pinhole_camera(tuple(origin), tuple(target), tuple(up), float(rng.uniform(20, 90)),
+                                                  *size)
+        c, x, y = (np.asarray(v, np.float32) for v in (corner, dx, dy))
+        out = {}
+        for prefix, l in (("or_", oracle()), ("ref_", lib)):
+            o = np.zeros(6, np.float32)
+            assert getattr(l, prefix + "texture_camera_differentials")(c.ctypes.data, x.ctypes.data, y.ctypes.data,
+                                                                       size[0], size[1], o.ctypes.data) == 0
+            out[prefix] = o
+        np.testing.assert_array_equal(out["or_"].view(np.uint32), out["ref_"].view(np.uint32))
+
+
+def test_library_texture_camera_differentials_match_oracle():
+    """The library's host search for the texture camera's minimum differentials (scene renders
+    use it per film size) equals the oracle's, bit for bit; the oracle's equals rypath's own."""
+    from rypath_b200 import scenes
+
+    rng = np.random.default_rng(46)
+    for size in ((32, 32), (1920, 1080), (640, 480)):
+        origin = rng.normal(size=3) * 3
+        cam = scenes.pinhole_camera(tuple(origin), tuple(origin + rng.normal(size=3)), (0, 1, 0), 45.0, *size)
+        c = abi.Camera()
+        c.origin[:], c.corner[:], c.dx[:], c.dy[:] = cam[0], cam[1], cam[2], cam[3]
+        mx, my = np.zeros(3, np.float32), np.zeros(3, np.float32)
+        native.check(native.lib().rp_cuda_texture_camera_differentials(C.byref(c), size[0], size[1], mx.ctypes.data,
+                                                                        my.ctypes.data, None, 0))
+        o = np.zeros(6, np.float32)
+        corner, dx, dy = (np.asarray(v, np.float32) for v in cam[1:])
+        assert oracle().or_texture_camera_differentials(corner.ctypes.data, dx.ctypes.data, dy.ctypes.data, size[0],
+                                                        size[1], o.ctypes.data) == 0
+        np.testing.assert_array_equal(np.concatenate([mx, my]).view(np.uint32), o.view(np.uint32))
