@@ -176,6 +176,7 @@ typedef struct rp_images {
     uint32_t frame_count;      const float *frames;
     const uint32_t *instance_frame_begin; /* instance_count entries (RP_NONE: untextured) */
     float world_from_camera[9], camera_from_world[9];
+    const float *ewa_weights; /* 128 floats: rypath_ewa::weights (src/ewa_weights.h), for EWA filters */
 } rp_images;
 
 typedef struct rp_area_emission { /* wire::AreaEmission subset, src/render_wire.h:219 */

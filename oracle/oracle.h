@@ -91,12 +91,14 @@ int or_scalar_film_add(const rp_scalar_result *results, size_t count, const doub
  * ref_environment_tables and ref_environment_queries: texture lookups of texture `index`
  * (6 floats {u, v, dudx, dvdx, dudy, dvdy} -> 4 {rgb[3], scalar}); RGB reconstruction
  * (4 {r, g, b, wavelength} -> 2 {bounded, unbounded}); the environment tables of a square
- * image; environment queries (8 {direction[3], wavelength, u[2], unused[2]} -> 12 {radiance,
+ * image (the EWA filter reads the 128 weights given); environment queries (8 {direction[3],
+ * wavelength, u[2], unused[2]} -> 12 {radiance,
  * compensated pdf, full pdf, sample ok, direction[3], pdf, full-table sample ok,
  * direction[3]}). */
 void or_image_lookup(const void *textures, uint32_t texture_count, uint32_t index, const void *levels,
                      uint32_t level_count, const uint32_t *texels, uint32_t words, const float *transfer,
-                     uint32_t transfer_count, const float *queries, uint32_t count, float *results);
+                     uint32_t transfer_count, const float *queries, uint32_t count, float *results,
+                     const float *ewa_weights);
 void or_rgb_spectrum(const float *table, const float *queries, uint32_t count, float *results);
 int or_environment_tables(const void *textures, uint32_t index, const void *levels, const uint32_t *texels,
                           uint32_t words, const float *transfer, const float *table, const float *illuminant,

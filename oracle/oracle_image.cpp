@@ -225,6 +225,8 @@ std::string load_images(const rp_images *in, u32 instance_count, Images &out) {
         out.inst_frame_begin.assign(in->instance_frame_begin, in->instance_frame_begin + instance_count);
     std::copy(in->world_from_camera, in->world_from_camera + 9, out.world_from_camera);
     std::copy(in->camera_from_world, in->camera_from_world + 9, out.camera_from_world);
+    if (in->ewa_weights)
+        out.ewa_weights.assign(in->ewa_weights, in->ewa_weights + 128);
     out.textures.assign(in->textures, in->textures + in->texture_count);
     out.levels.assign(in->levels, in->levels + in->level_count);
     out.texels.assign(in->texels, in->texels + in->texel_word_count);
@@ -272,19 +274,21 @@ extern "C" {
 
 void or_image_lookup(const void *textures, uint32_t texture_count, uint32_t index, const void *levels,
                      uint32_t level_count, const uint32_t *texels, uint32_t words, const float *transfer,
-                     uint32_t transfer_count, const float *q, uint32_t count, float *out) {
-    const oracle::Images im =
+                     uint32_t transfer_count, const float *q, uint32_t count, float *out, const float *ewa_weights) {
+    oracle::Images im =
         probe_images(textures, texture_count, levels, level_count, texels, words, transfer, transfer_count);
+    if (ewa_weights)
+        im.ewa_weights.assign(ewa_weights, ewa_weights + 128);
     const rp_image_texture &t = im.textures[index];
     for (uint32_t i = 0; i < count; ++i) {
         const float *a = q + 6 * i;
         float *o = out + 4 * i;
         const oracle::F2 uv{a[0], a[1]}, dx{a[2], a[3]}, dy{a[4], a[5]};
-        const oracle::Rgb c = oracle::image_lookup_standard(im, t, uv, dx, dy, false, false);
+        const oracle::Rgb c = oracle::image_lookup(im, t, uv, dx, dy, false, false);
         o[0] = c.r;
         o[1] = c.g;
         o[2] = c.b;
-        o[3] = oracle::image_lookup_standard(im, t, uv, dx, dy, true, false).r;
+        o[3] = oracle::image_lookup(im, t, uv, dx, dy, true, false).r;
     }
 }
 

@@ -40,6 +40,7 @@ struct Images {
     std::vector<std::array<F3, 2>> frames;
     std::vector<u32> inst_uv_begin, inst_frame_begin;
     float world_from_camera[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, camera_from_world[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    std::vector<float> ewa_weights; // PBRT's 128-entry EWA Gaussian table (rypath_ewa::weights)
 };
 
 // shaders/image_texture.h:14-27
@@ -195,6 +196,195 @@ inline Rgb image_lookup_standard(const Images &im, const rp_image_texture &t, F2
     const float delta = lod - float(index);
     return {(1.0f - delta) * lower.r + delta * upper.r, (1.0f - delta) * lower.g + delta * upper.g,
             (1.0f - delta) * lower.b + delta * upper.b};
+}
+
+// ---------------------------------------------------------------- EWA (PBRT's elliptically
+// weighted average over the two mip levels around the footprint's minor axis)
+inline u32 ewa_magnitude(float v) { return std::bit_cast<u32>(v) & 0x7fffffffu; }
+inline bool ewa_subnormal(u32 m) { return m != 0u && m < 0x00800000u; }
+// shaders/image_texture.h:168-204: value * scale rounded to nearest even with gradual underflow,
+// reconstructed from the significands where an operand or the product is subnormal
+inline float ewa_product(float value, float scale) {
+    const float mapped = value * scale;
+    const u32 a = ewa_magnitude(value), b = ewa_magnitude(scale);
+    if (a == 0u || b == 0u || (ewa_magnitude(mapped) != 0u && !ewa_subnormal(a) && !ewa_subnormal(b)))
+        return mapped;
+    const int a_exp = int(a >> 23), b_exp = int(b >> 23);
+    const u32 a_sig = (a & 0x007fffffu) | (a_exp == 0 ? 0u : 0x00800000u);
+    const u32 b_sig = (b & 0x007fffffu) | (b_exp == 0 ? 0u : 0x00800000u);
+    const uint64_t product = uint64_t(a_sig) * b_sig;
+    const int exponent = std::max(1, a_exp) + std::max(1, b_exp) - 300;
+    const int leading = 63 - int(std::countl_zero(product));
+    const u32 sign = (std::bit_cast<u32>(value) ^ std::bit_cast<u32>(scale)) & 0x80000000u;
+    if (exponent + leading > 127)
+        return std::bit_cast<float>(sign | 0x7f800000u);
+    const int shift = std::max(leading - 23, -149 - exponent);
+    if (shift > 48)
+        return std::bit_cast<float>(sign);
+    u32 rounded;
+    if (shift <= 0) {
+        rounded = u32(product << -shift);
+    } else {
+        const uint64_t halfway = uint64_t(1) << (shift - 1);
+        const uint64_t truncated = product >> shift;
+        rounded = u32((product + halfway - 1u + (truncated & 1u)) >> shift);
+    }
+    return std::bit_cast<float>(sign | ((u32(exponent + shift + 149) << 23) + rounded));
+}
+// shaders/image_texture.h:206-211
+inline float ewa_lift(float v) {
+    const u32 m = ewa_magnitude(v);
+    if (ewa_subnormal(m))
+        return std::copysign(float(m) * 0x1p-125f, v);
+    return v * 0x1p24f;
+}
+// shaders/image_texture.h:141-152
+inline float ewa_center(float st, float dimension, u32 wrap) {
+    if (std::fabs(st) <= 64.0f || wrap == RP_WRAP_BLACK)
+        return st * dimension - 0.5f;
+    const float phase = std::fmod(st, 1.0f) * dimension;
+    if (wrap == RP_WRAP_REPEAT)
+        return phase - 0.5f;
+    return ((st < 0.0f ? -64.0f : dimension + 64.0f) + phase) - 0.5f;
+}
+// shaders/image_texture.h:154-159
+inline bool ewa_black_disjoint(F2 st, F2 dims, F2 radius) {
+    const auto axis = [](float s, float d, float r) {
+        return std::fabs(s) > 64.0f && (s < (0.5f - r) / d || s > ((d - 0.5f) + r) / d);
+    };
+    return axis(st.x, dims.x, radius.x) || axis(st.y, dims.y, radius.y);
+}
+// shaders/image_texture.h:134-139
+inline bool ewa_level_valid(const Images &im, const rp_texture_level &l, u32 format, u32 levels_above) {
+    return image_level_valid(im, l, format) && (l.width & (l.width - 1u)) == 0u && (l.height & (l.height - 1u)) == 0u &&
+           std::max(l.width, l.height) == (1u << levels_above);
+}
+// shaders/image_texture.h:213-256
+inline Rgb ewa_level(const Images &im, const rp_image_texture &t, const rp_texture_level &l, F2 st, F2 dx, F2 dy) {
+    const F2 dims{float(l.width), float(l.height)};
+    const F2 u{dx.x * dims.x, dx.y * dims.y}, v{dy.x * dims.x, dy.y * dims.y};
+    const float area = u.x * v.y - u.y * v.x;
+    const float determinant = ((1.0f + (u.x * u.x + u.y * u.y)) + (v.x * v.x + v.y * v.y)) + area * area;
+    const F2 radius{std::sqrt((1.0f + u.x * u.x) + v.x * v.x), std::sqrt((1.0f + u.y * u.y) + v.y * v.y)};
+    if (t.wrap == RP_WRAP_BLACK && ewa_black_disjoint(st, dims, radius))
+        return {};
+    const F2 center{ewa_center(st.x, dims.x, t.wrap), ewa_center(st.y, dims.y, t.wrap)};
+    const F2 begin{std::ceil(center.x - radius.x), std::ceil(center.y - radius.y)};
+    const F2 end{std::floor(center.x + radius.x), std::floor(center.y + radius.y)};
+    const F2 count{(end.x - begin.x) + 1.0f, (end.y - begin.y) + 1.0f};
+    if (!std::isfinite(begin.x) || !std::isfinite(begin.y) || !std::isfinite(end.x) || !std::isfinite(end.y) ||
+        std::fabs(begin.x) > 0x1p19f || std::fabs(begin.y) > 0x1p19f || std::fabs(end.x) > 0x1p19f ||
+        std::fabs(end.y) > 0x1p19f || count.x <= 0.0f || count.y <= 0.0f || count.x * count.y > 4096.0f)
+        return rgb_nan();
+    if (t.wrap == RP_WRAP_BLACK && (end.x < 0.0f || end.y < 0.0f || begin.x >= dims.x || begin.y >= dims.y))
+        return {};
+    const int x0 = int(begin.x), y0 = int(begin.y), x1 = int(end.x), y1 = int(end.y);
+    Rgb sum{};
+    float weight_sum = 0;
+    for (int y = y0; y <= y1; ++y)
+        for (int x = x0; x <= x1; ++x) {
+            const F2 d{float(x) - center.x, float(y) - center.y};
+            const float a = u.x * d.y - u.y * d.x, b = v.x * d.y - v.y * d.x;
+            const float r2 = (((d.x * d.x + d.y * d.y) + a * a) + b * b) / determinant;
+            if (r2 < 1.0f) {
+                const float w = im.ewa_weights[std::min(u32(128.0f * r2), 127u)];
+                const Rgb c = image_texel(im, l, x, y, t.wrap, t.texel_format, t.transfer_offset);
+                sum = {sum.r + w * c.r, sum.g + w * c.g, sum.b + w * c.b};
+                weight_sum += w;
+            }
+        }
+    if (!(std::isfinite(weight_sum) && weight_sum > 0.0f))
+        return rgb_nan();
+    return {sum.r / weight_sum, sum.g / weight_sum, sum.b / weight_sum};
+}
+// shaders/image_texture.h:258-388
+inline Rgb image_lookup_ewa(const Images &im, const rp_image_texture &t, F2 uv, F2 dx, F2 dy, bool scalar, bool mapped) {
+    const float cap = t.max_anisotropy;
+    if (t.level_count > 14u || !(cap >= 1.0f && cap <= 16.0f) || !std::isfinite(t.uscale) || !std::isfinite(t.vscale) ||
+        !std::isfinite(t.udelta) || !std::isfinite(t.vdelta) || im.ewa_weights.size() < 128)
+        return rgb_nan();
+    if (!mapped) {
+        dx = {ewa_product(dx.x, t.uscale), ewa_product(dx.y, t.vscale)};
+        dy = {ewa_product(dy.x, t.uscale), ewa_product(dy.y, t.vscale)};
+    }
+    if (!std::isfinite(dx.x) || !std::isfinite(dx.y) || !std::isfinite(dy.x) || !std::isfinite(dy.y))
+        return rgb_nan();
+    const u32 top = t.level_count - 1u;
+    const rp_texture_level *mips = im.levels.data() + t.level_begin;
+    const u32 x_bits = std::max(ewa_magnitude(dx.x), ewa_magnitude(dx.y));
+    const u32 y_bits = std::max(ewa_magnitude(dy.x), ewa_magnitude(dy.y));
+    const bool zero = x_bits == 0u || y_bits == 0u;
+    float minor = 0.0f;
+    if (!zero) {
+        if (std::max(x_bits, y_bits) >= std::bit_cast<u32>(32.0f)) {
+            minor = 2.0f;
+        } else {
+            const bool lifted = ewa_subnormal(ewa_magnitude(dx.x)) || ewa_subnormal(ewa_magnitude(dx.y)) ||
+                                ewa_subnormal(ewa_magnitude(dy.x)) || ewa_subnormal(ewa_magnitude(dy.y));
+            const F2 a = lifted ? F2{ewa_lift(dx.x), ewa_lift(dx.y)} : dx;
+            const F2 b = lifted ? F2{ewa_lift(dy.x), ewa_lift(dy.y)} : dy;
+            const float x_scale = std::max(std::fabs(a.x), std::fabs(a.y));
+            const float y_scale = std::max(std::fabs(b.x), std::fabs(b.y));
+            const F2 x{a.x / x_scale, a.y / x_scale}, y{b.x / y_scale, b.y / y_scale};
+            const float x_norm = std::sqrt(x.x * x.x + x.y * x.y), y_norm = std::sqrt(y.x * y.x + y.y * y.y);
+            const float x_length = x_scale * x_norm, y_length = y_scale * y_norm;
+            const bool x_major = x_length >= y_length;
+            const float major = x_major ? x_length : y_length;
+            minor = x_major ? y_length : x_length;
+            const float capped = major / cap;
+            if (minor < capped) {
+                const float actual = lifted ? capped * 0x1p-24f : capped;
+                if (x_major)
+                    dy = {(y.x / y_norm) * actual, (y.y / y_norm) * actual};
+                else
+                    dx = {(x.x / x_norm) * actual, (x.y / x_norm) * actual};
+                minor = capped;
+            }
+            if (lifted)
+                minor *= 0x1p-24f;
+        }
+        if (minor >= 2.0f) {
+            if (!ewa_level_valid(im, mips[top], t.texel_format, 0))
+                return rgb_nan();
+            return image_texel(im, mips[top], 0, 0, t.wrap, t.texel_format, t.transfer_offset);
+        }
+    }
+    F2 st = uv;
+    if (!mapped)
+        st = {ewa_product(uv.x, t.uscale) + t.udelta, ewa_product(uv.y, t.vscale) + t.vdelta};
+    st.y = 1.0f - st.y;
+    if (!std::isfinite(st.x) || !std::isfinite(st.y))
+        return rgb_nan();
+    if (zero) {
+        if (!ewa_level_valid(im, mips[0], t.texel_format, top))
+            return rgb_nan();
+        const F2 dims{float(mips[0].width), float(mips[0].height)};
+        if (t.wrap == RP_WRAP_BLACK && ewa_black_disjoint(st, dims, {1.0f, 1.0f}))
+            return {};
+        const F2 center{ewa_center(st.x, dims.x, t.wrap), ewa_center(st.y, dims.y, t.wrap)};
+        return image_bilinear_texels(im, t, mips[0], center, scalar);
+    }
+    const float lod = std::max(0.0f, float(top) + std::log2(minor));
+    const u32 lower = std::min(u32(std::floor(lod)), top);
+    if (!ewa_level_valid(im, mips[lower], t.texel_format, top - lower))
+        return rgb_nan();
+    if (lower < top && (!ewa_level_valid(im, mips[lower + 1u], t.texel_format, top - lower - 1u) ||
+                        mips[lower + 1u].width != std::max(1u, mips[lower].width / 2u) ||
+                        mips[lower + 1u].height != std::max(1u, mips[lower].height / 2u)))
+        return rgb_nan();
+    const Rgb a = ewa_level(im, t, mips[lower], st, dx, dy);
+    const Rgb b = lower == top ? image_texel(im, mips[top], 0, 0, t.wrap, t.texel_format, t.transfer_offset)
+                               : ewa_level(im, t, mips[lower + 1u], st, dx, dy);
+    const float delta = lod - float(lower);
+    return {(1.0f - delta) * a.r + delta * b.r, (1.0f - delta) * a.g + delta * b.g, (1.0f - delta) * a.b + delta * b.b};
+}
+// shaders/image_texture.h:541-554 (lookup_filtered): EWA or the standard filters
+inline Rgb image_lookup(const Images &im, const rp_image_texture &t, F2 uv, F2 dx, F2 dy, bool scalar, bool mapped) {
+    if (t.filter != RP_TEXTURE_EWA)
+        return image_lookup_standard(im, t, uv, dx, dy, scalar, mapped);
+    if (!image_lookup_valid(im, t, uv, dx, dy))
+        return rgb_nan();
+    return image_lookup_ewa(im, t, uv, dx, dy, scalar, mapped);
 }
 
 // shaders/image_texture.h:458-499 (rypath_image::spectrum)

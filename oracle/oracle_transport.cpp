@@ -511,7 +511,7 @@ static void hero_step(const Ctx &c, LaneState &st) {
                 break;
             }
             const rp_image_texture &t = s.images.textures[material.image_texture];
-            image_rgb = image_lookup_standard(s.images, t, uvst, dstdx, dstdy, false, false);
+            image_rgb = image_lookup(s.images, t, uvst, dstdx, dstdy, false, false);
             image_rgb = {image_rgb.r * t.scale, image_rgb.g * t.scale, image_rgb.b * t.scale};
             if (t.invert)
                 image_rgb = {1 - image_rgb.r, 1 - image_rgb.g, 1 - image_rgb.b};

@@ -79,6 +79,7 @@ class Images(C.Structure):
         ("uv_count", u32), ("uvs", P(f32)), ("instance_uv_begin", P(u32)),
         ("frame_count", u32), ("frames", P(f32)), ("instance_frame_begin", P(u32)),
         ("world_from_camera", f32 * 9), ("camera_from_world", f32 * 9),
+        ("ewa_weights", P(f32)),
     ]
 
 
@@ -251,6 +252,6 @@ EXPECTED_SIZES = {
     "rp_view": (View, 80), "rp_batch_config": (BatchConfig, 24), "rp_batch_request": (BatchRequest, 64),
     "rp_adjoint_request": (AdjointRequest, 104),
     "rp_image_texture": (ImageTexture, 72), "rp_texture_level": (TextureLevel, 12),
-    "rp_images": (Images, 240),
+    "rp_images": (Images, 248),
     "rp_frame_config": (FrameConfig, 32), "rp_frame_request": (FrameRequest, 24), "rp_frame_info": (FrameInfo, 56),
 }

@@ -9,14 +9,19 @@
 // Beyond that boundary, cuda_backend::FilmRenderer (cuda_render.hpp) renders whole batches into
 // rypath's Film on the device (the PacketFilmBatch reduction done there, film_fold.hpp).
 #include "cuda_render.hpp"
+#include "ewa_weights.h"
 #include "film_fold.hpp"
 #include "frame_session.hpp"
+#include "image_texture.hpp"
 #include "metal_render.hpp"
+#include "rgb_spectrum.hpp"
 #include "sampling.hpp"
+#include "texture_footprint.hpp"
 
 #include <rypath_cuda.h>
 
 #include <algorithm>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -59,6 +64,12 @@ template <class Array> void copy_spectrum(const Array &from, float (&to)[RP_SPEC
 // deep-copies everything).
 struct Arena {
     std::vector<float> positions, normals, environment;
+    // images in the wire layout (src/render_wire.h:35-95)
+    std::vector<rp_image_texture> textures;
+    std::vector<rp_texture_level> levels;
+    std::vector<std::uint32_t> texels, uv_begin, frame_begin;
+    std::vector<float> transfer, uvs, frames;
+    rp_images images{};
     std::vector<std::uint32_t> triangles;
     std::vector<rp_instance> instances;
     std::vector<rp_material> materials;
@@ -73,6 +84,115 @@ std::uint32_t append_knots(const std::vector<SpectralKnot> &from, Arena &a) {
     for (const auto &k : from)
         a.knots.push_back({k.wavelength, k.value});
     return begin;
+}
+
+// The scene's images as the backend reads them (RenderScene::image_textures, texture_camera,
+// instance_texture_frames and environment_image, src/render.hpp:251-261): each distinct
+// pyramid's levels once, rypath's sRGB and linear transfer tables (then any custom ones), the
+// uvs of the meshes of textured instances and each instance's triangle frames.  The sRGB
+// reconstruction table, D65 and the EWA weights are rypath's own.
+std::string describe_images(const RenderScene &s, Arena &a) {
+    if (s.image_textures.empty() && s.environment_image == UINT32_MAX)
+        return {};
+    a.transfer.resize(512);
+    std::ranges::copy(image_transfer_table(ImageEncoding::srgb), a.transfer.begin());
+    std::ranges::copy(image_transfer_table(ImageEncoding::linear), a.transfer.begin() + 256);
+    std::map<const std::array<float, 256> *, std::uint32_t> custom;
+    std::map<const ImagePyramid *, std::uint32_t> chains;
+    for (const ImageTexture &texture : s.image_textures) {
+        if (!texture.image)
+            return "image texture without a pyramid";
+        if (texture.gltf_sampler)
+            return "the CUDA backend does not render glTF image textures";
+        const ImagePyramid &image = *texture.image;
+        rp_image_texture t{};
+        t.filter = texture.filter == ImageFilter::point       ? RP_TEXTURE_POINT
+                   : texture.filter == ImageFilter::trilinear ? RP_TEXTURE_TRILINEAR
+                   : texture.filter == ImageFilter::ewa       ? RP_TEXTURE_EWA
+                                                              : RP_TEXTURE_BILINEAR;
+        t.texel_format = image.storage == ImageStorage::linear_float  ? RP_TEXELS_FLOAT
+                         : image.storage == ImageStorage::linear_half ? RP_TEXELS_HALF
+                         : image.encoding != ImageEncoding::srgb      ? RP_TEXELS_LINEAR8
+                                                                      : RP_TEXELS_SRGB8;
+        t.transfer_offset = image.encoding == ImageEncoding::srgb ? 0 : 256;
+        if (image.custom_transfer) {
+            const auto [it, fresh] = custom.try_emplace(image.custom_transfer.get(), std::uint32_t(a.transfer.size()));
+            t.transfer_offset = it->second;
+            if (fresh)
+                a.transfer.insert(a.transfer.end(), image.custom_transfer->begin(), image.custom_transfer->end());
+        }
+        const auto [chain, added] = chains.try_emplace(&image, std::uint32_t(a.levels.size()));
+        if (added) {
+            const auto base = std::uint32_t(a.texels.size());
+            for (const ImageMipLevel &l : image.levels)
+                a.levels.push_back({l.width, l.height, base + l.offset});
+            a.texels.insert(a.texels.end(), image.texels.begin(), image.texels.end());
+        }
+        t.level_begin = chain->second;
+        t.level_count = std::uint32_t(image.levels.size());
+        t.wrap = std::uint32_t(image.wrap);
+        t.uscale = texture.uscale;
+        t.vscale = texture.vscale;
+        t.udelta = texture.udelta;
+        t.vdelta = texture.vdelta;
+        t.scale = texture.scale;
+        t.invert = texture.invert ? 1u : 0u;
+        t.max_anisotropy = texture.max_anisotropy;
+        t.channels = image.source_channels;
+        t.wrap_t = 10497;
+        t.min_filter = 9987;
+        t.mag_filter = 9729;
+        a.textures.push_back(t);
+    }
+    // texture coordinates of the instances whose shading reads a texture context
+    std::map<std::uint32_t, std::uint32_t> mesh_uvs;
+    const bool framed = !s.instance_texture_frames.empty();
+    for (std::size_t i = 0; i < s.geometry.instances.size(); ++i) {
+        std::uint32_t uv = RP_NONE, frame = RP_NONE;
+        const std::uint32_t mesh_index = s.geometry.instances[i].mesh_index;
+        const GeometryMesh &mesh = s.geometry.meshes[mesh_index];
+        if (framed && !s.instance_texture_frames[i].empty()) {
+            frame = std::uint32_t(a.frames.size() / 6);
+            for (const TextureTriangleFrame &f : s.instance_texture_frames[i])
+                a.frames.insert(a.frames.end(), {f.dpdu.x, f.dpdu.y, f.dpdu.z, f.dpdv.x, f.dpdv.y, f.dpdv.z});
+            if (!mesh.uvs.empty()) {
+                const auto [it, fresh] = mesh_uvs.try_emplace(mesh_index, std::uint32_t(a.uvs.size() / 2));
+                uv = it->second;
+                if (fresh)
+                    for (const auto &c : mesh.uvs)
+                        a.uvs.insert(a.uvs.end(), {c[0], c[1]});
+            }
+        }
+        a.uv_begin.push_back(uv);
+        a.frame_begin.push_back(frame);
+    }
+    rp_images &im = a.images;
+    im = {};
+    im.texture_count = std::uint32_t(a.textures.size());
+    im.textures = a.textures.data();
+    im.level_count = std::uint32_t(a.levels.size());
+    im.levels = a.levels.data();
+    im.texel_word_count = std::uint32_t(a.texels.size());
+    im.texels = a.texels.data();
+    im.transfer_count = std::uint32_t(a.transfer.size());
+    im.transfer = a.transfer.data();
+    im.rgb_table = srgb_reconstruction_table().data();
+    im.illuminant = pbrt_d65().data();
+    im.ewa_weights = rypath_ewa::weights;
+    im.environment_image = s.environment_image;
+    im.environment_scale = s.environment_image_scale;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+            im.environment_from_world[3 * r + c] = float(s.environment_texture_from_world.values[4 * r + c]);
+    im.uv_count = std::uint32_t(a.uvs.size() / 2);
+    im.uvs = a.uvs.data();
+    im.instance_uv_begin = a.uv_begin.data();
+    im.frame_count = std::uint32_t(a.frames.size() / 6);
+    im.frames = a.frames.data();
+    im.instance_frame_begin = a.frame_begin.data();
+    std::copy(s.texture_camera.world_from_camera.begin(), s.texture_camera.world_from_camera.end(), im.world_from_camera);
+    std::copy(s.texture_camera.camera_from_world.begin(), s.texture_camera.camera_from_world.end(), im.camera_from_world);
+    return {};
 }
 
 // RenderScene -> rp_scene_desc: what build_metal_renderer reads on the PT / hero path
@@ -99,8 +219,8 @@ std::string describe(const RenderScene &s, Arena &a, rp_scene_desc &d) {
                 a.normals.insert(a.normals.end(), {n.x, n.y, n.z});
         }
     }
-    if (!s.image_textures.empty() || s.environment_image != UINT32_MAX)
-        return "the CUDA backend renders constant and sampled spectra (no image textures)";
+    if (const std::string images = describe_images(s, a); !images.empty())
+        return images;
     for (std::size_t i = 0; i < s.geometry.instances.size(); ++i) {
         const GeometryInstance &g = s.geometry.instances[i];
         rp_instance in{};
@@ -136,6 +256,10 @@ std::string describe(const RenderScene &s, Arena &a, rp_scene_desc &d) {
         w.first_material = m.surface.first_material;
         w.second_material = m.surface.second_material;
         w.mix_amount = m.surface.mix_amount;
+        w.image_texture = m.image_texture;
+        if (m.kind == SpectralMaterialKind::rgb_sigmoid || m.kind == SpectralMaterialKind::texture_graph ||
+            m.bump_root != UINT32_MAX || m.normal_map != UINT32_MAX || m.table || m.texture_root != UINT32_MAX)
+            return "the CUDA backend renders sampled, constant, blackbody and image reflectance without surface detail";
         a.materials.push_back(w);
     }
     for (const AreaEmission &e : s.area_emissions) {
@@ -200,6 +324,7 @@ std::string describe(const RenderScene &s, Arena &a, rp_scene_desc &d) {
     d.media = a.media.data();
     d.camera_medium = s.camera_medium; // no_medium == RP_NONE
     d.environment = a.environment.data();
+    d.images = a.textures.empty() && s.environment_image == UINT32_MAX ? nullptr : &a.images;
     const RasterCamera &c = *s.raster_camera;
     const GeometryPoint *points[4] = {&c.origin, &c.corner, &c.dx, &c.dy};
     float *dst[4] = {d.camera.origin, d.camera.corner, d.camera.dx, d.camera.dy};

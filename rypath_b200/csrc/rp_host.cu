@@ -741,6 +741,8 @@ void upload_images(const rp_images *im, u32 instances, DImages &g, std::vector<v
         g.inst_uv_begin = dupload(own, im->instance_uv_begin, instances, stm);
     if (im->instance_frame_begin)
         g.inst_frame_begin = dupload(own, im->instance_frame_begin, instances, stm);
+    if (im->ewa_weights)
+        g.ewa_weights = dupload(own, im->ewa_weights, 128, stm);
     memcpy(g.world_from_camera, im->world_from_camera, sizeof(g.world_from_camera));
     memcpy(g.camera_from_world, im->camera_from_world, sizeof(g.camera_from_world));
     if (im->texture_count) {
@@ -1855,8 +1857,8 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
                 continue;
             if (!d->images || m.image_texture >= d->images->texture_count)
                 throw Invalid{"image reflectance names no image texture"};
-            if (d->images->textures[m.image_texture].filter == RP_TEXTURE_EWA)
-                throw NotBuilt{"EWA-filtered image reflectance is not built (point, bilinear and trilinear are)"};
+            if (d->images->textures[m.image_texture].filter == RP_TEXTURE_EWA && !d->images->ewa_weights)
+                throw Invalid{"an EWA-filtered image needs the EWA weight table"};
             if (!d->images->instance_frame_begin || (d->images->uv_count && !d->images->instance_uv_begin))
                 throw Invalid{"image reflectance needs per-instance texture frames"};
         }

@@ -53,6 +53,7 @@ struct DImages {
     u32 textured;
     float tex_spp_scale;
     float tex_min_dx[3], tex_min_dy[3];
+    const float *ewa_weights; // PBRT's 128-entry EWA Gaussian table
 };
 
 // The quiet NaN of C's NAN, so that failed lookups read like the host's
@@ -234,6 +235,194 @@ RP_DEV RGB lookup_standard(const DImages &im, const DImageTexture &t, F2 uv, F2 
     const float delta = lod - float(index);
     return rgb3((1.0f - delta) * lower.r + delta * upper.r, (1.0f - delta) * lower.g + delta * upper.g,
                 (1.0f - delta) * lower.b + delta * upper.b);
+}
+
+// ------------------------------------------------------------------ EWA
+// PBRT's elliptically weighted average (shaders/image_texture.h:134-388): the footprint's
+// ellipse, its minor axis capped by the anisotropy limit, filtered with a Gaussian on the two
+// power-of-two mip levels around the minor axis and blended between them.
+RP_DEV u32 ewa_magnitude(float v) { return __float_as_uint(v) & 0x7fffffffu; }
+RP_DEV bool ewa_subnormal(u32 m) { return m != 0u && m < 0x00800000u; }
+// value * scale, correctly rounded with gradual underflow, reconstructed from the
+// significands when an operand or the product is subnormal (shaders/image_texture.h:168-204)
+RP_DEV float ewa_product(float value, float scale) {
+    const float mapped = value * scale;
+    const u32 a = ewa_magnitude(value), b = ewa_magnitude(scale);
+    if (a == 0u || b == 0u || (ewa_magnitude(mapped) != 0u && !ewa_subnormal(a) && !ewa_subnormal(b)))
+        return mapped;
+    const int a_exp = int(a >> 23), b_exp = int(b >> 23);
+    const u32 a_sig = (a & 0x007fffffu) | (a_exp == 0 ? 0u : 0x00800000u);
+    const u32 b_sig = (b & 0x007fffffu) | (b_exp == 0 ? 0u : 0x00800000u);
+    const u64 product = u64(a_sig) * b_sig;
+    const int exponent = max(1, a_exp) + max(1, b_exp) - 300;
+    const int leading = 63 - __clzll((long long)product);
+    const u32 sign = (__float_as_uint(value) ^ __float_as_uint(scale)) & 0x80000000u;
+    if (exponent + leading > 127)
+        return __uint_as_float(sign | 0x7f800000u);
+    const int shift = max(leading - 23, -149 - exponent);
+    if (shift > 48)
+        return __uint_as_float(sign);
+    u32 rounded;
+    if (shift <= 0) {
+        rounded = u32(product << -shift);
+    } else {
+        const u64 halfway = u64(1) << (shift - 1);
+        const u64 truncated = product >> shift;
+        rounded = u32((product + halfway - 1u + (truncated & 1u)) >> shift);
+    }
+    return __uint_as_float(sign | ((u32(exponent + shift + 149) << 23) + rounded));
+}
+// shaders/image_texture.h:206-211
+RP_DEV float ewa_lift(float v) {
+    const u32 m = ewa_magnitude(v);
+    if (ewa_subnormal(m))
+        return copysignf(float(m) * 0x1p-125f, v);
+    return v * 0x1p24f;
+}
+// shaders/image_texture.h:141-152: the filter centre in texel space, keeping the sub-texel phase
+// of large coordinates
+RP_DEV float ewa_center(float st, float dimension, u32 wrap) {
+    if (fabsf(st) <= 64.0f || wrap == kWrapBlack)
+        return st * dimension - 0.5f;
+    const float phase = fmodf(st, 1.0f) * dimension;
+    if (wrap == kWrapRepeat)
+        return phase - 0.5f;
+    return ((st < 0.0f ? -64.0f : dimension + 64.0f) + phase) - 0.5f;
+}
+// shaders/image_texture.h:154-159
+RP_DEV bool ewa_black_axis(float s, float d, float r) {
+    return fabsf(s) > 64.0f && (s < (0.5f - r) / d || s > ((d - 0.5f) + r) / d);
+}
+// shaders/image_texture.h:134-139
+RP_DEV bool ewa_level_valid(const DImages &im, const DLevel &l, u32 format, u32 levels_above) {
+    return valid_level(l, im.texel_word_count, format) && (l.width & (l.width - 1u)) == 0u &&
+           (l.height & (l.height - 1u)) == 0u && max(l.width, l.height) == (1u << levels_above);
+}
+// shaders/image_texture.h:213-256
+RP_DEV RGB ewa_level(const DImages &im, const DImageTexture &t, const DLevel &l, F2 st, F2 dx, F2 dy) {
+    const F2 dims = f2(float(l.width), float(l.height));
+    const F2 u = f2(dx.x * dims.x, dx.y * dims.y), v = f2(dy.x * dims.x, dy.y * dims.y);
+    const float area = u.x * v.y - u.y * v.x;
+    const float determinant = ((1.0f + (u.x * u.x + u.y * u.y)) + (v.x * v.x + v.y * v.y)) + area * area;
+    const F2 radius = f2(sqrtf((1.0f + u.x * u.x) + v.x * v.x), sqrtf((1.0f + u.y * u.y) + v.y * v.y));
+    if (t.wrap == kWrapBlack && (ewa_black_axis(st.x, dims.x, radius.x) || ewa_black_axis(st.y, dims.y, radius.y)))
+        return rgb3(0, 0, 0);
+    const F2 center = f2(ewa_center(st.x, dims.x, t.wrap), ewa_center(st.y, dims.y, t.wrap));
+    const float bx = ceilf(center.x - radius.x), by = ceilf(center.y - radius.y);
+    const float ex = floorf(center.x + radius.x), ey = floorf(center.y + radius.y);
+    const float cx = (ex - bx) + 1.0f, cy = (ey - by) + 1.0f;
+    if (!isfinite(bx) || !isfinite(by) || !isfinite(ex) || !isfinite(ey) || fabsf(bx) > 0x1p19f || fabsf(by) > 0x1p19f ||
+        fabsf(ex) > 0x1p19f || fabsf(ey) > 0x1p19f || cx <= 0.0f || cy <= 0.0f || cx * cy > 4096.0f)
+        return rgb_nan();
+    if (t.wrap == kWrapBlack && (ex < 0.0f || ey < 0.0f || bx >= dims.x || by >= dims.y))
+        return rgb3(0, 0, 0);
+    const int x0 = int(bx), y0 = int(by), x1 = int(ex), y1 = int(ey);
+    RGB sum = rgb3(0, 0, 0);
+    float weight_sum = 0;
+    for (int y = y0; y <= y1; ++y)
+        for (int x = x0; x <= x1; ++x) {
+            const float ddx = float(x) - center.x, ddy = float(y) - center.y;
+            const float a = u.x * ddy - u.y * ddx, b = v.x * ddy - v.y * ddx;
+            const float r2 = (((ddx * ddx + ddy * ddy) + a * a) + b * b) / determinant;
+            if (r2 < 1.0f) {
+                const float w = __ldg(im.ewa_weights + min(u32(128.0f * r2), 127u));
+                const RGB c = texel(im, l, x, y, t.wrap, t.texel_format, t.transfer_offset);
+                sum = rgb3(sum.r + w * c.r, sum.g + w * c.g, sum.b + w * c.b);
+                weight_sum += w;
+            }
+        }
+    if (!(isfinite(weight_sum) && weight_sum > 0.0f))
+        return rgb_nan();
+    return rgb3(sum.r / weight_sum, sum.g / weight_sum, sum.b / weight_sum);
+}
+// shaders/image_texture.h:258-388
+RP_DEV RGB lookup_ewa(const DImages &im, const DImageTexture &t, F2 uv, F2 dx, F2 dy, bool scalar, bool mapped) {
+    const float cap = t.max_anisotropy;
+    if (t.level_count > 14u || !(cap >= 1.0f && cap <= 16.0f) || !isfinite(t.uscale) || !isfinite(t.vscale) ||
+        !isfinite(t.udelta) || !isfinite(t.vdelta) || !im.ewa_weights)
+        return rgb_nan();
+    if (!mapped) {
+        dx = f2(ewa_product(dx.x, t.uscale), ewa_product(dx.y, t.vscale));
+        dy = f2(ewa_product(dy.x, t.uscale), ewa_product(dy.y, t.vscale));
+    }
+    if (!isfinite(dx.x) || !isfinite(dx.y) || !isfinite(dy.x) || !isfinite(dy.y))
+        return rgb_nan();
+    const u32 top = t.level_count - 1u;
+    const DLevel *mips = im.levels + t.level_begin;
+    const u32 x_bits = max(ewa_magnitude(dx.x), ewa_magnitude(dx.y));
+    const u32 y_bits = max(ewa_magnitude(dy.x), ewa_magnitude(dy.y));
+    const bool zero = x_bits == 0u || y_bits == 0u;
+    float minor = 0.0f;
+    if (!zero) {
+        if (max(x_bits, y_bits) >= __float_as_uint(32.0f)) {
+            minor = 2.0f;
+        } else {
+            const bool lifted = ewa_subnormal(ewa_magnitude(dx.x)) || ewa_subnormal(ewa_magnitude(dx.y)) ||
+                                ewa_subnormal(ewa_magnitude(dy.x)) || ewa_subnormal(ewa_magnitude(dy.y));
+            const F2 a = lifted ? f2(ewa_lift(dx.x), ewa_lift(dx.y)) : dx;
+            const F2 b = lifted ? f2(ewa_lift(dy.x), ewa_lift(dy.y)) : dy;
+            const float x_scale = fmaxf(fabsf(a.x), fabsf(a.y)), y_scale = fmaxf(fabsf(b.x), fabsf(b.y));
+            const F2 x = f2(a.x / x_scale, a.y / x_scale), y = f2(b.x / y_scale, b.y / y_scale);
+            const float x_norm = sqrtf(x.x * x.x + x.y * x.y), y_norm = sqrtf(y.x * y.x + y.y * y.y);
+            const float x_length = x_scale * x_norm, y_length = y_scale * y_norm;
+            const bool x_major = x_length >= y_length;
+            const float major = x_major ? x_length : y_length;
+            minor = x_major ? y_length : x_length;
+            const float capped = major / cap;
+            if (minor < capped) {
+                const float actual = lifted ? capped * 0x1p-24f : capped;
+                if (x_major)
+                    dy = f2((y.x / y_norm) * actual, (y.y / y_norm) * actual);
+                else
+                    dx = f2((x.x / x_norm) * actual, (x.y / x_norm) * actual);
+                minor = capped;
+            }
+            if (lifted)
+                minor *= 0x1p-24f;
+        }
+        if (minor >= 2.0f) {
+            if (!ewa_level_valid(im, mips[top], t.texel_format, 0))
+                return rgb_nan();
+            return texel(im, mips[top], 0, 0, t.wrap, t.texel_format, t.transfer_offset);
+        }
+    }
+    F2 st = uv;
+    if (!mapped)
+        st = f2(ewa_product(uv.x, t.uscale) + t.udelta, ewa_product(uv.y, t.vscale) + t.vdelta);
+    st.y = 1.0f - st.y;
+    if (!isfinite(st.x) || !isfinite(st.y))
+        return rgb_nan();
+    if (zero) {
+        if (!ewa_level_valid(im, mips[0], t.texel_format, top))
+            return rgb_nan();
+        const F2 dims = f2(float(mips[0].width), float(mips[0].height));
+        if (t.wrap == kWrapBlack && (ewa_black_axis(st.x, dims.x, 1.0f) || ewa_black_axis(st.y, dims.y, 1.0f)))
+            return rgb3(0, 0, 0);
+        return bilinear_texels(im, t, mips[0], f2(ewa_center(st.x, dims.x, t.wrap), ewa_center(st.y, dims.y, t.wrap)),
+                               scalar);
+    }
+    const float lod = fmaxf(0.0f, float(top) + log2f(minor));
+    const u32 lower = min(u32(floorf(lod)), top);
+    if (!ewa_level_valid(im, mips[lower], t.texel_format, top - lower))
+        return rgb_nan();
+    if (lower < top && (!ewa_level_valid(im, mips[lower + 1u], t.texel_format, top - lower - 1u) ||
+                        mips[lower + 1u].width != max(1u, mips[lower].width / 2u) ||
+                        mips[lower + 1u].height != max(1u, mips[lower].height / 2u)))
+        return rgb_nan();
+    const RGB a = ewa_level(im, t, mips[lower], st, dx, dy);
+    const RGB b = lower == top ? texel(im, mips[top], 0, 0, t.wrap, t.texel_format, t.transfer_offset)
+                               : ewa_level(im, t, mips[lower + 1u], st, dx, dy);
+    const float delta = lod - float(lower);
+    return rgb3((1.0f - delta) * a.r + delta * b.r, (1.0f - delta) * a.g + delta * b.g,
+                (1.0f - delta) * a.b + delta * b.b);
+}
+// shaders/image_texture.h:541-554 (lookup_filtered)
+RP_DEV RGB lookup_filtered(const DImages &im, const DImageTexture &t, F2 uv, F2 dx, F2 dy, bool scalar, bool mapped) {
+    if (t.filter != kFilterEwa)
+        return lookup_standard(im, t, uv, dx, dy, scalar, mapped);
+    if (!valid_lookup(im, t, uv, dx, dy))
+        return rgb_nan();
+    return lookup_ewa(im, t, uv, dx, dy, scalar, mapped);
 }
 
 // ------------------------------------------------------------------ RGB -> spectrum

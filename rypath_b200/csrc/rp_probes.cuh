@@ -175,11 +175,11 @@ __global__ void k_probe_image_lookup(const DImages im, u32 index, const float *q
     float *o = out + 4 * i;
     const DImageTexture t = im.textures[index];
     const F2 uv = f2(a[0], a[1]), dx = f2(a[2], a[3]), dy = f2(a[4], a[5]);
-    const RGB c = lookup_standard(im, t, uv, dx, dy, false, false);
+    const RGB c = lookup_filtered(im, t, uv, dx, dy, false, false);
     o[0] = c.r;
     o[1] = c.g;
     o[2] = c.b;
-    o[3] = lookup_standard(im, t, uv, dx, dy, true, false).r;
+    o[3] = lookup_filtered(im, t, uv, dx, dy, true, false).r;
 }
 __global__ void k_probe_rgb_spectrum(const float *table, const float *q, u32 count, float *out) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -443,7 +443,7 @@ RP_DEV bool texture_context(const DeviceScene &s, const WaveParams &p, u32 pixel
 // (shaders/packet_walk.h:39-49)
 RP_DEV RGB image_reflectance_rgb(const DImages &im, u32 texture, F2 st, F2 dstdx, F2 dstdy) {
     const DImageTexture t = im.textures[texture];
-    RGB c = lookup_standard(im, t, st, dstdx, dstdy, false, false);
+    RGB c = lookup_filtered(im, t, st, dstdx, dstdy, false, false);
     c = rgb3(c.r * t.scale, c.g * t.scale, c.b * t.scale);
     if (t.invert)
         c = rgb3(1 - c.r, 1 - c.g, 1 - c.b);

@@ -19,6 +19,9 @@ to them:
   coefficients, binary32.  Stored byte-planed (every float's byte 0, then byte 1, ...) and
   xz-compressed; ``rgb_table()`` in ``rypath_b200/images.py`` restores it and checks the
   SHA-256 that rypath's extraction script pins.
+* ``ewa_weights.bin`` -- PBRT v4's 128-entry EWA filter table (``MIPFilterLUT`` of
+  ``src/pbrt/util/mipmap.cpp``; Apache-2.0), as rypath carries it in ``src/ewa_weights.h``:
+  128 binary32.
 * ``d65_dense.bin`` -- PBRT's luminance-normalised stdillum-D65 at 360..830 nm in 1 nm
   steps (471 binary32), the ``pbrt_d65()`` table of ``src/rgb_spectrum.hpp``, from
   ``third_party/pbrt/d65.inc``.
@@ -95,6 +98,15 @@ def d65_table(reference: Path) -> bytes:
     return struct.pack("<471f", *values)
 
 
+def ewa_table(reference: Path) -> bytes:
+    text = _strip_comments((reference / "src/ewa_weights.h").read_text())
+    body = text[text.index("weights[128] = {"):]
+    values = [float(v) for v in re.findall(r"([0-9.]+(?:e[-+]?\d+)?)f", body[: body.index("};")])]
+    if len(values) != 128:
+        raise SystemExit(f"expected 128 EWA weights, found {len(values)}")
+    return struct.pack("<128f", *values)
+
+
 def main() -> None:
     # the rypath checkout: the first argument, else the RYPATH_REFERENCE environment variable
     source = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RYPATH_REFERENCE")
@@ -106,6 +118,7 @@ def main() -> None:
     (out / "cie_xyz_1931.bin").write_bytes(cie_table(reference))
     (out / "srgb_spectrum.xz").write_bytes(srgb_table(reference))
     (out / "d65_dense.bin").write_bytes(d65_table(reference))
+    (out / "ewa_weights.bin").write_bytes(ewa_table(reference))
 
 
 if __name__ == "__main__":

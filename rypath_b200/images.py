@@ -47,6 +47,12 @@ def d65() -> np.ndarray:
     return np.frombuffer((DATA / "d65_dense.bin").read_bytes(), "<f4").copy()
 
 
+@functools.lru_cache(maxsize=1)
+def ewa_weights() -> np.ndarray:
+    """PBRT's 128-entry EWA Gaussian filter table (rypath_ewa::weights, src/ewa_weights.h)."""
+    return np.frombuffer((DATA / "ewa_weights.bin").read_bytes(), "<f4").copy()
+
+
 def srgb_transfer() -> np.ndarray:
     """8-bit sRGB code values to linear (IEC 61966-2-1), as 256 binary32."""
     c = np.arange(256, dtype=np.float64) / 255.0
@@ -167,6 +173,7 @@ class ImageSet:
             im.instance_frame_begin = arr(np.asarray(self.instance_frame_begin, np.uint32), C.c_uint32)
         im.world_from_camera[:] = list(self.world_from_camera)
         im.camera_from_world[:] = list(self.camera_from_world)
+        im.ewa_weights = arr(ewa_weights(), C.c_float)
         return im
 
 

@@ -371,7 +371,7 @@ def cornell_features(feature, width=32, height=32, spp=4, max_depth=8) -> Scene:
     env_image: the area light replaced by an equal-area octahedral sky image (float texels,
     a bright sun shining in through the open front), sampled by its importance tables;
     texture: image reflectance on the back wall (sRGB 8-bit, trilinear, tiled), the floor (float,
-    bilinear) and the tall box (half, point, clamped), under the area light.
+    EWA) and the tall box (half, point, clamped), under the area light.
     """
     if feature not in CORNELL_FEATURES:
         raise ValueError(f"unknown feature {feature!r}")
@@ -473,7 +473,7 @@ def textured_cornell(scene: Scene) -> None:
     back = s.add_image(codes, abi.TEXELS_SRGB8, abi.WRAP_REPEAT, abi.TEXTURE_TRILINEAR, uvscale=(3.0, 2.0))
     stripes = np.stack([0.3 + 0.6 * ((xx % 16) < 8), np.full((64, 64), 0.5), 0.2 + 0.7 * (yy / 63.0)], 2)
     floor = s.add_image([c.astype(np.float32) for c in images.box_pyramid(stripes[:32, :32])], abi.TEXELS_FLOAT,
-                        abi.WRAP_REPEAT, abi.TEXTURE_BILINEAR, uvscale=(2.0, 2.0), uvdelta=(0.25, 0.0))
+                        abi.WRAP_REPEAT, abi.TEXTURE_EWA, uvscale=(2.0, 2.0), uvdelta=(0.25, 0.0))
     noise = rng.uniform(0.05, 0.95, (16, 16, 3)).astype(np.float32)
     box = s.add_image(noise, abi.TEXELS_HALF, abi.WRAP_CLAMP, abi.TEXTURE_POINT)
     first = len(scene.materials)

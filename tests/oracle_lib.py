@@ -23,7 +23,8 @@ _ref_image = None
 
 def _image_args(lib, prefix):
     vp, u32, sz, fp = C.c_void_p, C.c_uint32, C.c_size_t, C.c_float
-    getattr(lib, prefix + "image_lookup").argtypes = [vp, u32, u32, vp, u32, vp, u32, vp, u32, vp, u32, vp]
+    getattr(lib, prefix + "image_lookup").argtypes = [vp, u32, u32, vp, u32, vp, u32, vp, u32, vp, u32, vp] + \
+        ([vp] if prefix == "or_" else [])
     getattr(lib, prefix + "rgb_spectrum").argtypes = [vp, vp, u32, vp]
     getattr(lib, prefix + "environment_queries").argtypes = [vp, u32, u32, vp, u32, vp, u32, vp, u32, vp, vp, vp,
                                                                u32, u32, u32, fp, vp, vp, u32, vp]

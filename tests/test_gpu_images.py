@@ -139,7 +139,7 @@ def test_texture_footprint_probe_bit_exact():
 
 
 def test_texture_statistics():
-    """The textured Cornell box (sRGB trilinear back wall, float bilinear floor, half point box)
+    """The textured Cornell box (sRGB trilinear back wall, float EWA floor, half point box)
     at 48 spp against oracle renders: 3 combined standard errors per pixel, relative RMSE below
     0.2 against a 4096-spp FP64 render and within 30% of an oracle render of the same spp."""
     scene = scenes.cornell_features("texture", 24, 24, 48)
@@ -147,8 +147,8 @@ def test_texture_statistics():
 
 
 def test_texture_refusals():
-    """Image reflectance needs a fixed sample budget; batched views and frame sessions of a
-    textured scene are refused as not built; EWA filtering is refused as not built."""
+    """Image reflectance needs a fixed sample budget; an EWA-filtered image needs the EWA
+    table."""
     scene = scenes.cornell_features("texture", 16, 16, 1)
     built = renderer.build_renderer(scene)
     assert built.status == abi.RP_SUCCESS, built.diagnostic
@@ -161,6 +161,9 @@ def test_texture_refusals():
     assert st == abi.RP_INVALID_ARGUMENT and b"fixed total sample budget" in diag.value
     built.scene.close()
     ewa = scenes.cornell_features("texture", 16, 16, 1)
-    ewa.images.textures[0].filter = abi.TEXTURE_EWA
-    bad = renderer.build_renderer(ewa)
-    assert bad.status == abi.RP_NOT_BUILT and "EWA" in bad.diagnostic
+    keep = []
+    desc = ewa.desc()
+    desc.images.contents.ewa_weights = None
+    out_scene = C.c_void_p()
+    st = native.lib().rp_cuda_scene_create(C.byref(desc), 0, C.byref(out_scene), diag, 256)
+    assert st == abi.RP_INVALID_ARGUMENT and b"EWA" in diag.value

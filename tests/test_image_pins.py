@@ -39,14 +39,15 @@ def wire(imset):
 def lookup(lib, prefix, w, index, q):
     out = np.zeros((q.shape[0], 4), np.float32)
     tex, nt, levels, nl, texels, nw, transfer, ntr = w
+    extra = [images.ewa_weights().ctypes.data] if prefix == "or_" else []
     getattr(lib, prefix + "image_lookup")(C.cast(tex, C.c_void_p), nt, index, levels.ctypes.data, nl,
                                           texels.ctypes.data, nw, transfer.ctypes.data, ntr, q.ctypes.data,
-                                          q.shape[0], out.ctypes.data)
+                                          q.shape[0], out.ctypes.data, *extra)
     return out
 
 
 def texture_set(rng):
-    """Textures of every texel format, wrap and restated filter over seeded mip chains."""
+    """Textures of every texel format, wrap and filter over seeded mip chains."""
     s = images.ImageSet()
     base = rng.uniform(0, 1, (16, 16, 3)).astype(np.float32)
     base[3, 5] = [1, 1, 1]
@@ -63,6 +64,11 @@ def texture_set(rng):
             s.add_image(code_chain, abi.TEXELS_SRGB8, wrap, filt, uvscale=(2.0, 2.0))
         s.add_image([odd], abi.TEXELS_FLOAT, wrap, abi.TEXTURE_BILINEAR)
         s.add_image([code], abi.TEXELS_LINEAR8, wrap, abi.TEXTURE_POINT)
+        # EWA over power-of-two chains, anisotropy caps from none to PBRT's largest
+        for cap in (1.0, 8.0, 16.0):
+            s.add_image([c.astype(np.float32) for c in chain], abi.TEXELS_FLOAT, wrap, abi.TEXTURE_EWA,
+                        uvscale=(1.25, 3.0), uvdelta=(0.3, 0.1), max_anisotropy=cap)
+        s.add_image(code_chain, abi.TEXELS_SRGB8, wrap, abi.TEXTURE_EWA, uvscale=(40.0, 70.0))
     return s
 
 
@@ -79,8 +85,8 @@ def lookup_queries(rng, n):
 
 
 def test_image_lookup_matches_reference():
-    """rypath_image::lookup / lookup_scalar (point, bilinear, trilinear) over float, half, sRGB
-    and linear 8-bit texels with repeat, clamp and black wrap."""
+    """rypath_image::lookup / lookup_scalar (point, bilinear, trilinear, EWA) over float, half,
+    sRGB and linear 8-bit texels with repeat, clamp and black wrap."""
     lib = need_ref()
     rng = np.random.default_rng(40)
     s = texture_set(rng)
