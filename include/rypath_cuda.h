@@ -77,6 +77,7 @@ enum { RP_MIX = 9 };
 enum {
     RP_REFLECTANCE_KNOTS = 0,
     RP_REFLECTANCE_CONSTANT = 1,
+    RP_REFLECTANCE_RGB = 2, /* wire::rgb_sigmoid_material: PBRT RGBAlbedoSpectrum coefficients */
     RP_REFLECTANCE_IMAGE = 3,
     RP_REFLECTANCE_BLACKBODY = 4
 };
@@ -126,6 +127,7 @@ typedef struct rp_material {
     uint32_t first_material, second_material; /* RP_MIX children (MaterialAuxiliary, src/render_wire.h:159) */
     float mix_amount;                         /* RP_MIX constant amount (src/render_wire.h:160) */
     uint32_t image_texture; /* RP_REFLECTANCE_IMAGE: index into images->textures */
+    float coefficients[3];  /* RP_REFLECTANCE_RGB: the sigmoid polynomial's c0 l^2 + c1 l + c2 */
 } rp_material;
 
 /* wire::ImageTexture (src/render_wire.h:68-87), field for field.  level_begin/level_count

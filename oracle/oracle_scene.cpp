@@ -297,7 +297,8 @@ bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error) {
         s.materials.push_back({m.scattering, m.kind, m.knot_begin, m.knot_count, m.scalar_value,
                                m.eta_begin, m.eta_count, m.k_begin, m.k_count, m.optical_extensions,
                                m.u_roughness, m.v_roughness, m.remap_roughness, m.first_material,
-                               m.second_material, m.mix_amount, m.image_texture});
+                               m.second_material, m.mix_amount, m.image_texture,
+                               {m.coefficients[0], m.coefficients[1], m.coefficients[2]}});
         if (m.scattering == RP_DIFFUSE && m.kind == RP_REFLECTANCE_IMAGE)
             s.textured = true;
     }

@@ -69,6 +69,7 @@ struct Material {
     u32 first = RP_NONE, second = RP_NONE; // mix children (MaterialAuxiliary, src/render_wire.h:159-161)
     float mix_amount = 0;
     u32 image_texture = RP_NONE; // RP_REFLECTANCE_IMAGE
+    float coefficients[3] = {0, 0, 0}; // RP_REFLECTANCE_RGB
 };
 struct Positional {
     F3 position;

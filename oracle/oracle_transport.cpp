@@ -52,6 +52,17 @@ static bool reflectance(const Scene &s, const Material &m, float w, const Rgb *i
         rho = m.scalar_value;
     } else if (m.kind == RP_REFLECTANCE_BLACKBODY) {
         rho = blackbody_reflectance(m.scalar_value, w);
+    } else if (m.kind == RP_REFLECTANCE_RGB) {
+        // shaders/render.metal:576-588 (sigmoid_reflectance)
+        const float q = std::fma(std::fma(m.coefficients[0], w, m.coefficients[1]), w, m.coefficients[2]);
+        if (!std::isfinite(q)) {
+            rho = NAN;
+        } else if (std::fabs(q) <= 1.0f) {
+            rho = 0.5f + 0.5f * (q / std::sqrt(1.0f + q * q));
+        } else {
+            const float inverse = 1.0f / q;
+            rho = 0.5f + 0.5f * std::copysign(1.0f / std::sqrt(1.0f + inverse * inverse), q);
+        }
     } else
         return false;
     return std::isfinite(rho) && rho >= 0 && rho <= 1;

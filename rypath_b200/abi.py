@@ -23,7 +23,7 @@ FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = 0, 1, 2
 DIFFUSE, CONDUCTOR, DIELECTRIC = 0, 1, 2
 INTERFACE = 10  # null interface: medium change (scalar transport), pass-through (hero transport)
 MIX = 9  # stochastic mix of two materials
-REFLECTANCE_KNOTS, REFLECTANCE_CONSTANT, REFLECTANCE_IMAGE, REFLECTANCE_BLACKBODY = 0, 1, 3, 4
+REFLECTANCE_KNOTS, REFLECTANCE_CONSTANT, REFLECTANCE_RGB, REFLECTANCE_IMAGE, REFLECTANCE_BLACKBODY = 0, 1, 2, 3, 4
 WRAP_REPEAT, WRAP_CLAMP, WRAP_BLACK = 0, 1, 2
 TEXTURE_BILINEAR, TEXTURE_TRILINEAR, TEXTURE_POINT, TEXTURE_EWA = 0, 1, 2, 3
 TEXELS_SRGB8, TEXELS_LINEAR8, TEXELS_HALF, TEXELS_FLOAT = 0, 1, 2, 3
@@ -52,7 +52,8 @@ class Material(C.Structure):
                 ("scalar_value", f32), ("eta_begin", u32), ("eta_count", u32), ("k_begin", u32),
                 ("k_count", u32), ("optical_extensions", u32), ("u_roughness", f32),
                 ("v_roughness", f32), ("remap_roughness", u32), ("first_material", u32),
-                ("second_material", u32), ("mix_amount", f32), ("image_texture", u32)]
+                ("second_material", u32), ("mix_amount", f32), ("image_texture", u32),
+                ("coefficients", f32 * 3)]
 
 
 class ImageTexture(C.Structure):
@@ -244,7 +245,7 @@ class FrameInfo(C.Structure):
 FRAME_PENDING, FRAME_COMPLETE, FRAME_FAILED = 0, 1, 2
 
 EXPECTED_SIZES = {
-    "rp_instance": (Instance, 88), "rp_material": (Material, 68), "rp_knot": (Knot, 8),
+    "rp_instance": (Instance, 88), "rp_material": (Material, 80), "rp_knot": (Knot, 8),
     "rp_area_emission": (AreaEmission, 1888), "rp_positional_light": (PositionalLight, 1948),
     "rp_medium": (Medium, 5656), "rp_camera": (Camera, 48), "rp_request": (Request, 64),
     "rp_packet_result": (PacketResult, 80), "rp_scalar_result": (ScalarResult, 44),

@@ -257,9 +257,10 @@ std::string describe(const RenderScene &s, Arena &a, rp_scene_desc &d) {
         w.second_material = m.surface.second_material;
         w.mix_amount = m.surface.mix_amount;
         w.image_texture = m.image_texture;
-        if (m.kind == SpectralMaterialKind::rgb_sigmoid || m.kind == SpectralMaterialKind::texture_graph ||
+        std::copy(m.coefficients.begin(), m.coefficients.end(), w.coefficients);
+        if (m.kind == SpectralMaterialKind::texture_graph ||
             m.bump_root != UINT32_MAX || m.normal_map != UINT32_MAX || m.table || m.texture_root != UINT32_MAX)
-            return "the CUDA backend renders sampled, constant, blackbody and image reflectance without surface detail";
+            return "the CUDA backend renders sampled, constant, RGB, blackbody and image reflectance without surface detail";
         a.materials.push_back(w);
     }
     for (const AreaEmission &e : s.area_emissions) {

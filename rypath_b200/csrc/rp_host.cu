@@ -1985,7 +1985,7 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             mats[i] = {m.scattering, m.kind,        m.knot_begin,        m.knot_count,      m.scalar_value,
                        m.eta_begin,  m.eta_count,   m.k_begin,           m.k_count,         m.optical_extensions,
                        m.u_roughness, m.v_roughness, m.remap_roughness,    m.first_material,  m.second_material,
-                       m.mix_amount,  m.image_texture};
+                       m.mix_amount,  m.image_texture, {m.coefficients[0], m.coefficients[1], m.coefficients[2]}};
         }
         ds.materials = dupload(own, mats.data(), mats.size(), stm);
         ds.material_count = d->material_count;

@@ -32,6 +32,7 @@ struct DMaterial {
     u32 first, second; // mix children
     float mix_amount;
     u32 image_texture; // image reflectance (kind 3)
+    float coefficients[3]; // RGB sigmoid reflectance (kind 2)
 };
 struct DPositional {
     float position[3];

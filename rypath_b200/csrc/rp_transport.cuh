@@ -450,6 +450,16 @@ RP_DEV RGB image_reflectance_rgb(const DImages &im, u32 texture, F2 st, F2 dstdx
     return c;
 }
 
+// PBRT's RGBAlbedoSpectrum of a material's sigmoid coefficients (shaders/render.metal:576-588)
+RP_DEV float sigmoid_reflectance(const float *c, float w) {
+    const float p = fmaf(fmaf(c[0], w, c[1]), w, c[2]);
+    if (!isfinite(p))
+        return image_nan();
+    if (fabsf(p) <= 1.0f)
+        return 0.5f + 0.5f * (p / sqrtf(1.0f + p * p));
+    const float inverse = 1.0f / p;
+    return 0.5f + 0.5f * copysignf(1.0f / sqrtf(1.0f + inverse * inverse), p);
+}
 // shaders/packet_walk.h:22-57 (sampled / constant / blackbody / image reflectance; image: the
 // hit's filtered RGB)
 RP_DEV bool material_reflectance(const DeviceScene &s, const DMaterial &m, float w, const RGB *image, float &rho) {
@@ -464,6 +474,8 @@ RP_DEV bool material_reflectance(const DeviceScene &s, const DMaterial &m, float
         rho = m.scalar_value;
     } else if (m.kind == 4) {
         rho = blackbody_reflectance(m.scalar_value, w);
+    } else if (m.kind == 2) {
+        rho = sigmoid_reflectance(m.coefficients, w);
     } else
         return false;
     return isfinite(rho) && rho >= 0 && rho <= 1;

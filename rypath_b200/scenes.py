@@ -371,7 +371,8 @@ def cornell_features(feature, width=32, height=32, spp=4, max_depth=8) -> Scene:
     env_image: the area light replaced by an equal-area octahedral sky image (float texels,
     a bright sun shining in through the open front), sampled by its importance tables;
     texture: image reflectance on the back wall (sRGB 8-bit, trilinear, tiled), the floor (float,
-    EWA) and the tall box (half, point, clamped), under the area light.
+    EWA) and the tall box (half, point, clamped), and RGB (sigmoid) reflectance on the short box,
+    under the area light.
     """
     if feature not in CORNELL_FEATURES:
         raise ValueError(f"unknown feature {feature!r}")
@@ -482,9 +483,15 @@ def textured_cornell(scene: Scene) -> None:
         m.scattering, m.kind, m.image_texture = abi.DIFFUSE, abi.REFLECTANCE_IMAGE, index
         m.remap_roughness = 1
         scene.materials.append(m)
+    # the short box: PBRT RGB reflectance (sigmoid polynomial coefficients, a warm orange)
+    rgb = abi.Material()
+    rgb.scattering, rgb.kind, rgb.remap_roughness = abi.DIFFUSE, abi.REFLECTANCE_RGB, 1
+    rgb.coefficients[:] = [-2.0e-4, 0.24, -68.0]
+    scene.materials.append(rgb)
     scene.instances[2].material = first
     scene.instances[0].material = first + 1
     scene.instances[6].material = first + 2
+    scene.instances[5].material = first + 3
     s.uvs = uv.astype(np.float32)
     s.instance_uv_begin = [inst.vertex_begin for inst in scene.instances]
     s.frames = triangle_frames(scene.positions, scene.triangles, s.uvs)
