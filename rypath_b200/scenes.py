@@ -500,6 +500,23 @@ def textured_cornell(scene: Scene) -> None:
     scene.images = s
 
 
+def with_environment_image(scene: Scene, width=256, seed=2, scale=0.03) -> Scene:
+    """Replace a scene's constant environment by a seeded equal-area octahedral sky image
+    (float texels, images.sky_image) of the given size and radiance scale, the sky's zenith
+    along the scene's +y."""
+    from . import images
+
+    s = scene.images if scene.images is not None else images.ImageSet()
+    s.environment_image = s.add_image(images.sky_image(width, seed=seed), abi.TEXELS_FLOAT, abi.WRAP_CLAMP)
+    s.environment_scale = scale
+    # environment frame: world +y is the map's +z (zenith), world +z its +x
+    s.environment_from_world = (0, 0, 1, 1, 0, 0, 0, 1, 0)
+    scene.images = s
+    scene.environment = None
+    scene.name = scene.name + "_env_image"
+    return scene
+
+
 def crop(scene: Scene, x0: int, y0: int, width: int, height: int) -> Scene:
     """The window [x0, x0 + width) x [y0, y0 + height) of a scene's film as a scene of its own:
     the same geometry, lights and materials, its raster camera narrowed to the window."""
