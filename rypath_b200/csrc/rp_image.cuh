@@ -430,15 +430,25 @@ RP_DEV float blend1(float t, float a, float b) { return (1.0f - t) * a + t * b; 
 // PBRT's sigmoid-polynomial reconstruction of a bounded reflectance from linear sRGB in
 // [0, 1] (Jakob & Hanika 2019 tables; shaders/image_texture.h:458-499): the largest channel
 // z picks a cell of the 64^3 grid, whose trilinearly blended coefficients give a quadratic
-// in the wavelength, squashed by s(x) = 1/2 + x / (2 sqrt(1 + x^2)).
-RP_DEV float rgb_spectrum(const float *table, RGB c, float wavelength) {
+// in the wavelength, squashed by s(x) = 1/2 + x / (2 sqrt(1 + x^2)).  The coefficients do not
+// depend on the wavelength, so they are blended once (rgb_polynomial) and the squashed
+// quadratic evaluated per wavelength (rgb_polynomial_at); rgb_spectrum does both.
+struct RgbPolynomial {
+    float c0, c1, c2;
+    float value; // the constant result of a grey or invalid input
+    bool constant;
+};
+RP_DEV RgbPolynomial rgb_polynomial(const float *table, RGB c) {
+    RgbPolynomial out{0, 0, 0, image_nan(), true};
     if (!finite_rgb(c))
-        return image_nan();
+        return out;
     c.r = fminf(fmaxf(c.r, 0.0f), 1.0f);
     c.g = fminf(fmaxf(c.g, 0.0f), 1.0f);
     c.b = fminf(fmaxf(c.b, 0.0f), 1.0f);
-    if (c.r == c.g && c.g == c.b)
-        return c.r;
+    if (c.r == c.g && c.g == c.b) {
+        out.value = c.r;
+        return out;
+    }
     const float ch[3] = {c.r, c.g, c.b};
     u32 channel = 0;
     if (c.g >= c.r)
@@ -472,13 +482,25 @@ RP_DEV float rgb_spectrum(const float *table, RGB c, float wavelength) {
                                 blend1(dy, blend1(dx, __ldg(cell + plane), __ldg(cell + plane + 3)),
                                        blend1(dx, __ldg(cell + plane + row), __ldg(cell + plane + row + 3))));
     }
-    const float poly = fmaf(fmaf(coefficient[0], wavelength, coefficient[1]), wavelength, coefficient[2]);
+    out.c0 = coefficient[0];
+    out.c1 = coefficient[1];
+    out.c2 = coefficient[2];
+    out.constant = false;
+    return out;
+}
+RP_DEV float rgb_polynomial_at(const RgbPolynomial &q, float wavelength) {
+    if (q.constant)
+        return q.value;
+    const float poly = fmaf(fmaf(q.c0, wavelength, q.c1), wavelength, q.c2);
     if (!isfinite(poly))
         return image_nan();
     if (fabsf(poly) <= 1.0f)
         return 0.5f + 0.5f * poly / sqrtf(1.0f + poly * poly);
     const float inv = 1.0f / poly;
     return 0.5f + 0.5f * copysignf(1.0f / sqrtf(1.0f + inv * inv), poly);
+}
+RP_DEV float rgb_spectrum(const float *table, RGB c, float wavelength) {
+    return rgb_polynomial_at(rgb_polynomial(table, c), wavelength);
 }
 // PBRT RGBUnboundedSpectrum: the reconstruction of rgb / (2 max) scaled back
 // (shaders/image_texture.h:500-507).
@@ -591,6 +613,61 @@ RP_DEV float environment_image_radiance(const DImages &im, V3 world_direction, f
     return im.env_scale * illuminant_spectrum(im, c, wavelength);
 }
 
+// environment_image_radiance at four wavelengths: the direction, the texel and the RGB's
+// reconstruction coefficients are found once (they do not depend on the wavelength)
+RP_DEV V4 environment_image_radiance4(const DImages &im, V3 world_direction, V4 lambda) {
+    V4 out = v4(image_nan());
+    if (im.env_image >= im.texture_count)
+        return out;
+    const DImageTexture t = im.textures[im.env_image];
+    const V3 d = unit_scaled(mat3_apply(im.env_from_world, world_direction));
+    if (!finite3(d) || !valid_lookup(im, t, f2(0, 0), f2(0, 0), f2(0, 0)) || t.level_count != 1u)
+        return out;
+    const DLevel level = im.levels[t.level_begin];
+    if (!valid_level(level, im.texel_word_count, t.texel_format) || level.width != level.height)
+        return out;
+    const int size = int(level.width);
+    const F2 uv = sphere_to_square(d, true);
+    int px = int(uv.x * float(size)), py = int(uv.y * float(size));
+    if (px == size) {
+        px = size - 1;
+        py = size - 1 - py;
+    }
+    if (py < 0) {
+        px = size - 1 - px;
+        py = -py;
+    } else if (py == size) {
+        px = size - 1 - px;
+        py = size - 1;
+    }
+    if (size == 1)
+        px = py = 0;
+    RGB c = texel(im, level, px, py, kWrapClamp, t.texel_format, t.transfer_offset);
+    // illuminant_spectrum (shaders/image_lighting.h:28-40) with the coefficients shared
+    const bool finite = finite_rgb(c);
+    c = rgb3(fmaxf(0.0f, c.r), fmaxf(0.0f, c.g), fmaxf(0.0f, c.b));
+    const float amplitude = 2.0f * fmaxf(fmaxf(c.r, c.g), c.b);
+    RgbPolynomial q{0, 0, 0, 0, true};
+    if (finite && amplitude != 0)
+        q = rgb_polynomial(im.rgb_table, rgb3(c.r / amplitude, c.g / amplitude, c.b / amplitude));
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float w = lambda.v[k];
+        float value;
+        if (!finite || !isfinite(w)) {
+            value = image_nan();
+        } else if (amplitude == 0) {
+            value = 0;
+        } else {
+            const float nearest = roundf(w);
+            value = nearest < 360.0f || nearest > 830.0f
+                        ? 0.0f
+                        : amplitude * rgb_polynomial_at(q, w) * __ldg(im.illuminant + (u32(nearest) - 360u));
+        }
+        out.v[k] = im.env_scale * value;
+    }
+    return out;
+}
 // shaders/image_lighting.h:210-219
 RP_DEV bool environment_tables_valid(const DImages &im, bool compensated) {
     const u32 w = im.env_width;

@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_const
                         const DMaterial material = s.materials[cmat];
                         // an image reflectance reads its texture at the hit's footprint
                         // (shaders/packet_pt_event_body.inc:147-163, packet_walk.h:39-49)
-                        RGB image_rgb;
+                        RgbPolynomial image_rgb;
                         bool image = false;
                         if constexpr (F == 0) {
                             if (s.img.textured && material.kind == 3 && material.image_texture < s.img.texture_count) {
@@ -316,7 +316,8 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_const
                                     status = 2;
                                     break;
                                 }
-                                image_rgb = image_reflectance_rgb(s.img, material.image_texture, st, dstdx, dstdy);
+                                image_rgb = rgb_polynomial(
+                                    s.img.rgb_table, image_reflectance_rgb(s.img, material.image_texture, st, dstdx, dstdy));
                                 image = true;
                             }
                         }
@@ -415,9 +416,7 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_const
                     bool emission_ok = true;
                     if (ctype == kEnvironment) {
                         if (s.img.env_image != kNone) {
-#pragma unroll
-                            for (int k = 0; k < 4; ++k)
-                                rad.v[k] = environment_image_radiance(s.img, rd, lambda.v[k]);
+                            rad = environment_image_radiance4(s.img, rd, lambda);
                         } else if (s.environment != kNone) {
 #pragma unroll
                             for (int k = 0; k < 4; ++k)
@@ -667,9 +666,7 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_nee(const __grid_constan
                                 if (!sample_environment_image(s.img, u1, u2, true, direction, epdf)) {
                                     li_ok = false;
                                 } else {
-#pragma unroll
-                                    for (int k = 0; k < 4; ++k)
-                                        lrad.v[k] = environment_image_radiance(s.img, direction, lambda.v[k]);
+                                    lrad = environment_image_radiance4(s.img, direction, lambda);
                                     spdf = epdf * choice.pmf;
                                     lp.position = cp.position + (2 * s.scene_radius) * direction;
                                     lp.geometric_normal = lp.shading_normal = -direction;

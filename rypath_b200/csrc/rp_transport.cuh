@@ -460,13 +460,14 @@ RP_DEV float sigmoid_reflectance(const float *c, float w) {
     const float inverse = 1.0f / p;
     return 0.5f + 0.5f * copysignf(1.0f / sqrtf(1.0f + inverse * inverse), p);
 }
-// shaders/packet_walk.h:22-57 (sampled / constant / blackbody / image reflectance; image: the
-// hit's filtered RGB)
-RP_DEV bool material_reflectance(const DeviceScene &s, const DMaterial &m, float w, const RGB *image, float &rho) {
+// shaders/packet_walk.h:22-57 (sampled / constant / blackbody / RGB / image reflectance; image:
+// the reconstruction of the hit's filtered RGB)
+RP_DEV bool material_reflectance(const DeviceScene &s, const DMaterial &m, float w, const RgbPolynomial *image,
+                                 float &rho) {
     if (m.scattering != 0) {
         rho = 1;
     } else if (m.kind == 3 && image && m.image_texture < s.img.texture_count) {
-        rho = rgb_spectrum(s.img.rgb_table, *image, w);
+        rho = rgb_polynomial_at(*image, w);
     } else if (m.kind == 0 && m.knot_count >= 2 && m.knot_begin <= s.knot_count &&
                m.knot_count <= s.knot_count - m.knot_begin) {
         rho = pbrt_reflectance(s.knots + m.knot_begin, m.knot_count, w);
@@ -483,7 +484,7 @@ RP_DEV bool material_reflectance(const DeviceScene &s, const DMaterial &m, float
 // shaders/hero_current_bsdf.h:72-101 with prepare_scattering (shaders/render.metal:2079-2160)
 template <int K>
 RP_DEV bool prepare_bsdf(const DeviceScene &s, const DMaterial &m, V4 lambda, u32 mask, HeroBsdf &out,
-                         const RGB *image = nullptr) {
+                         const RgbPolynomial *image = nullptr) {
     if (m.scattering != u32(K))
         return false;
     out.kind = m.scattering;
