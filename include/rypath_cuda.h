@@ -93,6 +93,10 @@ enum { RP_TEXELS_SRGB8 = 0, RP_TEXELS_LINEAR8 = 1, RP_TEXELS_HALF = 2, RP_TEXELS
 enum { RP_POINT_LIGHT = 0, RP_SPOT_LIGHT = 1 };
 /* Light selection (LightSamplerKind, src/render.hpp:217; wire word src/render_wire.h:304). */
 enum { RP_LIGHTS_BVH = 0, RP_LIGHTS_POWER = 1, RP_LIGHTS_UNIFORM = 2 };
+/* Scene model (RenderModel, src/render.hpp:135): PBRT scenes (raster camera, knot spectra, the
+ * PBRT film) or rypath's demo model (`--render-demo`: a look-at camera, 8-knot reflectances,
+ * a unit equal-energy sky sampled by the light sample, the demo film). */
+enum { RP_MODEL_PBRT = 0, RP_MODEL_DEMO = 1 };
 /* Spectral transport (SpectralTransport, src/render.hpp:218). */
 enum { RP_TRANSPORT_SCALAR = 0, RP_TRANSPORT_HERO = 2 };
 /* Hero wavelength sampling (HeroWavelengthSampling, src/render.hpp:220). */
@@ -128,6 +132,7 @@ typedef struct rp_material {
     float mix_amount;                         /* RP_MIX constant amount (src/render_wire.h:160) */
     uint32_t image_texture; /* RP_REFLECTANCE_IMAGE: index into images->textures */
     float coefficients[3];  /* RP_REFLECTANCE_RGB: the sigmoid polynomial's c0 l^2 + c1 l + c2 */
+    float reflectance[8];   /* RP_MODEL_DEMO sampled reflectance at the 8 demo knots (360 420 470 520 570 620 700 830 nm) */
 } rp_material;
 
 /* wire::ImageTexture (src/render_wire.h:68-87), field for field.  level_begin/level_count
@@ -236,6 +241,11 @@ typedef struct rp_scene_desc {
     /* RP_FILTER_GAUSSIAN: PBRT sigma; the radii are filter_x_radius / filter_y_radius. */
     float filter_sigma;
     const rp_images *images; /* NULL: no image textures and no environment image */
+    /* RP_MODEL_DEMO: the camera is RenderCamera's look-at basis -- camera.origin, camera.corner =
+     * forward, camera.dx = right, camera.dy = up (unit vectors, src/metal_render.mm:194-204) --
+     * and film_scale = tan(vertical fov / 2). */
+    uint32_t model;
+    float film_scale;
 } rp_scene_desc;
 
 /* RenderRequest (src/metal_render.hpp:14-32). */

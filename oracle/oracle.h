@@ -83,9 +83,10 @@ int or_sample_scalar(const or_scene *scene, const rp_request *request, rp_scalar
  * Le, distance, sigma_t, u, wo[3], wi[3], g, ux, uy} -> 8 floats {transmission, emission,
  * valid, flight, phase, sampled direction[3]}. */
 void or_probe_medium(const float *queries, uint32_t count, float *results);
-/* Film reduction of scalar samples in the given order (FilmBatch::add). */
+/* Film reduction of scalar samples in the given order (FilmBatch::add); demo: the demo
+ * model's film (wavelength_xyz, unweighted radiance). */
 int or_scalar_film_add(const rp_scalar_result *results, size_t count, const double *cie_xyz,
-                       uint32_t pixel_count, rp_film_pixel *film);
+                       uint32_t pixel_count, rp_film_pixel *film, int demo);
 
 /* Image probes, in the layouts of oracle/_ref's ref_image_lookup, ref_rgb_spectrum,
  * ref_environment_tables and ref_environment_queries: texture lookups of texture `index`

@@ -222,6 +222,15 @@ inline void primary_ray(const Scene &s, const Params &p, const Sample &smp, F3 &
         d = normalize3(scaled);
         return;
     }
+    if (s.model == RP_MODEL_DEMO) {
+        // the demo camera (shaders/render.metal:470-475): a look-at basis and tan(fov / 2)
+        const float x = (float(smp.pixel % p.width) + ux) / float(p.width);
+        const float y = (float(smp.pixel / p.width) + uy) / float(p.height);
+        const float aspect = float(p.width) / float(p.height);
+        d = normalize3((s.forward + (((2.0f * x - 1.0f) * aspect) * s.film_scale) * s.right) +
+                       ((1.0f - 2.0f * y) * s.film_scale) * s.up);
+        return;
+    }
     d = normalize3(dd / scale);
 }
 

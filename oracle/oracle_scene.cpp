@@ -298,7 +298,9 @@ bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error) {
                                m.eta_begin, m.eta_count, m.k_begin, m.k_count, m.optical_extensions,
                                m.u_roughness, m.v_roughness, m.remap_roughness, m.first_material,
                                m.second_material, m.mix_amount, m.image_texture,
-                               {m.coefficients[0], m.coefficients[1], m.coefficients[2]}});
+                               {m.coefficients[0], m.coefficients[1], m.coefficients[2]},
+                               {m.reflectance[0], m.reflectance[1], m.reflectance[2], m.reflectance[3],
+                                m.reflectance[4], m.reflectance[5], m.reflectance[6], m.reflectance[7]}});
         if (m.scattering == RP_DIFFUSE && m.kind == RP_REFLECTANCE_IMAGE)
             s.textured = true;
     }
@@ -326,6 +328,8 @@ bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error) {
         s.has_environment = std::any_of(s.environment.begin(), s.environment.end(),
                                         [](float v) { return v > 0; });
     }
+    s.model = d.model;
+    s.film_scale = d.film_scale;
     if (const std::string images = load_images(d.images, d.instance_count, s.images); !images.empty()) {
         error = images;
         return false;

@@ -70,6 +70,7 @@ struct Material {
     float mix_amount = 0;
     u32 image_texture = RP_NONE; // RP_REFLECTANCE_IMAGE
     float coefficients[3] = {0, 0, 0}; // RP_REFLECTANCE_RGB
+    float reflectance[8] = {0, 0, 0, 0, 0, 0, 0, 0}; // demo model
 };
 struct Positional {
     F3 position;
@@ -95,6 +96,8 @@ struct Scene {
     bool has_environment = false;
     Images images; // image textures and the environment image (env_image RP_NONE: none)
     bool textured = false; // a diffuse material reads an image
+    u32 model = RP_MODEL_PBRT; // RP_MODEL_DEMO: look-at camera, 8-knot reflectance, unit sky
+    float film_scale = 1;
     // media (scalar transport)
     std::vector<Medium> media;
     u32 camera_medium = RP_NONE, transport = RP_TRANSPORT_HERO;

@@ -365,7 +365,8 @@ Lane scalar_init(const Scene &s, const Params &p, u32 lane) {
     l.wavelength = 360.0f + 470.0f * sample_uniform(p, l.sample.words[2]);
     primary_ray(s, p, l.sample, l.o, l.d);
     l.prev_p = l.o;
-    l.E = s.environment[dense_index(l.wavelength)];
+    // sky_radiance (shaders/render.metal:813-819): the demo sky is unit equal-energy
+    l.E = s.model == RP_MODEL_DEMO ? 1.0f : s.environment[dense_index(l.wavelength)];
     l.current_medium = s.camera_medium;
     return l;
 }
@@ -541,7 +542,7 @@ bool scalar_event(const Ctx &c, Lane &l) {
     }
     if (miss) {
         // shaders/scalar_transport.h:421-433; constant environments have no light density
-        if (l.scatterings != 0u && !l.previous_delta)
+        if (s.model == RP_MODEL_PBRT && l.scatterings != 0u && !l.previous_delta)
             l.escape_weight = power_weight(l.previous_bsdf_pdf, 0.0f);
         l.radiance += l.throughput * l.escape_weight * l.E;
         return true;
@@ -602,8 +603,20 @@ bool scalar_event(const Ctx &c, Lane &l) {
     float rho = 0;
     if (surface.scattering != RP_DIFFUSE)
         return fail(RP_SAMPLE_INVALID_HIT);
-    if (surface.kind == RP_REFLECTANCE_KNOTS && surface.knot_count >= 2 && surface.knot_begin <= s.knots.size() &&
-        surface.knot_count <= s.knots.size() - surface.knot_begin) {
+    if (s.model == RP_MODEL_DEMO) {
+        // demo_reflectance (shaders/render.metal:537-546)
+        if (surface.kind != RP_REFLECTANCE_KNOTS)
+            return fail(RP_SAMPLE_INVALID_HIT);
+        static const float knots[8] = {360, 420, 470, 520, 570, 620, 700, 830};
+        rho = surface.reflectance[7];
+        for (int i = 1; i < 8; ++i)
+            if (l.wavelength <= knots[i]) {
+                const float t = (l.wavelength - knots[i - 1]) / (knots[i] - knots[i - 1]);
+                rho = surface.reflectance[i - 1] + (surface.reflectance[i] - surface.reflectance[i - 1]) * t;
+                break;
+            }
+    } else if (surface.kind == RP_REFLECTANCE_KNOTS && surface.knot_count >= 2 && surface.knot_begin <= s.knots.size() &&
+               surface.knot_count <= s.knots.size() - surface.knot_begin) {
         rho = pbrt_reflectance(s.knots.data() + surface.knot_begin, surface.knot_count, l.wavelength);
     } else if (surface.kind == RP_REFLECTANCE_CONSTANT) {
         rho = surface.scalar_value;
@@ -633,8 +646,36 @@ bool scalar_event(const Ctx &c, Lane &l) {
         return fail(RP_SAMPLE_INVALID_ARITHMETIC);
     const U4 light_words = draw_words(s, p, l.sample, l.index, 2 + 2 * bounce);
     const U4 bsdf_words = draw_words(s, p, l.sample, l.index, 1 + 2 * bounce);
-    // light sample, shaders/scalar_transport.h:783-835
-    {
+    // light sample: the demo sky, uniform on the sphere with the cosine-ratio weight
+    // (shaders/scalar_transport.h:709-781); PBRT lights, :783-835
+    if (s.model == RP_MODEL_DEMO) {
+        const float E = l.E;
+        const float uz = sample_uniform(p, light_words.x), uv = sample_uniform(p, light_words.y);
+        // sphere (shaders/render.metal:821-826)
+        const float z = 1.0f - 2.0f * uz;
+        const float r = std::sqrt(std::max(0.0f, 1.0f - z * z));
+        const float phi = 2.0f * pi_f * uv;
+        const F3 direction{r * std::cos(phi), r * std::sin(phi), z};
+        const float cosine = dot(n, direction);
+        if (E > 0.0f && cosine > 0.0f) {
+            const F3 origin = directional_offset ? spawn_toward(l.o, l.d, hit.t, point, direction) : area_reference;
+            if (!finite3(origin))
+                return fail(RP_SAMPLE_INVALID_ARITHMETIC);
+            const Transmission vis = connection_transmission(
+                c, l.wavelength, origin, direction, INFINITY,
+                outgoing_medium(instance, l.current_medium, point.geometric_normal, direction));
+            if (vis.status != RP_SAMPLE_SUCCESS)
+                return fail(vis.status);
+            if (vis.value > 0) {
+                // (4 cos) * light_weight(cos) (shaders/render.metal:838-841)
+                const float relative = 4.0f * cosine;
+                const float factor = relative * (1.0f / (1.0f + relative * relative));
+                if (!std::isfinite(factor))
+                    return fail(RP_SAMPLE_INVALID_ARITHMETIC);
+                l.radiance += l.throughput * rho * factor * E * vis.value;
+            }
+        }
+    } else {
         const Incident light = light_sample_scalar(s, l.wavelength, point.position, point.shading_normal,
                                                    sample_uniform(p, light_words.x), sample_uniform(p, light_words.y),
                                                    sample_uniform(p, light_words.z));
@@ -782,17 +823,33 @@ void or_probe_medium(const float *q, uint32_t count, float *r) {
 // FilmBatch::add for scalar samples (src/render.cpp:2355-2385) followed by the per-pixel
 // second moments; film rows are rp_film_pixel.  Returns 0, or 1 on an invalid sample.
 int or_scalar_film_add(const rp_scalar_result *results, size_t count, const double *cie_xyz, uint32_t pixel_count,
-                       rp_film_pixel *film) {
+                       rp_film_pixel *film, int demo) {
+    // the demo film's scale (wavelength_xyz, src/render.cpp:2131-2145; integrate_y, :70-77)
+    double integral = (cie_xyz[1] + cie_xyz[3 * 470 + 1]) / 2;
+    for (int i = 1; i + 1 < 471; ++i)
+        integral += cie_xyz[3 * i + 1];
+    const double scale = 470.0 / integral;
     for (size_t i = 0; i < count; ++i) {
         const rp_scalar_result &r = results[i];
         if (r.pixel >= pixel_count || r.status != RP_SAMPLE_SUCCESS || !(r.wavelength >= 360 && r.wavelength <= 830) ||
             !std::isfinite(r.radiance) || r.radiance < 0)
             return 1;
         rp_film_pixel &f = film[r.pixel];
-        const size_t row = size_t(std::round(double(r.wavelength)) - 360.0);
-        const double weighted = 470.0 * double(r.radiance);
+        double xyz[3], weighted;
+        if (demo) {
+            const double offset = double(r.wavelength) - 360.0;
+            const size_t lower = size_t(offset), upper = std::min<size_t>(lower + 1, 470);
+            for (int c = 0; c < 3; ++c)
+                xyz[c] = std::lerp(cie_xyz[3 * lower + c], cie_xyz[3 * upper + c], offset - double(lower)) * scale;
+            weighted = double(r.radiance);
+        } else {
+            const size_t row = size_t(std::round(double(r.wavelength)) - 360.0);
+            for (int c = 0; c < 3; ++c)
+                xyz[c] = cie_xyz[3 * row + c];
+            weighted = 470.0 * double(r.radiance);
+        }
         for (int c = 0; c < 3; ++c) {
-            const double v = cie_xyz[3 * row + c] * weighted;
+            const double v = xyz[c] * weighted;
             const double next = f.sum[c] + v;
             f.correction[c] += std::fabs(f.sum[c]) >= std::fabs(v) ? (f.sum[c] - next) + v : (v - next) + f.sum[c];
             f.sum[c] = next;

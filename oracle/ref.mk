@@ -23,7 +23,30 @@ IMAGE_SRC := $(HERE)ref_image_probe.cpp $(HERE)ref_image_host.cpp $(REF)/src/ima
 IMAGE_FLAGS := $(FLAGS) -I$(REF)/third_party/stb -I$(REF)/third_party/lodepng -I$(REF)/third_party/pbrt \
 	-DRYPATH_SRGB_BIN='"$(REF)/third_party/pbrt/srgb.bin"'
 
-all: $(OUT)/libref.so $(OUT)/libref_image.so $(OUT)/roulette_known_answers
+# the demo model: src/render.cpp with what it links, rypath's CPU demo reference
+# (tests/render_reference.cpp) and the CIE table header rypath's CMake generates from
+# third_party/cie (cmake/CieData.cmake); generated here the same way into the build folder
+DEMO_SRC := $(HERE)ref_demo_probe.cpp $(HERE)ref_image_host.cpp $(REF)/src/render.cpp $(REF)/tests/render_reference.cpp \
+	$(REF)/src/image_texture.cpp $(REF)/src/environment_sampling.cpp $(REF)/src/rgb_spectrum.cpp \
+	$(REF)/src/pbrt_spectra.cpp $(REF)/src/light_sampling.cpp $(REF)/src/png_allocator.cpp \
+	$(REF)/third_party/lodepng/lodepng.cpp $(REF)/src/texture_footprint.cpp $(REF)/src/geometry.cpp \
+	$(REF)/src/bilinear.cpp $(REF)/third_party/stb/jpeg.cpp $(REF)/src/gaussian_filter.cpp \
+	$(REF)/src/texture_graph.cpp $(REF)/src/bsdf_table.cpp $(REF)/src/sampling.cpp $(REF)/src/area_power.cpp \
+	$(REF)/src/packet_film.cpp
+
+all: $(OUT)/libref.so $(OUT)/libref_image.so $(OUT)/libref_demo.so $(OUT)/roulette_known_answers
+
+$(OUT)/gen/cie_xyz_data.hpp: $(REF)/third_party/cie/CIE_xyz_1931_2deg.csv
+	mkdir -p $(OUT)/gen
+	( echo '#pragma once'; echo '#include <array>'; echo 'namespace rypath::detail {'; \
+	  echo 'inline constexpr std::array<std::array<double, 3>, 471> cie_xyz{{'; \
+	  sed -E 's/^[0-9]+,(.*)$$/    {\1},/' $<; echo '}};'; echo '}' ) > $@
+
+$(OUT)/libref_demo.so: $(DEMO_SRC) $(OUT)/gen/cie_xyz_data.hpp
+	mkdir -p $(OUT)
+	$(CXX) $(BASE) -shared -I$(OUT)/gen -I$(REF)/src -I$(REF)/tests -I$(REF)/shaders -I$(REF)/third_party/pbrt \
+		-I$(REF)/third_party/stb -I$(REF)/third_party/lodepng -DRYPATH_SRGB_BIN='"$(REF)/third_party/pbrt/srgb.bin"' \
+		-Wl,--no-undefined -o $@ $(DEMO_SRC)
 
 $(OUT)/libref.so: $(SRC) $(HERE)ref_shim/metal_stdlib
 	mkdir -p $(OUT)

@@ -21,6 +21,7 @@ SAMPLER_INDEPENDENT, SAMPLER_SOBOL, SAMPLER_HALTON, SAMPLER_ZSOBOL = 0, 1, 2, 3
 RANDOMIZE_NONE, RANDOMIZE_PERMUTEDIGITS, RANDOMIZE_FASTOWEN, RANDOMIZE_OWEN = range(4)
 FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = 0, 1, 2
 DIFFUSE, CONDUCTOR, DIELECTRIC = 0, 1, 2
+MODEL_PBRT, MODEL_DEMO = 0, 1
 INTERFACE = 10  # null interface: medium change (scalar transport), pass-through (hero transport)
 MIX = 9  # stochastic mix of two materials
 REFLECTANCE_KNOTS, REFLECTANCE_CONSTANT, REFLECTANCE_RGB, REFLECTANCE_IMAGE, REFLECTANCE_BLACKBODY = 0, 1, 2, 3, 4
@@ -53,7 +54,7 @@ class Material(C.Structure):
                 ("k_count", u32), ("optical_extensions", u32), ("u_roughness", f32),
                 ("v_roughness", f32), ("remap_roughness", u32), ("first_material", u32),
                 ("second_material", u32), ("mix_amount", f32), ("image_texture", u32),
-                ("coefficients", f32 * 3)]
+                ("coefficients", f32 * 3), ("reflectance", f32 * 8)]
 
 
 class ImageTexture(C.Structure):
@@ -127,6 +128,7 @@ class SceneDesc(C.Structure):
         ("lens_radius", f32), ("focal_distance", f32), ("lens_x", f32 * 3), ("lens_y", f32 * 3),
         ("filter_sigma", f32),
         ("images", P(Images)),
+        ("model", u32), ("film_scale", f32),
     ]
 
 
@@ -245,7 +247,7 @@ class FrameInfo(C.Structure):
 FRAME_PENDING, FRAME_COMPLETE, FRAME_FAILED = 0, 1, 2
 
 EXPECTED_SIZES = {
-    "rp_instance": (Instance, 88), "rp_material": (Material, 80), "rp_knot": (Knot, 8),
+    "rp_instance": (Instance, 88), "rp_material": (Material, 112), "rp_knot": (Knot, 8),
     "rp_area_emission": (AreaEmission, 1888), "rp_positional_light": (PositionalLight, 1948),
     "rp_medium": (Medium, 5656), "rp_camera": (Camera, 48), "rp_request": (Request, 64),
     "rp_packet_result": (PacketResult, 80), "rp_scalar_result": (ScalarResult, 44),

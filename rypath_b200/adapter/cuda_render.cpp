@@ -21,7 +21,9 @@
 #include <rypath_cuda.h>
 
 #include <algorithm>
+#include <cmath>
 #include <map>
+#include <numbers>
 #include <memory>
 #include <string>
 #include <vector>
@@ -195,12 +197,14 @@ std::string describe_images(const RenderScene &s, Arena &a) {
     return {};
 }
 
-// RenderScene -> rp_scene_desc: what build_metal_renderer reads on the PT / hero path
-// (src/metal_render.mm:147-290, :505-700).  Returns a diagnostic for what the backend does not
-// build (the demo camera model, analytic shapes and bilinear patches, textures).
+// RenderScene -> rp_scene_desc: what build_metal_renderer reads on the PT / hero path and for
+// the demo model (src/metal_render.mm:147-290, :505-700).  Returns a diagnostic for what the
+// backend does not build (analytic shapes and bilinear patches, texture graphs and surface
+// detail, some light kinds).
 std::string describe(const RenderScene &s, Arena &a, rp_scene_desc &d) {
-    if (s.model != RenderModel::pbrt || !s.raster_camera)
-        return "the CUDA backend renders PBRT-model scenes (a raster camera)";
+    const bool demo = s.model == RenderModel::demo;
+    if (!demo && !s.raster_camera)
+        return "a PBRT-model scene needs its raster camera";
     std::vector<std::uint32_t> mesh_vertex(s.geometry.meshes.size()), mesh_triangle(s.geometry.meshes.size()),
         mesh_normal(s.geometry.meshes.size(), RP_NONE);
     for (std::size_t m = 0; m < s.geometry.meshes.size(); ++m) {
@@ -257,6 +261,7 @@ std::string describe(const RenderScene &s, Arena &a, rp_scene_desc &d) {
         w.second_material = m.surface.second_material;
         w.mix_amount = m.surface.mix_amount;
         w.image_texture = m.image_texture;
+        std::copy(m.reflectance.begin(), m.reflectance.end(), w.reflectance);
         std::copy(m.coefficients.begin(), m.coefficients.end(), w.coefficients);
         if (m.kind == SpectralMaterialKind::texture_graph ||
             m.bump_root != UINT32_MAX || m.normal_map != UINT32_MAX || m.table || m.texture_root != UINT32_MAX)
@@ -326,13 +331,40 @@ std::string describe(const RenderScene &s, Arena &a, rp_scene_desc &d) {
     d.camera_medium = s.camera_medium; // no_medium == RP_NONE
     d.environment = a.environment.data();
     d.images = a.textures.empty() && s.environment_image == UINT32_MAX ? nullptr : &a.images;
-    const RasterCamera &c = *s.raster_camera;
-    const GeometryPoint *points[4] = {&c.origin, &c.corner, &c.dx, &c.dy};
-    float *dst[4] = {d.camera.origin, d.camera.corner, d.camera.dx, d.camera.dy};
-    for (int k = 0; k < 4; ++k) {
-        dst[k][0] = points[k]->x;
-        dst[k][1] = points[k]->y;
-        dst[k][2] = points[k]->z;
+    if (demo) {
+        // the demo camera slots (src/metal_render.mm:194-206): the look-at basis in double,
+        // rounded to binary32, and tan(fov / 2)
+        const RenderCamera &c = s.camera;
+        const std::array<double, 3> o{c.origin.x, c.origin.y, c.origin.z};
+        std::array<double, 3> f{double{c.target.x} - o[0], double{c.target.y} - o[1], double{c.target.z} - o[2]};
+        const auto unit = [](std::array<double, 3> v) {
+            const double n = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            return std::array<double, 3>{v[0] / n, v[1] / n, v[2] / n};
+        };
+        const auto cross = [](const std::array<double, 3> &a, const std::array<double, 3> &b) {
+            return std::array<double, 3>{a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+        };
+        f = unit(f);
+        const auto r = unit(cross(f, {c.up.x, c.up.y, c.up.z}));
+        const auto u = cross(r, f);
+        for (int k = 0; k < 3; ++k) {
+            d.camera.origin[k] = float(o[k]);
+            d.camera.corner[k] = float(f[k]);
+            d.camera.dx[k] = float(r[k]);
+            d.camera.dy[k] = float(u[k]);
+        }
+        d.model = RP_MODEL_DEMO;
+        d.film_scale = float(std::tan(c.vertical_fov_degrees * (std::numbers::pi_v<double> / 360.0)));
+    } else {
+        const RasterCamera &c = *s.raster_camera;
+        const GeometryPoint *points[4] = {&c.origin, &c.corner, &c.dx, &c.dy};
+        float *dst[4] = {d.camera.origin, d.camera.corner, d.camera.dx, d.camera.dy};
+        for (int k = 0; k < 4; ++k) {
+            dst[k][0] = points[k]->x;
+            dst[k][1] = points[k]->y;
+            dst[k][2] = points[k]->z;
+        }
+        d.model = RP_MODEL_PBRT;
     }
     d.filter_kind = std::uint32_t(s.filter.kind);
     d.filter_x_radius = s.filter.x_radius;

@@ -895,6 +895,7 @@ struct rp_scene {
     u32 wide_levels = 0;     // levels of the compressed 8-wide traversal tree
     bool resolve = false;    // hero scene with pass-through or mix-root instances
     u32 tex_width = 0, tex_height = 0; // film size the texture camera differentials were found for
+    double demo_film_scale = 0;        // demo film: 470 / integral of the CIE y table
     float4 *world = nullptr; // world-space triangle vertices in original order
     BNode *nodes = nullptr;  // traversal layout (ds.nodes, ds.leaf_v)
     float4 *leaf_v = nullptr;
@@ -1851,6 +1852,17 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             throw Invalid{images};
         if (d->images && scalar && (d->images->environment_image != RP_NONE || d->images->texture_count))
             throw NotBuilt{"the scalar transport does not read images"};
+        if (d->model > RP_MODEL_DEMO)
+            throw Invalid{"invalid scene model"};
+        if (d->model == RP_MODEL_DEMO) {
+            // src/render.cpp:1823-1895: the demo model renders its sky and sampled reflectance
+            if (!scalar)
+                throw NotBuilt{"the demo model renders with the scalar transport"};
+            if (d->emission_count || d->positional_count || d->images || d->medium_count)
+                throw Invalid{"the demo model has no emitters, lights, images or media besides its sky"};
+            if (!(d->film_scale > 0) || !std::isfinite(d->film_scale))
+                throw Invalid{"the demo camera needs a positive finite film scale"};
+        }
         for (u32 i = 0; i < d->material_count; ++i) {
             const rp_material &m = d->materials[i];
             if (m.kind != RP_REFLECTANCE_IMAGE || m.scattering != RP_DIFFUSE)
@@ -1985,7 +1997,9 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             mats[i] = {m.scattering, m.kind,        m.knot_begin,        m.knot_count,      m.scalar_value,
                        m.eta_begin,  m.eta_count,   m.k_begin,           m.k_count,         m.optical_extensions,
                        m.u_roughness, m.v_roughness, m.remap_roughness,    m.first_material,  m.second_material,
-                       m.mix_amount,  m.image_texture, {m.coefficients[0], m.coefficients[1], m.coefficients[2]}};
+                       m.mix_amount,  m.image_texture, {m.coefficients[0], m.coefficients[1], m.coefficients[2]},
+                       {m.reflectance[0], m.reflectance[1], m.reflectance[2], m.reflectance[3], m.reflectance[4],
+                        m.reflectance[5], m.reflectance[6], m.reflectance[7]}};
         }
         ds.materials = dupload(own, mats.data(), mats.size(), stm);
         ds.material_count = d->material_count;
@@ -2192,6 +2206,8 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
         ds.forward = v3(d->camera.corner[0], d->camera.corner[1], d->camera.corner[2]);
         ds.right = v3(d->camera.dx[0], d->camera.dx[1], d->camera.dx[2]);
         ds.up = v3(d->camera.dy[0], d->camera.dy[1], d->camera.dy[2]);
+        ds.model = d->model == RP_MODEL_DEMO ? kModelDemo : kModelPbrt;
+        ds.film_scale = d->film_scale;
         ds.filter_kind = d->filter_kind;
         ds.filter_x = d->filter_x_radius;
         ds.filter_y = d->filter_y_radius;
@@ -2521,7 +2537,7 @@ static rp_status film_impl(rp_scene *s, const rp_film_request *r, rp_film_pixel 
                     s->mark(3);
                     k_scalar_film<<<grid_for(s->sm_count, pixels, 128, 16), 128, 0, s->stream>>>(
                         s->scalar_records, pixels, u32(spw), s->cie, reinterpret_cast<FilmPixel *>(staged),
-                        s->scalar_counters + 1);
+                        s->scalar_counters + 1, s->ds.model == kModelDemo ? 1u : 0u, s->demo_film_scale);
                     s->done();
                     RP_CHECK(cudaMemcpyAsync(&f, s->scalar_counters + 1, 4, cudaMemcpyDeviceToHost, s->stream));
                 } else {
@@ -2585,6 +2601,12 @@ rp_status rp_cuda_set_cie(rp_scene *s, const double *cie_xyz) {
             s->cie = dalloc<double>(s->owned, 3 * 471, s->stream);
         RP_CHECK(cudaMemcpyAsync(s->cie, cie_xyz, 3 * 471 * sizeof(double), cudaMemcpyHostToDevice, s->stream));
         RP_CHECK(cudaStreamSynchronize(s->stream));
+        // the demo film's scale: 470 / the trapezoidal integral of y (integrate_y,
+        // src/render.cpp:70-77)
+        double integral = (cie_xyz[1] + cie_xyz[3 * 470 + 1]) / 2;
+        for (int i = 1; i + 1 < 471; ++i)
+            integral += cie_xyz[3 * i + 1];
+        s->demo_film_scale = 470.0 / integral;
         return RP_SUCCESS;
     });
 }
@@ -3496,6 +3518,8 @@ rp_status rp_cuda_frame_session_create(rp_scene *s, const rp_frame_config *confi
             throw Invalid{"null argument"};
         if (s->ds.img.textured)
             throw NotBuilt{"frame sessions of scenes with image reflectance are not built (the texture camera follows the scene camera)"};
+        if (s->ds.model == kModelDemo)
+            throw NotBuilt{"frame sessions of demo-model scenes are not built (their sensor weights differ)"};
         rp_request q{};
         q.width = config->width;
         q.height = config->height;

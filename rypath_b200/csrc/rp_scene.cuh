@@ -7,6 +7,7 @@
 namespace rp {
 
 constexpr u32 kNone = 0xffffffffu;
+constexpr u32 kModelPbrt = 0, kModelDemo = 1;
 constexpr u32 kLeaf = 0x80000000u;
 
 // wire::Instance subset (src/render_wire.h:168-188), plus the first emitter slot
@@ -33,6 +34,7 @@ struct DMaterial {
     float mix_amount;
     u32 image_texture; // image reflectance (kind 3)
     float coefficients[3]; // RGB sigmoid reflectance (kind 2)
+    float reflectance[8];  // demo-model sampled reflectance at the demo knots
 };
 struct DPositional {
     float position[3];
@@ -139,6 +141,8 @@ struct DeviceScene {
     float filter_weight;
     const u32 *primes; // the first 1000 primes (Halton bases)
     DImages img;       // image textures and the environment image (env_image kNone: none)
+    u32 model;         // kModelPbrt or kModelDemo (RenderModel)
+    float film_scale;  // demo camera: tan(vertical fov / 2)
 };
 
 RP_DEV V3 load3(const float *p) { return v3(__ldg(p), __ldg(p + 1), __ldg(p + 2)); }

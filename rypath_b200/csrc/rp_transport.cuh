@@ -322,6 +322,16 @@ RP_DEV void primary_ray_from(const DeviceScene &s, const RasterCam &cam, const W
         d = normalize3(scaled);
         return;
     }
+    if (s.model == kModelDemo) {
+        // the demo camera (shaders/render.metal:470-475): forward, right and up are the look-at
+        // basis and film_scale = tan(fov / 2)
+        const float x = (float(b.pixel % p.width) + ux) / float(p.width);
+        const float y = (float(b.pixel / p.width) + uy) / float(p.height);
+        const float aspect = float(p.width) / float(p.height);
+        d = normalize3((cam.forward + (((2.0f * x - 1.0f) * aspect) * s.film_scale) * cam.right) +
+                       ((1.0f - 2.0f * y) * s.film_scale) * cam.up);
+        return;
+    }
     const float scale = fmaxf(fabsf(dd.x), fmaxf(fabsf(dd.y), fabsf(dd.z)));
     d = normalize3(dd / scale);
 }

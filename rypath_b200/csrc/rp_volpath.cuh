@@ -366,15 +366,30 @@ RP_DEV void scalar_start(const DeviceScene &s, const WaveParams &p, const Scalar
     path.medium_draw = 0;
     path.boundary_crossings = 0;
 }
+// sky_radiance (shaders/render.metal:813-819): the demo model's sky is a unit equal-energy
+// spectrum
 RP_DEV float environment_radiance(const DeviceScene &s, float wavelength) {
+    if (s.model == kModelDemo)
+        return 1.0f;
     return s.environment == kNone ? 0.0f : spectrum(s, s.environment, wavelength);
+}
+// demo_reflectance (shaders/render.metal:537-546) at the demo knots 360 420 470 520 570 620 700 830
+RP_DEV float demo_reflectance(const float *r, float w) {
+    const float knots[8] = {360, 420, 470, 520, 570, 620, 700, 830};
+#pragma unroll
+    for (int i = 1; i < 8; ++i)
+        if (w <= knots[i]) {
+            const float t = (w - knots[i - 1]) / (knots[i] - knots[i - 1]);
+            return r[i - 1] + (r[i] - r[i - 1]) * t;
+        }
+    return r[7];
 }
 
 // scalar_sky_step (shaders/scalar_transport.h:88-210): scenes without geometry.  Light
 // selection shares the flight draw and phase sampling takes the next medium block.
 // Returns true when the path finished.
 __device__ __noinline__ bool scalar_sky_step(const DeviceScene &s, const WaveParams &p, ScalarPath &path) {
-    if (!finite3(path.o) || !finite3(path.d)) {
+    if (s.model == kModelPbrt && (!finite3(path.o) || !finite3(path.d))) {
         path.status = S_ARITHMETIC;
         return true;
     }
@@ -694,7 +709,7 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
     }
     if (miss) {
         // escape (:421-433): a constant environment has no light-sampling density
-        if (path.scatterings != 0u && !path.previous_delta)
+        if (s.model == kModelPbrt && path.scatterings != 0u && !path.previous_delta)
             path.escape_weight = power_weight(path.previous_bsdf_pdf, 0.0f);
         path.radiance += path.throughput * path.escape_weight * environment_radiance(s, path.wavelength);
         return kEventFinished;
@@ -781,8 +796,14 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
         path.status = S_HIT; // microfacet surfaces are not built for the scalar transport
         return kEventFinished;
     }
-    if (surface.kind == 0 && surface.knot_count >= 2 && surface.knot_begin <= s.knot_count &&
-        surface.knot_count <= s.knot_count - surface.knot_begin) {
+    if (s.model == kModelDemo) {
+        if (surface.kind != 0) {
+            path.status = S_HIT;
+            return kEventFinished;
+        }
+        rho = demo_reflectance(surface.reflectance, path.wavelength);
+    } else if (surface.kind == 0 && surface.knot_count >= 2 && surface.knot_begin <= s.knot_count &&
+               surface.knot_count <= s.knot_count - surface.knot_begin) {
         rho = pbrt_reflectance(s.knots + surface.knot_begin, surface.knot_count, path.wavelength);
     } else if (surface.kind == 1) {
         rho = surface.scalar_value;
@@ -823,9 +844,42 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
     }
     const uint4 light_words = draw_words(s, p, path.pixel, path.slo, path.shi, path.index, 2 + 2 * bounce);
     const uint4 bsdf_words = draw_words(s, p, path.pixel, path.slo, path.shi, path.index, 1 + 2 * bounce);
-    // light sample with power-heuristic MIS (:783-835)
+    // light sample: the demo model's sky sampled uniformly over the sphere with the
+    // cosine-ratio weight (:709-781); PBRT scenes' lights with power-heuristic MIS (:783-835)
     bool connect = false;
-    {
+    if (s.model == kModelDemo) {
+        const float E = 1.0f; // sky_radiance of the demo model
+        const float uz = sample_uniform(p, light_words.x), uv = sample_uniform(p, light_words.y);
+        const float z = 1.0f - 2.0f * uz;
+        const float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+        const float phi = 2.0f * kPi * uv;
+        const V3 direction = v3(r * cosf(phi), r * sinf(phi), z);
+        const float cosine = dot(n, direction);
+        if (cosine > 0.0f) {
+            const V3 origin = directional_offset ? spawn_toward(path.o, path.d, hit.t, point, direction) : area_reference;
+            const float relative = 4.0f * cosine;
+            const float factor = relative * (1.0f / (1.0f + relative * relative)); // (4 cos) * light_weight(cos)
+            if (!finite3(origin) || !isfinite(factor)) {
+                path.status = S_ARITHMETIC;
+                return kEventFinished;
+            }
+            const u32 medium = outgoing_medium(instance, path.current_medium, point.geometric_normal, direction);
+            if (s.media_enabled) {
+                if (!connection_begin(origin, direction, finf(), medium, c)) {
+                    path.status = S_ARITHMETIC;
+                    return kEventFinished;
+                }
+            } else {
+                c.o = origin;
+                c.d = direction;
+                c.remaining = finf();
+                c.vacuum = true;
+            }
+            c.medium_sample = false;
+            c.a = ((path.throughput * rho) * factor) * E;
+            connect = true;
+        }
+    } else {
         const Incident light = scalar_light_sample(s, path.wavelength, point.position, point.shading_normal,
                                                    sample_uniform(p, light_words.x), sample_uniform(p, light_words.y),
                                                    sample_uniform(p, light_words.z));
@@ -1176,10 +1230,22 @@ __global__ void k_scalar_results(const __grid_constant__ DeviceScene s, const __
     }
 }
 
-// FilmBatch::add for scalar samples (src/render.cpp:2355-2385): XYZ = CIE(round(lambda)) *
-// 470 * L, FP64 Neumaier sums per pixel in canonical (absolute sample, pixel) order.
+// FilmBatch::add for scalar samples (src/render.cpp:2355-2385): PBRT scenes XYZ =
+// CIE(round(lambda)) * 470 * L, the demo model wavelength_xyz(lambda) * L; FP64 Neumaier sums
+// per pixel in canonical (absolute sample, pixel) order.
+// The demo film (wavelength_xyz, src/render.cpp:2131-2145): the CIE table linearly interpolated
+// at the wavelength (libstdc++'s std::lerp) times 470 / (the trapezoidal integral of y), and
+// the radiance unweighted.
+RP_DEV double film_lerp(double a, double b, double t) {
+    if ((a <= 0 && b >= 0) || (a >= 0 && b <= 0))
+        return __dadd_rn(__dmul_rn(t, b), __dmul_rn(__dadd_rn(1.0, -t), a));
+    if (t == 1)
+        return b;
+    const double x = __dadd_rn(a, __dmul_rn(t, __dadd_rn(b, -a)));
+    return (t > 1) == (b > a) ? (b < x ? x : b) : (b > x ? x : b);
+}
 __global__ void k_scalar_film(const uint4 *records, u32 pixel_count, u32 samples, const double *cie, FilmPixel *film,
-                              u32 *failures) {
+                              u32 *failures, u32 demo, double demo_scale) {
     for (u32 px = blockIdx.x * blockDim.x + threadIdx.x; px < pixel_count; px += gridDim.x * blockDim.x) {
         FilmPixel f = film[px];
         for (u32 si = 0; si < samples; ++si) {
@@ -1189,11 +1255,25 @@ __global__ void k_scalar_film(const uint4 *records, u32 pixel_count, u32 samples
                 atomicAdd(failures, 1u);
                 continue;
             }
-            const u32 row = u32(round(double(w)) - 360.0);
-            const double weighted = __dmul_rn(470.0, double(L));
+            double xyz[3], weighted;
+            if (demo) {
+                const double offset = __dadd_rn(double(w), -360.0);
+                const u32 lower = u32(offset), upper = min(lower + 1u, 470u);
+                const double t = __dadd_rn(offset, -double(lower));
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    xyz[c] = __dmul_rn(film_lerp(__ldg(cie + 3 * lower + c), __ldg(cie + 3 * upper + c), t), demo_scale);
+                weighted = double(L);
+            } else {
+                const u32 row = u32(round(double(w)) - 360.0);
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    xyz[c] = __ldg(cie + 3 * row + c);
+                weighted = __dmul_rn(470.0, double(L));
+            }
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const double v = __dmul_rn(__ldg(cie + 3 * row + c), weighted);
+                const double v = __dmul_rn(xyz[c], weighted);
                 add_compensated(v, f.sum[c], f.correction[c]);
                 f.square[c] = __dadd_rn(f.square[c], __dmul_rn(v, v));
             }

@@ -91,6 +91,10 @@ class Scene:
     lens: tuple = (0.0, 1e6, (1.0, 0.0, 0.0), (0.0, 1.0, 0.0))
     filter_sigma: float = 0.5
     images: object = None  # images.ImageSet: image textures and the environment image
+    # RenderModel: MODEL_PBRT, or MODEL_DEMO (camera = (origin, forward, right, up) of a look-at
+    # pose, film_scale = tan(fov / 2), materials' 8-knot reflectance, the unit sky)
+    model: int = abi.MODEL_PBRT
+    film_scale: float = 1.0
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -174,6 +178,7 @@ class Scene:
         tables = C.create_string_buffer(sobol_tables(), abi.RP_SOBOL_TABLE_BYTES)
         keep.append(tables)
         d.sobol_tables = C.cast(tables, C.c_void_p)
+        d.model, d.film_scale = self.model, self.film_scale
         if self.images is not None:
             im = self.images.to_c(keep)
             keep.append(im)
@@ -498,6 +503,92 @@ def textured_cornell(scene: Scene) -> None:
     s.instance_frame_begin = [inst.triangle_begin for inst in scene.instances]
     s.world_from_camera, s.camera_from_world = texture_camera((0, 1, 3.94), (0, 1, 0), (0, 1, 0))
     scene.images = s
+
+
+def demo_camera(origin, target, up, vfov_degrees):
+    """The demo model's camera slots (src/metal_render.mm:194-204): origin and the unit
+    forward / right / up of the look-at pose (double, rounded to binary32), and
+    tan(vfov / 2)."""
+    o, t, u = (np.asarray(v, np.float32).astype(np.float64) for v in (origin, target, up))  # RenderCamera is binary32
+    f = (t - o) / np.linalg.norm(t - o)
+    r = np.cross(f, u)
+    r /= np.linalg.norm(r)
+    up2 = np.cross(r, f)
+    scale = float(np.float32(math.tan(float(np.float32(vfov_degrees)) * (math.pi / 360.0))))
+    return (tuple(np.float32(o)), tuple(f.astype(np.float32)), tuple(r.astype(np.float32)),
+            tuple(up2.astype(np.float32))), scale
+
+
+def demo_material(reflectance):
+    m = abi.Material()
+    m.scattering, m.kind = abi.DIFFUSE, abi.REFLECTANCE_KNOTS
+    m.reflectance[:] = [float(v) for v in reflectance]
+    m.remap_roughness = 1
+    return m
+
+
+def _demo_box(offset, scale, angle):
+    """A unit box placement of the demo scene (box_transform, src/render.cpp:821-827), in binary32
+    with the C library's cosf / sinf."""
+    libm = C.CDLL("libm.so.6")
+    libm.cosf.restype = libm.sinf.restype = C.c_float
+    libm.cosf.argtypes = libm.sinf.argtypes = [C.c_float]
+    f = np.float32
+    x, y, z = (f(v) for v in offset)
+    w, h, d = (f(v) for v in scale)
+    c, s = f(libm.cosf(f(angle))), f(libm.sinf(f(angle)))
+    return [float(v) for v in (c * w, 0, s * d, x, 0, h, 0, y, -s * w, 0, c * d, z)]
+
+
+def demo_scene(width=256, height=192, spp=128, max_depth=5) -> Scene:
+    """rypath's `--render-demo` scene (demo-v1, make_demo_scene, src/render.cpp:2060-2106): a
+    floor and two walls, three rotated boxes, six 8-knot diffuse reflectances, under the demo
+    model's unit sky, through its look-at camera; scalar transport, depth 5."""
+    quads = [((-3, 0, -3), (-3, 0, 3), (3, 0, 3), (3, 0, -3)),
+             ((-3, 0, -3), (3, 0, -3), (3, 3.2, -3), (-3, 3.2, -3)),
+             ((-3, 0, 3), (-3, 0, -3), (-3, 3.2, -3), (-3, 3.2, 3))]
+    cube = np.array([(-0.5, 0, -0.5), (0.5, 0, -0.5), (0.5, 0, 0.5), (-0.5, 0, 0.5),
+                     (-0.5, 1, -0.5), (0.5, 1, -0.5), (0.5, 1, 0.5), (-0.5, 1, 0.5)], np.float32)
+    cube_tris = np.array([(0, 1, 2), (0, 2, 3), (4, 6, 5), (4, 7, 6), (0, 4, 5), (0, 5, 1), (1, 5, 6), (1, 6, 2),
+                          (2, 6, 7), (2, 7, 3), (3, 7, 4), (3, 4, 0)], np.uint32)
+    positions = [np.array(q, np.float32) for q in quads] + [cube]
+    triangles = [np.array([(0, 1, 2), (0, 2, 3)], np.uint32)] * 3 + [cube_tris]
+    vb = np.cumsum([0] + [len(p) for p in positions])
+    tb = np.cumsum([0] + [len(t) for t in triangles])
+    instances = [identity_instance(int(vb[i]), int(tb[i]), 2, i) for i in range(3)]
+    for k, box in enumerate([((-1.25, -0.05, -0.6), (1.25, 2.25, 1.25), 0.18),
+                             ((0.25, -0.05, 0.8), (1.45, 1.08, 1.3), -0.24),
+                             ((1.4, -0.05, -1.5), (1.07, 1.55, 1.06), 0.44)]):
+        inst = identity_instance(int(vb[3]), int(tb[3]), 12, 3 + k)
+        inst.matrix[:] = _demo_box(*box)
+        instances.append(inst)
+    reflectances = [(0.54, 0.54, 0.55, 0.58, 0.61, 0.63, 0.65, 0.65), (0.69, 0.68, 0.67, 0.65, 0.64, 0.62, 0.61, 0.61),
+                    (0.34, 0.34, 0.36, 0.43, 0.55, 0.61, 0.63, 0.63), (0.10, 0.10, 0.16, 0.52, 0.40, 0.09, 0.06, 0.06),
+                    (0.07, 0.08, 0.09, 0.13, 0.39, 0.73, 0.72, 0.72), (0.32, 0.47, 0.72, 0.23, 0.11, 0.08, 0.09, 0.09)]
+    scene = Scene("demo_v1", width, height, spp, np.concatenate(positions), np.concatenate(triangles), instances,
+                  [demo_material(r) for r in reflectances], max_depth=max_depth)
+    scene.camera, scene.film_scale = demo_camera((4.1, 3.0, 6.2), (0, 1, -0.45), (0, 1, 0), 42.0)
+    scene.model = abi.MODEL_DEMO
+    scene.transport = abi.TRANSPORT_SCALAR
+    return scene
+
+
+def demo_floor(reflectance=None, width=1, height=1) -> Scene:
+    """The demo model's analytic fixtures (tests/render_tests.cpp): with reflectance None, the
+    bare sky (no geometry); else an unbounded-looking Lambertian floor under the unit sky, seen
+    straight down from above, so every path hits the floor once and then escapes."""
+    if reflectance is None:
+        scene = Scene("demo_sky", width, height, 1, np.zeros((0, 3), np.float32), np.zeros((0, 3), np.uint32), [], [],
+                      max_depth=5)
+    else:
+        big = 1e4
+        pos = np.array([(-big, 0, -big), (-big, 0, big), (big, 0, big), (big, 0, -big)], np.float32)
+        scene = Scene("demo_floor", width, height, 1, pos, np.array([(0, 1, 2), (0, 2, 3)], np.uint32),
+                      [identity_instance(0, 0, 2, 0)], [demo_material(reflectance)], max_depth=5)
+    scene.camera, scene.film_scale = demo_camera((0, 1, 0), (0, 0, 0.0001), (0, 0, 1), 1.0)
+    scene.model = abi.MODEL_DEMO
+    scene.transport = abi.TRANSPORT_SCALAR
+    return scene
 
 
 def with_environment_image(scene: Scene, width=256, seed=2, scale=0.03) -> Scene:

@@ -61,7 +61,7 @@ def oracle():
         lib.or_film_add_clamped.argtypes = [vp, sz, vp, u32, C.c_double, C.c_double, vp]
         lib.or_sample_scalar.argtypes = [vp, C.POINTER(abi.Request), vp, sz, C.c_int]
         lib.or_probe_medium.argtypes = [vp, u32, vp]
-        lib.or_scalar_film_add.argtypes = [vp, sz, vp, u32, vp]
+        lib.or_scalar_film_add.argtypes = [vp, sz, vp, u32, vp, C.c_int]
         lib.or_adjoint.argtypes = [vp, C.POINTER(abi.FilmRequest), vp, u32, vp, vp, vp, C.c_int]
         lib.or_probe_qmc.argtypes = [vp, vp, u32, vp]
         lib.or_gaussian_filter.argtypes = [C.c_float, C.c_float, C.c_float, vp, sz, vp, vp, vp, u32, vp]
@@ -223,7 +223,7 @@ def oracle_film(scene, width, height, spp, seed=1, sampler=abi.SAMPLER_SOBOL, sc
         if scalar:
             lanes = o.sample_scalar(r, threads)
             rc = oracle().or_scalar_film_add(lanes.ctypes.data, lanes.size, cie.ctypes.data, width * height,
-                                             film.ctypes.data)
+                                             film.ctypes.data, int(scene.model == abi.MODEL_DEMO))
         else:
             lanes = o.sample(r, threads)
             rc = oracle().or_film_add(lanes.ctypes.data, lanes.size, cie.ctypes.data, width * height,

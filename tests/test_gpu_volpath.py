@@ -156,7 +156,7 @@ def test_device_film_equals_host_reduction_of_the_same_samples():
     host = np.zeros(256, abi.film_dtype())
     cie = np.ascontiguousarray(scenes.cie_xyz())
     samples = np.ascontiguousarray(res.samples)
-    assert oracle().or_scalar_film_add(samples.ctypes.data, samples.size, cie.ctypes.data, 256, host.ctypes.data) == 0
+    assert oracle().or_scalar_film_add(samples.ctypes.data, samples.size, cie.ctypes.data, 256, host.ctypes.data, 0) == 0
     np.testing.assert_array_equal(film["count"], host["count"])
     np.testing.assert_allclose(film["sum"] + film["correction"], host["sum"] + host["correction"], rtol=1e-12,
                                atol=1e-300)
@@ -173,7 +173,7 @@ def test_fog_film_statistics_agree_with_the_oracle():
     ref = OracleScene(scene).sample_scalar(request(16, 16, 256, seed=6, sampler=abi.SAMPLER_INDEPENDENT))
     host = np.zeros(256, abi.film_dtype())
     cie = np.ascontiguousarray(scenes.cie_xyz())
-    assert oracle().or_scalar_film_add(ref.ctypes.data, ref.size, cie.ctypes.data, 256, host.ctypes.data) == 0
+    assert oracle().or_scalar_film_add(ref.ctypes.data, ref.size, cie.ctypes.data, 256, host.ctypes.data, 0) == 0
 
     def moments(f):
         n = f["count"][:, None].astype(np.float64)

@@ -234,7 +234,7 @@ def test_scalar_film_reduction_matches_host_accumulation():
     out = OracleScene(scene).sample_scalar(request(8, 8, 4))
     film = np.zeros(64, abi.film_dtype())
     cie = np.ascontiguousarray(scenes.cie_xyz())
-    assert oracle().or_scalar_film_add(out.ctypes.data, out.size, cie.ctypes.data, 64, film.ctypes.data) == 0
+    assert oracle().or_scalar_film_add(out.ctypes.data, out.size, cie.ctypes.data, 64, film.ctypes.data, 0) == 0
     assert np.all(film["count"] == 4)
     expected = np.zeros((64, 3))
     for r in out:
