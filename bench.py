@@ -346,6 +346,39 @@ def bench_images(torch, plain_value):
                                  "untextured_value": box_value, "vs_untextured": tex_value / box_value}}
 
 
+def bench_demo(torch, cpu_seconds):
+    """`--render-demo` at its own defaults: rypath's demo scene (make_demo_scene) at 256x192,
+    128 spp, depth 5, the independent (Philox) sampler, scalar transport, into a device film;
+    the oracle's scalar demo lanes on the host cores beside it."""
+    from rypath_b200 import abi, renderer, scenes
+
+    from tests.oracle_lib import OracleScene, request
+
+    w, h, spp = 256, 192, 128
+    scene = scenes.demo_scene(w, h, spp)
+    rs = renderer.build_renderer(scene).scene
+    film = torch.zeros(w * h * abi.FILM_PIXEL_BYTES // 8, dtype=torch.float64, device="cuda")
+    settings = renderer.RenderSettings(w, h, samples=spp, batch_size=spp, seed=1, sampler=abi.SAMPLER_INDEPENDENT)
+    rs.render_film_device(renderer.RenderSettings(w, h, samples=8, batch_size=8, seed=1,
+                                                  sampler=abi.SAMPLER_INDEPENDENT), film.data_ptr(), fresh=True)
+    best = None
+    for _ in range(3):
+        rs.render_film_device(settings, film.data_ptr(), fresh=True)
+        t = rs.timing()
+        best = t if best is None or t.total_ms < best.total_ms else best
+    rs.close()
+    value = best.samples / best.total_ms / 1e3
+    orc = OracleScene(scene)
+    t0 = time.perf_counter()
+    out = orc.sample_scalar(request(w, h, 64, sampler=abi.SAMPLER_INDEPENDENT))
+    dt = time.perf_counter() - t0
+    return {"workload": "demo_v1_256x192_128spp_depth5 (rypath --render-demo defaults, scalar transport, "
+                        "independent sampler)",
+            "value": value, "unit": UNIT, "ms_per_step": best.total_ms,
+            "cpu_baseline": {"value": out.size / dt / 1e6, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                             "sample": f"{out.size} lanes (64 spp of every pixel), {dt:.2f} s"}}
+
+
 def bench_adjoint(torch, adam_steps):
     """Differentiation: 16 reflectance groups x 32 knots of the Cornell geometry, 512x512,
     32 spp, depth 8, L2 loss on film-mean XYZ against a 128-spp render of seeded true
@@ -656,7 +689,7 @@ def main():
     if line is not None and world == 1 and not args.no_secondary:
         line["secondary"] = {"volpath": bench_fog(torch, 4.0), "batched_views": bench_views(torch),
                              "adjoint": bench_adjoint(torch, args.adam_steps),
-                             "images": bench_images(torch, line["value"])}
+                             "images": bench_images(torch, line["value"]), "demo": bench_demo(torch, 4.0)}
     if dist:
         dist.barrier()
         dist.destroy_process_group()
