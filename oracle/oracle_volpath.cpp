@@ -134,6 +134,26 @@ float power_weight(float a, float b) {
     b /= scale;
     return a * a / (a * a + b * b);
 }
+// :2212-2219
+float scattering_direct(float f_cos, float bsdf_pdf, float light_pdf, bool invisible) {
+    if (!(f_cos >= 0) || !(bsdf_pdf >= 0) || !(light_pdf > 0) || !std::isfinite(f_cos) || !std::isfinite(bsdf_pdf) ||
+        !std::isfinite(light_pdf))
+        return NAN;
+    if (f_cos == 0)
+        return 0;
+    return (f_cos / light_pdf) * (invisible ? 1.0f : power_weight(light_pdf, bsdf_pdf));
+}
+// :180-198 with src/sampling_contract.h:17-42: Halton dimension 884 + bounce, (Z)Sobol
+// dimension 908 + bounce, else Philox block 0x80000000 | bounce
+u32 dielectric_lobe_word(const Scene &s, const Params &p, const Sample &smp, u64 index, u32 bounce) {
+    if (p.sampler == RP_SAMPLER_HALTON)
+        return fbits(qmc_radical(884u + bounce, index, p.randomization, p.seed_low));
+    if (p.sampler == RP_SAMPLER_ZSOBOL)
+        return zdraw(s, p, index, 908u + bounce);
+    if (p.sampler == RP_SAMPLER_SOBOL)
+        return sobol_word(*s.sobol, index, 908u + bounce, p.randomization, p.seed_low);
+    return philox(U4{smp.pixel, smp.sample_low, smp.sample_high, 0x80000000u | bounce}, p.seed_low, p.seed_high).x;
+}
 // :843-847
 float bsdf_weight(float cosine) {
     const float relative = 4.0f * cosine;
@@ -599,11 +619,15 @@ bool scalar_event(const Ctx &c, Lane &l) {
             return fail(mix_status);
     }
     const Material &surface = s.materials[material_index];
-    // reflectance, shaders/scalar_transport.h:580-625
+    // reflectance, shaders/scalar_transport.h:580-625; conductors and dielectrics carry their
+    // spectrum in the BSDF (rho = 1)
+    const bool microfacet = surface.scattering != RP_DIFFUSE;
     float rho = 0;
-    if (surface.scattering != RP_DIFFUSE)
-        return fail(RP_SAMPLE_INVALID_HIT);
-    if (s.model == RP_MODEL_DEMO) {
+    if (microfacet) {
+        if (surface.scattering != RP_CONDUCTOR && surface.scattering != RP_DIELECTRIC)
+            return fail(RP_SAMPLE_INVALID_HIT);
+        rho = 1.0f;
+    } else if (s.model == RP_MODEL_DEMO) {
         // demo_reflectance (shaders/render.metal:537-546)
         if (surface.kind != RP_REFLECTANCE_KNOTS)
             return fail(RP_SAMPLE_INVALID_HIT);
@@ -629,17 +653,44 @@ bool scalar_event(const Ctx &c, Lane &l) {
         return fail(RP_SAMPLE_INVALID_ARITHMETIC);
     if (rho == 0.0f)
         return true;
-    const bool authored_normals = instance.normal_begin != RP_NONE;
+    const bool authored_normals = instance.normal_begin != RP_NONE || microfacet;
     if (!authored_normals && bounce >= p.emergency_limit)
         return fail(RP_SAMPLE_EMERGENCY_DEPTH);
     if (!point_ready && !triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point))
         return fail(RP_SAMPLE_INVALID_ARITHMETIC);
     const float incident_cosine = dot(point.shading_normal, l.d);
-    if (authored_normals && incident_cosine == 0.0f)
+    if (authored_normals && !microfacet && incident_cosine == 0.0f)
         return true;
     if (bounce >= p.emergency_limit)
         return fail(RP_SAMPLE_EMERGENCY_DEPTH);
     const F3 n = incident_cosine > 0.0f ? -point.shading_normal : point.shading_normal;
+    // the BSDF in the shading frame of the normal (shaders/scalar_transport.h:677-694;
+    // prepare_scattering, shaders/render.metal:2079-2160)
+    LaneBsdf bsdf{};
+    Frame frame{};
+    F3 wo{0, 0, 0};
+    if (microfacet) {
+        const u32 total = u32(s.knots.size());
+        const float eta = optical_value(s.knots.data(), surface.eta_begin, surface.eta_count, total,
+                                        (surface.optical_extensions & 1u) != 0, l.wavelength);
+        const float kk = optical_value(s.knots.data(), surface.k_begin, surface.k_count, total,
+                                       (surface.optical_extensions & 2u) != 0, l.wavelength);
+        bsdf.kind = surface.scattering;
+        const bool prepared =
+            surface.scattering == RP_CONDUCTOR
+                ? conductor_prepare(eta, kk, surface.u_roughness, surface.v_roughness, surface.remap != 0, bsdf.conductor)
+                : dielectric_prepare(eta, surface.u_roughness, surface.v_roughness, surface.remap != 0, bsdf.dielectric);
+        F3 dpdu, dpdv;
+        coordinate_system(point.shading_normal, dpdu, dpdv);
+        if (!prepared || !scattering_frame(point.shading_normal, dpdu, frame))
+            return fail(RP_SAMPLE_INVALID_ARITHMETIC);
+        wo = frame.local(-l.d);
+        if (wo.z == 0)
+            return true;
+    }
+    const bool dirac = microfacet && delta_only(bsdf);
+    const bool both_hemispheres = microfacet && bsdf.kind == RP_DIELECTRIC;
+    const F3 context_normal = microfacet ? frame.z : point.shading_normal;
     const bool directional_offset = authored_normals;
     const F3 area_reference = directional_offset ? point.position : spawn_origin(l.o, l.d, hit.t, point, n);
     if (!finite3(area_reference))
@@ -647,7 +698,7 @@ bool scalar_event(const Ctx &c, Lane &l) {
     const U4 light_words = draw_words(s, p, l.sample, l.index, 2 + 2 * bounce);
     const U4 bsdf_words = draw_words(s, p, l.sample, l.index, 1 + 2 * bounce);
     // light sample: the demo sky, uniform on the sphere with the cosine-ratio weight
-    // (shaders/scalar_transport.h:709-781); PBRT lights, :783-835
+    // (shaders/scalar_transport.h:709-781); PBRT lights, :783-835; none at Dirac surfaces
     if (s.model == RP_MODEL_DEMO) {
         const float E = l.E;
         const float uz = sample_uniform(p, light_words.x), uv = sample_uniform(p, light_words.y);
@@ -656,8 +707,11 @@ bool scalar_event(const Ctx &c, Lane &l) {
         const float r = std::sqrt(std::max(0.0f, 1.0f - z * z));
         const float phi = 2.0f * pi_f * uv;
         const F3 direction{r * std::cos(phi), r * std::sin(phi), z};
-        const float cosine = dot(n, direction);
-        if (E > 0.0f && cosine > 0.0f) {
+        const F3 local_light = microfacet ? frame.local(direction) : F3{0, 0, 0};
+        const float cosine = both_hemispheres ? std::fabs(local_light.z)
+                             : microfacet     ? (wo.z > 0 ? local_light.z : -local_light.z)
+                                              : dot(n, direction);
+        if (!dirac && E > 0.0f && cosine > 0.0f) {
             const F3 origin = directional_offset ? spawn_toward(l.o, l.d, hit.t, point, direction) : area_reference;
             if (!finite3(origin))
                 return fail(RP_SAMPLE_INVALID_ARITHMETIC);
@@ -667,34 +721,42 @@ bool scalar_event(const Ctx &c, Lane &l) {
             if (vis.status != RP_SAMPLE_SUCCESS)
                 return fail(vis.status);
             if (vis.value > 0) {
-                // (4 cos) * light_weight(cos) (shaders/render.metal:838-841)
-                const float relative = 4.0f * cosine;
-                const float factor = relative * (1.0f / (1.0f + relative * relative));
+                float factor;
+                if (microfacet) {
+                    const Eval e = scalar_evaluate(bsdf, wo, local_light);
+                    factor = e.valid ? scattering_direct(e.f * cosine, e.pdf, 1.0f / (4.0f * pi_f), false) : NAN;
+                } else {
+                    // (4 cos) * light_weight(cos) (shaders/render.metal:838-841)
+                    const float relative = 4.0f * cosine;
+                    factor = relative * (1.0f / (1.0f + relative * relative));
+                }
                 if (!std::isfinite(factor))
                     return fail(RP_SAMPLE_INVALID_ARITHMETIC);
                 l.radiance += l.throughput * rho * factor * E * vis.value;
             }
         }
-    } else {
-        const Incident light = light_sample_scalar(s, l.wavelength, point.position, point.shading_normal,
+    } else if (!dirac) {
+        const Incident light = light_sample_scalar(s, l.wavelength, point.position, context_normal,
                                                    sample_uniform(p, light_words.x), sample_uniform(p, light_words.y),
                                                    sample_uniform(p, light_words.z));
         if (!light.valid)
             return fail(RP_SAMPLE_INVALID_ARITHMETIC);
         if (light.pdf > 0 && light.radiance > 0) {
-            const float cosine = dot(n, light.direction);
+            const F3 local_light = microfacet ? frame.local(light.direction) : F3{0, 0, 0};
+            const float cosine = both_hemispheres ? std::fabs(local_light.z)
+                                 : microfacet     ? (wo.z > 0 ? local_light.z : -local_light.z)
+                                                  : dot(n, light.direction);
             if (cosine > 0) {
-                const float f_cos = rho * cosine / pi_f;
-                const float bsdf_pdf = cosine / pi_f;
-                // scattering_direct, shaders/render.metal:2212-2219
-                float factor;
-                if (!(f_cos >= 0) || !(bsdf_pdf >= 0) || !(light.pdf > 0) || !std::isfinite(f_cos) ||
-                    !std::isfinite(bsdf_pdf) || !std::isfinite(light.pdf))
-                    factor = NAN;
-                else if (f_cos == 0)
-                    factor = 0;
-                else
-                    factor = (f_cos / light.pdf) * (delta_light(light) ? 1.0f : power_weight(light.pdf, bsdf_pdf));
+                float f_cos = rho * cosine / pi_f;
+                float bsdf_pdf = cosine / pi_f;
+                if (microfacet) {
+                    const Eval e = scalar_evaluate(bsdf, wo, local_light);
+                    if (!e.valid)
+                        return fail(RP_SAMPLE_INVALID_ARITHMETIC);
+                    f_cos = e.f * cosine;
+                    bsdf_pdf = e.pdf;
+                }
+                const float factor = scattering_direct(f_cos, bsdf_pdf, light.pdf, delta_light(light));
                 const F3 origin =
                     directional_offset ? spawn_toward(l.o, l.d, hit.t, point, light.direction) : area_reference;
                 const F3 cd = connection_direction(light, origin);
@@ -709,9 +771,32 @@ bool scalar_event(const Ctx &c, Lane &l) {
             }
         }
     }
-    // continuation, shaders/scalar_transport.h:837-900
-    const F3 wi = hemisphere(n, sample_uniform(p, bsdf_words.x), sample_uniform(p, bsdf_words.y));
-    l.throughput *= rho;
+    // continuation, shaders/scalar_transport.h:837-900; a microfacet sample is resolved in world
+    // space by resolve_scattering_continuation (shaders/render.metal:2006-2019)
+    F3 wi{0, 0, 0};
+    float continuation_pdf = 0, continuation_cosine = 0;
+    bool continuation_delta = false;
+    if (microfacet) {
+        const float lobe = bsdf.kind == RP_DIELECTRIC
+                               ? sample_uniform(p, dielectric_lobe_word(s, p, l.sample, l.index, bounce))
+                               : 0.0f; // the conductor draws no lobe
+        float sampled_eta;
+        BSample sampled = scalar_sample(bsdf, wo, lobe, sample_uniform(p, bsdf_words.x),
+                                        sample_uniform(p, bsdf_words.y), sampled_eta);
+        if (sampled.valid && sampled.accepted && !unit_vector(frame.world(sampled.wi), wi))
+            sampled.valid = false;
+        if (!sampled.valid)
+            return fail(RP_SAMPLE_INVALID_ARITHMETIC);
+        if (!sampled.accepted)
+            return true;
+        l.throughput *= sampled.weight;
+        continuation_pdf = sampled.pdf;
+        continuation_cosine = std::fabs(sampled.wi.z);
+        continuation_delta = sampled.delta;
+    } else {
+        wi = hemisphere(n, sample_uniform(p, bsdf_words.x), sample_uniform(p, bsdf_words.y));
+        l.throughput *= rho;
+    }
     if (!std::isfinite(l.throughput) || l.throughput < 0.0f)
         return fail(RP_SAMPLE_INVALID_ARITHMETIC);
     ++l.scatterings;
@@ -722,14 +807,16 @@ bool scalar_event(const Ctx &c, Lane &l) {
         if (!std::isfinite(l.throughput))
             return fail(RP_SAMPLE_INVALID_ARITHMETIC);
     }
-    const float cosine = dot(n, wi);
+    const float cosine = microfacet ? continuation_cosine : dot(n, wi);
     if (!(cosine > 0.0f))
         return fail(RP_SAMPLE_INVALID_ARITHMETIC);
-    l.previous_bsdf_pdf = cosine / pi_f;
-    l.previous_delta = false;
+    l.previous_bsdf_pdf = microfacet ? continuation_pdf : cosine / pi_f;
+    l.previous_delta = continuation_delta;
     l.prev_p = point.position;
-    l.prev_n = point.shading_normal;
-    l.escape_weight = bsdf_weight(cosine);
+    l.prev_n = context_normal;
+    l.escape_weight = continuation_delta ? 1.0f
+                      : microfacet       ? power_weight(l.previous_bsdf_pdf, 1.0f / (4.0f * pi_f))
+                                         : bsdf_weight(cosine);
     const F3 origin = directional_offset ? spawn_toward(l.o, l.d, hit.t, point, wi) : area_reference;
     if (!finite3(origin))
         return fail(RP_SAMPLE_INVALID_ARITHMETIC);

@@ -894,6 +894,7 @@ struct rp_scene {
     u32 tree_levels = 0;     // most internal nodes on a root-to-leaf path of the LBVH
     u32 wide_levels = 0;     // levels of the compressed 8-wide traversal tree
     bool resolve = false;    // hero scene with pass-through or mix-root instances
+    bool dielectrics = false; // a dielectric material: the QMC samplers' depth limit
     u32 tex_width = 0, tex_height = 0; // film size the texture camera differentials were found for
     double demo_film_scale = 0;        // demo film: 470 / integral of the CIE y table
     float4 *world = nullptr; // world-space triangle vertices in original order
@@ -1214,14 +1215,8 @@ u32 halton_scale(u32 resolution, u32 base) {
     return scale;
 }
 
-std::string validate_request(const rp_scene *s, const rp_request &r) {
-    if (!r.width || !r.height || !r.pixel_count || !r.sample_count)
-        return "Render request must have nonzero film, pixel and sample counts";
-    if (uint64_t(r.pixel_begin) + r.pixel_count > uint64_t(r.width) * r.height)
-        return "Render request pixels exceed the film";
-    if (uint64_t(r.pixel_count) * r.sample_count > 0xffffffffull)
-        return "Render request lanes exceed 2^32";
-    // validate_sampler_range (src/sampling.cpp:51-113)
+// validate_sampler_range (src/sampling.cpp:51-113)
+std::string validate_sampler_range(const rp_request &r) {
     if (r.sample_begin > UINT64_MAX - (r.sample_count - 1))
         return "Sampler range must be nonempty and fit the absolute sample indices";
     if (r.sampler_kind == RP_SAMPLER_INDEPENDENT)
@@ -1239,9 +1234,6 @@ std::string validate_request(const rp_scene *s, const rp_request &r) {
         const uint64_t stride = uint64_t(halton_scale(r.width, 2)) * halton_scale(r.height, 3);
         if (last > (uint64_t(INT64_MAX) - (stride - 1)) / stride)
             return "Halton absolute sample range exceeds the signed 64-bit index capacity";
-        const u32 depth_limit = s && s->transport == RP_TRANSPORT_SCALAR ? 124u : 1024u;
-        if (s && s->ds.max_depth > depth_limit)
-            return "Halton supports at most depth 124 for this transport";
         return {};
     }
     const u32 v = std::max(std::max(r.width, r.height), 1u) - 1;
@@ -1261,6 +1253,27 @@ std::string validate_request(const rp_scene *s, const rp_request &r) {
     }
     if (last >= (uint64_t(1) << (52 - 2 * m)))
         return "Sobol absolute sample range exceeds the 52-bit interval index capacity";
+    return {};
+}
+
+std::string validate_request(const rp_scene *s, const rp_request &r) {
+    if (!r.width || !r.height || !r.pixel_count || !r.sample_count)
+        return "Render request must have nonzero film, pixel and sample counts";
+    if (uint64_t(r.pixel_begin) + r.pixel_count > uint64_t(r.width) * r.height)
+        return "Render request pixels exceed the film";
+    if (uint64_t(r.pixel_count) * r.sample_count > 0xffffffffull)
+        return "Render request lanes exceed 2^32";
+    const std::string range = validate_sampler_range(r);
+    if (!range.empty())
+        return range;
+    // sampler_max_depth (src/sampling.cpp:129-135) as MetalRenderScene::sample applies it
+    // (src/metal_render.mm:1898-1904): QMC samplers need the PBRT model within their dimensions
+    if (s && r.sampler_kind != RP_SAMPLER_INDEPENDENT) {
+        const u32 limit = r.sampler_kind == RP_SAMPLER_HALTON ? (s->dielectrics ? 110u : 124u)
+                                                              : (s->dielectrics ? 113u : 127u);
+        if (s->ds.model != kModelPbrt || s->ds.max_depth > limit)
+            return "QMC sampling requires PBRT rendering with maxdepth at most " + std::to_string(limit);
+    }
     return {};
 }
 
@@ -1932,9 +1945,7 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             if (f > RP_DIELECTRIC && f != RP_INTERFACE && f != RP_MIX)
                 throw NotBuilt{"unsupported scattering family (diffuse, conductor, dielectric, mix and null "
                                "interfaces are built)"};
-            if (scalar && (f == RP_CONDUCTOR || f == RP_DIELECTRIC))
-                throw NotBuilt{"the scalar transport builds diffuse surfaces and null interfaces; conductor and "
-                               "dielectric surfaces render with the hero transport"};
+            s->dielectrics = s->dielectrics || f == RP_DIELECTRIC; // scene_has_dielectrics (src/render.cpp:927-932)
         }
         for (u32 i = 0; i < d->instance_count; ++i) {
             const auto &in = d->instances[i];

@@ -585,14 +585,73 @@ RP_DEV int connection_step(const DeviceScene &s, const ScalarParams &q, ScalarPa
             return kEventFinished;
         }
         path.radiance += c.b * value;
+    } else if (isnan(c.a)) {
+        // a light sample whose weight failed: invalid where the light is seen
+        if (T > 0) {
+            path.status = S_ARITHMETIC;
+            return kEventFinished;
+        }
     } else {
         path.radiance += c.a * T;
     }
     return apply_after(path, c.after);
 }
 
+// One wavelength of a conductor (kind 1) or dielectric (kind 2) surface: prepare_scattering
+// (shaders/render.metal:2079-2160) for constant roughness and tabulated optical constants, with
+// rypath_conductor::prepare (shaders/conductor.h:22-34) and rypath_dielectric::prepare
+// (shaders/dielectric.h:15-27; eta 1 is smooth).
+struct ScalarBsdf {
+    u32 kind;
+    float eta, k;
+    Ggx g;
+};
+RP_DEV bool prepare_scalar_bsdf(const DeviceScene &s, const DMaterial &m, float w, ScalarBsdf &b) {
+    b.kind = m.scattering;
+    const float u = m.u_roughness, v = m.v_roughness;
+    if (!isfinite(u) || !isfinite(v) || u < 0 || v < 0)
+        return false;
+    float eta = optical_value(s.knots, m.eta_begin, m.eta_count, s.knot_count, (m.optical_extensions & 1u) != 0, w);
+    b.k = 0;
+    if (m.scattering == 1) {
+        b.k = optical_value(s.knots, m.k_begin, m.k_count, s.knot_count, (m.optical_extensions & 2u) != 0, w);
+        if (!isfinite(eta) || !isfinite(b.k) || eta < 0 || b.k < 0 || (eta == 0 && b.k == 0))
+            return false;
+    } else {
+        if (!isfinite(eta) || eta < 0)
+            return false;
+        eta = eta == 0 ? 1 : eta;
+    }
+    b.eta = eta;
+    return prepare_roughness(u, v, m.remap != 0, m.scattering == 2 && eta == 1, b.g);
+}
+RP_DEV Eval scalar_bsdf_evaluate(const ScalarBsdf &b, V3 wo, V3 wi) {
+    return b.kind == 2 ? dielectric_evaluate(b.eta, b.g, wo, wi) : conductor_evaluate(b.eta, b.k, b.g, wo, wi);
+}
+// scattering_direct (shaders/render.metal:2212-2219)
+RP_DEV float scattering_direct(float f_cos, float bsdf_pdf, float light_pdf, bool invisible) {
+    if (!(f_cos >= 0) || !(bsdf_pdf >= 0) || !(light_pdf > 0) || !isfinite(f_cos) || !isfinite(bsdf_pdf) ||
+        !isfinite(light_pdf))
+        return fnan();
+    if (f_cos == 0)
+        return 0;
+    return (f_cos / light_pdf) * (invisible ? 1.0f : power_weight(light_pdf, bsdf_pdf));
+}
+// The dielectric lobe choice of one bounce (shaders/render.metal:180-198): Halton dimension
+// 884 + bounce, (Z)Sobol dimension 908 + bounce, else Philox block 0x80000000 | bounce.
+RP_DEV u32 dielectric_lobe_word(const DeviceScene &s, const WaveParams &p, u32 pixel, u32 slo, u32 shi, u64 index,
+                                u32 bounce) {
+    if (p.sampler == 2)
+        return float_bits(qmc_radical(s.primes, 884u + bounce, index, p.randomization, p.seed_low));
+    if (p.sampler == 3)
+        return zdraw(s, p, index, 908u + bounce);
+    if (p.sampler == 1)
+        return sobol_word(s.sobol, index, 908u + bounce, p.randomization, p.seed_low);
+    return philox(make_uint4(pixel, slo, shi, 0x80000000u | bounce), p.seed_low, p.seed_high).x;
+}
+
 // One event after the path ray's closest hit: scalar_shade (shaders/scalar_transport.h:286-900)
-// for diffuse surfaces and null interfaces.  A light sample that needs a connection leaves it in
+// for diffuse, conductor and dielectric surfaces and null interfaces.  A light sample that needs a connection leaves it in
 // `c` (returning kEventConnect) after the continuation has been sampled: the two use disjoint
 // draws, and the connection's contribution and status are applied before the continuation's.
 RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarParams &q, ScalarPath &path, bool ok,
@@ -791,12 +850,16 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
         }
     }
     const DMaterial surface = s.materials[material_index];
+    // conductors and dielectrics carry their spectrum in the BSDF: rho = 1 (:591-598)
+    const bool microfacet = surface.scattering != 0;
     float rho = 0;
-    if (surface.scattering != 0) {
-        path.status = S_HIT; // microfacet surfaces are not built for the scalar transport
-        return kEventFinished;
-    }
-    if (s.model == kModelDemo) {
+    if (microfacet) {
+        if (surface.scattering > 2) {
+            path.status = S_HIT;
+            return kEventFinished;
+        }
+        rho = 1.0f;
+    } else if (s.model == kModelDemo) {
         if (surface.kind != 0) {
             path.status = S_HIT;
             return kEventFinished;
@@ -819,7 +882,7 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
     }
     if (rho == 0.0f)
         return kEventFinished;
-    const bool authored_normals = instance.normal_begin != kNone;
+    const bool authored_normals = instance.normal_begin != kNone || microfacet;
     if (!authored_normals && bounce >= p.emergency_limit) {
         path.status = S_EMERGENCY;
         return kEventFinished;
@@ -829,13 +892,29 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
         return kEventFinished;
     }
     const float incident_cosine = dot(point.shading_normal, path.d);
-    if (authored_normals && incident_cosine == 0.0f)
+    if (authored_normals && !microfacet && incident_cosine == 0.0f)
         return kEventFinished;
     if (bounce >= p.emergency_limit) {
         path.status = S_EMERGENCY;
         return kEventFinished;
     }
     const V3 n = incident_cosine > 0.0f ? -point.shading_normal : point.shading_normal;
+    // the BSDF in the shading frame of the normal (:677-694)
+    ScalarBsdf bsdf{};
+    Frame frame{};
+    V3 wo = v3(0, 0, 0);
+    if (microfacet) {
+        if (!prepare_scalar_bsdf(s, surface, path.wavelength, bsdf) || !shading_frame(point.shading_normal, frame)) {
+            path.status = S_ARITHMETIC;
+            return kEventFinished;
+        }
+        wo = to_local(frame, -path.d);
+        if (wo.z == 0)
+            return kEventFinished;
+    }
+    const bool dirac = microfacet && bsdf.g.smooth; // delta_only (shaders/scattering.h:25-28)
+    const bool both_hemispheres = microfacet && bsdf.kind == 2;
+    const V3 context_normal = microfacet ? frame.z : point.shading_normal;
     const bool directional_offset = authored_normals;
     const V3 area_reference = directional_offset ? point.position : spawn_origin(path.o, path.d, hit.t, point, n);
     if (!finite3(area_reference)) {
@@ -845,7 +924,8 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
     const uint4 light_words = draw_words(s, p, path.pixel, path.slo, path.shi, path.index, 2 + 2 * bounce);
     const uint4 bsdf_words = draw_words(s, p, path.pixel, path.slo, path.shi, path.index, 1 + 2 * bounce);
     // light sample: the demo model's sky sampled uniformly over the sphere with the
-    // cosine-ratio weight (:709-781); PBRT scenes' lights with power-heuristic MIS (:783-835)
+    // cosine-ratio weight (:709-781); PBRT scenes' lights with power-heuristic MIS (:783-835).
+    // Dirac surfaces take no light sample.
     bool connect = false;
     if (s.model == kModelDemo) {
         const float E = 1.0f; // sky_radiance of the demo model
@@ -854,14 +934,23 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
         const float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
         const float phi = 2.0f * kPi * uv;
         const V3 direction = v3(r * cosf(phi), r * sinf(phi), z);
-        const float cosine = dot(n, direction);
-        if (cosine > 0.0f) {
+        const V3 local_light = microfacet ? to_local(frame, direction) : v3(0, 0, 0);
+        const float cosine = both_hemispheres ? fabsf(local_light.z)
+                             : microfacet     ? (wo.z > 0 ? local_light.z : -local_light.z)
+                                              : dot(n, direction);
+        if (!dirac && cosine > 0.0f) {
             const V3 origin = directional_offset ? spawn_toward(path.o, path.d, hit.t, point, direction) : area_reference;
-            const float relative = 4.0f * cosine;
-            const float factor = relative * (1.0f / (1.0f + relative * relative)); // (4 cos) * light_weight(cos)
-            if (!finite3(origin) || !isfinite(factor)) {
+            if (!finite3(origin)) {
                 path.status = S_ARITHMETIC;
                 return kEventFinished;
+            }
+            float factor;
+            if (microfacet) {
+                const Eval e = scalar_bsdf_evaluate(bsdf, wo, local_light);
+                factor = e.valid ? scattering_direct(e.f * cosine, e.pdf, 1.0f / (4.0f * kPi), false) : fnan();
+            } else {
+                const float relative = 4.0f * cosine;
+                factor = relative * (1.0f / (1.0f + relative * relative)); // (4 cos) * light_weight(cos)
             }
             const u32 medium = outgoing_medium(instance, path.current_medium, point.geometric_normal, direction);
             if (s.media_enabled) {
@@ -876,11 +965,13 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
                 c.vacuum = true;
             }
             c.medium_sample = false;
-            c.a = ((path.throughput * rho) * factor) * E;
+            // a factor that is not finite fails the sample only where the sky is seen (:747-767):
+            // the connection carries it as NaN
+            c.a = isfinite(factor) ? ((path.throughput * rho) * factor) * E : fnan();
             connect = true;
         }
-    } else {
-        const Incident light = scalar_light_sample(s, path.wavelength, point.position, point.shading_normal,
+    } else if (!dirac) {
+        const Incident light = scalar_light_sample(s, path.wavelength, point.position, context_normal,
                                                    sample_uniform(p, light_words.x), sample_uniform(p, light_words.y),
                                                    sample_uniform(p, light_words.z));
         if (!light.valid) {
@@ -888,19 +979,23 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
             return kEventFinished;
         }
         if (light.pdf > 0 && light.radiance > 0) {
-            const float cosine = dot(n, light.direction);
+            const V3 local_light = microfacet ? to_local(frame, light.direction) : v3(0, 0, 0);
+            const float cosine = both_hemispheres ? fabsf(local_light.z)
+                                 : microfacet     ? (wo.z > 0 ? local_light.z : -local_light.z)
+                                                  : dot(n, light.direction);
             if (cosine > 0) {
-                const float f_cos = rho * cosine / kPi;
-                const float bsdf_pdf = cosine / kPi;
-                // scattering_direct (shaders/render.metal:2212-2219)
-                float factor;
-                if (!(f_cos >= 0) || !(bsdf_pdf >= 0) || !(light.pdf > 0) || !isfinite(f_cos) || !isfinite(bsdf_pdf) ||
-                    !isfinite(light.pdf))
-                    factor = fnan();
-                else if (f_cos == 0)
-                    factor = 0;
-                else
-                    factor = (f_cos / light.pdf) * (incident_delta(light) ? 1.0f : power_weight(light.pdf, bsdf_pdf));
+                float f_cos = rho * cosine / kPi;
+                float bsdf_pdf = cosine / kPi;
+                if (microfacet) {
+                    const Eval e = scalar_bsdf_evaluate(bsdf, wo, local_light);
+                    if (!e.valid) {
+                        path.status = S_ARITHMETIC;
+                        return kEventFinished;
+                    }
+                    f_cos = e.f * cosine;
+                    bsdf_pdf = e.pdf;
+                }
+                const float factor = scattering_direct(f_cos, bsdf_pdf, light.pdf, incident_delta(light));
                 const V3 origin = directional_offset ? spawn_toward(path.o, path.d, hit.t, point, light.direction)
                                                      : area_reference;
                 V3 cd;
@@ -932,11 +1027,41 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
             }
         }
     }
-    // continuation (:837-900)
+    // continuation (:837-900); a microfacet sample is resolved in world space by
+    // resolve_scattering_continuation (shaders/render.metal:2006-2019)
     u32 after = kAfterContinue;
-    const V3 wi = cosine_hemisphere(n, sample_uniform(p, bsdf_words.x), sample_uniform(p, bsdf_words.y));
-    path.throughput *= rho;
-    if (!isfinite(path.throughput) || path.throughput < 0.0f) {
+    V3 wi = v3(0, 0, 0);
+    float continuation_pdf = 0, continuation_cosine = 0;
+    bool continuation_delta = false;
+    if (microfacet) {
+        const float ux = sample_uniform(p, bsdf_words.x), uy = sample_uniform(p, bsdf_words.y);
+        BSample sampled;
+        if (bsdf.kind == 2) {
+            const float lobe =
+                sample_uniform(p, dielectric_lobe_word(s, p, path.pixel, path.slo, path.shi, path.index, bounce));
+            float sampled_eta;
+            sampled = dielectric_sample(bsdf.eta, bsdf.g, wo, lobe, ux, uy, sampled_eta);
+        } else {
+            sampled = conductor_sample(bsdf.eta, bsdf.k, bsdf.g, wo, ux, uy);
+        }
+        if (sampled.valid && sampled.accepted && !unit_vector(to_world(frame, sampled.wi), wi))
+            sampled.valid = false;
+        if (!sampled.valid) {
+            after = kAfterFail | (S_ARITHMETIC << 8);
+        } else if (!sampled.accepted) {
+            after = kAfterFinish;
+        } else {
+            path.throughput *= sampled.weight;
+            continuation_pdf = sampled.pdf;
+            continuation_cosine = fabsf(sampled.wi.z);
+            continuation_delta = sampled.delta;
+        }
+    } else {
+        wi = cosine_hemisphere(n, sample_uniform(p, bsdf_words.x), sample_uniform(p, bsdf_words.y));
+        path.throughput *= rho;
+    }
+    if (after != kAfterContinue) {
+    } else if (!isfinite(path.throughput) || path.throughput < 0.0f) {
         after = kAfterFail | (S_ARITHMETIC << 8);
     } else {
         ++path.scatterings;
@@ -945,15 +1070,17 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
         } else {
             if (path.scatterings >= 3)
                 path.throughput /= 0.75f;
-            const float cosine = dot(n, wi);
+            const float cosine = microfacet ? continuation_cosine : dot(n, wi);
             if (!isfinite(path.throughput) || !(cosine > 0.0f)) {
                 after = kAfterFail | (S_ARITHMETIC << 8);
             } else {
-                path.previous_bsdf_pdf = cosine / kPi;
-                path.previous_delta = false;
+                path.previous_bsdf_pdf = microfacet ? continuation_pdf : cosine / kPi;
+                path.previous_delta = continuation_delta;
                 path.prev_p = point.position;
-                path.prev_n = point.shading_normal;
-                path.escape_weight = bsdf_weight(cosine);
+                path.prev_n = context_normal;
+                path.escape_weight = continuation_delta ? 1.0f
+                                     : microfacet       ? power_weight(path.previous_bsdf_pdf, 1.0f / (4.0f * kPi))
+                                                        : bsdf_weight(cosine);
                 const V3 origin = directional_offset ? spawn_toward(path.o, path.d, hit.t, point, wi) : area_reference;
                 if (!finite3(origin)) {
                     after = kAfterFail | (S_ARITHMETIC << 8);

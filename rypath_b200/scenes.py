@@ -415,6 +415,43 @@ def cornell_features(feature, width=32, height=32, spp=4, max_depth=8) -> Scene:
     return scene
 
 
+def conductor_material(scene, eta, k, u, v, remap=True):
+    """A GGX conductor with constant optical constants (32 knots each, extended)."""
+    m = abi.Material()
+    m.scattering, m.kind, m.scalar_value = abi.CONDUCTOR, abi.REFLECTANCE_CONSTANT, 1.0
+    m.eta_begin, m.eta_count = _append_knots(scene, eta), 32
+    m.k_begin, m.k_count = _append_knots(scene, k), 32
+    m.optical_extensions, m.u_roughness, m.v_roughness = 3, u, v
+    m.remap_roughness = int(remap)
+    return m
+
+
+def dielectric_material(scene, eta, roughness, remap=True):
+    """A GGX dielectric with a constant eta (32 knots, extended)."""
+    m = abi.Material()
+    m.scattering, m.kind, m.scalar_value = abi.DIELECTRIC, abi.REFLECTANCE_CONSTANT, 1.0
+    m.eta_begin, m.eta_count, m.optical_extensions = _append_knots(scene, eta), 32, 1
+    m.u_roughness = m.v_roughness = roughness
+    m.remap_roughness = int(remap)
+    return m
+
+
+def cornell_microfacets(width=32, height=32, spp=4, max_depth=8, transport=abi.TRANSPORT_SCALAR) -> Scene:
+    """The Cornell-style box with every microfacet case of the transport: the short box a rough
+    anisotropic conductor, the tall box rough glass (eta 1.5), the right wall a smooth (Dirac)
+    mirror, under the area light."""
+    scene = cornell_box(width, height, spp, max_depth)
+    scene.name = "cornell_microfacets"
+    base = len(scene.materials)
+    scene.materials += [conductor_material(scene, 0.2, 3.4, 0.3, 0.08), dielectric_material(scene, 1.5, 0.04),
+                        conductor_material(scene, 1.1, 4.0, 0.0, 0.0)]
+    scene.instances[5].material = base
+    scene.instances[6].material = base + 1
+    scene.instances[4].material = base + 2
+    scene.transport = transport
+    return scene
+
+
 def triangle_frames(positions, triangles, uvs):
     """PBRT's triangle texture partials (dp/du, dp/dv from the vertices' uvs; for a degenerate
     uv parameterisation a frame around the geometric normal), per triangle, as (T, 6) float32."""
@@ -570,6 +607,19 @@ def demo_scene(width=256, height=192, spp=128, max_depth=5) -> Scene:
     scene.camera, scene.film_scale = demo_camera((4.1, 3.0, 6.2), (0, 1, -0.45), (0, 1, 0), 42.0)
     scene.model = abi.MODEL_DEMO
     scene.transport = abi.TRANSPORT_SCALAR
+    return scene
+
+
+def demo_microfacets(width=64, height=48, spp=8, max_depth=5) -> Scene:
+    """The demo scene with its three boxes made a rough conductor, smooth glass and rough glass
+    (the demo model shades conductors and dielectrics with rho = 1 and the unit sky)."""
+    scene = demo_scene(width, height, spp, max_depth)
+    scene.name = "demo_microfacets"
+    base = len(scene.materials)
+    scene.materials += [conductor_material(scene, 0.25, 3.1, 0.12, 0.12), dielectric_material(scene, 1.45, 0.0),
+                        dielectric_material(scene, 1.6, 0.1)]
+    for k in range(3):
+        scene.instances[3 + k].material = base + k
     return scene
 
 

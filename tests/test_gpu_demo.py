@@ -54,7 +54,7 @@ def test_demo_device_meets_analytic_moments(case):
     assert np.all(np.abs(xyz - mean) <= 6 * se + 2e-5 * np.maximum(1, np.abs(mean))), (xyz, mean, se)
 
 
-@pytest.mark.parametrize("sampler", [abi.SAMPLER_INDEPENDENT, abi.SAMPLER_SOBOL])
+@pytest.mark.parametrize("sampler", [abi.SAMPLER_INDEPENDENT])  # QMC samplers need the PBRT model
 def test_demo_lanes_match_oracle(sampler):
     scene = scenes.demo_scene(64, 48, 8)
     rs = build(scene)
@@ -75,9 +75,10 @@ def test_demo_lanes_match_oracle(sampler):
 def test_demo_device_film_equals_host_reduction():
     scene = scenes.demo_scene(16, 12, 8)
     rs = build(scene)
-    st, diag, film = rs.render_film(renderer.RenderSettings(16, 12, samples=8, batch_size=4, seed=3))
+    st, diag, film = rs.render_film(renderer.RenderSettings(16, 12, samples=8, batch_size=4, seed=3,
+                                                            sampler=abi.SAMPLER_INDEPENDENT))
     assert st == abi.RP_SUCCESS, diag
-    res = rs.sample_scalar(renderer.RenderRequest(16, 12, seed=3, sample_count=8))
+    res = rs.sample_scalar(renderer.RenderRequest(16, 12, seed=3, sample_count=8, sampler=abi.SAMPLER_INDEPENDENT))
     rs.close()
     assert res.status == abi.RP_SUCCESS, res.diagnostic
     host = np.zeros(16 * 12, abi.film_dtype())

@@ -193,10 +193,10 @@ def test_scene_validation_for_the_two_transports():
     fog.transport = abi.TRANSPORT_HERO
     built = renderer.build_renderer(fog)
     assert built.status == abi.RP_INVALID_ARGUMENT and "vacuum" in built.diagnostic
-    mixed = scenes.cornell_box(8, 8, 1)
-    mixed.materials[0].scattering = abi.CONDUCTOR
-    mixed.transport = abi.TRANSPORT_SCALAR
-    built = renderer.build_renderer(mixed)
+    layered = scenes.cornell_box(8, 8, 1)
+    layered.materials[0].scattering = 5  # rypath's coated diffuse: not built for either transport
+    layered.transport = abi.TRANSPORT_SCALAR
+    built = renderer.build_renderer(layered)
     assert built.status == abi.RP_NOT_BUILT
     rs = build(scenes.cornell_fog(8, 8, 1))
     res = rs.sample(renderer.RenderRequest(8, 8))
