@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define RP_ABI_VERSION 2u
+#define RP_ABI_VERSION 3u
 #define RP_NONE 0xffffffffu
 #define RP_SPECTRUM_BINS 471u /* 360..830 nm at 1 nm, src/render.hpp:29-36 */
 #define RP_SOBOL_TABLE_BYTES 234208u /* sizeof(sobol::Tables), src/sobol_shared.h:42 */
@@ -104,6 +104,18 @@ enum { RP_HERO_UNIFORM = 0, RP_HERO_VISIBLE = 1 };
 
 typedef struct rp_knot { float wavelength, value; } rp_knot; /* wire::SpectralKnot */
 
+/* PBRT analytic shapes in object space (GeometryAnalytic, src/geometry.hpp:25-37, as the wire
+ * record geometry_wire::Analytic, src/geometry_wire.h:31-40): angles in radians; a sphere of
+ * `radius` clipped to z in [z_min, z_max] and phi in [0, phi_max]; a disk of `radius` and
+ * `inner_radius` in the plane z = height; a cylinder of `radius` over z in [z_min, z_max]
+ * without end caps.  `kind` is the wire tag RP_PRIMITIVE_ANALYTIC. */
+enum { RP_PRIMITIVE_TRIANGLE = 1, RP_PRIMITIVE_PATCH = 2, RP_PRIMITIVE_ANALYTIC = 4 };
+enum { RP_ANALYTIC_SPHERE = 1, RP_ANALYTIC_DISK = 2, RP_ANALYTIC_CYLINDER = 3 };
+typedef struct rp_analytic {
+    uint32_t kind, subtype;
+    float radius, z_min, z_max, phi_max, inner_radius, height;
+} rp_analytic;
+
 /* One mesh placement; the subset of wire::Instance (src/render_wire.h:168-188) the hot
  * path reads.  matrix is row-major 3x4 object-to-world. */
 typedef struct rp_instance {
@@ -115,6 +127,12 @@ typedef struct rp_instance {
     uint32_t normal_begin; /* index into normals or RP_NONE */
     uint32_t inside_medium, outside_medium; /* RP_NONE = vacuum */
     uint32_t invisible_emitter; /* nonzero: rays pass through it (RenderScene::instance_invisible_emitters) */
+    /* the placement's bilinear patches (GeometryMesh::patches) and analytic shapes
+     * (GeometryMesh::analytics): ranges of rp_scene_desc.patches / .analytics (wire::Instance
+     * patch_begin / patch_count / analytic_begin / analytic_count, src/render_wire.h:168-188);
+     * patch corners index the instance's vertices like its triangles */
+    uint32_t patch_begin, patch_count;
+    uint32_t analytic_begin, analytic_count;
 } rp_instance;
 
 /* The subset of wire::Material (src/render_wire.h:107-130) used by diffuse, conductor and
@@ -246,6 +264,10 @@ typedef struct rp_scene_desc {
      * and film_scale = tan(vertical fov / 2). */
     uint32_t model;
     float film_scale;
+    /* Bilinear patches: 4 vertex indices each in tensor-product order p00, p10, p01, p11
+     * (src/geometry.hpp:44-45); analytic shapes (rp_analytic). */
+    uint32_t patch_count;    const uint32_t *patches;
+    uint32_t analytic_count; const rp_analytic *analytics;
 } rp_scene_desc;
 
 /* RenderRequest (src/metal_render.hpp:14-32). */
@@ -566,6 +588,17 @@ rp_status rp_cuda_probe_environment(const rp_images *images, const float *querie
  * texture direction of the x ray[3], unused[3]}. */
 rp_status rp_cuda_probe_texture_footprint(const float *queries, uint32_t count, float *results,
                                           char *diag, size_t diag_capacity);
+/* Bilinear patch intersection (intersect_bilinear, shaders/bilinear.h: PBRT's ruled-surface
+ * solve in float pairs): per query 20 floats {p00[3], p10[3], p01[3], p11[3], origin[3],
+ * direction[3], t_min, t_max} -> 4 floats {hit, t, u, v}. */
+rp_status rp_cuda_probe_bilinear(const float *queries, uint32_t count, float *results, char *diag,
+                                 size_t diag_capacity);
+/* Analytic shape intersection and evaluation (intersect_analytic / evaluate_analytic,
+ * shaders/analytic.h): per query 16 words {rp_analytic (8 words), origin[3], direction[3],
+ * t_min, t_max} -> 16 floats {hit, t, u, v, then at the hit (u, v) the object-space
+ * position[3], normal[3], dpdu[3], dpdv[3]}. */
+rp_status rp_cuda_probe_analytic(const float *queries, uint32_t count, float *results, char *diag,
+                                 size_t diag_capacity);
 /* The minimum one-pixel camera-ray differentials a film of width x height gives the texture
  * footprints of a scene with image reflectance (prepare_texture_camera_differentials,
  * src/texture_footprint.cpp:199-232), on the host. */

@@ -101,6 +101,10 @@ void or_image_lookup(const void *textures, uint32_t texture_count, uint32_t inde
                      uint32_t transfer_count, const float *queries, uint32_t count, float *results,
                      const float *ewa_weights);
 void or_rgb_spectrum(const float *table, const float *queries, uint32_t count, float *results);
+/* Bilinear patch and analytic shape queries in the layouts of rp_cuda_probe_bilinear and
+ * rp_cuda_probe_analytic (oracle_shapes.hpp). */
+void or_probe_bilinear(const float *queries, uint32_t count, float *results);
+void or_probe_analytic(const float *queries, uint32_t count, float *results);
 int or_environment_tables(const void *textures, uint32_t index, const void *levels, const uint32_t *texels,
                           uint32_t words, const float *transfer, const float *table, const float *illuminant,
                           float *cdf, size_t capacity, uint32_t *width, uint32_t *compensated_offset,

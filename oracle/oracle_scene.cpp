@@ -281,6 +281,62 @@ static F3 world_point(const Instance &in, F3 p) {
            F3{in.m[3], in.m[7], in.m[11]};
 }
 
+// The world-to-object map of a row-major object-to-world 3x4 matrix, in double and rounded
+// once (as the backend's host code computes it).
+static bool invert_affine(const float *m, float *out) {
+    const double a = m[0], b = m[1], c = m[2], d = m[4], e = m[5], f = m[6], g = m[8], h = m[9], i = m[10];
+    const double A = e * i - f * h, B = f * g - d * i, Cc = d * h - e * g;
+    const double det = a * A + b * B + c * Cc;
+    if (!(std::abs(det) > 0) || !std::isfinite(det))
+        return false;
+    const double inv[9] = {A / det,  (c * h - b * i) / det, (b * f - c * e) / det,
+                           B / det,  (a * i - c * g) / det, (c * d - a * f) / det,
+                           Cc / det, (b * g - a * h) / det, (a * e - b * d) / det};
+    const double t[3] = {m[3], m[7], m[11]};
+    for (int r = 0; r < 3; ++r) {
+        double shift = 0;
+        for (int k = 0; k < 3; ++k) {
+            out[4 * r + k] = float(inv[3 * r + k]);
+            shift -= inv[3 * r + k] * t[k];
+        }
+        out[4 * r + 3] = float(shift);
+    }
+    for (int k = 0; k < 12; ++k)
+        if (!std::isfinite(out[k]))
+            return false;
+    return true;
+}
+
+// The world box of procedural primitive `prim` as the device builder forms it: the patch's
+// corners or the corners of the shape's object box, in world space, widened by 2^-18 of their
+// magnitude and extent.
+void procedural_box(const Scene &s, u32 prim, F3 &lo, F3 &hi) {
+    const Instance &in = s.instances[s.tri_instance[prim]];
+    const u32 local = s.tri_local[prim];
+    lo = F3{INFINITY, INFINITY, INFINITY};
+    hi = -lo;
+    auto grow = [&](F3 w) {
+        lo = F3{std::fmin(lo.x, w.x), std::fmin(lo.y, w.y), std::fmin(lo.z, w.z)};
+        hi = F3{std::fmax(hi.x, w.x), std::fmax(hi.y, w.y), std::fmax(hi.z, w.z)};
+    };
+    if (prim - s.tri_prims < s.patch_prims) {
+        for (int k = 0; k < 4; ++k)
+            grow(world_point(in, s.positions[in.vertex_begin + s.patches[in.patch_begin + local][k]]));
+    } else {
+        const Analytic &a = s.analytics[in.analytic_begin + local];
+        const float r = a.radius;
+        const float ol[3] = {-r, -r, a.subtype == 2u ? a.height : (a.subtype == 1u ? std::fmax(a.z_min, -r) : a.z_min)};
+        const float oh[3] = {r, r, a.subtype == 2u ? a.height : (a.subtype == 1u ? std::fmin(a.z_max, r) : a.z_max)};
+        for (int k = 0; k < 8; ++k)
+            grow(world_point(in, F3{k & 1 ? oh[0] : ol[0], k & 2 ? oh[1] : ol[1], k & 4 ? oh[2] : ol[2]}));
+    }
+    const F3 m{std::fmax(std::fabs(lo.x), std::fabs(hi.x)), std::fmax(std::fabs(lo.y), std::fabs(hi.y)),
+               std::fmax(std::fabs(lo.z), std::fabs(hi.z))};
+    const F3 pad = 0x1p-18f * (m + (hi - lo)) + F3{1e-30f, 1e-30f, 1e-30f};
+    lo = lo - pad;
+    hi = hi + pad;
+}
+
 bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error) {
     s = Scene{};
     s.positions.resize(d.vertex_count);
@@ -350,6 +406,19 @@ bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error) {
         in.inside_medium = q.inside_medium;
         in.outside_medium = q.outside_medium;
         in.invisible = q.invisible_emitter;
+        in.patch_begin = q.patch_count ? q.patch_begin : 0;
+        in.patch_count = q.patch_count;
+        in.analytic_begin = q.analytic_count ? q.analytic_begin : 0;
+        in.analytic_count = q.analytic_count;
+        if ((q.patch_count && uint64_t(q.patch_begin) + q.patch_count > d.patch_count) ||
+            (q.analytic_count && uint64_t(q.analytic_begin) + q.analytic_count > d.analytic_count)) {
+            error = "instance patches or analytic shapes out of range";
+            return false;
+        }
+        if ((q.patch_count || q.analytic_count) && !invert_affine(q.matrix, in.inverse)) {
+            error = "an instance with patches or analytic shapes needs an invertible transform";
+            return false;
+        }
         if (q.emission != RP_NONE) {
             in.emitter_begin = u32(s.emitters.size());
             for (u32 t = 0; t < q.triangle_count; ++t)
@@ -366,6 +435,50 @@ bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error) {
             s.tri_local.push_back(t);
         }
     }
+    // procedural primitives after the triangles: every instance's patches, then every
+    // instance's analytic shapes
+    s.tri_prims = u32(s.world.size());
+    for (u32 i = 0; i < d.patch_count; ++i)
+        s.patches.push_back({d.patches[4 * i], d.patches[4 * i + 1], d.patches[4 * i + 2], d.patches[4 * i + 3]});
+    for (u32 i = 0; i < d.analytic_count; ++i) {
+        const rp_analytic &a = d.analytics[i];
+        // validate_analytic (src/analytic.hpp:14-50), the checks the backend makes
+        bool ok = a.subtype >= 1 && a.subtype <= 3 && std::isfinite(a.radius) && std::isfinite(a.z_min) &&
+                  std::isfinite(a.z_max) && std::isfinite(a.phi_max) && std::isfinite(a.inner_radius) &&
+                  std::isfinite(a.height) && a.radius > 0 && std::isnormal(a.radius) && std::isnormal(a.phi_max) &&
+                  a.phi_max > 0 && a.phi_max <= 2 * float(M_PI);
+        if (ok && a.subtype == 2)
+            ok = a.inner_radius >= 0 && a.inner_radius < a.radius && a.radius - a.inner_radius >= 0x1p-16f;
+        else if (ok)
+            ok = a.z_min < a.z_max && std::isnormal(a.z_max - a.z_min) && a.z_max - a.z_min >= 0x1p-16f &&
+                 a.z_max - a.z_min <= 0x1p16f &&
+                 (a.subtype != 1 || (a.z_min >= -a.radius && a.z_max <= a.radius &&
+                                     std::acos(a.z_min / a.radius) > std::acos(a.z_max / a.radius)));
+        ok = ok && a.radius >= 0x1p-16f && a.radius <= 0x1p16f && a.phi_max >= 0x1p-16f && std::fabs(a.z_min) <= 0x1p16f &&
+             std::fabs(a.z_max) <= 0x1p16f && std::fabs(a.height) <= 0x1p16f;
+        if (!ok) {
+            error = "invalid analytic shape";
+            return false;
+        }
+        s.analytics.push_back({a.kind, a.subtype, a.radius, a.z_min, a.z_max, a.phi_max, a.inner_radius, a.height});
+    }
+    for (u32 i = 0; i < d.instance_count; ++i)
+        for (u32 k = 0; k < d.instances[i].patch_count; ++k) {
+            for (u32 c = 0; c < 4; ++c)
+                if (uint64_t(d.instances[i].vertex_begin) + s.patches[d.instances[i].patch_begin + k][c] >= d.vertex_count) {
+                    error = "patch vertex out of range";
+                    return false;
+                }
+            s.tri_instance.push_back(i);
+            s.tri_local.push_back(k);
+            ++s.patch_prims;
+        }
+    for (u32 i = 0; i < d.instance_count; ++i)
+        for (u32 k = 0; k < d.instances[i].analytic_count; ++k) {
+            s.tri_instance.push_back(i);
+            s.tri_local.push_back(k);
+        }
+    s.procedural_prims = u32(s.tri_instance.size()) - s.tri_prims;
     // camera (src/metal_render.mm:158-191)
     s.origin = F3{d.camera.origin[0], d.camera.origin[1], d.camera.origin[2]};
     s.forward = F3{d.camera.corner[0], d.camera.corner[1], d.camera.corner[2]};
@@ -414,7 +527,15 @@ bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error) {
                 lo[a] = std::min(lo[a], double(p[a]));
                 hi[a] = std::max(hi[a], double(p[a]));
             }
-    if (s.world.empty()) {
+    for (u32 k = 0; k < s.procedural_prims; ++k) {
+        F3 blo, bhi;
+        procedural_box(s, s.tri_prims + k, blo, bhi);
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], double(blo[a]));
+            hi[a] = std::max(hi[a], double(bhi[a]));
+        }
+    }
+    if (s.tri_instance.empty()) {
         s.scene_radius = 1;
     } else {
         double c[3], e[3];
@@ -766,7 +887,31 @@ static inline bool better(float t, u32 prim, const Hit &h) {
     return t < h.t || (t == h.t && prim < h.prim);
 }
 
+static ShapeHit procedural_hit(const Scene &s, u32 prim, F3 o, F3 d, float tmax);
+// The procedural primitives, tested one by one after the triangle tree (the device tree holds
+// them with the triangles; the closest hit is the same).
+static void procedural_closest(const Scene &s, F3 o, F3 d, float tmax, Hit &h) {
+    for (u32 k = 0; k < s.procedural_prims; ++k) {
+        const u32 prim = s.tri_prims + k;
+        const ShapeHit ph = procedural_hit(s, prim, o, d, tmax);
+        if (ph.hit && better(ph.t, prim, h))
+            h = Hit{ph.t, ph.u, ph.v, prim};
+    }
+}
+
 Hit trace_closest(const Scene &s, const Bvh &b, F3 o, F3 d, float tmax) {
+    Hit h = trace_triangles(s, b, o, d, tmax);
+    if (s.procedural_prims) {
+        if (h.prim == RP_NONE)
+            h.t = tmax;
+        procedural_closest(s, o, d, tmax, h);
+        if (h.prim == RP_NONE)
+            return Hit{};
+    }
+    return h;
+}
+
+Hit trace_triangles(const Scene &s, const Bvh &b, F3 o, F3 d, float tmax) {
     Hit h;
     h.t = tmax;
     if (b.n == 0)
@@ -823,6 +968,9 @@ Hit trace_closest(const Scene &s, const Bvh &b, F3 o, F3 d, float tmax) {
 }
 
 bool trace_any(const Scene &s, const Bvh &b, F3 o, F3 d, float tmax) {
+    for (u32 k = 0; k < s.procedural_prims; ++k)
+        if (procedural_hit(s, s.tri_prims + k, o, d, tmax).hit)
+            return true;
     if (b.n == 0)
         return false;
     const F3 inv{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
@@ -858,6 +1006,7 @@ Hit trace_closest_brute(const Scene &s, F3 o, F3 d, float tmax) {
         if (intersect_triangle(o, d, s.world[p], tmax, t, b1, b2) && better(t, p, h))
             h = Hit{t, b1, b2, p};
     }
+    procedural_closest(s, o, d, tmax, h);
     return h.prim == RP_NONE ? Hit{} : h;
 }
 
@@ -948,6 +1097,7 @@ static float triangle_extent(F3 e1, F3 e2) {
 bool triangle_surface_point(const Scene &s, u32 instance, u32 local, float u, float v,
                             bool native_hit, SurfacePoint &point) {
     const Instance &in = s.instances[instance];
+    point.curved = false;
     const auto &tri = s.triangles[in.triangle_begin + local];
     const F3 p0 = s.positions[in.vertex_begin + tri[0]];
     const F3 p1 = s.positions[in.vertex_begin + tri[1]];
@@ -1004,6 +1154,143 @@ bool triangle_surface_point(const Scene &s, u32 instance, u32 local, float u, fl
            finite3(point.shading_normal);
 }
 
+// shaders/render.metal:970-1062 (patch_surface_point)
+static bool patch_surface_point(const Scene &s, u32 instance, u32 local, float u, float v, SurfacePoint &point) {
+    const Instance &in = s.instances[instance];
+    point.curved = true;
+    const auto &idx = s.patches[in.patch_begin + local];
+    F3 p[4];
+    for (int i = 0; i < 4; ++i)
+        p[i] = s.positions[in.vertex_begin + idx[i]];
+    const F3 ax{in.m[0], in.m[1], in.m[2]}, ay{in.m[4], in.m[5], in.m[6]}, az{in.m[8], in.m[9], in.m[10]};
+    const F3 e10 = p[1] - p[0], e32 = p[3] - p[2], e20 = p[2] - p[0], e31 = p[3] - p[1];
+    const F3 du = e10 + v * (e32 - e10), dv = e20 + u * (e31 - e20);
+    const F3 wu{dot(ax, du), dot(ay, du), dot(az, du)}, wv{dot(ax, dv), dot(ay, dv), dot(az, dv)};
+    const F3 c = cross(wu, wv);
+    const float squared = dot(c, c);
+    if (!(squared >= FLT_MIN) || !std::isfinite(squared))
+        return false;
+    point.inverse_area_pdf = std::sqrt(squared);
+    point.geometric_normal = c / point.inverse_area_pdf;
+    if (in.reverse)
+        point.geometric_normal = -point.geometric_normal;
+    point.shading_normal = point.geometric_normal;
+    if (in.normal_begin != RP_NONE) {
+        F3 n[4];
+        for (int i = 0; i < 4; ++i) {
+            if (in.normal_begin >= s.normals.size() || idx[i] >= s.normals.size() - in.normal_begin)
+                return false;
+            n[i] = s.normals[in.normal_begin + idx[i]];
+        }
+        const F3 a = n[0] + v * (n[2] - n[0]), b = n[1] + v * (n[3] - n[1]);
+        const F3 interp = a + u * (b - a);
+        if (!finite3(interp))
+            return false;
+        const float scale = std::fmax(std::fmax(std::fabs(interp.x), std::fabs(interp.y)), std::fabs(interp.z));
+        if (scale > 0) {
+            const F3 sc = interp / scale;
+            point.shading_normal = sc / std::sqrt(dot(sc, sc));
+            if (dot(point.geometric_normal, sc) < 0)
+                point.geometric_normal = -point.geometric_normal;
+        }
+    }
+    Pair lp[3];
+    const F3 magnitude = ((fabs3(p[0]) + fabs3(p[1])) + fabs3(p[2])) + fabs3(p[3]);
+    for (int a = 0; a < 3; ++a) {
+        const Pair lo = pr(p[0][a]) + (pr(p[2][a]) - pr(p[0][a])) * pr(v);
+        const Pair hi = pr(p[1][a]) + (pr(p[3][a]) - pr(p[1][a])) * pr(v);
+        lp[a] = lo + (hi - lo) * pr(u);
+    }
+    const bool identity = in.m[3] == 0 && in.m[7] == 0 && in.m[11] == 0 && in.m[0] == 1 && in.m[1] == 0 &&
+                          in.m[2] == 0 && in.m[4] == 0 && in.m[5] == 1 && in.m[6] == 0 && in.m[8] == 0 &&
+                          in.m[9] == 0 && in.m[10] == 1;
+    for (int a = 0; a < 3; ++a) {
+        Pair world = pr(in.m[4 * a + 3]);
+        float bound = std::fabs(in.m[4 * a + 3]);
+        for (int j = 0; j < 3; ++j) {
+            world = world + lp[j] * pr(in.m[4 * a + j]);
+            bound += magnitude[j] * std::fabs(in.m[4 * a + j]);
+        }
+        point.position[a] = world.hi;
+        const float traversal = identity ? 0.0f : 0x1p-20f * bound;
+        point.error[a] = ((std::fabs(world.lo) + 0x1p-40f * bound) + traversal) + 128.0f * FLT_MIN;
+    }
+    point.world_extent = 0;
+    for (int i = 1; i < 4; ++i) {
+        const F3 e = p[i] - p[0];
+        const F3 w = fabs3(F3{dot(ax, e), dot(ay, e), dot(az, e)});
+        point.world_extent = std::fmax(point.world_extent, std::fmax(w.x, std::fmax(w.y, w.z)));
+    }
+    return finite3(point.position) && finite3(point.error) && finite3(point.geometric_normal) &&
+           finite3(point.shading_normal);
+}
+// shaders/analytic.h:81-85
+static float stable_length(F3 v) {
+    const float scale = std::fmax(std::fabs(v.x), std::fmax(std::fabs(v.y), std::fabs(v.z)));
+    return scale > 0 ? scale * length3(v / scale) : 0;
+}
+// shaders/render.metal:1080-1118 (analytic_surface_point)
+static bool analytic_surface_point(const Scene &s, u32 instance, u32 local, float u, float v, SurfacePoint &point) {
+    const Instance &in = s.instances[instance];
+    point.curved = true;
+    if (local >= in.analytic_count)
+        return false;
+    const Analytic &rec = s.analytics[in.analytic_begin + local];
+    const AnalyticSurface ls = evaluate_analytic(rec, u, v);
+    if (!ls.valid)
+        return false;
+    const F3 a{in.m[0], in.m[1], in.m[2]}, b{in.m[4], in.m[5], in.m[6]}, c{in.m[8], in.m[9], in.m[10]};
+    const F3 cofactor{dot(cross(b, c), ls.normal), dot(cross(c, a), ls.normal), dot(cross(a, b), ls.normal)};
+    const float jacobian = stable_length(cofactor);
+    if (!(jacobian > 0) || !std::isfinite(jacobian))
+        return false;
+    point.geometric_normal = cofactor / jacobian;
+    if (in.reverse)
+        point.geometric_normal = -point.geometric_normal;
+    point.shading_normal = point.geometric_normal;
+    const F3 shift{in.m[3], in.m[7], in.m[11]};
+    point.position = F3{dot(a, ls.position), dot(b, ls.position), dot(c, ls.position)} + shift;
+    point.error = F3{dot(fabs3(a), ls.error), dot(fabs3(b), ls.error), dot(fabs3(c), ls.error)} +
+                  gamma_bound(5) * (fabs3(point.position) + fabs3(shift));
+    point.inverse_area_pdf = analytic_area(rec) * jacobian;
+    point.world_extent = 2 * rec.radius * std::fmax(length3(a), std::fmax(length3(b), length3(c)));
+    return finite3(point.position) && finite3(point.error) && std::isfinite(point.inverse_area_pdf) &&
+           point.inverse_area_pdf >= FLT_MIN;
+}
+bool hit_surface_point(const Scene &s, u32 prim, u32 instance, u32 local, float b1, float b2, SurfacePoint &p) {
+    if (prim < s.tri_prims)
+        return triangle_surface_point(s, instance, local, b1, b2, true, p);
+    if (prim - s.tri_prims < s.patch_prims)
+        return patch_surface_point(s, instance, local, b1, b2, p);
+    return analytic_surface_point(s, instance, local, b1, b2, p);
+}
+void ray_point(F3 o, F3 d, float t, bool curved, F3 &position, F3 &error) {
+    position = fma3(F3{t, t, t}, d, o);
+    error = gamma_bound(2) * (fabs3(t * d) + fabs3(o));
+    if (curved)
+        for (int a = 0; a < 3; ++a) {
+            const Pair value = pr(t) * pr(d[a]) + pr(o[a]);
+            position[a] = value.hi;
+            error[a] = (std::fabs(value.lo) + 0x1p-40f * (std::fabs(t * d[a]) + std::fabs(o[a]))) + 128.0f * FLT_MIN;
+        }
+}
+// The hit of the world ray o + t d, t in [0, tmax], on procedural primitive `prim`.
+static ShapeHit procedural_hit(const Scene &s, u32 prim, F3 o, F3 d, float tmax) {
+    const Instance &in = s.instances[s.tri_instance[prim]];
+    const u32 local = s.tri_local[prim];
+    const float *w = in.inverse;
+    const F3 r0{w[0], w[1], w[2]}, r1{w[4], w[5], w[6]}, r2{w[8], w[9], w[10]};
+    const F3 oo = F3{dot(r0, o), dot(r1, o), dot(r2, o)} + F3{w[3], w[7], w[11]};
+    const F3 od{dot(r0, d), dot(r1, d), dot(r2, d)};
+    if (prim - s.tri_prims < s.patch_prims) {
+        const auto &idx = s.patches[in.patch_begin + local];
+        return intersect_bilinear(s.positions[in.vertex_begin + idx[0]], s.positions[in.vertex_begin + idx[1]],
+                                  s.positions[in.vertex_begin + idx[2]], s.positions[in.vertex_begin + idx[3]], oo, od,
+                                  0.0f, tmax);
+    }
+    return intersect_analytic(s.analytics[in.analytic_begin + local], oo, od, 0.0f, tmax);
+}
+
 // shaders/render.metal:1939-1977
 bool spawn_boundary(F3 o, F3 d, float t, const SurfacePoint &pt, F3 direction, F3 &origin) {
     if (!(t >= 0) || !std::isfinite(t))
@@ -1013,8 +1300,8 @@ bool spawn_boundary(F3 o, F3 d, float t, const SurfacePoint &pt, F3 direction, F
     const float facing = dot(n, direction);
     if (!(facing > gamma_bound(5) * dot(fabs3(n), fabs3(direction))))
         return false;
-    const F3 position = fma3(F3{t, t, t}, d, o);
-    const F3 ray_error = gamma_bound(2) * (fabs3(t * d) + fabs3(o));
+    F3 position, ray_error;
+    ray_point(o, d, t, pt.curved, position, ray_error);
     const F3 error = (pt.error + fabs3(pt.position - position)) + ray_error;
     const float norm_lower = dot(n, n) * (1 - gamma_bound(4));
     const float height = dot(fabs3(n), error) * (1 + gamma_bound(8)) / norm_lower;
@@ -1381,3 +1668,51 @@ bool light_geometry_sample(const Scene &s, u32 emitter, F3 reference, F3 normal,
 }
 
 } // namespace oracle
+
+extern "C" {
+
+void or_probe_bilinear(const float *q, uint32_t count, float *out) {
+    using namespace oracle;
+    for (uint32_t i = 0; i < count; ++i) {
+        const float *a = q + 20 * size_t(i);
+        const ShapeHit h = intersect_bilinear(F3{a[0], a[1], a[2]}, F3{a[3], a[4], a[5]}, F3{a[6], a[7], a[8]},
+                                              F3{a[9], a[10], a[11]}, F3{a[12], a[13], a[14]}, F3{a[15], a[16], a[17]},
+                                              a[18], a[19]);
+        float *o = out + 4 * size_t(i);
+        o[0] = h.hit ? 1.f : 0.f;
+        o[1] = h.t;
+        o[2] = h.u;
+        o[3] = h.v;
+    }
+}
+
+void or_probe_analytic(const float *q, uint32_t count, float *out) {
+    using namespace oracle;
+    for (uint32_t i = 0; i < count; ++i) {
+        const float *a = q + 16 * size_t(i);
+        Analytic rec;
+        std::memcpy(&rec.kind, a, 4);
+        std::memcpy(&rec.subtype, a + 1, 4);
+        rec.radius = a[2];
+        rec.z_min = a[3];
+        rec.z_max = a[4];
+        rec.phi_max = a[5];
+        rec.inner_radius = a[6];
+        rec.height = a[7];
+        const ShapeHit h = intersect_analytic(rec, F3{a[8], a[9], a[10]}, F3{a[11], a[12], a[13]}, a[14], a[15]);
+        float *o = out + 16 * size_t(i);
+        o[0] = h.hit ? 1.f : 0.f;
+        o[1] = h.t;
+        o[2] = h.u;
+        o[3] = h.v;
+        const AnalyticSurface e = evaluate_analytic(rec, h.hit ? h.u : 0.f, h.hit ? h.v : 0.f);
+        const F3 vs[4] = {e.position, e.normal, e.dpdu, e.dpdv};
+        for (int k = 0; k < 4; ++k) {
+            o[4 + 3 * k] = vs[k].x;
+            o[5 + 3 * k] = vs[k].y;
+            o[6 + 3 * k] = vs[k].z;
+        }
+    }
+}
+
+} // extern "C"

@@ -5,6 +5,7 @@
 
 #include "oracle_math.hpp"
 #include "oracle_image.hpp"
+#include "oracle_shapes.hpp"
 #include "../include/rypath_cuda.h"
 
 #include <functional>
@@ -54,6 +55,8 @@ struct Instance {
     u32 emitter_begin;
     u32 inside_medium = RP_NONE, outside_medium = RP_NONE;
     u32 invisible = 0; // RenderScene::instance_invisible_emitters
+    u32 patch_begin = 0, patch_count = 0, analytic_begin = 0, analytic_count = 0;
+    float inverse[12] = {}; // world-to-object 3x4 of instances with procedural primitives
 };
 // HomogeneousMedium (src/render.hpp:29-36)
 struct Medium {
@@ -121,9 +124,13 @@ struct Scene {
     u32 light_count = 0, environment_light = RP_NONE;
     const SobolTables *sobol = nullptr;
     std::vector<unsigned char> sobol_storage;
-    // world-space triangles and their owning instance (flattened)
+    // world-space triangles and their owning instance (flattened), then the procedural
+    // primitives: every instance's patches, then every instance's analytic shapes
     std::vector<std::array<F3, 3>> world;
     std::vector<u32> tri_instance, tri_local;
+    std::vector<std::array<u32, 4>> patches;
+    std::vector<Analytic> analytics;
+    u32 tri_prims = 0, patch_prims = 0, procedural_prims = 0;
 };
 bool load_scene(const rp_scene_desc &d, Scene &s, std::string &error);
 // compile_gaussian_filter (src/gaussian_filter.cpp:84-137); empty string on success
@@ -152,6 +159,8 @@ struct Hit {
 // Watertight ray/triangle test; returns true when t in (0, tmax) is found.
 bool intersect_triangle(F3 o, F3 d, const std::array<F3, 3> &v, float tmax, float &t, float &b1,
                         float &b2);
+// The closest triangle hit alone (the binary tree holds the triangles).
+Hit trace_triangles(const Scene &s, const Bvh &b, F3 o, F3 d, float tmax);
 Hit trace_closest(const Scene &s, const Bvh &bvh, F3 o, F3 d, float tmax);
 bool trace_any(const Scene &s, const Bvh &bvh, F3 o, F3 d, float tmax);
 Hit trace_closest_brute(const Scene &s, F3 o, F3 d, float tmax);
@@ -162,7 +171,12 @@ struct SurfacePoint {
     F3 position, error, geometric_normal, shading_normal;
     float inverse_area_pdf = 0;
     float world_extent = 0;
+    bool curved = false; // a patch or analytic point
 };
+// surface_point (shaders/render.metal:1120-1132) of flattened primitive `prim` at a native hit
+bool hit_surface_point(const Scene &s, u32 prim, u32 instance, u32 local, float b1, float b2, SurfacePoint &p);
+// The ray's point at t and its rounding bound (shaders/render.metal:1913-1929)
+void ray_point(F3 o, F3 d, float t, bool curved, F3 &position, F3 &error);
 bool triangle_surface_point(const Scene &s, u32 instance, u32 local, float u, float v,
                             bool native_hit, SurfacePoint &p);
 

@@ -259,7 +259,7 @@ static bool visible(const Ctx &c, Sample &smp, const Vertex &a, const Vertex &b)
             return false;
         SurfacePoint pt;
         F3 next;
-        if (!triangle_surface_point(s, inst, s.tri_local[h.prim], h.b1, h.b2, true, pt) ||
+        if (!hit_surface_point(s, h.prim, inst, s.tri_local[h.prim], h.b1, h.b2, pt) ||
             !spawn_boundary(o, d, h.t, pt, normalize3(d), next)) {
             smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
             return false;
@@ -481,7 +481,7 @@ static void hero_step(const Ctx &c, LaneState &st) {
         v.v = hit.b2;
         v.light = instance.emission == RP_NONE ? RP_NONE : instance.emitter_begin + local;
         v.wo = -rd;
-        if (!triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, v.point)) {
+        if (!hit_surface_point(s, hit.prim, inst, local, hit.b1, hit.b2, v.point)) {
             smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
             break;
         }
@@ -535,8 +535,8 @@ static void hero_step(const Ctx &c, LaneState &st) {
             smp.status = RP_SAMPLE_INVALID_ARITHMETIC;
             break;
         }
-        const F3 ray_position = fma3(F3{hit.t, hit.t, hit.t}, rd, ro);
-        const F3 ray_error = gamma_bound(2) * (fabs3(hit.t * rd) + fabs3(ro));
+        F3 ray_position, ray_error;
+        ray_point(ro, rd, hit.t, v.point.curved, ray_position, ray_error);
         v.point.error = v.point.error + (fabs3(v.point.position - ray_position) + ray_error);
         if (!finite3(v.point.error)) {
             smp.status = RP_SAMPLE_INVALID_ARITHMETIC;

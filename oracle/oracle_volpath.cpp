@@ -171,8 +171,8 @@ F3 hemisphere(F3 n, float u, float v) {
 }
 // :1912-1929
 F3 spawn_origin(F3 o, F3 d, float t, const SurfacePoint &pt, F3 n) {
-    const F3 ray_position = fma3(F3{t, t, t}, d, o);
-    const F3 ray_error = gamma_bound(2.0f) * (fabs3(t * d) + fabs3(o));
+    F3 ray_position, ray_error;
+    ray_point(o, d, t, pt.curved, ray_position, ray_error);
     const F3 error = (pt.error + fabs3(pt.position - ray_position)) + ray_error;
     return round_out(pt.position + dot(fabs3(n), error) * n, n);
 }
@@ -324,7 +324,7 @@ Transmission medium_connection(const Ctx &c, float wavelength, F3 o, F3 d, float
         if (crossings++ >= c.boundary_limit)
             return {0, RP_SAMPLE_BOUNDARY_EXHAUSTION};
         SurfacePoint pt;
-        if (!triangle_surface_point(s, inst, s.tri_local[h.prim], h.b1, h.b2, true, pt))
+        if (!hit_surface_point(s, h.prim, inst, s.tri_local[h.prim], h.b1, h.b2, pt))
             return {0, RP_SAMPLE_INVALID_ARITHMETIC};
         F3 next;
         if (!spawn_boundary(o, direction, h.t, pt, direction, next))
@@ -578,7 +578,7 @@ bool scalar_event(const Ctx &c, Lane &l) {
         // shaders/scalar_transport.h:450-472
         if (l.boundary_crossings++ >= c.boundary_limit)
             return fail(RP_SAMPLE_BOUNDARY_EXHAUSTION);
-        if (!triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point))
+        if (!hit_surface_point(s, hit.prim, inst, local, hit.b1, hit.b2, point))
             return fail(RP_SAMPLE_INVALID_ARITHMETIC);
         l.current_medium = outgoing_medium(instance, l.current_medium, point.geometric_normal, l.d);
         F3 origin;
@@ -590,7 +590,7 @@ bool scalar_event(const Ctx &c, Lane &l) {
     const bool emissive = instance.emission != RP_NONE;
     if (emissive) {
         // shaders/scalar_transport.h:473-520
-        if (!triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point))
+        if (!hit_surface_point(s, hit.prim, inst, local, hit.b1, hit.b2, point))
             return fail(RP_SAMPLE_INVALID_ARITHMETIC);
         const float Le = point.inverse_area_pdf == 0 ? 0.0f : s.emission[instance.emission][dense_index(l.wavelength)];
         if (Le > 0.0f && (s.emission_two_sided[instance.emission] || dot(point.geometric_normal, -l.d) >= 0.0f)) {
@@ -612,7 +612,7 @@ bool scalar_event(const Ctx &c, Lane &l) {
     bool point_ready = emissive;
     u32 material_index = instance.material;
     if (material.scattering == 9) {
-        if (!emissive && !triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point))
+        if (!emissive && !hit_surface_point(s, hit.prim, inst, local, hit.b1, hit.b2, point))
             return fail(RP_SAMPLE_INVALID_ARITHMETIC);
         point_ready = true;
         if (const u32 mix_status = resolve_mix(s, point.position, -l.d, material_index))
@@ -656,7 +656,7 @@ bool scalar_event(const Ctx &c, Lane &l) {
     const bool authored_normals = instance.normal_begin != RP_NONE || microfacet;
     if (!authored_normals && bounce >= p.emergency_limit)
         return fail(RP_SAMPLE_EMERGENCY_DEPTH);
-    if (!point_ready && !triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point))
+    if (!point_ready && !hit_surface_point(s, hit.prim, inst, local, hit.b1, hit.b2, point))
         return fail(RP_SAMPLE_INVALID_ARITHMETIC);
     const float incident_cosine = dot(point.shading_normal, l.d);
     if (authored_normals && !microfacet && incident_cosine == 0.0f)

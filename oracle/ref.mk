@@ -1,6 +1,8 @@
 # Compiles rypath's own host-compilable sources, where they lie in a rypath checkout, into
 # oracle/_ref/: libref.so, the pin for the oracle's restatement; libref_image.so, rypath's
-# image shader headers and host image sources (with the PNG / JPEG decoders they link); and
+# image shader headers and host image sources (with the PNG / JPEG decoders they link);
+# libref_demo.so, the demo model; libref_shapes.so, the bilinear patch and analytic shape
+# shaders; and
 # roulette_known_answers,
 # rypath's own roulette test program built against the oracle's restatement of the roulette
 # header (oracle/roulette_as_ref).  Test infrastructure only; not rypath's build system.
@@ -34,7 +36,12 @@ DEMO_SRC := $(HERE)ref_demo_probe.cpp $(HERE)ref_image_host.cpp $(REF)/src/rende
 	$(REF)/src/texture_graph.cpp $(REF)/src/bsdf_table.cpp $(REF)/src/sampling.cpp $(REF)/src/area_power.cpp \
 	$(REF)/src/packet_film.cpp
 
-all: $(OUT)/libref.so $(OUT)/libref_image.so $(OUT)/libref_demo.so $(OUT)/roulette_known_answers
+all: $(OUT)/libref.so $(OUT)/libref_image.so $(OUT)/libref_demo.so $(OUT)/libref_shapes.so $(OUT)/roulette_known_answers
+
+# the procedural primitive shaders (shaders/bilinear.h, shaders/analytic.h)
+$(OUT)/libref_shapes.so: $(HERE)ref_shape_probe.cpp $(REF)/shaders/bilinear.h $(REF)/shaders/analytic.h $(HERE)ref_shim/metal_stdlib
+	mkdir -p $(OUT)
+	$(CXX) $(FLAGS) -Wl,--no-undefined -o $@ $(HERE)ref_shape_probe.cpp
 
 $(OUT)/gen/cie_xyz_data.hpp: $(REF)/third_party/cie/CIE_xyz_1931_2deg.csv
 	mkdir -p $(OUT)/gen

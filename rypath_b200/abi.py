@@ -6,7 +6,7 @@ their sizes against the values the library itself reports.
 
 import ctypes as C
 
-RP_ABI_VERSION = 2
+RP_ABI_VERSION = 3
 RP_NONE = 0xFFFFFFFF
 RP_SPECTRUM_BINS = 471
 RP_SOBOL_TABLE_BYTES = 234208
@@ -45,7 +45,17 @@ class Instance(C.Structure):
     _fields_ = [("matrix", f32 * 12), ("vertex_begin", u32), ("triangle_begin", u32),
                 ("triangle_count", u32), ("material", u32), ("reverse_orientation", u32),
                 ("emission", u32), ("normal_begin", u32), ("inside_medium", u32),
-                ("outside_medium", u32), ("invisible_emitter", u32)]
+                ("outside_medium", u32), ("invisible_emitter", u32), ("patch_begin", u32),
+                ("patch_count", u32), ("analytic_begin", u32), ("analytic_count", u32)]
+
+
+PRIMITIVE_TRIANGLE, PRIMITIVE_PATCH, PRIMITIVE_ANALYTIC = 1, 2, 4
+ANALYTIC_SPHERE, ANALYTIC_DISK, ANALYTIC_CYLINDER = 1, 2, 3
+
+
+class Analytic(C.Structure):
+    _fields_ = [("kind", u32), ("subtype", u32), ("radius", f32), ("z_min", f32), ("z_max", f32),
+                ("phi_max", f32), ("inner_radius", f32), ("height", f32)]
 
 
 class Material(C.Structure):
@@ -129,6 +139,8 @@ class SceneDesc(C.Structure):
         ("filter_sigma", f32),
         ("images", P(Images)),
         ("model", u32), ("film_scale", f32),
+        ("patch_count", u32), ("patches", P(u32)),
+        ("analytic_count", u32), ("analytics", P(Analytic)),
     ]
 
 
@@ -247,7 +259,7 @@ class FrameInfo(C.Structure):
 FRAME_PENDING, FRAME_COMPLETE, FRAME_FAILED = 0, 1, 2
 
 EXPECTED_SIZES = {
-    "rp_instance": (Instance, 88), "rp_material": (Material, 112), "rp_knot": (Knot, 8),
+    "rp_instance": (Instance, 104), "rp_analytic": (Analytic, 32), "rp_material": (Material, 112), "rp_knot": (Knot, 8),
     "rp_area_emission": (AreaEmission, 1888), "rp_positional_light": (PositionalLight, 1948),
     "rp_medium": (Medium, 5656), "rp_camera": (Camera, 48), "rp_request": (Request, 64),
     "rp_packet_result": (PacketResult, 80), "rp_scalar_result": (ScalarResult, 44),

@@ -72,7 +72,8 @@ struct Arena {
     std::vector<std::uint32_t> texels, uv_begin, frame_begin;
     std::vector<float> transfer, uvs, frames;
     rp_images images{};
-    std::vector<std::uint32_t> triangles;
+    std::vector<std::uint32_t> triangles, patches;
+    std::vector<rp_analytic> analytics;
     std::vector<rp_instance> instances;
     std::vector<rp_material> materials;
     std::vector<rp_knot> knots;
@@ -199,18 +200,26 @@ std::string describe_images(const RenderScene &s, Arena &a) {
 
 // RenderScene -> rp_scene_desc: what build_metal_renderer reads on the PT / hero path and for
 // the demo model (src/metal_render.mm:147-290, :505-700).  Returns a diagnostic for what the
-// backend does not build (analytic shapes and bilinear patches, texture graphs and surface
-// detail, some light kinds).
+// backend does not build (texture graphs and surface detail, some light kinds).  Bilinear
+// patches (GeometryMesh::patches, corner order p00 p10 p01 p11) and analytic shapes
+// (GeometryMesh::analytics, packed as pack_analytic does, src/analytic.hpp:51-60) go with their
+// mesh.
 std::string describe(const RenderScene &s, Arena &a, rp_scene_desc &d) {
     const bool demo = s.model == RenderModel::demo;
     if (!demo && !s.raster_camera)
         return "a PBRT-model scene needs its raster camera";
     std::vector<std::uint32_t> mesh_vertex(s.geometry.meshes.size()), mesh_triangle(s.geometry.meshes.size()),
-        mesh_normal(s.geometry.meshes.size(), RP_NONE);
+        mesh_normal(s.geometry.meshes.size(), RP_NONE), mesh_patch(s.geometry.meshes.size()),
+        mesh_analytic(s.geometry.meshes.size());
     for (std::size_t m = 0; m < s.geometry.meshes.size(); ++m) {
         const GeometryMesh &mesh = s.geometry.meshes[m];
-        if (!mesh.patches.empty() || !mesh.analytics.empty())
-            return "the CUDA backend renders triangle meshes only";
+        mesh_patch[m] = std::uint32_t(a.patches.size() / 4);
+        for (const auto &q : mesh.patches)
+            a.patches.insert(a.patches.end(), q.begin(), q.end());
+        mesh_analytic[m] = std::uint32_t(a.analytics.size());
+        for (const GeometryAnalytic &g : mesh.analytics)
+            a.analytics.push_back({RP_PRIMITIVE_ANALYTIC, std::uint32_t(g.kind), g.radius, g.z_min, g.z_max, g.phi_max,
+                                   g.inner_radius, g.height});
         mesh_vertex[m] = std::uint32_t(a.positions.size() / 3);
         mesh_triangle[m] = std::uint32_t(a.triangles.size() / 3);
         for (const auto &p : mesh.positions)
@@ -232,6 +241,10 @@ std::string describe(const RenderScene &s, Arena &a, rp_scene_desc &d) {
         in.vertex_begin = mesh_vertex[g.mesh_index];
         in.triangle_begin = mesh_triangle[g.mesh_index];
         in.triangle_count = std::uint32_t(s.geometry.meshes[g.mesh_index].triangles.size());
+        in.patch_begin = mesh_patch[g.mesh_index];
+        in.patch_count = std::uint32_t(s.geometry.meshes[g.mesh_index].patches.size());
+        in.analytic_begin = mesh_analytic[g.mesh_index];
+        in.analytic_count = std::uint32_t(s.geometry.meshes[g.mesh_index].analytics.size());
         in.material = s.instance_materials[i];
         in.reverse_orientation = s.instance_reverse_orientation.empty() ? 0 : s.instance_reverse_orientation[i];
         in.emission = s.instance_emissions.empty() ? RP_NONE : s.instance_emissions[i];
@@ -316,6 +329,10 @@ std::string describe(const RenderScene &s, Arena &a, rp_scene_desc &d) {
     d.normals = a.normals.empty() ? nullptr : a.normals.data();
     d.triangle_count = std::uint32_t(a.triangles.size() / 3);
     d.triangles = a.triangles.data();
+    d.patch_count = std::uint32_t(a.patches.size() / 4);
+    d.patches = a.patches.empty() ? nullptr : a.patches.data();
+    d.analytic_count = std::uint32_t(a.analytics.size());
+    d.analytics = a.analytics.empty() ? nullptr : a.analytics.data();
     d.instance_count = std::uint32_t(a.instances.size());
     d.instances = a.instances.data();
     d.material_count = std::uint32_t(a.materials.size());

@@ -89,6 +89,42 @@ RP_DEV void block_min_max(int (&lmin)[6], int (&lmax)[6], int *gmin, int *gmax) 
     }
 }
 
+// The world box of procedural primitive `prim`: the patch's corners, or the corners of the
+// shape's object box, moved to world space and widened by 2^-18 of their magnitude and extent
+// (the hit test runs on the ray moved to object space, whose rounding the slab test must not
+// cut off).  False for a patch corner outside the vertex array.
+RP_DEV bool procedural_box(const DeviceScene &s, const DInstance &in, u32 prim, u32 vertex_count, V3 &lo, V3 &hi) {
+    const float inf = __int_as_float(0x7f800000);
+    lo = v3(inf, inf, inf);
+    hi = -lo;
+    const u32 local = s.tri_local[prim];
+    if (prim - s.tri_prims < s.patch_prims) {
+        const u32 *pt = s.patches + 4 * size_t(in.patch_begin + local);
+        for (int k = 0; k < 4; ++k) {
+            if ((unsigned long long)in.vertex_begin + pt[k] >= vertex_count)
+                return false;
+            const V3 w = world_point(in, load3(s.positions + 3 * size_t(in.vertex_begin + pt[k])));
+            lo = v3(fminf(lo.x, w.x), fminf(lo.y, w.y), fminf(lo.z, w.z));
+            hi = v3(fmaxf(hi.x, w.x), fmaxf(hi.y, w.y), fmaxf(hi.z, w.z));
+        }
+    } else {
+        float ol[3], oh[3];
+        analytic_bounds(s.analytics[in.analytic_begin + local], ol, oh);
+        for (int k = 0; k < 8; ++k) {
+            const V3 w = world_point(in, v3(k & 1 ? oh[0] : ol[0], k & 2 ? oh[1] : ol[1], k & 4 ? oh[2] : ol[2]));
+            lo = v3(fminf(lo.x, w.x), fminf(lo.y, w.y), fminf(lo.z, w.z));
+            hi = v3(fmaxf(hi.x, w.x), fmaxf(hi.y, w.y), fmaxf(hi.z, w.z));
+        }
+    }
+    const V3 pad = 0x1p-18f * (v3(fmaxf(fabsf(lo.x), fabsf(hi.x)), fmaxf(fabsf(lo.y), fabsf(hi.y)),
+                                  fmaxf(fabsf(lo.z), fabsf(hi.z))) +
+                               (hi - lo)) +
+                   v3(1e-30f, 1e-30f, 1e-30f);
+    lo = lo - pad;
+    hi = hi + pad;
+    return finite3(lo) && finite3(hi);
+}
+
 // World-space vertices, boxes, centroid bounds and vertex bounds of every triangle.  A vertex
 // index outside the vertex array sets kBuildVertexRange and is not read.
 __global__ void k_tri_prepare(const __grid_constant__ DeviceScene s, float4 *world, BuildTmp t) {
@@ -101,25 +137,36 @@ __global__ void k_tri_prepare(const __grid_constant__ DeviceScene s, float4 *wor
     }
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < s.prim_count; i += gridDim.x * blockDim.x) {
         const DInstance &in = s.instances[s.tri_instance[i]];
-        const u32 *tri = s.triangles + 3 * size_t(in.triangle_begin + s.tri_local[i]);
-        bool valid = true;
+        V3 lo, hi;
+        if (i >= s.tri_prims) {
+            if (!procedural_box(s, in, i, t.vertex_count, lo, hi)) {
+                atomicOr(t.error, kBuildVertexRange);
+                continue;
+            }
 #pragma unroll
-        for (int k = 0; k < 3; ++k)
-            valid = valid && (unsigned long long)in.vertex_begin + tri[k] < t.vertex_count;
-        if (!valid) {
-            atomicOr(t.error, kBuildVertexRange);
-            continue;
-        }
-        V3 v[3];
+            for (int k = 0; k < 3; ++k)
+                world[3 * size_t(i) + k] = make_float4(0, 0, 0, 0);
+        } else {
+            const u32 *tri = s.triangles + 3 * size_t(in.triangle_begin + s.tri_local[i]);
+            bool valid = true;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            v[k] = world_point(in, load3(s.positions + 3 * size_t(in.vertex_begin + tri[k])));
-            world[3 * size_t(i) + k] = make_float4(v[k].x, v[k].y, v[k].z, 0);
+            for (int k = 0; k < 3; ++k)
+                valid = valid && (unsigned long long)in.vertex_begin + tri[k] < t.vertex_count;
+            if (!valid) {
+                atomicOr(t.error, kBuildVertexRange);
+                continue;
+            }
+            V3 v[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                v[k] = world_point(in, load3(s.positions + 3 * size_t(in.vertex_begin + tri[k])));
+                world[3 * size_t(i) + k] = make_float4(v[k].x, v[k].y, v[k].z, 0);
+            }
+            lo = v3(fminf(fminf(v[0].x, v[1].x), v[2].x), fminf(fminf(v[0].y, v[1].y), v[2].y),
+                    fminf(fminf(v[0].z, v[1].z), v[2].z));
+            hi = v3(fmaxf(fmaxf(v[0].x, v[1].x), v[2].x), fmaxf(fmaxf(v[0].y, v[1].y), v[2].y),
+                    fmaxf(fmaxf(v[0].z, v[1].z), v[2].z));
         }
-        const V3 lo = v3(fminf(fminf(v[0].x, v[1].x), v[2].x), fminf(fminf(v[0].y, v[1].y), v[2].y),
-                         fminf(fminf(v[0].z, v[1].z), v[2].z));
-        const V3 hi = v3(fmaxf(fmaxf(v[0].x, v[1].x), v[2].x), fmaxf(fmaxf(v[0].y, v[1].y), v[2].y),
-                         fmaxf(fmaxf(v[0].z, v[1].z), v[2].z));
         t.box_lo[i] = make_float4(lo.x, lo.y, lo.z, 0);
         t.box_hi[i] = make_float4(hi.x, hi.y, hi.z, 0);
         const float c[3] = {0.5f * lo.x + 0.5f * hi.x, 0.5f * lo.y + 0.5f * hi.y, 0.5f * lo.z + 0.5f * hi.z};

@@ -64,6 +64,65 @@ struct LightInput {
 
 // Mix materials (src/render.cpp:302-315, :1955-1995): finite amounts, children in range, no
 // cycle, at most 64 nested levels, and no null interface as a child.  Empty when valid.
+// validate_analytic (src/analytic.hpp:14-50): known shapes with finite, representable
+// parameters inside the shaders' numerical domain.
+std::string validate_analytic(const rp_analytic &a) {
+    if (a.subtype < RP_ANALYTIC_SPHERE || a.subtype > RP_ANALYTIC_CYLINDER)
+        return "Unknown analytic shape kind";
+    for (const float x : {a.radius, a.z_min, a.z_max, a.phi_max, a.inner_radius, a.height})
+        if (!std::isfinite(x))
+            return "Analytic shape parameters must be finite";
+    if (!(a.radius > 0 && std::isnormal(a.radius)) ||
+        !(std::isnormal(a.phi_max) && a.phi_max > 0 && a.phi_max <= 2 * std::numbers::pi_v<float>))
+        return "Analytic radius and angular extent must be positive and representable";
+    if (a.subtype == RP_ANALYTIC_DISK) {
+        if (!(a.inner_radius >= 0 && a.inner_radius < a.radius))
+            return "Analytic disk requires 0 <= inner radius < radius";
+    } else {
+        if (!(a.z_min < a.z_max))
+            return "Analytic surface requires positive height";
+        if (!std::isnormal(a.z_max - a.z_min))
+            return "Analytic surface height overflows or collapses in binary32";
+        if (a.subtype == RP_ANALYTIC_SPHERE && (a.z_min < -a.radius || a.z_max > a.radius))
+            return "Analytic sphere clipping lies outside its radius";
+        if (a.subtype == RP_ANALYTIC_SPHERE && !(std::acos(a.z_min / a.radius) > std::acos(a.z_max / a.radius)))
+            return "Analytic sphere angular parameterization collapses in binary32";
+    }
+    constexpr float minimum = 0x1p-16f, maximum = 0x1p16f;
+    if (a.radius < minimum || a.radius > maximum || a.phi_max < minimum || std::abs(a.z_min) > maximum ||
+        std::abs(a.z_max) > maximum || std::abs(a.height) > maximum ||
+        (a.subtype == RP_ANALYTIC_DISK ? a.radius - a.inner_radius < minimum
+                                       : (a.z_max - a.z_min < minimum || a.z_max - a.z_min > maximum)))
+        return "Analytic parameters exceed the shader numerical domain (lengths 2^-16..2^16, angular extent >= 2^-16)";
+    return {};
+}
+
+// The world-to-object map of a row-major object-to-world 3x4 matrix, in double and rounded
+// once; false for a singular or non-finite matrix.
+bool invert_affine(const float *m, float *out) {
+    const double a = m[0], b = m[1], c = m[2], d = m[4], e = m[5], f = m[6], g = m[8], h = m[9], i = m[10];
+    const double A = e * i - f * h, B = f * g - d * i, Cc = d * h - e * g;
+    const double det = a * A + b * B + c * Cc;
+    if (!(std::abs(det) > 0) || !std::isfinite(det))
+        return false;
+    const double inv[9] = {A / det, (c * h - b * i) / det, (b * f - c * e) / det,
+                           B / det, (a * i - c * g) / det, (c * d - a * f) / det,
+                           Cc / det, (b * g - a * h) / det, (a * e - b * d) / det};
+    const double t[3] = {m[3], m[7], m[11]};
+    for (int r = 0; r < 3; ++r) {
+        double shift = 0;
+        for (int k = 0; k < 3; ++k) {
+            out[4 * r + k] = float(inv[3 * r + k]);
+            shift -= inv[3 * r + k] * t[k];
+        }
+        out[4 * r + 3] = float(shift);
+    }
+    for (int k = 0; k < 12; ++k)
+        if (!std::isfinite(out[k]))
+            return false;
+    return true;
+}
+
 std::string validate_mix(const rp_scene_desc *d) {
     const u32 n = d->material_count;
     std::vector<unsigned char> state(n, 0); // 0 unvisited, 1 on the walk, 2 done
@@ -1544,7 +1603,12 @@ void run_scalar_wave(rp_scene *s, const WaveParams &p, u32 boundary_limit) {
                 s->launches += 1;
                 continue;
             }
-            if (s->counting && short_stack)
+            const bool procedural = s->ds.prim_count != s->ds.tri_prims;
+            if (procedural && s->counting)
+                k_scalar_walk<true, kStackDepth, true><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, w, parity, s->stats);
+            else if (procedural)
+                k_scalar_walk<false, kStackDepth, true><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, w, parity, s->stats);
+            else if (s->counting && short_stack)
                 k_scalar_walk<true, kShortStack><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, w, parity, s->stats);
             else if (s->counting)
                 k_scalar_walk<true, kStackDepth><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, w, parity, s->stats);
@@ -1771,6 +1835,7 @@ rp_status rp_cuda_device_info(int device, rp_device_info *info, char *diag, size
 uint32_t rp_cuda_abi_size(const char *name) {
     const std::string n = name ? name : "";
     if (n == "rp_instance") return sizeof(rp_instance);
+    if (n == "rp_analytic") return sizeof(rp_analytic);
     if (n == "rp_material") return sizeof(rp_material);
     if (n == "rp_knot") return sizeof(rp_knot);
     if (n == "rp_area_emission") return sizeof(rp_area_emission);
@@ -1859,6 +1924,8 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
                     throw Invalid{"Packet/hero spectral transport requires a PBRT scene with vacuum media"};
             }
         }
+        if ((d->patch_count && !d->patches) || (d->analytic_count && !d->analytics))
+            throw Invalid{"patch or analytic shape array missing"};
         if (const std::string mix = validate_mix(d); !mix.empty())
             throw Invalid{mix};
         if (const std::string images = validate_images(d); !images.empty())
@@ -1930,6 +1997,17 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
                 throw Invalid{"instance material out of range"};
             if (in.emission != RP_NONE && in.emission >= d->emission_count)
                 throw Invalid{"instance emission out of range"};
+            if ((in.patch_count && uint64_t(in.patch_begin) + in.patch_count > d->patch_count) ||
+                (in.analytic_count && uint64_t(in.analytic_begin) + in.analytic_count > d->analytic_count))
+                throw Invalid{"instance patches or analytic shapes out of range"};
+            if ((in.patch_count || in.analytic_count) && in.emission != RP_NONE)
+                throw NotBuilt{"area emission from bilinear patches and analytic shapes is not built"};
+            if ((in.patch_count || in.analytic_count) && d->materials[in.material].kind == RP_REFLECTANCE_IMAGE)
+                throw NotBuilt{"image reflectance on bilinear patches and analytic shapes is not built"};
+            for (u32 k = 0; k < in.analytic_count; ++k)
+                if (const std::string e = validate_analytic(d->analytics[in.analytic_begin + k]); !e.empty())
+                    throw Invalid{e};
+            prims += uint64_t(in.patch_count) + in.analytic_count;
             if (in.emission != RP_NONE)
                 for (u32 t = 0; t < in.triangle_count; ++t)
                     for (int k = 0; k < 3; ++k)
@@ -1995,6 +2073,33 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             }
             prim_begin[i] = next_prim;
             next_prim += q.triangle_count;
+            in.patch_begin = q.patch_count ? q.patch_begin : 0;
+            in.patch_count = q.patch_count;
+            in.analytic_begin = q.analytic_count ? q.analytic_begin : 0;
+            in.analytic_count = q.analytic_count;
+        }
+        // procedural primitives follow the triangles: every instance's patches, then every
+        // instance's analytic shapes, each range in instance order
+        std::vector<u32> patch_begin(d->instance_count), analytic_begin(d->instance_count);
+        u32 patch_prims = 0, analytic_prims = 0;
+        for (u32 i = 0; i < d->instance_count; ++i) {
+            patch_begin[i] = patch_prims;
+            patch_prims += d->instances[i].patch_count;
+        }
+        for (u32 i = 0; i < d->instance_count; ++i) {
+            analytic_begin[i] = analytic_prims;
+            analytic_prims += d->instances[i].analytic_count;
+        }
+        // the hero walks test procedural leaves in the kernels that resolve hits
+        if (!scalar && (patch_prims || analytic_prims))
+            s->resolve = true;
+        // world-to-object maps of the instances (procedural hits test the ray in object space)
+        std::vector<float> inverse(size_t(12) * std::max<u32>(d->instance_count, 1), 0.0f);
+        for (u32 i = 0; i < d->instance_count; ++i) {
+            if (!d->instances[i].patch_count && !d->instances[i].analytic_count)
+                continue;
+            if (!invert_affine(d->instances[i].matrix, inverse.data() + 12 * size_t(i)))
+                throw Invalid{"an instance with patches or analytic shapes needs an invertible transform"};
         }
         ds.positions = dupload(own, d->positions, size_t(3) * d->vertex_count, stm);
         ds.normals = dupload(own, d->normals, size_t(3) * d->normal_count, stm);
@@ -2014,18 +2119,34 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
         }
         ds.materials = dupload(own, mats.data(), mats.size(), stm);
         ds.material_count = d->material_count;
-        ds.prim_count = next_prim;
-        u32 *tri_instance = dalloc<u32>(own, next_prim, stm), *tri_local = dalloc<u32>(own, next_prim, stm);
-        unsigned char *tri_family = dalloc<unsigned char>(own, next_prim, stm);
+        const u32 all_prims = next_prim + patch_prims + analytic_prims;
+        ds.prim_count = all_prims;
+        ds.tri_prims = next_prim;
+        ds.patch_prims = patch_prims;
+        u32 *tri_instance = dalloc<u32>(own, all_prims, stm), *tri_local = dalloc<u32>(own, all_prims, stm);
+        unsigned char *tri_family = dalloc<unsigned char>(own, all_prims, stm);
         ds.tri_instance = tri_instance;
         ds.tri_local = tri_local;
         ds.tri_family = tri_family;
-        if (next_prim) {
-            const u32 *prim_begin_dev = dupload(own, prim_begin.data(), prim_begin.size(), stm);
-            k_flatten<<<grid_for(s->sm_count, next_prim, 256, 8), 256, 0, stm>>>(
-                ds.instances, prim_begin_dev, d->instance_count, ds.materials, next_prim, tri_instance, tri_local,
-                tri_family);
+        const std::vector<u32> *ranges[3] = {&prim_begin, &patch_begin, &analytic_begin};
+        const u32 range_base[3] = {0, next_prim, next_prim + patch_prims};
+        const u32 range_count[3] = {next_prim, patch_prims, analytic_prims};
+        for (int k = 0; k < 3; ++k) {
+            if (!range_count[k])
+                continue;
+            const u32 *begin_dev = dupload(own, ranges[k]->data(), ranges[k]->size(), stm);
+            k_flatten<<<grid_for(s->sm_count, range_count[k], 256, 8), 256, 0, stm>>>(
+                ds.instances, begin_dev, d->instance_count, ds.materials, range_count[k], tri_instance + range_base[k],
+                tri_local + range_base[k], tri_family + range_base[k]);
         }
+        ds.patches = dupload(own, d->patches, size_t(4) * d->patch_count, stm);
+        std::vector<DAnalytic> analytics(d->analytic_count);
+        for (u32 i = 0; i < d->analytic_count; ++i) {
+            const rp_analytic &a = d->analytics[i];
+            analytics[i] = {a.kind, a.subtype, a.radius, a.z_min, a.z_max, a.phi_max, a.inner_radius, a.height};
+        }
+        ds.analytics = dupload(own, analytics.data(), analytics.size(), stm);
+        ds.inverse = dupload(own, inverse.data(), inverse.size(), stm);
         const auto t_prepare = std::chrono::steady_clock::now();
         build_prepare(s, d->vertex_count);
         const auto t_prepared = std::chrono::steady_clock::now();
@@ -3077,6 +3198,31 @@ rp_batch_config tune_batch(rp_scene *s, const rp_view *views, u32 count, const r
 
 } // namespace
 
+// A float-in, float-out probe kernel over `count` queries of `in` and `out` floats each.
+template <typename Launch>
+rp_status float_probe(const float *queries, uint32_t count, u32 in, u32 out, float *results, char *diag, size_t cap,
+                      Launch launch) {
+    return guarded(diag, cap, [&]() -> rp_status {
+        std::vector<void *> own;
+        struct Free {
+            std::vector<void *> &o;
+            ~Free() {
+                for (void *p : o)
+                    cudaFreeAsync(p, nullptr);
+                cudaStreamSynchronize(nullptr);
+            }
+        } fr{own};
+        if (count == 0)
+            return RP_SUCCESS;
+        const float *q = dupload(own, queries, size_t(in) * count, nullptr);
+        float *r = dalloc<float>(own, size_t(out) * count);
+        launch(q, r);
+        RP_CHECK(cudaGetLastError());
+        RP_CHECK(cudaMemcpy(results, r, size_t(out) * count * 4, cudaMemcpyDeviceToHost));
+        return RP_SUCCESS;
+    });
+}
+
 extern "C" {
 
 rp_status rp_cuda_tune_views(rp_scene *s, const rp_view *views, uint32_t count, const rp_batch_request *request,
@@ -3187,6 +3333,18 @@ rp_status rp_cuda_probe_philox(const uint32_t *queries, uint32_t count, uint32_t
         RP_CHECK(cudaGetLastError());
         RP_CHECK(cudaMemcpy(results, r, size_t(4) * count * 4, cudaMemcpyDeviceToHost));
         return RP_SUCCESS;
+    });
+}
+
+rp_status rp_cuda_probe_bilinear(const float *queries, uint32_t count, float *results, char *diag, size_t cap) {
+    return float_probe(queries, count, 20, 4, results, diag, cap, [&](const float *q, float *r) {
+        k_probe_bilinear<<<(count + 127) / 128, 128>>>(q, count, r);
+    });
+}
+
+rp_status rp_cuda_probe_analytic(const float *queries, uint32_t count, float *results, char *diag, size_t cap) {
+    return float_probe(queries, count, 16, 16, results, diag, cap, [&](const float *q, float *r) {
+        k_probe_analytic<<<(count + 127) / 128, 128>>>(q, count, r);
     });
 }
 
@@ -3748,7 +3906,7 @@ rp_status rp_cuda_sample_device_static(rp_scene *s, const rp_request *request, r
         if (capacity < p.lanes)
             throw Invalid{"output capacity is smaller than the request lanes"};
         if (s->resolve)
-            throw Invalid{"the allocation-free entry point renders scenes without pass-through or mix surfaces"};
+            throw Invalid{"the allocation-free entry point renders scenes without pass-through, mix or procedural surfaces"};
         const u32 max_lanes = RP_STATIC_MAX_LANES;
         if (p.lanes > max_lanes) {
             set_diag(diag, cap,

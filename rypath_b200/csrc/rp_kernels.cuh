@@ -90,7 +90,7 @@ __device__ __noinline__ u32 resolve_hit(const DeviceScene &s, const PathPool &po
             break;
         }
         SurfacePoint pt;
-        if (!triangle_surface_point(s, inst, s.tri_local[h.prim], h.b1, h.b2, true, pt)) {
+        if (!hit_surface_point(s, h.prim, inst, s.tri_local[h.prim], h.b1, h.b2, pt)) {
             prim = kHitArithmetic;
             break;
         }
@@ -107,7 +107,7 @@ __device__ __noinline__ u32 resolve_hit(const DeviceScene &s, const PathPool &po
             ro = origin;
             moved = true;
             ++rays;
-            if (!walk_closest<Count, Stack>(s, ro, rd, __int_as_float(0x7f800000), h, stack, stride, nodes, tris)) {
+            if (!walk_closest<Count, Stack, true>(s, ro, rd, __int_as_float(0x7f800000), h, stack, stride, nodes, tris)) {
                 prim = kHitInvalid;
                 break;
             }
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1
                 const float4 o = pool.ray_o[path], d = pool.ray_d[path];
                 const u32 walks_before = rays;
                 Hit h;
-                const bool ok = walk_closest<Count, Stack>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z),
+                const bool ok = walk_closest<Count, Stack, Resolve>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z),
                                                            __int_as_float(0x7f800000), h, stack + threadIdx.x, Block,
                                                            nodes, tris);
                 ++rays;
@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_const
                         ctype = kSurface;
                         clight = instance.emission == kNone ? kNone : instance.emitter_begin + clocal;
                         cwo = -rd;
-                        if (!triangle_surface_point(s, cinst, clocal, b1, b2, true, cp)) {
+                        if (!hit_surface_point(s, prim, cinst, clocal, b1, b2, cp)) {
                             status = 2;
                             break;
                         }
@@ -326,8 +326,8 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_const
                             status = 2;
                             break;
                         }
-                        const V3 ray_position = fma3(v3(t, t, t), rd, ro);
-                        const V3 ray_error = gamma_bound(2) * (vabs(t * rd) + vabs(ro));
+                        V3 ray_position, ray_error;
+                        ray_point(ro, rd, t, cp.curved, ray_position, ray_error);
                         cp.error = cp.error + (vabs(cp.position - ray_position) + ray_error);
                         if (!finite3(cp.error)) {
                             status = 2;
@@ -753,7 +753,7 @@ __device__ __noinline__ u32 pass_through_visible(const DeviceScene &s, V3 o, V3 
     for (u32 crossings = 0; crossings <= boundary_limit; ++crossings) {
         Hit h;
         ++rays;
-        if (!walk_closest<Count, Stack>(s, o, d, tmax, h, stack, stride, nodes, tris))
+        if (!walk_closest<Count, Stack, true>(s, o, d, tmax, h, stack, stride, nodes, tris))
             return 3;
         if (h.prim == kNone) {
             occluded = false;
@@ -766,7 +766,7 @@ __device__ __noinline__ u32 pass_through_visible(const DeviceScene &s, V3 o, V3 
         if (!(in.resolve & kPassThrough))
             return 0;
         SurfacePoint pt;
-        if (!triangle_surface_point(s, inst, s.tri_local[h.prim], h.b1, h.b2, true, pt))
+        if (!hit_surface_point(s, h.prim, inst, s.tri_local[h.prim], h.b1, h.b2, pt))
             return 2;
         V3 next;
         if (!spawn_boundary(o, d, h.t, pt, normalize3(d), next))
@@ -799,7 +799,7 @@ __global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1
                                                          occluded, stack + threadIdx.x, Block, boundary_limit, nodes,
                                                          tris, rays);
         } else {
-            if (!walk_any<Count, Stack>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), o.w, occluded, stack + threadIdx.x,
+            if (!walk_any<Count, Stack, false>(s, v3(o.x, o.y, o.z), v3(d.x, d.y, d.z), o.w, occluded, stack + threadIdx.x,
                                         Block, nodes, tris))
                 failure = 3;
             ++rays;

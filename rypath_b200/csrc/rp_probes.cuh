@@ -181,6 +181,49 @@ __global__ void k_probe_image_lookup(const DImages im, u32 index, const float *q
     o[2] = c.b;
     o[3] = lookup_filtered(im, t, uv, dx, dy, true, false).r;
 }
+// Bilinear patch intersection: 20 floats per query -> {hit, t, u, v}.
+__global__ void k_probe_bilinear(const float *q, u32 count, float *out) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count)
+        return;
+    const float *a = q + 20 * i;
+    const ShapeHit h = intersect_bilinear(v3(a[0], a[1], a[2]), v3(a[3], a[4], a[5]), v3(a[6], a[7], a[8]),
+                                          v3(a[9], a[10], a[11]), v3(a[12], a[13], a[14]), v3(a[15], a[16], a[17]),
+                                          a[18], a[19]);
+    out[4 * i] = h.hit ? 1.f : 0.f;
+    out[4 * i + 1] = h.t;
+    out[4 * i + 2] = h.u;
+    out[4 * i + 3] = h.v;
+}
+// Analytic shape intersection and evaluation at the hit: 16 words per query -> 16 floats.
+__global__ void k_probe_analytic(const float *q, u32 count, float *out) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count)
+        return;
+    const float *a = q + 16 * i;
+    DAnalytic rec;
+    rec.kind = __float_as_uint(a[0]);
+    rec.subtype = __float_as_uint(a[1]);
+    rec.radius = a[2];
+    rec.z_min = a[3];
+    rec.z_max = a[4];
+    rec.phi_max = a[5];
+    rec.inner_radius = a[6];
+    rec.height = a[7];
+    const ShapeHit h = intersect_analytic(rec, v3(a[8], a[9], a[10]), v3(a[11], a[12], a[13]), a[14], a[15]);
+    float *o = out + 16 * i;
+    o[0] = h.hit ? 1.f : 0.f;
+    o[1] = h.t;
+    o[2] = h.u;
+    o[3] = h.v;
+    const AnalyticSurface e = evaluate_analytic(rec, h.hit ? h.u : 0.f, h.hit ? h.v : 0.f);
+    const V3 vs[4] = {e.position, e.normal, e.dpdu, e.dpdv};
+    for (int k = 0; k < 4; ++k) {
+        o[4 + 3 * k] = vs[k].x;
+        o[5 + 3 * k] = vs[k].y;
+        o[6 + 3 * k] = vs[k].z;
+    }
+}
 __global__ void k_probe_rgb_spectrum(const float *table, const float *q, u32 count, float *out) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count)

@@ -3,6 +3,7 @@
 #pragma once
 
 #include "rp_image.cuh"
+#include "rp_shapes.cuh"
 
 namespace rp {
 
@@ -16,6 +17,7 @@ struct DInstance {
     u32 vertex_begin, triangle_begin, triangle_count, material, reverse, emission, normal_begin, emitter_begin;
     u32 inside_medium, outside_medium; // kNone = vacuum
     u32 resolve;                       // kPassThrough | kMixRoot: hits resolve before shading
+    u32 patch_begin, patch_count, analytic_begin, analytic_count; // procedural primitives
 };
 constexpr u32 kMixScattering = 9, kInterfaceScattering = 10;
 // DInstance::resolve bits: the hero transport passes through the instance (an invisible
@@ -143,6 +145,13 @@ struct DeviceScene {
     DImages img;       // image textures and the environment image (env_image kNone: none)
     u32 model;         // kModelPbrt or kModelDemo (RenderModel)
     float film_scale;  // demo camera: tan(vertical fov / 2)
+    // procedural primitives: flattened primitives [0, tri_prims) are triangles, the next
+    // patch_prims bilinear patches, the rest analytic shapes; tri_local holds the index within
+    // the instance's primitives of that kind
+    u32 tri_prims, patch_prims;
+    const u32 *patches;        // 4 vertex indices each (p00 p10 p01 p11), instance-local
+    const DAnalytic *analytics;
+    const float *inverse;      // per instance: world-to-object 3x4, row-major
 };
 
 RP_DEV V3 load3(const float *p) { return v3(__ldg(p), __ldg(p + 1), __ldg(p + 2)); }
@@ -160,6 +169,7 @@ struct SurfacePoint {
     V3 position, error, geometric_normal, shading_normal;
     float inverse_area_pdf;
     float world_extent;
+    bool curved; // a patch or analytic point: ray positions carry their rounding in float pairs
 };
 // shaders/render.metal:865-868
 RP_DEV float triangle_extent(V3 e1, V3 e2) {
@@ -182,6 +192,7 @@ __device__ __noinline__ bool triangle_surface_point(const DeviceScene &s, u32 in
     const V3 we2 = v3(dot(ax, e2), dot(ay, e2), dot(az, e2));
     const V3 ce = cross(we1, we2);
     const float n2 = dot(ce, ce);
+    point.curved = false;
     if (n2 == 0.0f && !native_hit) {
         point.position = point.error = point.geometric_normal = point.shading_normal = v3(0, 0, 0);
         point.inverse_area_pdf = 0;
@@ -226,6 +237,177 @@ __device__ __noinline__ bool triangle_surface_point(const DeviceScene &s, u32 in
     point.error = v3(dot(vabs(ax), ein), dot(vabs(ay), ein), dot(vabs(az), ein)) + gamma_bound(4.0f) * vabs(shift);
     return finite3(point.position) && finite3(point.error) && finite3(point.geometric_normal) &&
            finite3(point.shading_normal);
+}
+
+// shaders/render.metal:970-1062 (patch_surface_point): the parametric point, the normal of the
+// world-space partials, vertex normals interpolated bilinearly, the position in float pairs
+// with its retained roundoff.
+__device__ __noinline__ bool patch_surface_point(const DeviceScene &s, u32 instance, u32 local, float u, float v,
+                                                 SurfacePoint &point) {
+    const DInstance &in = s.instances[instance];
+    point.curved = true;
+    const u32 *pt = s.patches + 4 * size_t(in.patch_begin + local);
+    u32 idx[4];
+    V3 p[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        idx[i] = __ldg(pt + i);
+        p[i] = load3(s.positions + 3 * size_t(in.vertex_begin + idx[i]));
+    }
+    const V3 ax = v3(in.m[0], in.m[1], in.m[2]), ay = v3(in.m[4], in.m[5], in.m[6]), az = v3(in.m[8], in.m[9], in.m[10]);
+    const V3 e10 = p[1] - p[0], e32 = p[3] - p[2], e20 = p[2] - p[0], e31 = p[3] - p[1];
+    const V3 du = e10 + (e32 - e10) * v, dv = e20 + (e31 - e20) * u;
+    const V3 wu = v3(dot(ax, du), dot(ay, du), dot(az, du)), wv = v3(dot(ax, dv), dot(ay, dv), dot(az, dv));
+    const V3 c = cross(wu, wv);
+    const float squared = dot(c, c);
+    if (!(squared >= kFltMin) || !isfinite(squared))
+        return false;
+    point.inverse_area_pdf = sqrtf(squared);
+    point.geometric_normal = c / point.inverse_area_pdf;
+    if (in.reverse)
+        point.geometric_normal = -point.geometric_normal;
+    point.shading_normal = point.geometric_normal;
+    if (in.normal_begin != kNone) {
+        V3 n[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if (in.normal_begin >= s.normal_count || idx[i] >= s.normal_count - in.normal_begin)
+                return false;
+            n[i] = load3(s.normals + 3 * size_t(in.normal_begin + idx[i]));
+        }
+        const V3 a = n[0] + (n[2] - n[0]) * v, b = n[1] + (n[3] - n[1]) * v;
+        const V3 interp = a + (b - a) * u;
+        if (!finite3(interp))
+            return false;
+        const float scale = max3(vabs(interp));
+        if (scale > 0) {
+            const V3 sc = interp / scale;
+            point.shading_normal = normalize3(sc);
+            if (dot(point.geometric_normal, sc) < 0)
+                point.geometric_normal = -point.geometric_normal;
+        }
+    }
+    Pair local_p[3];
+    const V3 magnitude = ((vabs(p[0]) + vabs(p[1])) + vabs(p[2])) + vabs(p[3]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const Pair lo = pr(comp(p[0], a)) + (pr(comp(p[2], a)) - pr(comp(p[0], a))) * pr(v);
+        const Pair hi = pr(comp(p[1], a)) + (pr(comp(p[3], a)) - pr(comp(p[1], a))) * pr(v);
+        local_p[a] = lo + (hi - lo) * pr(u);
+    }
+    const bool identity = in.m[3] == 0 && in.m[7] == 0 && in.m[11] == 0 && in.m[0] == 1 && in.m[1] == 0 &&
+                          in.m[2] == 0 && in.m[4] == 0 && in.m[5] == 1 && in.m[6] == 0 && in.m[8] == 0 &&
+                          in.m[9] == 0 && in.m[10] == 1;
+    float pos[3], err[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        Pair world = pr(in.m[4 * a + 3]);
+        float bound = fabsf(in.m[4 * a + 3]);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            world = world + local_p[j] * pr(in.m[4 * a + j]);
+            bound += comp(magnitude, j) * fabsf(in.m[4 * a + j]);
+        }
+        pos[a] = world.hi;
+        const float traversal = identity ? 0.0f : 0x1p-20f * bound;
+        err[a] = ((fabsf(world.lo) + 0x1p-40f * bound) + traversal) + 128.0f * kFltMin;
+    }
+    point.position = v3(pos[0], pos[1], pos[2]);
+    point.error = v3(err[0], err[1], err[2]);
+    point.world_extent = 0;
+#pragma unroll
+    for (int i = 1; i < 4; ++i) {
+        const V3 e = p[i] - p[0];
+        const V3 w = vabs(v3(dot(ax, e), dot(ay, e), dot(az, e)));
+        point.world_extent = fmaxf(point.world_extent, fmaxf(w.x, fmaxf(w.y, w.z)));
+    }
+    return finite3(point.position) && finite3(point.error) && finite3(point.geometric_normal) &&
+           finite3(point.shading_normal);
+}
+// shaders/analytic.h:81-85 (analytic_stable_length)
+RP_DEV float stable_length(V3 v) {
+    const float scale = fmaxf(fabsf(v.x), fmaxf(fabsf(v.y), fabsf(v.z)));
+    return scale > 0 ? scale * length3(v / scale) : 0;
+}
+// shaders/render.metal:1080-1118 (analytic_surface_point): the shape's point moved to world
+// space, its normal by the cofactor matrix, the area density scaled by the transform.
+__device__ __noinline__ bool analytic_surface_point(const DeviceScene &s, u32 instance, u32 local, float u, float v,
+                                                    SurfacePoint &point) {
+    const DInstance &in = s.instances[instance];
+    point.curved = true;
+    if (local >= in.analytic_count)
+        return false;
+    const DAnalytic rec = s.analytics[in.analytic_begin + local];
+    const AnalyticSurface ls = evaluate_analytic(rec, u, v);
+    if (!ls.valid)
+        return false;
+    const V3 a = v3(in.m[0], in.m[1], in.m[2]), b = v3(in.m[4], in.m[5], in.m[6]), c = v3(in.m[8], in.m[9], in.m[10]);
+    const V3 cofactor = v3(dot(cross(b, c), ls.normal), dot(cross(c, a), ls.normal), dot(cross(a, b), ls.normal));
+    const float jacobian = stable_length(cofactor);
+    if (!(jacobian > 0) || !isfinite(jacobian))
+        return false;
+    point.geometric_normal = cofactor / jacobian;
+    if (in.reverse)
+        point.geometric_normal = -point.geometric_normal;
+    point.shading_normal = point.geometric_normal;
+    const V3 shift = v3(in.m[3], in.m[7], in.m[11]);
+    point.position = v3(dot(a, ls.position), dot(b, ls.position), dot(c, ls.position)) + shift;
+    point.error = v3(dot(vabs(a), ls.error), dot(vabs(b), ls.error), dot(vabs(c), ls.error)) +
+                  gamma_bound(5) * (vabs(point.position) + vabs(shift));
+    point.inverse_area_pdf = analytic_area(rec) * jacobian;
+    point.world_extent = 2 * rec.radius * fmaxf(length3(a), fmaxf(length3(b), length3(c)));
+    return finite3(point.position) && finite3(point.error) && isfinite(point.inverse_area_pdf) &&
+           point.inverse_area_pdf >= kFltMin;
+}
+// surface_point (shaders/render.metal:1120-1132) of flattened primitive `prim` of `instance`
+// (its `local` primitive of that kind) at the hit's coordinates.
+RP_DEV bool hit_surface_point(const DeviceScene &s, u32 prim, u32 instance, u32 local, float b1, float b2,
+                              SurfacePoint &point) {
+    if (prim < s.tri_prims)
+        return triangle_surface_point(s, instance, local, b1, b2, true, point);
+    if (prim - s.tri_prims < s.patch_prims)
+        return patch_surface_point(s, instance, local, b1, b2, point);
+    return analytic_surface_point(s, instance, local, b1, b2, point);
+}
+// The ray's point at t and the rounding that bounds it (shaders/render.metal:1913-1929): in
+// plain float at triangles, in float pairs at patch and analytic points.
+RP_DEV void ray_point(V3 o, V3 d, float t, bool curved, V3 &position, V3 &error) {
+    position = fma3(v3(t, t, t), d, o);
+    error = gamma_bound(2.0f) * (vabs(t * d) + vabs(o));
+    if (curved) {
+        float p[3], e[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const Pair value = pr(t) * pr(comp(d, a)) + pr(comp(o, a));
+            p[a] = value.hi;
+            e[a] = (fabsf(value.lo) + 0x1p-40f * (fabsf(t * comp(d, a)) + fabsf(comp(o, a)))) + 128.0f * kFltMin;
+        }
+        position = v3(p[0], p[1], p[2]);
+        error = v3(e[0], e[1], e[2]);
+    }
+}
+// The world ray in the object space of an instance (world-to-object 3x4 `w`): the same t.
+RP_DEV void object_ray(const float *w, V3 o, V3 d, V3 &oo, V3 &od) {
+    const V3 r0 = v3(__ldg(w), __ldg(w + 1), __ldg(w + 2)), r1 = v3(__ldg(w + 4), __ldg(w + 5), __ldg(w + 6)),
+             r2 = v3(__ldg(w + 8), __ldg(w + 9), __ldg(w + 10));
+    oo = v3(dot(r0, o), dot(r1, o), dot(r2, o)) + v3(__ldg(w + 3), __ldg(w + 7), __ldg(w + 11));
+    od = v3(dot(r0, d), dot(r1, d), dot(r2, d));
+}
+// The hit of the world ray o + t d, t in [0, tmax], on procedural primitive `prim`.
+__device__ __noinline__ ShapeHit procedural_hit(const DeviceScene &s, u32 prim, V3 o, V3 d, float tmax) {
+    const u32 inst = __ldg(s.tri_instance + prim), local = __ldg(s.tri_local + prim);
+    const DInstance &in = s.instances[inst];
+    V3 oo, od;
+    object_ray(s.inverse + 12 * size_t(inst), o, d, oo, od);
+    if (prim - s.tri_prims < s.patch_prims) {
+        const u32 *pt = s.patches + 4 * size_t(in.patch_begin + local);
+        V3 p[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            p[i] = load3(s.positions + 3 * size_t(in.vertex_begin + __ldg(pt + i)));
+        return intersect_bilinear(p[0], p[1], p[2], p[3], oo, od, 0.0f, tmax);
+    }
+    return intersect_analytic(s.analytics[in.analytic_begin + local], oo, od, 0.0f, tmax);
 }
 
 // PBRT's alpha hash (MurmurHash64A over the binary32 words of origin, direction and t;
@@ -712,14 +894,25 @@ struct Hit {
 // most that many levels, and kStackDepth otherwise (deeper trees report an invalid hit).
 constexpr int kStackDepth = 40, kShortStack = 16;
 
-// Closest-hit triangle test of wide leaf `index`: keeps the minimum (t, primitive id).
-template <bool Count>
+// Closest-hit triangle test of wide leaf `index`: keeps the minimum (t, primitive id).  Proc:
+// the scene has procedural primitives (their leaves take the object-space tests).
+template <bool Count, bool Proc>
 RP_DEV void closest_leaf(const DeviceScene &s, const WalkRay &r, float tmax, Hit &h, u32 index, u32 &tris_tested) {
     const float4 a = __ldg(s.wtri + 3 * index), b = __ldg(s.wtri + 3 * index + 1), c = __ldg(s.wtri + 3 * index + 2);
     const u32 prim = __float_as_uint(a.w);
     float t, b1, b2;
     if (Count)
         ++tris_tested;
+    if (Proc && prim >= s.tri_prims) {
+        const ShapeHit ph = procedural_hit(s, prim, r.o, r.d, tmax);
+        if (ph.hit && (ph.t < h.t || (ph.t == h.t && prim < h.prim))) {
+            h.t = ph.t;
+            h.b1 = ph.u;
+            h.b2 = ph.v;
+            h.prim = prim;
+        }
+        return;
+    }
     if (intersect_triangle(r, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tmax, t, b1, b2) &&
         (t < h.t || (t == h.t && prim < h.prim))) {
         h.t = t;
@@ -729,12 +922,15 @@ RP_DEV void closest_leaf(const DeviceScene &s, const WalkRay &r, float tmax, Hit
     }
 }
 // Any-hit triangle test of wide leaf `index` in (0, tmax).
-template <bool Count>
+template <bool Count, bool Proc>
 RP_DEV bool any_leaf(const DeviceScene &s, const WalkRay &r, float tmax, u32 index, u32 &tris_tested) {
     const float4 a = __ldg(s.wtri + 3 * index), b = __ldg(s.wtri + 3 * index + 1), c = __ldg(s.wtri + 3 * index + 2);
     float t, b1, b2;
     if (Count)
         ++tris_tested;
+    const u32 prim = __float_as_uint(a.w);
+    if (Proc && prim >= s.tri_prims)
+        return procedural_hit(s, prim, r.o, r.d, tmax).hit;
     return intersect_triangle(r, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tmax, t, b1, b2);
 }
 
@@ -835,7 +1031,7 @@ RP_DEV void wide_children(const WNode &n, V3 o, WideRay &w, float tmax, u32 orde
 // node group: the parent's child_base and internal mask, and the hit children not yet
 // visited.  A walk visits each wide node at most once; a stack deeper than Stack reports a
 // failed query.
-template <bool Count, int Stack = kStackDepth>
+template <bool Count, int Stack = kStackDepth, bool Proc = false>
 RP_DEV bool walk_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, uint2 *stack, int stride,
                          u32 &nodes_visited, u32 &tris_tested) {
     h.t = tmax;
@@ -845,7 +1041,7 @@ RP_DEV bool walk_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, u
         return true;
     const WalkRay r = walk_ray(o, d);
     if (s.prim_count == 1) {
-        closest_leaf<Count>(s, r, tmax, h, 0, tris_tested);
+        closest_leaf<Count, Proc>(s, r, tmax, h, 0, tris_tested);
         return true;
     }
     const u32 order = (d.x < 0 ? 1u : 0u) | (d.y < 0 ? 2u : 0u) | (d.z < 0 ? 4u : 0u);
@@ -868,7 +1064,7 @@ RP_DEV bool walk_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, u
         while (leaves) {
             const u32 k = __ffs(leaves) - 1;
             leaves &= leaves - 1;
-            closest_leaf<Count>(s, r, tmax, h, n.links.y + __popc(lmask & ((1u << k) - 1)), tris_tested);
+            closest_leaf<Count, Proc>(s, r, tmax, h, n.links.y + __popc(lmask & ((1u << k) - 1)), tris_tested);
         }
         const u32 imask = __float_as_uint(n.origin.w) >> 24;
         u32 base = n.links.x, group_mask = imask;
@@ -897,11 +1093,11 @@ RP_DEV bool walk_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, u
 template <bool Count>
 RP_DEV bool trace_closest(const DeviceScene &s, V3 o, V3 d, float tmax, Hit &h, uint2 *stack, int stride,
                           u32 &nodes_visited, u32 &tris_tested) {
-    return walk_closest<Count>(s, o, d, tmax, h, stack, stride, nodes_visited, tris_tested);
+    return walk_closest<Count, kStackDepth, true>(s, o, d, tmax, h, stack, stride, nodes_visited, tris_tested);
 }
 
 // Any hit in (0, tmax): the shadow-ray occlusion query, the same walk stopped at the first hit.
-template <bool Count, int Stack = kStackDepth>
+template <bool Count, int Stack = kStackDepth, bool Proc = false>
 RP_DEV bool walk_any(const DeviceScene &s, V3 o, V3 d, float tmax, bool &occluded, uint2 *stack, int stride,
                      u32 &nodes_visited, u32 &tris_tested) {
     occluded = false;
@@ -909,7 +1105,7 @@ RP_DEV bool walk_any(const DeviceScene &s, V3 o, V3 d, float tmax, bool &occlude
         return true;
     const WalkRay r = walk_ray(o, d);
     if (s.prim_count == 1) {
-        occluded = any_leaf<Count>(s, r, tmax, 0, tris_tested);
+        occluded = any_leaf<Count, Proc>(s, r, tmax, 0, tris_tested);
         return true;
     }
     const u32 order = (d.x < 0 ? 1u : 0u) | (d.y < 0 ? 2u : 0u) | (d.z < 0 ? 4u : 0u);
@@ -932,7 +1128,7 @@ RP_DEV bool walk_any(const DeviceScene &s, V3 o, V3 d, float tmax, bool &occlude
         while (leaves) {
             const u32 k = __ffs(leaves) - 1;
             leaves &= leaves - 1;
-            if (any_leaf<Count>(s, r, tmax, n.links.y + __popc(lmask & ((1u << k) - 1)), tris_tested)) {
+            if (any_leaf<Count, Proc>(s, r, tmax, n.links.y + __popc(lmask & ((1u << k) - 1)), tris_tested)) {
                 occluded = true;
                 return true;
             }
@@ -964,7 +1160,7 @@ RP_DEV bool walk_any(const DeviceScene &s, V3 o, V3 d, float tmax, bool &occlude
 template <bool Count>
 RP_DEV bool trace_any(const DeviceScene &s, V3 o, V3 d, float tmax, bool &occluded, uint2 *stack, int stride,
                       u32 &nodes_visited, u32 &tris_tested) {
-    return walk_any<Count>(s, o, d, tmax, occluded, stack, stride, nodes_visited, tris_tested);
+    return walk_any<Count, kStackDepth, true>(s, o, d, tmax, occluded, stack, stride, nodes_visited, tris_tested);
 }
 
 } // namespace rp

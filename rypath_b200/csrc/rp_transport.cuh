@@ -684,8 +684,8 @@ RP_DEV bool spawn_boundary(V3 o, V3 d, float t, const SurfacePoint &pt, V3 direc
     const float facing = dot(n, direction);
     if (!(facing > gamma_bound(5) * dot(vabs(n), vabs(direction))))
         return false;
-    const V3 position = fma3(v3(t, t, t), d, o);
-    const V3 ray_error = gamma_bound(2) * (vabs(t * d) + vabs(o));
+    V3 position, ray_error;
+    ray_point(o, d, t, pt.curved, position, ray_error);
     const V3 error = (pt.error + vabs(pt.position - position)) + ray_error;
     const float norm_lower = dot(n, n) * (1 - gamma_bound(4));
     const float height = dot(vabs(n), error) * (1 + gamma_bound(8)) / norm_lower;

@@ -165,10 +165,10 @@ RP_DEV V3 cosine_hemisphere(V3 n, float u, float v) {
     const V3 b = cross(n, t);
     return normalize3((r * cosf(phi)) * t + (r * sinf(phi)) * b + sqrtf(1.0f - u) * n);
 }
-// :1912-1929 (triangles): conservative offset of a hit along n, rounded outward
+// :1912-1929: conservative offset of a hit along n, rounded outward
 RP_DEV V3 spawn_origin(V3 o, V3 d, float t, const SurfacePoint &pt, V3 n) {
-    const V3 ray_position = fma3(v3(t, t, t), d, o);
-    const V3 ray_error = gamma_bound(2.0f) * (vabs(t * d) + vabs(o));
+    V3 ray_position, ray_error;
+    ray_point(o, d, t, pt.curved, ray_position, ray_error);
     const V3 error = (pt.error + vabs(pt.position - ray_position)) + ray_error;
     return round_out(pt.position + dot(vabs(n), error) * n, n);
 }
@@ -549,7 +549,7 @@ RP_DEV int connection_step(const DeviceScene &s, const ScalarParams &q, ScalarPa
                 }
                 SurfacePoint pt;
                 V3 next;
-                if (!triangle_surface_point(s, inst, s.tri_local[h.prim], h.b1, h.b2, true, pt) ||
+                if (!hit_surface_point(s, h.prim, inst, s.tri_local[h.prim], h.b1, h.b2, pt) ||
                     !spawn_boundary(c.o, c.d, h.t, pt, c.d, next)) {
                     path.status = S_ARITHMETIC;
                     return kEventFinished;
@@ -792,7 +792,7 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
             path.status = S_BOUNDARY;
             return kEventFinished;
         }
-        if (!triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point)) {
+        if (!hit_surface_point(s, hit.prim, inst, local, hit.b1, hit.b2, point)) {
             path.status = S_ARITHMETIC;
             return kEventFinished;
         }
@@ -808,7 +808,7 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
     const bool emissive = instance.emission != kNone;
     if (emissive) {
         // area emission with MIS against the light sampler (:473-520)
-        if (!triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point)) {
+        if (!hit_surface_point(s, hit.prim, inst, local, hit.b1, hit.b2, point)) {
             path.status = S_ARITHMETIC;
             return kEventFinished;
         }
@@ -838,7 +838,7 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
     bool point_ready = emissive;
     u32 material_index = instance.material;
     if (material.scattering == kMixScattering) {
-        if (!emissive && !triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point)) {
+        if (!emissive && !hit_surface_point(s, hit.prim, inst, local, hit.b1, hit.b2, point)) {
             path.status = S_ARITHMETIC;
             return kEventFinished;
         }
@@ -887,7 +887,7 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
         path.status = S_EMERGENCY;
         return kEventFinished;
     }
-    if (!point_ready && !triangle_surface_point(s, inst, local, hit.b1, hit.b2, true, point)) {
+    if (!point_ready && !hit_surface_point(s, hit.prim, inst, local, hit.b1, hit.b2, point)) {
         path.status = S_ARITHMETIC;
         return kEventFinished;
     }
@@ -1172,7 +1172,8 @@ RP_DEV bool hits_interface(const DeviceScene &s, const Hit &hit) {
     return material < s.material_count && s.materials[material].scattering == kInterfaceScattering;
 }
 
-template <bool Count, int Stack = kStackDepth>
+// Proc: the scene has procedural primitives.
+template <bool Count, int Stack = kStackDepth, bool Proc = false>
 __global__ void __launch_bounds__(kTraceBlock, Stack <= kShortStack ? 1024 / kTraceBlock : 1)
     k_scalar_walk(const __grid_constant__ DeviceScene s, const __grid_constant__ WaveParams p, ScalarSlots w,
                   int parity, unsigned long long *stats) {
@@ -1206,7 +1207,7 @@ __global__ void __launch_bounds__(kTraceBlock, Stack <= kShortStack ? 1024 / kTr
                     Hit hit;
                     u32 nodes = 0, tris = 0;
                     const bool ok =
-                        walk_closest<Count, Stack>(s, ro, rd, tmax, hit, stack + threadIdx.x, kTraceBlock, nodes, tris);
+                        walk_closest<Count, Stack, Proc>(s, ro, rd, tmax, hit, stack + threadIdx.x, kTraceBlock, nodes, tris);
                     w.hit[i] = hit;
                     w.mode[i] = mode | (ok ? kWalkOk : 0u);
                     scatter = ok && mode == kEventPath && predicts_medium_scatter(s, p, path, hit);

@@ -53,6 +53,8 @@ def lib():
         "rp_cuda_probe_raygen": (st, [vp, C.POINTER(abi.Request), vp, vp, sz, cp, sz]),
         "rp_cuda_probe_bsdf": (st, [vp, u32, vp, cp, sz]),
         "rp_cuda_probe_hero": (st, [vp, u32, vp, cp, sz]),
+        "rp_cuda_probe_bilinear": (st, [vp, u32, vp, cp, sz]),
+        "rp_cuda_probe_analytic": (st, [vp, u32, vp, cp, sz]),
         "rp_cuda_probe_texture_footprint": (st, [vp, u32, vp, cp, sz]),
         "rp_cuda_texture_camera_differentials": (st, [C.POINTER(abi.Camera), u32, u32, vp, vp, cp, sz]),
         "rp_cuda_probe_image_lookup": (st, [vp, u32, vp, u32, vp, cp, sz]),

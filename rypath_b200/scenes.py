@@ -95,6 +95,10 @@ class Scene:
     # pose, film_scale = tan(fov / 2), materials' 8-knot reflectance, the unit sky)
     model: int = abi.MODEL_PBRT
     film_scale: float = 1.0
+    # bilinear patches ((N, 4) vertex indices p00 p10 p01 p11, instance-local like triangles)
+    # and analytic shapes (abi.Analytic records), referenced by the instances' ranges
+    patches: np.ndarray | None = None
+    analytics: list = field(default_factory=list)
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -179,6 +183,13 @@ class Scene:
         keep.append(tables)
         d.sobol_tables = C.cast(tables, C.c_void_p)
         d.model, d.film_scale = self.model, self.film_scale
+        if self.patches is not None and len(self.patches):
+            pt = np.ascontiguousarray(self.patches, dtype=np.uint32).reshape(-1, 4)
+            d.patch_count, d.patches = pt.shape[0], arr(pt, C.c_uint32)
+        if self.analytics:
+            an = (abi.Analytic * len(self.analytics))(*self.analytics)
+            keep.append(an)
+            d.analytic_count, d.analytics = len(self.analytics), C.cast(an, C.POINTER(abi.Analytic))
         if self.images is not None:
             im = self.images.to_c(keep)
             keep.append(im)
@@ -195,6 +206,8 @@ def identity_instance(vertex_begin, triangle_begin, triangle_count, material, em
     inst.reverse_orientation = 0
     inst.normal_begin = abi.RP_NONE
     inst.inside_medium = inst.outside_medium = abi.RP_NONE
+    inst.patch_begin = inst.analytic_begin = abi.RP_NONE
+    inst.patch_count = inst.analytic_count = 0
     return inst
 
 
@@ -448,6 +461,97 @@ def cornell_microfacets(width=32, height=32, spp=4, max_depth=8, transport=abi.T
     scene.instances[5].material = base
     scene.instances[6].material = base + 1
     scene.instances[4].material = base + 2
+    scene.transport = transport
+    return scene
+
+
+def _procedural_instance(material, vertex_begin=0, patches=(0, 0), analytics=(0, 0), matrix=None):
+    inst = identity_instance(vertex_begin, 0, 0, material)
+    inst.patch_begin, inst.patch_count = patches
+    inst.analytic_begin, inst.analytic_count = analytics
+    if matrix is not None:
+        inst.matrix[:] = [float(v) for v in np.asarray(matrix, np.float32).reshape(-1)]
+    return inst
+
+
+def _rotation_y(degrees, translation=(0, 0, 0), scale=(1, 1, 1)):
+    c, s = math.cos(math.radians(degrees)), math.sin(math.radians(degrees))
+    r = np.array([[c, 0, s], [0, 1, 0], [-s, 0, c]]) @ np.diag(scale)
+    return np.concatenate([r, np.asarray(translation, np.float64)[:, None]], axis=1)
+
+
+def add_patches(scene: Scene, corners, material, matrix=None) -> None:
+    """Append an instance of bilinear patches; `corners` is (N, 4, 3), each p00 p10 p01 p11."""
+    corners = np.asarray(corners, np.float32).reshape(-1, 4, 3)
+    begin = 0 if scene.patches is None else scene.patches.shape[0]
+    vb = scene.positions.shape[0]
+    idx = np.arange(4 * corners.shape[0], dtype=np.uint32).reshape(-1, 4)
+    scene.positions = np.concatenate([scene.positions, corners.reshape(-1, 3)])
+    scene.patches = idx if scene.patches is None else np.concatenate([scene.patches, idx])
+    scene.instances.append(_procedural_instance(material, vb, patches=(begin, corners.shape[0]), matrix=matrix))
+
+
+def add_analytics(scene: Scene, records, material, matrix=None) -> None:
+    """Append an instance of analytic shapes (abi.Analytic records)."""
+    begin = len(scene.analytics)
+    scene.analytics = list(scene.analytics) + list(records)
+    scene.instances.append(_procedural_instance(material, analytics=(begin, len(records)), matrix=matrix))
+
+
+def analytic(subtype, radius, z_min=-1.0, z_max=1.0, phi_max=2 * math.pi, inner_radius=0.0, height=0.0):
+    a = abi.Analytic()
+    a.kind, a.subtype = abi.PRIMITIVE_ANALYTIC, subtype
+    a.radius, a.z_min, a.z_max, a.phi_max, a.inner_radius, a.height = radius, z_min, z_max, phi_max, inner_radius, height
+    return a
+
+
+def cornell_shapes(width=32, height=32, spp=4, max_depth=8, transport=abi.TRANSPORT_HERO) -> Scene:
+    """The Cornell-style box with procedural primitives: the left wall a planar bilinear patch,
+    a warped patch 'sail' in front of the back wall (rotated instance), the tall box replaced by
+    a capped cylinder (a cylinder and a holed disk, axis along +y by the instance rotation), and
+    a rough-glass ellipsoid (a sphere scaled by the instance) on the short box."""
+    scene = cornell_box(width, height, spp, max_depth)
+    scene.name = "cornell_shapes"
+    # left wall: the patch of its quad's corners, replacing its two triangles
+    scene.instances[3].triangle_count = 0
+    add_patches(scene, [[(-1, 0, -1), (-1, 2, -1), (-1, 0, 1), (-1, 2, 1)]], 1)
+    add_patches(scene, [[(-0.6, 0.9, -0.1), (0.2, 1.1, -0.05), (-0.7, 1.7, -0.15), (0.3, 1.6, 0.1)]], 2,
+                matrix=_rotation_y(12.0, (0.1, 0.0, -0.75)))
+    scene.instances[6].triangle_count = 0  # the tall box
+    axis_y = np.array([[1, 0, 0, -0.45], [0, 0, 1, 0.0], [0, -1, 0, -0.4]])
+    add_analytics(scene, [analytic(abi.ANALYTIC_CYLINDER, 0.28, 0.0, 1.1),
+                          analytic(abi.ANALYTIC_DISK, 0.28, 0, 0, 2 * math.pi, 0.08, 1.1)], 0, matrix=axis_y)
+    scene.materials.append(dielectric_material(scene, 1.5, 0.05))
+    add_analytics(scene, [analytic(abi.ANALYTIC_SPHERE, 0.2, -0.2, 0.2)], len(scene.materials) - 1,
+                  matrix=_rotation_y(30.0, (0.4, 0.78, 0.2), (1.0, 0.8, 1.2)))
+    scene.transport = transport
+    return scene
+
+
+def shape_furnace(kind, width=16, height=16, spp=4, rho=0.5, transport=abi.TRANSPORT_HERO) -> Scene:
+    """One convex diffuse object of constant reflectance rho under a constant environment of
+    radiance 1 at every wavelength (kind: 'sphere', 'disk', 'cylinder' -- open, seen from the
+    side -- or 'patch', a flat one): no ray leaving it meets it again, so every camera ray that
+    hits it returns rho on average and every other 1."""
+    scene = Scene(f"furnace_{kind}", width, height, spp, np.zeros((0, 3), np.float32), np.zeros((0, 3), np.uint32),
+                  [], [], max_depth=8)
+    m = abi.Material()
+    m.scattering, m.kind, m.scalar_value = abi.DIFFUSE, abi.REFLECTANCE_CONSTANT, rho
+    scene.materials = [m]
+    tilt = _rotation_y(25.0, (0, 0, 0))
+    if kind == "sphere":
+        add_analytics(scene, [analytic(abi.ANALYTIC_SPHERE, 0.6, -0.6, 0.6)], 0, matrix=tilt)
+    elif kind == "disk":
+        add_analytics(scene, [analytic(abi.ANALYTIC_DISK, 0.7, 0, 0, 2 * math.pi, 0.2, 0.1)], 0,
+                      matrix=np.array([[1, 0, 0, 0], [0, 0.8, 0.6, 0], [0, -0.6, 0.8, 0]]))
+    elif kind == "cylinder":
+        add_analytics(scene, [analytic(abi.ANALYTIC_CYLINDER, 0.4, -0.6, 0.6)], 0,
+                      matrix=np.array([[1, 0, 0, 0], [0, 0, 1, 0], [0, -1, 0, 0]]))
+    else:
+        add_patches(scene, [[(-0.7, -0.6, 0.2), (0.7, -0.5, -0.1), (-0.6, 0.7, -0.2), (0.8, 0.8, -0.5)]], 0,
+                    matrix=tilt)  # a parallelogram: flat
+    scene.environment = np.ones(471, np.float32)
+    scene.camera = pinhole_camera((0, 0, 3.0), (0, 0, 0), (0, 1, 0), 40.0, width, height)
     scene.transport = transport
     return scene
 

@@ -46,7 +46,8 @@ def test_raygen_words_and_rays_bit_exact(sampler, mode, lens):
     lanes = words.shape[0]
     cw = np.zeros((lanes, 11), np.uint32)
     cr = np.zeros((lanes, 6), np.float32)
-    assert oracle().or_probe_raygen(OracleScene(scene).handle, C.byref(q), cw.ctypes.data, cr.ctypes.data, lanes) == 0
+    orc = OracleScene(scene)  # held: the oracle scene must outlive the call
+    assert oracle().or_probe_raygen(orc.handle, C.byref(q), cw.ctypes.data, cr.ctypes.data, lanes) == 0
     np.testing.assert_array_equal(words, cw)
     if lens:
         np.testing.assert_allclose(rays, cr, rtol=0, atol=2e-6)

@@ -142,4 +142,4 @@ def test_the_allocation_free_entry_point_refuses_resolve_scenes():
     req = renderer.RenderRequest(8, 8, sample_count=1).to_c()
     st = native.lib().rp_cuda_sample_device_static(rs.handle, C.byref(req), C.c_void_p(out.data_ptr()), 64, None,
                                                    diag, 256)
-    assert st == abi.RP_INVALID_ARGUMENT and b"pass-through or mix" in diag.value
+    assert st == abi.RP_INVALID_ARGUMENT and b"pass-through, mix" in diag.value
