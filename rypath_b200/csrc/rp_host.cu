@@ -954,6 +954,7 @@ struct rp_scene {
     u32 wide_levels = 0;     // levels of the compressed 8-wide traversal tree
     bool resolve = false;    // hero scene with pass-through or mix-root instances
     bool dielectrics = false; // a dielectric material: the QMC samplers' depth limit
+    bool scalar_full = false; // conductors, dielectrics or procedural primitives: the full scalar step kernel
     u32 tex_width = 0, tex_height = 0; // film size the texture camera differentials were found for
     double demo_film_scale = 0;        // demo film: 470 / integral of the CIE y table
     float4 *world = nullptr; // world-space triangle vertices in original order
@@ -1336,6 +1337,16 @@ std::string validate_request(const rp_scene *s, const rp_request &r) {
     return {};
 }
 
+// The scalar step kernel: the plain one, or the full one for scenes with conductors,
+// dielectrics or procedural primitives.
+void launch_scalar_step(const rp_scene *s, unsigned grid, const WaveParams &p, const ScalarParams &q,
+                        const ScalarSlots &w, int parity) {
+    if (s->scalar_full)
+        k_scalar_step<true><<<grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q, w, parity);
+    else
+        k_scalar_step<false><<<grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q, w, parity);
+}
+
 // The closest-hit and shadow kernels with the traversal stack the built tree needs, resolving
 // pass-through and mix-root hits when the scene has them.
 template <bool Count, int Block, int Stack>
@@ -1563,7 +1574,10 @@ void run_scalar_wave(rp_scene *s, const WaveParams &p, u32 boundary_limit) {
     s->ensure_scalar(p.lanes);
     if (!s->step_blocks) {
         int per_sm = 0;
-        RP_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scalar_step, kTraceBlock, 0));
+        if (s->scalar_full)
+            RP_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scalar_step<true>, kTraceBlock, 0));
+        else
+            RP_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scalar_step<false>, kTraceBlock, 0));
         s->step_blocks = std::max(1, per_sm);
     }
     s->mark(3);
@@ -1587,7 +1601,7 @@ void run_scalar_wave(rp_scene *s, const WaveParams &p, u32 boundary_limit) {
     const bool short_stack = s->wide_levels <= u32(kShortStack);
     s->mark(2, 2);
     k_scalar_slots_init<<<grid_for(s->sm_count, slots, 256, 8), 256, 0, s->stream>>>(w.mode, slots);
-    k_scalar_step<<<step_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q, w, -1);
+    launch_scalar_step(s, step_grid, p, q, w, -1);
     const bool walks = s->ds.instance_count != 0; // geometry-free scenes take the sky step
     int parity = 0;
     RP_CHECK(cudaGetLastError());
@@ -1599,7 +1613,7 @@ void run_scalar_wave(rp_scene *s, const WaveParams &p, u32 boundary_limit) {
             throw Invalid{"scalar wave did not finish"};
         for (int k = 0; k < kScalarTripsPerCheck; ++k) {
             if (!walks) {
-                k_scalar_step<<<step_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q, w, -1);
+                launch_scalar_step(s, step_grid, p, q, w, -1);
                 s->launches += 1;
                 continue;
             }
@@ -1616,7 +1630,7 @@ void run_scalar_wave(rp_scene *s, const WaveParams &p, u32 boundary_limit) {
                 k_scalar_walk<false, kShortStack><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, w, parity, s->stats);
             else
                 k_scalar_walk<false, kStackDepth><<<walk_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, w, parity, s->stats);
-            k_scalar_step<<<step_grid, kTraceBlock, 0, s->stream>>>(s->ds, p, q, w, parity);
+            launch_scalar_step(s, step_grid, p, q, w, parity);
             s->launches += 2;
             parity ^= 1;
         }
@@ -2024,6 +2038,7 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
                 throw NotBuilt{"unsupported scattering family (diffuse, conductor, dielectric, mix and null "
                                "interfaces are built)"};
             s->dielectrics = s->dielectrics || f == RP_DIELECTRIC; // scene_has_dielectrics (src/render.cpp:927-932)
+            s->scalar_full = s->scalar_full || f == RP_CONDUCTOR || f == RP_DIELECTRIC;
         }
         for (u32 i = 0; i < d->instance_count; ++i) {
             const auto &in = d->instances[i];
@@ -2093,6 +2108,7 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
         // the hero walks test procedural leaves in the kernels that resolve hits
         if (!scalar && (patch_prims || analytic_prims))
             s->resolve = true;
+        s->scalar_full = s->scalar_full || patch_prims || analytic_prims;
         // world-to-object maps of the instances (procedural hits test the ray in object space)
         std::vector<float> inverse(size_t(12) * std::max<u32>(d->instance_count, 1), 0.0f);
         for (u32 i = 0; i < d->instance_count; ++i) {

@@ -369,22 +369,28 @@ RP_DEV bool hit_surface_point(const DeviceScene &s, u32 prim, u32 instance, u32 
         return patch_surface_point(s, instance, local, b1, b2, point);
     return analytic_surface_point(s, instance, local, b1, b2, point);
 }
+// The float-pair ray point at a patch or analytic point (out of line: triangle hits, the
+// common case, do not carry its code).
+__device__ __noinline__ void curved_ray_point(V3 o, V3 d, float t, V3 &position, V3 &error) {
+    float p[3], e[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const Pair value = pr(t) * pr(comp(d, a)) + pr(comp(o, a));
+        p[a] = value.hi;
+        e[a] = (fabsf(value.lo) + 0x1p-40f * (fabsf(t * comp(d, a)) + fabsf(comp(o, a)))) + 128.0f * kFltMin;
+    }
+    position = v3(p[0], p[1], p[2]);
+    error = v3(e[0], e[1], e[2]);
+}
 // The ray's point at t and the rounding that bounds it (shaders/render.metal:1913-1929): in
 // plain float at triangles, in float pairs at patch and analytic points.
 RP_DEV void ray_point(V3 o, V3 d, float t, bool curved, V3 &position, V3 &error) {
+    if (curved) {
+        curved_ray_point(o, d, t, position, error);
+        return;
+    }
     position = fma3(v3(t, t, t), d, o);
     error = gamma_bound(2.0f) * (vabs(t * d) + vabs(o));
-    if (curved) {
-        float p[3], e[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const Pair value = pr(t) * pr(comp(d, a)) + pr(comp(o, a));
-            p[a] = value.hi;
-            e[a] = (fabsf(value.lo) + 0x1p-40f * (fabsf(t * comp(d, a)) + fabsf(comp(o, a)))) + 128.0f * kFltMin;
-        }
-        position = v3(p[0], p[1], p[2]);
-        error = v3(e[0], e[1], e[2]);
-    }
 }
 // The world ray in the object space of an instance (world-to-object 3x4 `w`): the same t.
 RP_DEV void object_ray(const float *w, V3 o, V3 d, V3 &oo, V3 &od) {

@@ -606,7 +606,8 @@ struct ScalarBsdf {
     float eta, k;
     Ggx g;
 };
-RP_DEV bool prepare_scalar_bsdf(const DeviceScene &s, const DMaterial &m, float w, ScalarBsdf &b) {
+// Out of line: the step kernel's diffuse and medium events do not carry their registers.
+__device__ __noinline__ bool prepare_scalar_bsdf(const DeviceScene &s, const DMaterial &m, float w, ScalarBsdf &b) {
     b.kind = m.scattering;
     const float u = m.u_roughness, v = m.v_roughness;
     if (!isfinite(u) || !isfinite(v) || u < 0 || v < 0)
@@ -625,8 +626,13 @@ RP_DEV bool prepare_scalar_bsdf(const DeviceScene &s, const DMaterial &m, float 
     b.eta = eta;
     return prepare_roughness(u, v, m.remap != 0, m.scattering == 2 && eta == 1, b.g);
 }
-RP_DEV Eval scalar_bsdf_evaluate(const ScalarBsdf &b, V3 wo, V3 wi) {
+__device__ __noinline__ Eval scalar_bsdf_evaluate(const ScalarBsdf &b, V3 wo, V3 wi) {
     return b.kind == 2 ? dielectric_evaluate(b.eta, b.g, wo, wi) : conductor_evaluate(b.eta, b.k, b.g, wo, wi);
+}
+__device__ __noinline__ BSample scalar_bsdf_sample(const ScalarBsdf &b, V3 wo, float lobe, float ux, float uy) {
+    float sampled_eta;
+    return b.kind == 2 ? dielectric_sample(b.eta, b.g, wo, lobe, ux, uy, sampled_eta)
+                       : conductor_sample(b.eta, b.k, b.g, wo, ux, uy);
 }
 // scattering_direct (shaders/render.metal:2212-2219)
 RP_DEV float scattering_direct(float f_cos, float bsdf_pdf, float light_pdf, bool invisible) {
@@ -654,6 +660,17 @@ RP_DEV u32 dielectric_lobe_word(const DeviceScene &s, const WaveParams &p, u32 p
 // for diffuse, conductor and dielectric surfaces and null interfaces.  A light sample that needs a connection leaves it in
 // `c` (returning kEventConnect) after the continuation has been sampled: the two use disjoint
 // draws, and the connection's contribution and status are applied before the continuation's.
+// The surface point of a path hit: any primitive kind, or triangles alone in the plain kernel.
+template <bool Full>
+RP_DEV bool scalar_surface_point(const DeviceScene &s, u32 prim, u32 inst, u32 local, float b1, float b2,
+                                 SurfacePoint &point) {
+    if (Full)
+        return hit_surface_point(s, prim, inst, local, b1, b2, point);
+    return triangle_surface_point(s, inst, local, b1, b2, true, point);
+}
+// Full: the scene has conductor or dielectric surfaces or procedural primitives (their code is
+// compiled out of the plain step kernel).
+template <bool Full>
 RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarParams &q, ScalarPath &path, bool ok,
                        const Hit &hit, Connection &c) {
     if (!ok) {
@@ -792,7 +809,7 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
             path.status = S_BOUNDARY;
             return kEventFinished;
         }
-        if (!hit_surface_point(s, hit.prim, inst, local, hit.b1, hit.b2, point)) {
+        if (!scalar_surface_point<Full>(s, hit.prim, inst, local, hit.b1, hit.b2, point)) {
             path.status = S_ARITHMETIC;
             return kEventFinished;
         }
@@ -808,7 +825,7 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
     const bool emissive = instance.emission != kNone;
     if (emissive) {
         // area emission with MIS against the light sampler (:473-520)
-        if (!hit_surface_point(s, hit.prim, inst, local, hit.b1, hit.b2, point)) {
+        if (!scalar_surface_point<Full>(s, hit.prim, inst, local, hit.b1, hit.b2, point)) {
             path.status = S_ARITHMETIC;
             return kEventFinished;
         }
@@ -838,7 +855,7 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
     bool point_ready = emissive;
     u32 material_index = instance.material;
     if (material.scattering == kMixScattering) {
-        if (!emissive && !hit_surface_point(s, hit.prim, inst, local, hit.b1, hit.b2, point)) {
+        if (!emissive && !scalar_surface_point<Full>(s, hit.prim, inst, local, hit.b1, hit.b2, point)) {
             path.status = S_ARITHMETIC;
             return kEventFinished;
         }
@@ -851,8 +868,12 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
     }
     const DMaterial surface = s.materials[material_index];
     // conductors and dielectrics carry their spectrum in the BSDF: rho = 1 (:591-598)
-    const bool microfacet = surface.scattering != 0;
+    const bool microfacet = Full && surface.scattering != 0;
     float rho = 0;
+    if (!Full && surface.scattering != 0) {
+        path.status = S_HIT;
+        return kEventFinished;
+    }
     if (microfacet) {
         if (surface.scattering > 2) {
             path.status = S_HIT;
@@ -887,7 +908,7 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
         path.status = S_EMERGENCY;
         return kEventFinished;
     }
-    if (!point_ready && !hit_surface_point(s, hit.prim, inst, local, hit.b1, hit.b2, point)) {
+    if (!point_ready && !scalar_surface_point<Full>(s, hit.prim, inst, local, hit.b1, hit.b2, point)) {
         path.status = S_ARITHMETIC;
         return kEventFinished;
     }
@@ -1035,15 +1056,10 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
     bool continuation_delta = false;
     if (microfacet) {
         const float ux = sample_uniform(p, bsdf_words.x), uy = sample_uniform(p, bsdf_words.y);
-        BSample sampled;
-        if (bsdf.kind == 2) {
-            const float lobe =
-                sample_uniform(p, dielectric_lobe_word(s, p, path.pixel, path.slo, path.shi, path.index, bounce));
-            float sampled_eta;
-            sampled = dielectric_sample(bsdf.eta, bsdf.g, wo, lobe, ux, uy, sampled_eta);
-        } else {
-            sampled = conductor_sample(bsdf.eta, bsdf.k, bsdf.g, wo, ux, uy);
-        }
+        const float lobe = bsdf.kind == 2 ? sample_uniform(p, dielectric_lobe_word(s, p, path.pixel, path.slo, path.shi,
+                                                                                path.index, bounce))
+                                          : 0.0f; // the conductor draws no lobe
+        BSample sampled = scalar_bsdf_sample(bsdf, wo, lobe, ux, uy);
         if (sampled.valid && sampled.accepted && !unit_vector(to_world(frame, sampled.wi), wi))
             sampled.valid = false;
         if (!sampled.valid) {
@@ -1250,6 +1266,7 @@ __global__ void k_scalar_slots_init(u32 *mode, u32 count) {
 // events and the other path events; parity < 0: every slot (the wave's first fill, and geometry-free scenes, which
 // take no walk).  Four blocks of 128 per SM (128 registers, a few spilled) hide more of the
 // slot loads' latency than three at 154 registers: 133 against 143 ms on the fog box.
+template <bool Full>
 __global__ void __launch_bounds__(kTraceBlock, 4) k_scalar_step(const __grid_constant__ DeviceScene s,
                                                              const __grid_constant__ WaveParams p, ScalarParams q,
                                                              ScalarSlots w, int parity) {
@@ -1294,7 +1311,7 @@ __global__ void __launch_bounds__(kTraceBlock, 4) k_scalar_step(const __grid_con
                 } else {
                     const Hit hit = w.hit[i];
                     const bool ok = (m & kWalkOk) != 0;
-                    mode = mode == kEventPath ? shade_event(s, p, q, path, ok, hit, c)
+                    mode = mode == kEventPath ? shade_event<Full>(s, p, q, path, ok, hit, c)
                                               : connection_step(s, q, path, c, ok, hit);
                 }
                 if (mode == kEventFinished) {
