@@ -269,12 +269,30 @@ Incident light_sample_scalar(const Scene &s, float wavelength, F3 position, F3 n
         r.radiance = intensity / d2;
         r.pdf = chosen.pmf;
     } else if (id == s.environment_light) {
-        return r;
+        // shaders/scalar_lighting.h:102-113: the environment image's compensated table
+        if (s.images.env_image == RP_NONE)
+            return r;
+        float conditional = 0;
+        r.valid = env_image_sample(s.images, ux, uy, true, r.direction, conditional);
+        if (!r.valid)
+            return r;
+        r.pdf = chosen.pmf * conditional;
+        r.radiance = env_image_radiance(s.images, r.direction, wavelength);
     } else {
         r.valid = false;
     }
     r.valid = r.valid && std::isfinite(r.radiance) && r.radiance >= 0 && std::isfinite(r.pdf) && r.pdf >= 0;
     return r;
+}
+// shaders/scalar_lighting.h:14-23 (environment_pdf)
+float environment_pdf(const Scene &s, F3 position, F3 normal, F3 direction) {
+    if (s.images.env_image == RP_NONE || s.environment_light == RP_NONE)
+        return 0.0f;
+    return light_pmf(s, position, normal, s.environment_light) * env_image_pdf(s.images, direction, true);
+}
+// the sky's radiance along a direction: the environment image, else the lane's constant
+float sky(const Scene &s, float E, F3 direction, float wavelength) {
+    return s.images.env_image != RP_NONE ? env_image_radiance(s.images, direction, wavelength) : E;
 }
 bool delta_light(const Incident &l) { return l.kind == positional_light || l.kind == distant_light; }
 
@@ -354,6 +372,8 @@ Transmission connection_transmission(const Ctx &c, float wavelength, F3 o, F3 d,
 }
 // shaders/scalar_lighting.h:123-134 (connection)
 F3 connection_direction(const Incident &light, F3 origin) {
+    if (light.kind == environment_light)
+        return light.direction;
     if (light.kind == area_light) {
         const F3 delta = light.target.position - origin;
         return shadow_segment_direction(origin, delta, light.target, dot(light.target.geometric_normal, -delta));
@@ -468,7 +488,7 @@ bool sky_step(const Ctx &c, Lane &l) {
             return false;
         }
     }
-    l.radiance = l.E;
+    l.radiance = sky(s, l.E, l.d, l.wavelength);
     return true;
 }
 
@@ -528,7 +548,8 @@ bool scalar_event(const Ctx &c, Lane &l) {
                     if (light.pdf > 0 && light.radiance != 0) {
                         const Transmission tr = medium_connection(c, l.wavelength, position,
                                                                   connection_direction(light, position),
-                                                                  0x1.fffffep-1f, l.current_medium);
+                                                                  light.kind == environment_light ? INFINITY : 0x1.fffffep-1f,
+                                                                  l.current_medium);
                         if (tr.status != RP_SAMPLE_SUCCESS)
                             return fail(tr.status);
                         const float ph = phase(-direction, light.direction, m.g);
@@ -561,10 +582,10 @@ bool scalar_event(const Ctx &c, Lane &l) {
         }
     }
     if (miss) {
-        // shaders/scalar_transport.h:421-433; constant environments have no light density
+        // shaders/scalar_transport.h:421-433; MIS against the environment image's light samples
         if (s.model == RP_MODEL_PBRT && l.scatterings != 0u && !l.previous_delta)
-            l.escape_weight = power_weight(l.previous_bsdf_pdf, 0.0f);
-        l.radiance += l.throughput * l.escape_weight * l.E;
+            l.escape_weight = power_weight(l.previous_bsdf_pdf, environment_pdf(s, l.prev_p, l.prev_n, l.d));
+        l.radiance += l.throughput * l.escape_weight * sky(s, l.E, l.d, l.wavelength);
         return true;
     }
     const u32 bounce = l.scatterings;
@@ -763,7 +784,7 @@ bool scalar_event(const Ctx &c, Lane &l) {
                 if (!std::isfinite(factor) || !finite3(cd) || !(dot(cd, light.direction) > 0))
                     return fail(RP_SAMPLE_INVALID_ARITHMETIC);
                 const Transmission vis = connection_transmission(
-                    c, l.wavelength, origin, cd, 0x1.fffffep-1f,
+                    c, l.wavelength, origin, cd, light.kind == environment_light ? INFINITY : 0x1.fffffep-1f,
                     outgoing_medium(instance, l.current_medium, point.geometric_normal, light.direction));
                 if (vis.status != RP_SAMPLE_SUCCESS)
                     return fail(vis.status);

@@ -1944,8 +1944,10 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             throw Invalid{mix};
         if (const std::string images = validate_images(d); !images.empty())
             throw Invalid{images};
-        if (d->images && scalar && (d->images->environment_image != RP_NONE || d->images->texture_count))
-            throw NotBuilt{"the scalar transport does not read images"};
+        if (scalar)
+            for (u32 i = 0; i < d->material_count; ++i)
+                if (d->materials[i].kind == RP_REFLECTANCE_IMAGE)
+                    throw NotBuilt{"the scalar transport reads the environment image, not image reflectance"};
         if (d->model > RP_MODEL_DEMO)
             throw Invalid{"invalid scene model"};
         if (d->model == RP_MODEL_DEMO) {

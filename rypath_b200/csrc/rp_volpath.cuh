@@ -228,7 +228,8 @@ struct Incident {
     u32 kind;
     bool valid;
 };
-// :23-121 (area, point and spot lights; a constant environment offers no light sample)
+// :23-121 (area, point and spot lights, the environment image; a constant environment offers
+// no light sample)
 __device__ __noinline__ Incident scalar_light_sample(const DeviceScene &s, float wavelength, V3 position, V3 normal,
                                                      float selection, float ux, float uy) {
     Incident r;
@@ -279,12 +280,26 @@ __device__ __noinline__ Incident scalar_light_sample(const DeviceScene &s, float
         r.radiance = intensity / d2;
         r.pdf = chosen.pmf;
     } else if (id == s.environment_light) {
-        return r;
+        if (s.img.env_image == kNone)
+            return r;
+        float conditional = 0;
+        r.valid = sample_environment_image(s.img, ux, uy, true, r.direction, conditional);
+        if (!r.valid)
+            return r;
+        r.pdf = chosen.pmf * conditional;
+        r.radiance = environment_image_radiance(s.img, r.direction, wavelength);
     } else {
         r.valid = false;
     }
     r.valid = r.valid && isfinite(r.radiance) && r.radiance >= 0 && isfinite(r.pdf) && r.pdf >= 0;
     return r;
+}
+// environment_pdf (shaders/scalar_lighting.h:14-23): the light sampler's density of an escaped
+// direction, zero for a constant environment (continuation alone reaches it)
+RP_DEV float scalar_environment_pdf(const DeviceScene &s, V3 position, V3 normal, V3 direction) {
+    if (s.img.env_image == kNone || s.environment_light == kNone)
+        return 0.0f;
+    return light_pmf(s, position, normal, s.environment_light) * environment_image_pdf(s.img, direction, true);
 }
 RP_DEV bool incident_delta(const Incident &l) { return l.kind == kIncidentPositional || l.kind == kIncidentDistant; }
 
@@ -464,7 +479,8 @@ __device__ __noinline__ bool scalar_sky_step(const DeviceScene &s, const WavePar
             return false;
         }
     }
-    path.radiance = environment_radiance(s, path.wavelength);
+    path.radiance = s.img.env_image != kNone ? environment_image_radiance(s.img, path.d, path.wavelength)
+                                             : environment_radiance(s, path.wavelength);
     return true;
 }
 
@@ -734,14 +750,16 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
                 bool connect = false;
                 if (light.pdf > 0 && light.radiance != 0) {
                     V3 cd;
+                    // connection (shaders/scalar_lighting.h:121-133): the environment's is unbounded
+                    const bool unbounded = light.kind == kIncidentEnvironment;
                     if (light.kind == kIncidentArea) {
                         const V3 delta = light.target.position - position;
                         cd = shadow_segment_direction(position, delta, light.target,
                                                       dot(light.target.geometric_normal, -delta));
                     } else {
-                        cd = light.endpoint - position;
+                        cd = unbounded ? light.direction : light.endpoint - position;
                     }
-                    if (!connection_begin(position, cd, kOneMinusEps, path.current_medium, c)) {
+                    if (!connection_begin(position, cd, unbounded ? finf() : kOneMinusEps, path.current_medium, c)) {
                         path.status = S_ARITHMETIC;
                         return kEventFinished;
                     }
@@ -784,10 +802,14 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
         }
     }
     if (miss) {
-        // escape (:421-433): a constant environment has no light-sampling density
+        // escape (:421-433): MIS against the environment image's light samples (a constant
+        // environment has no light-sampling density)
+        const float Le = s.img.env_image != kNone ? environment_image_radiance(s.img, path.d, path.wavelength)
+                                                  : environment_radiance(s, path.wavelength);
         if (s.model == kModelPbrt && path.scatterings != 0u && !path.previous_delta)
-            path.escape_weight = power_weight(path.previous_bsdf_pdf, 0.0f);
-        path.radiance += path.throughput * path.escape_weight * environment_radiance(s, path.wavelength);
+            path.escape_weight = power_weight(path.previous_bsdf_pdf,
+                                              scalar_environment_pdf(s, path.prev_p, path.prev_n, path.d));
+        path.radiance += path.throughput * path.escape_weight * Le;
         return kEventFinished;
     }
     const u32 bounce = path.scatterings;
@@ -1020,11 +1042,12 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
                 const V3 origin = directional_offset ? spawn_toward(path.o, path.d, hit.t, point, light.direction)
                                                      : area_reference;
                 V3 cd;
+                const bool unbounded = light.kind == kIncidentEnvironment;
                 if (light.kind == kIncidentArea) {
                     const V3 delta = light.target.position - origin;
                     cd = shadow_segment_direction(origin, delta, light.target, dot(light.target.geometric_normal, -delta));
                 } else {
-                    cd = light.endpoint - origin;
+                    cd = unbounded ? light.direction : light.endpoint - origin;
                 }
                 if (!isfinite(factor) || !finite3(cd) || !(dot(cd, light.direction) > 0)) {
                     path.status = S_ARITHMETIC;
@@ -1032,14 +1055,14 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
                 }
                 const u32 medium = outgoing_medium(instance, path.current_medium, point.geometric_normal, light.direction);
                 if (s.media_enabled) {
-                    if (!connection_begin(origin, cd, kOneMinusEps, medium, c)) {
+                    if (!connection_begin(origin, cd, unbounded ? finf() : kOneMinusEps, medium, c)) {
                         path.status = S_ARITHMETIC;
                         return kEventFinished;
                     }
                 } else {
                     c.o = origin;
                     c.d = cd;
-                    c.remaining = kOneMinusEps;
+                    c.remaining = unbounded ? finf() : kOneMinusEps;
                     c.vacuum = true;
                 }
                 c.medium_sample = false;

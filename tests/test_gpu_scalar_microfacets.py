@@ -4,8 +4,9 @@
   1e-3 and the same scattering count for at least 97% of lanes (sin / cos / sqrt round
   differently on the device, so a few paths take another branch) on the Cornell-style box
   with a rough anisotropic conductor, rough glass and a mirror (Sobol, Halton, independent),
-  the box with smooth dispersive glass, the fog-filled box with a rough glass box, and the demo
-  scene with metal and glass boxes.
+  the box with smooth dispersive glass, the fog-filled box with a rough glass box, the demo
+  scene with metal and glass boxes, and, under an environment image (light samples from its
+  importance table, MIS on escape), the Cornell-style box and the fog-filled box.
 * The device film's per-pixel XYZ within 3 sigma of the oracle's on independent seeds.
 * The demo model's mirror floor reflects F(1) of the sky on every path.
 * The QMC samplers' depth limits of rypath (sampler_max_depth, src/sampling.cpp:129-135):
@@ -45,7 +46,7 @@ def cauchy(width, height, spp):
 
 CASES = [("microfacets", abi.SAMPLER_SOBOL), ("microfacets", abi.SAMPLER_HALTON),
          ("microfacets", abi.SAMPLER_INDEPENDENT), ("cauchy", abi.SAMPLER_SOBOL), ("fog_glass", abi.SAMPLER_SOBOL),
-         ("demo", abi.SAMPLER_INDEPENDENT)]
+         ("demo", abi.SAMPLER_INDEPENDENT), ("env_image", abi.SAMPLER_SOBOL), ("fog_env", abi.SAMPLER_SOBOL)]
 
 
 def make(name, width, height, spp):
@@ -55,6 +56,14 @@ def make(name, width, height, spp):
         return cauchy(width, height, spp)
     if name == "fog_glass":
         return fog_glass(width, height, spp)
+    if name == "env_image":
+        scene = scenes.cornell_features("env_image", width, height, spp)
+        scene.transport = abi.TRANSPORT_SCALAR
+        return scene
+    if name == "fog_env":
+        from test_scalar_environment import fog_under_sky
+
+        return fog_under_sky(width, height, spp)
     return scenes.demo_microfacets(width, height, spp)
 
 
