@@ -173,6 +173,9 @@ struct SurfacePoint {
     float world_extent = 0;
     bool curved = false; // a patch or analytic point
 };
+// The reflectance of a material at one wavelength (shaders/packet_walk.h:22-57); `image` is the
+// hit's filtered, scaled linear RGB for image reflectance
+bool reflectance(const Scene &s, const Material &m, float w, const Rgb *image, float &rho);
 // surface_point (shaders/render.metal:1120-1132) of flattened primitive `prim` at a native hit
 bool hit_surface_point(const Scene &s, u32 prim, u32 instance, u32 local, float b1, float b2, SurfacePoint &p);
 // The ray's point at t and its rounding bound (shaders/render.metal:1913-1929)

@@ -40,7 +40,7 @@ static F3 offset(const Vertex &v, F3 direction) {
 
 // shaders/packet_walk.h:22-57 (packet_reflectance) for sampled/constant/blackbody/image; image:
 // the hit's filtered, scaled linear RGB
-static bool reflectance(const Scene &s, const Material &m, float w, const Rgb *image, float &rho) {
+bool reflectance(const Scene &s, const Material &m, float w, const Rgb *image, float &rho) {
     if (m.scattering != 0) {
         rho = 1;
     } else if (m.kind == RP_REFLECTANCE_IMAGE && image && m.image_texture < s.images.textures.size()) {

@@ -667,6 +667,23 @@ bool scalar_event(const Ctx &c, Lane &l) {
         rho = surface.scalar_value;
     } else if (surface.kind == RP_REFLECTANCE_BLACKBODY) {
         rho = blackbody_reflectance(surface.scalar_value, l.wavelength);
+    } else if (surface.kind == RP_REFLECTANCE_RGB) {
+        reflectance(s, surface, l.wavelength, nullptr, rho); // sigmoid_reflectance; range checked below
+    } else if (surface.kind == RP_REFLECTANCE_IMAGE && surface.image_texture < s.images.textures.size()) {
+        // image_reflectance (shaders/render.metal:1154-1240) at the hit's footprint
+        if (!point_ready && !hit_surface_point(s, hit.prim, inst, local, hit.b1, hit.b2, point))
+            return fail(RP_SAMPLE_INVALID_ARITHMETIC);
+        point_ready = true;
+        F2 uvst, dstdx, dstdy;
+        if (!texture_context(s, c.p, l.sample, inst, local, hit.b1, hit.b2, point.geometric_normal, l.d, l.scatterings,
+                             uvst, dstdx, dstdy))
+            return fail(RP_SAMPLE_INVALID_ARITHMETIC);
+        const rp_image_texture &t = s.images.textures[surface.image_texture];
+        Rgb rgb = image_lookup(s.images, t, uvst, dstdx, dstdy, false, false);
+        rgb = {rgb.r * t.scale, rgb.g * t.scale, rgb.b * t.scale};
+        if (t.invert)
+            rgb = {1 - rgb.r, 1 - rgb.g, 1 - rgb.b};
+        rho = srgb_spectrum(s.images.rgb_table.data(), rgb, l.wavelength);
     } else {
         return fail(RP_SAMPLE_INVALID_HIT);
     }

@@ -1944,10 +1944,6 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
             throw Invalid{mix};
         if (const std::string images = validate_images(d); !images.empty())
             throw Invalid{images};
-        if (scalar)
-            for (u32 i = 0; i < d->material_count; ++i)
-                if (d->materials[i].kind == RP_REFLECTANCE_IMAGE)
-                    throw NotBuilt{"the scalar transport reads the environment image, not image reflectance"};
         if (d->model > RP_MODEL_DEMO)
             throw Invalid{"invalid scene model"};
         if (d->model == RP_MODEL_DEMO) {
@@ -2213,6 +2209,7 @@ rp_status rp_cuda_scene_create(const rp_scene_desc *d, int device, rp_scene **ou
         for (u32 i = 0; i < d->material_count; ++i)
             if (d->materials[i].kind == RP_REFLECTANCE_IMAGE && d->materials[i].scattering == RP_DIFFUSE)
                 ds.img.textured = 1;
+        s->scalar_full = s->scalar_full || ds.img.textured;
         // scene sphere (src/metal_render.mm:213-276) over the world vertices of k_tri_prepare
         int bounds[12];
         const auto t_wait = std::chrono::steady_clock::now();
@@ -2551,6 +2548,7 @@ rp_status rp_cuda_sample_scalar(rp_scene *s, const rp_request *request, rp_scala
             throw Invalid{err};
         if (s->transport != RP_TRANSPORT_SCALAR)
             throw Invalid{"the scene was built for the hero transport; sample it with rp_cuda_sample"};
+        apply_texture_request(s, *request);
         const WaveParams p = wave_params(*request);
         if (capacity < p.lanes)
             throw Invalid{"output capacity is smaller than the request lanes"};

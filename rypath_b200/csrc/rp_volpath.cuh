@@ -684,8 +684,8 @@ RP_DEV bool scalar_surface_point(const DeviceScene &s, u32 prim, u32 inst, u32 l
         return hit_surface_point(s, prim, inst, local, b1, b2, point);
     return triangle_surface_point(s, inst, local, b1, b2, true, point);
 }
-// Full: the scene has conductor or dielectric surfaces or procedural primitives (their code is
-// compiled out of the plain step kernel).
+// Full: the scene has conductor or dielectric surfaces, procedural primitives or image
+// reflectance (their code is compiled out of the plain step kernel).
 template <bool Full>
 RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarParams &q, ScalarPath &path, bool ok,
                        const Hit &hit, Connection &c) {
@@ -915,6 +915,23 @@ RP_DEV int shade_event(const DeviceScene &s, const WaveParams &p, const ScalarPa
         rho = surface.scalar_value;
     } else if (surface.kind == 4) {
         rho = blackbody_reflectance(surface.scalar_value, path.wavelength);
+    } else if (surface.kind == 2) {
+        rho = sigmoid_reflectance(surface.coefficients, path.wavelength);
+    } else if (Full && surface.kind == 3 && s.img.textured && surface.image_texture < s.img.texture_count) {
+        // image_reflectance (shaders/render.metal:1154-1240) at the hit's footprint
+        if (!point_ready && !scalar_surface_point<Full>(s, hit.prim, inst, local, hit.b1, hit.b2, point)) {
+            path.status = S_ARITHMETIC;
+            return kEventFinished;
+        }
+        point_ready = true;
+        F2 st, dstdx, dstdy;
+        if (!texture_context(s, p, path.pixel, path.slo, path.shi, inst, local, hit.b1, hit.b2, point.geometric_normal,
+                             path.d, path.scatterings, st, dstdx, dstdy)) {
+            path.status = S_ARITHMETIC;
+            return kEventFinished;
+        }
+        rho = rgb_spectrum(s.img.rgb_table, image_reflectance_rgb(s.img, surface.image_texture, st, dstdx, dstdy),
+                           path.wavelength);
     } else {
         path.status = S_HIT;
         return kEventFinished;

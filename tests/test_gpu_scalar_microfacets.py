@@ -6,7 +6,8 @@
   with a rough anisotropic conductor, rough glass and a mirror (Sobol, Halton, independent),
   the box with smooth dispersive glass, the fog-filled box with a rough glass box, the demo
   scene with metal and glass boxes, and, under an environment image (light samples from its
-  importance table, MIS on escape), the Cornell-style box and the fog-filled box.
+  importance table, MIS on escape), the Cornell-style box and the fog-filled box, and the
+  textured box (image reflectance at the hit's footprint).
 * The device film's per-pixel XYZ within 3 sigma of the oracle's on independent seeds.
 * The demo model's mirror floor reflects F(1) of the sky on every path.
 * The QMC samplers' depth limits of rypath (sampler_max_depth, src/sampling.cpp:129-135):
@@ -46,7 +47,8 @@ def cauchy(width, height, spp):
 
 CASES = [("microfacets", abi.SAMPLER_SOBOL), ("microfacets", abi.SAMPLER_HALTON),
          ("microfacets", abi.SAMPLER_INDEPENDENT), ("cauchy", abi.SAMPLER_SOBOL), ("fog_glass", abi.SAMPLER_SOBOL),
-         ("demo", abi.SAMPLER_INDEPENDENT), ("env_image", abi.SAMPLER_SOBOL), ("fog_env", abi.SAMPLER_SOBOL)]
+         ("demo", abi.SAMPLER_INDEPENDENT), ("env_image", abi.SAMPLER_SOBOL), ("fog_env", abi.SAMPLER_SOBOL),
+         ("texture", abi.SAMPLER_SOBOL)]
 
 
 def make(name, width, height, spp):
@@ -56,8 +58,8 @@ def make(name, width, height, spp):
         return cauchy(width, height, spp)
     if name == "fog_glass":
         return fog_glass(width, height, spp)
-    if name == "env_image":
-        scene = scenes.cornell_features("env_image", width, height, spp)
+    if name in ("env_image", "texture"):
+        scene = scenes.cornell_features(name, width, height, spp)
         scene.transport = abi.TRANSPORT_SCALAR
         return scene
     if name == "fog_env":
