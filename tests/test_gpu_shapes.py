@@ -158,3 +158,30 @@ def test_shape_validation():
     wide = scenes.shape_furnace("patch")
     wide.instances[0].patch_count = 5
     assert renderer.build_renderer(wide).status == abi.RP_INVALID_ARGUMENT
+
+
+@pytest.mark.parametrize("transport", [abi.TRANSPORT_HERO, abi.TRANSPORT_SCALAR])
+def test_shape_film_statistics_agree_with_the_oracle(transport):
+    """Per-pixel XYZ of the device film of the shapes box within 3 sigma of the oracle's film on
+    independent seeds."""
+    from oracle_lib import oracle_film
+
+    scene = scenes.cornell_shapes(16, 16, 64, transport=transport)
+    rs = build(scene)
+    st, diag, film = rs.render_film(renderer.RenderSettings(16, 16, samples=512, batch_size=128, seed=5,
+                                                            sampler=abi.SAMPLER_INDEPENDENT))
+    rs.close()
+    assert st == abi.RP_SUCCESS, diag
+    host = oracle_film(scene, 16, 16, 512, seed=6, sampler=abi.SAMPLER_INDEPENDENT,
+                       scalar=transport == abi.TRANSPORT_SCALAR, chunk=128)
+
+    def moments(f):
+        n = f["count"][:, None].astype(np.float64)
+        mean = (f["sum"] + f["correction"]) / n
+        return mean, np.maximum(f["square"] / n - mean ** 2, 0) / n
+
+    m1, v1 = moments(film)
+    m2, v2 = moments(host)
+    z = np.abs(m1 - m2) / np.sqrt(v1 + v2 + 1e-30)
+    assert np.mean(z < 3) > 0.97, np.mean(z < 3)
+    assert abs(m1.sum() / m2.sum() - 1) < 0.03
