@@ -1384,8 +1384,8 @@ void launch_shadow(const rp_scene *s, const PathPool &pool, unsigned grid, size_
 // Each reads only its own bin and appends to the path and shadow queues with atomics, so the
 // queue order may differ from a serial launch but no path's result does (every later kernel
 // reads a path by its id, and the film reduces by lane).
-template <bool Adjoint>
-void launch_shade(rp_scene *s, const WaveParams &p, const PathPool &pool, int in, unsigned grid, size_t smem) {
+template <bool Adjoint, bool Img>
+void launch_shade_img(rp_scene *s, const WaveParams &p, const PathPool &pool, int in, unsigned grid, size_t smem) {
     RP_CHECK(cudaEventRecord(s->forked, s->stream));
     for (int k = 0; k < 3; ++k)
         RP_CHECK(cudaStreamWaitEvent(s->family[k], s->forked, 0));
@@ -1397,31 +1397,42 @@ void launch_shade(rp_scene *s, const WaveParams &p, const PathPool &pool, int in
         on[1] = on[2] = on[3] = s->stream;
     if (timed)
         s->mark_family(0, on[0]);
-    k_shade<0, 128, Adjoint><<<grid, 128, smem, on[0]>>>(s->ds, p, pool, in);
-    k_nee<0><<<grid, 128, 0, on[0]>>>(s->ds, p, pool);
+    k_shade<0, 128, Adjoint, Img><<<grid, 128, smem, on[0]>>>(s->ds, p, pool, in);
+    k_nee<0, 128, Img><<<grid, 128, 0, on[0]>>>(s->ds, p, pool);
     if (timed) {
         s->done_family(on[0]);
         s->mark_family(1, on[1]);
     }
-    k_shade<1, 128, Adjoint><<<grid, 128, smem, on[1]>>>(s->ds, p, pool, in);
-    k_nee<1><<<grid, 128, 0, on[1]>>>(s->ds, p, pool);
+    k_shade<1, 128, Adjoint, Img><<<grid, 128, smem, on[1]>>>(s->ds, p, pool, in);
+    k_nee<1, 128, Img><<<grid, 128, 0, on[1]>>>(s->ds, p, pool);
     if (timed) {
         s->done_family(on[1]);
         s->mark_family(2, on[2]);
     }
-    k_shade<2, 128, Adjoint><<<grid, 128, smem, on[2]>>>(s->ds, p, pool, in);
-    k_nee<2><<<grid, 128, 0, on[2]>>>(s->ds, p, pool);
+    k_shade<2, 128, Adjoint, Img><<<grid, 128, smem, on[2]>>>(s->ds, p, pool, in);
+    k_nee<2, 128, Img><<<grid, 128, 0, on[2]>>>(s->ds, p, pool);
     if (timed) {
         s->done_family(on[2]);
         s->mark_family(3, on[3]);
     }
-    k_shade<3, 128, Adjoint><<<grid, 128, smem, on[3]>>>(s->ds, p, pool, in);
+    k_shade<3, 128, Adjoint, Img><<<grid, 128, smem, on[3]>>>(s->ds, p, pool, in);
     if (timed)
         s->done_family(on[3]);
     for (int k = 0; k < 3; ++k) {
         RP_CHECK(cudaEventRecord(s->family_done[k], s->family[k]));
         RP_CHECK(cudaStreamWaitEvent(s->stream, s->family_done[k], 0));
     }
+}
+// The plain shade kernels for scenes without images (the adjoint keeps the full ones).
+template <bool Adjoint>
+void launch_shade(rp_scene *s, const WaveParams &p, const PathPool &pool, int in, unsigned grid, size_t smem) {
+    if constexpr (!Adjoint) {
+        if (!s->ds.img.textured && s->ds.img.env_image == kNone) {
+            launch_shade_img<false, false>(s, p, pool, in, grid, smem);
+            return;
+        }
+    }
+    launch_shade_img<Adjoint, true>(s, p, pool, in, grid, smem);
 }
 
 // Sobol sampler with Owen randomisation: attaches the table of the first kOwenPrefixBits

@@ -197,7 +197,9 @@ __global__ void __launch_bounds__(Block, Stack <= kShortStack ? 1024 / Block : 1
 // four 128-thread blocks fit an SM; the escape kernel (F = 3) fits without spilling, the
 // other families spill about 500 bytes to L1 and still run a little faster than three blocks
 // at 168 registers (113.5 against 115.0 ms per 1080p 16-spp frame of the mixed scene).
-template <int F, int Block = 128, bool Adjoint = false>
+// Img: the scene has image reflectance or an environment image (their code is compiled out of
+// the plain kernels).
+template <int F, int Block = 128, bool Adjoint = false, bool Img = true>
 __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_constant__ DeviceScene s,
                                                               const __grid_constant__ WaveParams p, PathPool pool, int in) {
     extern __shared__ float sgrad[]; // adjoint only
@@ -309,7 +311,7 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_const
                         RgbPolynomial image_rgb;
                         bool image = false;
                         if constexpr (F == 0) {
-                            if (s.img.textured && material.kind == 3 && material.image_texture < s.img.texture_count) {
+                            if (Img && s.img.textured && material.kind == 3 && material.image_texture < s.img.texture_count) {
                                 F2 st, dstdx, dstdy;
                                 if (!texture_context(s, p, ident.x, ident.y, ident.z, cinst, clocal, b1, b2,
                                                      cp.geometric_normal, rd, cnt - 1, st, dstdx, dstdy)) {
@@ -415,7 +417,7 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_const
                     V4 rad = v4(0);
                     bool emission_ok = true;
                     if (ctype == kEnvironment) {
-                        if (s.img.env_image != kNone) {
+                        if (Img && s.img.env_image != kNone) {
                             rad = environment_image_radiance4(s.img, rd, lambda);
                         } else if (s.environment != kNone) {
 #pragma unroll
@@ -458,7 +460,7 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_const
                             if (ctype == kEnvironment) {
                                 // the constant environment has no unidirectional proposal;
                                 // the image's is its compensated table
-                                lpdf = s.img.env_image != kNone ? environment_image_pdf(s.img, rd, true) * selection
+                                lpdf = (Img && s.img.env_image != kNone) ? environment_image_pdf(s.img, rd, true) * selection
                                                                 : 0.0f * selection;
                             } else {
                                 const V3 dl = cp.position - latest.position;
@@ -564,7 +566,7 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_shade(const __grid_const
 // queued for the shadow kernel.  Its own failures (invalid arithmetic) fail the path.  Split
 // from the shade kernel, which leaves the request (write_nee_request), so that each kernel
 // holds half the live state.
-template <int F, int Block = 128>
+template <int F, int Block = 128, bool Img = true>
 __global__ void __launch_bounds__(Block, 512 / Block) k_nee(const __grid_constant__ DeviceScene s,
                                                             const __grid_constant__ WaveParams p, PathPool pool) {
     const u32 count = pool.counters[8 + F];
@@ -604,7 +606,7 @@ __global__ void __launch_bounds__(Block, 512 / Block) k_nee(const __grid_constan
                         // sample_li (shaders/packet_transport.h:470-553)
                         const Selected choice = light_sample(s, cp.position, cp.shading_normal, u0);
                         float u1 = 0, u2 = 0;
-                        const bool env_image = s.img.env_image != kNone && choice.light == s.environment_light;
+                        const bool env_image = Img && s.img.env_image != kNone && choice.light == s.environment_light;
                         if (choice.pmf > 0 && (choice.light < s.emitter_count || env_image)) {
                             const uint4 w = draw_words(s, p, ident.x, ident.y, ident.z, index, block);
                             u1 = sample_uniform(p, w.y);
